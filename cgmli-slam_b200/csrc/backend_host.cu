@@ -1,0 +1,614 @@
+// Host runtime of the B200 backend solver: topology preprocessing, device
+// buffers, the launch sequence and the C ABI of include/cgmli_backend.h.
+//
+// The reference rebuilds CSR rows, columns and per-point support sets on the
+// host for every new topology (VisualCudaBatch.cu:450-490) and ping-pongs
+// the host every LM iteration (:595-597).  Here the topology is built once per
+// set of windows (support sets, tiles of <= 32 observations, slabs of tiles)
+// and the whole LM loop runs on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cgmli_backend.h"
+#include "backend_internal.h"
+
+namespace cgmli {
+size_t linearizeSmemBytes(int maxNpc, int stageStride);
+size_t factorSmemBytes(int maxNr);
+cudaError_t configureKernels(size_t linSmem, size_t facSmem);
+int launchIteration(const DevBatch& B, const int2* tiles, const int* slabTile0, int stageStride, size_t linSmem, size_t facSmem,
+                    int refinement, int maxIterations, int probe, double* Sdebug, cudaStream_t s);
+int launchLmInit(const DevBatch& B, double lambda0, cudaStream_t s);
+}  // namespace cgmli
+
+using namespace cgmli;
+
+namespace {
+thread_local std::string g_error = "ok";
+
+int fail(int code, const std::string& msg) {
+    g_error = msg;
+    return code;
+}
+int cudaFail(cudaError_t e, const char* what) {
+    g_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return CGMLI_E_CUDA;
+}
+#define CK(call)                                                 \
+    do {                                                         \
+        cudaError_t e_ = (call);                                 \
+        if (e_ != cudaSuccess) return cudaFail(e_, #call);      \
+    } while (0)
+
+// Grow-only device array (src/common/CudaArray.hpp:10-39 keeps the same policy).
+template <class T>
+struct DArray {
+    T* p = nullptr;
+    size_t cap = 0;
+    cudaError_t reserve(size_t n) {
+        if (n <= cap) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        const cudaError_t e = cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T));
+        if (e == cudaSuccess) cap = n;
+        return e;
+    }
+    cudaError_t upload(const std::vector<T>& v, cudaStream_t s) {
+        cudaError_t e = reserve(v.size());
+        if (e != cudaSuccess || v.empty()) return e;
+        return cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+    }
+    void release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
+};
+}  // namespace
+
+struct cgmli_solver {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cgmli_solver_options opt{};
+    // topology (host copies)
+    std::vector<WinDesc> win;
+    std::vector<Slab> slabs;
+    std::vector<int2> tiles;
+    std::vector<int> slabTile0;
+    int stageStride = 0, maxNpc = 0, maxNr = 0;
+    size_t linSmem = 0, facSmem = 0;
+    int totalKf = 0, totalExt = 0, totalCam = 0, totalLm = 0, totalObs = 0, totalImu = 0;
+    // device arrays
+    DArray<WinDesc> dWin;
+    DArray<WinLM> dLm;
+    DArray<Slab> dSlabs;
+    DArray<int2> dTiles;
+    DArray<int> dSlabTile0;
+    DArray<double> camR, camT;
+    DArray<int> camExt;
+    DArray<int> lmWin, lmKf, lmCam, lmObsBegin, lmNs, lmSupp0, supp;
+    DArray<long long> lmC0;
+    DArray<double> lmBearing, lmVel, lmTime, lmC, lmD, lmG, lmCost, lmDelta, lmPred, lmTrial, lmMaxInc;
+    DArray<int> lmValid, lmTrialValid;
+    DArray<int> obKf, obKfl, obCam, obSlot;
+    DArray<double> obBearing, obP, obVel, obTime;
+    DArray<double> pose[2], sb[2], ext[2], td[2], rho[2];
+    DArray<double> imu;
+    DArray<int> imuKf;
+    DArray<int> priorKind, priorIndex, priorCol, priorOff;
+    DArray<double> priorA, priorR0, priorRef;
+    DArray<double> Hret, gret, costRet, trialRet, acc, dr, rhs, Sglob, imuScratch, priorScratch, predState, out, Sdebug;
+    DArray<int> retValid, solveStatus;
+    DevBatch B{};
+    double lastMs = 0;
+    int lastLaunches = 0;
+
+    ~cgmli_solver() {
+        if (stream) cudaStreamSynchronize(stream);
+        DArray<double>* dbl[] = {&camR, &camT, &lmBearing, &lmVel, &lmTime, &lmC, &lmD, &lmG, &lmCost, &lmDelta, &lmPred, &lmTrial,
+                                 &lmMaxInc, &obBearing, &obP, &obVel, &obTime, &pose[0], &pose[1], &sb[0], &sb[1], &ext[0], &ext[1],
+                                 &td[0], &td[1], &rho[0], &rho[1], &imu, &priorA, &priorR0, &priorRef, &Hret, &gret, &costRet,
+                                 &trialRet, &acc, &dr, &rhs, &Sglob, &imuScratch, &priorScratch, &predState, &out, &Sdebug};
+        for (auto* a : dbl) a->release();
+        DArray<int>* ints[] = {&camExt, &lmWin, &lmKf, &lmCam, &lmObsBegin, &lmNs, &lmSupp0, &supp, &lmValid, &lmTrialValid, &obKf,
+                               &obKfl, &obCam, &obSlot, &imuKf, &priorKind, &priorIndex, &priorCol, &priorOff, &retValid,
+                               &solveStatus, &dSlabTile0};
+        for (auto* a : ints) a->release();
+        lmC0.release(); dWin.release(); dLm.release(); dSlabs.release(); dTiles.release();
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+int tangentOf(int kind) { return kind == CGMLI_PRIOR_SPEED_BIAS ? 9 : kind == CGMLI_PRIOR_TIME_OFFSET ? 1 : 6; }
+int ambientOf(int kind) { return kind == CGMLI_PRIOR_SPEED_BIAS ? 9 : kind == CGMLI_PRIOR_TIME_OFFSET ? 1 : 7; }
+
+int validateWindow(const cgmli_window& w, int index) {
+    char buf[256];
+    auto bad = [&](const char* what) {
+        std::snprintf(buf, sizeof buf, "window %d: %s", index, what);
+        return fail(CGMLI_E_INVALID, buf);
+    };
+    if (w.num_keyframes < 1 || w.num_cameras < 1 || w.num_extrinsics < 1 || w.num_landmarks < 0 || w.num_observations < 0 ||
+        w.num_imu < 0 || w.prior_rank < 0)
+        return bad("negative or empty sizes");
+    if (!w.poses || !w.speed_bias || !w.extrinsics || (w.num_landmarks && !w.rho) || !w.cam_R || !w.cam_t || !w.cam_ext)
+        return bad("missing state or rig arrays");
+    if (w.num_landmarks && (!w.lm_anchor_kf || !w.lm_anchor_cam || !w.lm_obs_begin || !w.lm_anchor_bearing))
+        return bad("missing landmark arrays");
+    if (w.num_observations && (!w.obs_kf || !w.obs_cam || !w.obs_bearing || !w.obs_P)) return bad("missing observation arrays");
+    if (w.num_imu && (!w.imu || !w.imu_kf)) return bad("missing IMU arrays");
+    if (w.estimate_td && !w.td) return bad("estimate_td requires a td value");
+    for (int c = 0; c < w.num_cameras; ++c)
+        if (w.cam_ext[c] < 0 || w.cam_ext[c] >= w.num_extrinsics) return bad("camera extrinsic index out of range");
+    if (w.num_landmarks && (w.lm_obs_begin[0] != 0 || w.lm_obs_begin[w.num_landmarks] != w.num_observations))
+        return bad("landmark observation ranges do not cover the observations");
+    for (int l = 0; l < w.num_landmarks; ++l) {
+        if (w.lm_obs_begin[l + 1] < w.lm_obs_begin[l]) return bad("landmark observation ranges not sorted");
+        if (w.lm_obs_begin[l + 1] - w.lm_obs_begin[l] > kMaxTrackChunk) return bad("more than 32 observations of one landmark");
+        if (w.lm_anchor_kf[l] < 0 || w.lm_anchor_kf[l] >= w.num_keyframes) return bad("anchor keyframe out of range");
+        if (w.lm_anchor_cam[l] < 0 || w.lm_anchor_cam[l] >= w.num_cameras) return bad("anchor camera out of range");
+    }
+    for (int f = 0; f < w.num_observations; ++f) {
+        if (w.obs_kf[f] < 0 || w.obs_kf[f] >= w.num_keyframes) return bad("observer keyframe out of range");
+        if (w.obs_cam[f] < 0 || w.obs_cam[f] >= w.num_cameras) return bad("observer camera out of range");
+    }
+    for (int i = 0; i < w.num_imu; ++i)
+        if (w.imu_kf[i] < 0 || w.imu_kf[i] + 1 >= w.num_keyframes) return bad("IMU keyframe out of range");
+    if (w.prior_rank > 0) {
+        if (!w.prior_block_kind || !w.prior_block_index || !w.prior_ref || !w.prior_A || !w.prior_r0 || w.prior_num_blocks < 1)
+            return bad("missing prior arrays");
+        for (int b = 0; b < w.prior_num_blocks; ++b) {
+            const int k = w.prior_block_kind[b], i = w.prior_block_index[b];
+            if (k < 0 || k > 3) return bad("prior block kind");
+            if ((k <= 1 && (i < 0 || i >= w.num_keyframes)) || (k == 2 && (i < 0 || i >= w.num_extrinsics)) || (k == 3 && !w.td))
+                return bad("prior block index");
+        }
+    }
+    const int ncal = (w.estimate_extrinsics ? 6 * w.num_extrinsics : 0) + (w.estimate_td ? 1 : 0);
+    if (6 * w.num_keyframes + ncal > 400) return fail(CGMLI_E_LIMIT, "window visual dimension above 400");
+    return CGMLI_OK;
+}
+}  // namespace
+
+extern "C" {
+
+const char* cgmli_last_error(void) { return g_error.c_str(); }
+
+void cgmli_default_options(cgmli_solver_options* o) {
+    o->precision = CGMLI_PRECISION_FP64;
+    o->refinement_steps = 0;
+    o->initial_lambda = 1e-4;
+    o->slabs_per_window = 0;
+    o->threads_per_block = 0;
+}
+
+int cgmli_solver_create(int device, const cgmli_solver_options* options, cgmli_solver** out) {
+    if (!out) return fail(CGMLI_E_INVALID, "null output handle");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) return fail(CGMLI_E_CUDA, "no CUDA device available");
+    if (device < 0 || device >= count) return fail(CGMLI_E_INVALID, "device index out of range");
+    CK(cudaSetDevice(device));
+    auto* s = new cgmli_solver();
+    s->device = device;
+    if (options) s->opt = *options; else cgmli_default_options(&s->opt);
+    if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreate(&s->ev0)) != cudaSuccess || (e = cudaEventCreate(&s->ev1)) != cudaSuccess) {
+        delete s;
+        return cudaFail(e, "stream/event creation");
+    }
+    *out = s;
+    return CGMLI_OK;
+}
+
+void cgmli_solver_destroy(cgmli_solver* s) { delete s; }
+
+int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int count) {
+    if (!S || !windows || count < 1) return fail(CGMLI_E_INVALID, "null solver or empty window list");
+    for (int i = 0; i < count; ++i) {
+        const int st = validateWindow(windows[i], i);
+        if (st != CGMLI_OK) return st;
+    }
+    CK(cudaSetDevice(S->device));
+    cudaStream_t st = S->stream;
+    S->win.assign(count, WinDesc{});
+    S->slabs.clear(); S->tiles.clear(); S->slabTile0.clear();
+    int kf = 0, ex = 0, cam = 0, lm = 0, ob = 0, im = 0, pblk = 0, vec = 0;
+    long long dense = 0, acc = 0, pA = 0, pR = 0, pRef = 0, imuS = 0, priS = 0, cOff = 0;
+    S->maxNpc = 0; S->maxNr = 0; S->stageStride = 0;
+    std::vector<double> camR, camT, lmBearing, lmVel, lmTime, obBearing, obP, obVel, obTime;
+    std::vector<int> camExt, lmWin, lmKf, lmCam, lmObsBegin, lmNs, lmSupp0, supp, obKf, obKfl, obCam, obSlot, imuKf;
+    std::vector<long long> lmC0;
+    std::vector<int> priorKind, priorIndex, priorCol, priorOff;
+    std::vector<double> priorA, priorR0, priorRef, imuData;
+    std::vector<double> pose, sbv, extv, tdv, rhov;
+    // total tiles first (slab sizing)
+    long long totalTiles = 0;
+    for (int i = 0; i < count; ++i) {
+        const auto& w = windows[i];
+        int acc32 = 0;
+        for (int l = 0; l < w.num_landmarks; ++l) {
+            const int n = w.lm_obs_begin[l + 1] - w.lm_obs_begin[l];
+            if (acc32 == 0 || acc32 + n > kMaxTrackChunk) { ++totalTiles; acc32 = 0; }
+            acc32 += n;
+        }
+    }
+    int tilesPerSlab = S->opt.slabs_per_window > 0 ? 0 : (int)std::min<long long>(64, std::max<long long>(1, (totalTiles + 295) / 296));
+    for (int i = 0; i < count; ++i) {
+        const auto& w = windows[i];
+        WinDesc& d = S->win[i];
+        d.K = w.num_keyframes; d.E = w.num_extrinsics; d.C = w.num_cameras; d.L = w.num_landmarks; d.F = w.num_observations;
+        d.nImu = w.num_imu;
+        d.estExt = w.estimate_extrinsics != 0; d.estTd = w.estimate_td != 0 && w.td; d.hasTd = w.td != nullptr;
+        d.ncalib = (d.estExt ? 6 * d.E : 0) + (d.estTd ? 1 : 0);
+        d.Npc = 6 * d.K + d.ncalib;
+        d.Nr = 15 * d.K + d.ncalib;
+        d.kf0 = kf; d.ext0 = ex; d.cam0 = cam; d.lm0 = lm; d.obs0 = ob; d.imu0 = im;
+        d.vec0 = vec; d.dense0 = dense; d.acc0 = acc;
+        d.huber = w.huber_scale; d.minInv = w.min_inverse_distance;
+        S->maxNpc = std::max(S->maxNpc, d.Npc);
+        S->maxNr = std::max(S->maxNr, d.Nr);
+        vec += d.Nr;
+        dense += (long long)d.Nr * d.Nr;
+        acc += (long long)d.Npc * (d.Npc + 1) / 2 + 3ll * d.Npc;
+        // states
+        pose.insert(pose.end(), w.poses, w.poses + 7 * d.K);
+        sbv.insert(sbv.end(), w.speed_bias, w.speed_bias + 9 * d.K);
+        extv.insert(extv.end(), w.extrinsics, w.extrinsics + 7 * d.E);
+        tdv.push_back(w.td ? *w.td : 0.0);
+        rhov.insert(rhov.end(), w.rho, w.rho + d.L);
+        // rig
+        camR.insert(camR.end(), w.cam_R, w.cam_R + 9 * d.C);
+        camT.insert(camT.end(), w.cam_t, w.cam_t + 3 * d.C);
+        for (int c = 0; c < d.C; ++c) camExt.push_back(ex + w.cam_ext[c]);
+        // landmarks, support sets and observations
+        int slabTiles = 0, tileObs = 0, tileStage = 0;
+        const int tps = S->opt.slabs_per_window > 0
+                            ? std::max(1, (int)((d.L + 1) / std::max(1, S->opt.slabs_per_window)))
+                            : tilesPerSlab;
+        auto closeTile = [&](int lEnd) {
+            if (!S->tiles.empty() && S->tiles.back().y < 0) S->tiles.back().y = lEnd;
+        };
+        for (int l = 0; l < d.L; ++l) {
+            const int b = w.lm_obs_begin[l], e = w.lm_obs_begin[l + 1];
+            const int a = w.lm_anchor_kf[l];
+            std::vector<int> kfs{a};
+            for (int f = b; f < e; ++f)
+                if (std::find(kfs.begin(), kfs.end(), w.obs_kf[f]) == kfs.end()) kfs.push_back(w.obs_kf[f]);
+            std::sort(kfs.begin() + 1, kfs.end());
+            if ((int)kfs.size() > kMaxSupport) return fail(CGMLI_E_LIMIT, "landmark support above 64 keyframes");
+            const int ns = 6 * (int)kfs.size() + d.ncalib;
+            // tile / slab bookkeeping (tiles never mix windows)
+            const int nobs = e - b;
+            if (l == 0 || tileObs + nobs > kMaxTrackChunk) {
+                closeTile(lm + l);
+                if (l == 0 || slabTiles >= (tps > 0 ? tps : 1)) {
+                    S->slabs.push_back(Slab{i, lm + l, 0, 0});
+                    S->slabTile0.push_back((int)S->tiles.size());
+                    slabTiles = 0;
+                }
+                S->tiles.push_back(make_int2(lm + l, -1));
+                ++slabTiles;
+                tileObs = 0;
+                tileStage = 0;
+            }
+            tileObs += nobs;
+            tileStage += ns;
+            S->stageStride = std::max(S->stageStride, tileStage);
+            lmWin.push_back(i);
+            lmKf.push_back(kf + a);
+            lmCam.push_back(cam + w.lm_anchor_cam[l]);
+            lmObsBegin.push_back(ob + b);
+            for (int k = 0; k < 3; ++k) lmBearing.push_back(w.lm_anchor_bearing[3 * l + k]);
+            for (int k = 0; k < 3; ++k) lmVel.push_back(w.lm_anchor_velocity ? w.lm_anchor_velocity[3 * l + k] : 0.0);
+            lmTime.push_back(w.lm_anchor_time ? w.lm_anchor_time[l] : 0.0);
+            lmNs.push_back((int)kfs.size());
+            lmSupp0.push_back((int)supp.size());
+            supp.insert(supp.end(), kfs.begin(), kfs.end());
+            lmC0.push_back(cOff);
+            cOff += ns;
+            for (int f = b; f < e; ++f) {
+                obKf.push_back(kf + w.obs_kf[f]);
+                obKfl.push_back(w.obs_kf[f]);
+                obCam.push_back(cam + w.obs_cam[f]);
+                obSlot.push_back((int)(std::find(kfs.begin(), kfs.end(), w.obs_kf[f]) - kfs.begin()));
+                for (int k = 0; k < 3; ++k) obBearing.push_back(w.obs_bearing[3 * f + k]);
+                for (int k = 0; k < 6; ++k) obP.push_back(w.obs_P[6 * f + k]);
+                for (int k = 0; k < 3; ++k) obVel.push_back(w.obs_velocity ? w.obs_velocity[3 * f + k] : 0.0);
+                obTime.push_back(w.obs_time ? w.obs_time[f] : 0.0);
+            }
+        }
+        closeTile(lm + d.L);
+        d.slab0 = 0;
+        // IMU
+        for (int q = 0; q < d.nImu; ++q) {
+            const double* raw = reinterpret_cast<const double*>(&w.imu[q]);
+            imuData.insert(imuData.end(), raw, raw + sizeof(cgmli_frozen_imu) / sizeof(double));
+            imuKf.push_back(kf + w.imu_kf[q]);
+        }
+        d.imuScratch0 = imuS;
+        imuS += 465ll * d.nImu;
+        // prior
+        d.priorRank = w.prior_rank;
+        d.priorBlk0 = pblk;
+        d.priorBlocks = w.prior_rank > 0 ? w.prior_num_blocks : 0;
+        int cols = 0, amb = 0;
+        for (int b2 = 0; b2 < d.priorBlocks; ++b2) {
+            const int kind = w.prior_block_kind[b2], idx = w.prior_block_index[b2];
+            priorKind.push_back(kind);
+            int gidx = idx, col = -1;
+            if (kind == CGMLI_PRIOR_POSE) { gidx = kf + idx; col = 15 * idx; }
+            else if (kind == CGMLI_PRIOR_SPEED_BIAS) { gidx = kf + idx; col = 15 * idx + 6; }
+            else if (kind == CGMLI_PRIOR_EXTRINSIC) { gidx = ex + idx; col = d.estExt ? 15 * d.K + 6 * idx : -1; }
+            else { gidx = i; col = d.estTd ? 15 * d.K + (d.estExt ? 6 * d.E : 0) : -1; }
+            priorIndex.push_back(gidx);
+            priorCol.push_back(col);
+            priorOff.push_back(cols);
+            cols += tangentOf(kind);
+            amb += ambientOf(kind);
+        }
+        d.priorCols = cols;
+        d.priorA0 = pA; d.priorR00 = pR; d.priorRef0 = pRef;
+        if (d.priorRank > 0) {
+            priorA.insert(priorA.end(), w.prior_A, w.prior_A + (long long)d.priorRank * cols);
+            priorR0.insert(priorR0.end(), w.prior_r0, w.prior_r0 + d.priorRank);
+            priorRef.insert(priorRef.end(), w.prior_ref, w.prior_ref + amb);
+        }
+        pA += (long long)d.priorRank * cols;
+        pR += d.priorRank;
+        pRef += d.priorRank > 0 ? amb : 0;
+        pblk += d.priorBlocks;
+        d.priorScratch0 = priS;
+        priS += d.priorRank > 0 ? (long long)cols * 7 + d.priorRank + (long long)d.priorRank * cols : 0;
+        kf += d.K; ex += d.E; cam += d.C; lm += d.L; ob += d.F; im += d.nImu;
+    }
+    for (size_t t = 0; t < S->slabs.size(); ++t) {
+        const int e = t + 1 < S->slabs.size() ? S->slabTile0[t + 1] : (int)S->tiles.size();
+        S->slabs[t].lmEnd = S->tiles[e - 1].y;
+    }
+    S->slabTile0.push_back((int)S->tiles.size());
+    lmObsBegin.push_back(ob);
+    S->totalKf = kf; S->totalExt = ex; S->totalCam = cam; S->totalLm = lm; S->totalObs = ob; S->totalImu = im;
+    S->stageStride = std::max(8, S->stageStride);
+    S->linSmem = linearizeSmemBytes(S->maxNpc, S->stageStride);
+    S->facSmem = factorSmemBytes(S->maxNr);
+    if (S->linSmem > 227 * 1024) return fail(CGMLI_E_LIMIT, "visual accumulator exceeds shared memory");
+    CK(configureKernels(S->linSmem, S->facSmem));
+    // uploads
+    CK(S->dWin.upload(S->win, st));
+    CK(S->dLm.reserve(count));
+    CK(S->dSlabs.upload(S->slabs, st));
+    CK(S->dTiles.upload(S->tiles, st));
+    CK(S->dSlabTile0.upload(S->slabTile0, st));
+    CK(S->camR.upload(camR, st)); CK(S->camT.upload(camT, st)); CK(S->camExt.upload(camExt, st));
+    CK(S->lmWin.upload(lmWin, st)); CK(S->lmKf.upload(lmKf, st)); CK(S->lmCam.upload(lmCam, st));
+    CK(S->lmObsBegin.upload(lmObsBegin, st)); CK(S->lmNs.upload(lmNs, st)); CK(S->lmSupp0.upload(lmSupp0, st));
+    CK(S->supp.upload(supp, st)); CK(S->lmC0.upload(lmC0, st));
+    CK(S->lmBearing.upload(lmBearing, st)); CK(S->lmVel.upload(lmVel, st)); CK(S->lmTime.upload(lmTime, st));
+    CK(S->obKf.upload(obKf, st)); CK(S->obKfl.upload(obKfl, st)); CK(S->obCam.upload(obCam, st)); CK(S->obSlot.upload(obSlot, st));
+    CK(S->obBearing.upload(obBearing, st)); CK(S->obP.upload(obP, st)); CK(S->obVel.upload(obVel, st));
+    CK(S->obTime.upload(obTime, st));
+    CK(S->pose[0].upload(pose, st)); CK(S->sb[0].upload(sbv, st)); CK(S->ext[0].upload(extv, st));
+    CK(S->td[0].upload(tdv, st)); CK(S->rho[0].upload(rhov, st));
+    CK(S->pose[1].reserve(pose.size())); CK(S->sb[1].reserve(sbv.size())); CK(S->ext[1].reserve(extv.size()));
+    CK(S->td[1].reserve(tdv.size())); CK(S->rho[1].reserve(rhov.size()));
+    CK(S->imu.upload(imuData, st)); CK(S->imuKf.upload(imuKf, st));
+    CK(S->priorKind.upload(priorKind, st)); CK(S->priorIndex.upload(priorIndex, st));
+    CK(S->priorCol.upload(priorCol, st)); CK(S->priorOff.upload(priorOff, st));
+    CK(S->priorA.upload(priorA, st)); CK(S->priorR0.upload(priorR0, st)); CK(S->priorRef.upload(priorRef, st));
+    CK(S->lmC.reserve(cOff)); CK(S->lmD.reserve(lm)); CK(S->lmG.reserve(lm)); CK(S->lmCost.reserve(lm));
+    CK(S->lmDelta.reserve(lm)); CK(S->lmPred.reserve(lm)); CK(S->lmTrial.reserve(lm)); CK(S->lmMaxInc.reserve(lm));
+    CK(S->lmValid.reserve(lm)); CK(S->lmTrialValid.reserve(lm));
+    CK(S->Hret.reserve(dense)); CK(S->Sglob.reserve(dense)); CK(S->gret.reserve(vec)); CK(S->dr.reserve(vec)); CK(S->rhs.reserve(vec));
+    CK(S->acc.reserve(acc)); CK(S->imuScratch.reserve(imuS)); CK(S->priorScratch.reserve(priS));
+    CK(S->costRet.reserve(count)); CK(S->trialRet.reserve(count)); CK(S->retValid.reserve(count));
+    CK(S->predState.reserve(count)); CK(S->solveStatus.reserve(count)); CK(S->out.reserve(4ll * count));
+    DevBatch& B = S->B;
+    B = DevBatch{};
+    B.numWindows = count; B.numLandmarks = lm; B.numObs = ob; B.numKf = kf; B.numExt = ex; B.numCam = cam; B.numImu = im;
+    B.numSlabs = (int)S->slabs.size();
+    B.win = S->dWin.p; B.lm = S->dLm.p; B.slabs = S->dSlabs.p;
+    B.camR = S->camR.p; B.camT = S->camT.p; B.camExt = S->camExt.p;
+    B.lmWin = S->lmWin.p; B.lmKf = S->lmKf.p; B.lmCam = S->lmCam.p; B.lmObsBegin = S->lmObsBegin.p;
+    B.lmBearing = S->lmBearing.p; B.lmVel = S->lmVel.p; B.lmTime = S->lmTime.p;
+    B.lmNs = S->lmNs.p; B.lmSupp0 = S->lmSupp0.p; B.supp = S->supp.p; B.lmC0 = S->lmC0.p;
+    B.lmC = S->lmC.p; B.lmD = S->lmD.p; B.lmG = S->lmG.p; B.lmCost = S->lmCost.p; B.lmValid = S->lmValid.p;
+    B.lmDelta = S->lmDelta.p; B.lmPred = S->lmPred.p; B.lmTrial = S->lmTrial.p; B.lmMaxInc = S->lmMaxInc.p;
+    B.lmTrialValid = S->lmTrialValid.p;
+    B.obKf = S->obKf.p; B.obKfl = S->obKfl.p; B.obCam = S->obCam.p; B.obSlot = S->obSlot.p;
+    B.obBearing = S->obBearing.p; B.obP = S->obP.p; B.obVel = S->obVel.p; B.obTime = S->obTime.p;
+    for (int k = 0; k < 2; ++k) {
+        B.pose[k] = S->pose[k].p; B.sb[k] = S->sb[k].p; B.ext[k] = S->ext[k].p; B.td[k] = S->td[k].p; B.rho[k] = S->rho[k].p;
+    }
+    B.imu = S->imu.p; B.imuKf = S->imuKf.p;
+    B.priorKind = S->priorKind.p; B.priorIndex = S->priorIndex.p; B.priorCol = S->priorCol.p; B.priorOff = S->priorOff.p;
+    B.priorA = S->priorA.p; B.priorR0 = S->priorR0.p; B.priorRef = S->priorRef.p;
+    B.Hret = S->Hret.p; B.gret = S->gret.p; B.costRet = S->costRet.p; B.trialRet = S->trialRet.p; B.retValid = S->retValid.p;
+    B.acc = S->acc.p; B.dr = S->dr.p; B.rhs = S->rhs.p; B.Sglob = S->Sglob.p;
+    B.imuScratch = S->imuScratch.p; B.priorScratch = S->priorScratch.p; B.predState = S->predState.p;
+    B.solveStatus = S->solveStatus.p; B.out = S->out.p;
+    CK(cudaMemsetAsync(S->costRet.p, 0, count * sizeof(double), st));
+    CK(cudaMemsetAsync(S->trialRet.p, 0, count * sizeof(double), st));
+    CK(cudaStreamSynchronize(st));
+    return CGMLI_OK;
+}
+
+int cgmli_solver_upload_states(cgmli_solver* S, const cgmli_window* windows, int count) {
+    if (!S || !windows || count != (int)S->win.size()) return fail(CGMLI_E_INVALID, "window count differs from the configured batch");
+    CK(cudaSetDevice(S->device));
+    for (int i = 0; i < count; ++i) {
+        const WinDesc& d = S->win[i];
+        const auto& w = windows[i];
+        if (w.num_keyframes != d.K || w.num_landmarks != d.L || w.num_extrinsics != d.E)
+            return fail(CGMLI_E_INVALID, "state upload with a different topology");
+        CK(cudaMemcpyAsync(S->pose[0].p + 7ll * d.kf0, w.poses, 7ll * d.K * sizeof(double), cudaMemcpyHostToDevice, S->stream));
+        CK(cudaMemcpyAsync(S->sb[0].p + 9ll * d.kf0, w.speed_bias, 9ll * d.K * sizeof(double), cudaMemcpyHostToDevice, S->stream));
+        CK(cudaMemcpyAsync(S->ext[0].p + 7ll * d.ext0, w.extrinsics, 7ll * d.E * sizeof(double), cudaMemcpyHostToDevice, S->stream));
+        if (w.td) CK(cudaMemcpyAsync(S->td[0].p + i, w.td, sizeof(double), cudaMemcpyHostToDevice, S->stream));
+        if (d.L) CK(cudaMemcpyAsync(S->rho[0].p + d.lm0, w.rho, d.L * sizeof(double), cudaMemcpyHostToDevice, S->stream));
+    }
+    return CGMLI_OK;
+}
+
+static int runIterations(cgmli_solver* S, int iterations, int probe, double* Sdebug) {
+    cudaStream_t st = S->stream;
+    CK(cudaEventRecord(S->ev0, st));
+    int launches = launchLmInit(S->B, S->opt.initial_lambda, st);
+    for (int it = 0; it < iterations; ++it)
+        launches += launchIteration(S->B, S->dTiles.p, S->dSlabTile0.p, S->stageStride, S->linSmem, S->facSmem, S->opt.refinement_steps,
+                                    iterations, probe, Sdebug, st);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(S->ev1, st));
+    S->lastLaunches = launches;
+    return CGMLI_OK;
+}
+
+int cgmli_solver_solve(cgmli_solver* S, int max_iterations) {
+    if (!S || S->win.empty()) return fail(CGMLI_E_INVALID, "solver has no windows");
+    if (max_iterations < 1) return fail(CGMLI_E_INVALID, "max_iterations < 1");
+    CK(cudaSetDevice(S->device));
+    return runIterations(S, max_iterations, 0, nullptr);
+}
+
+int cgmli_solver_synchronize(cgmli_solver* S) {
+    if (!S) return fail(CGMLI_E_INVALID, "null solver");
+    CK(cudaStreamSynchronize(S->stream));
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, S->ev0, S->ev1) == cudaSuccess) S->lastMs = ms;
+    return CGMLI_OK;
+}
+
+int cgmli_solver_step(cgmli_solver* S, double lambda) {
+    if (!S || S->win.empty()) return fail(CGMLI_E_INVALID, "solver has no windows");
+    if (!(lambda > 0) || !std::isfinite(lambda)) return fail(CGMLI_E_INVALID, "lambda must be positive");
+    CK(cudaSetDevice(S->device));
+    long long dense = 0;
+    for (const auto& d : S->win) dense += (long long)d.Nr * d.Nr;
+    CK(S->Sdebug.reserve(dense));
+    const double saved = S->opt.initial_lambda;
+    S->opt.initial_lambda = lambda;
+    const int r = runIterations(S, 1, 1, S->Sdebug.p);
+    S->opt.initial_lambda = saved;
+    if (r != CGMLI_OK) return r;
+    return cgmli_solver_synchronize(S);
+}
+
+int cgmli_solver_window_dims(cgmli_solver* S, int w, int* retained, int* landmarks) {
+    if (!S || w < 0 || w >= (int)S->win.size()) return fail(CGMLI_E_INVALID, "window index");
+    if (retained) *retained = S->win[w].Nr;
+    if (landmarks) *landmarks = S->win[w].L;
+    return CGMLI_OK;
+}
+
+int cgmli_solver_read_step(cgmli_solver* S, int w, double* increment, double* cost, double* predicted, double* trial_cost,
+                           int* trial_valid) {
+    if (!S || w < 0 || w >= (int)S->win.size()) return fail(CGMLI_E_INVALID, "window index");
+    CK(cudaSetDevice(S->device));
+    const WinDesc& d = S->win[w];
+    WinLM lmst;
+    CK(cudaMemcpy(&lmst, S->dLm.p + w, sizeof(WinLM), cudaMemcpyDeviceToHost));
+    if (increment) {
+        CK(cudaMemcpy(increment, S->dr.p + d.vec0, d.Nr * sizeof(double), cudaMemcpyDeviceToHost));
+        if (d.L) CK(cudaMemcpy(increment + d.Nr, S->lmDelta.p + d.lm0, d.L * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    if (cost) *cost = lmst.linCost;
+    if (predicted) *predicted = lmst.predicted;
+    if (trial_cost) *trial_cost = lmst.trialCost;
+    if (trial_valid) *trial_valid = lmst.trialValid;
+    if (lmst.status != CGMLI_OK) return fail(lmst.status, "window step failed");
+    return CGMLI_OK;
+}
+
+int cgmli_solver_read_reduced(cgmli_solver* S, int w, double* Sout, double* rhs) {
+    if (!S || w < 0 || w >= (int)S->win.size() || !S->Sdebug.p) return fail(CGMLI_E_INVALID, "no reduced system recorded");
+    CK(cudaSetDevice(S->device));
+    const WinDesc& d = S->win[w];
+    if (Sout) CK(cudaMemcpy(Sout, S->Sdebug.p + d.dense0, (size_t)d.Nr * d.Nr * sizeof(double), cudaMemcpyDeviceToHost));
+    if (rhs) {
+        // rhs is recomputed from the accumulators (it equals -(g_r - B_v))
+        std::vector<double> g(d.Nr), accv((size_t)d.Npc * (d.Npc + 1) / 2 + 3 * d.Npc);
+        CK(cudaMemcpy(g.data(), S->gret.p + d.vec0, d.Nr * sizeof(double), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(accv.data(), S->acc.p + d.acc0, accv.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        const size_t nS = (size_t)d.Npc * (d.Npc + 1) / 2;
+        for (int i = 0; i < d.Nr; ++i) {
+            double v = g[i];
+            int p = -1;
+            if (i >= 15 * d.K) p = 6 * d.K + (i - 15 * d.K);
+            else if (i % 15 < 6) p = 6 * (i / 15) + i % 15;
+            if (p >= 0) v += accv[nS + d.Npc + p] - accv[nS + 2 * d.Npc + p];
+            rhs[i] = -v;
+        }
+    }
+    return CGMLI_OK;
+}
+
+int cgmli_solver_read_states(cgmli_solver* S, cgmli_window* windows, int count) {
+    if (!S || !windows || count != (int)S->win.size()) return fail(CGMLI_E_INVALID, "window count differs from the configured batch");
+    CK(cudaSetDevice(S->device));
+    CK(cudaStreamSynchronize(S->stream));
+    for (int i = 0; i < count; ++i) {
+        const WinDesc& d = S->win[i];
+        auto& w = windows[i];
+        CK(cudaMemcpy(w.poses, S->pose[0].p + 7ll * d.kf0, 7ll * d.K * sizeof(double), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(w.speed_bias, S->sb[0].p + 9ll * d.kf0, 9ll * d.K * sizeof(double), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(w.extrinsics, S->ext[0].p + 7ll * d.ext0, 7ll * d.E * sizeof(double), cudaMemcpyDeviceToHost));
+        if (w.td) CK(cudaMemcpy(w.td, S->td[0].p + i, sizeof(double), cudaMemcpyDeviceToHost));
+        if (d.L) CK(cudaMemcpy(w.rho, S->rho[0].p + d.lm0, d.L * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    return CGMLI_OK;
+}
+
+int cgmli_solver_read_reports(cgmli_solver* S, cgmli_solve_report* reports, int count) {
+    if (!S || !reports || count != (int)S->win.size()) return fail(CGMLI_E_INVALID, "report count differs from the configured batch");
+    CK(cudaSetDevice(S->device));
+    std::vector<WinLM> lm(count);
+    CK(cudaMemcpyAsync(lm.data(), S->dLm.p, count * sizeof(WinLM), cudaMemcpyDeviceToHost, S->stream));
+    CK(cudaStreamSynchronize(S->stream));
+    for (int i = 0; i < count; ++i) {
+        auto& r = reports[i];
+        r.initial_cost = lm[i].initialCost; r.final_cost = lm[i].cost; r.lambda = lm[i].lambda;
+        r.predicted_reduction = lm[i].predicted; r.max_increment = lm[i].maxInc;
+        r.iterations = lm[i].iterations; r.accepted_steps = lm[i].accepted; r.converged = lm[i].converged; r.status = lm[i].status;
+    }
+    return CGMLI_OK;
+}
+
+int cgmli_solver_last_timing(cgmli_solver* S, double* ms, int* launches) {
+    if (!S) return fail(CGMLI_E_INVALID, "null solver");
+    if (ms) *ms = S->lastMs;
+    if (launches) *launches = S->lastLaunches;
+    return CGMLI_OK;
+}
+
+int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) {
+    (void)S; (void)victim_kf; (void)policy;
+    return fail(CGMLI_E_UNSUPPORTED, "marginalization not built yet");
+}
+int cgmli_solver_read_prior(cgmli_solver* S, int window, int* rank, int* cols, int* num_blocks, int* block_kind, int* block_index,
+                            double* reference, double* A, double* r0, double* formation) {
+    (void)S; (void)window; (void)rank; (void)cols; (void)num_blocks; (void)block_kind; (void)block_index; (void)reference; (void)A;
+    (void)r0; (void)formation;
+    return fail(CGMLI_E_UNSUPPORTED, "marginalization not built yet");
+}
+int cgmli_marg_eigen(const double* H, int n, double* eigenvalues, double* eigenvectors) {
+    (void)H; (void)n; (void)eigenvalues; (void)eigenvectors;
+    return fail(CGMLI_E_UNSUPPORTED, "not built yet");
+}
+int cgmli_marg_psd_solve(const double* H, const double* rhs, int n, int columns, double a, double r, double* x) {
+    (void)H; (void)rhs; (void)n; (void)columns; (void)a; (void)r; (void)x;
+    return fail(CGMLI_E_UNSUPPORTED, "not built yet");
+}
+int cgmli_marg_subtract(const double* coupling, const double* solution, int nm, int nr, double* H, double* g) {
+    (void)coupling; (void)solution; (void)nm; (void)nr; (void)H; (void)g;
+    return fail(CGMLI_E_UNSUPPORTED, "not built yet");
+}
+
+}  // extern "C"

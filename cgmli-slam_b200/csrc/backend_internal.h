@@ -1,0 +1,87 @@
+// Device layout of a batch of windows (host runtime <-> kernels).
+//
+// All windows of a solver are concatenated.  Per-window metadata lives in
+// WinDesc; per-window LM state in WinLM (device-resident, updated by the
+// kernels so that no host round trip is needed between LM iterations).
+//
+// Column spaces of window w:
+//   retained  [0, Nr)   keyframe k: pose 15k..15k+5, speed/bias 15k+6..15k+14;
+//                       then 6 per estimated extrinsic, then td.
+//   visual    [0, Npc)  the columns a bearing factor can touch:
+//                       pose k -> 6k, extrinsic e -> 6K+6e, td -> 6K+6E'.
+//   landmark-local       support slot j -> 6j (slot 0 = anchor keyframe),
+//                       then the window's calibration columns.
+#pragma once
+#include <cstdint>
+
+namespace cgmli {
+
+constexpr int kMaxTrackChunk = 32;     // factors per warp pass
+constexpr int kMaxSupport = 64;        // keyframe slots per landmark
+constexpr int kLinThreads = 256;       // linearization CTA
+constexpr int kFactorThreads = 512;    // factorization CTA
+constexpr int kSmemPackedMax = 232;    // Nr up to which the packed factor fits in shared memory
+
+struct WinDesc {
+    int K, E, C, L, F, nImu;
+    int Nr, Npc, ncalib;
+    int estExt, estTd, hasTd;
+    int kf0, ext0, cam0, lm0, obs0, imu0;
+    int priorRank, priorCols, priorBlocks, priorBlk0;
+    int slab0, nslab;
+    int vec0;            // offset of Nr-vectors (gret, dr, rhs)
+    long long dense0;    // offset of Nr*Nr matrices (Hret, factor scratch)
+    long long acc0;      // offset of the visual accumulator: Npc(Npc+1)/2 + 3*Npc
+    long long priorA0, priorR00, priorRef0;
+    long long imuScratch0;  // nImu * 465 doubles
+    long long priorScratch0;  // priorRank*priorCols + priorCols*6 doubles
+    double huber, minInv;
+};
+
+struct WinLM {
+    double lambda, nu, cost, initialCost, linCost, trialCost, predicted, maxInc;
+    int mode;        // kModeLinearize, kModeResolve, kModeDone
+    int iterations, accepted, converged, status, acceptNow, trialValid, pad;
+};
+enum { kModeLinearize = 0, kModeResolve = 1, kModeDone = 2 };
+
+struct Slab { int win, lmBegin, lmEnd, pad; };
+
+// Pointers to every device array (filled by the host runtime).
+struct DevBatch {
+    int numWindows, numLandmarks, numObs, numKf, numExt, numCam, numImu, numSlabs;
+    const WinDesc* win;
+    WinLM* lm;
+    const Slab* slabs;
+    // cameras
+    const double* camR; const double* camT; const int* camExt;  // camExt: global extrinsic index
+    // landmarks
+    const int* lmWin; const int* lmKf; const int* lmCam; const int* lmObsBegin;  // lmObsBegin: numLandmarks+1
+    const double* lmBearing; const double* lmVel; const double* lmTime;
+    const int* lmNs; const int* lmSupp0; const int* supp;  // support keyframes (local index), anchor first
+    const long long* lmC0;                                // offset of the landmark's cross vector
+    double* lmC; double* lmD; double* lmG; double* lmCost; int* lmValid;
+    double* lmDelta; double* lmPred; double* lmTrial; double* lmMaxInc; int* lmTrialValid;
+    // observations
+    const int* obKf; const int* obKfl; const int* obCam; const int* obSlot;
+    const double* obBearing; const double* obP; const double* obVel; const double* obTime;
+    // states: [0] accepted, [1] candidate
+    double* pose[2]; double* sb[2]; double* ext[2]; double* td[2]; double* rho[2];
+    // IMU and priors
+    const double* imu;  // numImu * sizeof(cgmli_frozen_imu)/8
+    const int* imuKf;   // global keyframe index of the first state
+    const int* priorKind; const int* priorIndex; const int* priorCol; const int* priorOff;  // per prior block
+    const double* priorA; const double* priorR0; const double* priorRef;
+    // per-window dense storage
+    double* Hret; double* gret; double* costRet; double* trialRet; int* retValid;
+    double* acc;     // visual accumulators
+    double* dr;      // state increments (Nr per window)
+    double* rhs;
+    double* Sglob;   // factor scratch when Nr exceeds the shared-memory limit
+    double* imuScratch; double* priorScratch;
+    double* predState;
+    int* solveStatus;
+    double* out;     // per-window scratch for read-back (costs)
+};
+
+}  // namespace cgmli

@@ -1,0 +1,860 @@
+// sm_100a kernels of the sliding-window backend hot path.
+//
+// One LM iteration over a batch of windows is the launch sequence
+//   zero_acc -> linearize -> retained -> factor -> candidate -> backsub_trial
+//   -> retained_trial -> lm_update -> accept
+// with every decision of the damped LM loop (BackendOptimizer.cpp:167-307)
+// taken on the device from per-window state (WinLM), so that a whole solve
+// runs without a host round trip and can be captured in a CUDA graph.
+#include <cuda_runtime.h>
+
+#include "../../include/cgmli_backend.h"
+#include "backend_internal.h"
+#include "device_math.cuh"
+
+namespace cgmli {
+
+__device__ __forceinline__ double warpSum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warpMax(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+// packed upper triangle, row-major: (i <= j)
+__device__ __forceinline__ long long upIdx(int i, int j, int n) { return (long long)i * n - (long long)i * (i - 1) / 2 + (j - i); }
+// packed lower triangle, column-major: (i >= j)
+__device__ __forceinline__ int loIdx(int i, int j, int n) { return j * n - j * (j - 1) / 2 + (i - j); }
+
+// Visual column of retained column c (or -1 for speed/bias columns).
+__device__ __forceinline__ int pcOfRetained(int c, int K) {
+    if (c >= 15 * K) return 6 * K + (c - 15 * K);
+    const int w = c % 15;
+    return w < 6 ? 6 * (c / 15) + w : -1;
+}
+__device__ __forceinline__ int retainedOfPc(int p, int K) {
+    if (p >= 6 * K) return 15 * K + (p - 6 * K);
+    return 15 * (p / 6) + (p % 6);
+}
+
+// Gathers the inputs of observation f of landmark l from state buffer `buf`.
+__device__ __forceinline__ void gatherFactor(const DevBatch& B, const WinDesc& wd, int wdx, int l, int f, int buf, FactorIn& in,
+                                             int& kfa, int& kfb, int& ea, int& eb) {
+    kfa = B.lmKf[l];
+    kfb = B.obKf[f];
+    const int cama = B.lmCam[l], camb = B.obCam[f];
+    ea = B.camExt[cama];
+    eb = B.camExt[camb];
+    in.xa = B.pose[buf] + 7ll * kfa;
+    in.xb = B.pose[buf] + 7ll * kfb;
+    in.xea = B.ext[buf] + 7ll * ea;
+    in.xeb = B.ext[buf] + 7ll * eb;
+    in.Rca = B.camR + 9ll * cama; in.tca = B.camT + 3ll * cama;
+    in.Rcb = B.camR + 9ll * camb; in.tcb = B.camT + 3ll * camb;
+    in.anchor = ld3(B.lmBearing + 3ll * l);
+    in.anchorVel = ld3(B.lmVel + 3ll * l);
+    in.measured = ld3(B.obBearing + 3ll * f);
+    in.measuredVel = ld3(B.obVel + 3ll * f);
+    in.meas = B.obP + 6ll * f;
+    in.rho = B.rho[buf][l];
+    in.anchorTime = B.lmTime[l];
+    in.measuredTime = B.obTime[f];
+    in.td = wd.hasTd ? B.td[buf][wdx] : in.anchorTime;
+    in.sameKf = kfa == kfb;
+    in.splitExt = ea != eb;
+    in.wantExt = wd.estExt != 0;
+    in.wantTd = wd.estTd != 0;
+}
+
+// ---------------------------------------------------------------------------------------
+// zero the visual accumulators of windows that will be (re)linearized
+__global__ void k_zero_acc(DevBatch B) {
+    const int w = blockIdx.x;
+    if (B.lm[w].mode == kModeDone) return;
+    const WinDesc& wd = B.win[w];
+    const long long n = (long long)wd.Npc * (wd.Npc + 1) / 2 + 3ll * wd.Npc;
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) B.acc[wd.acc0 + i] = 0.0;
+}
+
+// ---------------------------------------------------------------------------------------
+// Linearization of the bearing factors of one slab (contiguous landmarks of
+// one window), fused with the per-landmark Schur complement at the window's
+// current lambda.  Per landmark l with scalar inverse distance:
+//   d_l = sum J_rho^T J_rho, g_l = sum J_rho^T r, c_l = sum J_x^T J_rho
+//   S  += sum_f J_f^T J_f - c_l c_l^T / (d_l + lambda max(d_l, 1e-6))
+//   rhs correction  += c_l g_l / (d_l + lambda max(d_l, 1e-6))
+// (accumulateVisualPairs + subtractPointSchur, VisualCudaBatch.cu:74-96,149-161).
+// Accumulation is FP64 in shared memory, flushed once per CTA.
+// Warps take tiles of consecutive landmarks holding at most 32 observations;
+// lane = observation.  Tile table: tiles[t] = {lmBegin, lmEnd}.
+__global__ void __launch_bounds__(kLinThreads) k_linearize(DevBatch B, const int2* tiles, const int* slabTile0, int stageStride) {
+    const Slab sl = B.slabs[blockIdx.x];
+    const int wdx = sl.win;
+    if (B.lm[wdx].mode == kModeDone) return;
+    const WinDesc wd = B.win[wdx];
+    const double lambda = B.lm[wdx].lambda;
+    extern __shared__ double smem[];
+    const int Npc = wd.Npc, K = wd.K;
+    const long long nS = (long long)Npc * (Npc + 1) / 2;
+    double* Sv = smem;
+    double* Dv = Sv + nS;
+    double* Gv = Dv + Npc;
+    double* Bv = Gv + Npc;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    double* stage = Bv + Npc + (long long)warp * (stageStride + 4 * 32);
+    double* lmD = stage + stageStride;  // per tile-landmark: d, g, cost, valid
+    double* lmGs = lmD + 32;
+    double* lmCs = lmGs + 32;
+    double* lmVs = lmCs + 32;
+    for (long long i = threadIdx.x; i < nS + 3ll * Npc; i += blockDim.x) smem[i] = 0.0;
+    __syncthreads();
+    const int tdCol = 6 * K + (wd.estExt ? 6 * wd.E : 0);
+    const int t0 = slabTile0[blockIdx.x], t1 = slabTile0[blockIdx.x + 1];
+    for (int t = t0 + warp; t < t1; t += nwarps) {
+        const int2 tile = tiles[t];
+        const int lb = tile.x, le = tile.y, nl = le - lb;
+        const int ob = B.lmObsBegin[lb], oe = B.lmObsBegin[le];
+        // staging offsets of each landmark's cross vector
+        int stageOff = 0, myStage = 0;
+        for (int q = 0; q < nl; ++q) {
+            const int ns = 6 * B.lmNs[lb + q] + wd.ncalib;
+            if (q == lane) myStage = stageOff;
+            stageOff += ns;
+        }
+        for (int i = lane; i < stageOff; i += 32) stage[i] = 0.0;
+        if (lane < nl) { lmD[lane] = 0; lmGs[lane] = 0; lmCs[lane] = 0; lmVs[lane] = 1; }
+        __syncwarp();
+        const int f = ob + lane;
+        if (f < oe) {
+            // landmark of this observation (tiles are small: linear search)
+            int q = 0;
+            while (B.lmObsBegin[lb + q + 1] <= f) ++q;
+            const int l = lb + q;
+            int qs = 0;
+            for (int p = 0; p < q; ++p) qs += 6 * B.lmNs[lb + p] + wd.ncalib;
+            const int s = B.lmNs[l];
+            double* cst = stage + qs;
+            FactorIn in;
+            int kfa, kfb, ea, eb;
+            gatherFactor(B, wd, wdx, l, f, 0, in, kfa, kfb, ea, eb);
+            FactorOut o;
+            const bool ok = evalBearingFactor(in, true, o);
+            if (!ok) {
+                lmVs[q] = 0;  // benign race: every writer stores 0
+            } else {
+                const double sq = o.r[0] * o.r[0] + o.r[1] * o.r[1];
+                const double wgt = huberWeight(wd.huber, sq);
+                atomicAdd(&lmCs[q], huberCost(wd.huber, sq));
+                const double rw0 = wgt * o.r[0], rw1 = wgt * o.r[1];
+                const double jr0 = wgt * o.Jrho[0], jr1 = wgt * o.Jrho[1];
+                atomicAdd(&lmD[q], jr0 * jr0 + jr1 * jr1);
+                atomicAdd(&lmGs[q], jr0 * rw0 + jr1 * rw1);
+                // retained entries of this factor: (visual column, local column, J row0, J row1)
+                int pcs[25], lcs[25];
+                double j0[25], j1[25];
+                int n = 0;
+                const int kfal = kfa - wd.kf0, kfbl = kfb - wd.kf0;
+                const bool same = in.sameKf && !in.splitExt;
+                if (!in.sameKf) {
+                    const int slot = B.obSlot[f];
+                    for (int c = 0; c < 6; ++c) { pcs[n] = 6 * kfal + c; lcs[n] = c; j0[n] = wgt * o.Ja[c]; j1[n] = wgt * o.Ja[6 + c]; ++n; }
+                    for (int c = 0; c < 6; ++c) { pcs[n] = 6 * kfbl + c; lcs[n] = 6 * slot + c; j0[n] = wgt * o.Jb[c]; j1[n] = wgt * o.Jb[6 + c]; ++n; }
+                }
+                if (wd.estExt && !same) {
+                    const int eal = ea - wd.ext0, ebl = eb - wd.ext0;
+                    for (int c = 0; c < 6; ++c) { pcs[n] = 6 * K + 6 * eal + c; lcs[n] = 6 * s + 6 * eal + c; j0[n] = wgt * o.Jea[c]; j1[n] = wgt * o.Jea[6 + c]; ++n; }
+                    if (in.splitExt)
+                        for (int c = 0; c < 6; ++c) { pcs[n] = 6 * K + 6 * ebl + c; lcs[n] = 6 * s + 6 * ebl + c; j0[n] = wgt * o.Jeb[c]; j1[n] = wgt * o.Jeb[6 + c]; ++n; }
+                }
+                if (wd.estTd) { pcs[n] = tdCol; lcs[n] = 6 * s + (tdCol - 6 * K); j0[n] = wgt * o.Jtd[0]; j1[n] = wgt * o.Jtd[1]; ++n; }
+                for (int a = 0; a < n; ++a) {
+                    atomicAdd(&Dv[pcs[a]], j0[a] * j0[a] + j1[a] * j1[a]);
+                    atomicAdd(&Gv[pcs[a]], j0[a] * rw0 + j1[a] * rw1);
+                    atomicAdd(&cst[lcs[a]], j0[a] * jr0 + j1[a] * jr1);
+                    for (int b = a; b < n; ++b) {
+                        const int pa = pcs[a], pb = pcs[b];
+                        const long long idx = pa <= pb ? upIdx(pa, pb, Npc) : upIdx(pb, pa, Npc);
+                        const double v = (j0[a] * j0[b] + j1[a] * j1[b]) * (pa == pb && a != b ? 2.0 : 1.0);
+                        atomicAdd(&Sv[idx], v);
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        // per-landmark Schur complement, one landmark at a time across the warp
+        int qs = 0;
+        for (int q = 0; q < nl; ++q) {
+            const int l = lb + q;
+            const int s = B.lmNs[l], ns = 6 * s + wd.ncalib;
+            const double d = lmD[q], g = lmGs[q];
+            const double* c = stage + qs;
+            const double inv = 1.0 / (d + lambda * fmax(d, 1e-6));
+            const int* sk = B.supp + B.lmSupp0[l];
+            const long long c0 = B.lmC0[l];
+            for (int i = lane; i < ns; i += 32) {
+                const double ci = c[i];
+                B.lmC[c0 + i] = ci;
+                const int pi = i < 6 * s ? 6 * sk[i / 6] + i % 6 : 6 * K + (i - 6 * s);
+                atomicAdd(&Bv[pi], inv * ci * g);
+            }
+            for (int i = 0; i < ns; ++i) {
+                const double ci = c[i];
+                if (ci == 0.0) continue;
+                const int pi = i < 6 * s ? 6 * sk[i / 6] + i % 6 : 6 * K + (i - 6 * s);
+                for (int j = i + lane; j < ns; j += 32) {
+                    const double cj = c[j];
+                    if (cj == 0.0) continue;
+                    const int pj = j < 6 * s ? 6 * sk[j / 6] + j % 6 : 6 * K + (j - 6 * s);
+                    const long long idx = pi <= pj ? upIdx(pi, pj, Npc) : upIdx(pj, pi, Npc);
+                    atomicAdd(&Sv[idx], -inv * ci * cj * (pi == pj && i != j ? 2.0 : 1.0));
+                }
+            }
+            if (lane == 0) {
+                B.lmD[l] = d; B.lmG[l] = g; B.lmCost[l] = lmCs[q]; B.lmValid[l] = lmVs[q] != 0.0;
+            }
+            qs += ns;
+        }
+        (void)myStage;
+        __syncwarp();
+    }
+    __syncthreads();
+    double* dst = B.acc + wd.acc0;
+    for (long long i = threadIdx.x; i < nS + 3ll * Npc; i += blockDim.x) {
+        const double v = smem[i];
+        if (v != 0.0) atomicAdd(&dst[i], v);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Frozen IMU factor, evaluateImu of GpuRetainedFactorMath.hpp:53-140.
+// r: 15 whitened; J: 15 x 30 row-major over [pose_i 6 | sb_i 9 | pose_j 6 | sb_j 9].
+struct Sensor { d3 p, v, arm, lever; qd q; };
+__device__ inline Sensor sensorState(const cgmli_frozen_imu& imu, const double* pose, const double* sb, int end) {
+    const qd q = qnormalized(ldq(pose + 3));
+    Sensor s;
+    s.q = qnormalized(qmul(q, ldq(imu.sensor_quaternion)));
+    s.arm = qapply(q, ld3(imu.sensor_position));
+    s.lever = cross(qapply(s.q, ld3(imu.gyros + 3 * end) - ld3(sb + 3)), s.arm);
+    s.p = ld3(pose) + s.arm;
+    s.v = ld3(sb) + s.lever;
+    return s;
+}
+__device__ inline bool evalImu(const cgmli_frozen_imu& imu, const double* p0, const double* sb0, const double* p1, const double* sb1,
+                               double* r, double* J) {
+    const Sensor s0 = sensorState(imu, p0, sb0, 0), s1 = sensorState(imu, p1, sb1, 1);
+    const m3 A = colmajor(imu.rotation_gyro), V = colmajor(imu.velocity_gyro), P = colmajor(imu.position_gyro),
+             Va = colmajor(imu.velocity_accel), Pa = colmajor(imu.position_accel);
+    const m3 R = qrot(qconj(s0.q));
+    const double dt = imu.duration;
+    const d3 gravity = {0, 0, imu.gravity};
+    const d3 bg = ld3(sb0 + 3) - ld3(imu.reference_bias), ba = ld3(sb0 + 6) - ld3(imu.reference_bias + 3);
+    const d3 dp = (s0.p - s1.p) + dt * s0.v - (0.5 * dt * dt) * gravity;
+    const d3 dv = (s0.v - s1.v) - dt * gravity;
+    const d3 phi = -1.0 * mv(A, bg);
+    const qd correction = rotationExp(phi), dq = qmul(correction, ldq(imu.delta_quaternion));
+    const qd tail = qmul(qmul(ldq(imu.delta_quaternion), qconj(s1.q)), s0.q);
+    double e[15];
+    const d3 e0 = mv(R, dp) + ld3(imu.delta_position) + mv(P, bg) - mv(Pa, ba);
+    const d3 e1 = 2.0 * qvec(qmul(dq, qmul(qconj(s1.q), s0.q)));
+    const d3 e2 = mv(R, dv) + ld3(imu.delta_velocity) + mv(V, bg) - mv(Va, ba);
+    e[0] = e0.x; e[1] = e0.y; e[2] = e0.z; e[3] = e1.x; e[4] = e1.y; e[5] = e1.z; e[6] = e2.x; e[7] = e2.y; e[8] = e2.z;
+    for (int i = 0; i < 6; ++i) e[9 + i] = sb0[3 + i] - sb1[3 + i];
+    for (int i = 0; i < 15; ++i) {
+        double v = 0;
+        for (int k = 0; k < 15; ++k) v += imu.whitening[i + 15 * k] * e[k];
+        r[i] = v;
+        if (!isfinite(v)) return false;
+    }
+    if (!J) return true;
+    const m3 gyroAngle = mscl(-1, mul(rotationJacobian(-1.0 * phi), A));
+    m3 Jrot, Jbias;
+    for (int j = 0; j < 3; ++j) {
+        const qd ax = {j == 0 ? 1.0 : 0.0, j == 1 ? 1.0 : 0.0, j == 2 ? 1.0 : 0.0, 0.0};
+        const qd db = {gyroAngle.a[j], gyroAngle.a[3 + j], gyroAngle.a[6 + j], 0.0};
+        const d3 c1 = qvec(qmul(qmul(qmul(dq, qconj(s1.q)), ax), s0.q));
+        const d3 c2 = qvec(qmul(qmul(correction, db), tail));
+        Jrot.a[j] = c1.x; Jrot.a[3 + j] = c1.y; Jrot.a[6 + j] = c1.z;
+        Jbias.a[j] = c2.x; Jbias.a[3 + j] = c2.y; Jbias.a[6 + j] = c2.z;
+    }
+    for (int i = 0; i < 450; ++i) J[i] = 0;
+    const int width[4] = {6, 9, 6, 9}, col0[4] = {0, 6, 15, 21};
+    for (int k = 0; k < 4; ++k) {
+        const bool first = k < 2;
+        const double sign = first ? 1 : -1;
+        const Sensor& s = first ? s0 : s1;
+        double Jk[15 * 9];
+        for (int i = 0; i < 135; ++i) Jk[i] = 0;
+        auto put = [&](int r0, int c0, const m3& m, bool accumulate) {
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    double& t = Jk[9 * (r0 + i) + c0 + j];
+                    t = accumulate ? t + m.a[3 * i + j] : m.a[3 * i + j];
+                }
+        };
+        if (k % 2 == 0) {
+            put(0, 0, mscl(sign, R), false);
+            put(0, 3, mscl(-sign, mul(R, skew(s.p))), false);
+            put(3, 3, mscl(sign, Jrot), false);
+            put(6, 3, mscl(-sign, mul(R, skew(s.lever))), false);
+            if (first) {
+                put(0, 3, mul(R, msub(skew(dp), mscl(dt, skew(s.lever)))), true);
+                put(6, 3, mul(R, skew(dv)), true);
+            }
+        } else {
+            const m3 leverBias = mul(skew(s.arm), qrot(s.q));
+            put(6, 0, mscl(sign, R), false);
+            put(6, 3, mscl(sign, mul(R, leverBias)), false);
+            put(9, 3, mscl(sign, eye3()), false);
+            put(12, 6, mscl(sign, eye3()), false);
+            if (first) {
+                put(0, 0, mscl(dt, R), false);
+                put(0, 3, madd(mscl(dt, mul(R, leverBias)), P), false);
+                put(0, 6, mscl(-1, Pa), false);
+                put(3, 3, Jbias, false);
+                put(6, 3, V, true);
+                put(6, 6, mscl(-1, Va), false);
+            }
+        }
+        for (int j = 0; j < width[k]; ++j)
+            for (int i = 0; i < 15; ++i) {
+                double v = 0;
+                for (int m = 0; m < 15; ++m) v += imu.whitening[i + 15 * m] * Jk[9 * m + j];
+                if (!isfinite(v)) return false;
+                J[30 * i + col0[k] + j] = v;
+            }
+    }
+    return true;
+}
+
+__device__ __forceinline__ const double* blockValue(const DevBatch& B, int buf, int kind, int index, int wdx) {
+    switch (kind) {
+        case CGMLI_PRIOR_POSE: return B.pose[buf] + 7ll * index;
+        case CGMLI_PRIOR_SPEED_BIAS: return B.sb[buf] + 9ll * index;
+        case CGMLI_PRIOR_EXTRINSIC: return B.ext[buf] + 7ll * index;
+        default: return B.td[buf] + wdx;
+    }
+}
+
+__device__ double blockSum(double v, double* red) {
+    v = warpSum(v);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double t = 0;
+    for (int i = 0; i < nw; ++i) t += red[i];
+    __syncthreads();
+    return t;
+}
+
+// Retained (IMU + prior) normal blocks of each window that is at a new point:
+// evaluateRetained + accumulateRetained (VisualCudaBatch.cu:626-642) written
+// as block-structured accumulation.  Also evaluates the residual cost of the
+// candidate state when `trial` is set (launchTrial, :715-721).
+__global__ void __launch_bounds__(256) k_retained(DevBatch B, int trial) {
+    const int wdx = blockIdx.x;
+    const int mode = B.lm[wdx].mode;
+    if (mode == kModeDone || (!trial && mode != kModeLinearize)) return;
+    const WinDesc wd = B.win[wdx];
+    const int Nr = wd.Nr, buf = trial ? 1 : 0;
+    __shared__ double red[32];
+    __shared__ int bad;
+    if (threadIdx.x == 0) bad = 0;
+    double* H = B.Hret + wd.dense0;
+    double* g = B.gret + wd.vec0;
+    if (!trial) {
+        for (long long i = threadIdx.x; i < (long long)Nr * Nr; i += blockDim.x) H[i] = 0.0;
+        for (int i = threadIdx.x; i < Nr; i += blockDim.x) g[i] = 0.0;
+    }
+    __syncthreads();
+    double cost = 0;
+    const cgmli_frozen_imu* imus = reinterpret_cast<const cgmli_frozen_imu*>(B.imu);
+    double* scratch = B.imuScratch + wd.imuScratch0;
+    for (int i = threadIdx.x; i < wd.nImu; i += blockDim.x) {
+        const int gi = wd.imu0 + i;
+        const int k = B.imuKf[gi];
+        double* r = scratch + 465ll * i;
+        const bool ok = evalImu(imus[gi], B.pose[buf] + 7ll * k, B.sb[buf] + 9ll * k, B.pose[buf] + 7ll * (k + 1),
+                                B.sb[buf] + 9ll * (k + 1), r, trial ? nullptr : r + 15);
+        if (!ok) atomicOr(&bad, 1);
+        else for (int m = 0; m < 15; ++m) cost += 0.5 * r[m] * r[m];
+    }
+    __syncthreads();
+    if (!trial) {
+        for (int i = 0; i < wd.nImu; ++i) {
+            const int k = B.imuKf[wd.imu0 + i] - wd.kf0;
+            const double* r = scratch + 465ll * i;
+            const double* J = r + 15;
+            for (int e = threadIdx.x; e < 930; e += blockDim.x) {
+                const int a = e < 900 ? e / 30 : e - 900, b = e % 30;
+                if (e < 900) {
+                    double v = 0;
+                    for (int m = 0; m < 15; ++m) v += J[30 * m + a] * J[30 * m + b];
+                    H[(long long)(15 * k + a) * Nr + 15 * k + b] += v;
+                } else {
+                    double v = 0;
+                    for (int m = 0; m < 15; ++m) v += J[30 * m + a] * r[m];
+                    g[15 * k + a] += v;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (wd.priorRank > 0) {
+        const int rank = wd.priorRank, cols = wd.priorCols;
+        double* ps = B.priorScratch + wd.priorScratch0;
+        double* delta = ps;           // cols
+        double* D = delta + cols;     // cols x 6
+        double* r = D + 6ll * cols;   // rank
+        double* J = r + rank;         // rank x cols
+        for (int b = threadIdx.x; b < wd.priorBlocks; b += blockDim.x) {
+            const int pb = wd.priorBlk0 + b;
+            const int kind = B.priorKind[pb], off = B.priorOff[pb];
+            const double* x = blockValue(B, buf, kind, B.priorIndex[pb], wdx);
+            // reference offset: ambient sizes accumulate in block order
+            int aoff = 0;
+            for (int q = wd.priorBlk0; q < pb; ++q) {
+                const int kq = B.priorKind[q];
+                aoff += kq == CGMLI_PRIOR_SPEED_BIAS ? 9 : kq == CGMLI_PRIOR_TIME_OFFSET ? 1 : 7;
+            }
+            const double* ref = B.priorRef + wd.priorRef0 + aoff;
+            if (kind == CGMLI_PRIOR_POSE || kind == CGMLI_PRIOR_EXTRINSIC) {
+                poseMinus(x, ref, delta + off);
+                if (!trial) se3LeftJacobianInverse(delta + off, D + 6ll * off);
+            } else {
+                const int t = kind == CGMLI_PRIOR_SPEED_BIAS ? 9 : 1;
+                for (int i = 0; i < t; ++i) delta[off + i] = x[i] - ref[i];
+            }
+        }
+        __syncthreads();
+        const double* A = B.priorA + wd.priorA0;
+        const double* r0 = B.priorR0 + wd.priorR00;
+        for (int i = threadIdx.x; i < rank; i += blockDim.x) {
+            double v = r0[i];
+            for (int c = 0; c < cols; ++c) v += A[(long long)i * cols + c] * delta[c];
+            r[i] = v;
+            if (!isfinite(v)) atomicOr(&bad, 1);
+            cost += 0.5 * v * v;
+        }
+        if (!trial) {
+            // J = A * blockdiag(D)
+            for (long long e = threadIdx.x; e < (long long)rank * cols; e += blockDim.x) {
+                const int i = (int)(e / cols), c = (int)(e % cols);
+                // block of column c
+                int pb = wd.priorBlk0;
+                while (pb + 1 < wd.priorBlk0 + wd.priorBlocks && B.priorOff[pb + 1] <= c) ++pb;
+                const int kind = B.priorKind[pb], off = B.priorOff[pb];
+                double v;
+                if (kind == CGMLI_PRIOR_POSE || kind == CGMLI_PRIOR_EXTRINSIC) {
+                    v = 0;
+                    for (int j = 0; j < 6; ++j) v += A[(long long)i * cols + off + j] * D[6ll * (off + j) + (c - off)];
+                } else {
+                    v = A[(long long)i * cols + c];
+                }
+                J[e] = v;
+            }
+            __syncthreads();
+            for (long long e = threadIdx.x; e < (long long)cols * (cols + 1); e += blockDim.x) {
+                const int p = (int)(e / cols), q = (int)(e % cols);
+                int bp = wd.priorBlk0, bq = wd.priorBlk0;
+                const int pp = p < cols ? p : q;
+                while (bp + 1 < wd.priorBlk0 + wd.priorBlocks && B.priorOff[bp + 1] <= pp) ++bp;
+                while (bq + 1 < wd.priorBlk0 + wd.priorBlocks && B.priorOff[bq + 1] <= q) ++bq;
+                const int colP = B.priorCol[bp], colQ = B.priorCol[bq];
+                if (p < cols) {
+                    if (colP < 0 || colQ < 0) continue;
+                    double v = 0;
+                    for (int i = 0; i < rank; ++i) v += J[(long long)i * cols + p] * J[(long long)i * cols + q];
+                    H[(long long)(colP + p - B.priorOff[bp]) * Nr + colQ + q - B.priorOff[bq]] += v;
+                } else {
+                    if (colQ < 0) continue;
+                    double v = 0;
+                    for (int i = 0; i < rank; ++i) v += J[(long long)i * cols + q] * r[i];
+                    g[colQ + q - B.priorOff[bq]] += v;
+                }
+            }
+        }
+    }
+    cost = blockSum(cost, red);
+    if (threadIdx.x == 0) {
+        if (trial) { B.trialRet[wdx] = cost; B.retValid[wdx] = bad ? 0 : 1; }
+        else { B.costRet[wdx] = cost; B.retValid[wdx] = bad ? 0 : 1; }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Damped reduced system, FP64 Cholesky and solve (prepareStateSolve + potrf +
+// potrs + clampStateStep + statePrediction, VisualCudaBatch.cu:163-189,564-580).
+//   S = H_ret + S_visual + lambda * max(diag(H_total), 1e-6),  rhs = -(g_r - B_v)
+// The factor is kept packed lower/column-major in shared memory when it fits.
+__device__ __forceinline__ double assembleEntry(const DevBatch& B, const WinDesc& wd, int i, int j, double lambda, bool damp) {
+    const int Nr = wd.Nr, Npc = wd.Npc, K = wd.K;
+    const double* H = B.Hret + wd.dense0;
+    const double* acc = B.acc + wd.acc0;
+    double v = H[(long long)i * Nr + j];
+    const int pi = pcOfRetained(i, K), pj = pcOfRetained(j, K);
+    if (pi >= 0 && pj >= 0) v += acc[pi <= pj ? upIdx(pi, pj, Npc) : upIdx(pj, pi, Npc)];
+    if (damp && i == j) {
+        double h = H[(long long)i * Nr + i];
+        if (pi >= 0) h += acc[(long long)Npc * (Npc + 1) / 2 + pi];
+        v += lambda * fmax(h, 1e-6);
+    }
+    return v;
+}
+
+__global__ void __launch_bounds__(kFactorThreads) k_factor(DevBatch B, int refinement, double* Sdebug) {
+    const int wdx = blockIdx.x;
+    if (B.lm[wdx].mode == kModeDone) return;
+    const WinDesc wd = B.win[wdx];
+    const int Nr = wd.Nr, Npc = wd.Npc, K = wd.K;
+    const double lambda = B.lm[wdx].lambda;
+    extern __shared__ double smem[];
+    __shared__ int failed;
+    __shared__ double red[32];
+    const bool inSmem = Nr <= kSmemPackedMax;
+    double* L = inSmem ? smem : B.Sglob + wd.dense0;
+    double* x = (inSmem ? smem : B.Sglob + wd.dense0) + (long long)Nr * (Nr + 1) / 2;  // working vector
+    const double* acc = B.acc + wd.acc0;
+    const long long nS = (long long)Npc * (Npc + 1) / 2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) failed = 0;
+    for (int j = warp; j < Nr; j += nw)
+        for (int i = j + lane; i < Nr; i += 32) {
+            const double v = assembleEntry(B, wd, i, j, lambda, true);
+            L[loIdx(i, j, Nr)] = v;
+            if (Sdebug) { Sdebug[wd.dense0 + (long long)i * Nr + j] = v; Sdebug[wd.dense0 + (long long)j * Nr + i] = v; }
+        }
+    double* rhsOut = B.rhs + wd.vec0;
+    for (int i = threadIdx.x; i < Nr; i += blockDim.x) {
+        double g = B.gret[wd.vec0 + i];
+        const int p = pcOfRetained(i, K);
+        if (p >= 0) g += acc[nS + Npc + p] - acc[nS + 2ll * Npc + p];
+        x[i] = -g;
+        rhsOut[i] = -g;
+    }
+    __syncthreads();
+    for (int k = 0; k < Nr; ++k) {
+        if (threadIdx.x == 0) {
+            const double v = L[loIdx(k, k, Nr)];
+            if (!(v > 0) || !isfinite(v)) failed = 1;
+            else L[loIdx(k, k, Nr)] = sqrt(v);
+        }
+        __syncthreads();
+        if (failed) break;
+        const double lkk = L[loIdx(k, k, Nr)];
+        for (int i = k + 1 + threadIdx.x; i < Nr; i += blockDim.x) L[loIdx(i, k, Nr)] /= lkk;
+        __syncthreads();
+        for (int j = k + 1 + warp; j < Nr; j += nw) {
+            const double ljk = L[loIdx(j, k, Nr)];
+            for (int i = j + lane; i < Nr; i += 32) L[loIdx(i, j, Nr)] -= L[loIdx(i, k, Nr)] * ljk;
+        }
+        __syncthreads();
+    }
+    if (failed) {
+        if (threadIdx.x == 0) B.solveStatus[wdx] = CGMLI_E_NOT_PD;
+        return;
+    }
+    // solves with one warp: L y = x (column-oriented), L^T z = y (row-oriented)
+    auto solveInPlace = [&](double* v) {
+        if (warp == 0) {
+            for (int k = 0; k < Nr; ++k) {
+                const double yk = v[k] / L[loIdx(k, k, Nr)];
+                __syncwarp();
+                if (lane == 0) v[k] = yk;
+                for (int i = k + 1 + lane; i < Nr; i += 32) v[i] -= L[loIdx(i, k, Nr)] * yk;
+                __syncwarp();
+            }
+            for (int k = Nr - 1; k >= 0; --k) {
+                double s = 0;
+                for (int i = k + 1 + lane; i < Nr; i += 32) s += L[loIdx(i, k, Nr)] * v[i];
+                s = warpSum(s);
+                if (lane == 0) v[k] = (v[k] - s) / L[loIdx(k, k, Nr)];
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+    };
+    solveInPlace(x);
+    double* dr = B.dr + wd.vec0;
+    for (int i = threadIdx.x; i < Nr; i += blockDim.x) dr[i] = x[i];
+    __syncthreads();
+    // iterative refinement against the assembled FP64 system
+    for (int it = 0; it < refinement; ++it) {
+        for (int i = threadIdx.x; i < Nr; i += blockDim.x) {
+            double g = B.gret[wd.vec0 + i];
+            const int p = pcOfRetained(i, K);
+            if (p >= 0) g += acc[nS + Npc + p] - acc[nS + 2ll * Npc + p];
+            double v = -g;
+            for (int j = 0; j < Nr; ++j) v -= assembleEntry(B, wd, i, j, lambda, true) * dr[j];
+            x[i] = v;
+        }
+        __syncthreads();
+        solveInPlace(x);
+        for (int i = threadIdx.x; i < Nr; i += blockDim.x) dr[i] += x[i];
+        __syncthreads();
+    }
+    // predicted reduction of the state part with the undamped (S_visual + H_ret):
+    //   -dx^T (g_r + 0.5 (S_v + H_ret) dx); the landmark terms are added per landmark.
+    double pred = 0;
+    for (int i = threadIdx.x; i < Nr; i += blockDim.x) {
+        double hd = 0;
+        for (int j = 0; j < Nr; ++j) hd += assembleEntry(B, wd, i, j, lambda, false) * dr[j];
+        double g = B.gret[wd.vec0 + i];
+        const int p = pcOfRetained(i, K);
+        if (p >= 0) g += acc[nS + Npc + p];
+        pred += -dr[i] * (g + 0.5 * hd);
+    }
+    pred = blockSum(pred, red);
+    if (threadIdx.x == 0) { B.predState[wdx] = pred; B.solveStatus[wdx] = CGMLI_OK; }
+}
+
+// ---------------------------------------------------------------------------------------
+// Candidate states x [+] dx of the retained blocks (residentTrial, VisualCudaBatch.cu:323-340).
+__global__ void k_candidate(DevBatch B) {
+    const int wdx = blockIdx.x;
+    if (B.lm[wdx].mode == kModeDone) return;
+    const WinDesc wd = B.win[wdx];
+    const double* dr = B.dr + wd.vec0;
+    __shared__ double red[32];
+    double mx = 0;
+    int bad = 0;
+    for (int i = threadIdx.x; i < wd.Nr; i += blockDim.x) {
+        if (!isfinite(dr[i])) bad = 1; else mx = fmax(mx, fabs(dr[i]));
+    }
+    for (int k = threadIdx.x; k < wd.K; k += blockDim.x) {
+        const int gk = wd.kf0 + k;
+        posePlus(B.pose[0] + 7ll * gk, dr + 15 * k, B.pose[1] + 7ll * gk);
+        for (int j = 0; j < 9; ++j) B.sb[1][9ll * gk + j] = B.sb[0][9ll * gk + j] + dr[15 * k + 6 + j];
+    }
+    for (int e = threadIdx.x; e < wd.E; e += blockDim.x) {
+        const int ge = wd.ext0 + e;
+        if (wd.estExt) posePlus(B.ext[0] + 7ll * ge, dr + 15 * wd.K + 6 * e, B.ext[1] + 7ll * ge);
+        else for (int j = 0; j < 7; ++j) B.ext[1][7ll * ge + j] = B.ext[0][7ll * ge + j];
+    }
+    if (threadIdx.x == 0)
+        B.td[1][wdx] = B.td[0][wdx] + (wd.estTd ? dr[15 * wd.K + (wd.estExt ? 6 * wd.E : 0)] : 0.0);
+    mx = warpMax(mx);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    bad = __any_sync(0xffffffffu, bad);
+    if (lane == 0) red[warp] = bad ? -1.0 : mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0;
+        bool anyBad = false;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) { if (red[i] < 0) anyBad = true; else m = fmax(m, red[i]); }
+        B.out[4ll * wdx + 0] = m;
+        B.out[4ll * wdx + 1] = anyBad ? 0.0 : 1.0;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Back-substitution of the inverse distances (backSubstitute,
+// VisualCudaBatch.cu:191-205) and the robust cost of the candidate point.
+// Warp per tile; lane = landmark for the back-substitution, lane =
+// observation for the trial residuals.
+__global__ void __launch_bounds__(kLinThreads) k_backsub_trial(DevBatch B, const int2* tiles, const int* slabTile0) {
+    const Slab sl = B.slabs[blockIdx.x];
+    const int wdx = sl.win;
+    if (B.lm[wdx].mode == kModeDone) return;
+    const WinDesc wd = B.win[wdx];
+    const double lambda = B.lm[wdx].lambda;
+    const int K = wd.K;
+    const double* dr = B.dr + wd.vec0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    __shared__ double tcost[kLinThreads / 32][32];
+    __shared__ int tvalid[kLinThreads / 32][32];
+    const int t0 = slabTile0[blockIdx.x], t1 = slabTile0[blockIdx.x + 1];
+    for (int t = t0 + warp; t < t1; t += nwarps) {
+        const int2 tile = tiles[t];
+        const int lb = tile.x, le = tile.y, nl = le - lb;
+        if (lane < nl) {
+            const int l = lb + lane;
+            const int s = B.lmNs[l], ns = 6 * s + wd.ncalib;
+            const double* c = B.lmC + B.lmC0[l];
+            const int* sk = B.supp + B.lmSupp0[l];
+            double cd = 0;
+            for (int i = 0; i < ns; ++i) {
+                const int p = i < 6 * s ? 6 * sk[i / 6] + i % 6 : 6 * K + (i - 6 * s);
+                cd += c[i] * dr[retainedOfPc(p, K)];
+            }
+            const double d = B.lmD[l], g = B.lmG[l];
+            const double dt = d + lambda * fmax(d, 1e-6);
+            double dl = -(g + cd) / dt;
+            const double x = B.rho[0][l];
+            if (isfinite(dl)) dl = fmax(wd.minInv - x, dl);
+            B.lmDelta[l] = dl;
+            // landmark terms of -dx^T (g + 0.5 H dx): the cross term c.dx_r is
+            // split between the state part (via S_v) and this correction
+            B.lmPred[l] = -0.5 * cd * cd / dt - dl * (g + cd + 0.5 * d * dl);
+            B.lmMaxInc[l] = isfinite(dl) ? fabs(dl) : -1.0;
+            B.rho[1][l] = fmax(wd.minInv, x + dl);
+            tcost[warp][lane] = 0;
+            tvalid[warp][lane] = isfinite(dl) ? 1 : 0;
+        }
+        __syncwarp();
+        const int ob = B.lmObsBegin[lb], oe = B.lmObsBegin[le];
+        const int f = ob + lane;
+        if (f < oe) {
+            int q = 0;
+            while (B.lmObsBegin[lb + q + 1] <= f) ++q;
+            const int l = lb + q;
+            FactorIn in;
+            int kfa, kfb, ea, eb;
+            gatherFactor(B, wd, wdx, l, f, 1, in, kfa, kfb, ea, eb);
+            FactorOut o;
+            if (!evalBearingFactor(in, false, o)) tvalid[warp][q] = 0;
+            else atomicAdd(&tcost[warp][q], huberCost(wd.huber, o.r[0] * o.r[0] + o.r[1] * o.r[1]));
+        }
+        __syncwarp();
+        if (lane < nl) {
+            B.lmTrial[lb + lane] = tcost[warp][lane];
+            B.lmTrialValid[lb + lane] = tvalid[warp][lane];
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Per-window reductions and the LM decision (BackendOptimizer.cpp:232-306).
+// probe != 0: record the step's scalars without changing the LM state.
+__global__ void __launch_bounds__(256) k_lm_update(DevBatch B, int maxIterations, int probe) {
+    const int wdx = blockIdx.x;
+    WinLM& st = B.lm[wdx];
+    if (st.mode == kModeDone) { if (threadIdx.x == 0) st.acceptNow = 0; return; }
+    const WinDesc wd = B.win[wdx];
+    __shared__ double red[32];
+    double cost = 0, pred = 0, trial = 0, mx = 0;
+    int valid = 1, tvalid = 1;
+    for (int i = threadIdx.x; i < wd.L; i += blockDim.x) {
+        const int l = wd.lm0 + i;
+        cost += B.lmCost[l];
+        pred += B.lmPred[l];
+        trial += B.lmTrial[l];
+        valid &= B.lmValid[l];
+        tvalid &= B.lmTrialValid[l];
+        const double m = B.lmMaxInc[l];
+        if (m < 0) tvalid = 0; else mx = fmax(mx, m);
+    }
+    cost = blockSum(cost, red);
+    pred = blockSum(pred, red);
+    trial = blockSum(trial, red);
+    mx = warpMax(mx);
+    __shared__ double mxs[32];
+    __shared__ int vs[32], tvs[32];
+    valid = __all_sync(0xffffffffu, valid);
+    tvalid = __all_sync(0xffffffffu, tvalid);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) { mxs[warp] = mx; vs[warp] = valid; tvs[warp] = tvalid; }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) { mx = fmax(mx, mxs[i]); valid &= vs[i]; tvalid &= tvs[i]; }
+    mx = fmax(mx, B.out[4ll * wdx + 0]);
+    tvalid = tvalid && B.out[4ll * wdx + 1] != 0.0 && B.retValid[wdx];
+    const double linCost = cost + B.costRet[wdx];
+    const double predicted = pred + B.predState[wdx];
+    const double trialCost = trial + B.trialRet[wdx];
+    if (st.mode == kModeLinearize) {
+        st.linCost = linCost;
+        if (!valid || !isfinite(linCost)) { st.status = CGMLI_E_NONFINITE; st.mode = kModeDone; st.acceptNow = 0; return; }
+        if (st.iterations == 0) st.cost = st.initialCost = linCost;
+        else if (fabs(linCost - st.cost) > 1e-8 * fmax(1.0, st.cost)) {
+            st.status = CGMLI_E_COST_MISMATCH; st.mode = kModeDone; st.acceptNow = 0; return;
+        }
+    }
+    st.predicted = predicted;
+    st.trialCost = trialCost;
+    st.trialValid = tvalid;
+    st.maxInc = mx;
+    if (B.solveStatus[wdx] != CGMLI_OK) { st.status = B.solveStatus[wdx]; st.mode = kModeDone; st.acceptNow = 0; return; }
+    if (probe) { st.acceptNow = 0; return; }
+    st.iterations += 1;
+    st.acceptNow = 0;
+    if (tvalid && mx < 1e-10) {
+        st.converged = 1; st.mode = kModeDone;
+    } else {
+        double gain = -1;
+        if (tvalid && predicted > 0 && isfinite(predicted)) gain = (st.cost - trialCost) / predicted;
+        if (gain > 1e-3) {
+            st.acceptNow = 1;
+            st.accepted += 1;
+            const bool conv = st.cost - trialCost <= 1e-6 * fmax(1.0, st.cost);
+            st.cost = trialCost;
+            const double t = 2 * gain - 1;
+            st.lambda = fmax(1e-12, st.lambda * fmax(1.0 / 3, 1 - t * t * t));
+            st.nu = 2;
+            st.converged = conv;
+            st.mode = conv ? kModeDone : kModeLinearize;
+        } else {
+            st.lambda *= st.nu;
+            st.nu *= 2;
+            st.mode = kModeResolve;
+        }
+    }
+    if (st.iterations >= maxIterations && st.mode != kModeDone) st.mode = kModeDone;
+    if (st.mode == kModeDone && st.status == CGMLI_OK && !st.accepted && !st.converged) st.status = CGMLI_E_NO_STEP;
+}
+
+// Copy the candidate into the accepted state of windows that accepted a step
+// (acceptResident, VisualCudaBatch.cu:702).
+__global__ void k_accept(DevBatch B) {
+    const int wdx = blockIdx.x;
+    if (!B.lm[wdx].acceptNow) return;
+    const WinDesc wd = B.win[wdx];
+    for (int i = threadIdx.x; i < 7 * wd.K; i += blockDim.x) B.pose[0][7ll * wd.kf0 + i] = B.pose[1][7ll * wd.kf0 + i];
+    for (int i = threadIdx.x; i < 9 * wd.K; i += blockDim.x) B.sb[0][9ll * wd.kf0 + i] = B.sb[1][9ll * wd.kf0 + i];
+    for (int i = threadIdx.x; i < 7 * wd.E; i += blockDim.x) B.ext[0][7ll * wd.ext0 + i] = B.ext[1][7ll * wd.ext0 + i];
+    if (threadIdx.x == 0) B.td[0][wdx] = B.td[1][wdx];
+    for (int i = threadIdx.x; i < wd.L; i += blockDim.x) B.rho[0][wd.lm0 + i] = B.rho[1][wd.lm0 + i];
+}
+
+__global__ void k_lm_init(DevBatch B, double lambda0) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= B.numWindows) return;
+    WinLM& st = B.lm[w];
+    st.lambda = lambda0; st.nu = 2; st.cost = 0; st.initialCost = 0; st.linCost = 0; st.trialCost = 0; st.predicted = 0;
+    st.maxInc = 0; st.mode = kModeLinearize; st.iterations = 0; st.accepted = 0; st.converged = 0; st.status = CGMLI_OK;
+    st.acceptNow = 0; st.trialValid = 0;
+}
+
+// ---------------------------------------------------------------------------------------
+// host-side launchers (called by backend_host.cu)
+size_t linearizeSmemBytes(int maxNpc, int stageStride) {
+    const size_t nS = (size_t)maxNpc * (maxNpc + 1) / 2 + 3ull * maxNpc;
+    return (nS + (size_t)(kLinThreads / 32) * (stageStride + 4 * 32)) * sizeof(double);
+}
+size_t factorSmemBytes(int maxNr) {
+    // windows with Nr <= kSmemPackedMax factor in shared memory; larger ones in global memory
+    const size_t n = (size_t)(maxNr < kSmemPackedMax ? maxNr : kSmemPackedMax);
+    return (n * (n + 1) / 2 + n) * sizeof(double);
+}
+
+cudaError_t configureKernels(size_t linSmem, size_t facSmem) {
+    cudaError_t e = cudaFuncSetAttribute(k_linearize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)linSmem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)facSmem);
+}
+
+int launchIteration(const DevBatch& B, const int2* tiles, const int* slabTile0, int stageStride, size_t linSmem, size_t facSmem,
+                    int refinement, int maxIterations, int probe, double* Sdebug, cudaStream_t s) {
+    const int W = B.numWindows;
+    int n = 0;
+    k_zero_acc<<<W, 256, 0, s>>>(B); ++n;
+    if (B.numSlabs > 0) { k_linearize<<<B.numSlabs, kLinThreads, linSmem, s>>>(B, tiles, slabTile0, stageStride); ++n; }
+    k_retained<<<W, 256, 0, s>>>(B, 0); ++n;
+    k_factor<<<W, kFactorThreads, facSmem, s>>>(B, refinement, Sdebug); ++n;
+    k_candidate<<<W, 128, 0, s>>>(B); ++n;
+    if (B.numSlabs > 0) { k_backsub_trial<<<B.numSlabs, kLinThreads, 0, s>>>(B, tiles, slabTile0); ++n; }
+    k_retained<<<W, 256, 0, s>>>(B, 1); ++n;
+    k_lm_update<<<W, 256, 0, s>>>(B, maxIterations, probe); ++n;
+    if (!probe) { k_accept<<<W, 256, 0, s>>>(B); ++n; }
+    return n;
+}
+int launchLmInit(const DevBatch& B, double lambda0, cudaStream_t s) {
+    k_lm_init<<<(B.numWindows + 127) / 128, 128, 0, s>>>(B, lambda0);
+    return 1;
+}
+
+}  // namespace cgmli

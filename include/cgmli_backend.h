@@ -1,0 +1,203 @@
+/*
+ * cgmli_backend.h - C ABI of the B200 sliding-window backend solver.
+ *
+ * This is the device boundary that sits behind the reference's
+ * `estimator_parameters.backend_visual_batch: schur` switch.  The reference
+ * crosses it through the C++ classes `VisualCudaBatch` and
+ * `MarginalCudaWorkspace` (src/backend/VisualCudaBatch.hpp:44-104); this
+ * header exports the same operations with plain pointers and sizes so that a
+ * C++ backend (or a ctypes / cgo / JNI binding) can call them without any
+ * C++ or torch types in the signatures.
+ *
+ * Conventions (identical to the reference, src/backend/README.md:44-47,
+ * src/backend/LeftSE3Manifold.hpp:151-156):
+ *   - pose ambient      [p_WB(3), qx, qy, qz, qw], tangent [rho(3), theta(3)],
+ *                       Plus(T, d) = Exp(d) * T (left SE(3));
+ *   - speed/bias        [v_W(3), b_g(3), b_a(3)], Euclidean;
+ *   - rig extrinsic     T_BR, same chart as a pose;
+ *   - landmark          one inverse distance rho along a fixed anchor bearing;
+ *   - camera pose       T_WC = T_WB * T_BR[e(c)] * T_RC[c].
+ * Tangent columns of a window: keyframe k owns [15k, 15k+6) (pose) and
+ * [15k+6, 15k+15) (speed/bias); then 6 columns per estimated extrinsic
+ * block; then one column for an estimated time offset.  N_r is their total.
+ *
+ * Every entry point returns 0 on success or one of the CGMLI_E_* codes;
+ * cgmli_last_error() returns a thread-local message for the last failure.
+ * There is no CPU fallback behind any entry point: a failure is reported to
+ * the caller, which decides what to do (the reference falls back to Ceres,
+ * src/backend/BackendOptimizer.cpp:964-989).
+ */
+#ifndef CGMLI_BACKEND_H
+#define CGMLI_BACKEND_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    CGMLI_OK = 0,
+    CGMLI_E_INVALID = 1,      /* malformed input (sizes, indices, layout) */
+    CGMLI_E_NONFINITE = 2,    /* a factor or state evaluated to NaN/Inf */
+    CGMLI_E_NOMEM = 3,        /* device or pinned allocation failed */
+    CGMLI_E_CUDA = 4,         /* CUDA runtime error (see cgmli_last_error) */
+    CGMLI_E_NOT_PD = 5,       /* damped reduced system is not positive definite */
+    CGMLI_E_INDEFINITE = 6,   /* marginal information significantly negative */
+    CGMLI_E_UNSUPPORTED = 7,  /* layout outside what the kernels implement */
+    CGMLI_E_NO_STEP = 8,      /* LM found no acceptable step */
+    CGMLI_E_LIMIT = 9,        /* size beyond a documented maximum */
+    CGMLI_E_COST_MISMATCH = 10 /* relinearized cost disagrees with accepted trial */
+};
+
+enum { CGMLI_PRECISION_FP64 = 0, CGMLI_PRECISION_MIXED = 1 };
+enum { CGMLI_PRIOR_POSE = 0, CGMLI_PRIOR_SPEED_BIAS = 1, CGMLI_PRIOR_EXTRINSIC = 2, CGMLI_PRIOR_TIME_OFFSET = 3 };
+enum { CGMLI_MARGIN_OLD = 0, CGMLI_MARGIN_SECOND_NEW = 1 };
+
+/* Frozen IMU preintegration of one keyframe interval.  Same fields and
+ * storage order as the reference's FrozenImuData
+ * (src/backend/GpuRetainedFactors.hpp:7-13): 3x3 matrices and the 15x15
+ * whitening are column-major, quaternions are [x, y, z, w]. */
+typedef struct cgmli_frozen_imu {
+    double duration, gravity;
+    double sensor_position[3], sensor_quaternion[4], gyros[6];
+    double delta_quaternion[4], delta_velocity[3], delta_position[3], reference_bias[6];
+    double rotation_gyro[9], velocity_gyro[9], position_gyro[9], velocity_accel[9], position_accel[9];
+    double whitening[225];
+} cgmli_frozen_imu;
+
+/* One sliding window in structure-of-arrays form.  Observations are
+ * landmark-major: the observations of landmark l are
+ * [lm_obs_begin[l], lm_obs_begin[l+1]).  The anchor observation of a
+ * landmark has no residual and is not listed (src/backend/README.md:62-64).
+ * State arrays are read by cgmli_solver_set_windows and written back by
+ * cgmli_solver_read_states. */
+typedef struct cgmli_window {
+    int num_keyframes;          /* K */
+    int num_cameras;            /* C fixed rig cameras */
+    int num_extrinsics;         /* E >= 1 T_BR blocks; camera c uses cam_ext[c] */
+    int estimate_extrinsics;    /* 1: extrinsic blocks are free variables */
+    int estimate_td;            /* 1: the time offset is a free scalar */
+    int num_landmarks;          /* L */
+    int num_observations;       /* F visual factors */
+    int num_imu;                /* frozen IMU factors */
+    int prior_rank;             /* rows of the square-root prior (0: none) */
+    int prior_num_blocks;       /* blocks in the prior's column order */
+    double huber_scale;         /* whitened Huber delta, <= 0 disables */
+    double min_inverse_distance;/* lower bound of every rho */
+    double *poses;              /* K*7 */
+    double *speed_bias;         /* K*9 */
+    double *extrinsics;         /* E*7 */
+    double *td;                 /* 1, or NULL: td equals each anchor's reference time */
+    double *rho;                /* L */
+    const double *cam_R;        /* C*9 row-major R_RC */
+    const double *cam_t;        /* C*3 t_RC */
+    const int *cam_ext;         /* C, extrinsic block of each camera */
+    const int *lm_anchor_kf;    /* L */
+    const int *lm_anchor_cam;   /* L */
+    const int *lm_obs_begin;    /* L+1 */
+    const double *lm_anchor_bearing;  /* L*3 */
+    const double *lm_anchor_velocity; /* L*3 bearing velocity, or NULL */
+    const double *lm_anchor_time;     /* L reference time offset, or NULL (0) */
+    const int *obs_kf;          /* F observer keyframe */
+    const int *obs_cam;         /* F observer camera */
+    const double *obs_bearing;  /* F*3 measured unit bearing */
+    const double *obs_P;        /* F*6 sqrtInfo * basis^T, 2x3 row-major */
+    const double *obs_velocity; /* F*3 or NULL */
+    const double *obs_time;     /* F or NULL */
+    const cgmli_frozen_imu *imu;/* num_imu */
+    const int *imu_kf;          /* num_imu: factor links keyframe imu_kf[i] -> imu_kf[i]+1 */
+    const int *prior_block_kind;  /* prior_num_blocks, CGMLI_PRIOR_* */
+    const int *prior_block_index; /* prior_num_blocks */
+    const double *prior_ref;    /* concatenated ambient references (7, 9, 7 or 1 per block) */
+    const double *prior_A;      /* prior_rank x (sum of tangent sizes), row-major */
+    const double *prior_r0;     /* prior_rank */
+} cgmli_window;
+
+typedef struct cgmli_solver_options {
+    int precision;           /* CGMLI_PRECISION_FP64 or _MIXED (FP32 Jacobians, FP64 sums) */
+    int refinement_steps;    /* iterative refinement after the FP64 Cholesky (0..2) */
+    double initial_lambda;   /* reference: 1e-4 */
+    int slabs_per_window;    /* CTAs per window in the linearization, 0 = choose */
+    int threads_per_block;   /* linearization CTA size, 0 = choose (autotuned) */
+} cgmli_solver_options;
+
+typedef struct cgmli_solve_report {
+    double initial_cost, final_cost, lambda, predicted_reduction, max_increment;
+    int iterations, accepted_steps, converged, status;
+} cgmli_solve_report;
+
+typedef struct cgmli_solver cgmli_solver;
+
+/* Message of the last failed call on this thread (never NULL). */
+const char *cgmli_last_error(void);
+
+void cgmli_default_options(cgmli_solver_options *options);
+
+/* Replaces VisualCudaWorkspace construction (src/backend/BackendOptimizer.cpp:334-341). */
+int cgmli_solver_create(int device, const cgmli_solver_options *options, cgmli_solver **out);
+void cgmli_solver_destroy(cgmli_solver *solver);
+
+/* Topology + upload of a batch of windows (VisualCudaBatch::linearizeSchur with
+ * newTopology=true, configureRetained and configureResident;
+ * src/backend/VisualCudaBatch.cu:433-511,606-624,673-691).  All later calls
+ * operate on these windows, in this order. */
+int cgmli_solver_set_windows(cgmli_solver *solver, const cgmli_window *windows, int count);
+/* Upload new state values only (same topology). */
+int cgmli_solver_upload_states(cgmli_solver *solver, const cgmli_window *windows, int count);
+
+/* Device-resident damped LM over every window (the native loop of
+ * solveVisualSchur, src/backend/BackendOptimizer.cpp:167-307, with the
+ * lambda schedule evaluated on the device).  Asynchronous on the solver's
+ * stream; no host round trip between iterations. */
+int cgmli_solver_solve(cgmli_solver *solver, int max_iterations);
+int cgmli_solver_synchronize(cgmli_solver *solver);
+/* VisualCudaBatch::readResident (src/backend/VisualCudaBatch.cu:704-713). */
+int cgmli_solver_read_states(cgmli_solver *solver, cgmli_window *windows, int count);
+int cgmli_solver_read_reports(cgmli_solver *solver, cgmli_solve_report *reports, int count);
+
+/* One damped step at fixed lambda from the current states, without moving
+ * them: linearizeSchur + linearizeRetained + solveOnline
+ * (src/backend/VisualCudaBatch.cu:530-604).  Writes, for window w, the
+ * increment (N_r state tangents then L inverse distances), the linearized
+ * cost, the predicted reduction, the trial cost and whether it is valid. */
+int cgmli_solver_step(cgmli_solver *solver, double lambda);
+int cgmli_solver_read_step(cgmli_solver *solver, int window, double *increment, double *cost,
+                           double *predicted, double *trial_cost, int *trial_valid);
+/* Reduced system of the last linearization/step of window w:
+ * S (N_r x N_r row-major, damped at that lambda) and its right-hand side. */
+int cgmli_solver_read_reduced(cgmli_solver *solver, int window, double *S, double *rhs);
+/* Sizes: N_r of window w. */
+int cgmli_solver_window_dims(cgmli_solver *solver, int window, int *retained, int *landmarks);
+
+/* Elapsed device milliseconds of the last cgmli_solver_solve / _step measured
+ * with CUDA events on the solver's stream, and the number of kernel launches. */
+int cgmli_solver_last_timing(cgmli_solver *solver, double *milliseconds, int *launches);
+
+/* Schur marginalization of one keyframe per window at the current states
+ * (Marginalizer::compute, src/backend/Marginalizer.cpp:284-474, with the
+ * elimination set of SlidingWindowManager::marginalize,
+ * src/backend/SlidingWindowManager.cpp:627-652).  victim_kf[w] is the
+ * keyframe removed from window w; policy is CGMLI_MARGIN_OLD or
+ * CGMLI_MARGIN_SECOND_NEW. */
+int cgmli_solver_marginalize(cgmli_solver *solver, const int *victim_kf, int policy);
+/* Result of window w: rank and separator width, then (when the buffers are
+ * not NULL) the separator blocks, their ambient references, A
+ * (rank x cols, row-major) and r0.  Call once with NULL buffers for sizes. */
+int cgmli_solver_read_prior(cgmli_solver *solver, int window, int *rank, int *cols, int *num_blocks,
+                            int *block_kind, int *block_index, double *reference, double *A, double *r0,
+                            double *formation /* 4: robust cost, linearized |r|^2, eliminated reduction, cutoff */);
+
+/* Dense FP64 marginalization helpers with the semantics of
+ * MarginalCudaWorkspace (src/backend/VisualCudaBatch.cu:911-957).
+ * Matrices are column-major, host memory in and out. */
+int cgmli_marg_eigen(const double *H, int n, double *eigenvalues, double *eigenvectors);
+int cgmli_marg_psd_solve(const double *H, const double *rhs, int n, int columns,
+                         double absolute_cutoff, double relative_cutoff, double *solution);
+int cgmli_marg_subtract(const double *coupling, const double *solution, int eliminated, int retained,
+                        double *H, double *g);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

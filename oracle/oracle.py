@@ -1,0 +1,157 @@
+"""ctypes binding of the FP64 CPU oracle (oracle/cgmli_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline arm of bench.py as the checker; never by the product path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import importlib.util
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def _pkg():
+    name = "cgmli_slam_b200"
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(
+            name, ROOT / "cgmli-slam_b200" / "__init__.py", submodule_search_locations=[str(ROOT / "cgmli-slam_b200")])
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
+
+
+_pkg()
+from cgmli_slam_b200 import abi  # noqa: E402
+from cgmli_slam_b200.build import build_oracle  # noqa: E402
+
+dp = abi.c_double_p
+ip = abi.c_int_p
+W = C.POINTER(abi.Window)
+_LIB = None
+
+
+def lib() -> C.CDLL:
+    global _LIB
+    if _LIB is None:
+        L = C.CDLL(str(build_oracle()))
+        P = abi._proto
+        P(L, "oracle_version", C.c_int, [])
+        P(L, "oracle_visual_factor", C.c_int, [W, C.c_int, C.c_int, C.c_int, dp, dp, ip])
+        P(L, "oracle_visual_residual_numeric", C.c_int, [W, C.c_int, C.c_int, dp])
+        P(L, "oracle_imu_factor", C.c_int, [C.POINTER(abi.FrozenImu), dp, dp, dp, dp, dp, dp])
+        P(L, "oracle_pose_plus", None, [dp, dp, dp])
+        P(L, "oracle_pose_minus", None, [dp, dp, dp])
+        P(L, "oracle_chart_derivative", None, [dp, dp, C.c_int, dp])
+        P(L, "oracle_prior_factor", C.c_int, [W, C.c_int, dp, dp])
+        P(L, "oracle_linearize", C.c_int, [W, dp, dp, dp, dp, dp])
+        P(L, "oracle_step", C.c_int, [W, C.c_double, C.c_int, dp, dp, dp, dp, dp, dp, dp])
+        P(L, "oracle_window_cost", C.c_int, [W, dp])
+        P(L, "oracle_lm_solve", C.c_int, [W, C.c_int, C.c_double, C.c_int, C.POINTER(abi.SolveReport)])
+        P(L, "oracle_lm_solve_batch", C.c_int, [W, C.c_int, C.c_int, C.c_int, C.POINTER(abi.SolveReport)])
+        P(L, "oracle_eigen_sym", C.c_int, [C.c_int, dp, dp, dp])
+        P(L, "oracle_psd_solve", C.c_int, [C.c_int, dp, C.c_int, dp, C.c_double, C.c_double, dp])
+        P(L, "oracle_marginalize_system", C.c_int,
+          [C.c_int, dp, dp, C.c_int, ip, ip, ip, dp, dp, dp, dp, dp])
+        P(L, "oracle_marginalize_window", C.c_int,
+          [W, C.c_int, C.c_int, ip, ip, ip, ip, ip, dp, dp, dp, dp, dp, dp])
+        _LIB = L
+    return _LIB
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(dp)
+
+
+def visual_factor(win, l, f, derivatives=True):
+    r = np.zeros(2)
+    J = np.zeros((2, 26))
+    flags = np.zeros(2, dtype=np.int32)
+    ok = lib().oracle_visual_factor(C.byref(win), l, f, int(derivatives), _p(r), _p(J), flags.ctypes.data_as(ip))
+    return bool(ok), r, J, flags
+
+
+def linearize(win, nr, L):
+    H = np.zeros((nr, nr)); g = np.zeros(nr + L); d = np.zeros(L); Cm = np.zeros((L, nr)); cost = np.zeros(1)
+    st = lib().oracle_linearize(C.byref(win), _p(H), _p(g), _p(d), _p(Cm), _p(cost))
+    return st, H, g, d, Cm, float(cost[0])
+
+
+def step(win, nr, L, lam, refinement=0):
+    delta = np.zeros(nr + L); S = np.zeros((nr, nr)); rhs = np.zeros(nr)
+    cost, pred, trial, maxinc = np.zeros(1), np.zeros(1), np.zeros(1), np.zeros(1)
+    st = lib().oracle_step(C.byref(win), lam, refinement, _p(delta), _p(S), _p(rhs), _p(cost), _p(pred), _p(trial), _p(maxinc))
+    return dict(status=st, delta=delta, S=S, rhs=rhs, cost=float(cost[0]), predicted=float(pred[0]),
+                trial_cost=float(trial[0]), max_increment=float(maxinc[0]))
+
+
+def lm_solve(win, iterations, initial_lambda=1e-4, refinement=0):
+    rep = abi.SolveReport()
+    st = lib().oracle_lm_solve(C.byref(win), iterations, initial_lambda, refinement, C.byref(rep))
+    return st, rep
+
+
+def window_cost(win):
+    c = np.zeros(1)
+    st = lib().oracle_window_cost(C.byref(win), _p(c))
+    return st, float(c[0])
+
+
+def eigen_sym(H):
+    n = H.shape[0]
+    Hc = np.ascontiguousarray(H, dtype=np.float64)
+    ev = np.zeros(n); V = np.zeros((n, n))
+    st = lib().oracle_eigen_sym(n, _p(Hc), _p(ev), _p(V))
+    return st, ev, V
+
+
+def psd_solve(H, rhs, abs_cut=1e-12, rel_cut=1e-9):
+    H = np.ascontiguousarray(H, dtype=np.float64)
+    rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+    if rhs.ndim == 1:
+        rhs = rhs[:, None]
+    x = np.zeros_like(rhs)
+    st = lib().oracle_psd_solve(H.shape[0], _p(H), rhs.shape[1], _p(rhs), abs_cut, rel_cut, _p(x))
+    return st, x
+
+
+def marginalize_system(H, b, blocks):
+    """blocks: list of (size, eliminate, landmark)."""
+    n = H.shape[0]
+    H = np.ascontiguousarray(H, dtype=np.float64); b = np.ascontiguousarray(b, dtype=np.float64)
+    desc = np.array([v for bl in blocks for v in bl], dtype=np.int32)
+    rank, nr = np.zeros(1, np.int32), np.zeros(1, np.int32)
+    Hp = np.zeros(n * n); bp = np.zeros(n); A = np.zeros(n * n); r0 = np.zeros(n); stats = np.zeros(3)
+    st = lib().oracle_marginalize_system(n, _p(H), _p(b), len(blocks), desc.ctypes.data_as(ip), rank.ctypes.data_as(ip),
+                                         nr.ctypes.data_as(ip), _p(Hp), _p(bp), _p(A), _p(r0), _p(stats))
+    k, m = int(rank[0]), int(nr[0])
+    return dict(status=st, rank=k, nr=m, H=Hp[:m * m].reshape(m, m), b=bp[:m], A=A[:k * m].reshape(k, m), r0=r0[:k],
+                eliminated_reduction=stats[0], cutoff=stats[1], new_reference_norm=stats[2])
+
+
+def marginalize_window(win, victim, policy=abi.MARGIN_OLD):
+    rank, cols, nb = np.zeros(1, np.int32), np.zeros(1, np.int32), np.zeros(1, np.int32)
+    st = lib().oracle_marginalize_window(C.byref(win), victim, policy, rank.ctypes.data_as(ip), cols.ctypes.data_as(ip),
+                                         nb.ctypes.data_as(ip), None, None, None, None, None, None, None, None)
+    if st != 0:
+        return dict(status=st)
+    k, m, b = int(rank[0]), int(cols[0]), int(nb[0])
+    kinds, idx = np.zeros(b, np.int32), np.zeros(b, np.int32)
+    ref = np.zeros(7 * b + 9 * b); Hp = np.zeros(m * m); bp = np.zeros(m); A = np.zeros(k * m); r0 = np.zeros(k)
+    form = np.zeros(4)
+    st = lib().oracle_marginalize_window(C.byref(win), victim, policy, rank.ctypes.data_as(ip), cols.ctypes.data_as(ip),
+                                         nb.ctypes.data_as(ip), kinds.ctypes.data_as(ip), idx.ctypes.data_as(ip), _p(ref),
+                                         _p(Hp), _p(bp), _p(A), _p(r0), _p(form))
+    return dict(status=st, rank=k, cols=m, kinds=kinds, index=idx, reference=ref, H=Hp.reshape(m, m), b=bp,
+                A=A.reshape(k, m), r0=r0, robust_cost=form[0], rss=form[1], eliminated_reduction=form[2], cutoff=form[3])
+
+
+def lm_solve_batch(windows_array, count, iterations, threads):
+    reps = (abi.SolveReport * count)()
+    st = lib().oracle_lm_solve_batch(windows_array, count, iterations, threads, reps)
+    return st, reps
