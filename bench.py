@@ -1,0 +1,375 @@
+#!/usr/bin/env python
+"""Window solves/sec of the batched sliding-window backend solve on B200.
+
+Workload (default): the batched configuration - 512 independent windows from
+distinct seeds, keyframes U{6..15}, landmarks log-U(200, 5000), track length
+2-10, 4-camera rig with per-window extrinsic perturbation (1 cm / 0.3 deg),
+IMU factors and a seeded square-root prior, online per-camera extrinsics +
+time offset, 5 damped LM iterations per window.  One step = one batched solve
+of all windows (device-side LM, no host round trip), started from the same
+initial states every step.  Seeded synthetic inputs stand in for the Hilti
+2023 replays.
+
+Lines printed (rank 0): one JSON object.  ``--impl reference`` times the
+reference algorithm's CPU path instead (the FP64 CPU oracle: the reference's
+Ceres/Eigen build cannot be compiled offline).
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+
+
+def _load_package():
+    name = "cgmli_slam_b200"
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(
+            name, ROOT / "cgmli-slam_b200" / "__init__.py", submodule_search_locations=[str(ROOT / "cgmli-slam_b200")])
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
+
+
+_load_package()
+import numpy as np  # noqa: E402
+
+from cgmli_slam_b200 import abi, synth  # noqa: E402
+
+METRIC = "window solves/sec"
+UNIT = "windows/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--windows", type=int, default=512)
+    p.add_argument("--iterations", type=int, default=5)
+    p.add_argument("--seed", type=int, default=20260101)
+    p.add_argument("--cpu-sample", type=int, default=24, help="windows timed on the host for the CPU baseline")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--plain-windows", type=int, default=16, help="single-window solves timed for the plain path")
+    return p.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def config_dict(args, world):
+    return {
+        "workload": "batched windows: K~U{6..15}, L~logU(200,5000), 4 cams, IMU+prior, 24+1 calib, 5 LM it",
+        "windows_per_gpu": args.windows, "lm_iterations": args.iterations, "seed": args.seed,
+        "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (no flush needed)",
+        "precision": "fp64 factor eval and accumulation, fp64 Cholesky",
+    }
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except Exception:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def window_bytes(w) -> tuple[int, int]:
+    """Host bytes uploaded by set_windows for one window, and state bytes read back."""
+    W = w.window
+    K, E, C, L, F = W.num_keyframes, W.num_extrinsics, W.num_cameras, W.num_landmarks, W.num_observations
+    cols = 0
+    if W.prior_rank:
+        kinds = np.ctypeslib.as_array(W.prior_block_kind, shape=(W.prior_num_blocks,))
+        cols = int(sum(9 if k == 1 else 1 if k == 3 else 6 for k in kinds))
+        amb = int(sum(9 if k == 1 else 1 if k == 3 else 7 for k in kinds))
+    state = 8 * (16 * K + 7 * E + 1 + L)
+    h2d = state + 8 * (12 * C) + 4 * C + L * (4 * 4 + 8 * 7) + F * (4 * 2 + 8 * 13) + W.num_imu * (8 * 295 + 4)
+    if W.prior_rank:
+        h2d += 8 * (W.prior_rank * cols + W.prior_rank + amb) + 8 * W.prior_num_blocks
+    return h2d, state
+
+
+def algorithmic_linearize_bytes(w) -> int:
+    """Bytes one linearization must move for a window: observation stream (44 B
+    static / 76 B with bearing velocity), landmark stream (28 B), and the
+    reduced visual system written once."""
+    W = w.window
+    moving = W.obs_velocity is not None and bool(W.obs_velocity)
+    per_obs = 76 if moving else 44
+    K = W.num_keyframes
+    ncal = (6 * W.num_extrinsics if W.estimate_extrinsics else 0) + (1 if W.estimate_td else 0)
+    npc = 6 * K + ncal
+    return per_obs * W.num_observations + 28 * W.num_landmarks + 8 * (npc * (npc + 1) // 2 + 3 * npc)
+
+
+def peaks():
+    try:
+        d = json.load(open(ROOT / "MEASURED_PEAKS.json"))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def run_reference(args, world, rank):
+    """CPU path of the reference algorithm on the host cores (FP64 oracle)."""
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O  # CPU arm: the only place bench.py runs the oracle besides cpu_baseline
+
+    n = max(1, args.cpu_sample)
+    threads = os.cpu_count() or 1
+    windows = synth.make_windows("c4", n, seed=args.seed)
+    init = [w.state_vector() for w in windows]
+    arr = synth.window_array(windows)
+    for _ in range(max(0, min(args.warmup, 1))):
+        O.lm_solve_batch(arr, n, args.iterations, threads)
+        for w, x in zip(windows, init):
+            w.set_state_vector(x)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        st, reps = O.lm_solve_batch(arr, n, args.iterations, threads)
+        times.append(time.perf_counter() - t0)
+        for w, x in zip(windows, init):
+            w.set_state_vector(x)
+    total = sum(times)
+    value = n * len(times) / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000 * total / len(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_dict(args, world),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{n} windows of the batched workload per step, {args.iterations} LM iterations, FP64 oracle"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference Ceres/Eigen CPU path cannot be built offline; the FP64 C++ restatement runs on all host threads",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    from cgmli_slam_b200 import backend
+
+    windows = synth.make_windows("c4", args.windows, seed=args.seed + 100000 * rank)
+    init = [w.state_vector() for w in windows]
+    solver = backend.Solver(device=local)
+    solver.set_windows(windows)
+    solver.checkpoint()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up
+    for _ in range(max(3, args.warmup)):
+        solver.rollback()
+        solver.solve(args.iterations)
+        solver.synchronize()
+    # timed region: device time per step from CUDA events on the solver's stream
+    solver.kernel_times(enable=1)
+    barrier()
+    dev_ms = []
+    with ClockSampler(local) as clocks:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            solver.rollback()
+            solver.solve(args.iterations)
+            solver.synchronize()
+            dev_ms.append(solver.timing()[0])
+        barrier()
+        wall = time.perf_counter() - t0
+    ktimes = solver.kernel_times(enable=-1)
+    solver.kernel_times(enable=0)
+    launches = solver.timing()[1] * args.steps
+    reports = solver.reports()
+    total_ms = sum(dev_ms)
+    if dist is not None:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * args.windows * args.steps / (total_ms / 1000.0)
+
+    # roofline of the dominant kernel (linearization)
+    lin_ms, lin_calls = ktimes["linearize"]
+    lin_passes = sum(r.iterations for r in reports)  # window-linearizations per solve
+    bytes_per_solve = sum(algorithmic_linearize_bytes(w) * r.iterations for w, r in zip(windows, reports))
+    achieved = bytes_per_solve * args.steps / (lin_ms / 1000.0) / 1e9 if lin_ms > 0 else 0.0
+    peak, peak_kind = peaks()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "kernel": "k_linearize", "peak_source": peak_kind,
+                "launch_avg_ms": lin_ms / max(1, lin_calls), "window_linearizations_per_step": lin_passes,
+                "kernel_ms_per_step": {k: v[0] / args.steps for k, v in ktimes.items()}}
+
+    # end to end through the C ABI with host buffers: topology + upload, solve, read back
+    h2d = sum(window_bytes(w)[0] for w in windows)
+    d2h = sum(window_bytes(w)[1] for w in windows)
+    e2e_times = []
+    e2e_solver = backend.Solver(device=local)
+    for it in range(1 + max(1, args.steps // 2)):
+        for w, x in zip(windows, init):
+            w.set_state_vector(x)
+        barrier()
+        t1 = time.perf_counter()
+        e2e_solver.set_windows(windows)
+        e2e_solver.solve(args.iterations)
+        e2e_solver.synchronize()
+        e2e_solver.read_states()
+        dt = time.perf_counter() - t1
+        if it > 0:
+            e2e_times.append(dt)
+    e2e_s = sum(e2e_times) / len(e2e_times)
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": world * args.windows / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+           "includes": "host topology build + H2D of all window data + device LM + D2H of states"}
+
+    # plain single-window path: the configuration-2 window solved alone, one at a time
+    plain = None
+    if rank == 0 and args.plain_windows > 0:
+        pw = synth.make_windows("c2", args.plain_windows, seed=args.seed + 7)
+        ps = backend.Solver(device=local)
+        lat = []
+        for i, w in enumerate(pw):
+            ps.set_windows([w])
+            ps.checkpoint()
+            for rep in range(2):
+                ps.rollback()
+                ps.solve(args.iterations)
+                ps.synchronize()
+                if rep == 1:
+                    lat.append(ps.timing()[0])
+        lat.sort()
+        plain = {"windows_per_s": 1000.0 / statistics.mean(lat), "p50_ms": lat[len(lat) // 2],
+                 "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))], "windows": len(lat),
+                 "workload": "one configuration-2 window (10 KF, 3000 lm, 24+1 calib, prior) per solve"}
+
+    statuses = {}
+    for r in reports:
+        statuses[abi.ERRORS.get(r.status, r.status)] = statuses.get(abi.ERRORS.get(r.status, r.status), 0) + 1
+
+    cpu_baseline = None
+    if rank == 0 and not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle as O  # cpu_baseline leg
+
+        n = max(1, min(args.cpu_sample, args.windows))
+        threads = os.cpu_count() or 1
+        sample = windows[:n]
+        for w, x in zip(sample, init):
+            w.set_state_vector(x)
+        arr = synth.window_array(sample)
+        t2 = time.perf_counter()
+        st, reps = O.lm_solve_batch(arr, n, args.iterations, threads)
+        cpu_s = time.perf_counter() - t2
+        # states of the same windows solved on the GPU, against the FP64 oracle
+        gpu_states = []
+        solver.rollback()
+        solver.solve(args.iterations)
+        solver.synchronize()
+        cpu_states = [w.state_vector() for w in sample]
+        solver.read_states()
+        errs = []
+        for w, xc, x0 in zip(sample, cpu_states, init[:n]):
+            xg = w.state_vector()
+            errs.append(float(np.linalg.norm(xg - xc) / max(np.linalg.norm(xc - x0), 1e-300)))
+        for w, x in zip(windows, init):
+            w.set_state_vector(x)
+        cpu_baseline = {"value": n / cpu_s, "unit": UNIT, "cores": threads, "kind": "port",
+                        "sample": f"first {n} windows of the batch, {args.iterations} LM iterations, FP64 oracle on {threads} threads",
+                        "final_state_rel_err_vs_fp64_max": max(errs)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup),
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": config_dict(args, world),
+            "clocks": clocks.summary(), "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
+            "cpu_baseline": cpu_baseline, "plain_path": plain,
+            "served_vs_plain": (value / world) / plain["windows_per_s"] if plain else None,
+            "batch_latency_ms": {"p50": sorted(dev_ms)[len(dev_ms) // 2], "p99": max(dev_ms)},
+            "window_status": statuses, "wall_s": wall,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    e2e_solver.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

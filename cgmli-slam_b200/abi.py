@@ -101,6 +101,9 @@ def declare_backend(lib: C.CDLL) -> C.CDLL:
     _proto(lib, "cgmli_solver_marginalize", C.c_int, [S, c_int_p, C.c_int])
     _proto(lib, "cgmli_solver_read_prior", C.c_int,
            [S, C.c_int, c_int_p, c_int_p, c_int_p, c_int_p, c_int_p, c_double_p, c_double_p, c_double_p, c_double_p])
+    _proto(lib, "cgmli_solver_checkpoint", C.c_int, [S])
+    _proto(lib, "cgmli_solver_rollback", C.c_int, [S])
+    _proto(lib, "cgmli_solver_kernel_times", C.c_int, [S, C.c_int, c_double_p, c_int_p])
     _proto(lib, "cgmli_marg_eigen", C.c_int, [c_double_p, C.c_int, c_double_p, c_double_p])
     _proto(lib, "cgmli_marg_psd_solve", C.c_int,
            [c_double_p, c_double_p, C.c_int, C.c_int, C.c_double, C.c_double, c_double_p])
@@ -124,4 +127,6 @@ BACKEND_SYMBOLS = [
     "cgmli_solver_read_states", "cgmli_solver_read_reports", "cgmli_solver_step", "cgmli_solver_read_step",
     "cgmli_solver_read_reduced", "cgmli_solver_window_dims", "cgmli_solver_last_timing", "cgmli_solver_marginalize",
     "cgmli_solver_read_prior", "cgmli_marg_eigen", "cgmli_marg_psd_solve", "cgmli_marg_subtract",
+    "cgmli_solver_checkpoint", "cgmli_solver_rollback", "cgmli_solver_kernel_times",
 ]
+KERNEL_NAMES = ["zero_acc", "linearize", "retained", "factor", "candidate", "backsub_trial", "retained_trial", "lm_update", "accept"]

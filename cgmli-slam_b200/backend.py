@@ -113,6 +113,19 @@ class Solver:
         _check(lib().cgmli_solver_read_reduced(self._h, w, _p(S), _p(rhs)), "cgmli_solver_read_reduced")
         return S, rhs
 
+    def checkpoint(self) -> None:
+        _check(lib().cgmli_solver_checkpoint(self._h), "cgmli_solver_checkpoint")
+
+    def rollback(self) -> None:
+        _check(lib().cgmli_solver_rollback(self._h), "cgmli_solver_rollback")
+
+    def kernel_times(self, enable: int = -1) -> dict:
+        ms = np.zeros(len(abi.KERNEL_NAMES))
+        calls = np.zeros(len(abi.KERNEL_NAMES), dtype=np.int32)
+        _check(lib().cgmli_solver_kernel_times(self._h, enable, _p(ms), calls.ctypes.data_as(abi.c_int_p)),
+               "cgmli_solver_kernel_times")
+        return {n: (float(ms[i]), int(calls[i])) for i, n in enumerate(abi.KERNEL_NAMES)}
+
     def timing(self) -> tuple[float, int]:
         ms, n = C.c_double(), C.c_int()
         _check(lib().cgmli_solver_last_timing(self._h, C.byref(ms), C.byref(n)), "cgmli_solver_last_timing")

@@ -23,7 +23,7 @@ size_t linearizeSmemBytes(int maxNpc, int stageStride);
 size_t factorSmemBytes(int maxNr);
 cudaError_t configureKernels(size_t linSmem, size_t facSmem);
 int launchIteration(const DevBatch& B, const int2* tiles, const int* slabTile0, int stageStride, size_t linSmem, size_t facSmem,
-                    int refinement, int maxIterations, int probe, double* Sdebug, cudaStream_t s);
+                    int refinement, int maxIterations, int probe, double* Sdebug, cudaStream_t s, LaunchHook hook, void* ctx);
 int launchLmInit(const DevBatch& B, double lambda0, cudaStream_t s);
 }  // namespace cgmli
 
@@ -106,6 +106,35 @@ struct cgmli_solver {
     DevBatch B{};
     double lastMs = 0;
     int lastLaunches = 0;
+    // checkpoint of the accepted states
+    DArray<double> snapPose, snapSb, snapExt, snapTd, snapRho;
+    bool haveSnapshot = false;
+    // per-kernel event timing
+    bool profile = false;
+    std::vector<cudaEvent_t> evPool;
+    std::vector<std::pair<int, int>> evUsed;  // (kind, index of start event)
+    size_t evNext = 0;
+    double kernelMs[CGMLI_KERNEL_KINDS] = {};
+    int kernelCalls[CGMLI_KERNEL_KINDS] = {};
+    cudaEvent_t nextEvent() {
+        if (evNext == evPool.size()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            evPool.push_back(e);
+        }
+        return evPool[evNext++];
+    }
+    void collectKernelTimes() {
+        for (const auto& u : evUsed) {
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, evPool[u.second], evPool[u.second + 1]) == cudaSuccess) {
+                kernelMs[u.first] += ms;
+                kernelCalls[u.first] += 1;
+            }
+        }
+        evUsed.clear();
+        evNext = 0;
+    }
 
     ~cgmli_solver() {
         if (stream) cudaStreamSynchronize(stream);
@@ -119,6 +148,8 @@ struct cgmli_solver {
                                &solveStatus, &dSlabTile0};
         for (auto* a : ints) a->release();
         lmC0.release(); dWin.release(); dLm.release(); dSlabs.release(); dTiles.release();
+        snapPose.release(); snapSb.release(); snapExt.release(); snapTd.release(); snapRho.release();
+        for (auto e : evPool) cudaEventDestroy(e);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
@@ -220,6 +251,7 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     CK(cudaSetDevice(S->device));
     cudaStream_t st = S->stream;
     S->win.assign(count, WinDesc{});
+    S->haveSnapshot = false;
     S->slabs.clear(); S->tiles.clear(); S->slabTile0.clear();
     int kf = 0, ex = 0, cam = 0, lm = 0, ob = 0, im = 0, pblk = 0, vec = 0;
     long long dense = 0, acc = 0, pA = 0, pR = 0, pRef = 0, imuS = 0, priS = 0, cOff = 0;
@@ -458,13 +490,21 @@ int cgmli_solver_upload_states(cgmli_solver* S, const cgmli_window* windows, int
     return CGMLI_OK;
 }
 
+static void profileHook(void* ctx, int kind, int phase) {
+    auto* S = static_cast<cgmli_solver*>(ctx);
+    cudaEvent_t e = S->nextEvent();
+    if (phase == 0) S->evUsed.push_back({kind, (int)S->evNext - 1});
+    cudaEventRecord(e, S->stream);
+}
+
 static int runIterations(cgmli_solver* S, int iterations, int probe, double* Sdebug) {
     cudaStream_t st = S->stream;
+    if (S->profile) S->collectKernelTimes();
     CK(cudaEventRecord(S->ev0, st));
     int launches = launchLmInit(S->B, S->opt.initial_lambda, st);
     for (int it = 0; it < iterations; ++it)
         launches += launchIteration(S->B, S->dTiles.p, S->dSlabTile0.p, S->stageStride, S->linSmem, S->facSmem, S->opt.refinement_steps,
-                                    iterations, probe, Sdebug, st);
+                                    iterations, probe, Sdebug, st, S->profile ? profileHook : nullptr, S);
     CK(cudaGetLastError());
     CK(cudaEventRecord(S->ev1, st));
     S->lastLaunches = launches;
@@ -483,6 +523,49 @@ int cgmli_solver_synchronize(cgmli_solver* S) {
     CK(cudaStreamSynchronize(S->stream));
     float ms = 0;
     if (cudaEventElapsedTime(&ms, S->ev0, S->ev1) == cudaSuccess) S->lastMs = ms;
+    if (S->profile) S->collectKernelTimes();
+    return CGMLI_OK;
+}
+
+int cgmli_solver_checkpoint(cgmli_solver* S) {
+    if (!S || S->win.empty()) return fail(CGMLI_E_INVALID, "solver has no windows");
+    CK(cudaSetDevice(S->device));
+    const size_t np = 7ull * S->totalKf, ns = 9ull * S->totalKf, ne = 7ull * S->totalExt, nt = S->win.size(), nl = S->totalLm;
+    CK(S->snapPose.reserve(np)); CK(S->snapSb.reserve(ns)); CK(S->snapExt.reserve(ne)); CK(S->snapTd.reserve(nt));
+    CK(S->snapRho.reserve(nl));
+    CK(cudaMemcpyAsync(S->snapPose.p, S->pose[0].p, np * 8, cudaMemcpyDeviceToDevice, S->stream));
+    CK(cudaMemcpyAsync(S->snapSb.p, S->sb[0].p, ns * 8, cudaMemcpyDeviceToDevice, S->stream));
+    CK(cudaMemcpyAsync(S->snapExt.p, S->ext[0].p, ne * 8, cudaMemcpyDeviceToDevice, S->stream));
+    CK(cudaMemcpyAsync(S->snapTd.p, S->td[0].p, nt * 8, cudaMemcpyDeviceToDevice, S->stream));
+    if (nl) CK(cudaMemcpyAsync(S->snapRho.p, S->rho[0].p, nl * 8, cudaMemcpyDeviceToDevice, S->stream));
+    S->haveSnapshot = true;
+    return CGMLI_OK;
+}
+
+int cgmli_solver_rollback(cgmli_solver* S) {
+    if (!S || !S->haveSnapshot) return fail(CGMLI_E_INVALID, "no checkpoint to roll back to");
+    CK(cudaSetDevice(S->device));
+    const size_t np = 7ull * S->totalKf, ns = 9ull * S->totalKf, ne = 7ull * S->totalExt, nt = S->win.size(), nl = S->totalLm;
+    CK(cudaMemcpyAsync(S->pose[0].p, S->snapPose.p, np * 8, cudaMemcpyDeviceToDevice, S->stream));
+    CK(cudaMemcpyAsync(S->sb[0].p, S->snapSb.p, ns * 8, cudaMemcpyDeviceToDevice, S->stream));
+    CK(cudaMemcpyAsync(S->ext[0].p, S->snapExt.p, ne * 8, cudaMemcpyDeviceToDevice, S->stream));
+    CK(cudaMemcpyAsync(S->td[0].p, S->snapTd.p, nt * 8, cudaMemcpyDeviceToDevice, S->stream));
+    if (nl) CK(cudaMemcpyAsync(S->rho[0].p, S->snapRho.p, nl * 8, cudaMemcpyDeviceToDevice, S->stream));
+    return CGMLI_OK;
+}
+
+int cgmli_solver_kernel_times(cgmli_solver* S, int enable, double* ms, int* calls) {
+    if (!S) return fail(CGMLI_E_INVALID, "null solver");
+    if (enable >= 0) {
+        S->profile = enable != 0;
+        for (int k = 0; k < CGMLI_KERNEL_KINDS; ++k) { S->kernelMs[k] = 0; S->kernelCalls[k] = 0; }
+        S->evUsed.clear();
+        S->evNext = 0;
+    }
+    for (int k = 0; k < CGMLI_KERNEL_KINDS; ++k) {
+        if (ms) ms[k] = S->kernelMs[k];
+        if (calls) calls[k] = S->kernelCalls[k];
+    }
     return CGMLI_OK;
 }
 

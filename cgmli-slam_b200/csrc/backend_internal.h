@@ -84,4 +84,8 @@ struct DevBatch {
     double* out;     // per-window scratch for read-back (costs)
 };
 
+// Called before (phase 0) and after (phase 1) every kernel launch of an
+// iteration; used for per-kernel event timing.
+typedef void (*LaunchHook)(void* ctx, int kind, int phase);
+
 }  // namespace cgmli

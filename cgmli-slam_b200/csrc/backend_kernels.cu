@@ -831,25 +831,44 @@ size_t factorSmemBytes(int maxNr) {
     return (n * (n + 1) / 2 + n) * sizeof(double);
 }
 
+// The dynamic shared-memory cap is a per-function attribute shared by every
+// solver in the process, so it is raised once to the device's opt-in maximum
+// (each launch still requests only what its batch needs).
 cudaError_t configureKernels(size_t linSmem, size_t facSmem) {
-    cudaError_t e = cudaFuncSetAttribute(k_linearize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)linSmem);
+    int device = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)facSmem);
+    cudaFuncAttributes la, fa;
+    if ((e = cudaFuncGetAttributes(&la, k_linearize)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&fa, k_factor)) != cudaSuccess) return e;
+    const size_t linMax = (size_t)optin - la.sharedSizeBytes, facMax = (size_t)optin - fa.sharedSizeBytes;
+    if (linSmem > linMax || facSmem > facMax) return cudaErrorInvalidValue;
+    if ((e = cudaFuncSetAttribute(k_linearize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)linMax)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)facMax);
 }
 
 int launchIteration(const DevBatch& B, const int2* tiles, const int* slabTile0, int stageStride, size_t linSmem, size_t facSmem,
-                    int refinement, int maxIterations, int probe, double* Sdebug, cudaStream_t s) {
+                    int refinement, int maxIterations, int probe, double* Sdebug, cudaStream_t s, LaunchHook hook, void* ctx) {
     const int W = B.numWindows;
     int n = 0;
-    k_zero_acc<<<W, 256, 0, s>>>(B); ++n;
-    if (B.numSlabs > 0) { k_linearize<<<B.numSlabs, kLinThreads, linSmem, s>>>(B, tiles, slabTile0, stageStride); ++n; }
-    k_retained<<<W, 256, 0, s>>>(B, 0); ++n;
-    k_factor<<<W, kFactorThreads, facSmem, s>>>(B, refinement, Sdebug); ++n;
-    k_candidate<<<W, 128, 0, s>>>(B); ++n;
-    if (B.numSlabs > 0) { k_backsub_trial<<<B.numSlabs, kLinThreads, 0, s>>>(B, tiles, slabTile0); ++n; }
-    k_retained<<<W, 256, 0, s>>>(B, 1); ++n;
-    k_lm_update<<<W, 256, 0, s>>>(B, maxIterations, probe); ++n;
-    if (!probe) { k_accept<<<W, 256, 0, s>>>(B); ++n; }
+    auto run = [&](int kind, auto&& launch) {
+        if (hook) hook(ctx, kind, 0);
+        launch();
+        if (hook) hook(ctx, kind, 1);
+        ++n;
+    };
+    run(CGMLI_KERNEL_ZERO, [&] { k_zero_acc<<<W, 256, 0, s>>>(B); });
+    if (B.numSlabs > 0)
+        run(CGMLI_KERNEL_LINEARIZE, [&] { k_linearize<<<B.numSlabs, kLinThreads, linSmem, s>>>(B, tiles, slabTile0, stageStride); });
+    run(CGMLI_KERNEL_RETAINED, [&] { k_retained<<<W, 256, 0, s>>>(B, 0); });
+    run(CGMLI_KERNEL_FACTOR, [&] { k_factor<<<W, kFactorThreads, facSmem, s>>>(B, refinement, Sdebug); });
+    run(CGMLI_KERNEL_CANDIDATE, [&] { k_candidate<<<W, 128, 0, s>>>(B); });
+    if (B.numSlabs > 0)
+        run(CGMLI_KERNEL_BACKSUB_TRIAL, [&] { k_backsub_trial<<<B.numSlabs, kLinThreads, 0, s>>>(B, tiles, slabTile0); });
+    run(CGMLI_KERNEL_RETAINED_TRIAL, [&] { k_retained<<<W, 256, 0, s>>>(B, 1); });
+    run(CGMLI_KERNEL_LM_UPDATE, [&] { k_lm_update<<<W, 256, 0, s>>>(B, maxIterations, probe); });
+    if (!probe) run(CGMLI_KERNEL_ACCEPT, [&] { k_accept<<<W, 256, 0, s>>>(B); });
     return n;
 }
 int launchLmInit(const DevBatch& B, double lambda0, cudaStream_t s) {

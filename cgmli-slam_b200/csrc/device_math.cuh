@@ -127,12 +127,12 @@ __device__ inline void se3LeftJacobianInverse(const double* xi, double* D) {
     if (t < 0.1) {
         c1 = 1.0 / 6 - t2 / 120 + t2 * t2 / 5040 - t2 * t2 * t2 / 362880;
         c2 = 1.0 / 24 - t2 / 720 + t2 * t2 / 40320 - t2 * t2 * t2 / 3628800;
-        c3 = 0.5 * (c2 + 3 * (1.0 / 120 - t2 / 5040 + t2 * t2 / 362880 - t2 * t2 * t2 / 39916800));
+        c3 = 0.5 * (c2 - 3 * (1.0 / 120 - t2 / 5040 + t2 * t2 / 362880 - t2 * t2 * t2 / 39916800));
     } else {
         const double s = sin(t), c = cos(t);
         c1 = (t - s) / (t2 * t);
         c2 = (t2 / 2 + c - 1) / (t2 * t2);
-        c3 = 0.5 * (c2 - 3 * (t - s - t2 * t / 6) / (t2 * t2 * t));
+        c3 = 0.5 * (c2 + 3 * (t - s - t2 * t / 6) / (t2 * t2 * t));
     }
     const double cj = t2 < 1e-10 ? 1.0 / 12 + t2 / 720 : (1 - 0.5 * t / tan(0.5 * t)) / t2;
     const m3 WR = mul(W, R), RW = mul(R, W), WRW = mul(WR, W);

@@ -8,6 +8,8 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import os
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field, replace
 
 import numpy as np
@@ -150,13 +152,20 @@ class SynthWindow:
         return out
 
 
-def make_windows(spec_or_name, count: int, seed: int = 0) -> list[SynthWindow]:
-    """``count`` windows with consecutive seeds; ``"c4"`` draws sizes per window."""
+def make_windows(spec_or_name, count: int, seed: int = 0, threads: int | None = None) -> list[SynthWindow]:
+    """``count`` windows with consecutive seeds; ``"c4"`` draws sizes per window.
+
+    Generation runs on a thread pool (the C generator releases the GIL)."""
     if spec_or_name == "c4":
         rng = np.random.default_rng(seed)
-        return [SynthWindow(c4_spec(rng), seed + i) for i in range(count)]
-    spec = {"c1": C1, "c2": C2, "c3": C3}.get(spec_or_name, spec_or_name)
-    return [SynthWindow(spec, seed + i) for i in range(count)]
+        specs = [c4_spec(rng) for _ in range(count)]
+    else:
+        spec = {"c1": C1, "c2": C2, "c3": C3}.get(spec_or_name, spec_or_name)
+        specs = [spec] * count
+    lib()
+    threads = threads or min(32, os.cpu_count() or 1)
+    with ThreadPoolExecutor(max_workers=threads) as pool:
+        return list(pool.map(lambda i: SynthWindow(specs[i], seed + i), range(count)))
 
 
 def window_array(windows: list[SynthWindow]):

@@ -466,15 +466,25 @@ std::unique_ptr<Store> make(const Params& P, uint64_t seed) {
         for (int i = 0; i < 3; ++i) s.trueExt[7 * e + i] = tBRtrue[e][i];
         setQuat(&s.trueExt[7 * e + 3], RBRtrue[e]);
     }
-    // Landmarks and tracks.
-    auto camPose = [&](int k, int c, M3& R, V3& t) {
-        R = mul(Rwb[k], RBCt[c]);
-        t = add(mv(Rwb[k], tBCt[c]), pwb[k]);
-    };
+    // Landmarks and tracks.  Camera poses at keyframe times (and +-1 ms for
+    // bearing velocities) are computed once.
+    std::vector<M3> Rwc((size_t)K * C), Rwp((size_t)K * C), Rwm((size_t)K * C);
+    std::vector<V3> twc((size_t)K * C), twp((size_t)K * C), twm((size_t)K * C);
+    const double ve = 1e-3;
+    for (int k = 0; k < K; ++k) {
+        const M3 Rp = tj.R(tk[k] + ve), Rm = tj.R(tk[k] - ve);
+        const V3 pp = tj.p(tk[k] + ve), pm = tj.p(tk[k] - ve);
+        for (int c = 0; c < C; ++c) {
+            const size_t i = (size_t)k * C + c;
+            Rwc[i] = mul(Rwb[k], RBCt[c]); twc[i] = add(mv(Rwb[k], tBCt[c]), pwb[k]);
+            Rwp[i] = mul(Rp, RBCt[c]); twp[i] = add(mv(Rp, tBCt[c]), pp);
+            Rwm[i] = mul(Rm, RBCt[c]); twm[i] = add(mv(Rm, tBCt[c]), pm);
+        }
+    }
+    auto camPose = [&](int k, int c, M3& R, V3& t) { R = Rwc[(size_t)k * C + c]; t = twc[(size_t)k * C + c]; };
     auto project = [&](const V3& pW, int k, int c, double& u, double& v, V3& pc) {
-        M3 R; V3 t;
-        camPose(k, c, R, t);
-        pc = mv(tr(R), sub(pW, t));
+        const size_t i = (size_t)k * C + c;
+        pc = mv(tr(Rwc[i]), sub(pW, twc[i]));
         if (pc[2] < 0.1) return false;
         u = cam.fx * pc[0] / pc[2] + cam.cx;
         v = cam.fy * pc[1] / pc[2] + cam.cy;
@@ -482,14 +492,9 @@ std::unique_ptr<Store> make(const Params& P, uint64_t seed) {
     };
     auto bearingVelocity = [&](const V3& pW, int k, int c) {
         // d/dt of the unit bearing at keyframe time, from the true motion.
-        const double e = 1e-3;
-        auto bearingAt = [&](double t) {
-            const M3 R = mul(tj.R(t), RBCt[c]);
-            const V3 tt = add(mv(tj.R(t), tBCt[c]), tj.p(t));
-            const V3 pc = mv(tr(R), sub(pW, tt));
-            return scl(1 / nrm(pc), pc);
-        };
-        return scl(1 / (2 * e), sub(bearingAt(tk[k] + e), bearingAt(tk[k] - e)));
+        const size_t i = (size_t)k * C + c;
+        const V3 a = mv(tr(Rwp[i]), sub(pW, twp[i])), b = mv(tr(Rwm[i]), sub(pW, twm[i]));
+        return scl(1 / (2 * ve), sub(scl(1 / nrm(a), a), scl(1 / nrm(b), b)));
     };
     const double sigma = P.pixel_sigma;
     s.lmBegin.push_back(0);
@@ -525,7 +530,10 @@ std::unique_ptr<Store> make(const Params& P, uint64_t seed) {
                     std::min(cam.height - 1e-3, std::max(0.0, v0 + sigma * N01(rng))), sigma, ab, Pa)) continue;
         s.lmKf.push_back(a); s.lmCam.push_back(ca);
         for (int i = 0; i < 3; ++i) s.lmBearing.push_back(ab[i]);
-        const V3 av = P.with_velocity ? bearingVelocity(pW, a, ca) : V3{0, 0, 0};
+        // bearing velocities are tangent to the measured bearing (the factor's
+        // time model moves the measured ray along a great circle)
+        auto tangent = [](const V3& v, const V3& b) { return sub(v, scl(dot(v, b), b)); };
+        const V3 av = P.with_velocity ? tangent(bearingVelocity(pW, a, ca), ab) : V3{0, 0, 0};
         for (int i = 0; i < 3; ++i) s.lmVel.push_back(av[i]);
         s.trueRho.push_back(1.0 / dist);
         s.rho.push_back((1.0 / dist) * std::max(0.2, 1 + 0.05 * N01(rng)));
@@ -542,7 +550,7 @@ std::unique_ptr<Store> make(const Params& P, uint64_t seed) {
             s.obsKf.push_back(cd.k); s.obsCam.push_back(cd.c);
             for (int i = 0; i < 3; ++i) s.obsBearing.push_back(b[i]);
             for (int i = 0; i < 6; ++i) s.obsP.push_back(Pm[i]);
-            const V3 bv = P.with_velocity ? bearingVelocity(pW, cd.k, cd.c) : V3{0, 0, 0};
+            const V3 bv = P.with_velocity ? tangent(bearingVelocity(pW, cd.k, cd.c), b) : V3{0, 0, 0};
             for (int i = 0; i < 3; ++i) s.obsVel.push_back(bv[i]);
             s.obsOutlier.push_back(outlier);
         }

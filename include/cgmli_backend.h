@@ -174,6 +174,21 @@ int cgmli_solver_window_dims(cgmli_solver *solver, int window, int *retained, in
  * with CUDA events on the solver's stream, and the number of kernel launches. */
 int cgmli_solver_last_timing(cgmli_solver *solver, double *milliseconds, int *launches);
 
+/* Device-side snapshot of the accepted states and its restore: the numeric
+ * checkpoint / rollback of a backend transaction
+ * (src/backend/BackendOptimizer.cpp:609-641, FixedLagBackend.cpp:171-179). */
+int cgmli_solver_checkpoint(cgmli_solver *solver);
+int cgmli_solver_rollback(cgmli_solver *solver);
+
+/* Per-kernel CUDA-event timing.  enable=1 starts recording events around every
+ * launch (and clears the totals); ms[k] / calls[k] return the accumulated time
+ * and launch count of kernel kind k since then, for k in
+ * CGMLI_KERNEL_* (ms and calls hold CGMLI_KERNEL_KINDS entries). */
+enum { CGMLI_KERNEL_ZERO = 0, CGMLI_KERNEL_LINEARIZE, CGMLI_KERNEL_RETAINED, CGMLI_KERNEL_FACTOR, CGMLI_KERNEL_CANDIDATE,
+       CGMLI_KERNEL_BACKSUB_TRIAL, CGMLI_KERNEL_RETAINED_TRIAL, CGMLI_KERNEL_LM_UPDATE, CGMLI_KERNEL_ACCEPT,
+       CGMLI_KERNEL_KINDS };
+int cgmli_solver_kernel_times(cgmli_solver *solver, int enable, double *ms, int *calls);
+
 /* Schur marginalization of one keyframe per window at the current states
  * (Marginalizer::compute, src/backend/Marginalizer.cpp:284-474, with the
  * elimination set of SlidingWindowManager::marginalize,

@@ -134,12 +134,12 @@ static void se3LeftJacobianInverse(const double* xi, double* D /*6x6 row-major*/
     if (t < 0.1) {
         c1 = 1.0 / 6 - t2 / 120 + t2 * t2 / 5040 - t2 * t2 * t2 / 362880;
         c2 = 1.0 / 24 - t2 / 720 + t2 * t2 / 40320 - t2 * t2 * t2 / 3628800;
-        c3 = 0.5 * (c2 + 3 * (1.0 / 120 - t2 / 5040 + t2 * t2 / 362880 - t2 * t2 * t2 / 39916800));
+        c3 = 0.5 * (c2 - 3 * (1.0 / 120 - t2 / 5040 + t2 * t2 / 362880 - t2 * t2 * t2 / 39916800));
     } else {
         const double s = std::sin(t), c = std::cos(t);
         c1 = (t - s) / (t2 * t);
         c2 = (t2 / 2 + c - 1) / (t2 * t2);
-        c3 = 0.5 * (c2 - 3 * (t - s - t2 * t / 6) / (t2 * t2 * t));
+        c3 = 0.5 * (c2 + 3 * (t - s - t2 * t / 6) / (t2 * t2 * t));
     }
     cj = t2 < 1e-10 ? 1.0 / 12 + t2 / 720 : (1 - 0.5 * t / std::tan(0.5 * t)) / t2;
     const M3 WR = mul(W, R), RW = mul(R, W), WRW = mul(WR, W);
@@ -1483,6 +1483,30 @@ int oracle_lm_solve_batch(cgmli_window* windows, int count, int max_iterations, 
     for (int t = 0; t < threads; ++t) pool.emplace_back(work);
     for (auto& t : pool) t.join();
     return worst;
+}
+
+// Robust normal equations of one residual block (rows x cols, row-major J):
+// Ceres' Huber corrector scales r and J by sqrt(rho') (rho'' <= 0), as
+// Marginalizer::linearize / accumulateNormalEquations consume them
+// (Marginalizer.cpp:18-64,185-198).
+int oracle_robust_normal(int rows, int cols, const double* J, const double* r, double huber, double* H, double* g, double* cost,
+                         double* rss) {
+    double s = 0;
+    for (int i = 0; i < rows; ++i) s += r[i] * r[i];
+    const double w = orc::huberWeight(huber, s);
+    *cost = orc::huberCost(huber, s);
+    *rss = w * w * s;
+    for (int a = 0; a < cols; ++a) {
+        double v = 0;
+        for (int i = 0; i < rows; ++i) v += J[(size_t)i * cols + a] * r[i];
+        g[a] = w * w * v;
+        for (int b = 0; b < cols; ++b) {
+            double h = 0;
+            for (int i = 0; i < rows; ++i) h += J[(size_t)i * cols + a] * J[(size_t)i * cols + b];
+            H[(size_t)a * cols + b] = w * w * h;
+        }
+    }
+    return CGMLI_OK;
 }
 
 int oracle_eigen_sym(int n, const double* H, double* evals, double* evecs) {

@@ -54,6 +54,7 @@ def lib() -> C.CDLL:
         P(L, "oracle_window_cost", C.c_int, [W, dp])
         P(L, "oracle_lm_solve", C.c_int, [W, C.c_int, C.c_double, C.c_int, C.POINTER(abi.SolveReport)])
         P(L, "oracle_lm_solve_batch", C.c_int, [W, C.c_int, C.c_int, C.c_int, C.POINTER(abi.SolveReport)])
+        P(L, "oracle_robust_normal", C.c_int, [C.c_int, C.c_int, dp, dp, C.c_double, dp, dp, dp, dp])
         P(L, "oracle_eigen_sym", C.c_int, [C.c_int, dp, dp, dp])
         P(L, "oracle_psd_solve", C.c_int, [C.c_int, dp, C.c_int, dp, C.c_double, C.c_double, dp])
         P(L, "oracle_marginalize_system", C.c_int,
@@ -100,6 +101,14 @@ def window_cost(win):
     c = np.zeros(1)
     st = lib().oracle_window_cost(C.byref(win), _p(c))
     return st, float(c[0])
+
+
+def robust_normal(J, r, huber):
+    J = np.ascontiguousarray(J, dtype=np.float64); r = np.ascontiguousarray(r, dtype=np.float64)
+    rows, cols = J.shape
+    H = np.zeros((cols, cols)); g = np.zeros(cols); cost = np.zeros(1); rss = np.zeros(1)
+    lib().oracle_robust_normal(rows, cols, _p(J), _p(r), huber, _p(H), _p(g), _p(cost), _p(rss))
+    return H, g, float(cost[0]), float(rss[0])
 
 
 def eigen_sym(H):
