@@ -4,7 +4,8 @@
 // The reference rebuilds CSR rows, columns and per-point support sets on the
 // host for every new topology (VisualCudaBatch.cu:450-490) and ping-pongs
 // the host every LM iteration (:595-597).  Here the topology is built once per
-// set of windows (support sets, tiles of <= 32 observations, slabs of tiles)
+// set of windows (support sets, landmarks sorted by support, tiles of <= 32
+// observations, warp runs of tiles)
 // and the whole LM loop runs on the device.
 #include <cuda_runtime.h>
 
@@ -19,10 +20,10 @@
 #include "backend_internal.h"
 
 namespace cgmli {
-size_t linearizeSmemBytes(int maxNpc, int stageStride);
+size_t linearizeSmemBytes();
 size_t factorSmemBytes(int maxNr);
 cudaError_t configureKernels(size_t linSmem, size_t facSmem);
-int launchIteration(const DevBatch& B, const int2* tiles, const int* slabTile0, int stageStride, size_t linSmem, size_t facSmem,
+int launchIteration(const DevBatch& B, const int4* runs, const int2* tiles, size_t linSmem, size_t facSmem,
                     int refinement, int maxIterations, int probe, double* Sdebug, cudaStream_t s, LaunchHook hook, void* ctx);
 int launchLmInit(const DevBatch& B, double lambda0, cudaStream_t s);
 }  // namespace cgmli
@@ -76,25 +77,24 @@ struct cgmli_solver {
     cgmli_solver_options opt{};
     // topology (host copies)
     std::vector<WinDesc> win;
-    std::vector<Slab> slabs;
-    std::vector<int2> tiles;
-    std::vector<int> slabTile0;
-    int stageStride = 0, maxNpc = 0, maxNr = 0;
+    std::vector<int4> runs;       // {window, first tile, end tile, -}
+    std::vector<int2> tiles;      // {first landmark, end landmark} (device order)
+    std::vector<int> lmPerm;      // device landmark -> landmark index within its window
+    int maxNpc = 0, maxNr = 0;
     size_t linSmem = 0, facSmem = 0;
     int totalKf = 0, totalExt = 0, totalCam = 0, totalLm = 0, totalObs = 0, totalImu = 0;
     // device arrays
     DArray<WinDesc> dWin;
     DArray<WinLM> dLm;
-    DArray<Slab> dSlabs;
+    DArray<int4> dRuns;
     DArray<int2> dTiles;
-    DArray<int> dSlabTile0;
     DArray<double> camR, camT;
     DArray<int> camExt;
-    DArray<int> lmWin, lmKf, lmCam, lmObsBegin, lmNs, lmSupp0, supp;
+    DArray<int> lmWin, lmKf, lmCam, lmObsBegin, lmNs, lmNx, lmSupp0, supp, lmGroup;
     DArray<long long> lmC0;
     DArray<double> lmBearing, lmVel, lmTime, lmC, lmD, lmG, lmCost, lmDelta, lmPred, lmTrial, lmMaxInc;
     DArray<int> lmValid, lmTrialValid;
-    DArray<int> obKf, obKfl, obCam, obSlot;
+    DArray<int> obKf, obKfl, obCam, obSlot, obXslot;
     DArray<double> obBearing, obP, obVel, obTime;
     DArray<double> pose[2], sb[2], ext[2], td[2], rho[2];
     DArray<double> imu;
@@ -145,9 +145,9 @@ struct cgmli_solver {
         for (auto* a : dbl) a->release();
         DArray<int>* ints[] = {&camExt, &lmWin, &lmKf, &lmCam, &lmObsBegin, &lmNs, &lmSupp0, &supp, &lmValid, &lmTrialValid, &obKf,
                                &obKfl, &obCam, &obSlot, &imuKf, &priorKind, &priorIndex, &priorCol, &priorOff, &retValid,
-                               &solveStatus, &dSlabTile0};
+                               &solveStatus, &lmGroup, &lmNx, &obXslot};
         for (auto* a : ints) a->release();
-        lmC0.release(); dWin.release(); dLm.release(); dSlabs.release(); dTiles.release();
+        lmC0.release(); dWin.release(); dLm.release(); dRuns.release(); dTiles.release();
         snapPose.release(); snapSb.release(); snapExt.release(); snapTd.release(); snapRho.release();
         for (auto e : evPool) cudaEventDestroy(e);
         if (ev0) cudaEventDestroy(ev0);
@@ -252,28 +252,21 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     cudaStream_t st = S->stream;
     S->win.assign(count, WinDesc{});
     S->haveSnapshot = false;
-    S->slabs.clear(); S->tiles.clear(); S->slabTile0.clear();
-    int kf = 0, ex = 0, cam = 0, lm = 0, ob = 0, im = 0, pblk = 0, vec = 0;
+    S->runs.clear(); S->tiles.clear(); S->lmPerm.clear();
+    int kf = 0, ex = 0, cam = 0, lm = 0, ob = 0, im = 0, pblk = 0, vec = 0, groups = 0;
     long long dense = 0, acc = 0, pA = 0, pR = 0, pRef = 0, imuS = 0, priS = 0, cOff = 0;
-    S->maxNpc = 0; S->maxNr = 0; S->stageStride = 0;
+    S->maxNpc = 0; S->maxNr = 0;
     std::vector<double> camR, camT, lmBearing, lmVel, lmTime, obBearing, obP, obVel, obTime;
-    std::vector<int> camExt, lmWin, lmKf, lmCam, lmObsBegin, lmNs, lmSupp0, supp, obKf, obKfl, obCam, obSlot, imuKf;
+    std::vector<int> camExt, lmWin, lmKf, lmCam, lmObsBegin, lmNs, lmNx, lmSupp0, supp, lmGroup, obKf, obKfl, obCam, obSlot, obXslot, imuKf;
     std::vector<long long> lmC0;
     std::vector<int> priorKind, priorIndex, priorCol, priorOff;
     std::vector<double> priorA, priorR0, priorRef, imuData;
     std::vector<double> pose, sbv, extv, tdv, rhov;
-    // total tiles first (slab sizing)
-    long long totalTiles = 0;
-    for (int i = 0; i < count; ++i) {
-        const auto& w = windows[i];
-        int acc32 = 0;
-        for (int l = 0; l < w.num_landmarks; ++l) {
-            const int n = w.lm_obs_begin[l + 1] - w.lm_obs_begin[l];
-            if (acc32 == 0 || acc32 + n > kMaxTrackChunk) { ++totalTiles; acc32 = 0; }
-            acc32 += n;
-        }
-    }
-    int tilesPerSlab = S->opt.slabs_per_window > 0 ? 0 : (int)std::min<long long>(64, std::max<long long>(1, (totalTiles + 295) / 296));
+    long long totalLm = 0;
+    for (int i = 0; i < count; ++i) totalLm += windows[i].num_landmarks;
+    // landmarks per warp run: enough runs to fill the GPU, long runs for large batches
+    const long long targetRuns = 148ll * 6 * 4;
+    const int runLen = (int)std::max<long long>(4, std::min<long long>(64, totalLm / targetRuns));
     for (int i = 0; i < count; ++i) {
         const auto& w = windows[i];
         WinDesc& d = S->win[i];
@@ -291,75 +284,106 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
         vec += d.Nr;
         dense += (long long)d.Nr * d.Nr;
         acc += (long long)d.Npc * (d.Npc + 1) / 2 + 3ll * d.Npc;
-        // states
         pose.insert(pose.end(), w.poses, w.poses + 7 * d.K);
         sbv.insert(sbv.end(), w.speed_bias, w.speed_bias + 9 * d.K);
         extv.insert(extv.end(), w.extrinsics, w.extrinsics + 7 * d.E);
         tdv.push_back(w.td ? *w.td : 0.0);
-        rhov.insert(rhov.end(), w.rho, w.rho + d.L);
-        // rig
         camR.insert(camR.end(), w.cam_R, w.cam_R + 9 * d.C);
         camT.insert(camT.end(), w.cam_t, w.cam_t + 3 * d.C);
         for (int c = 0; c < d.C; ++c) camExt.push_back(ex + w.cam_ext[c]);
-        // landmarks, support sets and observations
-        int slabTiles = 0, tileObs = 0, tileStage = 0;
-        const int tps = S->opt.slabs_per_window > 0
-                            ? std::max(1, (int)((d.L + 1) / std::max(1, S->opt.slabs_per_window)))
-                            : tilesPerSlab;
-        auto closeTile = [&](int lEnd) {
-            if (!S->tiles.empty() && S->tiles.back().y < 0) S->tiles.back().y = lEnd;
-        };
+        // support of each landmark: keyframes (anchor first, then observers
+        // ascending), then the extrinsic blocks its observations touch (the
+        // anchor camera's first, then the others ascending) when estimated
+        std::vector<std::vector<int>> sup(d.L);
+        std::vector<int> nkf(d.L), nx(d.L);
         for (int l = 0; l < d.L; ++l) {
-            const int b = w.lm_obs_begin[l], e = w.lm_obs_begin[l + 1];
             const int a = w.lm_anchor_kf[l];
-            std::vector<int> kfs{a};
-            for (int f = b; f < e; ++f)
+            std::vector<int> kfs{a}, exs;
+            if (d.estExt) exs.push_back(w.cam_ext[w.lm_anchor_cam[l]]);
+            for (int f = w.lm_obs_begin[l]; f < w.lm_obs_begin[l + 1]; ++f) {
                 if (std::find(kfs.begin(), kfs.end(), w.obs_kf[f]) == kfs.end()) kfs.push_back(w.obs_kf[f]);
+                const int e = w.cam_ext[w.obs_cam[f]];
+                if (d.estExt && std::find(exs.begin(), exs.end(), e) == exs.end()) exs.push_back(e);
+            }
             std::sort(kfs.begin() + 1, kfs.end());
+            if (exs.size() > 1) std::sort(exs.begin() + 1, exs.end());
             if ((int)kfs.size() > kMaxSupport) return fail(CGMLI_E_LIMIT, "landmark support above 64 keyframes");
-            const int ns = 6 * (int)kfs.size() + d.ncalib;
-            // tile / slab bookkeeping (tiles never mix windows)
-            const int nobs = e - b;
-            if (l == 0 || tileObs + nobs > kMaxTrackChunk) {
-                closeTile(lm + l);
-                if (l == 0 || slabTiles >= (tps > 0 ? tps : 1)) {
-                    S->slabs.push_back(Slab{i, lm + l, 0, 0});
-                    S->slabTile0.push_back((int)S->tiles.size());
-                    slabTiles = 0;
-                }
-                S->tiles.push_back(make_int2(lm + l, -1));
-                ++slabTiles;
-                tileObs = 0;
-                tileStage = 0;
+            nkf[l] = (int)kfs.size();
+            nx[l] = (int)exs.size();
+            sup[l] = kfs;
+            sup[l].push_back(-1);  // separator keeps keyframe and extrinsic lists distinct in the sort key
+            sup[l].insert(sup[l].end(), exs.begin(), exs.end());
+        }
+        // device order: landmarks sorted by support (stable), so that equal supports are adjacent
+        std::vector<int> order(d.L);
+        for (int l = 0; l < d.L; ++l) order[l] = l;
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+            if (sup[x].size() != sup[y].size()) return sup[x].size() < sup[y].size();
+            return sup[x] < sup[y];
+        });
+        int tileObs = 0, runTiles = 0, runLms = 0;
+        for (int q = 0; q < d.L; ++q) {
+            const int l = order[q];
+            const auto& key = sup[l];
+            const int ns = 6 * (nkf[l] + nx[l]) + (d.estTd ? 1 : 0);
+            const bool newGroup = q == 0 || sup[order[q - 1]] != key;
+            if (newGroup) ++groups;
+            const int b = w.lm_obs_begin[l], e = w.lm_obs_begin[l + 1], nobs = e - b;
+            // run / tile bookkeeping: runs end at group boundaries once long enough
+            if (q == 0 || (runLms >= runLen && newGroup) || runLms >= 4 * runLen) {
+                if (!S->runs.empty() && S->runs.back().z < 0) S->runs.back().z = (int)S->tiles.size();
+                if (!S->tiles.empty() && S->tiles.back().y < 0) S->tiles.back().y = lm + q;
+                S->runs.push_back(make_int4(i, (int)S->tiles.size(), -1, 0));
+                S->tiles.push_back(make_int2(lm + q, -1));
+                tileObs = 0; runLms = 0; runTiles = 1;
+            } else if (tileObs + nobs > kMaxTrackChunk) {
+                S->tiles.back().y = lm + q;
+                S->tiles.push_back(make_int2(lm + q, -1));
+                tileObs = 0; ++runTiles;
             }
             tileObs += nobs;
-            tileStage += ns;
-            S->stageStride = std::max(S->stageStride, tileStage);
+            ++runLms;
+            S->lmPerm.push_back(l);
+            lmGroup.push_back(groups);
             lmWin.push_back(i);
-            lmKf.push_back(kf + a);
+            lmKf.push_back(kf + w.lm_anchor_kf[l]);
             lmCam.push_back(cam + w.lm_anchor_cam[l]);
-            lmObsBegin.push_back(ob + b);
+            lmObsBegin.push_back(ob + (int)obKf.size() - ob);
             for (int k = 0; k < 3; ++k) lmBearing.push_back(w.lm_anchor_bearing[3 * l + k]);
             for (int k = 0; k < 3; ++k) lmVel.push_back(w.lm_anchor_velocity ? w.lm_anchor_velocity[3 * l + k] : 0.0);
             lmTime.push_back(w.lm_anchor_time ? w.lm_anchor_time[l] : 0.0);
-            lmNs.push_back((int)kfs.size());
+            lmNs.push_back(nkf[l]);
+            lmNx.push_back(nx[l]);
             lmSupp0.push_back((int)supp.size());
-            supp.insert(supp.end(), kfs.begin(), kfs.end());
+            supp.insert(supp.end(), key.begin(), key.begin() + nkf[l]);
+            supp.insert(supp.end(), key.begin() + nkf[l] + 1, key.end());
             lmC0.push_back(cOff);
             cOff += ns;
-            for (int f = b; f < e; ++f) {
+            rhov.push_back(w.rho[l]);
+            // observations of the landmark sorted by observer keyframe (slot order)
+            std::vector<int> fo(nobs);
+            for (int k = 0; k < nobs; ++k) fo[k] = b + k;
+            std::stable_sort(fo.begin(), fo.end(), [&](int x, int y) { return w.obs_kf[x] < w.obs_kf[y]; });
+            for (int f : fo) {
                 obKf.push_back(kf + w.obs_kf[f]);
                 obKfl.push_back(w.obs_kf[f]);
                 obCam.push_back(cam + w.obs_cam[f]);
-                obSlot.push_back((int)(std::find(kfs.begin(), kfs.end(), w.obs_kf[f]) - kfs.begin()));
+                obSlot.push_back((int)(std::find(key.begin(), key.begin() + nkf[l], w.obs_kf[f]) - key.begin()));
+                {
+                    const auto xb = key.begin() + nkf[l] + 1;
+                    obXslot.push_back(d.estExt ? (int)(std::find(xb, key.end(), w.cam_ext[w.obs_cam[f]]) - xb) : 0);
+                }
                 for (int k = 0; k < 3; ++k) obBearing.push_back(w.obs_bearing[3 * f + k]);
                 for (int k = 0; k < 6; ++k) obP.push_back(w.obs_P[6 * f + k]);
                 for (int k = 0; k < 3; ++k) obVel.push_back(w.obs_velocity ? w.obs_velocity[3 * f + k] : 0.0);
                 obTime.push_back(w.obs_time ? w.obs_time[f] : 0.0);
             }
         }
-        closeTile(lm + d.L);
-        d.slab0 = 0;
+        if (d.L) {
+            S->tiles.back().y = lm + d.L;
+            S->runs.back().z = (int)S->tiles.size();
+        }
+        (void)runTiles;
         // IMU
         for (int q = 0; q < d.nImu; ++q) {
             const double* raw = reinterpret_cast<const double*>(&w.imu[q]);
@@ -402,28 +426,20 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
         priS += d.priorRank > 0 ? (long long)cols * 7 + d.priorRank + (long long)d.priorRank * cols : 0;
         kf += d.K; ex += d.E; cam += d.C; lm += d.L; ob += d.F; im += d.nImu;
     }
-    for (size_t t = 0; t < S->slabs.size(); ++t) {
-        const int e = t + 1 < S->slabs.size() ? S->slabTile0[t + 1] : (int)S->tiles.size();
-        S->slabs[t].lmEnd = S->tiles[e - 1].y;
-    }
-    S->slabTile0.push_back((int)S->tiles.size());
-    lmObsBegin.push_back(ob);
+    lmObsBegin.push_back((int)obKf.size());
     S->totalKf = kf; S->totalExt = ex; S->totalCam = cam; S->totalLm = lm; S->totalObs = ob; S->totalImu = im;
-    S->stageStride = std::max(8, S->stageStride);
-    S->linSmem = linearizeSmemBytes(S->maxNpc, S->stageStride);
+    S->linSmem = linearizeSmemBytes();
     S->facSmem = factorSmemBytes(S->maxNr);
-    if (S->linSmem > 227 * 1024) return fail(CGMLI_E_LIMIT, "visual accumulator exceeds shared memory");
     CK(configureKernels(S->linSmem, S->facSmem));
-    // uploads
     CK(S->dWin.upload(S->win, st));
     CK(S->dLm.reserve(count));
-    CK(S->dSlabs.upload(S->slabs, st));
+    CK(S->dRuns.upload(S->runs, st));
     CK(S->dTiles.upload(S->tiles, st));
-    CK(S->dSlabTile0.upload(S->slabTile0, st));
     CK(S->camR.upload(camR, st)); CK(S->camT.upload(camT, st)); CK(S->camExt.upload(camExt, st));
     CK(S->lmWin.upload(lmWin, st)); CK(S->lmKf.upload(lmKf, st)); CK(S->lmCam.upload(lmCam, st));
     CK(S->lmObsBegin.upload(lmObsBegin, st)); CK(S->lmNs.upload(lmNs, st)); CK(S->lmSupp0.upload(lmSupp0, st));
-    CK(S->supp.upload(supp, st)); CK(S->lmC0.upload(lmC0, st));
+    CK(S->supp.upload(supp, st)); CK(S->lmC0.upload(lmC0, st)); CK(S->lmGroup.upload(lmGroup, st));
+    CK(S->lmNx.upload(lmNx, st)); CK(S->obXslot.upload(obXslot, st));
     CK(S->lmBearing.upload(lmBearing, st)); CK(S->lmVel.upload(lmVel, st)); CK(S->lmTime.upload(lmTime, st));
     CK(S->obKf.upload(obKf, st)); CK(S->obKfl.upload(obKfl, st)); CK(S->obCam.upload(obCam, st)); CK(S->obSlot.upload(obSlot, st));
     CK(S->obBearing.upload(obBearing, st)); CK(S->obP.upload(obP, st)); CK(S->obVel.upload(obVel, st));
@@ -446,12 +462,13 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     DevBatch& B = S->B;
     B = DevBatch{};
     B.numWindows = count; B.numLandmarks = lm; B.numObs = ob; B.numKf = kf; B.numExt = ex; B.numCam = cam; B.numImu = im;
-    B.numSlabs = (int)S->slabs.size();
-    B.win = S->dWin.p; B.lm = S->dLm.p; B.slabs = S->dSlabs.p;
+    B.numRuns = (int)S->runs.size();
+    B.win = S->dWin.p; B.lm = S->dLm.p;
     B.camR = S->camR.p; B.camT = S->camT.p; B.camExt = S->camExt.p;
     B.lmWin = S->lmWin.p; B.lmKf = S->lmKf.p; B.lmCam = S->lmCam.p; B.lmObsBegin = S->lmObsBegin.p;
     B.lmBearing = S->lmBearing.p; B.lmVel = S->lmVel.p; B.lmTime = S->lmTime.p;
-    B.lmNs = S->lmNs.p; B.lmSupp0 = S->lmSupp0.p; B.supp = S->supp.p; B.lmC0 = S->lmC0.p;
+    B.lmNs = S->lmNs.p; B.lmNx = S->lmNx.p; B.lmSupp0 = S->lmSupp0.p; B.supp = S->supp.p; B.lmC0 = S->lmC0.p;
+    B.lmGroup = S->lmGroup.p; B.obXslot = S->obXslot.p;
     B.lmC = S->lmC.p; B.lmD = S->lmD.p; B.lmG = S->lmG.p; B.lmCost = S->lmCost.p; B.lmValid = S->lmValid.p;
     B.lmDelta = S->lmDelta.p; B.lmPred = S->lmPred.p; B.lmTrial = S->lmTrial.p; B.lmMaxInc = S->lmMaxInc.p;
     B.lmTrialValid = S->lmTrialValid.p;
@@ -485,7 +502,12 @@ int cgmli_solver_upload_states(cgmli_solver* S, const cgmli_window* windows, int
         CK(cudaMemcpyAsync(S->sb[0].p + 9ll * d.kf0, w.speed_bias, 9ll * d.K * sizeof(double), cudaMemcpyHostToDevice, S->stream));
         CK(cudaMemcpyAsync(S->ext[0].p + 7ll * d.ext0, w.extrinsics, 7ll * d.E * sizeof(double), cudaMemcpyHostToDevice, S->stream));
         if (w.td) CK(cudaMemcpyAsync(S->td[0].p + i, w.td, sizeof(double), cudaMemcpyHostToDevice, S->stream));
-        if (d.L) CK(cudaMemcpyAsync(S->rho[0].p + d.lm0, w.rho, d.L * sizeof(double), cudaMemcpyHostToDevice, S->stream));
+        if (d.L) {
+            // device order is sorted by support; lmPerm maps it back to the caller's order
+            std::vector<double> r(d.L);
+            for (int q = 0; q < d.L; ++q) r[q] = w.rho[S->lmPerm[d.lm0 + q]];
+            CK(cudaMemcpy(S->rho[0].p + d.lm0, r.data(), d.L * sizeof(double), cudaMemcpyHostToDevice));
+        }
     }
     return CGMLI_OK;
 }
@@ -503,7 +525,7 @@ static int runIterations(cgmli_solver* S, int iterations, int probe, double* Sde
     CK(cudaEventRecord(S->ev0, st));
     int launches = launchLmInit(S->B, S->opt.initial_lambda, st);
     for (int it = 0; it < iterations; ++it)
-        launches += launchIteration(S->B, S->dTiles.p, S->dSlabTile0.p, S->stageStride, S->linSmem, S->facSmem, S->opt.refinement_steps,
+        launches += launchIteration(S->B, S->dRuns.p, S->dTiles.p, S->linSmem, S->facSmem, S->opt.refinement_steps,
                                     iterations, probe, Sdebug, st, S->profile ? profileHook : nullptr, S);
     CK(cudaGetLastError());
     CK(cudaEventRecord(S->ev1, st));
@@ -600,7 +622,11 @@ int cgmli_solver_read_step(cgmli_solver* S, int w, double* increment, double* co
     CK(cudaMemcpy(&lmst, S->dLm.p + w, sizeof(WinLM), cudaMemcpyDeviceToHost));
     if (increment) {
         CK(cudaMemcpy(increment, S->dr.p + d.vec0, d.Nr * sizeof(double), cudaMemcpyDeviceToHost));
-        if (d.L) CK(cudaMemcpy(increment + d.Nr, S->lmDelta.p + d.lm0, d.L * sizeof(double), cudaMemcpyDeviceToHost));
+        if (d.L) {
+            std::vector<double> r(d.L);
+            CK(cudaMemcpy(r.data(), S->lmDelta.p + d.lm0, d.L * sizeof(double), cudaMemcpyDeviceToHost));
+            for (int q = 0; q < d.L; ++q) increment[d.Nr + S->lmPerm[d.lm0 + q]] = r[q];
+        }
     }
     if (cost) *cost = lmst.linCost;
     if (predicted) *predicted = lmst.predicted;
@@ -644,7 +670,11 @@ int cgmli_solver_read_states(cgmli_solver* S, cgmli_window* windows, int count) 
         CK(cudaMemcpy(w.speed_bias, S->sb[0].p + 9ll * d.kf0, 9ll * d.K * sizeof(double), cudaMemcpyDeviceToHost));
         CK(cudaMemcpy(w.extrinsics, S->ext[0].p + 7ll * d.ext0, 7ll * d.E * sizeof(double), cudaMemcpyDeviceToHost));
         if (w.td) CK(cudaMemcpy(w.td, S->td[0].p + i, sizeof(double), cudaMemcpyDeviceToHost));
-        if (d.L) CK(cudaMemcpy(w.rho, S->rho[0].p + d.lm0, d.L * sizeof(double), cudaMemcpyDeviceToHost));
+        if (d.L) {
+            std::vector<double> r(d.L);
+            CK(cudaMemcpy(r.data(), S->rho[0].p + d.lm0, d.L * sizeof(double), cudaMemcpyDeviceToHost));
+            for (int q = 0; q < d.L; ++q) w.rho[S->lmPerm[d.lm0 + q]] = r[q];
+        }
     }
     return CGMLI_OK;
 }

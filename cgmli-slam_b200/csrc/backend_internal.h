@@ -9,8 +9,9 @@
 //                       then 6 per estimated extrinsic, then td.
 //   visual    [0, Npc)  the columns a bearing factor can touch:
 //                       pose k -> 6k, extrinsic e -> 6K+6e, td -> 6K+6E'.
-//   landmark-local       support slot j -> 6j (slot 0 = anchor keyframe),
-//                       then the window's calibration columns.
+//   landmark-local       keyframe slot j -> 6j (slot 0 = anchor keyframe), then
+//                       one 6-column slot per extrinsic the landmark's observations
+//                       touch (slot 0 = the anchor camera's), then td.
 #pragma once
 #include <cstdint>
 
@@ -45,25 +46,25 @@ struct WinLM {
 };
 enum { kModeLinearize = 0, kModeResolve = 1, kModeDone = 2 };
 
-struct Slab { int win, lmBegin, lmEnd, pad; };
+struct Slab { int win, lmBegin, lmEnd, pad; };  // unused legacy name kept for the layout comment
 
 // Pointers to every device array (filled by the host runtime).
 struct DevBatch {
-    int numWindows, numLandmarks, numObs, numKf, numExt, numCam, numImu, numSlabs;
+    int numWindows, numLandmarks, numObs, numKf, numExt, numCam, numImu, numRuns;
     const WinDesc* win;
     WinLM* lm;
-    const Slab* slabs;
     // cameras
     const double* camR; const double* camT; const int* camExt;  // camExt: global extrinsic index
     // landmarks
     const int* lmWin; const int* lmKf; const int* lmCam; const int* lmObsBegin;  // lmObsBegin: numLandmarks+1
     const double* lmBearing; const double* lmVel; const double* lmTime;
-    const int* lmNs; const int* lmSupp0; const int* supp;  // support keyframes (local index), anchor first
+    const int* lmNs; const int* lmNx; const int* lmSupp0; const int* supp;  // support: s keyframes (anchor first), then x extrinsics
+    const int* lmGroup;                                   // equal for consecutive landmarks with the same support
     const long long* lmC0;                                // offset of the landmark's cross vector
     double* lmC; double* lmD; double* lmG; double* lmCost; int* lmValid;
     double* lmDelta; double* lmPred; double* lmTrial; double* lmMaxInc; int* lmTrialValid;
     // observations
-    const int* obKf; const int* obKfl; const int* obCam; const int* obSlot;
+    const int* obKf; const int* obKfl; const int* obCam; const int* obSlot; const int* obXslot;
     const double* obBearing; const double* obP; const double* obVel; const double* obTime;
     // states: [0] accepted, [1] candidate
     double* pose[2]; double* sb[2]; double* ext[2]; double* td[2]; double* rho[2];

@@ -80,152 +80,233 @@ __global__ void k_zero_acc(DevBatch B) {
 }
 
 // ---------------------------------------------------------------------------------------
-// Linearization of the bearing factors of one slab (contiguous landmarks of
-// one window), fused with the per-landmark Schur complement at the window's
-// current lambda.  Per landmark l with scalar inverse distance:
-//   d_l = sum J_rho^T J_rho, g_l = sum J_rho^T r, c_l = sum J_x^T J_rho
+// Linearization of the bearing factors fused with the per-landmark Schur
+// complement at the window's current lambda.  Per landmark l (scalar inverse
+// distance) with observations f:
+//   d_l = sum J_rho^T J_rho,  g_l = sum J_rho^T r,  c_l = sum J_x^T J_rho
 //   S  += sum_f J_f^T J_f - c_l c_l^T / (d_l + lambda max(d_l, 1e-6))
-//   rhs correction  += c_l g_l / (d_l + lambda max(d_l, 1e-6))
+//   rhs correction += c_l g_l / (d_l + lambda max(d_l, 1e-6))
 // (accumulateVisualPairs + subtractPointSchur, VisualCudaBatch.cu:74-96,149-161).
-// Accumulation is FP64 in shared memory, flushed once per CTA.
-// Warps take tiles of consecutive landmarks holding at most 32 observations;
-// lane = observation.  Tile table: tiles[t] = {lmBegin, lmEnd}.
-__global__ void __launch_bounds__(kLinThreads) k_linearize(DevBatch B, const int2* tiles, const int* slabTile0, int stageStride) {
-    const Slab sl = B.slabs[blockIdx.x];
-    const int wdx = sl.win;
+//
+// Work unit: a run = consecutive landmarks of one window, sorted by their
+// keyframe support, processed by one warp in tiles of <= 32 observations
+// (lane = observation for the evaluation).  The weighted Jacobians of a tile
+// are staged in shared memory; each landmark's dense local block over its
+// support (6 columns per keyframe slot + the calibration columns) is formed
+// with lanes over distinct entries and added to a warp-private FP64 group
+// buffer.  Landmarks with the same support share the buffer; it is flushed to
+// the window accumulator with global FP64 reductions when the support changes.
+constexpr int kLinWarps = 6;
+constexpr int kStage = 56;          // doubles staged per observation
+constexpr int kGroupMaxNs = 64;     // largest support width that is buffered
+constexpr int kGroupBuf = kGroupMaxNs * (kGroupMaxNs + 1) / 2 + 3 * kGroupMaxNs;
+constexpr int kMaxNs = 6 * (kMaxSupport + 8) + 1;
+constexpr int kCompact = 25;        // anchor pose 6 | observer pose 6 | ext_a 6 | ext_b 6 | td 1
+constexpr int kPairs = kCompact * (kCompact + 1) / 2;
+struct LinWarpSmem {
+    double stage[32][kStage];  // compact weighted row pair: row0 at [0,25), row1 at [25,50), Jrho 50,51 | r 52,53 | cost 54
+    short map[32][kCompact];        // local column of each compact column, -1 if absent
+    int flags[32];                  // 1 valid
+    double c[kMaxNs];
+    double gbuf[kGroupBuf];
+};
+__constant__ unsigned char kPairA[kPairs], kPairB[kPairs];
+
+// Local column -> visual column for a support (s keyframe slots, x extrinsic slots, td).
+__device__ __forceinline__ int pcOfLocal(int i, int s, int x, const int* sk, int K, int tdCol) {
+    if (i < 6 * s) return 6 * sk[i / 6] + i % 6;
+    if (i < 6 * (s + x)) return 6 * K + 6 * sk[s + (i - 6 * s) / 6] + i % 6;
+    return tdCol;
+}
+
+// Adds a group buffer (local coordinates of a support) into the window accumulator.
+__device__ void flushGroup(const double* gbuf, int ns, int s, int x, const int* sk, int K, int tdCol, int Npc, double* acc,
+                           int lane) {
+    const int ntri = ns * (ns + 1) / 2;
+    const long long nS = (long long)Npc * (Npc + 1) / 2;
+    int i = 0, j = lane;
+    while (j >= ns && i < ns) { ++i; j = j - ns + i; }
+    for (int e = lane; e < ntri; e += 32) {
+        const double v = gbuf[e];
+        if (v != 0.0) {
+            const int pi = pcOfLocal(i, s, x, sk, K, tdCol), pj = pcOfLocal(j, s, x, sk, K, tdCol);
+            atomicAdd(&acc[pi <= pj ? upIdx(pi, pj, Npc) : upIdx(pj, pi, Npc)], v);
+        }
+        j += 32;
+        while (j >= ns && i < ns) { ++i; j = j - ns + i; }
+    }
+    for (int t = lane; t < 3 * ns; t += 32) {
+        const double v = gbuf[ntri + t];
+        if (v != 0.0) atomicAdd(&acc[nS + (long long)(t / ns) * Npc + pcOfLocal(t % ns, s, x, sk, K, tdCol)], v);
+    }
+}
+
+__device__ __forceinline__ int localUp(int i, int j, int ns) { return i * ns - i * (i - 1) / 2 + (j - i); }
+
+__global__ void __launch_bounds__(kLinWarps * 32) k_linearize(DevBatch B, const int4* runs, const int2* tiles) {
+    extern __shared__ double smemRaw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int runIdx = blockIdx.x * kLinWarps + warp;
+    if (runIdx >= B.numRuns) return;
+    const int4 run = runs[runIdx];  // {window, tile begin, tile end, -}
+    const int wdx = run.x;
     if (B.lm[wdx].mode == kModeDone) return;
+    LinWarpSmem& sm = reinterpret_cast<LinWarpSmem*>(smemRaw)[warp];
     const WinDesc wd = B.win[wdx];
     const double lambda = B.lm[wdx].lambda;
-    extern __shared__ double smem[];
-    const int Npc = wd.Npc, K = wd.K;
-    const long long nS = (long long)Npc * (Npc + 1) / 2;
-    double* Sv = smem;
-    double* Dv = Sv + nS;
-    double* Gv = Dv + Npc;
-    double* Bv = Gv + Npc;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-    double* stage = Bv + Npc + (long long)warp * (stageStride + 4 * 32);
-    double* lmD = stage + stageStride;  // per tile-landmark: d, g, cost, valid
-    double* lmGs = lmD + 32;
-    double* lmCs = lmGs + 32;
-    double* lmVs = lmCs + 32;
-    for (long long i = threadIdx.x; i < nS + 3ll * Npc; i += blockDim.x) smem[i] = 0.0;
-    __syncthreads();
+    const int K = wd.K, Npc = wd.Npc;
     const int tdCol = 6 * K + (wd.estExt ? 6 * wd.E : 0);
-    const int t0 = slabTile0[blockIdx.x], t1 = slabTile0[blockIdx.x + 1];
-    for (int t = t0 + warp; t < t1; t += nwarps) {
+    double* acc = B.acc + wd.acc0;
+    const long long nS = (long long)Npc * (Npc + 1) / 2;
+    int curGroup = -1, curNs = 0, curS = 0, curX = 0;
+    const int* curSk = nullptr;
+    bool buffered = false;
+    for (int t = run.y; t < run.z; ++t) {
         const int2 tile = tiles[t];
-        const int lb = tile.x, le = tile.y, nl = le - lb;
+        const int lb = tile.x, le = tile.y;
         const int ob = B.lmObsBegin[lb], oe = B.lmObsBegin[le];
-        // staging offsets of each landmark's cross vector
-        int stageOff = 0, myStage = 0;
-        for (int q = 0; q < nl; ++q) {
-            const int ns = 6 * B.lmNs[lb + q] + wd.ncalib;
-            if (q == lane) myStage = stageOff;
-            stageOff += ns;
-        }
-        for (int i = lane; i < stageOff; i += 32) stage[i] = 0.0;
-        if (lane < nl) { lmD[lane] = 0; lmGs[lane] = 0; lmCs[lane] = 0; lmVs[lane] = 1; }
-        __syncwarp();
+        // ---- evaluation: lane = observation; stage the weighted compact rows
         const int f = ob + lane;
         if (f < oe) {
-            // landmark of this observation (tiles are small: linear search)
             int q = 0;
             while (B.lmObsBegin[lb + q + 1] <= f) ++q;
             const int l = lb + q;
-            int qs = 0;
-            for (int p = 0; p < q; ++p) qs += 6 * B.lmNs[lb + p] + wd.ncalib;
-            const int s = B.lmNs[l];
-            double* cst = stage + qs;
             FactorIn in;
             int kfa, kfb, ea, eb;
             gatherFactor(B, wd, wdx, l, f, 0, in, kfa, kfb, ea, eb);
             FactorOut o;
+            double* st = sm.stage[lane];
+            short* mp = sm.map[lane];
             const bool ok = evalBearingFactor(in, true, o);
-            if (!ok) {
-                lmVs[q] = 0;  // benign race: every writer stores 0
-            } else {
+            const int s = B.lmNs[l], x = B.lmNx[l];
+            const bool same = in.sameKf && !in.splitExt;
+            const int obSlot = B.obSlot[f], obX = B.obXslot[f];
+            for (int c = 0; c < 6; ++c) {
+                mp[c] = in.sameKf ? -1 : c;
+                mp[6 + c] = in.sameKf ? -1 : 6 * obSlot + c;
+                mp[12 + c] = (wd.estExt && !same) ? 6 * s + c : -1;  // anchor camera's extrinsic = ext slot 0
+                mp[18 + c] = (wd.estExt && in.splitExt) ? 6 * (s + obX) + c : -1;
+            }
+            mp[24] = wd.estTd ? 6 * (s + x) : -1;
+            sm.flags[lane] = ok ? 1 : 0;
+            if (ok) {
                 const double sq = o.r[0] * o.r[0] + o.r[1] * o.r[1];
-                const double wgt = huberWeight(wd.huber, sq);
-                atomicAdd(&lmCs[q], huberCost(wd.huber, sq));
-                const double rw0 = wgt * o.r[0], rw1 = wgt * o.r[1];
-                const double jr0 = wgt * o.Jrho[0], jr1 = wgt * o.Jrho[1];
-                atomicAdd(&lmD[q], jr0 * jr0 + jr1 * jr1);
-                atomicAdd(&lmGs[q], jr0 * rw0 + jr1 * rw1);
-                // retained entries of this factor: (visual column, local column, J row0, J row1)
-                int pcs[25], lcs[25];
-                double j0[25], j1[25];
-                int n = 0;
-                const int kfal = kfa - wd.kf0, kfbl = kfb - wd.kf0;
-                const bool same = in.sameKf && !in.splitExt;
-                if (!in.sameKf) {
-                    const int slot = B.obSlot[f];
-                    for (int c = 0; c < 6; ++c) { pcs[n] = 6 * kfal + c; lcs[n] = c; j0[n] = wgt * o.Ja[c]; j1[n] = wgt * o.Ja[6 + c]; ++n; }
-                    for (int c = 0; c < 6; ++c) { pcs[n] = 6 * kfbl + c; lcs[n] = 6 * slot + c; j0[n] = wgt * o.Jb[c]; j1[n] = wgt * o.Jb[6 + c]; ++n; }
+                const double w = huberWeight(wd.huber, sq);
+#pragma unroll
+                for (int r = 0; r < 2; ++r) {
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) {
+                        st[25 * r + c] = w * o.Ja[6 * r + c];
+                        st[25 * r + 6 + c] = w * o.Jb[6 * r + c];
+                        st[25 * r + 12 + c] = w * o.Jea[6 * r + c];
+                        st[25 * r + 18 + c] = w * o.Jeb[6 * r + c];
+                    }
+                    st[25 * r + 24] = w * o.Jtd[r];
                 }
-                if (wd.estExt && !same) {
-                    const int eal = ea - wd.ext0, ebl = eb - wd.ext0;
-                    for (int c = 0; c < 6; ++c) { pcs[n] = 6 * K + 6 * eal + c; lcs[n] = 6 * s + 6 * eal + c; j0[n] = wgt * o.Jea[c]; j1[n] = wgt * o.Jea[6 + c]; ++n; }
-                    if (in.splitExt)
-                        for (int c = 0; c < 6; ++c) { pcs[n] = 6 * K + 6 * ebl + c; lcs[n] = 6 * s + 6 * ebl + c; j0[n] = wgt * o.Jeb[c]; j1[n] = wgt * o.Jeb[6 + c]; ++n; }
+                st[50] = w * o.Jrho[0]; st[51] = w * o.Jrho[1];
+                st[52] = w * o.r[0]; st[53] = w * o.r[1];
+                st[54] = huberCost(wd.huber, sq);
+            } else {
+                for (int k = 0; k < kStage; ++k) st[k] = 0.0;
+            }
+        }
+        __syncwarp();
+        // ---- per landmark of the tile
+        for (int l = lb; l < le; ++l) {
+            const int fb = B.lmObsBegin[l] - ob, fe = B.lmObsBegin[l + 1] - ob;
+            const int s = B.lmNs[l], x = B.lmNx[l], ns = 6 * (s + x) + (wd.estTd ? 1 : 0);
+            const int* sk = B.supp + B.lmSupp0[l];
+            const int group = B.lmGroup[l];
+            if (group != curGroup) {
+                if (buffered) { __syncwarp(); flushGroup(sm.gbuf, curNs, curS, curX, curSk, K, tdCol, Npc, acc, lane); }
+                curGroup = group; curNs = ns; curS = s; curX = x; curSk = sk;
+                buffered = ns <= kGroupMaxNs;
+                __syncwarp();
+                if (buffered) {
+                    const int n = ns * (ns + 1) / 2 + 3 * ns;
+                    for (int e = lane; e < n; e += 32) sm.gbuf[e] = 0.0;
                 }
-                if (wd.estTd) { pcs[n] = tdCol; lcs[n] = 6 * s + (tdCol - 6 * K); j0[n] = wgt * o.Jtd[0]; j1[n] = wgt * o.Jtd[1]; ++n; }
-                for (int a = 0; a < n; ++a) {
-                    atomicAdd(&Dv[pcs[a]], j0[a] * j0[a] + j1[a] * j1[a]);
-                    atomicAdd(&Gv[pcs[a]], j0[a] * rw0 + j1[a] * rw1);
-                    atomicAdd(&cst[lcs[a]], j0[a] * jr0 + j1[a] * jr1);
-                    for (int b = a; b < n; ++b) {
-                        const int pa = pcs[a], pb = pcs[b];
-                        const long long idx = pa <= pb ? upIdx(pa, pb, Npc) : upIdx(pb, pa, Npc);
-                        const double v = (j0[a] * j0[b] + j1[a] * j1[b]) * (pa == pb && a != b ? 2.0 : 1.0);
-                        atomicAdd(&Sv[idx], v);
+                __syncwarp();
+            }
+            const int ntri = ns * (ns + 1) / 2;
+            // scalars: d, g, cost, validity
+            double d = 0, g = 0, cost = 0;
+            int valid = 1;
+            for (int k = fb + lane; k < fe; k += 32) {
+                const double* st = sm.stage[k];
+                d += st[50] * st[50] + st[51] * st[51];
+                g += st[50] * st[52] + st[51] * st[53];
+                cost += st[54];
+                valid &= sm.flags[k];
+            }
+            d = warpSum(d); g = warpSum(g); cost = warpSum(cost);
+            valid = __all_sync(0xffffffffu, valid);
+            const double inv = 1.0 / (d + lambda * fmax(d, 1e-6));
+            for (int i = lane; i < ns; i += 32) sm.c[i] = 0.0;
+            __syncwarp();
+            // per observation: cross vector, diag(H) and gradient over the compact columns
+            for (int k = fb; k < fe; ++k) {
+                const double* st = sm.stage[k];
+                const short* mp = sm.map[k];
+                if (lane < kCompact) {
+                    const int li = mp[lane];
+                    if (li >= 0) {
+                        const double a0 = st[lane], a1 = st[25 + lane];
+                        sm.c[li] += a0 * st[50] + a1 * st[51];
+                        const double hd = a0 * a0 + a1 * a1, gr = a0 * st[52] + a1 * st[53];
+                        if (buffered) { sm.gbuf[ntri + li] += hd; sm.gbuf[ntri + ns + li] += gr; }
+                        else {
+                            const int p = pcOfLocal(li, s, x, sk, K, tdCol);
+                            atomicAdd(&acc[nS + p], hd);
+                            atomicAdd(&acc[nS + Npc + p], gr);
+                        }
                     }
                 }
+                __syncwarp();
+                // J^T J over the compact pairs
+                for (int pidx = lane; pidx < kPairs; pidx += 32) {
+                    const int a = kPairA[pidx], b = kPairB[pidx];
+                    const int la = mp[a], lb2 = mp[b];
+                    if (la < 0 || lb2 < 0) continue;
+                    const double v = st[a] * st[b] + st[25 + a] * st[25 + b];
+                    if (v == 0.0) continue;
+                    const int i = la < lb2 ? la : lb2, j = la < lb2 ? lb2 : la;
+                    if (buffered) sm.gbuf[localUp(i, j, ns)] += v;
+                    else {
+                        const int pi = pcOfLocal(i, s, x, sk, K, tdCol), pj = pcOfLocal(j, s, x, sk, K, tdCol);
+                        atomicAdd(&acc[pi <= pj ? upIdx(pi, pj, Npc) : upIdx(pj, pi, Npc)], v);
+                    }
+                }
+                __syncwarp();
             }
-        }
-        __syncwarp();
-        // per-landmark Schur complement, one landmark at a time across the warp
-        int qs = 0;
-        for (int q = 0; q < nl; ++q) {
-            const int l = lb + q;
-            const int s = B.lmNs[l], ns = 6 * s + wd.ncalib;
-            const double d = lmD[q], g = lmGs[q];
-            const double* c = stage + qs;
-            const double inv = 1.0 / (d + lambda * fmax(d, 1e-6));
-            const int* sk = B.supp + B.lmSupp0[l];
+            // Schur complement of the inverse distance and the rhs correction
             const long long c0 = B.lmC0[l];
             for (int i = lane; i < ns; i += 32) {
-                const double ci = c[i];
+                const double ci = sm.c[i];
                 B.lmC[c0 + i] = ci;
-                const int pi = i < 6 * s ? 6 * sk[i / 6] + i % 6 : 6 * K + (i - 6 * s);
-                atomicAdd(&Bv[pi], inv * ci * g);
+                const double bc = inv * ci * g;
+                if (buffered) sm.gbuf[ntri + 2 * ns + i] += bc;
+                else if (bc != 0.0) atomicAdd(&acc[nS + 2ll * Npc + pcOfLocal(i, s, x, sk, K, tdCol)], bc);
             }
-            for (int i = 0; i < ns; ++i) {
-                const double ci = c[i];
-                if (ci == 0.0) continue;
-                const int pi = i < 6 * s ? 6 * sk[i / 6] + i % 6 : 6 * K + (i - 6 * s);
-                for (int j = i + lane; j < ns; j += 32) {
-                    const double cj = c[j];
-                    if (cj == 0.0) continue;
-                    const int pj = j < 6 * s ? 6 * sk[j / 6] + j % 6 : 6 * K + (j - 6 * s);
-                    const long long idx = pi <= pj ? upIdx(pi, pj, Npc) : upIdx(pj, pi, Npc);
-                    atomicAdd(&Sv[idx], -inv * ci * cj * (pi == pj && i != j ? 2.0 : 1.0));
+            {
+                int i = 0, j = lane;
+                while (j >= ns && i < ns) { ++i; j = j - ns + i; }
+                for (int e = lane; e < ntri; e += 32) {
+                    const double v = -inv * sm.c[i] * sm.c[j];
+                    if (buffered) sm.gbuf[e] += v;
+                    else if (v != 0.0) {
+                        const int pi = pcOfLocal(i, s, x, sk, K, tdCol), pj = pcOfLocal(j, s, x, sk, K, tdCol);
+                        atomicAdd(&acc[pi <= pj ? upIdx(pi, pj, Npc) : upIdx(pj, pi, Npc)], v);
+                    }
+                    j += 32;
+                    while (j >= ns && i < ns) { ++i; j = j - ns + i; }
                 }
             }
-            if (lane == 0) {
-                B.lmD[l] = d; B.lmG[l] = g; B.lmCost[l] = lmCs[q]; B.lmValid[l] = lmVs[q] != 0.0;
-            }
-            qs += ns;
+            if (lane == 0) { B.lmD[l] = d; B.lmG[l] = g; B.lmCost[l] = cost; B.lmValid[l] = valid; }
+            __syncwarp();
         }
-        (void)myStage;
-        __syncwarp();
     }
-    __syncthreads();
-    double* dst = B.acc + wd.acc0;
-    for (long long i = threadIdx.x; i < nS + 3ll * Npc; i += blockDim.x) {
-        const double v = smem[i];
-        if (v != 0.0) atomicAdd(&dst[i], v);
-    }
+    if (buffered) { __syncwarp(); flushGroup(sm.gbuf, curNs, curS, curX, curSk, K, tdCol, Npc, acc, lane); }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -655,42 +736,41 @@ __global__ void k_candidate(DevBatch B) {
 // VisualCudaBatch.cu:191-205) and the robust cost of the candidate point.
 // Warp per tile; lane = landmark for the back-substitution, lane =
 // observation for the trial residuals.
-__global__ void __launch_bounds__(kLinThreads) k_backsub_trial(DevBatch B, const int2* tiles, const int* slabTile0) {
-    const Slab sl = B.slabs[blockIdx.x];
-    const int wdx = sl.win;
+__global__ void __launch_bounds__(kLinWarps * 32) k_backsub_trial(DevBatch B, const int4* runs, const int2* tiles) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __shared__ double tcost[kLinWarps][32];
+    __shared__ int tvalid[kLinWarps][32];
+    const int runIdx = blockIdx.x * kLinWarps + warp;
+    if (runIdx >= B.numRuns) return;
+    const int4 run = runs[runIdx];
+    const int wdx = run.x;
     if (B.lm[wdx].mode == kModeDone) return;
     const WinDesc wd = B.win[wdx];
     const double lambda = B.lm[wdx].lambda;
     const int K = wd.K;
     const double* dr = B.dr + wd.vec0;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-    __shared__ double tcost[kLinThreads / 32][32];
-    __shared__ int tvalid[kLinThreads / 32][32];
-    const int t0 = slabTile0[blockIdx.x], t1 = slabTile0[blockIdx.x + 1];
-    for (int t = t0 + warp; t < t1; t += nwarps) {
+    for (int t = run.y; t < run.z; ++t) {
         const int2 tile = tiles[t];
         const int lb = tile.x, le = tile.y, nl = le - lb;
         if (lane < nl) {
             const int l = lb + lane;
-            const int s = B.lmNs[l], ns = 6 * s + wd.ncalib;
+            const int s = B.lmNs[l], x = B.lmNx[l], ns = 6 * (s + x) + (wd.estTd ? 1 : 0);
             const double* c = B.lmC + B.lmC0[l];
             const int* sk = B.supp + B.lmSupp0[l];
+            const int tdCol = 6 * K + (wd.estExt ? 6 * wd.E : 0);
             double cd = 0;
-            for (int i = 0; i < ns; ++i) {
-                const int p = i < 6 * s ? 6 * sk[i / 6] + i % 6 : 6 * K + (i - 6 * s);
-                cd += c[i] * dr[retainedOfPc(p, K)];
-            }
+            for (int i = 0; i < ns; ++i) cd += c[i] * dr[retainedOfPc(pcOfLocal(i, s, x, sk, K, tdCol), K)];
             const double d = B.lmD[l], g = B.lmG[l];
             const double dt = d + lambda * fmax(d, 1e-6);
             double dl = -(g + cd) / dt;
-            const double x = B.rho[0][l];
-            if (isfinite(dl)) dl = fmax(wd.minInv - x, dl);
+            const double rho0 = B.rho[0][l];
+            if (isfinite(dl)) dl = fmax(wd.minInv - rho0, dl);
             B.lmDelta[l] = dl;
             // landmark terms of -dx^T (g + 0.5 H dx): the cross term c.dx_r is
             // split between the state part (via S_v) and this correction
             B.lmPred[l] = -0.5 * cd * cd / dt - dl * (g + cd + 0.5 * d * dl);
             B.lmMaxInc[l] = isfinite(dl) ? fabs(dl) : -1.0;
-            B.rho[1][l] = fmax(wd.minInv, x + dl);
+            B.rho[1][l] = fmax(wd.minInv, rho0 + dl);
             tcost[warp][lane] = 0;
             tvalid[warp][lane] = isfinite(dl) ? 1 : 0;
         }
@@ -821,10 +901,7 @@ __global__ void k_lm_init(DevBatch B, double lambda0) {
 
 // ---------------------------------------------------------------------------------------
 // host-side launchers (called by backend_host.cu)
-size_t linearizeSmemBytes(int maxNpc, int stageStride) {
-    const size_t nS = (size_t)maxNpc * (maxNpc + 1) / 2 + 3ull * maxNpc;
-    return (nS + (size_t)(kLinThreads / 32) * (stageStride + 4 * 32)) * sizeof(double);
-}
+size_t linearizeSmemBytes() { return kLinWarps * sizeof(LinWarpSmem); }
 size_t factorSmemBytes(int maxNr) {
     // windows with Nr <= kSmemPackedMax factor in shared memory; larger ones in global memory
     const size_t n = (size_t)(maxNr < kSmemPackedMax ? maxNr : kSmemPackedMax);
@@ -844,11 +921,17 @@ cudaError_t configureKernels(size_t linSmem, size_t facSmem) {
     if ((e = cudaFuncGetAttributes(&fa, k_factor)) != cudaSuccess) return e;
     const size_t linMax = (size_t)optin - la.sharedSizeBytes, facMax = (size_t)optin - fa.sharedSizeBytes;
     if (linSmem > linMax || facSmem > facMax) return cudaErrorInvalidValue;
+    unsigned char pa[kPairs], pb[kPairs];
+    int n = 0;
+    for (int a = 0; a < kCompact; ++a)
+        for (int b = a; b < kCompact; ++b) { pa[n] = (unsigned char)a; pb[n] = (unsigned char)b; ++n; }
+    if ((e = cudaMemcpyToSymbol(kPairA, pa, sizeof pa)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyToSymbol(kPairB, pb, sizeof pb)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_linearize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)linMax)) != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)facMax);
 }
 
-int launchIteration(const DevBatch& B, const int2* tiles, const int* slabTile0, int stageStride, size_t linSmem, size_t facSmem,
+int launchIteration(const DevBatch& B, const int4* runs, const int2* tiles, size_t linSmem, size_t facSmem,
                     int refinement, int maxIterations, int probe, double* Sdebug, cudaStream_t s, LaunchHook hook, void* ctx) {
     const int W = B.numWindows;
     int n = 0;
@@ -859,13 +942,14 @@ int launchIteration(const DevBatch& B, const int2* tiles, const int* slabTile0, 
         ++n;
     };
     run(CGMLI_KERNEL_ZERO, [&] { k_zero_acc<<<W, 256, 0, s>>>(B); });
-    if (B.numSlabs > 0)
-        run(CGMLI_KERNEL_LINEARIZE, [&] { k_linearize<<<B.numSlabs, kLinThreads, linSmem, s>>>(B, tiles, slabTile0, stageStride); });
+    const int runBlocks = (B.numRuns + kLinWarps - 1) / kLinWarps;
+    if (B.numRuns > 0)
+        run(CGMLI_KERNEL_LINEARIZE, [&] { k_linearize<<<runBlocks, kLinWarps * 32, linSmem, s>>>(B, runs, tiles); });
     run(CGMLI_KERNEL_RETAINED, [&] { k_retained<<<W, 256, 0, s>>>(B, 0); });
     run(CGMLI_KERNEL_FACTOR, [&] { k_factor<<<W, kFactorThreads, facSmem, s>>>(B, refinement, Sdebug); });
     run(CGMLI_KERNEL_CANDIDATE, [&] { k_candidate<<<W, 128, 0, s>>>(B); });
-    if (B.numSlabs > 0)
-        run(CGMLI_KERNEL_BACKSUB_TRIAL, [&] { k_backsub_trial<<<B.numSlabs, kLinThreads, 0, s>>>(B, tiles, slabTile0); });
+    if (B.numRuns > 0)
+        run(CGMLI_KERNEL_BACKSUB_TRIAL, [&] { k_backsub_trial<<<runBlocks, kLinWarps * 32, 0, s>>>(B, runs, tiles); });
     run(CGMLI_KERNEL_RETAINED_TRIAL, [&] { k_retained<<<W, 256, 0, s>>>(B, 1); });
     run(CGMLI_KERNEL_LM_UPDATE, [&] { k_lm_update<<<W, 256, 0, s>>>(B, maxIterations, probe); });
     if (!probe) run(CGMLI_KERNEL_ACCEPT, [&] { k_accept<<<W, 256, 0, s>>>(B); });

@@ -144,7 +144,9 @@ def test_checkpoint_rollback_restores_states(backend):
     s.solve(3)
     s.synchronize()
     s.read_states()
-    assert np.array_equal(w.state_vector(), first)
+    # the re-solve repeats the same arithmetic; only the order of the FP64
+    # reductions into the window accumulator may differ between runs
+    assert rel(w.state_vector() - x0, first - x0) < 1e-10
 
 
 def test_invalid_factor_is_reported_not_hidden(backend):
