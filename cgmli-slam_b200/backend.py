@@ -131,6 +131,56 @@ class Solver:
         _check(lib().cgmli_solver_last_timing(self._h, C.byref(ms), C.byref(n)), "cgmli_solver_last_timing")
         return ms.value, n.value
 
+    def marginalize(self, victims, policy: int = abi.MARGIN_OLD) -> None:
+        """Schur marginalization of victims[w] (or -1 to skip) in every window."""
+        v = np.ascontiguousarray(victims, dtype=np.int32)
+        _check(lib().cgmli_solver_marginalize(self._h, v.ctypes.data_as(abi.c_int_p), policy), "cgmli_solver_marginalize")
+
+    def read_prior(self, w: int) -> dict:
+        """Square-root prior of window w: separator blocks, reference values, A (rank x cols), r0."""
+        rank, cols, nb = C.c_int(), C.c_int(), C.c_int()
+        code = lib().cgmli_solver_read_prior(self._h, w, C.byref(rank), C.byref(cols), C.byref(nb), None, None, None, None, None,
+                                             None)
+        if code != 0:
+            return dict(status=code)
+        k, m, b = rank.value, cols.value, nb.value
+        kinds, idx = np.zeros(b, np.int32), np.zeros(b, np.int32)
+        ref, A, r0, form = np.zeros(9 * b + 1), np.zeros(k * m), np.zeros(k), np.zeros(4)
+        ip = abi.c_int_p
+        code = lib().cgmli_solver_read_prior(self._h, w, C.byref(rank), C.byref(cols), C.byref(nb), kinds.ctypes.data_as(ip),
+                                             idx.ctypes.data_as(ip), _p(ref), _p(A), _p(r0), _p(form))
+        amb = int(sum(9 if t == abi.PRIOR_SPEED_BIAS else 1 if t == abi.PRIOR_TIME_OFFSET else 7 for t in kinds))
+        return dict(status=code, rank=k, cols=m, kinds=kinds, index=idx, reference=ref[:amb], A=A.reshape(k, m), r0=r0,
+                    robust_cost=form[0], rss=form[1], eliminated_reduction=form[2], cutoff=form[3])
+
+
+def marg_eigen(H: np.ndarray):
+    """Ascending eigenvalues and column eigenvectors of the symmetric H (lower triangle read)."""
+    n = H.shape[0]
+    Hc = np.asfortranarray(H, dtype=np.float64)
+    ev, U = np.zeros(n), np.zeros((n, n), order="F")
+    _check(lib().cgmli_marg_eigen(_p(Hc), n, _p(ev), _p(U)), "cgmli_marg_eigen")
+    return ev, U
+
+
+def marg_psd_solve(H: np.ndarray, rhs: np.ndarray, absolute_cutoff: float = 1e-12, relative_cutoff: float = 1e-9):
+    n = H.shape[0]
+    rhs2 = rhs.reshape(n, -1)
+    Hc, Rc = np.asfortranarray(H, dtype=np.float64), np.asfortranarray(rhs2, dtype=np.float64)
+    x = np.zeros(Rc.shape, order="F")
+    _check(lib().cgmli_marg_psd_solve(_p(Hc), _p(Rc), n, Rc.shape[1], absolute_cutoff, relative_cutoff, _p(x)),
+           "cgmli_marg_psd_solve")
+    return x.reshape(rhs.shape)
+
+
+def marg_subtract(coupling: np.ndarray, solution: np.ndarray, H: np.ndarray, g: np.ndarray):
+    """[H | g] -= coupling^T solution, coupling nm x nr, solution nm x (nr + 1); returns new (H, g)."""
+    nm, nr = coupling.shape
+    Cc, Sc = np.asfortranarray(coupling, dtype=np.float64), np.asfortranarray(solution, dtype=np.float64)
+    Ho, go = np.array(H, dtype=np.float64, order="F"), np.array(g, dtype=np.float64)
+    _check(lib().cgmli_marg_subtract(_p(Cc), _p(Sc), nm, nr, _p(Ho), _p(go)), "cgmli_marg_subtract")
+    return Ho, go
+
 
 def _window_array(windows):
     arr = (abi.Window * len(windows))()

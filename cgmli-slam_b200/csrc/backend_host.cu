@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -26,6 +27,13 @@ cudaError_t configureKernels(size_t linSmem, size_t facSmem);
 int launchIteration(const DevBatch& B, const int4* runs, const int2* tiles, size_t linSmem, size_t facSmem,
                     int refinement, int maxIterations, int probe, double* Sdebug, cudaStream_t s, LaunchHook hook, void* ctx);
 int launchLmInit(const DevBatch& B, double lambda0, cudaStream_t s);
+size_t margVisualSmemBytes(int maxNc);
+cudaError_t configureMarginalization(size_t visualSmem);
+int launchMarginalization(const DevBatch& B, const MargBatch& M, size_t visualSmem, cudaStream_t s);
+void launchDenseEigen(const double* H, int n, double* work, double* evals, double* evecs, int* status, cudaStream_t s);
+void launchDensePsd(const double* evals, const double* U, const double* rhs, int n, int columns, double absCut, double relCut,
+                    double* projected, double* solution, int* status, cudaStream_t s);
+void launchDenseSubtract(const double* coupling, const double* solution, int nm, int nr, double* Hg, cudaStream_t s);
 }  // namespace cgmli
 
 using namespace cgmli;
@@ -106,6 +114,17 @@ struct cgmli_solver {
     DevBatch B{};
     double lastMs = 0;
     int lastLaunches = 0;
+    // host copies of the topology (device order, global indices) for elimination sets
+    std::vector<int> hLmKf, hLmCam, hLmObsBegin, hObKf, hObCam, hCamExt, hImuKf, hPriorKind, hPriorIndex;
+    // marginalization
+    std::vector<MargWin> margWin;
+    std::vector<std::vector<int>> sepKind, sepIndex;  // separator blocks per window (window-local index)
+    DArray<MargWin> dMargWin;
+    DArray<MargElim> dMargElim;
+    DArray<int> margCols, margObsMap, margPoseCol, margSbCol, margExtCol, margRank, margStatus;
+    DArray<double> margH, margB, margSepH, margSepV, margSepB, margEvals, margA, margR0, margX, margMaxD, margStats;
+    MargBatch MB{};
+    bool haveMarg = false;
     // checkpoint of the accepted states
     DArray<double> snapPose, snapSb, snapExt, snapTd, snapRho;
     bool haveSnapshot = false;
@@ -149,6 +168,11 @@ struct cgmli_solver {
         for (auto* a : ints) a->release();
         lmC0.release(); dWin.release(); dLm.release(); dRuns.release(); dTiles.release();
         snapPose.release(); snapSb.release(); snapExt.release(); snapTd.release(); snapRho.release();
+        dMargWin.release(); dMargElim.release();
+        DArray<int>* mi[] = {&margCols, &margObsMap, &margPoseCol, &margSbCol, &margExtCol, &margRank, &margStatus};
+        for (auto* a : mi) a->release();
+        DArray<double>* md[] = {&margH, &margB, &margSepH, &margSepV, &margSepB, &margEvals, &margA, &margR0, &margX, &margMaxD, &margStats};
+        for (auto* a : md) a->release();
         for (auto e : evPool) cudaEventDestroy(e);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -484,6 +508,9 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     B.acc = S->acc.p; B.dr = S->dr.p; B.rhs = S->rhs.p; B.Sglob = S->Sglob.p;
     B.imuScratch = S->imuScratch.p; B.priorScratch = S->priorScratch.p; B.predState = S->predState.p;
     B.solveStatus = S->solveStatus.p; B.out = S->out.p;
+    S->hLmKf = lmKf; S->hLmCam = lmCam; S->hLmObsBegin = lmObsBegin; S->hObKf = obKf; S->hObCam = obCam;
+    S->hCamExt = camExt; S->hImuKf = imuKf; S->hPriorKind = priorKind; S->hPriorIndex = priorIndex;
+    S->haveMarg = false;
     CK(cudaMemsetAsync(S->costRet.p, 0, count * sizeof(double), st));
     CK(cudaMemsetAsync(S->trialRet.p, 0, count * sizeof(double), st));
     CK(cudaStreamSynchronize(st));
@@ -701,27 +728,300 @@ int cgmli_solver_last_timing(cgmli_solver* S, double* ms, int* launches) {
     return CGMLI_OK;
 }
 
+// Elimination set (SlidingWindowManager.cpp:627-652): landmarks anchored at the
+// victim, plus under OLD those observed at it; all their observations, the IMU
+// factors touching the victim and the prior are consumed.  Every block a
+// consumed factor touches joins the system, frozen calibration included
+// (BackendProblem.hpp:75-80 with honorConstant=false).
 int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) {
-    (void)S; (void)victim_kf; (void)policy;
-    return fail(CGMLI_E_UNSUPPORTED, "marginalization not built yet");
+    if (!S || S->win.empty() || !victim_kf) return fail(CGMLI_E_INVALID, "solver has no windows or no victim list");
+    if (policy != CGMLI_MARGIN_OLD && policy != CGMLI_MARGIN_SECOND_NEW) return fail(CGMLI_E_INVALID, "unknown marginalization policy");
+    const int W = (int)S->win.size();
+    for (int w = 0; w < W; ++w)
+        if (victim_kf[w] < -1 || victim_kf[w] >= S->win[w].K) return fail(CGMLI_E_INVALID, "victim keyframe out of range");
+    CK(cudaSetDevice(S->device));
+    std::vector<MargWin> mwv(W);
+    std::vector<MargElim> elims;
+    std::vector<int> cols, obsMap;
+    std::vector<int> poseCol(S->totalKf, -1), sbCol(S->totalKf, -1), extCol(S->totalExt, -1);
+    S->sepKind.assign(W, {});
+    S->sepIndex.assign(W, {});
+    long long H0 = 0, sep0 = 0, vec0 = 0, x0 = 0;
+    int maxNc = 0;
+    for (int w = 0; w < W; ++w) {
+        const WinDesc& d = S->win[w];
+        const int v = victim_kf[w];
+        MargWin& mw = mwv[w];
+        mw = MargWin{};
+        mw.imu[0] = mw.imu[1] = -1;
+        mw.tdCol = -1;
+        mw.huber = d.huber;
+        mw.H0 = H0; mw.sep0 = sep0; mw.vec0 = vec0; mw.x0 = x0;
+        mw.elim0 = (int)elims.size();
+        if (v < 0) continue;
+        std::vector<char> poseUsed(d.K, 0), sbUsed(d.K, 0), extUsed(d.E, 0);
+        bool tdUsed = false;
+        std::vector<int> elimLm;
+        for (int q = 0; q < d.L; ++q) {
+            const int g = d.lm0 + q, a = S->hLmKf[g] - d.kf0;
+            bool e = a == v;
+            for (int f = S->hLmObsBegin[g]; f < S->hLmObsBegin[g + 1] && !e && policy == CGMLI_MARGIN_OLD; ++f)
+                e = S->hObKf[f] - d.kf0 == v;
+            if (!e) continue;
+            elimLm.push_back(g);
+            for (int f = S->hLmObsBegin[g]; f < S->hLmObsBegin[g + 1]; ++f) {
+                poseUsed[a] = 1;
+                poseUsed[S->hObKf[f] - d.kf0] = 1;
+                extUsed[S->hCamExt[S->hLmCam[g]] - d.ext0] = 1;
+                extUsed[S->hCamExt[S->hObCam[f]] - d.ext0] = 1;
+                tdUsed = true;
+            }
+        }
+        int nImu = 0;
+        for (int i = 0; i < d.nImu; ++i) {
+            const int k = S->hImuKf[d.imu0 + i] - d.kf0;
+            if (k != v && k + 1 != v) continue;
+            if (nImu == 2) return fail(CGMLI_E_LIMIT, "more than two IMU factors touch the victim keyframe");
+            mw.imu[nImu++] = d.imu0 + i;
+            poseUsed[k] = poseUsed[k + 1] = sbUsed[k] = sbUsed[k + 1] = 1;
+        }
+        for (int b = 0; b < d.priorBlocks; ++b) {
+            const int kind = S->hPriorKind[d.priorBlk0 + b], gi = S->hPriorIndex[d.priorBlk0 + b];
+            if (kind == CGMLI_PRIOR_POSE) poseUsed[gi - d.kf0] = 1;
+            else if (kind == CGMLI_PRIOR_SPEED_BIAS) sbUsed[gi - d.kf0] = 1;
+            else if (kind == CGMLI_PRIOR_EXTRINSIC) extUsed[gi - d.ext0] = 1;
+            else tdUsed = true;
+        }
+        // columns: victim first, then the separator in block order
+        int n = 0;
+        if (poseUsed[v]) { poseCol[d.kf0 + v] = n; n += 6; }
+        if (sbUsed[v]) { sbCol[d.kf0 + v] = n; n += 9; }
+        mw.nm = n;
+        auto sep = [&](int kind, int index) { S->sepKind[w].push_back(kind); S->sepIndex[w].push_back(index); };
+        for (int k = 0; k < d.K; ++k) {
+            if (k == v) continue;
+            if (poseUsed[k]) { poseCol[d.kf0 + k] = n; n += 6; sep(CGMLI_PRIOR_POSE, k); }
+            if (sbUsed[k]) { sbCol[d.kf0 + k] = n; n += 9; sep(CGMLI_PRIOR_SPEED_BIAS, k); }
+        }
+        for (int e = 0; e < d.E; ++e)
+            if (extUsed[e]) { extCol[d.ext0 + e] = n; n += 6; sep(CGMLI_PRIOR_EXTRINSIC, e); }
+        if (tdUsed && d.hasTd) { mw.tdCol = n; n += 1; sep(CGMLI_PRIOR_TIME_OFFSET, 0); }
+        mw.m = n;
+        mw.nr = n - mw.nm;
+        if (mw.nr > kMargMaxSep) return fail(CGMLI_E_LIMIT, "marginalization separator above 1024 columns");
+        // eliminated landmarks: local column blocks in order of first use
+        for (int g : elimLm) {
+            MargElim me{g, w, 0, (int)cols.size(), (int)(obsMap.size() / 5)};
+            std::vector<int> blkStart, blkLocal;
+            auto localOf = [&](int start, int size) {
+                if (start < 0) return -1;
+                for (size_t i = 0; i < blkStart.size(); ++i)
+                    if (blkStart[i] == start) return blkLocal[i];
+                blkStart.push_back(start);
+                blkLocal.push_back(me.nc);
+                for (int c = 0; c < size; ++c) cols.push_back(start + c);
+                me.nc += size;
+                return blkLocal.back();
+            };
+            const int a = S->hLmKf[g], ea = S->hCamExt[S->hLmCam[g]];
+            for (int f = S->hLmObsBegin[g]; f < S->hLmObsBegin[g + 1]; ++f) {
+                const int b = S->hObKf[f], eb = S->hCamExt[S->hObCam[f]];
+                obsMap.push_back(localOf(poseCol[a], 6));
+                obsMap.push_back(localOf(poseCol[b], 6));
+                obsMap.push_back(localOf(extCol[ea], 6));
+                obsMap.push_back(localOf(extCol[eb], 6));
+                obsMap.push_back(mw.tdCol >= 0 ? localOf(mw.tdCol, 1) : -1);
+            }
+            if (me.nc > kMargMaxNc) return fail(CGMLI_E_LIMIT, "eliminated landmark touches more than 200 marginalization columns");
+            maxNc = std::max(maxNc, me.nc);
+            elims.push_back(me);
+        }
+        mw.nElim = (int)elims.size() - mw.elim0;
+        H0 += (long long)mw.m * mw.m;
+        sep0 += (long long)mw.nr * mw.nr;
+        vec0 += mw.m;
+        x0 += 2ll * 15 * (mw.nr + 1);
+    }
+    cudaStream_t st = S->stream;
+    const size_t smem = margVisualSmemBytes(std::max(maxNc, 1));
+    CK(configureMarginalization(smem));
+    CK(S->dMargWin.upload(mwv, st));
+    CK(S->dMargElim.upload(elims, st));
+    CK(S->margCols.upload(cols, st));
+    CK(S->margObsMap.upload(obsMap, st));
+    CK(S->margPoseCol.upload(poseCol, st));
+    CK(S->margSbCol.upload(sbCol, st));
+    CK(S->margExtCol.upload(extCol, st));
+    CK(S->margH.reserve(H0)); CK(S->margB.reserve(vec0)); CK(S->margSepH.reserve(sep0)); CK(S->margSepV.reserve(sep0));
+    CK(S->margSepB.reserve(vec0)); CK(S->margEvals.reserve(vec0)); CK(S->margA.reserve(sep0)); CK(S->margR0.reserve(vec0));
+    CK(S->margX.reserve(x0)); CK(S->margMaxD.reserve(W)); CK(S->margStats.reserve(4ll * W));
+    CK(S->margRank.reserve(W)); CK(S->margStatus.reserve(W));
+    if (H0) CK(cudaMemsetAsync(S->margH.p, 0, H0 * sizeof(double), st));
+    if (vec0) CK(cudaMemsetAsync(S->margB.p, 0, vec0 * sizeof(double), st));
+    CK(cudaMemsetAsync(S->margMaxD.p, 0, W * sizeof(double), st));
+    CK(cudaMemsetAsync(S->margStats.p, 0, 4ll * W * sizeof(double), st));
+    CK(cudaMemsetAsync(S->margStatus.p, 0, W * sizeof(int), st));
+    CK(cudaMemsetAsync(S->margRank.p, 0, W * sizeof(int), st));
+    MargBatch& M = S->MB;
+    M = MargBatch{};
+    M.numWindows = W;
+    M.numElim = (int)elims.size();
+    M.win = S->dMargWin.p; M.elim = S->dMargElim.p; M.cols = S->margCols.p; M.obsMap = S->margObsMap.p;
+    M.poseCol = S->margPoseCol.p; M.sbCol = S->margSbCol.p; M.extCol = S->margExtCol.p;
+    M.H = S->margH.p; M.b = S->margB.p; M.sepH = S->margSepH.p; M.sepV = S->margSepV.p; M.sepB = S->margSepB.p;
+    M.evals = S->margEvals.p; M.A = S->margA.p; M.r0 = S->margR0.p; M.X = S->margX.p;
+    M.maxD = S->margMaxD.p; M.stats = S->margStats.p; M.rank = S->margRank.p; M.status = S->margStatus.p;
+    S->margWin = mwv;
+    CK(cudaEventRecord(S->ev0, st));
+    S->lastLaunches = launchMarginalization(S->B, M, smem, st);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(S->ev1, st));
+    S->haveMarg = true;
+    return CGMLI_OK;
 }
+
 int cgmli_solver_read_prior(cgmli_solver* S, int window, int* rank, int* cols, int* num_blocks, int* block_kind, int* block_index,
                             double* reference, double* A, double* r0, double* formation) {
-    (void)S; (void)window; (void)rank; (void)cols; (void)num_blocks; (void)block_kind; (void)block_index; (void)reference; (void)A;
-    (void)r0; (void)formation;
-    return fail(CGMLI_E_UNSUPPORTED, "marginalization not built yet");
+    if (!S || !S->haveMarg) return fail(CGMLI_E_INVALID, "no marginalization recorded");
+    if (window < 0 || window >= (int)S->margWin.size()) return fail(CGMLI_E_INVALID, "window index");
+    if (!rank || !cols || !num_blocks) return fail(CGMLI_E_INVALID, "null size outputs");
+    CK(cudaSetDevice(S->device));
+    CK(cudaStreamSynchronize(S->stream));
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, S->ev0, S->ev1) == cudaSuccess) S->lastMs = ms;
+    const MargWin& mw = S->margWin[window];
+    const WinDesc& d = S->win[window];
+    int status = CGMLI_OK, rk = 0;
+    CK(cudaMemcpy(&status, S->margStatus.p + window, sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&rk, S->margRank.p + window, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status != CGMLI_OK) return fail(status, "window marginalization failed (invalid factor or indefinite information)");
+    *rank = mw.m ? rk : 0;
+    *cols = mw.m ? mw.nr : 0;
+    *num_blocks = mw.m ? (int)S->sepKind[window].size() : 0;
+    if (!mw.m) return CGMLI_OK;
+    const auto& kinds = S->sepKind[window];
+    const auto& idx = S->sepIndex[window];
+    if (block_kind) std::copy(kinds.begin(), kinds.end(), block_kind);
+    if (block_index) std::copy(idx.begin(), idx.end(), block_index);
+    if (reference) {
+        std::vector<double> pose(7ull * d.K), sb(9ull * d.K), ext(7ull * d.E);
+        double td = 0;
+        CK(cudaMemcpy(pose.data(), S->pose[0].p + 7ll * d.kf0, pose.size() * 8, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(sb.data(), S->sb[0].p + 9ll * d.kf0, sb.size() * 8, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(ext.data(), S->ext[0].p + 7ll * d.ext0, ext.size() * 8, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&td, S->td[0].p + window, 8, cudaMemcpyDeviceToHost));
+        double* out = reference;
+        for (size_t b = 0; b < kinds.size(); ++b) {
+            const double* src = kinds[b] == CGMLI_PRIOR_POSE ? &pose[7ull * idx[b]] : kinds[b] == CGMLI_PRIOR_SPEED_BIAS ? &sb[9ull * idx[b]]
+                                : kinds[b] == CGMLI_PRIOR_EXTRINSIC ? &ext[7ull * idx[b]] : &td;
+            const int n = ambientOf(kinds[b]);
+            std::copy(src, src + n, out);
+            out += n;
+        }
+    }
+    if (A && rk) CK(cudaMemcpy(A, S->margA.p + mw.sep0, (size_t)rk * mw.nr * sizeof(double), cudaMemcpyDeviceToHost));
+    if (r0 && rk) CK(cudaMemcpy(r0, S->margR0.p + mw.vec0, (size_t)rk * sizeof(double), cudaMemcpyDeviceToHost));
+    if (formation) CK(cudaMemcpy(formation, S->margStats.p + 4ll * window, 4 * sizeof(double), cudaMemcpyDeviceToHost));
+    return CGMLI_OK;
 }
+
+// ---- dense helpers: one process-wide workspace on the current device, serialized
+namespace {
+struct DenseWorkspace {
+    std::mutex mu;
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    DArray<double> H, work, evals, U, rhs, projected, solution;
+    DArray<int> status;
+};
+DenseWorkspace g_dense;
+
+int denseBegin(int n) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (g_dense.device != dev) {
+        if (g_dense.stream) cudaStreamDestroy(g_dense.stream);
+        g_dense.stream = nullptr;
+        DArray<double>* a[] = {&g_dense.H, &g_dense.work, &g_dense.evals, &g_dense.U, &g_dense.rhs, &g_dense.projected, &g_dense.solution};
+        for (auto* x : a) x->release();
+        g_dense.status.release();
+        CK(cudaStreamCreateWithFlags(&g_dense.stream, cudaStreamNonBlocking));
+        g_dense.device = dev;
+    }
+    CK(g_dense.status.reserve(1));
+    CK(cudaMemsetAsync(g_dense.status.p, 0, sizeof(int), g_dense.stream));
+    (void)n;
+    return CGMLI_OK;
+}
+// eigen-decomposition of H into g_dense.evals (ascending) / g_dense.U
+int denseDecompose(const double* H, int n) {
+    const size_t nn = (size_t)n * n;
+    CK(g_dense.H.reserve(nn)); CK(g_dense.work.reserve(2 * nn)); CK(g_dense.evals.reserve(2ull * n)); CK(g_dense.U.reserve(nn));
+    CK(cudaMemcpyAsync(g_dense.H.p, H, nn * sizeof(double), cudaMemcpyHostToDevice, g_dense.stream));
+    launchDenseEigen(g_dense.H.p, n, g_dense.work.p, g_dense.evals.p, g_dense.U.p, g_dense.status.p, g_dense.stream);
+    CK(cudaGetLastError());
+    return CGMLI_OK;
+}
+int denseStatus() {
+    int st = 0;
+    CK(cudaMemcpyAsync(&st, g_dense.status.p, sizeof(int), cudaMemcpyDeviceToHost, g_dense.stream));
+    CK(cudaStreamSynchronize(g_dense.stream));
+    return st;
+}
+}  // namespace
+
 int cgmli_marg_eigen(const double* H, int n, double* eigenvalues, double* eigenvectors) {
-    (void)H; (void)n; (void)eigenvalues; (void)eigenvectors;
-    return fail(CGMLI_E_UNSUPPORTED, "not built yet");
+    if (!H || !eigenvalues || !eigenvectors || n < 1) return fail(CGMLI_E_INVALID, "eigen: null buffers or n < 1");
+    if (n > kMargMaxSep) return fail(CGMLI_E_LIMIT, "eigen: n above 1024");
+    std::lock_guard<std::mutex> lock(g_dense.mu);
+    int r = denseBegin(n);
+    if (r != CGMLI_OK || (r = denseDecompose(H, n)) != CGMLI_OK) return r;
+    CK(cudaMemcpyAsync(eigenvalues, g_dense.evals.p, n * sizeof(double), cudaMemcpyDeviceToHost, g_dense.stream));
+    CK(cudaMemcpyAsync(eigenvectors, g_dense.U.p, (size_t)n * n * sizeof(double), cudaMemcpyDeviceToHost, g_dense.stream));
+    const int st = denseStatus();
+    if (st == CGMLI_E_CUDA) return st;
+    if (st != CGMLI_OK) return fail(st, "eigen: non-finite eigenvalue");
+    return CGMLI_OK;
 }
-int cgmli_marg_psd_solve(const double* H, const double* rhs, int n, int columns, double a, double r, double* x) {
-    (void)H; (void)rhs; (void)n; (void)columns; (void)a; (void)r; (void)x;
-    return fail(CGMLI_E_UNSUPPORTED, "not built yet");
+
+int cgmli_marg_psd_solve(const double* H, const double* rhs, int n, int columns, double absolute_cutoff, double relative_cutoff,
+                         double* solution) {
+    if (!H || !rhs || !solution || n < 1) return fail(CGMLI_E_INVALID, "psd_solve: null buffers or n < 1");
+    if (columns < 1 || columns > 4001) return fail(CGMLI_E_INVALID, "psd_solve: columns outside 1..4001");
+    if (n > kMargMaxSep) return fail(CGMLI_E_LIMIT, "psd_solve: n above 1024");
+    std::lock_guard<std::mutex> lock(g_dense.mu);
+    int r = denseBegin(n);
+    if (r != CGMLI_OK || (r = denseDecompose(H, n)) != CGMLI_OK) return r;
+    const size_t count = (size_t)n * columns;
+    CK(g_dense.rhs.reserve(count)); CK(g_dense.projected.reserve(count)); CK(g_dense.solution.reserve(count));
+    CK(cudaMemcpyAsync(g_dense.rhs.p, rhs, count * sizeof(double), cudaMemcpyHostToDevice, g_dense.stream));
+    launchDensePsd(g_dense.evals.p, g_dense.U.p, g_dense.rhs.p, n, columns, absolute_cutoff, relative_cutoff, g_dense.projected.p,
+                   g_dense.solution.p, g_dense.status.p, g_dense.stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(solution, g_dense.solution.p, count * sizeof(double), cudaMemcpyDeviceToHost, g_dense.stream));
+    const int st = denseStatus();
+    if (st != CGMLI_OK) return fail(st, "psd_solve: indefinite or non-finite information");
+    return CGMLI_OK;
 }
+
 int cgmli_marg_subtract(const double* coupling, const double* solution, int nm, int nr, double* H, double* g) {
-    (void)coupling; (void)solution; (void)nm; (void)nr; (void)H; (void)g;
-    return fail(CGMLI_E_UNSUPPORTED, "not built yet");
+    if (!coupling || !solution || !H || !g) return fail(CGMLI_E_INVALID, "subtract: null buffers");
+    if (nm < 1 || nr < 1 || nm > 4000 || nr > 4000) return fail(CGMLI_E_INVALID, "subtract: sizes outside 1..4000");
+    std::lock_guard<std::mutex> lock(g_dense.mu);
+    int r = denseBegin(nr);
+    if (r != CGMLI_OK) return r;
+    const size_t nc = (size_t)nm * nr, ns = (size_t)nm * (nr + 1), nh = (size_t)nr * nr;
+    CK(g_dense.U.reserve(nc)); CK(g_dense.rhs.reserve(ns)); CK(g_dense.solution.reserve(nh + nr));
+    CK(cudaMemcpyAsync(g_dense.U.p, coupling, nc * sizeof(double), cudaMemcpyHostToDevice, g_dense.stream));
+    CK(cudaMemcpyAsync(g_dense.rhs.p, solution, ns * sizeof(double), cudaMemcpyHostToDevice, g_dense.stream));
+    CK(cudaMemcpyAsync(g_dense.solution.p, H, nh * sizeof(double), cudaMemcpyHostToDevice, g_dense.stream));
+    CK(cudaMemcpyAsync(g_dense.solution.p + nh, g, nr * sizeof(double), cudaMemcpyHostToDevice, g_dense.stream));
+    launchDenseSubtract(g_dense.U.p, g_dense.rhs.p, nm, nr, g_dense.solution.p, g_dense.stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(H, g_dense.solution.p, nh * sizeof(double), cudaMemcpyDeviceToHost, g_dense.stream));
+    CK(cudaMemcpyAsync(g, g_dense.solution.p + nh, nr * sizeof(double), cudaMemcpyDeviceToHost, g_dense.stream));
+    CK(cudaStreamSynchronize(g_dense.stream));
+    return CGMLI_OK;
 }
 
 }  // extern "C"

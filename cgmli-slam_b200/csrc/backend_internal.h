@@ -85,6 +85,42 @@ struct DevBatch {
     double* out;     // per-window scratch for read-back (costs)
 };
 
+// ---- marginalization (one victim keyframe per window) ----------------------------
+// Column space of window w: victim pose and speed/bias [0, nm), then the
+// separator [nm, m) in block order (keyframes ascending with pose before
+// speed/bias, then extrinsics, then td).  H holds the upper triangle
+// (row <= column) of the m x m information, row-major.
+constexpr int kMargMaxNc = 200;     // marginalization columns touched by one eliminated landmark
+constexpr int kMargMaxSep = 1024;   // separator columns (Jacobi pair tables hold 512 pairs)
+constexpr int kMargThreads = 512;   // victim / eigen CTAs
+constexpr int kMargLmThreads = 128; // one CTA per eliminated landmark
+
+struct MargWin {
+    int m, nm, nr;          // m = 0: window not marginalized
+    int elim0, nElim;       // eliminated landmarks in MargBatch::elim
+    int imu[2];             // consumed IMU factors (global index) or -1
+    int tdCol;              // column of td or -1
+    long long H0;           // m * m
+    long long sep0;         // nr * nr: separator information, eigenvectors, A
+    long long vec0;         // m
+    long long x0;           // 2 * 15 * (nr + 1): victim solve scratch
+    double huber;
+};
+struct MargElim { int lm, win, nc, col0, obs0; };  // device landmark, window, local columns, offsets
+struct MargBatch {
+    int numWindows, numElim;
+    const MargWin* win;
+    const MargElim* elim;
+    const int* cols;     // local column -> marginalization column
+    const int* obsMap;   // 5 per observation of an eliminated landmark: local start of
+                         // anchor pose, observer pose, anchor extrinsic, observer extrinsic, td (-1 if none)
+    const int* poseCol; const int* sbCol; const int* extCol;  // global keyframe / extrinsic -> column or -1
+    double* H; double* b; double* sepH; double* sepV; double* sepB; double* evals; double* A; double* r0; double* X;
+    double* maxD;        // per window: largest eliminated landmark information
+    double* stats;       // 4 per window: robust cost, whitened |r|^2, eliminated reduction, cutoff
+    int* rank; int* status;
+};
+
 // Called before (phase 0) and after (phase 1) every kernel launch of an
 // iteration; used for per-kernel event timing.
 typedef void (*LaunchHook)(void* ctx, int kind, int phase);

@@ -1,0 +1,651 @@
+// sm_100a kernels of the Schur-complement marginalization prior
+// (Marginalizer::compute, src/backend/Marginalizer.cpp:284-474) and of the
+// dense helpers of MarginalCudaWorkspace (src/backend/VisualCudaBatch.cu:898-957).
+//
+// Per window the consumed factors (all observations of the eliminated inverse
+// distances, the IMU factors touching the victim keyframe, the previous prior)
+// are linearized at the accepted states, with the Huber loss and with frozen
+// calibration blocks differentiated too, into an FP64 system over
+// [victim pose+speed/bias | separator]:
+//   k_marg_dmax      largest eliminated-landmark information of each window
+//                    (the scalar cutoff max(1e-12, 1e-9 max d) of psdSolve)
+//   k_marg_visual    one CTA per eliminated landmark: its factors' normal
+//                    blocks and its own scalar Schur term -c c^T / d are
+//                    summed in shared memory, then added to the window once
+//   k_marg_retained  IMU factors of the victim and the previous prior
+//   k_marg_victim    victim block removed by the eigen-based PSD solve
+//   k_marg_eigen     Jacobi eigendecomposition of the separator information,
+//                    rank cutoff, A = sqrt(lambda) u^T, r0 = u^T b / sqrt(lambda)
+#include <cuda_runtime.h>
+
+#include "../../include/cgmli_backend.h"
+#include "backend_internal.h"
+#include "device_math.cuh"
+#include "factor_eval.cuh"
+
+namespace cgmli {
+
+namespace {
+__device__ __forceinline__ double mWarpSum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+// block-wide sum; every thread gets the result
+__device__ double mBlockSum(double v, double* red) {
+    v = mWarpSum(v);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double t = 0;
+    for (int i = 0; i < nw; ++i) t += red[i];
+    __syncthreads();
+    return t;
+}
+__device__ double mBlockMax(double v, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double t = red[0];
+    for (int i = 1; i < nw; ++i) t = fmax(t, red[i]);
+    __syncthreads();
+    return t;
+}
+// non-negative doubles order like their bit patterns
+__device__ __forceinline__ void atomicMaxNonNegative(double* a, double v) {
+    atomicMax(reinterpret_cast<unsigned long long*>(a), (unsigned long long)__double_as_longlong(v));
+}
+__device__ __forceinline__ int packedUp(int i, int j, int n) { return i * n - i * (i - 1) / 2 + (j - i); }
+// symmetric entry of an upper-stored row-major matrix
+__device__ __forceinline__ double symAt(const double* H, int i, int j, int m) {
+    return i <= j ? H[(long long)i * m + j] : H[(long long)j * m + i];
+}
+
+// Weighted factor of observation f of eliminated landmark l, with the
+// marginalization's derivative set (extrinsics always, td whenever the window
+// has one).  Returns false on an invalid linearization point.
+__device__ bool margFactor(const DevBatch& B, const WinDesc& wd, int w, int l, int f, FactorIn& in, FactorOut& o, double& wgt,
+                           double& sq) {
+    int kfa, kfb, ea, eb;
+    gatherFactor(B, wd, w, l, f, 0, in, kfa, kfb, ea, eb);
+    in.wantExt = true;
+    in.wantTd = wd.hasTd != 0;
+    if (!(in.rho > 0) || !isfinite(in.rho) || !isfinite(in.td)) return false;
+    if (!evalBearingFactor(in, true, o)) return false;
+    sq = o.r[0] * o.r[0] + o.r[1] * o.r[1];
+    wgt = huberWeight(wd.huber, sq);
+    return true;
+}
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+// One warp per eliminated landmark, one lane per observation.
+__global__ void k_marg_dmax(DevBatch B, MargBatch M) {
+    const int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (e >= M.numElim) return;
+    const MargElim me = M.elim[e];
+    const WinDesc wd = B.win[me.win];
+    const int ob = B.lmObsBegin[me.lm], oe = B.lmObsBegin[me.lm + 1];
+    double d = 0;
+    for (int f = ob + lane; f < oe; f += 32) {
+        FactorIn in;
+        FactorOut o;
+        double wgt, sq;
+        if (!margFactor(B, wd, me.win, me.lm, f, in, o, wgt, sq)) { atomicExch(&M.status[me.win], CGMLI_E_NONFINITE); continue; }
+        d += wgt * wgt * (o.Jrho[0] * o.Jrho[0] + o.Jrho[1] * o.Jrho[1]);
+    }
+    d = mWarpSum(d);
+    if (lane == 0) atomicMaxNonNegative(&M.maxD[me.win], d);
+}
+
+// One CTA per eliminated landmark.  Shared memory: the landmark's local
+// information (packed upper, nc x nc), its cross vector c and gradient, then
+// the staged weighted rows of its observations.
+__global__ void __launch_bounds__(kMargLmThreads) k_marg_visual(DevBatch B, MargBatch M) {
+    extern __shared__ double smem[];
+    const int e = blockIdx.x;
+    const MargElim me = M.elim[e];
+    const int w = me.win, nc = me.nc;
+    const MargWin mw = M.win[w];
+    const WinDesc wd = B.win[w];
+    const int ob = B.lmObsBegin[me.lm], nobs = B.lmObsBegin[me.lm + 1] - ob;
+    const int npk = nc * (nc + 1) / 2;
+    double* hl = smem;                    // npk
+    double* cl = hl + npk;                // nc
+    double* gl = cl + nc;                 // nc
+    double* jst = gl + nc;                // 32 x 50: weighted rows over the observation's columns
+    double* rp = jst + 32 * 50;           // 32 x 4: weighted r0, r1, rho derivative 0, 1
+    short* lcol = reinterpret_cast<short*>(rp + 32 * 4);  // 32 x 25 local columns
+    int* nn = reinterpret_cast<int*>(lcol + 32 * 25);     // 32 column counts
+    __shared__ double red[kMargLmThreads / 32];
+    for (int i = threadIdx.x; i < npk + 2 * nc; i += blockDim.x) hl[i] = 0.0;
+    double cost = 0, rss = 0;
+    if (threadIdx.x < nobs) {
+        const int t = threadIdx.x, f = ob + t;
+        FactorIn in;
+        FactorOut o;
+        double wgt, sq;
+        int n = 0;
+        if (margFactor(B, wd, w, me.lm, f, in, o, wgt, sq)) {
+            cost = huberCost(wd.huber, sq);
+            rss = wgt * wgt * sq;
+            const int* map = M.obsMap + 5ll * (me.obs0 + t);
+            double* J = jst + 50 * t;
+            short* lc = lcol + 25 * t;
+            auto push = [&](int base, const double* Jb, int width) {
+                for (int c = 0; c < width; ++c) {
+                    lc[n] = (short)(base + c);
+                    J[n] = wgt * Jb[c];
+                    J[25 + n] = wgt * Jb[width + c];
+                    ++n;
+                }
+            };
+            const bool same = in.sameKf && !in.splitExt;
+            if (!in.sameKf) { push(map[0], o.Ja, 6); push(map[1], o.Jb, 6); }
+            if (!same) push(map[2], o.Jea, 6);
+            if (in.splitExt) push(map[3], o.Jeb, 6);
+            if (map[4] >= 0) push(map[4], o.Jtd, 1);
+            rp[4 * t + 0] = wgt * o.r[0];
+            rp[4 * t + 1] = wgt * o.r[1];
+            rp[4 * t + 2] = wgt * o.Jrho[0];
+            rp[4 * t + 3] = wgt * o.Jrho[1];
+        } else {
+            atomicExch(&M.status[w], CGMLI_E_NONFINITE);
+            for (int k = 0; k < 4; ++k) rp[4 * t + k] = 0.0;
+        }
+        nn[t] = n;
+    }
+    cost = mBlockSum(cost, red);
+    rss = mBlockSum(rss, red);
+    // factor normal blocks: the columns of one observation are distinct, so
+    // the threads of one observation write distinct entries
+    for (int t = 0; t < nobs; ++t) {
+        const int n = nn[t], pairs = n * (n + 1) / 2;
+        const double* J = jst + 50 * t;
+        const short* lc = lcol + 25 * t;
+        for (int q = threadIdx.x; q < pairs; q += blockDim.x) {
+            int i = 0, rem = q;
+            while (rem >= n - i) { rem -= n - i; ++i; }
+            const int j = i + rem;
+            const int a = lc[i], c = lc[j];
+            hl[a <= c ? packedUp(a, c, nc) : packedUp(c, a, nc)] += J[i] * J[j] + J[25 + i] * J[25 + j];
+        }
+        if (threadIdx.x < n) {
+            const int i = threadIdx.x, a = lc[i];
+            cl[a] += J[i] * rp[4 * t + 2] + J[25 + i] * rp[4 * t + 3];
+            gl[a] += J[i] * rp[4 * t + 0] + J[25 + i] * rp[4 * t + 1];
+        }
+        __syncthreads();
+    }
+    double d = 0, bl = 0;
+    for (int t = 0; t < nobs; ++t) {
+        d += rp[4 * t + 2] * rp[4 * t + 2] + rp[4 * t + 3] * rp[4 * t + 3];
+        bl += rp[4 * t + 2] * rp[4 * t + 0] + rp[4 * t + 3] * rp[4 * t + 1];
+    }
+    // scalar elimination with the diagonal PSD rule
+    const double cutoff = fmax(1e-12, 1e-9 * fmax(0.0, M.maxD[w]));
+    const bool eliminate = d > cutoff;
+    const double inv = eliminate ? 1.0 / d : 0.0;
+    const int* cols = M.cols + me.col0;
+    double* H = M.H + mw.H0;
+    double* bw = M.b + mw.vec0;
+    for (int q = threadIdx.x; q < npk; q += blockDim.x) {
+        int i = 0, rem = q;
+        while (rem >= nc - i) { rem -= nc - i; ++i; }
+        const int j = i + rem;
+        const double v = hl[q] - inv * cl[i] * cl[j];
+        if (v == 0.0) continue;
+        const int ci = cols[i], cj = cols[j];
+        atomicAdd(&H[ci <= cj ? (long long)ci * mw.m + cj : (long long)cj * mw.m + ci], v);
+    }
+    for (int i = threadIdx.x; i < nc; i += blockDim.x) {
+        const double v = gl[i] - inv * cl[i] * bl;
+        if (v != 0.0) atomicAdd(&bw[cols[i]], v);
+    }
+    if (threadIdx.x == 0) {
+        atomicAdd(&M.stats[4 * w + 0], cost);
+        atomicAdd(&M.stats[4 * w + 1], rss);
+        if (eliminate) atomicAdd(&M.stats[4 * w + 2], 0.5 * bl * bl * inv);
+    }
+}
+
+// IMU factors touching the victim and the previous prior, one CTA per window.
+__global__ void __launch_bounds__(256) k_marg_retained(DevBatch B, MargBatch M) {
+    const int w = blockIdx.x;
+    const MargWin mw = M.win[w];
+    if (mw.m == 0) return;
+    const WinDesc wd = B.win[w];
+    const int m = mw.m;
+    double* H = M.H + mw.H0;
+    double* g = M.b + mw.vec0;
+    __shared__ double sc[2 * 465];
+    __shared__ double red[8];
+    __shared__ int bad;
+    if (threadIdx.x == 0) bad = 0;
+    __syncthreads();
+    const cgmli_frozen_imu* imus = reinterpret_cast<const cgmli_frozen_imu*>(B.imu);
+    double cost = 0;
+    if (threadIdx.x < 2 && mw.imu[threadIdx.x] >= 0) {
+        const int gi = mw.imu[threadIdx.x], k = B.imuKf[gi];
+        double* r = sc + 465 * threadIdx.x;
+        if (!evalImu(imus[gi], B.pose[0] + 7ll * k, B.sb[0] + 9ll * k, B.pose[0] + 7ll * (k + 1), B.sb[0] + 9ll * (k + 1), r, r + 15))
+            bad = 1;
+        else
+            for (int i = 0; i < 15; ++i) cost += 0.5 * r[i] * r[i];
+    }
+    __syncthreads();
+    for (int q = 0; q < 2; ++q) {
+        if (mw.imu[q] < 0 || bad) continue;
+        const int k = B.imuKf[mw.imu[q]];
+        const double* r = sc + 465 * q;
+        const double* J = r + 15;
+        auto colOf = [&](int a) {
+            return a < 6 ? M.poseCol[k] + a : a < 15 ? M.sbCol[k] + a - 6 : a < 21 ? M.poseCol[k + 1] + a - 15 : M.sbCol[k + 1] + a - 21;
+        };
+        for (int e = threadIdx.x; e < 930; e += blockDim.x) {
+            if (e < 900) {
+                const int a = e / 30, c = e % 30, ca = colOf(a), cc = colOf(c);
+                if (ca > cc) continue;  // upper triangle: each unordered pair once
+                double v = 0;
+                for (int i = 0; i < 15; ++i) v += J[30 * i + a] * J[30 * i + c];
+                H[(long long)ca * m + cc] += v;
+            } else {
+                const int a = e - 900;
+                double v = 0;
+                for (int i = 0; i < 15; ++i) v += J[30 * i + a] * r[i];
+                g[colOf(a)] += v;
+            }
+        }
+        __syncthreads();
+    }
+    if (wd.priorRank > 0 && !bad) {
+        const int rank = wd.priorRank, cols = wd.priorCols;
+        double* ps = B.priorScratch + wd.priorScratch0;
+        double* delta = ps;
+        double* D = delta + cols;
+        double* r = D + 6ll * cols;
+        double* J = r + rank;
+        for (int bk = threadIdx.x; bk < wd.priorBlocks; bk += blockDim.x) {
+            const int pb = wd.priorBlk0 + bk;
+            const int kind = B.priorKind[pb], off = B.priorOff[pb];
+            int aoff = 0;
+            for (int q = wd.priorBlk0; q < pb; ++q) {
+                const int kq = B.priorKind[q];
+                aoff += kq == CGMLI_PRIOR_SPEED_BIAS ? 9 : kq == CGMLI_PRIOR_TIME_OFFSET ? 1 : 7;
+            }
+            const double* ref = B.priorRef + wd.priorRef0 + aoff;
+            const double* x = blockValue(B, 0, kind, B.priorIndex[pb], w);
+            if (kind == CGMLI_PRIOR_POSE || kind == CGMLI_PRIOR_EXTRINSIC) {
+                poseMinus(x, ref, delta + off);
+                se3LeftJacobianInverse(delta + off, D + 6ll * off);
+            } else {
+                const int t = kind == CGMLI_PRIOR_SPEED_BIAS ? 9 : 1;
+                for (int i = 0; i < t; ++i) delta[off + i] = x[i] - ref[i];
+            }
+        }
+        __syncthreads();
+        const double* A = B.priorA + wd.priorA0;
+        const double* r0 = B.priorR0 + wd.priorR00;
+        for (int i = threadIdx.x; i < rank; i += blockDim.x) {
+            double v = r0[i];
+            for (int c = 0; c < cols; ++c) v += A[(long long)i * cols + c] * delta[c];
+            r[i] = v;
+            if (!isfinite(v)) bad = 1;
+            cost += 0.5 * v * v;
+        }
+        auto blockOf = [&](int c) {
+            int pb = wd.priorBlk0;
+            while (pb + 1 < wd.priorBlk0 + wd.priorBlocks && B.priorOff[pb + 1] <= c) ++pb;
+            return pb;
+        };
+        for (long long e = threadIdx.x; e < (long long)rank * cols; e += blockDim.x) {
+            const int i = (int)(e / cols), c = (int)(e % cols);
+            const int pb = blockOf(c);
+            const int kind = B.priorKind[pb], off = B.priorOff[pb];
+            double v;
+            if (kind == CGMLI_PRIOR_POSE || kind == CGMLI_PRIOR_EXTRINSIC) {
+                v = 0;
+                for (int j = 0; j < 6; ++j) v += A[(long long)i * cols + off + j] * D[6ll * (off + j) + (c - off)];
+            } else {
+                v = A[(long long)i * cols + c];
+            }
+            J[e] = v;
+        }
+        __syncthreads();
+        auto colOf = [&](int c) {
+            const int pb = blockOf(c);
+            const int kind = B.priorKind[pb], gi = B.priorIndex[pb], off = B.priorOff[pb];
+            const int base = kind == CGMLI_PRIOR_POSE ? M.poseCol[gi] : kind == CGMLI_PRIOR_SPEED_BIAS ? M.sbCol[gi]
+                             : kind == CGMLI_PRIOR_EXTRINSIC ? M.extCol[gi] : mw.tdCol;
+            return base + (c - off);
+        };
+        for (long long e = threadIdx.x; e < (long long)cols * (cols + 1); e += blockDim.x) {
+            const int p = (int)(e / cols), q = (int)(e % cols);
+            const int cq = colOf(q);
+            if (p < cols) {
+                const int cp = colOf(p);
+                if (cp > cq) continue;
+                double v = 0;
+                for (int i = 0; i < rank; ++i) v += J[(long long)i * cols + p] * J[(long long)i * cols + q];
+                H[(long long)cp * m + cq] += v;
+            } else {
+                double v = 0;
+                for (int i = 0; i < rank; ++i) v += J[(long long)i * cols + q] * r[i];
+                g[cq] += v;
+            }
+        }
+    }
+    cost = mBlockSum(cost, red);
+    if (threadIdx.x == 0) {
+        M.stats[4 * w + 0] += cost;
+        M.stats[4 * w + 1] += 2 * cost;
+        if (bad) M.status[w] = CGMLI_E_NONFINITE;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Cyclic Jacobi eigensolver of a symmetric n x n row-major matrix A (n <= 1024),
+// one CTA.  Each round applies n/2 rotations on disjoint index pairs (the
+// round-robin ordering), which commute, so a round is one row pass and one
+// column pass.  A pair is rotated only while |a_pq| > 1e-16 sqrt|a_pp a_qq|;
+// a sweep without rotation ends the iteration.  On return the diagonal of A
+// holds the eigenvalues and the columns of V the eigenvectors.
+__device__ void jacobiEigen(double* A, double* V, int n, int maxSweeps) {
+    __shared__ short pairP[512], pairQ[512];
+    __shared__ double rc[512], rs[512];
+    __shared__ int rotated;
+    const int np = (n + 1) & ~1;  // even count; index n (if odd) is a dummy
+    const int half = np / 2;
+    for (long long i = threadIdx.x; i < (long long)n * n; i += blockDim.x) V[i] = (i / n == i % n) ? 1.0 : 0.0;
+    __syncthreads();
+    for (int sweep = 0; sweep < maxSweeps; ++sweep) {
+        if (threadIdx.x == 0) rotated = 0;
+        __syncthreads();
+        for (int round = 0; round < np - 1; ++round) {
+            for (int i = threadIdx.x; i < half; i += blockDim.x) {
+                const int a = i == 0 ? 0 : 1 + (i - 1 + round) % (np - 1);
+                const int b = 1 + (np - 2 - i + round) % (np - 1);
+                const int p = a < b ? a : b, q = a < b ? b : a;
+                pairP[i] = (short)p;
+                pairQ[i] = (short)q;
+                double c = 1, s = 0;
+                if (q < n) {
+                    const double apq = A[(long long)p * n + q], app = A[(long long)p * n + p], aqq = A[(long long)q * n + q];
+                    if (fabs(apq) > 1e-16 * sqrt(fabs(app * aqq)) && apq != 0.0) {
+                        const double tau = (aqq - app) / (2 * apq);
+                        const double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1 + tau * tau));
+                        c = 1 / sqrt(1 + t * t);
+                        s = t * c;
+                        rotated = 1;
+                    }
+                }
+                rc[i] = c;
+                rs[i] = s;
+            }
+            __syncthreads();
+            // rows p, q of A
+            for (int t = threadIdx.x; t < half * n; t += blockDim.x) {
+                const int i = t / n, k = t % n;
+                if (rs[i] == 0.0) continue;
+                const long long p = pairP[i], q = pairQ[i];
+                const double c = rc[i], s = rs[i];
+                const double apk = A[p * n + k], aqk = A[q * n + k];
+                A[p * n + k] = c * apk - s * aqk;
+                A[q * n + k] = s * apk + c * aqk;
+            }
+            __syncthreads();
+            // columns p, q of A and V
+            for (int t = threadIdx.x; t < half * n; t += blockDim.x) {
+                const int k = t / half, i = t % half;
+                if (rs[i] == 0.0) continue;
+                const int p = pairP[i], q = pairQ[i];
+                const double c = rc[i], s = rs[i];
+                const long long row = (long long)k * n;
+                const double akp = A[row + p], akq = A[row + q];
+                A[row + p] = c * akp - s * akq;
+                A[row + q] = s * akp + c * akq;
+                const double vkp = V[row + p], vkq = V[row + q];
+                V[row + p] = c * vkp - s * vkq;
+                V[row + q] = s * vkp + c * vkq;
+            }
+            __syncthreads();
+        }
+        if (!rotated) break;
+        __syncthreads();
+    }
+}
+
+// Ascending position of each eigenvalue (ties by index); pos has n entries.
+__device__ void ascendingPositions(const double* ev, int n, int* pos) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double v = ev[i];
+        int p = 0;
+        for (int j = 0; j < n; ++j) p += ev[j] < v || (ev[j] == v && j < i);
+        pos[i] = p;
+    }
+    __syncthreads();
+}
+
+// Victim elimination: X = pinv(Hmm) [Hmr | bm] with the eigen cutoff, then the
+// symmetrized separator information Hrr - Hmr^T X and gradient br - Hmr^T y.
+__global__ void __launch_bounds__(kMargThreads) k_marg_victim(MargBatch M) {
+    const int w = blockIdx.x;
+    const MargWin mw = M.win[w];
+    const int m = mw.m, nm = mw.nm, nr = mw.nr, cols = nr + 1;
+    if (m == 0 || nr == 0 || M.status[w] != CGMLI_OK) return;
+    const double* H = M.H + mw.H0;
+    const double* bw = M.b + mw.vec0;
+    double* E = M.sepH + mw.sep0;
+    double* bs = M.sepB + mw.vec0;
+    __shared__ double Hm[15 * 15], Um[15 * 15], ev[15];
+    __shared__ double red[kMargThreads / 32];
+    double reduction = 0;
+    if (nm > 0) {
+        for (int i = threadIdx.x; i < nm * nm; i += blockDim.x) Hm[i] = symAt(H, i / nm, i % nm, m);
+        __syncthreads();
+        jacobiEigen(Hm, Um, nm, 60);
+        double vmax = -INFINITY, vmin = INFINITY;
+        for (int i = 0; i < nm; ++i) { vmax = fmax(vmax, Hm[i * nm + i]); vmin = fmin(vmin, Hm[i * nm + i]); }
+        const double cutoff = fmax(1e-12, 1e-9 * fmax(0.0, vmax));
+        if (vmin < -10 * cutoff || !isfinite(vmin) || !isfinite(vmax)) {
+            if (threadIdx.x == 0) M.status[w] = CGMLI_E_INDEFINITE;
+            return;
+        }
+        if (threadIdx.x < nm) ev[threadIdx.x] = Hm[threadIdx.x * nm + threadIdx.x];
+        __syncthreads();
+        double* P = M.X + mw.x0;              // nm x cols: U^T rhs / lambda
+        double* X = P + (long long)nm * cols; // nm x cols
+        for (int t = threadIdx.x; t < nm * cols; t += blockDim.x) {
+            const int i = t / cols, c = t % cols;
+            double v = 0;
+            for (int k = 0; k < nm; ++k) v += Um[k * nm + i] * (c < nr ? H[(long long)k * m + nm + c] : bw[k]);
+            P[t] = ev[i] > cutoff ? v / ev[i] : 0.0;
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < nm * cols; t += blockDim.x) {
+            const int i = t / cols, c = t % cols;
+            double v = 0;
+            for (int k = 0; k < nm; ++k) v += Um[i * nm + k] * P[(long long)k * cols + c];
+            X[t] = v;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < nm; i += blockDim.x) reduction += 0.5 * bw[i] * X[(long long)i * cols + nr];
+        for (long long t = threadIdx.x; t < (long long)nr * nr; t += blockDim.x) {
+            const int i = (int)(t / nr), j = (int)(t % nr);
+            double v1 = symAt(H, nm + i, nm + j, m), v2 = v1;
+            for (int k = 0; k < nm; ++k) {
+                v1 -= H[(long long)k * m + nm + i] * X[(long long)k * cols + j];
+                v2 -= H[(long long)k * m + nm + j] * X[(long long)k * cols + i];
+            }
+            E[t] = 0.5 * (v1 + v2);
+        }
+        for (int i = threadIdx.x; i < nr; i += blockDim.x) {
+            double v = bw[nm + i];
+            for (int k = 0; k < nm; ++k) v -= H[(long long)k * m + nm + i] * X[(long long)k * cols + nr];
+            bs[i] = v;
+        }
+    } else {
+        for (long long t = threadIdx.x; t < (long long)nr * nr; t += blockDim.x)
+            E[t] = symAt(H, (int)(t / nr), (int)(t % nr), m);
+        for (int i = threadIdx.x; i < nr; i += blockDim.x) bs[i] = bw[i];
+    }
+    reduction = mBlockSum(reduction, red);
+    if (threadIdx.x == 0) M.stats[4 * w + 2] += reduction;
+}
+
+// Eigendecomposition of the separator information and the square-root prior,
+// rows in ascending eigenvalue order.
+__global__ void __launch_bounds__(kMargThreads) k_marg_eigen(MargBatch M) {
+    const int w = blockIdx.x;
+    const MargWin mw = M.win[w];
+    const int nr = mw.nr;
+    if (mw.m == 0 || nr == 0 || M.status[w] != CGMLI_OK) {
+        if (threadIdx.x == 0) M.rank[w] = 0;
+        return;
+    }
+    double* E = M.sepH + mw.sep0;
+    double* V = M.sepV + mw.sep0;
+    double* ev = M.evals + mw.vec0;
+    const double* bs = M.sepB + mw.vec0;
+    __shared__ int pos[kMargMaxSep];
+    __shared__ double red[kMargThreads / 32];
+    jacobiEigen(E, V, nr, 60);
+    for (int i = threadIdx.x; i < nr; i += blockDim.x) ev[i] = E[(long long)i * nr + i];
+    __syncthreads();
+    double vmax = -INFINITY, vmin = INFINITY;
+    bool finite = true;
+    for (int i = threadIdx.x; i < nr; i += blockDim.x) {
+        vmax = fmax(vmax, ev[i]);
+        vmin = fmin(vmin, ev[i]);
+        finite = finite && isfinite(ev[i]);
+    }
+    vmax = mBlockMax(vmax, red);
+    vmin = -mBlockMax(-vmin, red);
+    const double nonFinite = mBlockMax(finite ? 0.0 : 1.0, red);
+    const double cutoff = fmax(1e-12, 1e-9 * fmax(0.0, vmax));
+    if (nonFinite > 0 || vmin < -10 * cutoff) {
+        if (threadIdx.x == 0) { M.status[w] = nonFinite > 0 ? CGMLI_E_NONFINITE : CGMLI_E_INDEFINITE; M.rank[w] = 0; }
+        return;
+    }
+    ascendingPositions(ev, nr, pos);
+    double low = 0;
+    for (int i = threadIdx.x; i < nr; i += blockDim.x) low += ev[i] > cutoff ? 0.0 : 1.0;
+    const int nLow = (int)mBlockSum(low, red);
+    double* A = M.A + mw.sep0;
+    double* r0 = M.r0 + mw.vec0;
+    for (long long t = threadIdx.x; t < (long long)nr * nr; t += blockDim.x) {
+        const int i = (int)(t / nr), k = (int)(t % nr);  // eigenpair i, component k
+        if (!(ev[i] > cutoff)) continue;
+        A[(long long)(pos[i] - nLow) * nr + k] = sqrt(ev[i]) * V[(long long)k * nr + i];
+    }
+    for (int i = threadIdx.x; i < nr; i += blockDim.x) {
+        if (!(ev[i] > cutoff)) continue;
+        double ub = 0;
+        for (int k = 0; k < nr; ++k) ub += V[(long long)k * nr + i] * bs[k];
+        r0[pos[i] - nLow] = ub / sqrt(ev[i]);
+    }
+    if (threadIdx.x == 0) {
+        M.rank[w] = nr - nLow;
+        M.stats[4 * w + 3] = cutoff;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Dense helpers (one CTA).  H, rhs, solution column-major; H is read from its
+// lower triangle like cusolverDnDsyevd with CUBLAS_FILL_MODE_LOWER.
+__global__ void __launch_bounds__(kMargThreads) k_dense_eigen(const double* H, int n, double* work, double* evals, double* evecs,
+                                                              int* status) {
+    double* A = work;
+    double* V = work + (long long)n * n;
+    __shared__ int pos[kMargMaxSep];
+    for (long long t = threadIdx.x; t < (long long)n * n; t += blockDim.x) {
+        const int i = (int)(t / n), j = (int)(t % n);
+        A[t] = i >= j ? H[i + (long long)j * n] : H[j + (long long)i * n];
+    }
+    __syncthreads();
+    jacobiEigen(A, V, n, 60);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        evals[n + i] = A[(long long)i * n + i];  // unsorted copy in the upper half of evals
+        if (!isfinite(evals[n + i])) *status = CGMLI_E_NONFINITE;
+    }
+    __syncthreads();
+    ascendingPositions(evals + n, n, pos);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) evals[pos[i]] = evals[n + i];
+    for (long long t = threadIdx.x; t < (long long)n * n; t += blockDim.x) {
+        const int k = (int)(t / n), i = (int)(t % n);  // row k of V, eigenpair i
+        evecs[k + (long long)pos[i] * n] = V[t];
+    }
+}
+// projected = U^T rhs with the cutoff (eigenvalues ascending, U column-major).
+__global__ void k_dense_psd_project(const double* evals, const double* U, const double* rhs, int n, int columns, double absCut,
+                                    double relCut, double* projected, int* status) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n * columns) return;
+    const int i = (int)(t % n), c = (int)(t / n);
+    const double cutoff = fmax(absCut, relCut * fmax(0.0, evals[n - 1])), v = evals[i];
+    if (v < -10 * cutoff || !isfinite(v)) *status = CGMLI_E_INDEFINITE;
+    double s = 0;
+    for (int k = 0; k < n; ++k) s += U[k + (long long)i * n] * rhs[k + (long long)c * n];
+    projected[t] = v > cutoff ? s / v : 0.0;
+}
+// solution = U projected
+__global__ void k_dense_psd_expand(const double* U, const double* projected, int n, int columns, double* solution) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n * columns) return;
+    const int i = (int)(t % n), c = (int)(t / n);
+    double s = 0;
+    for (int k = 0; k < n; ++k) s += U[i + (long long)k * n] * projected[k + (long long)c * n];
+    solution[t] = s;
+}
+// [H | g] -= coupling^T solution; coupling nm x nr, solution nm x (nr + 1).
+__global__ void k_dense_subtract(const double* coupling, const double* solution, int nm, int nr, double* Hg) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nr * (nr + 1)) return;
+    const int i = (int)(t % nr), c = (int)(t / nr);
+    double s = 0;
+    for (int k = 0; k < nm; ++k) s += coupling[k + (long long)i * nm] * solution[k + (long long)c * nm];
+    Hg[t] -= s;
+}
+
+// ---------------------------------------------------------------------------------------
+size_t margVisualSmemBytes(int maxNc) {
+    return sizeof(double) * ((size_t)maxNc * (maxNc + 1) / 2 + 2 * maxNc + 32 * 50 + 32 * 4) + sizeof(short) * 32 * 25 +
+           sizeof(int) * 32;
+}
+cudaError_t configureMarginalization(size_t visualSmem) {
+    return cudaFuncSetAttribute(k_marg_visual, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)visualSmem);
+}
+// Returns the number of launches.
+int launchMarginalization(const DevBatch& B, const MargBatch& M, size_t visualSmem, cudaStream_t s) {
+    int n = 0;
+    if (M.numElim > 0) {
+        const int warps = 8;
+        k_marg_dmax<<<(M.numElim + warps - 1) / warps, 32 * warps, 0, s>>>(B, M);
+        k_marg_visual<<<M.numElim, kMargLmThreads, visualSmem, s>>>(B, M);
+        n += 2;
+    }
+    k_marg_retained<<<M.numWindows, 256, 0, s>>>(B, M);
+    k_marg_victim<<<M.numWindows, kMargThreads, 0, s>>>(M);
+    k_marg_eigen<<<M.numWindows, kMargThreads, 0, s>>>(M);
+    return n + 3;
+}
+void launchDenseEigen(const double* H, int n, double* work, double* evals, double* evecs, int* status, cudaStream_t s) {
+    k_dense_eigen<<<1, kMargThreads, 0, s>>>(H, n, work, evals, evecs, status);
+}
+void launchDensePsd(const double* evals, const double* U, const double* rhs, int n, int columns, double absCut, double relCut,
+                    double* projected, double* solution, int* status, cudaStream_t s) {
+    const long long count = (long long)n * columns;
+    const int blocks = (int)((count + 127) / 128);
+    k_dense_psd_project<<<blocks, 128, 0, s>>>(evals, U, rhs, n, columns, absCut, relCut, projected, status);
+    k_dense_psd_expand<<<blocks, 128, 0, s>>>(U, projected, n, columns, solution);
+}
+void launchDenseSubtract(const double* coupling, const double* solution, int nm, int nr, double* Hg, cudaStream_t s) {
+    const long long count = (long long)nr * (nr + 1);
+    k_dense_subtract<<<(int)((count + 127) / 128), 128, 0, s>>>(coupling, solution, nm, nr, Hg);
+}
+
+}  // namespace cgmli
