@@ -28,7 +28,7 @@ int launchIteration(const DevBatch& B, const int4* runs, const int2* tiles, size
                     int refinement, int maxIterations, int probe, double* Sdebug, cudaStream_t s, LaunchHook hook, void* ctx);
 int launchLmInit(const DevBatch& B, double lambda0, cudaStream_t s);
 size_t margVisualSmemBytes(int maxNc);
-cudaError_t configureMarginalization(size_t visualSmem);
+cudaError_t configureMarginalization(size_t visualSmem, int maxNr, long long* eigenSmem);
 int launchMarginalization(const DevBatch& B, const MargBatch& M, size_t visualSmem, cudaStream_t s);
 void launchDenseEigen(const double* H, int n, double* work, double* evals, double* evecs, int* status, cudaStream_t s);
 void launchDensePsd(const double* evals, const double* U, const double* rhs, int n, int columns, double absCut, double relCut,
@@ -844,7 +844,10 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
     }
     cudaStream_t st = S->stream;
     const size_t smem = margVisualSmemBytes(std::max(maxNc, 1));
-    CK(configureMarginalization(smem));
+    int maxNr = 1;
+    for (const auto& mw : mwv) maxNr = std::max(maxNr, mw.nr);
+    long long eigenSmem = 0;
+    CK(configureMarginalization(smem, maxNr, &eigenSmem));
     CK(S->dMargWin.upload(mwv, st));
     CK(S->dMargElim.upload(elims, st));
     CK(S->margCols.upload(cols, st));
@@ -866,6 +869,7 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
     M = MargBatch{};
     M.numWindows = W;
     M.numElim = (int)elims.size();
+    M.eigenSmem = eigenSmem;
     M.win = S->dMargWin.p; M.elim = S->dMargElim.p; M.cols = S->margCols.p; M.obsMap = S->margObsMap.p;
     M.poseCol = S->margPoseCol.p; M.sbCol = S->margSbCol.p; M.extCol = S->margExtCol.p;
     M.H = S->margH.p; M.b = S->margB.p; M.sepH = S->margSepH.p; M.sepV = S->margSepV.p; M.sepB = S->margSepB.p;

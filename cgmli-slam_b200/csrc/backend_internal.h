@@ -109,6 +109,7 @@ struct MargWin {
 struct MargElim { int lm, win, nc, col0, obs0; };  // device landmark, window, local columns, offsets
 struct MargBatch {
     int numWindows, numElim;
+    long long eigenSmem;  // dynamic shared memory of the eigen CTA (packed separator, eigenvectors when they fit)
     const MargWin* win;
     const MargElim* elim;
     const int* cols;     // local column -> marginalization column

@@ -351,17 +351,25 @@ __global__ void __launch_bounds__(256) k_marg_retained(DevBatch B, MargBatch M) 
 // Cyclic Jacobi eigensolver of a symmetric n x n row-major matrix A (n <= 1024),
 // one CTA.  Each round applies n/2 rotations on disjoint index pairs (the
 // round-robin ordering), which commute, so a round is one row pass and one
-// column pass.  A pair is rotated only while |a_pq| > 1e-16 sqrt|a_pp a_qq|;
-// a sweep without rotation ends the iteration.  On return the diagonal of A
+// column pass.  A pair is rotated only while |a_pq| > 1e-15 sqrt|a_pp a_qq|
+// and |a_pq| > 1e-16 |A|_F: entries at the rounding level of a rotation are
+// left alone (rotating them only makes new noise), so the off-diagonal mass
+// left at the end is below n 1e-16 |A|_F; a sweep without rotation ends the
+// iteration.  On return the diagonal of A
 // holds the eigenvalues and the columns of V the eigenvectors.
 __device__ void jacobiEigen(double* A, double* V, int n, int maxSweeps) {
     __shared__ short pairP[512], pairQ[512];
     __shared__ double rc[512], rs[512];
     __shared__ int rotated;
+    __shared__ double normRed[32];
     const int np = (n + 1) & ~1;  // even count; index n (if odd) is a dummy
     const int half = np / 2;
-    for (long long i = threadIdx.x; i < (long long)n * n; i += blockDim.x) V[i] = (i / n == i % n) ? 1.0 : 0.0;
-    __syncthreads();
+    double fro = 0;
+    for (long long i = threadIdx.x; i < (long long)n * n; i += blockDim.x) {
+        V[i] = (i / n == i % n) ? 1.0 : 0.0;
+        fro += A[i] * A[i];
+    }
+    const double floorAbs = 1e-16 * sqrt(mBlockSum(fro, normRed));
     for (int sweep = 0; sweep < maxSweeps; ++sweep) {
         if (threadIdx.x == 0) rotated = 0;
         __syncthreads();
@@ -375,7 +383,7 @@ __device__ void jacobiEigen(double* A, double* V, int n, int maxSweeps) {
                 double c = 1, s = 0;
                 if (q < n) {
                     const double apq = A[(long long)p * n + q], app = A[(long long)p * n + p], aqq = A[(long long)q * n + q];
-                    if (fabs(apq) > 1e-16 * sqrt(fabs(app * aqq)) && apq != 0.0) {
+                    if (fabs(apq) > 1e-15 * sqrt(fabs(app * aqq)) && fabs(apq) > floorAbs) {
                         const double tau = (aqq - app) / (2 * apq);
                         const double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1 + tau * tau));
                         c = 1 / sqrt(1 + t * t);
@@ -411,6 +419,104 @@ __device__ void jacobiEigen(double* A, double* V, int n, int maxSweeps) {
                 const double vkp = V[row + p], vkq = V[row + q];
                 V[row + p] = c * vkp - s * vkq;
                 V[row + q] = s * vkp + c * vkq;
+            }
+            __syncthreads();
+        }
+        if (!rotated) break;
+        __syncthreads();
+    }
+}
+
+// The same Jacobi iteration on a symmetric matrix kept as its packed upper
+// triangle (row-major, r <= c), typically in shared memory.  Rotations of
+// disjoint pairs commute, so one round updates every 2x2 block between pairs
+// i <= j once: B' = R_i^T B R_j with R = [[c, s], [-s, c]].  Eigenvectors are
+// accumulated as the ROWS of Vt (Vt' = R^T Vt), so their updates are
+// contiguous.  On return Ap's diagonal holds the eigenvalues.
+__device__ __forceinline__ int pkUp(int r, int c, int n) { return r * n - r * (r - 1) / 2 + (c - r); }
+__device__ __forceinline__ int pkSym(int r, int c, int n) { return r <= c ? pkUp(r, c, n) : pkUp(c, r, n); }
+__device__ void jacobiPacked(double* Ap, double* Vt, int n, int maxSweeps) {
+    __shared__ short pairP[512], pairQ[512];
+    __shared__ double rc[512], rs[512];
+    __shared__ int rotated;
+    __shared__ double normRed[32];
+    const int np = (n + 1) & ~1;
+    const int half = np / 2;
+    const int blocks = half * (half + 1) / 2;
+    for (long long i = threadIdx.x; i < (long long)n * n; i += blockDim.x) Vt[i] = (i / n == i % n) ? 1.0 : 0.0;
+    double fro = 0;
+    for (int r = threadIdx.x; r < n; r += blockDim.x)
+        for (int c = r; c < n; ++c) fro += (r == c ? 1.0 : 2.0) * Ap[pkUp(r, c, n)] * Ap[pkUp(r, c, n)];
+    const double floorAbs = 1e-16 * sqrt(mBlockSum(fro, normRed));
+    for (int sweep = 0; sweep < maxSweeps; ++sweep) {
+        if (threadIdx.x == 0) rotated = 0;
+        __syncthreads();
+        for (int round = 0; round < np - 1; ++round) {
+            for (int i = threadIdx.x; i < half; i += blockDim.x) {
+                const int a = i == 0 ? 0 : 1 + (i - 1 + round) % (np - 1);
+                const int b = 1 + (np - 2 - i + round) % (np - 1);
+                const int p = a < b ? a : b, q = a < b ? b : a;
+                pairP[i] = (short)p;
+                pairQ[i] = (short)q;
+                double c = 1, s = 0;
+                if (q < n) {
+                    const double apq = Ap[pkUp(p, q, n)], app = Ap[pkUp(p, p, n)], aqq = Ap[pkUp(q, q, n)];
+                    if (fabs(apq) > 1e-15 * sqrt(fabs(app * aqq)) && fabs(apq) > floorAbs) {
+                        const double tau = (aqq - app) / (2 * apq);
+                        const double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1 + tau * tau));
+                        c = 1 / sqrt(1 + t * t);
+                        s = t * c;
+                        rotated = 1;
+                    }
+                }
+                rc[i] = c;
+                rs[i] = s;
+            }
+            __syncthreads();
+            for (int bidx = threadIdx.x; bidx < blocks; bidx += blockDim.x) {
+                // (i, j), i <= j, from the packed-upper enumeration of a half x half triangle
+                int i = (int)((2.0f * half + 1 - sqrtf((2.0f * half + 1) * (2.0f * half + 1) - 8.0f * bidx)) * 0.5f);
+                if (i < 0) i = 0;
+                while (i > 0 && i * half - i * (i - 1) / 2 > bidx) --i;
+                while ((i + 1) * half - (i + 1) * i / 2 <= bidx) ++i;
+                const int j = i + (bidx - (i * half - i * (i - 1) / 2));
+                const double si = rs[i], sj = rs[j];
+                if (si == 0.0 && sj == 0.0) continue;
+                const double ci = rc[i], cj = rc[j];
+                const int pi = pairP[i], qi = pairQ[i], pj = pairP[j], qj = pairQ[j];
+                if (i == j) {
+                    const int kpp = pkUp(pi, pi, n), kpq = pkUp(pi, qi, n), kqq = pkUp(qi, qi, n);
+                    const double app = Ap[kpp], apq = Ap[kpq], aqq = Ap[kqq];
+                    const double t00 = ci * app - si * apq, t01 = si * app + ci * apq;
+                    const double t10 = ci * apq - si * aqq, t11 = si * apq + ci * aqq;
+                    Ap[kpp] = ci * t00 - si * t10;
+                    Ap[kpq] = ci * t01 - si * t11;
+                    Ap[kqq] = si * t01 + ci * t11;
+                } else {
+                    const bool rowQ = qi < n, colQ = qj < n;
+                    const int k00 = pkSym(pi, pj, n);
+                    const int k01 = colQ ? pkSym(pi, qj, n) : 0;
+                    const int k10 = rowQ ? pkSym(qi, pj, n) : 0;
+                    const int k11 = rowQ && colQ ? pkSym(qi, qj, n) : 0;
+                    const double b00 = Ap[k00], b01 = colQ ? Ap[k01] : 0.0, b10 = rowQ ? Ap[k10] : 0.0,
+                                 b11 = rowQ && colQ ? Ap[k11] : 0.0;
+                    const double t00 = cj * b00 - sj * b01, t01 = sj * b00 + cj * b01;
+                    const double t10 = cj * b10 - sj * b11, t11 = sj * b10 + cj * b11;
+                    Ap[k00] = ci * t00 - si * t10;
+                    if (colQ) Ap[k01] = ci * t01 - si * t11;
+                    if (rowQ) Ap[k10] = si * t00 + ci * t10;
+                    if (rowQ && colQ) Ap[k11] = si * t01 + ci * t11;
+                }
+            }
+            for (int t = threadIdx.x; t < half * n; t += blockDim.x) {
+                const int i = t / n, k = t % n;
+                const double s = rs[i];
+                if (s == 0.0) continue;
+                const double c = rc[i];
+                const long long p = pairP[i], q = pairQ[i];
+                const double vp = Vt[p * n + k], vq = Vt[q * n + k];
+                Vt[p * n + k] = c * vp - s * vq;
+                Vt[q * n + k] = s * vp + c * vq;
             }
             __syncthreads();
         }
@@ -507,14 +613,33 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_eigen(MargBatch M) {
         if (threadIdx.x == 0) M.rank[w] = 0;
         return;
     }
+    extern __shared__ double eigSmem[];
     double* E = M.sepH + mw.sep0;
-    double* V = M.sepV + mw.sep0;
     double* ev = M.evals + mw.vec0;
     const double* bs = M.sepB + mw.vec0;
     __shared__ int pos[kMargMaxSep];
     __shared__ double red[kMargThreads / 32];
-    jacobiEigen(E, V, nr, 60);
-    for (int i = threadIdx.x; i < nr; i += blockDim.x) ev[i] = E[(long long)i * nr + i];
+    // component k of eigenvector i is Vv[i * si + k * sk]
+    const double* Vv;
+    long long si, sk;
+    const long long packed = (long long)nr * (nr + 1) / 2;
+    if (packed * 8 <= M.eigenSmem) {
+        double* Ap = eigSmem;
+        double* Vt = (packed + (long long)nr * nr) * 8 <= M.eigenSmem ? eigSmem + packed : M.sepV + mw.sep0;
+        for (long long t = threadIdx.x; t < (long long)nr * nr; t += blockDim.x) {
+            const int i = (int)(t / nr), j = (int)(t % nr);
+            if (i <= j) Ap[pkUp(i, j, nr)] = E[t];
+        }
+        __syncthreads();
+        jacobiPacked(Ap, Vt, nr, 60);
+        for (int i = threadIdx.x; i < nr; i += blockDim.x) ev[i] = Ap[pkUp(i, i, nr)];
+        Vv = Vt; si = nr; sk = 1;
+    } else {
+        double* V = M.sepV + mw.sep0;
+        jacobiEigen(E, V, nr, 60);
+        for (int i = threadIdx.x; i < nr; i += blockDim.x) ev[i] = E[(long long)i * nr + i];
+        Vv = V; si = 1; sk = nr;
+    }
     __syncthreads();
     double vmax = -INFINITY, vmin = INFINITY;
     bool finite = true;
@@ -540,12 +665,12 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_eigen(MargBatch M) {
     for (long long t = threadIdx.x; t < (long long)nr * nr; t += blockDim.x) {
         const int i = (int)(t / nr), k = (int)(t % nr);  // eigenpair i, component k
         if (!(ev[i] > cutoff)) continue;
-        A[(long long)(pos[i] - nLow) * nr + k] = sqrt(ev[i]) * V[(long long)k * nr + i];
+        A[(long long)(pos[i] - nLow) * nr + k] = sqrt(ev[i]) * Vv[i * si + k * sk];
     }
     for (int i = threadIdx.x; i < nr; i += blockDim.x) {
         if (!(ev[i] > cutoff)) continue;
         double ub = 0;
-        for (int k = 0; k < nr; ++k) ub += V[(long long)k * nr + i] * bs[k];
+        for (int k = 0; k < nr; ++k) ub += Vv[i * si + k * sk] * bs[k];
         r0[pos[i] - nLow] = ub / sqrt(ev[i]);
     }
     if (threadIdx.x == 0) {
@@ -616,8 +741,23 @@ size_t margVisualSmemBytes(int maxNc) {
     return sizeof(double) * ((size_t)maxNc * (maxNc + 1) / 2 + 2 * maxNc + 32 * 50 + 32 * 4) + sizeof(short) * 32 * 25 +
            sizeof(int) * 32;
 }
-cudaError_t configureMarginalization(size_t visualSmem) {
-    return cudaFuncSetAttribute(k_marg_visual, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)visualSmem);
+// Sets the dynamic shared memory limits of the marginalization kernels for a
+// batch whose largest separator has maxNr columns; returns the eigen CTA's
+// dynamic shared memory in eigenSmem.
+cudaError_t configureMarginalization(size_t visualSmem, int maxNr, long long* eigenSmem) {
+    cudaError_t e = cudaFuncSetAttribute(k_marg_visual, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)visualSmem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, optin = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess) return e;
+    cudaFuncAttributes fa;
+    if ((e = cudaFuncGetAttributes(&fa, k_marg_eigen)) != cudaSuccess) return e;
+    const long long avail = (long long)optin - (long long)fa.sharedSizeBytes;
+    const long long n = maxNr, want = 8 * (n * (n + 1) / 2 + n * n), packedOnly = 8 * (n * (n + 1) / 2);
+    long long use = want <= avail ? want : (packedOnly <= avail ? avail : 0);
+    if (use < 0) use = 0;
+    *eigenSmem = use;
+    return cudaFuncSetAttribute(k_marg_eigen, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)use);
 }
 // Returns the number of launches.
 int launchMarginalization(const DevBatch& B, const MargBatch& M, size_t visualSmem, cudaStream_t s) {
@@ -630,7 +770,7 @@ int launchMarginalization(const DevBatch& B, const MargBatch& M, size_t visualSm
     }
     k_marg_retained<<<M.numWindows, 256, 0, s>>>(B, M);
     k_marg_victim<<<M.numWindows, kMargThreads, 0, s>>>(M);
-    k_marg_eigen<<<M.numWindows, kMargThreads, 0, s>>>(M);
+    k_marg_eigen<<<M.numWindows, kMargThreads, (size_t)M.eigenSmem, s>>>(M);
     return n + 3;
 }
 void launchDenseEigen(const double* H, int n, double* work, double* evals, double* evecs, int* status, cudaStream_t s) {
