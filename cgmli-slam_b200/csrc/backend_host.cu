@@ -247,6 +247,15 @@ void cgmli_default_options(cgmli_solver_options* o) {
 int cgmli_solver_create(int device, const cgmli_solver_options* options, cgmli_solver** out) {
     if (!out) return fail(CGMLI_E_INVALID, "null output handle");
     *out = nullptr;
+    if (options) {
+        if (options->precision != CGMLI_PRECISION_FP64 && options->precision != CGMLI_PRECISION_MIXED)
+            return fail(CGMLI_E_INVALID, "unknown precision");
+        if (options->precision == CGMLI_PRECISION_MIXED) return fail(CGMLI_E_UNSUPPORTED, "mixed precision is not built");
+        if (options->refinement_steps < 0 || options->refinement_steps > 2) return fail(CGMLI_E_INVALID, "refinement_steps outside 0..2");
+        if (!(options->initial_lambda > 0)) return fail(CGMLI_E_INVALID, "initial_lambda must be positive");
+        if (options->slabs_per_window != 0 || options->threads_per_block != 0)
+            return fail(CGMLI_E_UNSUPPORTED, "slabs_per_window / threads_per_block are reserved and must be 0");
+    }
     int count = 0;
     cudaError_t e = cudaGetDeviceCount(&count);
     if (e != cudaSuccess || count == 0) return fail(CGMLI_E_CUDA, "no CUDA device available");

@@ -115,11 +115,12 @@ typedef struct cgmli_window {
 } cgmli_window;
 
 typedef struct cgmli_solver_options {
-    int precision;           /* CGMLI_PRECISION_FP64 or _MIXED (FP32 Jacobians, FP64 sums) */
+    int precision;           /* CGMLI_PRECISION_FP64; _MIXED (FP32 Jacobians, FP64 sums) is
+                                rejected with CGMLI_E_UNSUPPORTED by this build */
     int refinement_steps;    /* iterative refinement after the FP64 Cholesky (0..2) */
     double initial_lambda;   /* reference: 1e-4 */
-    int slabs_per_window;    /* CTAs per window in the linearization, 0 = choose */
-    int threads_per_block;   /* linearization CTA size, 0 = choose (autotuned) */
+    int slabs_per_window;    /* reserved, must be 0 */
+    int threads_per_block;   /* reserved, must be 0 */
 } cgmli_solver_options;
 
 typedef struct cgmli_solve_report {
