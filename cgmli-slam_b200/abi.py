@@ -129,4 +129,5 @@ BACKEND_SYMBOLS = [
     "cgmli_solver_read_prior", "cgmli_marg_eigen", "cgmli_marg_psd_solve", "cgmli_marg_subtract",
     "cgmli_solver_checkpoint", "cgmli_solver_rollback", "cgmli_solver_kernel_times",
 ]
-KERNEL_NAMES = ["zero_acc", "linearize", "retained", "factor", "candidate", "backsub_trial", "retained_trial", "lm_update", "accept"]
+KERNEL_NAMES = ["zero_acc", "linearize", "retained", "factor", "candidate", "backsub_trial", "retained_trial", "lm_update", "accept",
+                "lin_pairs", "lin_schur"]

@@ -21,11 +21,12 @@
 #include "backend_internal.h"
 
 namespace cgmli {
-size_t linearizeSmemBytes();
+size_t linearizeSmemBytes(int maxNs);
 size_t factorSmemBytes(int maxNr);
 cudaError_t configureKernels(size_t linSmem, size_t facSmem);
-int launchIteration(const DevBatch& B, const int4* runs, const int2* tiles, size_t linSmem, size_t facSmem,
-                    int refinement, int maxIterations, int probe, double* Sdebug, cudaStream_t s, LaunchHook hook, void* ctx);
+int schurRowsPerChunk(int Npc);
+int launchIteration(const DevBatch& B, const LaunchPlan& P, int refinement, int maxIterations, int probe, double* Sdebug,
+                    cudaStream_t s, LaunchHook hook, void* ctx);
 int launchLmInit(const DevBatch& B, double lambda0, cudaStream_t s);
 size_t margVisualSmemBytes(int maxNc);
 cudaError_t configureMarginalization(size_t visualSmem, int maxNr, long long* eigenSmem);
@@ -88,7 +89,9 @@ struct cgmli_solver {
     std::vector<int4> runs;       // {window, first tile, end tile, -}
     std::vector<int2> tiles;      // {first landmark, end landmark} (device order)
     std::vector<int> lmPerm;      // device landmark -> landmark index within its window
-    int maxNpc = 0, maxNr = 0;
+    std::vector<int4> pairChunks; // {window, first key-ordered observation, end, -}
+    std::vector<int4> schurChunks;// {window, first landmark, end landmark, -}
+    int maxNpc = 0, maxNr = 0, maxNs = 1;
     size_t linSmem = 0, facSmem = 0;
     int totalKf = 0, totalExt = 0, totalCam = 0, totalLm = 0, totalObs = 0, totalImu = 0;
     // device arrays
@@ -96,6 +99,9 @@ struct cgmli_solver {
     DArray<WinLM> dLm;
     DArray<int4> dRuns;
     DArray<int2> dTiles;
+    DArray<int4> dPairChunks, dSchurChunks;
+    DArray<int> obLm, keyOrder;
+    DArray<double> sch;
     DArray<double> camR, camT;
     DArray<int> camExt;
     DArray<int> lmWin, lmKf, lmCam, lmObsBegin, lmNs, lmNx, lmSupp0, supp, lmGroup;
@@ -143,6 +149,14 @@ struct cgmli_solver {
         }
         return evPool[evNext++];
     }
+    LaunchPlan plan() const {
+        LaunchPlan P{};
+        P.runs = dRuns.p; P.tiles = dTiles.p;
+        P.pairChunks = dPairChunks.p; P.numPairChunks = (int)pairChunks.size();
+        P.schurChunks = dSchurChunks.p; P.numSchurChunks = (int)schurChunks.size();
+        P.linSmem = linSmem; P.facSmem = facSmem; P.maxNs = maxNs;
+        return P;
+    }
     void collectKernelTimes() {
         for (const auto& u : evUsed) {
             float ms = 0;
@@ -167,6 +181,7 @@ struct cgmli_solver {
                                &solveStatus, &lmGroup, &lmNx, &obXslot};
         for (auto* a : ints) a->release();
         lmC0.release(); dWin.release(); dLm.release(); dRuns.release(); dTiles.release();
+        dPairChunks.release(); dSchurChunks.release(); obLm.release(); keyOrder.release(); sch.release();
         snapPose.release(); snapSb.release(); snapExt.release(); snapTd.release(); snapRho.release();
         dMargWin.release(); dMargElim.release();
         DArray<int>* mi[] = {&margCols, &margObsMap, &margPoseCol, &margSbCol, &margExtCol, &margRank, &margStatus};
@@ -285,9 +300,10 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     cudaStream_t st = S->stream;
     S->win.assign(count, WinDesc{});
     S->haveSnapshot = false;
-    S->runs.clear(); S->tiles.clear(); S->lmPerm.clear();
+    S->runs.clear(); S->tiles.clear(); S->lmPerm.clear(); S->pairChunks.clear(); S->schurChunks.clear();
     int kf = 0, ex = 0, cam = 0, lm = 0, ob = 0, im = 0, pblk = 0, vec = 0, groups = 0;
-    long long dense = 0, acc = 0, pA = 0, pR = 0, pRef = 0, imuS = 0, priS = 0, cOff = 0;
+    long long dense = 0, acc = 0, schOff = 0, pA = 0, pR = 0, pRef = 0, imuS = 0, priS = 0, cOff = 0;
+    std::vector<int> obLmv, keyOrderv;
     S->maxNpc = 0; S->maxNr = 0;
     std::vector<double> camR, camT, lmBearing, lmVel, lmTime, obBearing, obP, obVel, obTime;
     std::vector<int> camExt, lmWin, lmKf, lmCam, lmObsBegin, lmNs, lmNx, lmSupp0, supp, lmGroup, obKf, obKfl, obCam, obSlot, obXslot, imuKf;
@@ -310,13 +326,14 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
         d.Npc = 6 * d.K + d.ncalib;
         d.Nr = 15 * d.K + d.ncalib;
         d.kf0 = kf; d.ext0 = ex; d.cam0 = cam; d.lm0 = lm; d.obs0 = ob; d.imu0 = im;
-        d.vec0 = vec; d.dense0 = dense; d.acc0 = acc;
+        d.vec0 = vec; d.dense0 = dense; d.acc0 = acc; d.sch0 = schOff;
         d.huber = w.huber_scale; d.minInv = w.min_inverse_distance;
         S->maxNpc = std::max(S->maxNpc, d.Npc);
         S->maxNr = std::max(S->maxNr, d.Nr);
         vec += d.Nr;
         dense += (long long)d.Nr * d.Nr;
         acc += (long long)d.Npc * (d.Npc + 1) / 2 + 3ll * d.Npc;
+        schOff += (long long)d.Npc * (d.Npc + 1) / 2;
         pose.insert(pose.end(), w.poses, w.poses + 7 * d.K);
         sbv.insert(sbv.end(), w.speed_bias, w.speed_bias + 9 * d.K);
         extv.insert(extv.end(), w.extrinsics, w.extrinsics + 7 * d.E);
@@ -398,6 +415,7 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
             for (int k = 0; k < nobs; ++k) fo[k] = b + k;
             std::stable_sort(fo.begin(), fo.end(), [&](int x, int y) { return w.obs_kf[x] < w.obs_kf[y]; });
             for (int f : fo) {
+                obLmv.push_back(lm + q);
                 obKf.push_back(kf + w.obs_kf[f]);
                 obKfl.push_back(w.obs_kf[f]);
                 obCam.push_back(cam + w.obs_cam[f]);
@@ -415,6 +433,37 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
         if (d.L) {
             S->tiles.back().y = lm + d.L;
             S->runs.back().z = (int)S->tiles.size();
+        }
+        // observations of the window in key order (anchor kf, observer kf, anchor ext,
+        // observer ext): the J^T J pass sums the observations of one key together
+        {
+            const int F = (int)obKf.size() - ob;  // device observations of this window: [ob, ob + F)
+            auto keyOf = [&](int g) {
+                const int l = obLmv[g] - lm;  // device landmark within the window
+                const int a = lmKf[lm + l] - kf, b = obKf[g] - kf;
+                const int ea = camExt[lmCam[lm + l]] - ex, eb = camExt[obCam[g]] - ex;
+                return ((long long)(a * d.K + b) * d.E + ea) * d.E + eb;
+            };
+            const long long buckets = (long long)d.K * d.K * d.E * d.E;
+            std::vector<int> order(F);
+            if (buckets <= 4ll * F + 4096) {
+                std::vector<int> count(buckets + 1, 0);
+                for (int g = 0; g < F; ++g) ++count[keyOf(ob + g) + 1];
+                for (long long k = 0; k < buckets; ++k) count[k + 1] += count[k];
+                for (int g = 0; g < F; ++g) order[count[keyOf(ob + g)]++] = ob + g;
+            } else {
+                std::vector<std::pair<long long, int>> kv(F);
+                for (int g = 0; g < F; ++g) kv[g] = {keyOf(ob + g), ob + g};
+                std::sort(kv.begin(), kv.end());
+                for (int g = 0; g < F; ++g) order[g] = kv[g].second;
+            }
+            const int base = (int)keyOrderv.size();
+            keyOrderv.insert(keyOrderv.end(), order.begin(), order.end());
+            for (int c0 = 0; c0 < F; c0 += 32)
+                S->pairChunks.push_back(make_int4(i, base + c0, base + std::min(F, c0 + 32), 0));
+            const int rows = schurRowsPerChunk(d.Npc);
+            for (int l0 = 0; l0 < d.L; l0 += rows)
+                S->schurChunks.push_back(make_int4(i, lm + l0, lm + std::min(d.L, l0 + rows), 0));
         }
         (void)runTiles;
         // IMU
@@ -461,7 +510,10 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     }
     lmObsBegin.push_back((int)obKf.size());
     S->totalKf = kf; S->totalExt = ex; S->totalCam = cam; S->totalLm = lm; S->totalObs = ob; S->totalImu = im;
-    S->linSmem = linearizeSmemBytes();
+    S->maxNs = 1;
+    for (size_t q = 0; q < lmNs.size(); ++q)
+        S->maxNs = std::max(S->maxNs, 6 * (lmNs[q] + lmNx[q]) + (S->win[lmWin[q]].estTd ? 1 : 0));
+    S->linSmem = linearizeSmemBytes(S->maxNs);
     S->facSmem = factorSmemBytes(S->maxNr);
     CK(configureKernels(S->linSmem, S->facSmem));
     CK(S->dWin.upload(S->win, st));
@@ -489,7 +541,9 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     CK(S->lmDelta.reserve(lm)); CK(S->lmPred.reserve(lm)); CK(S->lmTrial.reserve(lm)); CK(S->lmMaxInc.reserve(lm));
     CK(S->lmValid.reserve(lm)); CK(S->lmTrialValid.reserve(lm));
     CK(S->Hret.reserve(dense)); CK(S->Sglob.reserve(dense)); CK(S->gret.reserve(vec)); CK(S->dr.reserve(vec)); CK(S->rhs.reserve(vec));
-    CK(S->acc.reserve(acc)); CK(S->imuScratch.reserve(imuS)); CK(S->priorScratch.reserve(priS));
+    CK(S->acc.reserve(acc)); CK(S->sch.reserve(schOff)); CK(S->imuScratch.reserve(imuS)); CK(S->priorScratch.reserve(priS));
+    CK(S->obLm.upload(obLmv, st)); CK(S->keyOrder.upload(keyOrderv, st));
+    CK(S->dPairChunks.upload(S->pairChunks, st)); CK(S->dSchurChunks.upload(S->schurChunks, st));
     CK(S->costRet.reserve(count)); CK(S->trialRet.reserve(count)); CK(S->retValid.reserve(count));
     CK(S->predState.reserve(count)); CK(S->solveStatus.reserve(count)); CK(S->out.reserve(4ll * count));
     DevBatch& B = S->B;
@@ -506,6 +560,7 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     B.lmDelta = S->lmDelta.p; B.lmPred = S->lmPred.p; B.lmTrial = S->lmTrial.p; B.lmMaxInc = S->lmMaxInc.p;
     B.lmTrialValid = S->lmTrialValid.p;
     B.obKf = S->obKf.p; B.obKfl = S->obKfl.p; B.obCam = S->obCam.p; B.obSlot = S->obSlot.p;
+    B.obLm = S->obLm.p; B.keyOrder = S->keyOrder.p;
     B.obBearing = S->obBearing.p; B.obP = S->obP.p; B.obVel = S->obVel.p; B.obTime = S->obTime.p;
     for (int k = 0; k < 2; ++k) {
         B.pose[k] = S->pose[k].p; B.sb[k] = S->sb[k].p; B.ext[k] = S->ext[k].p; B.td[k] = S->td[k].p; B.rho[k] = S->rho[k].p;
@@ -514,7 +569,7 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     B.priorKind = S->priorKind.p; B.priorIndex = S->priorIndex.p; B.priorCol = S->priorCol.p; B.priorOff = S->priorOff.p;
     B.priorA = S->priorA.p; B.priorR0 = S->priorR0.p; B.priorRef = S->priorRef.p;
     B.Hret = S->Hret.p; B.gret = S->gret.p; B.costRet = S->costRet.p; B.trialRet = S->trialRet.p; B.retValid = S->retValid.p;
-    B.acc = S->acc.p; B.dr = S->dr.p; B.rhs = S->rhs.p; B.Sglob = S->Sglob.p;
+    B.acc = S->acc.p; B.sch = S->sch.p; B.dr = S->dr.p; B.rhs = S->rhs.p; B.Sglob = S->Sglob.p;
     B.imuScratch = S->imuScratch.p; B.priorScratch = S->priorScratch.p; B.predState = S->predState.p;
     B.solveStatus = S->solveStatus.p; B.out = S->out.p;
     S->hLmKf = lmKf; S->hLmCam = lmCam; S->hLmObsBegin = lmObsBegin; S->hObKf = obKf; S->hObCam = obCam;
@@ -561,8 +616,8 @@ static int runIterations(cgmli_solver* S, int iterations, int probe, double* Sde
     CK(cudaEventRecord(S->ev0, st));
     int launches = launchLmInit(S->B, S->opt.initial_lambda, st);
     for (int it = 0; it < iterations; ++it)
-        launches += launchIteration(S->B, S->dRuns.p, S->dTiles.p, S->linSmem, S->facSmem, S->opt.refinement_steps,
-                                    iterations, probe, Sdebug, st, S->profile ? profileHook : nullptr, S);
+        launches += launchIteration(S->B, S->plan(), S->opt.refinement_steps, iterations, probe, Sdebug, st,
+                                    S->profile ? profileHook : nullptr, S);
     CK(cudaGetLastError());
     CK(cudaEventRecord(S->ev1, st));
     S->lastLaunches = launches;

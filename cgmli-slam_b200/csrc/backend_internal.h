@@ -33,6 +33,7 @@ struct WinDesc {
     int vec0;            // offset of Nr-vectors (gret, dr, rhs)
     long long dense0;    // offset of Nr*Nr matrices (Hret, factor scratch)
     long long acc0;      // offset of the visual accumulator: Npc(Npc+1)/2 + 3*Npc
+    long long sch0;      // offset of the Schur term: Npc(Npc+1)/2
     long long priorA0, priorR00, priorRef0;
     long long imuScratch0;  // nImu * 465 doubles
     long long priorScratch0;  // priorRank*priorCols + priorCols*6 doubles
@@ -65,6 +66,8 @@ struct DevBatch {
     double* lmDelta; double* lmPred; double* lmTrial; double* lmMaxInc; int* lmTrialValid;
     // observations
     const int* obKf; const int* obKfl; const int* obCam; const int* obSlot; const int* obXslot;
+    const int* obLm;      // landmark (device index) of each observation
+    const int* keyOrder;  // observations of each window sorted by (anchor kf, observer kf, anchor ext, observer ext)
     const double* obBearing; const double* obP; const double* obVel; const double* obTime;
     // states: [0] accepted, [1] candidate
     double* pose[2]; double* sb[2]; double* ext[2]; double* td[2]; double* rho[2];
@@ -75,7 +78,8 @@ struct DevBatch {
     const double* priorA; const double* priorR0; const double* priorRef;
     // per-window dense storage
     double* Hret; double* gret; double* costRet; double* trialRet; int* retValid;
-    double* acc;     // visual accumulators
+    double* acc;     // visual accumulators: J^T J (packed upper), unused, G_v, B_v
+    double* sch;     // Schur term sum_l c_l c_l^T / dt_l (packed upper)
     double* dr;      // state increments (Nr per window)
     double* rhs;
     double* Sglob;   // factor scratch when Nr exceeds the shared-memory limit
@@ -125,5 +129,17 @@ struct MargBatch {
 // Called before (phase 0) and after (phase 1) every kernel launch of an
 // iteration; used for per-kernel event timing.
 typedef void (*LaunchHook)(void* ctx, int kind, int phase);
+
+// Work decomposition of one batch (device pointers and counts).
+struct LaunchPlan {
+    const int4* runs;        // {window, first tile, end tile, -}: one warp each (landmark order)
+    const int2* tiles;       // {first landmark, end landmark}, <= 32 observations
+    const int4* pairChunks;  // {window, first key-ordered index, end, -}: <= 32 observations, one warp each
+    int numPairChunks;
+    const int4* schurChunks; // {window, first landmark, end landmark, -}: one CTA each
+    int numSchurChunks;
+    int maxNs;               // widest landmark support of the batch (local columns)
+    size_t linSmem, facSmem;
+};
 
 }  // namespace cgmli

@@ -1,8 +1,8 @@
 // sm_100a kernels of the sliding-window backend hot path.
 //
 // One LM iteration over a batch of windows is the launch sequence
-//   zero_acc -> linearize -> retained -> factor -> candidate -> backsub_trial
-//   -> retained_trial -> lm_update -> accept
+//   zero_acc -> lin_landmark -> lin_pairs -> lin_schur -> retained -> factor
+//   -> candidate -> backsub_trial -> retained_trial -> lm_update -> accept
 // with every decision of the damped LM loop (BackendOptimizer.cpp:167-307)
 // taken on the device from per-window state (WinLM), so that a whole solve
 // runs without a host round trip and can be captured in a CUDA graph.
@@ -42,47 +42,57 @@ __device__ __forceinline__ int retainedOfPc(int p, int K) {
 }
 
 // ---------------------------------------------------------------------------------------
-// zero the visual accumulators of windows that will be (re)linearized
+// Zeroes the visual accumulators: J^T J and J^T r of windows at a new point,
+// the Schur term and B_v of every window still iterating (they depend on lambda).
+// Accumulator of a window: [J^T J packed upper (Npc(Npc+1)/2) | unused Npc | G_v | B_v],
+// Schur buffer: packed upper Npc(Npc+1)/2.
 __global__ void k_zero_acc(DevBatch B) {
     const int w = blockIdx.x;
-    if (B.lm[w].mode == kModeDone) return;
+    const int mode = B.lm[w].mode;
+    if (mode == kModeDone) return;
     const WinDesc& wd = B.win[w];
-    const long long n = (long long)wd.Npc * (wd.Npc + 1) / 2 + 3ll * wd.Npc;
-    for (long long i = threadIdx.x; i < n; i += blockDim.x) B.acc[wd.acc0 + i] = 0.0;
+    const long long nS = (long long)wd.Npc * (wd.Npc + 1) / 2;
+    double* acc = B.acc + wd.acc0;
+    if (mode == kModeLinearize)
+        for (long long i = threadIdx.x; i < nS + 2ll * wd.Npc; i += blockDim.x) acc[i] = 0.0;
+    for (long long i = threadIdx.x; i < wd.Npc; i += blockDim.x) acc[nS + 2ll * wd.Npc + i] = 0.0;
+    double* sch = B.sch + wd.sch0;
+    for (long long i = threadIdx.x; i < nS; i += blockDim.x) sch[i] = 0.0;
 }
 
 // ---------------------------------------------------------------------------------------
-// Linearization of the bearing factors fused with the per-landmark Schur
-// complement at the window's current lambda.  Per landmark l (scalar inverse
-// distance) with observations f:
-//   d_l = sum J_rho^T J_rho,  g_l = sum J_rho^T r,  c_l = sum J_x^T J_rho
-//   S  += sum_f J_f^T J_f - c_l c_l^T / (d_l + lambda max(d_l, 1e-6))
-//   rhs correction += c_l g_l / (d_l + lambda max(d_l, 1e-6))
-// (accumulateVisualPairs + subtractPointSchur, VisualCudaBatch.cu:74-96,149-161).
-//
-// Work unit: a run = consecutive landmarks of one window, sorted by their
-// keyframe support, processed by one warp in tiles of <= 32 observations
-// (lane = observation for the evaluation).  The weighted Jacobians of a tile
-// are staged in shared memory; each landmark's dense local block over its
-// support (6 columns per keyframe slot + the calibration columns) is formed
-// with lanes over distinct entries and added to a warp-private FP64 group
-// buffer.  Landmarks with the same support share the buffer; it is flushed to
-// the window accumulator with global FP64 reductions when the support changes.
-constexpr int kLinWarps = 6;
-constexpr int kStage = 56;          // doubles staged per observation
-constexpr int kGroupMaxNs = 64;     // largest support width that is buffered
-constexpr int kGroupBuf = kGroupMaxNs * (kGroupMaxNs + 1) / 2 + 3 * kGroupMaxNs;
-constexpr int kMaxNs = 6 * (kMaxSupport + 8) + 1;
+// Linearization of the bearing factors and the per-landmark Schur complement
+// at the window's current lambda (accumulateVisualPairs + subtractPointSchur,
+// VisualCudaBatch.cu:74-96,149-161).  With J the weighted Jacobian rows over the
+// visual columns and, per landmark l (scalar inverse distance),
+//   d_l = sum J_rho^T J_rho,  g_l = sum J_rho^T r,  c_l = sum J_x^T J_rho,
+//   dt_l = d_l + lambda max(d_l, 1e-6),
+// the reduced visual system is
+//   S_v = J^T J - sum_l c_l c_l^T / dt_l,   B_v = sum_l c_l g_l / dt_l.
+// It is formed by three kernels:
+//   k_lin_landmark  landmark order: c_l, d_l, g_l, cost, validity per landmark
+//                   (no reductions into shared window state)
+//   k_lin_pairs     observations sorted by (anchor keyframe, observer keyframe,
+//                   anchor extrinsic, observer extrinsic): every observation of a
+//                   key adds to the same entries of J^T J and J^T r, so a warp
+//                   sums a key's observations in registers and adds them once
+//   k_lin_schur     per window: the c_l / sqrt(dt_l) of a chunk of landmarks are
+//                   expanded into dense shared-memory rows and the Schur term is
+//                   a register-tiled FP64 SYRK (plus the B_v column)
+// Only k_lin_schur depends on lambda, so a rejected step re-runs it alone.
+constexpr int kLinWarps = 6;        // warps per CTA of the run-based kernels
 constexpr int kCompact = 25;        // anchor pose 6 | observer pose 6 | ext_a 6 | ext_b 6 | td 1
 constexpr int kPairs = kCompact * (kCompact + 1) / 2;
-struct LinWarpSmem {
-    double stage[32][kStage];  // compact weighted row pair: row0 at [0,25), row1 at [25,50), Jrho 50,51 | r 52,53 | cost 54
-    short map[32][kCompact];        // local column of each compact column, -1 if absent
-    int flags[32];                  // 1 valid
-    double c[kMaxNs];
-    double gbuf[kGroupBuf];
-};
-__constant__ unsigned char kPairA[kPairs], kPairB[kPairs];
+constexpr int kPairSlots = (kPairs + 31) / 32;  // compact pairs per lane
+constexpr int kPairWarps = 8;       // warps per CTA of k_lin_pairs
+constexpr int kSchurThreads = 256;
+constexpr int kSchurSmemDoubles = 12800;  // dense rows of a Schur chunk
+// A factor's FactorOut is staged per lane in shared memory with an odd stride
+// (conflict-free lane rows); slot 54 carries the squared robust weight.
+constexpr int kOut = 55;
+static_assert(sizeof(FactorOut) == 54 * sizeof(double), "FactorOut layout: r, Ja, Jb, Jea, Jeb, Jtd, Jrho");
+// Offset in FactorOut of row r of compact column c.
+__device__ __forceinline__ int compactOff(int r, int c) { return c < 24 ? 2 + 12 * (c / 6) + 6 * r + c % 6 : 50 + r; }
 
 // Local column -> visual column for a support (s keyframe slots, x extrinsic slots, td).
 __device__ __forceinline__ int pcOfLocal(int i, int s, int x, const int* sk, int K, int tdCol) {
@@ -91,53 +101,35 @@ __device__ __forceinline__ int pcOfLocal(int i, int s, int x, const int* sk, int
     return tdCol;
 }
 
-// Adds a group buffer (local coordinates of a support) into the window accumulator.
-__device__ void flushGroup(const double* gbuf, int ns, int s, int x, const int* sk, int K, int tdCol, int Npc, double* acc,
-                           int lane) {
-    const int ntri = ns * (ns + 1) / 2;
-    const long long nS = (long long)Npc * (Npc + 1) / 2;
-    int i = 0, j = lane;
-    while (j >= ns && i < ns) { ++i; j = j - ns + i; }
-    for (int e = lane; e < ntri; e += 32) {
-        const double v = gbuf[e];
-        if (v != 0.0) {
-            const int pi = pcOfLocal(i, s, x, sk, K, tdCol), pj = pcOfLocal(j, s, x, sk, K, tdCol);
-            atomicAdd(&acc[pi <= pj ? upIdx(pi, pj, Npc) : upIdx(pj, pi, Npc)], v);
-        }
-        j += 32;
-        while (j >= ns && i < ns) { ++i; j = j - ns + i; }
-    }
-    for (int t = lane; t < 3 * ns; t += 32) {
-        const double v = gbuf[ntri + t];
-        if (v != 0.0) atomicAdd(&acc[nS + (long long)(t / ns) * Npc + pcOfLocal(t % ns, s, x, sk, K, tdCol)], v);
-    }
+// ---- L1: per-landmark scalars and cross vectors --------------------------------------
+// Work unit: a run = consecutive landmarks of one window processed by one warp in
+// tiles of <= 32 observations (lane = observation for the evaluation).  Per-warp
+// shared memory: 32 staged factors (overwritten in place by the weighted cross
+// products J_x^T J_rho over the compact columns at [0, 25) and d, g, cost at
+// 25, 26, 27), the compact -> local column maps, flags, and the landmark's
+// cross vector (maxNs doubles, the batch's widest support).
+__host__ __device__ constexpr size_t landmarkWarpBytes(int maxNs) {
+    return sizeof(double) * (32 * kOut + maxNs) + sizeof(short) * 32 * kCompact + sizeof(int) * 32;
 }
 
-__device__ __forceinline__ int localUp(int i, int j, int ns) { return i * ns - i * (i - 1) / 2 + (j - i); }
-
-__global__ void __launch_bounds__(kLinWarps * 32) k_linearize(DevBatch B, const int4* runs, const int2* tiles) {
+__global__ void __launch_bounds__(kLinWarps * 32, 2) k_lin_landmark(DevBatch B, const int4* runs, const int2* tiles, int maxNs) {
     extern __shared__ double smemRaw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int runIdx = blockIdx.x * kLinWarps + warp;
     if (runIdx >= B.numRuns) return;
     const int4 run = runs[runIdx];  // {window, tile begin, tile end, -}
     const int wdx = run.x;
-    if (B.lm[wdx].mode == kModeDone) return;
-    LinWarpSmem& sm = reinterpret_cast<LinWarpSmem*>(smemRaw)[warp];
+    if (B.lm[wdx].mode != kModeLinearize) return;
+    char* base = reinterpret_cast<char*>(smemRaw) + landmarkWarpBytes(maxNs) * warp;
+    double* out = reinterpret_cast<double*>(base);
+    double* cvec = out + 32 * kOut;
+    short* map = reinterpret_cast<short*>(cvec + maxNs);
+    int* flags = reinterpret_cast<int*>(map + 32 * kCompact);
     const WinDesc wd = B.win[wdx];
-    const double lambda = B.lm[wdx].lambda;
-    const int K = wd.K, Npc = wd.Npc;
-    const int tdCol = 6 * K + (wd.estExt ? 6 * wd.E : 0);
-    double* acc = B.acc + wd.acc0;
-    const long long nS = (long long)Npc * (Npc + 1) / 2;
-    int curGroup = -1, curNs = 0, curS = 0, curX = 0;
-    const int* curSk = nullptr;
-    bool buffered = false;
     for (int t = run.y; t < run.z; ++t) {
         const int2 tile = tiles[t];
         const int lb = tile.x, le = tile.y;
         const int ob = B.lmObsBegin[lb], oe = B.lmObsBegin[le];
-        // ---- evaluation: lane = observation; stage the weighted compact rows
         const int f = ob + lane;
         if (f < oe) {
             int q = 0;
@@ -146,13 +138,12 @@ __global__ void __launch_bounds__(kLinWarps * 32) k_linearize(DevBatch B, const 
             FactorIn in;
             int kfa, kfb, ea, eb;
             gatherFactor(B, wd, wdx, l, f, 0, in, kfa, kfb, ea, eb);
-            FactorOut o;
-            double* st = sm.stage[lane];
-            short* mp = sm.map[lane];
-            const bool ok = evalBearingFactor(in, true, o);
+            double* st = out + kOut * lane;
+            const bool ok = evalBearingFactor(in, true, *reinterpret_cast<FactorOut*>(st));
             const int s = B.lmNs[l], x = B.lmNx[l];
             const bool same = in.sameKf && !in.splitExt;
             const int obSlot = B.obSlot[f], obX = B.obXslot[f];
+            short* mp = map + kCompact * lane;
             for (int c = 0; c < 6; ++c) {
                 mp[c] = in.sameKf ? -1 : c;
                 mp[6 + c] = in.sameKf ? -1 : 6 * obSlot + c;
@@ -160,125 +151,219 @@ __global__ void __launch_bounds__(kLinWarps * 32) k_linearize(DevBatch B, const 
                 mp[18 + c] = (wd.estExt && in.splitExt) ? 6 * (s + obX) + c : -1;
             }
             mp[24] = wd.estTd ? 6 * (s + x) : -1;
-            sm.flags[lane] = ok ? 1 : 0;
+            flags[lane] = ok ? 1 : 0;
             if (ok) {
-                const double sq = o.r[0] * o.r[0] + o.r[1] * o.r[1];
-                const double w = huberWeight(wd.huber, sq);
+                const double r0 = st[0], r1 = st[1], p0 = st[52], p1 = st[53];
+                const double sq = r0 * r0 + r1 * r1;
+                const double w = huberWeight(wd.huber, sq), w2 = w * w;
+                const double d = w2 * (p0 * p0 + p1 * p1), g = w2 * (p0 * r0 + p1 * r1), cost = huberCost(wd.huber, sq);
+                // in place: column c reads offsets >= c + 2, all later than slot c
 #pragma unroll
-                for (int r = 0; r < 2; ++r) {
-#pragma unroll
-                    for (int c = 0; c < 6; ++c) {
-                        st[25 * r + c] = w * o.Ja[6 * r + c];
-                        st[25 * r + 6 + c] = w * o.Jb[6 * r + c];
-                        st[25 * r + 12 + c] = w * o.Jea[6 * r + c];
-                        st[25 * r + 18 + c] = w * o.Jeb[6 * r + c];
-                    }
-                    st[25 * r + 24] = w * o.Jtd[r];
-                }
-                st[50] = w * o.Jrho[0]; st[51] = w * o.Jrho[1];
-                st[52] = w * o.r[0]; st[53] = w * o.r[1];
-                st[54] = huberCost(wd.huber, sq);
+                for (int c = 0; c < kCompact; ++c) st[c] = w2 * (st[compactOff(0, c)] * p0 + st[compactOff(1, c)] * p1);
+                st[25] = d; st[26] = g; st[27] = cost;
             } else {
-                for (int k = 0; k < kStage; ++k) st[k] = 0.0;
+                for (int c = 0; c < 28; ++c) st[c] = 0.0;
             }
         }
         __syncwarp();
-        // ---- per landmark of the tile
         for (int l = lb; l < le; ++l) {
             const int fb = B.lmObsBegin[l] - ob, fe = B.lmObsBegin[l + 1] - ob;
             const int s = B.lmNs[l], x = B.lmNx[l], ns = 6 * (s + x) + (wd.estTd ? 1 : 0);
-            const int* sk = B.supp + B.lmSupp0[l];
-            const int group = B.lmGroup[l];
-            if (group != curGroup) {
-                if (buffered) { __syncwarp(); flushGroup(sm.gbuf, curNs, curS, curX, curSk, K, tdCol, Npc, acc, lane); }
-                curGroup = group; curNs = ns; curS = s; curX = x; curSk = sk;
-                buffered = ns <= kGroupMaxNs;
-                __syncwarp();
-                if (buffered) {
-                    const int n = ns * (ns + 1) / 2 + 3 * ns;
-                    for (int e = lane; e < n; e += 32) sm.gbuf[e] = 0.0;
-                }
-                __syncwarp();
-            }
-            const int ntri = ns * (ns + 1) / 2;
-            // scalars: d, g, cost, validity
             double d = 0, g = 0, cost = 0;
             int valid = 1;
             for (int k = fb + lane; k < fe; k += 32) {
-                const double* st = sm.stage[k];
-                d += st[50] * st[50] + st[51] * st[51];
-                g += st[50] * st[52] + st[51] * st[53];
-                cost += st[54];
-                valid &= sm.flags[k];
+                const double* st = out + kOut * k;
+                d += st[25];
+                g += st[26];
+                cost += st[27];
+                valid &= flags[k];
             }
             d = warpSum(d); g = warpSum(g); cost = warpSum(cost);
             valid = __all_sync(0xffffffffu, valid);
-            const double inv = 1.0 / (d + lambda * fmax(d, 1e-6));
-            for (int i = lane; i < ns; i += 32) sm.c[i] = 0.0;
+            for (int i = lane; i < ns; i += 32) cvec[i] = 0.0;
             __syncwarp();
-            // per observation: cross vector, diag(H) and gradient over the compact columns
+            // the compact columns of one observation map to distinct local columns
             for (int k = fb; k < fe; ++k) {
-                const double* st = sm.stage[k];
-                const short* mp = sm.map[k];
                 if (lane < kCompact) {
-                    const int li = mp[lane];
-                    if (li >= 0) {
-                        const double a0 = st[lane], a1 = st[25 + lane];
-                        sm.c[li] += a0 * st[50] + a1 * st[51];
-                        const double hd = a0 * a0 + a1 * a1, gr = a0 * st[52] + a1 * st[53];
-                        if (buffered) { sm.gbuf[ntri + li] += hd; sm.gbuf[ntri + ns + li] += gr; }
-                        else {
-                            const int p = pcOfLocal(li, s, x, sk, K, tdCol);
-                            atomicAdd(&acc[nS + p], hd);
-                            atomicAdd(&acc[nS + Npc + p], gr);
-                        }
-                    }
-                }
-                __syncwarp();
-                // J^T J over the compact pairs
-                for (int pidx = lane; pidx < kPairs; pidx += 32) {
-                    const int a = kPairA[pidx], b = kPairB[pidx];
-                    const int la = mp[a], lb2 = mp[b];
-                    if (la < 0 || lb2 < 0) continue;
-                    const double v = st[a] * st[b] + st[25 + a] * st[25 + b];
-                    if (v == 0.0) continue;
-                    const int i = la < lb2 ? la : lb2, j = la < lb2 ? lb2 : la;
-                    if (buffered) sm.gbuf[localUp(i, j, ns)] += v;
-                    else {
-                        const int pi = pcOfLocal(i, s, x, sk, K, tdCol), pj = pcOfLocal(j, s, x, sk, K, tdCol);
-                        atomicAdd(&acc[pi <= pj ? upIdx(pi, pj, Npc) : upIdx(pj, pi, Npc)], v);
-                    }
+                    const int li = map[kCompact * k + lane];
+                    if (li >= 0) cvec[li] += out[kOut * k + lane];
                 }
                 __syncwarp();
             }
-            // Schur complement of the inverse distance and the rhs correction
             const long long c0 = B.lmC0[l];
-            for (int i = lane; i < ns; i += 32) {
-                const double ci = sm.c[i];
-                B.lmC[c0 + i] = ci;
-                const double bc = inv * ci * g;
-                if (buffered) sm.gbuf[ntri + 2 * ns + i] += bc;
-                else if (bc != 0.0) atomicAdd(&acc[nS + 2ll * Npc + pcOfLocal(i, s, x, sk, K, tdCol)], bc);
-            }
-            {
-                int i = 0, j = lane;
-                while (j >= ns && i < ns) { ++i; j = j - ns + i; }
-                for (int e = lane; e < ntri; e += 32) {
-                    const double v = -inv * sm.c[i] * sm.c[j];
-                    if (buffered) sm.gbuf[e] += v;
-                    else if (v != 0.0) {
-                        const int pi = pcOfLocal(i, s, x, sk, K, tdCol), pj = pcOfLocal(j, s, x, sk, K, tdCol);
-                        atomicAdd(&acc[pi <= pj ? upIdx(pi, pj, Npc) : upIdx(pj, pi, Npc)], v);
-                    }
-                    j += 32;
-                    while (j >= ns && i < ns) { ++i; j = j - ns + i; }
-                }
-            }
+            for (int i = lane; i < ns; i += 32) B.lmC[c0 + i] = cvec[i];
             if (lane == 0) { B.lmD[l] = d; B.lmG[l] = g; B.lmCost[l] = cost; B.lmValid[l] = valid; }
             __syncwarp();
         }
     }
-    if (buffered) { __syncwarp(); flushGroup(sm.gbuf, curNs, curS, curX, curSk, K, tdCol, Npc, acc, lane); }
+}
+
+// ---- L2: J^T J and J^T r by observation key ------------------------------------------
+// Work unit: a chunk of <= 32 observations of one window in key order; lane =
+// observation for the evaluation, then every lane owns fixed compact pairs
+// (a <= b) whose products it sums over each run of equal keys in registers.
+__host__ __device__ constexpr size_t pairCtaBytes() { return sizeof(double) * kPairWarps * 32 * kOut; }
+
+__global__ void __launch_bounds__(kPairWarps * 32, 2) k_lin_pairs(DevBatch B, const int4* chunks, int numChunks) {
+    extern __shared__ double smemRaw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ci = blockIdx.x * kPairWarps + warp;
+    if (ci >= numChunks) return;
+    const int4 ch = chunks[ci];  // {window, first sorted index, end, -}
+    const int wdx = ch.x;
+    if (B.lm[wdx].mode != kModeLinearize) return;
+    double* out = smemRaw + (size_t)warp * 32 * kOut;
+    const WinDesc wd = B.win[wdx];
+    const int n = ch.z - ch.y;
+    int kfa = -1, kfb = -1, ea = -1, eb = -1;
+    if (lane < n) {
+        const int f = B.keyOrder[ch.y + lane];
+        const int l = B.obLm[f];
+        FactorIn in;
+        gatherFactor(B, wd, wdx, l, f, 0, in, kfa, kfb, ea, eb);
+        double* st = out + kOut * lane;
+        if (evalBearingFactor(in, true, *reinterpret_cast<FactorOut*>(st))) {
+            const double w = huberWeight(wd.huber, st[0] * st[0] + st[1] * st[1]);
+            st[54] = w * w;
+        } else {
+            for (int k = 0; k < kOut; ++k) st[k] = 0.0;
+        }
+    }
+    // this lane's compact pairs: a | b << 8 | off(0,a) << 16 | off(0,b) << 24
+    unsigned pr[kPairSlots];
+#pragma unroll
+    for (int j = 0; j < kPairSlots; ++j) {
+        const int p = lane + 32 * j;
+        int a = 0, rem = p;
+        while (a < kCompact && rem >= kCompact - a) { rem -= kCompact - a; ++a; }
+        const int b = a + rem;
+        pr[j] = p < kPairs ? (unsigned)a | (unsigned)b << 8 | (unsigned)compactOff(0, a) << 16 | (unsigned)compactOff(0, b) << 24
+                           : 0xffffffffu;
+    }
+    // runs of equal key
+    const int pa = __shfl_up_sync(0xffffffffu, kfa, 1), pb = __shfl_up_sync(0xffffffffu, kfb, 1);
+    const int pea = __shfl_up_sync(0xffffffffu, ea, 1), peb = __shfl_up_sync(0xffffffffu, eb, 1);
+    const bool start = lane < n && (lane == 0 || pa != kfa || pb != kfb || pea != ea || peb != eb);
+    unsigned starts = __ballot_sync(0xffffffffu, start);
+    __syncwarp();
+    const int K = wd.K, Npc = wd.Npc;
+    const int tdCol = 6 * K + (wd.estExt ? 6 * wd.E : 0);
+    double* JJ = B.acc + wd.acc0;
+    double* Gv = JJ + (long long)Npc * (Npc + 1) / 2 + Npc;
+    const int goff0 = lane < kCompact ? compactOff(0, lane) : 0, gstep = lane < 24 ? 6 : 1;
+    while (starts) {
+        const int s0 = __ffs(starts) - 1;
+        starts &= starts - 1;
+        const int s1 = starts ? __ffs(starts) - 1 : n;
+        const int ka = __shfl_sync(0xffffffffu, kfa, s0) - wd.kf0, kb = __shfl_sync(0xffffffffu, kfb, s0) - wd.kf0;
+        const int xa = __shfl_sync(0xffffffffu, ea, s0) - wd.ext0, xb = __shfl_sync(0xffffffffu, eb, s0) - wd.ext0;
+        const bool sameKf = ka == kb, split = xa != xb, same = sameKf && !split;
+        auto colOf = [&](int c) -> int {
+            if (c < 6) return sameKf ? -1 : 6 * ka + c;
+            if (c < 12) return sameKf ? -1 : 6 * kb + c - 6;
+            if (c < 18) return (wd.estExt && !same) ? 6 * K + 6 * xa + c - 12 : -1;
+            if (c < 24) return (wd.estExt && split) ? 6 * K + 6 * xb + c - 18 : -1;
+            return wd.estTd ? tdCol : -1;
+        };
+        double acc[kPairSlots];
+#pragma unroll
+        for (int j = 0; j < kPairSlots; ++j) acc[j] = 0.0;
+        double gr = 0.0;
+        for (int k = s0; k < s1; ++k) {
+            const double* st = out + kOut * k;
+            const double w2 = st[54];
+#pragma unroll
+            for (int j = 0; j < kPairSlots; ++j) {
+                if (pr[j] == 0xffffffffu) continue;
+                const int a = pr[j] & 0xff, b = (pr[j] >> 8) & 0xff, oa = (pr[j] >> 16) & 0xff, ob2 = pr[j] >> 24;
+                const int da = a < 24 ? 6 : 1, db = b < 24 ? 6 : 1;
+                acc[j] += w2 * (st[oa] * st[ob2] + st[oa + da] * st[ob2 + db]);
+            }
+            if (lane < kCompact) gr += w2 * (st[goff0] * st[0] + st[goff0 + gstep] * st[1]);
+        }
+#pragma unroll
+        for (int j = 0; j < kPairSlots; ++j) {
+            if (pr[j] == 0xffffffffu || acc[j] == 0.0) continue;
+            const int ca = colOf(pr[j] & 0xff), cb = colOf((pr[j] >> 8) & 0xff);
+            if (ca < 0 || cb < 0) continue;
+            atomicAdd(&JJ[ca <= cb ? upIdx(ca, cb, Npc) : upIdx(cb, ca, Npc)], acc[j]);
+        }
+        if (lane < kCompact && gr != 0.0) {
+            const int c = colOf(lane);
+            if (c >= 0) atomicAdd(&Gv[c], gr);
+        }
+    }
+}
+
+// ---- L3: Schur term as a dense SYRK per chunk of landmarks ----------------------------
+// Shared memory: rows x W1 doubles, W1 = Npc + 1 (the last column carries
+// g_l / sqrt(dt_l) for B_v).  Each thread owns 4x4 output tiles of the upper
+// triangle and accumulates them in registers over the chunk's rows.
+__global__ void __launch_bounds__(kSchurThreads) k_lin_schur(DevBatch B, const int4* chunks) {
+    extern __shared__ double Ct[];
+    const int4 ch = chunks[blockIdx.x];  // {window, first landmark, end landmark, rows}
+    const int wdx = ch.x;
+    const int mode = B.lm[wdx].mode;
+    if (mode == kModeDone) return;
+    const WinDesc wd = B.win[wdx];
+    const double lambda = B.lm[wdx].lambda;
+    const int K = wd.K, Npc = wd.Npc, W1 = Npc + 1;
+    const int tdCol = 6 * K + (wd.estExt ? 6 * wd.E : 0);
+    const int rows = ch.z - ch.y;
+    for (int i = threadIdx.x; i < rows * W1; i += blockDim.x) Ct[i] = 0.0;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int r = warp; r < rows; r += kSchurThreads / 32) {
+        const int l = ch.y + r;
+        const int s = B.lmNs[l], x = B.lmNx[l], ns = 6 * (s + x) + (wd.estTd ? 1 : 0);
+        const int* sk = B.supp + B.lmSupp0[l];
+        const double d = B.lmD[l];
+        const double scale = 1.0 / sqrt(d + lambda * fmax(d, 1e-6));
+        const double* c = B.lmC + B.lmC0[l];
+        double* row = Ct + (long long)r * W1;
+        for (int i = lane; i < ns; i += 32) row[pcOfLocal(i, s, x, sk, K, tdCol)] = scale * c[i];
+        if (lane == 0) row[Npc] = scale * B.lmG[l];
+    }
+    __syncthreads();
+    const int nt = (W1 + 3) / 4, tiles = nt * (nt + 1) / 2;
+    double* sch = B.sch + wd.sch0;
+    double* Bv = B.acc + wd.acc0 + (long long)Npc * (Npc + 1) / 2 + 2ll * Npc;
+    for (int tIdx = threadIdx.x; tIdx < tiles; tIdx += blockDim.x) {
+        // (ti, tj), ti <= tj, from the packed-upper enumeration of an nt x nt triangle
+        int ti = (int)((2.0f * nt + 1 - sqrtf((2.0f * nt + 1) * (2.0f * nt + 1) - 8.0f * tIdx)) * 0.5f);
+        if (ti < 0) ti = 0;
+        while (ti > 0 && ti * nt - ti * (ti - 1) / 2 > tIdx) --ti;
+        while ((ti + 1) * nt - (ti + 1) * ti / 2 <= tIdx) ++ti;
+        const int tj = ti + (tIdx - (ti * nt - ti * (ti - 1) / 2));
+        const int i0 = 4 * ti, j0 = 4 * tj;
+        double acc[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+        for (int r = 0; r < rows; ++r) {
+            const double* row = Ct + (long long)r * W1;
+            double u[4], v[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                u[a] = i0 + a < W1 ? row[i0 + a] : 0.0;
+                v[a] = j0 + a < W1 ? row[j0 + a] : 0.0;
+            }
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) acc[a][b] += u[a] * v[b];
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int i = i0 + a, j = j0 + b;
+                if (i > j || j >= W1 || i >= Npc || acc[a][b] == 0.0) continue;
+                if (j < Npc) atomicAdd(&sch[upIdx(i, j, Npc)], acc[a][b]);
+                else atomicAdd(&Bv[i], acc[a][b]);
+            }
+    }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -437,13 +522,17 @@ __global__ void __launch_bounds__(256) k_retained(DevBatch B, int trial) {
 __device__ __forceinline__ double assembleEntry(const DevBatch& B, const WinDesc& wd, int i, int j, double lambda, bool damp) {
     const int Nr = wd.Nr, Npc = wd.Npc, K = wd.K;
     const double* H = B.Hret + wd.dense0;
-    const double* acc = B.acc + wd.acc0;
+    const double* JJ = B.acc + wd.acc0;
+    const double* sch = B.sch + wd.sch0;
     double v = H[(long long)i * Nr + j];
     const int pi = pcOfRetained(i, K), pj = pcOfRetained(j, K);
-    if (pi >= 0 && pj >= 0) v += acc[pi <= pj ? upIdx(pi, pj, Npc) : upIdx(pj, pi, Npc)];
+    if (pi >= 0 && pj >= 0) {
+        const long long e = pi <= pj ? upIdx(pi, pj, Npc) : upIdx(pj, pi, Npc);
+        v += JJ[e] - sch[e];
+    }
     if (damp && i == j) {
         double h = H[(long long)i * Nr + i];
-        if (pi >= 0) h += acc[(long long)Npc * (Npc + 1) / 2 + pi];
+        if (pi >= 0) h += JJ[upIdx(pi, pi, Npc)];
         v += lambda * fmax(h, 1e-6);
     }
     return v;
@@ -764,7 +853,12 @@ __global__ void k_lm_init(DevBatch B, double lambda0) {
 
 // ---------------------------------------------------------------------------------------
 // host-side launchers (called by backend_host.cu)
-size_t linearizeSmemBytes() { return kLinWarps * sizeof(LinWarpSmem); }
+size_t linearizeSmemBytes(int maxNs) { return kLinWarps * landmarkWarpBytes(maxNs); }
+size_t schurSmemBytes() { return kSchurSmemDoubles * sizeof(double); }
+int schurRowsPerChunk(int Npc) {
+    const int rows = kSchurSmemDoubles / (Npc + 1);
+    return rows < 128 ? rows : 128;
+}
 size_t factorSmemBytes(int maxNr) {
     // windows with Nr <= kSmemPackedMax factor in shared memory; larger ones in global memory
     const size_t n = (size_t)(maxNr < kSmemPackedMax ? maxNr : kSmemPackedMax);
@@ -779,23 +873,24 @@ cudaError_t configureKernels(size_t linSmem, size_t facSmem) {
     cudaError_t e = cudaGetDevice(&device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     if (e != cudaSuccess) return e;
-    cudaFuncAttributes la, fa;
-    if ((e = cudaFuncGetAttributes(&la, k_linearize)) != cudaSuccess) return e;
+    cudaFuncAttributes la, fa, sa, pa;
+    if ((e = cudaFuncGetAttributes(&la, k_lin_landmark)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&pa, k_lin_pairs)) != cudaSuccess) return e;
     if ((e = cudaFuncGetAttributes(&fa, k_factor)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&sa, k_lin_schur)) != cudaSuccess) return e;
     const size_t linMax = (size_t)optin - la.sharedSizeBytes, facMax = (size_t)optin - fa.sharedSizeBytes;
-    if (linSmem > linMax || facSmem > facMax) return cudaErrorInvalidValue;
-    unsigned char pa[kPairs], pb[kPairs];
-    int n = 0;
-    for (int a = 0; a < kCompact; ++a)
-        for (int b = a; b < kCompact; ++b) { pa[n] = (unsigned char)a; pb[n] = (unsigned char)b; ++n; }
-    if ((e = cudaMemcpyToSymbol(kPairA, pa, sizeof pa)) != cudaSuccess) return e;
-    if ((e = cudaMemcpyToSymbol(kPairB, pb, sizeof pb)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k_linearize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)linMax)) != cudaSuccess) return e;
+    const size_t schMax = (size_t)optin - sa.sharedSizeBytes;
+    if (linSmem > linMax || facSmem > facMax || schurSmemBytes() > schMax || pairCtaBytes() > (size_t)optin - pa.sharedSizeBytes)
+        return cudaErrorInvalidValue;
+    if ((e = cudaFuncSetAttribute(k_lin_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pairCtaBytes())) != cudaSuccess)
+        return e;
+    if ((e = cudaFuncSetAttribute(k_lin_landmark, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)linMax)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_lin_schur, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)schMax)) != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)facMax);
 }
 
-int launchIteration(const DevBatch& B, const int4* runs, const int2* tiles, size_t linSmem, size_t facSmem,
-                    int refinement, int maxIterations, int probe, double* Sdebug, cudaStream_t s, LaunchHook hook, void* ctx) {
+int launchIteration(const DevBatch& B, const LaunchPlan& P, int refinement, int maxIterations, int probe, double* Sdebug,
+                    cudaStream_t s, LaunchHook hook, void* ctx) {
     const int W = B.numWindows;
     int n = 0;
     auto run = [&](int kind, auto&& launch) {
@@ -807,12 +902,19 @@ int launchIteration(const DevBatch& B, const int4* runs, const int2* tiles, size
     run(CGMLI_KERNEL_ZERO, [&] { k_zero_acc<<<W, 256, 0, s>>>(B); });
     const int runBlocks = (B.numRuns + kLinWarps - 1) / kLinWarps;
     if (B.numRuns > 0)
-        run(CGMLI_KERNEL_LINEARIZE, [&] { k_linearize<<<runBlocks, kLinWarps * 32, linSmem, s>>>(B, runs, tiles); });
+        run(CGMLI_KERNEL_LINEARIZE, [&] { k_lin_landmark<<<runBlocks, kLinWarps * 32, P.linSmem, s>>>(B, P.runs, P.tiles, P.maxNs); });
+    if (P.numPairChunks > 0)
+        run(CGMLI_KERNEL_LIN_PAIRS, [&] {
+            k_lin_pairs<<<(P.numPairChunks + kPairWarps - 1) / kPairWarps, kPairWarps * 32, pairCtaBytes(), s>>>(B, P.pairChunks,
+                                                                                                     P.numPairChunks);
+        });
+    if (P.numSchurChunks > 0)
+        run(CGMLI_KERNEL_LIN_SCHUR, [&] { k_lin_schur<<<P.numSchurChunks, kSchurThreads, schurSmemBytes(), s>>>(B, P.schurChunks); });
     run(CGMLI_KERNEL_RETAINED, [&] { k_retained<<<W, 256, 0, s>>>(B, 0); });
-    run(CGMLI_KERNEL_FACTOR, [&] { k_factor<<<W, kFactorThreads, facSmem, s>>>(B, refinement, Sdebug); });
+    run(CGMLI_KERNEL_FACTOR, [&] { k_factor<<<W, kFactorThreads, P.facSmem, s>>>(B, refinement, Sdebug); });
     run(CGMLI_KERNEL_CANDIDATE, [&] { k_candidate<<<W, 128, 0, s>>>(B); });
     if (B.numRuns > 0)
-        run(CGMLI_KERNEL_BACKSUB_TRIAL, [&] { k_backsub_trial<<<runBlocks, kLinWarps * 32, 0, s>>>(B, runs, tiles); });
+        run(CGMLI_KERNEL_BACKSUB_TRIAL, [&] { k_backsub_trial<<<runBlocks, kLinWarps * 32, 0, s>>>(B, P.runs, P.tiles); });
     run(CGMLI_KERNEL_RETAINED_TRIAL, [&] { k_retained<<<W, 256, 0, s>>>(B, 1); });
     run(CGMLI_KERNEL_LM_UPDATE, [&] { k_lm_update<<<W, 256, 0, s>>>(B, maxIterations, probe); });
     if (!probe) run(CGMLI_KERNEL_ACCEPT, [&] { k_accept<<<W, 256, 0, s>>>(B); });

@@ -187,7 +187,10 @@ int cgmli_solver_rollback(cgmli_solver *solver);
  * CGMLI_KERNEL_* (ms and calls hold CGMLI_KERNEL_KINDS entries). */
 enum { CGMLI_KERNEL_ZERO = 0, CGMLI_KERNEL_LINEARIZE, CGMLI_KERNEL_RETAINED, CGMLI_KERNEL_FACTOR, CGMLI_KERNEL_CANDIDATE,
        CGMLI_KERNEL_BACKSUB_TRIAL, CGMLI_KERNEL_RETAINED_TRIAL, CGMLI_KERNEL_LM_UPDATE, CGMLI_KERNEL_ACCEPT,
-       CGMLI_KERNEL_KINDS };
+       CGMLI_KERNEL_LIN_PAIRS, CGMLI_KERNEL_LIN_SCHUR, CGMLI_KERNEL_KINDS };
+/* CGMLI_KERNEL_LINEARIZE is the per-landmark pass of the linearization (factor
+ * evaluation, cross vectors); _LIN_PAIRS the J^T J / J^T r pass; _LIN_SCHUR the
+ * lambda-dependent Schur term. */
 int cgmli_solver_kernel_times(cgmli_solver *solver, int enable, double *ms, int *calls);
 
 /* Schur marginalization of one keyframe per window at the current states
