@@ -85,6 +85,7 @@ def declare_backend(lib: C.CDLL) -> C.CDLL:
     S = C.c_void_p
     _proto(lib, "cgmli_last_error", C.c_char_p, [])
     _proto(lib, "cgmli_default_options", None, [C.POINTER(SolverOptions)])
+    _proto(lib, "cgmli_topology_check", C.c_int, [W, C.c_int, C.c_int, c_double_p])
     _proto(lib, "cgmli_solver_create", C.c_int, [C.c_int, C.POINTER(SolverOptions), C.POINTER(C.c_void_p)])
     _proto(lib, "cgmli_solver_destroy", None, [S])
     _proto(lib, "cgmli_solver_set_windows", C.c_int, [S, W, C.c_int])
@@ -127,7 +128,7 @@ BACKEND_SYMBOLS = [
     "cgmli_solver_read_states", "cgmli_solver_read_reports", "cgmli_solver_step", "cgmli_solver_read_step",
     "cgmli_solver_read_reduced", "cgmli_solver_window_dims", "cgmli_solver_last_timing", "cgmli_solver_marginalize",
     "cgmli_solver_read_prior", "cgmli_marg_eigen", "cgmli_marg_psd_solve", "cgmli_marg_subtract",
-    "cgmli_solver_checkpoint", "cgmli_solver_rollback", "cgmli_solver_kernel_times",
+    "cgmli_solver_checkpoint", "cgmli_solver_rollback", "cgmli_solver_kernel_times", "cgmli_topology_check",
 ]
 KERNEL_NAMES = ["zero_acc", "linearize", "retained", "factor", "candidate", "backsub_trial", "retained_trial", "lm_update", "accept",
                 "lin_pairs", "lin_schur"]

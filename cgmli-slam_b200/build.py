@@ -19,8 +19,10 @@ ROOT = PKG.parent
 LIB = PKG / "lib"
 INCLUDE = ROOT / "include"
 
-BACKEND_SOURCES = [PKG / "csrc" / "backend_kernels.cu", PKG / "csrc" / "marginal_kernels.cu", PKG / "csrc" / "backend_host.cu"]
+BACKEND_SOURCES = [PKG / "csrc" / "backend_kernels.cu", PKG / "csrc" / "marginal_kernels.cu", PKG / "csrc" / "backend_host.cu",
+                   PKG / "csrc" / "topology.cpp"]
 BACKEND_HEADERS = [PKG / "csrc" / "device_math.cuh", PKG / "csrc" / "factor_eval.cuh", PKG / "csrc" / "backend_internal.h",
+                   PKG / "csrc" / "topology.h",
                    INCLUDE / "cgmli_backend.h"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",

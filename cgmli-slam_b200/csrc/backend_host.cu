@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -19,6 +20,7 @@
 
 #include "../../include/cgmli_backend.h"
 #include "backend_internal.h"
+#include "topology.h"
 
 namespace cgmli {
 size_t linearizeSmemBytes(int maxNs);
@@ -70,7 +72,8 @@ struct DArray {
         if (e == cudaSuccess) cap = n;
         return e;
     }
-    cudaError_t upload(const std::vector<T>& v, cudaStream_t s) {
+    template <class V>
+    cudaError_t upload(const V& v, cudaStream_t s) {
         cudaError_t e = reserve(v.size());
         if (e != cudaSuccess || v.empty()) return e;
         return cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
@@ -86,11 +89,6 @@ struct cgmli_solver {
     cgmli_solver_options opt{};
     // topology (host copies)
     std::vector<WinDesc> win;
-    std::vector<int4> runs;       // {window, first tile, end tile, -}
-    std::vector<int2> tiles;      // {first landmark, end landmark} (device order)
-    std::vector<int> lmPerm;      // device landmark -> landmark index within its window
-    std::vector<int4> pairChunks; // {window, first key-ordered observation, end, -}
-    std::vector<int4> schurChunks;// {window, first landmark, end landmark, -}
     int maxNpc = 0, maxNr = 0, maxNs = 1;
     size_t linSmem = 0, facSmem = 0;
     int totalKf = 0, totalExt = 0, totalCam = 0, totalLm = 0, totalObs = 0, totalImu = 0;
@@ -104,11 +102,11 @@ struct cgmli_solver {
     DArray<double> sch;
     DArray<double> camR, camT;
     DArray<int> camExt;
-    DArray<int> lmWin, lmKf, lmCam, lmObsBegin, lmNs, lmNx, lmSupp0, supp, lmGroup;
+    DArray<int> lmKf, lmCam, lmObsBegin, lmNs, lmNx, lmSupp0, supp;
     DArray<long long> lmC0;
     DArray<double> lmBearing, lmVel, lmTime, lmC, lmD, lmG, lmCost, lmDelta, lmPred, lmTrial, lmMaxInc;
     DArray<int> lmValid, lmTrialValid;
-    DArray<int> obKf, obKfl, obCam, obSlot, obXslot;
+    DArray<int> obKf, obCam, obSlot, obXslot;
     DArray<double> obBearing, obP, obVel, obTime;
     DArray<double> pose[2], sb[2], ext[2], td[2], rho[2];
     DArray<double> imu;
@@ -120,8 +118,9 @@ struct cgmli_solver {
     DevBatch B{};
     double lastMs = 0;
     int lastLaunches = 0;
-    // host copies of the topology (device order, global indices) for elimination sets
-    std::vector<int> hLmKf, hLmCam, hLmObsBegin, hObKf, hObCam, hCamExt, hImuKf, hPriorKind, hPriorIndex;
+    // host side of the batch (pinned; also the host copies of the topology the
+    // elimination sets are built from, and the staging of state read-back)
+    HostBatch hb;
     // marginalization
     std::vector<MargWin> margWin;
     std::vector<std::vector<int>> sepKind, sepIndex;  // separator blocks per window (window-local index)
@@ -152,8 +151,8 @@ struct cgmli_solver {
     LaunchPlan plan() const {
         LaunchPlan P{};
         P.runs = dRuns.p; P.tiles = dTiles.p;
-        P.pairChunks = dPairChunks.p; P.numPairChunks = (int)pairChunks.size();
-        P.schurChunks = dSchurChunks.p; P.numSchurChunks = (int)schurChunks.size();
+        P.pairChunks = dPairChunks.p; P.numPairChunks = (int)hb.pairChunks.size();
+        P.schurChunks = dSchurChunks.p; P.numSchurChunks = (int)hb.schurChunks.size();
         P.linSmem = linSmem; P.facSmem = facSmem; P.maxNs = maxNs;
         return P;
     }
@@ -176,9 +175,9 @@ struct cgmli_solver {
                                  &td[0], &td[1], &rho[0], &rho[1], &imu, &priorA, &priorR0, &priorRef, &Hret, &gret, &costRet,
                                  &trialRet, &acc, &dr, &rhs, &Sglob, &imuScratch, &priorScratch, &predState, &out, &Sdebug};
         for (auto* a : dbl) a->release();
-        DArray<int>* ints[] = {&camExt, &lmWin, &lmKf, &lmCam, &lmObsBegin, &lmNs, &lmSupp0, &supp, &lmValid, &lmTrialValid, &obKf,
-                               &obKfl, &obCam, &obSlot, &imuKf, &priorKind, &priorIndex, &priorCol, &priorOff, &retValid,
-                               &solveStatus, &lmGroup, &lmNx, &obXslot};
+        DArray<int>* ints[] = {&camExt, &lmKf, &lmCam, &lmObsBegin, &lmNs, &lmSupp0, &supp, &lmValid, &lmTrialValid, &obKf,
+                               &obCam, &obSlot, &imuKf, &priorKind, &priorIndex, &priorCol, &priorOff, &retValid,
+                               &solveStatus, &lmNx, &obXslot};
         for (auto* a : ints) a->release();
         lmC0.release(); dWin.release(); dLm.release(); dRuns.release(); dTiles.release();
         dPairChunks.release(); dSchurChunks.release(); obLm.release(); keyOrder.release(); sch.release();
@@ -196,60 +195,27 @@ struct cgmli_solver {
 };
 
 namespace {
-int tangentOf(int kind) { return kind == CGMLI_PRIOR_SPEED_BIAS ? 9 : kind == CGMLI_PRIOR_TIME_OFFSET ? 1 : 6; }
 int ambientOf(int kind) { return kind == CGMLI_PRIOR_SPEED_BIAS ? 9 : kind == CGMLI_PRIOR_TIME_OFFSET ? 1 : 7; }
 
-int validateWindow(const cgmli_window& w, int index) {
-    char buf[256];
-    auto bad = [&](const char* what) {
-        std::snprintf(buf, sizeof buf, "window %d: %s", index, what);
-        return fail(CGMLI_E_INVALID, buf);
-    };
-    if (w.num_keyframes < 1 || w.num_cameras < 1 || w.num_extrinsics < 1 || w.num_landmarks < 0 || w.num_observations < 0 ||
-        w.num_imu < 0 || w.prior_rank < 0)
-        return bad("negative or empty sizes");
-    if (!w.poses || !w.speed_bias || !w.extrinsics || (w.num_landmarks && !w.rho) || !w.cam_R || !w.cam_t || !w.cam_ext)
-        return bad("missing state or rig arrays");
-    if (w.num_landmarks && (!w.lm_anchor_kf || !w.lm_anchor_cam || !w.lm_obs_begin || !w.lm_anchor_bearing))
-        return bad("missing landmark arrays");
-    if (w.num_observations && (!w.obs_kf || !w.obs_cam || !w.obs_bearing || !w.obs_P)) return bad("missing observation arrays");
-    if (w.num_imu && (!w.imu || !w.imu_kf)) return bad("missing IMU arrays");
-    if (w.estimate_td && !w.td) return bad("estimate_td requires a td value");
-    for (int c = 0; c < w.num_cameras; ++c)
-        if (w.cam_ext[c] < 0 || w.cam_ext[c] >= w.num_extrinsics) return bad("camera extrinsic index out of range");
-    if (w.num_landmarks && (w.lm_obs_begin[0] != 0 || w.lm_obs_begin[w.num_landmarks] != w.num_observations))
-        return bad("landmark observation ranges do not cover the observations");
-    for (int l = 0; l < w.num_landmarks; ++l) {
-        if (w.lm_obs_begin[l + 1] < w.lm_obs_begin[l]) return bad("landmark observation ranges not sorted");
-        if (w.lm_obs_begin[l + 1] - w.lm_obs_begin[l] > kMaxTrackChunk) return bad("more than 32 observations of one landmark");
-        if (w.lm_anchor_kf[l] < 0 || w.lm_anchor_kf[l] >= w.num_keyframes) return bad("anchor keyframe out of range");
-        if (w.lm_anchor_cam[l] < 0 || w.lm_anchor_cam[l] >= w.num_cameras) return bad("anchor camera out of range");
-    }
-    for (int f = 0; f < w.num_observations; ++f) {
-        if (w.obs_kf[f] < 0 || w.obs_kf[f] >= w.num_keyframes) return bad("observer keyframe out of range");
-        if (w.obs_cam[f] < 0 || w.obs_cam[f] >= w.num_cameras) return bad("observer camera out of range");
-    }
-    for (int i = 0; i < w.num_imu; ++i)
-        if (w.imu_kf[i] < 0 || w.imu_kf[i] + 1 >= w.num_keyframes) return bad("IMU keyframe out of range");
-    if (w.prior_rank > 0) {
-        if (!w.prior_block_kind || !w.prior_block_index || !w.prior_ref || !w.prior_A || !w.prior_r0 || w.prior_num_blocks < 1)
-            return bad("missing prior arrays");
-        for (int b = 0; b < w.prior_num_blocks; ++b) {
-            const int k = w.prior_block_kind[b], i = w.prior_block_index[b];
-            if (k < 0 || k > 3) return bad("prior block kind");
-            if ((k <= 1 && (i < 0 || i >= w.num_keyframes)) || (k == 2 && (i < 0 || i >= w.num_extrinsics)) || (k == 3 && !w.td))
-                return bad("prior block index");
-        }
-    }
-    const int ncal = (w.estimate_extrinsics ? 6 * w.num_extrinsics : 0) + (w.estimate_td ? 1 : 0);
-    if (6 * w.num_keyframes + ncal > 400) return fail(CGMLI_E_LIMIT, "window visual dimension above 400");
-    return CGMLI_OK;
-}
 }  // namespace
 
 extern "C" {
 
 const char* cgmli_last_error(void) { return g_error.c_str(); }
+
+int cgmli_topology_check(const cgmli_window* windows, int count, int threads, double* seconds) {
+    if (!windows || count < 1) return fail(CGMLI_E_INVALID, "empty window list");
+    const auto t0 = std::chrono::steady_clock::now();
+    HostBatch hb;
+    std::string why;
+    int st = buildHostBatch(windows, count, threads, hb, why);
+    const auto t1 = std::chrono::steady_clock::now();
+    if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+    if (st != CGMLI_OK) return fail(st, why);
+    st = checkHostBatch(windows, count, hb, why);
+    if (st != CGMLI_OK) return fail(st, why);
+    return CGMLI_OK;
+}
 
 void cgmli_default_options(cgmli_solver_options* o) {
     o->precision = CGMLI_PRECISION_FP64;
@@ -292,274 +258,72 @@ void cgmli_solver_destroy(cgmli_solver* s) { delete s; }
 
 int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int count) {
     if (!S || !windows || count < 1) return fail(CGMLI_E_INVALID, "null solver or empty window list");
-    for (int i = 0; i < count; ++i) {
-        const int st = validateWindow(windows[i], i);
-        if (st != CGMLI_OK) return st;
-    }
     CK(cudaSetDevice(S->device));
     cudaStream_t st = S->stream;
-    S->win.assign(count, WinDesc{});
+    // the previous batch's uploads read the pinned host arrays that are rebuilt now
+    CK(cudaStreamSynchronize(st));
     S->haveSnapshot = false;
-    S->runs.clear(); S->tiles.clear(); S->lmPerm.clear(); S->pairChunks.clear(); S->schurChunks.clear();
-    int kf = 0, ex = 0, cam = 0, lm = 0, ob = 0, im = 0, pblk = 0, vec = 0, groups = 0;
-    long long dense = 0, acc = 0, schOff = 0, pA = 0, pR = 0, pRef = 0, imuS = 0, priS = 0, cOff = 0;
-    std::vector<int> obLmv, keyOrderv;
-    S->maxNpc = 0; S->maxNr = 0;
-    std::vector<double> camR, camT, lmBearing, lmVel, lmTime, obBearing, obP, obVel, obTime;
-    std::vector<int> camExt, lmWin, lmKf, lmCam, lmObsBegin, lmNs, lmNx, lmSupp0, supp, lmGroup, obKf, obKfl, obCam, obSlot, obXslot, imuKf;
-    std::vector<long long> lmC0;
-    std::vector<int> priorKind, priorIndex, priorCol, priorOff;
-    std::vector<double> priorA, priorR0, priorRef, imuData;
-    std::vector<double> pose, sbv, extv, tdv, rhov;
-    long long totalLm = 0;
-    for (int i = 0; i < count; ++i) totalLm += windows[i].num_landmarks;
-    // landmarks per warp run: enough runs to fill the GPU, long runs for large batches
-    const long long targetRuns = 148ll * 6 * 4;
-    const int runLen = (int)std::max<long long>(4, std::min<long long>(64, totalLm / targetRuns));
-    for (int i = 0; i < count; ++i) {
-        const auto& w = windows[i];
-        WinDesc& d = S->win[i];
-        d.K = w.num_keyframes; d.E = w.num_extrinsics; d.C = w.num_cameras; d.L = w.num_landmarks; d.F = w.num_observations;
-        d.nImu = w.num_imu;
-        d.estExt = w.estimate_extrinsics != 0; d.estTd = w.estimate_td != 0 && w.td; d.hasTd = w.td != nullptr;
-        d.ncalib = (d.estExt ? 6 * d.E : 0) + (d.estTd ? 1 : 0);
-        d.Npc = 6 * d.K + d.ncalib;
-        d.Nr = 15 * d.K + d.ncalib;
-        d.kf0 = kf; d.ext0 = ex; d.cam0 = cam; d.lm0 = lm; d.obs0 = ob; d.imu0 = im;
-        d.vec0 = vec; d.dense0 = dense; d.acc0 = acc; d.sch0 = schOff;
-        d.huber = w.huber_scale; d.minInv = w.min_inverse_distance;
-        S->maxNpc = std::max(S->maxNpc, d.Npc);
-        S->maxNr = std::max(S->maxNr, d.Nr);
-        vec += d.Nr;
-        dense += (long long)d.Nr * d.Nr;
-        acc += (long long)d.Npc * (d.Npc + 1) / 2 + 3ll * d.Npc;
-        schOff += (long long)d.Npc * (d.Npc + 1) / 2;
-        pose.insert(pose.end(), w.poses, w.poses + 7 * d.K);
-        sbv.insert(sbv.end(), w.speed_bias, w.speed_bias + 9 * d.K);
-        extv.insert(extv.end(), w.extrinsics, w.extrinsics + 7 * d.E);
-        tdv.push_back(w.td ? *w.td : 0.0);
-        camR.insert(camR.end(), w.cam_R, w.cam_R + 9 * d.C);
-        camT.insert(camT.end(), w.cam_t, w.cam_t + 3 * d.C);
-        for (int c = 0; c < d.C; ++c) camExt.push_back(ex + w.cam_ext[c]);
-        // support of each landmark: keyframes (anchor first, then observers
-        // ascending), then the extrinsic blocks its observations touch (the
-        // anchor camera's first, then the others ascending) when estimated
-        std::vector<std::vector<int>> sup(d.L);
-        std::vector<int> nkf(d.L), nx(d.L);
-        for (int l = 0; l < d.L; ++l) {
-            const int a = w.lm_anchor_kf[l];
-            std::vector<int> kfs{a}, exs;
-            if (d.estExt) exs.push_back(w.cam_ext[w.lm_anchor_cam[l]]);
-            for (int f = w.lm_obs_begin[l]; f < w.lm_obs_begin[l + 1]; ++f) {
-                if (std::find(kfs.begin(), kfs.end(), w.obs_kf[f]) == kfs.end()) kfs.push_back(w.obs_kf[f]);
-                const int e = w.cam_ext[w.obs_cam[f]];
-                if (d.estExt && std::find(exs.begin(), exs.end(), e) == exs.end()) exs.push_back(e);
-            }
-            std::sort(kfs.begin() + 1, kfs.end());
-            if (exs.size() > 1) std::sort(exs.begin() + 1, exs.end());
-            if ((int)kfs.size() > kMaxSupport) return fail(CGMLI_E_LIMIT, "landmark support above 64 keyframes");
-            nkf[l] = (int)kfs.size();
-            nx[l] = (int)exs.size();
-            sup[l] = kfs;
-            sup[l].push_back(-1);  // separator keeps keyframe and extrinsic lists distinct in the sort key
-            sup[l].insert(sup[l].end(), exs.begin(), exs.end());
-        }
-        // device order: landmarks sorted by support (stable), so that equal supports are adjacent
-        std::vector<int> order(d.L);
-        for (int l = 0; l < d.L; ++l) order[l] = l;
-        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-            if (sup[x].size() != sup[y].size()) return sup[x].size() < sup[y].size();
-            return sup[x] < sup[y];
-        });
-        int tileObs = 0, runTiles = 0, runLms = 0;
-        for (int q = 0; q < d.L; ++q) {
-            const int l = order[q];
-            const auto& key = sup[l];
-            const int ns = 6 * (nkf[l] + nx[l]) + (d.estTd ? 1 : 0);
-            const bool newGroup = q == 0 || sup[order[q - 1]] != key;
-            if (newGroup) ++groups;
-            const int b = w.lm_obs_begin[l], e = w.lm_obs_begin[l + 1], nobs = e - b;
-            // run / tile bookkeeping: runs end at group boundaries once long enough
-            if (q == 0 || (runLms >= runLen && newGroup) || runLms >= 4 * runLen) {
-                if (!S->runs.empty() && S->runs.back().z < 0) S->runs.back().z = (int)S->tiles.size();
-                if (!S->tiles.empty() && S->tiles.back().y < 0) S->tiles.back().y = lm + q;
-                S->runs.push_back(make_int4(i, (int)S->tiles.size(), -1, 0));
-                S->tiles.push_back(make_int2(lm + q, -1));
-                tileObs = 0; runLms = 0; runTiles = 1;
-            } else if (tileObs + nobs > kMaxTrackChunk) {
-                S->tiles.back().y = lm + q;
-                S->tiles.push_back(make_int2(lm + q, -1));
-                tileObs = 0; ++runTiles;
-            }
-            tileObs += nobs;
-            ++runLms;
-            S->lmPerm.push_back(l);
-            lmGroup.push_back(groups);
-            lmWin.push_back(i);
-            lmKf.push_back(kf + w.lm_anchor_kf[l]);
-            lmCam.push_back(cam + w.lm_anchor_cam[l]);
-            lmObsBegin.push_back(ob + (int)obKf.size() - ob);
-            for (int k = 0; k < 3; ++k) lmBearing.push_back(w.lm_anchor_bearing[3 * l + k]);
-            for (int k = 0; k < 3; ++k) lmVel.push_back(w.lm_anchor_velocity ? w.lm_anchor_velocity[3 * l + k] : 0.0);
-            lmTime.push_back(w.lm_anchor_time ? w.lm_anchor_time[l] : 0.0);
-            lmNs.push_back(nkf[l]);
-            lmNx.push_back(nx[l]);
-            lmSupp0.push_back((int)supp.size());
-            supp.insert(supp.end(), key.begin(), key.begin() + nkf[l]);
-            supp.insert(supp.end(), key.begin() + nkf[l] + 1, key.end());
-            lmC0.push_back(cOff);
-            cOff += ns;
-            rhov.push_back(w.rho[l]);
-            // observations of the landmark sorted by observer keyframe (slot order)
-            std::vector<int> fo(nobs);
-            for (int k = 0; k < nobs; ++k) fo[k] = b + k;
-            std::stable_sort(fo.begin(), fo.end(), [&](int x, int y) { return w.obs_kf[x] < w.obs_kf[y]; });
-            for (int f : fo) {
-                obLmv.push_back(lm + q);
-                obKf.push_back(kf + w.obs_kf[f]);
-                obKfl.push_back(w.obs_kf[f]);
-                obCam.push_back(cam + w.obs_cam[f]);
-                obSlot.push_back((int)(std::find(key.begin(), key.begin() + nkf[l], w.obs_kf[f]) - key.begin()));
-                {
-                    const auto xb = key.begin() + nkf[l] + 1;
-                    obXslot.push_back(d.estExt ? (int)(std::find(xb, key.end(), w.cam_ext[w.obs_cam[f]]) - xb) : 0);
-                }
-                for (int k = 0; k < 3; ++k) obBearing.push_back(w.obs_bearing[3 * f + k]);
-                for (int k = 0; k < 6; ++k) obP.push_back(w.obs_P[6 * f + k]);
-                for (int k = 0; k < 3; ++k) obVel.push_back(w.obs_velocity ? w.obs_velocity[3 * f + k] : 0.0);
-                obTime.push_back(w.obs_time ? w.obs_time[f] : 0.0);
-            }
-        }
-        if (d.L) {
-            S->tiles.back().y = lm + d.L;
-            S->runs.back().z = (int)S->tiles.size();
-        }
-        // observations of the window in key order (anchor kf, observer kf, anchor ext,
-        // observer ext): the J^T J pass sums the observations of one key together
-        {
-            const int F = (int)obKf.size() - ob;  // device observations of this window: [ob, ob + F)
-            auto keyOf = [&](int g) {
-                const int l = obLmv[g] - lm;  // device landmark within the window
-                const int a = lmKf[lm + l] - kf, b = obKf[g] - kf;
-                const int ea = camExt[lmCam[lm + l]] - ex, eb = camExt[obCam[g]] - ex;
-                return ((long long)(a * d.K + b) * d.E + ea) * d.E + eb;
-            };
-            const long long buckets = (long long)d.K * d.K * d.E * d.E;
-            std::vector<int> order(F);
-            if (buckets <= 4ll * F + 4096) {
-                std::vector<int> count(buckets + 1, 0);
-                for (int g = 0; g < F; ++g) ++count[keyOf(ob + g) + 1];
-                for (long long k = 0; k < buckets; ++k) count[k + 1] += count[k];
-                for (int g = 0; g < F; ++g) order[count[keyOf(ob + g)]++] = ob + g;
-            } else {
-                std::vector<std::pair<long long, int>> kv(F);
-                for (int g = 0; g < F; ++g) kv[g] = {keyOf(ob + g), ob + g};
-                std::sort(kv.begin(), kv.end());
-                for (int g = 0; g < F; ++g) order[g] = kv[g].second;
-            }
-            const int base = (int)keyOrderv.size();
-            keyOrderv.insert(keyOrderv.end(), order.begin(), order.end());
-            for (int c0 = 0; c0 < F; c0 += 32)
-                S->pairChunks.push_back(make_int4(i, base + c0, base + std::min(F, c0 + 32), 0));
-            const int rows = schurRowsPerChunk(d.Npc);
-            for (int l0 = 0; l0 < d.L; l0 += rows)
-                S->schurChunks.push_back(make_int4(i, lm + l0, lm + std::min(d.L, l0 + rows), 0));
-        }
-        (void)runTiles;
-        // IMU
-        for (int q = 0; q < d.nImu; ++q) {
-            const double* raw = reinterpret_cast<const double*>(&w.imu[q]);
-            imuData.insert(imuData.end(), raw, raw + sizeof(cgmli_frozen_imu) / sizeof(double));
-            imuKf.push_back(kf + w.imu_kf[q]);
-        }
-        d.imuScratch0 = imuS;
-        imuS += 465ll * d.nImu;
-        // prior
-        d.priorRank = w.prior_rank;
-        d.priorBlk0 = pblk;
-        d.priorBlocks = w.prior_rank > 0 ? w.prior_num_blocks : 0;
-        int cols = 0, amb = 0;
-        for (int b2 = 0; b2 < d.priorBlocks; ++b2) {
-            const int kind = w.prior_block_kind[b2], idx = w.prior_block_index[b2];
-            priorKind.push_back(kind);
-            int gidx = idx, col = -1;
-            if (kind == CGMLI_PRIOR_POSE) { gidx = kf + idx; col = 15 * idx; }
-            else if (kind == CGMLI_PRIOR_SPEED_BIAS) { gidx = kf + idx; col = 15 * idx + 6; }
-            else if (kind == CGMLI_PRIOR_EXTRINSIC) { gidx = ex + idx; col = d.estExt ? 15 * d.K + 6 * idx : -1; }
-            else { gidx = i; col = d.estTd ? 15 * d.K + (d.estExt ? 6 * d.E : 0) : -1; }
-            priorIndex.push_back(gidx);
-            priorCol.push_back(col);
-            priorOff.push_back(cols);
-            cols += tangentOf(kind);
-            amb += ambientOf(kind);
-        }
-        d.priorCols = cols;
-        d.priorA0 = pA; d.priorR00 = pR; d.priorRef0 = pRef;
-        if (d.priorRank > 0) {
-            priorA.insert(priorA.end(), w.prior_A, w.prior_A + (long long)d.priorRank * cols);
-            priorR0.insert(priorR0.end(), w.prior_r0, w.prior_r0 + d.priorRank);
-            priorRef.insert(priorRef.end(), w.prior_ref, w.prior_ref + amb);
-        }
-        pA += (long long)d.priorRank * cols;
-        pR += d.priorRank;
-        pRef += d.priorRank > 0 ? amb : 0;
-        pblk += d.priorBlocks;
-        d.priorScratch0 = priS;
-        priS += d.priorRank > 0 ? (long long)cols * 7 + d.priorRank + (long long)d.priorRank * cols : 0;
-        kf += d.K; ex += d.E; cam += d.C; lm += d.L; ob += d.F; im += d.nImu;
-    }
-    lmObsBegin.push_back((int)obKf.size());
-    S->totalKf = kf; S->totalExt = ex; S->totalCam = cam; S->totalLm = lm; S->totalObs = ob; S->totalImu = im;
-    S->maxNs = 1;
-    for (size_t q = 0; q < lmNs.size(); ++q)
-        S->maxNs = std::max(S->maxNs, 6 * (lmNs[q] + lmNx[q]) + (S->win[lmWin[q]].estTd ? 1 : 0));
+    S->haveMarg = false;
+    S->win.clear();
+    HostBatch& hb = S->hb;
+    std::string why;
+    const int built = buildHostBatch(windows, count, 0, hb, why);
+    if (built != CGMLI_OK) return fail(built, why);
+    S->win = hb.win;
+    S->totalKf = hb.totalKf; S->totalExt = hb.totalExt; S->totalCam = hb.totalCam; S->totalLm = hb.totalLm;
+    S->totalObs = hb.totalObs; S->totalImu = hb.totalImu;
+    S->maxNpc = hb.maxNpc; S->maxNr = hb.maxNr; S->maxNs = hb.maxNs;
     S->linSmem = linearizeSmemBytes(S->maxNs);
     S->facSmem = factorSmemBytes(S->maxNr);
     CK(configureKernels(S->linSmem, S->facSmem));
+    const long long lm = hb.totalLm;
     CK(S->dWin.upload(S->win, st));
     CK(S->dLm.reserve(count));
-    CK(S->dRuns.upload(S->runs, st));
-    CK(S->dTiles.upload(S->tiles, st));
-    CK(S->camR.upload(camR, st)); CK(S->camT.upload(camT, st)); CK(S->camExt.upload(camExt, st));
-    CK(S->lmWin.upload(lmWin, st)); CK(S->lmKf.upload(lmKf, st)); CK(S->lmCam.upload(lmCam, st));
-    CK(S->lmObsBegin.upload(lmObsBegin, st)); CK(S->lmNs.upload(lmNs, st)); CK(S->lmSupp0.upload(lmSupp0, st));
-    CK(S->supp.upload(supp, st)); CK(S->lmC0.upload(lmC0, st)); CK(S->lmGroup.upload(lmGroup, st));
-    CK(S->lmNx.upload(lmNx, st)); CK(S->obXslot.upload(obXslot, st));
-    CK(S->lmBearing.upload(lmBearing, st)); CK(S->lmVel.upload(lmVel, st)); CK(S->lmTime.upload(lmTime, st));
-    CK(S->obKf.upload(obKf, st)); CK(S->obKfl.upload(obKfl, st)); CK(S->obCam.upload(obCam, st)); CK(S->obSlot.upload(obSlot, st));
-    CK(S->obBearing.upload(obBearing, st)); CK(S->obP.upload(obP, st)); CK(S->obVel.upload(obVel, st));
-    CK(S->obTime.upload(obTime, st));
-    CK(S->pose[0].upload(pose, st)); CK(S->sb[0].upload(sbv, st)); CK(S->ext[0].upload(extv, st));
-    CK(S->td[0].upload(tdv, st)); CK(S->rho[0].upload(rhov, st));
-    CK(S->pose[1].reserve(pose.size())); CK(S->sb[1].reserve(sbv.size())); CK(S->ext[1].reserve(extv.size()));
-    CK(S->td[1].reserve(tdv.size())); CK(S->rho[1].reserve(rhov.size()));
-    CK(S->imu.upload(imuData, st)); CK(S->imuKf.upload(imuKf, st));
-    CK(S->priorKind.upload(priorKind, st)); CK(S->priorIndex.upload(priorIndex, st));
-    CK(S->priorCol.upload(priorCol, st)); CK(S->priorOff.upload(priorOff, st));
-    CK(S->priorA.upload(priorA, st)); CK(S->priorR0.upload(priorR0, st)); CK(S->priorRef.upload(priorRef, st));
-    CK(S->lmC.reserve(cOff)); CK(S->lmD.reserve(lm)); CK(S->lmG.reserve(lm)); CK(S->lmCost.reserve(lm));
+    CK(S->dRuns.upload(hb.runs, st));
+    CK(S->dTiles.upload(hb.tiles, st));
+    CK(S->dPairChunks.upload(hb.pairChunks, st));
+    CK(S->dSchurChunks.upload(hb.schurChunks, st));
+    CK(S->camR.upload(hb.camR, st)); CK(S->camT.upload(hb.camT, st)); CK(S->camExt.upload(hb.camExt, st));
+    CK(S->lmKf.upload(hb.lmKf, st)); CK(S->lmCam.upload(hb.lmCam, st)); CK(S->lmObsBegin.upload(hb.lmObsBegin, st));
+    CK(S->lmNs.upload(hb.lmNs, st)); CK(S->lmNx.upload(hb.lmNx, st)); CK(S->lmSupp0.upload(hb.lmSupp0, st));
+    CK(S->supp.upload(hb.supp, st)); CK(S->lmC0.upload(hb.lmC0, st));
+    CK(S->lmBearing.upload(hb.lmBearing, st)); CK(S->lmVel.upload(hb.lmVel, st)); CK(S->lmTime.upload(hb.lmTime, st));
+    CK(S->obKf.upload(hb.obKf, st)); CK(S->obCam.upload(hb.obCam, st)); CK(S->obSlot.upload(hb.obSlot, st));
+    CK(S->obXslot.upload(hb.obXslot, st)); CK(S->obLm.upload(hb.obLm, st)); CK(S->keyOrder.upload(hb.keyOrder, st));
+    CK(S->obBearing.upload(hb.obBearing, st)); CK(S->obP.upload(hb.obP, st)); CK(S->obVel.upload(hb.obVel, st));
+    CK(S->obTime.upload(hb.obTime, st));
+    CK(S->pose[0].upload(hb.pose, st)); CK(S->sb[0].upload(hb.sb, st)); CK(S->ext[0].upload(hb.ext, st));
+    CK(S->td[0].upload(hb.td, st)); CK(S->rho[0].upload(hb.rho, st));
+    CK(S->pose[1].reserve(hb.pose.size())); CK(S->sb[1].reserve(hb.sb.size())); CK(S->ext[1].reserve(hb.ext.size()));
+    CK(S->td[1].reserve(hb.td.size())); CK(S->rho[1].reserve(hb.rho.size()));
+    CK(S->imu.upload(hb.imu, st)); CK(S->imuKf.upload(hb.imuKf, st));
+    CK(S->priorKind.upload(hb.priorKind, st)); CK(S->priorIndex.upload(hb.priorIndex, st));
+    CK(S->priorCol.upload(hb.priorCol, st)); CK(S->priorOff.upload(hb.priorOff, st));
+    CK(S->priorA.upload(hb.priorA, st)); CK(S->priorR0.upload(hb.priorR0, st)); CK(S->priorRef.upload(hb.priorRef, st));
+    CK(S->lmC.reserve(hb.cross)); CK(S->lmD.reserve(lm)); CK(S->lmG.reserve(lm)); CK(S->lmCost.reserve(lm));
     CK(S->lmDelta.reserve(lm)); CK(S->lmPred.reserve(lm)); CK(S->lmTrial.reserve(lm)); CK(S->lmMaxInc.reserve(lm));
     CK(S->lmValid.reserve(lm)); CK(S->lmTrialValid.reserve(lm));
-    CK(S->Hret.reserve(dense)); CK(S->Sglob.reserve(dense)); CK(S->gret.reserve(vec)); CK(S->dr.reserve(vec)); CK(S->rhs.reserve(vec));
-    CK(S->acc.reserve(acc)); CK(S->sch.reserve(schOff)); CK(S->imuScratch.reserve(imuS)); CK(S->priorScratch.reserve(priS));
-    CK(S->obLm.upload(obLmv, st)); CK(S->keyOrder.upload(keyOrderv, st));
-    CK(S->dPairChunks.upload(S->pairChunks, st)); CK(S->dSchurChunks.upload(S->schurChunks, st));
+    CK(S->Hret.reserve(hb.dense)); CK(S->Sglob.reserve(hb.dense)); CK(S->gret.reserve(hb.vec)); CK(S->dr.reserve(hb.vec));
+    CK(S->rhs.reserve(hb.vec));
+    CK(S->acc.reserve(hb.acc)); CK(S->sch.reserve(hb.sch)); CK(S->imuScratch.reserve(hb.imuScratch));
+    CK(S->priorScratch.reserve(hb.priorScratch));
     CK(S->costRet.reserve(count)); CK(S->trialRet.reserve(count)); CK(S->retValid.reserve(count));
     CK(S->predState.reserve(count)); CK(S->solveStatus.reserve(count)); CK(S->out.reserve(4ll * count));
     DevBatch& B = S->B;
     B = DevBatch{};
-    B.numWindows = count; B.numLandmarks = lm; B.numObs = ob; B.numKf = kf; B.numExt = ex; B.numCam = cam; B.numImu = im;
-    B.numRuns = (int)S->runs.size();
+    B.numWindows = count; B.numLandmarks = hb.totalLm; B.numObs = hb.totalObs; B.numKf = hb.totalKf; B.numExt = hb.totalExt;
+    B.numCam = hb.totalCam; B.numImu = hb.totalImu;
+    B.numRuns = (int)hb.runs.size();
     B.win = S->dWin.p; B.lm = S->dLm.p;
     B.camR = S->camR.p; B.camT = S->camT.p; B.camExt = S->camExt.p;
-    B.lmWin = S->lmWin.p; B.lmKf = S->lmKf.p; B.lmCam = S->lmCam.p; B.lmObsBegin = S->lmObsBegin.p;
+    B.lmKf = S->lmKf.p; B.lmCam = S->lmCam.p; B.lmObsBegin = S->lmObsBegin.p;
     B.lmBearing = S->lmBearing.p; B.lmVel = S->lmVel.p; B.lmTime = S->lmTime.p;
     B.lmNs = S->lmNs.p; B.lmNx = S->lmNx.p; B.lmSupp0 = S->lmSupp0.p; B.supp = S->supp.p; B.lmC0 = S->lmC0.p;
-    B.lmGroup = S->lmGroup.p; B.obXslot = S->obXslot.p;
+    B.obXslot = S->obXslot.p;
     B.lmC = S->lmC.p; B.lmD = S->lmD.p; B.lmG = S->lmG.p; B.lmCost = S->lmCost.p; B.lmValid = S->lmValid.p;
     B.lmDelta = S->lmDelta.p; B.lmPred = S->lmPred.p; B.lmTrial = S->lmTrial.p; B.lmMaxInc = S->lmMaxInc.p;
     B.lmTrialValid = S->lmTrialValid.p;
-    B.obKf = S->obKf.p; B.obKfl = S->obKfl.p; B.obCam = S->obCam.p; B.obSlot = S->obSlot.p;
+    B.obKf = S->obKf.p; B.obCam = S->obCam.p; B.obSlot = S->obSlot.p;
     B.obLm = S->obLm.p; B.keyOrder = S->keyOrder.p;
     B.obBearing = S->obBearing.p; B.obP = S->obP.p; B.obVel = S->obVel.p; B.obTime = S->obTime.p;
     for (int k = 0; k < 2; ++k) {
@@ -572,34 +336,35 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     B.acc = S->acc.p; B.sch = S->sch.p; B.dr = S->dr.p; B.rhs = S->rhs.p; B.Sglob = S->Sglob.p;
     B.imuScratch = S->imuScratch.p; B.priorScratch = S->priorScratch.p; B.predState = S->predState.p;
     B.solveStatus = S->solveStatus.p; B.out = S->out.p;
-    S->hLmKf = lmKf; S->hLmCam = lmCam; S->hLmObsBegin = lmObsBegin; S->hObKf = obKf; S->hObCam = obCam;
-    S->hCamExt = camExt; S->hImuKf = imuKf; S->hPriorKind = priorKind; S->hPriorIndex = priorIndex;
-    S->haveMarg = false;
     CK(cudaMemsetAsync(S->costRet.p, 0, count * sizeof(double), st));
     CK(cudaMemsetAsync(S->trialRet.p, 0, count * sizeof(double), st));
-    CK(cudaStreamSynchronize(st));
     return CGMLI_OK;
 }
 
 int cgmli_solver_upload_states(cgmli_solver* S, const cgmli_window* windows, int count) {
     if (!S || !windows || count != (int)S->win.size()) return fail(CGMLI_E_INVALID, "window count differs from the configured batch");
-    CK(cudaSetDevice(S->device));
     for (int i = 0; i < count; ++i) {
         const WinDesc& d = S->win[i];
         const auto& w = windows[i];
-        if (w.num_keyframes != d.K || w.num_landmarks != d.L || w.num_extrinsics != d.E)
+        if (w.num_keyframes != d.K || w.num_landmarks != d.L || w.num_extrinsics != d.E || (w.td != nullptr) != (d.hasTd != 0))
             return fail(CGMLI_E_INVALID, "state upload with a different topology");
-        CK(cudaMemcpyAsync(S->pose[0].p + 7ll * d.kf0, w.poses, 7ll * d.K * sizeof(double), cudaMemcpyHostToDevice, S->stream));
-        CK(cudaMemcpyAsync(S->sb[0].p + 9ll * d.kf0, w.speed_bias, 9ll * d.K * sizeof(double), cudaMemcpyHostToDevice, S->stream));
-        CK(cudaMemcpyAsync(S->ext[0].p + 7ll * d.ext0, w.extrinsics, 7ll * d.E * sizeof(double), cudaMemcpyHostToDevice, S->stream));
-        if (w.td) CK(cudaMemcpyAsync(S->td[0].p + i, w.td, sizeof(double), cudaMemcpyHostToDevice, S->stream));
-        if (d.L) {
-            // device order is sorted by support; lmPerm maps it back to the caller's order
-            std::vector<double> r(d.L);
-            for (int q = 0; q < d.L; ++q) r[q] = w.rho[S->lmPerm[d.lm0 + q]];
-            CK(cudaMemcpy(S->rho[0].p + d.lm0, r.data(), d.L * sizeof(double), cudaMemcpyHostToDevice));
-        }
     }
+    CK(cudaSetDevice(S->device));
+    cudaStream_t st = S->stream;
+    CK(cudaStreamSynchronize(st));  // the pinned host arrays are the staging of earlier copies
+    HostBatch& hb = S->hb;
+    for (int i = 0; i < count; ++i) {
+        const WinDesc& d = S->win[i];
+        const auto& w = windows[i];
+        std::memcpy(&hb.pose[7ll * d.kf0], w.poses, 7ull * d.K * sizeof(double));
+        std::memcpy(&hb.sb[9ll * d.kf0], w.speed_bias, 9ull * d.K * sizeof(double));
+        std::memcpy(&hb.ext[7ll * d.ext0], w.extrinsics, 7ull * d.E * sizeof(double));
+        hb.td[i] = w.td ? *w.td : 0.0;
+        // device order is sorted by support; lmPerm maps it back to the caller's order
+        for (int q = 0; q < d.L; ++q) hb.rho[d.lm0 + q] = w.rho[hb.lmPerm[d.lm0 + q]];
+    }
+    CK(S->pose[0].upload(hb.pose, st)); CK(S->sb[0].upload(hb.sb, st)); CK(S->ext[0].upload(hb.ext, st));
+    CK(S->td[0].upload(hb.td, st)); CK(S->rho[0].upload(hb.rho, st));
     return CGMLI_OK;
 }
 
@@ -716,7 +481,7 @@ int cgmli_solver_read_step(cgmli_solver* S, int w, double* increment, double* co
         if (d.L) {
             std::vector<double> r(d.L);
             CK(cudaMemcpy(r.data(), S->lmDelta.p + d.lm0, d.L * sizeof(double), cudaMemcpyDeviceToHost));
-            for (int q = 0; q < d.L; ++q) increment[d.Nr + S->lmPerm[d.lm0 + q]] = r[q];
+            for (int q = 0; q < d.L; ++q) increment[d.Nr + S->hb.lmPerm[d.lm0 + q]] = r[q];
         }
     }
     if (cost) *cost = lmst.linCost;
@@ -753,19 +518,23 @@ int cgmli_solver_read_reduced(cgmli_solver* S, int w, double* Sout, double* rhs)
 int cgmli_solver_read_states(cgmli_solver* S, cgmli_window* windows, int count) {
     if (!S || !windows || count != (int)S->win.size()) return fail(CGMLI_E_INVALID, "window count differs from the configured batch");
     CK(cudaSetDevice(S->device));
-    CK(cudaStreamSynchronize(S->stream));
+    // one copy per state array into the pinned host arrays, then a scatter to the windows
+    HostBatch& hb = S->hb;
+    cudaStream_t st = S->stream;
+    CK(cudaMemcpyAsync(hb.pose.data(), S->pose[0].p, hb.pose.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hb.sb.data(), S->sb[0].p, hb.sb.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hb.ext.data(), S->ext[0].p, hb.ext.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hb.td.data(), S->td[0].p, hb.td.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (!hb.rho.empty()) CK(cudaMemcpyAsync(hb.rho.data(), S->rho[0].p, hb.rho.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
     for (int i = 0; i < count; ++i) {
         const WinDesc& d = S->win[i];
         auto& w = windows[i];
-        CK(cudaMemcpy(w.poses, S->pose[0].p + 7ll * d.kf0, 7ll * d.K * sizeof(double), cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(w.speed_bias, S->sb[0].p + 9ll * d.kf0, 9ll * d.K * sizeof(double), cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(w.extrinsics, S->ext[0].p + 7ll * d.ext0, 7ll * d.E * sizeof(double), cudaMemcpyDeviceToHost));
-        if (w.td) CK(cudaMemcpy(w.td, S->td[0].p + i, sizeof(double), cudaMemcpyDeviceToHost));
-        if (d.L) {
-            std::vector<double> r(d.L);
-            CK(cudaMemcpy(r.data(), S->rho[0].p + d.lm0, d.L * sizeof(double), cudaMemcpyDeviceToHost));
-            for (int q = 0; q < d.L; ++q) w.rho[S->lmPerm[d.lm0 + q]] = r[q];
-        }
+        std::memcpy(w.poses, &hb.pose[7ll * d.kf0], 7ull * d.K * sizeof(double));
+        std::memcpy(w.speed_bias, &hb.sb[9ll * d.kf0], 9ull * d.K * sizeof(double));
+        std::memcpy(w.extrinsics, &hb.ext[7ll * d.ext0], 7ull * d.E * sizeof(double));
+        if (w.td) *w.td = hb.td[i];
+        for (int q = 0; q < d.L; ++q) w.rho[hb.lmPerm[d.lm0 + q]] = hb.rho[d.lm0 + q];
     }
     return CGMLI_OK;
 }
@@ -827,30 +596,30 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
         bool tdUsed = false;
         std::vector<int> elimLm;
         for (int q = 0; q < d.L; ++q) {
-            const int g = d.lm0 + q, a = S->hLmKf[g] - d.kf0;
+            const int g = d.lm0 + q, a = S->hb.lmKf[g] - d.kf0;
             bool e = a == v;
-            for (int f = S->hLmObsBegin[g]; f < S->hLmObsBegin[g + 1] && !e && policy == CGMLI_MARGIN_OLD; ++f)
-                e = S->hObKf[f] - d.kf0 == v;
+            for (int f = S->hb.lmObsBegin[g]; f < S->hb.lmObsBegin[g + 1] && !e && policy == CGMLI_MARGIN_OLD; ++f)
+                e = S->hb.obKf[f] - d.kf0 == v;
             if (!e) continue;
             elimLm.push_back(g);
-            for (int f = S->hLmObsBegin[g]; f < S->hLmObsBegin[g + 1]; ++f) {
+            for (int f = S->hb.lmObsBegin[g]; f < S->hb.lmObsBegin[g + 1]; ++f) {
                 poseUsed[a] = 1;
-                poseUsed[S->hObKf[f] - d.kf0] = 1;
-                extUsed[S->hCamExt[S->hLmCam[g]] - d.ext0] = 1;
-                extUsed[S->hCamExt[S->hObCam[f]] - d.ext0] = 1;
+                poseUsed[S->hb.obKf[f] - d.kf0] = 1;
+                extUsed[S->hb.camExt[S->hb.lmCam[g]] - d.ext0] = 1;
+                extUsed[S->hb.camExt[S->hb.obCam[f]] - d.ext0] = 1;
                 tdUsed = true;
             }
         }
         int nImu = 0;
         for (int i = 0; i < d.nImu; ++i) {
-            const int k = S->hImuKf[d.imu0 + i] - d.kf0;
+            const int k = S->hb.imuKf[d.imu0 + i] - d.kf0;
             if (k != v && k + 1 != v) continue;
             if (nImu == 2) return fail(CGMLI_E_LIMIT, "more than two IMU factors touch the victim keyframe");
             mw.imu[nImu++] = d.imu0 + i;
             poseUsed[k] = poseUsed[k + 1] = sbUsed[k] = sbUsed[k + 1] = 1;
         }
         for (int b = 0; b < d.priorBlocks; ++b) {
-            const int kind = S->hPriorKind[d.priorBlk0 + b], gi = S->hPriorIndex[d.priorBlk0 + b];
+            const int kind = S->hb.priorKind[d.priorBlk0 + b], gi = S->hb.priorIndex[d.priorBlk0 + b];
             if (kind == CGMLI_PRIOR_POSE) poseUsed[gi - d.kf0] = 1;
             else if (kind == CGMLI_PRIOR_SPEED_BIAS) sbUsed[gi - d.kf0] = 1;
             else if (kind == CGMLI_PRIOR_EXTRINSIC) extUsed[gi - d.ext0] = 1;
@@ -887,9 +656,9 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
                 me.nc += size;
                 return blkLocal.back();
             };
-            const int a = S->hLmKf[g], ea = S->hCamExt[S->hLmCam[g]];
-            for (int f = S->hLmObsBegin[g]; f < S->hLmObsBegin[g + 1]; ++f) {
-                const int b = S->hObKf[f], eb = S->hCamExt[S->hObCam[f]];
+            const int a = S->hb.lmKf[g], ea = S->hb.camExt[S->hb.lmCam[g]];
+            for (int f = S->hb.lmObsBegin[g]; f < S->hb.lmObsBegin[g + 1]; ++f) {
+                const int b = S->hb.obKf[f], eb = S->hb.camExt[S->hb.obCam[f]];
                 obsMap.push_back(localOf(poseCol[a], 6));
                 obsMap.push_back(localOf(poseCol[b], 6));
                 obsMap.push_back(localOf(extCol[ea], 6));

@@ -29,7 +29,6 @@ struct WinDesc {
     int estExt, estTd, hasTd;
     int kf0, ext0, cam0, lm0, obs0, imu0;
     int priorRank, priorCols, priorBlocks, priorBlk0;
-    int slab0, nslab;
     int vec0;            // offset of Nr-vectors (gret, dr, rhs)
     long long dense0;    // offset of Nr*Nr matrices (Hret, factor scratch)
     long long acc0;      // offset of the visual accumulator: Npc(Npc+1)/2 + 3*Npc
@@ -47,7 +46,6 @@ struct WinLM {
 };
 enum { kModeLinearize = 0, kModeResolve = 1, kModeDone = 2 };
 
-struct Slab { int win, lmBegin, lmEnd, pad; };  // unused legacy name kept for the layout comment
 
 // Pointers to every device array (filled by the host runtime).
 struct DevBatch {
@@ -57,15 +55,14 @@ struct DevBatch {
     // cameras
     const double* camR; const double* camT; const int* camExt;  // camExt: global extrinsic index
     // landmarks
-    const int* lmWin; const int* lmKf; const int* lmCam; const int* lmObsBegin;  // lmObsBegin: numLandmarks+1
+    const int* lmKf; const int* lmCam; const int* lmObsBegin;  // lmObsBegin: numLandmarks+1
     const double* lmBearing; const double* lmVel; const double* lmTime;
     const int* lmNs; const int* lmNx; const int* lmSupp0; const int* supp;  // support: s keyframes (anchor first), then x extrinsics
-    const int* lmGroup;                                   // equal for consecutive landmarks with the same support
     const long long* lmC0;                                // offset of the landmark's cross vector
     double* lmC; double* lmD; double* lmG; double* lmCost; int* lmValid;
     double* lmDelta; double* lmPred; double* lmTrial; double* lmMaxInc; int* lmTrialValid;
     // observations
-    const int* obKf; const int* obKfl; const int* obCam; const int* obSlot; const int* obXslot;
+    const int* obKf; const int* obCam; const int* obSlot; const int* obXslot;
     const int* obLm;      // landmark (device index) of each observation
     const int* keyOrder;  // observations of each window sorted by (anchor kf, observer kf, anchor ext, observer ext)
     const double* obBearing; const double* obP; const double* obVel; const double* obTime;

@@ -1,0 +1,516 @@
+// Host-side device layout of a batch of windows; see topology.h.
+#include "topology.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <thread>
+
+namespace cgmli {
+
+// A 64-byte header records how the block was obtained.
+void* pinnedAllocate(size_t bytes) {
+    constexpr size_t kHeader = 64;
+    void* raw = nullptr;
+    long long kind = 1;
+    if (cudaHostAlloc(&raw, bytes + kHeader, cudaHostAllocPortable) != cudaSuccess) {
+        (void)cudaGetLastError();
+        raw = std::malloc(bytes + kHeader);
+        kind = 0;
+        if (!raw) return nullptr;
+    }
+    *static_cast<long long*>(raw) = kind;
+    return static_cast<char*>(raw) + kHeader;
+}
+void pinnedFree(void* p) {
+    if (!p) return;
+    void* raw = static_cast<char*>(p) - 64;
+    if (*static_cast<long long*>(raw) == 1) cudaFreeHost(raw);
+    else std::free(raw);
+}
+
+namespace {
+int tangentOf(int kind) { return kind == CGMLI_PRIOR_SPEED_BIAS ? 9 : kind == CGMLI_PRIOR_TIME_OFFSET ? 1 : 6; }
+int ambientOf(int kind) { return kind == CGMLI_PRIOR_SPEED_BIAS ? 9 : kind == CGMLI_PRIOR_TIME_OFFSET ? 1 : 7; }
+
+// Runs fn(i) for i in [0, n) on up to `threads` host threads.
+template <class Fn>
+void parallelFor(int n, int threads, Fn&& fn) {
+    if (threads <= 1 || n <= 1) {
+        for (int i = 0; i < n; ++i) fn(i);
+        return;
+    }
+    std::atomic<int> next{0};
+    auto body = [&] {
+        for (int i = next++; i < n; i = next++) fn(i);
+    };
+    std::vector<std::thread> pool;
+    const int t = std::min(threads, n);
+    for (int k = 1; k < t; ++k) pool.emplace_back(body);
+    body();
+    for (auto& th : pool) th.join();
+}
+
+// Landmarks per warp run: enough runs to fill the GPU, long runs for large batches.
+int runLength(long long totalLm) {
+    const long long targetRuns = 148ll * 6 * 4;
+    return (int)std::max<long long>(4, std::min<long long>(64, totalLm / targetRuns));
+}
+
+// Per-window results whose global position is only known after a prefix sum.
+struct WindowPart {
+    std::vector<int> supp;          // support lists (keyframes then extrinsics), window-local offsets
+    std::vector<int2> tiles;        // global landmark indices
+    std::vector<int4> runs;         // window-local tile indices
+    std::vector<int4> pairChunks;
+    std::vector<int4> schurChunks;
+    long long cross = 0;            // sum of support widths
+    int maxNs = 1;
+    int status = CGMLI_OK;
+    std::string why;
+};
+}  // namespace
+
+int validateWindow(const cgmli_window& w, int index, std::string& why) {
+    char buf[256];
+    auto bad = [&](const char* what) {
+        std::snprintf(buf, sizeof buf, "window %d: %s", index, what);
+        why = buf;
+        return CGMLI_E_INVALID;
+    };
+    if (w.num_keyframes < 1 || w.num_cameras < 1 || w.num_extrinsics < 1 || w.num_landmarks < 0 || w.num_observations < 0 ||
+        w.num_imu < 0 || w.prior_rank < 0)
+        return bad("negative or empty sizes");
+    if (!w.poses || !w.speed_bias || !w.extrinsics || (w.num_landmarks && !w.rho) || !w.cam_R || !w.cam_t || !w.cam_ext)
+        return bad("missing state or rig arrays");
+    if (w.num_landmarks && (!w.lm_anchor_kf || !w.lm_anchor_cam || !w.lm_obs_begin || !w.lm_anchor_bearing))
+        return bad("missing landmark arrays");
+    if (w.num_observations && (!w.obs_kf || !w.obs_cam || !w.obs_bearing || !w.obs_P)) return bad("missing observation arrays");
+    if (w.num_imu && (!w.imu || !w.imu_kf)) return bad("missing IMU arrays");
+    if (w.estimate_td && !w.td) return bad("estimate_td requires a td value");
+    for (int c = 0; c < w.num_cameras; ++c)
+        if (w.cam_ext[c] < 0 || w.cam_ext[c] >= w.num_extrinsics) return bad("camera extrinsic index out of range");
+    if (w.num_landmarks && (w.lm_obs_begin[0] != 0 || w.lm_obs_begin[w.num_landmarks] != w.num_observations))
+        return bad("landmark observation ranges do not cover the observations");
+    if (!w.num_landmarks && w.num_observations) return bad("observations without landmarks");
+    for (int l = 0; l < w.num_landmarks; ++l) {
+        if (w.lm_obs_begin[l + 1] < w.lm_obs_begin[l]) return bad("landmark observation ranges not sorted");
+        if (w.lm_obs_begin[l + 1] - w.lm_obs_begin[l] > kMaxTrackChunk) return bad("more than 32 observations of one landmark");
+        if (w.lm_anchor_kf[l] < 0 || w.lm_anchor_kf[l] >= w.num_keyframes) return bad("anchor keyframe out of range");
+        if (w.lm_anchor_cam[l] < 0 || w.lm_anchor_cam[l] >= w.num_cameras) return bad("anchor camera out of range");
+    }
+    for (int f = 0; f < w.num_observations; ++f) {
+        if (w.obs_kf[f] < 0 || w.obs_kf[f] >= w.num_keyframes) return bad("observer keyframe out of range");
+        if (w.obs_cam[f] < 0 || w.obs_cam[f] >= w.num_cameras) return bad("observer camera out of range");
+    }
+    for (int i = 0; i < w.num_imu; ++i)
+        if (w.imu_kf[i] < 0 || w.imu_kf[i] + 1 >= w.num_keyframes) return bad("IMU keyframe out of range");
+    if (w.prior_rank > 0) {
+        if (!w.prior_block_kind || !w.prior_block_index || !w.prior_ref || !w.prior_A || !w.prior_r0 || w.prior_num_blocks < 1)
+            return bad("missing prior arrays");
+        for (int b = 0; b < w.prior_num_blocks; ++b) {
+            const int k = w.prior_block_kind[b], i = w.prior_block_index[b];
+            if (k < 0 || k > 3) return bad("prior block kind");
+            if ((k <= 1 && (i < 0 || i >= w.num_keyframes)) || (k == 2 && (i < 0 || i >= w.num_extrinsics)) || (k == 3 && !w.td))
+                return bad("prior block index");
+        }
+    }
+    const int ncal = (w.estimate_extrinsics ? 6 * w.num_extrinsics : 0) + (w.estimate_td ? 1 : 0);
+    if (6 * w.num_keyframes + ncal > 400) {
+        std::snprintf(buf, sizeof buf, "window %d: visual dimension above 400", index);
+        why = buf;
+        return CGMLI_E_LIMIT;
+    }
+    return CGMLI_OK;
+}
+
+int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatch& hb, std::string& why) {
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    threads = std::min(threads, 64);
+    // ---- validation (parallel)
+    std::vector<int> vst(count, CGMLI_OK);
+    std::vector<std::string> vwhy(count);
+    parallelFor(count, threads, [&](int i) { vst[i] = validateWindow(windows[i], i, vwhy[i]); });
+    for (int i = 0; i < count; ++i)
+        if (vst[i] != CGMLI_OK) { why = vwhy[i]; return vst[i]; }
+    // ---- phase 0: offsets from the windows' sizes
+    hb.win.assign(count, WinDesc{});
+    hb.maxNpc = 0; hb.maxNr = 0; hb.maxNs = 1;
+    std::vector<long long> pA0(count), pR0(count), pRef0(count);
+    std::vector<int> pblk0(count);
+    int kf = 0, ex = 0, cam = 0, lm = 0, ob = 0, im = 0, pblk = 0;
+    long long vec = 0, dense = 0, acc = 0, sch = 0, imuS = 0, priS = 0, pA = 0, pR = 0, pRef = 0;
+    for (int i = 0; i < count; ++i) {
+        const auto& w = windows[i];
+        WinDesc& d = hb.win[i];
+        d.K = w.num_keyframes; d.E = w.num_extrinsics; d.C = w.num_cameras; d.L = w.num_landmarks; d.F = w.num_observations;
+        d.nImu = w.num_imu;
+        d.estExt = w.estimate_extrinsics != 0; d.estTd = w.estimate_td != 0 && w.td; d.hasTd = w.td != nullptr;
+        d.ncalib = (d.estExt ? 6 * d.E : 0) + (d.estTd ? 1 : 0);
+        d.Npc = 6 * d.K + d.ncalib;
+        d.Nr = 15 * d.K + d.ncalib;
+        d.kf0 = kf; d.ext0 = ex; d.cam0 = cam; d.lm0 = lm; d.obs0 = ob; d.imu0 = im;
+        d.vec0 = (int)vec; d.dense0 = dense; d.acc0 = acc; d.sch0 = sch;
+        d.huber = w.huber_scale; d.minInv = w.min_inverse_distance;
+        hb.maxNpc = std::max(hb.maxNpc, d.Npc);
+        hb.maxNr = std::max(hb.maxNr, d.Nr);
+        vec += d.Nr;
+        dense += (long long)d.Nr * d.Nr;
+        acc += (long long)d.Npc * (d.Npc + 1) / 2 + 3ll * d.Npc;
+        sch += (long long)d.Npc * (d.Npc + 1) / 2;
+        d.imuScratch0 = imuS;
+        imuS += 465ll * d.nImu;
+        d.priorRank = w.prior_rank;
+        d.priorBlk0 = pblk;
+        d.priorBlocks = w.prior_rank > 0 ? w.prior_num_blocks : 0;
+        int cols = 0, amb = 0;
+        for (int b = 0; b < d.priorBlocks; ++b) {
+            cols += tangentOf(w.prior_block_kind[b]);
+            amb += ambientOf(w.prior_block_kind[b]);
+        }
+        d.priorCols = cols;
+        d.priorA0 = pA; d.priorR00 = pR; d.priorRef0 = pRef;
+        pA0[i] = pA; pR0[i] = pR; pRef0[i] = pRef; pblk0[i] = pblk;
+        pA += (long long)d.priorRank * cols;
+        pR += d.priorRank;
+        pRef += d.priorRank > 0 ? amb : 0;
+        pblk += d.priorBlocks;
+        d.priorScratch0 = priS;
+        priS += d.priorRank > 0 ? (long long)cols * 7 + d.priorRank + (long long)d.priorRank * cols : 0;
+        kf += d.K; ex += d.E; cam += d.C; lm += d.L; ob += d.F; im += d.nImu;
+    }
+    hb.totalKf = kf; hb.totalExt = ex; hb.totalCam = cam; hb.totalLm = lm; hb.totalObs = ob; hb.totalImu = im;
+    hb.vec = vec; hb.dense = dense; hb.acc = acc; hb.sch = sch; hb.imuScratch = imuS; hb.priorScratch = priS;
+    constexpr int kImuDoubles = sizeof(cgmli_frozen_imu) / sizeof(double);
+    hb.camR.resize(9ll * cam); hb.camT.resize(3ll * cam); hb.camExt.resize(cam);
+    hb.lmKf.resize(lm); hb.lmCam.resize(lm); hb.lmObsBegin.resize(lm + 1ll); hb.lmNs.resize(lm); hb.lmNx.resize(lm);
+    hb.lmSupp0.resize(lm); hb.lmC0.resize(lm); hb.lmPerm.resize(lm);
+    hb.lmBearing.resize(3ll * lm); hb.lmVel.resize(3ll * lm); hb.lmTime.resize(lm);
+    hb.obKf.resize(ob); hb.obCam.resize(ob); hb.obSlot.resize(ob); hb.obXslot.resize(ob); hb.obLm.resize(ob);
+    hb.keyOrder.resize(ob);
+    hb.obBearing.resize(3ll * ob); hb.obP.resize(6ll * ob); hb.obVel.resize(3ll * ob); hb.obTime.resize(ob);
+    hb.pose.resize(7ll * kf); hb.sb.resize(9ll * kf); hb.ext.resize(7ll * ex); hb.td.resize(count); hb.rho.resize(lm);
+    hb.imu.resize((size_t)kImuDoubles * im); hb.imuKf.resize(im);
+    hb.priorKind.resize(pblk); hb.priorIndex.resize(pblk); hb.priorCol.resize(pblk); hb.priorOff.resize(pblk);
+    hb.priorA.resize(pA); hb.priorR0.resize(pR); hb.priorRef.resize(pRef);
+    hb.lmObsBegin[lm] = ob;
+    const int runLen = runLength(lm);
+    // ---- phase 1: every window on its own thread
+    std::vector<WindowPart> part(count);
+    parallelFor(count, threads, [&](int i) {
+        const auto& w = windows[i];
+        const WinDesc& d = hb.win[i];
+        WindowPart& P = part[i];
+        // states, rig, IMU, prior
+        std::memcpy(&hb.pose[7ll * d.kf0], w.poses, sizeof(double) * 7 * d.K);
+        std::memcpy(&hb.sb[9ll * d.kf0], w.speed_bias, sizeof(double) * 9 * d.K);
+        std::memcpy(&hb.ext[7ll * d.ext0], w.extrinsics, sizeof(double) * 7 * d.E);
+        hb.td[i] = w.td ? *w.td : 0.0;
+        std::memcpy(&hb.camR[9ll * d.cam0], w.cam_R, sizeof(double) * 9 * d.C);
+        std::memcpy(&hb.camT[3ll * d.cam0], w.cam_t, sizeof(double) * 3 * d.C);
+        for (int c = 0; c < d.C; ++c) hb.camExt[d.cam0 + c] = d.ext0 + w.cam_ext[c];
+        if (d.nImu) std::memcpy(&hb.imu[(size_t)kImuDoubles * d.imu0], w.imu, sizeof(cgmli_frozen_imu) * d.nImu);
+        for (int q = 0; q < d.nImu; ++q) hb.imuKf[d.imu0 + q] = d.kf0 + w.imu_kf[q];
+        {
+            int cols = 0, amb = 0;
+            for (int b = 0; b < d.priorBlocks; ++b) {
+                const int kind = w.prior_block_kind[b], idx = w.prior_block_index[b], g = pblk0[i] + b;
+                int gidx = idx, col = -1;
+                if (kind == CGMLI_PRIOR_POSE) { gidx = d.kf0 + idx; col = 15 * idx; }
+                else if (kind == CGMLI_PRIOR_SPEED_BIAS) { gidx = d.kf0 + idx; col = 15 * idx + 6; }
+                else if (kind == CGMLI_PRIOR_EXTRINSIC) { gidx = d.ext0 + idx; col = d.estExt ? 15 * d.K + 6 * idx : -1; }
+                else { gidx = i; col = d.estTd ? 15 * d.K + (d.estExt ? 6 * d.E : 0) : -1; }
+                hb.priorKind[g] = kind; hb.priorIndex[g] = gidx; hb.priorCol[g] = col; hb.priorOff[g] = cols;
+                cols += tangentOf(kind);
+                amb += ambientOf(kind);
+            }
+            if (d.priorRank > 0) {
+                std::memcpy(&hb.priorA[pA0[i]], w.prior_A, sizeof(double) * (size_t)d.priorRank * cols);
+                std::memcpy(&hb.priorR0[pR0[i]], w.prior_r0, sizeof(double) * d.priorRank);
+                std::memcpy(&hb.priorRef[pRef0[i]], w.prior_ref, sizeof(double) * amb);
+            }
+        }
+        // supports: keyframes (anchor first, then observers ascending), then the
+        // extrinsic blocks the observations touch (anchor camera's first, then ascending)
+        const int L = d.L;
+        std::vector<int> supStart(L + 1), nkf(L), nx(L);
+        std::vector<int> flat;
+        flat.reserve((size_t)2 * d.F + 2 * L + 1);
+        for (int l = 0; l < L; ++l) {
+            supStart[l] = (int)flat.size();
+            const int b = w.lm_obs_begin[l], e = w.lm_obs_begin[l + 1];
+            const int s0 = (int)flat.size();
+            flat.push_back(w.lm_anchor_kf[l]);
+            for (int f = b; f < e; ++f) {
+                const int k = w.obs_kf[f];
+                bool seen = false;
+                for (int j = s0; j < (int)flat.size(); ++j) seen = seen || flat[j] == k;
+                if (!seen) {  // insertion into the sorted tail (after the anchor)
+                    flat.push_back(k);
+                    for (int j = (int)flat.size() - 1; j > s0 + 1 && flat[j - 1] > flat[j]; --j) std::swap(flat[j - 1], flat[j]);
+                }
+            }
+            nkf[l] = (int)flat.size() - s0;
+            if (nkf[l] > kMaxSupport) {
+                P.status = CGMLI_E_LIMIT;
+                P.why = "landmark support above 64 keyframes";
+                return;
+            }
+            const int x0 = (int)flat.size();
+            if (d.estExt) {
+                flat.push_back(w.cam_ext[w.lm_anchor_cam[l]]);
+                for (int f = b; f < e; ++f) {
+                    const int x = w.cam_ext[w.obs_cam[f]];
+                    bool seen = false;
+                    for (int j = x0; j < (int)flat.size(); ++j) seen = seen || flat[j] == x;
+                    if (!seen) {
+                        flat.push_back(x);
+                        for (int j = (int)flat.size() - 1; j > x0 + 1 && flat[j - 1] > flat[j]; --j) std::swap(flat[j - 1], flat[j]);
+                    }
+                }
+            }
+            nx[l] = (int)flat.size() - x0;
+        }
+        supStart[L] = (int)flat.size();
+        // device order: landmarks sorted (stably) by support, so that equal supports are adjacent;
+        // key: (support length, keyframes, separator, extrinsics)
+        std::vector<int> order(L);
+        for (int l = 0; l < L; ++l) order[l] = l;
+        auto lessSupport = [&](int a, int b) {
+            const int la = supStart[a + 1] - supStart[a], lb = supStart[b + 1] - supStart[b];
+            if (la != lb) return la < lb;
+            const int* pa = &flat[supStart[a]];
+            const int* pb = &flat[supStart[b]];
+            const int n = std::min(nkf[a], nkf[b]);
+            for (int j = 0; j < n; ++j)
+                if (pa[j] != pb[j]) return pa[j] < pb[j];
+            if (nkf[a] != nkf[b]) return nkf[a] < nkf[b];  // the shorter keyframe list meets the separator first
+            for (int j = nkf[a]; j < la; ++j)
+                if (pa[j] != pb[j]) return pa[j] < pb[j];
+            return false;
+        };
+        std::stable_sort(order.begin(), order.end(), lessSupport);
+        // landmark and observation arrays in device order
+        int obPos = d.obs0;
+        int tileObs = 0, runLms = 0;
+        auto sameSupport = [&](int a, int b) { return !lessSupport(a, b) && !lessSupport(b, a); };
+        for (int q = 0; q < L; ++q) {
+            const int l = order[q], g = d.lm0 + q;
+            const int b = w.lm_obs_begin[l], e = w.lm_obs_begin[l + 1], nobs = e - b;
+            const bool newGroup = q == 0 || !sameSupport(order[q - 1], l);
+            if (q == 0 || (runLms >= runLen && newGroup) || runLms >= 4 * runLen) {
+                if (!P.runs.empty()) P.runs.back().z = (int)P.tiles.size();
+                if (!P.tiles.empty()) P.tiles.back().y = g;
+                P.runs.push_back(make_int4(i, (int)P.tiles.size(), -1, 0));
+                P.tiles.push_back(make_int2(g, -1));
+                tileObs = 0;
+                runLms = 0;
+            } else if (tileObs + nobs > kMaxTrackChunk) {
+                P.tiles.back().y = g;
+                P.tiles.push_back(make_int2(g, -1));
+                tileObs = 0;
+            }
+            tileObs += nobs;
+            ++runLms;
+            hb.lmPerm[g] = l;
+            hb.lmKf[g] = d.kf0 + w.lm_anchor_kf[l];
+            hb.lmCam[g] = d.cam0 + w.lm_anchor_cam[l];
+            hb.lmObsBegin[g] = obPos;
+            for (int k = 0; k < 3; ++k) {
+                hb.lmBearing[3ll * g + k] = w.lm_anchor_bearing[3 * l + k];
+                hb.lmVel[3ll * g + k] = w.lm_anchor_velocity ? w.lm_anchor_velocity[3 * l + k] : 0.0;
+            }
+            hb.lmTime[g] = w.lm_anchor_time ? w.lm_anchor_time[l] : 0.0;
+            hb.lmNs[g] = nkf[l];
+            hb.lmNx[g] = nx[l];
+            hb.lmSupp0[g] = (int)P.supp.size();  // window-local, fixed up after the prefix sum
+            const int* sl = &flat[supStart[l]];
+            P.supp.insert(P.supp.end(), sl, sl + nkf[l] + nx[l]);
+            const int ns = 6 * (nkf[l] + nx[l]) + (d.estTd ? 1 : 0);
+            hb.lmC0[g] = P.cross;  // window-local
+            P.cross += ns;
+            P.maxNs = std::max(P.maxNs, ns);
+            hb.rho[g] = w.rho[l];
+            // observations sorted by observer keyframe (slot order), stable
+            int fo[kMaxTrackChunk];
+            for (int k = 0; k < nobs; ++k) {
+                int j = k;
+                fo[j] = b + k;
+                while (j > 0 && w.obs_kf[fo[j - 1]] > w.obs_kf[fo[j]]) { std::swap(fo[j - 1], fo[j]); --j; }
+            }
+            for (int k = 0; k < nobs; ++k) {
+                const int f = fo[k], o = obPos++;
+                hb.obLm[o] = g;
+                hb.obKf[o] = d.kf0 + w.obs_kf[f];
+                hb.obCam[o] = d.cam0 + w.obs_cam[f];
+                int slot = 0;
+                while (sl[slot] != w.obs_kf[f]) ++slot;
+                hb.obSlot[o] = slot;
+                int xs = 0;
+                if (d.estExt) {
+                    const int x = w.cam_ext[w.obs_cam[f]];
+                    while (sl[nkf[l] + xs] != x) ++xs;
+                }
+                hb.obXslot[o] = xs;
+                for (int k2 = 0; k2 < 3; ++k2) {
+                    hb.obBearing[3ll * o + k2] = w.obs_bearing[3 * f + k2];
+                    hb.obVel[3ll * o + k2] = w.obs_velocity ? w.obs_velocity[3 * f + k2] : 0.0;
+                }
+                for (int k2 = 0; k2 < 6; ++k2) hb.obP[6ll * o + k2] = w.obs_P[6 * f + k2];
+                hb.obTime[o] = w.obs_time ? w.obs_time[f] : 0.0;
+            }
+        }
+        if (L) {
+            P.tiles.back().y = d.lm0 + L;
+            P.runs.back().z = (int)P.tiles.size();
+        }
+        // key order (anchor kf, observer kf, anchor ext, observer ext) of the J^T J pass
+        const int F = d.F;
+        auto keyOf = [&](int o) {
+            const int g = hb.obLm[o];
+            const int a = hb.lmKf[g] - d.kf0, bkf = hb.obKf[o] - d.kf0;
+            const int ea = hb.camExt[hb.lmCam[g]] - d.ext0, eb = hb.camExt[hb.obCam[o]] - d.ext0;
+            return ((long long)(a * d.K + bkf) * d.E + ea) * d.E + eb;
+        };
+        const long long buckets = (long long)d.K * d.K * d.E * d.E;
+        int* ko = F ? &hb.keyOrder[d.obs0] : nullptr;
+        if (buckets <= 4ll * F + 4096) {
+            std::vector<int> cnt(buckets + 1, 0);
+            for (int g = 0; g < F; ++g) ++cnt[keyOf(d.obs0 + g) + 1];
+            for (long long k = 0; k < buckets; ++k) cnt[k + 1] += cnt[k];
+            for (int g = 0; g < F; ++g) ko[cnt[keyOf(d.obs0 + g)]++] = d.obs0 + g;
+        } else {
+            std::vector<std::pair<long long, int>> kv(F);
+            for (int g = 0; g < F; ++g) kv[g] = {keyOf(d.obs0 + g), d.obs0 + g};
+            std::sort(kv.begin(), kv.end());
+            for (int g = 0; g < F; ++g) ko[g] = kv[g].second;
+        }
+        for (int c0 = 0; c0 < F; c0 += 32)
+            P.pairChunks.push_back(make_int4(i, d.obs0 + c0, d.obs0 + std::min(F, c0 + 32), 0));
+        const int rows = schurRowsPerChunk(d.Npc);
+        for (int l0 = 0; l0 < L; l0 += rows) P.schurChunks.push_back(make_int4(i, d.lm0 + l0, d.lm0 + std::min(L, l0 + rows), 0));
+    });
+    for (int i = 0; i < count; ++i)
+        if (part[i].status != CGMLI_OK) {
+            char buf[256];
+            std::snprintf(buf, sizeof buf, "window %d: %s", i, part[i].why.c_str());
+            why = buf;
+            return part[i].status;
+        }
+    // ---- phase 2: prefix sums and fix-ups
+    std::vector<long long> suppBase(count + 1, 0), crossBase(count + 1, 0);
+    std::vector<int> tileBase(count + 1, 0), runBase(count + 1, 0), pairBase(count + 1, 0), schurBase(count + 1, 0);
+    for (int i = 0; i < count; ++i) {
+        suppBase[i + 1] = suppBase[i] + (long long)part[i].supp.size();
+        crossBase[i + 1] = crossBase[i] + part[i].cross;
+        tileBase[i + 1] = tileBase[i] + (int)part[i].tiles.size();
+        runBase[i + 1] = runBase[i] + (int)part[i].runs.size();
+        pairBase[i + 1] = pairBase[i] + (int)part[i].pairChunks.size();
+        schurBase[i + 1] = schurBase[i] + (int)part[i].schurChunks.size();
+        hb.maxNs = std::max(hb.maxNs, part[i].maxNs);
+    }
+    hb.cross = crossBase[count];
+    hb.supp.resize(suppBase[count]);
+    hb.tiles.resize(tileBase[count]);
+    hb.runs.resize(runBase[count]);
+    hb.pairChunks.resize(pairBase[count]);
+    hb.schurChunks.resize(schurBase[count]);
+    parallelFor(count, threads, [&](int i) {
+        const WinDesc& d = hb.win[i];
+        WindowPart& P = part[i];
+        std::copy(P.supp.begin(), P.supp.end(), hb.supp.begin() + suppBase[i]);
+        for (int q = 0; q < d.L; ++q) {
+            hb.lmSupp0[d.lm0 + q] += (int)suppBase[i];
+            hb.lmC0[d.lm0 + q] += crossBase[i];
+        }
+        std::copy(P.tiles.begin(), P.tiles.end(), hb.tiles.begin() + tileBase[i]);
+        for (size_t r = 0; r < P.runs.size(); ++r) {
+            int4 run = P.runs[r];
+            run.y += tileBase[i];
+            run.z += tileBase[i];
+            hb.runs[runBase[i] + r] = run;
+        }
+        std::copy(P.pairChunks.begin(), P.pairChunks.end(), hb.pairChunks.begin() + pairBase[i]);
+        std::copy(P.schurChunks.begin(), P.schurChunks.end(), hb.schurChunks.begin() + schurBase[i]);
+    });
+    return CGMLI_OK;
+}
+
+int checkHostBatch(const cgmli_window* windows, int count, const HostBatch& hb, std::string& why) {
+    char buf[256];
+    auto bad = [&](int i, const char* what) {
+        std::snprintf(buf, sizeof buf, "window %d: %s", i, what);
+        why = buf;
+        return CGMLI_E_INVALID;
+    };
+    for (int i = 0; i < count; ++i) {
+        const auto& w = windows[i];
+        const WinDesc& d = hb.win[i];
+        // lmPerm is a permutation of the window's landmarks, the observation ranges
+        // partition the window's observations and follow the caller's landmarks
+        std::vector<char> seen(d.L, 0);
+        for (int q = 0; q < d.L; ++q) {
+            const int g = d.lm0 + q, l = hb.lmPerm[g];
+            if (l < 0 || l >= d.L || seen[l]) return bad(i, "landmark order is not a permutation");
+            seen[l] = 1;
+            if (hb.lmObsBegin[g + 1] - hb.lmObsBegin[g] != w.lm_obs_begin[l + 1] - w.lm_obs_begin[l])
+                return bad(i, "observation range of a landmark changed size");
+            if (hb.lmKf[g] != d.kf0 + w.lm_anchor_kf[l]) return bad(i, "anchor keyframe");
+            for (int o = hb.lmObsBegin[g]; o < hb.lmObsBegin[g + 1]; ++o) {
+                if (hb.obLm[o] != g) return bad(i, "observation -> landmark map");
+                if (o > hb.lmObsBegin[g] && hb.obKf[o - 1] > hb.obKf[o]) return bad(i, "observations not sorted by keyframe");
+                const int* sl = &hb.supp[hb.lmSupp0[g]];
+                if (d.kf0 + sl[hb.obSlot[o]] != hb.obKf[o]) return bad(i, "observation slot");
+                if (d.estExt && d.ext0 + sl[hb.lmNs[g] + hb.obXslot[o]] != hb.camExt[hb.obCam[o]]) return bad(i, "extrinsic slot");
+            }
+            if (q > 0 && hb.lmNs[g] + hb.lmNx[g] < hb.lmNs[g - 1] + hb.lmNx[g - 1]) return bad(i, "landmarks not sorted by support");
+        }
+        if (d.L && (hb.lmObsBegin[d.lm0] != d.obs0 || hb.lmObsBegin[d.lm0 + d.L] != d.obs0 + d.F))
+            return bad(i, "observation ranges do not cover the window");
+        // key order: a permutation of the window's observations, keys non-decreasing
+        std::vector<char> oseen(d.F, 0);
+        long long prev = -1;
+        for (int k = 0; k < d.F; ++k) {
+            const int o = hb.keyOrder[d.obs0 + k];
+            if (o < d.obs0 || o >= d.obs0 + d.F || oseen[o - d.obs0]) return bad(i, "key order is not a permutation");
+            oseen[o - d.obs0] = 1;
+            const int g = hb.obLm[o];
+            const long long key = ((long long)((hb.lmKf[g] - d.kf0) * d.K + hb.obKf[o] - d.kf0) * d.E +
+                                   (hb.camExt[hb.lmCam[g]] - d.ext0)) * d.E + (hb.camExt[hb.obCam[o]] - d.ext0);
+            if (key < prev) return bad(i, "key order not sorted");
+            prev = key;
+        }
+    }
+    // work units cover every landmark / observation exactly once, within one window
+    std::vector<int> lmCover(hb.totalLm, 0);
+    for (const int4& r : hb.runs)
+        for (int t = r.y; t < r.z; ++t) {
+            const int2 tile = hb.tiles[t];
+            const WinDesc& d = hb.win[r.x];
+            if (tile.x < d.lm0 || tile.y > d.lm0 + d.L || tile.x >= tile.y) return bad(r.x, "tile outside its window");
+            if (hb.lmObsBegin[tile.y] - hb.lmObsBegin[tile.x] > kMaxTrackChunk) return bad(r.x, "tile above 32 observations");
+            for (int g = tile.x; g < tile.y; ++g) ++lmCover[g];
+        }
+    for (int g = 0; g < hb.totalLm; ++g)
+        if (lmCover[g] != 1) return bad(-1, "runs do not cover every landmark once");
+    std::vector<int> obCover(hb.totalObs, 0);
+    for (const int4& c : hb.pairChunks) {
+        const WinDesc& d = hb.win[c.x];
+        if (c.y < d.obs0 || c.z > d.obs0 + d.F || c.z - c.y > 32 || c.y >= c.z) return bad(c.x, "pair chunk");
+        for (int k = c.y; k < c.z; ++k) ++obCover[k];
+    }
+    for (int o = 0; o < hb.totalObs; ++o)
+        if (obCover[o] != 1) return bad(-1, "pair chunks do not cover every observation once");
+    std::vector<int> schCover(hb.totalLm, 0);
+    for (const int4& c : hb.schurChunks) {
+        const WinDesc& d = hb.win[c.x];
+        if (c.y < d.lm0 || c.z > d.lm0 + d.L || c.z - c.y > schurRowsPerChunk(d.Npc)) return bad(c.x, "Schur chunk");
+        for (int g = c.y; g < c.z; ++g) ++schCover[g];
+    }
+    for (int g = 0; g < hb.totalLm; ++g)
+        if (schCover[g] != 1) return bad(-1, "Schur chunks do not cover every landmark once");
+    return CGMLI_OK;
+}
+
+}  // namespace cgmli

@@ -1,0 +1,98 @@
+// Host-side device layout of a batch of windows (no CUDA calls).
+//
+// buildHostBatch turns the caller's windows into the concatenated arrays the
+// kernels read: landmarks reordered by support, observations of a landmark
+// sorted by observer keyframe, the key order of the J^T J pass, the warp work
+// units (runs of tiles, pair chunks, Schur chunks) and the per-window
+// descriptors.  Windows are independent, so the build runs on host threads in
+// parallel; every array position is known from the windows' sizes except the
+// support lists and cross-vector offsets, which are fixed up after a prefix sum.
+#pragma once
+#include <cuda_runtime.h>  // int2 / int4
+
+#include <cstdlib>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/cgmli_backend.h"
+#include "backend_internal.h"
+
+namespace cgmli {
+
+// Page-locked host memory for the arrays uploaded to (and read back from) the
+// device, so that the copies run at DMA speed; plain memory where no CUDA
+// device is present (the host-only diagnostic path).  Elements are
+// default-initialized: every position is written by the builder, and a batch
+// of the same size reuses the capacity without touching it first.
+void* pinnedAllocate(size_t bytes);
+void pinnedFree(void* p);
+template <class T>
+struct PinnedAllocator {
+    using value_type = T;
+    PinnedAllocator() = default;
+    template <class U>
+    PinnedAllocator(const PinnedAllocator<U>&) {}
+    T* allocate(size_t n) {
+        void* p = pinnedAllocate(n * sizeof(T));
+        if (!p) throw std::bad_alloc();
+        return static_cast<T*>(p);
+    }
+    void deallocate(T* p, size_t) { pinnedFree(p); }
+    template <class U>
+    void construct(U* p) { ::new ((void*)p) U; }
+    template <class U, class... A>
+    void construct(U* p, A&&... a) { ::new ((void*)p) U(static_cast<A&&>(a)...); }
+    template <class U>
+    bool operator==(const PinnedAllocator<U>&) const { return true; }
+    template <class U>
+    bool operator!=(const PinnedAllocator<U>&) const { return false; }
+};
+template <class T>
+using HVec = std::vector<T, PinnedAllocator<T>>;
+
+struct HostBatch {
+    std::vector<WinDesc> win;
+    HVec<int4> runs;         // {window, first tile, end tile, -}
+    HVec<int2> tiles;        // {first landmark, end landmark}
+    HVec<int4> pairChunks;   // {window, first key-ordered position, end, -}
+    HVec<int4> schurChunks;  // {window, first landmark, end landmark, -}
+    HVec<int> lmPerm;        // device landmark -> landmark index within its window
+    // cameras
+    HVec<double> camR, camT;
+    HVec<int> camExt;        // global extrinsic of each global camera
+    // landmarks (device order)
+    HVec<int> lmKf, lmCam, lmObsBegin, lmNs, lmNx, lmSupp0, supp;
+    HVec<long long> lmC0;
+    HVec<double> lmBearing, lmVel, lmTime;
+    // observations (device order)
+    HVec<int> obKf, obCam, obSlot, obXslot, obLm, keyOrder;
+    HVec<double> obBearing, obP, obVel, obTime;
+    // states
+    HVec<double> pose, sb, ext, td, rho;
+    // IMU and priors
+    HVec<double> imu;
+    HVec<int> imuKf;
+    HVec<int> priorKind, priorIndex, priorCol, priorOff;
+    HVec<double> priorA, priorR0, priorRef;
+    // totals
+    int totalKf = 0, totalExt = 0, totalCam = 0, totalLm = 0, totalObs = 0, totalImu = 0;
+    int maxNpc = 0, maxNr = 0, maxNs = 1;
+    long long vec = 0, dense = 0, acc = 0, sch = 0, imuScratch = 0, priorScratch = 0, cross = 0;
+};
+
+// Structural checks of one window (sizes, index ranges, limits).  Returns a
+// CGMLI_* code and the reason.
+int validateWindow(const cgmli_window& w, int index, std::string& why);
+
+// Builds the batch with up to `threads` host threads (0: hardware concurrency).
+// Returns a CGMLI_* code and the reason.
+int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatch& out, std::string& why);
+
+// Invariants of a built batch (used by the diagnostic entry point and tests).
+int checkHostBatch(const cgmli_window* windows, int count, const HostBatch& hb, std::string& why);
+
+// Schur chunk rows of a window with Npc visual columns (defined with the kernels).
+int schurRowsPerChunk(int Npc);
+
+}  // namespace cgmli

@@ -135,6 +135,18 @@ const char *cgmli_last_error(void);
 
 void cgmli_default_options(cgmli_solver_options *options);
 
+/* Host-only check of a batch: builds the device layout of the windows on up to
+ * `threads` host threads (0: all) without touching a CUDA device, and verifies
+ * its invariants (the landmark order is a permutation of each window's
+ * landmarks, observation ranges and slots match the caller's data, the key
+ * order of the J^T J pass is sorted, every work unit stays in its window and
+ * covers each landmark / observation once).  Returns the windows' validation
+ * code, or CGMLI_E_INVALID naming the failed invariant; *seconds (may be NULL)
+ * receives the build time.  A diagnostic of this library for callers that
+ * prepare windows on machines without a GPU; it has no counterpart in the
+ * reference. */
+int cgmli_topology_check(const cgmli_window *windows, int count, int threads, double *seconds);
+
 /* Replaces VisualCudaWorkspace construction (src/backend/BackendOptimizer.cpp:334-341). */
 int cgmli_solver_create(int device, const cgmli_solver_options *options, cgmli_solver **out);
 void cgmli_solver_destroy(cgmli_solver *solver);

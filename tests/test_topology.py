@@ -1,0 +1,75 @@
+"""Host-side batch layout on CPU (no GPU): cgmli_topology_check builds the
+device layout of a batch of windows and verifies its invariants - landmark
+order is a permutation, observation ranges and keyframe/extrinsic slots match
+the caller's data, the key order of the J^T J pass is sorted, and every work
+unit (runs of tiles, pair chunks, Schur chunks) stays inside its window and
+covers each landmark / observation exactly once."""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import replace
+
+import pytest
+
+from cgmli_slam_b200 import abi, synth
+from cgmli_slam_b200.build import build_backend
+
+
+@pytest.fixture(scope="module")
+def lib():
+    return abi.declare_backend(C.CDLL(str(build_backend())))
+
+
+def check(lib, windows, threads=0):
+    arr = synth.window_array(windows)
+    sec = C.c_double()
+    code = lib.cgmli_topology_check(arr, len(arr), threads, C.byref(sec))
+    return code, sec.value, lib.cgmli_last_error().decode()
+
+
+SPECS = {
+    "c1": synth.C1,
+    "c2": synth.C2,
+    "shared_calib_td": replace(synth.C1, landmarks=400, estimate_extrinsics=True, estimate_td=True, with_velocity=True,
+                               with_prior=True),
+    "no_imu": replace(synth.C1, keyframes=6, landmarks=300, with_imu=False),
+    "imu_only": replace(synth.C1, keyframes=5, landmarks=0, with_prior=True),
+    "long_tracks_8cam": replace(synth.C3, keyframes=12, landmarks=1500),
+}
+
+
+@pytest.mark.parametrize("name", list(SPECS))
+def test_single_window_layout(lib, name):
+    code, _, why = check(lib, [synth.SynthWindow(SPECS[name], 3)])
+    assert code == 0, why
+
+
+@pytest.mark.parametrize("threads", [1, 4, 0])
+def test_batched_layout_any_thread_count(lib, threads):
+    windows = synth.make_windows("c4", 24, seed=5)
+    code, sec, why = check(lib, windows, threads)
+    assert code == 0, why
+    assert sec > 0
+
+
+def test_large_window_layout(lib):
+    code, _, why = check(lib, [synth.SynthWindow(replace(synth.C3, landmarks=6000), 2)])
+    assert code == 0, why
+
+
+def test_malformed_window_is_rejected(lib):
+    w = synth.SynthWindow(replace(synth.C1, keyframes=4, landmarks=60), 9)
+    arr = synth.window_array([w])
+    arr[0].num_keyframes = 2  # observations now reference missing keyframes
+    code = lib.cgmli_topology_check(arr, 1, 0, None)
+    assert code == 1
+    assert b"window 0" in lib.cgmli_last_error()
+
+
+def test_window_above_visual_limit_is_rejected(lib):
+    w = synth.SynthWindow(replace(synth.C1, keyframes=4, landmarks=60), 9)
+    arr = synth.window_array([w])
+    arr[0].num_extrinsics = 80  # 6K + 6E + 1 > 400 with per-camera extrinsics estimated
+    arr[0].estimate_extrinsics = 1
+    code = lib.cgmli_topology_check(arr, 1, 0, None)
+    assert code == 9  # CGMLI_E_LIMIT
