@@ -19,6 +19,7 @@ PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 PRIOR_POSE, PRIOR_SPEED_BIAS, PRIOR_EXTRINSIC, PRIOR_TIME_OFFSET = 0, 1, 2, 3
 MARGIN_OLD, MARGIN_SECOND_NEW = 0, 1
+MARG_EIGEN_NOALLOC_MAX_N = 256  # CGMLI_MARG_EIGEN_NOALLOC_MAX_N
 
 
 class FrozenImu(C.Structure):
@@ -109,6 +110,7 @@ def declare_backend(lib: C.CDLL) -> C.CDLL:
     _proto(lib, "cgmli_marg_psd_solve", C.c_int,
            [c_double_p, c_double_p, C.c_int, C.c_int, C.c_double, C.c_double, c_double_p])
     _proto(lib, "cgmli_marg_subtract", C.c_int, [c_double_p, c_double_p, C.c_int, C.c_int, c_double_p, c_double_p])
+    _proto(lib, "cgmli_marg_eigen_noalloc", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p])
     return lib
 
 
@@ -129,6 +131,7 @@ BACKEND_SYMBOLS = [
     "cgmli_solver_read_reduced", "cgmli_solver_window_dims", "cgmli_solver_last_timing", "cgmli_solver_marginalize",
     "cgmli_solver_read_prior", "cgmli_marg_eigen", "cgmli_marg_psd_solve", "cgmli_marg_subtract",
     "cgmli_solver_checkpoint", "cgmli_solver_rollback", "cgmli_solver_kernel_times", "cgmli_topology_check",
+    "cgmli_marg_eigen_noalloc",
 ]
 KERNEL_NAMES = ["zero_acc", "linearize", "retained", "factor", "candidate", "backsub_trial", "retained_trial", "lm_update", "accept",
                 "lin_pairs", "lin_schur"]

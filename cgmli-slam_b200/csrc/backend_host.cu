@@ -41,6 +41,10 @@ void launchDenseSubtract(const double* coupling, const double* solution, int nm,
 
 using namespace cgmli;
 
+namespace cgmli {
+int setLastError(int code, const char* message);
+}
+
 namespace {
 thread_local std::string g_error = "ok";
 
@@ -862,3 +866,6 @@ int cgmli_marg_subtract(const double* coupling, const double* solution, int nm, 
 }
 
 }  // extern "C"
+
+// Message of a failure reported by another translation unit of the library.
+int cgmli::setLastError(int code, const char* message) { return fail(code, message); }

@@ -228,6 +228,23 @@ int cgmli_marg_psd_solve(const double *H, const double *rhs, int n, int columns,
 int cgmli_marg_subtract(const double *coupling, const double *solution, int eliminated, int retained,
                         double *H, double *g);
 
+/* Allocation-free form of cgmli_marg_eigen, for callers that must not
+ * allocate device memory: a process whose GPU also runs latency-critical work
+ * (cudaFree synchronizes the whole device), or whose device memory is owned by
+ * another allocator.  This entry point has no counterpart in the reference.
+ * H (n x n, column-major, lower triangle read), eigenvalues (n, ascending) and
+ * eigenvectors (n x n, column-major) are DEVICE pointers owned by the caller;
+ * stream is a cudaStream_t (NULL: the default stream), synchronized before
+ * returning.  The solver's work arrays live in one fixed device array of about
+ * 1 MiB that every GPU loading the library holds until the process exits, so
+ * n is limited to CGMLI_MARG_EIGEN_NOALLOC_MAX_N (larger n: CGMLI_E_LIMIT).
+ * The first call on a device looks the array's address up (set-up); make that
+ * first call before any stream capture.  All calls share the array: calls
+ * that overlap on the GPU (other host threads or streams) race and must be
+ * serialized by the caller. */
+#define CGMLI_MARG_EIGEN_NOALLOC_MAX_N 256
+int cgmli_marg_eigen_noalloc(const double *H, int n, double *eigenvalues, double *eigenvectors, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
