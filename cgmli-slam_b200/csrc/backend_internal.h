@@ -21,7 +21,6 @@ constexpr int kMaxTrackChunk = 32;     // factors per warp pass
 constexpr int kMaxSupport = 64;        // keyframe slots per landmark
 constexpr int kLinThreads = 256;       // linearization CTA
 constexpr int kFactorThreads = 512;    // factorization CTA
-constexpr int kSmemPackedMax = 232;    // Nr up to which the packed factor fits in shared memory
 
 struct WinDesc {
     int K, E, C, L, F, nImu;
@@ -79,7 +78,7 @@ struct DevBatch {
     double* sch;     // Schur term sum_l c_l c_l^T / dt_l (packed upper)
     double* dr;      // state increments (Nr per window)
     double* rhs;
-    double* Sglob;   // factor scratch when Nr exceeds the shared-memory limit
+    double* Sglob;   // damped reduced system and its Cholesky factor (Nr x Nr column-major, lower)
     double* imuScratch; double* priorScratch;
     double* predState;
     int* solveStatus;

@@ -518,50 +518,127 @@ __global__ void __launch_bounds__(256) k_retained(DevBatch B, int trial) {
 // Damped reduced system, FP64 Cholesky and solve (prepareStateSolve + potrf +
 // potrs + clampStateStep + statePrediction, VisualCudaBatch.cu:163-189,564-580).
 //   S = H_ret + S_visual + lambda * max(diag(H_total), 1e-6),  rhs = -(g_r - B_v)
-// The factor is kept packed lower/column-major in shared memory when it fits.
-__device__ __forceinline__ double assembleEntry(const DevBatch& B, const WinDesc& wd, int i, int j, double lambda, bool damp) {
+
+// Blocked right-looking Cholesky of one window per CTA.  The damped system is
+// assembled into the window's slot of Sglob (n x n column-major, lower
+// triangle; L2-resident), factored panel by panel: a panel of kPanel columns
+// is staged in shared memory and factored there, then the trailing lower
+// triangle is updated with 4x4 register tiles (A22 -= L21 L21^T).  The
+// triangular solves proceed by the same panels, with each 16x16 diagonal
+// block in shared memory.
+constexpr int kPanel = 16;
+
+// Entry (i, j) of the damped (or undamped) reduced system, reading the
+// symmetric H_ret along the column j so that consecutive i are coalesced.
+__device__ __forceinline__ double assembleEntryCol(const DevBatch& B, const WinDesc& wd, int i, int j, double lambda, bool damp) {
     const int Nr = wd.Nr, Npc = wd.Npc, K = wd.K;
-    const double* H = B.Hret + wd.dense0;
     const double* JJ = B.acc + wd.acc0;
     const double* sch = B.sch + wd.sch0;
-    double v = H[(long long)i * Nr + j];
+    double v = B.Hret[wd.dense0 + (long long)j * Nr + i];
     const int pi = pcOfRetained(i, K), pj = pcOfRetained(j, K);
     if (pi >= 0 && pj >= 0) {
         const long long e = pi <= pj ? upIdx(pi, pj, Npc) : upIdx(pj, pi, Npc);
         v += JJ[e] - sch[e];
     }
     if (damp && i == j) {
-        double h = H[(long long)i * Nr + i];
+        double h = B.Hret[wd.dense0 + (long long)i * Nr + i];
         if (pi >= 0) h += JJ[upIdx(pi, pi, Npc)];
         v += lambda * fmax(h, 1e-6);
     }
     return v;
 }
 
+// (a, b) with b <= a from the column-by-column enumeration of the lower
+// triangle of an m x m tile grid (index of (a, b) = b m - b (b - 1) / 2 + a - b).
+__device__ __forceinline__ void lowerTile(int t, int m, int& a, int& b) {
+    b = (int)((2.0f * m + 1 - sqrtf((2.0f * m + 1) * (2.0f * m + 1) - 8.0f * t)) * 0.5f);
+    if (b < 0) b = 0;
+    while (b > 0 && b * m - b * (b - 1) / 2 > t) --b;
+    while ((b + 1) * m - (b + 1) * b / 2 <= t) ++b;
+    a = b + (t - (b * m - b * (b - 1) / 2));
+}
+
+// Solves L y = v (forward) then L^T z = y (backward) in place; L lower,
+// column-major with leading dimension n, in global memory.
+__device__ void blockedSolve(const double* L, int n, double* v, double* blk) {
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+    for (int k0 = 0; k0 < n; k0 += kPanel) {
+        const int bw = min(kPanel, n - k0);
+        for (int t = tid; t < bw * bw; t += blockDim.x) {
+            const int c = t / bw, r = t % bw;
+            blk[r + c * kPanel] = r >= c ? L[(k0 + r) + (long long)(k0 + c) * n] : 0.0;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            for (int c = 0; c < bw; ++c) {
+                const double yc = v[k0 + c] / blk[c + c * kPanel];
+                __syncwarp();
+                if (lane == 0) v[k0 + c] = yc;
+                if (lane > c && lane < bw) v[k0 + lane] -= blk[lane + c * kPanel] * yc;
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        for (int r = k0 + bw + tid; r < n; r += blockDim.x) {
+            double s = 0;
+            for (int c = 0; c < bw; ++c) s += L[r + (long long)(k0 + c) * n] * v[k0 + c];
+            v[r] -= s;
+        }
+        __syncthreads();
+    }
+    for (int k0 = ((n - 1) / kPanel) * kPanel; k0 >= 0; k0 -= kPanel) {
+        const int bw = min(kPanel, n - k0);
+        // v[k0 + c] -= sum_{r >= k0 + bw} L[r, k0 + c] v[r]
+        for (int c = warp; c < bw; c += nw) {
+            double s = 0;
+            for (int r = k0 + bw + lane; r < n; r += 32) s += L[r + (long long)(k0 + c) * n] * v[r];
+            s = warpSum(s);
+            if (lane == 0) v[k0 + c] -= s;
+        }
+        for (int t = tid; t < bw * bw; t += blockDim.x) {
+            const int c = t / bw, r = t % bw;
+            blk[r + c * kPanel] = r >= c ? L[(k0 + r) + (long long)(k0 + c) * n] : 0.0;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            for (int c = bw - 1; c >= 0; --c) {
+                double s = (lane > c && lane < bw) ? blk[lane + c * kPanel] * v[k0 + lane] : 0.0;
+                s = warpSum(s);
+                if (lane == 0) v[k0 + c] = (v[k0 + c] - s) / blk[c + c * kPanel];
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void __launch_bounds__(kFactorThreads) k_factor(DevBatch B, int refinement, double* Sdebug) {
     const int wdx = blockIdx.x;
     if (B.lm[wdx].mode == kModeDone) return;
     const WinDesc wd = B.win[wdx];
-    const int Nr = wd.Nr, Npc = wd.Npc, K = wd.K;
+    const int n = wd.Nr, Npc = wd.Npc, K = wd.K;
     const double lambda = B.lm[wdx].lambda;
     extern __shared__ double smem[];
+    double* x = smem;                        // n: right-hand side, then the increment
+    double* blk = smem + n;                  // kPanel x kPanel diagonal block of the solves
+    double* P = blk + kPanel * kPanel;       // panel: n rows x kPanel, column-major, leading dim m
     __shared__ int failed;
     __shared__ double red[32];
-    const bool inSmem = Nr <= kSmemPackedMax;
-    double* L = inSmem ? smem : B.Sglob + wd.dense0;
-    double* x = (inSmem ? smem : B.Sglob + wd.dense0) + (long long)Nr * (Nr + 1) / 2;  // working vector
+    double* A = B.Sglob + wd.dense0;
     const double* acc = B.acc + wd.acc0;
     const long long nS = (long long)Npc * (Npc + 1) / 2;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    if (threadIdx.x == 0) failed = 0;
-    for (int j = warp; j < Nr; j += nw)
-        for (int i = j + lane; i < Nr; i += 32) {
-            const double v = assembleEntry(B, wd, i, j, lambda, true);
-            L[loIdx(i, j, Nr)] = v;
-            if (Sdebug) { Sdebug[wd.dense0 + (long long)i * Nr + j] = v; Sdebug[wd.dense0 + (long long)j * Nr + i] = v; }
-        }
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+    if (tid == 0) failed = 0;
+    // assembly: lower triangle, column-major
+    for (long long t = tid; t < (long long)n * n; t += blockDim.x) {
+        const int j = (int)(t / n), i = (int)(t % n);
+        if (i < j) continue;
+        const double v = assembleEntryCol(B, wd, i, j, lambda, true);
+        A[i + (long long)j * n] = v;
+        if (Sdebug) { Sdebug[wd.dense0 + (long long)i * n + j] = v; Sdebug[wd.dense0 + (long long)j * n + i] = v; }
+    }
     double* rhsOut = B.rhs + wd.vec0;
-    for (int i = threadIdx.x; i < Nr; i += blockDim.x) {
+    for (int i = tid; i < n; i += blockDim.x) {
         double g = B.gret[wd.vec0 + i];
         const int p = pcOfRetained(i, K);
         if (p >= 0) g += acc[nS + Npc + p] - acc[nS + 2ll * Npc + p];
@@ -569,79 +646,113 @@ __global__ void __launch_bounds__(kFactorThreads) k_factor(DevBatch B, int refin
         rhsOut[i] = -g;
     }
     __syncthreads();
-    for (int k = 0; k < Nr; ++k) {
-        if (threadIdx.x == 0) {
-            const double v = L[loIdx(k, k, Nr)];
-            if (!(v > 0) || !isfinite(v)) failed = 1;
-            else L[loIdx(k, k, Nr)] = sqrt(v);
+    for (int k0 = 0; k0 < n; k0 += kPanel) {
+        const int bw = min(kPanel, n - k0), m = n - k0;
+        for (int t = tid; t < m * bw; t += blockDim.x) {
+            const int c = t / m, r = t % m;
+            P[r + c * m] = r >= c ? A[(k0 + r) + (long long)(k0 + c) * n] : 0.0;
         }
         __syncthreads();
+        for (int c = 0; c < bw; ++c) {
+            if (tid == 0) {
+                const double d = P[c + c * m];
+                if (!(d > 0) || !isfinite(d)) failed = 1;
+                else P[c + c * m] = sqrt(d);
+            }
+            __syncthreads();
+            if (failed) break;
+            const double pcc = P[c + c * m];
+            for (int r = c + 1 + tid; r < m; r += blockDim.x) P[r + c * m] /= pcc;
+            __syncthreads();
+            const int rest = bw - c - 1;
+            for (int t = tid; t < rest * m; t += blockDim.x) {
+                const int cc = c + 1 + t / m, r = t % m;
+                if (r >= cc) P[r + cc * m] -= P[r + c * m] * P[cc + c * m];
+            }
+            __syncthreads();
+        }
         if (failed) break;
-        const double lkk = L[loIdx(k, k, Nr)];
-        for (int i = k + 1 + threadIdx.x; i < Nr; i += blockDim.x) L[loIdx(i, k, Nr)] /= lkk;
-        __syncthreads();
-        for (int j = k + 1 + warp; j < Nr; j += nw) {
-            const double ljk = L[loIdx(j, k, Nr)];
-            for (int i = j + lane; i < Nr; i += 32) L[loIdx(i, j, Nr)] -= L[loIdx(i, k, Nr)] * ljk;
+        for (int t = tid; t < m * bw; t += blockDim.x) {
+            const int c = t / m, r = t % m;
+            if (r >= c) A[(k0 + r) + (long long)(k0 + c) * n] = P[r + c * m];
+        }
+        const int m2 = m - bw;
+        if (m2 > 0) {
+            const int g4 = (m2 + 3) / 4, tiles = g4 * (g4 + 1) / 2;
+            for (int t = tid; t < tiles; t += blockDim.x) {
+                int a, b;
+                lowerTile(t, g4, a, b);  // row tile a >= column tile b
+                double accT[4][4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+#pragma unroll
+                    for (int p = 0; p < 4; ++p) accT[q][p] = 0.0;
+                const int r0 = bw + 4 * a, c0 = bw + 4 * b;
+                for (int c = 0; c < bw; ++c) {
+                    double u[4], v[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        u[q] = r0 + q < m ? P[(r0 + q) + c * m] : 0.0;
+                        v[q] = c0 + q < m ? P[(c0 + q) + c * m] : 0.0;
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+#pragma unroll
+                        for (int p = 0; p < 4; ++p) accT[q][p] += u[q] * v[p];
+                }
+#pragma unroll
+                for (int p = 0; p < 4; ++p)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int i = k0 + r0 + q, j = k0 + c0 + p;
+                        if (i < n && j < n && i >= j) A[i + (long long)j * n] -= accT[q][p];
+                    }
+            }
         }
         __syncthreads();
     }
     if (failed) {
-        if (threadIdx.x == 0) B.solveStatus[wdx] = CGMLI_E_NOT_PD;
+        if (tid == 0) B.solveStatus[wdx] = CGMLI_E_NOT_PD;
         return;
     }
-    // solves with one warp: L y = x (column-oriented), L^T z = y (row-oriented)
-    auto solveInPlace = [&](double* v) {
-        if (warp == 0) {
-            for (int k = 0; k < Nr; ++k) {
-                const double yk = v[k] / L[loIdx(k, k, Nr)];
-                __syncwarp();
-                if (lane == 0) v[k] = yk;
-                for (int i = k + 1 + lane; i < Nr; i += 32) v[i] -= L[loIdx(i, k, Nr)] * yk;
-                __syncwarp();
-            }
-            for (int k = Nr - 1; k >= 0; --k) {
-                double s = 0;
-                for (int i = k + 1 + lane; i < Nr; i += 32) s += L[loIdx(i, k, Nr)] * v[i];
-                s = warpSum(s);
-                if (lane == 0) v[k] = (v[k] - s) / L[loIdx(k, k, Nr)];
-                __syncwarp();
-            }
-        }
-        __syncthreads();
-    };
-    solveInPlace(x);
+    blockedSolve(A, n, x, blk);
     double* dr = B.dr + wd.vec0;
-    for (int i = threadIdx.x; i < Nr; i += blockDim.x) dr[i] = x[i];
+    for (int i = tid; i < n; i += blockDim.x) dr[i] = x[i];
     __syncthreads();
     // iterative refinement against the assembled FP64 system
     for (int it = 0; it < refinement; ++it) {
-        for (int i = threadIdx.x; i < Nr; i += blockDim.x) {
-            double g = B.gret[wd.vec0 + i];
-            const int p = pcOfRetained(i, K);
-            if (p >= 0) g += acc[nS + Npc + p] - acc[nS + 2ll * Npc + p];
-            double v = -g;
-            for (int j = 0; j < Nr; ++j) v -= assembleEntry(B, wd, i, j, lambda, true) * dr[j];
-            x[i] = v;
+        for (int i = warp; i < n; i += nw) {
+            double s = 0;
+            for (int j = lane; j < n; j += 32) s += assembleEntryCol(B, wd, j, i, lambda, true) * dr[j];
+            s = warpSum(s);
+            if (lane == 0) {
+                double g = B.gret[wd.vec0 + i];
+                const int p = pcOfRetained(i, K);
+                if (p >= 0) g += acc[nS + Npc + p] - acc[nS + 2ll * Npc + p];
+                x[i] = -g - s;
+            }
         }
         __syncthreads();
-        solveInPlace(x);
-        for (int i = threadIdx.x; i < Nr; i += blockDim.x) dr[i] += x[i];
+        blockedSolve(A, n, x, blk);
+        for (int i = tid; i < n; i += blockDim.x) dr[i] += x[i];
         __syncthreads();
     }
     // predicted reduction of the state part with the undamped (S_visual + H_ret):
     //   -dx^T (g_r + 0.5 (S_v + H_ret) dx); the landmark terms are added per landmark.
     double pred = 0;
-    for (int i = threadIdx.x; i < Nr; i += blockDim.x) {
+    for (int i = warp; i < n; i += nw) {
         double hd = 0;
-        for (int j = 0; j < Nr; ++j) hd += assembleEntry(B, wd, i, j, lambda, false) * dr[j];
-        double g = B.gret[wd.vec0 + i];
-        const int p = pcOfRetained(i, K);
-        if (p >= 0) g += acc[nS + Npc + p];
-        pred += -dr[i] * (g + 0.5 * hd);
+        for (int j = lane; j < n; j += 32) hd += assembleEntryCol(B, wd, j, i, lambda, false) * dr[j];
+        hd = warpSum(hd);
+        if (lane == 0) {
+            double g = B.gret[wd.vec0 + i];
+            const int p = pcOfRetained(i, K);
+            if (p >= 0) g += acc[nS + Npc + p];
+            pred += -dr[i] * (g + 0.5 * hd);
+        }
     }
     pred = blockSum(pred, red);
-    if (threadIdx.x == 0) { B.predState[wdx] = pred; B.solveStatus[wdx] = CGMLI_OK; }
+    if (tid == 0) { B.predState[wdx] = pred; B.solveStatus[wdx] = CGMLI_OK; }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -860,9 +971,8 @@ int schurRowsPerChunk(int Npc) {
     return rows < 128 ? rows : 128;
 }
 size_t factorSmemBytes(int maxNr) {
-    // windows with Nr <= kSmemPackedMax factor in shared memory; larger ones in global memory
-    const size_t n = (size_t)(maxNr < kSmemPackedMax ? maxNr : kSmemPackedMax);
-    return (n * (n + 1) / 2 + n) * sizeof(double);
+    // increment vector, diagonal block of the solves, one panel of kPanel columns
+    return ((size_t)maxNr + kPanel * kPanel + (size_t)maxNr * kPanel) * sizeof(double);
 }
 
 // The dynamic shared-memory cap is a per-function attribute shared by every
