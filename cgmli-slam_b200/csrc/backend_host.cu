@@ -106,7 +106,7 @@ struct cgmli_solver {
     DArray<double> sch;
     DArray<double> camR, camT;
     DArray<int> camExt;
-    DArray<int> lmKf, lmCam, lmObsBegin, lmNs, lmNx, lmSupp0, supp;
+    DArray<int> lmWin, lmKf, lmCam, lmObsBegin, lmNs, lmNx, lmSupp0, supp;
     DArray<long long> lmC0;
     DArray<double> lmBearing, lmVel, lmTime, lmC, lmD, lmG, lmCost, lmDelta, lmPred, lmTrial, lmMaxInc;
     DArray<int> lmValid, lmTrialValid;
@@ -154,7 +154,7 @@ struct cgmli_solver {
     }
     LaunchPlan plan() const {
         LaunchPlan P{};
-        P.runs = dRuns.p; P.tiles = dTiles.p;
+        P.runs = dRuns.p; P.tiles = dTiles.p; P.numTiles = (int)hb.tiles.size();
         P.pairChunks = dPairChunks.p; P.numPairChunks = (int)hb.pairChunks.size();
         P.schurChunks = dSchurChunks.p; P.numSchurChunks = (int)hb.schurChunks.size();
         P.linSmem = linSmem; P.facSmem = facSmem; P.maxNs = maxNs;
@@ -179,7 +179,7 @@ struct cgmli_solver {
                                  &td[0], &td[1], &rho[0], &rho[1], &imu, &priorA, &priorR0, &priorRef, &Hret, &gret, &costRet,
                                  &trialRet, &acc, &dr, &rhs, &Sglob, &imuScratch, &priorScratch, &predState, &out, &Sdebug};
         for (auto* a : dbl) a->release();
-        DArray<int>* ints[] = {&camExt, &lmKf, &lmCam, &lmObsBegin, &lmNs, &lmSupp0, &supp, &lmValid, &lmTrialValid, &obKf,
+        DArray<int>* ints[] = {&camExt, &lmWin, &lmKf, &lmCam, &lmObsBegin, &lmNs, &lmSupp0, &supp, &lmValid, &lmTrialValid, &obKf,
                                &obCam, &obSlot, &imuKf, &priorKind, &priorIndex, &priorCol, &priorOff, &retValid,
                                &solveStatus, &lmNx, &obXslot};
         for (auto* a : ints) a->release();
@@ -288,7 +288,7 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     CK(S->dPairChunks.upload(hb.pairChunks, st));
     CK(S->dSchurChunks.upload(hb.schurChunks, st));
     CK(S->camR.upload(hb.camR, st)); CK(S->camT.upload(hb.camT, st)); CK(S->camExt.upload(hb.camExt, st));
-    CK(S->lmKf.upload(hb.lmKf, st)); CK(S->lmCam.upload(hb.lmCam, st)); CK(S->lmObsBegin.upload(hb.lmObsBegin, st));
+    CK(S->lmWin.upload(hb.lmWin, st)); CK(S->lmKf.upload(hb.lmKf, st)); CK(S->lmCam.upload(hb.lmCam, st)); CK(S->lmObsBegin.upload(hb.lmObsBegin, st));
     CK(S->lmNs.upload(hb.lmNs, st)); CK(S->lmNx.upload(hb.lmNx, st)); CK(S->lmSupp0.upload(hb.lmSupp0, st));
     CK(S->supp.upload(hb.supp, st)); CK(S->lmC0.upload(hb.lmC0, st));
     CK(S->lmBearing.upload(hb.lmBearing, st)); CK(S->lmVel.upload(hb.lmVel, st)); CK(S->lmTime.upload(hb.lmTime, st));
@@ -320,7 +320,7 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     B.numRuns = (int)hb.runs.size();
     B.win = S->dWin.p; B.lm = S->dLm.p;
     B.camR = S->camR.p; B.camT = S->camT.p; B.camExt = S->camExt.p;
-    B.lmKf = S->lmKf.p; B.lmCam = S->lmCam.p; B.lmObsBegin = S->lmObsBegin.p;
+    B.lmWin = S->lmWin.p; B.lmKf = S->lmKf.p; B.lmCam = S->lmCam.p; B.lmObsBegin = S->lmObsBegin.p;
     B.lmBearing = S->lmBearing.p; B.lmVel = S->lmVel.p; B.lmTime = S->lmTime.p;
     B.lmNs = S->lmNs.p; B.lmNx = S->lmNx.p; B.lmSupp0 = S->lmSupp0.p; B.supp = S->supp.p; B.lmC0 = S->lmC0.p;
     B.obXslot = S->obXslot.p;

@@ -54,7 +54,7 @@ struct DevBatch {
     // cameras
     const double* camR; const double* camT; const int* camExt;  // camExt: global extrinsic index
     // landmarks
-    const int* lmKf; const int* lmCam; const int* lmObsBegin;  // lmObsBegin: numLandmarks+1
+    const int* lmWin; const int* lmKf; const int* lmCam; const int* lmObsBegin;  // lmObsBegin: numLandmarks+1
     const double* lmBearing; const double* lmVel; const double* lmTime;
     const int* lmNs; const int* lmNx; const int* lmSupp0; const int* supp;  // support: s keyframes (anchor first), then x extrinsics
     const long long* lmC0;                                // offset of the landmark's cross vector
@@ -130,6 +130,7 @@ typedef void (*LaunchHook)(void* ctx, int kind, int phase);
 struct LaunchPlan {
     const int4* runs;        // {window, first tile, end tile, -}: one warp each (landmark order)
     const int2* tiles;       // {first landmark, end landmark}, <= 32 observations
+    int numTiles;
     const int4* pairChunks;  // {window, first key-ordered index, end, -}: <= 32 observations, one warp each
     int numPairChunks;
     const int4* schurChunks; // {window, first landmark, end landmark, -}: one CTA each

@@ -796,67 +796,80 @@ __global__ void k_candidate(DevBatch B) {
 
 // ---------------------------------------------------------------------------------------
 // Back-substitution of the inverse distances (backSubstitute,
-// VisualCudaBatch.cu:191-205) and the robust cost of the candidate point.
-// Warp per tile; lane = landmark for the back-substitution, lane =
-// observation for the trial residuals.
-__global__ void __launch_bounds__(kLinWarps * 32) k_backsub_trial(DevBatch B, const int4* runs, const int2* tiles) {
+// VisualCudaBatch.cu:191-205): eight lanes per landmark form c_l . dx_r.
+__global__ void __launch_bounds__(256) k_backsub(DevBatch B) {
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int l = gt >> 3, sub = threadIdx.x & 7;
+    const bool inRange = l < B.numLandmarks;
+    const int wdx = inRange ? B.lmWin[l] : 0;
+    const bool active = inRange && B.lm[wdx].mode != kModeDone;
+    double cd = 0;
+    int K = 0, s = 0, x = 0, ns = 0, tdCol = 0;
+    const WinDesc* wd = B.win + wdx;
+    if (active) {
+        K = wd->K;
+        s = B.lmNs[l];
+        x = B.lmNx[l];
+        ns = 6 * (s + x) + (wd->estTd ? 1 : 0);
+        tdCol = 6 * K + (wd->estExt ? 6 * wd->E : 0);
+        const double* c = B.lmC + B.lmC0[l];
+        const int* sk = B.supp + B.lmSupp0[l];
+        const double* dr = B.dr + wd->vec0;
+        for (int i = sub; i < ns; i += 8) cd += c[i] * dr[retainedOfPc(pcOfLocal(i, s, x, sk, K, tdCol), K)];
+    }
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) cd += __shfl_xor_sync(0xffffffffu, cd, o);
+    if (!active || sub != 0) return;
+    const double lambda = B.lm[wdx].lambda;
+    const double d = B.lmD[l], g = B.lmG[l];
+    const double dt = d + lambda * fmax(d, 1e-6);
+    double dl = -(g + cd) / dt;
+    const double rho0 = B.rho[0][l], minInv = wd->minInv;
+    if (isfinite(dl)) dl = fmax(minInv - rho0, dl);
+    B.lmDelta[l] = dl;
+    // landmark terms of -dx^T (g + 0.5 H dx): the cross term c.dx_r is
+    // split between the state part (via S_v) and this correction
+    B.lmPred[l] = -0.5 * cd * cd / dt - dl * (g + cd + 0.5 * d * dl);
+    B.lmMaxInc[l] = isfinite(dl) ? fabs(dl) : -1.0;
+    B.rho[1][l] = fmax(minInv, rho0 + dl);
+}
+
+// Robust cost of the candidate point (launchTrial, VisualCudaBatch.cu:715-721):
+// one warp per tile of <= 32 observations, lane = observation.
+constexpr int kTrialWarps = 8;
+__global__ void __launch_bounds__(kTrialWarps * 32, 2) k_trial(DevBatch B, const int2* tiles, int numTiles) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __shared__ double tcost[kLinWarps][32];
-    __shared__ int tvalid[kLinWarps][32];
-    const int runIdx = blockIdx.x * kLinWarps + warp;
-    if (runIdx >= B.numRuns) return;
-    const int4 run = runs[runIdx];
-    const int wdx = run.x;
+    __shared__ double tcost[kTrialWarps][32];
+    __shared__ int tvalid[kTrialWarps][32];
+    const int t = blockIdx.x * kTrialWarps + warp;
+    if (t >= numTiles) return;
+    const int2 tile = tiles[t];
+    const int lb = tile.x, le = tile.y, nl = le - lb;
+    const int wdx = B.lmWin[lb];
     if (B.lm[wdx].mode == kModeDone) return;
     const WinDesc wd = B.win[wdx];
-    const double lambda = B.lm[wdx].lambda;
-    const int K = wd.K;
-    const double* dr = B.dr + wd.vec0;
-    for (int t = run.y; t < run.z; ++t) {
-        const int2 tile = tiles[t];
-        const int lb = tile.x, le = tile.y, nl = le - lb;
-        if (lane < nl) {
-            const int l = lb + lane;
-            const int s = B.lmNs[l], x = B.lmNx[l], ns = 6 * (s + x) + (wd.estTd ? 1 : 0);
-            const double* c = B.lmC + B.lmC0[l];
-            const int* sk = B.supp + B.lmSupp0[l];
-            const int tdCol = 6 * K + (wd.estExt ? 6 * wd.E : 0);
-            double cd = 0;
-            for (int i = 0; i < ns; ++i) cd += c[i] * dr[retainedOfPc(pcOfLocal(i, s, x, sk, K, tdCol), K)];
-            const double d = B.lmD[l], g = B.lmG[l];
-            const double dt = d + lambda * fmax(d, 1e-6);
-            double dl = -(g + cd) / dt;
-            const double rho0 = B.rho[0][l];
-            if (isfinite(dl)) dl = fmax(wd.minInv - rho0, dl);
-            B.lmDelta[l] = dl;
-            // landmark terms of -dx^T (g + 0.5 H dx): the cross term c.dx_r is
-            // split between the state part (via S_v) and this correction
-            B.lmPred[l] = -0.5 * cd * cd / dt - dl * (g + cd + 0.5 * d * dl);
-            B.lmMaxInc[l] = isfinite(dl) ? fabs(dl) : -1.0;
-            B.rho[1][l] = fmax(wd.minInv, rho0 + dl);
-            tcost[warp][lane] = 0;
-            tvalid[warp][lane] = isfinite(dl) ? 1 : 0;
-        }
-        __syncwarp();
-        const int ob = B.lmObsBegin[lb], oe = B.lmObsBegin[le];
-        const int f = ob + lane;
-        if (f < oe) {
-            int q = 0;
-            while (B.lmObsBegin[lb + q + 1] <= f) ++q;
-            const int l = lb + q;
-            FactorIn in;
-            int kfa, kfb, ea, eb;
-            gatherFactor(B, wd, wdx, l, f, 1, in, kfa, kfb, ea, eb);
-            FactorOut o;
-            if (!evalBearingFactor(in, false, o)) tvalid[warp][q] = 0;
-            else atomicAdd(&tcost[warp][q], huberCost(wd.huber, o.r[0] * o.r[0] + o.r[1] * o.r[1]));
-        }
-        __syncwarp();
-        if (lane < nl) {
-            B.lmTrial[lb + lane] = tcost[warp][lane];
-            B.lmTrialValid[lb + lane] = tvalid[warp][lane];
-        }
-        __syncwarp();
+    if (lane < nl) {
+        tcost[warp][lane] = 0.0;
+        tvalid[warp][lane] = B.lmMaxInc[lb + lane] >= 0.0 ? 1 : 0;  // -1 marks a non-finite step
+    }
+    __syncwarp();
+    const int ob = B.lmObsBegin[lb], oe = B.lmObsBegin[le];
+    const int f = ob + lane;
+    if (f < oe) {
+        int q = 0;
+        while (B.lmObsBegin[lb + q + 1] <= f) ++q;
+        const int l = lb + q;
+        FactorIn in;
+        int kfa, kfb, ea, eb;
+        gatherFactor(B, wd, wdx, l, f, 1, in, kfa, kfb, ea, eb);
+        FactorOut o;
+        if (!evalBearingFactor(in, false, o)) tvalid[warp][q] = 0;
+        else atomicAdd(&tcost[warp][q], huberCost(wd.huber, o.r[0] * o.r[0] + o.r[1] * o.r[1]));
+    }
+    __syncwarp();
+    if (lane < nl) {
+        B.lmTrial[lb + lane] = tcost[warp][lane];
+        B.lmTrialValid[lb + lane] = tvalid[warp][lane];
     }
 }
 
@@ -1023,8 +1036,12 @@ int launchIteration(const DevBatch& B, const LaunchPlan& P, int refinement, int 
     run(CGMLI_KERNEL_RETAINED, [&] { k_retained<<<W, 256, 0, s>>>(B, 0); });
     run(CGMLI_KERNEL_FACTOR, [&] { k_factor<<<W, kFactorThreads, P.facSmem, s>>>(B, refinement, Sdebug); });
     run(CGMLI_KERNEL_CANDIDATE, [&] { k_candidate<<<W, 128, 0, s>>>(B); });
-    if (B.numRuns > 0)
-        run(CGMLI_KERNEL_BACKSUB_TRIAL, [&] { k_backsub_trial<<<runBlocks, kLinWarps * 32, 0, s>>>(B, P.runs, P.tiles); });
+    if (B.numLandmarks > 0) {
+        run(CGMLI_KERNEL_BACKSUB_TRIAL, [&] { k_backsub<<<(B.numLandmarks * 8 + 255) / 256, 256, 0, s>>>(B); });
+        run(CGMLI_KERNEL_BACKSUB_TRIAL, [&] {
+            k_trial<<<(P.numTiles + kTrialWarps - 1) / kTrialWarps, kTrialWarps * 32, 0, s>>>(B, P.tiles, P.numTiles);
+        });
+    }
     run(CGMLI_KERNEL_RETAINED_TRIAL, [&] { k_retained<<<W, 256, 0, s>>>(B, 1); });
     run(CGMLI_KERNEL_LM_UPDATE, [&] { k_lm_update<<<W, 256, 0, s>>>(B, maxIterations, probe); });
     if (!probe) run(CGMLI_KERNEL_ACCEPT, [&] { k_accept<<<W, 256, 0, s>>>(B); });

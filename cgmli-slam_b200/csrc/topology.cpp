@@ -184,7 +184,7 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
     hb.vec = vec; hb.dense = dense; hb.acc = acc; hb.sch = sch; hb.imuScratch = imuS; hb.priorScratch = priS;
     constexpr int kImuDoubles = sizeof(cgmli_frozen_imu) / sizeof(double);
     hb.camR.resize(9ll * cam); hb.camT.resize(3ll * cam); hb.camExt.resize(cam);
-    hb.lmKf.resize(lm); hb.lmCam.resize(lm); hb.lmObsBegin.resize(lm + 1ll); hb.lmNs.resize(lm); hb.lmNx.resize(lm);
+    hb.lmWin.resize(lm); hb.lmKf.resize(lm); hb.lmCam.resize(lm); hb.lmObsBegin.resize(lm + 1ll); hb.lmNs.resize(lm); hb.lmNx.resize(lm);
     hb.lmSupp0.resize(lm); hb.lmC0.resize(lm); hb.lmPerm.resize(lm);
     hb.lmBearing.resize(3ll * lm); hb.lmVel.resize(3ll * lm); hb.lmTime.resize(lm);
     hb.obKf.resize(ob); hb.obCam.resize(ob); hb.obSlot.resize(ob); hb.obXslot.resize(ob); hb.obLm.resize(ob);
@@ -314,6 +314,7 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
             tileObs += nobs;
             ++runLms;
             hb.lmPerm[g] = l;
+            hb.lmWin[g] = i;
             hb.lmKf[g] = d.kf0 + w.lm_anchor_kf[l];
             hb.lmCam[g] = d.cam0 + w.lm_anchor_cam[l];
             hb.lmObsBegin[g] = obPos;

@@ -62,7 +62,7 @@ struct HostBatch {
     HVec<double> camR, camT;
     HVec<int> camExt;        // global extrinsic of each global camera
     // landmarks (device order)
-    HVec<int> lmKf, lmCam, lmObsBegin, lmNs, lmNx, lmSupp0, supp;
+    HVec<int> lmWin, lmKf, lmCam, lmObsBegin, lmNs, lmNx, lmSupp0, supp;
     HVec<long long> lmC0;
     HVec<double> lmBearing, lmVel, lmTime;
     // observations (device order)
