@@ -103,6 +103,7 @@ struct cgmli_solver {
     DArray<int2> dTiles;
     DArray<int4> dPairChunks, dSchurChunks;
     DArray<int> obLm, keyOrder;
+    DArray<double> keyRows;
     DArray<double> sch;
     DArray<double> camR, camT;
     DArray<int> camExt;
@@ -184,7 +185,7 @@ struct cgmli_solver {
                                &solveStatus, &lmNx, &obXslot};
         for (auto* a : ints) a->release();
         lmC0.release(); dWin.release(); dLm.release(); dRuns.release(); dTiles.release();
-        dPairChunks.release(); dSchurChunks.release(); obLm.release(); keyOrder.release(); sch.release();
+        dPairChunks.release(); dSchurChunks.release(); obLm.release(); keyOrder.release(); keyRows.release(); sch.release();
         snapPose.release(); snapSb.release(); snapExt.release(); snapTd.release(); snapRho.release();
         dMargWin.release(); dMargElim.release();
         DArray<int>* mi[] = {&margCols, &margObsMap, &margPoseCol, &margSbCol, &margExtCol, &margRank, &margStatus};
@@ -294,6 +295,7 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     CK(S->lmBearing.upload(hb.lmBearing, st)); CK(S->lmVel.upload(hb.lmVel, st)); CK(S->lmTime.upload(hb.lmTime, st));
     CK(S->obKf.upload(hb.obKf, st)); CK(S->obCam.upload(hb.obCam, st)); CK(S->obSlot.upload(hb.obSlot, st));
     CK(S->obXslot.upload(hb.obXslot, st)); CK(S->obLm.upload(hb.obLm, st)); CK(S->keyOrder.upload(hb.keyOrder, st));
+    CK(S->keyRows.reserve((size_t)hb.totalObs * 56));
     CK(S->obBearing.upload(hb.obBearing, st)); CK(S->obP.upload(hb.obP, st)); CK(S->obVel.upload(hb.obVel, st));
     CK(S->obTime.upload(hb.obTime, st));
     CK(S->pose[0].upload(hb.pose, st)); CK(S->sb[0].upload(hb.sb, st)); CK(S->ext[0].upload(hb.ext, st));
@@ -328,7 +330,7 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     B.lmDelta = S->lmDelta.p; B.lmPred = S->lmPred.p; B.lmTrial = S->lmTrial.p; B.lmMaxInc = S->lmMaxInc.p;
     B.lmTrialValid = S->lmTrialValid.p;
     B.obKf = S->obKf.p; B.obCam = S->obCam.p; B.obSlot = S->obSlot.p;
-    B.obLm = S->obLm.p; B.keyOrder = S->keyOrder.p;
+    B.obLm = S->obLm.p; B.keyOrder = S->keyOrder.p; B.keyRows = S->keyRows.p;
     B.obBearing = S->obBearing.p; B.obP = S->obP.p; B.obVel = S->obVel.p; B.obTime = S->obTime.p;
     for (int k = 0; k < 2; ++k) {
         B.pose[k] = S->pose[k].p; B.sb[k] = S->sb[k].p; B.ext[k] = S->ext[k].p; B.td[k] = S->td[k].p; B.rho[k] = S->rho[k].p;

@@ -64,6 +64,7 @@ struct DevBatch {
     const int* obKf; const int* obCam; const int* obSlot; const int* obXslot;
     const int* obLm;      // landmark (device index) of each observation
     const int* keyOrder;  // observations of each window sorted by (anchor kf, observer kf, anchor ext, observer ext)
+    double* keyRows;      // weighted compact factor rows per observation (k_lin_landmark -> k_lin_pairs)
     const double* obBearing; const double* obP; const double* obVel; const double* obTime;
     // states: [0] accepted, [1] candidate
     double* pose[2]; double* sb[2]; double* ext[2]; double* td[2]; double* rho[2];

@@ -84,7 +84,7 @@ constexpr int kLinWarps = 6;        // warps per CTA of the run-based kernels
 constexpr int kCompact = 25;        // anchor pose 6 | observer pose 6 | ext_a 6 | ext_b 6 | td 1
 constexpr int kPairs = kCompact * (kCompact + 1) / 2;
 constexpr int kPairSlots = (kPairs + 31) / 32;  // compact pairs per lane
-constexpr int kPairWarps = 8;       // warps per CTA of k_lin_pairs
+constexpr int kPairWarps = 4;       // warps per CTA of k_lin_pairs
 constexpr int kSchurThreads = 256;
 constexpr int kSchurSmemDoubles = 12800;  // dense rows of a Schur chunk
 // A factor's FactorOut is staged per lane in shared memory with an odd stride
@@ -109,7 +109,16 @@ __device__ __forceinline__ int pcOfLocal(int i, int s, int x, const int* sk, int
 // 25, 26, 27), the compact -> local column maps, flags, and the landmark's
 // cross vector (maxNs doubles, the batch's widest support).
 __host__ __device__ constexpr size_t landmarkWarpBytes(int maxNs) {
-    return sizeof(double) * (32 * kOut + maxNs) + sizeof(short) * 32 * kCompact + sizeof(int) * 32;
+    return sizeof(double) * (32 * kOut + maxNs) + sizeof(long long) * 32 + sizeof(short) * 32 * kCompact + sizeof(int) * 32;
+}
+// Staged row of one factor, written by k_lin_landmark (in observation order)
+// and gathered in key order by k_lin_pairs:
+// weighted J row 0 over the compact columns [0, 25), row 1 [25, 50), weighted
+// residual 50, 51, the packed key (anchor kf | observer kf << 16 | anchor ext << 32 |
+// observer ext << 48, window-local) at 52; 53..55 pad the row to 448 bytes.
+constexpr int kKeyRow = 56;
+__device__ __forceinline__ long long packKey(int a, int b, int ea, int eb) {
+    return (long long)a | (long long)b << 16 | (long long)ea << 32 | (long long)eb << 48;
 }
 
 __global__ void __launch_bounds__(kLinWarps * 32, 2) k_lin_landmark(DevBatch B, const int4* runs, const int2* tiles, int maxNs) {
@@ -123,7 +132,8 @@ __global__ void __launch_bounds__(kLinWarps * 32, 2) k_lin_landmark(DevBatch B, 
     char* base = reinterpret_cast<char*>(smemRaw) + landmarkWarpBytes(maxNs) * warp;
     double* out = reinterpret_cast<double*>(base);
     double* cvec = out + 32 * kOut;
-    short* map = reinterpret_cast<short*>(cvec + maxNs);
+    long long* keys = reinterpret_cast<long long*>(cvec + maxNs);
+    short* map = reinterpret_cast<short*>(keys + 32);
     int* flags = reinterpret_cast<int*>(map + 32 * kCompact);
     const WinDesc wd = B.win[wdx];
     for (int t = run.y; t < run.z; ++t) {
@@ -152,18 +162,36 @@ __global__ void __launch_bounds__(kLinWarps * 32, 2) k_lin_landmark(DevBatch B, 
             }
             mp[24] = wd.estTd ? 6 * (s + x) : -1;
             flags[lane] = ok ? 1 : 0;
-            if (ok) {
-                const double r0 = st[0], r1 = st[1], p0 = st[52], p1 = st[53];
-                const double sq = r0 * r0 + r1 * r1;
-                const double w = huberWeight(wd.huber, sq), w2 = w * w;
-                const double d = w2 * (p0 * p0 + p1 * p1), g = w2 * (p0 * r0 + p1 * r1), cost = huberCost(wd.huber, sq);
-                // in place: column c reads offsets >= c + 2, all later than slot c
+            keys[lane] = packKey(kfa - wd.kf0, kfb - wd.kf0, ea - wd.ext0, eb - wd.ext0);
+            if (ok) st[54] = huberWeight(wd.huber, st[0] * st[0] + st[1] * st[1]);
+            else for (int k = 0; k < kOut; ++k) st[k] = 0.0;
+        }
+        __syncwarp();
+        // weighted compact row of this lane's observation (unrolled: constant offsets)
+        if (f < oe) {
+            const double* st = out + kOut * lane;
+            const double w = st[54];
+            double2* row = reinterpret_cast<double2*>(B.keyRows + (size_t)f * kKeyRow);
 #pragma unroll
-                for (int c = 0; c < kCompact; ++c) st[c] = w2 * (st[compactOff(0, c)] * p0 + st[compactOff(1, c)] * p1);
-                st[25] = d; st[26] = g; st[27] = cost;
-            } else {
-                for (int c = 0; c < 28; ++c) st[c] = 0.0;
+            for (int q = 0; q < 25; ++q) {
+                const int c0 = 2 * q, c1 = 2 * q + 1;
+                row[q] = make_double2(w * st[c0 < 25 ? compactOff(0, c0) : compactOff(1, c0 - 25)],
+                                      w * st[c1 < 25 ? compactOff(0, c1) : compactOff(1, c1 - 25)]);
             }
+            row[25] = make_double2(w * st[0], w * st[1]);
+            row[26] = make_double2(__longlong_as_double(keys[lane]), 0.0);
+        }
+        __syncwarp();
+        if (f < oe && flags[lane]) {
+            double* st = out + kOut * lane;
+            const double r0 = st[0], r1 = st[1], p0 = st[52], p1 = st[53];
+            const double sq = r0 * r0 + r1 * r1;
+            const double w = st[54], w2 = w * w;
+            const double d = w2 * (p0 * p0 + p1 * p1), g = w2 * (p0 * r0 + p1 * r1), cost = huberCost(wd.huber, sq);
+            // in place: column c reads offsets >= c + 2, all later than slot c
+#pragma unroll
+            for (int c = 0; c < kCompact; ++c) st[c] = w2 * (st[compactOff(0, c)] * p0 + st[compactOff(1, c)] * p1);
+            st[25] = d; st[26] = g; st[27] = cost;
         }
         __syncwarp();
         for (int l = lb; l < le; ++l) {
@@ -199,64 +227,86 @@ __global__ void __launch_bounds__(kLinWarps * 32, 2) k_lin_landmark(DevBatch B, 
 }
 
 // ---- L2: J^T J and J^T r by observation key ------------------------------------------
-// Work unit: a chunk of <= 32 observations of one window in key order; lane =
-// observation for the evaluation, then every lane owns fixed compact pairs
-// (a <= b) whose products it sums over each run of equal keys in registers.
-__host__ __device__ constexpr size_t pairCtaBytes() { return sizeof(double) * kPairWarps * 32 * kOut; }
+// Work unit: a chunk of <= 32 consecutive positions of one window's key order.
+// The warp gathers the chunk's staged rows (written by k_lin_landmark) into
+// shared memory.  For each run of equal keys the Gram matrix G = J'^T J' of the
+// run's weighted rows is formed on the FP64 tensor path (mma.sync m8n8k4):
+// J' is the 2x25 compact Jacobian of each observation with the weighted
+// residual appended as column 25 and zero-padded to 32 columns, so that G's
+// upper 25x25 block is J^T J and G[i][25] = (J^T r)_i.  One k-step of 4 rows
+// covers two observations; the ten upper 8x8 tiles of the 32x32 G live in
+// registers (two doubles per lane each) and are added to the window once per run.
+constexpr int kPairStride = kKeyRow + 1;  // odd stride
+__host__ __device__ constexpr size_t pairCtaBytes() { return sizeof(double) * kPairWarps * 32 * kPairStride; }
 
-__global__ void __launch_bounds__(kPairWarps * 32, 2) k_lin_pairs(DevBatch B, const int4* chunks, int numChunks) {
+__device__ __forceinline__ void mmaF64(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(kPairWarps * 32) k_lin_pairs(DevBatch B, const int4* chunks, int numChunks) {
     extern __shared__ double smemRaw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ci = blockIdx.x * kPairWarps + warp;
     if (ci >= numChunks) return;
-    const int4 ch = chunks[ci];  // {window, first sorted index, end, -}
+    const int4 ch = chunks[ci];  // {window, first key-ordered position, end, -}
     const int wdx = ch.x;
     if (B.lm[wdx].mode != kModeLinearize) return;
-    double* out = smemRaw + (size_t)warp * 32 * kOut;
+    double* rows = smemRaw + (size_t)warp * 32 * kPairStride;
     const WinDesc wd = B.win[wdx];
     const int n = ch.z - ch.y;
-    int kfa = -1, kfb = -1, ea = -1, eb = -1;
-    if (lane < n) {
-        const int f = B.keyOrder[ch.y + lane];
-        const int l = B.obLm[f];
-        FactorIn in;
-        gatherFactor(B, wd, wdx, l, f, 0, in, kfa, kfb, ea, eb);
-        double* st = out + kOut * lane;
-        if (evalBearingFactor(in, true, *reinterpret_cast<FactorOut*>(st))) {
-            const double w = huberWeight(wd.huber, st[0] * st[0] + st[1] * st[1]);
-            st[54] = w * w;
-        } else {
-            for (int k = 0; k < kOut; ++k) st[k] = 0.0;
+    {
+        // gather: each lane loads its own key-ordered row (unrolled 16-byte loads)
+        if (lane < n) {
+            const double2* src = reinterpret_cast<const double2*>(B.keyRows + (size_t)B.keyOrder[ch.y + lane] * kKeyRow);
+            double* dst = rows + lane * kPairStride;
+#pragma unroll
+            for (int q = 0; q < 27; ++q) {
+                const double2 v = src[q];
+                dst[2 * q] = v.x;
+                dst[2 * q + 1] = v.y;
+            }
         }
     }
-    // this lane's compact pairs: a | b << 8 | off(0,a) << 16 | off(0,b) << 24
-    unsigned pr[kPairSlots];
-#pragma unroll
-    for (int j = 0; j < kPairSlots; ++j) {
-        const int p = lane + 32 * j;
-        int a = 0, rem = p;
-        while (a < kCompact && rem >= kCompact - a) { rem -= kCompact - a; ++a; }
-        const int b = a + rem;
-        pr[j] = p < kPairs ? (unsigned)a | (unsigned)b << 8 | (unsigned)compactOff(0, a) << 16 | (unsigned)compactOff(0, b) << 24
-                           : 0xffffffffu;
-    }
-    // runs of equal key
-    const int pa = __shfl_up_sync(0xffffffffu, kfa, 1), pb = __shfl_up_sync(0xffffffffu, kfb, 1);
-    const int pea = __shfl_up_sync(0xffffffffu, ea, 1), peb = __shfl_up_sync(0xffffffffu, eb, 1);
-    const bool start = lane < n && (lane == 0 || pa != kfa || pb != kfb || pea != ea || peb != eb);
-    unsigned starts = __ballot_sync(0xffffffffu, start);
     __syncwarp();
+    const long long key = lane < n ? __double_as_longlong(rows[lane * kPairStride + 52]) : -1ll;
+    const long long prev = __shfl_up_sync(0xffffffffu, key, 1);
+    unsigned starts = __ballot_sync(0xffffffffu, lane < n && (lane == 0 || prev != key));
     const int K = wd.K, Npc = wd.Npc;
     const int tdCol = 6 * K + (wd.estExt ? 6 * wd.E : 0);
     double* JJ = B.acc + wd.acc0;
     double* Gv = JJ + (long long)Npc * (Npc + 1) / 2 + Npc;
-    const int goff0 = lane < kCompact ? compactOff(0, lane) : 0, gstep = lane < 24 ? 6 : 1;
+    // fragment coordinates: k-step row kr = lane % 4 (observation kr / 2, row kr % 2),
+    // column lane / 4 within an 8-column block; accumulator row lane / 4, columns 2 (lane % 4) + {0, 1}
+    const int kr = lane & 3, cIn = lane >> 2;
     while (starts) {
         const int s0 = __ffs(starts) - 1;
         starts &= starts - 1;
         const int s1 = starts ? __ffs(starts) - 1 : n;
-        const int ka = __shfl_sync(0xffffffffu, kfa, s0) - wd.kf0, kb = __shfl_sync(0xffffffffu, kfb, s0) - wd.kf0;
-        const int xa = __shfl_sync(0xffffffffu, ea, s0) - wd.ext0, xb = __shfl_sync(0xffffffffu, eb, s0) - wd.ext0;
+        double g[10][2];
+#pragma unroll
+        for (int t = 0; t < 10; ++t) g[t][0] = g[t][1] = 0.0;
+        for (int m = s0; m < s1; m += 2) {
+            const int o = m + (kr >> 1), r = kr & 1;
+            const double* st = rows + o * kPairStride;
+            double frag[4];
+#pragma unroll
+            for (int I = 0; I < 4; ++I) {
+                const int col = 8 * I + cIn;
+                double v = 0.0;
+                if (o < s1) v = col < 25 ? st[25 * r + col] : (col == 25 ? st[50 + r] : 0.0);
+                frag[I] = v;
+            }
+            int t = 0;
+#pragma unroll
+            for (int I = 0; I < 4; ++I)
+#pragma unroll
+                for (int J = I; J < 4; ++J, ++t) mmaF64(g[t][0], g[t][1], frag[I], frag[J]);
+        }
+        const long long kk = __shfl_sync(0xffffffffu, key, s0);
+        const int ka = (int)(kk & 0xffff), kb = (int)((kk >> 16) & 0xffff);
+        const int xa = (int)((kk >> 32) & 0xffff), xb = (int)((kk >> 48) & 0xffff);
         const bool sameKf = ka == kb, split = xa != xb, same = sameKf && !split;
         auto colOf = [&](int c) -> int {
             if (c < 6) return sameKf ? -1 : 6 * ka + c;
@@ -265,33 +315,23 @@ __global__ void __launch_bounds__(kPairWarps * 32, 2) k_lin_pairs(DevBatch B, co
             if (c < 24) return (wd.estExt && split) ? 6 * K + 6 * xb + c - 18 : -1;
             return wd.estTd ? tdCol : -1;
         };
-        double acc[kPairSlots];
+        int t = 0;
 #pragma unroll
-        for (int j = 0; j < kPairSlots; ++j) acc[j] = 0.0;
-        double gr = 0.0;
-        for (int k = s0; k < s1; ++k) {
-            const double* st = out + kOut * k;
-            const double w2 = st[54];
+        for (int I = 0; I < 4; ++I)
 #pragma unroll
-            for (int j = 0; j < kPairSlots; ++j) {
-                if (pr[j] == 0xffffffffu) continue;
-                const int a = pr[j] & 0xff, b = (pr[j] >> 8) & 0xff, oa = (pr[j] >> 16) & 0xff, ob2 = pr[j] >> 24;
-                const int da = a < 24 ? 6 : 1, db = b < 24 ? 6 : 1;
-                acc[j] += w2 * (st[oa] * st[ob2] + st[oa + da] * st[ob2 + db]);
-            }
-            if (lane < kCompact) gr += w2 * (st[goff0] * st[0] + st[goff0 + gstep] * st[1]);
-        }
+            for (int J = I; J < 4; ++J, ++t)
 #pragma unroll
-        for (int j = 0; j < kPairSlots; ++j) {
-            if (pr[j] == 0xffffffffu || acc[j] == 0.0) continue;
-            const int ca = colOf(pr[j] & 0xff), cb = colOf((pr[j] >> 8) & 0xff);
-            if (ca < 0 || cb < 0) continue;
-            atomicAdd(&JJ[ca <= cb ? upIdx(ca, cb, Npc) : upIdx(cb, ca, Npc)], acc[j]);
-        }
-        if (lane < kCompact && gr != 0.0) {
-            const int c = colOf(lane);
-            if (c >= 0) atomicAdd(&Gv[c], gr);
-        }
+                for (int e = 0; e < 2; ++e) {
+                    const int i = 8 * I + cIn, j = 8 * J + 2 * kr + e;
+                    const double v = g[t][e];
+                    if (v == 0.0 || i > j || i >= 25 || j > 25) continue;
+                    const int ci2 = colOf(i);
+                    if (ci2 < 0) continue;
+                    if (j == 25) { atomicAdd(&Gv[ci2], v); continue; }
+                    const int cj = colOf(j);
+                    if (cj < 0) continue;
+                    atomicAdd(&JJ[ci2 <= cj ? upIdx(ci2, cj, Npc) : upIdx(cj, ci2, Npc)], v);
+                }
     }
 }
 
@@ -612,7 +652,7 @@ __device__ void blockedSolve(const double* L, int n, double* v, double* blk) {
     }
 }
 
-__global__ void __launch_bounds__(kFactorThreads) k_factor(DevBatch B, int refinement, double* Sdebug) {
+__global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int refinement, double* Sdebug) {
     const int wdx = blockIdx.x;
     if (B.lm[wdx].mode == kModeDone) return;
     const WinDesc wd = B.win[wdx];
