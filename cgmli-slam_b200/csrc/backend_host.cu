@@ -31,7 +31,7 @@ int launchIteration(const DevBatch& B, const LaunchPlan& P, int refinement, int 
                     cudaStream_t s, LaunchHook hook, void* ctx);
 int launchLmInit(const DevBatch& B, double lambda0, cudaStream_t s);
 size_t margVisualSmemBytes(int maxNc);
-cudaError_t configureMarginalization(size_t visualSmem, int maxNr, long long* eigenSmem);
+cudaError_t configureMarginalization(size_t visualSmem, int maxNr, int numWindows, long long* eigenSmem);
 int launchMarginalization(const DevBatch& B, const MargBatch& M, size_t visualSmem, cudaStream_t s);
 void launchDenseEigen(const double* H, int n, double* work, double* evals, double* evecs, int* status, cudaStream_t s);
 void launchDensePsd(const double* evals, const double* U, const double* rhs, int n, int columns, double absCut, double relCut,
@@ -686,7 +686,7 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
     int maxNr = 1;
     for (const auto& mw : mwv) maxNr = std::max(maxNr, mw.nr);
     long long eigenSmem = 0;
-    CK(configureMarginalization(smem, maxNr, &eigenSmem));
+    CK(configureMarginalization(smem, maxNr, W, &eigenSmem));
     CK(S->dMargWin.upload(mwv, st));
     CK(S->dMargElim.upload(elims, st));
     CK(S->margCols.upload(cols, st));

@@ -93,7 +93,8 @@ struct DevBatch {
 // (row <= column) of the m x m information, row-major.
 constexpr int kMargMaxNc = 200;     // marginalization columns touched by one eliminated landmark
 constexpr int kMargMaxSep = 1024;   // separator columns (Jacobi pair tables hold 512 pairs)
-constexpr int kMargThreads = 512;   // victim / eigen CTAs
+constexpr int kMargThreads = 512;   // victim CTAs
+constexpr int kEigenThreads = 512;  // eigen CTAs
 constexpr int kMargLmThreads = 128; // one CTA per eliminated landmark
 
 struct MargWin {

@@ -448,6 +448,27 @@ __device__ void jacobiPacked(double* Ap, double* Vt, int n, int maxSweeps) {
     for (int r = threadIdx.x; r < n; r += blockDim.x)
         for (int c = r; c < n; ++c) fro += (r == c ? 1.0 : 2.0) * Ap[pkUp(r, c, n)] * Ap[pkUp(r, c, n)];
     const double floorAbs = 1e-16 * sqrt(mBlockSum(fro, normRed));
+    // This thread's blocks (i, j) of the pair grid are the same in every round:
+    // decode them once (packed i | j << 16).
+    constexpr int kMaxBlk = 16;
+    const bool cached = blocks <= kMaxBlk * (int)blockDim.x;
+    int myBlk[kMaxBlk];
+#pragma unroll
+    for (int m = 0; m < kMaxBlk; ++m) {
+        const int bidx = threadIdx.x + m * blockDim.x;
+        myBlk[m] = -1;
+        if (cached && bidx < blocks) {
+            int i = (int)((2.0f * half + 1 - sqrtf((2.0f * half + 1) * (2.0f * half + 1) - 8.0f * bidx)) * 0.5f);
+            if (i < 0) i = 0;
+            while (i > 0 && i * half - i * (i - 1) / 2 > bidx) --i;
+            while ((i + 1) * half - (i + 1) * i / 2 <= bidx) ++i;
+            myBlk[m] = i | (i + (bidx - (i * half - i * (i - 1) / 2))) << 16;
+        }
+    }
+    // eigenvector update: a fixed column k per thread and every step-th pair
+    const int vStep = n <= (int)blockDim.x ? (int)blockDim.x / n : 0;
+    const int vk = vStep ? (int)threadIdx.x % n : 0, vi0 = vStep ? (int)threadIdx.x / n : 0;
+    const bool vActive = vStep && (int)threadIdx.x < vStep * n;
     for (int sweep = 0; sweep < maxSweeps; ++sweep) {
         if (threadIdx.x == 0) rotated = 0;
         __syncthreads();
@@ -461,10 +482,12 @@ __device__ void jacobiPacked(double* Ap, double* Vt, int n, int maxSweeps) {
                 double c = 1, s = 0;
                 if (q < n) {
                     const double apq = Ap[pkUp(p, q, n)], app = Ap[pkUp(p, p, n)], aqq = Ap[pkUp(q, q, n)];
-                    if (fabs(apq) > 1e-15 * sqrt(fabs(app * aqq)) && fabs(apq) > floorAbs) {
-                        const double tau = (aqq - app) / (2 * apq);
-                        const double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1 + tau * tau));
-                        c = 1 / sqrt(1 + t * t);
+                    if (apq * apq > 1e-30 * fabs(app * aqq) && fabs(apq) > floorAbs) {
+                        // tan of the rotation angle, t = sgn(d) e / (|d| + sqrt(d^2 + e^2)) with
+                        // d = a_qq - a_pp, e = 2 a_pq: the smaller root of t^2 + 2 (d / e) t - 1 = 0
+                        const double d = aqq - app, e = 2 * apq;
+                        const double t = (d >= 0 ? e : -e) / (fabs(d) + sqrt(d * d + e * e));
+                        c = rsqrt(1 + t * t);
                         s = t * c;
                         rotated = 1;
                     }
@@ -473,15 +496,9 @@ __device__ void jacobiPacked(double* Ap, double* Vt, int n, int maxSweeps) {
                 rs[i] = s;
             }
             __syncthreads();
-            for (int bidx = threadIdx.x; bidx < blocks; bidx += blockDim.x) {
-                // (i, j), i <= j, from the packed-upper enumeration of a half x half triangle
-                int i = (int)((2.0f * half + 1 - sqrtf((2.0f * half + 1) * (2.0f * half + 1) - 8.0f * bidx)) * 0.5f);
-                if (i < 0) i = 0;
-                while (i > 0 && i * half - i * (i - 1) / 2 > bidx) --i;
-                while ((i + 1) * half - (i + 1) * i / 2 <= bidx) ++i;
-                const int j = i + (bidx - (i * half - i * (i - 1) / 2));
+            auto rotateBlock = [&](int i, int j) {
                 const double si = rs[i], sj = rs[j];
-                if (si == 0.0 && sj == 0.0) continue;
+                if (si == 0.0 && sj == 0.0) return;
                 const double ci = rc[i], cj = rc[j];
                 const int pi = pairP[i], qi = pairQ[i], pj = pairP[j], qj = pairQ[j];
                 if (i == j) {
@@ -507,16 +524,35 @@ __device__ void jacobiPacked(double* Ap, double* Vt, int n, int maxSweeps) {
                     if (rowQ) Ap[k10] = si * t00 + ci * t10;
                     if (rowQ && colQ) Ap[k11] = si * t01 + ci * t11;
                 }
+            };
+            if (cached) {
+#pragma unroll
+                for (int m = 0; m < kMaxBlk; ++m)
+                    if (myBlk[m] >= 0) rotateBlock(myBlk[m] & 0xffff, myBlk[m] >> 16);
+            } else {
+                for (int bidx = threadIdx.x; bidx < blocks; bidx += blockDim.x) {
+                    // (i, j), i <= j, from the packed-upper enumeration of a half x half triangle
+                    int i = (int)((2.0f * half + 1 - sqrtf((2.0f * half + 1) * (2.0f * half + 1) - 8.0f * bidx)) * 0.5f);
+                    if (i < 0) i = 0;
+                    while (i > 0 && i * half - i * (i - 1) / 2 > bidx) --i;
+                    while ((i + 1) * half - (i + 1) * i / 2 <= bidx) ++i;
+                    rotateBlock(i, i + (bidx - (i * half - i * (i - 1) / 2)));
+                }
             }
-            for (int t = threadIdx.x; t < half * n; t += blockDim.x) {
-                const int i = t / n, k = t % n;
+            auto rotateVt = [&](int i, int k) {
                 const double s = rs[i];
-                if (s == 0.0) continue;
+                if (s == 0.0) return;
                 const double c = rc[i];
                 const long long p = pairP[i], q = pairQ[i];
                 const double vp = Vt[p * n + k], vq = Vt[q * n + k];
                 Vt[p * n + k] = c * vp - s * vq;
                 Vt[q * n + k] = s * vp + c * vq;
+            };
+            if (vStep) {
+                if (vActive)
+                    for (int i = vi0; i < half; i += vStep) rotateVt(i, vk);
+            } else {
+                for (int t = threadIdx.x; t < half * n; t += blockDim.x) rotateVt(t / n, t % n);
             }
             __syncthreads();
         }
@@ -605,7 +641,7 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_victim(MargBatch M) {
 
 // Eigendecomposition of the separator information and the square-root prior,
 // rows in ascending eigenvalue order.
-__global__ void __launch_bounds__(kMargThreads) k_marg_eigen(MargBatch M) {
+__global__ void __launch_bounds__(kEigenThreads) k_marg_eigen(MargBatch M) {
     const int w = blockIdx.x;
     const MargWin mw = M.win[w];
     const int nr = mw.nr;
@@ -618,7 +654,7 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_eigen(MargBatch M) {
     double* ev = M.evals + mw.vec0;
     const double* bs = M.sepB + mw.vec0;
     __shared__ int pos[kMargMaxSep];
-    __shared__ double red[kMargThreads / 32];
+    __shared__ double red[kEigenThreads / 32];
     // component k of eigenvector i is Vv[i * si + k * sk]
     const double* Vv;
     long long si, sk;
@@ -744,7 +780,7 @@ size_t margVisualSmemBytes(int maxNc) {
 // Sets the dynamic shared memory limits of the marginalization kernels for a
 // batch whose largest separator has maxNr columns; returns the eigen CTA's
 // dynamic shared memory in eigenSmem.
-cudaError_t configureMarginalization(size_t visualSmem, int maxNr, long long* eigenSmem) {
+cudaError_t configureMarginalization(size_t visualSmem, int maxNr, int numWindows, long long* eigenSmem) {
     cudaError_t e = cudaFuncSetAttribute(k_marg_visual, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)visualSmem);
     if (e != cudaSuccess) return e;
     int dev = 0, optin = 0;
@@ -753,8 +789,10 @@ cudaError_t configureMarginalization(size_t visualSmem, int maxNr, long long* ei
     cudaFuncAttributes fa;
     if ((e = cudaFuncGetAttributes(&fa, k_marg_eigen)) != cudaSuccess) return e;
     const long long avail = (long long)optin - (long long)fa.sharedSizeBytes;
+    // eigenvectors in shared memory too when they fit
     const long long n = maxNr, want = 8 * (n * (n + 1) / 2 + n * n), packedOnly = 8 * (n * (n + 1) / 2);
-    long long use = want <= avail ? want : (packedOnly <= avail ? avail : 0);
+    long long use = want <= avail ? want : (packedOnly <= avail ? packedOnly : 0);
+    (void)numWindows;
     if (use < 0) use = 0;
     *eigenSmem = use;
     return cudaFuncSetAttribute(k_marg_eigen, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)use);
@@ -770,7 +808,7 @@ int launchMarginalization(const DevBatch& B, const MargBatch& M, size_t visualSm
     }
     k_marg_retained<<<M.numWindows, 256, 0, s>>>(B, M);
     k_marg_victim<<<M.numWindows, kMargThreads, 0, s>>>(M);
-    k_marg_eigen<<<M.numWindows, kMargThreads, (size_t)M.eigenSmem, s>>>(M);
+    k_marg_eigen<<<M.numWindows, kEigenThreads, (size_t)M.eigenSmem, s>>>(M);
     return n + 3;
 }
 void launchDenseEigen(const double* H, int n, double* work, double* evals, double* evecs, int* status, cudaStream_t s) {
