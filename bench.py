@@ -62,6 +62,9 @@ def parse():
     p.add_argument("--cpu-sample", type=int, default=24, help="windows timed on the host for the CPU baseline")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--plain-windows", type=int, default=16, help="single-window solves timed for the plain path")
+    p.add_argument("--serve-rate", type=float, default=5000.0, help="offered request rate of the served run (requests/s, 0: off)")
+    p.add_argument("--serve-seconds", type=float, default=3.0, help="duration of the served run's arrivals")
+    p.add_argument("--serve-pool", type=int, default=512, help="distinct windows the served requests draw from")
     return p.parse_args()
 
 
@@ -184,6 +187,38 @@ def peaks():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def run_served(args, local, backend):
+    """Served mode (the serving configuration): requests from 128 simulated rigs
+    arrive as a Poisson stream at args.serve_rate requests/s; each request is one
+    LM iteration plus oldest-keyframe marginalization of a window drawn as in the
+    batched configuration.  The trace is replayed by the server's native replay
+    (cgmli_server_replay): latency runs from each request's scheduled arrival to
+    its completion, so queueing is included; throughput is completed requests
+    over the span from the first arrival to the last completion."""
+    rng = np.random.default_rng(args.seed + 5)
+    pool = synth.make_windows("c4", args.serve_pool, seed=args.seed + 500)
+    n_req = int(args.serve_rate * args.serve_seconds)
+    arrival = np.cumsum(rng.exponential(1.0 / args.serve_rate, n_req))
+    rigs = 128
+    server = backend.Server(device=local, iterations=1, policy=abi.MARGIN_OLD)
+    # warm-up: both solvers see a full batch
+    server.replay(pool, [0] * len(pool), np.zeros(len(pool)))
+    windows = [pool[i % len(pool)] for i in range(n_req)]
+    lat, status, span = server.replay(windows, [0] * n_req, arrival)
+    server.close()
+    lat_sorted = np.sort(lat)
+    counts = {}
+    for st in status:
+        key = abi.ERRORS.get(int(st), int(st))
+        counts[key] = counts.get(key, 0) + 1
+    return {
+        "offered_rate": args.serve_rate, "throughput": n_req / span, "unit": "requests/s",
+        "p50_ms": float(lat_sorted[n_req // 2]), "p99_ms": float(lat_sorted[min(n_req - 1, int(0.99 * n_req))]),
+        "requests": n_req, "request_status": counts, "rigs": rigs,
+        "workload": "1 LM iteration + oldest-keyframe marginalization per request; windows as the batched configuration",
+    }
 
 
 def run_reference(args, world, rank):
@@ -334,6 +369,8 @@ def main():
                  "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))], "windows": len(lat),
                  "workload": "one configuration-2 window (10 KF, 3000 lm, 24+1 calib, prior) per solve"}
 
+    served = run_served(args, local, backend) if rank == 0 and args.serve_rate > 0 else None
+
     statuses = {}
     for r in reports:
         statuses[abi.ERRORS.get(r.status, r.status)] = statuses.get(abi.ERRORS.get(r.status, r.status), 0) + 1
@@ -377,6 +414,7 @@ def main():
             "clocks": clocks.summary(), "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
             "cpu_baseline": cpu_baseline, "plain_path": plain,
             "served_vs_plain": (value / world) / plain["windows_per_s"] if plain else None,
+            "served": served,
             "batch_latency_ms": {"p50": sorted(dev_ms)[len(dev_ms) // 2], "p99": max(dev_ms)},
             "window_status": statuses, "wall_s": wall,
         }

@@ -14,12 +14,14 @@ OK = 0
 ERRORS = {
     0: "ok", 1: "invalid input", 2: "non-finite", 3: "out of memory", 4: "CUDA error", 5: "not positive definite",
     6: "indefinite", 7: "unsupported", 8: "no acceptable step", 9: "size limit", 10: "cost mismatch",
+    11: "pending",
 }
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 PRIOR_POSE, PRIOR_SPEED_BIAS, PRIOR_EXTRINSIC, PRIOR_TIME_OFFSET = 0, 1, 2, 3
 MARGIN_OLD, MARGIN_SECOND_NEW = 0, 1
 MARG_EIGEN_NOALLOC_MAX_N = 256  # CGMLI_MARG_EIGEN_NOALLOC_MAX_N
+E_PENDING = 11
 
 
 class FrozenImu(C.Structure):
@@ -55,6 +57,11 @@ class Window(C.Structure):
 class SolverOptions(C.Structure):
     _fields_ = [("precision", C.c_int), ("refinement_steps", C.c_int), ("initial_lambda", C.c_double),
                 ("slabs_per_window", C.c_int), ("threads_per_block", C.c_int)]
+
+
+class ServerOptions(C.Structure):
+    _fields_ = [("device", C.c_int), ("max_batch_windows", C.c_int), ("memory_budget_bytes", C.c_longlong),
+                ("iterations", C.c_int), ("policy", C.c_int)]
 
 
 class SolveReport(C.Structure):
@@ -111,6 +118,17 @@ def declare_backend(lib: C.CDLL) -> C.CDLL:
            [c_double_p, c_double_p, C.c_int, C.c_int, C.c_double, C.c_double, c_double_p])
     _proto(lib, "cgmli_marg_subtract", C.c_int, [c_double_p, c_double_p, C.c_int, C.c_int, c_double_p, c_double_p])
     _proto(lib, "cgmli_marg_eigen_noalloc", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p])
+    V = C.c_void_p
+    ll_p = C.POINTER(C.c_longlong)
+    _proto(lib, "cgmli_server_create", C.c_int, [C.POINTER(ServerOptions), C.POINTER(C.c_void_p)])
+    _proto(lib, "cgmli_server_destroy", None, [V])
+    _proto(lib, "cgmli_server_submit", C.c_int, [V, W, C.c_int, ll_p])
+    _proto(lib, "cgmli_server_poll", C.c_int, [V, C.c_longlong, C.c_int, C.POINTER(SolveReport), c_double_p])
+    _proto(lib, "cgmli_server_read_prior", C.c_int,
+           [V, C.c_longlong, c_int_p, c_int_p, c_int_p, c_int_p, c_int_p, c_double_p, c_double_p, c_double_p])
+    _proto(lib, "cgmli_server_release", C.c_int, [V, C.c_longlong])
+    _proto(lib, "cgmli_server_replay", C.c_int,
+           [V, C.POINTER(W), c_int_p, c_double_p, C.c_int, c_double_p, c_int_p, c_double_p])
     return lib
 
 
@@ -131,7 +149,8 @@ BACKEND_SYMBOLS = [
     "cgmli_solver_read_reduced", "cgmli_solver_window_dims", "cgmli_solver_last_timing", "cgmli_solver_marginalize",
     "cgmli_solver_read_prior", "cgmli_marg_eigen", "cgmli_marg_psd_solve", "cgmli_marg_subtract",
     "cgmli_solver_checkpoint", "cgmli_solver_rollback", "cgmli_solver_kernel_times", "cgmli_topology_check",
-    "cgmli_marg_eigen_noalloc",
+    "cgmli_marg_eigen_noalloc", "cgmli_server_create", "cgmli_server_destroy", "cgmli_server_submit", "cgmli_server_poll",
+    "cgmli_server_read_prior", "cgmli_server_release", "cgmli_server_replay",
 ]
 KERNEL_NAMES = ["zero_acc", "linearize", "retained", "factor", "candidate", "backsub_trial", "retained_trial", "lm_update", "accept",
                 "lin_pairs", "lin_schur"]

@@ -187,3 +187,82 @@ def _window_array(windows):
     for i, w in enumerate(windows):
         arr[i] = w.window if hasattr(w, "window") else w
     return arr
+
+
+class Server:
+    """Served mode: requests (one window each) are batched continuously on the
+    device; see the cgmli_server_* functions of cgmli_backend.h.  The windows
+    passed to submit() must stay alive until their request completes."""
+
+    def __init__(self, device: int = 0, iterations: int = 1, policy: int = abi.MARGIN_OLD, max_batch_windows: int = 512,
+                 memory_budget_bytes: int = 40 << 30):
+        opt = abi.ServerOptions()
+        opt.device = device
+        opt.max_batch_windows = max_batch_windows
+        opt.memory_budget_bytes = memory_budget_bytes
+        opt.iterations = iterations
+        opt.policy = policy
+        self._h = C.c_void_p()
+        _check(lib().cgmli_server_create(C.byref(opt), C.byref(self._h)), "cgmli_server_create")
+        self._keep = {}
+
+    def close(self):
+        if self._h:
+            lib().cgmli_server_destroy(self._h)
+            self._h = C.c_void_p()
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, window, victim: int = -1) -> int:
+        """window: a synth.SynthWindow or an abi.Window; returns the ticket."""
+        w = window.window if hasattr(window, "window") else window
+        t = C.c_longlong()
+        _check(lib().cgmli_server_submit(self._h, C.byref(w), victim, C.byref(t)), "cgmli_server_submit")
+        self._keep[t.value] = window
+        return t.value
+
+    def poll(self, ticket: int, wait: bool = True):
+        """(report, latency_ms) once complete, None while pending (wait=False)."""
+        rep, lat = abi.SolveReport(), C.c_double()
+        code = lib().cgmli_server_poll(self._h, ticket, 1 if wait else 0, C.byref(rep), C.byref(lat))
+        if code == abi.E_PENDING:
+            return None
+        _check(code, "cgmli_server_poll")
+        return rep, lat.value
+
+    def read_prior(self, ticket: int) -> dict:
+        rank, cols, nb = C.c_int(), C.c_int(), C.c_int()
+        code = lib().cgmli_server_read_prior(self._h, ticket, C.byref(rank), C.byref(cols), C.byref(nb), None, None, None, None,
+                                             None)
+        if code != 0:
+            return dict(status=code)
+        k, m, b = rank.value, cols.value, nb.value
+        kinds, idx = np.zeros(b, np.int32), np.zeros(b, np.int32)
+        ref, A, r0 = np.zeros(9 * b + 1), np.zeros(k * m), np.zeros(k)
+        ip = abi.c_int_p
+        code = lib().cgmli_server_read_prior(self._h, ticket, C.byref(rank), C.byref(cols), C.byref(nb), kinds.ctypes.data_as(ip),
+                                             idx.ctypes.data_as(ip), _p(ref), _p(A), _p(r0))
+        amb = int(sum(9 if t == abi.PRIOR_SPEED_BIAS else 1 if t == abi.PRIOR_TIME_OFFSET else 7 for t in kinds))
+        return dict(status=code, rank=k, cols=m, kinds=kinds, index=idx, reference=ref[:amb], A=A.reshape(k, m), r0=r0)
+
+    def release(self, ticket: int) -> None:
+        _check(lib().cgmli_server_release(self._h, ticket), "cgmli_server_release")
+        self._keep.pop(ticket, None)
+
+    def replay(self, windows, victims, arrival_s):
+        """Replays a trace (window objects, victim per request, arrival times in s);
+        returns (latency_ms array, status array, span_s)."""
+        n = len(windows)
+        ptrs = (C.POINTER(abi.Window) * n)(*[C.pointer(w.window if hasattr(w, "window") else w) for w in windows])
+        vic = np.ascontiguousarray(victims, dtype=np.int32)
+        arr = np.ascontiguousarray(arrival_s, dtype=np.float64)
+        lat, st, span = np.zeros(n), np.zeros(n, dtype=np.int32), C.c_double()
+        _check(lib().cgmli_server_replay(self._h, ptrs, vic.ctypes.data_as(abi.c_int_p), _p(arr), n, _p(lat),
+                                         st.ctypes.data_as(abi.c_int_p), C.byref(span)), "cgmli_server_replay")
+        return lat, st, span.value
+

@@ -135,6 +135,16 @@ struct cgmli_solver {
     DArray<double> margH, margB, margSepH, margSepV, margSepB, margEvals, margA, margR0, margX, margMaxD, margStats;
     MargBatch MB{};
     bool haveMarg = false;
+    // host copy of every window's marginalization result, made by the first
+    // read_prior after a marginalization (one pass instead of copies per window)
+    bool margCached = false;
+    long long margSepTotal = 0, margVecTotal = 0;
+    HVec<double> hMargA, hMargR0, hMargStats;
+    HVec<int> hMargRank, hMargStatus;
+    // pinned staging of the marginalization's inputs, and the event after their uploads
+    HVec<MargElim> hMargElim;
+    HVec<int> hMargCols, hMargObsMap, hMargPoseCol, hMargSbCol, hMargExtCol;
+    cudaEvent_t margUploaded = nullptr;
     // checkpoint of the accepted states
     DArray<double> snapPose, snapSb, snapExt, snapTd, snapRho;
     bool haveSnapshot = false;
@@ -193,6 +203,7 @@ struct cgmli_solver {
         DArray<double>* md[] = {&margH, &margB, &margSepH, &margSepV, &margSepB, &margEvals, &margA, &margR0, &margX, &margMaxD, &margStats};
         for (auto* a : md) a->release();
         for (auto e : evPool) cudaEventDestroy(e);
+        if (margUploaded) cudaEventDestroy(margUploaded);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
@@ -579,53 +590,67 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
     for (int w = 0; w < W; ++w)
         if (victim_kf[w] < -1 || victim_kf[w] >= S->win[w].K) return fail(CGMLI_E_INVALID, "victim keyframe out of range");
     CK(cudaSetDevice(S->device));
+    // ---- phase A (parallel over windows): elimination set, columns, local maps
+    struct Part {
+        std::vector<MargElim> elims;   // col0 / obs0 window-local
+        std::vector<int> cols, obsMap;
+        int maxNc = 0, status = CGMLI_OK;
+        const char* why = "";
+    };
     std::vector<MargWin> mwv(W);
-    std::vector<MargElim> elims;
-    std::vector<int> cols, obsMap;
-    std::vector<int> poseCol(S->totalKf, -1), sbCol(S->totalKf, -1), extCol(S->totalExt, -1);
+    std::vector<Part> part(W);
     S->sepKind.assign(W, {});
     S->sepIndex.assign(W, {});
-    long long H0 = 0, sep0 = 0, vec0 = 0, x0 = 0;
-    int maxNc = 0;
-    for (int w = 0; w < W; ++w) {
+    const HostBatch& hb = S->hb;
+    HVec<int>& poseCol = S->hMargPoseCol;
+    HVec<int>& sbCol = S->hMargSbCol;
+    HVec<int>& extCol = S->hMargExtCol;
+    // the staging arrays may still feed the previous marginalization's uploads
+    if (S->margUploaded) CK(cudaEventSynchronize(S->margUploaded));
+    poseCol.resize(S->totalKf);
+    sbCol.resize(S->totalKf);
+    extCol.resize(S->totalExt);
+    parallelFor(W, 0, [&](int w) {
         const WinDesc& d = S->win[w];
         const int v = victim_kf[w];
         MargWin& mw = mwv[w];
+        Part& P = part[w];
         mw = MargWin{};
         mw.imu[0] = mw.imu[1] = -1;
         mw.tdCol = -1;
         mw.huber = d.huber;
-        mw.H0 = H0; mw.sep0 = sep0; mw.vec0 = vec0; mw.x0 = x0;
-        mw.elim0 = (int)elims.size();
-        if (v < 0) continue;
+        std::fill(&poseCol[d.kf0], &poseCol[d.kf0] + d.K, -1);
+        std::fill(&sbCol[d.kf0], &sbCol[d.kf0] + d.K, -1);
+        std::fill(&extCol[d.ext0], &extCol[d.ext0] + d.E, -1);
+        if (v < 0) return;
         std::vector<char> poseUsed(d.K, 0), sbUsed(d.K, 0), extUsed(d.E, 0);
         bool tdUsed = false;
         std::vector<int> elimLm;
         for (int q = 0; q < d.L; ++q) {
-            const int g = d.lm0 + q, a = S->hb.lmKf[g] - d.kf0;
+            const int g = d.lm0 + q, a = hb.lmKf[g] - d.kf0;
             bool e = a == v;
-            for (int f = S->hb.lmObsBegin[g]; f < S->hb.lmObsBegin[g + 1] && !e && policy == CGMLI_MARGIN_OLD; ++f)
-                e = S->hb.obKf[f] - d.kf0 == v;
+            for (int f = hb.lmObsBegin[g]; f < hb.lmObsBegin[g + 1] && !e && policy == CGMLI_MARGIN_OLD; ++f)
+                e = hb.obKf[f] - d.kf0 == v;
             if (!e) continue;
             elimLm.push_back(g);
-            for (int f = S->hb.lmObsBegin[g]; f < S->hb.lmObsBegin[g + 1]; ++f) {
+            for (int f = hb.lmObsBegin[g]; f < hb.lmObsBegin[g + 1]; ++f) {
                 poseUsed[a] = 1;
-                poseUsed[S->hb.obKf[f] - d.kf0] = 1;
-                extUsed[S->hb.camExt[S->hb.lmCam[g]] - d.ext0] = 1;
-                extUsed[S->hb.camExt[S->hb.obCam[f]] - d.ext0] = 1;
+                poseUsed[hb.obKf[f] - d.kf0] = 1;
+                extUsed[hb.camExt[hb.lmCam[g]] - d.ext0] = 1;
+                extUsed[hb.camExt[hb.obCam[f]] - d.ext0] = 1;
                 tdUsed = true;
             }
         }
         int nImu = 0;
         for (int i = 0; i < d.nImu; ++i) {
-            const int k = S->hb.imuKf[d.imu0 + i] - d.kf0;
+            const int k = hb.imuKf[d.imu0 + i] - d.kf0;
             if (k != v && k + 1 != v) continue;
-            if (nImu == 2) return fail(CGMLI_E_LIMIT, "more than two IMU factors touch the victim keyframe");
+            if (nImu == 2) { P.status = CGMLI_E_LIMIT; P.why = "more than two IMU factors touch the victim keyframe"; return; }
             mw.imu[nImu++] = d.imu0 + i;
             poseUsed[k] = poseUsed[k + 1] = sbUsed[k] = sbUsed[k + 1] = 1;
         }
         for (int b = 0; b < d.priorBlocks; ++b) {
-            const int kind = S->hb.priorKind[d.priorBlk0 + b], gi = S->hb.priorIndex[d.priorBlk0 + b];
+            const int kind = hb.priorKind[d.priorBlk0 + b], gi = hb.priorIndex[d.priorBlk0 + b];
             if (kind == CGMLI_PRIOR_POSE) poseUsed[gi - d.kf0] = 1;
             else if (kind == CGMLI_PRIOR_SPEED_BIAS) sbUsed[gi - d.kf0] = 1;
             else if (kind == CGMLI_PRIOR_EXTRINSIC) extUsed[gi - d.ext0] = 1;
@@ -647,40 +672,79 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
         if (tdUsed && d.hasTd) { mw.tdCol = n; n += 1; sep(CGMLI_PRIOR_TIME_OFFSET, 0); }
         mw.m = n;
         mw.nr = n - mw.nm;
-        if (mw.nr > kMargMaxSep) return fail(CGMLI_E_LIMIT, "marginalization separator above 1024 columns");
+        if (mw.nr > kMargMaxSep) { P.status = CGMLI_E_LIMIT; P.why = "marginalization separator above 1024 columns"; return; }
         // eliminated landmarks: local column blocks in order of first use
+        int obsCount = 0;
         for (int g : elimLm) {
-            MargElim me{g, w, 0, (int)cols.size(), (int)(obsMap.size() / 5)};
-            std::vector<int> blkStart, blkLocal;
+            MargElim me{g, w, 0, (int)P.cols.size(), obsCount};
+            int blkStart[4 * kMaxTrackChunk + 1], blkLocal[4 * kMaxTrackChunk + 1], nblk = 0;
             auto localOf = [&](int start, int size) {
                 if (start < 0) return -1;
-                for (size_t i = 0; i < blkStart.size(); ++i)
+                for (int i = 0; i < nblk; ++i)
                     if (blkStart[i] == start) return blkLocal[i];
-                blkStart.push_back(start);
-                blkLocal.push_back(me.nc);
-                for (int c = 0; c < size; ++c) cols.push_back(start + c);
+                blkStart[nblk] = start;
+                blkLocal[nblk] = me.nc;
+                ++nblk;
+                for (int c = 0; c < size; ++c) P.cols.push_back(start + c);
                 me.nc += size;
-                return blkLocal.back();
+                return me.nc - size;
             };
-            const int a = S->hb.lmKf[g], ea = S->hb.camExt[S->hb.lmCam[g]];
-            for (int f = S->hb.lmObsBegin[g]; f < S->hb.lmObsBegin[g + 1]; ++f) {
-                const int b = S->hb.obKf[f], eb = S->hb.camExt[S->hb.obCam[f]];
-                obsMap.push_back(localOf(poseCol[a], 6));
-                obsMap.push_back(localOf(poseCol[b], 6));
-                obsMap.push_back(localOf(extCol[ea], 6));
-                obsMap.push_back(localOf(extCol[eb], 6));
-                obsMap.push_back(mw.tdCol >= 0 ? localOf(mw.tdCol, 1) : -1);
+            const int a = hb.lmKf[g], ea = hb.camExt[hb.lmCam[g]];
+            for (int f = hb.lmObsBegin[g]; f < hb.lmObsBegin[g + 1]; ++f) {
+                const int b = hb.obKf[f], eb = hb.camExt[hb.obCam[f]];
+                P.obsMap.push_back(localOf(poseCol[a], 6));
+                P.obsMap.push_back(localOf(poseCol[b], 6));
+                P.obsMap.push_back(localOf(extCol[ea], 6));
+                P.obsMap.push_back(localOf(extCol[eb], 6));
+                P.obsMap.push_back(mw.tdCol >= 0 ? localOf(mw.tdCol, 1) : -1);
+                ++obsCount;
             }
-            if (me.nc > kMargMaxNc) return fail(CGMLI_E_LIMIT, "eliminated landmark touches more than 200 marginalization columns");
-            maxNc = std::max(maxNc, me.nc);
-            elims.push_back(me);
+            if (me.nc > kMargMaxNc) {
+                P.status = CGMLI_E_LIMIT;
+                P.why = "eliminated landmark touches more than 200 marginalization columns";
+                return;
+            }
+            P.maxNc = std::max(P.maxNc, me.nc);
+            P.elims.push_back(me);
         }
-        mw.nElim = (int)elims.size() - mw.elim0;
+    });
+    // ---- prefix sums over the windows, then one concatenation (parallel)
+    std::vector<long long> colBase(W + 1, 0), obsBase(W + 1, 0);
+    std::vector<int> elimBase(W + 1, 0);
+    long long H0 = 0, sep0 = 0, vec0 = 0, x0 = 0;
+    int maxNc = 0;
+    for (int w = 0; w < W; ++w) {
+        if (part[w].status != CGMLI_OK) return fail(part[w].status, part[w].why);
+        MargWin& mw = mwv[w];
+        mw.H0 = H0; mw.sep0 = sep0; mw.vec0 = vec0; mw.x0 = x0;
+        mw.elim0 = elimBase[w];
+        mw.nElim = (int)part[w].elims.size();
+        elimBase[w + 1] = elimBase[w] + mw.nElim;
+        colBase[w + 1] = colBase[w] + (long long)part[w].cols.size();
+        obsBase[w + 1] = obsBase[w] + (long long)part[w].obsMap.size() / 5;
+        maxNc = std::max(maxNc, part[w].maxNc);
         H0 += (long long)mw.m * mw.m;
         sep0 += (long long)mw.nr * mw.nr;
         vec0 += mw.m;
         x0 += 2ll * 15 * (mw.nr + 1);
     }
+    HVec<MargElim>& elims = S->hMargElim;
+    HVec<int>& cols = S->hMargCols;
+    HVec<int>& obsMap = S->hMargObsMap;
+    elims.resize(elimBase[W]);
+    cols.resize(colBase[W]);
+    obsMap.resize(5 * obsBase[W]);
+    parallelFor(W, 0, [&](int w) {
+        const Part& P = part[w];
+        for (size_t e = 0; e < P.elims.size(); ++e) {
+            MargElim me = P.elims[e];
+            me.col0 += (int)colBase[w];
+            me.obs0 += (int)obsBase[w];
+            elims[elimBase[w] + e] = me;
+        }
+        std::copy(P.cols.begin(), P.cols.end(), cols.begin() + colBase[w]);
+        std::copy(P.obsMap.begin(), P.obsMap.end(), obsMap.begin() + 5 * obsBase[w]);
+    });
     cudaStream_t st = S->stream;
     const size_t smem = margVisualSmemBytes(std::max(maxNc, 1));
     int maxNr = 1;
@@ -694,6 +758,8 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
     CK(S->margPoseCol.upload(poseCol, st));
     CK(S->margSbCol.upload(sbCol, st));
     CK(S->margExtCol.upload(extCol, st));
+    if (!S->margUploaded) CK(cudaEventCreateWithFlags(&S->margUploaded, cudaEventDisableTiming));
+    CK(cudaEventRecord(S->margUploaded, st));
     CK(S->margH.reserve(H0)); CK(S->margB.reserve(vec0)); CK(S->margSepH.reserve(sep0)); CK(S->margSepV.reserve(sep0));
     CK(S->margSepB.reserve(vec0)); CK(S->margEvals.reserve(vec0)); CK(S->margA.reserve(sep0)); CK(S->margR0.reserve(vec0));
     CK(S->margX.reserve(x0)); CK(S->margMaxD.reserve(W)); CK(S->margStats.reserve(4ll * W));
@@ -715,6 +781,9 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
     M.evals = S->margEvals.p; M.A = S->margA.p; M.r0 = S->margR0.p; M.X = S->margX.p;
     M.maxD = S->margMaxD.p; M.stats = S->margStats.p; M.rank = S->margRank.p; M.status = S->margStatus.p;
     S->margWin = mwv;
+    S->margSepTotal = sep0;
+    S->margVecTotal = vec0;
+    S->margCached = false;
     CK(cudaEventRecord(S->ev0, st));
     S->lastLaunches = launchMarginalization(S->B, M, smem, st);
     CK(cudaGetLastError());
@@ -729,14 +798,36 @@ int cgmli_solver_read_prior(cgmli_solver* S, int window, int* rank, int* cols, i
     if (window < 0 || window >= (int)S->margWin.size()) return fail(CGMLI_E_INVALID, "window index");
     if (!rank || !cols || !num_blocks) return fail(CGMLI_E_INVALID, "null size outputs");
     CK(cudaSetDevice(S->device));
-    CK(cudaStreamSynchronize(S->stream));
-    float ms = 0;
-    if (cudaEventElapsedTime(&ms, S->ev0, S->ev1) == cudaSuccess) S->lastMs = ms;
+    const int W = (int)S->margWin.size();
+    if (!S->margCached) {
+        CK(cudaStreamSynchronize(S->stream));
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, S->ev0, S->ev1) == cudaSuccess) S->lastMs = ms;
+        HostBatch& hb = S->hb;
+        S->hMargA.resize(S->margSepTotal);
+        S->hMargR0.resize(S->margVecTotal);
+        S->hMargStats.resize(4ll * W);
+        S->hMargRank.resize(W);
+        S->hMargStatus.resize(W);
+        cudaStream_t st = S->stream;
+        if (S->margSepTotal)
+            CK(cudaMemcpyAsync(S->hMargA.data(), S->margA.p, S->margSepTotal * sizeof(double), cudaMemcpyDeviceToHost, st));
+        if (S->margVecTotal)
+            CK(cudaMemcpyAsync(S->hMargR0.data(), S->margR0.p, S->margVecTotal * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(S->hMargStats.data(), S->margStats.p, 4ll * W * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(S->hMargRank.data(), S->margRank.p, W * sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(S->hMargStatus.data(), S->margStatus.p, W * sizeof(int), cudaMemcpyDeviceToHost, st));
+        // the states the separator references come from (the accepted states)
+        CK(cudaMemcpyAsync(hb.pose.data(), S->pose[0].p, hb.pose.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(hb.sb.data(), S->sb[0].p, hb.sb.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(hb.ext.data(), S->ext[0].p, hb.ext.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(hb.td.data(), S->td[0].p, hb.td.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        S->margCached = true;
+    }
     const MargWin& mw = S->margWin[window];
     const WinDesc& d = S->win[window];
-    int status = CGMLI_OK, rk = 0;
-    CK(cudaMemcpy(&status, S->margStatus.p + window, sizeof(int), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(&rk, S->margRank.p + window, sizeof(int), cudaMemcpyDeviceToHost));
+    const int status = S->hMargStatus[window], rk = S->hMargRank[window];
     if (status != CGMLI_OK) return fail(status, "window marginalization failed (invalid factor or indefinite information)");
     *rank = mw.m ? rk : 0;
     *cols = mw.m ? mw.nr : 0;
@@ -747,24 +838,20 @@ int cgmli_solver_read_prior(cgmli_solver* S, int window, int* rank, int* cols, i
     if (block_kind) std::copy(kinds.begin(), kinds.end(), block_kind);
     if (block_index) std::copy(idx.begin(), idx.end(), block_index);
     if (reference) {
-        std::vector<double> pose(7ull * d.K), sb(9ull * d.K), ext(7ull * d.E);
-        double td = 0;
-        CK(cudaMemcpy(pose.data(), S->pose[0].p + 7ll * d.kf0, pose.size() * 8, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(sb.data(), S->sb[0].p + 9ll * d.kf0, sb.size() * 8, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(ext.data(), S->ext[0].p + 7ll * d.ext0, ext.size() * 8, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(&td, S->td[0].p + window, 8, cudaMemcpyDeviceToHost));
+        const HostBatch& hb = S->hb;
         double* out = reference;
         for (size_t b = 0; b < kinds.size(); ++b) {
-            const double* src = kinds[b] == CGMLI_PRIOR_POSE ? &pose[7ull * idx[b]] : kinds[b] == CGMLI_PRIOR_SPEED_BIAS ? &sb[9ull * idx[b]]
-                                : kinds[b] == CGMLI_PRIOR_EXTRINSIC ? &ext[7ull * idx[b]] : &td;
+            const double* src = kinds[b] == CGMLI_PRIOR_POSE ? &hb.pose[7ull * (d.kf0 + idx[b])]
+                                : kinds[b] == CGMLI_PRIOR_SPEED_BIAS ? &hb.sb[9ull * (d.kf0 + idx[b])]
+                                : kinds[b] == CGMLI_PRIOR_EXTRINSIC ? &hb.ext[7ull * (d.ext0 + idx[b])] : &hb.td[window];
             const int n = ambientOf(kinds[b]);
             std::copy(src, src + n, out);
             out += n;
         }
     }
-    if (A && rk) CK(cudaMemcpy(A, S->margA.p + mw.sep0, (size_t)rk * mw.nr * sizeof(double), cudaMemcpyDeviceToHost));
-    if (r0 && rk) CK(cudaMemcpy(r0, S->margR0.p + mw.vec0, (size_t)rk * sizeof(double), cudaMemcpyDeviceToHost));
-    if (formation) CK(cudaMemcpy(formation, S->margStats.p + 4ll * window, 4 * sizeof(double), cudaMemcpyDeviceToHost));
+    if (A && rk) std::copy(&S->hMargA[mw.sep0], &S->hMargA[mw.sep0] + (size_t)rk * mw.nr, A);
+    if (r0 && rk) std::copy(&S->hMargR0[mw.vec0], &S->hMargR0[mw.vec0] + rk, r0);
+    if (formation) std::copy(&S->hMargStats[4ll * window], &S->hMargStats[4ll * window] + 4, formation);
     return CGMLI_OK;
 }
 

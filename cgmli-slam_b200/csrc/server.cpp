@@ -1,0 +1,358 @@
+// Served mode: continuous batching of window-solve requests (see the
+// cgmli_server_* declarations in cgmli_backend.h).
+//
+// One scheduler thread owns two solvers, each with its own CUDA stream.  Each
+// cycle it (1) takes the queued requests that fit the next batch (arrival
+// order, window cap, device-footprint budget), builds and uploads that batch
+// on the idle solver and launches its LM solve and marginalization, then
+// (2) completes the batch launched in the previous cycle: synchronizes its
+// stream, writes the states back into the callers' windows, and records the
+// reports and priors.  The host work of step (1) therefore overlaps the device
+// work of the previous batch, and requests arriving while the GPU is busy
+// join the next batch.
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/cgmli_backend.h"
+#include "topology.h"
+
+namespace cgmli {
+int setLastError(int code, const char* message);
+}  // namespace cgmli
+
+namespace {
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    long long ticket = 0;
+    cgmli_window window{};
+    int victim = -1;
+    Clock::time_point submitted, completed;
+    bool complete = false;
+    cgmli_solve_report report{};
+    // prior of a request with a victim
+    int rank = 0, cols = 0, numBlocks = 0;
+    std::vector<int> kinds, index;
+    std::vector<double> reference, A, r0;
+};
+
+// Device bytes a window occupies in a batch (observation, landmark and dense
+// per-window arrays, both state buffers, the staged rows and the marginalization).
+long long footprint(const cgmli_window& w) {
+    const long long F = w.num_observations, L = w.num_landmarks, K = w.num_keyframes;
+    const long long ncal = (w.estimate_extrinsics ? 6ll * w.num_extrinsics : 0) + (w.estimate_td ? 1 : 0);
+    const long long Nr = 15 * K + ncal, Npc = 6 * K + ncal, m = 15 * K + 6ll * w.num_extrinsics + 1;
+    return F * (120 + 448) + L * (160 + 8 * (6 * 12 + 7)) + 8 * (3 * Nr * Nr + Npc * Npc + 4 * m * m) + 4096;
+}
+}  // namespace
+
+struct cgmli_server {
+    cgmli_server_options opt{};
+    cgmli_solver* solver[2] = {nullptr, nullptr};
+    std::mutex mu;
+    std::condition_variable work, done;
+    std::deque<Request*> queue;
+    std::unordered_map<long long, std::unique_ptr<Request>> requests;
+    long long nextTicket = 1;
+    bool stopping = false;
+    std::thread worker;
+
+    struct Batch {
+        std::vector<Request*> reqs;
+        std::vector<cgmli_window> windows;
+        int solver = 0;
+        bool marg = false;
+        int status = CGMLI_OK;
+    };
+
+    // Launches a batch on solver s (asynchronous on its stream).
+    void launch(Batch& b) {
+        cgmli_solver* S = solver[b.solver];
+        const int n = (int)b.reqs.size();
+        b.windows.resize(n);
+        std::vector<int> victims(n, -1);
+        for (int i = 0; i < n; ++i) {
+            b.windows[i] = b.reqs[i]->window;
+            victims[i] = b.reqs[i]->victim;
+            b.marg = b.marg || victims[i] >= 0;
+        }
+        b.status = cgmli_solver_set_windows(S, b.windows.data(), n);
+        if (b.status == CGMLI_OK) b.status = cgmli_solver_solve(S, opt.iterations);
+        if (b.status == CGMLI_OK && b.marg) b.status = cgmli_solver_marginalize(S, victims.data(), opt.policy);
+    }
+
+    // Waits for a launched batch and records its results.
+    void complete(Batch& b) {
+        cgmli_solver* S = solver[b.solver];
+        const int n = (int)b.reqs.size();
+        std::vector<cgmli_solve_report> reps(n);
+        int st = b.status;
+        if (st == CGMLI_OK) st = cgmli_solver_synchronize(S);
+        if (st == CGMLI_OK) st = cgmli_solver_read_states(S, b.windows.data(), n);
+        if (st == CGMLI_OK) st = cgmli_solver_read_reports(S, reps.data(), n);
+        for (int i = 0; i < n; ++i) {
+            Request* r = b.reqs[i];
+            if (st != CGMLI_OK) {
+                r->report = cgmli_solve_report{};
+                r->report.status = st;
+                continue;
+            }
+            r->report = reps[i];
+            if (r->victim >= 0 && r->report.status == CGMLI_OK) {
+                int rank = 0, cols = 0, nb = 0;
+                int ps = cgmli_solver_read_prior(S, i, &rank, &cols, &nb, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+                if (ps == CGMLI_OK) {
+                    r->kinds.resize(nb);
+                    r->index.resize(nb);
+                    r->reference.resize(9ull * nb + 1);
+                    r->A.resize((size_t)rank * cols);
+                    r->r0.resize(rank);
+                    ps = cgmli_solver_read_prior(S, i, &rank, &cols, &nb, r->kinds.data(), r->index.data(), r->reference.data(),
+                                                 r->A.data(), r->r0.data(), nullptr);
+                }
+                if (ps != CGMLI_OK) r->report.status = ps;
+                r->rank = rank;
+                r->cols = cols;
+                r->numBlocks = nb;
+            }
+        }
+        const auto now = Clock::now();
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            for (Request* r : b.reqs) {
+                r->completed = now;
+                r->complete = true;
+            }
+        }
+        done.notify_all();
+        b.reqs.clear();
+    }
+
+    void run() {
+        Batch inflight;
+        bool haveInflight = false;
+        int cur = 0;
+        const long long budget = opt.memory_budget_bytes;
+        for (;;) {
+            Batch next;
+            {
+                std::unique_lock<std::mutex> lock(mu);
+                if (!haveInflight) work.wait(lock, [&] { return stopping || !queue.empty(); });
+                if (queue.empty() && !haveInflight && stopping) return;
+                long long bytes = 0;
+                while (!queue.empty() && (int)next.reqs.size() < opt.max_batch_windows) {
+                    const long long f = footprint(queue.front()->window);
+                    if (!next.reqs.empty() && bytes + f > budget) break;
+                    bytes += f;
+                    next.reqs.push_back(queue.front());
+                    queue.pop_front();
+                }
+            }
+            if (!next.reqs.empty()) {
+                next.solver = cur;
+                launch(next);
+                cur ^= 1;
+            }
+            if (haveInflight) complete(inflight);
+            haveInflight = !next.reqs.empty();
+            if (haveInflight) inflight = std::move(next);
+        }
+    }
+};
+
+using cgmli::setLastError;
+
+extern "C" {
+
+int cgmli_server_create(const cgmli_server_options* options, cgmli_server** out) {
+    if (!options || !out) return setLastError(CGMLI_E_INVALID, "server: null options or output handle");
+    *out = nullptr;
+    if (options->iterations < 1) return setLastError(CGMLI_E_INVALID, "server: iterations < 1");
+    if (options->policy != CGMLI_MARGIN_OLD && options->policy != CGMLI_MARGIN_SECOND_NEW)
+        return setLastError(CGMLI_E_INVALID, "server: unknown marginalization policy");
+    auto* s = new cgmli_server();
+    s->opt = *options;
+    if (s->opt.max_batch_windows <= 0) s->opt.max_batch_windows = 512;
+    if (s->opt.memory_budget_bytes <= 0) s->opt.memory_budget_bytes = 40ll << 30;
+    for (int k = 0; k < 2; ++k) {
+        const int st = cgmli_solver_create(options->device, nullptr, &s->solver[k]);
+        if (st != CGMLI_OK) {
+            for (auto* sv : s->solver) cgmli_solver_destroy(sv);
+            delete s;
+            return st;
+        }
+    }
+    s->worker = std::thread([s] { s->run(); });
+    *out = s;
+    return CGMLI_OK;
+}
+
+void cgmli_server_destroy(cgmli_server* s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->stopping = true;
+    }
+    s->work.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    for (auto* sv : s->solver) cgmli_solver_destroy(sv);
+    delete s;
+}
+
+namespace {
+int submitAt(cgmli_server* s, cgmli_window* window, int victim_kf, Clock::time_point arrival, long long* ticket);
+}
+
+int cgmli_server_submit(cgmli_server* s, cgmli_window* window, int victim_kf, long long* ticket) {
+    return submitAt(s, window, victim_kf, Clock::now(), ticket);
+}
+
+namespace {
+int submitAt(cgmli_server* s, cgmli_window* window, int victim_kf, Clock::time_point arrival, long long* ticket) {
+    if (!s || !window || !ticket) return setLastError(CGMLI_E_INVALID, "server: null server, window or ticket");
+    std::string why;
+    const int st = cgmli::validateWindow(*window, 0, why);
+    if (st != CGMLI_OK) return setLastError(st, why.c_str());
+    if (victim_kf < -1 || victim_kf >= window->num_keyframes) return setLastError(CGMLI_E_INVALID, "server: victim keyframe out of range");
+    auto r = std::make_unique<Request>();
+    r->window = *window;
+    r->victim = victim_kf;
+    r->submitted = arrival;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        if (s->stopping) return setLastError(CGMLI_E_INVALID, "server: stopping");
+        r->ticket = s->nextTicket++;
+        *ticket = r->ticket;
+        s->queue.push_back(r.get());
+        s->requests.emplace(r->ticket, std::move(r));
+    }
+    s->work.notify_one();
+    return CGMLI_OK;
+}
+}  // namespace
+
+int cgmli_server_replay(cgmli_server* s, cgmli_window* const* windows, const int* victims, const double* arrival_s, int count,
+                        double* latency_ms, int* status, double* span_s) {
+    if (!s || !windows || !victims || !arrival_s || !latency_ms || !status || count < 1)
+        return setLastError(CGMLI_E_INVALID, "server replay: null arrays or empty trace");
+    for (int i = 0; i < count; ++i)
+        if (!windows[i] || (i > 0 && arrival_s[i] < arrival_s[i - 1]))
+            return setLastError(CGMLI_E_INVALID, "server replay: null window or arrival times not sorted");
+    std::vector<long long> tickets(count, 0);
+    std::mutex qmu;
+    std::condition_variable qcv;
+    int submitted = 0;
+    bool failed = false;
+    std::unordered_map<const cgmli_window*, int> lastUse;  // window -> last request using it
+    std::vector<char> finished(count, 0);
+    std::mutex fmu;
+    std::condition_variable fcv;
+    // collector: waits for the requests in submission order
+    std::thread collector([&] {
+        for (int i = 0; i < count; ++i) {
+            long long t = 0;
+            {
+                std::unique_lock<std::mutex> lock(qmu);
+                qcv.wait(lock, [&] { return submitted > i || failed; });
+                if (submitted <= i) break;
+                t = tickets[i];
+            }
+            cgmli_solve_report rep{};
+            double ms = 0;
+            cgmli_server_poll(s, t, 1, &rep, &ms);
+            latency_ms[i] = ms;
+            status[i] = rep.status;
+            cgmli_server_release(s, t);
+            {
+                std::lock_guard<std::mutex> lock(fmu);
+                finished[i] = 1;
+            }
+            fcv.notify_all();
+        }
+    });
+    const auto t0 = Clock::now();
+    int rc = CGMLI_OK;
+    for (int i = 0; i < count; ++i) {
+        const auto due = t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(arrival_s[i]));
+        std::this_thread::sleep_until(due);
+        // a window is reused only after its earlier request completed
+        auto it = lastUse.find(windows[i]);
+        if (it != lastUse.end()) {
+            const int prev = it->second;
+            std::unique_lock<std::mutex> lock(fmu);
+            fcv.wait(lock, [&] { return finished[prev] != 0; });
+        }
+        lastUse[windows[i]] = i;
+        long long t = 0;
+        rc = submitAt(s, windows[i], victims[i], due, &t);
+        {
+            std::lock_guard<std::mutex> lock(qmu);
+            if (rc != CGMLI_OK) { failed = true; }
+            else { tickets[i] = t; ++submitted; }
+        }
+        qcv.notify_all();
+        if (rc != CGMLI_OK) break;
+    }
+    collector.join();
+    if (span_s) *span_s = std::chrono::duration<double>(Clock::now() - t0).count();
+    return rc;
+}
+
+int cgmli_server_poll(cgmli_server* s, long long ticket, int wait, cgmli_solve_report* report, double* latency_ms) {
+    if (!s) return setLastError(CGMLI_E_INVALID, "server: null server");
+    std::unique_lock<std::mutex> lock(s->mu);
+    auto it = s->requests.find(ticket);
+    if (it == s->requests.end()) return setLastError(CGMLI_E_INVALID, "server: unknown ticket");
+    Request* r = it->second.get();
+    if (!r->complete) {
+        if (!wait) return CGMLI_E_PENDING;
+        s->done.wait(lock, [&] { return r->complete; });
+    }
+    if (report) *report = r->report;
+    if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->completed - r->submitted).count();
+    return CGMLI_OK;
+}
+
+int cgmli_server_read_prior(cgmli_server* s, long long ticket, int* rank, int* cols, int* num_blocks, int* block_kind,
+                            int* block_index, double* reference, double* A, double* r0) {
+    if (!s || !rank || !cols || !num_blocks) return setLastError(CGMLI_E_INVALID, "server: null server or size outputs");
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->requests.find(ticket);
+    if (it == s->requests.end()) return setLastError(CGMLI_E_INVALID, "server: unknown ticket");
+    const Request* r = it->second.get();
+    if (!r->complete) return CGMLI_E_PENDING;
+    if (r->victim < 0) return setLastError(CGMLI_E_INVALID, "server: request had no victim keyframe");
+    if (r->report.status != CGMLI_OK) return setLastError(r->report.status, "server: request failed");
+    *rank = r->rank;
+    *cols = r->cols;
+    *num_blocks = r->numBlocks;
+    if (block_kind) std::copy(r->kinds.begin(), r->kinds.end(), block_kind);
+    if (block_index) std::copy(r->index.begin(), r->index.end(), block_index);
+    if (reference) {
+        size_t amb = 0;
+        for (int k : r->kinds) amb += k == CGMLI_PRIOR_SPEED_BIAS ? 9 : k == CGMLI_PRIOR_TIME_OFFSET ? 1 : 7;
+        std::copy(r->reference.begin(), r->reference.begin() + amb, reference);
+    }
+    if (A) std::copy(r->A.begin(), r->A.end(), A);
+    if (r0) std::copy(r->r0.begin(), r->r0.end(), r0);
+    return CGMLI_OK;
+}
+
+int cgmli_server_release(cgmli_server* s, long long ticket) {
+    if (!s) return setLastError(CGMLI_E_INVALID, "server: null server");
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->requests.find(ticket);
+    if (it == s->requests.end()) return setLastError(CGMLI_E_INVALID, "server: unknown ticket");
+    if (!it->second->complete) return setLastError(CGMLI_E_PENDING, "server: request not complete");
+    s->requests.erase(it);
+    return CGMLI_OK;
+}
+
+}  // extern "C"

@@ -34,24 +34,6 @@ namespace {
 int tangentOf(int kind) { return kind == CGMLI_PRIOR_SPEED_BIAS ? 9 : kind == CGMLI_PRIOR_TIME_OFFSET ? 1 : 6; }
 int ambientOf(int kind) { return kind == CGMLI_PRIOR_SPEED_BIAS ? 9 : kind == CGMLI_PRIOR_TIME_OFFSET ? 1 : 7; }
 
-// Runs fn(i) for i in [0, n) on up to `threads` host threads.
-template <class Fn>
-void parallelFor(int n, int threads, Fn&& fn) {
-    if (threads <= 1 || n <= 1) {
-        for (int i = 0; i < n; ++i) fn(i);
-        return;
-    }
-    std::atomic<int> next{0};
-    auto body = [&] {
-        for (int i = next++; i < n; i = next++) fn(i);
-    };
-    std::vector<std::thread> pool;
-    const int t = std::min(threads, n);
-    for (int k = 1; k < t; ++k) pool.emplace_back(body);
-    body();
-    for (auto& th : pool) th.join();
-}
-
 // Landmarks per warp run: enough runs to fill the GPU, long runs for large batches.
 int runLength(long long totalLm) {
     const long long targetRuns = 148ll * 6 * 4;

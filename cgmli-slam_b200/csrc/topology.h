@@ -10,15 +10,37 @@
 #pragma once
 #include <cuda_runtime.h>  // int2 / int4
 
+#include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/cgmli_backend.h"
 #include "backend_internal.h"
 
 namespace cgmli {
+
+// Runs fn(i) for i in [0, n) on up to `threads` host threads (0: all cores).
+template <class Fn>
+void parallelFor(int n, int threads, Fn&& fn) {
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    if (threads <= 1 || n <= 1) {
+        for (int i = 0; i < n; ++i) fn(i);
+        return;
+    }
+    std::atomic<int> next{0};
+    auto body = [&] {
+        for (int i = next++; i < n; i = next++) fn(i);
+    };
+    std::vector<std::thread> pool;
+    const int t = std::min(threads, n);
+    for (int k = 1; k < t; ++k) pool.emplace_back(body);
+    body();
+    for (auto& th : pool) th.join();
+}
 
 // Page-locked host memory for the arrays uploaded to (and read back from) the
 // device, so that the copies run at DMA speed; plain memory where no CUDA

@@ -47,7 +47,8 @@ enum {
     CGMLI_E_UNSUPPORTED = 7,  /* layout outside what the kernels implement */
     CGMLI_E_NO_STEP = 8,      /* LM found no acceptable step */
     CGMLI_E_LIMIT = 9,        /* size beyond a documented maximum */
-    CGMLI_E_COST_MISMATCH = 10 /* relinearized cost disagrees with accepted trial */
+    CGMLI_E_COST_MISMATCH = 10,/* relinearized cost disagrees with accepted trial */
+    CGMLI_E_PENDING = 11       /* served request not complete yet */
 };
 
 enum { CGMLI_PRECISION_FP64 = 0, CGMLI_PRECISION_MIXED = 1 };
@@ -244,6 +245,55 @@ int cgmli_marg_subtract(const double *coupling, const double *solution, int elim
  * serialized by the caller. */
 #define CGMLI_MARG_EIGEN_NOALLOC_MAX_N 256
 int cgmli_marg_eigen_noalloc(const double *H, int n, double *eigenvalues, double *eigenvectors, void *stream);
+
+/* ---- Served mode: continuous batching of window solves ---------------------
+ * Windows from many rigs arrive as independent requests.  A request is one
+ * window (its arrays are the caller's and must stay valid and unmodified until
+ * the request completes; the solved states are written back into them),
+ * solved with options.iterations damped LM iterations and, when victim_kf >= 0,
+ * marginalized (options.policy).  A scheduler thread admits queued requests in
+ * arrival order into the next batch while the batch stays within
+ * max_batch_windows windows and its estimated device footprint within
+ * memory_budget_bytes; the host build and upload of one batch overlap the
+ * device work of the previous one (two solvers on two streams), so requests
+ * that arrive while the GPU is busy join the next batch.  Every window of a
+ * batch is solved exactly as alone (same arithmetic up to the order of FP64
+ * reductions).  The reference solves one window per backend step and has no
+ * served mode; this is the batched form of its solveVisualSchur +
+ * Marginalizer::compute. */
+typedef struct cgmli_server_options {
+    int device;
+    int max_batch_windows;          /* 0: 512 */
+    long long memory_budget_bytes;  /* 0: 40 GiB */
+    int iterations;                 /* LM iterations per request, >= 1 */
+    int policy;                     /* CGMLI_MARGIN_OLD or _SECOND_NEW for requests with a victim */
+} cgmli_server_options;
+typedef struct cgmli_server cgmli_server;
+
+int cgmli_server_create(const cgmli_server_options *options, cgmli_server **out);
+/* Completes every submitted request, then releases the server. */
+void cgmli_server_destroy(cgmli_server *server);
+/* Queues a request; the window is validated here (CGMLI_E_INVALID / _LIMIT). */
+int cgmli_server_submit(cgmli_server *server, cgmli_window *window, int victim_kf, long long *ticket);
+/* CGMLI_OK with the report (status of the solve, or of the marginalization when
+ * that failed) and the submit-to-completion latency once the request is
+ * complete; CGMLI_E_PENDING while it is not and wait == 0.  wait != 0 blocks. */
+int cgmli_server_poll(cgmli_server *server, long long ticket, int wait, cgmli_solve_report *report, double *latency_ms);
+/* Prior of a completed request with a victim, laid out as cgmli_solver_read_prior
+ * (sizes first with NULL buffers). */
+int cgmli_server_read_prior(cgmli_server *server, long long ticket, int *rank, int *cols, int *num_blocks, int *block_kind,
+                            int *block_index, double *reference, double *A, double *r0);
+/* Frees a completed request's record. */
+int cgmli_server_release(cgmli_server *server, long long ticket);
+/* Replays a request trace from a host thread (load testing): request i submits
+ * windows[i] with victims[i] at arrival_s[i] seconds (non-decreasing) after the
+ * call starts; latency_ms[i] is measured from that scheduled arrival to the
+ * completion, so queueing delay is included; status[i] is the request's solve
+ * status; span_s the time from the start to the last completion.  A window
+ * listed again is resubmitted only after its earlier request completed.
+ * Returns after every submitted request completed. */
+int cgmli_server_replay(cgmli_server *server, cgmli_window *const *windows, const int *victims, const double *arrival_s,
+                        int count, double *latency_ms, int *status, double *span_s);
 
 #ifdef __cplusplus
 }
