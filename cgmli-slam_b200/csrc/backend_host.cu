@@ -31,7 +31,7 @@ int launchIteration(const DevBatch& B, const LaunchPlan& P, int refinement, int 
                     cudaStream_t s, LaunchHook hook, void* ctx);
 int launchLmInit(const DevBatch& B, double lambda0, cudaStream_t s);
 size_t margVisualSmemBytes(int maxNc);
-cudaError_t configureMarginalization(size_t visualSmem, int maxNr, int numWindows, long long* eigenSmem);
+cudaError_t configureMarginalization(size_t visualSmem, int maxNr, int maxFastNr, long long* eigenSmem, long long* fastSmem);
 int launchMarginalization(const DevBatch& B, const MargBatch& M, size_t visualSmem, cudaStream_t s);
 void launchDenseEigen(const double* H, int n, double* work, double* evals, double* evecs, int* status, cudaStream_t s);
 void launchDensePsd(const double* evals, const double* U, const double* rhs, int n, int columns, double absCut, double relCut,
@@ -131,7 +131,7 @@ struct cgmli_solver {
     std::vector<std::vector<int>> sepKind, sepIndex;  // separator blocks per window (window-local index)
     DArray<MargWin> dMargWin;
     DArray<MargElim> dMargElim;
-    DArray<int> margCols, margObsMap, margPoseCol, margSbCol, margExtCol, margRank, margStatus;
+    DArray<int> margCols, margObsMap, margPoseCol, margSbCol, margExtCol, margRank, margStatus, margFast;
     DArray<double> margH, margB, margSepH, margSepV, margSepB, margEvals, margA, margR0, margX, margMaxD, margStats;
     MargBatch MB{};
     bool haveMarg = false;
@@ -198,7 +198,7 @@ struct cgmli_solver {
         dPairChunks.release(); dSchurChunks.release(); obLm.release(); keyOrder.release(); keyRows.release(); sch.release();
         snapPose.release(); snapSb.release(); snapExt.release(); snapTd.release(); snapRho.release();
         dMargWin.release(); dMargElim.release();
-        DArray<int>* mi[] = {&margCols, &margObsMap, &margPoseCol, &margSbCol, &margExtCol, &margRank, &margStatus};
+        DArray<int>* mi[] = {&margCols, &margObsMap, &margPoseCol, &margSbCol, &margExtCol, &margRank, &margStatus, &margFast};
         for (auto* a : mi) a->release();
         DArray<double>* md[] = {&margH, &margB, &margSepH, &margSepV, &margSepB, &margEvals, &margA, &margR0, &margX, &margMaxD, &margStats};
         for (auto* a : md) a->release();
@@ -619,6 +619,7 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
         mw.imu[0] = mw.imu[1] = -1;
         mw.tdCol = -1;
         mw.huber = d.huber;
+        mw.hasPrior = d.priorRank > 0;
         std::fill(&poseCol[d.kf0], &poseCol[d.kf0] + d.K, -1);
         std::fill(&sbCol[d.kf0], &sbCol[d.kf0] + d.K, -1);
         std::fill(&extCol[d.ext0], &extCol[d.ext0] + d.E, -1);
@@ -747,10 +748,13 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
     });
     cudaStream_t st = S->stream;
     const size_t smem = margVisualSmemBytes(std::max(maxNc, 1));
-    int maxNr = 1;
-    for (const auto& mw : mwv) maxNr = std::max(maxNr, mw.nr);
-    long long eigenSmem = 0;
-    CK(configureMarginalization(smem, maxNr, W, &eigenSmem));
+    int maxNr = 1, maxFastNr = 0;
+    for (const auto& mw : mwv) {
+        maxNr = std::max(maxNr, mw.nr);
+        if (mw.hasPrior) maxFastNr = std::max(maxFastNr, mw.nr);
+    }
+    long long eigenSmem = 0, fastSmem = 0;
+    CK(configureMarginalization(smem, maxNr, maxFastNr, &eigenSmem, &fastSmem));
     CK(S->dMargWin.upload(mwv, st));
     CK(S->dMargElim.upload(elims, st));
     CK(S->margCols.upload(cols, st));
@@ -763,7 +767,7 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
     CK(S->margH.reserve(H0)); CK(S->margB.reserve(vec0)); CK(S->margSepH.reserve(sep0)); CK(S->margSepV.reserve(sep0));
     CK(S->margSepB.reserve(vec0)); CK(S->margEvals.reserve(vec0)); CK(S->margA.reserve(sep0)); CK(S->margR0.reserve(vec0));
     CK(S->margX.reserve(x0)); CK(S->margMaxD.reserve(W)); CK(S->margStats.reserve(4ll * W));
-    CK(S->margRank.reserve(W)); CK(S->margStatus.reserve(W));
+    CK(S->margRank.reserve(W)); CK(S->margStatus.reserve(W)); CK(S->margFast.reserve(W));
     if (H0) CK(cudaMemsetAsync(S->margH.p, 0, H0 * sizeof(double), st));
     if (vec0) CK(cudaMemsetAsync(S->margB.p, 0, vec0 * sizeof(double), st));
     CK(cudaMemsetAsync(S->margMaxD.p, 0, W * sizeof(double), st));
@@ -775,11 +779,13 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
     M.numWindows = W;
     M.numElim = (int)elims.size();
     M.eigenSmem = eigenSmem;
+    M.fastSmem = fastSmem;
     M.win = S->dMargWin.p; M.elim = S->dMargElim.p; M.cols = S->margCols.p; M.obsMap = S->margObsMap.p;
     M.poseCol = S->margPoseCol.p; M.sbCol = S->margSbCol.p; M.extCol = S->margExtCol.p;
     M.H = S->margH.p; M.b = S->margB.p; M.sepH = S->margSepH.p; M.sepV = S->margSepV.p; M.sepB = S->margSepB.p;
     M.evals = S->margEvals.p; M.A = S->margA.p; M.r0 = S->margR0.p; M.X = S->margX.p;
     M.maxD = S->margMaxD.p; M.stats = S->margStats.p; M.rank = S->margRank.p; M.status = S->margStatus.p;
+    M.fast = S->margFast.p;
     S->margWin = mwv;
     S->margSepTotal = sep0;
     S->margVecTotal = vec0;

@@ -102,16 +102,18 @@ struct MargWin {
     int elim0, nElim;       // eliminated landmarks in MargBatch::elim
     int imu[2];             // consumed IMU factors (global index) or -1
     int tdCol;              // column of td or -1
+    int hasPrior;           // the window carries a prior (gauge fixed: the full-rank fast path is tried)
     long long H0;           // m * m
     long long sep0;         // nr * nr: separator information, eigenvectors, A
     long long vec0;         // m
-    long long x0;           // 2 * 15 * (nr + 1): victim solve scratch
+    long long x0;           // 2 * 15 * (nr + 1): victim solve scratch, then the fast path's vectors
     double huber;
 };
 struct MargElim { int lm, win, nc, col0, obs0; };  // device landmark, window, local columns, offsets
 struct MargBatch {
     int numWindows, numElim;
     long long eigenSmem;  // dynamic shared memory of the eigen CTA (packed separator, eigenvectors when they fit)
+    long long fastSmem;   // dynamic shared memory of the full-rank fast path
     const MargWin* win;
     const MargElim* elim;
     const int* cols;     // local column -> marginalization column
@@ -122,6 +124,7 @@ struct MargBatch {
     double* maxD;        // per window: largest eliminated landmark information
     double* stats;       // 4 per window: robust cost, whitened |r|^2, eliminated reduction, cutoff
     int* rank; int* status;
+    int* fast;           // per window: 1 when the full-rank fast path formed the prior
 };
 
 // Called before (phase 0) and after (phase 1) every kernel launch of an

@@ -639,12 +639,194 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_victim(MargBatch M) {
     if (threadIdx.x == 0) M.stats[4 * w + 2] += reduction;
 }
 
+// ---------------------------------------------------------------------------------------
+// Full-rank fast path, one CTA per window with the separator information E in
+// shared memory (n <= kFastMaxN).  When every eigenvalue of E exceeds the
+// cutoff max(1e-12, 1e-9 lambda_max) nothing is cut, and any square root gives
+// the same prior: with E = L L^T (Cholesky), A = L^T and r0 = L^{-1} b satisfy
+// A^T A = E and A^T r0 = b, exactly the prior sqrt(lambda) u^T, u^T b /
+// sqrt(lambda) over all eigenpairs.  The eigenvalue facts come from a
+// Householder tridiagonalization T of E: lambda_max by Sturm-sequence
+// multisection on T (the number of eigenvalues below x is the number of
+// negative pivots of T - x I), and the rank test as a single count at twice
+// the cutoff.  Windows without a prior (gauge freedom, rank deficient) and
+// windows that fail the test are left to k_marg_eigen.
+constexpr int kFastMaxN = 160;
+__host__ __device__ constexpr size_t fastSmemBytes(int n) { return sizeof(double) * ((size_t)n * n + 5 * (size_t)n); }
+
+// Number of eigenvalues of the symmetric tridiagonal (d, e) below x, e[i]
+// coupling i and i + 1.
+__device__ int sturmCount(const double* d, const double* e, int n, double x, double pivmin) {
+    int c = 0;
+    double q = d[0] - x;
+    if (fabs(q) < pivmin) q = -pivmin;
+    if (q < 0) ++c;
+    for (int i = 1; i < n; ++i) {
+        q = d[i] - x - e[i - 1] * e[i - 1] / q;
+        if (fabs(q) < pivmin) q = -pivmin;
+        if (q < 0) ++c;
+    }
+    return c;
+}
+
+__global__ void __launch_bounds__(kMargThreads) k_marg_fast(MargBatch M) {
+    const int w = blockIdx.x;
+    const MargWin mw = M.win[w];
+    const int n = mw.nr;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+    if (tid == 0) M.fast[w] = 0;
+    if (mw.m == 0 || n == 0 || n > kFastMaxN || !mw.hasPrior || M.status[w] != CGMLI_OK) return;
+    extern __shared__ double fsm[];
+    double* S = fsm;          // n x n row-major
+    double* v = S + n * n;
+    double* p = v + n;
+    double* wv = p + n;
+    double* d = wv + n;
+    double* e = d + n;
+    __shared__ double sc[4];
+    const double* E = M.sepH + mw.sep0;
+    for (int t = tid; t < n * n; t += blockDim.x) S[t] = E[t];
+    __syncthreads();
+    // Householder tridiagonalization (eigenvalues only)
+    for (int k = 0; k + 2 < n; ++k) {
+        const int m = n - k - 1;
+        if (warp == 0) {
+            double sigma = 0;
+            for (int i = lane; i < m; i += 32) {
+                const double x = S[(k + 1 + i) * n + k];
+                v[i] = x;
+                sigma += x * x;
+            }
+            sigma = mWarpSum(sigma);
+            __syncwarp();
+            if (lane == 0) {
+                d[k] = S[k * n + k];
+                if (sigma == 0.0) {
+                    e[k] = 0.0;
+                    sc[0] = 0.0;
+                } else {
+                    const double x0 = v[0];
+                    const double alpha = x0 >= 0 ? -sqrt(sigma) : sqrt(sigma);
+                    e[k] = alpha;
+                    v[0] = x0 - alpha;
+                    sc[0] = 1.0 / (sigma - x0 * alpha);
+                }
+            }
+        }
+        __syncthreads();
+        const double tau = sc[0];
+        if (tau == 0.0) {
+            __syncthreads();  // every warp has read sc before warp 0 writes the next column's
+            continue;
+        }
+        for (int i = warp; i < m; i += nw) {
+            const double* row = S + (k + 1 + i) * n + (k + 1);
+            double sum = 0;
+            for (int j = lane; j < m; j += 32) sum += row[j] * v[j];
+            sum = mWarpSum(sum);
+            if (lane == 0) p[i] = tau * sum;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            double pv = 0;
+            for (int i = lane; i < m; i += 32) pv += p[i] * v[i];
+            const double K = 0.5 * tau * mWarpSum(pv);
+            for (int i = lane; i < m; i += 32) wv[i] = p[i] - K * v[i];
+        }
+        __syncthreads();
+        for (int i = warp; i < m; i += nw) {
+            double* row = S + (k + 1 + i) * n + (k + 1);
+            const double vi = v[i], wi = wv[i];
+            for (int j = lane; j < m; j += 32) row[j] -= vi * wv[j] + wi * v[j];
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        if (n >= 2) {
+            d[n - 2] = S[(n - 2) * n + (n - 2)];
+            e[n - 2] = S[(n - 1) * n + (n - 2)];
+        }
+        d[n - 1] = S[(n - 1) * n + (n - 1)];
+        e[n - 1] = 0.0;
+        double lo = INFINITY, hi = -INFINITY, emax = 0;
+        for (int i = 0; i < n; ++i) {
+            const double r = fabs(e[i]) + (i > 0 ? fabs(e[i - 1]) : 0.0);
+            lo = fmin(lo, d[i] - r);
+            hi = fmax(hi, d[i] + r);
+            emax = fmax(emax, e[i] * e[i]);
+        }
+        sc[0] = lo;
+        sc[1] = hi;
+        sc[2] = fmax(1e-300, 1e-30 * emax);  // pivot guard of the Sturm counts
+    }
+    __syncthreads();
+    // lambda_max: the point where the Sturm count reaches n, by multisection
+    double lo = sc[0], hi = sc[1];
+    const double pivmin = sc[2];
+    const int T = blockDim.x;
+    for (int round = 0; round < 8 && hi - lo > 1e-15 * fmax(fabs(hi), fabs(lo)); ++round) {
+        const double x = lo + (hi - lo) * (tid + 1) / (T + 1);
+        const int below = __syncthreads_count(sturmCount(d, e, n, x, pivmin) < n);  // points still below lambda_max
+        const double nlo = below > 0 ? lo + (hi - lo) * below / (T + 1) : lo;
+        const double nhi = below < T ? lo + (hi - lo) * (below + 1) / (T + 1) : hi;
+        lo = nlo;
+        hi = nhi;
+    }
+    const double lmax = hi;
+    const double cutoff = fmax(1e-12, 1e-9 * fmax(0.0, lmax));
+    if (tid == 0) sc[3] = sturmCount(d, e, n, 2.0 * cutoff, pivmin) == 0 ? 1.0 : 0.0;
+    __syncthreads();
+    if (sc[3] == 0.0) return;  // an eigenvalue within twice the cutoff: eigen path
+    // Cholesky E = L L^T (lower triangle of S)
+    for (int t = tid; t < n * n; t += blockDim.x) S[t] = E[t];
+    __syncthreads();
+    for (int k = 0; k < n; ++k) {
+        const double dkk = S[k * n + k];
+        if (!(dkk > 0)) return;  // not positive definite after all: eigen path (uniform)
+        const double lkk = sqrt(dkk);
+        for (int i = k + 1 + tid; i < n; i += blockDim.x) p[i] = S[i * n + k] / lkk;
+        __syncthreads();
+        if (tid == 0) S[k * n + k] = lkk;
+        for (int i = k + 1 + tid; i < n; i += blockDim.x) S[i * n + k] = p[i];
+        for (int i = k + 1 + warp; i < n; i += nw) {
+            const double lik = p[i];
+            for (int j = k + 1 + lane; j <= i; j += 32) S[i * n + j] -= lik * p[j];
+        }
+        __syncthreads();
+    }
+    // r0 = L^{-1} b (column sweep by one warp), A = L^T
+    const double* bs = M.sepB + mw.vec0;
+    if (warp == 0) {
+        for (int i = lane; i < n; i += 32) v[i] = bs[i];
+        __syncwarp();
+        for (int k = 0; k < n; ++k) {
+            const double yk = v[k] / S[k * n + k];
+            __syncwarp();
+            if (lane == 0) v[k] = yk;
+            for (int i = k + 1 + lane; i < n; i += 32) v[i] -= S[i * n + k] * yk;
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    double* A = M.A + mw.sep0;
+    double* r0 = M.r0 + mw.vec0;
+    for (int i = warp; i < n; i += nw)
+        for (int k = lane; k < n; k += 32) A[(long long)i * n + k] = k >= i ? S[k * n + i] : 0.0;
+    for (int i = tid; i < n; i += blockDim.x) r0[i] = v[i];
+    if (tid == 0) {
+        M.rank[w] = n;
+        M.stats[4 * w + 3] = cutoff;
+        M.fast[w] = 1;
+    }
+}
+
 // Eigendecomposition of the separator information and the square-root prior,
 // rows in ascending eigenvalue order.
 __global__ void __launch_bounds__(kEigenThreads) k_marg_eigen(MargBatch M) {
     const int w = blockIdx.x;
     const MargWin mw = M.win[w];
     const int nr = mw.nr;
+    if (M.fast[w]) return;  // prior formed by k_marg_classify
     if (mw.m == 0 || nr == 0 || M.status[w] != CGMLI_OK) {
         if (threadIdx.x == 0) M.rank[w] = 0;
         return;
@@ -780,9 +962,13 @@ size_t margVisualSmemBytes(int maxNc) {
 // Sets the dynamic shared memory limits of the marginalization kernels for a
 // batch whose largest separator has maxNr columns; returns the eigen CTA's
 // dynamic shared memory in eigenSmem.
-cudaError_t configureMarginalization(size_t visualSmem, int maxNr, int numWindows, long long* eigenSmem) {
+cudaError_t configureMarginalization(size_t visualSmem, int maxNr, int maxFastNr, long long* eigenSmem, long long* fastSmem) {
     cudaError_t e = cudaFuncSetAttribute(k_marg_visual, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)visualSmem);
     if (e != cudaSuccess) return e;
+    *fastSmem = maxFastNr > 0 ? (long long)fastSmemBytes(maxFastNr < kFastMaxN ? maxFastNr : kFastMaxN) : 0;
+    if ((e = cudaFuncSetAttribute(k_marg_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fastSmemBytes(kFastMaxN))) !=
+        cudaSuccess)
+        return e;
     int dev = 0, optin = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess) return e;
@@ -792,7 +978,6 @@ cudaError_t configureMarginalization(size_t visualSmem, int maxNr, int numWindow
     // eigenvectors in shared memory too when they fit
     const long long n = maxNr, want = 8 * (n * (n + 1) / 2 + n * n), packedOnly = 8 * (n * (n + 1) / 2);
     long long use = want <= avail ? want : (packedOnly <= avail ? packedOnly : 0);
-    (void)numWindows;
     if (use < 0) use = 0;
     *eigenSmem = use;
     return cudaFuncSetAttribute(k_marg_eigen, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)use);
@@ -808,8 +993,9 @@ int launchMarginalization(const DevBatch& B, const MargBatch& M, size_t visualSm
     }
     k_marg_retained<<<M.numWindows, 256, 0, s>>>(B, M);
     k_marg_victim<<<M.numWindows, kMargThreads, 0, s>>>(M);
+    k_marg_fast<<<M.numWindows, kMargThreads, (size_t)M.fastSmem, s>>>(M);
     k_marg_eigen<<<M.numWindows, kEigenThreads, (size_t)M.eigenSmem, s>>>(M);
-    return n + 3;
+    return n + 4;
 }
 void launchDenseEigen(const double* H, int n, double* work, double* evals, double* evecs, int* status, cudaStream_t s) {
     k_dense_eigen<<<1, kMargThreads, 0, s>>>(H, n, work, evals, evecs, status);
