@@ -31,7 +31,9 @@ int launchIteration(const DevBatch& B, const LaunchPlan& P, int refinement, int 
                     cudaStream_t s, LaunchHook hook, void* ctx);
 int launchLmInit(const DevBatch& B, double lambda0, cudaStream_t s);
 size_t margVisualSmemBytes(int maxNc);
-cudaError_t configureMarginalization(size_t visualSmem, int maxNr, int maxFastNr, long long* eigenSmem, long long* fastSmem);
+size_t margRowsSmemBytes(int maxNv);
+cudaError_t configureMarginalization(size_t visualSmem, size_t rowsSmem, int maxNr, int maxFastNr, long long* eigenSmem,
+                                     long long* fastSmem);
 int launchMarginalization(const DevBatch& B, const MargBatch& M, size_t visualSmem, cudaStream_t s);
 void launchDenseEigen(const double* H, int n, double* work, double* evals, double* evecs, int* status, cudaStream_t s);
 void launchDensePsd(const double* evals, const double* U, const double* rhs, int n, int columns, double absCut, double relCut,
@@ -132,6 +134,8 @@ struct cgmli_solver {
     DArray<MargWin> dMargWin;
     DArray<MargElim> dMargElim;
     DArray<int> margCols, margObsMap, margPoseCol, margSbCol, margExtCol, margRank, margStatus, margFast;
+    DArray<int> margVisCol, margVisPose, margVisExt, margSlow;
+    DArray<int4> margChunks, margItems;
     DArray<double> margH, margB, margSepH, margSepV, margSepB, margEvals, margA, margR0, margX, margMaxD, margStats;
     MargBatch MB{};
     bool haveMarg = false;
@@ -144,6 +148,9 @@ struct cgmli_solver {
     // pinned staging of the marginalization's inputs, and the event after their uploads
     HVec<MargElim> hMargElim;
     HVec<int> hMargCols, hMargObsMap, hMargPoseCol, hMargSbCol, hMargExtCol;
+    HVec<int> hMargVisCol, hMargVisPose, hMargVisExt, hMargSlow;
+    HVec<int4> hMargChunks, hMargItems;
+    int numSMs = 0;
     cudaEvent_t margUploaded = nullptr;
     // checkpoint of the accepted states
     DArray<double> snapPose, snapSb, snapExt, snapTd, snapRho;
@@ -198,8 +205,10 @@ struct cgmli_solver {
         dPairChunks.release(); dSchurChunks.release(); obLm.release(); keyOrder.release(); keyRows.release(); sch.release();
         snapPose.release(); snapSb.release(); snapExt.release(); snapTd.release(); snapRho.release();
         dMargWin.release(); dMargElim.release();
-        DArray<int>* mi[] = {&margCols, &margObsMap, &margPoseCol, &margSbCol, &margExtCol, &margRank, &margStatus, &margFast};
+        DArray<int>* mi[] = {&margCols, &margObsMap, &margPoseCol, &margSbCol, &margExtCol, &margRank, &margStatus, &margFast,
+                             &margVisCol, &margVisPose, &margVisExt, &margSlow};
         for (auto* a : mi) a->release();
+        margChunks.release(); margItems.release();
         DArray<double>* md[] = {&margH, &margB, &margSepH, &margSepV, &margSepB, &margEvals, &margA, &margR0, &margX, &margMaxD, &margStats};
         for (auto* a : md) a->release();
         for (auto e : evPool) cudaEventDestroy(e);
@@ -594,6 +603,8 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
     struct Part {
         std::vector<MargElim> elims;   // col0 / obs0 window-local
         std::vector<int> cols, obsMap;
+        std::vector<int> visCols;      // visual column -> marginalization column
+        std::vector<int4> chunks;      // window-local eliminated landmarks and staged observations
         int maxNc = 0, status = CGMLI_OK;
         const char* why = "";
     };
@@ -605,11 +616,15 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
     HVec<int>& poseCol = S->hMargPoseCol;
     HVec<int>& sbCol = S->hMargSbCol;
     HVec<int>& extCol = S->hMargExtCol;
+    HVec<int>& visPose = S->hMargVisPose;
+    HVec<int>& visExt = S->hMargVisExt;
     // the staging arrays may still feed the previous marginalization's uploads
     if (S->margUploaded) CK(cudaEventSynchronize(S->margUploaded));
     poseCol.resize(S->totalKf);
     sbCol.resize(S->totalKf);
     extCol.resize(S->totalExt);
+    visPose.resize(S->totalKf);
+    visExt.resize(S->totalExt);
     parallelFor(W, 0, [&](int w) {
         const WinDesc& d = S->win[w];
         const int v = victim_kf[w];
@@ -618,11 +633,14 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
         mw = MargWin{};
         mw.imu[0] = mw.imu[1] = -1;
         mw.tdCol = -1;
+        mw.visTd = -1;
         mw.huber = d.huber;
         mw.hasPrior = d.priorRank > 0;
         std::fill(&poseCol[d.kf0], &poseCol[d.kf0] + d.K, -1);
         std::fill(&sbCol[d.kf0], &sbCol[d.kf0] + d.K, -1);
         std::fill(&extCol[d.ext0], &extCol[d.ext0] + d.E, -1);
+        std::fill(&visPose[d.kf0], &visPose[d.kf0] + d.K, -1);
+        std::fill(&visExt[d.ext0], &visExt[d.ext0] + d.E, -1);
         if (v < 0) return;
         std::vector<char> poseUsed(d.K, 0), sbUsed(d.K, 0), extUsed(d.E, 0);
         bool tdUsed = false;
@@ -674,6 +692,19 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
         mw.m = n;
         mw.nr = n - mw.nm;
         if (mw.nr > kMargMaxSep) { P.status = CGMLI_E_LIMIT; P.why = "marginalization separator above 1024 columns"; return; }
+        // visual columns (poses, extrinsics, td) in column order
+        auto addVis = [&](int col, int width) {
+            for (int c = 0; c < width; ++c) P.visCols.push_back(col + c);
+            return (int)P.visCols.size() - width;
+        };
+        if (poseUsed[v]) visPose[d.kf0 + v] = addVis(poseCol[d.kf0 + v], 6);
+        for (int k = 0; k < d.K; ++k)
+            if (k != v && poseUsed[k]) visPose[d.kf0 + k] = addVis(poseCol[d.kf0 + k], 6);
+        for (int e = 0; e < d.E; ++e)
+            if (extUsed[e]) visExt[d.ext0 + e] = addVis(extCol[d.ext0 + e], 6);
+        if (mw.tdCol >= 0) mw.visTd = addVis(mw.tdCol, 1);
+        mw.nv = (int)P.visCols.size();
+        mw.rowsPath = mw.nv <= kRowsMaxN;
         // eliminated landmarks: local column blocks in order of first use
         int obsCount = 0;
         for (int g : elimLm) {
@@ -708,12 +739,27 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
             P.maxNc = std::max(P.maxNc, me.nc);
             P.elims.push_back(me);
         }
+        // dense-row chunks: 2 rows per observation and 1 per landmark, at most kRowsCap
+        if (mw.rowsPath && !P.elims.empty()) {
+            int4 ch{0, 0, 0, 0};
+            for (int e = 0; e < (int)P.elims.size(); ++e) {
+                const int nob = hb.lmObsBegin[P.elims[e].lm + 1] - hb.lmObsBegin[P.elims[e].lm];
+                const int rows = 2 * (ch.w - ch.z) + (ch.y - ch.x);
+                if (ch.y > ch.x && rows + 2 * nob + 1 > kRowsCap) {
+                    P.chunks.push_back(ch);
+                    ch = int4{e, e, ch.w, ch.w};
+                }
+                ch.y = e + 1;
+                ch.w += nob;
+            }
+            P.chunks.push_back(ch);
+        }
     });
     // ---- prefix sums over the windows, then one concatenation (parallel)
     std::vector<long long> colBase(W + 1, 0), obsBase(W + 1, 0);
-    std::vector<int> elimBase(W + 1, 0);
+    std::vector<int> elimBase(W + 1, 0), visBase(W + 1, 0), chunkBase(W + 1, 0);
     long long H0 = 0, sep0 = 0, vec0 = 0, x0 = 0;
-    int maxNc = 0;
+    int maxNc = 0, maxNv = 0, numSlow = 0;
     for (int w = 0; w < W; ++w) {
         if (part[w].status != CGMLI_OK) return fail(part[w].status, part[w].why);
         MargWin& mw = mwv[w];
@@ -721,6 +767,11 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
         mw.elim0 = elimBase[w];
         mw.nElim = (int)part[w].elims.size();
         elimBase[w + 1] = elimBase[w] + mw.nElim;
+        mw.vis0 = visBase[w];
+        visBase[w + 1] = visBase[w] + mw.nv;
+        chunkBase[w + 1] = chunkBase[w] + (int)part[w].chunks.size();
+        if (!part[w].chunks.empty()) maxNv = std::max(maxNv, mw.nv);
+        if (!mw.rowsPath) numSlow += mw.nElim;
         colBase[w + 1] = colBase[w] + (long long)part[w].cols.size();
         obsBase[w + 1] = obsBase[w] + (long long)part[w].obsMap.size() / 5;
         maxNc = std::max(maxNc, part[w].maxNc);
@@ -732,9 +783,13 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
     HVec<MargElim>& elims = S->hMargElim;
     HVec<int>& cols = S->hMargCols;
     HVec<int>& obsMap = S->hMargObsMap;
+    HVec<int>& visCol = S->hMargVisCol;
+    HVec<int4>& chunks = S->hMargChunks;
     elims.resize(elimBase[W]);
     cols.resize(colBase[W]);
     obsMap.resize(5 * obsBase[W]);
+    visCol.resize(std::max(visBase[W], 1));
+    chunks.resize(std::max(chunkBase[W], 1));
     parallelFor(W, 0, [&](int w) {
         const Part& P = part[w];
         for (size_t e = 0; e < P.elims.size(); ++e) {
@@ -745,16 +800,58 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
         }
         std::copy(P.cols.begin(), P.cols.end(), cols.begin() + colBase[w]);
         std::copy(P.obsMap.begin(), P.obsMap.end(), obsMap.begin() + 5 * obsBase[w]);
+        std::copy(P.visCols.begin(), P.visCols.end(), visCol.begin() + visBase[w]);
+        for (size_t c = 0; c < P.chunks.size(); ++c) {
+            const int4 ch = P.chunks[c];
+            chunks[chunkBase[w] + c] = int4{ch.x + elimBase[w], ch.y + elimBase[w], ch.z + (int)obsBase[w], ch.w + (int)obsBase[w]};
+        }
     });
+    // items: runs of one window's chunks of about equal work (rows x upper tiles),
+    // four per SM over the batch
+    if (!S->numSMs) CK(cudaDeviceGetAttribute(&S->numSMs, cudaDevAttrMultiProcessorCount, S->device));
+    auto chunkWork = [&](int w, const int4& ch) {
+        const long long nb = (mwv[w].nv + 31) / 32;
+        return (long long)(2 * (ch.w - ch.z) + (ch.y - ch.x)) * (nb * (nb + 1) / 2);
+    };
+    long long totalWork = 0;
+    for (int w = 0; w < W; ++w)
+        for (int c = chunkBase[w]; c < chunkBase[w + 1]; ++c) totalWork += chunkWork(w, chunks[c]);
+    const long long target = std::max(1ll, totalWork / (4ll * std::max(S->numSMs, 1)));
+    HVec<int4>& items = S->hMargItems;
+    HVec<int>& slow = S->hMargSlow;
+    items.clear();
+    slow.resize(std::max(numSlow, 1));
+    numSlow = 0;
+    for (int w = 0; w < W; ++w) {
+        if (!mwv[w].rowsPath) {
+            for (int e = elimBase[w]; e < elimBase[w + 1]; ++e) slow[numSlow++] = e;
+            continue;
+        }
+        int c0 = chunkBase[w];
+        long long work = 0;
+        for (int c = chunkBase[w]; c < chunkBase[w + 1]; ++c) {
+            const long long cw = chunkWork(w, chunks[c]);
+            if (c > c0 && work + cw > target) {
+                items.push_back(int4{w, c0, c, 0});
+                c0 = c;
+                work = 0;
+            }
+            work += cw;
+        }
+        if (chunkBase[w + 1] > c0) items.push_back(int4{w, c0, chunkBase[w + 1], 0});
+    }
+    const int numItems = (int)items.size();
+    if (items.empty()) items.push_back(int4{0, 0, 0, 0});
     cudaStream_t st = S->stream;
     const size_t smem = margVisualSmemBytes(std::max(maxNc, 1));
+    const size_t rowsSmem = margRowsSmemBytes(std::max(maxNv, 1));
     int maxNr = 1, maxFastNr = 0;
     for (const auto& mw : mwv) {
         maxNr = std::max(maxNr, mw.nr);
         if (mw.hasPrior) maxFastNr = std::max(maxFastNr, mw.nr);
     }
     long long eigenSmem = 0, fastSmem = 0;
-    CK(configureMarginalization(smem, maxNr, maxFastNr, &eigenSmem, &fastSmem));
+    CK(configureMarginalization(smem, rowsSmem, maxNr, maxFastNr, &eigenSmem, &fastSmem));
     CK(S->dMargWin.upload(mwv, st));
     CK(S->dMargElim.upload(elims, st));
     CK(S->margCols.upload(cols, st));
@@ -762,6 +859,12 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
     CK(S->margPoseCol.upload(poseCol, st));
     CK(S->margSbCol.upload(sbCol, st));
     CK(S->margExtCol.upload(extCol, st));
+    CK(S->margVisCol.upload(visCol, st));
+    CK(S->margVisPose.upload(visPose, st));
+    CK(S->margVisExt.upload(visExt, st));
+    CK(S->margChunks.upload(chunks, st));
+    CK(S->margItems.upload(items, st));
+    CK(S->margSlow.upload(slow, st));
     if (!S->margUploaded) CK(cudaEventCreateWithFlags(&S->margUploaded, cudaEventDisableTiming));
     CK(cudaEventRecord(S->margUploaded, st));
     CK(S->margH.reserve(H0)); CK(S->margB.reserve(vec0)); CK(S->margSepH.reserve(sep0)); CK(S->margSepV.reserve(sep0));
@@ -786,6 +889,14 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
     M.evals = S->margEvals.p; M.A = S->margA.p; M.r0 = S->margR0.p; M.X = S->margX.p;
     M.maxD = S->margMaxD.p; M.stats = S->margStats.p; M.rank = S->margRank.p; M.status = S->margStatus.p;
     M.fast = S->margFast.p;
+    M.rows = S->keyRows.p;
+    M.visCol = S->margVisCol.p; M.visPose = S->margVisPose.p; M.visExt = S->margVisExt.p;
+    M.chunks = S->margChunks.p;
+    M.items = S->margItems.p;
+    M.numItems = numItems;
+    M.rowsSmem = (long long)rowsSmem;
+    M.slowElim = S->margSlow.p;
+    M.numSlowElim = numSlow;
     S->margWin = mwv;
     S->margSepTotal = sep0;
     S->margVecTotal = vec0;

@@ -95,7 +95,11 @@ constexpr int kMargMaxNc = 200;     // marginalization columns touched by one el
 constexpr int kMargMaxSep = 1024;   // separator columns (Jacobi pair tables hold 512 pairs)
 constexpr int kMargThreads = 512;   // victim CTAs
 constexpr int kEigenThreads = 512;  // eigen CTAs
-constexpr int kMargLmThreads = 128; // one CTA per eliminated landmark
+constexpr int kMargLmThreads = 128; // one CTA per eliminated landmark (windows above kRowsMaxN)
+constexpr int kRowsMaxN = 256;      // visual columns of a window on the dense-row path
+constexpr int kRowsCap = 96;        // rows of one dense-row chunk (2 per observation + 1 per landmark)
+constexpr int kRowsThreads = 512;   // dense-row CTAs
+constexpr int kMargRecord = 56;     // staged doubles per observation of an eliminated landmark
 
 struct MargWin {
     int m, nm, nr;          // m = 0: window not marginalized
@@ -108,6 +112,10 @@ struct MargWin {
     long long vec0;         // m
     long long x0;           // 2 * 15 * (nr + 1): victim solve scratch, then the fast path's vectors
     double huber;
+    int nv;                 // visual columns (poses, extrinsics, td) in column order
+    int vis0;               // offset of the window's visual -> marginalization column map
+    int visTd;              // visual column of td or -1
+    int rowsPath;           // 1: eliminated landmarks accumulate through dense rows (nv <= kRowsMaxN)
 };
 struct MargElim { int lm, win, nc, col0, obs0; };  // device landmark, window, local columns, offsets
 struct MargBatch {
@@ -125,6 +133,16 @@ struct MargBatch {
     double* stats;       // 4 per window: robust cost, whitened |r|^2, eliminated reduction, cutoff
     int* rank; int* status;
     int* fast;           // per window: 1 when the full-rank fast path formed the prior
+    // dense-row path
+    double* rows;        // kMargRecord per eliminated observation (staged factor rows)
+    const int* visCol;   // visual column -> marginalization column, per window from MargWin::vis0
+    const int* visPose; const int* visExt;  // global keyframe / extrinsic -> visual column or -1
+    const int4* chunks;  // {first, end eliminated landmark, first, end staged observation}: <= kRowsCap rows
+    const int4* items;   // {window, first chunk, end chunk, -}: one CTA each
+    int numItems;
+    long long rowsSmem;  // dynamic shared memory of a dense-row CTA
+    const int* slowElim; // eliminated landmarks of windows above kRowsMaxN (one CTA each)
+    int numSlowElim;
 };
 
 // Called before (phase 0) and after (phase 1) every kernel launch of an

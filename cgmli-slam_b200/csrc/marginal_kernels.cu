@@ -7,11 +7,15 @@
 // are linearized at the accepted states, with the Huber loss and with frozen
 // calibration blocks differentiated too, into an FP64 system over
 // [victim pose+speed/bias | separator]:
-//   k_marg_dmax      largest eliminated-landmark information of each window
-//                    (the scalar cutoff max(1e-12, 1e-9 max d) of psdSolve)
-//   k_marg_visual    one CTA per eliminated landmark: its factors' normal
-//                    blocks and its own scalar Schur term -c c^T / d are
-//                    summed in shared memory, then added to the window once
+//   k_marg_eval      the eliminated landmarks' factors: largest information
+//                    d of each window (the scalar cutoff max(1e-12, 1e-9 max d)
+//                    of psdSolve) and the staged weighted rows
+//   k_marg_rows      dense-row accumulation per run of a window's eliminated
+//                    landmarks: factor rows and Schur rows c / sqrt(d) of the
+//                    scalar eliminations, register-tiled rank updates
+//   k_marg_visual    windows above kRowsMaxN visual columns: one CTA per
+//                    eliminated landmark, its factors' normal blocks and its
+//                    own scalar Schur term -c c^T / d summed in shared memory
 //   k_marg_retained  IMU factors of the victim and the previous prior
 //   k_marg_victim    victim block removed by the eigen-based PSD solve
 //   k_marg_eigen     Jacobi eigendecomposition of the separator information,
@@ -69,8 +73,7 @@ __device__ __forceinline__ double symAt(const double* H, int i, int j, int m) {
 // marginalization's derivative set (extrinsics always, td whenever the window
 // has one).  Returns false on an invalid linearization point.
 __device__ bool margFactor(const DevBatch& B, const WinDesc& wd, int w, int l, int f, FactorIn& in, FactorOut& o, double& wgt,
-                           double& sq) {
-    int kfa, kfb, ea, eb;
+                           double& sq, int& kfa, int& kfb, int& ea, int& eb) {
     gatherFactor(B, wd, w, l, f, 0, in, kfa, kfb, ea, eb);
     in.wantExt = true;
     in.wantTd = wd.hasTd != 0;
@@ -83,31 +86,259 @@ __device__ bool margFactor(const DevBatch& B, const WinDesc& wd, int w, int l, i
 }  // namespace
 
 // ---------------------------------------------------------------------------------------
-// One warp per eliminated landmark, one lane per observation.
-__global__ void k_marg_dmax(DevBatch B, MargBatch M) {
+// One warp per eliminated landmark, one lane per observation: the landmark's
+// information d (for the window's cutoff) and, for windows on the dense-row
+// path, the staged record of each observation:
+//   [0, 25)  weighted row 0 over the observation's columns in block order
+//            (anchor pose, observer pose, anchor extrinsic, observer extrinsic, td)
+//   [25, 50) weighted row 1
+//   50..53   weighted r0, r1, d r0 / d rho, d r1 / d rho
+//   54       robust cost
+//   55       the four block starts as visual columns (int16, -1 absent)
+__global__ void k_marg_eval(DevBatch B, MargBatch M) {
     const int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (e >= M.numElim) return;
     const MargElim me = M.elim[e];
     const WinDesc wd = B.win[me.win];
+    const bool stage = M.win[me.win].rowsPath != 0;
     const int ob = B.lmObsBegin[me.lm], oe = B.lmObsBegin[me.lm + 1];
     double d = 0;
     for (int f = ob + lane; f < oe; f += 32) {
         FactorIn in;
         FactorOut o;
         double wgt, sq;
-        if (!margFactor(B, wd, me.win, me.lm, f, in, o, wgt, sq)) { atomicExch(&M.status[me.win], CGMLI_E_NONFINITE); continue; }
+        int kfa, kfb, ea, eb;
+        double* rec = M.rows + (long long)kMargRecord * (me.obs0 + (f - ob));
+        if (!margFactor(B, wd, me.win, me.lm, f, in, o, wgt, sq, kfa, kfb, ea, eb)) {
+            atomicExch(&M.status[me.win], CGMLI_E_NONFINITE);
+            if (stage) {
+                // no block: only a td column can map, to slot 0 of each row
+                rec[0] = rec[25] = 0.0;
+                for (int k = 50; k < 55; ++k) rec[k] = 0.0;
+                rec[55] = __longlong_as_double(-1ll);
+            }
+            continue;
+        }
         d += wgt * wgt * (o.Jrho[0] * o.Jrho[0] + o.Jrho[1] * o.Jrho[1]);
+        if (!stage) continue;
+        int n = 0;
+        auto push = [&](const double* Jb, int width) {
+            for (int c = 0; c < width; ++c, ++n) {
+                rec[n] = wgt * Jb[c];
+                rec[25 + n] = wgt * Jb[width + c];
+            }
+        };
+        const bool same = in.sameKf && !in.splitExt;
+        int st[4] = {-1, -1, -1, -1};
+        if (!in.sameKf) { push(o.Ja, 6); push(o.Jb, 6); st[0] = M.visPose[kfa]; st[1] = M.visPose[kfb]; }
+        if (!same) { push(o.Jea, 6); st[2] = M.visExt[ea]; }
+        if (in.splitExt) { push(o.Jeb, 6); st[3] = M.visExt[eb]; }
+        if (in.wantTd) push(o.Jtd, 1);
+        rec[50] = wgt * o.r[0];
+        rec[51] = wgt * o.r[1];
+        rec[52] = wgt * o.Jrho[0];
+        rec[53] = wgt * o.Jrho[1];
+        rec[54] = huberCost(wd.huber, sq);
+        unsigned long long pk = 0;
+        for (int b = 0; b < 4; ++b) pk |= (unsigned long long)(unsigned short)(short)st[b] << (16 * b);
+        rec[55] = __longlong_as_double((long long)pk);
     }
     d = mWarpSum(d);
     if (lane == 0) atomicMaxNonNegative(&M.maxD[me.win], d);
 }
 
-// One CTA per eliminated landmark.  Shared memory: the landmark's local
+// Dense-row accumulation, one CTA per item (a run of chunks of one window's
+// eliminated landmarks).  Per chunk the staged records become dense rows over
+// the window's nv visual columns in shared memory: two weighted factor rows
+// per observation, then per landmark its Schur row c / sqrt(d) (zero below the
+// cutoff), with c = sum_k row_k dr_k/drho.  The item's visual information is
+//   sum_factor-rows v v^T - sum_Schur-rows s s^T
+// (the factor normal blocks minus c c^T / d) and its gradient
+//   sum v r - sum s bl / sqrt(d).
+// Each warp owns 32 x 32 tiles of the upper triangle, one lane a 4 x 8 block
+// of a tile in registers: held over the whole item when the tiles fit the
+// warps, else summed per chunk; then added to the window's H once.
+namespace {
+__device__ __forceinline__ void tileOf(int t, int nb, int& bi, int& bj) {
+    bi = 0;
+    while (t >= nb - bi) { t -= nb - bi; ++bi; }
+    bj = bi + t;
+}
+template <bool kSubtract>
+__device__ __forceinline__ void rankUpdate(double (&acc)[4][8], const double* Va, const double* Vb, int k0, int k1, int np) {
+#pragma unroll 2
+    for (int k = k0; k < k1; ++k) {
+        const double2 a01 = *reinterpret_cast<const double2*>(Va + (long long)k * np);
+        const double2 a23 = *reinterpret_cast<const double2*>(Va + (long long)k * np + 16);
+        double a[4] = {a01.x, a01.y, a23.x, a23.y};
+        if (kSubtract)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) a[r] = -a[r];
+        double b[8];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const double2 v = *reinterpret_cast<const double2*>(Vb + (long long)k * np + 8 * q);
+            b[2 * q] = v.x;
+            b[2 * q + 1] = v.y;
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int c = 0; c < 8; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+    }
+}
+__device__ __forceinline__ void flushTile(double (&acc)[4][8], int bi, int bj, int lane, int n, const int* visCol, double* H, int m) {
+    const int rg = lane >> 2, cg = lane & 3;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int i = bi * 32 + (r < 2 ? 2 * rg + r : 16 + 2 * rg + r - 2);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int j = bj * 32 + 8 * (c >> 1) + 2 * cg + (c & 1);
+            const double v = acc[r][c];
+            if (i < n && j < n && i <= j && v != 0.0) {
+                const int ci = visCol[i], cj = visCol[j];
+                atomicAdd(&H[ci <= cj ? (long long)ci * m + cj : (long long)cj * m + ci], v);
+            }
+        }
+    }
+}
+}  // namespace
+
+__global__ void __launch_bounds__(kRowsThreads, 1) k_marg_rows(DevBatch B, MargBatch M) {
+    extern __shared__ __align__(16) double smem[];
+    const int4 it = M.items[blockIdx.x];
+    const int w = it.x;
+    const MargWin mw = M.win[w];
+    const int n = mw.nv, np = (n + 31) & ~31, nb = np >> 5, ntiles = nb * (nb + 1) / 2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, rg = lane >> 2, cg = lane & 3;
+    constexpr int nw = kRowsThreads / 32;
+    const bool persistent = ntiles <= nw;
+    double* V = smem;                 // kRowsCap x np
+    double* rv = V + kRowsCap * np;   // kRowsCap: residual of each row
+    __shared__ double red[kRowsThreads / 32];
+    const double cutoff = fmax(1e-12, 1e-9 * fmax(0.0, M.maxD[w]));
+    const int* visCol = M.visCol + mw.vis0;
+    double* H = M.H + mw.H0;
+    const int gj = threadIdx.x - (kRowsThreads - np);  // the last np threads own one gradient column each
+    double g = 0, cost = 0, rss = 0, reduction = 0;
+    double acc[4][8];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 8; ++c) acc[r][c] = 0.0;
+    for (int ci = it.y; ci < it.z; ++ci) {
+        const int4 ch = M.chunks[ci];
+        const int kp = 2 * (ch.w - ch.z), K = kp + (ch.y - ch.x);
+        // ---- dense rows, one warp per landmark
+        for (int l = ch.x + warp; l < ch.y; l += nw) {
+            const MargElim me = M.elim[l];
+            const int nob = B.lmObsBegin[me.lm + 1] - B.lmObsBegin[me.lm];
+            const int row0 = 2 * (me.obs0 - ch.z);
+            double sc[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) sc[q] = 0.0;
+            double d = 0, bl = 0;
+            for (int t = 0; t < nob; ++t) {
+                const double* rec = M.rows + (long long)kMargRecord * (me.obs0 + t);
+                const double lo = rec[lane], hi = lane < kMargRecord - 32 ? rec[32 + lane] : 0.0;
+                const double wr0 = __shfl_sync(0xffffffffu, hi, 18), wr1 = __shfl_sync(0xffffffffu, hi, 19);
+                const double wj0 = __shfl_sync(0xffffffffu, hi, 20), wj1 = __shfl_sync(0xffffffffu, hi, 21);
+                const double oc = __shfl_sync(0xffffffffu, hi, 22);
+                const unsigned long long pk = (unsigned long long)__double_as_longlong(__shfl_sync(0xffffffffu, hi, 23));
+                d += wj0 * wj0 + wj1 * wj1;
+                bl += wj0 * wr0 + wj1 * wr1;
+                if (lane == 0) {
+                    cost += oc;
+                    rss += wr0 * wr0 + wr1 * wr1;
+                    rv[row0 + 2 * t] = wr0;
+                    rv[row0 + 2 * t + 1] = wr1;
+                }
+                double* v0row = V + (long long)(row0 + 2 * t) * np;
+                double* v1row = v0row + np;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    if (q >= nb) break;
+                    const int col = 32 * q + lane;
+                    int slot = -1, base = 0;
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        const int start = (int)(short)(unsigned short)(pk >> (16 * b));
+                        if (start >= 0) {
+                            if (col >= start && col < start + 6) slot = base + col - start;
+                            base += 6;
+                        }
+                    }
+                    if (mw.visTd >= 0 && col == mw.visTd) slot = base;
+                    const int s0 = slot < 0 ? 0 : slot, s1 = s0 + 25;
+                    const double x0 = __shfl_sync(0xffffffffu, lo, s0);
+                    const double x1lo = __shfl_sync(0xffffffffu, lo, s1 & 31);
+                    const double x1hi = __shfl_sync(0xffffffffu, hi, s1 & 31);
+                    const double v0 = slot < 0 ? 0.0 : x0;
+                    const double v1 = slot < 0 ? 0.0 : (s1 < 32 ? x1lo : x1hi);
+                    v0row[col] = v0;
+                    v1row[col] = v1;
+                    sc[q] += v0 * wj0 + v1 * wj1;
+                }
+            }
+            const bool eliminate = d > cutoff;
+            const double scale = eliminate ? 1.0 / sqrt(d) : 0.0;
+            const int sr = kp + (l - ch.x);
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                if (q < nb) V[(long long)sr * np + 32 * q + lane] = sc[q] * scale;
+            if (lane == 0) {
+                rv[sr] = bl * scale;
+                if (eliminate) reduction += 0.5 * bl * bl / d;
+            }
+        }
+        __syncthreads();
+        // ---- rank updates of the upper tiles, gradient columns
+        for (int t = warp; t < ntiles; t += nw) {
+            int bi, bj;
+            tileOf(t, nb, bi, bj);
+            if (!persistent)
+#pragma unroll
+                for (int r = 0; r < 4; ++r)
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) acc[r][c] = 0.0;
+            const double* Va = V + bi * 32 + 2 * rg;
+            const double* Vb = V + bj * 32 + 2 * cg;
+            rankUpdate<false>(acc, Va, Vb, 0, kp, np);
+            rankUpdate<true>(acc, Va, Vb, kp, K, np);
+            if (!persistent) flushTile(acc, bi, bj, lane, n, visCol, H, mw.m);
+        }
+        if (gj >= 0) {
+            double s = 0;
+            for (int k = 0; k < kp; ++k) s += V[(long long)k * np + gj] * rv[k];
+            for (int k = kp; k < K; ++k) s -= V[(long long)k * np + gj] * rv[k];
+            g += s;
+        }
+        __syncthreads();
+    }
+    if (persistent && warp < ntiles) {
+        int bi, bj;
+        tileOf(warp, nb, bi, bj);
+        flushTile(acc, bi, bj, lane, n, visCol, H, mw.m);
+    }
+    if (gj >= 0 && gj < n && g != 0.0) atomicAdd(&M.b[mw.vec0 + visCol[gj]], g);
+    cost = mBlockSum(cost, red);
+    rss = mBlockSum(rss, red);
+    reduction = mBlockSum(reduction, red);
+    if (threadIdx.x == 0) {
+        atomicAdd(&M.stats[4 * w + 0], cost);
+        atomicAdd(&M.stats[4 * w + 1], rss);
+        atomicAdd(&M.stats[4 * w + 2], reduction);
+    }
+}
+
+// One CTA per eliminated landmark of a window above kRowsMaxN visual columns.
+// Shared memory: the landmark's local
 // information (packed upper, nc x nc), its cross vector c and gradient, then
 // the staged weighted rows of its observations.
 __global__ void __launch_bounds__(kMargLmThreads) k_marg_visual(DevBatch B, MargBatch M) {
     extern __shared__ double smem[];
-    const int e = blockIdx.x;
+    const int e = M.slowElim[blockIdx.x];
     const MargElim me = M.elim[e];
     const int w = me.win, nc = me.nc;
     const MargWin mw = M.win[w];
@@ -129,8 +360,8 @@ __global__ void __launch_bounds__(kMargLmThreads) k_marg_visual(DevBatch B, Marg
         FactorIn in;
         FactorOut o;
         double wgt, sq;
-        int n = 0;
-        if (margFactor(B, wd, w, me.lm, f, in, o, wgt, sq)) {
+        int n = 0, kfa, kfb, ea, eb;
+        if (margFactor(B, wd, w, me.lm, f, in, o, wgt, sq, kfa, kfb, ea, eb)) {
             cost = huberCost(wd.huber, sq);
             rss = wgt * wgt * sq;
             const int* map = M.obsMap + 5ll * (me.obs0 + t);
@@ -962,9 +1193,16 @@ size_t margVisualSmemBytes(int maxNc) {
 // Sets the dynamic shared memory limits of the marginalization kernels for a
 // batch whose largest separator has maxNr columns; returns the eigen CTA's
 // dynamic shared memory in eigenSmem.
-cudaError_t configureMarginalization(size_t visualSmem, int maxNr, int maxFastNr, long long* eigenSmem, long long* fastSmem) {
+size_t margRowsSmemBytes(int maxNv) {
+    const size_t np = ((size_t)maxNv + 31) & ~(size_t)31;
+    return sizeof(double) * ((size_t)kRowsCap * np + kRowsCap);
+}
+cudaError_t configureMarginalization(size_t visualSmem, size_t rowsSmem, int maxNr, int maxFastNr, long long* eigenSmem,
+                                     long long* fastSmem) {
     cudaError_t e = cudaFuncSetAttribute(k_marg_visual, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)visualSmem);
     if (e != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_marg_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rowsSmem)) != cudaSuccess)
+        return e;
     *fastSmem = maxFastNr > 0 ? (long long)fastSmemBytes(maxFastNr < kFastMaxN ? maxFastNr : kFastMaxN) : 0;
     if ((e = cudaFuncSetAttribute(k_marg_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fastSmemBytes(kFastMaxN))) !=
         cudaSuccess)
@@ -987,9 +1225,16 @@ int launchMarginalization(const DevBatch& B, const MargBatch& M, size_t visualSm
     int n = 0;
     if (M.numElim > 0) {
         const int warps = 8;
-        k_marg_dmax<<<(M.numElim + warps - 1) / warps, 32 * warps, 0, s>>>(B, M);
-        k_marg_visual<<<M.numElim, kMargLmThreads, visualSmem, s>>>(B, M);
-        n += 2;
+        k_marg_eval<<<(M.numElim + warps - 1) / warps, 32 * warps, 0, s>>>(B, M);
+        ++n;
+    }
+    if (M.numItems > 0) {
+        k_marg_rows<<<M.numItems, kRowsThreads, (size_t)M.rowsSmem, s>>>(B, M);
+        ++n;
+    }
+    if (M.numSlowElim > 0) {
+        k_marg_visual<<<M.numSlowElim, kMargLmThreads, visualSmem, s>>>(B, M);
+        ++n;
     }
     k_marg_retained<<<M.numWindows, 256, 0, s>>>(B, M);
     k_marg_victim<<<M.numWindows, kMargThreads, 0, s>>>(M);

@@ -111,6 +111,18 @@ def test_large_window_second_new(oracle, backend):
     compare(s.read_prior(0), ref)
 
 
+def test_wide_window_landmark_path(oracle, backend):
+    """48 keyframes with 32-observation tracks: the eliminated landmarks touch
+    about 300 visual columns, above the dense-row path, so the per-landmark
+    kernel forms the visual part."""
+    w = synth.SynthWindow(replace(synth.C3, keyframes=48, landmarks=3000, track_max=32), 5)
+    ref = oracle.marginalize_window(w.window, 0, abi.MARGIN_OLD)
+    s = backend.Solver()
+    s.set_windows([w])
+    s.marginalize([0], abi.MARGIN_OLD)
+    compare(s.read_prior(0), ref)
+
+
 def test_invalid_point_reported(backend):
     """A non-positive inverse distance among the eliminated landmarks makes the
     linearization invalid; the status comes back instead of a prior."""
