@@ -32,6 +32,7 @@ int launchIteration(const DevBatch& B, const LaunchPlan& P, int refinement, int 
 int launchLmInit(const DevBatch& B, double lambda0, cudaStream_t s);
 size_t margVisualSmemBytes(int maxNc);
 size_t margRowsSmemBytes(int maxNv);
+int margRowsCap(int nv);
 cudaError_t configureMarginalization(size_t visualSmem, size_t rowsSmem, int maxNr, int maxFastNr, long long* eigenSmem,
                                      long long* fastSmem);
 int launchMarginalization(const DevBatch& B, const MargBatch& M, size_t visualSmem, cudaStream_t s);
@@ -739,13 +740,15 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
             P.maxNc = std::max(P.maxNc, me.nc);
             P.elims.push_back(me);
         }
-        // dense-row chunks: 2 rows per observation and 1 per landmark, at most kRowsCap
+        // dense-row chunks: 2 rows per observation and 1 per landmark, at most
+        // 96 (72 above 192 visual columns)
         if (mw.rowsPath && !P.elims.empty()) {
+            const int cap = margRowsCap(mw.nv);
             int4 ch{0, 0, 0, 0};
             for (int e = 0; e < (int)P.elims.size(); ++e) {
                 const int nob = hb.lmObsBegin[P.elims[e].lm + 1] - hb.lmObsBegin[P.elims[e].lm];
                 const int rows = 2 * (ch.w - ch.z) + (ch.y - ch.x);
-                if (ch.y > ch.x && rows + 2 * nob + 1 > kRowsCap) {
+                if (ch.y > ch.x && rows + 2 * nob + 1 > cap) {
                     P.chunks.push_back(ch);
                     ch = int4{e, e, ch.w, ch.w};
                 }
@@ -848,7 +851,7 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
     int maxNr = 1, maxFastNr = 0;
     for (const auto& mw : mwv) {
         maxNr = std::max(maxNr, mw.nr);
-        if (mw.hasPrior) maxFastNr = std::max(maxFastNr, mw.nr);
+        maxFastNr = std::max(maxFastNr, mw.nr);
     }
     long long eigenSmem = 0, fastSmem = 0;
     CK(configureMarginalization(smem, rowsSmem, maxNr, maxFastNr, &eigenSmem, &fastSmem));

@@ -106,7 +106,7 @@ struct MargWin {
     int elim0, nElim;       // eliminated landmarks in MargBatch::elim
     int imu[2];             // consumed IMU factors (global index) or -1
     int tdCol;              // column of td or -1
-    int hasPrior;           // the window carries a prior (gauge fixed: the full-rank fast path is tried)
+    int hasPrior;           // the window carries a prior
     long long H0;           // m * m
     long long sep0;         // nr * nr: separator information, eigenvectors, A
     long long vec0;         // m

@@ -22,6 +22,8 @@
 //                    rank cutoff, A = sqrt(lambda) u^T, r0 = u^T b / sqrt(lambda)
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "../../include/cgmli_backend.h"
 #include "backend_internal.h"
 #include "device_math.cuh"
@@ -148,16 +150,19 @@ __global__ void k_marg_eval(DevBatch B, MargBatch M) {
 }
 
 // Dense-row accumulation, one CTA per item (a run of chunks of one window's
-// eliminated landmarks).  Per chunk the staged records become dense rows over
-// the window's nv visual columns in shared memory: two weighted factor rows
-// per observation, then per landmark its Schur row c / sqrt(d) (zero below the
+// eliminated landmarks).  Per chunk the staged records (prefetched into shared
+// memory with cp.async while the previous chunk's rank updates run) become
+// dense rows over the window's nv visual columns: two weighted factor rows per
+// observation, then per landmark its Schur row c / sqrt(d) (zero below the
 // cutoff), with c = sum_k row_k dr_k/drho.  The item's visual information is
 //   sum_factor-rows v v^T - sum_Schur-rows s s^T
 // (the factor normal blocks minus c c^T / d) and its gradient
 //   sum v r - sum s bl / sqrt(d).
-// Each warp owns 32 x 32 tiles of the upper triangle, one lane a 4 x 8 block
-// of a tile in registers: held over the whole item when the tiles fit the
-// warps, else summed per chunk; then added to the window's H once.
+// The upper triangle is cut into 32 x 32 tiles, each lane holding a 4 x 8
+// block of one tile in registers.  When the tiles fit the warps, spare warps
+// split a tile's rows (k) between them and the blocks are held over the whole
+// item; else every warp sums its tiles per chunk.  Either way each block is
+// added to the window's H with atomics once per accumulation.
 namespace {
 __device__ __forceinline__ void tileOf(int t, int nb, int& bi, int& bj) {
     bi = 0;
@@ -165,9 +170,9 @@ __device__ __forceinline__ void tileOf(int t, int nb, int& bi, int& bj) {
     bj = bi + t;
 }
 template <bool kSubtract>
-__device__ __forceinline__ void rankUpdate(double (&acc)[4][8], const double* Va, const double* Vb, int k0, int k1, int np) {
+__device__ __forceinline__ void rankUpdate(double (&acc)[4][8], const double* Va, const double* Vb, int k0, int k1, int step, int np) {
 #pragma unroll 2
-    for (int k = k0; k < k1; ++k) {
+    for (int k = k0; k < k1; k += step) {
         const double2 a01 = *reinterpret_cast<const double2*>(Va + (long long)k * np);
         const double2 a23 = *reinterpret_cast<const double2*>(Va + (long long)k * np + 16);
         double a[4] = {a01.x, a01.y, a23.x, a23.y};
@@ -203,7 +208,24 @@ __device__ __forceinline__ void flushTile(double (&acc)[4][8], int bi, int bj, i
         }
     }
 }
+__device__ __forceinline__ void cpAsync16(void* dst, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+// staged records of one chunk into shared memory (16-byte pieces; records are
+// kMargRecord doubles, a multiple of 16 bytes, from a 256-byte aligned base)
+__device__ __forceinline__ void prefetchRecords(const MargBatch& M, const int4& ch, double* dst) {
+    const double* src = M.rows + (long long)kMargRecord * ch.z;
+    const int pieces = (ch.w - ch.z) * (kMargRecord / 2);
+    for (int i = threadIdx.x; i < pieces; i += blockDim.x) cpAsync16(dst + 2 * i, src + 2 * i);
+    cpAsyncCommit();
+}
 }  // namespace
+
+// rows of a chunk for a window of np (padded) visual columns
+__host__ __device__ inline int rowsCapOf(int np) { return np <= 192 ? kRowsCap : 72; }
 
 __global__ void __launch_bounds__(kRowsThreads, 1) k_marg_rows(DevBatch B, MargBatch M) {
     extern __shared__ __align__(16) double smem[];
@@ -214,8 +236,13 @@ __global__ void __launch_bounds__(kRowsThreads, 1) k_marg_rows(DevBatch B, MargB
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, rg = lane >> 2, cg = lane & 3;
     constexpr int nw = kRowsThreads / 32;
     const bool persistent = ntiles <= nw;
-    double* V = smem;                 // kRowsCap x np
-    double* rv = V + kRowsCap * np;   // kRowsCap: residual of each row
+    const int wpt = persistent ? nw / ntiles : 1;  // warps per tile (k split)
+    double* rec[2];
+    rec[0] = smem;                                  // kRowsCap / 2 records each
+    rec[1] = rec[0] + (kRowsCap / 2) * kMargRecord;
+    double* rv = rec[1] + (kRowsCap / 2) * kMargRecord;  // kRowsCap: residual of each row
+    double* jrv = rv + kRowsCap;                    // kRowsCap: rho derivative of each factor row
+    double* V = jrv + kRowsCap;                     // rows x np
     __shared__ double red[kRowsThreads / 32];
     const double cutoff = fmax(1e-12, 1e-9 * fmax(0.0, M.maxD[w]));
     const int* visCol = M.visCol + mw.vis0;
@@ -227,74 +254,71 @@ __global__ void __launch_bounds__(kRowsThreads, 1) k_marg_rows(DevBatch B, MargB
     for (int r = 0; r < 4; ++r)
 #pragma unroll
         for (int c = 0; c < 8; ++c) acc[r][c] = 0.0;
+    prefetchRecords(M, M.chunks[it.y], rec[0]);
+    cpAsyncWaitAll();
+    __syncthreads();
     for (int ci = it.y; ci < it.z; ++ci) {
         const int4 ch = M.chunks[ci];
-        const int kp = 2 * (ch.w - ch.z), K = kp + (ch.y - ch.x);
-        // ---- dense rows, one warp per landmark
+        const double* rc = rec[(ci - it.y) & 1];
+        const int nobs = ch.w - ch.z, kp = 2 * nobs, K = kp + (ch.y - ch.x);
+        // ---- factor rows, one warp per observation
+        for (int o = warp; o < nobs; o += nw) {
+            const double* r = rc + kMargRecord * o;
+            const unsigned long long pk = (unsigned long long)__double_as_longlong(r[55]);
+            if (lane == 0) {
+                rv[2 * o] = r[50];
+                rv[2 * o + 1] = r[51];
+                jrv[2 * o] = r[52];
+                jrv[2 * o + 1] = r[53];
+                cost += r[54];
+                rss += r[50] * r[50] + r[51] * r[51];
+            }
+            double* v0row = V + (long long)(2 * o) * np;
+            double* v1row = v0row + np;
+            for (int col = lane; col < np; col += 32) {
+                int slot = -1, base = 0;
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const int start = (int)(short)(unsigned short)(pk >> (16 * b));
+                    if (start >= 0) {
+                        if (col >= start && col < start + 6) slot = base + col - start;
+                        base += 6;
+                    }
+                }
+                if (mw.visTd >= 0 && col == mw.visTd) slot = base;
+                v0row[col] = slot < 0 ? 0.0 : r[slot];
+                v1row[col] = slot < 0 ? 0.0 : r[25 + slot];
+            }
+        }
+        __syncthreads();
+        // ---- Schur rows, one warp per landmark
         for (int l = ch.x + warp; l < ch.y; l += nw) {
             const MargElim me = M.elim[l];
             const int nob = B.lmObsBegin[me.lm + 1] - B.lmObsBegin[me.lm];
-            const int row0 = 2 * (me.obs0 - ch.z);
-            double sc[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) sc[q] = 0.0;
+            const int r0 = 2 * (me.obs0 - ch.z), r1 = r0 + 2 * nob;
             double d = 0, bl = 0;
-            for (int t = 0; t < nob; ++t) {
-                const double* rec = M.rows + (long long)kMargRecord * (me.obs0 + t);
-                const double lo = rec[lane], hi = lane < kMargRecord - 32 ? rec[32 + lane] : 0.0;
-                const double wr0 = __shfl_sync(0xffffffffu, hi, 18), wr1 = __shfl_sync(0xffffffffu, hi, 19);
-                const double wj0 = __shfl_sync(0xffffffffu, hi, 20), wj1 = __shfl_sync(0xffffffffu, hi, 21);
-                const double oc = __shfl_sync(0xffffffffu, hi, 22);
-                const unsigned long long pk = (unsigned long long)__double_as_longlong(__shfl_sync(0xffffffffu, hi, 23));
-                d += wj0 * wj0 + wj1 * wj1;
-                bl += wj0 * wr0 + wj1 * wr1;
-                if (lane == 0) {
-                    cost += oc;
-                    rss += wr0 * wr0 + wr1 * wr1;
-                    rv[row0 + 2 * t] = wr0;
-                    rv[row0 + 2 * t + 1] = wr1;
-                }
-                double* v0row = V + (long long)(row0 + 2 * t) * np;
-                double* v1row = v0row + np;
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    if (q >= nb) break;
-                    const int col = 32 * q + lane;
-                    int slot = -1, base = 0;
-#pragma unroll
-                    for (int b = 0; b < 4; ++b) {
-                        const int start = (int)(short)(unsigned short)(pk >> (16 * b));
-                        if (start >= 0) {
-                            if (col >= start && col < start + 6) slot = base + col - start;
-                            base += 6;
-                        }
-                    }
-                    if (mw.visTd >= 0 && col == mw.visTd) slot = base;
-                    const int s0 = slot < 0 ? 0 : slot, s1 = s0 + 25;
-                    const double x0 = __shfl_sync(0xffffffffu, lo, s0);
-                    const double x1lo = __shfl_sync(0xffffffffu, lo, s1 & 31);
-                    const double x1hi = __shfl_sync(0xffffffffu, hi, s1 & 31);
-                    const double v0 = slot < 0 ? 0.0 : x0;
-                    const double v1 = slot < 0 ? 0.0 : (s1 < 32 ? x1lo : x1hi);
-                    v0row[col] = v0;
-                    v1row[col] = v1;
-                    sc[q] += v0 * wj0 + v1 * wj1;
-                }
+            for (int k = r0; k < r1; ++k) {
+                d += jrv[k] * jrv[k];
+                bl += jrv[k] * rv[k];
             }
             const bool eliminate = d > cutoff;
             const double scale = eliminate ? 1.0 / sqrt(d) : 0.0;
             const int sr = kp + (l - ch.x);
-#pragma unroll
-            for (int q = 0; q < 8; ++q)
-                if (q < nb) V[(long long)sr * np + 32 * q + lane] = sc[q] * scale;
+            for (int col = lane; col < np; col += 32) {
+                double sc = 0;
+                for (int k = r0; k < r1; ++k) sc += V[(long long)k * np + col] * jrv[k];
+                V[(long long)sr * np + col] = sc * scale;
+            }
             if (lane == 0) {
                 rv[sr] = bl * scale;
                 if (eliminate) reduction += 0.5 * bl * bl / d;
             }
         }
         __syncthreads();
-        // ---- rank updates of the upper tiles, gradient columns
-        for (int t = warp; t < ntiles; t += nw) {
+        // ---- next chunk's records in flight; rank updates; gradient columns
+        if (ci + 1 < it.z) prefetchRecords(M, M.chunks[ci + 1], rec[(ci + 1 - it.y) & 1]);
+        for (int u = warp; u < ntiles * wpt; u += nw) {
+            const int t = u / wpt, part = u % wpt;
             int bi, bj;
             tileOf(t, nb, bi, bj);
             if (!persistent)
@@ -304,8 +328,8 @@ __global__ void __launch_bounds__(kRowsThreads, 1) k_marg_rows(DevBatch B, MargB
                     for (int c = 0; c < 8; ++c) acc[r][c] = 0.0;
             const double* Va = V + bi * 32 + 2 * rg;
             const double* Vb = V + bj * 32 + 2 * cg;
-            rankUpdate<false>(acc, Va, Vb, 0, kp, np);
-            rankUpdate<true>(acc, Va, Vb, kp, K, np);
+            rankUpdate<false>(acc, Va, Vb, part, kp, wpt, np);
+            rankUpdate<true>(acc, Va, Vb, kp + part, K, wpt, np);
             if (!persistent) flushTile(acc, bi, bj, lane, n, visCol, H, mw.m);
         }
         if (gj >= 0) {
@@ -314,11 +338,12 @@ __global__ void __launch_bounds__(kRowsThreads, 1) k_marg_rows(DevBatch B, MargB
             for (int k = kp; k < K; ++k) s -= V[(long long)k * np + gj] * rv[k];
             g += s;
         }
+        cpAsyncWaitAll();
         __syncthreads();
     }
-    if (persistent && warp < ntiles) {
+    if (persistent && warp < ntiles * wpt) {
         int bi, bj;
-        tileOf(warp, nb, bi, bj);
+        tileOf(warp / wpt, nb, bi, bj);
         flushTile(acc, bi, bj, lane, n, visCol, H, mw.m);
     }
     if (gj >= 0 && gj < n && g != 0.0) atomicAdd(&M.b[mw.vec0 + visCol[gj]], g);
@@ -871,19 +896,33 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_victim(MargBatch M) {
 }
 
 // ---------------------------------------------------------------------------------------
-// Full-rank fast path, one CTA per window with the separator information E in
-// shared memory (n <= kFastMaxN).  When every eigenvalue of E exceeds the
-// cutoff max(1e-12, 1e-9 lambda_max) nothing is cut, and any square root gives
-// the same prior: with E = L L^T (Cholesky), A = L^T and r0 = L^{-1} b satisfy
-// A^T A = E and A^T r0 = b, exactly the prior sqrt(lambda) u^T, u^T b /
-// sqrt(lambda) over all eigenpairs.  The eigenvalue facts come from a
-// Householder tridiagonalization T of E: lambda_max by Sturm-sequence
-// multisection on T (the number of eigenvalues below x is the number of
-// negative pivots of T - x I), and the rank test as a single count at twice
-// the cutoff.  Windows without a prior (gauge freedom, rank deficient) and
-// windows that fail the test are left to k_marg_eigen.
+// Fast path, one CTA per window with the separator information E in shared
+// memory (n <= kFastMaxN), for spectra with a clean gap at the cutoff
+// max(1e-12, 1e-9 lambda_max): nf eigenvalues within |lambda| < 1e-6 cutoff,
+// the other k = n - nf above twice the cutoff.  The eigen path then keeps
+// exactly the k large eigenpairs, and its prior (A = sqrt(lambda) u^T,
+// r0 = u^T b / sqrt(lambda)) is characterised by A^T A = E_k (E without its
+// negligible part) and A^T r0 = P b, P the orthogonal projector onto
+// range(E_k).  Here instead:
+//   - a Householder tridiagonalization T of E gives the spectral facts by
+//     Sturm counts (eigenvalues of T below x = negative pivots of T - x I):
+//     lambda_max and the smallest kept eigenvalue by multisection, the gap by
+//     three counts;
+//   - a diagonally pivoted Cholesky stopped after k pivots gives E ~ L L^T
+//     and A = L^T (k x n, in pivot order);
+//   - b is projected off null(A) explicitly: with N a basis of null(A) (one
+//     back substitution per free column), P b = b - N (N^T N)^{-1} N^T b,
+//     and r0 solves A^T r0 = P b by forward substitution over the pivots.
+// Accepted when every pivot exceeds cutoff / 10 and the uneliminated
+// remainder R satisfies |R|_F <= 1e-10 lambda_kept_min: by the sin-theta
+// bound null(A) is then within 1e-10 of the negligible eigenspace, so A^T A
+// and A^T r0 agree with the eigen path's far below its own rounding.  Other
+// windows are left to k_marg_eigen.
 constexpr int kFastMaxN = 160;
-__host__ __device__ constexpr size_t fastSmemBytes(int n) { return sizeof(double) * ((size_t)n * n + 5 * (size_t)n); }
+constexpr int kFastMaxFree = 16;  // null directions handled by the projection
+__host__ __device__ constexpr size_t fastSmemBytes(int n) {
+    return sizeof(double) * ((size_t)n * n + 5 * (size_t)n) + sizeof(int) * 3 * (size_t)n;
+}
 
 // Number of eigenvalues of the symmetric tridiagonal (d, e) below x, e[i]
 // coupling i and i + 1.
@@ -906,7 +945,7 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_fast(MargBatch M) {
     const int n = mw.nr;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
     if (tid == 0) M.fast[w] = 0;
-    if (mw.m == 0 || n == 0 || n > kFastMaxN || !mw.hasPrior || M.status[w] != CGMLI_OK) return;
+    if (mw.m == 0 || n == 0 || n > kFastMaxN || M.status[w] != CGMLI_OK) return;
     extern __shared__ double fsm[];
     double* S = fsm;          // n x n row-major
     double* v = S + n * n;
@@ -914,7 +953,12 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_fast(MargBatch M) {
     double* wv = p + n;
     double* d = wv + n;
     double* e = d + n;
-    __shared__ double sc[4];
+    int* piv = reinterpret_cast<int*>(e + n);  // pivot of each Cholesky step
+    int* stepOf = piv + n;                     // step at which an index was pivoted (n: never)
+    int* rem = stepOf + n;                     // indices not yet pivoted
+    __shared__ double sc[8];
+    __shared__ int isc[2];
+    __shared__ double G[kFastMaxFree * kFastMaxFree], h[kFastMaxFree];
     const double* E = M.sepH + mw.sep0;
     for (int t = tid; t < n * n; t += blockDim.x) S[t] = E[t];
     __syncthreads();
@@ -1005,47 +1049,187 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_fast(MargBatch M) {
     }
     const double lmax = hi;
     const double cutoff = fmax(1e-12, 1e-9 * fmax(0.0, lmax));
-    if (tid == 0) sc[3] = sturmCount(d, e, n, 2.0 * cutoff, pivmin) == 0 ? 1.0 : 0.0;
+    const double small = 1e-6 * cutoff;
+    if (tid == 0) {
+        const int c2 = sturmCount(d, e, n, 2.0 * cutoff, pivmin);
+        const bool gap = sturmCount(d, e, n, small, pivmin) == c2 && sturmCount(d, e, n, -small, pivmin) == 0 && c2 < n &&
+                         c2 <= kFastMaxFree;
+        isc[0] = gap ? c2 : -1;
+    }
     __syncthreads();
-    if (sc[3] == 0.0) return;  // an eigenvalue within twice the cutoff: eigen path
-    // Cholesky E = L L^T (lower triangle of S)
+    const int nf = isc[0];
+    if (nf < 0) return;  // eigenvalues near the cutoff (or too many below it): eigen path
+    const int k = n - nf;
+    // smallest kept eigenvalue: the point where the Sturm count passes nf
+    double keptMin = 2.0 * cutoff;
+    if (nf > 0) {
+        double klo = 2.0 * cutoff, khi = lmax;
+        for (int round = 0; round < 8 && khi - klo > 1e-3 * klo; ++round) {
+            const double x = klo + (khi - klo) * (tid + 1) / (T + 1);
+            const int below = __syncthreads_count(sturmCount(d, e, n, x, pivmin) <= nf);
+            const double nlo = below > 0 ? klo + (khi - klo) * below / (T + 1) : klo;
+            const double nhi = below < T ? klo + (khi - klo) * (below + 1) / (T + 1) : khi;
+            klo = nlo;
+            khi = nhi;
+        }
+        keptMin = klo;
+    }
+    // pivoted Cholesky on the full symmetric E: step s takes the largest
+    // remaining diagonal p, stores the column l (over the remaining indices)
+    // in column p of S and updates the remaining block by - l l^T
     for (int t = tid; t < n * n; t += blockDim.x) S[t] = E[t];
+    for (int x = tid; x < n; x += blockDim.x) {
+        rem[x] = x;
+        stepOf[x] = n;
+    }
     __syncthreads();
-    for (int k = 0; k < n; ++k) {
-        const double dkk = S[k * n + k];
-        if (!(dkk > 0)) return;  // not positive definite after all: eigen path (uniform)
-        const double lkk = sqrt(dkk);
-        for (int i = k + 1 + tid; i < n; i += blockDim.x) p[i] = S[i * n + k] / lkk;
+    int size = n;
+    for (int st = 0; st < k; ++st) {
+        if (warp == 0) {
+            double best = -INFINITY;
+            int bq = 0;
+            for (int q = lane; q < size; q += 32) {
+                const double x = S[rem[q] * n + rem[q]];
+                if (x > best) { best = x; bq = q; }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int oq = __shfl_xor_sync(0xffffffffu, bq, o);
+                if (ob > best || (ob == best && oq < bq)) { best = ob; bq = oq; }
+            }
+            if (lane == 0) {
+                const int pv = rem[bq];
+                sc[4] = best;
+                isc[1] = pv;
+                rem[bq] = rem[size - 1];
+                stepOf[pv] = st;
+                piv[st] = pv;
+            }
+        }
         __syncthreads();
-        if (tid == 0) S[k * n + k] = lkk;
-        for (int i = k + 1 + tid; i < n; i += blockDim.x) S[i * n + k] = p[i];
-        for (int i = k + 1 + warp; i < n; i += nw) {
-            const double lik = p[i];
-            for (int j = k + 1 + lane; j <= i; j += 32) S[i * n + j] -= lik * p[j];
+        const double dpp = sc[4];
+        const int pv = isc[1];
+        --size;
+        if (!(dpp > 0.1 * cutoff)) return;  // a weak pivot among the kept ones: eigen path (uniform)
+        const double lkk = sqrt(dpp);
+        for (int q = tid; q < size; q += blockDim.x) {
+            const int i = rem[q];
+            const double l = S[i * n + pv] / lkk;
+            v[q] = l;
+            S[i * n + pv] = l;
+        }
+        if (tid == 0) S[pv * n + pv] = lkk;
+        __syncthreads();
+        for (int qi = warp; qi < size; qi += nw) {
+            const double li = v[qi];
+            double* row = S + rem[qi] * n;
+            for (int qj = lane; qj < size; qj += 32) row[rem[qj]] -= li * v[qj];
         }
         __syncthreads();
     }
-    // r0 = L^{-1} b (column sweep by one warp), A = L^T
     const double* bs = M.sepB + mw.vec0;
+    if (nf > 0) {
+        // the remainder must be negligible against the kept spectrum
+        if (warp == 0) {
+            double f2 = 0;
+            for (int t = lane; t < nf * nf; t += 32) {
+                const double x = S[rem[t / nf] * n + rem[t % nf]];
+                f2 += x * x;
+            }
+            f2 = mWarpSum(f2);
+            if (lane == 0) sc[5] = sqrt(f2);
+        }
+        __syncthreads();
+        if (!(sc[5] <= 1e-10 * keptMin)) return;  // eigen path (uniform)
+        // null(A): for free index f, N_f = e_f + sum_s alpha_s e_{p_s} with
+        // A N_f = 0, by back substitution over the pivots; alpha_s is kept in
+        // S[p_s][f] (row p_s of a non-pivot column holds no factor entry)
+        for (int fq = warp; fq < nf; fq += nw) {
+            const int f = rem[fq];
+            for (int st = k - 1; st >= 0; --st) {
+                const int ps = piv[st];
+                double sum = 0;
+                for (int t = st + 1 + lane; t < k; t += 32) sum += S[piv[t] * n + ps] * S[piv[t] * n + f];
+                sum = mWarpSum(sum);
+                const double alpha = -(S[f * n + ps] + sum) / S[ps * n + ps];
+                if (lane == 0) S[ps * n + f] = alpha;
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        // G = N^T N, h = N^T b
+        for (int t = warp; t < nf * (nf + 1); t += nw) {
+            const int a = t / (nf + 1), c = t % (nf + 1);
+            const int fa = rem[a];
+            double sum = 0;
+            if (c < nf) {
+                const int fc = rem[c];
+                for (int st = lane; st < k; st += 32) sum += S[piv[st] * n + fa] * S[piv[st] * n + fc];
+            } else {
+                for (int st = lane; st < k; st += 32) sum += S[piv[st] * n + fa] * bs[piv[st]];
+            }
+            sum = mWarpSum(sum);
+            if (lane == 0) {
+                if (c < nf) G[a * nf + c] = sum + (a == c ? 1.0 : 0.0);
+                else h[a] = sum + bs[fa];
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {  // G y = h (G >= I), y into h
+            for (int j = 0; j < nf; ++j) {
+                double djj = G[j * nf + j];
+                for (int q = 0; q < j; ++q) djj -= G[j * nf + q] * G[j * nf + q];
+                djj = sqrt(djj);
+                G[j * nf + j] = djj;
+                for (int i = j + 1; i < nf; ++i) {
+                    double x = G[i * nf + j];
+                    for (int q = 0; q < j; ++q) x -= G[i * nf + q] * G[j * nf + q];
+                    G[i * nf + j] = x / djj;
+                }
+            }
+            for (int i = 0; i < nf; ++i) {
+                double x = h[i];
+                for (int q = 0; q < i; ++q) x -= G[i * nf + q] * h[q];
+                h[i] = x / G[i * nf + i];
+            }
+            for (int i = nf - 1; i >= 0; --i) {
+                double x = h[i];
+                for (int q = i + 1; q < nf; ++q) x -= G[q * nf + i] * h[q];
+                h[i] = x / G[i * nf + i];
+            }
+        }
+        __syncthreads();
+    }
+    // P b at the pivots (N's entries there are the alphas), in pivot order
+    for (int st = tid; st < k; st += blockDim.x) {
+        const int ps = piv[st];
+        double x = bs[ps];
+        for (int q = 0; q < nf; ++q) x -= h[q] * S[ps * n + rem[q]];
+        p[st] = x;
+    }
+    __syncthreads();
+    // r0: A^T r0 = P b over the pivot rows, A[s][p_t] = S[p_t][p_s] (t >= s)
     if (warp == 0) {
-        for (int i = lane; i < n; i += 32) v[i] = bs[i];
-        __syncwarp();
-        for (int k = 0; k < n; ++k) {
-            const double yk = v[k] / S[k * n + k];
+        for (int st = 0; st < k; ++st) {
+            const int ps = piv[st];
+            const double r = p[st] / S[ps * n + ps];
             __syncwarp();
-            if (lane == 0) v[k] = yk;
-            for (int i = k + 1 + lane; i < n; i += 32) v[i] -= S[i * n + k] * yk;
+            if (lane == 0) p[st] = r;
+            for (int t = st + 1 + lane; t < k; t += 32) p[t] -= S[piv[t] * n + ps] * r;
             __syncwarp();
         }
     }
     __syncthreads();
     double* A = M.A + mw.sep0;
     double* r0 = M.r0 + mw.vec0;
-    for (int i = warp; i < n; i += nw)
-        for (int k = lane; k < n; k += 32) A[(long long)i * n + k] = k >= i ? S[k * n + i] : 0.0;
-    for (int i = tid; i < n; i += blockDim.x) r0[i] = v[i];
+    for (int st = warp; st < k; st += nw) {
+        const int ps = piv[st];
+        for (int x = lane; x < n; x += 32) A[(long long)st * n + x] = stepOf[x] >= st ? S[x * n + ps] : 0.0;
+    }
+    for (int st = tid; st < k; st += blockDim.x) r0[st] = p[st];
     if (tid == 0) {
-        M.rank[w] = n;
+        M.rank[w] = k;
         M.stats[4 * w + 3] = cutoff;
         M.fast[w] = 1;
     }
@@ -1057,7 +1241,7 @@ __global__ void __launch_bounds__(kEigenThreads) k_marg_eigen(MargBatch M) {
     const int w = blockIdx.x;
     const MargWin mw = M.win[w];
     const int nr = mw.nr;
-    if (M.fast[w]) return;  // prior formed by k_marg_classify
+    if (M.fast[w]) return;  // prior formed by k_marg_fast
     if (mw.m == 0 || nr == 0 || M.status[w] != CGMLI_OK) {
         if (threadIdx.x == 0) M.rank[w] = 0;
         return;
@@ -1194,9 +1378,12 @@ size_t margVisualSmemBytes(int maxNc) {
 // batch whose largest separator has maxNr columns; returns the eigen CTA's
 // dynamic shared memory in eigenSmem.
 size_t margRowsSmemBytes(int maxNv) {
-    const size_t np = ((size_t)maxNv + 31) & ~(size_t)31;
-    return sizeof(double) * ((size_t)kRowsCap * np + kRowsCap);
+    const int np = (maxNv + 31) & ~31;
+    size_t v = 0;  // widest rows x np over the padded widths up to np
+    for (int p = 32; p <= np; p += 32) v = std::max(v, (size_t)rowsCapOf(p) * p);
+    return sizeof(double) * ((size_t)kRowsCap * kMargRecord + 2 * kRowsCap + v);
 }
+int margRowsCap(int nv) { return rowsCapOf((nv + 31) & ~31); }
 cudaError_t configureMarginalization(size_t visualSmem, size_t rowsSmem, int maxNr, int maxFastNr, long long* eigenSmem,
                                      long long* fastSmem) {
     cudaError_t e = cudaFuncSetAttribute(k_marg_visual, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)visualSmem);
