@@ -62,6 +62,7 @@ def parse():
     p.add_argument("--cpu-sample", type=int, default=24, help="windows timed on the host for the CPU baseline")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--plain-windows", type=int, default=16, help="single-window solves timed for the plain path")
+    p.add_argument("--marg-steps", type=int, default=3, help="timed batched marginalizations of the solved batch (0: off)")
     p.add_argument("--serve-rate", type=float, default=5000.0, help="offered request rate of the served run (requests/s, 0: off)")
     p.add_argument("--serve-seconds", type=float, default=3.0, help="duration of the served run's arrivals")
     p.add_argument("--serve-pool", type=int, default=512, help="distinct windows the served requests draw from")
@@ -328,6 +329,20 @@ def main():
                 "launch_avg_ms": lin_ms / max(1, lin_calls), "window_linearizations_per_step": lin_passes,
                 "kernel_ms_per_step": {k: v[0] / args.steps for k, v in ktimes.items()}}
 
+    # batched marginalization of the solved windows: oldest keyframe, OLD policy,
+    # device time of the whole formation (CUDA events on the solver's stream)
+    marg = None
+    if args.marg_steps > 0:
+        mms = []
+        for it in range(1 + args.marg_steps):
+            solver.marginalize([0] * args.windows, abi.MARGIN_OLD)
+            solver.synchronize()
+            if it > 0:
+                mms.append(solver.timing()[0])
+        marg_ms = max_over_ranks(sum(mms) / len(mms), dist)
+        marg = {"ms": marg_ms, "windows_per_s": world * args.windows / (marg_ms / 1e3), "launches": solver.timing()[1],
+                "workload": "Schur-complement prior of every window of the solved batch, oldest keyframe (OLD)"}
+
     # end to end through the C ABI with host buffers: topology + upload, solve, read back
     h2d = sum(window_bytes(w)[0] for w in windows)
     d2h = sum(window_bytes(w)[1] for w in windows)
@@ -414,7 +429,7 @@ def main():
             "clocks": clocks.summary(), "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
             "cpu_baseline": cpu_baseline, "plain_path": plain,
             "served_vs_plain": (value / world) / plain["windows_per_s"] if plain else None,
-            "served": served,
+            "served": served, "marginalization": marg,
             "batch_latency_ms": {"p50": sorted(dev_ms)[len(dev_ms) // 2], "p99": max(dev_ms)},
             "window_status": statuses, "wall_s": wall,
         }
