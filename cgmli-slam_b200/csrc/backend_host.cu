@@ -26,7 +26,6 @@ namespace cgmli {
 size_t linearizeSmemBytes(int maxNs);
 size_t factorSmemBytes(int maxNr);
 cudaError_t configureKernels(size_t linSmem, size_t facSmem);
-int schurRowsPerChunk(int Npc);
 int launchIteration(const DevBatch& B, const LaunchPlan& P, int refinement, int maxIterations, int probe, double* Sdebug,
                     cudaStream_t s, LaunchHook hook, void* ctx);
 int launchLmInit(const DevBatch& B, double lambda0, cudaStream_t s);
@@ -105,6 +104,8 @@ struct cgmli_solver {
     DArray<int4> dRuns;
     DArray<int2> dTiles;
     DArray<int4> dPairChunks, dSchurChunks;
+    DArray<int> schurCols;
+    DArray<unsigned short> lmUmap;
     DArray<int> obLm, keyOrder;
     DArray<double> keyRows;
     DArray<double> sch;
@@ -203,7 +204,7 @@ struct cgmli_solver {
                                &solveStatus, &lmNx, &obXslot};
         for (auto* a : ints) a->release();
         lmC0.release(); dWin.release(); dLm.release(); dRuns.release(); dTiles.release();
-        dPairChunks.release(); dSchurChunks.release(); obLm.release(); keyOrder.release(); keyRows.release(); sch.release();
+        dPairChunks.release(); dSchurChunks.release(); schurCols.release(); lmUmap.release(); obLm.release(); keyOrder.release(); keyRows.release(); sch.release();
         snapPose.release(); snapSb.release(); snapExt.release(); snapTd.release(); snapRho.release();
         dMargWin.release(); dMargElim.release();
         DArray<int>* mi[] = {&margCols, &margObsMap, &margPoseCol, &margSbCol, &margExtCol, &margRank, &margStatus, &margFast,
@@ -309,6 +310,8 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     CK(S->dTiles.upload(hb.tiles, st));
     CK(S->dPairChunks.upload(hb.pairChunks, st));
     CK(S->dSchurChunks.upload(hb.schurChunks, st));
+    CK(S->schurCols.upload(hb.schurCols, st));
+    CK(S->lmUmap.upload(hb.lmUmap, st));
     CK(S->camR.upload(hb.camR, st)); CK(S->camT.upload(hb.camT, st)); CK(S->camExt.upload(hb.camExt, st));
     CK(S->lmWin.upload(hb.lmWin, st)); CK(S->lmKf.upload(hb.lmKf, st)); CK(S->lmCam.upload(hb.lmCam, st)); CK(S->lmObsBegin.upload(hb.lmObsBegin, st));
     CK(S->lmNs.upload(hb.lmNs, st)); CK(S->lmNx.upload(hb.lmNx, st)); CK(S->lmSupp0.upload(hb.lmSupp0, st));
@@ -346,6 +349,7 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     B.lmWin = S->lmWin.p; B.lmKf = S->lmKf.p; B.lmCam = S->lmCam.p; B.lmObsBegin = S->lmObsBegin.p;
     B.lmBearing = S->lmBearing.p; B.lmVel = S->lmVel.p; B.lmTime = S->lmTime.p;
     B.lmNs = S->lmNs.p; B.lmNx = S->lmNx.p; B.lmSupp0 = S->lmSupp0.p; B.supp = S->supp.p; B.lmC0 = S->lmC0.p;
+    B.lmUmap = S->lmUmap.p; B.schurCols = S->schurCols.p;
     B.obXslot = S->obXslot.p;
     B.lmC = S->lmC.p; B.lmD = S->lmD.p; B.lmG = S->lmG.p; B.lmCost = S->lmCost.p; B.lmValid = S->lmValid.p;
     B.lmDelta = S->lmDelta.p; B.lmPred = S->lmPred.p; B.lmTrial = S->lmTrial.p; B.lmMaxInc = S->lmMaxInc.p;

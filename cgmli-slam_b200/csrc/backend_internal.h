@@ -20,7 +20,7 @@ namespace cgmli {
 constexpr int kMaxTrackChunk = 32;     // factors per warp pass
 constexpr int kMaxSupport = 64;        // keyframe slots per landmark
 constexpr int kLinThreads = 256;       // linearization CTA
-constexpr int kFactorThreads = 512;    // factorization CTA
+constexpr int kFactorThreads = 256;    // factorization CTA
 
 struct WinDesc {
     int K, E, C, L, F, nImu;
@@ -33,7 +33,7 @@ struct WinDesc {
     long long acc0;      // offset of the visual accumulator: Npc(Npc+1)/2 + 3*Npc
     long long sch0;      // offset of the Schur term: Npc(Npc+1)/2
     long long priorA0, priorR00, priorRef0;
-    long long imuScratch0;  // nImu * 465 doubles
+    long long imuScratch0;  // nImu * 930 doubles (raw and whitened factor)
     long long priorScratch0;  // priorRank*priorCols + priorCols*6 doubles
     double huber, minInv;
 };
@@ -58,6 +58,8 @@ struct DevBatch {
     const double* lmBearing; const double* lmVel; const double* lmTime;
     const int* lmNs; const int* lmNx; const int* lmSupp0; const int* supp;  // support: s keyframes (anchor first), then x extrinsics
     const long long* lmC0;                                // offset of the landmark's cross vector
+    const unsigned short* lmUmap;  // per cross-vector entry: its column within the landmark's Schur chunk
+    const int* schurCols;         // per Schur chunk: count, then the ascending visual columns
     double* lmC; double* lmD; double* lmG; double* lmCost; int* lmValid;
     double* lmDelta; double* lmPred; double* lmTrial; double* lmMaxInc; int* lmTrialValid;
     // observations
@@ -95,6 +97,15 @@ constexpr int kMargMaxNc = 200;     // marginalization columns touched by one el
 constexpr int kMargMaxSep = 1024;   // separator columns (Jacobi pair tables hold 512 pairs)
 constexpr int kMargThreads = 512;   // victim CTAs
 constexpr int kEigenThreads = 512;  // eigen CTAs
+// Schur chunks of the linearization (k_lin_schur): rows x padded width of the
+// chunk's column union + 1 fit the CTA's shared rows.
+constexpr int kSchurThreads = 256;
+constexpr int kSchurSmemDoubles = 12288;
+constexpr int kSchurMaxRows = 128;
+inline bool schurChunkFits(int rows, int unionCols) {
+    const int np = (unionCols + 1 + 31) / 32 * 32;
+    return rows <= kSchurMaxRows && (long long)rows * np <= kSchurSmemDoubles;
+}
 constexpr int kMargLmThreads = 128; // one CTA per eliminated landmark (windows above kRowsMaxN)
 constexpr int kRowsMaxN = 256;      // visual columns of a window on the dense-row path
 constexpr int kRowsCap = 96;        // rows of one dense-row chunk (2 per observation + 1 per landmark)

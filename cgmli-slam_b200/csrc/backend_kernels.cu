@@ -11,6 +11,7 @@
 #include "../../include/cgmli_backend.h"
 #include "backend_internal.h"
 #include "device_math.cuh"
+#include "dense_tiles.cuh"
 #include "factor_eval.cuh"
 
 namespace cgmli {
@@ -85,8 +86,6 @@ constexpr int kCompact = 25;        // anchor pose 6 | observer pose 6 | ext_a 6
 constexpr int kPairs = kCompact * (kCompact + 1) / 2;
 constexpr int kPairSlots = (kPairs + 31) / 32;  // compact pairs per lane
 constexpr int kPairWarps = 4;       // warps per CTA of k_lin_pairs
-constexpr int kSchurThreads = 256;
-constexpr int kSchurSmemDoubles = 12800;  // dense rows of a Schur chunk
 // A factor's FactorOut is staged per lane in shared memory with an odd stride
 // (conflict-free lane rows); slot 54 carries the squared robust weight.
 constexpr int kOut = 55;
@@ -335,74 +334,64 @@ __global__ void __launch_bounds__(kPairWarps * 32) k_lin_pairs(DevBatch B, const
     }
 }
 
-// ---- L3: Schur term as a dense SYRK per chunk of landmarks ----------------------------
-// Shared memory: rows x W1 doubles, W1 = Npc + 1 (the last column carries
-// g_l / sqrt(dt_l) for B_v).  Each thread owns 4x4 output tiles of the upper
-// triangle and accumulates them in registers over the chunk's rows.
-__global__ void __launch_bounds__(kSchurThreads) k_lin_schur(DevBatch B, const int4* chunks) {
-    extern __shared__ double Ct[];
-    const int4 ch = chunks[blockIdx.x];  // {window, first landmark, end landmark, rows}
+// ---- L3: Schur term as a compact SYRK per chunk of landmarks -------------------------
+// A chunk is a run of consecutive landmarks (support-sorted, so neighbours share
+// most columns) with the ascending union U of their visual support columns.
+// Each landmark's row c_l / sqrt(dt_l) is expanded over U in shared memory (its
+// local -> U map is built on the host), with g_l / sqrt(dt_l) as column |U| for
+// B_v.  The rank update uses 32 x 32 tiles, one per warp (4 x 8 per lane);
+// spare warps split the rows when the tiles are fewer than the warps.  Every
+// tile is added to the window's Schur sum once per chunk.
+__global__ void __launch_bounds__(kSchurThreads, 2) k_lin_schur(DevBatch B, const int4* chunks) {
+    extern __shared__ __align__(16) double Rw[];
+    const int4 ch = chunks[blockIdx.x];  // {window, first landmark, end landmark, offset of the column list}
     const int wdx = ch.x;
     const int mode = B.lm[wdx].mode;
     if (mode == kModeDone) return;
     const WinDesc wd = B.win[wdx];
     const double lambda = B.lm[wdx].lambda;
-    const int K = wd.K, Npc = wd.Npc, W1 = Npc + 1;
-    const int tdCol = 6 * K + (wd.estExt ? 6 * wd.E : 0);
+    const int Npc = wd.Npc;
+    const int nu = B.schurCols[ch.w];
+    const int* U = B.schurCols + ch.w + 1;
+    const int n = nu + 1, np = (n + 31) & ~31, nb = np >> 5, ntiles = nb * (nb + 1) / 2;
     const int rows = ch.z - ch.y;
-    for (int i = threadIdx.x; i < rows * W1; i += blockDim.x) Ct[i] = 0.0;
-    __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int r = warp; r < rows; r += kSchurThreads / 32) {
+    constexpr int nw = kSchurThreads / 32;
+    for (int r = warp; r < rows; r += nw) {
         const int l = ch.y + r;
-        const int s = B.lmNs[l], x = B.lmNx[l], ns = 6 * (s + x) + (wd.estTd ? 1 : 0);
-        const int* sk = B.supp + B.lmSupp0[l];
+        const int ns = 6 * (B.lmNs[l] + B.lmNx[l]) + (wd.estTd ? 1 : 0);
         const double d = B.lmD[l];
         const double scale = 1.0 / sqrt(d + lambda * fmax(d, 1e-6));
-        const double* c = B.lmC + B.lmC0[l];
-        double* row = Ct + (long long)r * W1;
-        for (int i = lane; i < ns; i += 32) row[pcOfLocal(i, s, x, sk, K, tdCol)] = scale * c[i];
-        if (lane == 0) row[Npc] = scale * B.lmG[l];
+        const long long c0 = B.lmC0[l];
+        double* row = Rw + (long long)r * np;
+        for (int c = lane; c < np; c += 32) row[c] = 0.0;
+        __syncwarp();
+        for (int i = lane; i < ns; i += 32) row[B.lmUmap[c0 + i]] = scale * B.lmC[c0 + i];
+        if (lane == 0) row[nu] = scale * B.lmG[l];
     }
     __syncthreads();
-    const int nt = (W1 + 3) / 4, tiles = nt * (nt + 1) / 2;
     double* sch = B.sch + wd.sch0;
     double* Bv = B.acc + wd.acc0 + (long long)Npc * (Npc + 1) / 2 + 2ll * Npc;
-    for (int tIdx = threadIdx.x; tIdx < tiles; tIdx += blockDim.x) {
-        // (ti, tj), ti <= tj, from the packed-upper enumeration of an nt x nt triangle
-        int ti = (int)((2.0f * nt + 1 - sqrtf((2.0f * nt + 1) * (2.0f * nt + 1) - 8.0f * tIdx)) * 0.5f);
-        if (ti < 0) ti = 0;
-        while (ti > 0 && ti * nt - ti * (ti - 1) / 2 > tIdx) --ti;
-        while ((ti + 1) * nt - (ti + 1) * ti / 2 <= tIdx) ++ti;
-        const int tj = ti + (tIdx - (ti * nt - ti * (ti - 1) / 2));
-        const int i0 = 4 * ti, j0 = 4 * tj;
-        double acc[4][4];
+    const int wpt = ntiles < nw ? nw / ntiles : 1;  // warps per tile (row split)
+    for (int u = warp; u < ntiles * wpt; u += nw) {
+        const int t = u / wpt, part = u % wpt;
+        int bi, bj;
+        tileOf(t, nb, bi, bj);
+        double acc[4][8];
+        zeroTile(acc);
+        rankUpdate<false>(acc, Rw + bi * 32 + 2 * (lane >> 2), Rw + bj * 32 + 2 * (lane & 3), part, rows, wpt, np);
 #pragma unroll
-        for (int a = 0; a < 4; ++a)
+        for (int r = 0; r < 4; ++r) {
+            const int i = tileRow(bi, lane, r);
 #pragma unroll
-            for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-        for (int r = 0; r < rows; ++r) {
-            const double* row = Ct + (long long)r * W1;
-            double u[4], v[4];
-#pragma unroll
-            for (int a = 0; a < 4; ++a) {
-                u[a] = i0 + a < W1 ? row[i0 + a] : 0.0;
-                v[a] = j0 + a < W1 ? row[j0 + a] : 0.0;
+            for (int c = 0; c < 8; ++c) {
+                const int j = tileCol(bj, lane, c);
+                const double v = acc[r][c];
+                if (i > j || j >= n || i >= nu || v == 0.0) continue;
+                if (j < nu) atomicAdd(&sch[upIdx(U[i], U[j], Npc)], v);
+                else atomicAdd(&Bv[U[i]], v);
             }
-#pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int b = 0; b < 4; ++b) acc[a][b] += u[a] * v[b];
         }
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                const int i = i0 + a, j = j0 + b;
-                if (i > j || j >= W1 || i >= Npc || acc[a][b] == 0.0) continue;
-                if (j < Npc) atomicAdd(&sch[upIdx(i, j, Npc)], acc[a][b]);
-                else atomicAdd(&Bv[i], acc[a][b]);
-            }
     }
 }
 
@@ -441,36 +430,54 @@ __global__ void __launch_bounds__(256) k_retained(DevBatch B, int trial) {
     __syncthreads();
     double cost = 0;
     const cgmli_frozen_imu* imus = reinterpret_cast<const cgmli_frozen_imu*>(B.imu);
+    // IMU factors: per factor 930 doubles of scratch, the raw error and Jacobian
+    // [e 15 | U 450] (one thread each), then the whitened [r 15 | J 450] = W [e | U]
+    // with one thread per output entry
     double* scratch = B.imuScratch + wd.imuScratch0;
     for (int i = threadIdx.x; i < wd.nImu; i += blockDim.x) {
         const int gi = wd.imu0 + i;
         const int k = B.imuKf[gi];
-        double* r = scratch + 465ll * i;
-        const bool ok = evalImu(imus[gi], B.pose[buf] + 7ll * k, B.sb[buf] + 9ll * k, B.pose[buf] + 7ll * (k + 1),
-                                B.sb[buf] + 9ll * (k + 1), r, trial ? nullptr : r + 15);
-        if (!ok) atomicOr(&bad, 1);
-        else for (int m = 0; m < 15; ++m) cost += 0.5 * r[m] * r[m];
+        double* raw = scratch + 930ll * i;
+        if (!evalImuRaw(imus[gi], B.pose[buf] + 7ll * k, B.sb[buf] + 9ll * k, B.pose[buf] + 7ll * (k + 1), B.sb[buf] + 9ll * (k + 1),
+                        raw, trial ? nullptr : raw + 15))
+            atomicOr(&bad, 1);
+    }
+    __syncthreads();
+    {
+        const int outs = trial ? 15 : 465;
+        for (int t = threadIdx.x; t < wd.nImu * outs; t += blockDim.x) {
+            const int f = t / outs, o = t % outs;
+            const double* W = imus[wd.imu0 + f].whitening;  // column-major 15 x 15
+            double* raw = scratch + 930ll * f;
+            // o < 15: residual row o; else Jacobian entry (row, column) of o - 15
+            const int row = o < 15 ? o : (o - 15) / 30;
+            const double* x = o < 15 ? raw : raw + 15 + (o - 15) % 30;
+            const int stride = o < 15 ? 1 : 30;
+            double v = 0;
+            for (int m = 0; m < 15; ++m) v += W[row + 15 * m] * x[stride * m];
+            raw[465 + o] = v;
+            if (!isfinite(v)) atomicOr(&bad, 1);
+            if (o < 15) cost += 0.5 * v * v;
+        }
     }
     __syncthreads();
     if (!trial) {
-        for (int i = 0; i < wd.nImu; ++i) {
+        for (long long t = threadIdx.x; t < 930ll * wd.nImu; t += blockDim.x) {
+            const int i = (int)(t / 930), e = (int)(t % 930);
             const int k = B.imuKf[wd.imu0 + i] - wd.kf0;
-            const double* r = scratch + 465ll * i;
+            const double* r = scratch + 930ll * i + 465;
             const double* J = r + 15;
-            for (int e = threadIdx.x; e < 930; e += blockDim.x) {
-                const int a = e < 900 ? e / 30 : e - 900, b = e % 30;
-                if (e < 900) {
-                    double v = 0;
-                    for (int m = 0; m < 15; ++m) v += J[30 * m + a] * J[30 * m + b];
-                    H[(long long)(15 * k + a) * Nr + 15 * k + b] += v;
-                } else {
-                    double v = 0;
-                    for (int m = 0; m < 15; ++m) v += J[30 * m + a] * r[m];
-                    g[15 * k + a] += v;
-                }
+            const int a = e < 900 ? e / 30 : e - 900, b = e % 30;
+            double v = 0;
+            if (e < 900) {
+                for (int m = 0; m < 15; ++m) v += J[30 * m + a] * J[30 * m + b];
+                atomicAdd(&H[(long long)(15 * k + a) * Nr + 15 * k + b], v);
+            } else {
+                for (int m = 0; m < 15; ++m) v += J[30 * m + a] * r[m];
+                atomicAdd(&g[15 * k + a], v);
             }
-            __syncthreads();
         }
+        __syncthreads();
     }
     if (wd.priorRank > 0) {
         const int rank = wd.priorRank, cols = wd.priorCols;
@@ -652,30 +659,83 @@ __device__ void blockedSolve(const double* L, int n, double* v, double* blk) {
     }
 }
 
+// Factorization panels of kFacPanel columns: the panel (rows k0.. of its
+// columns, padded to a multiple of 32 rows) is staged in shared memory and
+// factored left-looking by the whole CTA (column c of every row is reduced by
+// one dot product against the panel's earlier columns, then scaled), together
+// with the forward substitution of the right-hand side over the panel's
+// diagonal block.
+// The trailing lower triangle is then updated from the staged panel with the
+// 32 x 32 register tiles of dense_tiles.cuh (all warps), and the right-hand
+// side below the panel by a GEMV.  The backward substitution runs over the
+// same panels.  The undamped assembled system is kept in the strict upper
+// triangle of the window's slot (the factor uses the lower one) and its
+// diagonal in shared memory, for the prediction (and refinement) products.
+constexpr int kFacPanel = 32;
+
+// h = S_undamped v from the stored upper triangle (A[p + q n], p < q) and diagonal hd.
+__device__ void undampedProduct(const double* A, const double* hd, int n, const double* v, double* h) {
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+    for (int i = tid; i < n; i += blockDim.x) {  // columns j > i of row i: consecutive i coalesce
+        double s = hd[i] * v[i];
+        for (int j = i + 1; j < n; ++j) s += A[i + (long long)j * n] * v[j];
+        h[i] = s;
+    }
+    __syncthreads();
+    for (int i = warp; i < n; i += nw) {  // rows j < i of column i
+        double s = 0;
+        for (int j = lane; j < i; j += 32) s += A[j + (long long)i * n] * v[j];
+        s = warpSum(s);
+        if (lane == 0) h[i] += s;
+    }
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int refinement, double* Sdebug) {
     const int wdx = blockIdx.x;
     if (B.lm[wdx].mode == kModeDone) return;
     const WinDesc wd = B.win[wdx];
     const int n = wd.Nr, Npc = wd.Npc, K = wd.K;
     const double lambda = B.lm[wdx].lambda;
-    extern __shared__ double smem[];
-    double* x = smem;                        // n: right-hand side, then the increment
-    double* blk = smem + n;                  // kPanel x kPanel diagonal block of the solves
-    double* P = blk + kPanel * kPanel;       // panel: n rows x kPanel, column-major, leading dim m
+    extern __shared__ __align__(16) double smem[];
+    const int npad = ((n + 31) & ~31) + kFacPanel;
+    double* P = smem;                        // npad x kFacPanel, column-major (leading dimension mp <= npad)
+    double* x = P + (size_t)npad * kFacPanel;  // n: right-hand side -> y -> increment
+    double* hd = x + n;                      // n: undamped diagonal
+    double* da = hd + n;                     // n: damping added to the diagonal; then the product h
+    double* blk = da + n;                    // kFacPanel x kFacPanel diagonal block (solves)
     __shared__ int failed;
     __shared__ double red[32];
     double* A = B.Sglob + wd.dense0;
     const double* acc = B.acc + wd.acc0;
     const long long nS = (long long)Npc * (Npc + 1) / 2;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    constexpr int nw = kFactorThreads / 32;
     if (tid == 0) failed = 0;
-    // assembly: lower triangle, column-major
-    for (long long t = tid; t < (long long)n * n; t += blockDim.x) {
-        const int j = (int)(t / n), i = (int)(t % n);
-        if (i < j) continue;
-        const double v = assembleEntryCol(B, wd, i, j, lambda, true);
-        A[i + (long long)j * n] = v;
-        if (Sdebug) { Sdebug[wd.dense0 + (long long)i * n + j] = v; Sdebug[wd.dense0 + (long long)j * n + i] = v; }
+    for (int i = tid; i < n; i += blockDim.x) {
+        double h = B.Hret[wd.dense0 + (long long)i * n + i];
+        const int pi = pcOfRetained(i, K);
+        if (pi >= 0) h += acc[upIdx(pi, pi, Npc)];
+        da[i] = lambda * fmax(h, 1e-6);
+    }
+    __syncthreads();
+    // assembly: damped lower triangle (factored in place), undamped strict upper copy
+    for (int j = warp; j < n; j += nw)
+#pragma unroll 2
+    for (int i = j + lane; i < n; i += 32) {
+        const double v = assembleEntryCol(B, wd, i, j, lambda, false);
+        if (i == j) {
+            hd[i] = v;
+            A[i + (long long)j * n] = v + da[i];
+        } else {
+            A[i + (long long)j * n] = v;
+            A[j + (long long)i * n] = v;
+        }
+        if (Sdebug) {
+            const double dv = i == j ? v + da[i] : v;
+            Sdebug[wd.dense0 + (long long)i * n + j] = dv;
+            Sdebug[wd.dense0 + (long long)j * n + i] = dv;
+        }
     }
     double* rhsOut = B.rhs + wd.vec0;
     for (int i = tid; i < n; i += blockDim.x) {
@@ -686,67 +746,74 @@ __global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int re
         rhsOut[i] = -g;
     }
     __syncthreads();
-    for (int k0 = 0; k0 < n; k0 += kPanel) {
-        const int bw = min(kPanel, n - k0), m = n - k0;
-        for (int t = tid; t < m * bw; t += blockDim.x) {
-            const int c = t / m, r = t % m;
-            P[r + c * m] = r >= c ? A[(k0 + r) + (long long)(k0 + c) * n] : 0.0;
+    // ---- factorization with the forward substitution
+    for (int k0 = 0; k0 < n; k0 += kFacPanel) {
+        // rows padded so that the trailing rows [bw, mp) are whole 32-row tiles
+        const int bw = min(kFacPanel, n - k0), m = n - k0, mp = bw + ((m - bw + 31) & ~31);
+        for (int t = tid; t < mp * kFacPanel; t += blockDim.x) {
+            const int c = t / mp, r = t % mp;
+            P[r + c * mp] = (c < bw && r < m && r >= c) ? A[(k0 + r) + (long long)(k0 + c) * n] : 0.0;
         }
         __syncthreads();
         for (int c = 0; c < bw; ++c) {
-            if (tid == 0) {
-                const double d = P[c + c * m];
-                if (!(d > 0) || !isfinite(d)) failed = 1;
-                else P[c + c * m] = sqrt(d);
+            // column c of every row r >= c, less its products with the panel's earlier columns
+            for (int r = c + tid; r < m; r += blockDim.x) {
+                double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+                int k = 0;
+                for (; k + 4 <= c; k += 4) {
+                    s0 += P[r + k * mp] * P[c + k * mp];
+                    s1 += P[r + (k + 1) * mp] * P[c + (k + 1) * mp];
+                    s2 += P[r + (k + 2) * mp] * P[c + (k + 2) * mp];
+                    s3 += P[r + (k + 3) * mp] * P[c + (k + 3) * mp];
+                }
+                for (; k < c; ++k) s0 += P[r + k * mp] * P[c + k * mp];
+                P[r + c * mp] -= (s0 + s1) + (s2 + s3);
+            }
+            if (warp == nw - 1) {  // forward substitution: x_c - sum_{k<c} L[c][k] y_k
+                double t = lane < c ? P[c + lane * mp] * x[k0 + lane] : 0.0;
+                t = warpSum(t);
+                if (lane == 0) x[k0 + c] -= t;
             }
             __syncthreads();
-            if (failed) break;
-            const double pcc = P[c + c * m];
-            for (int r = c + 1 + tid; r < m; r += blockDim.x) P[r + c * m] /= pcc;
-            __syncthreads();
-            const int rest = bw - c - 1;
-            for (int t = tid; t < rest * m; t += blockDim.x) {
-                const int cc = c + 1 + t / m, r = t % m;
-                if (r >= cc) P[r + cc * m] -= P[r + c * m] * P[cc + c * m];
+            const double d = P[c + c * mp];  // the diagonal stays unscaled here; its root goes to A
+            if (!(d > 0) || !isfinite(d)) {
+                if (tid == 0) failed = 1;
+                break;  // uniform: every thread read the same d
             }
+            const double l = sqrt(d);
+            for (int r = c + 1 + tid; r < m; r += blockDim.x) P[r + c * mp] /= l;
+            if (tid == 0) x[k0 + c] /= l;
             __syncthreads();
         }
+        __syncthreads();
         if (failed) break;
-        for (int t = tid; t < m * bw; t += blockDim.x) {
-            const int c = t / m, r = t % m;
-            if (r >= c) A[(k0 + r) + (long long)(k0 + c) * n] = P[r + c * m];
-        }
+        for (int c = warp; c < bw; c += nw)
+            for (int r = c + lane; r < m; r += 32) A[(k0 + r) + (long long)(k0 + c) * n] = r == c ? sqrt(P[r + c * mp]) : P[r + c * mp];
         const int m2 = m - bw;
         if (m2 > 0) {
-            const int g4 = (m2 + 3) / 4, tiles = g4 * (g4 + 1) / 2;
-            for (int t = tid; t < tiles; t += blockDim.x) {
-                int a, b;
-                lowerTile(t, g4, a, b);  // row tile a >= column tile b
-                double accT[4][4];
+            // A22 -= L21 L21^T over the lower tiles of the m2 x m2 trailing block
+            const int nb2 = (m2 + 31) >> 5, tiles = nb2 * (nb2 + 1) / 2;
+            for (int t = warp; t < tiles; t += nw) {
+                int cb, rb;
+                tileOf(t, nb2, cb, rb);  // upper enumeration (cb <= rb): rows rb, columns cb
+                double tacc[4][8];
+                zeroTile(tacc);
+                rankUpdate<false>(tacc, P + bw + rb * 32 + 2 * (lane >> 2), P + bw + cb * 32 + 2 * (lane & 3), 0, bw, 1, mp);
 #pragma unroll
-                for (int q = 0; q < 4; ++q)
+                for (int r = 0; r < 4; ++r) {
+                    const int i = tileRow(rb, lane, r);
 #pragma unroll
-                    for (int p = 0; p < 4; ++p) accT[q][p] = 0.0;
-                const int r0 = bw + 4 * a, c0 = bw + 4 * b;
-                for (int c = 0; c < bw; ++c) {
-                    double u[4], v[4];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        u[q] = r0 + q < m ? P[(r0 + q) + c * m] : 0.0;
-                        v[q] = c0 + q < m ? P[(c0 + q) + c * m] : 0.0;
+                    for (int c = 0; c < 8; ++c) {
+                        const int j = tileCol(cb, lane, c);
+                        if (i < m2 && j < m2 && i >= j) A[(k0 + bw + i) + (long long)(k0 + bw + j) * n] -= tacc[r][c];
                     }
-#pragma unroll
-                    for (int q = 0; q < 4; ++q)
-#pragma unroll
-                        for (int p = 0; p < 4; ++p) accT[q][p] += u[q] * v[p];
                 }
-#pragma unroll
-                for (int p = 0; p < 4; ++p)
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int i = k0 + r0 + q, j = k0 + c0 + p;
-                        if (i < n && j < n && i >= j) A[i + (long long)j * n] -= accT[q][p];
-                    }
+            }
+            // right-hand side below the panel: y2 -= L21 y1
+            for (int i = tid; i < m2; i += blockDim.x) {
+                double s = 0;
+                for (int c = 0; c < bw; ++c) s += P[bw + i + c * mp] * x[k0 + c];
+                x[k0 + bw + i] -= s;
             }
         }
         __syncthreads();
@@ -755,22 +822,50 @@ __global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int re
         if (tid == 0) B.solveStatus[wdx] = CGMLI_E_NOT_PD;
         return;
     }
-    blockedSolve(A, n, x, blk);
+    // ---- backward substitution L^T x = y by panels (L lower in A)
+    for (int k0 = ((n - 1) / kFacPanel) * kFacPanel; k0 >= 0; k0 -= kFacPanel) {
+        const int bw = min(kFacPanel, n - k0);
+        for (int c = warp; c < bw; c += nw) {
+            double s = 0;
+            for (int r = k0 + bw + lane; r < n; r += 32) s += A[r + (long long)(k0 + c) * n] * x[r];
+            s = warpSum(s);
+            if (lane == 0) x[k0 + c] -= s;
+        }
+        for (int t = tid; t < bw * bw; t += blockDim.x) {
+            const int c = t / bw, r = t % bw;
+            blk[r + c * kFacPanel] = r >= c ? A[(k0 + r) + (long long)(k0 + c) * n] : 0.0;
+        }
+        __syncthreads();
+        if (warp == 0) {  // lane r holds y_r; column sweep x_c = y_c / L_cc, y_r -= L[c][r] x_c (r < c)
+            double y = lane < bw ? x[k0 + lane] : 0.0;
+            for (int c = bw - 1; c >= 0; --c) {
+                const double xc = __shfl_sync(0xffffffffu, y, c) / blk[c + c * kFacPanel];
+                if (lane < c) y -= blk[c + lane * kFacPanel] * xc;
+                if (lane == c) y = xc;
+            }
+            if (lane < bw) x[k0 + lane] = y;
+        }
+        __syncthreads();
+    }
     double* dr = B.dr + wd.vec0;
     for (int i = tid; i < n; i += blockDim.x) dr[i] = x[i];
     __syncthreads();
-    // iterative refinement against the assembled FP64 system
+    double* h = da;  // the damping is folded back below where needed
+    // ---- iterative refinement against the assembled FP64 system
     for (int it = 0; it < refinement; ++it) {
-        for (int i = warp; i < n; i += nw) {
-            double s = 0;
-            for (int j = lane; j < n; j += 32) s += assembleEntryCol(B, wd, j, i, lambda, true) * dr[j];
-            s = warpSum(s);
-            if (lane == 0) {
-                double g = B.gret[wd.vec0 + i];
-                const int p = pcOfRetained(i, K);
-                if (p >= 0) g += acc[nS + Npc + p] - acc[nS + 2ll * Npc + p];
-                x[i] = -g - s;
-            }
+        for (int i = tid; i < n; i += blockDim.x) {
+            const int pi = pcOfRetained(i, K);
+            double hh = B.Hret[wd.dense0 + (long long)i * n + i];
+            if (pi >= 0) hh += acc[upIdx(pi, pi, Npc)];
+            x[i] = lambda * fmax(hh, 1e-6);  // damping of row i, kept in x for this pass
+        }
+        __syncthreads();
+        undampedProduct(A, hd, n, dr, h);
+        for (int i = tid; i < n; i += blockDim.x) {
+            double g = B.gret[wd.vec0 + i];
+            const int p = pcOfRetained(i, K);
+            if (p >= 0) g += acc[nS + Npc + p] - acc[nS + 2ll * Npc + p];
+            x[i] = -g - (h[i] + x[i] * dr[i]);
         }
         __syncthreads();
         blockedSolve(A, n, x, blk);
@@ -779,17 +874,13 @@ __global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int re
     }
     // predicted reduction of the state part with the undamped (S_visual + H_ret):
     //   -dx^T (g_r + 0.5 (S_v + H_ret) dx); the landmark terms are added per landmark.
+    undampedProduct(A, hd, n, dr, h);
     double pred = 0;
-    for (int i = warp; i < n; i += nw) {
-        double hd = 0;
-        for (int j = lane; j < n; j += 32) hd += assembleEntryCol(B, wd, j, i, lambda, false) * dr[j];
-        hd = warpSum(hd);
-        if (lane == 0) {
-            double g = B.gret[wd.vec0 + i];
-            const int p = pcOfRetained(i, K);
-            if (p >= 0) g += acc[nS + Npc + p];
-            pred += -dr[i] * (g + 0.5 * hd);
-        }
+    for (int i = tid; i < n; i += blockDim.x) {
+        double g = B.gret[wd.vec0 + i];
+        const int p = pcOfRetained(i, K);
+        if (p >= 0) g += acc[nS + Npc + p];
+        pred += -dr[i] * (g + 0.5 * h[i]);
     }
     pred = blockSum(pred, red);
     if (tid == 0) { B.predState[wdx] = pred; B.solveStatus[wdx] = CGMLI_OK; }
@@ -1019,13 +1110,10 @@ __global__ void k_lm_init(DevBatch B, double lambda0) {
 // host-side launchers (called by backend_host.cu)
 size_t linearizeSmemBytes(int maxNs) { return kLinWarps * landmarkWarpBytes(maxNs); }
 size_t schurSmemBytes() { return kSchurSmemDoubles * sizeof(double); }
-int schurRowsPerChunk(int Npc) {
-    const int rows = kSchurSmemDoubles / (Npc + 1);
-    return rows < 128 ? rows : 128;
-}
 size_t factorSmemBytes(int maxNr) {
-    // increment vector, diagonal block of the solves, one panel of kPanel columns
-    return ((size_t)maxNr + kPanel * kPanel + (size_t)maxNr * kPanel) * sizeof(double);
+    // one panel of kFacPanel columns over the padded rows, three n-vectors, the diagonal block
+    const size_t npad = (((size_t)maxNr + 31) & ~(size_t)31) + kFacPanel;
+    return (npad * kFacPanel + 3 * (size_t)maxNr + kFacPanel * kFacPanel) * sizeof(double);
 }
 
 // The dynamic shared-memory cap is a per-function attribute shared by every

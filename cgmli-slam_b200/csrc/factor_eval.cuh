@@ -38,7 +38,10 @@ __device__ __forceinline__ void gatherFactor(const DevBatch& B, const WinDesc& w
 }
 
 // Frozen IMU factor, evaluateImu of GpuRetainedFactorMath.hpp:53-140.
-// r: 15 whitened; J: 15 x 30 row-major over [pose_i 6 | sb_i 9 | pose_j 6 | sb_j 9].
+// evalImuRaw gives the unwhitened error e (15) and its Jacobian U (15 x 30
+// row-major over [pose_i 6 | sb_i 9 | pose_j 6 | sb_j 9]); the factor's
+// residual and Jacobian are r = W e and J = W U with W the 15 x 15 whitening
+// (column-major in cgmli_frozen_imu).  evalImu applies W in the calling thread.
 struct Sensor { d3 p, v, arm, lever; qd q; };
 __device__ inline Sensor sensorState(const cgmli_frozen_imu& imu, const double* pose, const double* sb, int end) {
     const qd q = qnormalized(ldq(pose + 3));
@@ -50,8 +53,8 @@ __device__ inline Sensor sensorState(const cgmli_frozen_imu& imu, const double* 
     s.v = ld3(sb) + s.lever;
     return s;
 }
-__device__ inline bool evalImu(const cgmli_frozen_imu& imu, const double* p0, const double* sb0, const double* p1, const double* sb1,
-                               double* r, double* J) {
+__device__ inline bool evalImuRaw(const cgmli_frozen_imu& imu, const double* p0, const double* sb0, const double* p1,
+                                  const double* sb1, double* e, double* U) {
     const Sensor s0 = sensorState(imu, p0, sb0, 0), s1 = sensorState(imu, p1, sb1, 1);
     const m3 A = colmajor(imu.rotation_gyro), V = colmajor(imu.velocity_gyro), P = colmajor(imu.position_gyro),
              Va = colmajor(imu.velocity_accel), Pa = colmajor(imu.position_accel);
@@ -64,19 +67,14 @@ __device__ inline bool evalImu(const cgmli_frozen_imu& imu, const double* p0, co
     const d3 phi = -1.0 * mv(A, bg);
     const qd correction = rotationExp(phi), dq = qmul(correction, ldq(imu.delta_quaternion));
     const qd tail = qmul(qmul(ldq(imu.delta_quaternion), qconj(s1.q)), s0.q);
-    double e[15];
     const d3 e0 = mv(R, dp) + ld3(imu.delta_position) + mv(P, bg) - mv(Pa, ba);
     const d3 e1 = 2.0 * qvec(qmul(dq, qmul(qconj(s1.q), s0.q)));
     const d3 e2 = mv(R, dv) + ld3(imu.delta_velocity) + mv(V, bg) - mv(Va, ba);
     e[0] = e0.x; e[1] = e0.y; e[2] = e0.z; e[3] = e1.x; e[4] = e1.y; e[5] = e1.z; e[6] = e2.x; e[7] = e2.y; e[8] = e2.z;
     for (int i = 0; i < 6; ++i) e[9 + i] = sb0[3 + i] - sb1[3 + i];
-    for (int i = 0; i < 15; ++i) {
-        double v = 0;
-        for (int k = 0; k < 15; ++k) v += imu.whitening[i + 15 * k] * e[k];
-        r[i] = v;
-        if (!isfinite(v)) return false;
-    }
-    if (!J) return true;
+    for (int i = 0; i < 15; ++i)
+        if (!isfinite(e[i])) return false;
+    if (!U) return true;
     const m3 gyroAngle = mscl(-1, mul(rotationJacobian(-1.0 * phi), A));
     m3 Jrot, Jbias;
     for (int j = 0; j < 3; ++j) {
@@ -87,18 +85,16 @@ __device__ inline bool evalImu(const cgmli_frozen_imu& imu, const double* p0, co
         Jrot.a[j] = c1.x; Jrot.a[3 + j] = c1.y; Jrot.a[6 + j] = c1.z;
         Jbias.a[j] = c2.x; Jbias.a[3 + j] = c2.y; Jbias.a[6 + j] = c2.z;
     }
-    for (int i = 0; i < 450; ++i) J[i] = 0;
-    const int width[4] = {6, 9, 6, 9}, col0[4] = {0, 6, 15, 21};
+    for (int i = 0; i < 450; ++i) U[i] = 0;
+    const int col0[4] = {0, 6, 15, 21};
     for (int k = 0; k < 4; ++k) {
         const bool first = k < 2;
         const double sign = first ? 1 : -1;
         const Sensor& s = first ? s0 : s1;
-        double Jk[15 * 9];
-        for (int i = 0; i < 135; ++i) Jk[i] = 0;
         auto put = [&](int r0, int c0, const m3& m, bool accumulate) {
             for (int i = 0; i < 3; ++i)
                 for (int j = 0; j < 3; ++j) {
-                    double& t = Jk[9 * (r0 + i) + c0 + j];
+                    double& t = U[30 * (r0 + i) + col0[k] + c0 + j];
                     t = accumulate ? t + m.a[3 * i + j] : m.a[3 * i + j];
                 }
         };
@@ -126,13 +122,31 @@ __device__ inline bool evalImu(const cgmli_frozen_imu& imu, const double* p0, co
                 put(6, 6, mscl(-1, Va), false);
             }
         }
-        for (int j = 0; j < width[k]; ++j)
-            for (int i = 0; i < 15; ++i) {
-                double v = 0;
-                for (int m = 0; m < 15; ++m) v += imu.whitening[i + 15 * m] * Jk[9 * m + j];
-                if (!isfinite(v)) return false;
-                J[30 * i + col0[k] + j] = v;
-            }
+    }
+    for (int i = 0; i < 450; ++i)
+        if (!isfinite(U[i])) return false;
+    return true;
+}
+__device__ inline bool evalImu(const cgmli_frozen_imu& imu, const double* p0, const double* sb0, const double* p1, const double* sb1,
+                               double* r, double* J) {
+    double e[15];
+    if (!evalImuRaw(imu, p0, sb0, p1, sb1, e, J)) return false;
+    for (int i = 0; i < 15; ++i) {
+        double v = 0;
+        for (int k = 0; k < 15; ++k) v += imu.whitening[i + 15 * k] * e[k];
+        r[i] = v;
+        if (!isfinite(v)) return false;
+    }
+    if (!J) return true;
+    for (int c = 0; c < 30; ++c) {
+        double u[15];
+        for (int m = 0; m < 15; ++m) u[m] = J[30 * m + c];
+        for (int i = 0; i < 15; ++i) {
+            double v = 0;
+            for (int m = 0; m < 15; ++m) v += imu.whitening[i + 15 * m] * u[m];
+            if (!isfinite(v)) return false;
+            J[30 * i + c] = v;
+        }
     }
     return true;
 }

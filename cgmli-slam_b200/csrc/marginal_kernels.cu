@@ -27,6 +27,7 @@
 #include "../../include/cgmli_backend.h"
 #include "backend_internal.h"
 #include "device_math.cuh"
+#include "dense_tiles.cuh"
 #include "factor_eval.cuh"
 
 namespace cgmli {
@@ -164,42 +165,13 @@ __global__ void k_marg_eval(DevBatch B, MargBatch M) {
 // item; else every warp sums its tiles per chunk.  Either way each block is
 // added to the window's H with atomics once per accumulation.
 namespace {
-__device__ __forceinline__ void tileOf(int t, int nb, int& bi, int& bj) {
-    bi = 0;
-    while (t >= nb - bi) { t -= nb - bi; ++bi; }
-    bj = bi + t;
-}
-template <bool kSubtract>
-__device__ __forceinline__ void rankUpdate(double (&acc)[4][8], const double* Va, const double* Vb, int k0, int k1, int step, int np) {
-#pragma unroll 2
-    for (int k = k0; k < k1; k += step) {
-        const double2 a01 = *reinterpret_cast<const double2*>(Va + (long long)k * np);
-        const double2 a23 = *reinterpret_cast<const double2*>(Va + (long long)k * np + 16);
-        double a[4] = {a01.x, a01.y, a23.x, a23.y};
-        if (kSubtract)
-#pragma unroll
-            for (int r = 0; r < 4; ++r) a[r] = -a[r];
-        double b[8];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const double2 v = *reinterpret_cast<const double2*>(Vb + (long long)k * np + 8 * q);
-            b[2 * q] = v.x;
-            b[2 * q + 1] = v.y;
-        }
-#pragma unroll
-        for (int r = 0; r < 4; ++r)
-#pragma unroll
-            for (int c = 0; c < 8; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
-    }
-}
 __device__ __forceinline__ void flushTile(double (&acc)[4][8], int bi, int bj, int lane, int n, const int* visCol, double* H, int m) {
-    const int rg = lane >> 2, cg = lane & 3;
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-        const int i = bi * 32 + (r < 2 ? 2 * rg + r : 16 + 2 * rg + r - 2);
+        const int i = tileRow(bi, lane, r);
 #pragma unroll
         for (int c = 0; c < 8; ++c) {
-            const int j = bj * 32 + 8 * (c >> 1) + 2 * cg + (c & 1);
+            const int j = tileCol(bj, lane, c);
             const double v = acc[r][c];
             if (i < n && j < n && i <= j && v != 0.0) {
                 const int ci = visCol[i], cj = visCol[j];
@@ -321,11 +293,7 @@ __global__ void __launch_bounds__(kRowsThreads, 1) k_marg_rows(DevBatch B, MargB
             const int t = u / wpt, part = u % wpt;
             int bi, bj;
             tileOf(t, nb, bi, bj);
-            if (!persistent)
-#pragma unroll
-                for (int r = 0; r < 4; ++r)
-#pragma unroll
-                    for (int c = 0; c < 8; ++c) acc[r][c] = 0.0;
+            if (!persistent) zeroTile(acc);
             const double* Va = V + bi * 32 + 2 * rg;
             const double* Vb = V + bj * 32 + 2 * cg;
             rankUpdate<false>(acc, Va, Vb, part, kp, wpt, np);

@@ -46,7 +46,9 @@ struct WindowPart {
     std::vector<int2> tiles;        // global landmark indices
     std::vector<int4> runs;         // window-local tile indices
     std::vector<int4> pairChunks;
-    std::vector<int4> schurChunks;
+    std::vector<int4> schurChunks;  // .w: window-local offset in schurCols
+    std::vector<int> schurCols;     // per chunk: count, then ascending visual columns
+    std::vector<unsigned short> umap;  // per cross-vector entry (window-local): position in its chunk's columns
     long long cross = 0;            // sum of support widths
     int maxNs = 1;
     int status = CGMLI_OK;
@@ -142,7 +144,7 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
         acc += (long long)d.Npc * (d.Npc + 1) / 2 + 3ll * d.Npc;
         sch += (long long)d.Npc * (d.Npc + 1) / 2;
         d.imuScratch0 = imuS;
-        imuS += 465ll * d.nImu;
+        imuS += 930ll * d.nImu;
         d.priorRank = w.prior_rank;
         d.priorBlk0 = pblk;
         d.priorBlocks = w.prior_rank > 0 ? w.prior_num_blocks : 0;
@@ -371,8 +373,61 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
         }
         for (int c0 = 0; c0 < F; c0 += 32)
             P.pairChunks.push_back(make_int4(i, d.obs0 + c0, d.obs0 + std::min(F, c0 + 32), 0));
-        const int rows = schurRowsPerChunk(d.Npc);
-        for (int l0 = 0; l0 < L; l0 += rows) P.schurChunks.push_back(make_int4(i, d.lm0 + l0, d.lm0 + std::min(L, l0 + rows), 0));
+        // Schur chunks: runs of consecutive landmarks whose support columns
+        // together fit the chunk's shared rows (schurChunkFits); the column
+        // union of each chunk and every landmark's map into it
+        {
+            const int tdCol = 6 * d.K + (d.estExt ? 6 * d.E : 0);
+            const int words = (d.Npc + 63) / 64;
+            std::vector<unsigned long long> U(words, 0), Ul(words, 0);
+            std::vector<int> lc, pos(d.Npc, -1);
+            P.umap.assign(P.cross, 0);
+            int q0 = 0, nu = 0;
+            auto columnsOf = [&](int q) {
+                const int g = d.lm0 + q, ns_ = hb.lmNs[g], nx_ = hb.lmNx[g];
+                const int* sk = &P.supp[hb.lmSupp0[g]];
+                const int ns = 6 * (ns_ + nx_) + (d.estTd ? 1 : 0);
+                lc.resize(ns);
+                for (int c = 0; c < ns; ++c)
+                    lc[c] = c < 6 * ns_ ? 6 * sk[c / 6] + c % 6
+                          : c < 6 * (ns_ + nx_) ? 6 * d.K + 6 * sk[ns_ + (c - 6 * ns_) / 6] + c % 6 : tdCol;
+            };
+            auto closeChunk = [&](int q1) {
+                const int off = (int)P.schurCols.size();
+                P.schurCols.push_back(nu);
+                int k = 0;
+                for (int wi = 0; wi < words; ++wi)
+                    for (unsigned long long bits = U[wi]; bits; bits &= bits - 1) {
+                        const int col = 64 * wi + __builtin_ctzll(bits);
+                        P.schurCols.push_back(col);
+                        pos[col] = k++;
+                    }
+                for (int q = q0; q < q1; ++q) {
+                    columnsOf(q);
+                    const long long c0 = hb.lmC0[d.lm0 + q];  // window-local here
+                    for (size_t c = 0; c < lc.size(); ++c) P.umap[c0 + c] = (unsigned short)pos[lc[c]];
+                }
+                P.schurChunks.push_back(make_int4(i, d.lm0 + q0, d.lm0 + q1, off));
+                std::fill(U.begin(), U.end(), 0ull);
+                nu = 0;
+                q0 = q1;
+            };
+            for (int q = 0; q < L; ++q) {
+                columnsOf(q);
+                std::fill(Ul.begin(), Ul.end(), 0ull);
+                for (int c : lc) Ul[c >> 6] |= 1ull << (c & 63);
+                int nuNew = 0;
+                for (int wi = 0; wi < words; ++wi) nuNew += __builtin_popcountll(U[wi] | Ul[wi]);
+                if (q > q0 && !schurChunkFits(q - q0 + 1, nuNew)) {
+                    closeChunk(q);
+                    nuNew = 0;
+                    for (int wi = 0; wi < words; ++wi) nuNew += __builtin_popcountll(Ul[wi]);
+                }
+                for (int wi = 0; wi < words; ++wi) U[wi] |= Ul[wi];
+                nu = nuNew;
+            }
+            if (L > q0) closeChunk(L);
+        }
     });
     for (int i = 0; i < count; ++i)
         if (part[i].status != CGMLI_OK) {
@@ -383,7 +438,8 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
         }
     // ---- phase 2: prefix sums and fix-ups
     std::vector<long long> suppBase(count + 1, 0), crossBase(count + 1, 0);
-    std::vector<int> tileBase(count + 1, 0), runBase(count + 1, 0), pairBase(count + 1, 0), schurBase(count + 1, 0);
+    std::vector<int> tileBase(count + 1, 0), runBase(count + 1, 0), pairBase(count + 1, 0), schurBase(count + 1, 0),
+        schurColBase(count + 1, 0);
     for (int i = 0; i < count; ++i) {
         suppBase[i + 1] = suppBase[i] + (long long)part[i].supp.size();
         crossBase[i + 1] = crossBase[i] + part[i].cross;
@@ -391,6 +447,7 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
         runBase[i + 1] = runBase[i] + (int)part[i].runs.size();
         pairBase[i + 1] = pairBase[i] + (int)part[i].pairChunks.size();
         schurBase[i + 1] = schurBase[i] + (int)part[i].schurChunks.size();
+        schurColBase[i + 1] = schurColBase[i] + (int)part[i].schurCols.size();
         hb.maxNs = std::max(hb.maxNs, part[i].maxNs);
     }
     hb.cross = crossBase[count];
@@ -399,6 +456,8 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
     hb.runs.resize(runBase[count]);
     hb.pairChunks.resize(pairBase[count]);
     hb.schurChunks.resize(schurBase[count]);
+    hb.schurCols.resize(std::max(schurColBase[count], 1));
+    hb.lmUmap.resize(std::max(hb.cross, 1ll));
     parallelFor(count, threads, [&](int i) {
         const WinDesc& d = hb.win[i];
         WindowPart& P = part[i];
@@ -415,7 +474,13 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
             hb.runs[runBase[i] + r] = run;
         }
         std::copy(P.pairChunks.begin(), P.pairChunks.end(), hb.pairChunks.begin() + pairBase[i]);
-        std::copy(P.schurChunks.begin(), P.schurChunks.end(), hb.schurChunks.begin() + schurBase[i]);
+        for (size_t c = 0; c < P.schurChunks.size(); ++c) {
+            int4 chunk = P.schurChunks[c];
+            chunk.w += schurColBase[i];
+            hb.schurChunks[schurBase[i] + c] = chunk;
+        }
+        std::copy(P.schurCols.begin(), P.schurCols.end(), hb.schurCols.begin() + schurColBase[i]);
+        std::copy(P.umap.begin(), P.umap.end(), hb.lmUmap.begin() + crossBase[i]);
     });
     return CGMLI_OK;
 }
@@ -488,8 +553,21 @@ int checkHostBatch(const cgmli_window* windows, int count, const HostBatch& hb, 
     std::vector<int> schCover(hb.totalLm, 0);
     for (const int4& c : hb.schurChunks) {
         const WinDesc& d = hb.win[c.x];
-        if (c.y < d.lm0 || c.z > d.lm0 + d.L || c.z - c.y > schurRowsPerChunk(d.Npc)) return bad(c.x, "Schur chunk");
-        for (int g = c.y; g < c.z; ++g) ++schCover[g];
+        if (c.y < d.lm0 || c.z > d.lm0 + d.L || c.y >= c.z || c.w < 0 || c.w >= (long long)hb.schurCols.size())
+            return bad(c.x, "Schur chunk");
+        const int nu = hb.schurCols[c.w];
+        if (nu < 1 || nu > d.Npc || c.w + nu >= (long long)hb.schurCols.size() || !schurChunkFits(c.z - c.y, nu))
+            return bad(c.x, "Schur chunk columns");
+        for (int k = 1; k <= nu; ++k) {
+            const int col = hb.schurCols[c.w + k];
+            if (col < 0 || col >= d.Npc || (k > 1 && col <= hb.schurCols[c.w + k - 1])) return bad(c.x, "Schur chunk column list");
+        }
+        for (int g = c.y; g < c.z; ++g) {
+            ++schCover[g];
+            const int ns = 6 * (hb.lmNs[g] + hb.lmNx[g]) + (d.estTd ? 1 : 0);
+            for (int k = 0; k < ns; ++k)
+                if (hb.lmUmap[hb.lmC0[g] + k] >= nu) return bad(c.x, "Schur chunk map");
+        }
     }
     for (int g = 0; g < hb.totalLm; ++g)
         if (schCover[g] != 1) return bad(-1, "Schur chunks do not cover every landmark once");

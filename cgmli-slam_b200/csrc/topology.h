@@ -78,7 +78,9 @@ struct HostBatch {
     HVec<int4> runs;         // {window, first tile, end tile, -}
     HVec<int2> tiles;        // {first landmark, end landmark}
     HVec<int4> pairChunks;   // {window, first key-ordered position, end, -}
-    HVec<int4> schurChunks;  // {window, first landmark, end landmark, -}
+    HVec<int4> schurChunks;  // {window, first landmark, end landmark, offset in schurCols}
+    HVec<int> schurCols;     // per Schur chunk: count, then the ascending visual columns of its landmarks
+    HVec<unsigned short> lmUmap;  // per cross-vector entry: position of its column in the chunk's list
     HVec<int> lmPerm;        // device landmark -> landmark index within its window
     // cameras
     HVec<double> camR, camT;
@@ -113,8 +115,5 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
 
 // Invariants of a built batch (used by the diagnostic entry point and tests).
 int checkHostBatch(const cgmli_window* windows, int count, const HostBatch& hb, std::string& why);
-
-// Schur chunk rows of a window with Npc visual columns (defined with the kernels).
-int schurRowsPerChunk(int Npc);
 
 }  // namespace cgmli
