@@ -117,7 +117,7 @@ struct cgmli_solver {
     DArray<int> lmValid, lmTrialValid;
     DArray<int> obKf, obCam, obSlot, obXslot;
     DArray<double> obBearing, obP, obVel, obTime;
-    DArray<double> pose[2], sb[2], ext[2], td[2], rho[2];
+    DArray<double> pose[2], sb[2], ext[2], td[2], rho[2], rotKf[2], rotExt[2];
     DArray<double> imu;
     DArray<int> imuKf;
     DArray<int> priorKind, priorIndex, priorCol, priorOff;
@@ -196,6 +196,7 @@ struct cgmli_solver {
         if (stream) cudaStreamSynchronize(stream);
         DArray<double>* dbl[] = {&camR, &camT, &lmBearing, &lmVel, &lmTime, &lmC, &lmD, &lmG, &lmCost, &lmDelta, &lmPred, &lmTrial,
                                  &lmMaxInc, &obBearing, &obP, &obVel, &obTime, &pose[0], &pose[1], &sb[0], &sb[1], &ext[0], &ext[1],
+                                 &rotKf[0], &rotKf[1], &rotExt[0], &rotExt[1],
                                  &td[0], &td[1], &rho[0], &rho[1], &imu, &priorA, &priorR0, &priorRef, &Hret, &gret, &costRet,
                                  &trialRet, &acc, &dr, &rhs, &Sglob, &imuScratch, &priorScratch, &predState, &out, &Sdebug};
         for (auto* a : dbl) a->release();
@@ -325,6 +326,7 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     CK(S->pose[0].upload(hb.pose, st)); CK(S->sb[0].upload(hb.sb, st)); CK(S->ext[0].upload(hb.ext, st));
     CK(S->td[0].upload(hb.td, st)); CK(S->rho[0].upload(hb.rho, st));
     CK(S->pose[1].reserve(hb.pose.size())); CK(S->sb[1].reserve(hb.sb.size())); CK(S->ext[1].reserve(hb.ext.size()));
+    for (int k = 0; k < 2; ++k) { CK(S->rotKf[k].reserve(9ull * hb.totalKf)); CK(S->rotExt[k].reserve(9ull * hb.totalExt)); }
     CK(S->td[1].reserve(hb.td.size())); CK(S->rho[1].reserve(hb.rho.size()));
     CK(S->imu.upload(hb.imu, st)); CK(S->imuKf.upload(hb.imuKf, st));
     CK(S->priorKind.upload(hb.priorKind, st)); CK(S->priorIndex.upload(hb.priorIndex, st));
@@ -359,6 +361,7 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     B.obBearing = S->obBearing.p; B.obP = S->obP.p; B.obVel = S->obVel.p; B.obTime = S->obTime.p;
     for (int k = 0; k < 2; ++k) {
         B.pose[k] = S->pose[k].p; B.sb[k] = S->sb[k].p; B.ext[k] = S->ext[k].p; B.td[k] = S->td[k].p; B.rho[k] = S->rho[k].p;
+        B.rotKf[k] = S->rotKf[k].p; B.rotExt[k] = S->rotExt[k].p;
     }
     B.imu = S->imu.p; B.imuKf = S->imuKf.p;
     B.priorKind = S->priorKind.p; B.priorIndex = S->priorIndex.p; B.priorCol = S->priorCol.p; B.priorOff = S->priorOff.p;

@@ -70,6 +70,7 @@ struct DevBatch {
     const double* obBearing; const double* obP; const double* obVel; const double* obTime;
     // states: [0] accepted, [1] candidate
     double* pose[2]; double* sb[2]; double* ext[2]; double* td[2]; double* rho[2];
+    double* rotKf[2]; double* rotExt[2];  // rotation matrices of the poses / extrinsics of each state (9 each)
     // IMU and priors
     const double* imu;  // numImu * sizeof(cgmli_frozen_imu)/8
     const int* imuKf;   // global keyframe index of the first state

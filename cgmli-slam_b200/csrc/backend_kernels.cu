@@ -59,6 +59,9 @@ __global__ void k_zero_acc(DevBatch B) {
     for (long long i = threadIdx.x; i < wd.Npc; i += blockDim.x) acc[nS + 2ll * wd.Npc + i] = 0.0;
     double* sch = B.sch + wd.sch0;
     for (long long i = threadIdx.x; i < nS; i += blockDim.x) sch[i] = 0.0;
+    // rotations of the accepted state for this iteration's factors
+    for (int k = threadIdx.x; k < wd.K; k += blockDim.x) poseRotation(B.pose[0] + 7ll * (wd.kf0 + k), B.rotKf[0] + 9ll * (wd.kf0 + k));
+    for (int e = threadIdx.x; e < wd.E; e += blockDim.x) poseRotation(B.ext[0] + 7ll * (wd.ext0 + e), B.rotExt[0] + 9ll * (wd.ext0 + e));
 }
 
 // ---------------------------------------------------------------------------------------
@@ -140,10 +143,19 @@ __global__ void __launch_bounds__(kLinWarps * 32, 2) k_lin_landmark(DevBatch B, 
         const int lb = tile.x, le = tile.y;
         const int ob = B.lmObsBegin[lb], oe = B.lmObsBegin[le];
         const int f = ob + lane;
+        // per-landmark metadata of the tile, one landmark per lane (a tile holds <= 32 landmarks)
+        const int nl = le - lb;
+        int myBeg = 0, myEnd = 0, myNs = 0;
+        long long myC0 = 0;
+        if (lane < nl) {
+            const int l = lb + lane;
+            myBeg = B.lmObsBegin[l] - ob;
+            myEnd = B.lmObsBegin[l + 1] - ob;
+            myNs = 6 * (B.lmNs[l] + B.lmNx[l]) + (wd.estTd ? 1 : 0);
+            myC0 = B.lmC0[l];
+        }
         if (f < oe) {
-            int q = 0;
-            while (B.lmObsBegin[lb + q + 1] <= f) ++q;
-            const int l = lb + q;
+            const int l = B.obLm[f];
             FactorIn in;
             int kfa, kfb, ea, eb;
             gatherFactor(B, wd, wdx, l, f, 0, in, kfa, kfb, ea, eb);
@@ -193,33 +205,59 @@ __global__ void __launch_bounds__(kLinWarps * 32, 2) k_lin_landmark(DevBatch B, 
             st[25] = d; st[26] = g; st[27] = cost;
         }
         __syncwarp();
-        for (int l = lb; l < le; ++l) {
-            const int fb = B.lmObsBegin[l] - ob, fe = B.lmObsBegin[l + 1] - ob;
-            const int s = B.lmNs[l], x = B.lmNx[l], ns = 6 * (s + x) + (wd.estTd ? 1 : 0);
-            double d = 0, g = 0, cost = 0;
-            int valid = 1;
-            for (int k = fb + lane; k < fe; k += 32) {
-                const double* st = out + kOut * k;
-                d += st[25];
-                g += st[26];
-                cost += st[27];
-                valid &= flags[k];
+        // landmark sums of d, g, cost and validity: segmented inclusive scans over
+        // the tile's lanes (observations of one landmark are consecutive lanes)
+        {
+            const int seg = B.obLm[f < oe ? f : ob] - lb;  // landmark of this lane (lanes past the tile: any)
+            const double* st = out + kOut * lane;
+            const bool live = f < oe && flags[lane];
+            double d = live ? st[25] : 0.0, g = live ? st[26] : 0.0, cost = live ? st[27] : 0.0;
+            int bad = f < oe && !flags[lane] ? 1 : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const double d2 = __shfl_up_sync(0xffffffffu, d, o), g2 = __shfl_up_sync(0xffffffffu, g, o);
+                const double c2 = __shfl_up_sync(0xffffffffu, cost, o);
+                const int b2 = __shfl_up_sync(0xffffffffu, bad, o), s2 = __shfl_up_sync(0xffffffffu, seg, o);
+                if (lane >= o && s2 == seg) { d += d2; g += g2; cost += c2; bad |= b2; }
             }
-            d = warpSum(d); g = warpSum(g); cost = warpSum(cost);
-            valid = __all_sync(0xffffffffu, valid);
+            // the last lane of each landmark holds its sums
+            const int nextSeg = __shfl_down_sync(0xffffffffu, seg, 1);
+            if (f < oe && (lane == 31 || f + 1 >= oe || nextSeg != seg)) {
+                const int l = lb + seg;
+                B.lmD[l] = d; B.lmG[l] = g; B.lmCost[l] = cost; B.lmValid[l] = bad ? 0 : 1;
+            }
+        }
+        // cross vectors c_l: lane c < 25 owns compact column c, whose local column
+        // is the same run after run of observations (anchor pose, anchor
+        // extrinsic, td) or changes only with the observer (observer pose and
+        // extrinsic); different lanes never share a local column, so each lane
+        // sums in a register and adds to the landmark's vector when its column changes
+        for (int q = 0; q < nl; ++q) {
+            const int fb = __shfl_sync(0xffffffffu, myBeg, q), fe = __shfl_sync(0xffffffffu, myEnd, q);
+            const int ns = __shfl_sync(0xffffffffu, myNs, q);
+            const long long c0 = __shfl_sync(0xffffffffu, myC0, q);
+            if (fb == fe && lane == 0) {  // no observation in the window: nothing was summed above
+                const int l = lb + q;
+                B.lmD[l] = 0.0; B.lmG[l] = 0.0; B.lmCost[l] = 0.0; B.lmValid[l] = 1;
+            }
             for (int i = lane; i < ns; i += 32) cvec[i] = 0.0;
             __syncwarp();
-            // the compact columns of one observation map to distinct local columns
-            for (int k = fb; k < fe; ++k) {
-                if (lane < kCompact) {
+            if (lane < kCompact) {
+                int cur = -1;
+                double accv = 0.0;
+                for (int k = fb; k < fe; ++k) {
                     const int li = map[kCompact * k + lane];
-                    if (li >= 0) cvec[li] += out[kOut * k + lane];
+                    if (li != cur) {
+                        if (cur >= 0) cvec[cur] += accv;
+                        cur = li;
+                        accv = 0.0;
+                    }
+                    if (li >= 0 && flags[k]) accv += out[kOut * k + lane];
                 }
-                __syncwarp();
+                if (cur >= 0) cvec[cur] += accv;
             }
-            const long long c0 = B.lmC0[l];
+            __syncwarp();
             for (int i = lane; i < ns; i += 32) B.lmC[c0 + i] = cvec[i];
-            if (lane == 0) { B.lmD[l] = d; B.lmG[l] = g; B.lmCost[l] = cost; B.lmValid[l] = valid; }
             __syncwarp();
         }
     }
@@ -902,12 +940,14 @@ __global__ void k_candidate(DevBatch B) {
     for (int k = threadIdx.x; k < wd.K; k += blockDim.x) {
         const int gk = wd.kf0 + k;
         posePlus(B.pose[0] + 7ll * gk, dr + 15 * k, B.pose[1] + 7ll * gk);
+        poseRotation(B.pose[1] + 7ll * gk, B.rotKf[1] + 9ll * gk);
         for (int j = 0; j < 9; ++j) B.sb[1][9ll * gk + j] = B.sb[0][9ll * gk + j] + dr[15 * k + 6 + j];
     }
     for (int e = threadIdx.x; e < wd.E; e += blockDim.x) {
         const int ge = wd.ext0 + e;
         if (wd.estExt) posePlus(B.ext[0] + 7ll * ge, dr + 15 * wd.K + 6 * e, B.ext[1] + 7ll * ge);
         else for (int j = 0; j < 7; ++j) B.ext[1][7ll * ge + j] = B.ext[0][7ll * ge + j];
+        poseRotation(B.ext[1] + 7ll * ge, B.rotExt[1] + 9ll * ge);
     }
     if (threadIdx.x == 0)
         B.td[1][wdx] = B.td[0][wdx] + (wd.estTd ? dr[15 * wd.K + (wd.estExt ? 6 * wd.E : 0)] : 0.0);

@@ -160,6 +160,14 @@ __device__ __forceinline__ bool unitPose(const double* x) {
     return fabs(n - 1) <= 1e-6;
 }
 
+// Rotation matrix (row-major) of a pose's normalized quaternion; computed once
+// per keyframe and extrinsic per state and read by every factor that uses it.
+__device__ __forceinline__ void poseRotation(const double* x, double* R) {
+    const m3 m = qrot(qnormalized(ldq(x + 3)));
+#pragma unroll
+    for (int i = 0; i < 9; ++i) R[i] = m.a[i];
+}
+
 // ---- S^2 bearing factor -------------------------------------------------------------
 // Inputs of one factor, gathered by the caller.
 struct FactorIn {
@@ -167,6 +175,7 @@ struct FactorIn {
     const double* xb;   // observer pose
     const double* xea;  // extrinsic of the anchor camera
     const double* xeb;  // extrinsic of the observer camera
+    const double* Ra; const double* Rb; const double* Rea; const double* Reb;  // their rotations (poseRotation)
     const double* Rca; const double* tca;  // fixed T_RC of the anchor camera (row-major)
     const double* Rcb; const double* tcb;
     d3 anchor, anchorVel, measured, measuredVel;
@@ -237,9 +246,9 @@ __device__ inline bool evalBearingFactor(const FactorIn& in, bool derivatives, F
         pc = mtv(Rcb, local - tcb);
         cameraRotation = mul(tr(Rcb), Rca);
     } else {
-        Ra = qrot(qnormalized(ldq(in.xa + 3)));
-        Rb = qrot(qnormalized(ldq(in.xb + 3)));
-        const m3 Rea = qrot(qnormalized(ldq(in.xea + 3))), Reb = qrot(qnormalized(ldq(in.xeb + 3)));
+        Ra = ldm3(in.Ra);
+        Rb = ldm3(in.Rb);
+        const m3 Rea = ldm3(in.Rea), Reb = ldm3(in.Reb);
         const d3 tea = ld3(in.xea), teb = ld3(in.xeb);
         W = tr(mul(mul(Rb, Reb), Rcb));
         cameraRotation = mul(W, mul(mul(Ra, Rea), Rca));

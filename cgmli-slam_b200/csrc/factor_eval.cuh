@@ -20,6 +20,10 @@ __device__ __forceinline__ void gatherFactor(const DevBatch& B, const WinDesc& w
     in.xb = B.pose[buf] + 7ll * kfb;
     in.xea = B.ext[buf] + 7ll * ea;
     in.xeb = B.ext[buf] + 7ll * eb;
+    in.Ra = B.rotKf[buf] + 9ll * kfa;
+    in.Rb = B.rotKf[buf] + 9ll * kfb;
+    in.Rea = B.rotExt[buf] + 9ll * ea;
+    in.Reb = B.rotExt[buf] + 9ll * eb;
     in.Rca = B.camR + 9ll * cama; in.tca = B.camT + 3ll * cama;
     in.Rcb = B.camR + 9ll * camb; in.tcb = B.camT + 3ll * camb;
     in.anchor = ld3(B.lmBearing + 3ll * l);

@@ -1376,8 +1376,15 @@ cudaError_t configureMarginalization(size_t visualSmem, size_t rowsSmem, int max
     return cudaFuncSetAttribute(k_marg_eigen, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)use);
 }
 // Returns the number of launches.
+// Rotations of the accepted state (the factors' inputs), one thread per keyframe or extrinsic.
+__global__ void k_marg_rotations(DevBatch B) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < B.numKf) poseRotation(B.pose[0] + 7ll * t, B.rotKf[0] + 9ll * t);
+    else if (t < B.numKf + B.numExt) poseRotation(B.ext[0] + 7ll * (t - B.numKf), B.rotExt[0] + 9ll * (t - B.numKf));
+}
 int launchMarginalization(const DevBatch& B, const MargBatch& M, size_t visualSmem, cudaStream_t s) {
-    int n = 0;
+    int n = 1;
+    k_marg_rotations<<<(B.numKf + B.numExt + 255) / 256, 256, 0, s>>>(B);
     if (M.numElim > 0) {
         const int warps = 8;
         k_marg_eval<<<(M.numElim + warps - 1) / warps, 32 * warps, 0, s>>>(B, M);
