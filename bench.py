@@ -204,8 +204,10 @@ def run_served(args, local, backend):
     arrival = np.cumsum(rng.exponential(1.0 / args.serve_rate, n_req))
     rigs = 128
     server = backend.Server(device=local, iterations=1, policy=abi.MARGIN_OLD)
-    # warm-up: both solvers see a full batch
-    server.replay(pool, [0] * len(pool), np.zeros(len(pool)))
+    # warm-up: repeated full-pool bursts, so that both solvers reach their working
+    # size (growing pinned staging later would synchronize the device mid-trace)
+    for _ in range(4):
+        server.replay(pool, [0] * len(pool), np.zeros(len(pool)))
     windows = [pool[i % len(pool)] for i in range(n_req)]
     lat, status, span = server.replay(windows, [0] * n_req, arrival)
     server.close()

@@ -64,7 +64,9 @@ int cudaFail(cudaError_t e, const char* what) {
         if (e_ != cudaSuccess) return cudaFail(e_, #call);      \
     } while (0)
 
-// Grow-only device array (src/common/CudaArray.hpp:10-39 keeps the same policy).
+// Grow-only device array (src/common/CudaArray.hpp:10-39 keeps the same policy);
+// it grows by at least half its size, so batches of slowly rising size do not
+// reallocate at every call.
 template <class T>
 struct DArray {
     T* p = nullptr;
@@ -73,9 +75,10 @@ struct DArray {
         if (n <= cap) return cudaSuccess;
         if (p) cudaFree(p);
         p = nullptr;
+        const size_t want = std::max<size_t>(std::max(n, cap + cap / 2), 1);
         cap = 0;
-        const cudaError_t e = cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T));
-        if (e == cudaSuccess) cap = n;
+        const cudaError_t e = cudaMalloc(&p, want * sizeof(T));
+        if (e == cudaSuccess) cap = want;
         return e;
     }
     template <class V>
@@ -149,6 +152,8 @@ struct cgmli_solver {
     HVec<int> hMargRank, hMargStatus;
     // pinned staging of the marginalization's inputs, and the event after their uploads
     HVec<MargElim> hMargElim;
+    HVec<MargWin> hMargWin;      // pinned: a pageable upload would first wait for the stream's solve
+    HVec<WinDesc> hWin;
     HVec<int> hMargCols, hMargObsMap, hMargPoseCol, hMargSbCol, hMargExtCol;
     HVec<int> hMargVisCol, hMargVisPose, hMargVisExt, hMargSlow;
     HVec<int4> hMargChunks, hMargItems;
@@ -305,7 +310,8 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     S->facSmem = factorSmemBytes(S->maxNr);
     CK(configureKernels(S->linSmem, S->facSmem));
     const long long lm = hb.totalLm;
-    CK(S->dWin.upload(S->win, st));
+    S->hWin.assign(S->win.begin(), S->win.end());  // pinned staging: the copy stays asynchronous
+    CK(S->dWin.upload(S->hWin, st));
     CK(S->dLm.reserve(count));
     CK(S->dRuns.upload(hb.runs, st));
     CK(S->dTiles.upload(hb.tiles, st));
@@ -862,7 +868,8 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
     }
     long long eigenSmem = 0, fastSmem = 0;
     CK(configureMarginalization(smem, rowsSmem, maxNr, maxFastNr, &eigenSmem, &fastSmem));
-    CK(S->dMargWin.upload(mwv, st));
+    S->hMargWin.assign(mwv.begin(), mwv.end());  // guarded by margUploaded like the other staging
+    CK(S->dMargWin.upload(S->hMargWin, st));
     CK(S->dMargElim.upload(elims, st));
     CK(S->margCols.upload(cols, st));
     CK(S->margObsMap.upload(obsMap, st));

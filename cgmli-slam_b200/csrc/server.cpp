@@ -1,17 +1,18 @@
 // Served mode: continuous batching of window-solve requests (see the
 // cgmli_server_* declarations in cgmli_backend.h).
 //
-// One scheduler thread owns two solvers, each with its own CUDA stream.  Each
-// cycle it (1) takes the queued requests that fit the next batch (arrival
-// order, window cap, device-footprint budget), builds and uploads that batch
-// on the idle solver and launches its LM solve and marginalization, then
-// (2) completes the batch launched in the previous cycle: synchronizes its
-// stream, writes the states back into the callers' windows, and records the
-// reports and priors.  The host work of step (1) therefore overlaps the device
-// work of the previous batch, and requests arriving while the GPU is busy
-// join the next batch.
+// Two solvers, each with its own CUDA stream, and two threads.  The scheduler
+// takes the queued requests that fit the next batch (arrival order, window cap,
+// device-footprint budget) as soon as a solver is free, builds and uploads that
+// batch and launches its LM solve and marginalization.  The completion thread
+// waits for each launched batch in order, writes the states back into the
+// callers' windows, records the reports and priors, and frees the solver.  The
+// host work of one batch therefore overlaps both the device work and the
+// read-back of the other, and requests arriving meanwhile join the next batch.
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <deque>
 #include <memory>
 #include <mutex>
@@ -57,7 +58,7 @@ struct cgmli_server {
     cgmli_server_options opt{};
     cgmli_solver* solver[2] = {nullptr, nullptr};
     std::mutex mu;
-    std::condition_variable work, done;
+    std::condition_variable work, done, freed, launchedCv;
     std::deque<Request*> queue;
     std::unordered_map<long long, std::unique_ptr<Request>> requests;
     long long nextTicket = 1;
@@ -70,7 +71,12 @@ struct cgmli_server {
         int solver = 0;
         bool marg = false;
         int status = CGMLI_OK;
+        double launchMs = 0;
     };
+    bool busy[2] = {false, false};                 // solver has a launched, uncompleted batch
+    std::deque<std::unique_ptr<Batch>> launched;   // scheduler -> completion thread
+    bool schedulerDone = false;
+    bool trace = false;
 
     // Launches a batch on solver s (asynchronous on its stream).
     void launch(Batch& b) {
@@ -89,12 +95,15 @@ struct cgmli_server {
     }
 
     // Waits for a launched batch and records its results.
-    void complete(Batch& b) {
+    void complete(Batch& b, double* waitMs = nullptr, double* readMs = nullptr) {
         cgmli_solver* S = solver[b.solver];
         const int n = (int)b.reqs.size();
         std::vector<cgmli_solve_report> reps(n);
         int st = b.status;
+        const auto w0 = Clock::now();
         if (st == CGMLI_OK) st = cgmli_solver_synchronize(S);
+        const auto w1 = Clock::now();
+        if (waitMs) *waitMs = std::chrono::duration<double, std::milli>(w1 - w0).count();
         if (st == CGMLI_OK) st = cgmli_solver_read_states(S, b.windows.data(), n);
         if (st == CGMLI_OK) st = cgmli_solver_read_reports(S, reps.data(), n);
         for (int i = 0; i < n; ++i) {
@@ -124,6 +133,7 @@ struct cgmli_server {
             }
         }
         const auto now = Clock::now();
+        if (readMs) *readMs = std::chrono::duration<double, std::milli>(now - w1).count();
         {
             std::lock_guard<std::mutex> lock(mu);
             for (Request* r : b.reqs) {
@@ -135,34 +145,73 @@ struct cgmli_server {
         b.reqs.clear();
     }
 
+    // Scheduler: forms the next batch from the queue as soon as a solver is
+    // free, builds and launches it, and hands it to the completion thread.
     void run() {
-        Batch inflight;
-        bool haveInflight = false;
         int cur = 0;
         const long long budget = opt.memory_budget_bytes;
+        // CGMLI_SERVER_TRACE set: one line per batch on stderr (size, host launch
+        // time, the completion thread's wait and read-back; milliseconds)
+        trace = std::getenv("CGMLI_SERVER_TRACE") != nullptr;
+        std::thread completer([this] { completeLoop(); });
         for (;;) {
-            Batch next;
+            auto next = std::make_unique<Batch>();
             {
                 std::unique_lock<std::mutex> lock(mu);
-                if (!haveInflight) work.wait(lock, [&] { return stopping || !queue.empty(); });
-                if (queue.empty() && !haveInflight && stopping) return;
+                work.wait(lock, [&] { return stopping || (!queue.empty() && !busy[cur]); });
+                if (stopping && queue.empty()) break;
+                if (busy[cur]) freed.wait(lock, [&] { return !busy[cur]; });  // stopping with queued requests
                 long long bytes = 0;
-                while (!queue.empty() && (int)next.reqs.size() < opt.max_batch_windows) {
+                while (!queue.empty() && (int)next->reqs.size() < opt.max_batch_windows) {
                     const long long f = footprint(queue.front()->window);
-                    if (!next.reqs.empty() && bytes + f > budget) break;
+                    if (!next->reqs.empty() && bytes + f > budget) break;
                     bytes += f;
-                    next.reqs.push_back(queue.front());
+                    next->reqs.push_back(queue.front());
                     queue.pop_front();
                 }
+                busy[cur] = true;
             }
-            if (!next.reqs.empty()) {
-                next.solver = cur;
-                launch(next);
-                cur ^= 1;
+            const auto c0 = Clock::now();
+            next->solver = cur;
+            launch(*next);
+            next->launchMs = std::chrono::duration<double, std::milli>(Clock::now() - c0).count();
+            {
+                std::lock_guard<std::mutex> lock(mu);
+                launched.push_back(std::move(next));
             }
-            if (haveInflight) complete(inflight);
-            haveInflight = !next.reqs.empty();
-            if (haveInflight) inflight = std::move(next);
+            launchedCv.notify_one();
+            cur ^= 1;
+        }
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            schedulerDone = true;
+        }
+        launchedCv.notify_one();
+        completer.join();
+    }
+    // Completion thread: waits for each launched batch in launch order, records
+    // its results and frees its solver.
+    void completeLoop() {
+        for (;;) {
+            std::unique_ptr<Batch> b;
+            {
+                std::unique_lock<std::mutex> lock(mu);
+                launchedCv.wait(lock, [&] { return schedulerDone || !launched.empty(); });
+                if (launched.empty()) return;
+                b = std::move(launched.front());
+                launched.pop_front();
+            }
+            double waitMs = 0, readMs = 0;
+            const int size = (int)b->reqs.size();
+            const int sv = b->solver;
+            complete(*b, trace ? &waitMs : nullptr, trace ? &readMs : nullptr);
+            if (trace) std::fprintf(stderr, "batch %d launch %.3f wait %.3f read %.3f\n", size, b->launchMs, waitMs, readMs);
+            {
+                std::lock_guard<std::mutex> lock(mu);
+                busy[sv] = false;
+            }
+            freed.notify_all();
+            work.notify_all();
         }
     }
 };
