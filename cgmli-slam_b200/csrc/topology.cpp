@@ -319,10 +319,20 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
             hb.rho[g] = w.rho[l];
             // observations sorted by observer keyframe (slot order), stable
             int fo[kMaxTrackChunk];
+            bool inOrder = true;
             for (int k = 0; k < nobs; ++k) {
                 int j = k;
                 fo[j] = b + k;
-                while (j > 0 && w.obs_kf[fo[j - 1]] > w.obs_kf[fo[j]]) { std::swap(fo[j - 1], fo[j]); --j; }
+                while (j > 0 && w.obs_kf[fo[j - 1]] > w.obs_kf[fo[j]]) { std::swap(fo[j - 1], fo[j]); --j; inOrder = false; }
+            }
+            if (inOrder && nobs > 0) {  // the usual case: the observation arrays copy as runs
+                const size_t o0 = (size_t)obPos;
+                std::memcpy(&hb.obBearing[3 * o0], &w.obs_bearing[3ll * b], sizeof(double) * 3 * nobs);
+                std::memcpy(&hb.obP[6 * o0], &w.obs_P[6ll * b], sizeof(double) * 6 * nobs);
+                if (w.obs_velocity) std::memcpy(&hb.obVel[3 * o0], &w.obs_velocity[3ll * b], sizeof(double) * 3 * nobs);
+                else std::memset(&hb.obVel[3 * o0], 0, sizeof(double) * 3 * nobs);
+                if (w.obs_time) std::memcpy(&hb.obTime[o0], &w.obs_time[b], sizeof(double) * nobs);
+                else std::memset(&hb.obTime[o0], 0, sizeof(double) * nobs);
             }
             for (int k = 0; k < nobs; ++k) {
                 const int f = fo[k], o = obPos++;
@@ -338,6 +348,7 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
                     while (sl[nkf[l] + xs] != x) ++xs;
                 }
                 hb.obXslot[o] = xs;
+                if (inOrder) continue;
                 for (int k2 = 0; k2 < 3; ++k2) {
                     hb.obBearing[3ll * o + k2] = w.obs_bearing[3 * f + k2];
                     hb.obVel[3ll * o + k2] = w.obs_velocity ? w.obs_velocity[3 * f + k2] : 0.0;
@@ -375,37 +386,58 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
             P.pairChunks.push_back(make_int4(i, d.obs0 + c0, d.obs0 + std::min(F, c0 + 32), 0));
         // Schur chunks: runs of consecutive landmarks whose support columns
         // together fit the chunk's shared rows (schurChunkFits); the column
-        // union of each chunk and every landmark's map into it
+        // union of each chunk and every landmark's map into it.  Unions are kept
+        // as bit sets of column blocks: keyframe k, extrinsic K + e, td K + E.
         {
             const int tdCol = 6 * d.K + (d.estExt ? 6 * d.E : 0);
-            const int words = (d.Npc + 63) / 64;
+            const int tdBlk = d.K + d.E, nBlk = tdBlk + 1;
+            const int words = (nBlk + 63) / 64;
             std::vector<unsigned long long> U(words, 0), Ul(words, 0);
-            std::vector<int> lc, pos(d.Npc, -1);
+            std::vector<int> blkPos(nBlk, 0);
             P.umap.assign(P.cross, 0);
-            int q0 = 0, nu = 0;
-            auto columnsOf = [&](int q) {
+            auto blocksOf = [&](int q) {
+                std::fill(Ul.begin(), Ul.end(), 0ull);
                 const int g = d.lm0 + q, ns_ = hb.lmNs[g], nx_ = hb.lmNx[g];
                 const int* sk = &P.supp[hb.lmSupp0[g]];
-                const int ns = 6 * (ns_ + nx_) + (d.estTd ? 1 : 0);
-                lc.resize(ns);
-                for (int c = 0; c < ns; ++c)
-                    lc[c] = c < 6 * ns_ ? 6 * sk[c / 6] + c % 6
-                          : c < 6 * (ns_ + nx_) ? 6 * d.K + 6 * sk[ns_ + (c - 6 * ns_) / 6] + c % 6 : tdCol;
+                for (int j = 0; j < ns_; ++j) Ul[sk[j] >> 6] |= 1ull << (sk[j] & 63);
+                for (int j = 0; j < nx_; ++j) {
+                    const int b = d.K + sk[ns_ + j];
+                    Ul[b >> 6] |= 1ull << (b & 63);
+                }
+                if (d.estTd) Ul[tdBlk >> 6] |= 1ull << (tdBlk & 63);
             };
+            auto columnsIn = [&](const std::vector<unsigned long long>& a, const std::vector<unsigned long long>* b) {
+                int blocks = 0;
+                for (int wi = 0; wi < words; ++wi) blocks += __builtin_popcountll(a[wi] | (b ? (*b)[wi] : 0ull));
+                return d.estTd ? 6 * (blocks - 1) + 1 : 6 * blocks;
+            };
+            int q0 = 0, nu = 0;
             auto closeChunk = [&](int q1) {
                 const int off = (int)P.schurCols.size();
                 P.schurCols.push_back(nu);
                 int k = 0;
                 for (int wi = 0; wi < words; ++wi)
                     for (unsigned long long bits = U[wi]; bits; bits &= bits - 1) {
-                        const int col = 64 * wi + __builtin_ctzll(bits);
-                        P.schurCols.push_back(col);
-                        pos[col] = k++;
+                        const int blk = 64 * wi + __builtin_ctzll(bits);
+                        blkPos[blk] = k;
+                        if (blk == tdBlk && d.estTd) {
+                            P.schurCols.push_back(tdCol);
+                            k += 1;
+                        } else {
+                            const int col0 = blk < d.K ? 6 * blk : 6 * d.K + 6 * (blk - d.K);
+                            for (int c = 0; c < 6; ++c) P.schurCols.push_back(col0 + c);
+                            k += 6;
+                        }
                     }
                 for (int q = q0; q < q1; ++q) {
-                    columnsOf(q);
-                    const long long c0 = hb.lmC0[d.lm0 + q];  // window-local here
-                    for (size_t c = 0; c < lc.size(); ++c) P.umap[c0 + c] = (unsigned short)pos[lc[c]];
+                    const int g = d.lm0 + q, ns_ = hb.lmNs[g], nx_ = hb.lmNx[g];
+                    const int* sk = &P.supp[hb.lmSupp0[g]];
+                    const long long c0 = hb.lmC0[g];  // window-local here
+                    for (int j = 0; j < ns_; ++j)
+                        for (int c = 0; c < 6; ++c) P.umap[c0 + 6 * j + c] = (unsigned short)(blkPos[sk[j]] + c);
+                    for (int j = 0; j < nx_; ++j)
+                        for (int c = 0; c < 6; ++c) P.umap[c0 + 6 * (ns_ + j) + c] = (unsigned short)(blkPos[d.K + sk[ns_ + j]] + c);
+                    if (d.estTd) P.umap[c0 + 6 * (ns_ + nx_)] = (unsigned short)blkPos[tdBlk];
                 }
                 P.schurChunks.push_back(make_int4(i, d.lm0 + q0, d.lm0 + q1, off));
                 std::fill(U.begin(), U.end(), 0ull);
@@ -413,15 +445,11 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
                 q0 = q1;
             };
             for (int q = 0; q < L; ++q) {
-                columnsOf(q);
-                std::fill(Ul.begin(), Ul.end(), 0ull);
-                for (int c : lc) Ul[c >> 6] |= 1ull << (c & 63);
-                int nuNew = 0;
-                for (int wi = 0; wi < words; ++wi) nuNew += __builtin_popcountll(U[wi] | Ul[wi]);
+                blocksOf(q);
+                int nuNew = columnsIn(U, &Ul);
                 if (q > q0 && !schurChunkFits(q - q0 + 1, nuNew)) {
                     closeChunk(q);
-                    nuNew = 0;
-                    for (int wi = 0; wi < words; ++wi) nuNew += __builtin_popcountll(Ul[wi]);
+                    nuNew = columnsIn(Ul, nullptr);
                 }
                 for (int wi = 0; wi < words; ++wi) U[wi] |= Ul[wi];
                 nu = nuNew;
