@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(kLinWarps * 32, 2) k_lin_landmark(DevBatch B, 
 // ---- L2: J^T J and J^T r by observation key ------------------------------------------
 // Work unit: a chunk of <= 32 consecutive positions of one window's key order.
 // The warp gathers the chunk's staged rows (written by k_lin_landmark) into
-// shared memory.  For each run of equal keys the Gram matrix G = J'^T J' of the
+// shared memory, kPairRows at a time.  For each run of equal keys the Gram matrix G = J'^T J' of the
 // run's weighted rows is formed on the FP64 tensor path (mma.sync m8n8k4):
 // J' is the 2x25 compact Jacobian of each observation with the weighted
 // residual appended as column 25 and zero-padded to 32 columns, so that G's
@@ -274,7 +274,8 @@ __global__ void __launch_bounds__(kLinWarps * 32, 2) k_lin_landmark(DevBatch B, 
 // covers two observations; the ten upper 8x8 tiles of the 32x32 G live in
 // registers (two doubles per lane each) and are added to the window once per run.
 constexpr int kPairStride = kKeyRow + 1;  // odd stride
-__host__ __device__ constexpr size_t pairCtaBytes() { return sizeof(double) * kPairWarps * 32 * kPairStride; }
+constexpr int kPairRows = 16;             // rows staged per round: small staging, more resident warps
+__host__ __device__ constexpr size_t pairCtaBytes() { return sizeof(double) * kPairWarps * kPairRows * kPairStride; }
 
 __device__ __forceinline__ void mmaF64(double& d0, double& d1, double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
@@ -290,26 +291,8 @@ __global__ void __launch_bounds__(kPairWarps * 32) k_lin_pairs(DevBatch B, const
     const int4 ch = chunks[ci];  // {window, first key-ordered position, end, -}
     const int wdx = ch.x;
     if (B.lm[wdx].mode != kModeLinearize) return;
-    double* rows = smemRaw + (size_t)warp * 32 * kPairStride;
+    double* rows = smemRaw + (size_t)warp * kPairRows * kPairStride;
     const WinDesc wd = B.win[wdx];
-    const int n = ch.z - ch.y;
-    {
-        // gather: each lane loads its own key-ordered row (unrolled 16-byte loads)
-        if (lane < n) {
-            const double2* src = reinterpret_cast<const double2*>(B.keyRows + (size_t)B.keyOrder[ch.y + lane] * kKeyRow);
-            double* dst = rows + lane * kPairStride;
-#pragma unroll
-            for (int q = 0; q < 27; ++q) {
-                const double2 v = src[q];
-                dst[2 * q] = v.x;
-                dst[2 * q + 1] = v.y;
-            }
-        }
-    }
-    __syncwarp();
-    const long long key = lane < n ? __double_as_longlong(rows[lane * kPairStride + 52]) : -1ll;
-    const long long prev = __shfl_up_sync(0xffffffffu, key, 1);
-    unsigned starts = __ballot_sync(0xffffffffu, lane < n && (lane == 0 || prev != key));
     const int K = wd.K, Npc = wd.Npc;
     const int tdCol = 6 * K + (wd.estExt ? 6 * wd.E : 0);
     double* JJ = B.acc + wd.acc0;
@@ -317,33 +300,14 @@ __global__ void __launch_bounds__(kPairWarps * 32) k_lin_pairs(DevBatch B, const
     // fragment coordinates: k-step row kr = lane % 4 (observation kr / 2, row kr % 2),
     // column lane / 4 within an 8-column block; accumulator row lane / 4, columns 2 (lane % 4) + {0, 1}
     const int kr = lane & 3, cIn = lane >> 2;
-    while (starts) {
-        const int s0 = __ffs(starts) - 1;
-        starts &= starts - 1;
-        const int s1 = starts ? __ffs(starts) - 1 : n;
-        double g[10][2];
+    double g[10][2];
 #pragma unroll
-        for (int t = 0; t < 10; ++t) g[t][0] = g[t][1] = 0.0;
-        for (int m = s0; m < s1; m += 2) {
-            const int o = m + (kr >> 1), r = kr & 1;
-            const double* st = rows + o * kPairStride;
-            double frag[4];
-#pragma unroll
-            for (int I = 0; I < 4; ++I) {
-                const int col = 8 * I + cIn;
-                double v = 0.0;
-                if (o < s1) v = col < 25 ? st[25 * r + col] : (col == 25 ? st[50 + r] : 0.0);
-                frag[I] = v;
-            }
-            int t = 0;
-#pragma unroll
-            for (int I = 0; I < 4; ++I)
-#pragma unroll
-                for (int J = I; J < 4; ++J, ++t) mmaF64(g[t][0], g[t][1], frag[I], frag[J]);
-        }
-        const long long kk = __shfl_sync(0xffffffffu, key, s0);
-        const int ka = (int)(kk & 0xffff), kb = (int)((kk >> 16) & 0xffff);
-        const int xa = (int)((kk >> 32) & 0xffff), xb = (int)((kk >> 48) & 0xffff);
+    for (int t = 0; t < 10; ++t) g[t][0] = g[t][1] = 0.0;
+    long long cur = -1;  // key of the run held in g
+    auto flush = [&]() {
+        if (cur < 0) return;
+        const int ka = (int)(cur & 0xffff), kb = (int)((cur >> 16) & 0xffff);
+        const int xa = (int)((cur >> 32) & 0xffff), xb = (int)((cur >> 48) & 0xffff);
         const bool sameKf = ka == kb, split = xa != xb, same = sameKf && !split;
         auto colOf = [&](int c) -> int {
             if (c < 6) return sameKf ? -1 : 6 * ka + c;
@@ -361,6 +325,7 @@ __global__ void __launch_bounds__(kPairWarps * 32) k_lin_pairs(DevBatch B, const
                 for (int e = 0; e < 2; ++e) {
                     const int i = 8 * I + cIn, j = 8 * J + 2 * kr + e;
                     const double v = g[t][e];
+                    g[t][e] = 0.0;
                     if (v == 0.0 || i > j || i >= 25 || j > 25) continue;
                     const int ci2 = colOf(i);
                     if (ci2 < 0) continue;
@@ -369,7 +334,58 @@ __global__ void __launch_bounds__(kPairWarps * 32) k_lin_pairs(DevBatch B, const
                     if (cj < 0) continue;
                     atomicAdd(&JJ[ci2 <= cj ? upIdx(ci2, cj, Npc) : upIdx(cj, ci2, Npc)], v);
                 }
+        cur = -1;
+    };
+    // the chunk is staged kPairRows rows at a time; a run of equal keys that
+    // continues into the next round keeps its sums in registers
+    for (int h0 = ch.y; h0 < ch.z; h0 += kPairRows) {
+        const int n = min(kPairRows, ch.z - h0);
+        if (lane < n) {  // gather: each lane loads its own key-ordered row (unrolled 16-byte loads)
+            const double2* src = reinterpret_cast<const double2*>(B.keyRows + (size_t)B.keyOrder[h0 + lane] * kKeyRow);
+            double* dst = rows + lane * kPairStride;
+#pragma unroll
+            for (int q = 0; q < 27; ++q) {
+                const double2 v = src[q];
+                dst[2 * q] = v.x;
+                dst[2 * q + 1] = v.y;
+            }
+        }
+        __syncwarp();
+        const long long key = lane < n ? __double_as_longlong(rows[lane * kPairStride + 52]) : -1ll;
+        const long long prev = __shfl_up_sync(0xffffffffu, key, 1);
+        unsigned starts = __ballot_sync(0xffffffffu, lane < n && (lane == 0 || prev != key));
+        while (starts) {
+            const int s0 = __ffs(starts) - 1;
+            starts &= starts - 1;
+            const int s1 = starts ? __ffs(starts) - 1 : n;
+            const long long kk = __shfl_sync(0xffffffffu, key, s0);
+            if (kk != cur) {
+                flush();
+                cur = kk;
+            }
+            for (int m = s0; m < s1; m += 2) {
+                const int o = m + (kr >> 1), r = kr & 1;
+                double frag[4];
+#pragma unroll
+                for (int I = 0; I < 4; ++I) {
+                    const int col = 8 * I + cIn;
+                    double v = 0.0;
+                    if (o < s1) {
+                        const double* st = rows + o * kPairStride;
+                        v = col < 25 ? st[25 * r + col] : (col == 25 ? st[50 + r] : 0.0);
+                    }
+                    frag[I] = v;
+                }
+                int t = 0;
+#pragma unroll
+                for (int I = 0; I < 4; ++I)
+#pragma unroll
+                    for (int J = I; J < 4; ++J, ++t) mmaF64(g[t][0], g[t][1], frag[I], frag[J]);
+            }
+        }
+        __syncwarp();  // the next round's gather overwrites the staged rows
     }
+    flush();
 }
 
 // ---- L3: Schur term as a compact SYRK per chunk of landmarks -------------------------
