@@ -1022,12 +1022,12 @@ __global__ void __launch_bounds__(256) k_backsub(DevBatch B) {
 }
 
 // Robust cost of the candidate point (launchTrial, VisualCudaBatch.cu:715-721):
-// one warp per tile of <= 32 observations, lane = observation.
+// one warp per tile of <= 32 observations, lane = observation; the per-landmark
+// sums are segmented scans over the tile's lanes (a landmark's observations are
+// consecutive lanes), written by each landmark's last lane.
 constexpr int kTrialWarps = 8;
 __global__ void __launch_bounds__(kTrialWarps * 32, 2) k_trial(DevBatch B, const int2* tiles, int numTiles) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __shared__ double tcost[kTrialWarps][32];
-    __shared__ int tvalid[kTrialWarps][32];
     const int t = blockIdx.x * kTrialWarps + warp;
     if (t >= numTiles) return;
     const int2 tile = tiles[t];
@@ -1035,28 +1035,37 @@ __global__ void __launch_bounds__(kTrialWarps * 32, 2) k_trial(DevBatch B, const
     const int wdx = B.lmWin[lb];
     if (B.lm[wdx].mode == kModeDone) return;
     const WinDesc wd = B.win[wdx];
-    if (lane < nl) {
-        tcost[warp][lane] = 0.0;
-        tvalid[warp][lane] = B.lmMaxInc[lb + lane] >= 0.0 ? 1 : 0;  // -1 marks a non-finite step
-    }
-    __syncwarp();
     const int ob = B.lmObsBegin[lb], oe = B.lmObsBegin[le];
     const int f = ob + lane;
-    if (f < oe) {
-        int q = 0;
-        while (B.lmObsBegin[lb + q + 1] <= f) ++q;
-        const int l = lb + q;
+    const bool live = f < oe;
+    const int seg = live ? B.obLm[f] - lb : 32 + lane;  // lanes past the tile: segments of their own
+    double cost = 0.0;
+    int bad = 0;
+    if (live) {
         FactorIn in;
         int kfa, kfb, ea, eb;
-        gatherFactor(B, wd, wdx, l, f, 1, in, kfa, kfb, ea, eb);
+        gatherFactor(B, wd, wdx, lb + seg, f, 1, in, kfa, kfb, ea, eb);
         FactorOut o;
-        if (!evalBearingFactor(in, false, o)) tvalid[warp][q] = 0;
-        else atomicAdd(&tcost[warp][q], huberCost(wd.huber, o.r[0] * o.r[0] + o.r[1] * o.r[1]));
+        if (!evalBearingFactor(in, false, o)) bad = 1;
+        else cost = huberCost(wd.huber, o.r[0] * o.r[0] + o.r[1] * o.r[1]);
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double c2 = __shfl_up_sync(0xffffffffu, cost, o);
+        const int b2 = __shfl_up_sync(0xffffffffu, bad, o), s2 = __shfl_up_sync(0xffffffffu, seg, o);
+        if (lane >= o && s2 == seg) { cost += c2; bad |= b2; }
+    }
+    // landmarks of the tile without observations keep cost 0
+    if (lane < nl) {
+        B.lmTrial[lb + lane] = 0.0;
+        B.lmTrialValid[lb + lane] = B.lmMaxInc[lb + lane] >= 0.0 ? 1 : 0;  // -1 marks a non-finite step
     }
     __syncwarp();
-    if (lane < nl) {
-        B.lmTrial[lb + lane] = tcost[warp][lane];
-        B.lmTrialValid[lb + lane] = tvalid[warp][lane];
+    const int nextSeg = __shfl_down_sync(0xffffffffu, seg, 1);
+    if (live && (lane == 31 || f + 1 >= oe || nextSeg != seg)) {
+        const int l = lb + seg;
+        B.lmTrial[l] = cost;
+        B.lmTrialValid[l] = bad ? 0 : (B.lmMaxInc[l] >= 0.0 ? 1 : 0);
     }
 }
 
