@@ -300,8 +300,40 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     S->win.clear();
     HostBatch& hb = S->hb;
     std::string why;
-    const int built = buildHostBatch(windows, count, 0, hb, why);
+    // the landmark and observation arrays (most of the bytes) are uploaded range
+    // by range as the builder finishes them, overlapping the rest of the build
+    cudaError_t streamErr = cudaSuccess;
+    bool reserved = false;
+    auto part = [&](auto& dev, const auto& host, size_t first, size_t n) {
+        if (streamErr != cudaSuccess || n == 0) return;
+        streamErr = cudaMemcpyAsync(dev.p + first, host.data() + first, n * sizeof(host[0]), cudaMemcpyHostToDevice, st);
+    };
+    const std::function<void(int, int)> ready = [&](int w0, int w1) {
+        if (!reserved) {
+            reserved = true;
+            const size_t ob = hb.obKf.size(), lmn = hb.lmKf.size();
+            cudaError_t e = cudaSuccess;
+            auto res = [&](auto& dev, size_t n) { if (e == cudaSuccess) e = dev.reserve(n); };
+            res(S->obBearing, 3 * ob); res(S->obP, 6 * ob); res(S->obVel, 3 * ob); res(S->obTime, ob);
+            res(S->obKf, ob); res(S->obCam, ob); res(S->obSlot, ob); res(S->obXslot, ob); res(S->obLm, ob); res(S->keyOrder, ob);
+            res(S->lmWin, lmn); res(S->lmKf, lmn); res(S->lmCam, lmn); res(S->lmNs, lmn); res(S->lmNx, lmn);
+            res(S->lmBearing, 3 * lmn); res(S->lmVel, 3 * lmn); res(S->lmTime, lmn); res(S->rho[0], lmn);
+            streamErr = e;
+        }
+        const WinDesc& a = hb.win[w0];
+        const WinDesc& b = hb.win[w1 - 1];
+        const size_t o0 = a.obs0, on = (size_t)b.obs0 + b.F - o0, l0 = a.lm0, ln = (size_t)b.lm0 + b.L - l0;
+        part(S->obBearing, hb.obBearing, 3 * o0, 3 * on); part(S->obP, hb.obP, 6 * o0, 6 * on);
+        part(S->obVel, hb.obVel, 3 * o0, 3 * on); part(S->obTime, hb.obTime, o0, on);
+        part(S->obKf, hb.obKf, o0, on); part(S->obCam, hb.obCam, o0, on); part(S->obSlot, hb.obSlot, o0, on);
+        part(S->obXslot, hb.obXslot, o0, on); part(S->obLm, hb.obLm, o0, on); part(S->keyOrder, hb.keyOrder, o0, on);
+        part(S->lmWin, hb.lmWin, l0, ln); part(S->lmKf, hb.lmKf, l0, ln); part(S->lmCam, hb.lmCam, l0, ln);
+        part(S->lmNs, hb.lmNs, l0, ln); part(S->lmNx, hb.lmNx, l0, ln); part(S->lmBearing, hb.lmBearing, 3 * l0, 3 * ln);
+        part(S->lmVel, hb.lmVel, 3 * l0, 3 * ln); part(S->lmTime, hb.lmTime, l0, ln); part(S->rho[0], hb.rho, l0, ln);
+    };
+    const int built = buildHostBatch(windows, count, 0, hb, why, &ready);
     if (built != CGMLI_OK) return fail(built, why);
+    CK(streamErr);
     S->win = hb.win;
     S->totalKf = hb.totalKf; S->totalExt = hb.totalExt; S->totalCam = hb.totalCam; S->totalLm = hb.totalLm;
     S->totalObs = hb.totalObs; S->totalImu = hb.totalImu;
@@ -320,17 +352,12 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     CK(S->schurCols.upload(hb.schurCols, st));
     CK(S->lmUmap.upload(hb.lmUmap, st));
     CK(S->camR.upload(hb.camR, st)); CK(S->camT.upload(hb.camT, st)); CK(S->camExt.upload(hb.camExt, st));
-    CK(S->lmWin.upload(hb.lmWin, st)); CK(S->lmKf.upload(hb.lmKf, st)); CK(S->lmCam.upload(hb.lmCam, st)); CK(S->lmObsBegin.upload(hb.lmObsBegin, st));
-    CK(S->lmNs.upload(hb.lmNs, st)); CK(S->lmNx.upload(hb.lmNx, st)); CK(S->lmSupp0.upload(hb.lmSupp0, st));
+    CK(S->lmObsBegin.upload(hb.lmObsBegin, st));
+    CK(S->lmSupp0.upload(hb.lmSupp0, st));
     CK(S->supp.upload(hb.supp, st)); CK(S->lmC0.upload(hb.lmC0, st));
-    CK(S->lmBearing.upload(hb.lmBearing, st)); CK(S->lmVel.upload(hb.lmVel, st)); CK(S->lmTime.upload(hb.lmTime, st));
-    CK(S->obKf.upload(hb.obKf, st)); CK(S->obCam.upload(hb.obCam, st)); CK(S->obSlot.upload(hb.obSlot, st));
-    CK(S->obXslot.upload(hb.obXslot, st)); CK(S->obLm.upload(hb.obLm, st)); CK(S->keyOrder.upload(hb.keyOrder, st));
     CK(S->keyRows.reserve((size_t)hb.totalObs * 56));
-    CK(S->obBearing.upload(hb.obBearing, st)); CK(S->obP.upload(hb.obP, st)); CK(S->obVel.upload(hb.obVel, st));
-    CK(S->obTime.upload(hb.obTime, st));
     CK(S->pose[0].upload(hb.pose, st)); CK(S->sb[0].upload(hb.sb, st)); CK(S->ext[0].upload(hb.ext, st));
-    CK(S->td[0].upload(hb.td, st)); CK(S->rho[0].upload(hb.rho, st));
+    CK(S->td[0].upload(hb.td, st));
     CK(S->pose[1].reserve(hb.pose.size())); CK(S->sb[1].reserve(hb.sb.size())); CK(S->ext[1].reserve(hb.ext.size()));
     for (int k = 0; k < 2; ++k) { CK(S->rotKf[k].reserve(9ull * hb.totalKf)); CK(S->rotExt[k].reserve(9ull * hb.totalExt)); }
     CK(S->td[1].reserve(hb.td.size())); CK(S->rho[1].reserve(hb.rho.size()));

@@ -109,7 +109,8 @@ int validateWindow(const cgmli_window& w, int index, std::string& why) {
     return CGMLI_OK;
 }
 
-int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatch& hb, std::string& why) {
+int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatch& hb, std::string& why,
+                   const std::function<void(int, int)>* ready) {
     if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
     threads = std::min(threads, 64);
     // ---- validation (parallel)
@@ -182,7 +183,7 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
     const int runLen = runLength(lm);
     // ---- phase 1: every window on its own thread
     std::vector<WindowPart> part(count);
-    parallelFor(count, threads, [&](int i) {
+    auto phase1 = [&](int i) {
         const auto& w = windows[i];
         const WinDesc& d = hb.win[i];
         WindowPart& P = part[i];
@@ -456,7 +457,14 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
             }
             if (L > q0) closeChunk(L);
         }
-    });
+    };
+    // in up to four ranges of windows when a caller streams the finished ranges
+    const int ranges = ready && count >= 4 * threads ? 4 : 1;
+    for (int r = 0; r < ranges; ++r) {
+        const int w0 = (int)((long long)count * r / ranges), w1 = (int)((long long)count * (r + 1) / ranges);
+        parallelFor(w1 - w0, threads, [&](int k) { phase1(w0 + k); });
+        if (ready) (*ready)(w0, w1);
+    }
     for (int i = 0; i < count; ++i)
         if (part[i].status != CGMLI_OK) {
             char buf[256];

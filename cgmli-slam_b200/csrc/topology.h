@@ -12,6 +12,9 @@
 
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
 #include <cstdlib>
 #include <new>
 #include <string>
@@ -23,6 +26,77 @@
 
 namespace cgmli {
 
+// Process-wide worker threads for parallelFor, created on first use and kept
+// (thread start-up is a sizable part of a small batch's host build).  One loop
+// runs on the pool at a time; a concurrent caller gets false and spawns its own.
+class WorkPool {
+public:
+    static WorkPool& get() {
+        static WorkPool pool;
+        return pool;
+    }
+    bool run(int count, int threads, const std::function<void(int)>& fn) {
+        std::unique_lock<std::mutex> use(use_, std::try_to_lock);
+        if (!use.owns_lock()) return false;
+        const int helpers = std::min(threads, count) - 1;
+        {
+            std::lock_guard<std::mutex> lock(m_);
+            while ((int)workers_.size() < helpers) {
+                const int id = (int)workers_.size();
+                workers_.emplace_back([this, id] { loop(id); });
+            }
+            job_ = &fn;
+            count_ = count;
+            next_ = 0;
+            want_ = helpers;
+            active_ = helpers;
+            ++gen_;
+        }
+        cv_.notify_all();
+        for (int i = next_++; i < count; i = next_++) fn(i);
+        std::unique_lock<std::mutex> lock(m_);
+        done_.wait(lock, [&] { return active_ == 0; });
+        job_ = nullptr;
+        return true;
+    }
+    ~WorkPool() {
+        {
+            std::lock_guard<std::mutex> lock(m_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : workers_) t.join();
+    }
+
+private:
+    void loop(int id) {
+        unsigned long long seen = 0;
+        for (;;) {
+            const std::function<void(int)>* job;
+            int count;
+            {
+                std::unique_lock<std::mutex> lock(m_);
+                cv_.wait(lock, [&] { return stop_ || (gen_ != seen && id < want_); });
+                if (stop_) return;
+                seen = gen_;
+                job = job_;
+                count = count_;
+            }
+            for (int i = next_++; i < count; i = next_++) (*job)(i);
+            std::lock_guard<std::mutex> lock(m_);
+            if (--active_ == 0) done_.notify_all();
+        }
+    }
+    std::mutex use_, m_;
+    std::condition_variable cv_, done_;
+    std::vector<std::thread> workers_;
+    const std::function<void(int)>* job_ = nullptr;
+    int count_ = 0, want_ = 0, active_ = 0;
+    std::atomic<int> next_{0};
+    unsigned long long gen_ = 0;
+    bool stop_ = false;
+};
+
 // Runs fn(i) for i in [0, n) on up to `threads` host threads (0: all cores).
 template <class Fn>
 void parallelFor(int n, int threads, Fn&& fn) {
@@ -31,6 +105,8 @@ void parallelFor(int n, int threads, Fn&& fn) {
         for (int i = 0; i < n; ++i) fn(i);
         return;
     }
+    const std::function<void(int)> job = [&](int i) { fn(i); };
+    if (WorkPool::get().run(n, threads, job)) return;
     std::atomic<int> next{0};
     auto body = [&] {
         for (int i = next++; i < n; i = next++) fn(i);
@@ -111,7 +187,11 @@ int validateWindow(const cgmli_window& w, int index, std::string& why);
 
 // Builds the batch with up to `threads` host threads (0: hardware concurrency).
 // Returns a CGMLI_* code and the reason.
-int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatch& out, std::string& why);
+// `ready`, when given, is called (on the calling thread) each time the windows
+// [w0, w1) have their landmark and observation arrays final, before the rest of
+// the batch is built, so that their uploads can overlap the remaining host work.
+int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatch& out, std::string& why,
+                   const std::function<void(int, int)>* ready = nullptr);
 
 // Invariants of a built batch (used by the diagnostic entry point and tests).
 int checkHostBatch(const cgmli_window* windows, int count, const HostBatch& hb, std::string& why);
