@@ -466,7 +466,7 @@ __device__ double blockSum(double v, double* red) {
 // evaluateRetained + accumulateRetained (VisualCudaBatch.cu:626-642) written
 // as block-structured accumulation.  Also evaluates the residual cost of the
 // candidate state when `trial` is set (launchTrial, :715-721).
-__global__ void __launch_bounds__(256) k_retained(DevBatch B, int trial) {
+__global__ void __launch_bounds__(256, 2) k_retained(DevBatch B, int trial) {
     const int wdx = blockIdx.x;
     const int mode = B.lm[wdx].mode;
     if (mode == kModeDone || (!trial && mode != kModeLinearize)) return;
