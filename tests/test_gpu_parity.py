@@ -127,6 +127,34 @@ def test_batch_result_equals_alone(backend):
     assert all(r.status == 0 for r in s.reports())
 
 
+def test_large_batch_streamed_upload_equals_alone(backend):
+    """A batch of 72 windows (at least four per host thread on a 16-thread host)
+    is built and uploaded in ranges that overlap the rest of the build; windows
+    from every range solve as they do alone."""
+    windows = synth.make_windows("c4", 72, seed=78)
+    picks = [0, 25, 50, 71]
+    x0 = [w.state_vector() for w in windows]
+    alone = {}
+    for i in picks:
+        s = backend.Solver()
+        s.set_windows([windows[i]])
+        s.solve(2)
+        s.synchronize()
+        s.read_states()
+        alone[i] = windows[i].state_vector()
+        s.close()
+        windows[i].set_state_vector(x0[i])
+    s = backend.Solver()
+    s.set_windows(windows)
+    s.solve(2)
+    s.synchronize()
+    s.read_states()
+    for i in picks:
+        assert rel(windows[i].state_vector() - x0[i], alone[i] - x0[i]) < 1e-8
+    assert all(r.status == 0 for r in s.reports())
+    s.close()
+
+
 def test_checkpoint_rollback_restores_states(backend):
     w = synth.SynthWindow(SPECS["tiny"], 5)
     x0 = w.state_vector()
