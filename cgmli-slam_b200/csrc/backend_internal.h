@@ -101,7 +101,7 @@ constexpr int kEigenThreads = 512;  // eigen CTAs
 // Schur chunks of the linearization (k_lin_schur): rows x padded width of the
 // chunk's column union + 1 fit the CTA's shared rows.
 constexpr int kSchurThreads = 256;
-constexpr int kSchurSmemDoubles = 12288;
+constexpr int kSchurSmemDoubles = 8192;
 constexpr int kSchurMaxRows = 128;
 inline bool schurChunkFits(int rows, int unionCols) {
     const int np = (unionCols + 1 + 31) / 32 * 32;

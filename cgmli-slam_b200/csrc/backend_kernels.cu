@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(kPairWarps * 32) k_lin_pairs(DevBatch B, const
 // B_v.  The rank update uses 32 x 32 tiles, one per warp (4 x 8 per lane);
 // spare warps split the rows when the tiles are fewer than the warps.  Every
 // tile is added to the window's Schur sum once per chunk.
-__global__ void __launch_bounds__(kSchurThreads, 2) k_lin_schur(DevBatch B, const int4* chunks) {
+__global__ void __launch_bounds__(kSchurThreads, 3) k_lin_schur(DevBatch B, const int4* chunks) {
     extern __shared__ __align__(16) double Rw[];
     const int4 ch = chunks[blockIdx.x];  // {window, first landmark, end landmark, offset of the column list}
     const int wdx = ch.x;

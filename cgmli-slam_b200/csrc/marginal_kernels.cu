@@ -887,7 +887,7 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_victim(MargBatch M) {
 // and A^T r0 agree with the eigen path's far below its own rounding.  Other
 // windows are left to k_marg_eigen.
 constexpr int kFastMaxN = 160;
-constexpr int kFastMaxFree = 16;  // null directions handled by the projection
+constexpr int kFastMaxFree = 32;  // null directions handled by the projection
 __host__ __device__ constexpr size_t fastSmemBytes(int n) {
     return sizeof(double) * ((size_t)n * n + 5 * (size_t)n) + sizeof(int) * 3 * (size_t)n;
 }
