@@ -63,6 +63,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--plain-windows", type=int, default=16, help="single-window solves timed for the plain path")
     p.add_argument("--marg-steps", type=int, default=3, help="timed batched marginalizations of the solved batch (0: off)")
+    p.add_argument("--no-configs", action="store_true", help="skip the single-window configurations c1-c3")
     p.add_argument("--serve-rate", type=float, default=5000.0, help="offered request rate of the served run (requests/s, 0: off)")
     p.add_argument("--serve-seconds", type=float, default=3.0, help="duration of the served run's arrivals")
     p.add_argument("--serve-pool", type=int, default=512, help="distinct windows the served requests draw from")
@@ -228,6 +229,52 @@ def run_served(args, local, backend):
         "requests": n_req, "request_status": counts, "rigs": rigs,
         "workload": "1 LM iteration + oldest-keyframe marginalization per request; windows as the batched configuration",
     }
+
+
+def run_configs(args, local, backend):
+    """The single-window configurations, each alone on the device: c1 (10 KF, 800
+    landmarks, 1 LM iteration + OLD marginalization), c2 (10 KF, 3000 landmarks,
+    IMU + prior + 24+1 calibration, 5 iterations + OLD) and c3 (30 KF, 8 cameras,
+    20 000 landmarks, 10 iterations + SECOND_NEW).  Device time of the solve and of
+    the marginalization (CUDA events, median of the repetitions), and the final
+    states against the FP64 oracle solving the same window on the host."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O  # checker of the per-configuration states
+
+    out = {}
+    for name, policy in (("c1", abi.MARGIN_OLD), ("c2", abi.MARGIN_OLD), ("c3", abi.MARGIN_SECOND_NEW)):
+        it = synth.ITERATIONS[name]
+        w = synth.make_windows(name, 1, seed=args.seed + 11)[0]
+        x0 = w.state_vector()
+        s = backend.Solver(device=local)
+        s.set_windows([w])
+        s.checkpoint()
+        solve_ms, marg_ms = [], []
+        victim = 0 if policy == abi.MARGIN_OLD else w.spec.keyframes - 2
+        for rep in range(4):
+            s.rollback()
+            s.solve(it)
+            s.synchronize()
+            if rep:
+                solve_ms.append(s.timing()[0])
+            s.marginalize([victim], policy)
+            s.read_prior(0)
+            if rep:
+                marg_ms.append(s.timing()[0])
+        s.read_states()
+        xg = w.state_vector()
+        s.close()
+        w.set_state_vector(x0)
+        O.lm_solve(w.window, it)
+        xc = w.state_vector()
+        solve_ms.sort()
+        marg_ms.sort()
+        out[name] = {"iterations": it, "landmarks": w.window.num_landmarks, "observations": w.window.num_observations,
+                     "solve_ms_p50": solve_ms[len(solve_ms) // 2], "solves_per_s": 1000.0 / solve_ms[len(solve_ms) // 2],
+                     "marginalization_ms_p50": marg_ms[len(marg_ms) // 2],
+                     "marginalization": "OLD" if policy == abi.MARGIN_OLD else "SECOND_NEW",
+                     "final_state_rel_err_vs_fp64_oracle": float(np.linalg.norm(xg - xc) / max(np.linalg.norm(xc - x0), 1e-300))}
+    return out
 
 
 def run_reference(args, world, rank):
@@ -399,6 +446,7 @@ def main():
                  "workload": "one configuration-2 window (10 KF, 3000 lm, 24+1 calib, prior) per solve"}
 
     served = run_served(args, local, backend) if rank == 0 and args.serve_rate > 0 else None
+    configs = run_configs(args, local, backend) if rank == 0 and not args.no_configs else None
 
     statuses = {}
     for r in reports:
@@ -443,7 +491,7 @@ def main():
             "clocks": clocks.summary(), "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
             "cpu_baseline": cpu_baseline, "plain_path": plain,
             "served_vs_plain": (value / world) / plain["windows_per_s"] if plain else None,
-            "served": served, "marginalization": marg,
+            "served": served, "marginalization": marg, "configs": configs,
             "batch_latency_ms": {"p50": sorted(dev_ms)[len(dev_ms) // 2], "p99": max(dev_ms)},
             "window_status": statuses, "wall_s": wall,
         }
