@@ -17,6 +17,7 @@ Ceres/Eigen build cannot be compiled offline).
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import importlib.util
 import json
 import os
@@ -67,6 +68,8 @@ def parse():
     p.add_argument("--serve-rate", type=float, default=5000.0, help="offered request rate of the served run (requests/s, 0: off)")
     p.add_argument("--serve-seconds", type=float, default=3.0, help="duration of the served run's arrivals")
     p.add_argument("--serve-pool", type=int, default=512, help="distinct windows the served requests draw from")
+    p.add_argument("--imu-rigs", type=int, default=512, help="rigs of the IMU preintegration batch, 11 keyframes each (0: off)")
+    p.add_argument("--imu-cpu-sample", type=int, default=1024, help="intervals preintegrated by the oracle for its CPU rate")
     return p.parse_args()
 
 
@@ -277,6 +280,66 @@ def run_configs(args, local, backend):
     return out
 
 
+def run_imu(args, local, backend):
+    """Batched IMU preintegration: the frozen IMU factor of every keyframe
+    interval of args.imu_rigs rigs x 11 keyframes (0.3 s apart, 200 Hz samples,
+    so ~62 integration steps per interval), one cgmli_imu_preintegrate call per
+    step with host buffers (samples in, frozen factors out).  The reference
+    preintegrates on the host, one factor at a time (ImuError::redoPreintegration);
+    its CPU rate is the FP64 oracle's on one thread over a sample of the intervals."""
+    s = synth.imu_stream(args.imu_rigs, 11, args.seed + 13)
+    prm = synth.imu_parameters()
+    call = lambda: backend.imu_preintegrate(prm, s.time_ns, s.readings, s.ranges, s.t0_ns, s.t1_ns, s.bias)
+    for _ in range(3):
+        call()
+    kernel_ms, wall_s = [], []
+    for _ in range(max(3, args.steps)):
+        t0 = time.perf_counter()
+        got = call()
+        wall_s.append(time.perf_counter() - t0)
+        kernel_ms.append(backend.imu_last_timing())
+    kernel_ms.sort()
+    wall_s.sort()
+    k_ms = kernel_ms[len(kernel_ms) // 2]
+    e_s = wall_s[len(wall_s) // 2]
+    # integration steps: sample pairs from the one holding t0 to the one holding t1
+    steps = 0
+    for (b, e), t0, t1 in zip(s.ranges, s.t0_ns, s.t1_ns):
+        ts = s.time_ns[b:e]
+        steps += int(np.searchsorted(ts, t1, side="left")) - int(np.searchsorted(ts, t0, side="right")) + 1
+    lo, hi = int(s.ranges[:, 0].min()), int(s.ranges[:, 1].max())
+    h2d = (hi - lo) * (8 + 48) + s.count * (8 + 8 + 8 + 48)
+    d2h = s.count * (C.sizeof(abi.FrozenImu) + 4)
+    out = {"intervals": s.count, "steps": steps, "kernel_ms_p50": k_ms, "intervals_per_s": s.count / (k_ms / 1e3),
+           "ns_per_step": k_ms * 1e6 / steps,
+           "e2e": {"value": s.count / e_s, "unit": "intervals/s", "ms_p50": e_s * 1e3, "h2d_bytes_per_step": h2d,
+                   "d2h_bytes_per_step": d2h},
+           "fp64_gflops_covariance": 4320.0 * steps / (k_ms / 1e3) / 1e9,
+           "workload": f"{args.imu_rigs} rigs x 11 keyframes, 0.3 s intervals at 200 Hz"}
+    if args.imu_cpu_sample > 0:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle as O  # cpu_baseline leg and checker of the device factors
+
+        n = min(args.imu_cpu_sample, s.count)
+        t0 = time.perf_counter()
+        st, ref = O.imu_preintegrate(prm, s.time_ns, s.readings, s.ranges[:n], s.t0_ns[:n], s.t1_ns[:n], s.bias[:n])
+        cpu_s = time.perf_counter() - t0
+        worst = {"deltas_jacobians": 0.0, "information": 0.0}
+        for i in range(n):
+            for name in ("delta_quaternion", "delta_velocity", "delta_position", "rotation_gyro", "velocity_gyro",
+                         "position_gyro", "velocity_accel", "position_accel"):
+                a, b = np.array(getattr(got[i], name)), np.array(getattr(ref[i], name))
+                worst["deltas_jacobians"] = max(worst["deltas_jacobians"], float(np.linalg.norm(a - b) / np.linalg.norm(b)))
+            Wg = np.array(got[i].whitening).reshape(15, 15, order="F")
+            Wr = np.array(ref[i].whitening).reshape(15, 15, order="F")
+            Ig, Ir = Wg.T @ Wg, Wr.T @ Wr
+            worst["information"] = max(worst["information"], float(np.linalg.norm(Ig - Ir) / np.linalg.norm(Ir)))
+        out["cpu_baseline"] = {"value": n / cpu_s, "unit": "intervals/s", "cores": 1, "kind": "port",
+                               "sample": f"first {n} intervals, FP64 oracle (four dP/dsigma propagations, dense 15x15)"}
+        out["rel_err_vs_fp64_oracle_max"] = worst
+    return out
+
+
 def run_reference(args, world, rank):
     """CPU path of the reference algorithm on the host cores (FP64 oracle)."""
     if rank != 0:
@@ -447,6 +510,7 @@ def main():
 
     served = run_served(args, local, backend) if rank == 0 and args.serve_rate > 0 else None
     configs = run_configs(args, local, backend) if rank == 0 and not args.no_configs else None
+    imu = run_imu(args, local, backend) if rank == 0 and args.imu_rigs > 0 else None
 
     statuses = {}
     for r in reports:
@@ -491,7 +555,7 @@ def main():
             "clocks": clocks.summary(), "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
             "cpu_baseline": cpu_baseline, "plain_path": plain,
             "served_vs_plain": (value / world) / plain["windows_per_s"] if plain else None,
-            "served": served, "marginalization": marg, "configs": configs,
+            "served": served, "marginalization": marg, "configs": configs, "imu_preintegration": imu,
             "batch_latency_ms": {"p50": sorted(dev_ms)[len(dev_ms) // 2], "p99": max(dev_ms)},
             "window_status": statuses, "wall_s": wall,
         }

@@ -21,6 +21,8 @@ PRECISION_MIXED = 1
 PRIOR_POSE, PRIOR_SPEED_BIAS, PRIOR_EXTRINSIC, PRIOR_TIME_OFFSET = 0, 1, 2, 3
 MARGIN_OLD, MARGIN_SECOND_NEW = 0, 1
 MARG_EIGEN_NOALLOC_MAX_N = 256  # CGMLI_MARG_EIGEN_NOALLOC_MAX_N
+E_INVALID = 1
+E_NONFINITE = 2
 E_PENDING = 11
 
 
@@ -33,6 +35,14 @@ class FrozenImu(C.Structure):
         ("rotation_gyro", C.c_double * 9), ("velocity_gyro", C.c_double * 9), ("position_gyro", C.c_double * 9),
         ("velocity_accel", C.c_double * 9), ("position_accel", C.c_double * 9),
         ("whitening", C.c_double * 225),
+    ]
+
+
+class ImuParameters(C.Structure):
+    _fields_ = [
+        ("sigma_g_c", C.c_double), ("sigma_a_c", C.c_double), ("sigma_gw_c", C.c_double), ("sigma_aw_c", C.c_double),
+        ("g_max", C.c_double), ("a_max", C.c_double), ("g", C.c_double), ("max_sample_gap", C.c_double),
+        ("sensor_position", C.c_double * 3), ("sensor_quaternion", C.c_double * 4),
     ]
 
 
@@ -129,6 +139,10 @@ def declare_backend(lib: C.CDLL) -> C.CDLL:
     _proto(lib, "cgmli_server_release", C.c_int, [V, C.c_longlong])
     _proto(lib, "cgmli_server_replay", C.c_int,
            [V, C.POINTER(W), c_int_p, c_double_p, C.c_int, c_double_p, c_int_p, c_double_p])
+    _proto(lib, "cgmli_imu_preintegrate", C.c_int,
+           [C.POINTER(ImuParameters), ll_p, c_double_p, C.c_int, c_int_p, ll_p, ll_p, c_double_p, C.c_int,
+            C.POINTER(FrozenImu)])
+    _proto(lib, "cgmli_imu_last_timing", C.c_int, [c_double_p])
     return lib
 
 
@@ -150,7 +164,8 @@ BACKEND_SYMBOLS = [
     "cgmli_solver_read_prior", "cgmli_marg_eigen", "cgmli_marg_psd_solve", "cgmli_marg_subtract",
     "cgmli_solver_checkpoint", "cgmli_solver_rollback", "cgmli_solver_kernel_times", "cgmli_topology_check",
     "cgmli_marg_eigen_noalloc", "cgmli_server_create", "cgmli_server_destroy", "cgmli_server_submit", "cgmli_server_poll",
-    "cgmli_server_read_prior", "cgmli_server_release", "cgmli_server_replay",
+    "cgmli_server_read_prior", "cgmli_server_release", "cgmli_server_replay", "cgmli_imu_preintegrate",
+    "cgmli_imu_last_timing",
 ]
 KERNEL_NAMES = ["zero_acc", "linearize", "retained", "factor", "candidate", "backsub_trial", "retained_trial", "lm_update", "accept",
                 "lin_pairs", "lin_schur"]

@@ -182,6 +182,35 @@ def marg_subtract(coupling: np.ndarray, solution: np.ndarray, H: np.ndarray, g: 
     return Ho, go
 
 
+def imu_preintegrate(params: abi.ImuParameters, time_ns: np.ndarray, readings: np.ndarray, ranges: np.ndarray,
+                     t0_ns: np.ndarray, t1_ns: np.ndarray, bias: np.ndarray):
+    """Frozen IMU factors of len(t0_ns) intervals on the device (cgmli_imu_preintegrate).
+
+    time_ns: int64 sample times; readings: (samples, 6) [gyro, accelerometer];
+    ranges: (count, 2) sample index ranges [begin, end); bias: (count, 6) [b_g, b_a].
+    Returns a ctypes array of abi.FrozenImu."""
+    ll = C.POINTER(C.c_longlong)
+    time_ns = np.ascontiguousarray(time_ns, dtype=np.int64)
+    readings = np.ascontiguousarray(readings, dtype=np.float64)
+    ranges = np.ascontiguousarray(ranges, dtype=np.int32)
+    t0_ns = np.ascontiguousarray(t0_ns, dtype=np.int64)
+    t1_ns = np.ascontiguousarray(t1_ns, dtype=np.int64)
+    bias = np.ascontiguousarray(bias, dtype=np.float64)
+    count = len(t0_ns)
+    out = (abi.FrozenImu * max(count, 1))()
+    _check(lib().cgmli_imu_preintegrate(C.byref(params), time_ns.ctypes.data_as(ll), _p(readings), len(time_ns),
+                                        ranges.ctypes.data_as(abi.c_int_p), t0_ns.ctypes.data_as(ll), t1_ns.ctypes.data_as(ll),
+                                        _p(bias), count, out), "cgmli_imu_preintegrate")
+    return out
+
+
+def imu_last_timing() -> float:
+    """Kernel milliseconds of the last imu_preintegrate call."""
+    ms = C.c_double()
+    _check(lib().cgmli_imu_last_timing(C.byref(ms)), "cgmli_imu_last_timing")
+    return ms.value
+
+
 def _window_array(windows):
     arr = (abi.Window * len(windows))()
     for i, w in enumerate(windows):

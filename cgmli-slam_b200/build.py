@@ -20,7 +20,7 @@ LIB = PKG / "lib"
 INCLUDE = ROOT / "include"
 
 BACKEND_SOURCES = [PKG / "csrc" / "backend_kernels.cu", PKG / "csrc" / "marginal_kernels.cu", PKG / "csrc" / "backend_host.cu",
-                   PKG / "csrc" / "topology.cpp", PKG / "csrc" / "noalloc_eigen.cu",
+                   PKG / "csrc" / "topology.cpp", PKG / "csrc" / "noalloc_eigen.cu", PKG / "csrc" / "imu_preintegration.cu",
                    PKG / "csrc" / "server.cpp"]
 BACKEND_HEADERS = [PKG / "csrc" / "device_math.cuh", PKG / "csrc" / "factor_eval.cuh", PKG / "csrc" / "backend_internal.h",
                    PKG / "csrc" / "dense_tiles.cuh",

@@ -173,3 +173,85 @@ def window_array(windows: list[SynthWindow]):
     for i, w in enumerate(windows):
         arr[i] = w.window
     return arr
+
+
+# ---- IMU streams for preintegration ------------------------------------------------
+# Noise densities and saturation of the benchmark rig's IMU (sigma_g 1.7e-4,
+# sigma_a 2e-3, random walks 2e-5 / 3e-3, 200 Hz).
+IMU_DEFAULTS = dict(sigma_g_c=1.7e-4, sigma_a_c=2e-3, sigma_gw_c=2e-5, sigma_aw_c=3e-3, g_max=7.8, a_max=176.0, g=9.81,
+                    max_sample_gap=0.05)
+
+
+def imu_parameters(sensor_position=(0.0, 0.0, 0.0), sensor_quaternion=(0.0, 0.0, 0.0, 1.0), **overrides) -> abi.ImuParameters:
+    p = abi.ImuParameters()
+    for k, v in {**IMU_DEFAULTS, **overrides}.items():
+        setattr(p, k, float(v))
+    p.sensor_position[:] = list(sensor_position)
+    p.sensor_quaternion[:] = list(sensor_quaternion)
+    return p
+
+
+@dataclass
+class ImuStream:
+    """Samples of one or more rigs and the keyframe intervals to preintegrate."""
+    time_ns: np.ndarray   # (S,) int64, increasing within each rig
+    readings: np.ndarray  # (S, 6) gyro, accelerometer
+    ranges: np.ndarray    # (N, 2) sample range [begin, end) of each interval
+    t0_ns: np.ndarray     # (N,) int64
+    t1_ns: np.ndarray     # (N,) int64
+    bias: np.ndarray      # (N, 6) linearization bias [b_g, b_a]
+
+    @property
+    def count(self) -> int:
+        return len(self.t0_ns)
+
+
+def imu_stream(rigs: int, keyframes: int, seed: int, rate: float = 200.0, spacing_s: float = 0.3,
+               on_sample: bool = False) -> ImuStream:
+    """Seeded IMU readings of ``rigs`` independent rigs, each with ``keyframes``
+    keyframes ``spacing_s`` apart, and the keyframes-1 intervals of each rig.
+
+    Readings follow a smooth random motion (gyro up to ~0.6 rad/s, specific
+    force around gravity) with constant-plus-random-walk biases and white noise
+    at the rig's densities.  Keyframe times fall between samples (the first and
+    last step of every interval interpolate) unless ``on_sample``."""
+    rng = np.random.default_rng(seed)
+    h_ns = int(round(1e9 / rate))
+    span = spacing_s * (keyframes - 1) + 0.1
+    per_rig = int(np.ceil(span * rate)) + 4
+    times, reads, ranges, t0s, t1s, biases = [], [], [], [], [], []
+    offset = 0
+    for rig in range(rigs):
+        start_ns = int(1_000_000_000 * (1 + rig)) + int(rng.integers(0, h_ns))
+        t_ns = start_ns + h_ns * np.arange(per_rig, dtype=np.int64)
+        t = (t_ns - start_ns) * 1e-9
+        freq = rng.uniform(0.5, 2.0, size=(2, 3))
+        phase = rng.uniform(0, 2 * np.pi, size=(2, 3))
+        amp_w = rng.uniform(0.1, 0.6, size=3)
+        amp_a = rng.uniform(0.3, 2.0, size=3)
+        bg = 2e-3 * rng.standard_normal(3) + np.cumsum(2e-5 * np.sqrt(1 / rate) * rng.standard_normal((per_rig, 3)), axis=0)
+        ba = 2e-2 * rng.standard_normal(3) + np.cumsum(3e-3 * np.sqrt(1 / rate) * rng.standard_normal((per_rig, 3)), axis=0)
+        gyro = amp_w * np.sin(freq[0] * t[:, None] * 2 * np.pi + phase[0]) + bg
+        gyro += 1.7e-4 * np.sqrt(rate) * rng.standard_normal((per_rig, 3))
+        acc = amp_a * np.sin(freq[1] * t[:, None] * 2 * np.pi + phase[1]) + np.array([0.0, 0.0, 9.81]) + ba
+        acc += 2e-3 * np.sqrt(rate) * rng.standard_normal((per_rig, 3))
+        times.append(t_ns)
+        reads.append(np.hstack([gyro, acc]))
+        kf = start_ns + int(0.05e9) + np.round(np.arange(keyframes) * spacing_s * 1e9).astype(np.int64)
+        if on_sample:
+            kf = start_ns + h_ns * np.round((kf - start_ns) / h_ns).astype(np.int64)
+        else:
+            kf = kf + rng.integers(1, h_ns - 1, size=keyframes)
+        for k in range(keyframes - 1):
+            a, b = int(kf[k]), int(kf[k + 1])
+            lo = max(int(np.searchsorted(t_ns, a, side="right")) - 2, 0)
+            hi = min(int(np.searchsorted(t_ns, b, side="left")) + 2, per_rig)
+            ranges.append((offset + lo, offset + hi))
+            t0s.append(a)
+            t1s.append(b)
+            i = int(np.searchsorted(t_ns, a))
+            biases.append(np.concatenate([bg[i], ba[i]]) + np.concatenate([1e-4 * rng.standard_normal(3),
+                                                                            5e-3 * rng.standard_normal(3)]))
+        offset += per_rig
+    return ImuStream(np.concatenate(times), np.vstack(reads), np.array(ranges, dtype=np.int32), np.array(t0s, dtype=np.int64),
+                     np.array(t1s, dtype=np.int64), np.array(biases))

@@ -246,6 +246,44 @@ int cgmli_marg_subtract(const double *coupling, const double *solution, int elim
 #define CGMLI_MARG_EIGEN_NOALLOC_MAX_N 256
 int cgmli_marg_eigen_noalloc(const double *H, int n, double *eigenvalues, double *eigenvectors, void *stream);
 
+/* ---- IMU preintegration ------------------------------------------------------
+ * Batched construction of frozen IMU factors, the device form of what the
+ * reference does on the host per factor when it builds or refreshes a
+ * BodyImuCost (src/factor/BodyImuFactor.cpp:136-166, called on bias drift by
+ * src/backend/FixedLagBackend.cpp:395-411):
+ *   - the sample checks of validImuInterval (src/factor/BodyImuFactor.cpp:10-28);
+ *   - ImuError::redoPreintegration (src/factor/ImuError.cpp:254-462) at the
+ *     interval's linearization bias: rotation, velocity and position deltas,
+ *     their bias Jacobians, the noise covariance propagated through the 15x15
+ *     transition, and the whitening W = diag(1/sqrt(lambda)) U^T of
+ *     PseudoInverse::symmSqrtU (src/factor/PseudoInverse.hpp:117-145);
+ *   - the gyro readings at both ends (gyroAt, src/factor/BodyImuFactor.cpp:29-38)
+ *     and the sensor pose T_BS.
+ * Times are integer nanoseconds, as the reference's cgmli::Time; a difference
+ * converts to seconds as Duration::toSec does (whole seconds + 1e-9 * nsec). */
+typedef struct cgmli_imu_parameters {
+    double sigma_g_c, sigma_a_c;     /* gyro / accelerometer noise densities */
+    double sigma_gw_c, sigma_aw_c;   /* gyro / accelerometer bias random-walk densities */
+    double g_max, a_max;             /* saturation: a reading above it inflates that noise */
+    double g;                        /* gravity magnitude, copied to frozen.gravity */
+    double max_sample_gap;           /* seconds; a longer gap inside an interval is invalid */
+    double sensor_position[3], sensor_quaternion[4]; /* T_BS, quaternion [x, y, z, w] */
+} cgmli_imu_parameters;
+
+/* Preintegrates count intervals.  Sample j has time sample_time_ns[j] and
+ * readings sample_readings[6j..6j+5] = [gyro (rad/s), accelerometer (m/s^2)].
+ * Interval i integrates the samples [range[2i], range[2i+1]) (strictly
+ * increasing times, first <= t0_ns[i] < t1_ns[i] <= last; ranges may overlap)
+ * at the bias bias[6i..6i+5] = [b_g, b_a] and writes every field of frozen[i].
+ * CGMLI_E_INVALID names the first malformed interval in cgmli_last_error();
+ * CGMLI_E_NONFINITE reports an interval whose result is not finite. */
+int cgmli_imu_preintegrate(const cgmli_imu_parameters *params, const long long *sample_time_ns, const double *sample_readings,
+                           int num_samples, const int *range, const long long *t0_ns, const long long *t1_ns,
+                           const double *bias, int count, cgmli_frozen_imu *frozen);
+/* Device time (CUDA events around the kernel) of the last successful
+ * cgmli_imu_preintegrate call in this process. */
+int cgmli_imu_last_timing(double *kernel_ms);
+
 /* ---- Served mode: continuous batching of window solves ---------------------
  * Windows from many rigs arrive as independent requests.  A request is one
  * window (its arrays are the caller's and must stay valid and unmodified until

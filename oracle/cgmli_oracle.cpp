@@ -17,6 +17,9 @@
 //                                           src/backend/VisualCudaBatch.cu:291-340
 //   * marginalization                       src/backend/Marginalizer.cpp:240-474,
 //                                           src/backend/SlidingWindowManager.cpp:627-652
+//   * IMU preintegration                    src/factor/ImuError.cpp:254-462,
+//                                           src/factor/BodyImuFactor.cpp:10-38,136-166,
+//                                           src/factor/PseudoInverse.hpp:117-145
 // Parity is pinned by the reference's own known-answer tests
 // (src/backend/tests/ManagedWindowRegression.cpp:119-329), restated in tests/.
 #include "../include/cgmli_backend.h"
@@ -591,6 +594,244 @@ static bool imuFactor(const cgmli_frozen_imu& imu, const double* p0, const doubl
                 J[30 * i + col0[k] + j] = v;
             }
     }
+    return true;
+}
+
+// ---- IMU preintegration ------------------------------------------------------
+// Duration::toSec (src/utils/Duration.h:62-64) of a signed nanosecond count:
+// whole seconds (floor) plus 1e-9 * the non-negative remainder.
+static double nsToSec(long long ns) {
+    long long sec = ns / 1000000000LL, rem = ns % 1000000000LL;
+    if (rem < 0) { rem += 1000000000LL; sec -= 1; }
+    return (double)sec + 1e-9 * (double)rem;
+}
+// ode::sinc (src/factor/ode.hpp:15-27)
+static double odeSinc(double x) {
+    if (std::fabs(x) > 1e-6) return std::sin(x) / x;
+    const double x2 = x * x, x4 = x2 * x2, x6 = x2 * x2 * x2;
+    return 1.0 - x2 / 6.0 + x4 / 120.0 - x6 / 5040.0;
+}
+// kinematics::rightJacobian (src/kinematics/Transformation.hpp:47-62)
+static M3 rightJacobianSO3(const V3& phi) {
+    const double a = nrm(phi);
+    const M3 W = skew(phi), W2 = mul(W, W);
+    if (a < 1e-4) return madd(eye(), madd(mscl(-0.5, W), mscl(1.0 / 6.0, W2)));
+    return madd(eye(), madd(mscl(-(1.0 - std::cos(a)) / (a * a), W), mscl((a - std::sin(a)) / (a * a * a), W2)));
+}
+// validImuInterval (src/factor/BodyImuFactor.cpp:10-28) over samples [0, n)
+static bool imuIntervalValid(const long long* t, const double* m, int n, long long t0, long long t1, double maxGap) {
+    if (!std::isfinite(maxGap) || maxGap <= 0) return false;
+    if (n < 2 || t1 <= t0 || t[0] > t0 || t[n - 1] < t1) return false;
+    for (int i = 0; i < n; ++i) {
+        for (int k = 0; k < 6; ++k) if (!fin(m[6 * i + k])) return false;
+        if (i && t[i] <= t[i - 1]) return false;
+        if (i && t[i - 1] < t1 && t[i] > t0 && nsToSec(t[i] - t[i - 1]) > maxGap + 1e-9) return false;
+    }
+    return true;
+}
+// gyroAt (src/factor/BodyImuFactor.cpp:29-38): gyro reading interpolated at time e
+static V3 gyroReadingAt(const long long* t, const double* m, int n, long long e) {
+    int k = 0;
+    while (k < n && t[k] < e) ++k;  // first sample not before e
+    if (k == 0) return ld3(m);
+    if (k == n) return ld3(m + 6 * (n - 1));
+    const double alpha = nsToSec(e - t[k - 1]) / nsToSec(t[k] - t[k - 1]);
+    return add(scl(1 - alpha, ld3(m + 6 * (k - 1))), scl(alpha, ld3(m + 6 * k)));
+}
+// Cyclic Jacobi with a relative skip test |a_pq| <= 1e-14 sqrt(a_pp a_qq), so
+// that a graded positive definite matrix (the IMU covariance spans ~12 decades)
+// keeps its small eigenvalues and their eigenvectors accurate relative to
+// themselves; sweeps until one applies no rotation.  Row-major in, eigenvalues
+// ascending, eigenvectors as columns of V.
+static bool jacobiGraded(int n, const double* Ain, double* evals, double* V) {
+    std::vector<double> A(Ain, Ain + (size_t)n * n);
+    for (int i = 0; i < n; ++i) for (int j = 0; j < n; ++j) V[(size_t)i * n + j] = i == j;
+    for (int sweep = 0; sweep < 40; ++sweep) {
+        bool rotated = false;
+        for (int p = 0; p < n - 1; ++p)
+            for (int q = p + 1; q < n; ++q) {
+                const double apq = A[(size_t)p * n + q];
+                const double app = A[(size_t)p * n + p], aqq = A[(size_t)q * n + q];
+                if (apq == 0 || std::fabs(apq) <= 1e-14 * std::sqrt(std::fabs(app * aqq))) continue;
+                rotated = true;
+                const double tau = (aqq - app) / (2 * apq);
+                const double t = (tau >= 0 ? 1.0 : -1.0) / (std::fabs(tau) + std::sqrt(1 + tau * tau));
+                const double c = 1 / std::sqrt(1 + t * t), s = t * c;
+                for (int k = 0; k < n; ++k) {
+                    const double akp = A[(size_t)k * n + p], akq = A[(size_t)k * n + q];
+                    A[(size_t)k * n + p] = c * akp - s * akq;
+                    A[(size_t)k * n + q] = s * akp + c * akq;
+                    const double vkp = V[(size_t)k * n + p], vkq = V[(size_t)k * n + q];
+                    V[(size_t)k * n + p] = c * vkp - s * vkq;
+                    V[(size_t)k * n + q] = s * vkp + c * vkq;
+                }
+                for (int k = 0; k < n; ++k) {
+                    const double apk = A[(size_t)p * n + k], aqk = A[(size_t)q * n + k];
+                    A[(size_t)p * n + k] = c * apk - s * aqk;
+                    A[(size_t)q * n + k] = s * apk + c * aqk;
+                }
+            }
+        if (!rotated) break;
+    }
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return A[(size_t)x * n + x] < A[(size_t)y * n + y]; });
+    std::vector<double> Vs((size_t)n * n);
+    for (int j = 0; j < n; ++j) {
+        evals[j] = A[(size_t)order[j] * n + order[j]];
+        for (int i = 0; i < n; ++i) Vs[(size_t)i * n + j] = V[(size_t)i * n + order[j]];
+    }
+    std::copy(Vs.begin(), Vs.end(), V);
+    for (int i = 0; i < n; ++i) if (!fin(evals[i])) return false;
+    return true;
+}
+// 15x15 row-major helpers
+static void mat15Mul(const double* A, const double* B, double* C) {
+    for (int r = 0; r < 15; ++r)
+        for (int c = 0; c < 15; ++c) {
+            double s = 0;
+            for (int k = 0; k < 15; ++k) s += A[15 * r + k] * B[15 * k + c];
+            C[15 * r + c] = s;
+        }
+}
+static void setBlock15(double* F, int r0, int c0, const M3& b) {
+    for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) F[15 * (r0 + i) + c0 + j] = b[3 * i + j];
+}
+// ImuError::redoPreintegration (src/factor/ImuError.cpp:254-462) over samples
+// [0, n) from t0 to t1 at bias [b_g, b_a], with the four covariance
+// derivatives dP/dsigma^2 propagated separately and summed at the end as the
+// reference does, then PseudoInverse::symmSqrtU (src/factor/PseudoInverse.hpp:117-145).
+static bool preintegrateInterval(const cgmli_imu_parameters& prm, const long long* ts, const double* m, int n, long long t0,
+                                 long long t1, const double* bias, cgmli_frozen_imu& out, double* covariance) {
+    Q Dq{0, 0, 0, 1};
+    M3 Cint{}, Cdint{}, crossAcc{}, dAlphaDbg{}, dVelDbg{}, dPosDbg{};
+    V3 accInt{0, 0, 0}, accDint{0, 0, 0};
+    std::vector<double> dPdSigma(4 * 225, 0.0);
+    const V3 bg = ld3(bias), ba = ld3(bias + 3);
+    long long time = t0;
+    bool started = false;
+    int steps = 0;
+    for (int it = 0; it + 1 < n; ++it) {
+        V3 w0 = ld3(m + 6 * it), a0 = ld3(m + 6 * it + 3), w1 = ld3(m + 6 * it + 6), a1 = ld3(m + 6 * it + 9);
+        long long next = ts[it + 1];
+        double dt = nsToSec(next - time);
+        if (t1 < next) {  // the interval ends inside this sample pair: interpolate its end
+            const double interval = nsToSec(next - ts[it]);
+            next = t1;
+            dt = nsToSec(next - time);
+            const double r = dt / interval;
+            w1 = add(scl(1.0 - r, w0), scl(r, w1));
+            a1 = add(scl(1.0 - r, a0), scl(r, a1));
+        }
+        if (dt <= 0.0) continue;
+        if (!started) {  // first pair: move its start reading to t0
+            started = true;
+            const double r = dt / nsToSec(next - ts[it]);
+            w0 = add(scl(r, w0), scl(1.0 - r, w1));
+            a0 = add(scl(r, a0), scl(1.0 - r, a1));
+        }
+        double gyroSat = 1.0, accSat = 1.0;
+        for (int k = 0; k < 3; ++k) {
+            if (std::fabs(w0[k]) > prm.g_max || std::fabs(w1[k]) > prm.g_max) gyroSat = 100.0;
+            if (std::fabs(a0[k]) > prm.a_max || std::fabs(a1[k]) > prm.a_max) accSat = 100.0;
+        }
+        // orientation increment
+        const V3 omega = sub(scl(0.5, add(w0, w1)), bg);
+        const double halfAngle = nrm(omega) * 0.5 * dt;
+        const double sincHalf = odeSinc(halfAngle);
+        const Q dq{sincHalf * omega[0] * 0.5 * dt, sincHalf * omega[1] * 0.5 * dt, sincHalf * omega[2] * 0.5 * dt, std::cos(halfAngle)};
+        const Q Dq1 = qmul(Dq, dq);
+        const M3 C = qrot(Dq), C1 = qrot(Dq1), CC = madd(C, C1);
+        const V3 acc = sub(scl(0.5, add(a0, a1)), ba);
+        // rotation integrals
+        const M3 Cint1 = madd(Cint, mscl(dt, mscl(0.5, CC)));
+        const V3 accInt1 = add(accInt, scl(dt, mv(mscl(0.5, CC), acc)));
+        Cdint = madd(Cdint, madd(mscl(dt, Cint), mscl(dt * dt, mscl(0.25, CC))));
+        accDint = add(accDint, add(scl(dt, accInt), scl(dt * dt, mv(mscl(0.25, CC), acc))));
+        // bias Jacobians
+        const M3 Jr = rightJacobianSO3(scl(dt, omega));
+        dAlphaDbg = madd(dAlphaDbg, mscl(dt, mul(C1, Jr)));
+        const Q dqInv{-dq.x, -dq.y, -dq.z, dq.w};
+        const M3 cross1 = madd(mul(qrot(dqInv), crossAcc), mscl(dt, Jr));
+        const M3 ax = skew(acc);
+        const M3 both = madd(mul(mul(C, ax), crossAcc), mul(mul(C1, ax), cross1));
+        const M3 dVel1 = madd(dVelDbg, mscl(0.5 * dt, both));
+        dPosDbg = madd(dPosDbg, madd(mscl(dt, dVelDbg), mscl(0.25 * dt * dt, both)));
+        // transition of the 15-dimensional increment error
+        double F[225];
+        for (int i = 0; i < 225; ++i) F[i] = (i / 15 == i % 15) ? 1.0 : 0.0;
+        setBlock15(F, 0, 3, mscl(-1.0, skew(add(scl(dt, accInt), scl(dt * dt, mv(mscl(0.25, CC), acc))))));
+        setBlock15(F, 0, 6, mscl(dt, eye()));
+        setBlock15(F, 0, 9, madd(mscl(dt, dVelDbg), mscl(0.25 * dt * dt, both)));
+        setBlock15(F, 0, 12, madd(mscl(-dt, Cint), mscl(dt * dt, mscl(0.25, CC))));
+        setBlock15(F, 3, 9, mscl(-dt, C1));
+        setBlock15(F, 6, 3, mscl(-1.0, skew(scl(dt, mv(mscl(0.5, CC), acc)))));
+        setBlock15(F, 6, 9, mscl(0.5 * dt, both));
+        setBlock15(F, 6, 12, mscl(-dt, mscl(0.5, CC)));
+        double Ft[225];
+        for (int r = 0; r < 15; ++r) for (int c = 0; c < 15; ++c) Ft[15 * c + r] = F[15 * r + c];
+        // noise of each sigma^2 (K0 .. K3)
+        double noise[4][15] = {};
+        for (int i = 3; i < 6; ++i) noise[0][i] = gyroSat * dt;
+        for (int i = 0; i < 3; ++i) noise[1][i] = 0.5 * dt * dt * dt * accSat * accSat * accSat;
+        for (int i = 6; i < 9; ++i) noise[1][i] = accSat * dt;
+        for (int i = 9; i < 12; ++i) noise[2][i] = dt;
+        for (int i = 12; i < 15; ++i) noise[3][i] = dt;
+        for (int j = 0; j < 4; ++j) {
+            double T[225];
+            double* D = &dPdSigma[225 * j];
+            mat15Mul(F, D, T);
+            mat15Mul(T, Ft, D);
+            for (int i = 0; i < 15; ++i) D[16 * i] += noise[j][i];
+        }
+        Dq = Dq1; Cint = Cint1; accInt = accInt1; crossAcc = cross1; dVelDbg = dVel1;
+        time = next;
+        ++steps;
+        if (next == t1) break;
+    }
+    if (steps <= 0) return false;
+    // symmetrize each derivative, weight by the noise densities
+    const double s2[4] = {prm.sigma_g_c * prm.sigma_g_c, prm.sigma_a_c * prm.sigma_a_c, prm.sigma_gw_c * prm.sigma_gw_c,
+                          prm.sigma_aw_c * prm.sigma_aw_c};
+    double P[225] = {};
+    for (int j = 0; j < 4; ++j)
+        for (int r = 0; r < 15; ++r)
+            for (int c = 0; c < 15; ++c)
+                P[15 * r + c] += (0.5 * dPdSigma[225 * j + 15 * r + c] + 0.5 * dPdSigma[225 * j + 15 * c + r]) * s2[j];
+    if (covariance) std::copy(P, P + 225, covariance);
+    // W = diag(sqrt(1/lambda)) U^T with eigenvalues at or below the tolerance raised to it.
+    // The reference's Eigen::SelfAdjointEigenSolver is accurate to eps * lambda_max in
+    // every eigenvalue; the graded Jacobi is accurate relative to each one.
+    double lam[15], U[225];
+    if (!jacobiGraded(15, P, lam, U)) return false;
+    const double eps = std::numeric_limits<double>::epsilon();
+    double lmax = lam[0];
+    for (int i = 1; i < 15; ++i) lmax = std::max(lmax, lam[i]);
+    const double tol = std::max(eps, eps * 15 * lmax);
+    for (int r = 0; r < 15; ++r) {
+        const double s = std::sqrt(lam[r] > tol ? 1.0 / lam[r] : 1.0 / tol);
+        for (int c = 0; c < 15; ++c) out.whitening[r + 15 * c] = s * U[15 * c + r];
+    }
+    auto toColumnMajor = [](const M3& a, double* dst) {
+        for (int r = 0; r < 3; ++r) for (int c = 0; c < 3; ++c) dst[r + 3 * c] = a[3 * r + c];
+    };
+    out.delta_quaternion[0] = Dq.x; out.delta_quaternion[1] = Dq.y; out.delta_quaternion[2] = Dq.z; out.delta_quaternion[3] = Dq.w;
+    for (int i = 0; i < 3; ++i) { out.delta_velocity[i] = accInt[i]; out.delta_position[i] = accDint[i]; }
+    for (int i = 0; i < 6; ++i) out.reference_bias[i] = bias[i];
+    toColumnMajor(dAlphaDbg, out.rotation_gyro);
+    toColumnMajor(dVelDbg, out.velocity_gyro);
+    toColumnMajor(dPosDbg, out.position_gyro);
+    toColumnMajor(Cint, out.velocity_accel);
+    toColumnMajor(Cdint, out.position_accel);
+    out.duration = nsToSec(t1 - t0);
+    out.gravity = prm.g;
+    for (int i = 0; i < 3; ++i) out.sensor_position[i] = prm.sensor_position[i];
+    for (int i = 0; i < 4; ++i) out.sensor_quaternion[i] = prm.sensor_quaternion[i];
+    const V3 g0 = gyroReadingAt(ts, m, n, t0), g1 = gyroReadingAt(ts, m, n, t1);
+    for (int i = 0; i < 3; ++i) { out.gyros[i] = g0[i]; out.gyros[3 + i] = g1[i]; }
+    const double* all = &out.duration;
+    for (size_t i = 0; i < sizeof(cgmli_frozen_imu) / sizeof(double); ++i)
+        if (!fin(all[i])) return false;
     return true;
 }
 
@@ -1376,6 +1617,23 @@ static void marginalizeWindow(const cgmli_window& w, int victim, int policy, Win
 extern "C" {
 
 int oracle_version(void) { return 1; }
+
+// Batched IMU preintegration with the semantics of cgmli_imu_preintegrate
+// (status 0, CGMLI_E_INVALID for a malformed interval, CGMLI_E_NONFINITE).
+int oracle_imu_preintegrate(const cgmli_imu_parameters* prm, const long long* time_ns, const double* readings, int num_samples,
+                            const int* range, const long long* t0, const long long* t1, const double* bias, int count,
+                            cgmli_frozen_imu* frozen, double* covariance /* count x 225 row-major, or NULL */) {
+    for (int i = 0; i < count; ++i) {
+        const int b = range[2 * i], e = range[2 * i + 1];
+        if (b < 0 || e > num_samples || e - b < 2) return CGMLI_E_INVALID;
+        if (!orc::imuIntervalValid(time_ns + b, readings + 6 * (size_t)b, e - b, t0[i], t1[i], prm->max_sample_gap))
+            return CGMLI_E_INVALID;
+        if (!orc::preintegrateInterval(*prm, time_ns + b, readings + 6 * (size_t)b, e - b, t0[i], t1[i], bias + 6 * i, frozen[i],
+                                       covariance ? covariance + 225 * (size_t)i : nullptr))
+            return CGMLI_E_NONFINITE;
+    }
+    return CGMLI_OK;
+}
 
 // Per-factor residual and tangent Jacobians (unweighted).  J: 2 x 26 row-major
 // columns [anchor pose 6 | observer pose 6 | ext_a 6 | ext_b 6 | td | rho].

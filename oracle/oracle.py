@@ -61,6 +61,9 @@ def lib() -> C.CDLL:
           [C.c_int, dp, dp, C.c_int, ip, ip, ip, dp, dp, dp, dp, dp])
         P(L, "oracle_marginalize_window", C.c_int,
           [W, C.c_int, C.c_int, ip, ip, ip, ip, ip, dp, dp, dp, dp, dp, dp])
+        ll = C.POINTER(C.c_longlong)
+        P(L, "oracle_imu_preintegrate", C.c_int,
+          [C.POINTER(abi.ImuParameters), ll, dp, C.c_int, ip, ll, ll, dp, C.c_int, C.POINTER(abi.FrozenImu), dp])
         _LIB = L
     return _LIB
 
@@ -164,3 +167,22 @@ def lm_solve_batch(windows_array, count, iterations, threads):
     reps = (abi.SolveReport * count)()
     st = lib().oracle_lm_solve_batch(windows_array, count, iterations, threads, reps)
     return st, reps
+
+
+def imu_preintegrate(params, time_ns, readings, ranges, t0_ns, t1_ns, bias, covariance=False):
+    """Frozen IMU factors of count intervals (see cgmli_imu_preintegrate);
+    with covariance=True also the (count, 15, 15) preintegrated covariances."""
+    ll = C.POINTER(C.c_longlong)
+    time_ns = np.ascontiguousarray(time_ns, dtype=np.int64)
+    readings = np.ascontiguousarray(readings, dtype=np.float64)
+    ranges = np.ascontiguousarray(ranges, dtype=np.int32)
+    t0_ns = np.ascontiguousarray(t0_ns, dtype=np.int64)
+    t1_ns = np.ascontiguousarray(t1_ns, dtype=np.int64)
+    bias = np.ascontiguousarray(bias, dtype=np.float64)
+    count = len(t0_ns)
+    out = (abi.FrozenImu * max(count, 1))()
+    cov = np.zeros((max(count, 1), 15, 15)) if covariance else None
+    st = lib().oracle_imu_preintegrate(C.byref(params), time_ns.ctypes.data_as(ll), _p(readings), len(time_ns),
+                                       ranges.ctypes.data_as(ip), t0_ns.ctypes.data_as(ll), t1_ns.ctypes.data_as(ll),
+                                       _p(bias), count, out, _p(cov))
+    return (st, out, cov[:count]) if covariance else (st, out)
