@@ -143,6 +143,10 @@ def declare_backend(lib: C.CDLL) -> C.CDLL:
            [C.POINTER(ImuParameters), ll_p, c_double_p, C.c_int, c_int_p, ll_p, ll_p, c_double_p, C.c_int,
             C.POINTER(FrozenImu)])
     _proto(lib, "cgmli_imu_last_timing", C.c_int, [c_double_p])
+    _proto(lib, "cgmli_solver_set_imu_samples", C.c_int,
+           [S, C.POINTER(ImuParameters), ll_p, c_double_p, C.c_int, c_int_p, ll_p, ll_p])
+    _proto(lib, "cgmli_solver_refresh_imu", C.c_int, [S, C.c_double, C.c_double, c_int_p])
+    _proto(lib, "cgmli_solver_read_imu", C.c_int, [S, C.c_int, C.POINTER(FrozenImu)])
     return lib
 
 
@@ -165,7 +169,7 @@ BACKEND_SYMBOLS = [
     "cgmli_solver_checkpoint", "cgmli_solver_rollback", "cgmli_solver_kernel_times", "cgmli_topology_check",
     "cgmli_marg_eigen_noalloc", "cgmli_server_create", "cgmli_server_destroy", "cgmli_server_submit", "cgmli_server_poll",
     "cgmli_server_read_prior", "cgmli_server_release", "cgmli_server_replay", "cgmli_imu_preintegrate",
-    "cgmli_imu_last_timing",
+    "cgmli_imu_last_timing", "cgmli_solver_set_imu_samples", "cgmli_solver_refresh_imu", "cgmli_solver_read_imu",
 ]
 KERNEL_NAMES = ["zero_acc", "linearize", "retained", "factor", "candidate", "backsub_trial", "retained_trial", "lm_update", "accept",
                 "lin_pairs", "lin_schur"]

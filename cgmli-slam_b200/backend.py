@@ -89,6 +89,30 @@ class Solver:
         _check(lib().cgmli_solver_read_reports(self._h, reps, self.count), "cgmli_solver_read_reports")
         return list(reps)
 
+    def set_imu_samples(self, params: abi.ImuParameters, time_ns, readings, ranges, t0_ns, t1_ns) -> None:
+        """Samples of the batch's IMU factors (in window order) for refresh_imu."""
+        ll = C.POINTER(C.c_longlong)
+        time_ns = np.ascontiguousarray(time_ns, dtype=np.int64)
+        readings = np.ascontiguousarray(readings, dtype=np.float64)
+        ranges = np.ascontiguousarray(ranges, dtype=np.int32)
+        t0_ns = np.ascontiguousarray(t0_ns, dtype=np.int64)
+        t1_ns = np.ascontiguousarray(t1_ns, dtype=np.int64)
+        _check(lib().cgmli_solver_set_imu_samples(self._h, C.byref(params), time_ns.ctypes.data_as(ll), _p(readings), len(time_ns),
+                                                  ranges.ctypes.data_as(abi.c_int_p), t0_ns.ctypes.data_as(ll),
+                                                  t1_ns.ctypes.data_as(ll)), "cgmli_solver_set_imu_samples")
+
+    def refresh_imu(self, gyro_threshold: float = 0.0003, accel_threshold: float = 0.02, wait: bool = True):
+        """Re-preintegrates drifted IMU factors on the device; the count when wait."""
+        n = C.c_int()
+        _check(lib().cgmli_solver_refresh_imu(self._h, gyro_threshold, accel_threshold, C.byref(n) if wait else None),
+               "cgmli_solver_refresh_imu")
+        return n.value if wait else None
+
+    def read_imu(self, w: int, count: int):
+        out = (abi.FrozenImu * max(count, 1))()
+        _check(lib().cgmli_solver_read_imu(self._h, w, out), "cgmli_solver_read_imu")
+        return out
+
     def dims(self, w: int) -> tuple[int, int]:
         nr, nl = C.c_int(), C.c_int()
         _check(lib().cgmli_solver_window_dims(self._h, w, C.byref(nr), C.byref(nl)), "cgmli_solver_window_dims")

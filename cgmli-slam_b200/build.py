@@ -23,7 +23,7 @@ BACKEND_SOURCES = [PKG / "csrc" / "backend_kernels.cu", PKG / "csrc" / "marginal
                    PKG / "csrc" / "topology.cpp", PKG / "csrc" / "noalloc_eigen.cu", PKG / "csrc" / "imu_preintegration.cu",
                    PKG / "csrc" / "server.cpp"]
 BACKEND_HEADERS = [PKG / "csrc" / "device_math.cuh", PKG / "csrc" / "factor_eval.cuh", PKG / "csrc" / "backend_internal.h",
-                   PKG / "csrc" / "dense_tiles.cuh",
+                   PKG / "csrc" / "dense_tiles.cuh", PKG / "csrc" / "imu_preintegration.h",
                    PKG / "csrc" / "topology.h",
                    INCLUDE / "cgmli_backend.h"]
 NVCC_FLAGS = [

@@ -20,6 +20,7 @@
 
 #include "../../include/cgmli_backend.h"
 #include "backend_internal.h"
+#include "imu_preintegration.h"
 #include "topology.h"
 
 namespace cgmli {
@@ -159,6 +160,15 @@ struct cgmli_solver {
     HVec<int4> hMargChunks, hMargItems;
     int numSMs = 0;
     cudaEvent_t margUploaded = nullptr;
+    // IMU samples of the batch's factors, kept for cgmli_solver_refresh_imu
+    bool haveImuSamples = false;
+    cgmli_imu_parameters imuParams{};
+    int imuSampleOffset = 0;
+    DArray<long long> imuTimes, imuT0, imuT1;
+    DArray<double> imuReadings;
+    DArray<int> imuRanges, imuStatus, imuRefreshed;
+    DArray<cgmli_frozen_imu> imuRefreshScratch;
+    std::vector<int> hImuStatus, hImuRefreshed;
     // checkpoint of the accepted states
     DArray<double> snapPose, snapSb, snapExt, snapTd, snapRho;
     bool haveSnapshot = false;
@@ -212,6 +222,8 @@ struct cgmli_solver {
         lmC0.release(); dWin.release(); dLm.release(); dRuns.release(); dTiles.release();
         dPairChunks.release(); dSchurChunks.release(); schurCols.release(); lmUmap.release(); obLm.release(); keyOrder.release(); keyRows.release(); sch.release();
         snapPose.release(); snapSb.release(); snapExt.release(); snapTd.release(); snapRho.release();
+        imuTimes.release(); imuT0.release(); imuT1.release(); imuReadings.release(); imuRanges.release(); imuStatus.release();
+        imuRefreshed.release(); imuRefreshScratch.release();
         dMargWin.release(); dMargElim.release();
         DArray<int>* mi[] = {&margCols, &margObsMap, &margPoseCol, &margSbCol, &margExtCol, &margRank, &margStatus, &margFast,
                              &margVisCol, &margVisPose, &margVisExt, &margSlow};
@@ -297,6 +309,7 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     CK(cudaStreamSynchronize(st));
     S->haveSnapshot = false;
     S->haveMarg = false;
+    S->haveImuSamples = false;
     S->win.clear();
     HostBatch& hb = S->hb;
     std::string why;
@@ -461,6 +474,95 @@ int cgmli_solver_solve(cgmli_solver* S, int max_iterations) {
     if (max_iterations < 1) return fail(CGMLI_E_INVALID, "max_iterations < 1");
     CK(cudaSetDevice(S->device));
     return runIterations(S, max_iterations, 0, nullptr);
+}
+
+int cgmli_solver_set_imu_samples(cgmli_solver* S, const cgmli_imu_parameters* params, const long long* sample_time_ns,
+                                 const double* sample_readings, int num_samples, const int* range, const long long* t0_ns,
+                                 const long long* t1_ns) {
+    if (!S || S->win.empty()) return fail(CGMLI_E_INVALID, "solver has no windows");
+    const int count = S->totalImu;
+    if (!params) return fail(CGMLI_E_INVALID, "set_imu_samples: null parameters");
+    if (count == 0) {
+        S->haveImuSamples = false;
+        return CGMLI_OK;
+    }
+    if (!sample_time_ns || !sample_readings || !range || !t0_ns || !t1_ns || num_samples < 2)
+        return fail(CGMLI_E_INVALID, "set_imu_samples: null buffers or fewer than 2 samples");
+    int lo = num_samples, hi = 0;
+    for (int i = 0; i < count; ++i) {
+        const int b = range[2 * i], e = range[2 * i + 1];
+        if (b < 0 || e > num_samples || e - b < 2)
+            return fail(CGMLI_E_INVALID, "set_imu_samples: factor " + std::to_string(i) + ": sample range outside the samples or shorter than 2");
+        lo = std::min(lo, b);
+        hi = std::max(hi, e);
+    }
+    CK(cudaSetDevice(S->device));
+    cudaStream_t st = S->stream;
+    const size_t span = (size_t)(hi - lo);
+    CK(S->imuTimes.reserve(span)); CK(S->imuReadings.reserve(6 * span));
+    CK(S->imuRanges.reserve(2 * (size_t)count)); CK(S->imuT0.reserve(count)); CK(S->imuT1.reserve(count));
+    CK(S->imuStatus.reserve(count)); CK(S->imuRefreshed.reserve(count)); CK(S->imuRefreshScratch.reserve(count));
+    CK(cudaMemcpyAsync(S->imuTimes.p, sample_time_ns + lo, span * sizeof(long long), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(S->imuReadings.p, sample_readings + 6 * (size_t)lo, 6 * span * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(S->imuRanges.p, range, 2 * (size_t)count * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(S->imuT0.p, t0_ns, count * sizeof(long long), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(S->imuT1.p, t1_ns, count * sizeof(long long), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(S->imuStatus.p, 0, count * sizeof(int), st));
+    CK(cudaMemsetAsync(S->imuRefreshed.p, 0, count * sizeof(int), st));
+    // the caller's arrays may change once this returns (pageable copies are staged
+    // before cudaMemcpyAsync returns, so no wait is needed for them)
+    S->imuParams = *params;
+    S->imuSampleOffset = lo;
+    S->haveImuSamples = true;
+    return CGMLI_OK;
+}
+
+int cgmli_solver_refresh_imu(cgmli_solver* S, double gyro_threshold, double accel_threshold, int* refreshed) {
+    if (!S || S->win.empty()) return fail(CGMLI_E_INVALID, "solver has no windows");
+    if (!(gyro_threshold >= 0) || !(accel_threshold >= 0)) return fail(CGMLI_E_INVALID, "refresh_imu: negative or NaN threshold");
+    const int count = S->totalImu;
+    if (count > 0 && !S->haveImuSamples) return fail(CGMLI_E_INVALID, "refresh_imu: no IMU samples for this batch (set_imu_samples)");
+    CK(cudaSetDevice(S->device));
+    if (count > 0) {
+        ImuLaunch L{};
+        L.prm = S->imuParams;
+        L.times = S->imuTimes.p; L.readings = S->imuReadings.p; L.sampleOffset = S->imuSampleOffset;
+        L.ranges = S->imuRanges.p; L.t0s = S->imuT0.p; L.t1s = S->imuT1.p;
+        L.out = reinterpret_cast<cgmli_frozen_imu*>(S->imu.p);
+        L.status = S->imuStatus.p;
+        L.biases = nullptr;
+        L.sb = S->sb[0].p; L.kf = S->imuKf.p;
+        L.gyroThreshold = gyro_threshold; L.accelThreshold = accel_threshold;
+        L.scratch = S->imuRefreshScratch.p; L.refreshed = S->imuRefreshed.p;
+        CK(launchImuPreintegration(L, count, S->stream));
+    }
+    if (!refreshed) return CGMLI_OK;
+    *refreshed = 0;
+    if (count == 0) return CGMLI_OK;
+    S->hImuStatus.resize(count);
+    S->hImuRefreshed.resize(count);
+    CK(cudaMemcpyAsync(S->hImuStatus.data(), S->imuStatus.p, count * sizeof(int), cudaMemcpyDeviceToHost, S->stream));
+    CK(cudaMemcpyAsync(S->hImuRefreshed.data(), S->imuRefreshed.p, count * sizeof(int), cudaMemcpyDeviceToHost, S->stream));
+    CK(cudaStreamSynchronize(S->stream));
+    for (int i = 0; i < count; ++i) *refreshed += S->hImuRefreshed[i];
+    for (int i = 0; i < count; ++i)
+        if (S->hImuStatus[i] != CGMLI_OK)
+            return fail(S->hImuStatus[i], "refresh_imu: factor " + std::to_string(i) +
+                                              (S->hImuStatus[i] == CGMLI_E_INVALID ? ": invalid samples" : ": result not finite") +
+                                              "; it keeps its previous value");
+    return CGMLI_OK;
+}
+
+int cgmli_solver_read_imu(cgmli_solver* S, int window, cgmli_frozen_imu* imu) {
+    if (!S || window < 0 || window >= (int)S->win.size()) return fail(CGMLI_E_INVALID, "read_imu: bad window");
+    const WinDesc& d = S->win[window];
+    if (d.nImu == 0) return CGMLI_OK;
+    if (!imu) return fail(CGMLI_E_INVALID, "read_imu: null buffer");
+    CK(cudaSetDevice(S->device));
+    CK(cudaMemcpyAsync(imu, reinterpret_cast<const cgmli_frozen_imu*>(S->imu.p) + d.imu0, d.nImu * sizeof(cgmli_frozen_imu),
+                       cudaMemcpyDeviceToHost, S->stream));
+    CK(cudaStreamSynchronize(S->stream));
+    return CGMLI_OK;
 }
 
 int cgmli_solver_synchronize(cgmli_solver* S) {

@@ -44,6 +44,7 @@
 
 #include "../../include/cgmli_backend.h"
 #include "device_math.cuh"
+#include "imu_preintegration.h"
 
 namespace cgmli {
 int setLastError(int code, const char* message);
@@ -119,21 +120,38 @@ __device__ __forceinline__ void jacobiPair(int round, int m, int& p, int& q) {
     q = max(a, b);
 }
 
-__global__ void __launch_bounds__(kImuWarps * 32) k_imu_preintegrate(
-    cgmli_imu_parameters prm, const long long* __restrict__ times, const double* __restrict__ readings, int sampleOffset,
-    const int* __restrict__ ranges, const long long* __restrict__ t0s, const long long* __restrict__ t1s,
-    const double* __restrict__ biases, int count, cgmli_frozen_imu* __restrict__ out, int* __restrict__ status) {
+__global__ void __launch_bounds__(kImuWarps * 32) k_imu_preintegrate(const ImuLaunch L, int count) {
     extern __shared__ __align__(16) unsigned char smemRaw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int iv = blockIdx.x * kImuWarps + warp;
     if (iv >= count) return;
     ImuWarpSmem& S = reinterpret_cast<ImuWarpSmem*>(smemRaw)[warp];
     const unsigned full = 0xffffffffu;
+    const cgmli_imu_parameters& prm = L.prm;
+    int* status = L.status;
 
-    const int b = ranges[2 * iv] - sampleOffset, n = ranges[2 * iv + 1] - ranges[2 * iv];
-    const long long* ts = times + b;
-    const double* rd = readings + 6 * (size_t)b;
-    const long long t0 = t0s[iv], t1 = t1s[iv];
+    // linearization bias; a refresh first checks the drift from the factor's reference
+    const bool refresh = L.biases == nullptr;
+    d3 bg, ba;
+    if (!refresh) {
+        bg = ld3(L.biases + 6 * iv);
+        ba = ld3(L.biases + 6 * iv + 3);
+    } else {
+        const double* x = L.sb + 9ll * L.kf[iv];
+        bg = ld3(x + 3);
+        ba = ld3(x + 6);
+        const double* ref = L.out[iv].reference_bias;
+        const bool drift = norm(bg - ld3(ref)) > L.gyroThreshold || norm(ba - ld3(ref + 3)) > L.accelThreshold;
+        if (!drift) {
+            if (lane == 0) { status[iv] = CGMLI_OK; L.refreshed[iv] = 0; }
+            return;
+        }
+    }
+
+    const int b = L.ranges[2 * iv] - L.sampleOffset, n = L.ranges[2 * iv + 1] - L.ranges[2 * iv];
+    const long long* ts = L.times + b;
+    const double* rd = L.readings + 6 * (size_t)b;
+    const long long t0 = L.t0s[iv], t1 = L.t1s[iv];
 
     // ---- 1. sample checks (validImuInterval) and step bounds -------------------------
     bool bad = false;
@@ -158,12 +176,14 @@ __global__ void __launch_bounds__(kImuWarps * 32) k_imu_preintegrate(
     }
     const bool gapOk = isfinite(prm.max_sample_gap) && prm.max_sample_gap > 0;
     if (bad || !gapOk || n < 2 || t1 <= t0 || ts[0] > t0 || ts[n - 1] < t1) {
-        if (lane == 0) status[iv] = CGMLI_E_INVALID;
+        if (lane == 0) {
+            status[iv] = CGMLI_E_INVALID;
+            if (refresh) L.refreshed[iv] = 0;
+        }
         return;
     }
     const int first = nLE0 - 1, last = nLT1 - 1;  // steps (sample pairs) [first, last]
 
-    const d3 bg = ld3(biases + 6 * iv), ba = ld3(biases + 6 * iv + 3);
     const double sg2 = prm.sigma_g_c * prm.sigma_g_c, sa2 = prm.sigma_a_c * prm.sigma_a_c;
     const double sgw2 = prm.sigma_gw_c * prm.sigma_gw_c, saw2 = prm.sigma_aw_c * prm.sigma_aw_c;
 
@@ -416,7 +436,7 @@ __global__ void __launch_bounds__(kImuWarps * 32) k_imu_preintegrate(
         if (!rotated) break;
     }
 
-    cgmli_frozen_imu& o = out[iv];
+    cgmli_frozen_imu& o = refresh ? L.scratch[iv] : L.out[iv];
     bool finiteOut = true;
     {
         double lmax = A[0];
@@ -456,7 +476,7 @@ __global__ void __launch_bounds__(kImuWarps * 32) k_imu_preintegrate(
         for (int k = 0; k < 4; ++k) o.sensor_quaternion[k] = prm.sensor_quaternion[k];
         finiteOut = finiteOut && isfinite(qn2(Dq)) && finite3(accInt) && finite3(accDint);
     }
-    if (lane < 6) o.reference_bias[lane] = biases[6 * iv + lane];
+    if (lane < 6) o.reference_bias[lane] = lane < 3 ? compSel(bg, lane) : compSel(ba, lane - 3);
     if (lane < 6) {
         // gyroAt (src/factor/BodyImuFactor.cpp:29-38) at t0 (lanes 0..2) and t1 (lanes 3..5)
         const int end = lane / 3, axis = lane % 3;
@@ -473,6 +493,16 @@ __global__ void __launch_bounds__(kImuWarps * 32) k_imu_preintegrate(
         finiteOut = finiteOut && isfinite(g);
     }
     const bool anyBad = __any_sync(full, !finiteOut);
+    if (refresh) {
+        // replace the factor only with a finite result
+        __syncwarp();
+        if (!anyBad) {
+            const double* src = reinterpret_cast<const double*>(&L.scratch[iv]);
+            double* dst = reinterpret_cast<double*>(&L.out[iv]);
+            for (int k = lane; k < (int)(sizeof(cgmli_frozen_imu) / sizeof(double)); k += 32) dst[k] = src[k];
+        }
+        if (lane == 0) L.refreshed[iv] = anyBad ? 0 : 1;
+    }
     if (lane == 0) status[iv] = anyBad ? CGMLI_E_NONFINITE : CGMLI_OK;
 }
 
@@ -515,11 +545,8 @@ int cudaFailure(cudaError_t e, const char* what) {
 }  // namespace
 
 namespace cgmli {
-// Launches the preintegration of count intervals whose arrays are already on the
-// device (ranges index times / readings shifted by sampleOffset).
-cudaError_t launchImuPreintegration(const cgmli_imu_parameters& prm, const long long* times, const double* readings, int sampleOffset,
-                                    const int* ranges, const long long* t0, const long long* t1, const double* bias, int count,
-                                    cgmli_frozen_imu* out, int* status, cudaStream_t s) {
+// Launches the preintegration of count intervals whose arrays are already on the device.
+cudaError_t launchImuPreintegration(const ImuLaunch& L, int count, cudaStream_t s) {
     if (count <= 0) return cudaSuccess;
     static int configured[64] = {};
     int dev = 0;
@@ -531,8 +558,7 @@ cudaError_t launchImuPreintegration(const cgmli_imu_parameters& prm, const long 
         configured[dev] = 1;
     }
     const int blocks = (count + kImuWarps - 1) / kImuWarps;
-    k_imu_preintegrate<<<blocks, kImuWarps * 32, imuSmemBytes(), s>>>(prm, times, readings, sampleOffset, ranges, t0, t1, bias, count,
-                                                                       out, status);
+    k_imu_preintegrate<<<blocks, kImuWarps * 32, imuSmemBytes(), s>>>(L, count);
     return cudaGetLastError();
 }
 }  // namespace cgmli
@@ -597,8 +623,12 @@ int cgmli_imu_preintegrate(const cgmli_imu_parameters* params, const long long* 
     IMU_CK(cudaMemcpyAsync(g_imu.t1.p, t1_ns, count * sizeof(long long), cudaMemcpyHostToDevice, s));
     IMU_CK(cudaMemcpyAsync(g_imu.bias.p, bias, 6 * (size_t)count * sizeof(double), cudaMemcpyHostToDevice, s));
     IMU_CK(cudaEventRecord(g_imu.ev0, s));
-    IMU_CK(launchImuPreintegration(*params, g_imu.times.p, g_imu.readings.p, lo, g_imu.ranges.p, g_imu.t0.p, g_imu.t1.p, g_imu.bias.p,
-                                   count, g_imu.out.p, g_imu.status.p, s));
+    ImuLaunch L{};
+    L.prm = *params;
+    L.times = g_imu.times.p; L.readings = g_imu.readings.p; L.sampleOffset = lo;
+    L.ranges = g_imu.ranges.p; L.t0s = g_imu.t0.p; L.t1s = g_imu.t1.p;
+    L.out = g_imu.out.p; L.status = g_imu.status.p; L.biases = g_imu.bias.p;
+    IMU_CK(launchImuPreintegration(L, count, s));
     IMU_CK(cudaEventRecord(g_imu.ev1, s));
     g_imu.hostStatus.resize(count);
     IMU_CK(cudaMemcpyAsync(frozen, g_imu.out.p, count * sizeof(cgmli_frozen_imu), cudaMemcpyDeviceToHost, s));

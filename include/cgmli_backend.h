@@ -284,6 +284,28 @@ int cgmli_imu_preintegrate(const cgmli_imu_parameters *params, const long long *
  * cgmli_imu_preintegrate call in this process. */
 int cgmli_imu_last_timing(double *kernel_ms);
 
+/* Resident refresh of a solver's IMU factors.  cgmli_solver_set_imu_samples
+ * keeps on the device the samples of the current batch's IMU factors: factor q
+ * (windows in order, each window's imu[] in order) integrates samples
+ * [range[2q], range[2q+1]) from t0_ns[q] to t1_ns[q] with params (those the
+ * factors were built with).  The next cgmli_solver_set_windows drops them.
+ * cgmli_solver_refresh_imu then re-preintegrates, on the solver's stream at
+ * the accepted states, every factor whose first keyframe's bias moved from the
+ * factor's reference bias by more than gyro_threshold in |d b_g| or
+ * accel_threshold in |d b_a| (bodyImuNeedsRefresh + makeBodyImuFactor before
+ * each optimization, src/backend/FixedLagBackend.cpp:395-411, thresholds 0.0003
+ * and 0.02 there), replacing it in place for the next solve or marginalization;
+ * states and checkpoints are untouched.  With refreshed == NULL the call only
+ * enqueues the work (no host round trip); otherwise it waits, stores the number
+ * of replaced factors and returns CGMLI_E_INVALID / _E_NONFINITE for a factor
+ * whose samples or result were bad (such a factor keeps its previous value).
+ * cgmli_solver_read_imu copies window w's current factors (num_imu) to the host. */
+int cgmli_solver_set_imu_samples(cgmli_solver *solver, const cgmli_imu_parameters *params, const long long *sample_time_ns,
+                                 const double *sample_readings, int num_samples, const int *range, const long long *t0_ns,
+                                 const long long *t1_ns);
+int cgmli_solver_refresh_imu(cgmli_solver *solver, double gyro_threshold, double accel_threshold, int *refreshed);
+int cgmli_solver_read_imu(cgmli_solver *solver, int window, cgmli_frozen_imu *imu);
+
 /* ---- Served mode: continuous batching of window solves ---------------------
  * Windows from many rigs arrive as independent requests.  A request is one
  * window (its arrays are the caller's and must stay valid and unmodified until

@@ -143,3 +143,56 @@ def test_preintegrated_factor_solves_like_oracle(oracle, backend):
     sv.step(1e-4)
     g = sv.read_step(0)
     assert g["status"] == 0 and rel(g["delta"], ref["delta"]) < 1e-9
+
+
+def test_resident_refresh_replaces_drifted_factors(oracle, backend):
+    """set_imu_samples + refresh_imu: factors whose first keyframe's bias moved
+    past 3e-4 (gyro) or 0.02 (accelerometer) are re-preintegrated on the device at
+    the current bias; the others stay bit-identical; the next step uses them."""
+    from dataclasses import replace
+    w = synth.SynthWindow(replace(synth.C1, keyframes=6, landmarks=200), 33)
+    K, nimu = w.K, w.window.num_imu
+    kf = np.array([w.window.imu_kf[q] for q in range(nimu)])
+    s = synth.imu_stream(1, K, 34)
+    sel = kf  # interval k of the stream spans keyframes k -> k+1
+    prm = synth.imu_parameters()
+    sb = w.speed_bias().reshape(K, 9)
+    args = (s.time_ns, s.readings, s.ranges[sel], s.t0_ns[sel], s.t1_ns[sel])
+    built = backend.imu_preintegrate(prm, *args, sb[kf, 3:9])
+    for q in range(nimu):
+        w.window.imu[q] = built[q]
+    sb[kf[1], 3] += 1e-3   # gyro drift above 3e-4
+    sb[kf[3], 7] += 0.05   # accelerometer drift above 0.02
+    sb[kf[2], 4] += 1e-4   # below both thresholds
+    solver = backend.Solver()
+    solver.set_windows([w])
+    solver.set_imu_samples(prm, *args)
+    assert solver.refresh_imu() == 2
+    got = solver.read_imu(0, nimu)
+    st, ref, cov = oracle.imu_preintegrate(prm, *args, sb[kf, 3:9], covariance=True)
+    assert st == 0
+    for q in range(nimu):
+        if q in (1, 3):
+            compare(got[q], ref[q], cov[q])
+            assert list(got[q].reference_bias) == list(sb[kf[q], 3:9])
+        else:
+            assert bytes(got[q]) == bytes(built[q])
+    # a second refresh finds nothing left to do
+    assert solver.refresh_imu() == 0
+    for q in (1, 3):
+        w.window.imu[q] = ref[q]
+    nr, L = w.retained_dim(), w.L
+    ref_step = oracle.step(w.window, nr, L, 1e-4)
+    solver.step(1e-4)
+    g = solver.read_step(0)
+    assert g["status"] == 0 and rel(g["delta"], ref_step["delta"]) < 1e-9
+
+
+def test_refresh_without_samples_is_rejected(backend):
+    from dataclasses import replace
+    w = synth.SynthWindow(replace(synth.C1, keyframes=4, landmarks=60), 35)
+    solver = backend.Solver()
+    solver.set_windows([w])
+    with pytest.raises(backend.BackendError) as e:
+        solver.refresh_imu()
+    assert e.value.code == abi.E_INVALID
