@@ -46,6 +46,12 @@ class ImuParameters(C.Structure):
     ]
 
 
+class GateReport(C.Structure):
+    _fields_ = [("passes", C.c_int), ("rejected_pre", C.c_int), ("evaluated", C.c_int), ("rejected_last", C.c_int),
+                ("rejected_total", C.c_int),
+                ("nis_sum", C.c_double), ("nis_max", C.c_double)]
+
+
 class Window(C.Structure):
     _fields_ = [
         ("num_keyframes", C.c_int), ("num_cameras", C.c_int), ("num_extrinsics", C.c_int),
@@ -147,6 +153,8 @@ def declare_backend(lib: C.CDLL) -> C.CDLL:
            [S, C.POINTER(ImuParameters), ll_p, c_double_p, C.c_int, c_int_p, ll_p, ll_p])
     _proto(lib, "cgmli_solver_refresh_imu", C.c_int, [S, C.c_double, C.c_double, c_int_p])
     _proto(lib, "cgmli_solver_read_imu", C.c_int, [S, C.c_int, C.POINTER(FrozenImu)])
+    _proto(lib, "cgmli_solver_solve_gated", C.c_int, [S, C.c_int, C.c_double, C.c_int, C.c_int])
+    _proto(lib, "cgmli_solver_read_gate", C.c_int, [S, C.c_int, C.POINTER(GateReport), C.POINTER(C.c_ubyte)])
     return lib
 
 
@@ -170,6 +178,7 @@ BACKEND_SYMBOLS = [
     "cgmli_marg_eigen_noalloc", "cgmli_server_create", "cgmli_server_destroy", "cgmli_server_submit", "cgmli_server_poll",
     "cgmli_server_read_prior", "cgmli_server_release", "cgmli_server_replay", "cgmli_imu_preintegrate",
     "cgmli_imu_last_timing", "cgmli_solver_set_imu_samples", "cgmli_solver_refresh_imu", "cgmli_solver_read_imu",
+    "cgmli_solver_solve_gated", "cgmli_solver_read_gate",
 ]
 KERNEL_NAMES = ["zero_acc", "linearize", "retained", "factor", "candidate", "backsub_trial", "retained_trial", "lm_update", "accept",
                 "lin_pairs", "lin_schur"]

@@ -89,6 +89,19 @@ class Solver:
         _check(lib().cgmli_solver_read_reports(self._h, reps, self.count), "cgmli_solver_read_reports")
         return list(reps)
 
+    def solve_gated(self, iterations: int, nis_threshold: float = 9.210340371976184, max_refits: int = 3, pre_gate: bool = True):
+        _check(lib().cgmli_solver_solve_gated(self._h, iterations, nis_threshold, max_refits, int(pre_gate)),
+               "cgmli_solver_solve_gated")
+
+    def read_gate(self, w: int):
+        """(GateReport, rejected mask over the window's observations)."""
+        rep = abi.GateReport()
+        n = self._windows[w].num_observations
+        mask = np.zeros(max(n, 1), dtype=np.uint8)
+        _check(lib().cgmli_solver_read_gate(self._h, w, C.byref(rep), mask.ctypes.data_as(C.POINTER(C.c_ubyte))),
+               "cgmli_solver_read_gate")
+        return rep, mask[:n]
+
     def set_imu_samples(self, params: abi.ImuParameters, time_ns, readings, ranges, t0_ns, t1_ns) -> None:
         """Samples of the batch's IMU factors (in window order) for refresh_imu."""
         ll = C.POINTER(C.c_longlong)

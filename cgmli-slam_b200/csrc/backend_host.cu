@@ -30,6 +30,9 @@ cudaError_t configureKernels(size_t linSmem, size_t facSmem);
 int launchIteration(const DevBatch& B, const LaunchPlan& P, int refinement, int maxIterations, int probe, double* Sdebug,
                     cudaStream_t s, LaunchHook hook, void* ctx);
 int launchLmInit(const DevBatch& B, double lambda0, cudaStream_t s);
+int launchGate(const DevBatch& B, const LaunchPlan& P, int pass, int pre, double threshold, double* obP, unsigned char* rejected,
+               double* gateStats, int* gateCounts, cudaStream_t s);
+int launchRefit(const DevBatch& B, int pass, double lambda0, int maxIterations, const int* gateCounts, cudaStream_t s);
 size_t margVisualSmemBytes(int maxNc);
 size_t margRowsSmemBytes(int maxNv);
 int margRowsCap(int nv);
@@ -160,6 +163,11 @@ struct cgmli_solver {
     HVec<int4> hMargChunks, hMargItems;
     int numSMs = 0;
     cudaEvent_t margUploaded = nullptr;
+    // NIS gate: rejected observations (device order), per-window counters
+    // (kGateCounts each) and energies {sum, max} of the last gate
+    DArray<unsigned char> obRejected;
+    DArray<int> gateCounts;
+    DArray<double> gateStats;
     // IMU samples of the batch's factors, kept for cgmli_solver_refresh_imu
     bool haveImuSamples = false;
     cgmli_imu_parameters imuParams{};
@@ -224,6 +232,7 @@ struct cgmli_solver {
         snapPose.release(); snapSb.release(); snapExt.release(); snapTd.release(); snapRho.release();
         imuTimes.release(); imuT0.release(); imuT1.release(); imuReadings.release(); imuRanges.release(); imuStatus.release();
         imuRefreshed.release(); imuRefreshScratch.release();
+        obRejected.release(); gateCounts.release(); gateStats.release();
         dMargWin.release(); dMargElim.release();
         DArray<int>* mi[] = {&margCols, &margObsMap, &margPoseCol, &margSbCol, &margExtCol, &margRank, &margStatus, &margFast,
                              &margVisCol, &margVisPose, &margVisExt, &margSlow};
@@ -418,6 +427,11 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     B.solveStatus = S->solveStatus.p; B.out = S->out.p;
     CK(cudaMemsetAsync(S->costRet.p, 0, count * sizeof(double), st));
     CK(cudaMemsetAsync(S->trialRet.p, 0, count * sizeof(double), st));
+    CK(S->obRejected.reserve(std::max(1, S->totalObs))); CK(S->gateCounts.reserve((size_t)kGateCounts * count));
+    CK(S->gateStats.reserve(2ull * count));
+    CK(cudaMemsetAsync(S->obRejected.p, 0, std::max(1, S->totalObs), st));
+    CK(cudaMemsetAsync(S->gateCounts.p, 0, (size_t)kGateCounts * count * sizeof(int), st));
+    CK(cudaMemsetAsync(S->gateStats.p, 0, 2ull * count * sizeof(double), st));
     return CGMLI_OK;
 }
 
@@ -474,6 +488,61 @@ int cgmli_solver_solve(cgmli_solver* S, int max_iterations) {
     if (max_iterations < 1) return fail(CGMLI_E_INVALID, "max_iterations < 1");
     CK(cudaSetDevice(S->device));
     return runIterations(S, max_iterations, 0, nullptr);
+}
+
+int cgmli_solver_solve_gated(cgmli_solver* S, int max_iterations, double nis_threshold, int max_refits, int pre_gate) {
+    if (!S || S->win.empty()) return fail(CGMLI_E_INVALID, "solver has no windows");
+    if (max_iterations < 1) return fail(CGMLI_E_INVALID, "max_iterations < 1");
+    if (!(nis_threshold > 0)) return fail(CGMLI_E_INVALID, "solve_gated: nis_threshold must be positive");
+    if (max_refits < 0 || max_refits > 64) return fail(CGMLI_E_INVALID, "solve_gated: max_refits outside 0..64");
+    CK(cudaSetDevice(S->device));
+    cudaStream_t st = S->stream;
+    if (S->profile) S->collectKernelTimes();
+    const LaunchPlan P = S->plan();
+    CK(cudaEventRecord(S->ev0, st));
+    int launches = launchLmInit(S->B, S->opt.initial_lambda, st);
+    // the gate at the initial states removes factors before the first solve
+    if (pre_gate)
+        launches += launchGate(S->B, P, 0, 1, nis_threshold, S->obP.p, S->obRejected.p, S->gateStats.p, S->gateCounts.p, st);
+    for (int pass = 0; pass <= max_refits; ++pass) {
+        // pass 0 solves every window; a refit pass restarts the windows whose gate
+        // rejected factors (the others return at once from every kernel)
+        if (pass > 0) launches += launchRefit(S->B, pass, S->opt.initial_lambda, max_iterations, S->gateCounts.p, st);
+        for (int it = 0; it < max_iterations; ++it)
+            launches += launchIteration(S->B, P, S->opt.refinement_steps, max_iterations, 0, nullptr, st,
+                                        S->profile ? profileHook : nullptr, S);
+        launches += launchGate(S->B, P, pass, 0, nis_threshold, S->obP.p, S->obRejected.p, S->gateStats.p, S->gateCounts.p, st);
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(S->ev1, st));
+    S->lastLaunches = launches;
+    return CGMLI_OK;
+}
+
+int cgmli_solver_read_gate(cgmli_solver* S, int window, cgmli_gate_report* report, unsigned char* rejected) {
+    if (!S || window < 0 || window >= (int)S->win.size() || !report) return fail(CGMLI_E_INVALID, "read_gate: bad window or null report");
+    CK(cudaSetDevice(S->device));
+    const WinDesc& d = S->win[window];
+    WinLM lm;
+    int counts[kGateCounts];
+    double stats[2];
+    std::vector<unsigned char> mask(rejected ? d.F : 0);
+    CK(cudaMemcpyAsync(&lm, S->dLm.p + window, sizeof(WinLM), cudaMemcpyDeviceToHost, S->stream));
+    CK(cudaMemcpyAsync(counts, S->gateCounts.p + (long long)kGateCounts * window, sizeof(counts), cudaMemcpyDeviceToHost, S->stream));
+    CK(cudaMemcpyAsync(stats, S->gateStats.p + 2ll * window, sizeof(stats), cudaMemcpyDeviceToHost, S->stream));
+    if (rejected && d.F)
+        CK(cudaMemcpyAsync(mask.data(), S->obRejected.p + d.obs0, d.F, cudaMemcpyDeviceToHost, S->stream));
+    CK(cudaStreamSynchronize(S->stream));
+    report->passes = lm.pass + 1;
+    report->evaluated = counts[0];
+    report->rejected_last = counts[1];
+    report->rejected_total = counts[2];
+    report->rejected_pre = counts[4];
+    report->nis_sum = stats[0];
+    report->nis_max = stats[1];
+    if (rejected)
+        for (int o = 0; o < d.F; ++o) rejected[S->hb.obOrig[d.obs0 + o]] = mask[o];
+    return counts[3] ? fail(CGMLI_E_NONFINITE, "read_gate: a gated residual was not finite") : CGMLI_OK;
 }
 
 int cgmli_solver_set_imu_samples(cgmli_solver* S, const cgmli_imu_parameters* params, const long long* sample_time_ns,

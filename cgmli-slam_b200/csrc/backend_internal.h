@@ -41,7 +41,11 @@ struct WinDesc {
 struct WinLM {
     double lambda, nu, cost, initialCost, linCost, trialCost, predicted, maxInc;
     int mode;        // kModeLinearize, kModeResolve, kModeDone
-    int iterations, accepted, converged, status, acceptNow, trialValid, pad;
+    int iterations, accepted, converged, status, acceptNow, trialValid;
+    // outlier refits (a gated solve runs passes 0..R): iterations and accepted
+    // steps at the start of the window's current pass, iterations charged to the
+    // finished passes (at least one each), index of the window's current pass
+    int passStart, passAccepted, charged, pass, pad;
 };
 enum { kModeLinearize = 0, kModeResolve = 1, kModeDone = 2 };
 
@@ -160,6 +164,11 @@ struct MargBatch {
 // Called before (phase 0) and after (phase 1) every kernel launch of an
 // iteration; used for per-kernel event timing.
 typedef void (*LaunchHook)(void* ctx, int kind, int phase);
+
+// Per-window counters of the NIS gate: evaluated by the last gate, rejected by
+// the last gate after a solve, rejected in total, a residual was not finite,
+// rejected by the gate before the first solve; one spare.
+constexpr int kGateCounts = 6;
 
 // Work decomposition of one batch (device pointers and counts).
 struct LaunchPlan {

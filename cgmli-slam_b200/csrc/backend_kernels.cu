@@ -1111,8 +1111,12 @@ __global__ void __launch_bounds__(256) k_lm_update(DevBatch B, int maxIterations
     if (st.mode == kModeLinearize) {
         st.linCost = linCost;
         if (!valid || !isfinite(linCost)) { st.status = CGMLI_E_NONFINITE; st.mode = kModeDone; st.acceptNow = 0; return; }
-        if (st.iterations == 0) st.cost = st.initialCost = linCost;
-        else if (fabs(linCost - st.cost) > 1e-8 * fmax(1.0, st.cost)) {
+        // the first linearization of a pass sets its cost (a refit pass starts
+        // from the gated factor set, whose cost differs from the last accepted one)
+        if (st.iterations == st.passStart) {
+            st.cost = linCost;
+            if (st.iterations == 0) st.initialCost = linCost;
+        } else if (fabs(linCost - st.cost) > 1e-8 * fmax(1.0, st.cost)) {
             st.status = CGMLI_E_COST_MISMATCH; st.mode = kModeDone; st.acceptNow = 0; return;
         }
     }
@@ -1145,8 +1149,99 @@ __global__ void __launch_bounds__(256) k_lm_update(DevBatch B, int maxIterations
             st.mode = kModeResolve;
         }
     }
-    if (st.iterations >= maxIterations && st.mode != kModeDone) st.mode = kModeDone;
-    if (st.mode == kModeDone && st.status == CGMLI_OK && !st.accepted && !st.converged) st.status = CGMLI_E_NO_STEP;
+    // the pass may use what the finished passes left of the budget
+    if (st.iterations - st.passStart + st.charged >= maxIterations && st.mode != kModeDone) st.mode = kModeDone;
+    if (st.mode == kModeDone && st.status == CGMLI_OK && st.accepted == st.passAccepted && !st.converged) st.status = CGMLI_E_NO_STEP;
+}
+
+// ---------------------------------------------------------------------------------------
+// Whitened pre-loss NIS gate and outlier refits (BackendOptimizer::statisticalGate
+// and the refit loop of optimizeImpl, BackendOptimizer.cpp:394-472,1030-1079).
+// Visual factors are gated; IMU factors and the prior have an infinite threshold
+// there.  A rejected factor's whitening rows (obP) are zeroed, so every later
+// linearization, trial and marginalization sees a zero residual and Jacobian,
+// which is what leaving it out of the problem gives.
+
+// Rotations of the accepted states (the last iteration may have left the
+// candidate's in place) and the per-gate counters of the windows in this pass.
+__global__ void k_gate_prepare(DevBatch B, int pass, int pre, double* gateStats, int* gateCounts) {
+    const int w = blockIdx.x;
+    if (B.lm[w].pass != pass) return;
+    const WinDesc& wd = B.win[w];
+    for (int k = threadIdx.x; k < wd.K; k += blockDim.x) poseRotation(B.pose[0] + 7ll * (wd.kf0 + k), B.rotKf[0] + 9ll * (wd.kf0 + k));
+    for (int e = threadIdx.x; e < wd.E; e += blockDim.x) poseRotation(B.ext[0] + 7ll * (wd.ext0 + e), B.rotExt[0] + 9ll * (wd.ext0 + e));
+    if (threadIdx.x == 0) {
+        gateStats[2 * w] = 0.0;      // sum of the evaluated energies
+        gateStats[2 * w + 1] = 0.0;  // largest energy
+        int* c = gateCounts + kGateCounts * w;
+        c[0] = 0;             // evaluated
+        c[pre ? 4 : 1] = 0;   // rejected by this gate (before the first solve: slot 4)
+        c[3] = 0;             // a residual was not finite
+    }
+}
+
+// One warp per tile, one lane per observation (as k_trial).  Slot 2 of a
+// window's counters counts its rejections over all gates.
+__global__ void __launch_bounds__(kTrialWarps * 32) k_gate(DevBatch B, const int2* tiles, int numTiles, int pass, int pre, double threshold,
+                                                         double* obP, unsigned char* rejected, double* gateStats, int* gateCounts) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t = blockIdx.x * kTrialWarps + warp;
+    if (t >= numTiles) return;
+    const int2 tile = tiles[t];
+    const int lb = tile.x;
+    const int wdx = B.lmWin[lb];
+    const WinLM& st = B.lm[wdx];
+    if (st.pass != pass || st.status != CGMLI_OK) return;
+    const WinDesc wd = B.win[wdx];
+    const int ob = B.lmObsBegin[lb], oe = B.lmObsBegin[tile.y];
+    const int f = ob + lane;
+    if (f >= oe || rejected[f]) return;
+    FactorIn in;
+    int kfa, kfb, ea, eb;
+    gatherFactor(B, wd, wdx, B.obLm[f], f, 0, in, kfa, kfb, ea, eb);
+    FactorOut o;
+    const bool ok = evalBearingFactor(in, false, o);
+    const double energy = o.r[0] * o.r[0] + o.r[1] * o.r[1];
+    int* c = gateCounts + kGateCounts * wdx;
+    if (!ok || !isfinite(energy)) {
+        atomicOr(&c[3], 1);
+        return;
+    }
+    atomicAdd(&c[0], 1);
+    atomicAdd(&gateStats[2 * wdx], energy);
+    // energies are >= 0: their IEEE bit patterns order like the values
+    atomicMax(reinterpret_cast<unsigned long long*>(&gateStats[2 * wdx + 1]), (unsigned long long)__double_as_longlong(energy));
+    if (energy > threshold) {
+        rejected[f] = 1;
+        for (int k = 0; k < 6; ++k) obP[6ll * f + k] = 0.0;
+        atomicAdd(&c[pre ? 4 : 1], 1);
+        atomicAdd(&c[2], 1);
+    }
+}
+
+// Decides, after the gate of pass - 1, which windows run pass `pass`: those that
+// rejected factors there with iteration budget left, restarted from their
+// accepted state with the initial lambda (a fresh solve of the cleaned problem).
+// Every finished pass is charged at least one iteration.
+__global__ void k_lm_refit(DevBatch B, int pass, double lambda0, int maxIterations, const int* gateCounts) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= B.numWindows) return;
+    WinLM& st = B.lm[w];
+    if (st.pass != pass - 1) return;  // stopped refitting earlier
+    const int* c = gateCounts + kGateCounts * w;
+    if (c[3] && st.status == CGMLI_OK) st.status = CGMLI_E_NONFINITE;
+    st.charged += max(1, st.iterations - st.passStart);
+    st.mode = kModeDone;
+    st.acceptNow = 0;
+    if (st.status != CGMLI_OK || c[1] == 0 || st.charged >= maxIterations) return;
+    st.pass = pass;
+    st.mode = kModeLinearize;
+    st.lambda = lambda0;
+    st.nu = 2;
+    st.converged = 0;
+    st.trialValid = 0;
+    st.passStart = st.iterations;
+    st.passAccepted = st.accepted;
 }
 
 // Copy the candidate into the accepted state of windows that accepted a step
@@ -1169,6 +1264,7 @@ __global__ void k_lm_init(DevBatch B, double lambda0) {
     st.lambda = lambda0; st.nu = 2; st.cost = 0; st.initialCost = 0; st.linCost = 0; st.trialCost = 0; st.predicted = 0;
     st.maxInc = 0; st.mode = kModeLinearize; st.iterations = 0; st.accepted = 0; st.converged = 0; st.status = CGMLI_OK;
     st.acceptNow = 0; st.trialValid = 0;
+    st.passStart = 0; st.passAccepted = 0; st.charged = 0; st.pass = 0; st.pad = 0;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1239,6 +1335,18 @@ int launchIteration(const DevBatch& B, const LaunchPlan& P, int refinement, int 
     run(CGMLI_KERNEL_LM_UPDATE, [&] { k_lm_update<<<W, 256, 0, s>>>(B, maxIterations, probe); });
     if (!probe) run(CGMLI_KERNEL_ACCEPT, [&] { k_accept<<<W, 256, 0, s>>>(B); });
     return n;
+}
+int launchGate(const DevBatch& B, const LaunchPlan& P, int pass, int pre, double threshold, double* obP, unsigned char* rejected,
+               double* gateStats, int* gateCounts, cudaStream_t s) {
+    k_gate_prepare<<<B.numWindows, 128, 0, s>>>(B, pass, pre, gateStats, gateCounts);
+    if (P.numTiles > 0)
+        k_gate<<<(P.numTiles + kTrialWarps - 1) / kTrialWarps, kTrialWarps * 32, 0, s>>>(B, P.tiles, P.numTiles, pass, pre, threshold,
+                                                                                         obP, rejected, gateStats, gateCounts);
+    return P.numTiles > 0 ? 2 : 1;
+}
+int launchRefit(const DevBatch& B, int pass, double lambda0, int maxIterations, const int* gateCounts, cudaStream_t s) {
+    k_lm_refit<<<(B.numWindows + 127) / 128, 128, 0, s>>>(B, pass, lambda0, maxIterations, gateCounts);
+    return 1;
 }
 int launchLmInit(const DevBatch& B, double lambda0, cudaStream_t s) {
     k_lm_init<<<(B.numWindows + 127) / 128, 128, 0, s>>>(B, lambda0);

@@ -172,7 +172,7 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
     hb.lmWin.resize(lm); hb.lmKf.resize(lm); hb.lmCam.resize(lm); hb.lmObsBegin.resize(lm + 1ll); hb.lmNs.resize(lm); hb.lmNx.resize(lm);
     hb.lmSupp0.resize(lm); hb.lmC0.resize(lm); hb.lmPerm.resize(lm);
     hb.lmBearing.resize(3ll * lm); hb.lmVel.resize(3ll * lm); hb.lmTime.resize(lm);
-    hb.obKf.resize(ob); hb.obCam.resize(ob); hb.obSlot.resize(ob); hb.obXslot.resize(ob); hb.obLm.resize(ob);
+    hb.obKf.resize(ob); hb.obCam.resize(ob); hb.obSlot.resize(ob); hb.obXslot.resize(ob); hb.obLm.resize(ob); hb.obOrig.resize(ob);
     hb.keyOrder.resize(ob);
     hb.obBearing.resize(3ll * ob); hb.obP.resize(6ll * ob); hb.obVel.resize(3ll * ob); hb.obTime.resize(ob);
     hb.pose.resize(7ll * kf); hb.sb.resize(9ll * kf); hb.ext.resize(7ll * ex); hb.td.resize(count); hb.rho.resize(lm);
@@ -338,6 +338,7 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
             for (int k = 0; k < nobs; ++k) {
                 const int f = fo[k], o = obPos++;
                 hb.obLm[o] = g;
+                hb.obOrig[o] = f;
                 hb.obKf[o] = d.kf0 + w.obs_kf[f];
                 hb.obCam[o] = d.cam0 + w.obs_cam[f];
                 int slot = 0;

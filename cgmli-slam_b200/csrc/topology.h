@@ -167,6 +167,7 @@ struct HostBatch {
     HVec<double> lmBearing, lmVel, lmTime;
     // observations (device order)
     HVec<int> obKf, obCam, obSlot, obXslot, obLm, keyOrder;
+    HVec<int> obOrig;        // device observation -> observation index within its window
     HVec<double> obBearing, obP, obVel, obTime;
     // states
     HVec<double> pose, sb, ext, td, rho;

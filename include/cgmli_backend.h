@@ -246,6 +246,36 @@ int cgmli_marg_subtract(const double *coupling, const double *solution, int elim
 #define CGMLI_MARG_EIGEN_NOALLOC_MAX_N 256
 int cgmli_marg_eigen_noalloc(const double *H, int n, double *eigenvalues, double *eigenvectors, void *stream);
 
+/* ---- Outlier gate and refits ---------------------------------------------------
+ * cgmli_solver_solve_gated is cgmli_solver_solve with the reference's whitened
+ * pre-loss NIS gate and outlier refits (BackendOptimizer::statisticalGate and
+ * the gates and refit loop of optimizeImpl, src/backend/BackendOptimizer.cpp:
+ * 394-472,669-686,1030-1079): with pre_gate, the gate first runs at the initial
+ * states (the reference's pre-NIS, skipped by its skipPreNis); after each pass
+ * every visual factor of the window still in the
+ * problem is evaluated at the accepted state without the robust loss; those with
+ * |r|^2 above nis_threshold (the reference's visualNisThreshold, 9.21) are
+ * rejected for good; a window that rejected factors, has refits left (at most
+ * max_refits, the reference's maxOutlierRefits = 3) and iteration budget left
+ * is solved again from its state with the initial lambda.  All passes share
+ * max_iterations, each charged at least one iteration.  The factors rejected by
+ * the last gate stay rejected without a further refit.  IMU factors and the
+ * prior are not gated (infinite thresholds in the reference).  Everything runs
+ * on the device; a rejection persists until the next cgmli_solver_set_windows
+ * (checkpoint / rollback restore states only).
+ * cgmli_solver_read_gate reports window w's gate and, when rejected is not
+ * NULL, marks each of its num_observations factors (caller order) 1 if rejected. */
+typedef struct cgmli_gate_report {
+    int passes;          /* LM passes run: 1 + outlier refits */
+    int rejected_pre;    /* rejected by the gate before the first solve */
+    int evaluated;       /* visual factors evaluated by the last gate */
+    int rejected_last;   /* of them, rejected by the last gate (no refit followed) */
+    int rejected_total;  /* visual factors rejected since cgmli_solver_set_windows */
+    double nis_sum, nis_max; /* whitened pre-loss |r|^2 of the last gate's evaluated factors */
+} cgmli_gate_report;
+int cgmli_solver_solve_gated(cgmli_solver *solver, int max_iterations, double nis_threshold, int max_refits, int pre_gate);
+int cgmli_solver_read_gate(cgmli_solver *solver, int window, cgmli_gate_report *report, unsigned char *rejected);
+
 /* ---- IMU preintegration ------------------------------------------------------
  * Batched construction of frozen IMU factors, the device form of what the
  * reference does on the host per factor when it builds or refreshes a

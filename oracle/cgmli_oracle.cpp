@@ -1325,6 +1325,66 @@ static int lmSolve(cgmli_window& w, int maxIterations, cgmli_solve_report* rep, 
     return status;
 }
 
+// Whitened pre-loss NIS gate and outlier refits around the LM loop
+// (BackendOptimizer::statisticalGate and the refit loop of optimizeImpl,
+// BackendOptimizer.cpp:394-472,1030-1079), visual factors only.  A rejected
+// factor leaves the problem: its whitening rows are zeroed in a private copy.
+struct GateOut {
+    int passes = 0, rejectedPre = 0, evaluated = 0, rejectedLast = 0, rejectedTotal = 0;
+    double nisSum = 0, nisMax = 0;
+};
+static int lmSolveGated(cgmli_window& w, int maxIterations, double threshold, int maxRefits, bool preGate, double initialLambda,
+                        int refinement, cgmli_solve_report* rep, GateOut& g, unsigned char* rejected) {
+    std::vector<double> P(w.obs_P, w.obs_P + 6 * (size_t)w.num_observations);
+    const double* callerP = w.obs_P;
+    w.obs_P = P.data();
+    // one gate at the current states: statistics of the factors still in the
+    // problem, rejection of those above the threshold
+    auto gate = [&](int& rejectedNow) -> int {
+        g.evaluated = 0; g.nisSum = 0; g.nisMax = 0; rejectedNow = 0;
+        for (int l = 0; l < w.num_landmarks; ++l)
+            for (int f = w.lm_obs_begin[l]; f < w.lm_obs_begin[l + 1]; ++f) {
+                if (rejected[f]) continue;
+                Fac o;
+                const bool ok = visualFactor(w, l, f, false, o);
+                const double energy = o.r[0] * o.r[0] + o.r[1] * o.r[1];
+                if (!ok || !fin(energy)) return CGMLI_E_NONFINITE;
+                ++g.evaluated;
+                g.nisSum += energy;
+                g.nisMax = std::max(g.nisMax, energy);
+                if (energy > threshold) {
+                    rejected[f] = 1;
+                    for (int k = 0; k < 6; ++k) P[6 * (size_t)f + k] = 0.0;
+                    ++rejectedNow;
+                    ++g.rejectedTotal;
+                }
+            }
+        return CGMLI_OK;
+    };
+    cgmli_solve_report total{};
+    int charged = 0, status = CGMLI_OK;
+    if (preGate) status = gate(g.rejectedPre);
+    for (int pass = 0; pass <= maxRefits && status == CGMLI_OK; ++pass) {
+        cgmli_solve_report r{};
+        status = lmSolve(w, maxIterations - charged, &r, initialLambda, refinement);
+        ++g.passes;
+        if (pass == 0) total.initial_cost = r.initial_cost;
+        total.final_cost = r.final_cost; total.lambda = r.lambda;
+        total.predicted_reduction = r.predicted_reduction; total.max_increment = r.max_increment;
+        total.iterations += r.iterations; total.accepted_steps += r.accepted_steps;
+        total.converged = r.converged; total.status = status;
+        charged += std::max(1, r.iterations);  // every pass costs at least one iteration
+        if (status != CGMLI_OK) break;
+        status = gate(g.rejectedLast);
+        total.status = status;
+        if (status != CGMLI_OK || !g.rejectedLast || charged >= maxIterations || pass == maxRefits) break;
+    }
+    w.obs_P = callerP;
+    total.status = status;
+    if (rep) *rep = total;
+    return status;
+}
+
 // ---- marginalization --------------------------------------------------------------
 struct MargBlock { int kind, index, size, offset; bool eliminate, landmark; };
 struct MargOut {
@@ -1617,6 +1677,20 @@ static void marginalizeWindow(const cgmli_window& w, int victim, int policy, Win
 extern "C" {
 
 int oracle_version(void) { return 1; }
+
+// LM solve with the NIS gate and outlier refits; gate: {passes, rejected
+// before the first solve, evaluated by the last gate, rejected by it, rejected
+// in total}, nis: {sum, max} of the last gate; rejected: num_observations flags.
+int oracle_lm_solve_gated(cgmli_window* w, int max_iterations, double threshold, int max_refits, int pre_gate,
+                          cgmli_solve_report* report, int* gate, double* nis, unsigned char* rejected) {
+    orc::GateOut g;
+    std::vector<unsigned char> mask(w->num_observations, 0);
+    const int st = orc::lmSolveGated(*w, max_iterations, threshold, max_refits, pre_gate != 0, 1e-4, 0, report, g, mask.data());
+    gate[0] = g.passes; gate[1] = g.rejectedPre; gate[2] = g.evaluated; gate[3] = g.rejectedLast; gate[4] = g.rejectedTotal;
+    nis[0] = g.nisSum; nis[1] = g.nisMax;
+    std::copy(mask.begin(), mask.end(), rejected);
+    return st;
+}
 
 // Batched IMU preintegration with the semantics of cgmli_imu_preintegrate
 // (status 0, CGMLI_E_INVALID for a malformed interval, CGMLI_E_NONFINITE).

@@ -61,6 +61,8 @@ def lib() -> C.CDLL:
           [C.c_int, dp, dp, C.c_int, ip, ip, ip, dp, dp, dp, dp, dp])
         P(L, "oracle_marginalize_window", C.c_int,
           [W, C.c_int, C.c_int, ip, ip, ip, ip, ip, dp, dp, dp, dp, dp, dp])
+        P(L, "oracle_lm_solve_gated", C.c_int,
+          [W, C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(abi.SolveReport), ip, dp, C.POINTER(C.c_ubyte)])
         ll = C.POINTER(C.c_longlong)
         P(L, "oracle_imu_preintegrate", C.c_int,
           [C.POINTER(abi.ImuParameters), ll, dp, C.c_int, ip, ll, ll, dp, C.c_int, C.POINTER(abi.FrozenImu), dp])
@@ -186,3 +188,16 @@ def imu_preintegrate(params, time_ns, readings, ranges, t0_ns, t1_ns, bias, cova
                                        ranges.ctypes.data_as(ip), t0_ns.ctypes.data_as(ll), t1_ns.ctypes.data_as(ll),
                                        _p(bias), count, out, _p(cov))
     return (st, out, cov[:count]) if covariance else (st, out)
+
+
+def lm_solve_gated(win, iterations, threshold=9.210340371976184, max_refits=3, pre_gate=True):
+    """Gated LM solve in place; (status, report, gate dict, rejected mask)."""
+    rep = abi.SolveReport()
+    gate = np.zeros(5, dtype=np.int32)
+    nis = np.zeros(2)
+    mask = np.zeros(max(win.num_observations, 1), dtype=np.uint8)
+    st = lib().oracle_lm_solve_gated(C.byref(win), iterations, threshold, max_refits, int(pre_gate), C.byref(rep),
+                                     gate.ctypes.data_as(ip), _p(nis), mask.ctypes.data_as(C.POINTER(C.c_ubyte)))
+    g = dict(passes=int(gate[0]), rejected_pre=int(gate[1]), evaluated=int(gate[2]), rejected_last=int(gate[3]),
+             rejected_total=int(gate[4]), nis_sum=float(nis[0]), nis_max=float(nis[1]))
+    return st, rep, g, mask[:win.num_observations]
