@@ -68,6 +68,7 @@ def parse():
     p.add_argument("--serve-rate", type=float, default=5000.0, help="offered request rate of the served run (requests/s, 0: off)")
     p.add_argument("--serve-seconds", type=float, default=3.0, help="duration of the served run's arrivals")
     p.add_argument("--serve-pool", type=int, default=512, help="distinct windows the served requests draw from")
+    p.add_argument("--gate-iterations", type=int, default=10, help="iteration budget of the gated-solve row (0: off)")
     p.add_argument("--imu-rigs", type=int, default=512, help="rigs of the IMU preintegration batch, 11 keyframes each (0: off)")
     p.add_argument("--imu-cpu-sample", type=int, default=1024, help="intervals preintegrated by the oracle for its CPU rate")
     return p.parse_args()
@@ -278,6 +279,50 @@ def run_configs(args, local, backend):
                      "marginalization": "OLD" if policy == abi.MARGIN_OLD else "SECOND_NEW",
                      "final_state_rel_err_vs_fp64_oracle": float(np.linalg.norm(xg - xc) / max(np.linalg.norm(xc - x0), 1e-300))}
     return out
+
+
+def run_gated(args, local, backend, windows, init):
+    """The batch solved with the NIS gate and up to 3 outlier refits
+    (cgmli_solver_solve_gated, threshold 9.21, no pre-solve gate: the synthetic
+    windows start perturbed), against the plain solve at the same iteration
+    budget, both timed on the device.  Rejections persist on the device until
+    the next set_windows, so every repetition re-uploads the batch (untimed)."""
+    it = args.gate_iterations
+    gs = backend.Solver(device=local)
+    plain_ms, gated_ms = [], []
+    for rep in range(3):
+        for w, x in zip(windows, init):
+            w.set_state_vector(x)
+        gs.set_windows(windows)
+        gs.solve(it)
+        gs.synchronize()
+        if rep:
+            plain_ms.append(gs.timing()[0])
+        for w, x in zip(windows, init):
+            w.set_state_vector(x)
+        gs.set_windows(windows)
+        gs.solve_gated(it, pre_gate=False)
+        gs.synchronize()
+        if rep:
+            gated_ms.append(gs.timing()[0])
+    launches = gs.timing()[1]
+    passes, rejected, evaluated = {}, 0, 0
+    for i in range(len(windows)):
+        g, _ = gs.read_gate(i)
+        passes[g.passes] = passes.get(g.passes, 0) + 1
+        rejected += g.rejected_total
+    statuses = {}
+    for r in gs.reports():
+        k = abi.ERRORS.get(r.status, r.status)
+        statuses[k] = statuses.get(k, 0) + 1
+    for w, x in zip(windows, init):
+        w.set_state_vector(x)
+    gs.close()
+    g_ms, p_ms = statistics.median(gated_ms), statistics.median(plain_ms)
+    return {"iterations": it, "max_refits": 3, "nis_threshold": 9.210340371976184, "gated_ms": g_ms, "plain_ms": p_ms,
+            "gated_windows_per_s": len(windows) / (g_ms / 1e3), "overhead": g_ms / p_ms, "launches": launches,
+            "rejected_factors": rejected, "observations": sum(w.window.num_observations for w in windows),
+            "windows_by_passes": {str(k): v for k, v in sorted(passes.items())}, "window_status": statuses}
 
 
 def run_imu(args, local, backend):
@@ -511,6 +556,7 @@ def main():
     served = run_served(args, local, backend) if rank == 0 and args.serve_rate > 0 else None
     configs = run_configs(args, local, backend) if rank == 0 and not args.no_configs else None
     imu = run_imu(args, local, backend) if rank == 0 and args.imu_rigs > 0 else None
+    gated = run_gated(args, local, backend, windows, init) if rank == 0 and args.gate_iterations > 0 else None
 
     statuses = {}
     for r in reports:
@@ -556,6 +602,7 @@ def main():
             "cpu_baseline": cpu_baseline, "plain_path": plain,
             "served_vs_plain": (value / world) / plain["windows_per_s"] if plain else None,
             "served": served, "marginalization": marg, "configs": configs, "imu_preintegration": imu,
+            "nis_gate": gated,
             "batch_latency_ms": {"p50": sorted(dev_ms)[len(dev_ms) // 2], "p99": max(dev_ms)},
             "window_status": statuses, "wall_s": wall,
         }

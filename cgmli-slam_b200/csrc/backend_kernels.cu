@@ -1180,10 +1180,12 @@ __global__ void k_gate_prepare(DevBatch B, int pass, int pre, double* gateStats,
     }
 }
 
-// One warp per tile, one lane per observation (as k_trial).  Slot 2 of a
-// window's counters counts its rejections over all gates.
-__global__ void __launch_bounds__(kTrialWarps * 32) k_gate(DevBatch B, const int2* tiles, int numTiles, int pass, int pre, double threshold,
-                                                         double* obP, unsigned char* rejected, double* gateStats, int* gateCounts) {
+// One warp per tile, one lane per observation (as k_trial); a tile's landmarks
+// belong to one window, so the warp reduces its counters and energies before one
+// atomic each.  Slot 2 of a window's counters counts its rejections over all gates.
+__global__ void __launch_bounds__(kTrialWarps * 32, 2) k_gate(DevBatch B, const int2* tiles, int numTiles, int pass, int pre,
+                                                            double threshold, double* obP, unsigned char* rejected, double* gateStats,
+                                                            int* gateCounts) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int t = blockIdx.x * kTrialWarps + warp;
     if (t >= numTiles) return;
@@ -1195,27 +1197,49 @@ __global__ void __launch_bounds__(kTrialWarps * 32) k_gate(DevBatch B, const int
     const WinDesc wd = B.win[wdx];
     const int ob = B.lmObsBegin[lb], oe = B.lmObsBegin[tile.y];
     const int f = ob + lane;
-    if (f >= oe || rejected[f]) return;
-    FactorIn in;
-    int kfa, kfb, ea, eb;
-    gatherFactor(B, wd, wdx, B.obLm[f], f, 0, in, kfa, kfb, ea, eb);
-    FactorOut o;
-    const bool ok = evalBearingFactor(in, false, o);
-    const double energy = o.r[0] * o.r[0] + o.r[1] * o.r[1];
-    int* c = gateCounts + kGateCounts * wdx;
-    if (!ok || !isfinite(energy)) {
-        atomicOr(&c[3], 1);
-        return;
+    bool evaluated = false, bad = false, reject = false;
+    double energy = 0.0;
+    if (f < oe && !rejected[f]) {
+        FactorIn in;
+        int kfa, kfb, ea, eb;
+        gatherFactor(B, wd, wdx, B.obLm[f], f, 0, in, kfa, kfb, ea, eb);
+        FactorOut o;
+        const bool ok = evalBearingFactor(in, false, o);
+        energy = o.r[0] * o.r[0] + o.r[1] * o.r[1];
+        if (!ok || !isfinite(energy)) {
+            bad = true;
+            energy = 0.0;
+        } else {
+            evaluated = true;
+            reject = energy > threshold;
+        }
     }
-    atomicAdd(&c[0], 1);
-    atomicAdd(&gateStats[2 * wdx], energy);
-    // energies are >= 0: their IEEE bit patterns order like the values
-    atomicMax(reinterpret_cast<unsigned long long*>(&gateStats[2 * wdx + 1]), (unsigned long long)__double_as_longlong(energy));
-    if (energy > threshold) {
+    if (reject) {
         rejected[f] = 1;
         for (int k = 0; k < 6; ++k) obP[6ll * f + k] = 0.0;
-        atomicAdd(&c[pre ? 4 : 1], 1);
-        atomicAdd(&c[2], 1);
+    }
+    const unsigned full = 0xffffffffu;
+    const int nEval = __popc(__ballot_sync(full, evaluated)), nRej = __popc(__ballot_sync(full, reject));
+    const bool anyBad = __any_sync(full, bad);
+    double sum = energy, mx = energy;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sum += __shfl_xor_sync(full, sum, o);
+        mx = fmax(mx, __shfl_xor_sync(full, mx, o));
+    }
+    if (lane == 0) {
+        int* c = gateCounts + kGateCounts * wdx;
+        if (anyBad) atomicOr(&c[3], 1);
+        if (nEval) {
+            atomicAdd(&c[0], nEval);
+            atomicAdd(&gateStats[2 * wdx], sum);
+            // energies are >= 0: their IEEE bit patterns order like the values
+            atomicMax(reinterpret_cast<unsigned long long*>(&gateStats[2 * wdx + 1]), (unsigned long long)__double_as_longlong(mx));
+        }
+        if (nRej) {
+            atomicAdd(&c[pre ? 4 : 1], nRej);
+            atomicAdd(&c[2], nRej);
+        }
     }
 }
 

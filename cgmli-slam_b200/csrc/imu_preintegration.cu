@@ -321,16 +321,30 @@ __global__ void __launch_bounds__(kImuWarps * 32) k_imu_preintegrate(const ImuLa
             const double gs = st[kGsat * 32 + j], as = st[kAsat * 32 + j];
             __syncwarp();
             // ---- 3b. T = F P (rows 0..8) ---------------------------------------------
+            // pairs 0..2 read E columns 3..14, pairs 3..4 columns 9..11: fixed trip
+            // counts, so every shared load has an immediate offset
             const double* P = S.P[cur];
             double* Pn = S.P[cur ^ 1];
             {
                 const int half = lane >> 4, c = lane & 15;
                 if (c < 15) {
-                    for (int pr = 0; pr < 5; ++pr) {
+                    const double* Pc = P + c;
+#pragma unroll
+                    for (int pr = 0; pr < 3; ++pr) {
                         const int r = pairRow(pr, half);
-                        const int lo = eLo(r), hi = eHi(r);
-                        double s = P[15 * r + c];
-                        for (int k = lo; k < hi; ++k) s += S.E[12 * r + k - 3] * P[15 * k + c];
+                        const double* Er = S.E + 12 * r;
+                        double s = Pc[15 * r];
+#pragma unroll
+                        for (int k = 3; k < 15; ++k) s += Er[k - 3] * Pc[15 * k];
+                        S.T[15 * r + c] = s;
+                    }
+#pragma unroll
+                    for (int pr = 3; pr < 5; ++pr) {
+                        const int r = pairRow(pr, half);
+                        const double* Er = S.E + 12 * r;
+                        double s = Pc[15 * r];
+#pragma unroll
+                        for (int k = 9; k < 12; ++k) s += Er[k - 3] * Pc[15 * k];
                         S.T[15 * r + c] = s;
                     }
                 }
@@ -341,11 +355,23 @@ __global__ void __launch_bounds__(kImuWarps * 32) k_imu_preintegrate(const ImuLa
                 const int half = lane >> 4, r = lane & 15;
                 if (r < 15) {
                     const double* Tr = r < 9 ? S.T + 15 * r : P + 15 * r;  // rows 9..14 of F P are those of P
-                    for (int pc = 0; pc < 5; ++pc) {
+#pragma unroll
+                    for (int pc = 0; pc < 3; ++pc) {
                         const int c = pairRow(pc, half);
-                        const int lo = eLo(c), hi = eHi(c);
+                        const double* Ec = S.E + 12 * c;
                         double s = Tr[c];
-                        for (int k = lo; k < hi; ++k) s += S.E[12 * c + k - 3] * Tr[k];
+#pragma unroll
+                        for (int k = 3; k < 15; ++k) s += Ec[k - 3] * Tr[k];
+                        if (r == c) s += noiseDiag(c, dt, gs, as, sg2, sa2, sgw2, saw2);
+                        Pn[15 * r + c] = s;
+                    }
+#pragma unroll
+                    for (int pc = 3; pc < 5; ++pc) {
+                        const int c = pairRow(pc, half);
+                        const double* Ec = S.E + 12 * c;
+                        double s = Tr[c];
+#pragma unroll
+                        for (int k = 9; k < 12; ++k) s += Ec[k - 3] * Tr[k];
                         if (r == c) s += noiseDiag(c, dt, gs, as, sg2, sa2, sgw2, saw2);
                         Pn[15 * r + c] = s;
                     }
