@@ -19,7 +19,8 @@ ERRORS = {
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 PRIOR_POSE, PRIOR_SPEED_BIAS, PRIOR_EXTRINSIC, PRIOR_TIME_OFFSET = 0, 1, 2, 3
-MARGIN_OLD, MARGIN_SECOND_NEW = 0, 1
+MARGIN_OLD, MARGIN_SECOND_NEW, MARGIN_SECOND_NEW_IMU_MERGE = 0, 1, 2
+IMU_MERGE_NONE, IMU_MERGE_REINTEGRATED, IMU_MERGE_BRIDGE, IMU_MERGE_SUPPRESSED = 0, 1, 2, 3
 MARG_EIGEN_NOALLOC_MAX_N = 256  # CGMLI_MARG_EIGEN_NOALLOC_MAX_N
 E_INVALID = 1
 E_NONFINITE = 2
@@ -154,6 +155,8 @@ def declare_backend(lib: C.CDLL) -> C.CDLL:
     _proto(lib, "cgmli_solver_refresh_imu", C.c_int, [S, C.c_double, C.c_double, c_int_p])
     _proto(lib, "cgmli_solver_read_imu", C.c_int, [S, C.c_int, C.POINTER(FrozenImu)])
     _proto(lib, "cgmli_solver_solve_gated", C.c_int, [S, C.c_int, C.c_double, C.c_int, C.c_int])
+    _proto(lib, "cgmli_solver_set_imu_merge_limits", C.c_int, [S, C.c_double, C.c_int])
+    _proto(lib, "cgmli_solver_read_merged_imu", C.c_int, [S, C.c_int, c_int_p, C.POINTER(FrozenImu)])
     _proto(lib, "cgmli_solver_read_gate", C.c_int, [S, C.c_int, C.POINTER(GateReport), C.POINTER(C.c_ubyte)])
     return lib
 
@@ -178,7 +181,7 @@ BACKEND_SYMBOLS = [
     "cgmli_marg_eigen_noalloc", "cgmli_server_create", "cgmli_server_destroy", "cgmli_server_submit", "cgmli_server_poll",
     "cgmli_server_read_prior", "cgmli_server_release", "cgmli_server_replay", "cgmli_imu_preintegrate",
     "cgmli_imu_last_timing", "cgmli_solver_set_imu_samples", "cgmli_solver_refresh_imu", "cgmli_solver_read_imu",
-    "cgmli_solver_solve_gated", "cgmli_solver_read_gate",
+    "cgmli_solver_solve_gated", "cgmli_solver_read_gate", "cgmli_solver_set_imu_merge_limits", "cgmli_solver_read_merged_imu",
 ]
 KERNEL_NAMES = ["zero_acc", "linearize", "retained", "factor", "candidate", "backsub_trial", "retained_trial", "lm_update", "accept",
                 "lin_pairs", "lin_schur"]

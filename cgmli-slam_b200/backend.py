@@ -102,6 +102,16 @@ class Solver:
                "cgmli_solver_read_gate")
         return rep, mask[:n]
 
+    def set_imu_merge_limits(self, max_interval_s: float = 10.0, max_samples: int = 10000) -> None:
+        _check(lib().cgmli_solver_set_imu_merge_limits(self._h, max_interval_s, max_samples), "cgmli_solver_set_imu_merge_limits")
+
+    def read_merged_imu(self, w: int):
+        """(outcome CGMLI_IMU_MERGE_*, merged factor or None) of window w."""
+        state = C.c_int()
+        f = abi.FrozenImu()
+        _check(lib().cgmli_solver_read_merged_imu(self._h, w, C.byref(state), C.byref(f)), "cgmli_solver_read_merged_imu")
+        return state.value, (f if state.value == abi.IMU_MERGE_REINTEGRATED else None)
+
     def set_imu_samples(self, params: abi.ImuParameters, time_ns, readings, ranges, t0_ns, t1_ns) -> None:
         """Samples of the batch's IMU factors (in window order) for refresh_imu."""
         ll = C.POINTER(C.c_longlong)

@@ -177,6 +177,20 @@ struct cgmli_solver {
     DArray<int> imuRanges, imuStatus, imuRefreshed;
     DArray<cgmli_frozen_imu> imuRefreshScratch;
     std::vector<int> hImuStatus, hImuRefreshed;
+    std::vector<int> hImuRange;            // host copies of the factors' sample ranges and ends
+    std::vector<long long> hImuT0, hImuT1;
+    // SECOND_NEW with the IMU merge: per window its outcome (CGMLI_IMU_MERGE_*)
+    // and job index; per job the merged interval and the merged factor
+    double mergeMaxInterval = 10.0;
+    int mergeMaxSamples = 10000;
+    std::vector<int> mergeState, mergeJob;
+    HVec<int> hMergeRange, hMergeKf;
+    HVec<long long> hMergeT0, hMergeT1;
+    DArray<int> mergeRange, mergeKf, mergeStatus, mergeFlag;
+    DArray<long long> mergeT0, mergeT1;
+    DArray<cgmli_frozen_imu> mergeOut;
+    std::vector<int> hMergeStatus;
+    bool mergeRead = false;
     // checkpoint of the accepted states
     DArray<double> snapPose, snapSb, snapExt, snapTd, snapRho;
     bool haveSnapshot = false;
@@ -233,6 +247,8 @@ struct cgmli_solver {
         imuTimes.release(); imuT0.release(); imuT1.release(); imuReadings.release(); imuRanges.release(); imuStatus.release();
         imuRefreshed.release(); imuRefreshScratch.release();
         obRejected.release(); gateCounts.release(); gateStats.release();
+        mergeRange.release(); mergeKf.release(); mergeStatus.release(); mergeFlag.release(); mergeT0.release(); mergeT1.release();
+        mergeOut.release();
         dMargWin.release(); dMargElim.release();
         DArray<int>* mi[] = {&margCols, &margObsMap, &margPoseCol, &margSbCol, &margExtCol, &margRank, &margStatus, &margFast,
                              &margVisCol, &margVisPose, &margVisExt, &margSlow};
@@ -583,6 +599,9 @@ int cgmli_solver_set_imu_samples(cgmli_solver* S, const cgmli_imu_parameters* pa
     S->imuParams = *params;
     S->imuSampleOffset = lo;
     S->haveImuSamples = true;
+    S->hImuRange.assign(range, range + 2 * (size_t)count);
+    S->hImuT0.assign(t0_ns, t0_ns + count);
+    S->hImuT1.assign(t1_ns, t1_ns + count);
     return CGMLI_OK;
 }
 
@@ -804,9 +823,43 @@ int cgmli_solver_last_timing(cgmli_solver* S, double* ms, int* launches) {
 // factors touching the victim and the prior are consumed.  Every block a
 // consumed factor touches joins the system, frozen calibration included
 // (BackendProblem.hpp:75-80 with honorConstant=false).
+int cgmli_solver_set_imu_merge_limits(cgmli_solver* S, double max_interval_s, int max_samples) {
+    if (!S) return fail(CGMLI_E_INVALID, "null solver");
+    if (!(max_interval_s > 0) || !std::isfinite(max_interval_s) || max_samples < 4)
+        return fail(CGMLI_E_INVALID, "set_imu_merge_limits: interval must be positive and finite, samples >= 4");
+    S->mergeMaxInterval = max_interval_s;
+    S->mergeMaxSamples = max_samples;
+    return CGMLI_OK;
+}
+
+int cgmli_solver_read_merged_imu(cgmli_solver* S, int window, int* state, cgmli_frozen_imu* imu) {
+    if (!S || !S->haveMarg || !state) return fail(CGMLI_E_INVALID, "read_merged_imu: no marginalization recorded or null state");
+    if (window < 0 || window >= (int)S->mergeState.size()) return fail(CGMLI_E_INVALID, "read_merged_imu: window index");
+    CK(cudaSetDevice(S->device));
+    *state = S->mergeState[window];
+    const int job = S->mergeJob[window];
+    if (job < 0) return CGMLI_OK;
+    if (!S->mergeRead) {
+        S->hMergeStatus.resize(S->hMergeKf.size());
+        CK(cudaMemcpyAsync(S->hMergeStatus.data(), S->mergeStatus.p, S->hMergeStatus.size() * sizeof(int), cudaMemcpyDeviceToHost,
+                           S->stream));
+        CK(cudaStreamSynchronize(S->stream));
+        S->mergeRead = true;
+    }
+    if (S->hMergeStatus[job] != CGMLI_OK)
+        return fail(S->hMergeStatus[job], S->hMergeStatus[job] == CGMLI_E_INVALID ? "merged IMU interval: invalid samples"
+                                                                                   : "merged IMU interval: result not finite");
+    if (imu) {
+        CK(cudaMemcpyAsync(imu, S->mergeOut.p + job, sizeof(cgmli_frozen_imu), cudaMemcpyDeviceToHost, S->stream));
+        CK(cudaStreamSynchronize(S->stream));
+    }
+    return CGMLI_OK;
+}
+
 int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) {
     if (!S || S->win.empty() || !victim_kf) return fail(CGMLI_E_INVALID, "solver has no windows or no victim list");
-    if (policy != CGMLI_MARGIN_OLD && policy != CGMLI_MARGIN_SECOND_NEW) return fail(CGMLI_E_INVALID, "unknown marginalization policy");
+    if (policy != CGMLI_MARGIN_OLD && policy != CGMLI_MARGIN_SECOND_NEW && policy != CGMLI_MARGIN_SECOND_NEW_IMU_MERGE)
+        return fail(CGMLI_E_INVALID, "unknown marginalization policy");
     const int W = (int)S->win.size();
     for (int w = 0; w < W; ++w)
         if (victim_kf[w] < -1 || victim_kf[w] >= S->win[w].K) return fail(CGMLI_E_INVALID, "victim keyframe out of range");
@@ -822,6 +875,10 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
     };
     std::vector<MargWin> mwv(W);
     std::vector<Part> part(W);
+    // IMU merge: per window the outcome and the two edges of the victim
+    S->mergeState.assign(W, CGMLI_IMU_MERGE_NONE);
+    S->mergeJob.assign(W, -1);
+    std::vector<int2> mergeEdges(W, int2{-1, -1});
     S->sepKind.assign(W, {});
     S->sepIndex.assign(W, {});
     const HostBatch& hb = S->hb;
@@ -872,8 +929,46 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
                 tdUsed = true;
             }
         }
+        // SECOND_NEW with the IMU merge (SlidingWindowManager::prepareEviction,
+        // SlidingWindowManager.cpp:275-310): when the victim has exactly its two IMU
+        // edges left -> victim -> right, its speed/bias is not in the prior, and the
+        // edges' samples are on the device, the edges are re-integrated into one
+        // left -> right factor (mergeBodyImuRecords, BodyImuFactor.cpp:306-388) and
+        // do not enter the Schur step; otherwise they are consumed by it.
+        bool skipImu = false;
+        if (policy == CGMLI_MARGIN_SECOND_NEW_IMU_MERGE) {
+            int left = -1, right = -1, incident = 0;
+            for (int i = 0; i < d.nImu; ++i) {
+                const int k = hb.imuKf[d.imu0 + i] - d.kf0;
+                if (k + 1 == v) { left = d.imu0 + i; ++incident; }
+                else if (k == v) { right = d.imu0 + i; ++incident; }
+            }
+            bool sbInPrior = false;
+            for (int b = 0; b < d.priorBlocks; ++b)
+                sbInPrior = sbInPrior || (hb.priorKind[d.priorBlk0 + b] == CGMLI_PRIOR_SPEED_BIAS && hb.priorIndex[d.priorBlk0 + b] == d.kf0 + v);
+            S->mergeState[w] = CGMLI_IMU_MERGE_BRIDGE;
+            if (incident == 2 && left >= 0 && right >= 0 && !sbInPrior && S->haveImuSamples) {
+                const int lb = S->hImuRange[2 * left], le = S->hImuRange[2 * left + 1];
+                const int rb = S->hImuRange[2 * right], re = S->hImuRange[2 * right + 1];
+                if (S->hImuT1[left] != S->hImuT0[right] || rb < lb || rb > le || re < le) {
+                    P.status = CGMLI_E_INVALID;
+                    P.why = "IMU merge: the victim's two edges must meet at its time and share one contiguous sample range";
+                    return;
+                }
+                const long long span = S->hImuT1[right] - S->hImuT0[left];
+                const bool suppressed = (double)span * 1e-9 > S->mergeMaxInterval;
+                if (!suppressed && re - lb > S->mergeMaxSamples) {
+                    P.status = CGMLI_E_LIMIT;
+                    P.why = "IMU merge: merged interval exceeds the sample budget";
+                    return;
+                }
+                S->mergeState[w] = suppressed ? CGMLI_IMU_MERGE_SUPPRESSED : CGMLI_IMU_MERGE_REINTEGRATED;
+                mergeEdges[w] = int2{left, right};
+                skipImu = true;
+            }
+        }
         int nImu = 0;
-        for (int i = 0; i < d.nImu; ++i) {
+        for (int i = 0; i < d.nImu && !skipImu; ++i) {
             const int k = hb.imuKf[d.imu0 + i] - d.kf0;
             if (k != v && k + 1 != v) continue;
             if (nImu == 2) { P.status = CGMLI_E_LIMIT; P.why = "more than two IMU factors touch the victim keyframe"; return; }
@@ -1081,7 +1176,6 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
     CK(S->margItems.upload(items, st));
     CK(S->margSlow.upload(slow, st));
     if (!S->margUploaded) CK(cudaEventCreateWithFlags(&S->margUploaded, cudaEventDisableTiming));
-    CK(cudaEventRecord(S->margUploaded, st));
     CK(S->margH.reserve(H0)); CK(S->margB.reserve(vec0)); CK(S->margSepH.reserve(sep0)); CK(S->margSepV.reserve(sep0));
     CK(S->margSepB.reserve(vec0)); CK(S->margEvals.reserve(vec0)); CK(S->margA.reserve(sep0)); CK(S->margR0.reserve(vec0));
     CK(S->margX.reserve(x0)); CK(S->margMaxD.reserve(W)); CK(S->margStats.reserve(4ll * W));
@@ -1116,8 +1210,40 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
     S->margSepTotal = sep0;
     S->margVecTotal = vec0;
     S->margCached = false;
+    // merged IMU intervals: one job per reintegrated window
+    S->hMergeRange.clear(); S->hMergeKf.clear(); S->hMergeT0.clear(); S->hMergeT1.clear();
+    for (int w = 0; w < W; ++w) {
+        if (S->mergeState[w] != CGMLI_IMU_MERGE_REINTEGRATED) continue;
+        const int left = mergeEdges[w].x, right = mergeEdges[w].y;
+        S->mergeJob[w] = (int)S->hMergeKf.size();
+        S->hMergeRange.push_back(S->hImuRange[2 * left]);
+        S->hMergeRange.push_back(S->hImuRange[2 * right + 1]);
+        S->hMergeT0.push_back(S->hImuT0[left]);
+        S->hMergeT1.push_back(S->hImuT1[right]);
+        S->hMergeKf.push_back(hb.imuKf[left]);
+    }
+    const int jobs = (int)S->hMergeKf.size();
+    S->mergeRead = false;
+    if (jobs) {
+        CK(S->mergeRange.upload(S->hMergeRange, st)); CK(S->mergeKf.upload(S->hMergeKf, st));
+        CK(S->mergeT0.upload(S->hMergeT0, st)); CK(S->mergeT1.upload(S->hMergeT1, st));
+        CK(S->mergeStatus.reserve(jobs)); CK(S->mergeFlag.reserve(jobs)); CK(S->mergeOut.reserve(jobs));
+    }
+    CK(cudaEventRecord(S->margUploaded, st));
     CK(cudaEventRecord(S->ev0, st));
     S->lastLaunches = launchMarginalization(S->B, M, smem, st);
+    if (jobs) {
+        // at the left keyframe's accepted bias, as BodyImuCost builds the merged factor
+        ImuLaunch L{};
+        L.prm = S->imuParams;
+        L.times = S->imuTimes.p; L.readings = S->imuReadings.p; L.sampleOffset = S->imuSampleOffset;
+        L.ranges = S->mergeRange.p; L.t0s = S->mergeT0.p; L.t1s = S->mergeT1.p;
+        L.out = S->mergeOut.p; L.status = S->mergeStatus.p; L.biases = nullptr;
+        L.sb = S->sb[0].p; L.kf = S->mergeKf.p; L.force = 1;
+        L.scratch = nullptr; L.refreshed = S->mergeFlag.p;
+        CK(launchImuPreintegration(L, jobs, st));
+        S->lastLaunches += 1;
+    }
     CK(cudaGetLastError());
     CK(cudaEventRecord(S->ev1, st));
     S->haveMarg = true;

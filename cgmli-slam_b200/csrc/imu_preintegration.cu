@@ -140,13 +140,16 @@ __global__ void __launch_bounds__(kImuWarps * 32) k_imu_preintegrate(const ImuLa
         const double* x = L.sb + 9ll * L.kf[iv];
         bg = ld3(x + 3);
         ba = ld3(x + 6);
-        const double* ref = L.out[iv].reference_bias;
-        const bool drift = norm(bg - ld3(ref)) > L.gyroThreshold || norm(ba - ld3(ref + 3)) > L.accelThreshold;
-        if (!drift) {
-            if (lane == 0) { status[iv] = CGMLI_OK; L.refreshed[iv] = 0; }
-            return;
+        if (!L.force) {
+            const double* ref = L.out[iv].reference_bias;
+            const bool drift = norm(bg - ld3(ref)) > L.gyroThreshold || norm(ba - ld3(ref + 3)) > L.accelThreshold;
+            if (!drift) {
+                if (lane == 0) { status[iv] = CGMLI_OK; L.refreshed[iv] = 0; }
+                return;
+            }
         }
     }
+    const bool viaScratch = refresh && !L.force;
 
     const int b = L.ranges[2 * iv] - L.sampleOffset, n = L.ranges[2 * iv + 1] - L.ranges[2 * iv];
     const long long* ts = L.times + b;
@@ -462,7 +465,7 @@ __global__ void __launch_bounds__(kImuWarps * 32) k_imu_preintegrate(const ImuLa
         if (!rotated) break;
     }
 
-    cgmli_frozen_imu& o = refresh ? L.scratch[iv] : L.out[iv];
+    cgmli_frozen_imu& o = viaScratch ? L.scratch[iv] : L.out[iv];
     bool finiteOut = true;
     {
         double lmax = A[0];
@@ -519,7 +522,7 @@ __global__ void __launch_bounds__(kImuWarps * 32) k_imu_preintegrate(const ImuLa
         finiteOut = finiteOut && isfinite(g);
     }
     const bool anyBad = __any_sync(full, !finiteOut);
-    if (refresh) {
+    if (viaScratch) {
         // replace the factor only with a finite result
         __syncwarp();
         if (!anyBad) {
@@ -528,6 +531,8 @@ __global__ void __launch_bounds__(kImuWarps * 32) k_imu_preintegrate(const ImuLa
             for (int k = lane; k < (int)(sizeof(cgmli_frozen_imu) / sizeof(double)); k += 32) dst[k] = src[k];
         }
         if (lane == 0) L.refreshed[iv] = anyBad ? 0 : 1;
+    } else if (refresh && lane == 0) {
+        L.refreshed[iv] = anyBad ? 0 : 1;
     }
     if (lane == 0) status[iv] = anyBad ? CGMLI_E_NONFINITE : CGMLI_OK;
 }

@@ -29,6 +29,10 @@ struct ImuLaunch {
     double gyroThreshold, accelThreshold;
     cgmli_frozen_imu* scratch;
     int* refreshed;
+    // With force, every interval is integrated at the keyframe's current bias and
+    // written straight to out[i] (no drift check, no scratch): the merged IMU
+    // factor of a SECOND_NEW marginalization.
+    int force;
 };
 
 cudaError_t launchImuPreintegration(const ImuLaunch& L, int count, cudaStream_t s);

@@ -53,7 +53,12 @@ enum {
 
 enum { CGMLI_PRECISION_FP64 = 0, CGMLI_PRECISION_MIXED = 1 };
 enum { CGMLI_PRIOR_POSE = 0, CGMLI_PRIOR_SPEED_BIAS = 1, CGMLI_PRIOR_EXTRINSIC = 2, CGMLI_PRIOR_TIME_OFFSET = 3 };
-enum { CGMLI_MARGIN_OLD = 0, CGMLI_MARGIN_SECOND_NEW = 1 };
+enum { CGMLI_MARGIN_OLD = 0, CGMLI_MARGIN_SECOND_NEW = 1, CGMLI_MARGIN_SECOND_NEW_IMU_MERGE = 2 };
+/* Outcome of the IMU merge of a CGMLI_MARGIN_SECOND_NEW_IMU_MERGE marginalization. */
+enum { CGMLI_IMU_MERGE_NONE = 0,         /* no victim, or another policy */
+       CGMLI_IMU_MERGE_REINTEGRATED = 1, /* the two edges became one re-integrated factor */
+       CGMLI_IMU_MERGE_BRIDGE = 2,       /* conditions not met: the edges entered the Schur step */
+       CGMLI_IMU_MERGE_SUPPRESSED = 3 }; /* interval above the maximum: both edges dropped */
 
 /* Frozen IMU preintegration of one keyframe interval.  Same fields and
  * storage order as the reference's FrozenImuData
@@ -213,6 +218,25 @@ int cgmli_solver_kernel_times(cgmli_solver *solver, int enable, double *ms, int 
  * keyframe removed from window w; policy is CGMLI_MARGIN_OLD or
  * CGMLI_MARGIN_SECOND_NEW. */
 int cgmli_solver_marginalize(cgmli_solver *solver, const int *victim_kf, int policy);
+/* CGMLI_MARGIN_SECOND_NEW_IMU_MERGE is SECOND_NEW as the reference runs it in
+ * production (SlidingWindowManager::prepareEviction, src/backend/
+ * SlidingWindowManager.cpp:263-310, mergeBodyImuRecords, src/factor/
+ * BodyImuFactor.cpp:306-388): when the victim has exactly two IMU edges
+ * (left -> victim -> right), its speed/bias is not in the prior and the batch's
+ * samples are on the device (cgmli_solver_set_imu_samples, the two edges' ranges
+ * contiguous in one stream), the edges leave the problem instead of entering the
+ * Schur step and are replaced by one factor re-integrated over [t_left, t_right]
+ * at the left keyframe's accepted bias, computed on the device with the prior.
+ * An interval longer than the maximum duration drops both edges without a
+ * replacement (the reference's suppressed factor); otherwise the merged interval
+ * may hold at most the maximum number of samples (CGMLI_E_LIMIT).  Windows that
+ * do not meet the conditions keep the Schur bridge of CGMLI_MARGIN_SECOND_NEW.
+ * Limits default to the reference's maxImuIntervalSeconds = 10 and
+ * maxImuSamplesPerEpoch = 10000.  cgmli_solver_read_merged_imu gives window w's
+ * outcome (CGMLI_IMU_MERGE_*) and, when reintegrated, the new factor; a failed
+ * re-integration returns its CGMLI_E_* code. */
+int cgmli_solver_set_imu_merge_limits(cgmli_solver *solver, double max_interval_s, int max_samples);
+int cgmli_solver_read_merged_imu(cgmli_solver *solver, int window, int *state, cgmli_frozen_imu *imu);
 /* Result of window w: rank and separator width, then (when the buffers are
  * not NULL) the separator blocks, their ambient references, A
  * (rank x cols, row-major) and r0.  Call once with NULL buffers for sizes. */

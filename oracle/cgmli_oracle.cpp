@@ -1530,7 +1530,7 @@ struct WindowMarg {
     std::vector<int> sepKind, sepIndex;  // separator blocks in column order
     std::vector<double> sepRef;
 };
-static void marginalizeWindow(const cgmli_window& w, int victim, int policy, WindowMarg& res) {
+static void marginalizeWindow(const cgmli_window& w, int victim, int policy, WindowMarg& res, bool skipImu = false) {
     const Layout lay(w);
     const int L = lay.L;
     std::vector<char> elim(L, 0), consumeObs(w.num_observations, 0);
@@ -1554,7 +1554,7 @@ static void marginalizeWindow(const cgmli_window& w, int victim, int policy, Win
                 tdUsed = true;
             }
     std::vector<int> imuUsed;
-    for (int i = 0; i < w.num_imu; ++i)
+    for (int i = 0; i < w.num_imu && !skipImu; ++i)
         if (w.imu_kf[i] == victim || w.imu_kf[i] + 1 == victim) {
             imuUsed.push_back(i);
             const int k = w.imu_kf[i];
@@ -1673,10 +1673,82 @@ static void marginalizeWindow(const cgmli_window& w, int victim, int policy, Win
 }
 }  // namespace orc
 
+namespace orc {
+// SECOND_NEW with the IMU merge (SlidingWindowManager::prepareEviction,
+// SlidingWindowManager.cpp:263-310; mergeBodyImuRecords, BodyImuFactor.cpp:306-388).
+// Factor q of the window integrates samples [range[2q], range[2q+1]) of one
+// stream from t0[q] to t1[q].  The victim's two edges merge when they are its only
+// IMU factors and its speed/bias is not in the prior: the merged factor covers
+// [t0(left), t1(right)] at the left keyframe's bias, or, above maxInterval, both
+// edges are dropped.  skipImu tells the marginalization to leave the edges out.
+struct ImuStream {
+    const cgmli_imu_parameters* prm;
+    const long long* t;
+    const double* m;
+    int n;
+    const int* range;
+    const long long* t0;
+    const long long* t1;
+    double maxInterval;
+    int maxSamples;
+};
+static int planImuMerge(const cgmli_window& w, int victim, const ImuStream& s, int& state, cgmli_frozen_imu& merged, bool& skipImu) {
+    state = CGMLI_IMU_MERGE_BRIDGE;
+    skipImu = false;
+    int left = -1, right = -1, incident = 0;
+    for (int i = 0; i < w.num_imu; ++i) {
+        if (w.imu_kf[i] + 1 == victim) { left = i; ++incident; }
+        else if (w.imu_kf[i] == victim) { right = i; ++incident; }
+    }
+    bool sbInPrior = false;
+    for (int b = 0; b < w.prior_num_blocks; ++b)
+        sbInPrior = sbInPrior || (w.prior_block_kind[b] == CGMLI_PRIOR_SPEED_BIAS && w.prior_block_index[b] == victim);
+    if (incident != 2 || left < 0 || right < 0 || sbInPrior || !s.t) return CGMLI_OK;
+    const int lb = s.range[2 * left], le = s.range[2 * left + 1], rb = s.range[2 * right], re = s.range[2 * right + 1];
+    if (s.t1[left] != s.t0[right] || rb < lb || rb > le || re < le) return CGMLI_E_INVALID;
+    skipImu = true;
+    if (nsToSec(s.t1[right] - s.t0[left]) > s.maxInterval) {
+        state = CGMLI_IMU_MERGE_SUPPRESSED;
+        return CGMLI_OK;
+    }
+    if (re - lb > s.maxSamples) return CGMLI_E_LIMIT;
+    state = CGMLI_IMU_MERGE_REINTEGRATED;
+    const long long* t = s.t + lb;
+    const double* m = s.m + 6 * (size_t)lb;
+    if (!imuIntervalValid(t, m, re - lb, s.t0[left], s.t1[right], s.prm->max_sample_gap)) return CGMLI_E_INVALID;
+    const double* bias = w.speed_bias + 9 * w.imu_kf[left] + 3;
+    if (!preintegrateInterval(*s.prm, t, m, re - lb, s.t0[left], s.t1[right], bias, merged, nullptr)) return CGMLI_E_NONFINITE;
+    return CGMLI_OK;
+}
+}  // namespace orc
+
 // ================================ C ABI (tests / CPU baseline) =================
 extern "C" {
 
 int oracle_version(void) { return 1; }
+
+// SECOND_NEW window marginalization with the IMU merge: as
+// oracle_marginalize_window, plus the merge outcome (CGMLI_IMU_MERGE_*) and the
+// merged factor.
+int oracle_marginalize_window_merge(const cgmli_window* w, int victim, const cgmli_imu_parameters* prm, const long long* t,
+                                    const double* m, int n, const int* range, const long long* t0, const long long* t1,
+                                    double max_interval, int max_samples, int* rank, int* cols, int* num_blocks, int* block_kind,
+                                    int* block_index, double* reference, double* A, double* r0, int* state, cgmli_frozen_imu* merged) {
+    orc::ImuStream s{prm, t, m, n, range, t0, t1, max_interval, max_samples};
+    bool skipImu = false;
+    const int st = orc::planImuMerge(*w, victim, s, *state, *merged, skipImu);
+    if (st != CGMLI_OK) return st;
+    orc::WindowMarg res;
+    orc::marginalizeWindow(*w, victim, CGMLI_MARGIN_SECOND_NEW, res, skipImu);
+    if (res.out.status != CGMLI_OK) return res.out.status;
+    *rank = res.out.rank; *cols = res.out.nr; *num_blocks = (int)res.sepKind.size();
+    if (block_kind) std::copy(res.sepKind.begin(), res.sepKind.end(), block_kind);
+    if (block_index) std::copy(res.sepIndex.begin(), res.sepIndex.end(), block_index);
+    if (reference) std::copy(res.sepRef.begin(), res.sepRef.end(), reference);
+    if (A) std::copy(res.out.A.begin(), res.out.A.end(), A);
+    if (r0) std::copy(res.out.r0.begin(), res.out.r0.end(), r0);
+    return CGMLI_OK;
+}
 
 // LM solve with the NIS gate and outlier refits; gate: {passes, rejected
 // before the first solve, evaluated by the last gate, rejected by it, rejected

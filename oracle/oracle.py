@@ -64,6 +64,9 @@ def lib() -> C.CDLL:
         P(L, "oracle_lm_solve_gated", C.c_int,
           [W, C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(abi.SolveReport), ip, dp, C.POINTER(C.c_ubyte)])
         ll = C.POINTER(C.c_longlong)
+        P(L, "oracle_marginalize_window_merge", C.c_int,
+          [W, C.c_int, C.POINTER(abi.ImuParameters), ll, dp, C.c_int, ip, ll, ll, C.c_double, C.c_int, ip, ip, ip, ip, ip, dp, dp, dp,
+           ip, C.POINTER(abi.FrozenImu)])
         P(L, "oracle_imu_preintegrate", C.c_int,
           [C.POINTER(abi.ImuParameters), ll, dp, C.c_int, ip, ll, ll, dp, C.c_int, C.POINTER(abi.FrozenImu), dp])
         _LIB = L
@@ -201,3 +204,30 @@ def lm_solve_gated(win, iterations, threshold=9.210340371976184, max_refits=3, p
     g = dict(passes=int(gate[0]), rejected_pre=int(gate[1]), evaluated=int(gate[2]), rejected_last=int(gate[3]),
              rejected_total=int(gate[4]), nis_sum=float(nis[0]), nis_max=float(nis[1]))
     return st, rep, g, mask[:win.num_observations]
+
+
+def marginalize_window_merge(win, victim, params, time_ns, readings, ranges, t0_ns, t1_ns, max_interval=10.0, max_samples=10000):
+    """SECOND_NEW marginalization with the IMU merge; the prior (as
+    marginalize_window, without H/b) plus 'merge' (CGMLI_IMU_MERGE_*) and
+    'merged' (the re-integrated factor or None)."""
+    ll = C.POINTER(C.c_longlong)
+    time_ns = np.ascontiguousarray(time_ns, dtype=np.int64)
+    readings = np.ascontiguousarray(readings, dtype=np.float64)
+    ranges = np.ascontiguousarray(ranges, dtype=np.int32)
+    t0_ns = np.ascontiguousarray(t0_ns, dtype=np.int64)
+    t1_ns = np.ascontiguousarray(t1_ns, dtype=np.int64)
+    rank, cols, nb, state = (np.zeros(1, np.int32) for _ in range(4))
+    merged = abi.FrozenImu()
+    args = (C.byref(win), victim, C.byref(params), time_ns.ctypes.data_as(ll), _p(readings), len(time_ns),
+            ranges.ctypes.data_as(ip), t0_ns.ctypes.data_as(ll), t1_ns.ctypes.data_as(ll), max_interval, max_samples,
+            rank.ctypes.data_as(ip), cols.ctypes.data_as(ip), nb.ctypes.data_as(ip))
+    st = lib().oracle_marginalize_window_merge(*args, None, None, None, None, None, state.ctypes.data_as(ip), C.byref(merged))
+    if st != 0:
+        return dict(status=st)
+    k, m, b = int(rank[0]), int(cols[0]), int(nb[0])
+    kinds, idx = np.zeros(b, np.int32), np.zeros(b, np.int32)
+    ref = np.zeros(9 * b + 1); A = np.zeros(k * m); r0 = np.zeros(k)
+    st = lib().oracle_marginalize_window_merge(*args, kinds.ctypes.data_as(ip), idx.ctypes.data_as(ip), _p(ref), _p(A), _p(r0),
+                                               state.ctypes.data_as(ip), C.byref(merged))
+    return dict(status=st, rank=k, cols=m, kinds=kinds, index=idx, reference=ref, A=A.reshape(k, m), r0=r0,
+                merge=int(state[0]), merged=merged if int(state[0]) == abi.IMU_MERGE_REINTEGRATED else None)
