@@ -157,6 +157,9 @@ def declare_backend(lib: C.CDLL) -> C.CDLL:
     _proto(lib, "cgmli_solver_solve_gated", C.c_int, [S, C.c_int, C.c_double, C.c_int, C.c_int])
     _proto(lib, "cgmli_solver_set_imu_merge_limits", C.c_int, [S, C.c_double, C.c_int])
     _proto(lib, "cgmli_solver_read_merged_imu", C.c_int, [S, C.c_int, c_int_p, C.POINTER(FrozenImu)])
+    _proto(lib, "cgmli_solver_calibration_information", C.c_int, [S, C.c_int])
+    _proto(lib, "cgmli_solver_read_calibration_information", C.c_int,
+           [S, C.c_int, c_int_p, c_int_p, c_int_p, c_int_p, c_double_p, c_double_p])
     _proto(lib, "cgmli_solver_read_gate", C.c_int, [S, C.c_int, C.POINTER(GateReport), C.POINTER(C.c_ubyte)])
     return lib
 
@@ -182,6 +185,7 @@ BACKEND_SYMBOLS = [
     "cgmli_server_read_prior", "cgmli_server_release", "cgmli_server_replay", "cgmli_imu_preintegrate",
     "cgmli_imu_last_timing", "cgmli_solver_set_imu_samples", "cgmli_solver_refresh_imu", "cgmli_solver_read_imu",
     "cgmli_solver_solve_gated", "cgmli_solver_read_gate", "cgmli_solver_set_imu_merge_limits", "cgmli_solver_read_merged_imu",
+    "cgmli_solver_calibration_information", "cgmli_solver_read_calibration_information",
 ]
 KERNEL_NAMES = ["zero_acc", "linearize", "retained", "factor", "candidate", "backsub_trial", "retained_trial", "lm_update", "accept",
                 "lin_pairs", "lin_schur"]

@@ -102,6 +102,22 @@ class Solver:
                "cgmli_solver_read_gate")
         return rep, mask[:n]
 
+    def calibration_information(self, include_prior: bool = False) -> None:
+        _check(lib().cgmli_solver_calibration_information(self._h, int(include_prior)), "cgmli_solver_calibration_information")
+
+    def read_calibration_information(self, w: int) -> dict:
+        """Conditional calibration information of window w: blocks, matrix, eigenvalues."""
+        size, nb = C.c_int(), C.c_int()
+        code = lib().cgmli_solver_read_calibration_information(self._h, w, C.byref(size), C.byref(nb), None, None, None, None)
+        if code != 0:
+            return dict(status=code)
+        n, b = size.value, nb.value
+        kinds, idx = np.zeros(max(b, 1), np.int32), np.zeros(max(b, 1), np.int32)
+        cond, ev = np.zeros(max(n * n, 1)), np.zeros(max(n, 1))
+        code = lib().cgmli_solver_read_calibration_information(self._h, w, C.byref(size), C.byref(nb), kinds.ctypes.data_as(abi.c_int_p),
+                                                               idx.ctypes.data_as(abi.c_int_p), _p(cond), _p(ev))
+        return dict(status=code, kinds=kinds[:b], index=idx[:b], conditional=cond[:n * n].reshape(n, n), eigenvalues=ev[:n])
+
     def set_imu_merge_limits(self, max_interval_s: float = 10.0, max_samples: int = 10000) -> None:
         _check(lib().cgmli_solver_set_imu_merge_limits(self._h, max_interval_s, max_samples), "cgmli_solver_set_imu_merge_limits")
 

@@ -39,6 +39,8 @@ int margRowsCap(int nv);
 cudaError_t configureMarginalization(size_t visualSmem, size_t rowsSmem, int maxNr, int maxFastNr, long long* eigenSmem,
                                      long long* fastSmem);
 int launchMarginalization(const DevBatch& B, const MargBatch& M, size_t visualSmem, cudaStream_t s);
+int launchCalibration(const DevBatch& B, const MargBatch& M, size_t visualSmem, double* work, const long long* work0, double* cond,
+                      double* evals, cudaStream_t s);
 void launchDenseEigen(const double* H, int n, double* work, double* evals, double* evecs, int* status, cudaStream_t s);
 void launchDensePsd(const double* evals, const double* U, const double* rhs, int n, int columns, double absCut, double relCut,
                     double* projected, double* solution, int* status, cudaStream_t s);
@@ -191,6 +193,12 @@ struct cgmli_solver {
     DArray<cgmli_frozen_imu> mergeOut;
     std::vector<int> hMergeStatus;
     bool mergeRead = false;
+    // conditional calibration information (the marginalization's formation in
+    // calibration mode): per-window work offsets, results
+    bool haveCalib = false;
+    HVec<long long> hCalibWork0;
+    DArray<long long> calibWork0;
+    DArray<double> calibWork, calibCond, calibEvals;
     // checkpoint of the accepted states
     DArray<double> snapPose, snapSb, snapExt, snapTd, snapRho;
     bool haveSnapshot = false;
@@ -249,6 +257,7 @@ struct cgmli_solver {
         obRejected.release(); gateCounts.release(); gateStats.release();
         mergeRange.release(); mergeKf.release(); mergeStatus.release(); mergeFlag.release(); mergeT0.release(); mergeT1.release();
         mergeOut.release();
+        calibWork0.release(); calibWork.release(); calibCond.release(); calibEvals.release();
         dMargWin.release(); dMargElim.release();
         DArray<int>* mi[] = {&margCols, &margObsMap, &margPoseCol, &margSbCol, &margExtCol, &margRank, &margStatus, &margFast,
                              &margVisCol, &margVisPose, &margVisExt, &margSlow};
@@ -856,6 +865,12 @@ int cgmli_solver_read_merged_imu(cgmli_solver* S, int window, int* state, cgmli_
     return CGMLI_OK;
 }
 
+// The Schur formation shared by the marginalization and the calibration
+// information.  calib: every landmark eliminated, every IMU factor (and the
+// prior when includePrior) consumed, poses and speed/biases as the nuisance
+// block [0, nm), the calibration blocks as the separator; no victim.
+static int marginalizeImpl(cgmli_solver* S, const int* victim_kf, int policy, bool calib, bool includePrior);
+
 int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) {
     if (!S || S->win.empty() || !victim_kf) return fail(CGMLI_E_INVALID, "solver has no windows or no victim list");
     if (policy != CGMLI_MARGIN_OLD && policy != CGMLI_MARGIN_SECOND_NEW && policy != CGMLI_MARGIN_SECOND_NEW_IMU_MERGE)
@@ -863,6 +878,42 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
     const int W = (int)S->win.size();
     for (int w = 0; w < W; ++w)
         if (victim_kf[w] < -1 || victim_kf[w] >= S->win[w].K) return fail(CGMLI_E_INVALID, "victim keyframe out of range");
+    return marginalizeImpl(S, victim_kf, policy, false, false);
+}
+
+int cgmli_solver_calibration_information(cgmli_solver* S, int include_prior) {
+    if (!S || S->win.empty()) return fail(CGMLI_E_INVALID, "solver has no windows");
+    return marginalizeImpl(S, nullptr, CGMLI_MARGIN_OLD, true, include_prior != 0);
+}
+
+int cgmli_solver_read_calibration_information(cgmli_solver* S, int window, int* size, int* num_blocks, int* block_kind,
+                                              int* block_index, double* conditional, double* eigenvalues) {
+    if (!S || !S->haveCalib) return fail(CGMLI_E_INVALID, "no calibration information recorded");
+    if (window < 0 || window >= (int)S->margWin.size() || !size || !num_blocks) return fail(CGMLI_E_INVALID, "read_calibration_information: window index or null sizes");
+    CK(cudaSetDevice(S->device));
+    const MargWin& mw = S->margWin[window];
+    int status = CGMLI_OK;
+    CK(cudaMemcpyAsync(&status, S->margStatus.p + window, sizeof(int), cudaMemcpyDeviceToHost, S->stream));
+    CK(cudaStreamSynchronize(S->stream));
+    if (status != CGMLI_OK)
+        return fail(status, status == CGMLI_E_INDEFINITE ? "calibration information is indefinite"
+                            : status == CGMLI_E_INVALID ? "no calibration Jacobians in the window's factors"
+                                                        : "calibration information: invalid factor or non-finite result");
+    *size = mw.m ? mw.nr : 0;
+    *num_blocks = mw.m ? (int)S->sepKind[window].size() : 0;
+    if (!mw.m) return CGMLI_OK;
+    if (block_kind) std::copy(S->sepKind[window].begin(), S->sepKind[window].end(), block_kind);
+    if (block_index) std::copy(S->sepIndex[window].begin(), S->sepIndex[window].end(), block_index);
+    if (conditional)
+        CK(cudaMemcpyAsync(conditional, S->calibCond.p + mw.sep0, (size_t)mw.nr * mw.nr * sizeof(double), cudaMemcpyDeviceToHost, S->stream));
+    if (eigenvalues)
+        CK(cudaMemcpyAsync(eigenvalues, S->calibEvals.p + 2 * mw.vec0, mw.nr * sizeof(double), cudaMemcpyDeviceToHost, S->stream));
+    CK(cudaStreamSynchronize(S->stream));
+    return CGMLI_OK;
+}
+
+static int marginalizeImpl(cgmli_solver* S, const int* victim_kf, int policy, bool calib, bool includePrior) {
+    const int W = (int)S->win.size();
     CK(cudaSetDevice(S->device));
     // ---- phase A (parallel over windows): elimination set, columns, local maps
     struct Part {
@@ -896,7 +947,7 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
     visExt.resize(S->totalExt);
     parallelFor(W, 0, [&](int w) {
         const WinDesc& d = S->win[w];
-        const int v = victim_kf[w];
+        const int v = calib ? -1 : victim_kf[w];
         MargWin& mw = mwv[w];
         Part& P = part[w];
         mw = MargWin{};
@@ -904,20 +955,20 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
         mw.tdCol = -1;
         mw.visTd = -1;
         mw.huber = d.huber;
-        mw.hasPrior = d.priorRank > 0;
+        mw.hasPrior = (!calib || includePrior) && d.priorRank > 0;
         std::fill(&poseCol[d.kf0], &poseCol[d.kf0] + d.K, -1);
         std::fill(&sbCol[d.kf0], &sbCol[d.kf0] + d.K, -1);
         std::fill(&extCol[d.ext0], &extCol[d.ext0] + d.E, -1);
         std::fill(&visPose[d.kf0], &visPose[d.kf0] + d.K, -1);
         std::fill(&visExt[d.ext0], &visExt[d.ext0] + d.E, -1);
-        if (v < 0) return;
+        if (v < 0 && !calib) return;
         std::vector<char> poseUsed(d.K, 0), sbUsed(d.K, 0), extUsed(d.E, 0);
         bool tdUsed = false;
         std::vector<int> elimLm;
         for (int q = 0; q < d.L; ++q) {
             const int g = d.lm0 + q, a = hb.lmKf[g] - d.kf0;
-            bool e = a == v;
-            for (int f = hb.lmObsBegin[g]; f < hb.lmObsBegin[g + 1] && !e && policy == CGMLI_MARGIN_OLD; ++f)
+            bool e = calib ? hb.lmObsBegin[g + 1] > hb.lmObsBegin[g] : a == v;
+            for (int f = hb.lmObsBegin[g]; f < hb.lmObsBegin[g + 1] && !e && !calib && policy == CGMLI_MARGIN_OLD; ++f)
                 e = hb.obKf[f] - d.kf0 == v;
             if (!e) continue;
             elimLm.push_back(g);
@@ -967,6 +1018,14 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
                 skipImu = true;
             }
         }
+        if (calib) {
+            mw.imuAll = 1;
+            skipImu = true;
+            for (int i = 0; i < d.nImu; ++i) {
+                const int k = hb.imuKf[d.imu0 + i] - d.kf0;
+                poseUsed[k] = poseUsed[k + 1] = sbUsed[k] = sbUsed[k + 1] = 1;
+            }
+        }
         int nImu = 0;
         for (int i = 0; i < d.nImu && !skipImu; ++i) {
             const int k = hb.imuKf[d.imu0 + i] - d.kf0;
@@ -975,23 +1034,32 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
             mw.imu[nImu++] = d.imu0 + i;
             poseUsed[k] = poseUsed[k + 1] = sbUsed[k] = sbUsed[k + 1] = 1;
         }
-        for (int b = 0; b < d.priorBlocks; ++b) {
+        for (int b = 0; b < (mw.hasPrior ? d.priorBlocks : 0); ++b) {
             const int kind = hb.priorKind[d.priorBlk0 + b], gi = hb.priorIndex[d.priorBlk0 + b];
             if (kind == CGMLI_PRIOR_POSE) poseUsed[gi - d.kf0] = 1;
             else if (kind == CGMLI_PRIOR_SPEED_BIAS) sbUsed[gi - d.kf0] = 1;
             else if (kind == CGMLI_PRIOR_EXTRINSIC) extUsed[gi - d.ext0] = 1;
             else tdUsed = true;
         }
-        // columns: victim first, then the separator in block order
+        // columns: victim first, then the separator in block order (calibration
+        // information: every pose and speed/bias first, the calibration as separator)
         int n = 0;
-        if (poseUsed[v]) { poseCol[d.kf0 + v] = n; n += 6; }
-        if (sbUsed[v]) { sbCol[d.kf0 + v] = n; n += 9; }
-        mw.nm = n;
         auto sep = [&](int kind, int index) { S->sepKind[w].push_back(kind); S->sepIndex[w].push_back(index); };
-        for (int k = 0; k < d.K; ++k) {
-            if (k == v) continue;
-            if (poseUsed[k]) { poseCol[d.kf0 + k] = n; n += 6; sep(CGMLI_PRIOR_POSE, k); }
-            if (sbUsed[k]) { sbCol[d.kf0 + k] = n; n += 9; sep(CGMLI_PRIOR_SPEED_BIAS, k); }
+        if (calib) {
+            for (int k = 0; k < d.K; ++k) {
+                if (poseUsed[k]) { poseCol[d.kf0 + k] = n; n += 6; }
+                if (sbUsed[k]) { sbCol[d.kf0 + k] = n; n += 9; }
+            }
+            mw.nm = n;
+        } else {
+            if (poseUsed[v]) { poseCol[d.kf0 + v] = n; n += 6; }
+            if (sbUsed[v]) { sbCol[d.kf0 + v] = n; n += 9; }
+            mw.nm = n;
+            for (int k = 0; k < d.K; ++k) {
+                if (k == v) continue;
+                if (poseUsed[k]) { poseCol[d.kf0 + k] = n; n += 6; sep(CGMLI_PRIOR_POSE, k); }
+                if (sbUsed[k]) { sbCol[d.kf0 + k] = n; n += 9; sep(CGMLI_PRIOR_SPEED_BIAS, k); }
+            }
         }
         for (int e = 0; e < d.E; ++e)
             if (extUsed[e]) { extCol[d.ext0 + e] = n; n += 6; sep(CGMLI_PRIOR_EXTRINSIC, e); }
@@ -999,12 +1067,13 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
         mw.m = n;
         mw.nr = n - mw.nm;
         if (mw.nr > kMargMaxSep) { P.status = CGMLI_E_LIMIT; P.why = "marginalization separator above 1024 columns"; return; }
+        if (calib && mw.nm > kMargMaxSep) { P.status = CGMLI_E_LIMIT; P.why = "calibration information: more than 1024 nuisance columns"; return; }
         // visual columns (poses, extrinsics, td) in column order
         auto addVis = [&](int col, int width) {
             for (int c = 0; c < width; ++c) P.visCols.push_back(col + c);
             return (int)P.visCols.size() - width;
         };
-        if (poseUsed[v]) visPose[d.kf0 + v] = addVis(poseCol[d.kf0 + v], 6);
+        if (v >= 0 && poseUsed[v]) visPose[d.kf0 + v] = addVis(poseCol[d.kf0 + v], 6);
         for (int k = 0; k < d.K; ++k)
             if (k != v && poseUsed[k]) visPose[d.kf0 + k] = addVis(poseCol[d.kf0 + k], 6);
         for (int e = 0; e < d.E; ++e)
@@ -1229,9 +1298,27 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
         CK(S->mergeT0.upload(S->hMergeT0, st)); CK(S->mergeT1.upload(S->hMergeT1, st));
         CK(S->mergeStatus.reserve(jobs)); CK(S->mergeFlag.reserve(jobs)); CK(S->mergeOut.reserve(jobs));
     }
+    if (calib) {
+        // per window 2 nx^2 + 2 nx nc + 4 nc^2 doubles of work; results at the
+        // separator offsets (nc^2) and 2x the vector offsets (eigenvalues)
+        S->hCalibWork0.resize(W);
+        long long work = 0;
+        for (int w = 0; w < W; ++w) {
+            const long long nx = mwv[w].nm, nc = mwv[w].nr;
+            S->hCalibWork0[w] = work;
+            work += 2 * nx * nx + 2 * nx * nc + 4 * nc * nc;
+        }
+        CK(S->calibWork0.upload(S->hCalibWork0, st));
+        CK(S->calibWork.reserve(std::max(work, 1ll)));
+        CK(S->calibCond.reserve(std::max(sep0, 1ll)));
+        CK(S->calibEvals.reserve(std::max(2 * vec0, 1ll)));
+    }
     CK(cudaEventRecord(S->margUploaded, st));
     CK(cudaEventRecord(S->ev0, st));
-    S->lastLaunches = launchMarginalization(S->B, M, smem, st);
+    if (calib)
+        S->lastLaunches = launchCalibration(S->B, M, smem, S->calibWork.p, S->calibWork0.p, S->calibCond.p, S->calibEvals.p, st);
+    else
+        S->lastLaunches = launchMarginalization(S->B, M, smem, st);
     if (jobs) {
         // at the left keyframe's accepted bias, as BodyImuCost builds the merged factor
         ImuLaunch L{};
@@ -1246,7 +1333,9 @@ int cgmli_solver_marginalize(cgmli_solver* S, const int* victim_kf, int policy) 
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(S->ev1, st));
-    S->haveMarg = true;
+    // the formation buffers now hold one or the other result
+    S->haveMarg = !calib;
+    S->haveCalib = calib;
     return CGMLI_OK;
 }
 

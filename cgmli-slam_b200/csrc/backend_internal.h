@@ -132,6 +132,7 @@ struct MargWin {
     int vis0;               // offset of the window's visual -> marginalization column map
     int visTd;              // visual column of td or -1
     int rowsPath;           // 1: eliminated landmarks accumulate through dense rows (nv <= kRowsMaxN)
+    int imuAll;             // 1: every IMU factor of the window is consumed (calibration information)
 };
 struct MargElim { int lm, win, nc, col0, obs0; };  // device landmark, window, local columns, offsets
 struct MargBatch {

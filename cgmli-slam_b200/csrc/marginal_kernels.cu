@@ -453,40 +453,48 @@ __global__ void __launch_bounds__(256) k_marg_retained(DevBatch B, MargBatch M) 
     __syncthreads();
     const cgmli_frozen_imu* imus = reinterpret_cast<const cgmli_frozen_imu*>(B.imu);
     double cost = 0;
-    if (threadIdx.x < 2 && mw.imu[threadIdx.x] >= 0) {
-        const int gi = mw.imu[threadIdx.x], k = B.imuKf[gi];
-        double* r = sc + 465 * threadIdx.x;
-        if (!evalImu(imus[gi], B.pose[0] + 7ll * k, B.sb[0] + 9ll * k, B.pose[0] + 7ll * (k + 1), B.sb[0] + 9ll * (k + 1), r, r + 15))
-            bad = 1;
-        else
-            for (int i = 0; i < 15; ++i) cost += 0.5 * r[i] * r[i];
-    }
-    __syncthreads();
-    for (int q = 0; q < 2; ++q) {
-        if (mw.imu[q] < 0 || bad) continue;
-        const int k = B.imuKf[mw.imu[q]];
-        const double* r = sc + 465 * q;
-        const double* J = r + 15;
-        auto colOf = [&](int a) {
-            return a < 6 ? M.poseCol[k] + a : a < 15 ? M.sbCol[k] + a - 6 : a < 21 ? M.poseCol[k + 1] + a - 15 : M.sbCol[k + 1] + a - 21;
-        };
-        for (int e = threadIdx.x; e < 930; e += blockDim.x) {
-            if (e < 900) {
-                const int a = e / 30, c = e % 30, ca = colOf(a), cc = colOf(c);
-                if (ca > cc) continue;  // upper triangle: each unordered pair once
-                double v = 0;
-                for (int i = 0; i < 15; ++i) v += J[30 * i + a] * J[30 * i + c];
-                H[(long long)ca * m + cc] += v;
-            } else {
-                const int a = e - 900;
-                double v = 0;
-                for (int i = 0; i < 15; ++i) v += J[30 * i + a] * r[i];
-                g[colOf(a)] += v;
-            }
+    // the consumed IMU factors: the victim's (at most two), or every factor of the
+    // window (imuAll); evaluated two at a time into the scratch
+    const int nImu = mw.imuAll ? wd.nImu : 2;
+    auto factorAt = [&](int q) { return mw.imuAll ? (q < nImu ? wd.imu0 + q : -1) : mw.imu[q]; };
+    for (int q0 = 0; q0 < nImu; q0 += 2) {
+        if (threadIdx.x < 2 && factorAt(q0 + threadIdx.x) >= 0) {
+            const int gi = factorAt(q0 + threadIdx.x), k = B.imuKf[gi];
+            double* r = sc + 465 * threadIdx.x;
+            if (!evalImu(imus[gi], B.pose[0] + 7ll * k, B.sb[0] + 9ll * k, B.pose[0] + 7ll * (k + 1), B.sb[0] + 9ll * (k + 1), r,
+                         r + 15))
+                bad = 1;
+            else
+                for (int i = 0; i < 15; ++i) cost += 0.5 * r[i] * r[i];
         }
         __syncthreads();
+        for (int q = 0; q < 2; ++q) {
+            if (factorAt(q0 + q) < 0 || bad) continue;
+            const int k = B.imuKf[factorAt(q0 + q)];
+            const double* r = sc + 465 * q;
+            const double* J = r + 15;
+            auto colOf = [&](int a) {
+                return a < 6 ? M.poseCol[k] + a : a < 15 ? M.sbCol[k] + a - 6 : a < 21 ? M.poseCol[k + 1] + a - 15 : M.sbCol[k + 1] + a - 21;
+            };
+            for (int e = threadIdx.x; e < 930; e += blockDim.x) {
+                if (e < 900) {
+                    const int a = e / 30, c = e % 30, ca = colOf(a), cc = colOf(c);
+                    if (ca > cc) continue;  // upper triangle: each unordered pair once
+                    double v = 0;
+                    for (int i = 0; i < 15; ++i) v += J[30 * i + a] * J[30 * i + c];
+                    H[(long long)ca * m + cc] += v;
+                } else {
+                    const int a = e - 900;
+                    double v = 0;
+                    for (int i = 0; i < 15; ++i) v += J[30 * i + a] * r[i];
+                    g[colOf(a)] += v;
+                }
+            }
+            __syncthreads();
+        }
+        __syncthreads();  // the scratch is rewritten by the next pair
     }
-    if (wd.priorRank > 0 && !bad) {
+    if (mw.hasPrior && wd.priorRank > 0 && !bad) {
         const int rank = wd.priorRank, cols = wd.priorCols;
         double* ps = B.priorScratch + wd.priorScratch0;
         double* delta = ps;
@@ -1281,6 +1289,171 @@ __global__ void __launch_bounds__(kEigenThreads) k_marg_eigen(MargBatch M) {
 }
 
 // ---------------------------------------------------------------------------------------
+// Conditional information of the calibration blocks given every other state of
+// the window (BackendOptimizer::calibrationInformation,
+// BackendOptimizer.cpp:1084-1170), one CTA per window.  The formation kernels
+// have left H over [nuisance (poses, speed/biases) | calibration (extrinsics, td)]
+// with every landmark range eliminated; here
+//   C = Hcc - Hxc^T pinv(Hxx) Hxc,   pinv with the cutoff max(1e-12, 1e-9 lambda_max)
+// (Marginalizer::psdSolve; significantly negative eigenvalues are an error),
+// reported per extrinsic block as [theta, p] (the left-SE(3) tangent [rho, theta]
+// reordered, then dp = rho - [p]x dtheta: C' = B^T C B with B(p rows, theta cols)
+// = [p]x), td last; symmetrized, eigen-decomposed, negative round-off clamped.
+// work holds per window 2 nx^2 + 2 nx nc + 4 nc^2 doubles from work0[w].
+constexpr int kCalibMaxCols = 64;
+__global__ void __launch_bounds__(kMargThreads) k_calib_conditional(DevBatch B, MargBatch M, double* work, const long long* work0,
+                                                                  double* cond, double* evals) {
+    const int w = blockIdx.x;
+    const MargWin mw = M.win[w];
+    const int m = mw.m, nx = mw.nm, nc = mw.nr;
+    if (m == 0 || M.status[w] != CGMLI_OK) return;
+    if (nc == 0 || nc > kCalibMaxCols) {
+        if (threadIdx.x == 0) M.status[w] = nc == 0 ? CGMLI_E_INVALID : CGMLI_E_LIMIT;
+        return;
+    }
+    const WinDesc wd = B.win[w];
+    const double* H = M.H + mw.H0;
+    double* A = work + work0[w];
+    double* V = A + (long long)nx * nx;
+    double* P = V + (long long)nx * nx;  // nx x nc
+    double* X = P + (long long)nx * nc;  // nx x nc
+    double* Cr = X + (long long)nx * nc; // nc x nc
+    double* V2 = Cr + nc * nc;           // nc x nc
+    double* Cs = V2 + nc * nc;           // nc x nc
+    double* Bt = Cs + nc * nc;           // nc x nc
+    __shared__ double red[kMargThreads / 32];
+    __shared__ int report[kCalibMaxCols], extOf[kCalibMaxCols], blockStart[kCalibMaxCols], pos[kCalibMaxCols];
+    // separator layout: extrinsic blocks in index order, then td
+    if (threadIdx.x == 0) {
+        for (int j = 0; j < nc; ++j) { extOf[j] = -1; blockStart[j] = j; report[j] = j; }
+        for (int e = 0; e < wd.E; ++e) {
+            const int c = M.extCol[wd.ext0 + e];
+            if (c < nx) continue;
+            const int s0 = c - nx;
+            for (int t = 0; t < 6; ++t) {
+                extOf[s0 + t] = wd.ext0 + e;
+                blockStart[s0 + t] = s0;
+                report[s0 + t] = s0 + (t < 3 ? 3 + t : t - 3);  // [rho, theta] -> [theta, rho]
+            }
+        }
+    }
+    // 1. pseudo-inverse of the nuisance block applied to the coupling
+    for (long long t = threadIdx.x; t < (long long)nx * nx; t += blockDim.x) A[t] = symAt(H, (int)(t / nx), (int)(t % nx), m);
+    __syncthreads();
+    if (nx > 0) jacobiEigen(A, V, nx, 60);
+    __syncthreads();
+    double vmax = -INFINITY, vmin = INFINITY;
+    bool finite = true;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        const double v = A[(long long)i * nx + i];
+        vmax = fmax(vmax, v);
+        vmin = fmin(vmin, v);
+        finite = finite && isfinite(v);
+    }
+    vmax = mBlockMax(vmax, red);
+    vmin = -mBlockMax(-vmin, red);
+    const double bad = mBlockMax(finite ? 0.0 : 1.0, red);
+    const double cut = fmax(1e-12, 1e-9 * fmax(0.0, vmax));
+    if (bad > 0 || (nx > 0 && vmin < -10 * cut)) {
+        if (threadIdx.x == 0) M.status[w] = bad > 0 ? CGMLI_E_NONFINITE : CGMLI_E_INDEFINITE;
+        return;
+    }
+    for (long long t = threadIdx.x; t < (long long)nx * nc; t += blockDim.x) {
+        const int i = (int)(t / nc), c = (int)(t % nc);
+        const double lam = A[(long long)i * nx + i];
+        double v = 0;
+        if (lam > cut) {
+            for (int k = 0; k < nx; ++k) v += V[(long long)k * nx + i] * symAt(H, k, nx + c, m);
+            v /= lam;
+        }
+        P[t] = v;
+    }
+    __syncthreads();
+    for (long long t = threadIdx.x; t < (long long)nx * nc; t += blockDim.x) {
+        const int k = (int)(t / nc), c = (int)(t % nc);
+        double v = 0;
+        for (int i = 0; i < nx; ++i) v += V[(long long)k * nx + i] * P[(long long)i * nc + c];
+        X[t] = v;
+    }
+    __syncthreads();
+    // 2. C = Hcc - Hxc^T X, in report order
+    for (int t = threadIdx.x; t < nc * nc; t += blockDim.x) {
+        const int a = t / nc, c = t % nc;
+        double v = symAt(H, nx + a, nx + c, m);
+        for (int k = 0; k < nx; ++k) v -= symAt(H, k, nx + a, m) * X[(long long)k * nc + c];
+        Cs[report[a] * nc + report[c]] = v;
+    }
+    __syncthreads();
+    // 3. C' = B^T C B, B = I except [p]x in (p rows, theta cols) of each extrinsic block
+    auto basis = [&](int r, int c) -> double {  // B(r, c), report order
+        if (r == c) return 1.0;
+        const int e = extOf[r];
+        if (e < 0 || extOf[c] != e) return 0.0;
+        const int s0 = blockStart[r], i = r - s0, j = c - s0;
+        if (i < 3 || j >= 3) return 0.0;
+        const double* p = B.ext[0] + 7ll * e;  // [p]x (i - 3, j)
+        const int a = i - 3;
+        if (a == j) return 0.0;
+        const double pk = p[3 - a - j];
+        return (a + 1) % 3 == j ? -pk : pk;
+    };
+    for (int t = threadIdx.x; t < nc * nc; t += blockDim.x) {  // Bt = B^T C
+        const int r = t / nc, c = t % nc;
+        double v = 0;
+        for (int k = 0; k < nc; ++k) v += basis(k, r) * Cs[k * nc + c];
+        Bt[t] = v;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < nc * nc; t += blockDim.x) {  // Cr = Bt B
+        const int r = t / nc, c = t % nc;
+        double v = 0;
+        for (int k = 0; k < nc; ++k) v += Bt[r * nc + k] * basis(k, c);
+        Cr[t] = v;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < nc * nc; t += blockDim.x) {  // symmetrize
+        const int r = t / nc, c = t % nc;
+        Cs[t] = 0.5 * Cr[t] + 0.5 * Cr[c * nc + r];
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < nc * nc; t += blockDim.x) Cr[t] = Cs[t];
+    __syncthreads();
+    // 4. eigen-decomposition, clamp, recompose
+    jacobiEigen(Cr, V2, nc, 60);
+    __syncthreads();
+    double emax = -INFINITY, emin = INFINITY;
+    finite = true;
+    for (int i = threadIdx.x; i < nc; i += blockDim.x) {
+        const double v = Cr[i * nc + i];
+        emax = fmax(emax, v);
+        emin = fmin(emin, v);
+        finite = finite && isfinite(v);
+    }
+    emax = mBlockMax(emax, red);
+    emin = -mBlockMax(-emin, red);
+    const double bad2 = mBlockMax(finite ? 0.0 : 1.0, red);
+    const double cut2 = fmax(1e-12, 1e-9 * fmax(0.0, emax));
+    if (bad2 > 0 || emin < -10 * cut2) {
+        if (threadIdx.x == 0) M.status[w] = bad2 > 0 ? CGMLI_E_NONFINITE : CGMLI_E_INDEFINITE;
+        return;
+    }
+    double* ev = evals + 2 * mw.vec0;  // 2 m per window: sorted, then the unsorted copy
+    for (int i = threadIdx.x; i < nc; i += blockDim.x) ev[nc + i] = fmax(Cr[i * nc + i], 0.0);
+    __syncthreads();
+    ascendingPositions(ev + nc, nc, pos);
+    for (int i = threadIdx.x; i < nc; i += blockDim.x) ev[pos[i]] = ev[nc + i];
+    double* out = cond + mw.sep0;  // upper triangle computed, mirrored: exactly symmetric
+    for (int t = threadIdx.x; t < nc * nc; t += blockDim.x) {
+        const int r = t / nc, c = t % nc;
+        if (r > c) continue;
+        double v = 0;
+        for (int i = 0; i < nc; ++i) v += V2[r * nc + i] * ev[nc + i] * V2[c * nc + i];
+        out[t] = v;
+        out[c * nc + r] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
 // Dense helpers (one CTA).  H, rhs, solution column-major; H is read from its
 // lower triangle like cusolverDnDsyevd with CUBLAS_FILL_MODE_LOWER.
 __global__ void __launch_bounds__(kMargThreads) k_dense_eigen(const double* H, int n, double* work, double* evals, double* evecs,
@@ -1403,6 +1576,28 @@ int launchMarginalization(const DevBatch& B, const MargBatch& M, size_t visualSm
     k_marg_fast<<<M.numWindows, kMargThreads, (size_t)M.fastSmem, s>>>(M);
     k_marg_eigen<<<M.numWindows, kEigenThreads, (size_t)M.eigenSmem, s>>>(M);
     return n + 4;
+}
+
+int launchCalibration(const DevBatch& B, const MargBatch& M, size_t visualSmem, double* work, const long long* work0, double* cond,
+                      double* evals, cudaStream_t s) {
+    int n = 1;
+    k_marg_rotations<<<(B.numKf + B.numExt + 255) / 256, 256, 0, s>>>(B);
+    if (M.numElim > 0) {
+        const int warps = 8;
+        k_marg_eval<<<(M.numElim + warps - 1) / warps, 32 * warps, 0, s>>>(B, M);
+        ++n;
+    }
+    if (M.numItems > 0) {
+        k_marg_rows<<<M.numItems, kRowsThreads, (size_t)M.rowsSmem, s>>>(B, M);
+        ++n;
+    }
+    if (M.numSlowElim > 0) {
+        k_marg_visual<<<M.numSlowElim, kMargLmThreads, visualSmem, s>>>(B, M);
+        ++n;
+    }
+    k_marg_retained<<<M.numWindows, 256, 0, s>>>(B, M);
+    k_calib_conditional<<<M.numWindows, kMargThreads, 0, s>>>(B, M, work, work0, cond, evals);
+    return n + 2;
 }
 void launchDenseEigen(const double* H, int n, double* work, double* evals, double* evecs, int* status, cudaStream_t s) {
     k_dense_eigen<<<1, kMargThreads, 0, s>>>(H, n, work, evals, evecs, status);

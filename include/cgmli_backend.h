@@ -236,6 +236,29 @@ int cgmli_solver_marginalize(cgmli_solver *solver, const int *victim_kf, int pol
  * outcome (CGMLI_IMU_MERGE_*) and, when reintegrated, the new factor; a failed
  * re-integration returns its CGMLI_E_* code. */
 int cgmli_solver_set_imu_merge_limits(cgmli_solver *solver, double max_interval_s, int max_samples);
+
+/* Conditional information of the calibration blocks given every other state of
+ * each window at its accepted states (BackendOptimizer::calibrationInformation,
+ * src/backend/BackendOptimizer.cpp:1084-1170): the visual factors (Huber-weighted,
+ * with the derivatives of every extrinsic and the time offset whether estimated
+ * or not), every IMU factor and, with include_prior, the square-root prior are
+ * linearized; every landmark range is eliminated by its scalar Schur complement
+ * (ranges with information at or below max(1e-12, 1e-9 max) skipped); the poses
+ * and speed/biases are removed by the eigen-based PSD solve with the cutoff
+ * max(1e-12, 1e-9 lambda_max) (significantly negative eigenvalues:
+ * CGMLI_E_INDEFINITE).  A window without calibration Jacobians reports
+ * CGMLI_E_INVALID.  The result is laid out per block: each extrinsic as
+ * [theta(3), p(3)] (the physical translation, dp = rho - [p]x dtheta), the time
+ * offset as one entry; symmetrized, with negative round-off eigenvalues clamped
+ * to 0.  The reference lays out one camera extrinsic and the time offset (its
+ * first 7 entries); with several extrinsic blocks each gets its 6.  Results
+ * replace a previous marginalization's (read_prior then fails until the next
+ * cgmli_solver_marginalize). */
+int cgmli_solver_calibration_information(cgmli_solver *solver, int include_prior);
+/* size = calibration entries, blocks as CGMLI_PRIOR_EXTRINSIC / _TIME_OFFSET
+ * (kind, index); conditional size x size row-major; eigenvalues ascending. */
+int cgmli_solver_read_calibration_information(cgmli_solver *solver, int window, int *size, int *num_blocks, int *block_kind,
+                                              int *block_index, double *conditional, double *eigenvalues);
 int cgmli_solver_read_merged_imu(cgmli_solver *solver, int window, int *state, cgmli_frozen_imu *imu);
 /* Result of window w: rank and separator width, then (when the buffers are
  * not NULL) the separator blocks, their ambient references, A

@@ -1529,14 +1529,22 @@ struct WindowMarg {
     MargOut out;
     std::vector<int> sepKind, sepIndex;  // separator blocks in column order
     std::vector<double> sepRef;
+    // calibration information (calib mode): conditional in report order, eigenvalues ascending
+    std::vector<double> conditional, eigenvalues;
 };
-static void marginalizeWindow(const cgmli_window& w, int victim, int policy, WindowMarg& res, bool skipImu = false) {
+static void calibrationConditional(const cgmli_window& w, int n, const std::vector<double>& H, const std::vector<MargBlock>& blocks,
+                                   WindowMarg& res);
+// calib: the formation of BackendOptimizer::calibrationInformation instead of a
+// marginalization: every landmark with observations, every IMU factor and (with
+// calibPrior) the prior; poses and speed/biases are the nuisance block.
+static void marginalizeWindow(const cgmli_window& w, int victim, int policy, WindowMarg& res, bool skipImu = false, bool calib = false,
+                              bool calibPrior = false) {
     const Layout lay(w);
     const int L = lay.L;
     std::vector<char> elim(L, 0), consumeObs(w.num_observations, 0);
     for (int l = 0; l < L; ++l) {
-        bool e = w.lm_anchor_kf[l] == victim;
-        if (policy == CGMLI_MARGIN_OLD)
+        bool e = calib ? w.lm_obs_begin[l + 1] > w.lm_obs_begin[l] : w.lm_anchor_kf[l] == victim;
+        if (policy == CGMLI_MARGIN_OLD && !calib)
             for (int f = w.lm_obs_begin[l]; f < w.lm_obs_begin[l + 1]; ++f) e = e || w.obs_kf[f] == victim;
         elim[l] = e;
         if (e) for (int f = w.lm_obs_begin[l]; f < w.lm_obs_begin[l + 1]; ++f) consumeObs[f] = 1;
@@ -1555,12 +1563,13 @@ static void marginalizeWindow(const cgmli_window& w, int victim, int policy, Win
             }
     std::vector<int> imuUsed;
     for (int i = 0; i < w.num_imu && !skipImu; ++i)
-        if (w.imu_kf[i] == victim || w.imu_kf[i] + 1 == victim) {
+        if (calib || w.imu_kf[i] == victim || w.imu_kf[i] + 1 == victim) {
             imuUsed.push_back(i);
             const int k = w.imu_kf[i];
             poseUsed[k] = poseUsed[k + 1] = sbUsed[k] = sbUsed[k + 1] = 1;
         }
-    for (int b = 0; b < w.prior_num_blocks; ++b) {
+    const bool withPrior = (!calib || calibPrior) && w.prior_rank > 0;
+    for (int b = 0; b < (withPrior ? w.prior_num_blocks : 0); ++b) {
         const int kind = w.prior_block_kind[b], idx = w.prior_block_index[b];
         if (kind == CGMLI_PRIOR_POSE) poseUsed[idx] = 1;
         else if (kind == CGMLI_PRIOR_SPEED_BIAS) sbUsed[idx] = 1;
@@ -1578,8 +1587,8 @@ static void marginalizeWindow(const cgmli_window& w, int victim, int policy, Win
         return c;
     };
     for (int k = 0; k < lay.K; ++k) {
-        if (poseUsed[k]) poseCol[k] = addBlock(CGMLI_PRIOR_POSE, k, 6, k == victim);
-        if (sbUsed[k]) sbCol[k] = addBlock(CGMLI_PRIOR_SPEED_BIAS, k, 9, k == victim);
+        if (poseUsed[k]) poseCol[k] = addBlock(CGMLI_PRIOR_POSE, k, 6, calib || k == victim);
+        if (sbUsed[k]) sbCol[k] = addBlock(CGMLI_PRIOR_SPEED_BIAS, k, 9, calib || k == victim);
     }
     for (int e = 0; e < lay.E; ++e) if (extUsed[e]) extCol[e] = addBlock(CGMLI_PRIOR_EXTRINSIC, e, 6, false);
     if (tdUsed && w.td) tdCol = addBlock(CGMLI_PRIOR_TIME_OFFSET, 0, 1, false);
@@ -1649,7 +1658,7 @@ static void marginalizeWindow(const cgmli_window& w, int victim, int policy, Win
         addRows(15, J, cols, 30, r);
         for (double v : r) { robust += 0.5 * v * v; rss += v * v; }
     }
-    if (w.prior_rank > 0) {
+    if (withPrior) {
         std::vector<double> r, Jt;
         if (!priorFactor(w, r, &Jt)) { res.out.status = CGMLI_E_NONFINITE; return; }
         std::vector<int> cols;
@@ -1662,6 +1671,12 @@ static void marginalizeWindow(const cgmli_window& w, int victim, int policy, Win
     }
     res.out.robustCost = robust;
     res.out.rss = rss;
+    if (calib) {
+        for (const auto& bl : blocks)
+            if (!bl.eliminate) { res.sepKind.push_back(bl.kind); res.sepIndex.push_back(bl.index); }
+        calibrationConditional(w, n, H, blocks, res);
+        return;
+    }
     marginalizeSystem(n, H, b, blocks, res.out);
     for (const auto& bl : blocks)
         if (!bl.eliminate) {
@@ -1674,6 +1689,101 @@ static void marginalizeWindow(const cgmli_window& w, int victim, int policy, Win
 }  // namespace orc
 
 namespace orc {
+// BackendOptimizer::calibrationInformation (BackendOptimizer.cpp:1084-1170) on
+// the window's full normal matrix H (landmark ranges, nuisance, calibration).
+static void calibrationConditional(const cgmli_window& w, int n, const std::vector<double>& H, const std::vector<MargBlock>& blocks,
+                                   WindowMarg& res) {
+    std::vector<int> ranges, nuisance, calib, report;
+    std::vector<int> extOfCol;  // extrinsic index of each calibration column, -1 for td
+    for (const auto& bl : blocks) {
+        if (bl.landmark) { ranges.push_back(bl.offset); continue; }
+        if (bl.eliminate) { for (int j = 0; j < bl.size; ++j) nuisance.push_back(bl.offset + j); continue; }
+        const int base = (int)calib.size();
+        for (int j = 0; j < bl.size; ++j) {
+            calib.push_back(bl.offset + j);
+            // [rho, theta] -> [theta, rho]; td as is
+            report.push_back(bl.kind == CGMLI_PRIOR_EXTRINSIC ? base + (j < 3 ? 3 + j : j - 3) : base + j);
+            extOfCol.push_back(bl.kind == CGMLI_PRIOR_EXTRINSIC ? bl.index : -1);
+        }
+    }
+    const int nx = (int)nuisance.size(), nc = (int)calib.size();
+    if (!nc) { res.out.status = CGMLI_E_INVALID; return; }
+    auto h = [&](int i, int j) { return H[(size_t)i * n + j]; };
+    std::vector<double> Hxx((size_t)nx * nx), Hxc((size_t)nx * nc), Hcc((size_t)nc * nc);
+    for (int i = 0; i < nx; ++i) {
+        for (int j = 0; j < nx; ++j) Hxx[(size_t)i * nx + j] = h(nuisance[i], nuisance[j]);
+        for (int j = 0; j < nc; ++j) Hxc[(size_t)i * nc + j] = h(nuisance[i], calib[j]);
+    }
+    for (int i = 0; i < nc; ++i) for (int j = 0; j < nc; ++j) Hcc[(size_t)i * nc + j] = h(calib[i], calib[j]);
+    // independent scalar ranges: eliminated one by one above the cutoff
+    double dmax = 0;
+    for (int r : ranges) dmax = std::max(dmax, h(r, r));
+    const double cutoff = std::max(1e-12, 1e-9 * dmax);
+    std::vector<double> x(nx), c(nc);
+    for (int r : ranges) {
+        const double d = h(r, r);
+        if (d <= cutoff) continue;
+        const double scale = 1.0 / std::sqrt(d);
+        for (int j = 0; j < nx; ++j) x[j] = scale * h(r, nuisance[j]);
+        for (int j = 0; j < nc; ++j) c[j] = scale * h(r, calib[j]);
+        for (int i = 0; i < nx; ++i) {
+            for (int j = 0; j < nx; ++j) Hxx[(size_t)i * nx + j] -= x[i] * x[j];
+            for (int j = 0; j < nc; ++j) Hxc[(size_t)i * nc + j] -= x[i] * c[j];
+        }
+        for (int i = 0; i < nc; ++i) for (int j = 0; j < nc; ++j) Hcc[(size_t)i * nc + j] -= c[i] * c[j];
+    }
+    std::vector<double> solved((size_t)nx * nc, 0.0);
+    if (nx) {
+        const int st = psdSolve(nx, Hxx.data(), nc, Hxc.data(), 1e-12, 1e-9, solved.data());
+        if (st != CGMLI_OK) { res.out.status = st; return; }
+    }
+    std::vector<double> C((size_t)nc * nc);
+    for (int i = 0; i < nc; ++i)
+        for (int j = 0; j < nc; ++j) {
+            double v = Hcc[(size_t)i * nc + j];
+            for (int k = 0; k < nx; ++k) v -= Hxc[(size_t)k * nc + i] * solved[(size_t)k * nc + j];
+            C[(size_t)report[i] * nc + report[j]] = v;
+        }
+    // basis to [theta, p]: dp = rho - [p]x dtheta under the left SE(3) chart
+    std::vector<double> B((size_t)nc * nc, 0.0);
+    for (int i = 0; i < nc; ++i) B[(size_t)i * nc + i] = 1.0;
+    for (int s0 = 0; s0 < nc; ++s0) {
+        const int e = extOfCol[s0];
+        if (e < 0 || (s0 > 0 && extOfCol[s0 - 1] == e)) continue;  // block starts only
+        const M3 px = skew(ld3(w.extrinsics + 7 * e));
+        for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) B[(size_t)(s0 + 3 + i) * nc + s0 + j] = px[3 * i + j];
+    }
+    std::vector<double> BtC((size_t)nc * nc, 0.0), Cb((size_t)nc * nc, 0.0);
+    for (int i = 0; i < nc; ++i)
+        for (int j = 0; j < nc; ++j) {
+            double v = 0;
+            for (int k = 0; k < nc; ++k) v += B[(size_t)k * nc + i] * C[(size_t)k * nc + j];
+            BtC[(size_t)i * nc + j] = v;
+        }
+    for (int i = 0; i < nc; ++i)
+        for (int j = 0; j < nc; ++j) {
+            double v = 0;
+            for (int k = 0; k < nc; ++k) v += BtC[(size_t)i * nc + k] * B[(size_t)k * nc + j];
+            Cb[(size_t)i * nc + j] = v;
+        }
+    std::vector<double> S((size_t)nc * nc);
+    for (int i = 0; i < nc; ++i)
+        for (int j = 0; j < nc; ++j) S[(size_t)i * nc + j] = 0.5 * Cb[(size_t)i * nc + j] + 0.5 * Cb[(size_t)j * nc + i];
+    std::vector<double> ev(nc), V((size_t)nc * nc);
+    if (!eigenSym(nc, S.data(), ev.data(), V.data())) { res.out.status = CGMLI_E_NONFINITE; return; }
+    const double cut2 = std::max(1e-12, 1e-9 * std::max(0.0, ev[nc - 1]));
+    if (ev[0] < -10 * cut2) { res.out.status = CGMLI_E_INDEFINITE; return; }
+    for (double& v : ev) v = std::max(v, 0.0);
+    res.eigenvalues = ev;
+    res.conditional.assign((size_t)nc * nc, 0.0);
+    for (int i = 0; i < nc; ++i)
+        for (int j = i; j < nc; ++j) {
+            double v = 0;
+            for (int k = 0; k < nc; ++k) v += V[(size_t)i * nc + k] * ev[k] * V[(size_t)j * nc + k];
+            res.conditional[(size_t)i * nc + j] = res.conditional[(size_t)j * nc + i] = v;
+        }
+}
+
 // SECOND_NEW with the IMU merge (SlidingWindowManager::prepareEviction,
 // SlidingWindowManager.cpp:263-310; mergeBodyImuRecords, BodyImuFactor.cpp:306-388).
 // Factor q of the window integrates samples [range[2q], range[2q+1]) of one
@@ -1726,6 +1836,22 @@ static int planImuMerge(const cgmli_window& w, int victim, const ImuStream& s, i
 extern "C" {
 
 int oracle_version(void) { return 1; }
+
+// Conditional calibration information of a window (BackendOptimizer::
+// calibrationInformation); sizes first (buffers NULL), then the data.
+int oracle_calibration_information(const cgmli_window* w, int include_prior, int* size, int* num_blocks, int* block_kind,
+                                   int* block_index, double* conditional, double* eigenvalues) {
+    orc::WindowMarg res;
+    orc::marginalizeWindow(*w, -1, CGMLI_MARGIN_OLD, res, false, true, include_prior != 0);
+    if (res.out.status != CGMLI_OK) return res.out.status;
+    *size = (int)res.eigenvalues.size();
+    *num_blocks = (int)res.sepKind.size();
+    if (block_kind) std::copy(res.sepKind.begin(), res.sepKind.end(), block_kind);
+    if (block_index) std::copy(res.sepIndex.begin(), res.sepIndex.end(), block_index);
+    if (conditional) std::copy(res.conditional.begin(), res.conditional.end(), conditional);
+    if (eigenvalues) std::copy(res.eigenvalues.begin(), res.eigenvalues.end(), eigenvalues);
+    return CGMLI_OK;
+}
 
 // SECOND_NEW window marginalization with the IMU merge: as
 // oracle_marginalize_window, plus the merge outcome (CGMLI_IMU_MERGE_*) and the

@@ -64,6 +64,7 @@ def lib() -> C.CDLL:
         P(L, "oracle_lm_solve_gated", C.c_int,
           [W, C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(abi.SolveReport), ip, dp, C.POINTER(C.c_ubyte)])
         ll = C.POINTER(C.c_longlong)
+        P(L, "oracle_calibration_information", C.c_int, [W, C.c_int, ip, ip, ip, ip, dp, dp])
         P(L, "oracle_marginalize_window_merge", C.c_int,
           [W, C.c_int, C.POINTER(abi.ImuParameters), ll, dp, C.c_int, ip, ll, ll, C.c_double, C.c_int, ip, ip, ip, ip, ip, dp, dp, dp,
            ip, C.POINTER(abi.FrozenImu)])
@@ -231,3 +232,18 @@ def marginalize_window_merge(win, victim, params, time_ns, readings, ranges, t0_
                                                state.ctypes.data_as(ip), C.byref(merged))
     return dict(status=st, rank=k, cols=m, kinds=kinds, index=idx, reference=ref, A=A.reshape(k, m), r0=r0,
                 merge=int(state[0]), merged=merged if int(state[0]) == abi.IMU_MERGE_REINTEGRATED else None)
+
+
+def calibration_information(win, include_prior=False):
+    """Conditional calibration information of a window: blocks, matrix, eigenvalues."""
+    size, nb = np.zeros(1, np.int32), np.zeros(1, np.int32)
+    st = lib().oracle_calibration_information(C.byref(win), int(include_prior), size.ctypes.data_as(ip), nb.ctypes.data_as(ip),
+                                              None, None, None, None)
+    if st != 0:
+        return dict(status=st)
+    n, b = int(size[0]), int(nb[0])
+    kinds, idx = np.zeros(max(b, 1), np.int32), np.zeros(max(b, 1), np.int32)
+    cond, ev = np.zeros(max(n * n, 1)), np.zeros(max(n, 1))
+    st = lib().oracle_calibration_information(C.byref(win), int(include_prior), size.ctypes.data_as(ip), nb.ctypes.data_as(ip),
+                                              kinds.ctypes.data_as(ip), idx.ctypes.data_as(ip), _p(cond), _p(ev))
+    return dict(status=st, kinds=kinds[:b], index=idx[:b], conditional=cond[:n * n].reshape(n, n), eigenvalues=ev[:n])
