@@ -68,6 +68,7 @@ def parse():
     p.add_argument("--serve-rate", type=float, default=5000.0, help="offered request rate of the served run (requests/s, 0: off)")
     p.add_argument("--serve-seconds", type=float, default=3.0, help="duration of the served run's arrivals")
     p.add_argument("--serve-pool", type=int, default=512, help="distinct windows the served requests draw from")
+    p.add_argument("--calib-steps", type=int, default=2, help="timed calibration-information passes over the solved batch (0: off)")
     p.add_argument("--gate-iterations", type=int, default=10, help="iteration budget of the gated-solve row (0: off)")
     p.add_argument("--imu-rigs", type=int, default=512, help="rigs of the IMU preintegration batch, 11 keyframes each (0: off)")
     p.add_argument("--imu-cpu-sample", type=int, default=1024, help="intervals preintegrated by the oracle for its CPU rate")
@@ -512,6 +513,22 @@ def main():
         marg = {"ms": marg_ms, "windows_per_s": world * args.windows / (marg_ms / 1e3), "launches": solver.timing()[1],
                 "workload": "Schur-complement prior of every window of the solved batch, oldest keyframe (OLD)"}
 
+    # conditional calibration information of every solved window (prior included),
+    # device time of the whole batched call
+    calib = None
+    if args.calib_steps > 0:
+        cms = []
+        for it in range(1 + args.calib_steps):
+            solver.calibration_information(include_prior=True)
+            solver.synchronize()
+            if it > 0:
+                cms.append(solver.timing()[0])
+        ok = sum(1 for i in range(args.windows) if solver.read_calibration_information(i)["status"] == 0)
+        calib_ms = max_over_ranks(sum(cms) / len(cms), dist)
+        calib = {"ms": calib_ms, "windows_per_s": world * args.windows / (calib_ms / 1e3), "windows_ok": ok,
+                 "launches": solver.timing()[1],
+                 "workload": "conditional information of the calibration blocks of every solved window, prior included"}
+
     # end to end through the C ABI with host buffers: topology + upload, solve, read back
     h2d = sum(window_bytes(w)[0] for w in windows)
     d2h = sum(window_bytes(w)[1] for w in windows)
@@ -602,7 +619,7 @@ def main():
             "cpu_baseline": cpu_baseline, "plain_path": plain,
             "served_vs_plain": (value / world) / plain["windows_per_s"] if plain else None,
             "served": served, "marginalization": marg, "configs": configs, "imu_preintegration": imu,
-            "nis_gate": gated,
+            "nis_gate": gated, "calibration_information": calib,
             "batch_latency_ms": {"p50": sorted(dev_ms)[len(dev_ms) // 2], "p99": max(dev_ms)},
             "window_status": statuses, "wall_s": wall,
         }
