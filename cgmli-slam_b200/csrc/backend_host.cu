@@ -40,7 +40,7 @@ cudaError_t configureMarginalization(size_t visualSmem, size_t rowsSmem, int max
                                      long long* fastSmem);
 int launchMarginalization(const DevBatch& B, const MargBatch& M, size_t visualSmem, cudaStream_t s);
 int launchCalibration(const DevBatch& B, const MargBatch& M, size_t visualSmem, double* work, const long long* work0, double* cond,
-                      double* evals, cudaStream_t s);
+                      double* evals, int maxNuisance, cudaStream_t s);
 void launchDenseEigen(const double* H, int n, double* work, double* evals, double* evecs, int* status, cudaStream_t s);
 void launchDensePsd(const double* evals, const double* U, const double* rhs, int n, int columns, double absCut, double relCut,
                     double* projected, double* solution, int* status, cudaStream_t s);
@@ -1298,6 +1298,7 @@ static int marginalizeImpl(cgmli_solver* S, const int* victim_kf, int policy, bo
         CK(S->mergeT0.upload(S->hMergeT0, st)); CK(S->mergeT1.upload(S->hMergeT1, st));
         CK(S->mergeStatus.reserve(jobs)); CK(S->mergeFlag.reserve(jobs)); CK(S->mergeOut.reserve(jobs));
     }
+    int calibMaxNx = 0;
     if (calib) {
         // per window 2 nx^2 + 2 nx nc + 4 nc^2 doubles of work; results at the
         // separator offsets (nc^2) and 2x the vector offsets (eigenvalues)
@@ -1305,6 +1306,7 @@ static int marginalizeImpl(cgmli_solver* S, const int* victim_kf, int policy, bo
         long long work = 0;
         for (int w = 0; w < W; ++w) {
             const long long nx = mwv[w].nm, nc = mwv[w].nr;
+            calibMaxNx = std::max(calibMaxNx, (int)nx);
             S->hCalibWork0[w] = work;
             work += 2 * nx * nx + 2 * nx * nc + 4 * nc * nc;
         }
@@ -1316,7 +1318,8 @@ static int marginalizeImpl(cgmli_solver* S, const int* victim_kf, int policy, bo
     CK(cudaEventRecord(S->margUploaded, st));
     CK(cudaEventRecord(S->ev0, st));
     if (calib)
-        S->lastLaunches = launchCalibration(S->B, M, smem, S->calibWork.p, S->calibWork0.p, S->calibCond.p, S->calibEvals.p, st);
+        S->lastLaunches =
+            launchCalibration(S->B, M, smem, S->calibWork.p, S->calibWork0.p, S->calibCond.p, S->calibEvals.p, calibMaxNx, st);
     else
         S->lastLaunches = launchMarginalization(S->B, M, smem, st);
     if (jobs) {

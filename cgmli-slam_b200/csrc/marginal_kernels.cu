@@ -667,7 +667,10 @@ __device__ void jacobiEigen(double* A, double* V, int n, int maxSweeps) {
 // contiguous.  On return Ap's diagonal holds the eigenvalues.
 __device__ __forceinline__ int pkUp(int r, int c, int n) { return r * n - r * (r - 1) / 2 + (c - r); }
 __device__ __forceinline__ int pkSym(int r, int c, int n) { return r <= c ? pkUp(r, c, n) : pkUp(c, r, n); }
-__device__ void jacobiPacked(double* Ap, double* Vt, int n, int maxSweeps) {
+// With vCols >= 0 the rotations are applied to the rows (vCols long) of the
+// caller's Vt as given, instead of accumulating eigenvectors from the identity:
+// Vt ends as U^T Vt.
+__device__ void jacobiPacked(double* Ap, double* Vt, int n, int maxSweeps, int vCols = -1) {
     __shared__ short pairP[512], pairQ[512];
     __shared__ double rc[512], rs[512];
     __shared__ int rotated;
@@ -675,7 +678,10 @@ __device__ void jacobiPacked(double* Ap, double* Vt, int n, int maxSweeps) {
     const int np = (n + 1) & ~1;
     const int half = np / 2;
     const int blocks = half * (half + 1) / 2;
-    for (long long i = threadIdx.x; i < (long long)n * n; i += blockDim.x) Vt[i] = (i / n == i % n) ? 1.0 : 0.0;
+    if (vCols < 0) {
+        vCols = n;
+        for (long long i = threadIdx.x; i < (long long)n * n; i += blockDim.x) Vt[i] = (i / n == i % n) ? 1.0 : 0.0;
+    }
     double fro = 0;
     for (int r = threadIdx.x; r < n; r += blockDim.x)
         for (int c = r; c < n; ++c) fro += (r == c ? 1.0 : 2.0) * Ap[pkUp(r, c, n)] * Ap[pkUp(r, c, n)];
@@ -698,9 +704,9 @@ __device__ void jacobiPacked(double* Ap, double* Vt, int n, int maxSweeps) {
         }
     }
     // eigenvector update: a fixed column k per thread and every step-th pair
-    const int vStep = n <= (int)blockDim.x ? (int)blockDim.x / n : 0;
-    const int vk = vStep ? (int)threadIdx.x % n : 0, vi0 = vStep ? (int)threadIdx.x / n : 0;
-    const bool vActive = vStep && (int)threadIdx.x < vStep * n;
+    const int vStep = vCols > 0 && vCols <= (int)blockDim.x ? (int)blockDim.x / vCols : 0;
+    const int vk = vStep ? (int)threadIdx.x % vCols : 0, vi0 = vStep ? (int)threadIdx.x / vCols : 0;
+    const bool vActive = vStep && (int)threadIdx.x < vStep * vCols;
     for (int sweep = 0; sweep < maxSweeps; ++sweep) {
         if (threadIdx.x == 0) rotated = 0;
         __syncthreads();
@@ -776,15 +782,16 @@ __device__ void jacobiPacked(double* Ap, double* Vt, int n, int maxSweeps) {
                 if (s == 0.0) return;
                 const double c = rc[i];
                 const long long p = pairP[i], q = pairQ[i];
-                const double vp = Vt[p * n + k], vq = Vt[q * n + k];
-                Vt[p * n + k] = c * vp - s * vq;
-                Vt[q * n + k] = s * vp + c * vq;
+                if (q >= n) return;  // the dummy index of an odd n has no row
+                const double vp = Vt[p * vCols + k], vq = Vt[q * vCols + k];
+                Vt[p * vCols + k] = c * vp - s * vq;
+                Vt[q * vCols + k] = s * vp + c * vq;
             };
             if (vStep) {
                 if (vActive)
                     for (int i = vi0; i < half; i += vStep) rotateVt(i, vk);
-            } else {
-                for (int t = threadIdx.x; t < half * n; t += blockDim.x) rotateVt(t / n, t % n);
+            } else if (vCols > 0) {
+                for (int t = threadIdx.x; t < half * vCols; t += blockDim.x) rotateVt(t / vCols, t % vCols);
             }
             __syncthreads();
         }
@@ -1299,10 +1306,14 @@ __global__ void __launch_bounds__(kEigenThreads) k_marg_eigen(MargBatch M) {
 // reported per extrinsic block as [theta, p] (the left-SE(3) tangent [rho, theta]
 // reordered, then dp = rho - [p]x dtheta: C' = B^T C B with B(p rows, theta cols)
 // = [p]x), td last; symmetrized, eigen-decomposed, negative round-off clamped.
-// work holds per window 2 nx^2 + 2 nx nc + 4 nc^2 doubles from work0[w].
+// work holds per window 2 nx^2 + 2 nx nc + 4 nc^2 doubles from work0[w].  The
+// nuisance block's Jacobi runs on its packed upper triangle in dynamic shared
+// memory when it fits in packedSmem bytes (eigenvectors as rows in global
+// memory), in global memory otherwise.
 constexpr int kCalibMaxCols = 64;
 __global__ void __launch_bounds__(kMargThreads) k_calib_conditional(DevBatch B, MargBatch M, double* work, const long long* work0,
-                                                                  double* cond, double* evals) {
+                                                                  double* cond, double* evals, long long packedSmem) {
+    extern __shared__ double calibSmem[];
     const int w = blockIdx.x;
     const MargWin mw = M.win[w];
     const int m = mw.m, nx = mw.nm, nc = mw.nr;
@@ -1337,15 +1348,32 @@ __global__ void __launch_bounds__(kMargThreads) k_calib_conditional(DevBatch B, 
             }
         }
     }
-    // 1. pseudo-inverse of the nuisance block applied to the coupling
-    for (long long t = threadIdx.x; t < (long long)nx * nx; t += blockDim.x) A[t] = symAt(H, (int)(t / nx), (int)(t % nx), m);
+    // 1. eigen-decomposition of the nuisance block.  In shared memory the
+    // rotations act on Hxc's rows directly (Y = U^T Hxc, nc wide), so that
+    // C = Hcc - sum over lambda_i > cut of y_i y_i^T / lambda_i needs no U;
+    // otherwise U is accumulated in global memory and C = Hcc - Hxc^T U P.
+    const bool inShared = nx > 0 && (long long)nx * (nx + 1) / 2 * 8 <= packedSmem;
+    double* Ap = calibSmem;
+    if (inShared) {
+        for (long long t = threadIdx.x; t < (long long)nx * nx; t += blockDim.x) {
+            const int i = (int)(t / nx), j = (int)(t % nx);
+            if (i <= j) Ap[pkUp(i, j, nx)] = H[(long long)i * m + j];
+        }
+        for (long long t = threadIdx.x; t < (long long)nx * nc; t += blockDim.x)
+            P[t] = symAt(H, (int)(t / nc), nx + (int)(t % nc), m);
+        __syncthreads();
+        jacobiPacked(Ap, P, nx, 60, nc);
+    } else {
+        for (long long t = threadIdx.x; t < (long long)nx * nx; t += blockDim.x) A[t] = symAt(H, (int)(t / nx), (int)(t % nx), m);
+        __syncthreads();
+        if (nx > 0) jacobiEigen(A, V, nx, 60);
+    }
     __syncthreads();
-    if (nx > 0) jacobiEigen(A, V, nx, 60);
-    __syncthreads();
+    auto lam = [&](int i) { return inShared ? Ap[pkUp(i, i, nx)] : A[(long long)i * nx + i]; };
     double vmax = -INFINITY, vmin = INFINITY;
     bool finite = true;
     for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-        const double v = A[(long long)i * nx + i];
+        const double v = lam(i);
         vmax = fmax(vmax, v);
         vmin = fmin(vmin, v);
         finite = finite && isfinite(v);
@@ -1358,30 +1386,43 @@ __global__ void __launch_bounds__(kMargThreads) k_calib_conditional(DevBatch B, 
         if (threadIdx.x == 0) M.status[w] = bad > 0 ? CGMLI_E_NONFINITE : CGMLI_E_INDEFINITE;
         return;
     }
-    for (long long t = threadIdx.x; t < (long long)nx * nc; t += blockDim.x) {
-        const int i = (int)(t / nc), c = (int)(t % nc);
-        const double lam = A[(long long)i * nx + i];
-        double v = 0;
-        if (lam > cut) {
-            for (int k = 0; k < nx; ++k) v += V[(long long)k * nx + i] * symAt(H, k, nx + c, m);
-            v /= lam;
+    if (inShared) {
+        // 2. C = Hcc - sum y_i y_i^T / lambda_i, in report order
+        for (int t = threadIdx.x; t < nc * nc; t += blockDim.x) {
+            const int a = t / nc, c = t % nc;
+            double v = symAt(H, nx + a, nx + c, m);
+            for (int i = 0; i < nx; ++i) {
+                const double li = lam(i);
+                if (li > cut) v -= P[(long long)i * nc + a] * P[(long long)i * nc + c] / li;
+            }
+            Cs[report[a] * nc + report[c]] = v;
         }
-        P[t] = v;
-    }
-    __syncthreads();
-    for (long long t = threadIdx.x; t < (long long)nx * nc; t += blockDim.x) {
-        const int k = (int)(t / nc), c = (int)(t % nc);
-        double v = 0;
-        for (int i = 0; i < nx; ++i) v += V[(long long)k * nx + i] * P[(long long)i * nc + c];
-        X[t] = v;
-    }
-    __syncthreads();
-    // 2. C = Hcc - Hxc^T X, in report order
-    for (int t = threadIdx.x; t < nc * nc; t += blockDim.x) {
-        const int a = t / nc, c = t % nc;
-        double v = symAt(H, nx + a, nx + c, m);
-        for (int k = 0; k < nx; ++k) v -= symAt(H, k, nx + a, m) * X[(long long)k * nc + c];
-        Cs[report[a] * nc + report[c]] = v;
+    } else {
+        // 2. X = U diag(1/lambda) U^T Hxc, C = Hcc - Hxc^T X, in report order
+        for (long long t = threadIdx.x; t < (long long)nx * nc; t += blockDim.x) {
+            const int i = (int)(t / nc), c = (int)(t % nc);
+            const double li = lam(i);
+            double v = 0;
+            if (li > cut) {
+                for (int k = 0; k < nx; ++k) v += V[(long long)k * nx + i] * symAt(H, k, nx + c, m);
+                v /= li;
+            }
+            P[t] = v;
+        }
+        __syncthreads();
+        for (long long t = threadIdx.x; t < (long long)nx * nc; t += blockDim.x) {
+            const int k = (int)(t / nc), c = (int)(t % nc);
+            double v = 0;
+            for (int i = 0; i < nx; ++i) v += V[(long long)k * nx + i] * P[(long long)i * nc + c];
+            X[t] = v;
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < nc * nc; t += blockDim.x) {
+            const int a = t / nc, c = t % nc;
+            double v = symAt(H, nx + a, nx + c, m);
+            for (int k = 0; k < nx; ++k) v -= symAt(H, k, nx + a, m) * X[(long long)k * nc + c];
+            Cs[report[a] * nc + report[c]] = v;
+        }
     }
     __syncthreads();
     // 3. C' = B^T C B, B = I except [p]x in (p rows, theta cols) of each extrinsic block
@@ -1579,7 +1620,7 @@ int launchMarginalization(const DevBatch& B, const MargBatch& M, size_t visualSm
 }
 
 int launchCalibration(const DevBatch& B, const MargBatch& M, size_t visualSmem, double* work, const long long* work0, double* cond,
-                      double* evals, cudaStream_t s) {
+                      double* evals, int maxNuisance, cudaStream_t s) {
     int n = 1;
     k_marg_rotations<<<(B.numKf + B.numExt + 255) / 256, 256, 0, s>>>(B);
     if (M.numElim > 0) {
@@ -1596,7 +1637,17 @@ int launchCalibration(const DevBatch& B, const MargBatch& M, size_t visualSmem, 
         ++n;
     }
     k_marg_retained<<<M.numWindows, 256, 0, s>>>(B, M);
-    k_calib_conditional<<<M.numWindows, kMargThreads, 0, s>>>(B, M, work, work0, cond, evals);
+    // the packed nuisance block in shared memory when the widest one fits
+    long long use = 0;
+    int dev = 0, optin = 0;
+    cudaFuncAttributes fa;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess &&
+        cudaFuncGetAttributes(&fa, k_calib_conditional) == cudaSuccess) {
+        const long long want = 8ll * maxNuisance * (maxNuisance + 1) / 2, avail = (long long)optin - (long long)fa.sharedSizeBytes;
+        use = want <= avail ? want : 0;
+        if (cudaFuncSetAttribute(k_calib_conditional, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)use) != cudaSuccess) use = 0;
+    }
+    k_calib_conditional<<<M.numWindows, kMargThreads, (size_t)use, s>>>(B, M, work, work0, cond, evals, use);
     return n + 2;
 }
 void launchDenseEigen(const double* H, int n, double* work, double* evals, double* evecs, int* status, cudaStream_t s) {
