@@ -104,6 +104,11 @@ def max_over_ranks(value: float, dist, device: str = "cuda") -> float:
     return float(t.item())
 
 
+def min_over_ranks(value: float, dist, device: str = "cuda") -> float:
+    """Smallest value over the ranks (a throughput's slowest rank)."""
+    return -max_over_ranks(-value, dist, device)
+
+
 def aggregate_rate(world: int, windows_per_rank: int, steps: int, max_ms: float) -> float:
     """Whole-job windows/s: every rank's windows over the slowest rank's device time."""
     return world * windows_per_rank * steps / (max_ms / 1000.0)
@@ -280,6 +285,35 @@ def run_configs(args, local, backend):
                      "marginalization": "OLD" if policy == abi.MARGIN_OLD else "SECOND_NEW",
                      "final_state_rel_err_vs_fp64_oracle": float(np.linalg.norm(xg - xc) / max(np.linalg.norm(xc - x0), 1e-300))}
     return out
+
+
+def run_e2e_pipelined(args, local, backend, windows, rank):
+    """End to end through the served API (cgmli_server_*): the batch plus three
+    more batches of distinct windows drawn the same way (a solved window reused
+    would converge faster), all submitted at once, solved with the batch's LM
+    iterations and no marginalization.  The server's two solvers overlap each
+    batch's host build and upload with the other batch's solve; every request's
+    window goes host -> device and its states come back.  Throughput is the
+    windows over the span from the first submission to the last completion, so
+    the first batch's unoverlapped build is included."""
+    extra = synth.make_windows("c4", 3 * args.windows, seed=rank_seed(args.seed, rank) + 7777)
+    pool = list(windows) + extra
+    init = [w.state_vector() for w in pool]
+    server = backend.Server(device=local, iterations=args.iterations, policy=abi.MARGIN_OLD, max_batch_windows=args.windows)
+    victims = [-1] * len(pool)
+    for _ in range(2):  # warm-up: both solvers and their pinned staging reach the batch size
+        server.replay(pool, victims, np.zeros(len(pool)))
+        for w, x in zip(pool, init):
+            w.set_state_vector(x)
+    lat, status, span = server.replay(pool, victims, np.zeros(len(pool)))
+    for w, x in zip(pool, init):
+        w.set_state_vector(x)
+    server.close()
+    counts = {}
+    for st in status:
+        k = abi.ERRORS.get(int(st), int(st))
+        counts[k] = counts.get(k, 0) + 1
+    return len(pool) / span, len(pool), counts
 
 
 def run_gated(args, local, backend, windows, init):
@@ -547,8 +581,15 @@ def main():
         if it > 0:
             e2e_times.append(dt)
     e2e_s = max_over_ranks(sum(e2e_times) / len(e2e_times), dist)
-    e2e = {"value": world * args.windows / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-           "includes": "host topology build + H2D of all window data + device LM + D2H of states"}
+    sequential = {"value": world * args.windows / e2e_s, "unit": UNIT,
+                  "includes": "one solver: host topology build + H2D of all window data + device LM + D2H of states, in sequence"}
+    pipe_rate, pipe_windows, pipe_status = run_e2e_pipelined(args, local, backend, windows, rank)
+    pipe_rate = world * min_over_ranks(pipe_rate, dist)
+    e2e = {"value": pipe_rate, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+           "includes": f"served API, {pipe_windows} distinct windows submitted at once in batches of {args.windows}: host build + "
+                       "H2D of each window's data + device LM + D2H of its states; two solvers overlap one batch's host work "
+                       "with the other's solve",
+           "request_status": pipe_status, "sequential": sequential}
 
     # plain single-window path: the configuration-2 window solved alone, one at a time
     plain = None

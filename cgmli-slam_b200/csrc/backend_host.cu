@@ -636,8 +636,8 @@ int cgmli_solver_refresh_imu(cgmli_solver* S, double gyro_threshold, double acce
     if (!refreshed) return CGMLI_OK;
     *refreshed = 0;
     if (count == 0) return CGMLI_OK;
-    S->hImuStatus.resize(count);
-    S->hImuRefreshed.resize(count);
+    sizeTo(S->hImuStatus, count);
+    sizeTo(S->hImuRefreshed, count);
     CK(cudaMemcpyAsync(S->hImuStatus.data(), S->imuStatus.p, count * sizeof(int), cudaMemcpyDeviceToHost, S->stream));
     CK(cudaMemcpyAsync(S->hImuRefreshed.data(), S->imuRefreshed.p, count * sizeof(int), cudaMemcpyDeviceToHost, S->stream));
     CK(cudaStreamSynchronize(S->stream));
@@ -849,7 +849,7 @@ int cgmli_solver_read_merged_imu(cgmli_solver* S, int window, int* state, cgmli_
     const int job = S->mergeJob[window];
     if (job < 0) return CGMLI_OK;
     if (!S->mergeRead) {
-        S->hMergeStatus.resize(S->hMergeKf.size());
+        sizeTo(S->hMergeStatus, S->hMergeKf.size());
         CK(cudaMemcpyAsync(S->hMergeStatus.data(), S->mergeStatus.p, S->hMergeStatus.size() * sizeof(int), cudaMemcpyDeviceToHost,
                            S->stream));
         CK(cudaStreamSynchronize(S->stream));
@@ -940,11 +940,11 @@ static int marginalizeImpl(cgmli_solver* S, const int* victim_kf, int policy, bo
     HVec<int>& visExt = S->hMargVisExt;
     // the staging arrays may still feed the previous marginalization's uploads
     if (S->margUploaded) CK(cudaEventSynchronize(S->margUploaded));
-    poseCol.resize(S->totalKf);
-    sbCol.resize(S->totalKf);
-    extCol.resize(S->totalExt);
-    visPose.resize(S->totalKf);
-    visExt.resize(S->totalExt);
+    sizeTo(poseCol, S->totalKf);
+    sizeTo(sbCol, S->totalKf);
+    sizeTo(extCol, S->totalExt);
+    sizeTo(visPose, S->totalKf);
+    sizeTo(visExt, S->totalExt);
     parallelFor(W, 0, [&](int w) {
         const WinDesc& d = S->win[w];
         const int v = calib ? -1 : victim_kf[w];
@@ -1163,11 +1163,11 @@ static int marginalizeImpl(cgmli_solver* S, const int* victim_kf, int policy, bo
     HVec<int>& obsMap = S->hMargObsMap;
     HVec<int>& visCol = S->hMargVisCol;
     HVec<int4>& chunks = S->hMargChunks;
-    elims.resize(elimBase[W]);
-    cols.resize(colBase[W]);
-    obsMap.resize(5 * obsBase[W]);
-    visCol.resize(std::max(visBase[W], 1));
-    chunks.resize(std::max(chunkBase[W], 1));
+    sizeTo(elims, elimBase[W]);
+    sizeTo(cols, colBase[W]);
+    sizeTo(obsMap, 5 * obsBase[W]);
+    sizeTo(visCol, std::max(visBase[W], 1));
+    sizeTo(chunks, std::max(chunkBase[W], 1));
     parallelFor(W, 0, [&](int w) {
         const Part& P = part[w];
         for (size_t e = 0; e < P.elims.size(); ++e) {
@@ -1198,7 +1198,7 @@ static int marginalizeImpl(cgmli_solver* S, const int* victim_kf, int policy, bo
     HVec<int4>& items = S->hMargItems;
     HVec<int>& slow = S->hMargSlow;
     items.clear();
-    slow.resize(std::max(numSlow, 1));
+    sizeTo(slow, std::max(numSlow, 1));
     numSlow = 0;
     for (int w = 0; w < W; ++w) {
         if (!mwv[w].rowsPath) {
@@ -1302,7 +1302,7 @@ static int marginalizeImpl(cgmli_solver* S, const int* victim_kf, int policy, bo
     if (calib) {
         // per window 2 nx^2 + 2 nx nc + 4 nc^2 doubles of work; results at the
         // separator offsets (nc^2) and 2x the vector offsets (eigenvalues)
-        S->hCalibWork0.resize(W);
+        sizeTo(S->hCalibWork0, W);
         long long work = 0;
         for (int w = 0; w < W; ++w) {
             const long long nx = mwv[w].nm, nc = mwv[w].nr;
@@ -1354,11 +1354,11 @@ int cgmli_solver_read_prior(cgmli_solver* S, int window, int* rank, int* cols, i
         float ms = 0;
         if (cudaEventElapsedTime(&ms, S->ev0, S->ev1) == cudaSuccess) S->lastMs = ms;
         HostBatch& hb = S->hb;
-        S->hMargA.resize(S->margSepTotal);
-        S->hMargR0.resize(S->margVecTotal);
-        S->hMargStats.resize(4ll * W);
-        S->hMargRank.resize(W);
-        S->hMargStatus.resize(W);
+        sizeTo(S->hMargA, S->margSepTotal);
+        sizeTo(S->hMargR0, S->margVecTotal);
+        sizeTo(S->hMargStats, 4ll * W);
+        sizeTo(S->hMargRank, W);
+        sizeTo(S->hMargStatus, W);
         cudaStream_t st = S->stream;
         if (S->margSepTotal)
             CK(cudaMemcpyAsync(S->hMargA.data(), S->margA.p, S->margSepTotal * sizeof(double), cudaMemcpyDeviceToHost, st));

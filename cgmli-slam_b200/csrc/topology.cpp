@@ -168,17 +168,17 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
     hb.totalKf = kf; hb.totalExt = ex; hb.totalCam = cam; hb.totalLm = lm; hb.totalObs = ob; hb.totalImu = im;
     hb.vec = vec; hb.dense = dense; hb.acc = acc; hb.sch = sch; hb.imuScratch = imuS; hb.priorScratch = priS;
     constexpr int kImuDoubles = sizeof(cgmli_frozen_imu) / sizeof(double);
-    hb.camR.resize(9ll * cam); hb.camT.resize(3ll * cam); hb.camExt.resize(cam);
-    hb.lmWin.resize(lm); hb.lmKf.resize(lm); hb.lmCam.resize(lm); hb.lmObsBegin.resize(lm + 1ll); hb.lmNs.resize(lm); hb.lmNx.resize(lm);
-    hb.lmSupp0.resize(lm); hb.lmC0.resize(lm); hb.lmPerm.resize(lm);
-    hb.lmBearing.resize(3ll * lm); hb.lmVel.resize(3ll * lm); hb.lmTime.resize(lm);
-    hb.obKf.resize(ob); hb.obCam.resize(ob); hb.obSlot.resize(ob); hb.obXslot.resize(ob); hb.obLm.resize(ob); hb.obOrig.resize(ob);
-    hb.keyOrder.resize(ob);
-    hb.obBearing.resize(3ll * ob); hb.obP.resize(6ll * ob); hb.obVel.resize(3ll * ob); hb.obTime.resize(ob);
-    hb.pose.resize(7ll * kf); hb.sb.resize(9ll * kf); hb.ext.resize(7ll * ex); hb.td.resize(count); hb.rho.resize(lm);
-    hb.imu.resize((size_t)kImuDoubles * im); hb.imuKf.resize(im);
-    hb.priorKind.resize(pblk); hb.priorIndex.resize(pblk); hb.priorCol.resize(pblk); hb.priorOff.resize(pblk);
-    hb.priorA.resize(pA); hb.priorR0.resize(pR); hb.priorRef.resize(pRef);
+    sizeTo(hb.camR, 9ll * cam); sizeTo(hb.camT, 3ll * cam); sizeTo(hb.camExt, cam);
+    sizeTo(hb.lmWin, lm); sizeTo(hb.lmKf, lm); sizeTo(hb.lmCam, lm); sizeTo(hb.lmObsBegin, lm + 1ll); sizeTo(hb.lmNs, lm); sizeTo(hb.lmNx, lm);
+    sizeTo(hb.lmSupp0, lm); sizeTo(hb.lmC0, lm); sizeTo(hb.lmPerm, lm);
+    sizeTo(hb.lmBearing, 3ll * lm); sizeTo(hb.lmVel, 3ll * lm); sizeTo(hb.lmTime, lm);
+    sizeTo(hb.obKf, ob); sizeTo(hb.obCam, ob); sizeTo(hb.obSlot, ob); sizeTo(hb.obXslot, ob); sizeTo(hb.obLm, ob); sizeTo(hb.obOrig, ob);
+    sizeTo(hb.keyOrder, ob);
+    sizeTo(hb.obBearing, 3ll * ob); sizeTo(hb.obP, 6ll * ob); sizeTo(hb.obVel, 3ll * ob); sizeTo(hb.obTime, ob);
+    sizeTo(hb.pose, 7ll * kf); sizeTo(hb.sb, 9ll * kf); sizeTo(hb.ext, 7ll * ex); sizeTo(hb.td, count); sizeTo(hb.rho, lm);
+    sizeTo(hb.imu, (size_t)kImuDoubles * im); sizeTo(hb.imuKf, im);
+    sizeTo(hb.priorKind, pblk); sizeTo(hb.priorIndex, pblk); sizeTo(hb.priorCol, pblk); sizeTo(hb.priorOff, pblk);
+    sizeTo(hb.priorA, pA); sizeTo(hb.priorR0, pR); sizeTo(hb.priorRef, pRef);
     hb.lmObsBegin[lm] = ob;
     const int runLen = runLength(lm);
     // ---- phase 1: every window on its own thread
@@ -488,13 +488,13 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
         hb.maxNs = std::max(hb.maxNs, part[i].maxNs);
     }
     hb.cross = crossBase[count];
-    hb.supp.resize(suppBase[count]);
-    hb.tiles.resize(tileBase[count]);
-    hb.runs.resize(runBase[count]);
-    hb.pairChunks.resize(pairBase[count]);
-    hb.schurChunks.resize(schurBase[count]);
-    hb.schurCols.resize(std::max(schurColBase[count], 1));
-    hb.lmUmap.resize(std::max(hb.cross, 1ll));
+    sizeTo(hb.supp, suppBase[count]);
+    sizeTo(hb.tiles, tileBase[count]);
+    sizeTo(hb.runs, runBase[count]);
+    sizeTo(hb.pairChunks, pairBase[count]);
+    sizeTo(hb.schurChunks, schurBase[count]);
+    sizeTo(hb.schurCols, std::max(schurColBase[count], 1));
+    sizeTo(hb.lmUmap, std::max(hb.cross, 1ll));
     parallelFor(count, threads, [&](int i) {
         const WinDesc& d = hb.win[i];
         WindowPart& P = part[i];

@@ -148,6 +148,14 @@ struct PinnedAllocator {
 };
 template <class T>
 using HVec = std::vector<T, PinnedAllocator<T>>;
+// Resize with 1.5x headroom on growth: pinned memory is freed with
+// cudaFreeHost, which waits for the whole device, so a batch slightly larger
+// than every earlier one must not reallocate the staging again.
+template <class V>
+void sizeTo(V& v, size_t n) {
+    if (n > v.capacity()) v.reserve(std::max(n, v.capacity() + v.capacity() / 2));
+    v.resize(n);
+}
 
 struct HostBatch {
     std::vector<WinDesc> win;
