@@ -78,7 +78,8 @@ class SolverOptions(C.Structure):
 
 class ServerOptions(C.Structure):
     _fields_ = [("device", C.c_int), ("max_batch_windows", C.c_int), ("memory_budget_bytes", C.c_longlong),
-                ("iterations", C.c_int), ("policy", C.c_int)]
+                ("iterations", C.c_int), ("policy", C.c_int), ("nis_threshold", C.c_double), ("max_refits", C.c_int),
+                ("pre_gate", C.c_int)]
 
 
 class SolveReport(C.Structure):
@@ -144,6 +145,7 @@ def declare_backend(lib: C.CDLL) -> C.CDLL:
     _proto(lib, "cgmli_server_read_prior", C.c_int,
            [V, C.c_longlong, c_int_p, c_int_p, c_int_p, c_int_p, c_int_p, c_double_p, c_double_p, c_double_p])
     _proto(lib, "cgmli_server_release", C.c_int, [V, C.c_longlong])
+    _proto(lib, "cgmli_server_read_gate", C.c_int, [V, C.c_longlong, C.POINTER(GateReport), C.POINTER(C.c_ubyte)])
     _proto(lib, "cgmli_server_replay", C.c_int,
            [V, C.POINTER(W), c_int_p, c_double_p, C.c_int, c_double_p, c_int_p, c_double_p])
     _proto(lib, "cgmli_imu_preintegrate", C.c_int,
@@ -182,7 +184,7 @@ BACKEND_SYMBOLS = [
     "cgmli_solver_read_prior", "cgmli_marg_eigen", "cgmli_marg_psd_solve", "cgmli_marg_subtract",
     "cgmli_solver_checkpoint", "cgmli_solver_rollback", "cgmli_solver_kernel_times", "cgmli_topology_check",
     "cgmli_marg_eigen_noalloc", "cgmli_server_create", "cgmli_server_destroy", "cgmli_server_submit", "cgmli_server_poll",
-    "cgmli_server_read_prior", "cgmli_server_release", "cgmli_server_replay", "cgmli_imu_preintegrate",
+    "cgmli_server_read_prior", "cgmli_server_release", "cgmli_server_replay", "cgmli_server_read_gate", "cgmli_imu_preintegrate",
     "cgmli_imu_last_timing", "cgmli_solver_set_imu_samples", "cgmli_solver_refresh_imu", "cgmli_solver_read_imu",
     "cgmli_solver_solve_gated", "cgmli_solver_read_gate", "cgmli_solver_set_imu_merge_limits", "cgmli_solver_read_merged_imu",
     "cgmli_solver_calibration_information", "cgmli_solver_read_calibration_information",

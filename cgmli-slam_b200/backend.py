@@ -287,13 +287,16 @@ class Server:
     passed to submit() must stay alive until their request completes."""
 
     def __init__(self, device: int = 0, iterations: int = 1, policy: int = abi.MARGIN_OLD, max_batch_windows: int = 512,
-                 memory_budget_bytes: int = 40 << 30):
+                 memory_budget_bytes: int = 40 << 30, nis_threshold: float = 0.0, max_refits: int = 3, pre_gate: bool = False):
         opt = abi.ServerOptions()
         opt.device = device
         opt.max_batch_windows = max_batch_windows
         opt.memory_budget_bytes = memory_budget_bytes
         opt.iterations = iterations
         opt.policy = policy
+        opt.nis_threshold = nis_threshold
+        opt.max_refits = max_refits
+        opt.pre_gate = int(pre_gate)
         self._h = C.c_void_p()
         _check(lib().cgmli_server_create(C.byref(opt), C.byref(self._h)), "cgmli_server_create")
         self._keep = {}
@@ -345,6 +348,14 @@ class Server:
     def release(self, ticket: int) -> None:
         _check(lib().cgmli_server_release(self._h, ticket), "cgmli_server_release")
         self._keep.pop(ticket, None)
+
+    def read_gate(self, ticket: int, num_observations: int):
+        """(GateReport, rejected mask) of a completed gated request."""
+        rep = abi.GateReport()
+        mask = np.zeros(max(num_observations, 1), dtype=np.uint8)
+        _check(lib().cgmli_server_read_gate(self._h, ticket, C.byref(rep), mask.ctypes.data_as(C.POINTER(C.c_ubyte))),
+               "cgmli_server_read_gate")
+        return rep, mask[:num_observations]
 
     def replay(self, windows, victims, arrival_s):
         """Replays a trace (window objects, victim per request, arrival times in s);

@@ -42,6 +42,9 @@ struct Request {
     int rank = 0, cols = 0, numBlocks = 0;
     std::vector<int> kinds, index;
     std::vector<double> reference, A, r0;
+    // gated solve: the window's gate report and rejected factors
+    cgmli_gate_report gate{};
+    std::vector<unsigned char> rejected;
 };
 
 // Device bytes a window occupies in a batch (observation, landmark and dense
@@ -90,7 +93,9 @@ struct cgmli_server {
             b.marg = b.marg || victims[i] >= 0;
         }
         b.status = cgmli_solver_set_windows(S, b.windows.data(), n);
-        if (b.status == CGMLI_OK) b.status = cgmli_solver_solve(S, opt.iterations);
+        if (b.status == CGMLI_OK)
+            b.status = opt.nis_threshold > 0 ? cgmli_solver_solve_gated(S, opt.iterations, opt.nis_threshold, opt.max_refits, opt.pre_gate)
+                                             : cgmli_solver_solve(S, opt.iterations);
         if (b.status == CGMLI_OK && b.marg) b.status = cgmli_solver_marginalize(S, victims.data(), opt.policy);
     }
 
@@ -114,6 +119,11 @@ struct cgmli_server {
                 continue;
             }
             r->report = reps[i];
+            if (opt.nis_threshold > 0) {
+                r->rejected.resize(r->window.num_observations);
+                const int gs = cgmli_solver_read_gate(S, i, &r->gate, r->rejected.data());
+                if (gs != CGMLI_OK && r->report.status == CGMLI_OK) r->report.status = gs;
+            }
             if (r->victim >= 0 && r->report.status == CGMLI_OK) {
                 int rank = 0, cols = 0, nb = 0;
                 int ps = cgmli_solver_read_prior(S, i, &rank, &cols, &nb, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
@@ -226,6 +236,8 @@ int cgmli_server_create(const cgmli_server_options* options, cgmli_server** out)
     if (options->iterations < 1) return setLastError(CGMLI_E_INVALID, "server: iterations < 1");
     if (options->policy != CGMLI_MARGIN_OLD && options->policy != CGMLI_MARGIN_SECOND_NEW)
         return setLastError(CGMLI_E_INVALID, "server: unknown marginalization policy");
+    if (!(options->nis_threshold >= 0) || options->max_refits < 0 || options->max_refits > 64)
+        return setLastError(CGMLI_E_INVALID, "server: nis_threshold < 0 or max_refits outside 0..64");
     auto* s = new cgmli_server();
     s->opt = *options;
     if (s->opt.max_batch_windows <= 0) s->opt.max_batch_windows = 512;
@@ -391,6 +403,19 @@ int cgmli_server_read_prior(cgmli_server* s, long long ticket, int* rank, int* c
     }
     if (A) std::copy(r->A.begin(), r->A.end(), A);
     if (r0) std::copy(r->r0.begin(), r->r0.end(), r0);
+    return CGMLI_OK;
+}
+
+int cgmli_server_read_gate(cgmli_server* s, long long ticket, cgmli_gate_report* report, unsigned char* rejected) {
+    if (!s || !report) return setLastError(CGMLI_E_INVALID, "server: null server or report");
+    if (!(s->opt.nis_threshold > 0)) return setLastError(CGMLI_E_INVALID, "server: the gate is off (nis_threshold 0)");
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->requests.find(ticket);
+    if (it == s->requests.end()) return setLastError(CGMLI_E_INVALID, "server: unknown ticket");
+    const Request& r = *it->second;
+    if (!r.complete) return setLastError(CGMLI_E_PENDING, "server: request not complete");
+    *report = r.gate;
+    if (rejected && !r.rejected.empty()) std::copy(r.rejected.begin(), r.rejected.end(), rejected);
     return CGMLI_OK;
 }
 

@@ -404,6 +404,10 @@ typedef struct cgmli_server_options {
     long long memory_budget_bytes;  /* 0: 40 GiB */
     int iterations;                 /* LM iterations per request, >= 1 */
     int policy;                     /* CGMLI_MARGIN_OLD or _SECOND_NEW for requests with a victim */
+    double nis_threshold;           /* > 0: solve with the NIS gate and outlier refits
+                                       (cgmli_solver_solve_gated); 0: plain solve */
+    int max_refits;                 /* refits of the gated solve (reference: 3) */
+    int pre_gate;                   /* gated solve: gate at the submitted states first */
 } cgmli_server_options;
 typedef struct cgmli_server cgmli_server;
 
@@ -420,6 +424,9 @@ int cgmli_server_poll(cgmli_server *server, long long ticket, int wait, cgmli_so
  * (sizes first with NULL buffers). */
 int cgmli_server_read_prior(cgmli_server *server, long long ticket, int *rank, int *cols, int *num_blocks, int *block_kind,
                             int *block_index, double *reference, double *A, double *r0);
+/* Gate report and rejected factors (num_observations flags, or NULL) of a
+ * completed request of a server with nis_threshold > 0. */
+int cgmli_server_read_gate(cgmli_server *server, long long ticket, cgmli_gate_report *report, unsigned char *rejected);
 /* Frees a completed request's record. */
 int cgmli_server_release(cgmli_server *server, long long ticket);
 /* Replays a request trace from a host thread (load testing): request i submits

@@ -73,3 +73,32 @@ def test_invalid_request_rejected_at_submit(backend):
         server.submit(arr[0])
     assert e.value.code == 1
     server.close()
+
+
+def test_served_gated_equals_alone(backend):
+    """With nis_threshold set, every request is solved with the NIS gate and
+    outlier refits; its rejected factors and states equal the window's gated
+    solve alone."""
+    n, iterations = 5, 8
+    alone_windows = synth.make_windows("c4", n, seed=95)
+    served_windows = synth.make_windows("c4", n, seed=95)
+    alone = []
+    for w in alone_windows:
+        s = backend.Solver()
+        s.set_windows([w])
+        s.solve_gated(iterations, pre_gate=False)
+        s.synchronize()
+        s.read_states()
+        alone.append((w.state_vector(), s.read_gate(0)[1]))
+        s.close()
+    x0 = [w.state_vector() for w in served_windows]
+    srv = backend.Server(iterations=iterations, nis_threshold=9.210340371976184, max_refits=3, pre_gate=False)
+    tickets = [srv.submit(w) for w in served_windows]
+    for t, w, x, (xa, ma) in zip(tickets, served_windows, x0, alone):
+        rep, _ = srv.poll(t)
+        assert rep.status == 0
+        g, m = srv.read_gate(t, w.window.num_observations)
+        assert np.array_equal(m, ma) and g.rejected_total == int(ma.sum())
+        assert rel(w.state_vector() - x, xa - x) < 1e-8
+        srv.release(t)
+    srv.close()
