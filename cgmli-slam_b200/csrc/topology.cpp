@@ -2,6 +2,7 @@
 #include "topology.h"
 
 #include <algorithm>
+#include <memory>
 #include <atomic>
 #include <cstdio>
 #include <cstring>
@@ -48,7 +49,9 @@ struct WindowPart {
     std::vector<int4> pairChunks;
     std::vector<int4> schurChunks;  // .w: window-local offset in schurCols
     std::vector<int> schurCols;     // per chunk: count, then ascending visual columns
-    std::vector<unsigned short> umap;  // per cross-vector entry (window-local): position in its chunk's columns
+    // per cross-vector entry (window-local): position in its chunk's columns; every
+    // entry is written by the chunking, so the array is not zero-filled first
+    std::unique_ptr<unsigned short[]> umap;
     long long cross = 0;            // sum of support widths
     int maxNs = 1;
     int status = CGMLI_OK;
@@ -396,7 +399,7 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
             const int words = (nBlk + 63) / 64;
             std::vector<unsigned long long> U(words, 0), Ul(words, 0);
             std::vector<int> blkPos(nBlk, 0);
-            P.umap.assign(P.cross, 0);
+            P.umap.reset(new unsigned short[P.cross > 0 ? P.cross : 1]);
             auto blocksOf = [&](int q) {
                 std::fill(Ul.begin(), Ul.end(), 0ull);
                 const int g = d.lm0 + q, ns_ = hb.lmNs[g], nx_ = hb.lmNx[g];
@@ -517,7 +520,7 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
             hb.schurChunks[schurBase[i] + c] = chunk;
         }
         std::copy(P.schurCols.begin(), P.schurCols.end(), hb.schurCols.begin() + schurColBase[i]);
-        std::copy(P.umap.begin(), P.umap.end(), hb.lmUmap.begin() + crossBase[i]);
+        std::copy(P.umap.get(), P.umap.get() + P.cross, hb.lmUmap.begin() + crossBase[i]);
     });
     return CGMLI_OK;
 }
