@@ -707,6 +707,7 @@ __device__ void jacobiPacked(double* Ap, double* Vt, int n, int maxSweeps, int v
     const int vStep = vCols > 0 && vCols <= (int)blockDim.x ? (int)blockDim.x / vCols : 0;
     const int vk = vStep ? (int)threadIdx.x % vCols : 0, vi0 = vStep ? (int)threadIdx.x / vCols : 0;
     const bool vActive = vStep && (int)threadIdx.x < vStep * vCols;
+    const bool vGlobal = vCols > 0 && __isGlobal(Vt);
     for (int sweep = 0; sweep < maxSweeps; ++sweep) {
         if (threadIdx.x == 0) rotated = 0;
         __syncthreads();
@@ -787,9 +788,36 @@ __device__ void jacobiPacked(double* Ap, double* Vt, int n, int maxSweeps, int v
                 Vt[p * vCols + k] = c * vp - s * vq;
                 Vt[q * vCols + k] = s * vp + c * vq;
             };
-            if (vStep) {
+            if (vStep && !vGlobal) {
                 if (vActive)
                     for (int i = vi0; i < half; i += vStep) rotateVt(i, vk);
+            } else if (vStep) {
+                // a thread's pairs rotate disjoint rows: issue eight pairs' loads
+                // before their stores, so that global Vt keeps eight accesses in
+                // flight per thread instead of one dependent round trip per pair
+                constexpr int kVtBatch = 8;
+                if (vActive)
+                    for (int i0 = vi0; i0 < half; i0 += kVtBatch * vStep) {
+                        double vp[kVtBatch], vq[kVtBatch];
+                        bool live[kVtBatch];
+#pragma unroll
+                        for (int u = 0; u < kVtBatch; ++u) {
+                            const int i = i0 + u * vStep;
+                            live[u] = i < half && rs[i] != 0.0 && pairQ[i] < n;
+                            if (live[u]) {
+                                vp[u] = Vt[(long long)pairP[i] * vCols + vk];
+                                vq[u] = Vt[(long long)pairQ[i] * vCols + vk];
+                            }
+                        }
+#pragma unroll
+                        for (int u = 0; u < kVtBatch; ++u) {
+                            if (!live[u]) continue;
+                            const int i = i0 + u * vStep;
+                            const double c = rc[i], s = rs[i];
+                            Vt[(long long)pairP[i] * vCols + vk] = c * vp[u] - s * vq[u];
+                            Vt[(long long)pairQ[i] * vCols + vk] = s * vp[u] + c * vq[u];
+                        }
+                    }
             } else if (vCols > 0) {
                 for (int t = threadIdx.x; t < half * vCols; t += blockDim.x) rotateVt(t / vCols, t % vCols);
             }
