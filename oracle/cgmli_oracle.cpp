@@ -401,7 +401,8 @@ static bool visualFactor(const cgmli_window& w, int l, int f, bool derivatives, 
                 if (!liftPose(xea, t1, r1, o.Jea)) return false;
             }
         } else {
-            // separate anchor/observer extrinsic blocks (tangent derivation in DESIGN.md)
+            // separate anchor and observer extrinsic blocks: each takes the tangent form of its
+            // own camera chain (anchor [D R_a, -D R_a [b_a]x], observer [-D R_b, D R_b [o_b]x])
             const V3 world = add(rotatedBody, ld3(xa));
             if (a != b) {
                 tangentDirect(D, eye(), world, 1.0, o.Ja);
