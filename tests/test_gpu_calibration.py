@@ -58,6 +58,19 @@ def test_calibration_information_matches_oracle(oracle, backend, name, prior):
     compare(s.read_calibration_information(0), ref)
 
 
+def test_visual_only_window_is_indefinite(oracle, backend):
+    """Without IMU factors the poses keep a scale gauge that the extrinsic
+    translation couples to: the coupling leaves the nuisance block's range, the
+    conditional is indefinite, and both report CGMLI_E_INDEFINITE."""
+    w = synth.SynthWindow(replace(synth.C1, keyframes=6, landmarks=300, with_imu=False, outlier_fraction=0.0), 81)
+    ref = oracle.calibration_information(w.window, False)
+    assert ref["status"] == 6  # CGMLI_E_INDEFINITE
+    s = backend.Solver()
+    s.set_windows([w])
+    s.calibration_information(include_prior=False)
+    assert s.read_calibration_information(0)["status"] == ref["status"]
+
+
 def test_batch_after_solve(oracle, backend):
     """Solved windows of the batched workload, evaluated together; each as the
     oracle on the read-back states."""

@@ -117,3 +117,23 @@ def test_plain_solve_unchanged_by_gate_fields(oracle, backend):
     assert r.iterations == rep.iterations and rel(w.state_vector() - x0, xo - x0) < 1e-6
     g, mask = s.read_gate(0)
     assert g.rejected_total == 0 and mask.sum() == 0
+
+
+def test_unreachable_threshold_is_the_plain_solve(oracle, backend):
+    """A threshold no factor reaches: one pass, nothing rejected, and the plain
+    solve's iterations and states."""
+    w = synth.SynthWindow(replace(synth.C1, keyframes=5, landmarks=200), 59)
+    x0 = w.state_vector()
+    st, plain = oracle.lm_solve(w.window, 8)
+    xo = w.state_vector()
+    w.set_state_vector(x0)
+    s = backend.Solver()
+    s.set_windows([w])
+    s.solve_gated(8, nis_threshold=1e300, pre_gate=True)
+    s.synchronize()
+    s.read_states()
+    g, mask = s.read_gate(0)
+    r = s.reports()[0]
+    assert g.passes == 1 and g.rejected_total == 0 and not mask.any()
+    assert r.iterations == plain.iterations
+    assert rel(w.state_vector() - x0, xo - x0) < 1e-6
