@@ -284,6 +284,19 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
         int tileObs = 0, runLms = 0;
         auto sameSupport = [&](int a, int b) { return !lessSupport(a, b) && !lessSupport(b, a); };
         for (int q = 0; q < L; ++q) {
+            if (q + 8 < L) {  // the support order jumps through the caller's arrays: fetch ahead
+                const int lp = order[q + 8], bp = w.lm_obs_begin[lp];
+                __builtin_prefetch(&w.obs_kf[bp]);
+                __builtin_prefetch(&w.obs_cam[bp]);
+                __builtin_prefetch(&w.obs_bearing[3ll * bp]);
+                __builtin_prefetch(&w.obs_P[6ll * bp]);
+                __builtin_prefetch(&w.obs_P[6ll * bp + 8]);
+                if (w.obs_velocity) __builtin_prefetch(&w.obs_velocity[3ll * bp]);
+                if (w.obs_time) __builtin_prefetch(&w.obs_time[bp]);
+                __builtin_prefetch(&w.lm_anchor_bearing[3ll * lp]);
+                __builtin_prefetch(&w.rho[lp]);
+                __builtin_prefetch(&flat[supStart[lp]]);
+            }
             const int l = order[q], g = d.lm0 + q;
             const int b = w.lm_obs_begin[l], e = w.lm_obs_begin[l + 1], nobs = e - b;
             const bool newGroup = q == 0 || !sameSupport(order[q - 1], l);
