@@ -72,6 +72,7 @@ def parse():
     p.add_argument("--gate-iterations", type=int, default=10, help="iteration budget of the gated-solve row (0: off)")
     p.add_argument("--imu-rigs", type=int, default=512, help="rigs of the IMU preintegration batch, 11 keyframes each (0: off)")
     p.add_argument("--imu-cpu-sample", type=int, default=1024, help="intervals preintegrated by the oracle for its CPU rate")
+    p.add_argument("--mixed-steps", type=int, default=10, help="timed solves of the batch in mixed precision (0: off)")
     return p.parse_args()
 
 
@@ -420,6 +421,68 @@ def run_imu(args, local, backend):
     return out
 
 
+def run_mixed(args, local, backend, windows, init, solver, dist):
+    """The batch in CGMLI_PRECISION_MIXED: device time of the same solve, and its
+    accuracy against the FP64 path (first step dx of every window, final states)."""
+    for w, x in zip(windows, init):
+        w.set_state_vector(x)
+    mixed = backend.Solver(device=local, precision=abi.PRECISION_MIXED)
+    mixed.set_windows(windows)
+    mixed.checkpoint()
+    # first LM step at lambda = 1e-4 from the initial states, both precisions
+    solver.rollback()
+    solver.step(1e-4)
+    mixed.step(1e-4)
+    dx_retained, dx_all = 0.0, 0.0
+    for i, w in enumerate(windows):
+        nr = w.retained_dim()
+        a, b = mixed.read_step(i)["delta"], solver.read_step(i)["delta"]
+        dx_retained = max(dx_retained, float(np.linalg.norm(a[:nr] - b[:nr]) / max(np.linalg.norm(b[:nr]), 1e-300)))
+        dx_all = max(dx_all, float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)))
+    for _ in range(max(3, args.warmup)):
+        mixed.rollback()
+        mixed.solve(args.iterations)
+        mixed.synchronize()
+    mixed.kernel_times(enable=1)
+    ms = []
+    for _ in range(args.mixed_steps):
+        mixed.rollback()
+        mixed.solve(args.iterations)
+        mixed.synchronize()
+        ms.append(mixed.timing()[0])
+    kt = mixed.kernel_times(enable=-1)
+    mixed.kernel_times(enable=0)
+    total = max_over_ranks(sum(ms), dist)
+    # final states of both precisions, relative to the distance travelled
+    solver.rollback()
+    solver.solve(args.iterations)
+    solver.synchronize()
+    solver.read_states()
+    x64 = [w.state_vector() for w in windows]
+    c64 = [r.final_cost for r in solver.reports()]
+    a64 = [r.accepted_steps for r in solver.reports()]
+    mixed.read_states()
+    same = [i for i, r in enumerate(mixed.reports()) if r.accepted_steps == a64[i]]
+    state_err = max(float(np.linalg.norm(windows[i].state_vector() - x64[i]) / np.linalg.norm(x64[i])) for i in same)
+    cost_err = max(abs(mixed.reports()[i].final_cost - c64[i]) / abs(c64[i]) for i in same)
+    statuses = {}
+    for r in mixed.reports():
+        key = abi.ERRORS.get(r.status, r.status)
+        statuses[key] = statuses.get(key, 0) + 1
+    for w, x in zip(windows, init):
+        w.set_state_vector(x)
+    solver.rollback()
+    mixed.close()
+    return {"windows_per_s": args.windows * len(ms) / (total / 1e3), "ms_per_step": total / len(ms), "steps": len(ms),
+            "step_dx_rel_err_vs_fp64_max": {"retained": dx_retained, "all": dx_all, "bar": 1e-6},
+            "final_vs_fp64_max": {"state_rel": state_err, "cost_rel": cost_err, "windows_compared": len(same),
+                                  "windows_with_other_accept_count": len(windows) - len(same)},
+            "window_status": statuses,
+            "kernel_ms_per_step": {k: v[0] / len(ms) for k, v in kt.items()},
+            "precision": "fp32 Jacobians, robust weights, compensated fp32 landmark Hessian sums; fp64 residuals, gradients, "
+                         "reduced system, Cholesky"}
+
+
 def run_reference(args, world, rank):
     """CPU path of the reference algorithm on the host cores (FP64 oracle)."""
     if rank != 0:
@@ -615,6 +678,7 @@ def main():
     configs = run_configs(args, local, backend) if rank == 0 and not args.no_configs else None
     imu = run_imu(args, local, backend) if rank == 0 and args.imu_rigs > 0 else None
     gated = run_gated(args, local, backend, windows, init) if rank == 0 and args.gate_iterations > 0 else None
+    mixed = run_mixed(args, local, backend, windows, init, solver, dist) if args.mixed_steps > 0 else None
 
     statuses = {}
     for r in reports:
@@ -660,7 +724,7 @@ def main():
             "cpu_baseline": cpu_baseline, "plain_path": plain,
             "served_vs_plain": (value / world) / plain["windows_per_s"] if plain else None,
             "served": served, "marginalization": marg, "configs": configs, "imu_preintegration": imu,
-            "nis_gate": gated, "calibration_information": calib,
+            "nis_gate": gated, "calibration_information": calib, "mixed_precision": mixed,
             "batch_latency_ms": {"p50": sorted(dev_ms)[len(dev_ms) // 2], "p99": max(dev_ms)},
             "window_status": statuses, "wall_s": wall,
         }

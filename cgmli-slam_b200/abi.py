@@ -79,7 +79,7 @@ class SolverOptions(C.Structure):
 class ServerOptions(C.Structure):
     _fields_ = [("device", C.c_int), ("max_batch_windows", C.c_int), ("memory_budget_bytes", C.c_longlong),
                 ("iterations", C.c_int), ("policy", C.c_int), ("nis_threshold", C.c_double), ("max_refits", C.c_int),
-                ("pre_gate", C.c_int)]
+                ("pre_gate", C.c_int), ("precision", C.c_int)]
 
 
 class SolveReport(C.Structure):

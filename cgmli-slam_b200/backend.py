@@ -287,7 +287,8 @@ class Server:
     passed to submit() must stay alive until their request completes."""
 
     def __init__(self, device: int = 0, iterations: int = 1, policy: int = abi.MARGIN_OLD, max_batch_windows: int = 512,
-                 memory_budget_bytes: int = 40 << 30, nis_threshold: float = 0.0, max_refits: int = 3, pre_gate: bool = False):
+                 memory_budget_bytes: int = 40 << 30, nis_threshold: float = 0.0, max_refits: int = 3, pre_gate: bool = False,
+                 precision: int = abi.PRECISION_FP64):
         opt = abi.ServerOptions()
         opt.device = device
         opt.max_batch_windows = max_batch_windows
@@ -297,6 +298,7 @@ class Server:
         opt.nis_threshold = nis_threshold
         opt.max_refits = max_refits
         opt.pre_gate = int(pre_gate)
+        opt.precision = precision
         self._h = C.c_void_p()
         _check(lib().cgmli_server_create(C.byref(opt), C.byref(self._h)), "cgmli_server_create")
         self._keep = {}

@@ -24,7 +24,7 @@
 #include "topology.h"
 
 namespace cgmli {
-size_t linearizeSmemBytes(int maxNs);
+size_t linearizeSmemBytes(int maxNs, bool mixed);
 size_t factorSmemBytes(int maxNr);
 cudaError_t configureKernels(size_t linSmem, size_t facSmem);
 int launchIteration(const DevBatch& B, const LaunchPlan& P, int refinement, int maxIterations, int probe, double* Sdebug,
@@ -310,7 +310,6 @@ int cgmli_solver_create(int device, const cgmli_solver_options* options, cgmli_s
     if (options) {
         if (options->precision != CGMLI_PRECISION_FP64 && options->precision != CGMLI_PRECISION_MIXED)
             return fail(CGMLI_E_INVALID, "unknown precision");
-        if (options->precision == CGMLI_PRECISION_MIXED) return fail(CGMLI_E_UNSUPPORTED, "mixed precision is not built");
         if (options->refinement_steps < 0 || options->refinement_steps > 2) return fail(CGMLI_E_INVALID, "refinement_steps outside 0..2");
         if (!(options->initial_lambda > 0)) return fail(CGMLI_E_INVALID, "initial_lambda must be positive");
         if (options->slabs_per_window != 0 || options->threads_per_block != 0)
@@ -385,7 +384,7 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     S->totalKf = hb.totalKf; S->totalExt = hb.totalExt; S->totalCam = hb.totalCam; S->totalLm = hb.totalLm;
     S->totalObs = hb.totalObs; S->totalImu = hb.totalImu;
     S->maxNpc = hb.maxNpc; S->maxNr = hb.maxNr; S->maxNs = hb.maxNs;
-    S->linSmem = linearizeSmemBytes(S->maxNs);
+    S->linSmem = linearizeSmemBytes(S->maxNs, S->opt.precision == CGMLI_PRECISION_MIXED);
     S->facSmem = factorSmemBytes(S->maxNr);
     CK(configureKernels(S->linSmem, S->facSmem));
     const long long lm = hb.totalLm;
@@ -426,6 +425,7 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     B.numWindows = count; B.numLandmarks = hb.totalLm; B.numObs = hb.totalObs; B.numKf = hb.totalKf; B.numExt = hb.totalExt;
     B.numCam = hb.totalCam; B.numImu = hb.totalImu;
     B.numRuns = (int)hb.runs.size();
+    B.mixed = S->opt.precision == CGMLI_PRECISION_MIXED ? 1 : 0;
     B.win = S->dWin.p; B.lm = S->dLm.p;
     B.camR = S->camR.p; B.camT = S->camT.p; B.camExt = S->camExt.p;
     B.lmWin = S->lmWin.p; B.lmKf = S->lmKf.p; B.lmCam = S->lmCam.p; B.lmObsBegin = S->lmObsBegin.p;

@@ -53,6 +53,7 @@ enum { kModeLinearize = 0, kModeResolve = 1, kModeDone = 2 };
 // Pointers to every device array (filled by the host runtime).
 struct DevBatch {
     int numWindows, numLandmarks, numObs, numKf, numExt, numCam, numImu, numRuns;
+    int mixed;  // CGMLI_PRECISION_MIXED: FP32 Jacobians, weights and landmark sums in the linearization
     const WinDesc* win;
     WinLM* lm;
     // cameras

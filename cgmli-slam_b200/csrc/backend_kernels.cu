@@ -8,6 +8,8 @@
 // runs without a host round trip and can be captured in a CUDA graph.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "../../include/cgmli_backend.h"
 #include "backend_internal.h"
 #include "device_math.cuh"
@@ -107,33 +109,59 @@ __device__ __forceinline__ int pcOfLocal(int i, int s, int x, const int* sk, int
 // Work unit: a run = consecutive landmarks of one window processed by one warp in
 // tiles of <= 32 observations (lane = observation for the evaluation).  Per-warp
 // shared memory: 32 staged factors (overwritten in place by the weighted cross
-// products J_x^T J_rho over the compact columns at [0, 25) and d, g, cost at
-// 25, 26, 27), the compact -> local column maps, flags, and the landmark's
-// cross vector (maxNs doubles, the batch's widest support).
-__host__ __device__ constexpr size_t landmarkWarpBytes(int maxNs) {
-    return sizeof(double) * (32 * kOut + maxNs) + sizeof(long long) * 32 + sizeof(short) * 32 * kCompact + sizeof(int) * 32;
+// products J_x^T J_rho over the compact columns at [0, 25)), the compact -> local
+// column maps, flags, and the landmark's cross vector (maxNs doubles, the batch's
+// widest support).
+//
+// Mixed precision (Mixed = true): the Jacobians and the robust weight are FP32 and
+// the landmark Hessian blocks d_l and the runs of c_l are summed in FP32 with
+// compensation (error-free two-sum terms carried beside each sum, added in FP64 at
+// the end).  The residual, the cost and every gradient term (g_l here, J^T r in the
+// pairs pass: FP32 Jacobian entries times the FP64 residual) stay FP64.  A factor is
+// staged as kOutF floats (the FactorOut blocks without the residual, then the weight).
+constexpr int kOutF = 53;
+__device__ __forceinline__ int compactOffF(int r, int c) { return c < 24 ? 12 * (c / 6) + 6 * r + c % 6 : 48 + r; }
+__host__ __device__ constexpr size_t landmarkWarpBytes(int maxNs, bool mixed) {
+    return (mixed ? sizeof(float) * 32 * kOutF : sizeof(double) * 32 * kOut) + sizeof(double) * maxNs + sizeof(long long) * 32 +
+           sizeof(short) * 32 * kCompact + sizeof(int) * 32;
 }
+static_assert(sizeof(float) * 32 * kOutF % 16 == 0, "double-aligned cross vector after the FP32 staging");
 // Staged row of one factor, written by k_lin_landmark (in observation order)
-// and gathered in key order by k_lin_pairs:
-// weighted J row 0 over the compact columns [0, 25), row 1 [25, 50), weighted
-// residual 50, 51, the packed key (anchor kf | observer kf << 16 | anchor ext << 32 |
-// observer ext << 48, window-local) at 52; 53..55 pad the row to 448 bytes.
+// and gathered in key order by k_lin_pairs.  FP64 (448 bytes): weighted J row 0
+// over the compact columns [0, 25), row 1 [25, 50), weighted residual 50, 51, the
+// packed key (anchor kf | observer kf << 16 | anchor ext << 32 | observer ext << 48,
+// window-local) at 52; 53..55 pad.  Mixed (224 bytes): the weighted residual
+// (2 doubles) at bytes [0, 16), the weighted J rows as 50 floats at [16, 216),
+// the key at [216, 224).
 constexpr int kKeyRow = 56;
+constexpr int kKeyRowBytesF = 224;
 __device__ __forceinline__ long long packKey(int a, int b, int ea, int eb) {
     return (long long)a | (long long)b << 16 | (long long)ea << 32 | (long long)eb << 48;
 }
+// Compensated FP32 sums: s carries the rounded sum, e the accumulated rounding errors.
+__device__ __forceinline__ void twoSumAdd(float& s, float& e, float v) {
+    const float t = s + v, bp = t - s;
+    e += (s - (t - bp)) + (v - bp);
+    s = t;
+}
+__device__ __forceinline__ float huberWeightF(float scale, float squared) {
+    return scale > 0 && squared > scale * scale ? sqrtf(scale / sqrtf(squared)) : 1.0f;
+}
 
+template <bool Mixed>
 __global__ void __launch_bounds__(kLinWarps * 32, 2) k_lin_landmark(DevBatch B, const int4* runs, const int2* tiles, int maxNs) {
     extern __shared__ double smemRaw[];
+    constexpr int kStride = Mixed ? kOutF : kOut;
+    using St = typename std::conditional<Mixed, float, double>::type;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int runIdx = blockIdx.x * kLinWarps + warp;
     if (runIdx >= B.numRuns) return;
     const int4 run = runs[runIdx];  // {window, tile begin, tile end, -}
     const int wdx = run.x;
     if (B.lm[wdx].mode != kModeLinearize) return;
-    char* base = reinterpret_cast<char*>(smemRaw) + landmarkWarpBytes(maxNs) * warp;
-    double* out = reinterpret_cast<double*>(base);
-    double* cvec = out + 32 * kOut;
+    char* base = reinterpret_cast<char*>(smemRaw) + landmarkWarpBytes(maxNs, Mixed) * warp;
+    St* out = reinterpret_cast<St*>(base);
+    double* cvec = reinterpret_cast<double*>(out + 32 * kStride);
     long long* keys = reinterpret_cast<long long*>(cvec + maxNs);
     short* map = reinterpret_cast<short*>(keys + 32);
     int* flags = reinterpret_cast<int*>(map + 32 * kCompact);
@@ -154,13 +182,22 @@ __global__ void __launch_bounds__(kLinWarps * 32, 2) k_lin_landmark(DevBatch B, 
             myNs = 6 * (B.lmNs[l] + B.lmNx[l]) + (wd.estTd ? 1 : 0);
             myC0 = B.lmC0[l];
         }
+        double r0 = 0.0, r1 = 0.0;  // residual of this lane's factor (the mixed path keeps it in registers)
         if (f < oe) {
             const int l = B.obLm[f];
             FactorIn in;
             int kfa, kfb, ea, eb;
             gatherFactor(B, wd, wdx, l, f, 0, in, kfa, kfb, ea, eb);
-            double* st = out + kOut * lane;
-            const bool ok = evalBearingFactor(in, true, *reinterpret_cast<FactorOut*>(st));
+            St* st = out + kStride * lane;
+            bool ok;
+            if constexpr (Mixed) {
+                const FactorJac<float> jac = {st, st + 12, st + 24, st + 36, st + 48, st + 50};
+                double r[2];
+                ok = evalBearing<float>(in, r, &jac);
+                if (ok) { r0 = r[0]; r1 = r[1]; }
+            } else {
+                ok = evalBearingFactor(in, true, *reinterpret_cast<FactorOut*>(st));
+            }
             const int s = B.lmNs[l], x = B.lmNx[l];
             const bool same = in.sameKf && !in.splitExt;
             const int obSlot = B.obSlot[f], obX = B.obXslot[f];
@@ -174,57 +211,96 @@ __global__ void __launch_bounds__(kLinWarps * 32, 2) k_lin_landmark(DevBatch B, 
             mp[24] = wd.estTd ? 6 * (s + x) : -1;
             flags[lane] = ok ? 1 : 0;
             keys[lane] = packKey(kfa - wd.kf0, kfb - wd.kf0, ea - wd.ext0, eb - wd.ext0);
-            if (ok) st[54] = huberWeight(wd.huber, st[0] * st[0] + st[1] * st[1]);
-            else for (int k = 0; k < kOut; ++k) st[k] = 0.0;
+            if constexpr (Mixed) {
+                if (ok) st[52] = huberWeightF((float)wd.huber, (float)(r0 * r0 + r1 * r1));
+                else for (int k = 0; k < kOutF; ++k) st[k] = 0.0f;
+            } else {
+                if (ok) st[54] = huberWeight(wd.huber, st[0] * st[0] + st[1] * st[1]);
+                else for (int k = 0; k < kOut; ++k) st[k] = 0.0;
+            }
         }
         __syncwarp();
         // weighted compact row of this lane's observation (unrolled: constant offsets)
         if (f < oe) {
-            const double* st = out + kOut * lane;
-            const double w = st[54];
-            double2* row = reinterpret_cast<double2*>(B.keyRows + (size_t)f * kKeyRow);
+            const St* st = out + kStride * lane;
+            if constexpr (Mixed) {
+                const float w = st[52];
+                char* row = reinterpret_cast<char*>(B.keyRows) + (size_t)f * kKeyRowBytesF;
+                *reinterpret_cast<double2*>(row) = make_double2((double)w * r0, (double)w * r1);
+                float4* jr = reinterpret_cast<float4*>(row + 16);
+                auto at = [&](int k) { return w * st[k < 25 ? compactOffF(0, k) : compactOffF(1, k - 25)]; };
 #pragma unroll
-            for (int q = 0; q < 25; ++q) {
-                const int c0 = 2 * q, c1 = 2 * q + 1;
-                row[q] = make_double2(w * st[c0 < 25 ? compactOff(0, c0) : compactOff(1, c0 - 25)],
-                                      w * st[c1 < 25 ? compactOff(0, c1) : compactOff(1, c1 - 25)]);
+                for (int q = 0; q < 12; ++q) jr[q] = make_float4(at(4 * q), at(4 * q + 1), at(4 * q + 2), at(4 * q + 3));
+                *reinterpret_cast<float2*>(row + 16 + 192) = make_float2(at(48), at(49));
+                *reinterpret_cast<long long*>(row + 216) = keys[lane];
+            } else {
+                const double w = st[54];
+                double2* row = reinterpret_cast<double2*>(B.keyRows + (size_t)f * kKeyRow);
+#pragma unroll
+                for (int q = 0; q < 25; ++q) {
+                    const int c0 = 2 * q, c1 = 2 * q + 1;
+                    row[q] = make_double2(w * st[c0 < 25 ? compactOff(0, c0) : compactOff(1, c0 - 25)],
+                                          w * st[c1 < 25 ? compactOff(0, c1) : compactOff(1, c1 - 25)]);
+                }
+                row[25] = make_double2(w * st[0], w * st[1]);
+                row[26] = make_double2(__longlong_as_double(keys[lane]), 0.0);
             }
-            row[25] = make_double2(w * st[0], w * st[1]);
-            row[26] = make_double2(__longlong_as_double(keys[lane]), 0.0);
         }
         __syncwarp();
-        if (f < oe && flags[lane]) {
-            double* st = out + kOut * lane;
-            const double r0 = st[0], r1 = st[1], p0 = st[52], p1 = st[53];
-            const double sq = r0 * r0 + r1 * r1;
-            const double w = st[54], w2 = w * w;
-            const double d = w2 * (p0 * p0 + p1 * p1), g = w2 * (p0 * r0 + p1 * r1), cost = huberCost(wd.huber, sq);
-            // in place: column c reads offsets >= c + 2, all later than slot c
+        // this lane's contributions to d_l, g_l, the cost and (in place) the cross products
+        const bool live = f < oe && flags[lane];
+        double dD = 0.0, gD = 0.0, cost = 0.0;
+        float dS = 0.0f;
+        if (live) {
+            St* st = out + kStride * lane;
+            if constexpr (Mixed) {
+                cost = huberCost(wd.huber, r0 * r0 + r1 * r1);
+                const float p0 = st[50], p1 = st[51], w = st[52], w2 = w * w;
+                dS = w2 * (p0 * p0 + p1 * p1);
+                gD = (double)w2 * ((double)p0 * r0 + (double)p1 * r1);  // gradient: FP32 Jacobian, FP64 residual
+                // in place: column c reads offsets >= c, none overwritten before it is read
 #pragma unroll
-            for (int c = 0; c < kCompact; ++c) st[c] = w2 * (st[compactOff(0, c)] * p0 + st[compactOff(1, c)] * p1);
-            st[25] = d; st[26] = g; st[27] = cost;
+                for (int c = 0; c < kCompact; ++c) st[c] = w2 * (st[compactOffF(0, c)] * p0 + st[compactOffF(1, c)] * p1);
+            } else {
+                const double q0 = st[0], q1 = st[1], p0 = st[52], p1 = st[53];
+                const double w = st[54], w2 = w * w;
+                cost = huberCost(wd.huber, q0 * q0 + q1 * q1);
+                dD = w2 * (p0 * p0 + p1 * p1);
+                gD = w2 * (p0 * q0 + p1 * q1);
+                // in place: column c reads offsets >= c + 2, all later than slot c
+#pragma unroll
+                for (int c = 0; c < kCompact; ++c) st[c] = w2 * (st[compactOff(0, c)] * p0 + st[compactOff(1, c)] * p1);
+            }
         }
         __syncwarp();
         // landmark sums of d, g, cost and validity: segmented inclusive scans over
         // the tile's lanes (observations of one landmark are consecutive lanes)
         {
             const int seg = B.obLm[f < oe ? f : ob] - lb;  // landmark of this lane (lanes past the tile: any)
-            const double* st = out + kOut * lane;
-            const bool live = f < oe && flags[lane];
-            double d = live ? st[25] : 0.0, g = live ? st[26] : 0.0, cost = live ? st[27] : 0.0;
             int bad = f < oe && !flags[lane] ? 1 : 0;
+            float dE = 0.0f;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                const double d2 = __shfl_up_sync(0xffffffffu, d, o), g2 = __shfl_up_sync(0xffffffffu, g, o);
                 const double c2 = __shfl_up_sync(0xffffffffu, cost, o);
                 const int b2 = __shfl_up_sync(0xffffffffu, bad, o), s2 = __shfl_up_sync(0xffffffffu, seg, o);
-                if (lane >= o && s2 == seg) { d += d2; g += g2; cost += c2; bad |= b2; }
+                if constexpr (Mixed) {
+                    const float ds2 = __shfl_up_sync(0xffffffffu, dS, o), de2 = __shfl_up_sync(0xffffffffu, dE, o);
+                    const double g2 = __shfl_up_sync(0xffffffffu, gD, o);
+                    if (lane >= o && s2 == seg) {
+                        dE += de2; twoSumAdd(dS, dE, ds2);
+                        gD += g2; cost += c2; bad |= b2;
+                    }
+                } else {
+                    const double d2 = __shfl_up_sync(0xffffffffu, dD, o), g2 = __shfl_up_sync(0xffffffffu, gD, o);
+                    if (lane >= o && s2 == seg) { dD += d2; gD += g2; cost += c2; bad |= b2; }
+                }
             }
+            if constexpr (Mixed) dD = (double)dS + (double)dE;
             // the last lane of each landmark holds its sums
             const int nextSeg = __shfl_down_sync(0xffffffffu, seg, 1);
             if (f < oe && (lane == 31 || f + 1 >= oe || nextSeg != seg)) {
                 const int l = lb + seg;
-                B.lmD[l] = d; B.lmG[l] = g; B.lmCost[l] = cost; B.lmValid[l] = bad ? 0 : 1;
+                B.lmD[l] = dD; B.lmG[l] = gD; B.lmCost[l] = cost; B.lmValid[l] = bad ? 0 : 1;
             }
         }
         // cross vectors c_l: lane c < 25 owns compact column c, whose local column
@@ -244,17 +320,31 @@ __global__ void __launch_bounds__(kLinWarps * 32, 2) k_lin_landmark(DevBatch B, 
             __syncwarp();
             if (lane < kCompact) {
                 int cur = -1;
-                double accv = 0.0;
-                for (int k = fb; k < fe; ++k) {
-                    const int li = map[kCompact * k + lane];
-                    if (li != cur) {
-                        if (cur >= 0) cvec[cur] += accv;
-                        cur = li;
-                        accv = 0.0;
+                if constexpr (Mixed) {
+                    float accS = 0.0f, accE = 0.0f;
+                    for (int k = fb; k < fe; ++k) {
+                        const int li = map[kCompact * k + lane];
+                        if (li != cur) {
+                            if (cur >= 0) cvec[cur] += (double)accS + (double)accE;
+                            cur = li;
+                            accS = accE = 0.0f;
+                        }
+                        if (li >= 0 && flags[k]) twoSumAdd(accS, accE, out[kOutF * k + lane]);
                     }
-                    if (li >= 0 && flags[k]) accv += out[kOut * k + lane];
+                    if (cur >= 0) cvec[cur] += (double)accS + (double)accE;
+                } else {
+                    double accv = 0.0;
+                    for (int k = fb; k < fe; ++k) {
+                        const int li = map[kCompact * k + lane];
+                        if (li != cur) {
+                            if (cur >= 0) cvec[cur] += accv;
+                            cur = li;
+                            accv = 0.0;
+                        }
+                        if (li >= 0 && flags[k]) accv += out[kOut * k + lane];
+                    }
+                    if (cur >= 0) cvec[cur] += accv;
                 }
-                if (cur >= 0) cvec[cur] += accv;
             }
             __syncwarp();
             for (int i = lane; i < ns; i += 32) B.lmC[c0 + i] = cvec[i];
@@ -283,6 +373,7 @@ __device__ __forceinline__ void mmaF64(double& d0, double& d1, double a, double 
                  : "d"(a), "d"(b));
 }
 
+template <bool Mixed>
 __global__ void __launch_bounds__(kPairWarps * 32) k_lin_pairs(DevBatch B, const int4* chunks, int numChunks) {
     extern __shared__ double smemRaw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -341,13 +432,28 @@ __global__ void __launch_bounds__(kPairWarps * 32) k_lin_pairs(DevBatch B, const
     for (int h0 = ch.y; h0 < ch.z; h0 += kPairRows) {
         const int n = min(kPairRows, ch.z - h0);
         if (lane < n) {  // gather: each lane loads its own key-ordered row (unrolled 16-byte loads)
-            const double2* src = reinterpret_cast<const double2*>(B.keyRows + (size_t)B.keyOrder[h0 + lane] * kKeyRow);
             double* dst = rows + lane * kPairStride;
+            if constexpr (Mixed) {  // FP32 rows widened to FP64 for the Gram matrices
+                const char* src = reinterpret_cast<const char*>(B.keyRows) + (size_t)B.keyOrder[h0 + lane] * kKeyRowBytesF;
+                const double2 rv = *reinterpret_cast<const double2*>(src);
+                const float4* js = reinterpret_cast<const float4*>(src + 16);
 #pragma unroll
-            for (int q = 0; q < 27; ++q) {
-                const double2 v = src[q];
-                dst[2 * q] = v.x;
-                dst[2 * q + 1] = v.y;
+                for (int q = 0; q < 12; ++q) {
+                    const float4 v = js[q];
+                    dst[4 * q] = v.x; dst[4 * q + 1] = v.y; dst[4 * q + 2] = v.z; dst[4 * q + 3] = v.w;
+                }
+                const float2 t = *reinterpret_cast<const float2*>(src + 16 + 192);
+                dst[48] = t.x; dst[49] = t.y;
+                dst[50] = rv.x; dst[51] = rv.y;
+                dst[52] = __longlong_as_double(*reinterpret_cast<const long long*>(src + 216));
+            } else {
+                const double2* src = reinterpret_cast<const double2*>(B.keyRows + (size_t)B.keyOrder[h0 + lane] * kKeyRow);
+#pragma unroll
+                for (int q = 0; q < 27; ++q) {
+                    const double2 v = src[q];
+                    dst[2 * q] = v.x;
+                    dst[2 * q + 1] = v.y;
+                }
             }
         }
         __syncwarp();
@@ -1293,7 +1399,7 @@ __global__ void k_lm_init(DevBatch B, double lambda0) {
 
 // ---------------------------------------------------------------------------------------
 // host-side launchers (called by backend_host.cu)
-size_t linearizeSmemBytes(int maxNs) { return kLinWarps * landmarkWarpBytes(maxNs); }
+size_t linearizeSmemBytes(int maxNs, bool mixed) { return kLinWarps * landmarkWarpBytes(maxNs, mixed); }
 size_t schurSmemBytes() { return kSchurSmemDoubles * sizeof(double); }
 size_t factorSmemBytes(int maxNr) {
     // one panel of kFacPanel columns over the padded rows, three n-vectors, the diagonal block
@@ -1309,18 +1415,21 @@ cudaError_t configureKernels(size_t linSmem, size_t facSmem) {
     cudaError_t e = cudaGetDevice(&device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     if (e != cudaSuccess) return e;
-    cudaFuncAttributes la, fa, sa, pa;
-    if ((e = cudaFuncGetAttributes(&la, k_lin_landmark)) != cudaSuccess) return e;
-    if ((e = cudaFuncGetAttributes(&pa, k_lin_pairs)) != cudaSuccess) return e;
+    cudaFuncAttributes la, lm, fa, sa, pa, pm;
+    if ((e = cudaFuncGetAttributes(&la, k_lin_landmark<false>)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&lm, k_lin_landmark<true>)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&pa, k_lin_pairs<false>)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&pm, k_lin_pairs<true>)) != cudaSuccess) return e;
     if ((e = cudaFuncGetAttributes(&fa, k_factor)) != cudaSuccess) return e;
     if ((e = cudaFuncGetAttributes(&sa, k_lin_schur)) != cudaSuccess) return e;
-    const size_t linMax = (size_t)optin - la.sharedSizeBytes, facMax = (size_t)optin - fa.sharedSizeBytes;
+    const size_t linMax = (size_t)optin - std::max(la.sharedSizeBytes, lm.sharedSizeBytes), facMax = (size_t)optin - fa.sharedSizeBytes;
     const size_t schMax = (size_t)optin - sa.sharedSizeBytes;
-    if (linSmem > linMax || facSmem > facMax || schurSmemBytes() > schMax || pairCtaBytes() > (size_t)optin - pa.sharedSizeBytes)
-        return cudaErrorInvalidValue;
-    if ((e = cudaFuncSetAttribute(k_lin_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pairCtaBytes())) != cudaSuccess)
-        return e;
-    if ((e = cudaFuncSetAttribute(k_lin_landmark, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)linMax)) != cudaSuccess) return e;
+    const size_t pairMax = (size_t)optin - std::max(pa.sharedSizeBytes, pm.sharedSizeBytes);
+    if (linSmem > linMax || facSmem > facMax || schurSmemBytes() > schMax || pairCtaBytes() > pairMax) return cudaErrorInvalidValue;
+    for (auto k : {k_lin_pairs<false>, k_lin_pairs<true>})
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pairCtaBytes())) != cudaSuccess) return e;
+    for (auto k : {k_lin_landmark<false>, k_lin_landmark<true>})
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)linMax)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_lin_schur, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)schMax)) != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)facMax);
 }
@@ -1338,11 +1447,15 @@ int launchIteration(const DevBatch& B, const LaunchPlan& P, int refinement, int 
     run(CGMLI_KERNEL_ZERO, [&] { k_zero_acc<<<W, 256, 0, s>>>(B); });
     const int runBlocks = (B.numRuns + kLinWarps - 1) / kLinWarps;
     if (B.numRuns > 0)
-        run(CGMLI_KERNEL_LINEARIZE, [&] { k_lin_landmark<<<runBlocks, kLinWarps * 32, P.linSmem, s>>>(B, P.runs, P.tiles, P.maxNs); });
+        run(CGMLI_KERNEL_LINEARIZE, [&] {
+            if (B.mixed) k_lin_landmark<true><<<runBlocks, kLinWarps * 32, P.linSmem, s>>>(B, P.runs, P.tiles, P.maxNs);
+            else k_lin_landmark<false><<<runBlocks, kLinWarps * 32, P.linSmem, s>>>(B, P.runs, P.tiles, P.maxNs);
+        });
     if (P.numPairChunks > 0)
         run(CGMLI_KERNEL_LIN_PAIRS, [&] {
-            k_lin_pairs<<<(P.numPairChunks + kPairWarps - 1) / kPairWarps, kPairWarps * 32, pairCtaBytes(), s>>>(B, P.pairChunks,
-                                                                                                     P.numPairChunks);
+            const int blocks = (P.numPairChunks + kPairWarps - 1) / kPairWarps;
+            if (B.mixed) k_lin_pairs<true><<<blocks, kPairWarps * 32, pairCtaBytes(), s>>>(B, P.pairChunks, P.numPairChunks);
+            else k_lin_pairs<false><<<blocks, kPairWarps * 32, pairCtaBytes(), s>>>(B, P.pairChunks, P.numPairChunks);
         });
     if (P.numSchurChunks > 0)
         run(CGMLI_KERNEL_LIN_SCHUR, [&] { k_lin_schur<<<P.numSchurChunks, kSchurThreads, schurSmemBytes(), s>>>(B, P.schurChunks); });

@@ -238,12 +238,17 @@ int cgmli_server_create(const cgmli_server_options* options, cgmli_server** out)
         return setLastError(CGMLI_E_INVALID, "server: unknown marginalization policy");
     if (!(options->nis_threshold >= 0) || options->max_refits < 0 || options->max_refits > 64)
         return setLastError(CGMLI_E_INVALID, "server: nis_threshold < 0 or max_refits outside 0..64");
+    if (options->precision != CGMLI_PRECISION_FP64 && options->precision != CGMLI_PRECISION_MIXED)
+        return setLastError(CGMLI_E_INVALID, "server: unknown precision");
     auto* s = new cgmli_server();
     s->opt = *options;
     if (s->opt.max_batch_windows <= 0) s->opt.max_batch_windows = 512;
     if (s->opt.memory_budget_bytes <= 0) s->opt.memory_budget_bytes = 40ll << 30;
+    cgmli_solver_options so;
+    cgmli_default_options(&so);
+    so.precision = options->precision;
     for (int k = 0; k < 2; ++k) {
-        const int st = cgmli_solver_create(options->device, nullptr, &s->solver[k]);
+        const int st = cgmli_solver_create(options->device, &so, &s->solver[k]);
         if (st != CGMLI_OK) {
             for (auto* sv : s->solver) cgmli_solver_destroy(sv);
             delete s;

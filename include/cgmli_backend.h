@@ -121,8 +121,12 @@ typedef struct cgmli_window {
 } cgmli_window;
 
 typedef struct cgmli_solver_options {
-    int precision;           /* CGMLI_PRECISION_FP64; _MIXED (FP32 Jacobians, FP64 sums) is
-                                rejected with CGMLI_E_UNSUPPORTED by this build */
+    int precision;           /* CGMLI_PRECISION_FP64 (default) or _MIXED: the LM linearization
+                                evaluates the bearing factors' Jacobians and robust weights
+                                in FP32 and sums the landmark Hessian blocks (d, cross
+                                vectors) in compensated FP32; residuals, costs, gradients,
+                                the reduced system, its Cholesky and every marginalization
+                                stay FP64 */
     int refinement_steps;    /* iterative refinement after the FP64 Cholesky (0..2) */
     double initial_lambda;   /* reference: 1e-4 */
     int slabs_per_window;    /* reserved, must be 0 */
@@ -408,6 +412,7 @@ typedef struct cgmli_server_options {
                                        (cgmli_solver_solve_gated); 0: plain solve */
     int max_refits;                 /* refits of the gated solve (reference: 3) */
     int pre_gate;                   /* gated solve: gate at the submitted states first */
+    int precision;                  /* CGMLI_PRECISION_FP64 or _MIXED (cgmli_solver_options) */
 } cgmli_server_options;
 typedef struct cgmli_server cgmli_server;
 

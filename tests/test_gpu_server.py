@@ -23,8 +23,8 @@ def backend():
     return B
 
 
-def _alone(backend, w, victim, iterations):
-    s = backend.Solver()
+def _alone(backend, w, victim, iterations, precision=abi.PRECISION_FP64):
+    s = backend.Solver(precision=precision)
     s.set_windows([w])
     s.solve(iterations)
     prior = None
@@ -38,15 +38,19 @@ def _alone(backend, w, victim, iterations):
     return w.state_vector(), rep, prior
 
 
+@pytest.mark.parametrize("precision", [abi.PRECISION_FP64, abi.PRECISION_MIXED])
 @pytest.mark.parametrize("budget", [40 << 30, 1])  # 1 byte: every batch holds a single window
-def test_served_equals_alone(backend, budget):
+def test_served_equals_alone(backend, budget, precision):
+    """Also in mixed precision: a window's mixed linearization does not depend on
+    its batch neighbours, so the same bars hold."""
     n, iterations = 10, 1
     alone_windows = synth.make_windows("c4", n, seed=321)
     served_windows = synth.make_windows("c4", n, seed=321)
     x0 = [w.state_vector() for w in served_windows]
     victims = [0 if i % 3 else -1 for i in range(n)]
-    ref = [_alone(backend, w, v, iterations) for w, v in zip(alone_windows, victims)]
-    server = backend.Server(iterations=iterations, policy=abi.MARGIN_OLD, max_batch_windows=4, memory_budget_bytes=budget)
+    ref = [_alone(backend, w, v, iterations, precision) for w, v in zip(alone_windows, victims)]
+    server = backend.Server(iterations=iterations, policy=abi.MARGIN_OLD, max_batch_windows=4, memory_budget_bytes=budget,
+                            precision=precision)
     tickets = [server.submit(w, v) for w, v in zip(served_windows, victims)]
     for i, t in enumerate(tickets):
         rep, latency = server.poll(t, wait=True)
