@@ -101,6 +101,13 @@ struct cgmli_solver {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // CUDA graph of a whole solve: captured when the same launch sequence (device
+    // pointers, work decomposition, iteration budget, options) is solved a second
+    // time in a row, replayed while it stays the same; a new topology is solved
+    // eagerly, so a batch solved once pays no capture
+    cudaGraphExec_t graphExec = nullptr;
+    std::vector<char> graphKey, lastKey;
+    int graphLaunches = 0;
     cgmli_solver_options opt{};
     // topology (host copies)
     std::vector<WinDesc> win;
@@ -239,6 +246,7 @@ struct cgmli_solver {
 
     ~cgmli_solver() {
         if (stream) cudaStreamSynchronize(stream);
+        if (graphExec) cudaGraphExecDestroy(graphExec);
         DArray<double>* dbl[] = {&camR, &camT, &lmBearing, &lmVel, &lmTime, &lmC, &lmD, &lmG, &lmCost, &lmDelta, &lmPred, &lmTrial,
                                  &lmMaxInc, &obBearing, &obP, &obVel, &obTime, &pose[0], &pose[1], &sb[0], &sb[1], &ext[0], &ext[1],
                                  &rotKf[0], &rotKf[1], &rotExt[0], &rotExt[1],
@@ -494,9 +502,53 @@ static void profileHook(void* ctx, int kind, int phase) {
     cudaEventRecord(e, S->stream);
 }
 
+// Everything a captured solve depends on: the batch's device pointers and counts,
+// its work decomposition, the iteration budget and the options the kernels read.
+static std::vector<char> solveKey(const cgmli_solver* S, int iterations) {
+    const LaunchPlan P = S->plan();
+    const int ints[2] = {iterations, S->opt.refinement_steps};
+    const double lambda0 = S->opt.initial_lambda;
+    std::vector<char> k(sizeof(DevBatch) + sizeof(LaunchPlan) + sizeof(ints) + sizeof(lambda0));
+    char* p = k.data();
+    std::memcpy(p, &S->B, sizeof(DevBatch)); p += sizeof(DevBatch);
+    std::memcpy(p, &P, sizeof(LaunchPlan)); p += sizeof(LaunchPlan);
+    std::memcpy(p, ints, sizeof(ints)); p += sizeof(ints);
+    std::memcpy(p, &lambda0, sizeof(lambda0));
+    return k;
+}
+
 static int runIterations(cgmli_solver* S, int iterations, int probe, double* Sdebug) {
     cudaStream_t st = S->stream;
     if (S->profile) S->collectKernelTimes();
+    if (!probe && !Sdebug && !S->profile) {
+        std::vector<char> key = solveKey(S, iterations);
+        if (!(S->graphExec && key == S->graphKey) && key == S->lastKey) {
+            // second solve of the same sequence: capture it
+            if (S->graphExec) { cudaGraphExecDestroy(S->graphExec); S->graphExec = nullptr; }
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            int launches = launchLmInit(S->B, S->opt.initial_lambda, st);
+            for (int it = 0; it < iterations; ++it)
+                launches += launchIteration(S->B, S->plan(), S->opt.refinement_steps, iterations, 0, nullptr, st, nullptr, nullptr);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(st, &g);
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&S->graphExec, g, 0);
+            if (g) cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                S->graphExec = nullptr;
+                return cudaFail(e, "solve graph capture");
+            }
+            S->graphKey = key;
+            S->graphLaunches = launches;
+        }
+        S->lastKey = std::move(key);
+        if (S->graphExec && S->lastKey == S->graphKey) {
+            CK(cudaEventRecord(S->ev0, st));
+            CK(cudaGraphLaunch(S->graphExec, st));
+            CK(cudaEventRecord(S->ev1, st));
+            S->lastLaunches = S->graphLaunches;
+            return CGMLI_OK;
+        }
+    }
     CK(cudaEventRecord(S->ev0, st));
     int launches = launchLmInit(S->B, S->opt.initial_lambda, st);
     for (int it = 0; it < iterations; ++it)

@@ -908,7 +908,9 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_victim(MargBatch M) {
 
 // ---------------------------------------------------------------------------------------
 // Fast path, one CTA per window with the separator information E in shared
-// memory (n <= kFastMaxN), for spectra with a clean gap at the cutoff
+// memory (n <= kFastMaxN) or, for wider separators, in the window's eigenvector
+// scratch in global memory (the eigen path re-initializes it when this path
+// declines), for spectra with a clean gap at the cutoff
 // max(1e-12, 1e-9 lambda_max): nf eigenvalues within |lambda| < 1e-6 cutoff,
 // the other k = n - nf above twice the cutoff.  The eigen path then keeps
 // exactly the k large eigenpairs, and its prior (A = sqrt(lambda) u^T,
@@ -929,10 +931,11 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_victim(MargBatch M) {
 // bound null(A) is then within 1e-10 of the negligible eigenspace, so A^T A
 // and A^T r0 agree with the eigen path's far below its own rounding.  Other
 // windows are left to k_marg_eigen.
-constexpr int kFastMaxN = 160;
+constexpr int kFastMaxN = 160;    // E in shared memory up to this width
 constexpr int kFastMaxFree = 32;  // null directions handled by the projection
+__host__ __device__ constexpr size_t fastVecBytes(int n) { return sizeof(double) * 5 * (size_t)n + sizeof(int) * 3 * (size_t)n; }
 __host__ __device__ constexpr size_t fastSmemBytes(int n) {
-    return sizeof(double) * ((size_t)n * n + 5 * (size_t)n) + sizeof(int) * 3 * (size_t)n;
+    return n <= kFastMaxN ? sizeof(double) * (size_t)n * n + fastVecBytes(n) : fastVecBytes(n);
 }
 
 // Number of eigenvalues of the symmetric tridiagonal (d, e) below x, e[i]
@@ -956,10 +959,11 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_fast(MargBatch M) {
     const int n = mw.nr;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
     if (tid == 0) M.fast[w] = 0;
-    if (mw.m == 0 || n == 0 || n > kFastMaxN || M.status[w] != CGMLI_OK) return;
+    if (mw.m == 0 || n == 0 || n > kMargMaxSep || M.status[w] != CGMLI_OK) return;
     extern __shared__ double fsm[];
-    double* S = fsm;          // n x n row-major
-    double* v = S + n * n;
+    const bool inShared = n <= kFastMaxN;
+    double* S = inShared ? fsm : M.sepV + mw.sep0;  // n x n row-major
+    double* v = inShared ? fsm + n * n : fsm;
     double* p = v + n;
     double* wv = p + n;
     double* d = wv + n;
@@ -1600,7 +1604,9 @@ cudaError_t configureMarginalization(size_t visualSmem, size_t rowsSmem, int max
     if (e != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_marg_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rowsSmem)) != cudaSuccess)
         return e;
-    *fastSmem = maxFastNr > 0 ? (long long)fastSmemBytes(maxFastNr < kFastMaxN ? maxFastNr : kFastMaxN) : 0;
+    *fastSmem = maxFastNr > 0 ? (long long)std::max(fastSmemBytes(maxFastNr < kFastMaxN ? maxFastNr : kFastMaxN),
+                                                   fastSmemBytes(maxFastNr < kMargMaxSep ? maxFastNr : kMargMaxSep))
+                              : 0;
     if ((e = cudaFuncSetAttribute(k_marg_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fastSmemBytes(kFastMaxN))) !=
         cudaSuccess)
         return e;
