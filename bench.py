@@ -428,6 +428,7 @@ def run_mixed(args, local, backend, windows, init, solver, dist):
     for w, x in zip(windows, init):
         w.set_state_vector(x)
     mixed = backend.Solver(device=local, precision=abi.PRECISION_MIXED)
+    mixed.set_tuning(**solver.get_tuning())
     mixed.set_windows(windows)
     mixed.checkpoint()
     # first LM step at lambda = 1e-4 from the initial states, both precisions
@@ -547,7 +548,9 @@ def main():
     windows = synth.make_windows("c4", args.windows, seed=rank_seed(args.seed, rank))
     init = [w.state_vector() for w in windows]
     solver = backend.Solver(device=local)
-    solver.set_windows(windows)
+    # the work decomposition comes from the autotuner (timed on this batch); it
+    # leaves the batch set with the fastest one
+    tuning = solver.autotune(windows, args.iterations)
     solver.checkpoint()
 
     def barrier():
@@ -643,6 +646,7 @@ def main():
     d2h = sum(window_bytes(w)[1] for w in windows)
     e2e_times = []
     e2e_solver = backend.Solver(device=local)
+    e2e_solver.set_tuning(tuning["run_landmarks"], tuning["pair_chunk"], tuning["schur_rows"])
     for it in range(1 + max(1, args.steps // 2)):
         for w, x in zip(windows, init):
             w.set_state_vector(x)
@@ -731,7 +735,7 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup),
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic", "config": config_dict(args, world),
+            "dtype": "f64", "data": "synthetic", "config": dict(config_dict(args, world), tuning=tuning),
             "clocks": clocks.summary(), "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
             "cpu_baseline": cpu_baseline, "plain_path": plain,
             "served_vs_plain": (value / world) / plain["windows_per_s"] if plain else None,

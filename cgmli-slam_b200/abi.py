@@ -47,6 +47,10 @@ class ImuParameters(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("run_landmarks", C.c_int), ("pair_chunk", C.c_int), ("schur_rows", C.c_int), ("ms", C.c_double)]
+
+
 class GateReport(C.Structure):
     _fields_ = [("passes", C.c_int), ("rejected_pre", C.c_int), ("evaluated", C.c_int), ("rejected_last", C.c_int),
                 ("rejected_total", C.c_int),
@@ -112,6 +116,7 @@ def declare_backend(lib: C.CDLL) -> C.CDLL:
     _proto(lib, "cgmli_last_error", C.c_char_p, [])
     _proto(lib, "cgmli_default_options", None, [C.POINTER(SolverOptions)])
     _proto(lib, "cgmli_topology_check", C.c_int, [W, C.c_int, C.c_int, c_double_p])
+    _proto(lib, "cgmli_topology_check_tuned", C.c_int, [W, C.c_int, C.c_int, C.POINTER(Tuning), c_double_p])
     _proto(lib, "cgmli_solver_create", C.c_int, [C.c_int, C.POINTER(SolverOptions), C.POINTER(C.c_void_p)])
     _proto(lib, "cgmli_solver_destroy", None, [S])
     _proto(lib, "cgmli_solver_set_windows", C.c_int, [S, W, C.c_int])
@@ -157,6 +162,9 @@ def declare_backend(lib: C.CDLL) -> C.CDLL:
     _proto(lib, "cgmli_solver_refresh_imu", C.c_int, [S, C.c_double, C.c_double, c_int_p])
     _proto(lib, "cgmli_solver_read_imu", C.c_int, [S, C.c_int, C.POINTER(FrozenImu)])
     _proto(lib, "cgmli_solver_solve_gated", C.c_int, [S, C.c_int, C.c_double, C.c_int, C.c_int])
+    _proto(lib, "cgmli_solver_set_tuning", C.c_int, [S, C.POINTER(Tuning)])
+    _proto(lib, "cgmli_solver_get_tuning", C.c_int, [S, C.POINTER(Tuning)])
+    _proto(lib, "cgmli_solver_autotune", C.c_int, [S, W, C.c_int, C.c_int, C.POINTER(Tuning)])
     _proto(lib, "cgmli_solver_set_imu_merge_limits", C.c_int, [S, C.c_double, C.c_int])
     _proto(lib, "cgmli_solver_read_merged_imu", C.c_int, [S, C.c_int, c_int_p, C.POINTER(FrozenImu)])
     _proto(lib, "cgmli_solver_calibration_information", C.c_int, [S, C.c_int])
@@ -187,7 +195,8 @@ BACKEND_SYMBOLS = [
     "cgmli_server_read_prior", "cgmli_server_release", "cgmli_server_replay", "cgmli_server_read_gate", "cgmli_imu_preintegrate",
     "cgmli_imu_last_timing", "cgmli_solver_set_imu_samples", "cgmli_solver_refresh_imu", "cgmli_solver_read_imu",
     "cgmli_solver_solve_gated", "cgmli_solver_read_gate", "cgmli_solver_set_imu_merge_limits", "cgmli_solver_read_merged_imu",
-    "cgmli_solver_calibration_information", "cgmli_solver_read_calibration_information",
+    "cgmli_solver_calibration_information", "cgmli_solver_read_calibration_information", "cgmli_topology_check_tuned",
+    "cgmli_solver_set_tuning", "cgmli_solver_get_tuning", "cgmli_solver_autotune",
 ]
 KERNEL_NAMES = ["zero_acc", "linearize", "retained", "factor", "candidate", "backsub_trial", "retained_trial", "lm_update", "accept",
                 "lin_pairs", "lin_schur"]

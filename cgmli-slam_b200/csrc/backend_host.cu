@@ -105,6 +105,7 @@ struct cgmli_solver {
     // pointers, work decomposition, iteration budget, options) is solved a second
     // time in a row, replayed while it stays the same; a new topology is solved
     // eagerly, so a batch solved once pays no capture
+    PlanParams tune;  // work decomposition of the next set_windows (cgmli_tuning)
     cudaGraphExec_t graphExec = nullptr;
     std::vector<char> graphKey, lastKey;
     int graphLaunches = 0;
@@ -290,12 +291,31 @@ extern "C" {
 
 const char* cgmli_last_error(void) { return g_error.c_str(); }
 
+static int planOf(const cgmli_tuning* t, PlanParams& p) {
+    p = PlanParams();
+    if (!t) return CGMLI_OK;
+    if (t->run_landmarks < 0 || t->run_landmarks > 4096) return fail(CGMLI_E_INVALID, "tuning: run_landmarks outside 0..4096");
+    if (t->pair_chunk != 0 && (t->pair_chunk < 8 || t->pair_chunk > 1024)) return fail(CGMLI_E_INVALID, "tuning: pair_chunk outside 8..1024");
+    if (t->schur_rows != 0 && (t->schur_rows < 8 || t->schur_rows > kSchurMaxRows))
+        return fail(CGMLI_E_INVALID, "tuning: schur_rows outside 8..128");
+    p.runLandmarks = t->run_landmarks;
+    if (t->pair_chunk) p.pairChunk = t->pair_chunk;
+    if (t->schur_rows) p.schurRows = t->schur_rows;
+    return CGMLI_OK;
+}
+
 int cgmli_topology_check(const cgmli_window* windows, int count, int threads, double* seconds) {
+    return cgmli_topology_check_tuned(windows, count, threads, nullptr, seconds);
+}
+
+int cgmli_topology_check_tuned(const cgmli_window* windows, int count, int threads, const cgmli_tuning* tuning, double* seconds) {
     if (!windows || count < 1) return fail(CGMLI_E_INVALID, "empty window list");
+    PlanParams plan;
+    if (planOf(tuning, plan) != CGMLI_OK) return CGMLI_E_INVALID;
     const auto t0 = std::chrono::steady_clock::now();
     HostBatch hb;
     std::string why;
-    int st = buildHostBatch(windows, count, threads, hb, why);
+    int st = buildHostBatch(windows, count, threads, hb, why, nullptr, plan);
     const auto t1 = std::chrono::steady_clock::now();
     if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
     if (st != CGMLI_OK) return fail(st, why);
@@ -385,7 +405,7 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
         part(S->lmNs, hb.lmNs, l0, ln); part(S->lmNx, hb.lmNx, l0, ln); part(S->lmBearing, hb.lmBearing, 3 * l0, 3 * ln);
         part(S->lmVel, hb.lmVel, 3 * l0, 3 * ln); part(S->lmTime, hb.lmTime, l0, ln); part(S->rho[0], hb.rho, l0, ln);
     };
-    const int built = buildHostBatch(windows, count, 0, hb, why, &ready);
+    const int built = buildHostBatch(windows, count, 0, hb, why, &ready, S->tune);
     if (built != CGMLI_OK) return fail(built, why);
     CK(streamErr);
     S->win = hb.win;
@@ -565,6 +585,81 @@ int cgmli_solver_solve(cgmli_solver* S, int max_iterations) {
     if (max_iterations < 1) return fail(CGMLI_E_INVALID, "max_iterations < 1");
     CK(cudaSetDevice(S->device));
     return runIterations(S, max_iterations, 0, nullptr);
+}
+
+int cgmli_solver_set_tuning(cgmli_solver* S, const cgmli_tuning* tuning) {
+    if (!S || !tuning) return fail(CGMLI_E_INVALID, "set_tuning: null solver or tuning");
+    PlanParams p;
+    if (planOf(tuning, p) != CGMLI_OK) return CGMLI_E_INVALID;
+    S->tune = p;
+    return CGMLI_OK;
+}
+
+int cgmli_solver_get_tuning(cgmli_solver* S, cgmli_tuning* tuning) {
+    if (!S || !tuning) return fail(CGMLI_E_INVALID, "get_tuning: null solver or tuning");
+    tuning->run_landmarks = S->tune.runLandmarks;
+    tuning->pair_chunk = S->tune.pairChunk;
+    tuning->schur_rows = S->tune.schurRows;
+    tuning->ms = 0.0;
+    return CGMLI_OK;
+}
+
+// Coordinate search: each parameter mainly shapes one pass (runs: the landmark
+// and trial passes; pair chunks: the J^T J pass; Schur rows: the Schur pass), so
+// they are tuned one after the other, each over a few multiples of the current value.
+int cgmli_solver_autotune(cgmli_solver* S, const cgmli_window* windows, int count, int iterations, cgmli_tuning* best) {
+    if (!S || !windows || count < 1) return fail(CGMLI_E_INVALID, "autotune: null solver or empty window list");
+    if (iterations < 1) return fail(CGMLI_E_INVALID, "autotune: iterations < 1");
+    const bool profiled = S->profile;
+    S->profile = false;
+    auto measure = [&](const PlanParams& p, double& ms) -> int {
+        S->tune = p;
+        int st = cgmli_solver_set_windows(S, windows, count);
+        if (st == CGMLI_OK) st = cgmli_solver_checkpoint(S);
+        for (int rep = 0; rep < 2 && st == CGMLI_OK; ++rep) {  // the first solve warms caches and clocks
+            if (rep > 0) st = cgmli_solver_rollback(S);
+            if (st == CGMLI_OK) st = runIterations(S, iterations, 0, nullptr);
+            if (st == CGMLI_OK) {
+                float t = 0;
+                cudaError_t e = cudaEventSynchronize(S->ev1);
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&t, S->ev0, S->ev1);
+                if (e != cudaSuccess) st = cudaFail(e, "autotune timing");
+                ms = t;
+            }
+        }
+        return st;
+    };
+    PlanParams cur = S->tune;
+    if (cur.runLandmarks <= 0) {
+        long long lm = 0;
+        for (int i = 0; i < count; ++i) lm += windows[i].num_landmarks;
+        cur.runLandmarks = std::max<long long>(4, std::min<long long>(64, lm / (148ll * 6 * 4)));
+    }
+    double bestMs = 0;
+    int st = measure(cur, bestMs);
+    for (int param = 0; param < 3 && st == CGMLI_OK; ++param) {
+        const int base = param == 0 ? cur.runLandmarks : param == 1 ? cur.pairChunk : cur.schurRows;
+        const int lo = param == 0 ? 2 : 8, hi = param == 0 ? 4096 : param == 1 ? 1024 : kSchurMaxRows;
+        for (const int v : {base / 2, base * 2}) {
+            if (v < lo || v > hi) continue;
+            PlanParams p = cur;
+            (param == 0 ? p.runLandmarks : param == 1 ? p.pairChunk : p.schurRows) = v;
+            double ms = 0;
+            if ((st = measure(p, ms)) != CGMLI_OK) break;
+            if (ms < bestMs) { bestMs = ms; cur = p; }
+        }
+    }
+    S->profile = profiled;
+    S->tune = cur;
+    if (st != CGMLI_OK) return st;
+    if ((st = cgmli_solver_set_windows(S, windows, count)) != CGMLI_OK) return st;
+    if (best) {
+        best->run_landmarks = cur.runLandmarks;
+        best->pair_chunk = cur.pairChunk;
+        best->schur_rows = cur.schurRows;
+        best->ms = bestMs;
+    }
+    return CGMLI_OK;
 }
 
 int cgmli_solver_solve_gated(cgmli_solver* S, int max_iterations, double nis_threshold, int max_refits, int pre_gate) {

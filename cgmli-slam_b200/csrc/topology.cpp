@@ -113,7 +113,7 @@ int validateWindow(const cgmli_window& w, int index, std::string& why) {
 }
 
 int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatch& hb, std::string& why,
-                   const std::function<void(int, int)>* ready) {
+                   const std::function<void(int, int)>* ready, const PlanParams& plan) {
     if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
     threads = std::min(threads, 64);
     // ---- validation (parallel)
@@ -124,6 +124,7 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
         if (vst[i] != CGMLI_OK) { why = vwhy[i]; return vst[i]; }
     // ---- phase 0: offsets from the windows' sizes
     hb.win.assign(count, WinDesc{});
+    hb.plan = plan;
     hb.maxNpc = 0; hb.maxNr = 0; hb.maxNs = 1;
     std::vector<long long> pA0(count), pR0(count), pRef0(count);
     std::vector<int> pblk0(count);
@@ -183,7 +184,7 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
     sizeTo(hb.priorKind, pblk); sizeTo(hb.priorIndex, pblk); sizeTo(hb.priorCol, pblk); sizeTo(hb.priorOff, pblk);
     sizeTo(hb.priorA, pA); sizeTo(hb.priorR0, pR); sizeTo(hb.priorRef, pRef);
     hb.lmObsBegin[lm] = ob;
-    const int runLen = runLength(lm);
+    const int runLen = plan.runLandmarks > 0 ? plan.runLandmarks : runLength(lm);
     // ---- phase 1: every window on its own thread
     std::vector<WindowPart> part(count);
     auto phase1 = [&](int i) {
@@ -400,8 +401,8 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
             std::sort(kv.begin(), kv.end());
             for (int g = 0; g < F; ++g) ko[g] = kv[g].second;
         }
-        for (int c0 = 0; c0 < F; c0 += 32)
-            P.pairChunks.push_back(make_int4(i, d.obs0 + c0, d.obs0 + std::min(F, c0 + 32), 0));
+        for (int c0 = 0; c0 < F; c0 += plan.pairChunk)
+            P.pairChunks.push_back(make_int4(i, d.obs0 + c0, d.obs0 + std::min(F, c0 + plan.pairChunk), 0));
         // Schur chunks: runs of consecutive landmarks whose support columns
         // together fit the chunk's shared rows (schurChunkFits); the column
         // union of each chunk and every landmark's map into it.  Unions are kept
@@ -465,7 +466,7 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
             for (int q = 0; q < L; ++q) {
                 blocksOf(q);
                 int nuNew = columnsIn(U, &Ul);
-                if (q > q0 && !schurChunkFits(q - q0 + 1, nuNew)) {
+                if (q > q0 && (q - q0 + 1 > plan.schurRows || !schurChunkFits(q - q0 + 1, nuNew))) {
                     closeChunk(q);
                     nuNew = columnsIn(Ul, nullptr);
                 }
@@ -598,7 +599,7 @@ int checkHostBatch(const cgmli_window* windows, int count, const HostBatch& hb, 
     std::vector<int> obCover(hb.totalObs, 0);
     for (const int4& c : hb.pairChunks) {
         const WinDesc& d = hb.win[c.x];
-        if (c.y < d.obs0 || c.z > d.obs0 + d.F || c.z - c.y > 32 || c.y >= c.z) return bad(c.x, "pair chunk");
+        if (c.y < d.obs0 || c.z > d.obs0 + d.F || c.z - c.y > hb.plan.pairChunk || c.y >= c.z) return bad(c.x, "pair chunk");
         for (int k = c.y; k < c.z; ++k) ++obCover[k];
     }
     for (int o = 0; o < hb.totalObs; ++o)
@@ -609,7 +610,8 @@ int checkHostBatch(const cgmli_window* windows, int count, const HostBatch& hb, 
         if (c.y < d.lm0 || c.z > d.lm0 + d.L || c.y >= c.z || c.w < 0 || c.w >= (long long)hb.schurCols.size())
             return bad(c.x, "Schur chunk");
         const int nu = hb.schurCols[c.w];
-        if (nu < 1 || nu > d.Npc || c.w + nu >= (long long)hb.schurCols.size() || !schurChunkFits(c.z - c.y, nu))
+        if (nu < 1 || nu > d.Npc || c.w + nu >= (long long)hb.schurCols.size() || !schurChunkFits(c.z - c.y, nu) ||
+            c.z - c.y > hb.plan.schurRows)
             return bad(c.x, "Schur chunk columns");
         for (int k = 1; k <= nu; ++k) {
             const int col = hb.schurCols[c.w + k];

@@ -157,7 +157,15 @@ void sizeTo(V& v, size_t n) {
     v.resize(n);
 }
 
+// Work decomposition chosen by the caller or the autotuner (cgmli_tuning).
+struct PlanParams {
+    int runLandmarks = 0;  // 0: from the batch size
+    int pairChunk = 32;
+    int schurRows = kSchurMaxRows;
+};
+
 struct HostBatch {
+    PlanParams plan;  // the decomposition the batch was built with
     std::vector<WinDesc> win;
     HVec<int4> runs;         // {window, first tile, end tile, -}
     HVec<int2> tiles;        // {first landmark, end landmark}
@@ -200,7 +208,7 @@ int validateWindow(const cgmli_window& w, int index, std::string& why);
 // [w0, w1) have their landmark and observation arrays final, before the rest of
 // the batch is built, so that their uploads can overlap the remaining host work.
 int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatch& out, std::string& why,
-                   const std::function<void(int, int)>* ready = nullptr);
+                   const std::function<void(int, int)>* ready = nullptr, const PlanParams& plan = PlanParams());
 
 // Invariants of a built batch (used by the diagnostic entry point and tests).
 int checkHostBatch(const cgmli_window* windows, int count, const HostBatch& hb, std::string& why);

@@ -157,6 +157,19 @@ void cgmli_default_options(cgmli_solver_options *options);
  * reference. */
 int cgmli_topology_check(const cgmli_window *windows, int count, int threads, double *seconds);
 
+/* Work decomposition of a batch (the kernels' tile shapes are fixed; these are
+ * the shapes of the work units the host planner cuts for them). */
+typedef struct cgmli_tuning {
+    int run_landmarks;  /* landmarks per warp run of the linearization and trial passes;
+                           0: from the batch size (enough runs to fill the GPU) */
+    int pair_chunk;     /* key-ordered observations per warp of the J^T J pass, 8..1024 (0: 32) */
+    int schur_rows;     /* landmarks per chunk of the Schur pass, 8..128 (0: 128) */
+    double ms;          /* cgmli_solver_autotune: device time of the timed solve */
+} cgmli_tuning;
+/* cgmli_topology_check with a given work decomposition (NULL: the default). */
+int cgmli_topology_check_tuned(const cgmli_window *windows, int count, int threads, const cgmli_tuning *tuning,
+                               double *seconds);
+
 /* Replaces VisualCudaWorkspace construction (src/backend/BackendOptimizer.cpp:334-341). */
 int cgmli_solver_create(int device, const cgmli_solver_options *options, cgmli_solver **out);
 void cgmli_solver_destroy(cgmli_solver *solver);
@@ -165,6 +178,16 @@ void cgmli_solver_destroy(cgmli_solver *solver);
  * newTopology=true, configureRetained and configureResident;
  * src/backend/VisualCudaBatch.cu:433-511,606-624,673-691).  All later calls
  * operate on these windows, in this order. */
+/* Work decomposition used by the next cgmli_solver_set_windows (validated:
+ * CGMLI_E_INVALID outside the ranges of cgmli_tuning) and the one in use. */
+int cgmli_solver_set_tuning(cgmli_solver *solver, const cgmli_tuning *tuning);
+int cgmli_solver_get_tuning(cgmli_solver *solver, cgmli_tuning *tuning);
+/* Autotuner: builds the batch with candidate work decompositions (coordinate
+ * search over run_landmarks, pair_chunk and schur_rows from the current one),
+ * times `iterations` LM iterations of each from the windows' states on the
+ * device, keeps the fastest for later set_windows calls and leaves the batch
+ * set with it (states as given).  *best (may be NULL) receives it. */
+int cgmli_solver_autotune(cgmli_solver *solver, const cgmli_window *windows, int count, int iterations, cgmli_tuning *best);
 int cgmli_solver_set_windows(cgmli_solver *solver, const cgmli_window *windows, int count);
 /* Upload new state values only (same topology). */
 int cgmli_solver_upload_states(cgmli_solver *solver, const cgmli_window *windows, int count);

@@ -253,3 +253,38 @@ def test_graph_replay_matches_eager(backend):
         assert reports == base_reports and launches == base_launches
         for a, b in zip(states, base_states):
             assert rel(a, b) < 1e-9
+
+
+def test_tuning_keeps_the_step(backend):
+    """A work decomposition changes only how the passes split their work: the
+    step equals the default decomposition's (atomic reduction order aside)."""
+    windows = synth.make_windows("c4", 16, seed=71)
+    ref = backend.Solver()
+    ref.set_windows(windows)
+    ref.step(1e-4)
+    for tuning in ((3, 128, 16), (64, 8, 128)):
+        s = backend.Solver()
+        s.set_tuning(*tuning)
+        s.set_windows(windows)
+        assert s.get_tuning() == dict(zip(("run_landmarks", "pair_chunk", "schur_rows"), tuning))
+        s.step(1e-4)
+        for i in range(len(windows)):
+            a, b = s.read_step(i), ref.read_step(i)
+            assert a["status"] == b["status"] == 0
+            assert rel(a["delta"], b["delta"]) < 1e-9
+
+
+def test_autotune(backend):
+    windows = synth.make_windows("c4", 16, seed=73)
+    s = backend.Solver()
+    best = s.autotune(windows, 2)
+    assert best["ms"] > 0 and best["run_landmarks"] >= 2
+    assert 8 <= best["pair_chunk"] <= 1024 and 8 <= best["schur_rows"] <= 128
+    assert s.get_tuning() == {k: best[k] for k in ("run_landmarks", "pair_chunk", "schur_rows")}
+    # the batch is left set with the chosen decomposition and the given states
+    ref = backend.Solver()
+    ref.set_windows(windows)
+    ref.step(1e-4)
+    s.step(1e-4)
+    for i in range(len(windows)):
+        assert rel(s.read_step(i)["delta"], ref.read_step(i)["delta"]) < 1e-9

@@ -73,3 +73,23 @@ def test_window_above_visual_limit_is_rejected(lib):
     arr[0].estimate_extrinsics = 1
     code = lib.cgmli_topology_check(arr, 1, 0, None)
     assert code == 9  # CGMLI_E_LIMIT
+
+
+@pytest.mark.parametrize("tuning", [(2, 8, 8), (8, 64, 32), (64, 1024, 128), (0, 0, 0), (4096, 128, 16)])
+def test_tuned_layout(lib, tuning):
+    """Every work decomposition the autotuner may pick keeps the invariants
+    (runs cover each landmark once, pair chunks and Schur chunks within their
+    limits and windows)."""
+    windows = synth.make_windows("c4", 12, seed=17)
+    arr = synth.window_array(windows)
+    t = abi.Tuning(*tuning, 0.0)
+    code = lib.cgmli_topology_check_tuned(arr, len(arr), 0, C.byref(t), None)
+    assert code == 0, lib.cgmli_last_error().decode()
+
+
+@pytest.mark.parametrize("tuning", [(-1, 32, 128), (0, 4, 128), (0, 2048, 128), (0, 32, 4), (0, 32, 256)])
+def test_tuning_outside_its_ranges_is_rejected(lib, tuning):
+    windows = synth.make_windows("c4", 2, seed=3)
+    arr = synth.window_array(windows)
+    t = abi.Tuning(*tuning, 0.0)
+    assert lib.cgmli_topology_check_tuned(arr, len(arr), 0, C.byref(t), None) == abi.E_INVALID
