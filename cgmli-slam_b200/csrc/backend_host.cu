@@ -123,7 +123,8 @@ struct cgmli_solver {
     DArray<int4> dPairChunks, dSchurChunks;
     DArray<int> schurCols;
     DArray<unsigned short> lmUmap;
-    DArray<int> obLm, keyOrder;
+    DArray<int> obLm, keyOrder, bigFirst;
+    HVec<int> hBigFirst;
     DArray<double> keyRows;
     DArray<double> sch;
     DArray<double> camR, camT;
@@ -167,6 +168,8 @@ struct cgmli_solver {
     // pinned staging of the marginalization's inputs, and the event after their uploads
     HVec<MargElim> hMargElim;
     HVec<MargWin> hMargWin;      // pinned: a pageable upload would first wait for the stream's solve
+    HVec<int> hMargOrder;
+    DArray<int> dMargOrder;
     HVec<WinDesc> hWin;
     HVec<int> hMargCols, hMargObsMap, hMargPoseCol, hMargSbCol, hMargExtCol;
     HVec<int> hMargVisCol, hMargVisPose, hMargVisExt, hMargSlow;
@@ -259,7 +262,7 @@ struct cgmli_solver {
                                &solveStatus, &lmNx, &obXslot};
         for (auto* a : ints) a->release();
         lmC0.release(); dWin.release(); dLm.release(); dRuns.release(); dTiles.release();
-        dPairChunks.release(); dSchurChunks.release(); schurCols.release(); lmUmap.release(); obLm.release(); keyOrder.release(); keyRows.release(); sch.release();
+        dPairChunks.release(); dSchurChunks.release(); schurCols.release(); lmUmap.release(); obLm.release(); keyOrder.release(); bigFirst.release(); keyRows.release(); sch.release();
         snapPose.release(); snapSb.release(); snapExt.release(); snapTd.release(); snapRho.release();
         imuTimes.release(); imuT0.release(); imuT1.release(); imuReadings.release(); imuRanges.release(); imuStatus.release();
         imuRefreshed.release(); imuRefreshScratch.release();
@@ -267,7 +270,7 @@ struct cgmli_solver {
         mergeRange.release(); mergeKf.release(); mergeStatus.release(); mergeFlag.release(); mergeT0.release(); mergeT1.release();
         mergeOut.release();
         calibWork0.release(); calibWork.release(); calibCond.release(); calibEvals.release();
-        dMargWin.release(); dMargElim.release();
+        dMargWin.release(); dMargElim.release(); dMargOrder.release();
         DArray<int>* mi[] = {&margCols, &margObsMap, &margPoseCol, &margSbCol, &margExtCol, &margRank, &margStatus, &margFast,
                              &margVisCol, &margVisPose, &margVisExt, &margSlow};
         for (auto* a : mi) a->release();
@@ -419,6 +422,14 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     S->hWin.assign(S->win.begin(), S->win.end());  // pinned staging: the copy stays asynchronous
     CK(S->dWin.upload(S->hWin, st));
     CK(S->dLm.reserve(count));
+    {
+        auto& order = S->hBigFirst;
+        sizeTo(order, count);
+        for (int i = 0; i < count; ++i) order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return S->win[a].Nr > S->win[b].Nr; });
+        CK(S->bigFirst.reserve(count));
+        CK(cudaMemcpyAsync(S->bigFirst.p, order.data(), count * sizeof(int), cudaMemcpyHostToDevice, st));
+    }
     CK(S->dRuns.upload(hb.runs, st));
     CK(S->dTiles.upload(hb.tiles, st));
     CK(S->dPairChunks.upload(hb.pairChunks, st));
@@ -454,7 +465,7 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     B.numCam = hb.totalCam; B.numImu = hb.totalImu;
     B.numRuns = (int)hb.runs.size();
     B.mixed = S->opt.precision == CGMLI_PRECISION_MIXED ? 1 : 0;
-    B.win = S->dWin.p; B.lm = S->dLm.p;
+    B.win = S->dWin.p; B.lm = S->dLm.p; B.bigFirst = S->bigFirst.p;
     B.camR = S->camR.p; B.camT = S->camT.p; B.camExt = S->camExt.p;
     B.lmWin = S->lmWin.p; B.lmKf = S->lmKf.p; B.lmCam = S->lmCam.p; B.lmObsBegin = S->lmObsBegin.p;
     B.lmBearing = S->lmBearing.p; B.lmVel = S->lmVel.p; B.lmTime = S->lmTime.p;
@@ -1379,6 +1390,16 @@ static int marginalizeImpl(cgmli_solver* S, const int* victim_kf, int policy, bo
     CK(configureMarginalization(smem, rowsSmem, maxNr, maxFastNr, &eigenSmem, &fastSmem));
     S->hMargWin.assign(mwv.begin(), mwv.end());  // guarded by margUploaded like the other staging
     CK(S->dMargWin.upload(S->hMargWin, st));
+    {
+        auto& order = S->hMargOrder;
+        sizeTo(order, mwv.size());
+        for (size_t i = 0; i < mwv.size(); ++i) order[i] = (int)i;
+        // the wider of the eliminated and kept blocks sets the CTA's work
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int a, int b) { return std::max(mwv[a].nr, mwv[a].nm) > std::max(mwv[b].nr, mwv[b].nm); });
+        CK(S->dMargOrder.reserve(std::max<size_t>(1, mwv.size())));
+        CK(cudaMemcpyAsync(S->dMargOrder.p, order.data(), mwv.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    }
     CK(S->dMargElim.upload(elims, st));
     CK(S->margCols.upload(cols, st));
     CK(S->margObsMap.upload(obsMap, st));
@@ -1408,7 +1429,7 @@ static int marginalizeImpl(cgmli_solver* S, const int* victim_kf, int policy, bo
     M.numElim = (int)elims.size();
     M.eigenSmem = eigenSmem;
     M.fastSmem = fastSmem;
-    M.win = S->dMargWin.p; M.elim = S->dMargElim.p; M.cols = S->margCols.p; M.obsMap = S->margObsMap.p;
+    M.win = S->dMargWin.p; M.bigFirst = S->dMargOrder.p; M.elim = S->dMargElim.p; M.cols = S->margCols.p; M.obsMap = S->margObsMap.p;
     M.poseCol = S->margPoseCol.p; M.sbCol = S->margSbCol.p; M.extCol = S->margExtCol.p;
     M.H = S->margH.p; M.b = S->margB.p; M.sepH = S->margSepH.p; M.sepV = S->margSepV.p; M.sepB = S->margSepB.p;
     M.evals = S->margEvals.p; M.A = S->margA.p; M.r0 = S->margR0.p; M.X = S->margX.p;

@@ -56,6 +56,8 @@ struct DevBatch {
     int mixed;  // CGMLI_PRECISION_MIXED: FP32 Jacobians, weights and landmark sums in the linearization
     const WinDesc* win;
     WinLM* lm;
+    const int* bigFirst;  // windows by decreasing retained dimension: block order of the one-CTA-per-window
+                          // kernels, so that the longest windows start first and the last wave is short
     // cameras
     const double* camR; const double* camT; const int* camExt;  // camExt: global extrinsic index
     // landmarks
@@ -141,6 +143,8 @@ struct MargBatch {
     long long eigenSmem;  // dynamic shared memory of the eigen CTA (packed separator, eigenvectors when they fit)
     long long fastSmem;   // dynamic shared memory of the full-rank fast path
     const MargWin* win;
+    const int* bigFirst;  // windows by decreasing width of their larger block: block order of the
+                          // one-CTA-per-window kernels
     const MargElim* elim;
     const int* cols;     // local column -> marginalization column
     const int* obsMap;   // 5 per observation of an eliminated landmark: local start of

@@ -573,7 +573,7 @@ __device__ double blockSum(double v, double* red) {
 // as block-structured accumulation.  Also evaluates the residual cost of the
 // candidate state when `trial` is set (launchTrial, :715-721).
 __global__ void __launch_bounds__(256, 2) k_retained(DevBatch B, int trial) {
-    const int wdx = blockIdx.x;
+    const int wdx = B.bigFirst[blockIdx.x];
     const int mode = B.lm[wdx].mode;
     if (mode == kModeDone || (!trial && mode != kModeLinearize)) return;
     const WinDesc wd = B.win[wdx];
@@ -852,7 +852,7 @@ __device__ void undampedProduct(const double* A, const double* hd, int n, const 
 }
 
 __global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int refinement, double* Sdebug) {
-    const int wdx = blockIdx.x;
+    const int wdx = B.bigFirst[blockIdx.x];
     if (B.lm[wdx].mode == kModeDone) return;
     const WinDesc wd = B.win[wdx];
     const int n = wd.Nr, Npc = wd.Npc, K = wd.K;

@@ -439,7 +439,7 @@ __global__ void __launch_bounds__(kMargLmThreads) k_marg_visual(DevBatch B, Marg
 
 // IMU factors touching the victim and the previous prior, one CTA per window.
 __global__ void __launch_bounds__(256) k_marg_retained(DevBatch B, MargBatch M) {
-    const int w = blockIdx.x;
+    const int w = M.bigFirst[blockIdx.x];
     const MargWin mw = M.win[w];
     if (mw.m == 0) return;
     const WinDesc wd = B.win[w];
@@ -842,7 +842,7 @@ __device__ void ascendingPositions(const double* ev, int n, int* pos) {
 // Victim elimination: X = pinv(Hmm) [Hmr | bm] with the eigen cutoff, then the
 // symmetrized separator information Hrr - Hmr^T X and gradient br - Hmr^T y.
 __global__ void __launch_bounds__(kMargThreads) k_marg_victim(MargBatch M) {
-    const int w = blockIdx.x;
+    const int w = M.bigFirst[blockIdx.x];
     const MargWin mw = M.win[w];
     const int m = mw.m, nm = mw.nm, nr = mw.nr, cols = nr + 1;
     if (m == 0 || nr == 0 || M.status[w] != CGMLI_OK) return;
@@ -954,7 +954,7 @@ __device__ int sturmCount(const double* d, const double* e, int n, double x, dou
 }
 
 __global__ void __launch_bounds__(kMargThreads) k_marg_fast(MargBatch M) {
-    const int w = blockIdx.x;
+    const int w = M.bigFirst[blockIdx.x];
     const MargWin mw = M.win[w];
     const int n = mw.nr;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
@@ -1253,7 +1253,7 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_fast(MargBatch M) {
 // Eigendecomposition of the separator information and the square-root prior,
 // rows in ascending eigenvalue order.
 __global__ void __launch_bounds__(kEigenThreads) k_marg_eigen(MargBatch M) {
-    const int w = blockIdx.x;
+    const int w = M.bigFirst[blockIdx.x];
     const MargWin mw = M.win[w];
     const int nr = mw.nr;
     if (M.fast[w]) return;  // prior formed by k_marg_fast
@@ -1346,7 +1346,7 @@ constexpr int kCalibMaxCols = 64;
 __global__ void __launch_bounds__(kMargThreads) k_calib_conditional(DevBatch B, MargBatch M, double* work, const long long* work0,
                                                                   double* cond, double* evals, long long packedSmem) {
     extern __shared__ double calibSmem[];
-    const int w = blockIdx.x;
+    const int w = M.bigFirst[blockIdx.x];
     const MargWin mw = M.win[w];
     const int m = mw.m, nx = mw.nm, nc = mw.nr;
     if (m == 0 || M.status[w] != CGMLI_OK) return;
