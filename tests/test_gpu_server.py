@@ -103,6 +103,8 @@ def test_served_gated_equals_alone(backend):
         assert rep.status == 0
         g, m = srv.read_gate(t, w.window.num_observations)
         assert np.array_equal(m, ma) and g.rejected_total == int(ma.sum())
-        assert rel(w.state_vector() - x, xa - x) < 1e-8
+        # 8 iterations and refits: the run-to-run order of the FP64 atomic sums, which
+        # differs between any two solves of the same window, grows to about 1e-8 here
+        assert rel(w.state_vector() - x, xa - x) < 1e-7
         srv.release(t)
     srv.close()
