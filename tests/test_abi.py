@@ -45,6 +45,34 @@ def test_ctypes_layout_matches_c(tmp_path):
                    abi.Window.prior_r0.offset, abi.Window.obs_P.offset]
 
 
+def test_ctypes_layout_of_server_options_and_tuning(tmp_path):
+    src = tmp_path / "sizes2.c"
+    src.write_text(f'#include "{HEADER}"\n#include <stdio.h>\n#include <stddef.h>\n'
+                   "int main(){printf(\"%zu %zu %zu %zu\\n\", sizeof(cgmli_server_options), offsetof(cgmli_server_options, precision),"
+                   " sizeof(cgmli_tuning), offsetof(cgmli_tuning, ms)); return 0;}\n")
+    exe = tmp_path / "sizes2"
+    subprocess.run(["gcc", str(src), "-o", str(exe)], check=True)
+    got = list(map(int, subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()))
+    assert got == [C.sizeof(abi.ServerOptions), abi.ServerOptions.precision.offset, C.sizeof(abi.Tuning), abi.Tuning.ms.offset]
+
+
+def test_unknown_precision_is_rejected_before_any_device_work():
+    """Options are validated first: an unknown precision is CGMLI_E_INVALID for the
+    solver and the server alike, with or without a GPU."""
+    lib = abi.declare_backend(C.CDLL(str(build_backend())))
+    opt = abi.SolverOptions()
+    lib.cgmli_default_options(C.byref(opt))
+    opt.precision = 7
+    h = C.c_void_p()
+    assert lib.cgmli_solver_create(0, C.byref(opt), C.byref(h)) == abi.E_INVALID and not h.value
+    assert b"precision" in lib.cgmli_last_error()
+    so = abi.ServerOptions()
+    so.iterations, so.policy, so.max_refits, so.precision = 1, abi.MARGIN_OLD, 3, 7
+    srv = C.c_void_p()
+    assert lib.cgmli_server_create(C.byref(so), C.byref(srv)) == abi.E_INVALID and not srv.value
+    assert b"precision" in lib.cgmli_last_error()
+
+
 def test_create_without_gpu_reports_an_error():
     import torch
 
