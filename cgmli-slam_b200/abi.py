@@ -22,6 +22,9 @@ PRIOR_POSE, PRIOR_SPEED_BIAS, PRIOR_EXTRINSIC, PRIOR_TIME_OFFSET = 0, 1, 2, 3
 MARGIN_OLD, MARGIN_SECOND_NEW, MARGIN_SECOND_NEW_IMU_MERGE = 0, 1, 2
 IMU_MERGE_NONE, IMU_MERGE_REINTEGRATED, IMU_MERGE_BRIDGE, IMU_MERGE_SUPPRESSED = 0, 1, 2, 3
 MARG_EIGEN_NOALLOC_MAX_N = 256  # CGMLI_MARG_EIGEN_NOALLOC_MAX_N
+FIX_POSE, FIX_VELOCITY, FIX_BIAS = 1, 2, 4
+CHART_FULL, CHART_ROTATION_ONLY, CHART_FIXED = 0, 1, 2
+FACTOR_JACOBIAN = 52  # CGMLI_FACTOR_JACOBIAN: 2 x 26 per factor
 E_INVALID = 1
 E_NONFINITE = 2
 E_PENDING = 11
@@ -72,12 +75,13 @@ class Window(C.Structure):
         ("imu", C.POINTER(FrozenImu)), ("imu_kf", c_int_p),
         ("prior_block_kind", c_int_p), ("prior_block_index", c_int_p),
         ("prior_ref", c_double_p), ("prior_A", c_double_p), ("prior_r0", c_double_p),
+        ("kf_fixed", C.POINTER(C.c_ubyte)), ("ext_chart", C.POINTER(C.c_ubyte)), ("lm_fixed", C.POINTER(C.c_ubyte)),
     ]
 
 
 class SolverOptions(C.Structure):
     _fields_ = [("precision", C.c_int), ("refinement_steps", C.c_int), ("initial_lambda", C.c_double),
-                ("slabs_per_window", C.c_int), ("threads_per_block", C.c_int)]
+                ("min_iterations", C.c_int), ("time_budget_s", C.c_double)]
 
 
 class ServerOptions(C.Structure):
@@ -101,6 +105,11 @@ class SynthParams(C.Structure):
         ("extrinsic_jitter_m", C.c_double), ("extrinsic_jitter_rad", C.c_double),
         ("init_position_sigma", C.c_double), ("init_rotation_sigma", C.c_double),
     ]
+
+
+# cgmli_host_factor_fn(ctx, window, trial, poses, speed_bias, extrinsics, td, H, g, cost)
+HOST_FACTOR_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_int, c_double_p, c_double_p, c_double_p, c_double_p, c_double_p,
+                             c_double_p, c_double_p)
 
 
 def _proto(lib, name, restype, argtypes):
@@ -171,6 +180,11 @@ def declare_backend(lib: C.CDLL) -> C.CDLL:
     _proto(lib, "cgmli_solver_read_calibration_information", C.c_int,
            [S, C.c_int, c_int_p, c_int_p, c_int_p, c_int_p, c_double_p, c_double_p])
     _proto(lib, "cgmli_solver_read_gate", C.c_int, [S, C.c_int, C.POINTER(GateReport), C.POINTER(C.c_ubyte)])
+    _proto(lib, "cgmli_solver_device_bytes", C.c_int, [S, ll_p])
+    _proto(lib, "cgmli_server_device_bytes", C.c_int, [V, ll_p])
+    _proto(lib, "cgmli_solver_evaluate", C.c_int, [S, C.c_int])
+    _proto(lib, "cgmli_solver_read_factors", C.c_int, [S, C.c_int, c_double_p, c_int_p, c_double_p])
+    _proto(lib, "cgmli_solver_solve_host", C.c_int, [S, C.c_int, C.POINTER(C.c_ubyte), HOST_FACTOR_FN, C.c_void_p])
     return lib
 
 
@@ -197,6 +211,8 @@ BACKEND_SYMBOLS = [
     "cgmli_solver_solve_gated", "cgmli_solver_read_gate", "cgmli_solver_set_imu_merge_limits", "cgmli_solver_read_merged_imu",
     "cgmli_solver_calibration_information", "cgmli_solver_read_calibration_information", "cgmli_topology_check_tuned",
     "cgmli_solver_set_tuning", "cgmli_solver_get_tuning", "cgmli_solver_autotune",
+    "cgmli_solver_device_bytes", "cgmli_server_device_bytes", "cgmli_solver_evaluate", "cgmli_solver_read_factors",
+    "cgmli_solver_solve_host",
 ]
 KERNEL_NAMES = ["zero_acc", "linearize", "retained", "factor", "candidate", "backsub_trial", "retained_trial", "lm_update", "accept",
                 "lin_pairs", "lin_schur"]

@@ -42,13 +42,14 @@ class Solver:
     """Batched window solver on one GPU (one CUDA stream)."""
 
     def __init__(self, device: int = 0, precision: int = abi.PRECISION_FP64, refinement: int = 0,
-                 initial_lambda: float = 1e-4, slabs_per_window: int = 0):
+                 initial_lambda: float = 1e-4, min_iterations: int = 0, time_budget_s: float = 0.0):
         opt = abi.SolverOptions()
         lib().cgmli_default_options(C.byref(opt))
         opt.precision = precision
         opt.refinement_steps = refinement
         opt.initial_lambda = initial_lambda
-        opt.slabs_per_window = slabs_per_window
+        opt.min_iterations = min_iterations
+        opt.time_budget_s = time_budget_s
         h = C.c_void_p()
         _check(lib().cgmli_solver_create(device, C.byref(opt), C.byref(h)), "cgmli_solver_create")
         self._h = h
@@ -176,6 +177,63 @@ class Solver:
         self._windows = arr
         self.count = len(arr)
         return dict(run_landmarks=t.run_landmarks, pair_chunk=t.pair_chunk, schur_rows=t.schur_rows, ms=t.ms)
+
+    def device_bytes(self) -> int:
+        n = C.c_longlong()
+        _check(lib().cgmli_solver_device_bytes(self._h, C.byref(n)), "cgmli_solver_device_bytes")
+        return n.value
+
+    def evaluate(self, derivatives: bool = True) -> None:
+        """Per-factor residuals (and tangent Jacobians) of every window at its accepted states."""
+        _check(lib().cgmli_solver_evaluate(self._h, int(derivatives)), "cgmli_solver_evaluate")
+
+    def read_factors(self, w: int, jacobians: bool = True) -> dict:
+        """Window w's factors in its observation order: residuals (F, 2), valid (F,), Jacobians (F, 2, 26)."""
+        n = self._windows[w].num_observations
+        r = np.zeros(2 * max(n, 1))
+        v = np.zeros(max(n, 1), dtype=np.int32)
+        J = np.zeros(abi.FACTOR_JACOBIAN * max(n, 1)) if jacobians else None
+        _check(lib().cgmli_solver_read_factors(self._h, w, _p(r), v.ctypes.data_as(abi.c_int_p), _p(J) if J is not None else None),
+               "cgmli_solver_read_factors")
+        out = dict(residuals=r[:2 * n].reshape(n, 2), valid=v[:n].astype(bool))
+        if J is not None:
+            out["jacobians"] = J[:abi.FACTOR_JACOBIAN * n].reshape(n, 2, 26)
+        return out
+
+    def solve_host(self, iterations: int, fn, has_host=None) -> None:
+        """LM solve with caller-evaluated factors.  fn(window, trial, poses (K,7), speed_bias (K,9),
+        extrinsics (E,7), td) returns (H (Nr, Nr), g (Nr,), cost) at a linearization (trial False)
+        and the cost alone at a trial (trial True); None fails the call."""
+        dims = [self.dims(w)[0] for w in range(self.count)]
+        wins = self._windows
+
+        def cb(ctx, w, trial, poses, sb, ext, td, H, g, cost):
+            try:
+                K, E = wins[w].num_keyframes, wins[w].num_extrinsics
+                P = np.ctypeslib.as_array(poses, shape=(K, 7)).copy()
+                S = np.ctypeslib.as_array(sb, shape=(K, 9)).copy()
+                X = np.ctypeslib.as_array(ext, shape=(E, 7)).copy()
+                out = fn(w, bool(trial), P, S, X, float(td[0]))
+                if out is None:
+                    return 1
+                if trial:
+                    cost[0] = float(out)
+                    return 0
+                Hm, gv, c = out
+                n = dims[w]
+                np.ctypeslib.as_array(H, shape=(n * n,))[:] = np.asarray(Hm, dtype=np.float64).reshape(-1)
+                np.ctypeslib.as_array(g, shape=(n,))[:] = np.asarray(gv, dtype=np.float64)
+                cost[0] = float(c)
+                return 0
+            except Exception:  # noqa: BLE001 - reported to the library as a failed evaluation
+                return 1
+
+        cfn = abi.HOST_FACTOR_FN(cb)
+        mask = None
+        if has_host is not None:
+            m = np.ascontiguousarray(has_host, dtype=np.uint8)
+            mask = m.ctypes.data_as(C.POINTER(C.c_ubyte))
+        _check(lib().cgmli_solver_solve_host(self._h, iterations, mask, cfn, None), "cgmli_solver_solve_host")
 
     def step(self, lam: float) -> None:
         _check(lib().cgmli_solver_step(self._h, lam), "cgmli_solver_step")
@@ -366,6 +424,12 @@ class Server:
                                              idx.ctypes.data_as(ip), _p(ref), _p(A), _p(r0))
         amb = int(sum(9 if t == abi.PRIOR_SPEED_BIAS else 1 if t == abi.PRIOR_TIME_OFFSET else 7 for t in kinds))
         return dict(status=code, rank=k, cols=m, kinds=kinds, index=idx, reference=ref[:amb], A=A.reshape(k, m), r0=r0)
+
+    def device_bytes(self) -> int:
+        """Device bytes both solvers of the server hold."""
+        n = C.c_longlong()
+        _check(lib().cgmli_server_device_bytes(self._h, C.byref(n)), "cgmli_server_device_bytes")
+        return n.value
 
     def release(self, ticket: int) -> None:
         _check(lib().cgmli_server_release(self._h, ticket), "cgmli_server_release")

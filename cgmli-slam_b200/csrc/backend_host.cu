@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -29,6 +30,11 @@ size_t factorSmemBytes(int maxNr);
 cudaError_t configureKernels(size_t linSmem, size_t facSmem);
 int launchIteration(const DevBatch& B, const LaunchPlan& P, int refinement, int maxIterations, int probe, double* Sdebug,
                     cudaStream_t s, LaunchHook hook, void* ctx);
+int launchIterationParts(const DevBatch& B, const LaunchPlan& P, int refinement, int maxIterations, int probe, double* Sdebug,
+                         cudaStream_t s, LaunchHook hook, void* ctx, int parts);
+void launchEvaluate(const DevBatch& B, int derivatives, double* out, int* valid, cudaStream_t s);
+void launchAddHost(const DevBatch& B, const double* hostH, const double* hostG, const double* hostCost, const unsigned char* flag,
+                   int trial, cudaStream_t s);
 int launchLmInit(const DevBatch& B, double lambda0, cudaStream_t s);
 int launchGate(const DevBatch& B, const LaunchPlan& P, int pass, int pre, double threshold, double* obP, unsigned char* rejected,
                double* gateStats, int* gateCounts, cudaStream_t s);
@@ -142,6 +148,14 @@ struct cgmli_solver {
     DArray<double> priorA, priorR0, priorRef;
     DArray<double> Hret, gret, costRet, trialRet, acc, dr, rhs, Sglob, imuScratch, priorScratch, predState, out, Sdebug;
     DArray<int> retValid, solveStatus;
+    DArray<signed char> colChart;  // solve-time chart of every retained column
+    DArray<unsigned char> lmFixed;
+    // per-factor evaluation (cgmli_solver_evaluate) and caller-evaluated factors (cgmli_solver_solve_host)
+    DArray<double> evalOut;
+    DArray<int> evalValid;
+    bool haveEval = false, evalDerivatives = false;
+    DArray<double> hostH, hostG, hostCost;
+    DArray<unsigned char> hostFlag;
     DevBatch B{};
     double lastMs = 0;
     int lastLaunches = 0;
@@ -228,6 +242,25 @@ struct cgmli_solver {
         }
         return evPool[evNext++];
     }
+    // device bytes held by the solver's arrays (grow-only: they stay until destruction)
+    long long deviceBytes() const {
+        long long t = 0;
+        auto add = [&](const auto&... a) { ((t += (long long)(a.cap * sizeof(*a.p))), ...); };
+        add(dWin, dLm, dRuns, dTiles, dPairChunks, dSchurChunks, schurCols, lmUmap, obLm, keyOrder, bigFirst, keyRows, sch, camR, camT,
+            camExt, lmWin, lmKf, lmCam, lmObsBegin, lmNs, lmNx, lmSupp0, supp, lmC0, lmBearing, lmVel, lmTime, lmC, lmD, lmG, lmCost,
+            lmDelta, lmPred, lmTrial, lmMaxInc, lmValid, lmTrialValid, obKf, obCam, obSlot, obXslot, obBearing, obP, obVel, obTime);
+        for (int k = 0; k < 2; ++k) add(pose[k], sb[k], ext[k], td[k], rho[k], rotKf[k], rotExt[k]);
+        add(imu, imuKf, priorKind, priorIndex, priorCol, priorOff, priorA, priorR0, priorRef, Hret, gret, costRet, trialRet, acc, dr,
+            rhs, Sglob, imuScratch, priorScratch, predState, out, Sdebug, retValid, solveStatus);
+        add(dMargWin, dMargElim, margCols, margObsMap, margPoseCol, margSbCol, margExtCol, margRank, margStatus, margFast, margVisCol,
+            margVisPose, margVisExt, margSlow, margChunks, margItems, margH, margB, margSepH, margSepV, margSepB, margEvals, margA,
+            margR0, margX, margMaxD, margStats, dMargOrder);
+        add(colChart, lmFixed, evalOut, evalValid, hostH, hostG, hostCost, hostFlag);
+        add(obRejected, gateCounts, gateStats, imuTimes, imuT0, imuT1, imuReadings, imuRanges, imuStatus, imuRefreshed,
+            imuRefreshScratch, mergeRange, mergeKf, mergeStatus, mergeFlag, mergeT0, mergeT1, mergeOut, calibWork0, calibWork, calibCond,
+            calibEvals, snapPose, snapSb, snapExt, snapTd, snapRho);
+        return t;
+    }
     LaunchPlan plan() const {
         LaunchPlan P{};
         P.runs = dRuns.p; P.tiles = dTiles.p; P.numTiles = (int)hb.tiles.size();
@@ -270,6 +303,8 @@ struct cgmli_solver {
         mergeRange.release(); mergeKf.release(); mergeStatus.release(); mergeFlag.release(); mergeT0.release(); mergeT1.release();
         mergeOut.release();
         calibWork0.release(); calibWork.release(); calibCond.release(); calibEvals.release();
+        colChart.release(); lmFixed.release(); evalOut.release(); evalValid.release();
+        hostH.release(); hostG.release(); hostCost.release(); hostFlag.release();
         dMargWin.release(); dMargElim.release(); dMargOrder.release();
         DArray<int>* mi[] = {&margCols, &margObsMap, &margPoseCol, &margSbCol, &margExtCol, &margRank, &margStatus, &margFast,
                              &margVisCol, &margVisPose, &margVisExt, &margSlow};
@@ -331,8 +366,8 @@ void cgmli_default_options(cgmli_solver_options* o) {
     o->precision = CGMLI_PRECISION_FP64;
     o->refinement_steps = 0;
     o->initial_lambda = 1e-4;
-    o->slabs_per_window = 0;
-    o->threads_per_block = 0;
+    o->min_iterations = 0;
+    o->time_budget_s = 0.0;
 }
 
 int cgmli_solver_create(int device, const cgmli_solver_options* options, cgmli_solver** out) {
@@ -343,8 +378,8 @@ int cgmli_solver_create(int device, const cgmli_solver_options* options, cgmli_s
             return fail(CGMLI_E_INVALID, "unknown precision");
         if (options->refinement_steps < 0 || options->refinement_steps > 2) return fail(CGMLI_E_INVALID, "refinement_steps outside 0..2");
         if (!(options->initial_lambda > 0)) return fail(CGMLI_E_INVALID, "initial_lambda must be positive");
-        if (options->slabs_per_window != 0 || options->threads_per_block != 0)
-            return fail(CGMLI_E_UNSUPPORTED, "slabs_per_window / threads_per_block are reserved and must be 0");
+        if (options->min_iterations < 0) return fail(CGMLI_E_INVALID, "min_iterations < 0");
+        if (!std::isfinite(options->time_budget_s)) return fail(CGMLI_E_INVALID, "time_budget_s not finite");
     }
     int count = 0;
     cudaError_t e = cudaGetDeviceCount(&count);
@@ -374,6 +409,7 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     S->haveSnapshot = false;
     S->haveMarg = false;
     S->haveImuSamples = false;
+    S->haveEval = false;
     S->win.clear();
     HostBatch& hb = S->hb;
     std::string why;
@@ -447,6 +483,7 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     for (int k = 0; k < 2; ++k) { CK(S->rotKf[k].reserve(9ull * hb.totalKf)); CK(S->rotExt[k].reserve(9ull * hb.totalExt)); }
     CK(S->td[1].reserve(hb.td.size())); CK(S->rho[1].reserve(hb.rho.size()));
     CK(S->imu.upload(hb.imu, st)); CK(S->imuKf.upload(hb.imuKf, st));
+    CK(S->colChart.upload(hb.colChart, st)); CK(S->lmFixed.upload(hb.lmFixed, st));
     CK(S->priorKind.upload(hb.priorKind, st)); CK(S->priorIndex.upload(hb.priorIndex, st));
     CK(S->priorCol.upload(hb.priorCol, st)); CK(S->priorOff.upload(hb.priorOff, st));
     CK(S->priorA.upload(hb.priorA, st)); CK(S->priorR0.upload(hb.priorR0, st)); CK(S->priorRef.upload(hb.priorRef, st));
@@ -483,6 +520,9 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
         B.rotKf[k] = S->rotKf[k].p; B.rotExt[k] = S->rotExt[k].p;
     }
     B.imu = S->imu.p; B.imuKf = S->imuKf.p;
+    B.colChart = S->colChart.p; B.lmFixed = S->lmFixed.p;
+    B.minIterations = S->opt.min_iterations;
+    B.budgetNs = S->opt.time_budget_s > 0 ? std::max(1ll, (long long)std::llround(S->opt.time_budget_s * 1e9)) : 0;
     B.priorKind = S->priorKind.p; B.priorIndex = S->priorIndex.p; B.priorCol = S->priorCol.p; B.priorOff = S->priorOff.p;
     B.priorA = S->priorA.p; B.priorR0 = S->priorR0.p; B.priorRef = S->priorRef.p;
     B.Hret = S->Hret.p; B.gret = S->gret.p; B.costRet = S->costRet.p; B.trialRet = S->trialRet.p; B.retValid = S->retValid.p;
@@ -975,6 +1015,137 @@ int cgmli_solver_read_reports(cgmli_solver* S, cgmli_solve_report* reports, int 
         r.predicted_reduction = lm[i].predicted; r.max_increment = lm[i].maxInc;
         r.iterations = lm[i].iterations; r.accepted_steps = lm[i].accepted; r.converged = lm[i].converged; r.status = lm[i].status;
     }
+    return CGMLI_OK;
+}
+
+int cgmli_solver_device_bytes(cgmli_solver* S, long long* bytes) {
+    if (!S || !bytes) return fail(CGMLI_E_INVALID, "null solver or output");
+    *bytes = S->deviceBytes();
+    return CGMLI_OK;
+}
+
+int cgmli_solver_evaluate(cgmli_solver* S, int derivatives) {
+    if (!S || S->win.empty()) return fail(CGMLI_E_INVALID, "solver has no windows");
+    CK(cudaSetDevice(S->device));
+    const size_t F = std::max(1, S->totalObs);
+    CK(S->evalOut.reserve(F * (2 + CGMLI_FACTOR_JACOBIAN)));
+    CK(S->evalValid.reserve(F));
+    launchEvaluate(S->B, derivatives ? 1 : 0, S->evalOut.p, S->evalValid.p, S->stream);
+    CK(cudaGetLastError());
+    S->haveEval = true;
+    S->evalDerivatives = derivatives != 0;
+    return CGMLI_OK;
+}
+
+int cgmli_solver_read_factors(cgmli_solver* S, int w, double* residuals, int* valid, double* jacobians) {
+    if (!S || w < 0 || w >= (int)S->win.size()) return fail(CGMLI_E_INVALID, "window index out of range");
+    if (!S->haveEval) return fail(CGMLI_E_INVALID, "read_factors before cgmli_solver_evaluate");
+    if (jacobians && !S->evalDerivatives) return fail(CGMLI_E_INVALID, "read_factors: Jacobians requested but evaluated without derivatives");
+    const WinDesc& d = S->win[w];
+    if (d.F == 0) return CGMLI_OK;
+    constexpr int rec = 2 + CGMLI_FACTOR_JACOBIAN;
+    std::vector<double> out((size_t)rec * d.F);
+    std::vector<int> ok(d.F);
+    CK(cudaSetDevice(S->device));
+    CK(cudaMemcpyAsync(out.data(), S->evalOut.p + (size_t)rec * d.obs0, out.size() * sizeof(double), cudaMemcpyDeviceToHost, S->stream));
+    CK(cudaMemcpyAsync(ok.data(), S->evalValid.p + d.obs0, d.F * sizeof(int), cudaMemcpyDeviceToHost, S->stream));
+    CK(cudaStreamSynchronize(S->stream));
+    for (int q = 0; q < d.F; ++q) {
+        const int f = S->hb.obOrig[d.obs0 + q];  // caller's observation index
+        const double* src = out.data() + (size_t)rec * q;
+        if (residuals) { residuals[2 * f] = src[0]; residuals[2 * f + 1] = src[1]; }
+        if (valid) valid[f] = ok[q];
+        if (jacobians) std::memcpy(jacobians + (size_t)CGMLI_FACTOR_JACOBIAN * f, src + 2, CGMLI_FACTOR_JACOBIAN * sizeof(double));
+    }
+    return CGMLI_OK;
+}
+
+int cgmli_solver_solve_host(cgmli_solver* S, int max_iterations, const unsigned char* has_host, cgmli_host_factor_fn fn, void* ctx) {
+    if (!S || S->win.empty()) return fail(CGMLI_E_INVALID, "solver has no windows");
+    if (max_iterations < 1) return fail(CGMLI_E_INVALID, "max_iterations < 1");
+    if (!fn) return fail(CGMLI_E_INVALID, "solve_host: null factor callback");
+    CK(cudaSetDevice(S->device));
+    cudaStream_t st = S->stream;
+    const int W = (int)S->win.size();
+    HostBatch& hb = S->hb;
+    CK(S->hostH.reserve(std::max<long long>(1, hb.dense)));
+    CK(S->hostG.reserve(std::max<long long>(1, hb.vec)));
+    CK(S->hostCost.reserve(W));
+    CK(S->hostFlag.reserve(W));
+    std::vector<unsigned char> flag(W);
+    for (int w = 0; w < W; ++w) flag[w] = has_host ? (has_host[w] ? 1 : 0) : 1;
+    CK(cudaMemcpyAsync(S->hostFlag.p, flag.data(), W, cudaMemcpyHostToDevice, st));
+    // host staging of the callbacks' states and results
+    std::vector<WinLM> lm(W);
+    std::vector<double> Hh((size_t)std::max<long long>(1, hb.dense)), gh((size_t)std::max<long long>(1, hb.vec)), cost(W);
+    std::vector<double> pose(hb.pose.size()), sbv(hb.sb.size()), extv(hb.ext.size()), tdv(W);
+    auto download = [&](int buf) -> int {
+        CK(cudaMemcpyAsync(lm.data(), S->dLm.p, W * sizeof(WinLM), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(pose.data(), S->pose[buf].p, pose.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(sbv.data(), S->sb[buf].p, sbv.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(extv.data(), S->ext[buf].p, extv.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(tdv.data(), S->td[buf].p, W * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return CGMLI_OK;
+    };
+    const double nan = std::numeric_limits<double>::quiet_NaN();
+    CK(cudaEventRecord(S->ev0, st));
+    int launches = launchLmInit(S->B, S->opt.initial_lambda, st);
+    for (int it = 0; it < max_iterations; ++it) {
+        launches += launchIterationParts(S->B, S->plan(), S->opt.refinement_steps, max_iterations, 0, nullptr, st, nullptr, nullptr,
+                                         kIterLinearize);
+        int r = download(0);
+        if (r != CGMLI_OK) return r;
+        bool live = false;
+        for (int w = 0; w < W; ++w) live = live || lm[w].mode != kModeDone;
+        if (!live) break;  // every window has finished
+        bool any = false;
+        for (int w = 0; w < W; ++w) {
+            cost[w] = 0.0;
+            if (!flag[w] || lm[w].mode != kModeLinearize) continue;
+            any = true;
+            const WinDesc& d = S->win[w];
+            double* H = Hh.data() + d.dense0;
+            double* g = gh.data() + d.vec0;
+            std::fill(H, H + (size_t)d.Nr * d.Nr, 0.0);
+            std::fill(g, g + d.Nr, 0.0);
+            double c = 0;
+            const int rc = fn(ctx, w, 0, pose.data() + 7ll * d.kf0, sbv.data() + 9ll * d.kf0, extv.data() + 7ll * d.ext0, &tdv[w], H, g, &c);
+            cost[w] = rc == 0 && std::isfinite(c) ? c : nan;  // a failed evaluation fails the window (non-finite cost)
+            CK(cudaMemcpyAsync(S->hostH.p + d.dense0, H, (size_t)d.Nr * d.Nr * sizeof(double), cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(S->hostG.p + d.vec0, g, d.Nr * sizeof(double), cudaMemcpyHostToDevice, st));
+        }
+        if (any) {
+            CK(cudaMemcpyAsync(S->hostCost.p, cost.data(), W * sizeof(double), cudaMemcpyHostToDevice, st));
+            launchAddHost(S->B, S->hostH.p, S->hostG.p, S->hostCost.p, S->hostFlag.p, 0, st);
+            ++launches;
+        }
+        launches += launchIterationParts(S->B, S->plan(), S->opt.refinement_steps, max_iterations, 0, nullptr, st, nullptr, nullptr,
+                                         kIterStep);
+        if ((r = download(1)) != CGMLI_OK) return r;
+        any = false;
+        for (int w = 0; w < W; ++w) {
+            cost[w] = 0.0;
+            if (!flag[w] || lm[w].mode == kModeDone) continue;
+            any = true;
+            const WinDesc& d = S->win[w];
+            double c = 0;
+            const int rc = fn(ctx, w, 1, pose.data() + 7ll * d.kf0, sbv.data() + 9ll * d.kf0, extv.data() + 7ll * d.ext0, &tdv[w], nullptr,
+                              nullptr, &c);
+            cost[w] = rc == 0 && std::isfinite(c) ? c : nan;  // a failed trial evaluation rejects the step
+        }
+        if (any) {
+            CK(cudaMemcpyAsync(S->hostCost.p, cost.data(), W * sizeof(double), cudaMemcpyHostToDevice, st));
+            launchAddHost(S->B, S->hostH.p, S->hostG.p, S->hostCost.p, S->hostFlag.p, 1, st);
+            ++launches;
+        }
+        launches += launchIterationParts(S->B, S->plan(), S->opt.refinement_steps, max_iterations, 0, nullptr, st, nullptr, nullptr,
+                                         kIterDecide);
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(S->ev1, st));
+    S->lastLaunches = launches;
+    S->lastKey.clear();  // the next plain solve of this batch is not a repeat of a captured one
     return CGMLI_OK;
 }
 

@@ -36,7 +36,14 @@ struct WinDesc {
     long long imuScratch0;  // nImu * 930 doubles (raw and whitened factor)
     long long priorScratch0;  // priorRank*priorCols + priorCols*6 doubles
     double huber, minInv;
+    int charts;   // 1: some retained column is fixed or on the rotation-only chart (colChart)
+    int fixedLm;  // 1: some landmark's inverse distance is held constant (lmFixed)
 };
+// Solve-time chart of a retained column (DevBatch::colChart).  A rotation-only
+// extrinsic keeps its translation: its tangent theta maps to the full left
+// SE(3) tangent as [rho; theta] = [[p]x; I] theta, so its rho columns are
+// folded into its theta columns and then held like fixed columns.
+enum { kColFree = 0, kColFixed = 1, kColRotTheta = 2, kColRotRho = 3 };
 
 struct WinLM {
     double lambda, nu, cost, initialCost, linCost, trialCost, predicted, maxInc;
@@ -46,6 +53,7 @@ struct WinLM {
     // steps at the start of the window's current pass, iterations charged to the
     // finished passes (at least one each), index of the window's current pass
     int passStart, passAccepted, charged, pass, pad;
+    unsigned long long t0;  // device clock (ns) at the start of the solve, for the time budget
 };
 enum { kModeLinearize = 0, kModeResolve = 1, kModeDone = 2 };
 
@@ -54,6 +62,8 @@ enum { kModeLinearize = 0, kModeResolve = 1, kModeDone = 2 };
 struct DevBatch {
     int numWindows, numLandmarks, numObs, numKf, numExt, numCam, numImu, numRuns;
     int mixed;  // CGMLI_PRECISION_MIXED: FP32 Jacobians, weights and landmark sums in the linearization
+    int minIterations;   // iterations before the time budget may end a window's solve
+    long long budgetNs;  // time budget of a solve (0: none)
     const WinDesc* win;
     WinLM* lm;
     const int* bigFirst;  // windows by decreasing retained dimension: block order of the one-CTA-per-window
@@ -81,6 +91,8 @@ struct DevBatch {
     // IMU and priors
     const double* imu;  // numImu * sizeof(cgmli_frozen_imu)/8
     const int* imuKf;   // global keyframe index of the first state
+    const signed char* colChart;     // per retained column (WinDesc::vec0 offsets): kCol*
+    const unsigned char* lmFixed;    // per landmark: 1 = inverse distance held constant
     const int* priorKind; const int* priorIndex; const int* priorCol; const int* priorOff;  // per prior block
     const double* priorA; const double* priorR0; const double* priorRef;
     // per-window dense storage
@@ -166,6 +178,9 @@ struct MargBatch {
     const int* slowElim; // eliminated landmarks of windows above kRowsMaxN (one CTA each)
     int numSlowElim;
 };
+
+// Parts of one LM iteration's launch sequence (launchIterationParts).
+enum { kIterLinearize = 1, kIterStep = 2, kIterDecide = 4 };
 
 // Called before (phase 0) and after (phase 1) every kernel launch of an
 // iteration; used for per-kernel event timing.

@@ -18,6 +18,11 @@
 
 namespace cgmli {
 
+__device__ __forceinline__ unsigned long long globalTimerNs() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 __device__ __forceinline__ double warpSum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -521,7 +526,8 @@ __global__ void __launch_bounds__(kSchurThreads, 3) k_lin_schur(DevBatch B, cons
         const int l = ch.y + r;
         const int ns = 6 * (B.lmNs[l] + B.lmNx[l]) + (wd.estTd ? 1 : 0);
         const double d = B.lmD[l];
-        const double scale = 1.0 / sqrt(d + lambda * fmax(d, 1e-6));
+        // a landmark held constant is not eliminated: its row stays zero
+        const double scale = wd.fixedLm && B.lmFixed[l] ? 0.0 : 1.0 / sqrt(d + lambda * fmax(d, 1e-6));
         const long long c0 = B.lmC0[l];
         double* row = Rw + (long long)r * np;
         for (int c = lane; c < np; c += 32) row[c] = 0.0;
@@ -851,6 +857,80 @@ __device__ void undampedProduct(const double* A, const double* hd, int n, const 
     __syncthreads();
 }
 
+// Solve-time charts of one window's reduced system (kCol* per retained column),
+// the reference's constant blocks, bias-frozen speed/bias and rotation-only rig
+// extrinsic of a single solve (BackendOptimizer.cpp:44-66,83-91,783-795).  On
+// entry A holds the assembled system (lower triangle damped, strict upper
+// undamped), hd its undamped diagonal and x the right-hand side; dmp[i] is the
+// damping of column i.  A rotation-only extrinsic's tangent theta moves the full
+// left SE(3) tangent along [rho; theta] = [[p]x; I] theta, so the system is
+// restricted to those directions: its rho columns are folded into its theta
+// columns (columns, then rows, then the right-hand side), and the damping of a
+// theta column is lambda max(m^T H m, 1e-6) with m that direction and H the
+// undamped total information (retained + J^T J) of the block, as the damping of
+// a restricted tangent column is in the reference.  Fixed and folded columns
+// then become identity rows and columns with a zero right-hand side, so their
+// increments are exactly zero.  On exit A is the restricted damped system in the
+// same storage, hd its undamped diagonal (0 at fixed columns).
+__device__ void chartSystem(const DevBatch& B, const WinDesc& wd, double lambda, int n, double* A, double* x, double* hd,
+                            double* dmp) {
+    const signed char* cc = B.colChart + wd.vec0;
+    const int tid = threadIdx.x, K = wd.K, Npc = wd.Npc;
+    const double* acc = B.acc + wd.acc0;
+    for (int i = tid; i < n; i += blockDim.x) A[i + (long long)i * n] = hd[i];
+    __syncthreads();
+    for (int e = 0; wd.estExt && e < wd.E; ++e) {
+        const int c0 = 15 * K + 6 * e;
+        if (cc[c0] != kColRotRho) continue;  // uniform over the CTA
+        const double* pt = B.ext[0] + 7ll * (wd.ext0 + e);
+        const double P[9] = {0, -pt[2], pt[1], pt[2], 0, -pt[0], -pt[1], pt[0], 0};  // [p]x, row-major
+        if (tid < 3) {
+            const int k = tid;
+            double m[6];
+            for (int a = 0; a < 3; ++a) { m[a] = P[3 * a + k]; m[3 + a] = a == k ? 1.0 : 0.0; }
+            double v = 0;
+            for (int a = 0; a < 6; ++a)
+                for (int b = 0; b < 6; ++b) {
+                    const int pa = 6 * K + 6 * e + a, pb = 6 * K + 6 * e + b;
+                    const double h = B.Hret[wd.dense0 + (long long)(c0 + a) * n + c0 + b] + acc[pa <= pb ? upIdx(pa, pb, Npc) : upIdx(pb, pa, Npc)];
+                    v += m[a] * m[b] * h;
+                }
+            dmp[c0 + 3 + k] = lambda * fmax(v, 1e-6);
+        }
+        for (int r = tid; r < n; r += blockDim.x) {
+            const double a0 = A[r + (long long)c0 * n], a1 = A[r + (long long)(c0 + 1) * n], a2 = A[r + (long long)(c0 + 2) * n];
+            for (int k = 0; k < 3; ++k) A[r + (long long)(c0 + 3 + k) * n] += a0 * P[k] + a1 * P[3 + k] + a2 * P[6 + k];
+        }
+        __syncthreads();
+        for (int j = tid; j < n; j += blockDim.x) {
+            const double a0 = A[c0 + (long long)j * n], a1 = A[c0 + 1 + (long long)j * n], a2 = A[c0 + 2 + (long long)j * n];
+            for (int k = 0; k < 3; ++k) A[c0 + 3 + k + (long long)j * n] += a0 * P[k] + a1 * P[3 + k] + a2 * P[6 + k];
+        }
+        if (tid == 0)
+            for (int k = 0; k < 3; ++k) x[c0 + 3 + k] += x[c0] * P[k] + x[c0 + 1] * P[3 + k] + x[c0 + 2] * P[6 + k];
+        __syncthreads();
+    }
+    for (long long t = tid; t < (long long)n * n; t += blockDim.x) {
+        const int r = (int)(t % n), c = (int)(t / n);
+        const bool fr = cc[r] == kColFixed || cc[r] == kColRotRho, fc = cc[c] == kColFixed || cc[c] == kColRotRho;
+        if (fr || fc) A[t] = r == c ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += blockDim.x) {
+        if (cc[i] == kColFixed || cc[i] == kColRotRho) {
+            x[i] = 0.0; dmp[i] = 0.0; hd[i] = 0.0;
+        } else {
+            hd[i] = A[i + (long long)i * n];
+            A[i + (long long)i * n] += dmp[i];
+        }
+    }
+    __syncthreads();
+}
+__device__ __forceinline__ bool chartFixed(const DevBatch& B, const WinDesc& wd, int i) {
+    const signed char c = B.colChart[wd.vec0 + i];
+    return c == kColFixed || c == kColRotRho;
+}
+
 __global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int refinement, double* Sdebug) {
     const int wdx = B.bigFirst[blockIdx.x];
     if (B.lm[wdx].mode == kModeDone) return;
@@ -864,6 +944,8 @@ __global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int re
     double* hd = x + n;                      // n: undamped diagonal
     double* da = hd + n;                     // n: damping added to the diagonal; then the product h
     double* blk = da + n;                    // kFacPanel x kFacPanel diagonal block (solves)
+    double* dmp = blk + kFacPanel * kFacPanel;  // n: damping of each column (solve-time charts only)
+    const bool charts = wd.charts != 0;
     __shared__ int failed;
     __shared__ double red[32];
     double* A = B.Sglob + wd.dense0;
@@ -904,8 +986,14 @@ __global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int re
         if (p >= 0) g += acc[nS + Npc + p] - acc[nS + 2ll * Npc + p];
         x[i] = -g;
         rhsOut[i] = -g;
+        if (charts) dmp[i] = da[i];
     }
     __syncthreads();
+    if (charts) {
+        chartSystem(B, wd, lambda, n, A, x, hd, dmp);
+        for (int i = tid; i < n; i += blockDim.x) rhsOut[i] = x[i];  // the restricted right-hand side
+        __syncthreads();
+    }
     // ---- factorization with the forward substitution
     for (int k0 = 0; k0 < n; k0 += kFacPanel) {
         // rows padded so that the trailing rows [bw, mp) are whole 32-row tiles
@@ -1013,6 +1101,15 @@ __global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int re
     double* h = da;  // the damping is folded back below where needed
     // ---- iterative refinement against the assembled FP64 system
     for (int it = 0; it < refinement; ++it) {
+        if (charts) {
+            undampedProduct(A, hd, n, dr, h);
+            for (int i = tid; i < n; i += blockDim.x) x[i] = chartFixed(B, wd, i) ? 0.0 : rhsOut[i] - (h[i] + dmp[i] * dr[i]);
+            __syncthreads();
+            blockedSolve(A, n, x, blk);
+            for (int i = tid; i < n; i += blockDim.x) dr[i] += x[i];
+            __syncthreads();
+            continue;
+        }
         for (int i = tid; i < n; i += blockDim.x) {
             const int pi = pcOfRetained(i, K);
             double hh = B.Hret[wd.dense0 + (long long)i * n + i];
@@ -1035,14 +1132,37 @@ __global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int re
     // predicted reduction of the state part with the undamped (S_visual + H_ret):
     //   -dx^T (g_r + 0.5 (S_v + H_ret) dx); the landmark terms are added per landmark.
     undampedProduct(A, hd, n, dr, h);
-    double pred = 0;
-    for (int i = tid; i < n; i += blockDim.x) {
+    auto gradient = [&](int i) {  // g_r + G_v of column i (the full gradient, without the Schur term)
         double g = B.gret[wd.vec0 + i];
         const int p = pcOfRetained(i, K);
         if (p >= 0) g += acc[nS + Npc + p];
+        return g;
+    };
+    double pred = 0;
+    for (int i = tid; i < n; i += blockDim.x) {
+        double g = gradient(i);
+        if (charts) {
+            if (chartFixed(B, wd, i)) continue;
+            if (B.colChart[wd.vec0 + i] == kColRotTheta) {  // restricted gradient m^T g of a rotation-only column
+                const int e = (i - 15 * K) / 6, c0 = 15 * K + 6 * e, k = i - c0 - 3;
+                const double* pt = B.ext[0] + 7ll * (wd.ext0 + e);
+                const double P[9] = {0, -pt[2], pt[1], pt[2], 0, -pt[0], -pt[1], pt[0], 0};
+                g += gradient(c0) * P[k] + gradient(c0 + 1) * P[3 + k] + gradient(c0 + 2) * P[6 + k];
+            }
+        }
         pred += -dr[i] * (g + 0.5 * h[i]);
     }
     pred = blockSum(pred, red);
+    if (charts && wd.estExt) {
+        // full tangent of the rotation-only extrinsics for the back-substitution: rho = [p]x theta
+        for (int e = tid; e < wd.E; e += blockDim.x) {
+            const int c0 = 15 * K + 6 * e;
+            if (B.colChart[wd.vec0 + c0] != kColRotRho) continue;
+            const double* pt = B.ext[0] + 7ll * (wd.ext0 + e);
+            const double P[9] = {0, -pt[2], pt[1], pt[2], 0, -pt[0], -pt[1], pt[0], 0};
+            for (int a = 0; a < 3; ++a) dr[c0 + a] = P[3 * a] * dr[c0 + 3] + P[3 * a + 1] * dr[c0 + 4] + P[3 * a + 2] * dr[c0 + 5];
+        }
+    }
     if (tid == 0) { B.predState[wdx] = pred; B.solveStatus[wdx] = CGMLI_OK; }
 }
 
@@ -1059,15 +1179,24 @@ __global__ void k_candidate(DevBatch B) {
     for (int i = threadIdx.x; i < wd.Nr; i += blockDim.x) {
         if (!isfinite(dr[i])) bad = 1; else mx = fmax(mx, fabs(dr[i]));
     }
+    // solve-time charts: a fixed block is copied; a rotation-only extrinsic keeps its
+    // translation (Plus(T, theta) = (Exp(theta) R, p), GpuRetainedFactorMath.hpp:28-37)
+    const signed char* cc = wd.charts ? B.colChart + wd.vec0 : nullptr;
     for (int k = threadIdx.x; k < wd.K; k += blockDim.x) {
         const int gk = wd.kf0 + k;
-        posePlus(B.pose[0] + 7ll * gk, dr + 15 * k, B.pose[1] + 7ll * gk);
+        if (cc && cc[15 * k] == kColFixed)
+            for (int j = 0; j < 7; ++j) B.pose[1][7ll * gk + j] = B.pose[0][7ll * gk + j];
+        else
+            posePlus(B.pose[0] + 7ll * gk, dr + 15 * k, B.pose[1] + 7ll * gk);
         poseRotation(B.pose[1] + 7ll * gk, B.rotKf[1] + 9ll * gk);
-        for (int j = 0; j < 9; ++j) B.sb[1][9ll * gk + j] = B.sb[0][9ll * gk + j] + dr[15 * k + 6 + j];
+        for (int j = 0; j < 9; ++j)
+            B.sb[1][9ll * gk + j] = cc && cc[15 * k + 6 + j] == kColFixed ? B.sb[0][9ll * gk + j] : B.sb[0][9ll * gk + j] + dr[15 * k + 6 + j];
     }
     for (int e = threadIdx.x; e < wd.E; e += blockDim.x) {
         const int ge = wd.ext0 + e;
-        if (wd.estExt) posePlus(B.ext[0] + 7ll * ge, dr + 15 * wd.K + 6 * e, B.ext[1] + 7ll * ge);
+        const int chart = wd.estExt && cc ? cc[15 * wd.K + 6 * e] : kColFree;
+        if (wd.estExt && chart == kColFree) posePlus(B.ext[0] + 7ll * ge, dr + 15 * wd.K + 6 * e, B.ext[1] + 7ll * ge);
+        else if (wd.estExt && chart == kColRotRho) posePlusRotation(B.ext[0] + 7ll * ge, dr + 15 * wd.K + 6 * e + 3, B.ext[1] + 7ll * ge);
         else for (int j = 0; j < 7; ++j) B.ext[1][7ll * ge + j] = B.ext[0][7ll * ge + j];
         poseRotation(B.ext[1] + 7ll * ge, B.rotExt[1] + 9ll * ge);
     }
@@ -1118,6 +1247,13 @@ __global__ void __launch_bounds__(256) k_backsub(DevBatch B) {
     const double dt = d + lambda * fmax(d, 1e-6);
     double dl = -(g + cd) / dt;
     const double rho0 = B.rho[0][l], minInv = wd->minInv;
+    if (wd->fixedLm && B.lmFixed[l]) {  // held constant: no increment, no landmark term in the prediction
+        B.lmDelta[l] = 0.0;
+        B.lmPred[l] = 0.0;
+        B.lmMaxInc[l] = 0.0;
+        B.rho[1][l] = rho0;
+        return;
+    }
     if (isfinite(dl)) dl = fmax(minInv - rho0, dl);
     B.lmDelta[l] = dl;
     // landmark terms of -dx^T (g + 0.5 H dx): the cross term c.dx_r is
@@ -1226,11 +1362,18 @@ __global__ void __launch_bounds__(256) k_lm_update(DevBatch B, int maxIterations
             st.status = CGMLI_E_COST_MISMATCH; st.mode = kModeDone; st.acceptNow = 0; return;
         }
     }
+    if (B.solveStatus[wdx] != CGMLI_OK) { st.status = B.solveStatus[wdx]; st.mode = kModeDone; st.acceptNow = 0; return; }
+    // time budget (BackendOptimizer.cpp:177,242): after a step solved at pass iteration
+    // i >= min_iterations with a step already accepted, an elapsed budget ends the
+    // solve before this step's acceptance test
+    const bool expired = !probe && B.budgetNs > 0 && globalTimerNs() - st.t0 >= (unsigned long long)B.budgetNs;
+    if (expired && st.iterations - st.passStart >= B.minIterations && st.accepted > st.passAccepted) {
+        st.mode = kModeDone; st.acceptNow = 0; return;
+    }
     st.predicted = predicted;
     st.trialCost = trialCost;
     st.trialValid = tvalid;
     st.maxInc = mx;
-    if (B.solveStatus[wdx] != CGMLI_OK) { st.status = B.solveStatus[wdx]; st.mode = kModeDone; st.acceptNow = 0; return; }
     if (probe) { st.acceptNow = 0; return; }
     st.iterations += 1;
     st.acceptNow = 0;
@@ -1257,6 +1400,8 @@ __global__ void __launch_bounds__(256) k_lm_update(DevBatch B, int maxIterations
     }
     // the pass may use what the finished passes left of the budget
     if (st.iterations - st.passStart + st.charged >= maxIterations && st.mode != kModeDone) st.mode = kModeDone;
+    // an elapsed time budget ends the solve before the next iteration i >= max(min_iterations, 1)
+    if (expired && st.mode != kModeDone && st.iterations - st.passStart >= B.minIterations) st.mode = kModeDone;
     if (st.mode == kModeDone && st.status == CGMLI_OK && st.accepted == st.passAccepted && !st.converged) st.status = CGMLI_E_NO_STEP;
 }
 
@@ -1395,16 +1540,86 @@ __global__ void k_lm_init(DevBatch B, double lambda0) {
     st.maxInc = 0; st.mode = kModeLinearize; st.iterations = 0; st.accepted = 0; st.converged = 0; st.status = CGMLI_OK;
     st.acceptNow = 0; st.trialValid = 0;
     st.passStart = 0; st.passAccepted = 0; st.charged = 0; st.pass = 0; st.pad = 0;
+    st.t0 = globalTimerNs();
+}
+
+// ---------------------------------------------------------------------------------------
+// Per-factor evaluation at the accepted states (VisualCudaBatch::evaluate,
+// VisualCudaBatch.cu:11-21,404-431): one thread per observation writes the
+// whitened residual and, with derivatives, the 2 x 26 tangent Jacobian (anchor
+// pose, observer pose, anchor extrinsic, observer extrinsic, td, rho; before the
+// robust loss).  The accepted rotations are refreshed first by k_rotations.
+__global__ void k_rotations(DevBatch B) {
+    const WinDesc& wd = B.win[blockIdx.x];
+    for (int k = threadIdx.x; k < wd.K; k += blockDim.x) poseRotation(B.pose[0] + 7ll * (wd.kf0 + k), B.rotKf[0] + 9ll * (wd.kf0 + k));
+    for (int e = threadIdx.x; e < wd.E; e += blockDim.x) poseRotation(B.ext[0] + 7ll * (wd.ext0 + e), B.rotExt[0] + 9ll * (wd.ext0 + e));
+}
+constexpr int kFactorRecord = 2 + CGMLI_FACTOR_JACOBIAN;  // residual, then the Jacobian rows
+__global__ void __launch_bounds__(128) k_evaluate(DevBatch B, int derivatives, double* out, int* valid) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= B.numObs) return;
+    const int l = B.obLm[f], wdx = B.lmWin[l];
+    const WinDesc wd = B.win[wdx];
+    FactorIn in;
+    int kfa, kfb, ea, eb;
+    gatherFactor(B, wd, wdx, l, f, 0, in, kfa, kfb, ea, eb);
+    FactorOut o;
+    const bool ok = evalBearingFactor(in, derivatives != 0, o);
+    double* dst = out + (long long)kFactorRecord * f;
+    dst[0] = ok ? o.r[0] : 0.0;
+    dst[1] = ok ? o.r[1] : 0.0;
+    valid[f] = ok ? 1 : 0;
+    if (!derivatives) return;
+    for (int r = 0; r < 2; ++r) {
+        double* J = dst + 2 + 26 * r;
+        for (int c = 0; c < 6; ++c) {
+            J[c] = ok ? o.Ja[6 * r + c] : 0.0;
+            J[6 + c] = ok ? o.Jb[6 * r + c] : 0.0;
+            J[12 + c] = ok ? o.Jea[6 * r + c] : 0.0;
+            J[18 + c] = ok ? o.Jeb[6 * r + c] : 0.0;
+        }
+        J[24] = ok ? o.Jtd[r] : 0.0;
+        J[25] = ok ? o.Jrho[r] : 0.0;
+    }
+}
+
+// Caller-evaluated factors (solveOnline's retainedH / retainedG and the host
+// trial cost, BackendOptimizer.cpp:210-225,276-279): adds the host's normal
+// equations and cost to the retained system of each flagged window at a new
+// linearization point, or the host's trial cost to the trial.
+__global__ void k_add_host(DevBatch B, const double* hostH, const double* hostG, const double* hostCost, const unsigned char* flag,
+                           int trial) {
+    const int w = blockIdx.x;
+    if (!flag[w]) return;
+    const int mode = B.lm[w].mode;
+    if (mode == kModeDone || (!trial && mode != kModeLinearize)) return;
+    const WinDesc& wd = B.win[w];
+    if (trial) {
+        if (threadIdx.x == 0) B.trialRet[w] += hostCost[w];
+        return;
+    }
+    const long long nn = (long long)wd.Nr * wd.Nr;
+    for (long long i = threadIdx.x; i < nn; i += blockDim.x) B.Hret[wd.dense0 + i] += hostH[wd.dense0 + i];
+    for (int i = threadIdx.x; i < wd.Nr; i += blockDim.x) B.gret[wd.vec0 + i] += hostG[wd.vec0 + i];
+    if (threadIdx.x == 0) B.costRet[w] += hostCost[w];
 }
 
 // ---------------------------------------------------------------------------------------
 // host-side launchers (called by backend_host.cu)
+void launchEvaluate(const DevBatch& B, int derivatives, double* out, int* valid, cudaStream_t s) {
+    k_rotations<<<B.numWindows, 64, 0, s>>>(B);
+    if (B.numObs > 0) k_evaluate<<<(B.numObs + 127) / 128, 128, 0, s>>>(B, derivatives, out, valid);
+}
+void launchAddHost(const DevBatch& B, const double* hostH, const double* hostG, const double* hostCost, const unsigned char* flag,
+                   int trial, cudaStream_t s) {
+    k_add_host<<<B.numWindows, 256, 0, s>>>(B, hostH, hostG, hostCost, flag, trial);
+}
 size_t linearizeSmemBytes(int maxNs, bool mixed) { return kLinWarps * landmarkWarpBytes(maxNs, mixed); }
 size_t schurSmemBytes() { return kSchurSmemDoubles * sizeof(double); }
 size_t factorSmemBytes(int maxNr) {
-    // one panel of kFacPanel columns over the padded rows, three n-vectors, the diagonal block
+    // one panel of kFacPanel columns over the padded rows, four n-vectors, the diagonal block
     const size_t npad = (((size_t)maxNr + 31) & ~(size_t)31) + kFacPanel;
-    return (npad * kFacPanel + 3 * (size_t)maxNr + kFacPanel * kFacPanel) * sizeof(double);
+    return (npad * kFacPanel + 4 * (size_t)maxNr + kFacPanel * kFacPanel) * sizeof(double);
 }
 
 // The dynamic shared-memory cap is a per-function attribute shared by every
@@ -1434,8 +1649,12 @@ cudaError_t configureKernels(size_t linSmem, size_t facSmem) {
     return cudaFuncSetAttribute(k_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)facMax);
 }
 
-int launchIteration(const DevBatch& B, const LaunchPlan& P, int refinement, int maxIterations, int probe, double* Sdebug,
-                    cudaStream_t s, LaunchHook hook, void* ctx) {
+// One LM iteration in three parts (kIterLinearize: the linearization up to the
+// retained system; kIterStep: factorization, candidate, back-substitution and
+// trial costs; kIterDecide: the LM decision and acceptance), so that a
+// host-driven loop can add caller-evaluated factors between them.
+int launchIterationParts(const DevBatch& B, const LaunchPlan& P, int refinement, int maxIterations, int probe, double* Sdebug,
+                         cudaStream_t s, LaunchHook hook, void* ctx, int parts) {
     const int W = B.numWindows;
     int n = 0;
     auto run = [&](int kind, auto&& launch) {
@@ -1444,6 +1663,7 @@ int launchIteration(const DevBatch& B, const LaunchPlan& P, int refinement, int 
         if (hook) hook(ctx, kind, 1);
         ++n;
     };
+    if (parts & kIterLinearize) {
     run(CGMLI_KERNEL_ZERO, [&] { k_zero_acc<<<W, 256, 0, s>>>(B); });
     const int runBlocks = (B.numRuns + kLinWarps - 1) / kLinWarps;
     if (B.numRuns > 0)
@@ -1460,6 +1680,8 @@ int launchIteration(const DevBatch& B, const LaunchPlan& P, int refinement, int 
     if (P.numSchurChunks > 0)
         run(CGMLI_KERNEL_LIN_SCHUR, [&] { k_lin_schur<<<P.numSchurChunks, kSchurThreads, schurSmemBytes(), s>>>(B, P.schurChunks); });
     run(CGMLI_KERNEL_RETAINED, [&] { k_retained<<<W, 256, 0, s>>>(B, 0); });
+    }
+    if (parts & kIterStep) {
     run(CGMLI_KERNEL_FACTOR, [&] { k_factor<<<W, kFactorThreads, P.facSmem, s>>>(B, refinement, Sdebug); });
     run(CGMLI_KERNEL_CANDIDATE, [&] { k_candidate<<<W, 128, 0, s>>>(B); });
     if (B.numLandmarks > 0) {
@@ -1469,9 +1691,16 @@ int launchIteration(const DevBatch& B, const LaunchPlan& P, int refinement, int 
         });
     }
     run(CGMLI_KERNEL_RETAINED_TRIAL, [&] { k_retained<<<W, 256, 0, s>>>(B, 1); });
+    }
+    if (parts & kIterDecide) {
     run(CGMLI_KERNEL_LM_UPDATE, [&] { k_lm_update<<<W, 256, 0, s>>>(B, maxIterations, probe); });
     if (!probe) run(CGMLI_KERNEL_ACCEPT, [&] { k_accept<<<W, 256, 0, s>>>(B); });
+    }
     return n;
+}
+int launchIteration(const DevBatch& B, const LaunchPlan& P, int refinement, int maxIterations, int probe, double* Sdebug,
+                    cudaStream_t s, LaunchHook hook, void* ctx) {
+    return launchIterationParts(B, P, refinement, maxIterations, probe, Sdebug, s, hook, ctx, kIterLinearize | kIterStep | kIterDecide);
 }
 int launchGate(const DevBatch& B, const LaunchPlan& P, int pass, int pre, double threshold, double* obP, unsigned char* rejected,
                double* gateStats, int* gateCounts, cudaStream_t s) {

@@ -106,6 +106,13 @@ __device__ __forceinline__ void posePlus(const double* x, const double* d, doubl
     const qd out = qnormalized(qmul(q, ldq(x + 3)));
     y[0] = p.x; y[1] = p.y; y[2] = p.z; y[3] = out.x; y[4] = out.y; y[5] = out.z; y[6] = out.w;
 }
+// Rotation-only chart of a rig extrinsic: the translation stays, the rotation
+// moves on the left (posePlus with rotationOnly, GpuRetainedFactorMath.hpp:28-37).
+__device__ __forceinline__ void posePlusRotation(const double* x, const double* theta, double* y) {
+    const qd q = rotationExp(ld3(theta));
+    const qd out = qnormalized(qmul(q, ldq(x + 3)));
+    y[0] = x[0]; y[1] = x[1]; y[2] = x[2]; y[3] = out.x; y[4] = out.y; y[5] = out.z; y[6] = out.w;
+}
 __device__ __forceinline__ void poseMinus(const double* x, const double* ref, double* d) {
     qd q = qnormalized(qmul(ldq(x + 3), qconj(ldq(ref + 3))));
     if (q.w < 0) q = {-q.x, -q.y, -q.z, -q.w};

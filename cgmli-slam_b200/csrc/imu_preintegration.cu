@@ -35,6 +35,8 @@
 //      raised to it.
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
@@ -579,14 +581,16 @@ namespace cgmli {
 // Launches the preintegration of count intervals whose arrays are already on the device.
 cudaError_t launchImuPreintegration(const ImuLaunch& L, int count, cudaStream_t s) {
     if (count <= 0) return cudaSuccess;
-    static int configured[64] = {};
+    // the shared-memory attribute is set once per device; callers on several
+    // threads (the solver path and cgmli_imu_preintegrate) may race to do it
+    static std::atomic<int> configured[64] = {};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    if (dev >= 0 && dev < 64 && !configured[dev]) {
+    if (dev < 0 || dev >= 64 || !configured[dev].load(std::memory_order_acquire)) {
         e = cudaFuncSetAttribute(k_imu_preintegrate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)imuSmemBytes());
         if (e != cudaSuccess) return e;
-        configured[dev] = 1;
+        if (dev >= 0 && dev < 64) configured[dev].store(1, std::memory_order_release);
     }
     const int blocks = (count + kImuWarps - 1) / kImuWarps;
     k_imu_preintegrate<<<blocks, kImuWarps * 32, imuSmemBytes(), s>>>(L, count);
@@ -620,11 +624,18 @@ int cgmli_imu_preintegrate(const cgmli_imu_parameters* params, const long long* 
     if (ce != cudaSuccess) return cudaFailure(ce, "cudaGetDevice");
     if (g_imu.device != dev) {
         if (g_imu.device >= 0) {
-            // buffers of another device: drop them (their memory stays with that context)
-            g_imu.times = {}; g_imu.t0 = {}; g_imu.t1 = {}; g_imu.readings = {}; g_imu.bias = {};
-            g_imu.ranges = {}; g_imu.status = {}; g_imu.out = {};
+            // buffers, stream and events of the previous device: released with that device current
+            if ((ce = cudaSetDevice(g_imu.device)) != cudaSuccess) return cudaFailure(ce, "cudaSetDevice (previous device)");
+            if (g_imu.stream) cudaStreamSynchronize(g_imu.stream);
+            g_imu.times.release(); g_imu.t0.release(); g_imu.t1.release(); g_imu.readings.release(); g_imu.bias.release();
+            g_imu.ranges.release(); g_imu.status.release(); g_imu.out.release();
+            if (g_imu.stream) cudaStreamDestroy(g_imu.stream);
+            if (g_imu.ev0) cudaEventDestroy(g_imu.ev0);
+            if (g_imu.ev1) cudaEventDestroy(g_imu.ev1);
             g_imu.stream = nullptr;
             g_imu.ev0 = g_imu.ev1 = nullptr;
+            g_imu.device = -1;
+            if ((ce = cudaSetDevice(dev)) != cudaSuccess) return cudaFailure(ce, "cudaSetDevice");
         }
         if ((ce = cudaStreamCreateWithFlags(&g_imu.stream, cudaStreamNonBlocking)) != cudaSuccess)
             return cudaFailure(ce, "cudaStreamCreate");

@@ -49,6 +49,10 @@ struct Request {
 
 // Device bytes a window occupies in a batch (observation, landmark and dense
 // per-window arrays, both state buffers, the staged rows and the marginalization).
+// The solvers' device arrays are grow-only and grow by at least half their size,
+// so a batch whose windows need N bytes can leave a solver holding up to 1.5 N:
+// admission counts kGrowth times the footprint.
+constexpr double kGrowth = 1.5;
 long long footprint(const cgmli_window& w) {
     const long long F = w.num_observations, L = w.num_landmarks, K = w.num_keyframes;
     const long long ncal = (w.estimate_extrinsics ? 6ll * w.num_extrinsics : 0) + (w.estimate_td ? 1 : 0);
@@ -63,7 +67,8 @@ struct cgmli_server {
     std::mutex mu;
     std::condition_variable work, done, freed, launchedCv;
     std::deque<Request*> queue;
-    std::unordered_map<long long, std::unique_ptr<Request>> requests;
+    // shared: a poller waiting on a request keeps it alive if another thread releases it
+    std::unordered_map<long long, std::shared_ptr<Request>> requests;
     long long nextTicket = 1;
     bool stopping = false;
     std::thread worker;
@@ -77,6 +82,7 @@ struct cgmli_server {
         double launchMs = 0;
     };
     bool busy[2] = {false, false};                 // solver has a launched, uncompleted batch
+    long long solverBytes[2] = {0, 0};             // device bytes each solver holds (after its last launch)
     std::deque<std::unique_ptr<Batch>> launched;   // scheduler -> completion thread
     bool schedulerDone = false;
     bool trace = false;
@@ -159,7 +165,11 @@ struct cgmli_server {
     // free, builds and launches it, and hands it to the completion thread.
     void run() {
         int cur = 0;
-        const long long budget = opt.memory_budget_bytes;
+        // each solver keeps its device arrays between batches, so the budget is
+        // split: a batch may hold at most half of it, growth headroom included,
+        // and the two solvers together stay within the whole budget (a single
+        // window above that half still runs, alone in its batch)
+        const long long perSolver = opt.memory_budget_bytes / 2;
         // CGMLI_SERVER_TRACE set: one line per batch on stderr (size, host launch
         // time, the completion thread's wait and read-back; milliseconds)
         trace = std::getenv("CGMLI_SERVER_TRACE") != nullptr;
@@ -173,8 +183,8 @@ struct cgmli_server {
                 if (busy[cur]) freed.wait(lock, [&] { return !busy[cur]; });  // stopping with queued requests
                 long long bytes = 0;
                 while (!queue.empty() && (int)next->reqs.size() < opt.max_batch_windows) {
-                    const long long f = footprint(queue.front()->window);
-                    if (!next->reqs.empty() && bytes + f > budget) break;
+                    const long long f = (long long)(kGrowth * (double)footprint(queue.front()->window));
+                    if (!next->reqs.empty() && bytes + f > perSolver) break;
                     bytes += f;
                     next->reqs.push_back(queue.front());
                     queue.pop_front();
@@ -185,8 +195,11 @@ struct cgmli_server {
             next->solver = cur;
             launch(*next);
             next->launchMs = std::chrono::duration<double, std::milli>(Clock::now() - c0).count();
+            long long held = 0;  // the solver's device arrays after this batch's allocations (only this thread launches)
+            if (cgmli_solver_device_bytes(solver[cur], &held) != CGMLI_OK) held = 0;
             {
                 std::lock_guard<std::mutex> lock(mu);
+                solverBytes[cur] = held;
                 launched.push_back(std::move(next));
             }
             launchedCv.notify_one();
@@ -287,7 +300,7 @@ int submitAt(cgmli_server* s, cgmli_window* window, int victim_kf, Clock::time_p
     const int st = cgmli::validateWindow(*window, 0, why);
     if (st != CGMLI_OK) return setLastError(st, why.c_str());
     if (victim_kf < -1 || victim_kf >= window->num_keyframes) return setLastError(CGMLI_E_INVALID, "server: victim keyframe out of range");
-    auto r = std::make_unique<Request>();
+    auto r = std::make_shared<Request>();
     r->window = *window;
     r->victim = victim_kf;
     r->submitted = arrival;
@@ -297,7 +310,7 @@ int submitAt(cgmli_server* s, cgmli_window* window, int victim_kf, Clock::time_p
         r->ticket = s->nextTicket++;
         *ticket = r->ticket;
         s->queue.push_back(r.get());
-        s->requests.emplace(r->ticket, std::move(r));
+        s->requests.emplace(r->ticket, r);
     }
     s->work.notify_one();
     return CGMLI_OK;
@@ -376,7 +389,7 @@ int cgmli_server_poll(cgmli_server* s, long long ticket, int wait, cgmli_solve_r
     std::unique_lock<std::mutex> lock(s->mu);
     auto it = s->requests.find(ticket);
     if (it == s->requests.end()) return setLastError(CGMLI_E_INVALID, "server: unknown ticket");
-    Request* r = it->second.get();
+    const std::shared_ptr<Request> r = it->second;  // stays valid if the request is released while we wait
     if (!r->complete) {
         if (!wait) return CGMLI_E_PENDING;
         s->done.wait(lock, [&] { return r->complete; });
@@ -421,6 +434,13 @@ int cgmli_server_read_gate(cgmli_server* s, long long ticket, cgmli_gate_report*
     if (!r.complete) return setLastError(CGMLI_E_PENDING, "server: request not complete");
     *report = r.gate;
     if (rejected && !r.rejected.empty()) std::copy(r.rejected.begin(), r.rejected.end(), rejected);
+    return CGMLI_OK;
+}
+
+int cgmli_server_device_bytes(cgmli_server* s, long long* bytes) {
+    if (!s || !bytes) return setLastError(CGMLI_E_INVALID, "server: null server or output");
+    std::lock_guard<std::mutex> lock(s->mu);
+    *bytes = s->solverBytes[0] + s->solverBytes[1];
     return CGMLI_OK;
 }
 

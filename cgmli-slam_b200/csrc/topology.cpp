@@ -103,6 +103,15 @@ int validateWindow(const cgmli_window& w, int index, std::string& why) {
                 return bad("prior block index");
         }
     }
+    if (w.kf_fixed)
+        for (int k = 0; k < w.num_keyframes; ++k)
+            if (w.kf_fixed[k] & ~(CGMLI_FIX_POSE | CGMLI_FIX_VELOCITY | CGMLI_FIX_BIAS)) return bad("kf_fixed has unknown bits");
+    if (w.ext_chart && w.estimate_extrinsics)
+        for (int e = 0; e < w.num_extrinsics; ++e)
+            if (w.ext_chart[e] > CGMLI_CHART_FIXED) return bad("ext_chart outside CGMLI_CHART_*");
+    if (w.lm_fixed)
+        for (int l = 0; l < w.num_landmarks; ++l)
+            if (w.lm_fixed[l] > 1) return bad("lm_fixed entries must be 0 or 1");
     const int ncal = (w.estimate_extrinsics ? 6 * w.num_extrinsics : 0) + (w.estimate_td ? 1 : 0);
     if (6 * w.num_keyframes + ncal > 400) {
         std::snprintf(buf, sizeof buf, "window %d: visual dimension above 400", index);
@@ -142,6 +151,14 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
         d.kf0 = kf; d.ext0 = ex; d.cam0 = cam; d.lm0 = lm; d.obs0 = ob; d.imu0 = im;
         d.vec0 = (int)vec; d.dense0 = dense; d.acc0 = acc; d.sch0 = sch;
         d.huber = w.huber_scale; d.minInv = w.min_inverse_distance;
+        d.charts = 0;
+        if (w.kf_fixed)
+            for (int k = 0; k < d.K; ++k) d.charts |= w.kf_fixed[k] ? 1 : 0;
+        if (d.estExt && w.ext_chart)
+            for (int e = 0; e < d.E; ++e) d.charts |= w.ext_chart[e] ? 1 : 0;
+        d.fixedLm = 0;
+        if (w.lm_fixed)
+            for (int l = 0; l < d.L; ++l) d.fixedLm |= w.lm_fixed[l];
         hb.maxNpc = std::max(hb.maxNpc, d.Npc);
         hb.maxNr = std::max(hb.maxNr, d.Nr);
         vec += d.Nr;
@@ -180,6 +197,7 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
     sizeTo(hb.keyOrder, ob);
     sizeTo(hb.obBearing, 3ll * ob); sizeTo(hb.obP, 6ll * ob); sizeTo(hb.obVel, 3ll * ob); sizeTo(hb.obTime, ob);
     sizeTo(hb.pose, 7ll * kf); sizeTo(hb.sb, 9ll * kf); sizeTo(hb.ext, 7ll * ex); sizeTo(hb.td, count); sizeTo(hb.rho, lm);
+    sizeTo(hb.colChart, vec); sizeTo(hb.lmFixed, lm);
     sizeTo(hb.imu, (size_t)kImuDoubles * im); sizeTo(hb.imuKf, im);
     sizeTo(hb.priorKind, pblk); sizeTo(hb.priorIndex, pblk); sizeTo(hb.priorCol, pblk); sizeTo(hb.priorOff, pblk);
     sizeTo(hb.priorA, pA); sizeTo(hb.priorR0, pR); sizeTo(hb.priorRef, pRef);
@@ -193,6 +211,25 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
         WindowPart& P = part[i];
         // states, rig, IMU, prior
         std::memcpy(&hb.pose[7ll * d.kf0], w.poses, sizeof(double) * 7 * d.K);
+        {
+            // solve-time chart of every retained column (kColFree / kColFixed / the rotation-only pair)
+            signed char* cc = &hb.colChart[d.vec0];
+            for (int c = 0; c < d.Nr; ++c) cc[c] = kColFree;
+            if (w.kf_fixed)
+                for (int k = 0; k < d.K; ++k) {
+                    const int m = w.kf_fixed[k];
+                    for (int c = 0; c < 6; ++c) if (m & CGMLI_FIX_POSE) cc[15 * k + c] = kColFixed;
+                    for (int c = 6; c < 9; ++c) if (m & CGMLI_FIX_VELOCITY) cc[15 * k + c] = kColFixed;
+                    for (int c = 9; c < 15; ++c) if (m & CGMLI_FIX_BIAS) cc[15 * k + c] = kColFixed;
+                }
+            if (d.estExt && w.ext_chart)
+                for (int e = 0; e < d.E; ++e) {
+                    const int c0 = 15 * d.K + 6 * e;
+                    for (int c = 0; c < 6; ++c)
+                        cc[c0 + c] = w.ext_chart[e] == CGMLI_CHART_FIXED ? kColFixed
+                                     : w.ext_chart[e] == CGMLI_CHART_ROTATION_ONLY ? (c < 3 ? kColRotRho : kColRotTheta) : kColFree;
+                }
+        }
         std::memcpy(&hb.sb[9ll * d.kf0], w.speed_bias, sizeof(double) * 9 * d.K);
         std::memcpy(&hb.ext[7ll * d.ext0], w.extrinsics, sizeof(double) * 7 * d.E);
         hb.td[i] = w.td ? *w.td : 0.0;
@@ -335,6 +372,7 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
             P.cross += ns;
             P.maxNs = std::max(P.maxNs, ns);
             hb.rho[g] = w.rho[l];
+            hb.lmFixed[g] = w.lm_fixed ? w.lm_fixed[l] : 0;
             // observations sorted by observer keyframe (slot order), stable
             int fo[kMaxTrackChunk];
             bool inOrder = true;

@@ -187,6 +187,8 @@ struct HostBatch {
     HVec<double> obBearing, obP, obVel, obTime;
     // states
     HVec<double> pose, sb, ext, td, rho;
+    HVec<signed char> colChart;   // per retained column of each window (at WinDesc::vec0): kCol*
+    HVec<unsigned char> lmFixed;  // per device landmark: 1 = inverse distance held constant
     // IMU and priors
     HVec<double> imu;
     HVec<int> imuKf;

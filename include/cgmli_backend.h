@@ -54,6 +54,9 @@ enum {
 enum { CGMLI_PRECISION_FP64 = 0, CGMLI_PRECISION_MIXED = 1 };
 enum { CGMLI_PRIOR_POSE = 0, CGMLI_PRIOR_SPEED_BIAS = 1, CGMLI_PRIOR_EXTRINSIC = 2, CGMLI_PRIOR_TIME_OFFSET = 3 };
 enum { CGMLI_MARGIN_OLD = 0, CGMLI_MARGIN_SECOND_NEW = 1, CGMLI_MARGIN_SECOND_NEW_IMU_MERGE = 2 };
+/* Solve-time charts of cgmli_window (kf_fixed bits, ext_chart values). */
+enum { CGMLI_FIX_POSE = 1, CGMLI_FIX_VELOCITY = 2, CGMLI_FIX_BIAS = 4 };
+enum { CGMLI_CHART_FULL = 0, CGMLI_CHART_ROTATION_ONLY = 1, CGMLI_CHART_FIXED = 2 };
 /* Outcome of the IMU merge of a CGMLI_MARGIN_SECOND_NEW_IMU_MERGE marginalization. */
 enum { CGMLI_IMU_MERGE_NONE = 0,         /* no victim, or another policy */
        CGMLI_IMU_MERGE_REINTEGRATED = 1, /* the two edges became one re-integrated factor */
@@ -118,6 +121,17 @@ typedef struct cgmli_window {
     const double *prior_ref;    /* concatenated ambient references (7, 9, 7 or 1 per block) */
     const double *prior_A;      /* prior_rank x (sum of tangent sizes), row-major */
     const double *prior_r0;     /* prior_rank */
+    /* Solve-time charts: blocks held constant and restricted tangents for the LM
+     * solve only, as the reference sets them on its Ceres problem for one solve
+     * (constant blocks are not variables, BackendOptimizer.cpp:44-66; the
+     * bias-frozen speed/bias SubsetManifold and the rotation-only rig chart,
+     * :83-91,783-795).  NULL: every block free with its full chart.  The
+     * marginalization, the gate and the calibration information keep the full
+     * charts (the reference's graph, marginalizer and prior do too). */
+    const unsigned char *kf_fixed;  /* K or NULL: CGMLI_FIX_POSE | _VELOCITY | _BIAS (gyro and accel bias) bits */
+    const unsigned char *ext_chart; /* E or NULL (estimate_extrinsics = 1): CGMLI_CHART_FULL, _ROTATION_ONLY
+                                       (the translation stays; Plus(T, theta) = (Exp(theta) R, p)) or _FIXED */
+    const unsigned char *lm_fixed;  /* L or NULL: 1 holds the inverse distance constant (no Schur elimination) */
 } cgmli_window;
 
 typedef struct cgmli_solver_options {
@@ -129,8 +143,14 @@ typedef struct cgmli_solver_options {
                                 stay FP64 */
     int refinement_steps;    /* iterative refinement after the FP64 Cholesky (0..2) */
     double initial_lambda;   /* reference: 1e-4 */
-    int slabs_per_window;    /* reserved, must be 0 */
-    int threads_per_block;   /* reserved, must be 0 */
+    int min_iterations;      /* iterations a window always runs before the time budget may stop it
+                                (the reference's minIterations, BackendOptimizer.cpp:177,242) */
+    double time_budget_s;    /* <= 0: none.  Otherwise each window's solve stops, as the reference's
+                                realtime limit does (realtime_time_limit 0.04 s in its robot
+                                configuration): before iteration i >= max(min_iterations, 1) once the
+                                budget has elapsed, and after a step solved at i >= min_iterations once
+                                it has elapsed and a step was accepted (that step's trial is dropped).
+                                Elapsed time is device time since the solve's first kernel. */
 } cgmli_solver_options;
 
 typedef struct cgmli_solve_report {
@@ -219,6 +239,53 @@ int cgmli_solver_window_dims(cgmli_solver *solver, int window, int *retained, in
 /* Elapsed device milliseconds of the last cgmli_solver_solve / _step measured
  * with CUDA events on the solver's stream, and the number of kernel launches. */
 int cgmli_solver_last_timing(cgmli_solver *solver, double *milliseconds, int *launches);
+/* Device bytes the solver's grow-only arrays hold (they stay allocated until
+ * cgmli_solver_destroy).  A diagnostic of this library; no counterpart in the
+ * reference. */
+int cgmli_solver_device_bytes(cgmli_solver *solver, long long *bytes);
+
+/* Per-factor evaluation of every bearing factor of the batch at the accepted
+ * states (VisualCudaBatch::evaluate, src/backend/VisualCudaBatch.cu:404-431):
+ * the whitened residual, the validity and, with derivatives, the tangent
+ * Jacobian before the robust loss.  The reference returns ambient 2x7 blocks
+ * that its caller lifts by the PlusJacobian; these are the lifted (left SE(3)
+ * tangent) blocks directly.  cgmli_solver_read_factors copies window w's
+ * num_observations factors in the caller's observation order: residuals 2 per
+ * factor, valid 1 per factor, jacobians CGMLI_FACTOR_JACOBIAN per factor (NULL:
+ * skipped; needs derivatives), row-major 2 x 26 over the columns anchor pose
+ * [0, 6), observer pose [6, 12), anchor camera extrinsic [12, 18), observer
+ * camera extrinsic [18, 24), time offset 24, inverse distance 25.  A factor whose
+ * two cameras share one extrinsic block carries that block's whole derivative in
+ * [12, 18) and zeros in [18, 24); a same-epoch factor has zero pose columns, and
+ * with a shared extrinsic zero extrinsic columns too (the reference requires
+ * them to cancel exactly).  Extrinsic and time-offset columns are filled only
+ * for windows that estimate them.  Asynchronous; the read waits. */
+#define CGMLI_FACTOR_JACOBIAN 52
+int cgmli_solver_evaluate(cgmli_solver *solver, int derivatives);
+int cgmli_solver_read_factors(cgmli_solver *solver, int window, double *residuals, int *valid, double *jacobians);
+
+/* ---- Caller-evaluated factors --------------------------------------------------
+ * The reference keeps factors its device path does not support on the CPU and
+ * hands their normal equations to each solveOnline call (retainedH, retainedG;
+ * src/backend/VisualCudaBatch.hpp:61, evaluated at src/backend/BackendOptimizer.cpp:
+ * 210-221 and added to the trial cost at :276-279).  cgmli_solver_solve_host runs
+ * the same damped LM as cgmli_solver_solve with such factors: at every new
+ * linearization point of a window it calls fn with trial = 0, the window's
+ * accepted states (poses K*7, speed/bias K*9, extrinsics E*7, td 1) and zeroed
+ * H (N_r x N_r row-major, the window's retained tangent columns) and g (N_r);
+ * fn writes the factors' Gauss-Newton H = J^T J and gradient g = J^T r and their
+ * cost 0.5 |r|^2, which are added to the window's retained system and cost.
+ * Before each acceptance test it calls fn with trial = 1, the candidate states
+ * and H = g = NULL for the cost alone.  Windows with has_host[w] = 0 (or
+ * has_host NULL: every window) are not called.  fn returns 0, or nonzero to fail
+ * the window with CGMLI_E_NONFINITE.  Unlike cgmli_solver_solve the host takes
+ * part in every iteration: after each linearization and after each trial the
+ * library waits for the device and copies the states of the called windows,
+ * as the reference's non-resident loop does; fn runs on the calling thread. */
+typedef int (*cgmli_host_factor_fn)(void *ctx, int window, int trial, const double *poses, const double *speed_bias,
+                                    const double *extrinsics, const double *td, double *H, double *g, double *cost);
+int cgmli_solver_solve_host(cgmli_solver *solver, int max_iterations, const unsigned char *has_host, cgmli_host_factor_fn fn,
+                            void *ctx);
 
 /* Device-side snapshot of the accepted states and its restore: the numeric
  * checkpoint / rollback of a backend transaction
@@ -309,14 +376,16 @@ int cgmli_marg_subtract(const double *coupling, const double *solution, int elim
  * another allocator.  This entry point has no counterpart in the reference.
  * H (n x n, column-major, lower triangle read), eigenvalues (n, ascending) and
  * eigenvectors (n x n, column-major) are DEVICE pointers owned by the caller;
- * stream is a cudaStream_t (NULL: the default stream), synchronized before
- * returning.  The solver's work arrays live in one fixed device array of about
- * 1 MiB that every GPU loading the library holds until the process exits, so
- * n is limited to CGMLI_MARG_EIGEN_NOALLOC_MAX_N (larger n: CGMLI_E_LIMIT).
- * The first call on a device looks the array's address up (set-up); make that
- * first call before any stream capture.  All calls share the array: calls
- * that overlap on the GPU (other host threads or streams) race and must be
- * serialized by the caller. */
+ * stream is a cudaStream_t (NULL: the default stream).  Every call waits for
+ * the stream before it returns (it copies the solver's status word to the host
+ * and synchronizes), so it cannot be called while that stream, or any stream,
+ * is being captured into a CUDA graph.  The solver's work arrays live in one
+ * fixed device array of about 1 MiB that every GPU loading the library holds
+ * until the process exits, so n is limited to CGMLI_MARG_EIGEN_NOALLOC_MAX_N
+ * (larger n: CGMLI_E_LIMIT).  The first call on a device looks the array's
+ * address up (set-up).  All calls share the array: calls that overlap on the
+ * GPU (other host threads or streams) race and must be serialized by the
+ * caller. */
 #define CGMLI_MARG_EIGEN_NOALLOC_MAX_N 256
 int cgmli_marg_eigen_noalloc(const double *H, int n, double *eigenvalues, double *eigenvectors, void *stream);
 
@@ -428,7 +497,8 @@ int cgmli_solver_read_imu(cgmli_solver *solver, int window, cgmli_frozen_imu *im
 typedef struct cgmli_server_options {
     int device;
     int max_batch_windows;          /* 0: 512 */
-    long long memory_budget_bytes;  /* 0: 40 GiB */
+    long long memory_budget_bytes;  /* 0: 40 GiB; device bytes of both solvers together (see
+                                       cgmli_server_device_bytes) */
     int iterations;                 /* LM iterations per request, >= 1 */
     int policy;                     /* CGMLI_MARGIN_OLD or _SECOND_NEW for requests with a victim */
     double nis_threshold;           /* > 0: solve with the NIS gate and outlier refits
@@ -457,6 +527,13 @@ int cgmli_server_read_prior(cgmli_server *server, long long ticket, int *rank, i
 int cgmli_server_read_gate(cgmli_server *server, long long ticket, cgmli_gate_report *report, unsigned char *rejected);
 /* Frees a completed request's record. */
 int cgmli_server_release(cgmli_server *server, long long ticket);
+/* Device bytes both solvers of the server hold (each keeps its grow-only arrays
+ * between batches).  Admission keeps this within memory_budget_bytes: a batch
+ * may use at most half of the budget, counting the arrays' growth headroom (a
+ * window that alone exceeds that half still runs, alone in its batch, and can
+ * take the total above the budget).
+ * A diagnostic of this library; no counterpart in the reference. */
+int cgmli_server_device_bytes(cgmli_server *server, long long *bytes);
 /* Replays a request trace from a host thread (load testing): request i submits
  * windows[i] with victims[i] at arrival_s[i] seconds (non-decreasing) after the
  * call starts; latency_ms[i] is measured from that scheduled arrival to the

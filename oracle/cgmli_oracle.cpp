@@ -1147,13 +1147,64 @@ struct Step {
     int status = CGMLI_OK;
 };
 // solveOnline (VisualCudaBatch.cu:138-205,530-604) at fixed lambda.
+// Solve-time charts (the reference's constant blocks and restricted tangents of
+// one solve, BackendOptimizer.cpp:44-66,83-91,783-795): the columns of T map the
+// restricted tangent into the window's full tangent.  A free column is a unit
+// vector; a rotation-only extrinsic's theta_k moves [rho; theta] along
+// [[p]x e_k; e_k] (its Plus keeps the translation, GpuRetainedFactorMath.hpp:28-37);
+// fixed columns (constant blocks, frozen biases, the folded rho columns) have none.
+struct Charts {
+    std::vector<int> col;                 // restricted coordinate -> its full column (free or theta)
+    std::vector<std::vector<double>> T;   // restricted coordinate -> its full-tangent direction (n)
+    std::vector<char> fixed;              // per full column
+    bool any = false;
+};
+static Charts chartsOf(const cgmli_window& w) {
+    const Layout lay(w);
+    const int n = lay.Nr;
+    Charts c;
+    c.fixed.assign(n, 0);
+    std::vector<char> theta(n, 0);
+    if (w.kf_fixed)
+        for (int k = 0; k < lay.K; ++k) {
+            const int m = w.kf_fixed[k];
+            for (int j = 0; j < 6; ++j) if (m & CGMLI_FIX_POSE) c.fixed[lay.pose(k) + j] = 1;
+            for (int j = 0; j < 3; ++j) if (m & CGMLI_FIX_VELOCITY) c.fixed[lay.sb(k) + j] = 1;
+            for (int j = 3; j < 9; ++j) if (m & CGMLI_FIX_BIAS) c.fixed[lay.sb(k) + j] = 1;
+        }
+    if (lay.estExt && w.ext_chart)
+        for (int e = 0; e < lay.E; ++e) {
+            if (w.ext_chart[e] == CGMLI_CHART_FIXED) for (int j = 0; j < 6; ++j) c.fixed[lay.ext(e) + j] = 1;
+            if (w.ext_chart[e] == CGMLI_CHART_ROTATION_ONLY) {
+                for (int j = 0; j < 3; ++j) { c.fixed[lay.ext(e) + j] = 1; theta[lay.ext(e) + 3 + j] = 1; }
+            }
+        }
+    for (int i = 0; i < n; ++i) {
+        if (c.fixed[i]) { c.any = true; continue; }
+        std::vector<double> t(n, 0.0);
+        t[i] = 1.0;
+        if (theta[i]) {
+            const int e = (i - lay.ext0) / 6, c0 = lay.ext(e), k = i - c0 - 3;
+            const M3 P = skew(ld3(w.extrinsics + 7 * e));
+            for (int a = 0; a < 3; ++a) t[c0 + a] = P[3 * a + k];
+            c.any = true;
+        }
+        c.col.push_back(i);
+        c.T.push_back(std::move(t));
+    }
+    return c;
+}
+static bool landmarkFixed(const cgmli_window& w, int l) { return w.lm_fixed && w.lm_fixed[l]; }
+
 static Step schurStep(const cgmli_window& w, const Linear& lin, double lambda, int refinement = 0) {
     Step st;
     const int n = lin.Nr, L = lin.L;
+    const Charts ch = chartsOf(w);
     st.S = lin.H;
     st.rhs.assign(n, 0.0);
     for (int i = 0; i < n; ++i) st.rhs[i] = lin.g[i];
     for (int l = 0; l < L; ++l) {
+        if (landmarkFixed(w, l)) continue;  // held constant: not eliminated
         const double inv = 1 / dampedPoint(lin.d[l], lambda);
         const auto& c = lin.sc[l];
         const auto& v = lin.sv[l];
@@ -1162,21 +1213,69 @@ static Step schurStep(const cgmli_window& w, const Linear& lin, double lambda, i
             st.rhs[c[i]] -= inv * v[i] * lin.g[n + l];
         }
     }
-    for (int i = 0; i < n; ++i) st.S[(size_t)i * n + i] += lambda * std::max(lin.H[(size_t)i * n + i], 1e-6);
     for (int i = 0; i < n; ++i) st.rhs[i] = -st.rhs[i];
-    std::vector<double> Lm = st.S;
-    if (!cholesky(Lm, n)) { st.status = CGMLI_E_NOT_PD; return st; }
-    std::vector<double> x = st.rhs;
-    cholSolve(Lm, n, x);
-    for (int it = 0; it < refinement; ++it) {
-        std::vector<double> res(n);
-        for (int i = 0; i < n; ++i) {
-            double v = st.rhs[i];
-            for (int j = 0; j < n; ++j) v -= st.S[(size_t)i * n + j] * x[j];
-            res[i] = v;
+    std::vector<double> x(n, 0.0);
+    if (!ch.any) {
+        for (int i = 0; i < n; ++i) st.S[(size_t)i * n + i] += lambda * std::max(lin.H[(size_t)i * n + i], 1e-6);
+        std::vector<double> Lm = st.S;
+        if (!cholesky(Lm, n)) { st.status = CGMLI_E_NOT_PD; return st; }
+        x = st.rhs;
+        cholSolve(Lm, n, x);
+        for (int it = 0; it < refinement; ++it) {
+            std::vector<double> res(n);
+            for (int i = 0; i < n; ++i) {
+                double v = st.rhs[i];
+                for (int j = 0; j < n; ++j) v -= st.S[(size_t)i * n + j] * x[j];
+                res[i] = v;
+            }
+            cholSolve(Lm, n, res);
+            for (int i = 0; i < n; ++i) x[i] += res[i];
         }
-        cholSolve(Lm, n, res);
-        for (int i = 0; i < n; ++i) x[i] += res[i];
+    } else {
+        // restricted system S' = T^T S T damped by lambda max(diag(T^T H T), 1e-6), rhs' = T^T rhs;
+        // reported embedded in the full columns with identity rows at the fixed ones
+        const int m = (int)ch.col.size();
+        auto quad = [&](const std::vector<double>& M, const std::vector<double>& a, const std::vector<double>& b) {
+            double v = 0;
+            for (int i = 0; i < n; ++i) {
+                if (a[i] == 0) continue;
+                double r = 0;
+                for (int j = 0; j < n; ++j) r += M[(size_t)i * n + j] * b[j];
+                v += a[i] * r;
+            }
+            return v;
+        };
+        std::vector<double> Sr((size_t)m * m), Sd((size_t)m * m), rr(m);
+        for (int p = 0; p < m; ++p) {
+            for (int q = 0; q < m; ++q) Sr[(size_t)p * m + q] = quad(st.S, ch.T[p], ch.T[q]);
+            double v = 0;
+            for (int i = 0; i < n; ++i) v += ch.T[p][i] * st.rhs[i];
+            rr[p] = v;
+        }
+        Sd = Sr;
+        for (int p = 0; p < m; ++p) Sd[(size_t)p * m + p] += lambda * std::max(quad(lin.H, ch.T[p], ch.T[p]), 1e-6);
+        std::vector<double> Lm = Sd, y = rr;
+        if (!cholesky(Lm, m)) { st.status = CGMLI_E_NOT_PD; return st; }
+        cholSolve(Lm, m, y);
+        for (int it = 0; it < refinement; ++it) {
+            std::vector<double> res(m);
+            for (int p = 0; p < m; ++p) {
+                double v = rr[p];
+                for (int q = 0; q < m; ++q) v -= Sd[(size_t)p * m + q] * y[q];
+                res[p] = v;
+            }
+            cholSolve(Lm, m, res);
+            for (int p = 0; p < m; ++p) y[p] += res[p];
+        }
+        for (int p = 0; p < m; ++p)
+            for (int i = 0; i < n; ++i) x[i] += ch.T[p][i] * y[p];
+        std::fill(st.S.begin(), st.S.end(), 0.0);
+        std::fill(st.rhs.begin(), st.rhs.end(), 0.0);
+        for (int i = 0; i < n; ++i) if (ch.fixed[i]) st.S[(size_t)i * n + i] = 1.0;
+        for (int p = 0; p < m; ++p) {
+            st.rhs[ch.col[p]] = rr[p];
+            for (int q = 0; q < m; ++q) st.S[(size_t)ch.col[p] * n + ch.col[q]] = Sd[(size_t)p * m + q];
+        }
     }
     st.delta.assign(n + L, 0.0);
     for (int i = 0; i < n; ++i) st.delta[i] = x[i];  // states are unbounded: clampStateStep is the identity
@@ -1187,6 +1286,7 @@ static Step schurStep(const cgmli_window& w, const Linear& lin, double lambda, i
         pred += -x[i] * (lin.g[i] + 0.5 * hd);
     }
     for (int l = 0; l < L; ++l) {
+        if (landmarkFixed(w, l)) continue;  // no increment, no landmark term
         double c = 0;
         for (size_t i = 0; i < lin.sc[l].size(); ++i) c += lin.sv[l][i] * x[lin.sc[l][i]];
         const double gl = lin.g[n + l];
@@ -1231,15 +1331,26 @@ static bool applyStep(const cgmli_window& w, const std::vector<double>& delta, S
         else maxInc = std::max(maxInc, std::fabs(delta[i]));
     }
     if (!ok) return false;
+    // solve-time charts: fixed blocks stay as they are; a rotation-only extrinsic keeps its translation
+    const unsigned char fixPose = CGMLI_FIX_POSE;
     for (int k = 0; k < lay.K; ++k) {
-        posePlus(w.poses + 7 * k, delta.data() + lay.pose(k), out.poses.data() + 7 * k);
-        for (int j = 0; j < 9; ++j) out.sb[9 * k + j] = w.speed_bias[9 * k + j] + delta[lay.sb(k) + j];
+        const int m = w.kf_fixed ? w.kf_fixed[k] : 0;
+        if (!(m & fixPose)) posePlus(w.poses + 7 * k, delta.data() + lay.pose(k), out.poses.data() + 7 * k);
+        for (int j = 0; j < 9; ++j) {
+            const bool held = j < 3 ? (m & CGMLI_FIX_VELOCITY) != 0 : (m & CGMLI_FIX_BIAS) != 0;
+            if (!held) out.sb[9 * k + j] = w.speed_bias[9 * k + j] + delta[lay.sb(k) + j];
+        }
     }
     if (lay.estExt)
-        for (int e = 0; e < lay.E; ++e) posePlus(w.extrinsics + 7 * e, delta.data() + lay.ext(e), out.ext.data() + 7 * e);
+        for (int e = 0; e < lay.E; ++e) {
+            const int chart = w.ext_chart ? w.ext_chart[e] : CGMLI_CHART_FULL;
+            if (chart == CGMLI_CHART_FULL) posePlus(w.extrinsics + 7 * e, delta.data() + lay.ext(e), out.ext.data() + 7 * e);
+            else if (chart == CGMLI_CHART_ROTATION_ONLY)
+                posePlus(w.extrinsics + 7 * e, delta.data() + lay.ext(e) + 3, out.ext.data() + 7 * e, true);
+        }
     if (lay.estTd) out.td = *w.td + delta[lay.td()];
     for (int l = 0; l < lay.L; ++l)
-        out.rho[l] = std::max(w.min_inverse_distance, w.rho[l] + delta[lay.Nr + l]);
+        if (!landmarkFixed(w, l)) out.rho[l] = std::max(w.min_inverse_distance, w.rho[l] + delta[lay.Nr + l]);
     for (double v : out.poses) if (!fin(v)) return false;
     for (double v : out.sb) if (!fin(v)) return false;
     for (double v : out.rho) if (!fin(v)) return false;
@@ -1272,8 +1383,40 @@ static bool windowCost(const cgmli_window& w, double& cost) {
     return fin(cost);
 }
 
+// Options of the LM loop beyond the iteration budget: the reference's
+// minIterations and realtime budget (BackendOptimizer.cpp:177,242; the oracle
+// cannot see the device's clock, so the budget is either elapsed from the start
+// or never), and caller-evaluated factors (solveOnline's retainedH / retainedG,
+// :210-225, and the host trial cost, :276-279) through the C ABI's callback.
+struct LmOptions {
+    int minIterations = 0;
+    bool budgetElapsed = false;
+    cgmli_host_factor_fn host = nullptr;
+    void* hostCtx = nullptr;
+    int hostWindow = 0;
+};
+static bool hostLinearize(const cgmli_window& w, const LmOptions& o, Linear& lin) {
+    if (!o.host) return true;
+    const int n = lin.Nr;
+    std::vector<double> H((size_t)n * n, 0.0), g(n, 0.0);
+    double cost = 0, td = w.td ? *w.td : 0.0;
+    if (o.host(o.hostCtx, o.hostWindow, 0, w.poses, w.speed_bias, w.extrinsics, &td, H.data(), g.data(), &cost) != 0 || !fin(cost))
+        return false;
+    for (size_t i = 0; i < H.size(); ++i) lin.H[i] += H[i];
+    for (int i = 0; i < n; ++i) lin.g[i] += g[i];
+    lin.cost += cost;
+    return true;
+}
+static bool hostTrialCost(const cgmli_window& w, const LmOptions& o, double& cost) {
+    cost = 0;
+    if (!o.host) return true;
+    double td = w.td ? *w.td : 0.0;
+    return o.host(o.hostCtx, o.hostWindow, 1, w.poses, w.speed_bias, w.extrinsics, &td, nullptr, nullptr, &cost) == 0 && fin(cost);
+}
+
 // Resident LM loop of solveVisualSchur (BackendOptimizer.cpp:167-307).
-static int lmSolve(cgmli_window& w, int maxIterations, cgmli_solve_report* rep, double initialLambda, int refinement) {
+static int lmSolve(cgmli_window& w, int maxIterations, cgmli_solve_report* rep, double initialLambda, int refinement,
+                   const LmOptions& opt = LmOptions()) {
     cgmli_solve_report report{};
     double lambda = initialLambda, increase = 2, cost = 0;
     int accepted = 0;
@@ -1281,13 +1424,15 @@ static int lmSolve(cgmli_window& w, int maxIterations, cgmli_solve_report* rep, 
     Linear lin;
     int it = 0, status = CGMLI_OK;
     for (it = 0; it < maxIterations; ++it) {
+        if (it >= opt.minIterations && it > 0 && opt.budgetElapsed) break;
         if (newPoint) {
-            if (!linearize(w, lin)) { status = CGMLI_E_NONFINITE; break; }
+            if (!linearize(w, lin) || !hostLinearize(w, opt, lin)) { status = CGMLI_E_NONFINITE; break; }
             if (it > 0 && std::fabs(lin.cost - cost) > 1e-8 * std::max(1.0, cost)) { status = CGMLI_E_COST_MISMATCH; break; }
             if (it == 0) report.initial_cost = cost = lin.cost;
         }
         Step st = schurStep(w, lin, lambda, refinement);
         if (st.status != CGMLI_OK) { status = st.status; break; }
+        if (it >= opt.minIterations && accepted > 0 && opt.budgetElapsed) break;
         States cand;
         double maxInc = 0, trial = 0;
         bool trialValid = applyStep(w, st.delta, cand, maxInc);
@@ -1296,7 +1441,12 @@ static int lmSolve(cgmli_window& w, int maxIterations, cgmli_solve_report* rep, 
             cw.poses = cand.poses.data(); cw.speed_bias = cand.sb.data(); cw.extrinsics = cand.ext.data(); cw.rho = cand.rho.data();
             double tdv = cand.td;
             if (w.td) cw.td = &tdv;
+            double host = 0;
             trialValid = windowCost(cw, trial);
+            if (trialValid) {
+                if (hostTrialCost(cw, opt, host)) trial += host;
+                else trial = std::numeric_limits<double>::quiet_NaN();  // a failed host evaluation rejects the step
+            }
         }
         report.predicted_reduction = st.predicted;
         report.max_increment = maxInc;
@@ -1995,6 +2145,18 @@ int oracle_step(const cgmli_window* w, double lambda, int refinement, double* de
 int oracle_window_cost(const cgmli_window* w, double* cost) { return orc::windowCost(*w, *cost) ? CGMLI_OK : CGMLI_E_NONFINITE; }
 int oracle_lm_solve(cgmli_window* w, int max_iterations, double initial_lambda, int refinement, cgmli_solve_report* report) {
     return orc::lmSolve(*w, max_iterations, report, initial_lambda, refinement);
+}
+// The LM loop with the minimum iterations, a budget elapsed from the start (or
+// never) and caller-evaluated factors (fn may be NULL).
+int oracle_lm_solve_options(cgmli_window* w, int max_iterations, double initial_lambda, int refinement, int min_iterations,
+                            int budget_elapsed, cgmli_host_factor_fn fn, void* ctx, int window_index, cgmli_solve_report* report) {
+    orc::LmOptions o;
+    o.minIterations = min_iterations;
+    o.budgetElapsed = budget_elapsed != 0;
+    o.host = fn;
+    o.hostCtx = ctx;
+    o.hostWindow = window_index;
+    return orc::lmSolve(*w, max_iterations, report, initial_lambda, refinement, o);
 }
 // CPU baseline: LM over many windows on `threads` host threads.
 int oracle_lm_solve_batch(cgmli_window* windows, int count, int max_iterations, int threads, cgmli_solve_report* reports) {

@@ -54,6 +54,8 @@ def lib() -> C.CDLL:
         P(L, "oracle_window_cost", C.c_int, [W, dp])
         P(L, "oracle_lm_solve", C.c_int, [W, C.c_int, C.c_double, C.c_int, C.POINTER(abi.SolveReport)])
         P(L, "oracle_lm_solve_batch", C.c_int, [W, C.c_int, C.c_int, C.c_int, C.POINTER(abi.SolveReport)])
+        P(L, "oracle_lm_solve_options", C.c_int,
+          [W, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, abi.HOST_FACTOR_FN, C.c_void_p, C.c_int, C.POINTER(abi.SolveReport)])
         P(L, "oracle_robust_normal", C.c_int, [C.c_int, C.c_int, dp, dp, C.c_double, dp, dp, dp, dp])
         P(L, "oracle_eigen_sym", C.c_int, [C.c_int, dp, dp, dp])
         P(L, "oracle_psd_solve", C.c_int, [C.c_int, dp, C.c_int, dp, C.c_double, C.c_double, dp])
@@ -103,6 +105,41 @@ def step(win, nr, L, lam, refinement=0):
 def lm_solve(win, iterations, initial_lambda=1e-4, refinement=0):
     rep = abi.SolveReport()
     st = lib().oracle_lm_solve(C.byref(win), iterations, initial_lambda, refinement, C.byref(rep))
+    return st, rep
+
+
+def host_factor_callback(fn, nr, K, E):
+    """Wraps fn(window, trial, poses (K,7), speed_bias (K,9), extrinsics (E,7), td) -> (H, g, cost) or
+    cost (trial) in the cgmli_host_factor_fn form (the oracle calls it for one window)."""
+
+    def cb(ctx, w, trial, poses, sb, ext, td, H, g, cost):
+        try:
+            out = fn(w, bool(trial), np.ctypeslib.as_array(poses, shape=(K, 7)).copy(), np.ctypeslib.as_array(sb, shape=(K, 9)).copy(),
+                     np.ctypeslib.as_array(ext, shape=(E, 7)).copy(), float(td[0]))
+            if out is None:
+                return 1
+            if trial:
+                cost[0] = float(out)
+                return 0
+            Hm, gv, c = out
+            np.ctypeslib.as_array(H, shape=(nr * nr,))[:] = np.asarray(Hm, dtype=np.float64).reshape(-1)
+            np.ctypeslib.as_array(g, shape=(nr,))[:] = np.asarray(gv, dtype=np.float64)
+            cost[0] = float(c)
+            return 0
+        except Exception:  # noqa: BLE001 - a failed evaluation
+            return 1
+
+    return abi.HOST_FACTOR_FN(cb)
+
+
+def lm_solve_options(win, iterations, min_iterations=0, budget_elapsed=False, host=None, nr=0, window_index=0,
+                     initial_lambda=1e-4, refinement=0):
+    """LM solve in place with the minimum iterations, a budget elapsed from the start (or never) and
+    caller-evaluated factors host(window, trial, poses, speed_bias, extrinsics, td) (see backend.Solver.solve_host)."""
+    rep = abi.SolveReport()
+    cb = host_factor_callback(host, nr, win.num_keyframes, win.num_extrinsics) if host else abi.HOST_FACTOR_FN()
+    st = lib().oracle_lm_solve_options(C.byref(win), iterations, initial_lambda, refinement, min_iterations, int(budget_elapsed), cb,
+                                       None, window_index, C.byref(rep))
     return st, rep
 
 

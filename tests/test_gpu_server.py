@@ -108,3 +108,29 @@ def test_served_gated_equals_alone(backend):
         assert rel(w.state_vector() - x, xa - x) < 1e-7
         srv.release(t)
     srv.close()
+
+
+def _footprint(win):
+    """The server's per-window device estimate (server.cpp footprint())."""
+    F, L, K = win.num_observations, win.num_landmarks, win.num_keyframes
+    ncal = (6 * win.num_extrinsics if win.estimate_extrinsics else 0) + (1 if win.estimate_td else 0)
+    Nr, Npc, m = 15 * K + ncal, 6 * K + ncal, 15 * K + 6 * win.num_extrinsics + 1
+    return F * (120 + 448) + L * (160 + 8 * (6 * 12 + 7)) + 8 * (3 * Nr * Nr + Npc * Npc + 4 * m * m) + 4096
+
+
+def test_two_solvers_stay_within_the_memory_budget(backend):
+    """Both solvers keep their device arrays between batches; admission limits each batch to half
+    of memory_budget_bytes (growth headroom included), so what the two hold together stays within
+    the budget while batches of several windows still form."""
+    windows = synth.make_windows("c4", 16, seed=404)
+    biggest = max(_footprint(w.window) for w in windows)
+    budget = int(2 * 1.5 * 3 * biggest)
+    server = backend.Server(iterations=1, max_batch_windows=16, memory_budget_bytes=budget)
+    tickets = [server.submit(w, 0) for w in windows]
+    for t in tickets:
+        rep, _ = server.poll(t)
+        assert rep.status == 0
+        server.release(t)
+    held = server.device_bytes()
+    server.close()
+    assert 0 < held <= budget

@@ -6,7 +6,8 @@ the library allocate; this entry point keeps its work arrays in a fixed device
 array instead.  The test gives it device buffers (allocated here by the test,
 not by the library) and compares its results with cgmli_marg_eigen on the same
 matrices, within the dense-eigensolver tolerance of the other tests, on two
-calls in a row (the second reuses the shared array left by the first).
+calls in a row (the second reuses the shared array left by the first), and
+checks that the second call leaves the device's free memory unchanged.
 This file is collected last on purpose.
 """
 from __future__ import annotations
@@ -27,15 +28,20 @@ def _spd(rng, n, rank_deficit=2):
 
 
 def _noalloc(lib, torch, H):
+    """Runs the entry point on device buffers the test allocates; also returns the device's
+    free memory (cudaMemGetInfo) right before and right after the call."""
     n = H.shape[0]
     dH = torch.tensor(np.asfortranarray(H).ravel(order="F"), dtype=torch.float64, device="cuda")
     dev = torch.empty(n, dtype=torch.float64, device="cuda")
     dU = torch.empty(n * n, dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
     code = lib.cgmli_marg_eigen_noalloc(C.c_void_p(dH.data_ptr()), n, C.c_void_p(dev.data_ptr()), C.c_void_p(dU.data_ptr()),
                                         C.c_void_p(stream))
+    free1 = torch.cuda.mem_get_info()[0]
     assert code == 0, lib.cgmli_last_error()
-    return dev.cpu().numpy(), dU.cpu().numpy().reshape(n, n, order="F")
+    return dev.cpu().numpy(), dU.cpu().numpy().reshape(n, n, order="F"), free0, free1
 
 
 def test_noalloc_eigen_matches_allocating_entry_point_twice():
@@ -44,10 +50,12 @@ def test_noalloc_eigen_matches_allocating_entry_point_twice():
 
     lib = B.lib()
     rng = np.random.default_rng(11)
-    for n in (181, 7):  # two calls in a row, the second smaller than the first
+    for call, n in enumerate((181, 7)):  # two calls in a row, the second smaller than the first
         H = _spd(rng, n)
         ev_ref, U_ref = B.marg_eigen(H)
-        ev, U = _noalloc(lib, torch, H)
+        ev, U, free0, free1 = _noalloc(lib, torch, H)
+        if call == 1:  # after the set-up call, a call takes no device memory at all
+            assert free1 == free0
         scale = np.max(np.abs(ev_ref))
         assert np.max(np.abs(ev - ev_ref)) <= 1e-12 * scale
         # eigenvectors agree up to the sign of each column
