@@ -62,11 +62,12 @@ def parse():
     p.add_argument("--seed", type=int, default=20260101)
     p.add_argument("--cpu-sample", type=int, default=24, help="windows timed on the host for the CPU baseline")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--plain-windows", type=int, default=16, help="single-window solves timed for the plain path")
+    p.add_argument("--plain-windows", type=int, default=64, help="windows of the batch solved one at a time for the plain path")
     p.add_argument("--marg-steps", type=int, default=3, help="timed batched marginalizations of the solved batch (0: off)")
     p.add_argument("--no-configs", action="store_true", help="skip the single-window configurations c1-c3")
-    p.add_argument("--serve-rate", type=float, default=5000.0, help="offered request rate of the served run (requests/s, 0: off)")
-    p.add_argument("--serve-seconds", type=float, default=3.0, help="duration of the served run's arrivals")
+    p.add_argument("--serve-rates", default="5000,10000,20000,50000",
+                   help="offered request rates of the served sweep (requests/s, comma separated; empty: off)")
+    p.add_argument("--serve-requests", type=int, default=10000, help="requests per served rate (at least 1 s of arrivals)")
     p.add_argument("--serve-pool", type=int, default=512, help="distinct windows the served requests draw from")
     p.add_argument("--calib-steps", type=int, default=2, help="timed calibration-information passes over the solved batch (0: off)")
     p.add_argument("--gate-iterations", type=int, default=10, help="iteration budget of the gated-solve row (0: off)")
@@ -210,82 +211,164 @@ def peaks():
 
 
 def run_served(args, local, backend):
-    """Served mode (the serving configuration): requests from 128 simulated rigs
-    arrive as a Poisson stream at args.serve_rate requests/s; each request is one
-    LM iteration plus oldest-keyframe marginalization of a window drawn as in the
-    batched configuration.  The trace is replayed by the server's native replay
-    (cgmli_server_replay): latency runs from each request's scheduled arrival to
-    its completion, so queueing is included; throughput is completed requests
-    over the span from the first arrival to the last completion."""
-    rng = np.random.default_rng(args.seed + 5)
+    """Served mode (the serving configuration), swept over offered rates: requests
+    from 128 simulated rigs arrive as a Poisson stream at each rate; each request
+    is one LM iteration plus oldest-keyframe marginalization of a window drawn as
+    in the batched configuration.  Each trace is replayed by the server's native
+    replay (cgmli_server_replay): latency runs from each request's scheduled
+    arrival to its completion, so queueing is included; throughput is completed
+    requests over the span from the first arrival to the last completion."""
+    rates = [float(x) for x in args.serve_rates.split(",") if x.strip()]
     pool = synth.make_windows("c4", args.serve_pool, seed=args.seed + 500)
-    n_req = int(args.serve_rate * args.serve_seconds)
-    arrival = np.cumsum(rng.exponential(1.0 / args.serve_rate, n_req))
     rigs = 128
     server = backend.Server(device=local, iterations=1, policy=abi.MARGIN_OLD)
     # warm-up: repeated full-pool bursts, so that both solvers reach their working
     # size (growing pinned staging later would synchronize the device mid-trace)
     for _ in range(4):
         server.replay(pool, [0] * len(pool), np.zeros(len(pool)))
-    windows = [pool[i % len(pool)] for i in range(n_req)]
-    lat, status, span = server.replay(windows, [0] * n_req, arrival)
+    out = []
+    for k, rate in enumerate(rates):
+        rng = np.random.default_rng(args.seed + 5 + k)
+        n_req = max(args.serve_requests, int(rate))
+        arrival = np.cumsum(rng.exponential(1.0 / rate, n_req))
+        windows = [pool[i % len(pool)] for i in range(n_req)]
+        lat, status, span = server.replay(windows, [0] * n_req, arrival)
+        lat_sorted = np.sort(lat)
+        counts = {}
+        for st in status:
+            key = abi.ERRORS.get(int(st), int(st))
+            counts[key] = counts.get(key, 0) + 1
+        out.append({"offered_rate": rate, "throughput": n_req / span, "unit": "requests/s",
+                    "p50_ms": float(lat_sorted[n_req // 2]), "p99_ms": float(lat_sorted[min(n_req - 1, int(0.99 * n_req))]),
+                    "requests": n_req, "arrival_span_s": float(arrival[-1]), "request_status": counts})
+    device_bytes = server.device_bytes()
     server.close()
-    lat_sorted = np.sort(lat)
-    counts = {}
-    for st in status:
-        key = abi.ERRORS.get(int(st), int(st))
-        counts[key] = counts.get(key, 0) + 1
-    return {
-        "offered_rate": args.serve_rate, "throughput": n_req / span, "unit": "requests/s",
-        "p50_ms": float(lat_sorted[n_req // 2]), "p99_ms": float(lat_sorted[min(n_req - 1, int(0.99 * n_req))]),
-        "requests": n_req, "request_status": counts, "rigs": rigs,
-        "workload": "1 LM iteration + oldest-keyframe marginalization per request; windows as the batched configuration",
-    }
+    return {"rates": out, "rigs": rigs, "memory_budget_bytes": 40 << 30, "device_bytes_held": device_bytes,
+            "workload": "1 LM iteration + oldest-keyframe marginalization per request; windows as the batched configuration"}
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-300))
+
+
+def _prior_errors(got, ref):
+    """A is unique up to an orthogonal transform: compare A^T A and A^T r0."""
+    if got.get("status") != 0 or ref.get("status") != 0 or got["rank"] != ref["rank"]:
+        return {"status": [got.get("status"), ref.get("status")], "rank": [got.get("rank"), ref.get("rank")]}
+    Ag, Ar = got["A"], ref["A"]
+    return {"AtA": _rel(Ag.T @ Ag, Ar.T @ Ar), "Atr0": _rel(Ag.T @ got["r0"], Ar.T @ ref["r0"]), "rank": int(got["rank"]),
+            "columns": int(got["cols"]), "bar": 1e-8}
+
+
+def _c2_chain(backend, local, seed):
+    """Configuration 2's window: the sixth of a sliding sequence cut from one 15-keyframe
+    trajectory, its prior chained from five OLD marginalizations of the windows before it,
+    each solved (5 FP64 iterations) and marginalized on the device."""
+    long = synth.c2_long_window(seed)
+    prior = None
+    for i in range(6):
+        w = synth.SubWindow(long, i, 10)
+        if prior is not None:
+            w.set_prior(prior, 1)
+        if i == 5:
+            return w
+        s = backend.Solver(device=local)
+        s.set_windows([w])
+        s.solve(5)
+        s.marginalize([0], abi.MARGIN_OLD)
+        s.synchronize()
+        s.read_states()
+        prior = s.read_prior(0)
+        s.close()
+        w.store()
 
 
 def run_configs(args, local, backend):
-    """The single-window configurations, each alone on the device: c1 (10 KF, 800
-    landmarks, 1 LM iteration + OLD marginalization), c2 (10 KF, 3000 landmarks,
-    IMU + prior + 24+1 calibration, 5 iterations + OLD) and c3 (30 KF, 8 cameras,
-    20 000 landmarks, 10 iterations + SECOND_NEW).  Device time of the solve and of
-    the marginalization (CUDA events, median of the repetitions), and the final
-    states against the FP64 oracle solving the same window on the host."""
+    """The single-window configurations as stated, each alone on the device:
+    c1 (10 KF, 800 landmarks, FP64, 1 LM iteration + OLD marginalization);
+    c2 (10 KF, ~3000 landmarks, IMU, 24+1 calibration, prior chained from five
+    device marginalizations of the preceding windows; mixed precision, 5
+    iterations + OLD); c3 (30 KF, 8 cameras, 20 000 landmarks, mixed precision,
+    10 iterations + SECOND_NEW).  Device time of the solve and of the
+    marginalization (CUDA events, median of the repetitions); the mixed step dx
+    against the FP64 step, the final states against the FP64 oracle, the prior
+    against the oracle's; for c3 the linearization's algorithmic GB/s and the
+    factorization's FP64 rate from per-kernel CUDA events."""
     sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle as O  # checker of the per-configuration states
+    import oracle as O  # checker of the per-configuration results
 
     out = {}
-    for name, policy in (("c1", abi.MARGIN_OLD), ("c2", abi.MARGIN_OLD), ("c3", abi.MARGIN_SECOND_NEW)):
+    for name, policy, precision in (("c1", abi.MARGIN_OLD, abi.PRECISION_FP64), ("c2", abi.MARGIN_OLD, abi.PRECISION_MIXED),
+                                    ("c3", abi.MARGIN_SECOND_NEW, abi.PRECISION_MIXED)):
         it = synth.ITERATIONS[name]
-        w = synth.make_windows(name, 1, seed=args.seed + 11)[0]
+        w = _c2_chain(backend, local, args.seed + 11) if name == "c2" else synth.make_windows(name, 1, seed=args.seed + 11)[0]
         x0 = w.state_vector()
-        s = backend.Solver(device=local)
+        nr, L = w.retained_dim(), w.L
+        row = {"iterations": it, "landmarks": L, "observations": w.window.num_observations, "retained_columns": nr,
+               "precision": "mixed" if precision == abi.PRECISION_MIXED else "fp64",
+               "marginalization": "OLD" if policy == abi.MARGIN_OLD else "SECOND_NEW"}
+        if name == "c2":
+            row["prior"] = f"chained from 5 device marginalizations (rank {w.window.prior_rank})"
+        victim = 0 if policy == abi.MARGIN_OLD else w.K - 2
+        s = backend.Solver(device=local, precision=precision)
         s.set_windows([w])
         s.checkpoint()
+        if precision == abi.PRECISION_MIXED:  # first step at lambda 1e-4: mixed against FP64
+            s.step(1e-4)
+            dm = s.read_step(0)["delta"]
+            f64 = backend.Solver(device=local)
+            f64.set_windows([w])
+            f64.step(1e-4)
+            row["step_dx_rel_err_vs_fp64"] = {"all": _rel(dm, f64.read_step(0)["delta"]),
+                                              "retained": _rel(dm[:nr], f64.read_step(0)["delta"][:nr]), "bar": 1e-6}
+            f64.close()
         solve_ms, marg_ms = [], []
-        victim = 0 if policy == abi.MARGIN_OLD else w.spec.keyframes - 2
         for rep in range(4):
             s.rollback()
             s.solve(it)
             s.synchronize()
             if rep:
                 solve_ms.append(s.timing()[0])
+        if name == "c3":  # per-kernel events of one more solve
+            s.kernel_times(enable=1)
+            s.rollback()
+            s.solve(it)
+            s.synchronize()
+            kt = s.kernel_times(enable=-1)
+            s.kernel_times(enable=0)
+        rep_dev = s.reports()[0]
+        for rep in range(4):
             s.marginalize([victim], policy)
-            s.read_prior(0)
+            s.synchronize()
             if rep:
                 marg_ms.append(s.timing()[0])
+        prior = s.read_prior(0)
         s.read_states()
         xg = w.state_vector()
         s.close()
+        ref_prior = O.marginalize_window(w.window, victim, policy)  # at the device's solved states
         w.set_state_vector(x0)
         O.lm_solve(w.window, it)
         xc = w.state_vector()
+        w.set_state_vector(x0)
         solve_ms.sort()
         marg_ms.sort()
-        out[name] = {"iterations": it, "landmarks": w.window.num_landmarks, "observations": w.window.num_observations,
-                     "solve_ms_p50": solve_ms[len(solve_ms) // 2], "solves_per_s": 1000.0 / solve_ms[len(solve_ms) // 2],
-                     "marginalization_ms_p50": marg_ms[len(marg_ms) // 2],
-                     "marginalization": "OLD" if policy == abi.MARGIN_OLD else "SECOND_NEW",
-                     "final_state_rel_err_vs_fp64_oracle": float(np.linalg.norm(xg - xc) / max(np.linalg.norm(xc - x0), 1e-300))}
+        row.update({"solve_ms_p50": solve_ms[len(solve_ms) // 2], "solves_per_s": 1000.0 / solve_ms[len(solve_ms) // 2],
+                    "marginalization_ms_p50": marg_ms[len(marg_ms) // 2], "accepted_steps": rep_dev.accepted_steps,
+                    "final_state_rel_err_vs_fp64_oracle": float(np.linalg.norm(xg - xc) / max(np.linalg.norm(xc - x0), 1e-300)),
+                    "prior_rel_err_vs_fp64_oracle": _prior_errors(prior, ref_prior)})
+        if name == "c3":
+            lin_ms = sum(kt[k][0] for k in ("linearize", "lin_pairs", "lin_schur"))
+            lins = kt["linearize"][1]
+            fac_ms, facs = kt["factor"]
+            flops = nr ** 3 / 3.0 + 2.0 * nr * nr  # Cholesky + the two triangular solves
+            row["linearization"] = {"ms_per_launch": lin_ms / max(1, lins),
+                                    "algorithmic_GBps": algorithmic_linearize_bytes(w) * lins / (lin_ms / 1e3) / 1e9,
+                                    "hbm_peak_GBps": peaks()[0], "launches": lins}
+            row["factorization"] = {"ms_per_launch": fac_ms / max(1, facs), "fp64_GFLOPs": flops * facs / (fac_ms / 1e3) / 1e9,
+                                    "fp64_nominal_peak_GFLOPs": 37000.0, "launches": facs,
+                                    "flops_per_launch": flops}
+        out[name] = row
     return out
 
 
@@ -670,13 +753,15 @@ def main():
                        "with the other's solve",
            "request_status": pipe_status, "sequential": sequential}
 
-    # plain single-window path: the configuration-2 window solved alone, one at a time
+    # plain single-window path on equal work: windows of this batch (drawn as the
+    # batched configuration), solved one at a time with the same iterations
     plain = None
     if rank == 0 and args.plain_windows > 0:
-        pw = synth.make_windows("c2", args.plain_windows, seed=args.seed + 7)
+        pw = windows[:args.plain_windows]
         ps = backend.Solver(device=local)
         lat = []
         for i, w in enumerate(pw):
+            w.set_state_vector(init[i])
             ps.set_windows([w])
             ps.checkpoint()
             for rep in range(2):
@@ -685,12 +770,14 @@ def main():
                 ps.synchronize()
                 if rep == 1:
                     lat.append(ps.timing()[0])
+            w.set_state_vector(init[i])
+        ps.close()
         lat.sort()
         plain = {"windows_per_s": 1000.0 / statistics.mean(lat), "p50_ms": lat[len(lat) // 2],
                  "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))], "windows": len(lat),
-                 "workload": "one configuration-2 window (10 KF, 3000 lm, 24+1 calib, prior) per solve"}
+                 "workload": f"the first {len(lat)} windows of the batch, each solved alone ({args.iterations} LM iterations)"}
 
-    served = run_served(args, local, backend) if rank == 0 and args.serve_rate > 0 else None
+    served = run_served(args, local, backend) if rank == 0 and args.serve_rates.strip() else None
     configs = run_configs(args, local, backend) if rank == 0 and not args.no_configs else None
     imu = run_imu(args, local, backend) if rank == 0 and args.imu_rigs > 0 else None
     gated = run_gated(args, local, backend, windows, init) if rank == 0 and args.gate_iterations > 0 else None

@@ -961,21 +961,8 @@ int cgmli_solver_read_reduced(cgmli_solver* S, int w, double* Sout, double* rhs)
     CK(cudaSetDevice(S->device));
     const WinDesc& d = S->win[w];
     if (Sout) CK(cudaMemcpy(Sout, S->Sdebug.p + d.dense0, (size_t)d.Nr * d.Nr * sizeof(double), cudaMemcpyDeviceToHost));
-    if (rhs) {
-        // rhs is recomputed from the accumulators (it equals -(g_r - B_v))
-        std::vector<double> g(d.Nr), accv((size_t)d.Npc * (d.Npc + 1) / 2 + 3 * d.Npc);
-        CK(cudaMemcpy(g.data(), S->gret.p + d.vec0, d.Nr * sizeof(double), cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(accv.data(), S->acc.p + d.acc0, accv.size() * sizeof(double), cudaMemcpyDeviceToHost));
-        const size_t nS = (size_t)d.Npc * (d.Npc + 1) / 2;
-        for (int i = 0; i < d.Nr; ++i) {
-            double v = g[i];
-            int p = -1;
-            if (i >= 15 * d.K) p = 6 * d.K + (i - 15 * d.K);
-            else if (i % 15 < 6) p = 6 * (i / 15) + i % 15;
-            if (p >= 0) v += accv[nS + d.Npc + p] - accv[nS + 2 * d.Npc + p];
-            rhs[i] = -v;
-        }
-    }
+    // the right-hand side the factorization solved: -(g_r - B_v), restricted by the solve-time charts
+    if (rhs) CK(cudaMemcpy(rhs, S->rhs.p + d.vec0, d.Nr * sizeof(double), cudaMemcpyDeviceToHost));
     return CGMLI_OK;
 }
 

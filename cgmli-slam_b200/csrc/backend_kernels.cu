@@ -973,11 +973,6 @@ __global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int re
             A[i + (long long)j * n] = v;
             A[j + (long long)i * n] = v;
         }
-        if (Sdebug) {
-            const double dv = i == j ? v + da[i] : v;
-            Sdebug[wd.dense0 + (long long)i * n + j] = dv;
-            Sdebug[wd.dense0 + (long long)j * n + i] = dv;
-        }
     }
     double* rhsOut = B.rhs + wd.vec0;
     for (int i = tid; i < n; i += blockDim.x) {
@@ -994,6 +989,11 @@ __global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int re
         for (int i = tid; i < n; i += blockDim.x) rhsOut[i] = x[i];  // the restricted right-hand side
         __syncthreads();
     }
+    if (Sdebug)  // the damped system as it is factored (lower triangle), stored symmetric and row-major
+        for (long long t = tid; t < (long long)n * n; t += blockDim.x) {
+            const int r = (int)(t / n), c = (int)(t % n);
+            Sdebug[wd.dense0 + t] = r >= c ? A[r + (long long)c * n] : A[c + (long long)r * n];
+        }
     // ---- factorization with the forward substitution
     for (int k0 = 0; k0 < n; k0 += kFacPanel) {
         // rows padded so that the trailing rows [bw, mp) are whole 32-row tiles

@@ -255,3 +255,146 @@ def imu_stream(rigs: int, keyframes: int, seed: int, rate: float = 200.0, spacin
         offset += per_rig
     return ImuStream(np.concatenate(times), np.vstack(reads), np.array(ranges, dtype=np.int32), np.array(t0s, dtype=np.int64),
                      np.array(t1s, dtype=np.int64), np.array(biases))
+
+
+# ---- sliding-window sequences (configuration 2's chained prior) -----------------
+class SubWindow:
+    """Keyframes [start, start + K) of a long generated window, as a sliding
+    window holds them after `start` OLD marginalizations: landmarks with an
+    observation (or anchor) on an earlier keyframe were eliminated with it
+    (the OLD elimination set, SlidingWindowManager.cpp:627-652); a landmark's
+    observations beyond the window's last keyframe are not made yet.  States
+    are copied from the long window (its current estimates); the prior is set
+    by set_prior from the previous window's marginalization."""
+
+    def __init__(self, long: "SynthWindow", start: int, K: int):
+        src = long.window
+        Kt = src.num_keyframes
+        assert 0 <= start and start + K <= Kt
+        self.long, self.start, self.K = long, start, K
+        E, Cn = src.num_extrinsics, src.num_cameras
+        Lt = src.num_landmarks
+        begin = np.ctypeslib.as_array(src.lm_obs_begin, shape=(Lt + 1,))
+        Ft = int(begin[-1])
+        lm_kf = np.ctypeslib.as_array(src.lm_anchor_kf, shape=(Lt,))
+        obs_kf = np.ctypeslib.as_array(src.obs_kf, shape=(Ft,))
+        lms, obs, new_begin = [], [], [0]
+        for l in range(Lt):
+            a = int(lm_kf[l])
+            ks = obs_kf[begin[l]:begin[l + 1]]
+            if a < start or a >= start + K or np.any(ks < start):
+                continue
+            keep = [f for f in range(begin[l], begin[l + 1]) if obs_kf[f] < start + K]
+            if not keep:
+                continue
+            lms.append(l)
+            obs.extend(keep)
+            new_begin.append(len(obs))
+        self.lms = np.array(lms, dtype=np.int64)
+        self.obs = np.array(obs, dtype=np.int64)
+
+        def arr(ptr, n, dtype=np.float64):
+            return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dtype).copy() if ptr else None
+
+        L, F = len(lms), len(obs)
+        kf = slice(start, start + K)
+        a = {}
+        a["poses"] = long.poses().reshape(Kt, 7)[kf].ravel().copy()
+        a["sb"] = long.speed_bias().reshape(Kt, 9)[kf].ravel().copy()
+        a["ext"] = long.extrinsics().copy()
+        a["td"] = long.td().copy()
+        a["rho"] = long.rho()[self.lms].copy()
+        a["cam_R"], a["cam_t"] = arr(src.cam_R, 9 * Cn), arr(src.cam_t, 3 * Cn)
+        a["cam_ext"] = arr(src.cam_ext, Cn, np.int32)
+        a["lm_kf"] = (lm_kf[self.lms] - start).astype(np.int32)
+        a["lm_cam"] = np.ctypeslib.as_array(src.lm_anchor_cam, shape=(Lt,))[self.lms].astype(np.int32).copy()
+        a["lm_begin"] = np.array(new_begin, dtype=np.int32)
+        a["lm_bearing"] = np.ctypeslib.as_array(src.lm_anchor_bearing, shape=(Lt, 3))[self.lms].ravel().copy()
+        a["obs_kf"] = (obs_kf[self.obs] - start).astype(np.int32)
+        a["obs_cam"] = np.ctypeslib.as_array(src.obs_cam, shape=(Ft,))[self.obs].astype(np.int32).copy()
+        a["obs_bearing"] = np.ctypeslib.as_array(src.obs_bearing, shape=(Ft, 3))[self.obs].ravel().copy()
+        a["obs_P"] = np.ctypeslib.as_array(src.obs_P, shape=(Ft, 6))[self.obs].ravel().copy()
+        if src.lm_anchor_velocity:
+            a["lm_vel"] = np.ctypeslib.as_array(src.lm_anchor_velocity, shape=(Lt, 3))[self.lms].ravel().copy()
+        if src.obs_velocity:
+            a["obs_vel"] = np.ctypeslib.as_array(src.obs_velocity, shape=(Ft, 3))[self.obs].ravel().copy()
+        imu_kf = np.ctypeslib.as_array(src.imu_kf, shape=(src.num_imu,)) if src.num_imu else np.zeros(0, np.int32)
+        sel = [i for i in range(src.num_imu) if start <= imu_kf[i] and imu_kf[i] + 1 < start + K]
+        self.imu = (abi.FrozenImu * max(len(sel), 1))()
+        for j, i in enumerate(sel):
+            self.imu[j] = src.imu[i]
+        a["imu_kf"] = (imu_kf[sel] - start).astype(np.int32) if sel else np.zeros(1, np.int32)
+        self.arrays = a
+        w = abi.Window()
+        w.num_keyframes, w.num_cameras, w.num_extrinsics = K, Cn, E
+        w.estimate_extrinsics, w.estimate_td = src.estimate_extrinsics, src.estimate_td
+        w.num_landmarks, w.num_observations, w.num_imu = L, F, len(sel)
+        w.huber_scale, w.min_inverse_distance = src.huber_scale, src.min_inverse_distance
+        dp, ip = abi.c_double_p, abi.c_int_p
+        for name, key in (("poses", "poses"), ("speed_bias", "sb"), ("extrinsics", "ext"), ("td", "td"), ("rho", "rho"),
+                          ("cam_R", "cam_R"), ("cam_t", "cam_t"), ("lm_anchor_bearing", "lm_bearing"),
+                          ("obs_bearing", "obs_bearing"), ("obs_P", "obs_P")):
+            setattr(w, name, a[key].ctypes.data_as(dp))
+        for name, key in (("lm_anchor_velocity", "lm_vel"), ("obs_velocity", "obs_vel")):
+            if key in a:
+                setattr(w, name, a[key].ctypes.data_as(dp))
+        for name, key in (("cam_ext", "cam_ext"), ("lm_anchor_kf", "lm_kf"), ("lm_anchor_cam", "lm_cam"),
+                          ("lm_obs_begin", "lm_begin"), ("obs_kf", "obs_kf"), ("obs_cam", "obs_cam"), ("imu_kf", "imu_kf")):
+            setattr(w, name, a[key].ctypes.data_as(ip))
+        if sel:
+            w.imu = self.imu
+        self.window = w
+
+    @property
+    def L(self):
+        return self.window.num_landmarks
+
+    def retained_dim(self) -> int:
+        w = self.window
+        return 15 * w.num_keyframes + (6 * w.num_extrinsics if w.estimate_extrinsics else 0) + (1 if (w.estimate_td and w.td) else 0)
+
+    def set_prior(self, prior: dict, shift: int) -> None:
+        """The square-root prior of the previous window's marginalization (read_prior), its
+        keyframe blocks moved down by `shift` (the keyframes that left the window)."""
+        kinds = np.ascontiguousarray(prior["kinds"], dtype=np.int32)
+        idx = np.array([i - shift if k in (abi.PRIOR_POSE, abi.PRIOR_SPEED_BIAS) else i for k, i in zip(kinds, prior["index"])],
+                       dtype=np.int32)
+        assert np.all(idx >= 0)
+        amb = int(sum(9 if k == abi.PRIOR_SPEED_BIAS else 1 if k == abi.PRIOR_TIME_OFFSET else 7 for k in kinds))
+        self.prior = dict(kinds=kinds, index=idx, ref=np.ascontiguousarray(prior["reference"][:amb]),
+                          A=np.ascontiguousarray(prior["A"]).ravel().copy(), r0=np.ascontiguousarray(prior["r0"]).copy())
+        w, p = self.window, self.prior
+        w.prior_rank, w.prior_num_blocks = int(prior["rank"]), len(kinds)
+        w.prior_block_kind, w.prior_block_index = p["kinds"].ctypes.data_as(abi.c_int_p), p["index"].ctypes.data_as(abi.c_int_p)
+        w.prior_ref, w.prior_A, w.prior_r0 = (p[k].ctypes.data_as(abi.c_double_p) for k in ("ref", "A", "r0"))
+
+    def store(self) -> None:
+        """Writes this window's states back into the long window (the next window starts from them)."""
+        Kt = self.long.window.num_keyframes
+        kf = slice(self.start, self.start + self.K)
+        self.long.poses().reshape(Kt, 7)[kf] = self.arrays["poses"].reshape(self.K, 7)
+        self.long.speed_bias().reshape(Kt, 9)[kf] = self.arrays["sb"].reshape(self.K, 9)
+        self.long.extrinsics()[:] = self.arrays["ext"]
+        self.long.td()[:] = self.arrays["td"]
+        self.long.rho()[self.lms] = self.arrays["rho"]
+
+    def state_vector(self) -> np.ndarray:
+        a = self.arrays
+        return np.concatenate([a["poses"], a["sb"], a["ext"], a["td"], a["rho"]]).copy()
+
+    def set_state_vector(self, x: np.ndarray) -> None:
+        off = 0
+        for k in ("poses", "sb", "ext", "td", "rho"):
+            n = self.arrays[k].size
+            self.arrays[k][:] = x[off:off + n]
+            off += n
+
+
+# Configuration 2 as a sequence: 15 keyframes generated at once, sliding windows of 10; the
+# fifth window's prior comes from five chained OLD marginalizations of the ones before it.
+C2_CHAIN_KEYFRAMES = 15
+C2_CHAIN_LANDMARKS = 6000
+
+
+def c2_long_window(seed: int, landmarks: int = C2_CHAIN_LANDMARKS) -> "SynthWindow":
+    return SynthWindow(replace(C2, keyframes=C2_CHAIN_KEYFRAMES, landmarks=landmarks, with_prior=False), seed)

@@ -230,8 +230,11 @@ int cgmli_solver_read_reports(cgmli_solver *solver, cgmli_solve_report *reports,
 int cgmli_solver_step(cgmli_solver *solver, double lambda);
 int cgmli_solver_read_step(cgmli_solver *solver, int window, double *increment, double *cost,
                            double *predicted, double *trial_cost, int *trial_valid);
-/* Reduced system of the last linearization/step of window w:
- * S (N_r x N_r row-major, damped at that lambda) and its right-hand side. */
+/* Reduced system of the last cgmli_solver_step of window w: S (N_r x N_r
+ * row-major, damped at that lambda) and its right-hand side, as factored: with
+ * solve-time charts, restricted to the free directions (a rotation-only
+ * extrinsic's theta columns hold M^T S M, M = [[p]x; I]) with identity rows and
+ * zero right-hand side at the fixed and folded columns. */
 int cgmli_solver_read_reduced(cgmli_solver *solver, int window, double *S, double *rhs);
 /* Sizes: N_r of window w. */
 int cgmli_solver_window_dims(cgmli_solver *solver, int window, int *retained, int *landmarks);

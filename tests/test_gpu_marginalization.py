@@ -178,3 +178,21 @@ def test_dense_subtract(backend):
     Ho, go = backend.marg_subtract(C, Sx, H, g)
     full = np.hstack([H, g[:, None]]) - C.T @ Sx
     assert rel(Ho, full[:, :nr]) < 1e-14 and rel(go, full[:, nr]) < 1e-14
+
+
+def test_diagonal_psd_known_answer_on_device():
+    """untouchedPriorAndDiagonalKernel (ManagedWindowRegression.cpp:310-329) through
+    cgmli_marg_psd_solve: H = diag(2, 0, 1e-14, 5), rhs = ones(4, 2) gives rows 0.5, 0, 0, 0.2
+    within 1e-12; a negative diagonal information must fail."""
+    from cgmli_slam_b200 import backend as B
+
+    H = np.diag([2.0, 0.0, 1e-14, 5.0])
+    x = B.marg_psd_solve(H, np.ones((4, 2)))
+    expected = np.zeros((4, 2))
+    expected[0] = 0.5
+    expected[3] = 0.2
+    assert np.linalg.norm(x - expected) < 1e-12
+    H[2, 2] = -1.0
+    with pytest.raises(B.BackendError) as e:
+        B.marg_psd_solve(H, np.ones((4, 2)))
+    assert e.value.code == 6  # CGMLI_E_INDEFINITE

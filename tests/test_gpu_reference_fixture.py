@@ -143,3 +143,38 @@ def _evaluate_synth(ws):
     out = [s.read_factors(i) for i in range(len(ws))]
     s.close()
     return out
+
+
+def _audit_rel(a, b):
+    """relative() of VisualBatchAudit.cpp:23-25: |a - b| / max(1, |a|)."""
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(1.0, np.linalg.norm(a)))
+
+
+@pytest.mark.parametrize("name", ["c1", "c2"])
+def test_reference_audit_bars(oracle, name):
+    """The reference's runtime audit (VisualBatchAudit.cpp:24-113), device against the oracle on the
+    configuration-1 and -2 windows: stacked residuals and Jacobians within 1e-8, cost within
+    1e-8 max(1, |cost|), and the step of the reduced system damped by 1e-3 max(H_ii, 1e-6) (landmarks
+    included) within 1e-6."""
+    from cgmli_slam_b200 import backend
+
+    w = synth.make_windows(name, 1, seed=88)[0]
+    nr, L = w.retained_dim(), w.L
+    s = backend.Solver(device=0)
+    s.set_windows([w])
+    s.evaluate(True)
+    f = s.read_factors(0)
+    s.step(1e-3)
+    step = s.read_step(0)
+    s.close()
+    win = w.window
+    begin = np.ctypeslib.as_array(win.lm_obs_begin, shape=(L + 1,))
+    r_ref, J_ref = np.zeros((w.F, 2)), np.zeros((w.F, 2, 26))
+    for l in range(L):
+        for k in range(begin[l], begin[l + 1]):
+            ok, r_ref[k], J_ref[k], _ = oracle.visual_factor(win, l, k, True)
+    assert _audit_rel(r_ref.ravel(), f["residuals"].ravel()) < 1e-8
+    assert _audit_rel(J_ref.ravel(), f["jacobians"].ravel()) < 1e-8
+    ref = oracle.step(win, nr, L, 1e-3)
+    assert abs(step["cost"] - ref["cost"]) < 1e-8 * max(1.0, abs(ref["cost"]))
+    assert _audit_rel(ref["delta"], step["delta"]) < 1e-6
