@@ -729,7 +729,7 @@ def main():
     d2h = sum(window_bytes(w)[1] for w in windows)
     e2e_times = []
     e2e_solver = backend.Solver(device=local)
-    e2e_solver.set_tuning(tuning["run_landmarks"], tuning["pair_chunk"], tuning["schur_rows"])
+    e2e_solver.set_tuning(**{k: v for k, v in tuning.items() if k != "ms"})
     for it in range(1 + max(1, args.steps // 2)):
         for w, x in zip(windows, init):
             w.set_state_vector(x)

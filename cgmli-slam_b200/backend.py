@@ -158,15 +158,17 @@ class Solver:
         _check(lib().cgmli_solver_window_dims(self._h, w, C.byref(nr), C.byref(nl)), "cgmli_solver_window_dims")
         return nr.value, nl.value
 
-    def set_tuning(self, run_landmarks: int = 0, pair_chunk: int = 0, schur_rows: int = 0) -> None:
-        """Work decomposition of the next set_windows (0: the default of each)."""
-        t = abi.Tuning(run_landmarks, pair_chunk, schur_rows, 0.0)
+    def set_tuning(self, run_landmarks: int = 0, pair_chunk: int = 0, schur_rows: int = 0, lin_shape: int = 0,
+                   trial_shape: int = 0) -> None:
+        """Work decomposition and kernel shapes of the next set_windows (0: the default of each)."""
+        t = abi.Tuning(run_landmarks, pair_chunk, schur_rows, lin_shape, trial_shape, 0.0)
         _check(lib().cgmli_solver_set_tuning(self._h, C.byref(t)), "cgmli_solver_set_tuning")
 
     def get_tuning(self) -> dict:
         t = abi.Tuning()
         _check(lib().cgmli_solver_get_tuning(self._h, C.byref(t)), "cgmli_solver_get_tuning")
-        return dict(run_landmarks=t.run_landmarks, pair_chunk=t.pair_chunk, schur_rows=t.schur_rows)
+        return dict(run_landmarks=t.run_landmarks, pair_chunk=t.pair_chunk, schur_rows=t.schur_rows, lin_shape=t.lin_shape,
+                    trial_shape=t.trial_shape)
 
     def autotune(self, windows, iterations: int) -> dict:
         """Times candidate work decompositions on these windows, keeps the fastest
@@ -176,7 +178,8 @@ class Solver:
         _check(lib().cgmli_solver_autotune(self._h, arr, len(arr), iterations, C.byref(t)), "cgmli_solver_autotune")
         self._windows = arr
         self.count = len(arr)
-        return dict(run_landmarks=t.run_landmarks, pair_chunk=t.pair_chunk, schur_rows=t.schur_rows, ms=t.ms)
+        return dict(run_landmarks=t.run_landmarks, pair_chunk=t.pair_chunk, schur_rows=t.schur_rows, lin_shape=t.lin_shape,
+                    trial_shape=t.trial_shape, ms=t.ms)
 
     def device_bytes(self) -> int:
         n = C.c_longlong()

@@ -43,7 +43,7 @@ size_t margVisualSmemBytes(int maxNc);
 size_t margRowsSmemBytes(int maxNv);
 int margRowsCap(int nv);
 cudaError_t configureMarginalization(size_t visualSmem, size_t rowsSmem, int maxNr, int maxFastNr, long long* eigenSmem,
-                                     long long* fastSmem);
+                                     long long* fastSmem, long long* triSmem);
 int launchMarginalization(const DevBatch& B, const MargBatch& M, size_t visualSmem, cudaStream_t s);
 int launchCalibration(const DevBatch& B, const MargBatch& M, size_t visualSmem, double* work, const long long* work0, double* cond,
                       double* evals, int maxNuisance, cudaStream_t s);
@@ -266,7 +266,8 @@ struct cgmli_solver {
         P.runs = dRuns.p; P.tiles = dTiles.p; P.numTiles = (int)hb.tiles.size();
         P.pairChunks = dPairChunks.p; P.numPairChunks = (int)hb.pairChunks.size();
         P.schurChunks = dSchurChunks.p; P.numSchurChunks = (int)hb.schurChunks.size();
-        P.linSmem = linSmem; P.facSmem = facSmem; P.maxNs = maxNs;
+        P.facSmem = facSmem; P.maxNs = maxNs;
+        P.linShape = hb.plan.linShape; P.trialShape = hb.plan.trialShape;
         return P;
     }
     void collectKernelTimes() {
@@ -336,6 +337,10 @@ static int planOf(const cgmli_tuning* t, PlanParams& p) {
     if (t->pair_chunk != 0 && (t->pair_chunk < 8 || t->pair_chunk > 1024)) return fail(CGMLI_E_INVALID, "tuning: pair_chunk outside 8..1024");
     if (t->schur_rows != 0 && (t->schur_rows < 8 || t->schur_rows > kSchurMaxRows))
         return fail(CGMLI_E_INVALID, "tuning: schur_rows outside 8..128");
+    if (t->lin_shape < 0 || t->lin_shape >= kLinShapes) return fail(CGMLI_E_INVALID, "tuning: lin_shape outside 0..3");
+    if (t->trial_shape < 0 || t->trial_shape >= kTrialShapes) return fail(CGMLI_E_INVALID, "tuning: trial_shape outside 0..2");
+    p.linShape = t->lin_shape;
+    p.trialShape = t->trial_shape;
     p.runLandmarks = t->run_landmarks;
     if (t->pair_chunk) p.pairChunk = t->pair_chunk;
     if (t->schur_rows) p.schurRows = t->schur_rows;
@@ -651,13 +656,17 @@ int cgmli_solver_get_tuning(cgmli_solver* S, cgmli_tuning* tuning) {
     tuning->run_landmarks = S->tune.runLandmarks;
     tuning->pair_chunk = S->tune.pairChunk;
     tuning->schur_rows = S->tune.schurRows;
+    tuning->lin_shape = S->tune.linShape;
+    tuning->trial_shape = S->tune.trialShape;
     tuning->ms = 0.0;
     return CGMLI_OK;
 }
 
 // Coordinate search: each parameter mainly shapes one pass (runs: the landmark
 // and trial passes; pair chunks: the J^T J pass; Schur rows: the Schur pass), so
-// they are tuned one after the other, each over a few multiples of the current value.
+// they are tuned one after the other, each over a few multiples of the current
+// value; then the kernel shapes of the landmark and trial passes, each over all
+// of its compiled variants.
 int cgmli_solver_autotune(cgmli_solver* S, const cgmli_window* windows, int count, int iterations, cgmli_tuning* best) {
     if (!S || !windows || count < 1) return fail(CGMLI_E_INVALID, "autotune: null solver or empty window list");
     if (iterations < 1) return fail(CGMLI_E_INVALID, "autotune: iterations < 1");
@@ -700,6 +709,24 @@ int cgmli_solver_autotune(cgmli_solver* S, const cgmli_window* windows, int coun
             if (ms < bestMs) { bestMs = ms; cur = p; }
         }
     }
+    for (int shape = 0; shape < kLinShapes && st == CGMLI_OK; ++shape) {
+        if (shape == cur.linShape) continue;
+        PlanParams p = cur;
+        p.linShape = shape;
+        double ms = 0;
+        if ((st = measure(p, ms)) != CGMLI_OK) break;
+        if (ms < bestMs) { bestMs = ms; cur = p; }
+    }
+    const int linBest = cur.linShape;
+    for (int shape = 0; shape < kTrialShapes && st == CGMLI_OK; ++shape) {
+        if (shape == cur.trialShape) continue;
+        PlanParams p = cur;
+        p.trialShape = shape;
+        p.linShape = linBest;
+        double ms = 0;
+        if ((st = measure(p, ms)) != CGMLI_OK) break;
+        if (ms < bestMs) { bestMs = ms; cur = p; }
+    }
     S->profile = profiled;
     S->tune = cur;
     if (st != CGMLI_OK) return st;
@@ -708,6 +735,8 @@ int cgmli_solver_autotune(cgmli_solver* S, const cgmli_window* windows, int coun
         best->run_landmarks = cur.runLandmarks;
         best->pair_chunk = cur.pairChunk;
         best->schur_rows = cur.schurRows;
+        best->lin_shape = cur.linShape;
+        best->trial_shape = cur.trialShape;
         best->ms = bestMs;
     }
     return CGMLI_OK;
@@ -1544,8 +1573,8 @@ static int marginalizeImpl(cgmli_solver* S, const int* victim_kf, int policy, bo
         maxNr = std::max(maxNr, mw.nr);
         maxFastNr = std::max(maxFastNr, mw.nr);
     }
-    long long eigenSmem = 0, fastSmem = 0;
-    CK(configureMarginalization(smem, rowsSmem, maxNr, maxFastNr, &eigenSmem, &fastSmem));
+    long long eigenSmem = 0, fastSmem = 0, triSmem = 0;
+    CK(configureMarginalization(smem, rowsSmem, maxNr, maxFastNr, &eigenSmem, &fastSmem, &triSmem));
     S->hMargWin.assign(mwv.begin(), mwv.end());  // guarded by margUploaded like the other staging
     CK(S->dMargWin.upload(S->hMargWin, st));
     {
@@ -1587,6 +1616,7 @@ static int marginalizeImpl(cgmli_solver* S, const int* victim_kf, int policy, bo
     M.numElim = (int)elims.size();
     M.eigenSmem = eigenSmem;
     M.fastSmem = fastSmem;
+    M.triSmem = triSmem;
     M.win = S->dMargWin.p; M.bigFirst = S->dMargOrder.p; M.elim = S->dMargElim.p; M.cols = S->margCols.p; M.obsMap = S->margObsMap.p;
     M.poseCol = S->margPoseCol.p; M.sbCol = S->margSbCol.p; M.extCol = S->margExtCol.p;
     M.H = S->margH.p; M.b = S->margB.p; M.sepH = S->margSepH.p; M.sepV = S->margSepV.p; M.sepB = S->margSepB.p;

@@ -154,6 +154,7 @@ struct MargBatch {
     int numWindows, numElim;
     long long eigenSmem;  // dynamic shared memory of the eigen CTA (packed separator, eigenvectors when they fit)
     long long fastSmem;   // dynamic shared memory of the full-rank fast path
+    long long triSmem;    // dynamic shared memory of the tridiagonal eigen path
     const MargWin* win;
     const int* bigFirst;  // windows by decreasing width of their larger block: block order of the
                           // one-CTA-per-window kernels
@@ -166,7 +167,7 @@ struct MargBatch {
     double* maxD;        // per window: largest eliminated landmark information
     double* stats;       // 4 per window: robust cost, whitened |r|^2, eliminated reduction, cutoff
     int* rank; int* status;
-    int* fast;           // per window: 1 when the full-rank fast path formed the prior
+    int* fast;           // per window: 1 when the fast path formed the prior, 3 the tridiagonal eigen path, 0 neither
     // dense-row path
     double* rows;        // kMargRecord per eliminated observation (staged factor rows)
     const int* visCol;   // visual column -> marginalization column, per window from MargWin::vis0
@@ -191,6 +192,17 @@ typedef void (*LaunchHook)(void* ctx, int kind, int phase);
 // rejected by the gate before the first solve; one spare.
 constexpr int kGateCounts = 6;
 
+// Kernel shapes the autotuner chooses between: warps per CTA and the CTAs per SM
+// the register budget is compiled for (launch bounds), for the landmark pass
+// (k_lin_landmark) and the trial pass (k_trial).  More CTAs per SM cap the
+// registers lower (168 at 12 warps per SM, where the FP64 factor chain spills);
+// one CTA per SM lets a thread keep its chain in up to 255 registers.
+struct KernelShape { int warps, minBlocks; };
+constexpr int kLinShapes = 4;
+constexpr KernelShape kLinShapeTable[kLinShapes] = {{6, 2}, {8, 1}, {4, 3}, {6, 1}};
+constexpr int kTrialShapes = 3;
+constexpr KernelShape kTrialShapeTable[kTrialShapes] = {{8, 2}, {8, 1}, {4, 4}};
+
 // Work decomposition of one batch (device pointers and counts).
 struct LaunchPlan {
     const int4* runs;        // {window, first tile, end tile, -}: one warp each (landmark order)
@@ -201,7 +213,8 @@ struct LaunchPlan {
     const int4* schurChunks; // {window, first landmark, end landmark, -}: one CTA each
     int numSchurChunks;
     int maxNs;               // widest landmark support of the batch (local columns)
-    size_t linSmem, facSmem;
+    size_t facSmem;
+    int linShape, trialShape;  // kLinShapeTable / kTrialShapeTable entries
 };
 
 }  // namespace cgmli

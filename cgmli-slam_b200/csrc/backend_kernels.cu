@@ -8,6 +8,7 @@
 // runs without a host round trip and can be captured in a CUDA graph.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "../../include/cgmli_backend.h"
@@ -91,10 +92,8 @@ __global__ void k_zero_acc(DevBatch B) {
 //                   expanded into dense shared-memory rows and the Schur term is
 //                   a register-tiled FP64 SYRK (plus the B_v column)
 // Only k_lin_schur depends on lambda, so a rejected step re-runs it alone.
-constexpr int kLinWarps = 6;        // warps per CTA of the run-based kernels
 constexpr int kCompact = 25;        // anchor pose 6 | observer pose 6 | ext_a 6 | ext_b 6 | td 1
 constexpr int kPairs = kCompact * (kCompact + 1) / 2;
-constexpr int kPairSlots = (kPairs + 31) / 32;  // compact pairs per lane
 constexpr int kPairWarps = 4;       // warps per CTA of k_lin_pairs
 // A factor's FactorOut is staged per lane in shared memory with an odd stride
 // (conflict-free lane rows); slot 54 carries the squared robust weight.
@@ -118,19 +117,19 @@ __device__ __forceinline__ int pcOfLocal(int i, int s, int x, const int* sk, int
 // column maps, flags, and the landmark's cross vector (maxNs doubles, the batch's
 // widest support).
 //
-// Mixed precision (Mixed = true): the Jacobians and the robust weight are FP32 and
-// the landmark Hessian blocks d_l and the runs of c_l are summed in FP32 with
-// compensation (error-free two-sum terms carried beside each sum, added in FP64 at
-// the end).  The residual, the cost and every gradient term (g_l here, J^T r in the
-// pairs pass: FP32 Jacobian entries times the FP64 residual) stay FP64.  A factor is
-// staged as kOutF floats (the FactorOut blocks without the residual, then the weight).
-constexpr int kOutF = 53;
-__device__ __forceinline__ int compactOffF(int r, int c) { return c < 24 ? 12 * (c / 6) + 6 * r + c % 6 : 48 + r; }
-__host__ __device__ constexpr size_t landmarkWarpBytes(int maxNs, bool mixed) {
-    return (mixed ? sizeof(float) * 32 * kOutF : sizeof(double) * 32 * kOut) + sizeof(double) * maxNs + sizeof(long long) * 32 +
-           sizeof(short) * 32 * kCompact + sizeof(int) * 32;
+// Mixed precision (Mixed = true): the factor is formed in FP64 as on the FP64 path,
+// then its Jacobian blocks over the pose, extrinsic and td columns and its robust
+// weight are rounded once to FP32.  Those FP32 values are what the linearization
+// uses: the staged rows of the J^T J pass are stored in FP32 (half the bytes) and
+// the landmark terms d_l, g_l and the cross products w^2 J_x^T J_rho are formed in
+// FP64 from them, with the residual and the depth derivative J_rho kept FP64.  (An
+// FP32 derivative chain, measured, saved 5% of this pass and put the configuration-2
+// retained step 1.9e-6 away from FP64: its cancellations, not the storage rounding,
+// set the error.)
+__host__ __device__ constexpr size_t landmarkWarpBytes(int maxNs, bool) {
+    return sizeof(double) * 32 * kOut + sizeof(double) * maxNs + sizeof(long long) * 32 + sizeof(short) * 32 * kCompact +
+           sizeof(int) * 32;
 }
-static_assert(sizeof(float) * 32 * kOutF % 16 == 0, "double-aligned cross vector after the FP32 staging");
 // Staged row of one factor, written by k_lin_landmark (in observation order)
 // and gathered in key order by k_lin_pairs.  FP64 (448 bytes): weighted J row 0
 // over the compact columns [0, 25), row 1 [25, 50), weighted residual 50, 51, the
@@ -143,30 +142,21 @@ constexpr int kKeyRowBytesF = 224;
 __device__ __forceinline__ long long packKey(int a, int b, int ea, int eb) {
     return (long long)a | (long long)b << 16 | (long long)ea << 32 | (long long)eb << 48;
 }
-// Compensated FP32 sums: s carries the rounded sum, e the accumulated rounding errors.
-__device__ __forceinline__ void twoSumAdd(float& s, float& e, float v) {
-    const float t = s + v, bp = t - s;
-    e += (s - (t - bp)) + (v - bp);
-    s = t;
-}
-__device__ __forceinline__ float huberWeightF(float scale, float squared) {
-    return scale > 0 && squared > scale * scale ? sqrtf(scale / sqrtf(squared)) : 1.0f;
-}
 
-template <bool Mixed>
-__global__ void __launch_bounds__(kLinWarps * 32, 2) k_lin_landmark(DevBatch B, const int4* runs, const int2* tiles, int maxNs) {
+template <bool Mixed, int Warps, int MinBlocks>
+__global__ void __launch_bounds__(Warps * 32, MinBlocks) k_lin_landmark(DevBatch B, const int4* runs, const int2* tiles, int maxNs) {
     extern __shared__ double smemRaw[];
-    constexpr int kStride = Mixed ? kOutF : kOut;
-    using St = typename std::conditional<Mixed, float, double>::type;
+    constexpr int kStride = kOut;
+    using St = double;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int runIdx = blockIdx.x * kLinWarps + warp;
+    const int runIdx = blockIdx.x * Warps + warp;
     if (runIdx >= B.numRuns) return;
     const int4 run = runs[runIdx];  // {window, tile begin, tile end, -}
     const int wdx = run.x;
     if (B.lm[wdx].mode != kModeLinearize) return;
     char* base = reinterpret_cast<char*>(smemRaw) + landmarkWarpBytes(maxNs, Mixed) * warp;
     St* out = reinterpret_cast<St*>(base);
-    double* cvec = reinterpret_cast<double*>(out + 32 * kStride);
+    double* cvec = out + 32 * kStride;
     long long* keys = reinterpret_cast<long long*>(cvec + maxNs);
     short* map = reinterpret_cast<short*>(keys + 32);
     int* flags = reinterpret_cast<int*>(map + 32 * kCompact);
@@ -187,22 +177,13 @@ __global__ void __launch_bounds__(kLinWarps * 32, 2) k_lin_landmark(DevBatch B, 
             myNs = 6 * (B.lmNs[l] + B.lmNx[l]) + (wd.estTd ? 1 : 0);
             myC0 = B.lmC0[l];
         }
-        double r0 = 0.0, r1 = 0.0;  // residual of this lane's factor (the mixed path keeps it in registers)
         if (f < oe) {
             const int l = B.obLm[f];
             FactorIn in;
             int kfa, kfb, ea, eb;
             gatherFactor(B, wd, wdx, l, f, 0, in, kfa, kfb, ea, eb);
             St* st = out + kStride * lane;
-            bool ok;
-            if constexpr (Mixed) {
-                const FactorJac<float> jac = {st, st + 12, st + 24, st + 36, st + 48, st + 50};
-                double r[2];
-                ok = evalBearing<float>(in, r, &jac);
-                if (ok) { r0 = r[0]; r1 = r[1]; }
-            } else {
-                ok = evalBearingFactor(in, true, *reinterpret_cast<FactorOut*>(st));
-            }
+            const bool ok = evalBearingFactor(in, true, *reinterpret_cast<FactorOut*>(st));
             const int s = B.lmNs[l], x = B.lmNx[l];
             const bool same = in.sameKf && !in.splitExt;
             const int obSlot = B.obSlot[f], obX = B.obXslot[f];
@@ -216,12 +197,15 @@ __global__ void __launch_bounds__(kLinWarps * 32, 2) k_lin_landmark(DevBatch B, 
             mp[24] = wd.estTd ? 6 * (s + x) : -1;
             flags[lane] = ok ? 1 : 0;
             keys[lane] = packKey(kfa - wd.kf0, kfb - wd.kf0, ea - wd.ext0, eb - wd.ext0);
-            if constexpr (Mixed) {
-                if (ok) st[52] = huberWeightF((float)wd.huber, (float)(r0 * r0 + r1 * r1));
-                else for (int k = 0; k < kOutF; ++k) st[k] = 0.0f;
+            if (ok) {
+                st[54] = huberWeight(wd.huber, st[0] * st[0] + st[1] * st[1]);
+                if constexpr (Mixed) {  // the Jacobian blocks over the retained columns and the weight, rounded to FP32
+#pragma unroll
+                    for (int k = 2; k < 52; ++k) st[k] = (double)(float)st[k];
+                    st[54] = (double)(float)st[54];
+                }
             } else {
-                if (ok) st[54] = huberWeight(wd.huber, st[0] * st[0] + st[1] * st[1]);
-                else for (int k = 0; k < kOut; ++k) st[k] = 0.0;
+                for (int k = 0; k < kOut; ++k) st[k] = 0.0;
             }
         }
         __syncwarp();
@@ -229,11 +213,11 @@ __global__ void __launch_bounds__(kLinWarps * 32, 2) k_lin_landmark(DevBatch B, 
         if (f < oe) {
             const St* st = out + kStride * lane;
             if constexpr (Mixed) {
-                const float w = st[52];
+                const float w = (float)st[54];
                 char* row = reinterpret_cast<char*>(B.keyRows) + (size_t)f * kKeyRowBytesF;
-                *reinterpret_cast<double2*>(row) = make_double2((double)w * r0, (double)w * r1);
+                *reinterpret_cast<double2*>(row) = make_double2((double)w * st[0], (double)w * st[1]);
                 float4* jr = reinterpret_cast<float4*>(row + 16);
-                auto at = [&](int k) { return w * st[k < 25 ? compactOffF(0, k) : compactOffF(1, k - 25)]; };
+                auto at = [&](int k) { return w * (float)st[k < 25 ? compactOff(0, k) : compactOff(1, k - 25)]; };
 #pragma unroll
                 for (int q = 0; q < 12; ++q) jr[q] = make_float4(at(4 * q), at(4 * q + 1), at(4 * q + 2), at(4 * q + 3));
                 *reinterpret_cast<float2*>(row + 16 + 192) = make_float2(at(48), at(49));
@@ -255,27 +239,16 @@ __global__ void __launch_bounds__(kLinWarps * 32, 2) k_lin_landmark(DevBatch B, 
         // this lane's contributions to d_l, g_l, the cost and (in place) the cross products
         const bool live = f < oe && flags[lane];
         double dD = 0.0, gD = 0.0, cost = 0.0;
-        float dS = 0.0f;
         if (live) {
             St* st = out + kStride * lane;
-            if constexpr (Mixed) {
-                cost = huberCost(wd.huber, r0 * r0 + r1 * r1);
-                const float p0 = st[50], p1 = st[51], w = st[52], w2 = w * w;
-                dS = w2 * (p0 * p0 + p1 * p1);
-                gD = (double)w2 * ((double)p0 * r0 + (double)p1 * r1);  // gradient: FP32 Jacobian, FP64 residual
-                // in place: column c reads offsets >= c, none overwritten before it is read
+            const double q0 = st[0], q1 = st[1], p0 = st[52], p1 = st[53];
+            const double w = st[54], w2 = w * w;
+            cost = huberCost(wd.huber, q0 * q0 + q1 * q1);
+            dD = w2 * (p0 * p0 + p1 * p1);
+            gD = w2 * (p0 * q0 + p1 * q1);
+            // in place: column c reads offsets >= c + 2, all later than slot c
 #pragma unroll
-                for (int c = 0; c < kCompact; ++c) st[c] = w2 * (st[compactOffF(0, c)] * p0 + st[compactOffF(1, c)] * p1);
-            } else {
-                const double q0 = st[0], q1 = st[1], p0 = st[52], p1 = st[53];
-                const double w = st[54], w2 = w * w;
-                cost = huberCost(wd.huber, q0 * q0 + q1 * q1);
-                dD = w2 * (p0 * p0 + p1 * p1);
-                gD = w2 * (p0 * q0 + p1 * q1);
-                // in place: column c reads offsets >= c + 2, all later than slot c
-#pragma unroll
-                for (int c = 0; c < kCompact; ++c) st[c] = w2 * (st[compactOff(0, c)] * p0 + st[compactOff(1, c)] * p1);
-            }
+            for (int c = 0; c < kCompact; ++c) st[c] = w2 * (st[compactOff(0, c)] * p0 + st[compactOff(1, c)] * p1);
         }
         __syncwarp();
         // landmark sums of d, g, cost and validity: segmented inclusive scans over
@@ -283,24 +256,13 @@ __global__ void __launch_bounds__(kLinWarps * 32, 2) k_lin_landmark(DevBatch B, 
         {
             const int seg = B.obLm[f < oe ? f : ob] - lb;  // landmark of this lane (lanes past the tile: any)
             int bad = f < oe && !flags[lane] ? 1 : 0;
-            float dE = 0.0f;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const double c2 = __shfl_up_sync(0xffffffffu, cost, o);
                 const int b2 = __shfl_up_sync(0xffffffffu, bad, o), s2 = __shfl_up_sync(0xffffffffu, seg, o);
-                if constexpr (Mixed) {
-                    const float ds2 = __shfl_up_sync(0xffffffffu, dS, o), de2 = __shfl_up_sync(0xffffffffu, dE, o);
-                    const double g2 = __shfl_up_sync(0xffffffffu, gD, o);
-                    if (lane >= o && s2 == seg) {
-                        dE += de2; twoSumAdd(dS, dE, ds2);
-                        gD += g2; cost += c2; bad |= b2;
-                    }
-                } else {
-                    const double d2 = __shfl_up_sync(0xffffffffu, dD, o), g2 = __shfl_up_sync(0xffffffffu, gD, o);
-                    if (lane >= o && s2 == seg) { dD += d2; gD += g2; cost += c2; bad |= b2; }
-                }
+                const double d2 = __shfl_up_sync(0xffffffffu, dD, o), g2 = __shfl_up_sync(0xffffffffu, gD, o);
+                if (lane >= o && s2 == seg) { dD += d2; gD += g2; cost += c2; bad |= b2; }
             }
-            if constexpr (Mixed) dD = (double)dS + (double)dE;
             // the last lane of each landmark holds its sums
             const int nextSeg = __shfl_down_sync(0xffffffffu, seg, 1);
             if (f < oe && (lane == 31 || f + 1 >= oe || nextSeg != seg)) {
@@ -325,31 +287,17 @@ __global__ void __launch_bounds__(kLinWarps * 32, 2) k_lin_landmark(DevBatch B, 
             __syncwarp();
             if (lane < kCompact) {
                 int cur = -1;
-                if constexpr (Mixed) {
-                    float accS = 0.0f, accE = 0.0f;
-                    for (int k = fb; k < fe; ++k) {
-                        const int li = map[kCompact * k + lane];
-                        if (li != cur) {
-                            if (cur >= 0) cvec[cur] += (double)accS + (double)accE;
-                            cur = li;
-                            accS = accE = 0.0f;
-                        }
-                        if (li >= 0 && flags[k]) twoSumAdd(accS, accE, out[kOutF * k + lane]);
+                double accv = 0.0;
+                for (int k = fb; k < fe; ++k) {
+                    const int li = map[kCompact * k + lane];
+                    if (li != cur) {
+                        if (cur >= 0) cvec[cur] += accv;
+                        cur = li;
+                        accv = 0.0;
                     }
-                    if (cur >= 0) cvec[cur] += (double)accS + (double)accE;
-                } else {
-                    double accv = 0.0;
-                    for (int k = fb; k < fe; ++k) {
-                        const int li = map[kCompact * k + lane];
-                        if (li != cur) {
-                            if (cur >= 0) cvec[cur] += accv;
-                            cur = li;
-                            accv = 0.0;
-                        }
-                        if (li >= 0 && flags[k]) accv += out[kOut * k + lane];
-                    }
-                    if (cur >= 0) cvec[cur] += accv;
+                    if (li >= 0 && flags[k]) accv += out[kOut * k + lane];
                 }
+                if (cur >= 0) cvec[cur] += accv;
             }
             __syncwarp();
             for (int i = lane; i < ns; i += 32) B.lmC[c0 + i] = cvec[i];
@@ -504,7 +452,8 @@ __global__ void __launch_bounds__(kPairWarps * 32) k_lin_pairs(DevBatch B, const
 // most columns) with the ascending union U of their visual support columns.
 // Each landmark's row c_l / sqrt(dt_l) is expanded over U in shared memory (its
 // local -> U map is built on the host), with g_l / sqrt(dt_l) as column |U| for
-// B_v.  The rank update uses 32 x 32 tiles, one per warp (4 x 8 per lane);
+// B_v.  The rank update uses 32 x 32 tiles, one per warp, on the FP64 tensor
+// path (mma.sync m8n8k4, dense_tiles.cuh);
 // spare warps split the rows when the tiles are fewer than the warps.  Every
 // tile is added to the window's Schur sum once per chunk.
 __global__ void __launch_bounds__(kSchurThreads, 3) k_lin_schur(DevBatch B, const int4* chunks) {
@@ -545,10 +494,10 @@ __global__ void __launch_bounds__(kSchurThreads, 3) k_lin_schur(DevBatch B, cons
         tileOf(t, nb, bi, bj);
         double acc[4][8];
         zeroTile(acc);
-        rankUpdate<false>(acc, Rw + bi * 32 + 2 * (lane >> 2), Rw + bj * 32 + 2 * (lane & 3), part, rows, wpt, np);
+        rankUpdateMma<false>(acc, Rw, bi * 32, bj * 32, part, rows, wpt, np);
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-            const int i = tileRow(bi, lane, r);
+            const int i = tileRowMma(bi, lane, r);
 #pragma unroll
             for (int c = 0; c < 8; ++c) {
                 const int j = tileCol(bj, lane, c);
@@ -1046,10 +995,10 @@ __global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int re
                 tileOf(t, nb2, cb, rb);  // upper enumeration (cb <= rb): rows rb, columns cb
                 double tacc[4][8];
                 zeroTile(tacc);
-                rankUpdate<false>(tacc, P + bw + rb * 32 + 2 * (lane >> 2), P + bw + cb * 32 + 2 * (lane & 3), 0, bw, 1, mp);
+                rankUpdateMma<false>(tacc, P + bw, rb * 32, cb * 32, 0, bw, 1, mp);
 #pragma unroll
                 for (int r = 0; r < 4; ++r) {
-                    const int i = tileRow(rb, lane, r);
+                    const int i = tileRowMma(rb, lane, r);
 #pragma unroll
                     for (int c = 0; c < 8; ++c) {
                         const int j = tileCol(cb, lane, c);
@@ -1267,10 +1216,11 @@ __global__ void __launch_bounds__(256) k_backsub(DevBatch B) {
 // one warp per tile of <= 32 observations, lane = observation; the per-landmark
 // sums are segmented scans over the tile's lanes (a landmark's observations are
 // consecutive lanes), written by each landmark's last lane.
-constexpr int kTrialWarps = 8;
-__global__ void __launch_bounds__(kTrialWarps * 32, 2) k_trial(DevBatch B, const int2* tiles, int numTiles) {
+constexpr int kTrialWarps = 8;  // warps per CTA of the gate
+template <int Warps, int MinBlocks>
+__global__ void __launch_bounds__(Warps * 32, MinBlocks) k_trial(DevBatch B, const int2* tiles, int numTiles) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int t = blockIdx.x * kTrialWarps + warp;
+    const int t = blockIdx.x * Warps + warp;
     if (t >= numTiles) return;
     const int2 tile = tiles[t];
     const int lb = tile.x, le = tile.y, nl = le - lb;
@@ -1614,7 +1564,11 @@ void launchAddHost(const DevBatch& B, const double* hostH, const double* hostG, 
                    int trial, cudaStream_t s) {
     k_add_host<<<B.numWindows, 256, 0, s>>>(B, hostH, hostG, hostCost, flag, trial);
 }
-size_t linearizeSmemBytes(int maxNs, bool mixed) { return kLinWarps * landmarkWarpBytes(maxNs, mixed); }
+size_t linearizeSmemBytes(int maxNs, bool mixed) {  // the widest shape's
+    size_t m = 0;
+    for (const KernelShape& k : kLinShapeTable) m = std::max(m, (size_t)k.warps * landmarkWarpBytes(maxNs, mixed));
+    return m;
+}
 size_t schurSmemBytes() { return kSchurSmemDoubles * sizeof(double); }
 size_t factorSmemBytes(int maxNr) {
     // one panel of kFacPanel columns over the padded rows, four n-vectors, the diagonal block
@@ -1631,8 +1585,8 @@ cudaError_t configureKernels(size_t linSmem, size_t facSmem) {
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     if (e != cudaSuccess) return e;
     cudaFuncAttributes la, lm, fa, sa, pa, pm;
-    if ((e = cudaFuncGetAttributes(&la, k_lin_landmark<false>)) != cudaSuccess) return e;
-    if ((e = cudaFuncGetAttributes(&lm, k_lin_landmark<true>)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&la, k_lin_landmark<false, 6, 2>)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&lm, k_lin_landmark<true, 6, 2>)) != cudaSuccess) return e;
     if ((e = cudaFuncGetAttributes(&pa, k_lin_pairs<false>)) != cudaSuccess) return e;
     if ((e = cudaFuncGetAttributes(&pm, k_lin_pairs<true>)) != cudaSuccess) return e;
     if ((e = cudaFuncGetAttributes(&fa, k_factor)) != cudaSuccess) return e;
@@ -1643,10 +1597,45 @@ cudaError_t configureKernels(size_t linSmem, size_t facSmem) {
     if (linSmem > linMax || facSmem > facMax || schurSmemBytes() > schMax || pairCtaBytes() > pairMax) return cudaErrorInvalidValue;
     for (auto k : {k_lin_pairs<false>, k_lin_pairs<true>})
         if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pairCtaBytes())) != cudaSuccess) return e;
-    for (auto k : {k_lin_landmark<false>, k_lin_landmark<true>})
+    for (auto k : {k_lin_landmark<false, 6, 2>, k_lin_landmark<true, 6, 2>, k_lin_landmark<false, 8, 1>, k_lin_landmark<true, 8, 1>,
+                   k_lin_landmark<false, 4, 3>, k_lin_landmark<true, 4, 3>, k_lin_landmark<false, 6, 1>, k_lin_landmark<true, 6, 1>})
         if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)linMax)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_lin_schur, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)schMax)) != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)facMax);
+}
+
+// The landmark and trial passes in the kernel shape the plan names.
+template <bool Mixed, int Warps, int MinBlocks>
+void linLandmarkShape(const DevBatch& B, const LaunchPlan& P, cudaStream_t s) {
+    const int blocks = (B.numRuns + Warps - 1) / Warps;
+    k_lin_landmark<Mixed, Warps, MinBlocks><<<blocks, Warps * 32, Warps * landmarkWarpBytes(P.maxNs, Mixed), s>>>(B, P.runs, P.tiles,
+                                                                                                                P.maxNs);
+}
+template <bool Mixed>
+void linLandmarkMixed(const DevBatch& B, const LaunchPlan& P, cudaStream_t s) {
+    switch (P.linShape) {
+        case 1: linLandmarkShape<Mixed, 8, 1>(B, P, s); break;
+        case 2: linLandmarkShape<Mixed, 4, 3>(B, P, s); break;
+        case 3: linLandmarkShape<Mixed, 6, 1>(B, P, s); break;
+        default: linLandmarkShape<Mixed, 6, 2>(B, P, s); break;
+    }
+}
+static_assert(kLinShapes == 4 && kLinShapeTable[1].warps == 8 && kLinShapeTable[2].minBlocks == 3, "shape table and dispatch");
+void launchLinLandmark(const DevBatch& B, const LaunchPlan& P, cudaStream_t s) {
+    if (B.mixed) linLandmarkMixed<true>(B, P, s);
+    else linLandmarkMixed<false>(B, P, s);
+}
+template <int Warps, int MinBlocks>
+void trialShape(const DevBatch& B, const LaunchPlan& P, cudaStream_t s) {
+    k_trial<Warps, MinBlocks><<<(P.numTiles + Warps - 1) / Warps, Warps * 32, 0, s>>>(B, P.tiles, P.numTiles);
+}
+static_assert(kTrialShapes == 3 && kTrialShapeTable[1].minBlocks == 1 && kTrialShapeTable[2].warps == 4, "shape table and dispatch");
+void launchTrial(const DevBatch& B, const LaunchPlan& P, cudaStream_t s) {
+    switch (P.trialShape) {
+        case 1: trialShape<8, 1>(B, P, s); break;
+        case 2: trialShape<4, 4>(B, P, s); break;
+        default: trialShape<8, 2>(B, P, s); break;
+    }
 }
 
 // One LM iteration in three parts (kIterLinearize: the linearization up to the
@@ -1665,12 +1654,7 @@ int launchIterationParts(const DevBatch& B, const LaunchPlan& P, int refinement,
     };
     if (parts & kIterLinearize) {
     run(CGMLI_KERNEL_ZERO, [&] { k_zero_acc<<<W, 256, 0, s>>>(B); });
-    const int runBlocks = (B.numRuns + kLinWarps - 1) / kLinWarps;
-    if (B.numRuns > 0)
-        run(CGMLI_KERNEL_LINEARIZE, [&] {
-            if (B.mixed) k_lin_landmark<true><<<runBlocks, kLinWarps * 32, P.linSmem, s>>>(B, P.runs, P.tiles, P.maxNs);
-            else k_lin_landmark<false><<<runBlocks, kLinWarps * 32, P.linSmem, s>>>(B, P.runs, P.tiles, P.maxNs);
-        });
+    if (B.numRuns > 0) run(CGMLI_KERNEL_LINEARIZE, [&] { launchLinLandmark(B, P, s); });
     if (P.numPairChunks > 0)
         run(CGMLI_KERNEL_LIN_PAIRS, [&] {
             const int blocks = (P.numPairChunks + kPairWarps - 1) / kPairWarps;
@@ -1686,9 +1670,7 @@ int launchIterationParts(const DevBatch& B, const LaunchPlan& P, int refinement,
     run(CGMLI_KERNEL_CANDIDATE, [&] { k_candidate<<<W, 128, 0, s>>>(B); });
     if (B.numLandmarks > 0) {
         run(CGMLI_KERNEL_BACKSUB_TRIAL, [&] { k_backsub<<<(B.numLandmarks * 8 + 255) / 256, 256, 0, s>>>(B); });
-        run(CGMLI_KERNEL_BACKSUB_TRIAL, [&] {
-            k_trial<<<(P.numTiles + kTrialWarps - 1) / kTrialWarps, kTrialWarps * 32, 0, s>>>(B, P.tiles, P.numTiles);
-        });
+        run(CGMLI_KERNEL_BACKSUB_TRIAL, [&] { launchTrial(B, P, s); });
     }
     run(CGMLI_KERNEL_RETAINED_TRIAL, [&] { k_retained<<<W, 256, 0, s>>>(B, 1); });
     }

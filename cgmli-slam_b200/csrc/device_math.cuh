@@ -233,265 +233,8 @@ __device__ __forceinline__ void poseBlock(const double* M, d3 v, double sign, do
 }
 
 
-// ---- Jacobian section, templated on its arithmetic type -----------------------------
-// The residual chain runs in FP64 (the residual feeds the gradient and the cost).
-// The derivatives run in T: FP64 for the FP64 path, FP32 for the mixed-precision
-// linearization, from the FP64 intermediates rounded once.
-template <class T> struct v3t { T x, y, z; };
-template <class T> struct m3t { T a[9]; };  // row-major
-template <class T> __device__ __forceinline__ v3t<T> operator+(v3t<T> a, v3t<T> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
-template <class T> __device__ __forceinline__ v3t<T> operator-(v3t<T> a, v3t<T> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
-template <class T> __device__ __forceinline__ v3t<T> operator*(T s, v3t<T> a) { return {s * a.x, s * a.y, s * a.z}; }
-template <class T> __device__ __forceinline__ T dot(v3t<T> a, v3t<T> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-template <class T> __device__ __forceinline__ v3t<T> cross(v3t<T> a, v3t<T> b) {
-    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
-}
-template <class T> __device__ __forceinline__ m3t<T> skew(v3t<T> v) { return {{0, -v.z, v.y, v.z, 0, -v.x, -v.y, v.x, 0}}; }
-template <class T> __device__ __forceinline__ m3t<T> mul(const m3t<T>& A, const m3t<T>& B) {
-    m3t<T> r;
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) r.a[3 * i + j] = A.a[3 * i] * B.a[j] + A.a[3 * i + 1] * B.a[3 + j] + A.a[3 * i + 2] * B.a[6 + j];
-    return r;
-}
-template <class T> __device__ __forceinline__ m3t<T> tr(const m3t<T>& A) {
-    return {{A.a[0], A.a[3], A.a[6], A.a[1], A.a[4], A.a[7], A.a[2], A.a[5], A.a[8]}};
-}
-template <class T> __device__ __forceinline__ m3t<T> madd(const m3t<T>& A, const m3t<T>& B) {
-    m3t<T> r;
-#pragma unroll
-    for (int i = 0; i < 9; ++i) r.a[i] = A.a[i] + B.a[i];
-    return r;
-}
-template <class T> __device__ __forceinline__ m3t<T> msub(const m3t<T>& A, const m3t<T>& B) {
-    m3t<T> r;
-#pragma unroll
-    for (int i = 0; i < 9; ++i) r.a[i] = A.a[i] - B.a[i];
-    return r;
-}
-template <class T> __device__ __forceinline__ m3t<T> mscl(T s, const m3t<T>& A) {
-    m3t<T> r;
-#pragma unroll
-    for (int i = 0; i < 9; ++i) r.a[i] = s * A.a[i];
-    return r;
-}
-template <class T> __device__ __forceinline__ m3t<T> outer(v3t<T> a, v3t<T> b) {
-    return {{a.x * b.x, a.x * b.y, a.x * b.z, a.y * b.x, a.y * b.y, a.y * b.z, a.z * b.x, a.z * b.y, a.z * b.z}};
-}
-template <class T> __device__ __forceinline__ m3t<T> eye3t() { return {{1, 0, 0, 0, 1, 0, 0, 0, 1}}; }
-template <class T> __device__ __forceinline__ void rowTimesM(const T* A, const m3t<T>& B, T* out) {  // (2x3)(3x3)
-#pragma unroll
-    for (int r = 0; r < 2; ++r)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) out[3 * r + c] = A[3 * r] * B.a[c] + A[3 * r + 1] * B.a[3 + c] + A[3 * r + 2] * B.a[6 + c];
-}
-// J = sign * [M, -M [v]x] for a 2x3 M
-template <class T> __device__ __forceinline__ void poseBlock(const T* M, v3t<T> v, T sign, T* J) {
-    T Ms[6];
-    rowTimesM(M, skew(v), Ms);
-#pragma unroll
-    for (int r = 0; r < 2; ++r)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) { J[6 * r + c] = sign * M[3 * r + c]; J[6 * r + 3 + c] = -sign * Ms[3 * r + c]; }
-}
-template <class T> __device__ __forceinline__ v3t<T> cvt(d3 v) { return {(T)v.x, (T)v.y, (T)v.z}; }
-template <class T> __device__ __forceinline__ m3t<T> cvt(const m3& m) {
-    m3t<T> r;
-#pragma unroll
-    for (int i = 0; i < 9; ++i) r.a[i] = (T)m.a[i];
-    return r;
-}
-
-// Jacobian outputs of one factor (2x6 tangent blocks row-major, then td and rho).
-template <class T> struct FactorJac { T *Ja, *Jb, *Jea, *Jeb, *Jtd, *Jrho; };
-
-// Inputs of the derivative section, produced by the residual chain.
-template <class T> struct JacIn {
-    T P[6], meas[6];  // transported and raw 2x3 measurement rows
-    v3t<T> u, bb, n, world, bodyA, observerBody, ba, measured, da, db, logarithm;
-    m3t<T> W, Ra, Rb, cameraRotation, K;
-    T f, g, c, range, rho, denominator;
-    T jrho[2];  // the depth derivative, formed in FP64 by the caller
-    bool same, sameKf, splitExt, wantExt, timeDerivative, moving;
-};
-
-template <class T> __device__ __forceinline__ bool bearingJacobians(const JacIn<T>& q, const FactorJac<T>& o) {
-    T red[6];
-#pragma unroll
-    for (int r = 0; r < 2; ++r) {
-        const v3t<T> Pr = {q.P[3 * r], q.P[3 * r + 1], q.P[3 * r + 2]};
-        const T Pu = dot(Pr, q.u), Pb = dot(Pr, q.bb);
-        const v3t<T> proj = q.f * Pr + (q.g * Pu - q.f * Pb) * q.bb;
-        const T pn = dot(proj, q.n);
-        red[3 * r] = (proj.x - pn * q.n.x) / q.range;
-        red[3 * r + 1] = (proj.y - pn * q.n.y) / q.range;
-        red[3 * r + 2] = (proj.z - pn * q.n.z) / q.range;
-    }
-#pragma unroll
-    for (int i = 0; i < 12; ++i) { o.Ja[i] = 0; o.Jb[i] = 0; o.Jea[i] = 0; o.Jeb[i] = 0; }
-    if (!q.same) {
-        T D[6];
-        rowTimesM(red, q.W, D);
-        if (!q.sameKf) {
-            poseBlock(D, q.world, T(1), o.Ja);
-            poseBlock(D, q.world, T(-1), o.Jb);
-        }
-        if (q.wantExt) {
-            T DR[6];
-            rowTimesM(D, q.Ra, DR);
-            poseBlock(DR, q.bodyA, T(1), o.Jea);
-            rowTimesM(D, q.Rb, DR);
-            poseBlock(DR, q.observerBody, T(-1), q.splitExt ? o.Jeb : o.Jb);  // temporarily in Jb when shared
-            if (!q.splitExt) {
-                // shared extrinsic: sum both sides into Jea, restore the observer pose block
-#pragma unroll
-                for (int i = 0; i < 12; ++i) o.Jea[i] += o.Jb[i];
-                if (!q.sameKf) poseBlock(D, q.world, T(-1), o.Jb);
-                else for (int i = 0; i < 12; ++i) o.Jb[i] = 0;
-            }
-        }
-    }
-    o.Jrho[0] = q.jrho[0];
-    o.Jrho[1] = q.jrho[1];
-    if (!isfinite(o.Jrho[0]) || !isfinite(o.Jrho[1])) return false;
-    o.Jtd[0] = o.Jtd[1] = 0;
-    if (q.timeDerivative && q.moving) {
-        const m3t<T> Jn = madd(mscl(q.f, msub(mscl(T(-1), outer(q.bb, q.n)), mscl(q.c, eye3t<T>()))), mscl(q.g, outer(q.u, q.n)));
-        const m3t<T> dK = skew(cross(q.measured, q.db));
-        const m3t<T> dR = msub(madd(dK, mscl(T(1) / q.denominator, madd(mul(dK, q.K), mul(q.K, dK)))),
-                               mscl(dot(q.measured, q.db) / (q.denominator * q.denominator), mul(q.K, q.K)));
-        T RC[6], PJ[6], MdR[6];
-        rowTimesM(red, q.cameraRotation, RC);
-        rowTimesM(q.P, Jn, PJ);
-        rowTimesM(q.meas, tr(dR), MdR);
-        const v3t<T> qv = (T(1) / q.rho) * q.da;
-#pragma unroll
-        for (int r = 0; r < 2; ++r)
-            o.Jtd[r] = RC[3 * r] * qv.x + RC[3 * r + 1] * qv.y + RC[3 * r + 2] * qv.z + PJ[3 * r] * q.db.x + PJ[3 * r + 1] * q.db.y +
-                       PJ[3 * r + 2] * q.db.z + MdR[3 * r] * q.logarithm.x + MdR[3 * r + 1] * q.logarithm.y +
-                       MdR[3 * r + 2] * q.logarithm.z;
-        if (!isfinite(o.Jtd[0]) || !isfinite(o.Jtd[1])) return false;
-    }
-    return true;
-}
-
-// Residual (FP64) and, when `jac` is given, the Jacobians in T (the mixed-precision
-// linearization instantiates T = float).  Returns false for an invalid factor (the
-// reference's valid = 0).  The FP64 path uses evalBearingFactor below: same
-// formulas, all in double.
-template <class T>
-__device__ __forceinline__ bool evalBearing(const FactorIn& in, double* res, const FactorJac<T>* jac) {
-    const double rho = in.rho;
-    if (!(rho > 0) || !isfinite(rho) || !isfinite(in.td)) return false;
-    if (!validPose(in.xa) || !validPose(in.xb) || !validPose(in.xea) || !validPose(in.xeb)) return false;
-    const bool derivatives = jac != nullptr;
-    const bool same = in.sameKf && !in.splitExt;
-    const bool timeDerivative = derivatives && in.wantTd;
-    const bool movingAnchor = dot(in.anchorVel, in.anchorVel) > 0, movingMeasured = dot(in.measuredVel, in.measuredVel) > 0;
-    d3 ba = (1 / norm(in.anchor)) * in.anchor, bb = (1 / norm(in.measured)) * in.measured, da = {0, 0, 0}, db = {0, 0, 0};
-    if (movingAnchor) ba = timeBearing(in.anchor, in.anchorVel, in.anchorTime - in.td, timeDerivative, da);
-    if (movingMeasured) bb = timeBearing(in.measured, in.measuredVel, in.measuredTime - in.td, timeDerivative, db);
-    if (!finite3(ba) || !finite3(bb)) return false;
-    const m3 Rca = ldm3(in.Rca), Rcb = ldm3(in.Rcb);
-    const d3 tca = ld3(in.tca), tcb = ld3(in.tcb);
-    const d3 local = mv(Rca, (1 / rho) * ba) + tca;
-    m3 Ra, Rb, W, cameraRotation;
-    d3 pc, bodyA, world, observerBody;
-    if (same) {
-        pc = mtv(Rcb, local - tcb);
-        cameraRotation = mul(tr(Rcb), Rca);
-    } else {
-        Ra = ldm3(in.Ra);
-        Rb = ldm3(in.Rb);
-        const m3 Rea = ldm3(in.Rea), Reb = ldm3(in.Reb);
-        const d3 tea = ld3(in.xea), teb = ld3(in.xeb);
-        W = tr(mul(mul(Rb, Reb), Rcb));
-        cameraRotation = mul(W, mul(mul(Ra, Rea), Rca));
-        bodyA = mv(Rea, local) + tea;
-        const d3 separation = ld3(in.xa) - ld3(in.xb);
-        if (!in.splitExt) {
-            const d3 offset = mv(W, (mv(Ra, mv(Rea, tca) + tea) - mv(Rb, mv(Reb, tcb) + teb)) + separation);
-            pc = mv(cameraRotation, (1 / rho) * ba) + offset;
-        } else {
-            const d3 wpt = mv(Ra, bodyA) + ld3(in.xa);
-            const d3 ob = mtv(Rb, wpt - ld3(in.xb));
-            pc = mtv(Rcb, mtv(Reb, ob - teb) - tcb);
-        }
-        const d3 rotated = mv(Ra, bodyA);
-        world = rotated + ld3(in.xa);
-        observerBody = mtv(Rb, rotated + separation);
-    }
-    const double range = norm(pc);
-    if (!finite3(pc) || !isfinite(range) || range < 1e-10) return false;
-    const d3 n = (1 / range) * pc;
-    const double c = fmin(1.0, fmax(-1.0, dot(bb, n))), s = norm(cross(bb, n));
-    const double denominator = movingMeasured ? 1 + dot(in.measured, bb) : 2;
-    if (c < -1 + 1e-8 || denominator < 1e-8) return false;
-    const d3 u = n - c * bb;
-    const double d = 1 - c;
-    const bool series = c > 0 && s < 1e-3;
-    const double theta = series ? 0 : atan2(s, c);
-    const double f = s < 1e-8 ? 1.0 : (series ? 1 + d / 3 + 2 * d * d / 15 + 2 * d * d * d / 35 : theta / s);
-    const d3 logarithm = f * u;
-    double P[6];
-#pragma unroll
-    for (int i = 0; i < 6; ++i) P[i] = in.meas[i];
-    m3 K = {{0, 0, 0, 0, 0, 0, 0, 0, 0}};
-    if (movingMeasured) {
-        K = skew(cross(in.measured, bb));
-        const m3 transport = madd(madd(eye3(), K), mscl(1 / denominator, mul(K, K)));
-        rowTimesM(in.meas, tr(transport), P);
-    }
-    res[0] = P[0] * logarithm.x + P[1] * logarithm.y + P[2] * logarithm.z;
-    res[1] = P[3] * logarithm.x + P[4] * logarithm.y + P[5] * logarithm.z;
-    if (!isfinite(res[0]) || !isfinite(res[1])) return false;
-    if (!derivatives) return true;
-    const double g = s < 1e-8 ? 0.0 : (series ? (-1.0 / 3.0 - 4 * d / 15.0 - 6 * d * d / 35.0) : (theta * c - s) / (s * s * s));
-    // reference checks: unit quaternions of differentiated pose blocks (writePose)
-    if (!same && (!unitPose(in.xa) || !unitPose(in.xb))) return false;
-    if (!same && in.wantExt && (!unitPose(in.xea) || !unitPose(in.xeb))) return false;
-    JacIn<T> q;
-    {
-        // The depth derivative is the point gradient dotted with the anchor ray; for an
-        // observer that sees the point almost along that ray the product nearly cancels,
-        // and it alone sets the landmark information d_l: formed in FP64, rounded once.
-        double red[6], RC[6];
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            const d3 Pr = {P[3 * r], P[3 * r + 1], P[3 * r + 2]};
-            const double Pu = dot(Pr, u), Pb = dot(Pr, bb);
-            const d3 proj = f * Pr + (g * Pu - f * Pb) * bb;
-            const double pn = dot(proj, n);
-            red[3 * r] = (proj.x - pn * n.x) / range;
-            red[3 * r + 1] = (proj.y - pn * n.y) / range;
-            red[3 * r + 2] = (proj.z - pn * n.z) / range;
-        }
-        rowTimesM(red, cameraRotation, RC);
-        const d3 qv = (-1 / (rho * rho)) * ba;
-        q.jrho[0] = (T)(RC[0] * qv.x + RC[1] * qv.y + RC[2] * qv.z);
-        q.jrho[1] = (T)(RC[3] * qv.x + RC[4] * qv.y + RC[5] * qv.z);
-    }
-#pragma unroll
-    for (int i = 0; i < 6; ++i) { q.P[i] = (T)P[i]; q.meas[i] = (T)in.meas[i]; }
-    q.u = cvt<T>(u); q.bb = cvt<T>(bb); q.n = cvt<T>(n); q.ba = cvt<T>(ba);
-    q.cameraRotation = cvt<T>(cameraRotation);
-    q.f = (T)f; q.g = (T)g; q.c = (T)c; q.range = (T)range; q.rho = (T)rho;
-    q.same = same; q.sameKf = in.sameKf; q.splitExt = in.splitExt; q.wantExt = in.wantExt;
-    q.timeDerivative = timeDerivative; q.moving = movingAnchor || movingMeasured;
-    if (!same) {
-        q.W = cvt<T>(W); q.Ra = cvt<T>(Ra); q.Rb = cvt<T>(Rb);
-        q.world = cvt<T>(world); q.bodyA = cvt<T>(bodyA); q.observerBody = cvt<T>(observerBody);
-    }
-    if (q.timeDerivative && q.moving) {
-        q.K = cvt<T>(K); q.denominator = (T)denominator; q.measured = cvt<T>(in.measured);
-        q.da = cvt<T>(da); q.db = cvt<T>(db); q.logarithm = cvt<T>(logarithm);
-    }
-    return bearingJacobians(q, *jac);
-}
-
-// FP64 factor: residual and Jacobians in double, one straight-line routine (the
-// templated form above keeps more values live and spills more at 168 registers).
+// The bearing factor: residual and Jacobians in FP64, one straight-line routine.
+// Returns false for an invalid factor (the reference's valid = 0).
 __device__ inline bool evalBearingFactor(const FactorIn& in, bool derivatives, FactorOut& o) {
     const double rho = in.rho;
     if (!(rho > 0) || !isfinite(rho) || !isfinite(in.td)) return false;

@@ -83,9 +83,6 @@ __device__ __forceinline__ double odeSinc(double x) {
     return 1.0 - x2 / 6.0 + x4 / 120.0 - x6 / 5040.0;
 }
 
-// Rows of E with nonzero columns [3, 15) (rows 0..2 and 6..8) or [9, 12) (rows 3..5).
-__device__ __forceinline__ int eLo(int r) { return (r >= 3 && r < 6) ? 9 : 3; }
-__device__ __forceinline__ int eHi(int r) { return (r >= 3 && r < 6) ? 12 : 15; }
 // The five row (or column) pairs a warp's two half-warps handle together;
 // pairs share their E column range.  Pair 4 is row 5 in both halves.
 __device__ __forceinline__ int pairRow(int pair, int half) {

@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cfloat>
 
 #include "../../include/cgmli_backend.h"
 #include "backend_internal.h"
@@ -159,8 +160,9 @@ __global__ void k_marg_eval(DevBatch B, MargBatch M) {
 //   sum_factor-rows v v^T - sum_Schur-rows s s^T
 // (the factor normal blocks minus c c^T / d) and its gradient
 //   sum v r - sum s bl / sqrt(d).
-// The upper triangle is cut into 32 x 32 tiles, each lane holding a 4 x 8
-// block of one tile in registers.  When the tiles fit the warps, spare warps
+// The upper triangle is cut into 32 x 32 tiles, each warp holding one tile's
+// FP64 tensor-path accumulators (mma.sync m8n8k4, dense_tiles.cuh) in
+// registers.  When the tiles fit the warps, spare warps
 // split a tile's rows (k) between them and the blocks are held over the whole
 // item; else every warp sums its tiles per chunk.  Either way each block is
 // added to the window's H with atomics once per accumulation.
@@ -168,7 +170,7 @@ namespace {
 __device__ __forceinline__ void flushTile(double (&acc)[4][8], int bi, int bj, int lane, int n, const int* visCol, double* H, int m) {
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-        const int i = tileRow(bi, lane, r);
+        const int i = tileRowMma(bi, lane, r);
 #pragma unroll
         for (int c = 0; c < 8; ++c) {
             const int j = tileCol(bj, lane, c);
@@ -205,7 +207,7 @@ __global__ void __launch_bounds__(kRowsThreads, 1) k_marg_rows(DevBatch B, MargB
     const int w = it.x;
     const MargWin mw = M.win[w];
     const int n = mw.nv, np = (n + 31) & ~31, nb = np >> 5, ntiles = nb * (nb + 1) / 2;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, rg = lane >> 2, cg = lane & 3;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     constexpr int nw = kRowsThreads / 32;
     const bool persistent = ntiles <= nw;
     const int wpt = persistent ? nw / ntiles : 1;  // warps per tile (k split)
@@ -294,10 +296,8 @@ __global__ void __launch_bounds__(kRowsThreads, 1) k_marg_rows(DevBatch B, MargB
             int bi, bj;
             tileOf(t, nb, bi, bj);
             if (!persistent) zeroTile(acc);
-            const double* Va = V + bi * 32 + 2 * rg;
-            const double* Vb = V + bj * 32 + 2 * cg;
-            rankUpdate<false>(acc, Va, Vb, part, kp, wpt, np);
-            rankUpdate<true>(acc, Va, Vb, kp + part, K, wpt, np);
+            rankUpdateMma<false>(acc, V, bi * 32, bj * 32, part, kp, wpt, np);
+            rankUpdateMma<true>(acc, V, bi * 32, bj * 32, kp + part, K, wpt, np);
             if (!persistent) flushTile(acc, bi, bj, lane, n, visCol, H, mw.m);
         }
         if (gj >= 0) {
@@ -1252,11 +1252,352 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_fast(MargBatch M) {
 
 // Eigendecomposition of the separator information and the square-root prior,
 // rows in ascending eigenvalue order.
+// ---------------------------------------------------------------------------------------
+// Eigen path by the tridiagonal form, one CTA per window the fast path left:
+//   1. Householder tridiagonalization E = Q T Q^T, keeping each reflector
+//      H_k = I - tau_k v_k v_k^T (v_k in column k below the subdiagonal);
+//   2. implicit QL iterations with Wilkinson shifts on T (the QL algorithm of
+//      Bowdler, Martin, Reinsch and Wilkinson, Handbook for Automatic
+//      Computation vol. II, 1971).  QL converges fastest when T grows toward
+//      its bottom; a separator's tridiagonal form usually ends in its near-null
+//      directions, so T is flipped (T' = P T P, P the reversal) when its top
+//      diagonal entry is the larger end, as LAPACK's steqr picks QL or QR.  An
+//      off-diagonal e_i is negligible when e_i^2 <= eps^2 |T| (|d_i| + |d_i+1|),
+//      between the absolute test (eps |T|) and the relative one (eps |d|):
+//      eigenvalues keep an absolute error of order eps |T|, as the reference's
+//      own solver does, and the near-null cluster deflates in a few sweeps
+//      (under the relative test alone it took up to 60 iterations for one
+//      eigenvalue).  Warp 0 runs the iterations: a ballot over 32 indices finds
+//      the block, lane 0 chases the bulge and logs its plane rotations into one
+//      of two buffers; meanwhile the other warps apply the previous iteration's
+//      rotations to the rows of V (thread per component, the running row in a
+//      register, the next rows loaded ahead), so a chase and the application of
+//      its predecessor overlap.  V stays orthogonal to rounding by construction;
+//   3. U = Q V by the reflectors in reverse order (warp per eigenvector).
+// Eigenvectors are kept as the rows of Vt (Vt[j n + r] = component r of
+// eigenvector j), so both the rotations (thread per component) and the
+// reflectors (lanes over components) touch consecutive addresses.  The prior
+// is then formed from (lambda, U) exactly as the Jacobi path does.
+// S and Vt live in shared memory up to kTriSmemN columns (when the launch's
+// shared memory holds them), else in the window's eigenvector scratch (S) and
+// in its separator information (Vt; E is copied into S first).  A window whose
+// QL does not converge within 60 iterations per eigenvalue (NaN entries never
+// converge) is left to the Jacobi kernel (fast[w] stays 0) when E is still
+// intact (shared memory), and fails with CGMLI_E_NONFINITE otherwise.
+constexpr int kTriSmemN = 110;
+constexpr int kQlMaxIterations = 60;
+__host__ __device__ constexpr size_t triVecBytes(int n) { return sizeof(double) * 7 * (size_t)n; }  // d, e, tau, 2 x (cos, sin)
+__host__ __device__ constexpr size_t triSmemBytes(int n) {
+    return (n <= kTriSmemN ? sizeof(double) * 2 * (size_t)n * n : 0) + triVecBytes(n);
+}
+__global__ void __launch_bounds__(kEigenThreads) k_marg_tridiag(MargBatch M) {
+    const int w = M.bigFirst[blockIdx.x];
+    const MargWin mw = M.win[w];
+    const int n = mw.nr;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+    if (M.fast[w] || mw.m == 0 || n == 0 || n > kMargMaxSep || M.status[w] != CGMLI_OK) return;
+    extern __shared__ double tsm[];
+    const bool inShared = n <= kTriSmemN && (long long)triSmemBytes(n) <= M.triSmem;
+    double* S = inShared ? tsm : M.sepV + mw.sep0;          // n x n row-major
+    double* Vt = inShared ? tsm + (size_t)n * n : M.sepH + mw.sep0;
+    double* d = inShared ? tsm + 2 * (size_t)n * n : tsm;
+    double* e = d + n;
+    double* tau = e + n;
+    double* rc = tau + n;  // rotations of a QL chase (cos, sin; two buffers), also the reflector scratch
+    double* rs = rc + 2 * n;
+    __shared__ double sc[4];
+    __shared__ int isc[4];
+    __shared__ int qlMid[2], qlCount[2];  // per rotation buffer: the chase's block end m and its rotation count
+    __shared__ double red[kEigenThreads / 32];
+    __shared__ int pos[kMargMaxSep];
+    const double* E = M.sepH + mw.sep0;
+    for (long long t = tid; t < (long long)n * n; t += blockDim.x) S[t] = E[t];
+    __syncthreads();
+    // 1. tridiagonalization; the trailing block is updated on both triangles
+    for (int k = 0; k + 2 < n; ++k) {
+        const int m = n - k - 1;
+        double* v = rc;  // the reflector of this column
+        double* p = rs;
+        if (warp == 0) {
+            double sigma = 0;
+            for (int i = lane; i < m; i += 32) {
+                const double x = S[(size_t)(k + 1 + i) * n + k];
+                v[i] = x;
+                sigma += x * x;
+            }
+            sigma = mWarpSum(sigma);
+            __syncwarp();
+            if (lane == 0) {
+                d[k] = S[(size_t)k * n + k];
+                if (sigma == 0.0) {
+                    e[k] = 0.0;
+                    sc[0] = 0.0;
+                } else {
+                    const double x0 = v[0];
+                    const double alpha = x0 >= 0 ? -sqrt(sigma) : sqrt(sigma);
+                    e[k] = alpha;
+                    v[0] = x0 - alpha;
+                    sc[0] = 1.0 / (sigma - x0 * alpha);
+                }
+                tau[k] = sc[0];
+            }
+        }
+        __syncthreads();
+        const double tk = sc[0];
+        if (tk == 0.0) {
+            __syncthreads();  // every warp has read sc before warp 0 writes the next column's
+            continue;
+        }
+        for (int i = warp; i < m; i += nw) {  // p = tau S v over the trailing block
+            const double* row = S + (size_t)(k + 1 + i) * n + (k + 1);
+            double sum = 0;
+            for (int j = lane; j < m; j += 32) sum += row[j] * v[j];
+            sum = mWarpSum(sum);
+            if (lane == 0) p[i] = tk * sum;
+        }
+        __syncthreads();
+        if (warp == 0) {  // w = p - (tau p^T v / 2) v, kept in p
+            double pv = 0;
+            for (int i = lane; i < m; i += 32) pv += p[i] * v[i];
+            const double K = 0.5 * tk * mWarpSum(pv);
+            __syncwarp();
+            for (int i = lane; i < m; i += 32) p[i] -= K * v[i];
+        }
+        __syncthreads();
+        for (int i = warp; i < m; i += nw) {
+            double* row = S + (size_t)(k + 1 + i) * n + (k + 1);
+            const double vi = v[i], wi = p[i];
+            for (int j = lane; j < m; j += 32) row[j] -= vi * p[j] + wi * v[j];
+        }
+        __syncthreads();
+        for (int i = tid; i < m; i += blockDim.x) S[(size_t)(k + 1 + i) * n + k] = v[i];  // keep the reflector
+        __syncthreads();
+    }
+    if (tid == 0) {
+        if (n >= 2) {
+            d[n - 2] = S[(size_t)(n - 2) * n + (n - 2)];
+            e[n - 2] = S[(size_t)(n - 1) * n + (n - 2)];
+            tau[n - 2] = 0.0;
+        }
+        d[n - 1] = S[(size_t)(n - 1) * n + (n - 1)];
+        e[n - 1] = 0.0;
+        tau[n - 1] = 0.0;
+        double norm = 0;
+        for (int i = 0; i < n; ++i) norm = fmax(norm, fmax(fabs(d[i]), fabs(e[i])));
+        sc[1] = norm;
+        isc[3] = fabs(d[0]) > fabs(d[n - 1]) ? 1 : 0;
+    }
+    __syncthreads();
+    const bool flipped = isc[3] != 0;
+    const double deflation = DBL_EPSILON * DBL_EPSILON * sc[1];
+    if (flipped) {  // T' = P T P: d reversed, e reversed over its n - 1 couplings
+        for (int i = tid; i < n / 2; i += blockDim.x) {
+            const double t = d[i];
+            d[i] = d[n - 1 - i];
+            d[n - 1 - i] = t;
+        }
+        for (int i = tid; i < (n - 1) / 2; i += blockDim.x) {
+            const double t = e[i];
+            e[i] = e[n - 2 - i];
+            e[n - 2 - i] = t;
+        }
+    }
+    // V starts as the identity in T's coordinates: P itself when T was flipped
+    for (long long t = tid; t < (long long)n * n; t += blockDim.x) {
+        const int j = (int)(t / n), r = (int)(t % n);
+        Vt[t] = (flipped ? j + r == n - 1 : j == r) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    // 2. implicit QL; e[i] couples i and i + 1.  Step s: warp 0 runs one iteration into
+    // buffer s & 1 while the other warps apply the rotations of step s - 1.
+    int l = 0, iter = 0;  // warp 0's position (uniform over the warp)
+    int qlEnd = 0;        // -1: converged, -2: an eigenvalue did not converge
+    for (int step = 0;; ++step) {
+        const int b = step & 1;
+        if (warp == 0) {
+            int m = l, count = -1;
+            while (l < n) {  // the first negligible coupling at or after l (n - 1: none)
+                for (int base = l;; base += 32) {
+                    const int i = base + lane;
+                    bool negligible = i >= n - 1;
+                    if (!negligible) {
+                        const double ei = e[i];
+                        negligible = fabs(ei) < DBL_MIN || ei * ei <= deflation * (fabs(d[i]) + fabs(d[i + 1]));
+                    }
+                    const unsigned hit = __ballot_sync(0xffffffffu, negligible);
+                    if (hit) {
+                        m = base + __ffs(hit) - 1;
+                        break;
+                    }
+                }
+                if (m != l) break;
+                ++l;  // d[l] is an eigenvalue
+                iter = 0;
+            }
+            if (l < n) {
+                if (iter >= kQlMaxIterations) {
+                    count = -2;
+                } else {
+                    if (lane == 0) {  // chase the bulge from m up to l, logging each rotation
+                        double* cb = rc + b * n;
+                        double* sb = rs + b * n;
+                        double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+                        double r = hypot(g, 1.0);
+                        g = d[m] - d[l] + e[l] / (g + (g >= 0 ? r : -r));
+                        double s = 1.0, c = 1.0, p = 0.0;
+                        bool split = false;
+                        count = 0;
+                        for (int i = m - 1; i >= l; --i) {
+                            const double f = s * e[i], bq = c * e[i];
+                            const double q = f * f + g * g;
+                            if (q > 1e-280 && q < 1e280) {  // one reciprocal square root for r, c and s
+                                const double rq = rsqrt(q);
+                                r = q * rq;
+                                s = f * rq;
+                                c = g * rq;
+                            } else {
+                                r = hypot(f, g);
+                                if (r != 0.0) {
+                                    s = f / r;
+                                    c = g / r;
+                                }
+                            }
+                            e[i + 1] = r;
+                            if (r == 0.0) {  // the bulge vanished: deflate and restart the chase
+                                d[i + 1] -= p;
+                                e[m] = 0.0;
+                                split = true;
+                                break;
+                            }
+                            g = d[i + 1] - p;
+                            r = (d[i] - g) * s + 2.0 * c * bq;
+                            p = s * r;
+                            d[i + 1] = g + p;
+                            g = c * r - bq;
+                            cb[count] = c;
+                            sb[count] = s;
+                            ++count;
+                        }
+                        if (!split) {
+                            d[l] -= p;
+                            e[l] = g;
+                            e[m] = 0.0;
+                        }
+                    }
+                    count = __shfl_sync(0xffffffffu, count, 0);
+                    ++iter;
+                    __syncwarp();  // lane 0's d, e before the next scan
+                }
+            }
+            if (lane == 0) {
+                qlMid[b] = m;
+                qlCount[b] = count;
+            }
+        } else if (step > 0) {
+            // rotation q of the previous chase acts on rows (m - 1 - q, m - q) of V
+            const int pb = b ^ 1, m = qlMid[pb], count = qlCount[pb];
+            const double* cb = rc + pb * n;
+            const double* sb = rs + pb * n;
+            for (int r = tid - 32; count > 0 && r < n; r += blockDim.x - 32) {
+                double carry = Vt[(size_t)m * n + r];
+                int q = 0;
+                for (; q + 8 <= count; q += 8) {
+                    double a[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) a[u] = Vt[(size_t)(m - 1 - q - u) * n + r];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        const double c = cb[q + u], s = sb[q + u];
+                        Vt[(size_t)(m - q - u) * n + r] = s * a[u] + c * carry;
+                        carry = c * a[u] - s * carry;
+                    }
+                }
+                for (; q < count; ++q) {
+                    const double a = Vt[(size_t)(m - 1 - q) * n + r];
+                    const double c = cb[q], s = sb[q];
+                    Vt[(size_t)(m - q) * n + r] = s * a + c * carry;
+                    carry = c * a - s * carry;
+                }
+                Vt[(size_t)(m - count) * n + r] = carry;
+            }
+        }
+        __syncthreads();
+        // the buffer written in this step is rewritten two steps on, after another barrier
+        if (qlCount[b] < 0) {
+            qlEnd = qlCount[b];
+            break;
+        }
+    }
+    if (qlEnd == -2) {  // not converged (uniform): the Jacobi kernel takes the window while E is intact
+        if (!inShared && tid == 0) { M.status[w] = CGMLI_E_NONFINITE; M.rank[w] = 0; M.fast[w] = 3; }
+        return;
+    }
+    // 3. U = Q V: H_k acts on components k + 1.. of every eigenvector, for k = n - 3 down to 0
+    for (int k = n - 3; k >= 0; --k) {
+        const double tk = tau[k];
+        if (tk == 0.0) continue;  // uniform
+        const int m = n - k - 1;
+        for (int i = tid; i < m; i += blockDim.x) rc[i] = S[(size_t)(k + 1 + i) * n + k];
+        __syncthreads();
+        for (int j = warp; j < n; j += nw) {
+            double* u = Vt + (size_t)j * n + (k + 1);
+            double z = 0;
+            for (int i = lane; i < m; i += 32) z += rc[i] * u[i];
+            z = tk * mWarpSum(z);
+            for (int i = lane; i < m; i += 32) u[i] -= z * rc[i];
+        }
+        __syncthreads();
+    }
+    // the prior from (lambda, U) as the Jacobi path forms it; eigenvector i is column i of V
+    double* ev = M.evals + mw.vec0;
+    const double* bs = M.sepB + mw.vec0;
+    for (int i = tid; i < n; i += blockDim.x) ev[i] = d[i];
+    __syncthreads();
+    double vmax = -INFINITY, vmin = INFINITY;
+    bool finite = true;
+    for (int i = tid; i < n; i += blockDim.x) {
+        vmax = fmax(vmax, ev[i]);
+        vmin = fmin(vmin, ev[i]);
+        finite = finite && isfinite(ev[i]);
+    }
+    vmax = mBlockMax(vmax, red);
+    vmin = -mBlockMax(-vmin, red);
+    const double nonFinite = mBlockMax(finite ? 0.0 : 1.0, red);
+    const double cutoff = fmax(1e-12, 1e-9 * fmax(0.0, vmax));
+    if (nonFinite > 0 || vmin < -10 * cutoff) {
+        if (tid == 0) { M.status[w] = nonFinite > 0 ? CGMLI_E_NONFINITE : CGMLI_E_INDEFINITE; M.rank[w] = 0; M.fast[w] = 3; }
+        return;
+    }
+    ascendingPositions(ev, n, pos);
+    double low = 0;
+    for (int i = tid; i < n; i += blockDim.x) low += ev[i] > cutoff ? 0.0 : 1.0;
+    const int nLow = (int)mBlockSum(low, red);
+    double* A = M.A + mw.sep0;
+    double* r0 = M.r0 + mw.vec0;
+    for (long long t = tid; t < (long long)n * n; t += blockDim.x) {
+        const int i = (int)(t / n), k = (int)(t % n);  // eigenpair i, component k
+        if (!(ev[i] > cutoff)) continue;
+        A[(long long)(pos[i] - nLow) * n + k] = sqrt(ev[i]) * Vt[t];
+    }
+    for (int i = warp; i < n; i += nw) {
+        if (!(ev[i] > cutoff)) continue;  // uniform over the warp
+        double ub = 0;
+        for (int k = lane; k < n; k += 32) ub += Vt[(size_t)i * n + k] * bs[k];
+        ub = mWarpSum(ub);
+        if (lane == 0) r0[pos[i] - nLow] = ub / sqrt(ev[i]);
+    }
+    if (tid == 0) {
+        M.rank[w] = n - nLow;
+        M.stats[4 * w + 3] = cutoff;
+        M.fast[w] = 3;  // formed here: the Jacobi kernel skips the window
+    }
+}
+
 __global__ void __launch_bounds__(kEigenThreads) k_marg_eigen(MargBatch M) {
     const int w = M.bigFirst[blockIdx.x];
     const MargWin mw = M.win[w];
     const int nr = mw.nr;
-    if (M.fast[w]) return;  // prior formed by k_marg_fast
+    if (M.fast[w]) return;  // prior formed by k_marg_fast or k_marg_tridiag
     if (mw.m == 0 || nr == 0 || M.status[w] != CGMLI_OK) {
         if (threadIdx.x == 0) M.rank[w] = 0;
         return;
@@ -1599,7 +1940,7 @@ size_t margRowsSmemBytes(int maxNv) {
 }
 int margRowsCap(int nv) { return rowsCapOf((nv + 31) & ~31); }
 cudaError_t configureMarginalization(size_t visualSmem, size_t rowsSmem, int maxNr, int maxFastNr, long long* eigenSmem,
-                                     long long* fastSmem) {
+                                     long long* fastSmem, long long* triSmem) {
     cudaError_t e = cudaFuncSetAttribute(k_marg_visual, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)visualSmem);
     if (e != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_marg_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rowsSmem)) != cudaSuccess)
@@ -1621,7 +1962,14 @@ cudaError_t configureMarginalization(size_t visualSmem, size_t rowsSmem, int max
     long long use = want <= avail ? want : (packedOnly <= avail ? packedOnly : 0);
     if (use < 0) use = 0;
     *eigenSmem = use;
-    return cudaFuncSetAttribute(k_marg_eigen, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)use);
+    if ((e = cudaFuncSetAttribute(k_marg_eigen, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)use)) != cudaSuccess) return e;
+    cudaFuncAttributes ta;
+    if ((e = cudaFuncGetAttributes(&ta, k_marg_tridiag)) != cudaSuccess) return e;
+    // windows up to kTriSmemN columns in shared memory, the vectors of the widest one
+    const int triN = maxNr < 1 ? 1 : (maxNr > kMargMaxSep ? kMargMaxSep : maxNr);
+    *triSmem = (long long)std::max(triSmemBytes(triN < kTriSmemN ? triN : kTriSmemN), triVecBytes(triN));
+    if (*triSmem > (long long)optin - (long long)ta.sharedSizeBytes) return cudaErrorInvalidValue;
+    return cudaFuncSetAttribute(k_marg_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<long long>(*triSmem, 1));
 }
 // Returns the number of launches.
 // Rotations of the accepted state (the factors' inputs), one thread per keyframe or extrinsic.
@@ -1649,8 +1997,9 @@ int launchMarginalization(const DevBatch& B, const MargBatch& M, size_t visualSm
     k_marg_retained<<<M.numWindows, 256, 0, s>>>(B, M);
     k_marg_victim<<<M.numWindows, kMargThreads, 0, s>>>(M);
     k_marg_fast<<<M.numWindows, kMargThreads, (size_t)M.fastSmem, s>>>(M);
+    k_marg_tridiag<<<M.numWindows, kEigenThreads, (size_t)M.triSmem, s>>>(M);
     k_marg_eigen<<<M.numWindows, kEigenThreads, (size_t)M.eigenSmem, s>>>(M);
-    return n + 4;
+    return n + 5;
 }
 
 int launchCalibration(const DevBatch& B, const MargBatch& M, size_t visualSmem, double* work, const long long* work0, double* cond,

@@ -162,6 +162,8 @@ struct PlanParams {
     int runLandmarks = 0;  // 0: from the batch size
     int pairChunk = 32;
     int schurRows = kSchurMaxRows;
+    int linShape = 0;      // kLinShapeTable entry of the landmark pass
+    int trialShape = 0;    // kTrialShapeTable entry of the trial pass
 };
 
 struct HostBatch {

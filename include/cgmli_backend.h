@@ -136,11 +136,12 @@ typedef struct cgmli_window {
 
 typedef struct cgmli_solver_options {
     int precision;           /* CGMLI_PRECISION_FP64 (default) or _MIXED: the LM linearization
-                                evaluates the bearing factors' Jacobians and robust weights
-                                in FP32 and sums the landmark Hessian blocks (d, cross
-                                vectors) in compensated FP32; residuals, costs, gradients,
-                                the reduced system, its Cholesky and every marginalization
-                                stay FP64 */
+                                rounds the bearing factors' Jacobian blocks over the pose,
+                                extrinsic and td columns and their robust weights to FP32
+                                once formed, and stages the weighted rows of the J^T J pass
+                                in FP32; residuals, the depth derivative, costs, gradients,
+                                the landmark sums, the reduced system, its Cholesky and every
+                                marginalization stay FP64 */
     int refinement_steps;    /* iterative refinement after the FP64 Cholesky (0..2) */
     double initial_lambda;   /* reference: 1e-4 */
     int min_iterations;      /* iterations a window always runs before the time budget may stop it
@@ -177,13 +178,18 @@ void cgmli_default_options(cgmli_solver_options *options);
  * reference. */
 int cgmli_topology_check(const cgmli_window *windows, int count, int threads, double *seconds);
 
-/* Work decomposition of a batch (the kernels' tile shapes are fixed; these are
- * the shapes of the work units the host planner cuts for them). */
+/* Work decomposition of a batch and the kernel shapes it is launched with: the
+ * work units the host planner cuts, and the compiled variants of the landmark
+ * and trial passes (warps per CTA, and the CTAs per SM their register budget is
+ * compiled for). */
 typedef struct cgmli_tuning {
     int run_landmarks;  /* landmarks per warp run of the linearization and trial passes;
                            0: from the batch size (enough runs to fill the GPU) */
     int pair_chunk;     /* key-ordered observations per warp of the J^T J pass, 8..1024 (0: 32) */
     int schur_rows;     /* landmarks per chunk of the Schur pass, 8..128 (0: 128) */
+    int lin_shape;      /* landmark pass: 0: 6 warps x 2 CTAs per SM (168 registers), 1: 8 x 1 (255),
+                           2: 4 x 3 (168), 3: 6 x 1 (255) */
+    int trial_shape;    /* trial pass: 0: 8 warps x 2 CTAs per SM (128 registers), 1: 8 x 1 (255), 2: 4 x 4 (128) */
     double ms;          /* cgmli_solver_autotune: device time of the timed solve */
 } cgmli_tuning;
 /* cgmli_topology_check with a given work decomposition (NULL: the default). */
@@ -202,11 +208,12 @@ void cgmli_solver_destroy(cgmli_solver *solver);
  * CGMLI_E_INVALID outside the ranges of cgmli_tuning) and the one in use. */
 int cgmli_solver_set_tuning(cgmli_solver *solver, const cgmli_tuning *tuning);
 int cgmli_solver_get_tuning(cgmli_solver *solver, cgmli_tuning *tuning);
-/* Autotuner: builds the batch with candidate work decompositions (coordinate
- * search over run_landmarks, pair_chunk and schur_rows from the current one),
- * times `iterations` LM iterations of each from the windows' states on the
- * device, keeps the fastest for later set_windows calls and leaves the batch
- * set with it (states as given).  *best (may be NULL) receives it. */
+/* Autotuner: builds the batch with candidate work decompositions and kernel
+ * shapes (coordinate search over run_landmarks, pair_chunk and schur_rows from
+ * the current ones, then every lin_shape and trial_shape), times `iterations` LM
+ * iterations of each from the windows' states on the device, keeps the fastest
+ * for later set_windows calls and leaves the batch set with it (states as
+ * given).  *best (may be NULL) receives it. */
 int cgmli_solver_autotune(cgmli_solver *solver, const cgmli_window *windows, int count, int iterations, cgmli_tuning *best);
 int cgmli_solver_set_windows(cgmli_solver *solver, const cgmli_window *windows, int count);
 /* Upload new state values only (same topology). */

@@ -256,17 +256,17 @@ def test_graph_replay_matches_eager(backend):
 
 
 def test_tuning_keeps_the_step(backend):
-    """A work decomposition changes only how the passes split their work: the
-    step equals the default decomposition's (atomic reduction order aside)."""
+    """A work decomposition or kernel shape changes only how the passes split their
+    work: the step equals the default's (atomic reduction order aside)."""
     windows = synth.make_windows("c4", 16, seed=71)
     ref = backend.Solver()
     ref.set_windows(windows)
     ref.step(1e-4)
-    for tuning in ((3, 128, 16), (64, 8, 128)):
+    for tuning in ((3, 128, 16, 1, 1), (64, 8, 128, 2, 2), (8, 32, 64, 3, 0)):
         s = backend.Solver()
         s.set_tuning(*tuning)
         s.set_windows(windows)
-        assert s.get_tuning() == dict(zip(("run_landmarks", "pair_chunk", "schur_rows"), tuning))
+        assert s.get_tuning() == dict(zip(("run_landmarks", "pair_chunk", "schur_rows", "lin_shape", "trial_shape"), tuning))
         s.step(1e-4)
         for i in range(len(windows)):
             a, b = s.read_step(i), ref.read_step(i)
@@ -280,7 +280,8 @@ def test_autotune(backend):
     best = s.autotune(windows, 2)
     assert best["ms"] > 0 and best["run_landmarks"] >= 2
     assert 8 <= best["pair_chunk"] <= 1024 and 8 <= best["schur_rows"] <= 128
-    assert s.get_tuning() == {k: best[k] for k in ("run_landmarks", "pair_chunk", "schur_rows")}
+    assert 0 <= best["lin_shape"] <= 3 and 0 <= best["trial_shape"] <= 2
+    assert s.get_tuning() == {k: best[k] for k in ("run_landmarks", "pair_chunk", "schur_rows", "lin_shape", "trial_shape")}
     # the batch is left set with the chosen decomposition and the given states
     ref = backend.Solver()
     ref.set_windows(windows)

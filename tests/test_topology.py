@@ -75,7 +75,7 @@ def test_window_above_visual_limit_is_rejected(lib):
     assert code == 9  # CGMLI_E_LIMIT
 
 
-@pytest.mark.parametrize("tuning", [(2, 8, 8), (8, 64, 32), (64, 1024, 128), (0, 0, 0), (4096, 128, 16)])
+@pytest.mark.parametrize("tuning", [(2, 8, 8, 0, 0), (8, 64, 32, 1, 2), (64, 1024, 128, 3, 1), (0, 0, 0, 2, 0), (4096, 128, 16, 0, 0)])
 def test_tuned_layout(lib, tuning):
     """Every work decomposition the autotuner may pick keeps the invariants
     (runs cover each landmark once, pair chunks and Schur chunks within their
@@ -87,7 +87,8 @@ def test_tuned_layout(lib, tuning):
     assert code == 0, lib.cgmli_last_error().decode()
 
 
-@pytest.mark.parametrize("tuning", [(-1, 32, 128), (0, 4, 128), (0, 2048, 128), (0, 32, 4), (0, 32, 256)])
+@pytest.mark.parametrize("tuning", [(-1, 32, 128, 0, 0), (0, 4, 128, 0, 0), (0, 2048, 128, 0, 0), (0, 32, 4, 0, 0), (0, 32, 256, 0, 0),
+                                    (0, 32, 128, 4, 0), (0, 32, 128, 0, 3), (0, 32, 128, -1, 0)])
 def test_tuning_outside_its_ranges_is_rejected(lib, tuning):
     windows = synth.make_windows("c4", 2, seed=3)
     arr = synth.window_array(windows)
