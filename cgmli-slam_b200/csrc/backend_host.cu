@@ -27,7 +27,9 @@
 namespace cgmli {
 size_t linearizeSmemBytes(int maxNs, bool mixed);
 size_t factorSmemBytes(int maxNr);
-cudaError_t configureKernels(size_t linSmem, size_t facSmem);
+size_t widePanelSmemBytes(int maxNr);
+size_t wideFinishSmemBytes(int maxNr);
+cudaError_t configureKernels(size_t linSmem, size_t facSmem, size_t wideSmem);
 int launchIteration(const DevBatch& B, const LaunchPlan& P, int refinement, int maxIterations, int probe, double* Sdebug,
                     cudaStream_t s, LaunchHook hook, void* ctx);
 int launchIterationParts(const DevBatch& B, const LaunchPlan& P, int refinement, int maxIterations, int probe, double* Sdebug,
@@ -120,6 +122,12 @@ struct cgmli_solver {
     std::vector<WinDesc> win;
     int maxNpc = 0, maxNr = 0, maxNs = 1;
     size_t linSmem = 0, facSmem = 0;
+    // wide windows (isWideWindow): factored by the multi-launch sequence
+    int numWide = 0, wideCols = 0, wideCharts = 0;
+    size_t widePanelSmem = 0, wideFinishSmem = 0;
+    HVec<int> hWideList;
+    DArray<int> wideList, facFailed;
+    DArray<double> facVec;
     int totalKf = 0, totalExt = 0, totalCam = 0, totalLm = 0, totalObs = 0, totalImu = 0;
     // device arrays
     DArray<WinDesc> dWin;
@@ -255,7 +263,7 @@ struct cgmli_solver {
         add(dMargWin, dMargElim, margCols, margObsMap, margPoseCol, margSbCol, margExtCol, margRank, margStatus, margFast, margVisCol,
             margVisPose, margVisExt, margSlow, margChunks, margItems, margH, margB, margSepH, margSepV, margSepB, margEvals, margA,
             margR0, margX, margMaxD, margStats, dMargOrder);
-        add(colChart, lmFixed, evalOut, evalValid, hostH, hostG, hostCost, hostFlag);
+        add(colChart, lmFixed, evalOut, evalValid, hostH, hostG, hostCost, hostFlag, wideList, facFailed, facVec);
         add(obRejected, gateCounts, gateStats, imuTimes, imuT0, imuT1, imuReadings, imuRanges, imuStatus, imuRefreshed,
             imuRefreshScratch, mergeRange, mergeKf, mergeStatus, mergeFlag, mergeT0, mergeT1, mergeOut, calibWork0, calibWork, calibCond,
             calibEvals, snapPose, snapSb, snapExt, snapTd, snapRho);
@@ -268,6 +276,8 @@ struct cgmli_solver {
         P.schurChunks = dSchurChunks.p; P.numSchurChunks = (int)hb.schurChunks.size();
         P.facSmem = facSmem; P.maxNs = maxNs;
         P.linShape = hb.plan.linShape; P.trialShape = hb.plan.trialShape;
+        P.numWide = numWide; P.wideCols = wideCols; P.wideCharts = wideCharts;
+        P.widePanelSmem = widePanelSmem; P.wideFinishSmem = wideFinishSmem;
         return P;
     }
     void collectKernelTimes() {
@@ -298,6 +308,7 @@ struct cgmli_solver {
         lmC0.release(); dWin.release(); dLm.release(); dRuns.release(); dTiles.release();
         dPairChunks.release(); dSchurChunks.release(); schurCols.release(); lmUmap.release(); obLm.release(); keyOrder.release(); bigFirst.release(); keyRows.release(); sch.release();
         snapPose.release(); snapSb.release(); snapExt.release(); snapTd.release(); snapRho.release();
+        wideList.release(); facFailed.release(); facVec.release();
         imuTimes.release(); imuT0.release(); imuT1.release(); imuReadings.release(); imuRanges.release(); imuStatus.release();
         imuRefreshed.release(); imuRefreshScratch.release();
         obRejected.release(); gateCounts.release(); gateStats.release();
@@ -457,8 +468,30 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     S->totalObs = hb.totalObs; S->totalImu = hb.totalImu;
     S->maxNpc = hb.maxNpc; S->maxNr = hb.maxNr; S->maxNs = hb.maxNs;
     S->linSmem = linearizeSmemBytes(S->maxNs, S->opt.precision == CGMLI_PRECISION_MIXED);
-    S->facSmem = factorSmemBytes(S->maxNr);
-    CK(configureKernels(S->linSmem, S->facSmem));
+    {
+        // windows of at least kWideCols retained columns take the wide sequence; k_factor's
+        // shared memory is sized by the others
+        int narrow = 0, wide = 0;
+        for (int i = 0; i < count; ++i) wide += isWideWindow(S->win[i].Nr) ? 1 : 0;
+        auto& wl = S->hWideList;
+        sizeTo(wl, wide);  // pinned staging: the upload stays asynchronous
+        S->wideCols = 0; S->wideCharts = 0;
+        for (int i = 0, k = 0; i < count; ++i) {
+            const WinDesc& d = S->win[i];
+            if (isWideWindow(d.Nr)) {
+                wl[k++] = i;
+                S->wideCols = std::max(S->wideCols, d.Nr);
+                S->wideCharts |= d.charts ? 1 : 0;
+            } else {
+                narrow = std::max(narrow, d.Nr);
+            }
+        }
+        S->numWide = wide;
+        S->facSmem = factorSmemBytes(narrow);
+        S->widePanelSmem = S->numWide ? widePanelSmemBytes(S->wideCols) : 0;
+        S->wideFinishSmem = S->numWide ? wideFinishSmemBytes(S->wideCols) : 0;
+    }
+    CK(configureKernels(S->linSmem, S->facSmem, std::max(S->widePanelSmem, S->wideFinishSmem)));
     const long long lm = hb.totalLm;
     S->hWin.assign(S->win.begin(), S->win.end());  // pinned staging: the copy stays asynchronous
     CK(S->dWin.upload(S->hWin, st));
@@ -497,6 +530,11 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     CK(S->lmValid.reserve(lm)); CK(S->lmTrialValid.reserve(lm));
     CK(S->Hret.reserve(hb.dense)); CK(S->Sglob.reserve(hb.dense)); CK(S->gret.reserve(hb.vec)); CK(S->dr.reserve(hb.vec));
     CK(S->rhs.reserve(hb.vec));
+    if (S->numWide) {
+        CK(S->wideList.upload(S->hWideList, st));
+        CK(S->facVec.reserve(3 * (size_t)hb.vec));
+        CK(S->facFailed.reserve(count));
+    }
     CK(S->acc.reserve(hb.acc)); CK(S->sch.reserve(hb.sch)); CK(S->imuScratch.reserve(hb.imuScratch));
     CK(S->priorScratch.reserve(hb.priorScratch));
     CK(S->costRet.reserve(count)); CK(S->trialRet.reserve(count)); CK(S->retValid.reserve(count));
@@ -534,6 +572,9 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     B.acc = S->acc.p; B.sch = S->sch.p; B.dr = S->dr.p; B.rhs = S->rhs.p; B.Sglob = S->Sglob.p;
     B.imuScratch = S->imuScratch.p; B.priorScratch = S->priorScratch.p; B.predState = S->predState.p;
     B.solveStatus = S->solveStatus.p; B.out = S->out.p;
+    B.wideList = S->numWide ? S->wideList.p : nullptr;
+    B.facVec = S->numWide ? S->facVec.p : nullptr;
+    B.facFailed = S->numWide ? S->facFailed.p : nullptr;
     CK(cudaMemsetAsync(S->costRet.p, 0, count * sizeof(double), st));
     CK(cudaMemsetAsync(S->trialRet.p, 0, count * sizeof(double), st));
     CK(S->obRejected.reserve(std::max(1, S->totalObs))); CK(S->gateCounts.reserve((size_t)kGateCounts * count));

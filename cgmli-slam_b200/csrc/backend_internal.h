@@ -21,6 +21,10 @@ constexpr int kMaxTrackChunk = 32;     // factors per warp pass
 constexpr int kMaxSupport = 64;        // keyframe slots per landmark
 constexpr int kLinThreads = 256;       // linearization CTA
 constexpr int kFactorThreads = 256;    // factorization CTA
+// Reduced systems of at least kWideCols columns are factored by the wide
+// sequence (several launches over the GPU) instead of one CTA per window.
+constexpr int kWideCols = 288;
+constexpr bool isWideWindow(int Nr) { return Nr >= kWideCols; }  // device code calls it too (relaxed constexpr)
 
 struct WinDesc {
     int K, E, C, L, F, nImu;
@@ -105,6 +109,11 @@ struct DevBatch {
     double* imuScratch; double* priorScratch;
     double* predState;
     int* solveStatus;
+    // wide windows (isWideWindow): their indices, x / undamped diagonal / damping
+    // (3 Nr per window at 3 vec0) and a factorization-failed flag per window
+    const int* wideList;
+    double* facVec;
+    int* facFailed;
     double* out;     // per-window scratch for read-back (costs)
 };
 
@@ -167,7 +176,8 @@ struct MargBatch {
     double* maxD;        // per window: largest eliminated landmark information
     double* stats;       // 4 per window: robust cost, whitened |r|^2, eliminated reduction, cutoff
     int* rank; int* status;
-    int* fast;           // per window: 1 when the fast path formed the prior, 3 the tridiagonal eigen path, 0 neither
+    int* fast;           // per window: 1 when the fast path formed the prior, 3 the tridiagonal eigen path, 0 neither;
+                         // 2 while the fast path's saved tridiagonal form waits for the eigen path
     // dense-row path
     double* rows;        // kMargRecord per eliminated observation (staged factor rows)
     const int* visCol;   // visual column -> marginalization column, per window from MargWin::vis0
@@ -213,8 +223,12 @@ struct LaunchPlan {
     const int4* schurChunks; // {window, first landmark, end landmark, -}: one CTA each
     int numSchurChunks;
     int maxNs;               // widest landmark support of the batch (local columns)
-    size_t facSmem;
+    size_t facSmem;          // k_factor (windows below kWideCols)
     int linShape, trialShape;  // kLinShapeTable / kTrialShapeTable entries
+    int numWide;             // wide windows (B.wideList)
+    int wideCols;            // largest wide Nr: panels and trailing tiles of the sequence
+    int wideCharts;          // some wide window has solve-time charts
+    size_t widePanelSmem, wideFinishSmem;
 };
 
 }  // namespace cgmli

@@ -93,7 +93,6 @@ __global__ void k_zero_acc(DevBatch B) {
 //                   a register-tiled FP64 SYRK (plus the B_v column)
 // Only k_lin_schur depends on lambda, so a rejected step re-runs it alone.
 constexpr int kCompact = 25;        // anchor pose 6 | observer pose 6 | ext_a 6 | ext_b 6 | td 1
-constexpr int kPairs = kCompact * (kCompact + 1) / 2;
 constexpr int kPairWarps = 4;       // warps per CTA of k_lin_pairs
 // A factor's FactorOut is staged per lane in shared memory with an odd stride
 // (conflict-free lane rows); slot 54 carries the squared robust weight.
@@ -880,145 +879,102 @@ __device__ __forceinline__ bool chartFixed(const DevBatch& B, const WinDesc& wd,
     return c == kColFixed || c == kColRotRho;
 }
 
-__global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int refinement, double* Sdebug) {
-    const int wdx = B.bigFirst[blockIdx.x];
-    if (B.lm[wdx].mode == kModeDone) return;
-    const WinDesc wd = B.win[wdx];
+// Damping lambda max(diag(H_total)_i, 1e-6) of retained column i.
+__device__ __forceinline__ double dampingOf(const DevBatch& B, const WinDesc& wd, int i, double lambda) {
+    double h = B.Hret[wd.dense0 + (long long)i * wd.Nr + i];
+    const int pi = pcOfRetained(i, wd.K);
+    if (pi >= 0) h += B.acc[wd.acc0 + upIdx(pi, pi, wd.Npc)];
+    return lambda * fmax(h, 1e-6);
+}
+
+// Right-hand side -(g_r - B_v) of retained column i.
+__device__ __forceinline__ double rhsOf(const DevBatch& B, const WinDesc& wd, int i) {
+    const long long nS = (long long)wd.Npc * (wd.Npc + 1) / 2;
+    const double* acc = B.acc + wd.acc0;
+    double g = B.gret[wd.vec0 + i];
+    const int p = pcOfRetained(i, wd.K);
+    if (p >= 0) g += acc[nS + wd.Npc + p] - acc[nS + 2ll * wd.Npc + p];
+    return -g;
+}
+
+// Left-looking factorization of one staged panel: P holds rows [0, m) of the
+// panel's bw columns (column-major, leading dimension mp); column c of every
+// row r >= c is reduced by one dot product against the panel's earlier columns,
+// then scaled by the root of its pivot.  The diagonal stays unscaled in P (its
+// root goes to A).  xp[0, bw) is forward-substituted on the way.  Returns false
+// (uniform over the CTA) when a pivot is not positive and finite.
+__device__ bool factorPanel(double* P, int mp, int m, int bw, double* xp, int* failed) {
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+    for (int c = 0; c < bw; ++c) {
+        for (int r = c + tid; r < m; r += blockDim.x) {
+            double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+            int k = 0;
+            for (; k + 4 <= c; k += 4) {
+                s0 += P[r + k * mp] * P[c + k * mp];
+                s1 += P[r + (k + 1) * mp] * P[c + (k + 1) * mp];
+                s2 += P[r + (k + 2) * mp] * P[c + (k + 2) * mp];
+                s3 += P[r + (k + 3) * mp] * P[c + (k + 3) * mp];
+            }
+            for (; k < c; ++k) s0 += P[r + k * mp] * P[c + k * mp];
+            P[r + c * mp] -= (s0 + s1) + (s2 + s3);
+        }
+        if (warp == nw - 1) {  // forward substitution: x_c - sum_{k<c} L[c][k] y_k
+            double t = lane < c ? P[c + lane * mp] * xp[lane] : 0.0;
+            t = warpSum(t);
+            if (lane == 0) xp[c] -= t;
+        }
+        __syncthreads();
+        const double d = P[c + c * mp];
+        if (!(d > 0) || !isfinite(d)) {
+            if (tid == 0) *failed = 1;
+            return false;  // uniform: every thread read the same d
+        }
+        const double l = sqrt(d);
+        for (int r = c + 1 + tid; r < m; r += blockDim.x) P[r + c * mp] /= l;
+        if (tid == 0) xp[c] /= l;
+        __syncthreads();
+    }
+    return true;
+}
+
+// The factored panel into A: L's columns (rows k0 + c.., the diagonal as its root).
+__device__ __forceinline__ void storePanel(const double* P, int mp, int m, int bw, double* A, int n, int k0) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int c = warp; c < bw; c += nw)
+        for (int r = c + lane; r < m; r += 32) A[(k0 + r) + (long long)(k0 + c) * n] = r == c ? sqrt(P[r + c * mp]) : P[r + c * mp];
+}
+
+// One 32 x 32 lower tile (row block rb >= column block cb) of the trailing update
+// A22 -= L21 L21^T after the panel at k0 (bw columns, m2 trailing rows), on the
+// FP64 tensor path.  V is L21 by panel column: V + k ldv is column k's rows.
+__device__ __forceinline__ void trailingTile(const double* V, long long ldv, int rb, int cb, int bw, int m2, double* A, int n, int k0) {
+    const int lane = threadIdx.x & 31;
+    double tacc[4][8];
+    zeroTile(tacc);
+    rankUpdateMma<false>(tacc, V, rb * 32, cb * 32, 0, bw, 1, (int)ldv);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int i = tileRowMma(rb, lane, r);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int j = tileCol(cb, lane, c);
+            if (i < m2 && j < m2 && i >= j) A[(k0 + bw + i) + (long long)(k0 + bw + j) * n] -= tacc[r][c];
+        }
+    }
+}
+
+// After the factorization (x = y = L^-1 rhs): the backward substitution, the
+// refinement steps against the assembled FP64 system and the predicted
+// reduction of the state part; writes dr, predState and solveStatus.  x, hd,
+// h (scratch), blk and dmp are the CTA's shared vectors.
+__device__ void factorTail(const DevBatch& B, const WinDesc& wd, int wdx, double lambda, int refinement, const double* A, double* x,
+                           const double* hd, double* h, double* blk, const double* dmp, double* red) {
     const int n = wd.Nr, Npc = wd.Npc, K = wd.K;
-    const double lambda = B.lm[wdx].lambda;
-    extern __shared__ __align__(16) double smem[];
-    const int npad = ((n + 31) & ~31) + kFacPanel;
-    double* P = smem;                        // npad x kFacPanel, column-major (leading dimension mp <= npad)
-    double* x = P + (size_t)npad * kFacPanel;  // n: right-hand side -> y -> increment
-    double* hd = x + n;                      // n: undamped diagonal
-    double* da = hd + n;                     // n: damping added to the diagonal; then the product h
-    double* blk = da + n;                    // kFacPanel x kFacPanel diagonal block (solves)
-    double* dmp = blk + kFacPanel * kFacPanel;  // n: damping of each column (solve-time charts only)
     const bool charts = wd.charts != 0;
-    __shared__ int failed;
-    __shared__ double red[32];
-    double* A = B.Sglob + wd.dense0;
     const double* acc = B.acc + wd.acc0;
     const long long nS = (long long)Npc * (Npc + 1) / 2;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    constexpr int nw = kFactorThreads / 32;
-    if (tid == 0) failed = 0;
-    for (int i = tid; i < n; i += blockDim.x) {
-        double h = B.Hret[wd.dense0 + (long long)i * n + i];
-        const int pi = pcOfRetained(i, K);
-        if (pi >= 0) h += acc[upIdx(pi, pi, Npc)];
-        da[i] = lambda * fmax(h, 1e-6);
-    }
-    __syncthreads();
-    // assembly: damped lower triangle (factored in place), undamped strict upper copy
-    for (int j = warp; j < n; j += nw)
-#pragma unroll 2
-    for (int i = j + lane; i < n; i += 32) {
-        const double v = assembleEntryCol(B, wd, i, j, lambda, false);
-        if (i == j) {
-            hd[i] = v;
-            A[i + (long long)j * n] = v + da[i];
-        } else {
-            A[i + (long long)j * n] = v;
-            A[j + (long long)i * n] = v;
-        }
-    }
-    double* rhsOut = B.rhs + wd.vec0;
-    for (int i = tid; i < n; i += blockDim.x) {
-        double g = B.gret[wd.vec0 + i];
-        const int p = pcOfRetained(i, K);
-        if (p >= 0) g += acc[nS + Npc + p] - acc[nS + 2ll * Npc + p];
-        x[i] = -g;
-        rhsOut[i] = -g;
-        if (charts) dmp[i] = da[i];
-    }
-    __syncthreads();
-    if (charts) {
-        chartSystem(B, wd, lambda, n, A, x, hd, dmp);
-        for (int i = tid; i < n; i += blockDim.x) rhsOut[i] = x[i];  // the restricted right-hand side
-        __syncthreads();
-    }
-    if (Sdebug)  // the damped system as it is factored (lower triangle), stored symmetric and row-major
-        for (long long t = tid; t < (long long)n * n; t += blockDim.x) {
-            const int r = (int)(t / n), c = (int)(t % n);
-            Sdebug[wd.dense0 + t] = r >= c ? A[r + (long long)c * n] : A[c + (long long)r * n];
-        }
-    // ---- factorization with the forward substitution
-    for (int k0 = 0; k0 < n; k0 += kFacPanel) {
-        // rows padded so that the trailing rows [bw, mp) are whole 32-row tiles
-        const int bw = min(kFacPanel, n - k0), m = n - k0, mp = bw + ((m - bw + 31) & ~31);
-        for (int t = tid; t < mp * kFacPanel; t += blockDim.x) {
-            const int c = t / mp, r = t % mp;
-            P[r + c * mp] = (c < bw && r < m && r >= c) ? A[(k0 + r) + (long long)(k0 + c) * n] : 0.0;
-        }
-        __syncthreads();
-        for (int c = 0; c < bw; ++c) {
-            // column c of every row r >= c, less its products with the panel's earlier columns
-            for (int r = c + tid; r < m; r += blockDim.x) {
-                double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-                int k = 0;
-                for (; k + 4 <= c; k += 4) {
-                    s0 += P[r + k * mp] * P[c + k * mp];
-                    s1 += P[r + (k + 1) * mp] * P[c + (k + 1) * mp];
-                    s2 += P[r + (k + 2) * mp] * P[c + (k + 2) * mp];
-                    s3 += P[r + (k + 3) * mp] * P[c + (k + 3) * mp];
-                }
-                for (; k < c; ++k) s0 += P[r + k * mp] * P[c + k * mp];
-                P[r + c * mp] -= (s0 + s1) + (s2 + s3);
-            }
-            if (warp == nw - 1) {  // forward substitution: x_c - sum_{k<c} L[c][k] y_k
-                double t = lane < c ? P[c + lane * mp] * x[k0 + lane] : 0.0;
-                t = warpSum(t);
-                if (lane == 0) x[k0 + c] -= t;
-            }
-            __syncthreads();
-            const double d = P[c + c * mp];  // the diagonal stays unscaled here; its root goes to A
-            if (!(d > 0) || !isfinite(d)) {
-                if (tid == 0) failed = 1;
-                break;  // uniform: every thread read the same d
-            }
-            const double l = sqrt(d);
-            for (int r = c + 1 + tid; r < m; r += blockDim.x) P[r + c * mp] /= l;
-            if (tid == 0) x[k0 + c] /= l;
-            __syncthreads();
-        }
-        __syncthreads();
-        if (failed) break;
-        for (int c = warp; c < bw; c += nw)
-            for (int r = c + lane; r < m; r += 32) A[(k0 + r) + (long long)(k0 + c) * n] = r == c ? sqrt(P[r + c * mp]) : P[r + c * mp];
-        const int m2 = m - bw;
-        if (m2 > 0) {
-            // A22 -= L21 L21^T over the lower tiles of the m2 x m2 trailing block
-            const int nb2 = (m2 + 31) >> 5, tiles = nb2 * (nb2 + 1) / 2;
-            for (int t = warp; t < tiles; t += nw) {
-                int cb, rb;
-                tileOf(t, nb2, cb, rb);  // upper enumeration (cb <= rb): rows rb, columns cb
-                double tacc[4][8];
-                zeroTile(tacc);
-                rankUpdateMma<false>(tacc, P + bw, rb * 32, cb * 32, 0, bw, 1, mp);
-#pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    const int i = tileRowMma(rb, lane, r);
-#pragma unroll
-                    for (int c = 0; c < 8; ++c) {
-                        const int j = tileCol(cb, lane, c);
-                        if (i < m2 && j < m2 && i >= j) A[(k0 + bw + i) + (long long)(k0 + bw + j) * n] -= tacc[r][c];
-                    }
-                }
-            }
-            // right-hand side below the panel: y2 -= L21 y1
-            for (int i = tid; i < m2; i += blockDim.x) {
-                double s = 0;
-                for (int c = 0; c < bw; ++c) s += P[bw + i + c * mp] * x[k0 + c];
-                x[k0 + bw + i] -= s;
-            }
-        }
-        __syncthreads();
-    }
-    if (failed) {
-        if (tid == 0) B.solveStatus[wdx] = CGMLI_E_NOT_PD;
-        return;
-    }
+    const double* rhsOut = B.rhs + wd.vec0;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
     // ---- backward substitution L^T x = y by panels (L lower in A)
     for (int k0 = ((n - 1) / kFacPanel) * kFacPanel; k0 >= 0; k0 -= kFacPanel) {
         const int bw = min(kFacPanel, n - k0);
@@ -1047,7 +1003,6 @@ __global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int re
     double* dr = B.dr + wd.vec0;
     for (int i = tid; i < n; i += blockDim.x) dr[i] = x[i];
     __syncthreads();
-    double* h = da;  // the damping is folded back below where needed
     // ---- iterative refinement against the assembled FP64 system
     for (int it = 0; it < refinement; ++it) {
         if (charts) {
@@ -1059,20 +1014,10 @@ __global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int re
             __syncthreads();
             continue;
         }
-        for (int i = tid; i < n; i += blockDim.x) {
-            const int pi = pcOfRetained(i, K);
-            double hh = B.Hret[wd.dense0 + (long long)i * n + i];
-            if (pi >= 0) hh += acc[upIdx(pi, pi, Npc)];
-            x[i] = lambda * fmax(hh, 1e-6);  // damping of row i, kept in x for this pass
-        }
+        for (int i = tid; i < n; i += blockDim.x) x[i] = dampingOf(B, wd, i, lambda);  // damping of row i, kept in x for this pass
         __syncthreads();
         undampedProduct(A, hd, n, dr, h);
-        for (int i = tid; i < n; i += blockDim.x) {
-            double g = B.gret[wd.vec0 + i];
-            const int p = pcOfRetained(i, K);
-            if (p >= 0) g += acc[nS + Npc + p] - acc[nS + 2ll * Npc + p];
-            x[i] = -g - (h[i] + x[i] * dr[i]);
-        }
+        for (int i = tid; i < n; i += blockDim.x) x[i] = rhsOf(B, wd, i) - (h[i] + x[i] * dr[i]);
         __syncthreads();
         blockedSolve(A, n, x, blk);
         for (int i = tid; i < n; i += blockDim.x) dr[i] += x[i];
@@ -1113,6 +1058,237 @@ __global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int re
         }
     }
     if (tid == 0) { B.predState[wdx] = pred; B.solveStatus[wdx] = CGMLI_OK; }
+}
+
+// The damped system as it is factored (lower triangle), stored symmetric and row-major.
+__device__ __forceinline__ void storeSdebug(const double* A, int n, double* out) {
+    for (long long t = threadIdx.x; t < (long long)n * n; t += blockDim.x) {
+        const int r = (int)(t / n), c = (int)(t % n);
+        out[t] = r >= c ? A[r + (long long)c * n] : A[c + (long long)r * n];
+    }
+}
+
+__global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int refinement, double* Sdebug) {
+    const int wdx = B.bigFirst[blockIdx.x];
+    if (B.lm[wdx].mode == kModeDone) return;
+    const WinDesc wd = B.win[wdx];
+    const int n = wd.Nr;
+    if (isWideWindow(n)) return;  // factored by the wide sequence (k_wide_*)
+    const double lambda = B.lm[wdx].lambda;
+    extern __shared__ __align__(16) double smem[];
+    const int npad = ((n + 31) & ~31) + kFacPanel;
+    double* P = smem;                        // npad x kFacPanel, column-major (leading dimension mp <= npad)
+    double* x = P + (size_t)npad * kFacPanel;  // n: right-hand side -> y -> increment
+    double* hd = x + n;                      // n: undamped diagonal
+    double* da = hd + n;                     // n: damping added to the diagonal; then the product h
+    double* blk = da + n;                    // kFacPanel x kFacPanel diagonal block (solves)
+    double* dmp = blk + kFacPanel * kFacPanel;  // n: damping of each column (solve-time charts only)
+    const bool charts = wd.charts != 0;
+    __shared__ int failed;
+    __shared__ double red[32];
+    double* A = B.Sglob + wd.dense0;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    constexpr int nw = kFactorThreads / 32;
+    if (tid == 0) failed = 0;
+    for (int i = tid; i < n; i += blockDim.x) da[i] = dampingOf(B, wd, i, lambda);
+    __syncthreads();
+    // assembly: damped lower triangle (factored in place), undamped strict upper copy
+    for (int j = warp; j < n; j += nw)
+#pragma unroll 2
+    for (int i = j + lane; i < n; i += 32) {
+        const double v = assembleEntryCol(B, wd, i, j, lambda, false);
+        if (i == j) {
+            hd[i] = v;
+            A[i + (long long)j * n] = v + da[i];
+        } else {
+            A[i + (long long)j * n] = v;
+            A[j + (long long)i * n] = v;
+        }
+    }
+    double* rhsOut = B.rhs + wd.vec0;
+    for (int i = tid; i < n; i += blockDim.x) {
+        const double r = rhsOf(B, wd, i);
+        x[i] = r;
+        rhsOut[i] = r;
+        if (charts) dmp[i] = da[i];
+    }
+    __syncthreads();
+    if (charts) {
+        chartSystem(B, wd, lambda, n, A, x, hd, dmp);
+        for (int i = tid; i < n; i += blockDim.x) rhsOut[i] = x[i];  // the restricted right-hand side
+        __syncthreads();
+    }
+    if (Sdebug) storeSdebug(A, n, Sdebug + wd.dense0);
+    // ---- factorization with the forward substitution
+    for (int k0 = 0; k0 < n; k0 += kFacPanel) {
+        // rows padded so that the trailing rows [bw, mp) are whole 32-row tiles
+        const int bw = min(kFacPanel, n - k0), m = n - k0, mp = bw + ((m - bw + 31) & ~31);
+        for (int t = tid; t < mp * kFacPanel; t += blockDim.x) {
+            const int c = t / mp, r = t % mp;
+            P[r + c * mp] = (c < bw && r < m && r >= c) ? A[(k0 + r) + (long long)(k0 + c) * n] : 0.0;
+        }
+        __syncthreads();
+        if (!factorPanel(P, mp, m, bw, x + k0, &failed)) break;
+        __syncthreads();
+        storePanel(P, mp, m, bw, A, n, k0);
+        const int m2 = m - bw;
+        if (m2 > 0) {
+            const int nb2 = (m2 + 31) >> 5, tiles = nb2 * (nb2 + 1) / 2;
+            for (int t = warp; t < tiles; t += nw) {
+                int cb, rb;
+                tileOf(t, nb2, cb, rb);  // upper enumeration (cb <= rb): rows rb, columns cb
+                trailingTile(P + bw, mp, rb, cb, bw, m2, A, n, k0);
+            }
+            // right-hand side below the panel: y2 -= L21 y1
+            for (int i = tid; i < m2; i += blockDim.x) {
+                double s = 0;
+                for (int c = 0; c < bw; ++c) s += P[bw + i + c * mp] * x[k0 + c];
+                x[k0 + bw + i] -= s;
+            }
+        }
+        __syncthreads();
+    }
+    if (failed) {
+        if (tid == 0) B.solveStatus[wdx] = CGMLI_E_NOT_PD;
+        return;
+    }
+    factorTail(B, wd, wdx, lambda, refinement, A, x, hd, da, blk, dmp, red);
+}
+
+// ---- wide windows -----------------------------------------------------------------------
+// A window whose reduced system has kWideCols columns or more (configuration 3's
+// single large window) is factored by a launch sequence that spreads the work over
+// the GPU instead of one CTA: the assembly by column blocks (k_wide_assemble), the
+// solve-time charts and the debug copy (k_wide_prepare, one CTA), then per panel of
+// kFacPanel columns its left-looking factorization with the forward substitution
+// (k_wide_panel, one CTA per window) and the trailing update A22 -= L21 L21^T with
+// one warp per 32 x 32 tile (k_wide_trailing, L21 read from the L2-resident slot),
+// and finally the backward substitution, the refinement steps and the prediction
+// (k_wide_finish, one CTA).  The arithmetic is k_factor's operation for operation
+// (a trailing tile sums the same products in the same order), so both paths give
+// the same increment bit for bit.  Per-window vectors between the kernels:
+// B.facVec + 3 vec0 holds x (n), the undamped diagonal (n) and the damping (n).
+__global__ void __launch_bounds__(256) k_wide_assemble(DevBatch B) {
+    const int wdx = B.wideList[blockIdx.x];
+    if (B.lm[wdx].mode == kModeDone) return;
+    const WinDesc wd = B.win[wdx];
+    const int n = wd.Nr, j0 = 32 * blockIdx.y;
+    if (j0 >= n) return;
+    const double lambda = B.lm[wdx].lambda;
+    double* A = B.Sglob + wd.dense0;
+    double* x = B.facVec + 3ll * wd.vec0;
+    double* hd = x + n;
+    double* dmp = hd + n;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int j = j0 + warp; j < min(n, j0 + 32); j += nw)
+        for (int i = j + lane; i < n; i += 32) {
+            const double v = assembleEntryCol(B, wd, i, j, lambda, false);
+            if (i == j) {
+                hd[i] = v;
+                A[i + (long long)j * n] = v + dampingOf(B, wd, i, lambda);
+            } else {
+                A[i + (long long)j * n] = v;
+                A[j + (long long)i * n] = v;
+            }
+        }
+    if (blockIdx.y == 0) {
+        double* rhsOut = B.rhs + wd.vec0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const double r = rhsOf(B, wd, i);
+            x[i] = r;
+            rhsOut[i] = r;
+            dmp[i] = dampingOf(B, wd, i, lambda);
+        }
+        if (threadIdx.x == 0) B.facFailed[wdx] = 0;
+    }
+}
+
+__global__ void __launch_bounds__(kFactorThreads) k_wide_prepare(DevBatch B, double* Sdebug) {
+    const int wdx = B.wideList[blockIdx.x];
+    if (B.lm[wdx].mode == kModeDone) return;
+    const WinDesc wd = B.win[wdx];
+    const int n = wd.Nr;
+    double* A = B.Sglob + wd.dense0;
+    if (wd.charts) {
+        double* x = B.facVec + 3ll * wd.vec0;
+        chartSystem(B, wd, B.lm[wdx].lambda, n, A, x, x + n, x + 2 * n);
+        double* rhsOut = B.rhs + wd.vec0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) rhsOut[i] = x[i];  // the restricted right-hand side
+        __syncthreads();
+    }
+    if (Sdebug) storeSdebug(A, n, Sdebug + wd.dense0);
+}
+
+__global__ void __launch_bounds__(kFactorThreads) k_wide_panel(DevBatch B, int k0) {
+    const int wdx = B.wideList[blockIdx.x];
+    if (B.lm[wdx].mode == kModeDone) return;
+    const WinDesc wd = B.win[wdx];
+    const int n = wd.Nr;
+    if (k0 >= n || B.facFailed[wdx]) return;
+    extern __shared__ __align__(16) double smem[];
+    __shared__ int failed;
+    double* P = smem;
+    double* A = B.Sglob + wd.dense0;
+    double* x = B.facVec + 3ll * wd.vec0;
+    const int tid = threadIdx.x;
+    const int bw = min(kFacPanel, n - k0), m = n - k0, mp = bw + ((m - bw + 31) & ~31);
+    if (tid == 0) failed = 0;
+    for (int t = tid; t < mp * kFacPanel; t += blockDim.x) {
+        const int c = t / mp, r = t % mp;
+        P[r + c * mp] = (c < bw && r < m && r >= c) ? A[(k0 + r) + (long long)(k0 + c) * n] : 0.0;
+    }
+    __syncthreads();
+    if (!factorPanel(P, mp, m, bw, x + k0, &failed)) {
+        if (tid == 0) B.facFailed[wdx] = 1;
+        return;
+    }
+    __syncthreads();
+    storePanel(P, mp, m, bw, A, n, k0);
+    for (int i = tid; i < m - bw; i += blockDim.x) {  // right-hand side below the panel: y2 -= L21 y1
+        double s = 0;
+        for (int c = 0; c < bw; ++c) s += P[bw + i + c * mp] * x[k0 + c];
+        x[k0 + bw + i] -= s;
+    }
+}
+
+__global__ void __launch_bounds__(kFactorThreads) k_wide_trailing(DevBatch B, int k0) {
+    const int wdx = B.wideList[blockIdx.x];
+    if (B.lm[wdx].mode == kModeDone) return;
+    const WinDesc wd = B.win[wdx];
+    const int n = wd.Nr;
+    if (k0 >= n || B.facFailed[wdx]) return;
+    const int bw = min(kFacPanel, n - k0), m2 = n - k0 - bw;
+    const int nb2 = (m2 + 31) >> 5, tiles = nb2 * (nb2 + 1) / 2;
+    const int t = blockIdx.y * (kFactorThreads / 32) + (threadIdx.x >> 5);
+    if (m2 <= 0 || t >= tiles) return;  // per warp: the kernel has no barrier
+    int cb, rb;
+    tileOf(t, nb2, cb, rb);
+    double* A = B.Sglob + wd.dense0;
+    // L21 column k = A's column k0 + k from row k0 + bw; rows past n (padding of the
+    // last tile) read the next column's top, inside the slot, and only reach masked entries
+    trailingTile(A + (k0 + bw) + (long long)k0 * n, n, rb, cb, bw, m2, A, n, k0);
+}
+
+__global__ void __launch_bounds__(kFactorThreads) k_wide_finish(DevBatch B, int refinement) {
+    const int wdx = B.wideList[blockIdx.x];
+    if (B.lm[wdx].mode == kModeDone) return;
+    const WinDesc wd = B.win[wdx];
+    const int n = wd.Nr;
+    if (B.facFailed[wdx]) {
+        if (threadIdx.x == 0) B.solveStatus[wdx] = CGMLI_E_NOT_PD;
+        return;
+    }
+    extern __shared__ __align__(16) double smem[];
+    __shared__ double red[32];
+    double* x = smem;
+    double* hd = x + n;
+    double* dmp = hd + n;
+    double* h = dmp + n;
+    double* blk = h + n;
+    const double* src = B.facVec + 3ll * wd.vec0;
+    for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) x[i] = src[i];
+    __syncthreads();
+    factorTail(B, wd, wdx, B.lm[wdx].lambda, refinement, B.Sglob + wd.dense0, x, hd, h, blk, dmp, red);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1570,6 +1746,11 @@ size_t linearizeSmemBytes(int maxNs, bool mixed) {  // the widest shape's
     return m;
 }
 size_t schurSmemBytes() { return kSchurSmemDoubles * sizeof(double); }
+size_t widePanelSmemBytes(int maxNr) {  // one staged panel over the padded rows
+    const size_t npad = (((size_t)maxNr + 31) & ~(size_t)31) + kFacPanel;
+    return npad * kFacPanel * sizeof(double);
+}
+size_t wideFinishSmemBytes(int maxNr) { return (4 * (size_t)maxNr + kFacPanel * kFacPanel) * sizeof(double); }
 size_t factorSmemBytes(int maxNr) {
     // one panel of kFacPanel columns over the padded rows, four n-vectors, the diagonal block
     const size_t npad = (((size_t)maxNr + 31) & ~(size_t)31) + kFacPanel;
@@ -1579,7 +1760,7 @@ size_t factorSmemBytes(int maxNr) {
 // The dynamic shared-memory cap is a per-function attribute shared by every
 // solver in the process, so it is raised once to the device's opt-in maximum
 // (each launch still requests only what its batch needs).
-cudaError_t configureKernels(size_t linSmem, size_t facSmem) {
+cudaError_t configureKernels(size_t linSmem, size_t facSmem, size_t wideSmem) {
     int device = 0, optin = 0;
     cudaError_t e = cudaGetDevice(&device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
@@ -1591,6 +1772,13 @@ cudaError_t configureKernels(size_t linSmem, size_t facSmem) {
     if ((e = cudaFuncGetAttributes(&pm, k_lin_pairs<true>)) != cudaSuccess) return e;
     if ((e = cudaFuncGetAttributes(&fa, k_factor)) != cudaSuccess) return e;
     if ((e = cudaFuncGetAttributes(&sa, k_lin_schur)) != cudaSuccess) return e;
+    cudaFuncAttributes wp, wf;
+    if ((e = cudaFuncGetAttributes(&wp, k_wide_panel)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&wf, k_wide_finish)) != cudaSuccess) return e;
+    const size_t wideMax = (size_t)optin - std::max(wp.sharedSizeBytes, wf.sharedSizeBytes);
+    if (wideSmem > wideMax) return cudaErrorInvalidValue;
+    for (auto k : {k_wide_panel, k_wide_finish})
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wideMax)) != cudaSuccess) return e;
     const size_t linMax = (size_t)optin - std::max(la.sharedSizeBytes, lm.sharedSizeBytes), facMax = (size_t)optin - fa.sharedSizeBytes;
     const size_t schMax = (size_t)optin - sa.sharedSizeBytes;
     const size_t pairMax = (size_t)optin - std::max(pa.sharedSizeBytes, pm.sharedSizeBytes);
@@ -1667,6 +1855,20 @@ int launchIterationParts(const DevBatch& B, const LaunchPlan& P, int refinement,
     }
     if (parts & kIterStep) {
     run(CGMLI_KERNEL_FACTOR, [&] { k_factor<<<W, kFactorThreads, P.facSmem, s>>>(B, refinement, Sdebug); });
+    if (P.numWide > 0) {  // the wide sequence (windows of at least kWideCols columns)
+        run(CGMLI_KERNEL_FACTOR, [&] { k_wide_assemble<<<dim3(P.numWide, (P.wideCols + 31) / 32), 256, 0, s>>>(B); });
+        if (P.wideCharts || Sdebug) run(CGMLI_KERNEL_FACTOR, [&] { k_wide_prepare<<<P.numWide, kFactorThreads, 0, s>>>(B, Sdebug); });
+        for (int k0 = 0; k0 < P.wideCols; k0 += kFacPanel) {
+            run(CGMLI_KERNEL_FACTOR, [&] { k_wide_panel<<<P.numWide, kFactorThreads, P.widePanelSmem, s>>>(B, k0); });
+            const int m2 = P.wideCols - k0 - kFacPanel;
+            if (m2 > 0) {
+                const int nb2 = (m2 + 31) >> 5, tiles = nb2 * (nb2 + 1) / 2;
+                const dim3 grid(P.numWide, (tiles + kFactorThreads / 32 - 1) / (kFactorThreads / 32));
+                run(CGMLI_KERNEL_FACTOR, [&] { k_wide_trailing<<<grid, kFactorThreads, 0, s>>>(B, k0); });
+            }
+        }
+        run(CGMLI_KERNEL_FACTOR, [&] { k_wide_finish<<<P.numWide, kFactorThreads, P.wideFinishSmem, s>>>(B, refinement); });
+    }
     run(CGMLI_KERNEL_CANDIDATE, [&] { k_candidate<<<W, 128, 0, s>>>(B); });
     if (B.numLandmarks > 0) {
         run(CGMLI_KERNEL_BACKSUB_TRIAL, [&] { k_backsub<<<(B.numLandmarks * 8 + 255) / 256, 256, 0, s>>>(B); });

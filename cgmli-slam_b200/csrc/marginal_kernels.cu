@@ -930,7 +930,9 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_victim(MargBatch M) {
 // remainder R satisfies |R|_F <= 1e-10 lambda_kept_min: by the sin-theta
 // bound null(A) is then within 1e-10 of the negligible eigenspace, so A^T A
 // and A^T r0 agree with the eigen path's far below its own rounding.  Other
-// windows are left to k_marg_eigen.
+// windows are left to the eigen path (k_marg_tridiag), which takes over this
+// path's tridiagonal form: the reflectors in the window's prior slot, d, e and
+// tau in its victim scratch (fast[w] = 2).
 constexpr int kFastMaxN = 160;    // E in shared memory up to this width
 constexpr int kFastMaxFree = 32;  // null directions handled by the projection
 __host__ __device__ constexpr size_t fastVecBytes(int n) { return sizeof(double) * 5 * (size_t)n + sizeof(int) * 3 * (size_t)n; }
@@ -973,6 +975,11 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_fast(MargBatch M) {
     int* rem = stepOf + n;                     // indices not yet pivoted
     __shared__ double sc[8];
     __shared__ int isc[2];
+    // the tridiagonal form for the eigen path, should this path decline the window:
+    // each reflector in its column of the prior's slot (row-major, below the
+    // subdiagonal), d, e and tau in the victim solve's scratch
+    double* reflectors = M.A + mw.sep0;
+    double* saved = M.X + mw.x0;
     __shared__ double G[kFastMaxFree * kFastMaxFree], h[kFastMaxFree];
     const double* E = M.sepH + mw.sep0;
     for (int t = tid; t < n * n; t += blockDim.x) S[t] = E[t];
@@ -1001,6 +1008,7 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_fast(MargBatch M) {
                     v[0] = x0 - alpha;
                     sc[0] = 1.0 / (sigma - x0 * alpha);
                 }
+                saved[2 * n + k] = sc[0];
             }
         }
         __syncthreads();
@@ -1029,6 +1037,7 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_fast(MargBatch M) {
             const double vi = v[i], wi = wv[i];
             for (int j = lane; j < m; j += 32) row[j] -= vi * wv[j] + wi * v[j];
         }
+        for (int i = tid; i < m; i += blockDim.x) reflectors[(k + 1 + i) * n + k] = v[i];
         __syncthreads();
     }
     if (tid == 0) {
@@ -1048,8 +1057,14 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_fast(MargBatch M) {
         sc[0] = lo;
         sc[1] = hi;
         sc[2] = fmax(1e-300, 1e-30 * emax);  // pivot guard of the Sturm counts
+        for (int k = (n >= 2 ? n - 2 : 0); k < n; ++k) saved[2 * n + k] = 0.0;
+        M.fast[w] = 2;  // the tridiagonal form is saved; 1 replaces it if this path forms the prior
     }
     __syncthreads();
+    for (int i = tid; i < n; i += blockDim.x) {
+        saved[i] = d[i];
+        saved[n + i] = e[i];
+    }
     // lambda_max: the point where the Sturm count reaches n, by multisection
     double lo = sc[0], hi = sc[1];
     const double pivmin = sc[2];
@@ -1295,10 +1310,13 @@ __global__ void __launch_bounds__(kEigenThreads) k_marg_tridiag(MargBatch M) {
     const MargWin mw = M.win[w];
     const int n = mw.nr;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
-    if (M.fast[w] || mw.m == 0 || n == 0 || n > kMargMaxSep || M.status[w] != CGMLI_OK) return;
+    // fast[w] == 2: the fast path declined the window after its tridiagonalization,
+    // which is this kernel's step 1 operation for operation, and saved it
+    const bool saved = M.fast[w] == 2;
+    if ((M.fast[w] && !saved) || mw.m == 0 || n == 0 || n > kMargMaxSep || M.status[w] != CGMLI_OK) return;
     extern __shared__ double tsm[];
     const bool inShared = n <= kTriSmemN && (long long)triSmemBytes(n) <= M.triSmem;
-    double* S = inShared ? tsm : M.sepV + mw.sep0;          // n x n row-major
+    double* S = inShared ? tsm : saved ? M.A + mw.sep0 : M.sepV + mw.sep0;  // n x n row-major
     double* Vt = inShared ? tsm + (size_t)n * n : M.sepH + mw.sep0;
     double* d = inShared ? tsm + 2 * (size_t)n * n : tsm;
     double* e = d + n;
@@ -1311,10 +1329,17 @@ __global__ void __launch_bounds__(kEigenThreads) k_marg_tridiag(MargBatch M) {
     __shared__ double red[kEigenThreads / 32];
     __shared__ int pos[kMargMaxSep];
     const double* E = M.sepH + mw.sep0;
-    for (long long t = tid; t < (long long)n * n; t += blockDim.x) S[t] = E[t];
+    if (saved) {  // the reflectors from the prior's slot, d, e and tau from the victim scratch
+        if (inShared)
+            for (long long t = tid; t < (long long)n * n; t += blockDim.x) S[t] = M.A[mw.sep0 + t];
+        const double* sv = M.X + mw.x0;
+        for (int i = tid; i < 3 * n; i += blockDim.x) d[i] = sv[i];  // d, e, tau are consecutive
+    } else {
+        for (long long t = tid; t < (long long)n * n; t += blockDim.x) S[t] = E[t];
+    }
     __syncthreads();
     // 1. tridiagonalization; the trailing block is updated on both triangles
-    for (int k = 0; k + 2 < n; ++k) {
+    for (int k = 0; !saved && k + 2 < n; ++k) {
         const int m = n - k - 1;
         double* v = rc;  // the reflector of this column
         double* p = rs;
@@ -1374,14 +1399,16 @@ __global__ void __launch_bounds__(kEigenThreads) k_marg_tridiag(MargBatch M) {
         __syncthreads();
     }
     if (tid == 0) {
-        if (n >= 2) {
-            d[n - 2] = S[(size_t)(n - 2) * n + (n - 2)];
-            e[n - 2] = S[(size_t)(n - 1) * n + (n - 2)];
-            tau[n - 2] = 0.0;
+        if (!saved) {
+            if (n >= 2) {
+                d[n - 2] = S[(size_t)(n - 2) * n + (n - 2)];
+                e[n - 2] = S[(size_t)(n - 1) * n + (n - 2)];
+                tau[n - 2] = 0.0;
+            }
+            d[n - 1] = S[(size_t)(n - 1) * n + (n - 1)];
+            e[n - 1] = 0.0;
+            tau[n - 1] = 0.0;
         }
-        d[n - 1] = S[(size_t)(n - 1) * n + (n - 1)];
-        e[n - 1] = 0.0;
-        tau[n - 1] = 0.0;
         double norm = 0;
         for (int i = 0; i < n; ++i) norm = fmax(norm, fmax(fabs(d[i]), fabs(e[i])));
         sc[1] = norm;
@@ -1529,7 +1556,10 @@ __global__ void __launch_bounds__(kEigenThreads) k_marg_tridiag(MargBatch M) {
         }
     }
     if (qlEnd == -2) {  // not converged (uniform): the Jacobi kernel takes the window while E is intact
-        if (!inShared && tid == 0) { M.status[w] = CGMLI_E_NONFINITE; M.rank[w] = 0; M.fast[w] = 3; }
+        if (tid == 0) {
+            if (inShared) M.fast[w] = 0;
+            else { M.status[w] = CGMLI_E_NONFINITE; M.rank[w] = 0; M.fast[w] = 3; }
+        }
         return;
     }
     // 3. U = Q V: H_k acts on components k + 1.. of every eigenvector, for k = n - 3 down to 0

@@ -80,6 +80,7 @@ struct cgmli_server {
         bool marg = false;
         int status = CGMLI_OK;
         double launchMs = 0;
+        double phaseMs[3] = {0, 0, 0};  // host time of set_windows, the solve launch, the marginalization launch
     };
     bool busy[2] = {false, false};                 // solver has a launched, uncompleted batch
     long long solverBytes[2] = {0, 0};             // device bytes each solver holds (after its last launch)
@@ -98,11 +99,18 @@ struct cgmli_server {
             victims[i] = b.reqs[i]->victim;
             b.marg = b.marg || victims[i] >= 0;
         }
+        const auto t0 = Clock::now();
         b.status = cgmli_solver_set_windows(S, b.windows.data(), n);
+        const auto t1 = Clock::now();
         if (b.status == CGMLI_OK)
             b.status = opt.nis_threshold > 0 ? cgmli_solver_solve_gated(S, opt.iterations, opt.nis_threshold, opt.max_refits, opt.pre_gate)
                                              : cgmli_solver_solve(S, opt.iterations);
+        const auto t2 = Clock::now();
         if (b.status == CGMLI_OK && b.marg) b.status = cgmli_solver_marginalize(S, victims.data(), opt.policy);
+        const auto t3 = Clock::now();
+        b.phaseMs[0] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        b.phaseMs[1] = std::chrono::duration<double, std::milli>(t2 - t1).count();
+        b.phaseMs[2] = std::chrono::duration<double, std::milli>(t3 - t2).count();
     }
 
     // Waits for a launched batch and records its results.
@@ -171,7 +179,8 @@ struct cgmli_server {
         // window above that half still runs, alone in its batch)
         const long long perSolver = opt.memory_budget_bytes / 2;
         // CGMLI_SERVER_TRACE set: one line per batch on stderr (size, host launch
-        // time, the completion thread's wait and read-back; milliseconds)
+        // time and its set_windows / solve / marginalize parts, the completion
+        // thread's wait and read-back; milliseconds)
         trace = std::getenv("CGMLI_SERVER_TRACE") != nullptr;
         std::thread completer([this] { completeLoop(); });
         for (;;) {
@@ -228,7 +237,9 @@ struct cgmli_server {
             const int size = (int)b->reqs.size();
             const int sv = b->solver;
             complete(*b, trace ? &waitMs : nullptr, trace ? &readMs : nullptr);
-            if (trace) std::fprintf(stderr, "batch %d launch %.3f wait %.3f read %.3f\n", size, b->launchMs, waitMs, readMs);
+            if (trace)
+                std::fprintf(stderr, "batch %d launch %.3f (set %.3f solve %.3f marg %.3f) wait %.3f read %.3f\n", size, b->launchMs,
+                             b->phaseMs[0], b->phaseMs[1], b->phaseMs[2], waitMs, readMs);
             {
                 std::lock_guard<std::mutex> lock(mu);
                 busy[sv] = false;

@@ -31,8 +31,8 @@ def backend():
     return B
 
 
-def _charted(seed, kind):
-    w = synth.SynthWindow(SPEC, seed)
+def _charted(seed, kind, spec=SPEC):
+    w = synth.SynthWindow(spec, seed)
     K, E, L = w.K, w.window.num_extrinsics, w.L
     if kind == "constant":
         kf = np.zeros(K, np.uint8)
@@ -76,6 +76,30 @@ def test_charted_step_matches_oracle(oracle, backend, kind):
     assert np.array_equal(got["delta"] == 0.0, ref["delta"] == 0.0)  # the same increments are exactly zero
     assert abs(got["predicted"] - ref["predicted"]) <= 1e-9 * abs(ref["predicted"])
     assert got["trial_valid"] and abs(got["trial_cost"] - ref["trial_cost"]) <= 1e-10 * abs(ref["trial_cost"])
+
+
+@pytest.mark.parametrize("kind", ["constant", "rotation"])
+def test_charted_step_on_a_wide_window(oracle, backend, kind):
+    """The charts on a window of 319 retained columns (18 keyframes, 8 cameras with
+    their own extrinsics), which the wide factorization sequence takes (charts
+    applied by k_wide_prepare), inside one batch with a narrow window: both
+    against the oracle."""
+    wide = _charted(33, kind, replace(synth.C3, keyframes=18, landmarks=1500, per_camera_extrinsics=True))
+    narrow = _charted(34, kind)
+    assert wide.retained_dim() >= 288 > narrow.retained_dim()
+    s = backend.Solver()
+    s.set_windows([narrow, wide])
+    s.step(1e-3)
+    for i, w in enumerate([narrow, wide]):
+        ref = oracle.step(w.window, w.retained_dim(), w.L, 1e-3)
+        got = s.read_step(i)
+        S, rhs = s.read_reduced(i)
+        assert got["status"] == 0 and ref["status"] == 0
+        assert rel(S, ref["S"]) < 1e-12
+        assert rel(rhs, ref["rhs"]) < 1e-11
+        assert rel(got["delta"], ref["delta"]) < 1e-9
+        assert np.array_equal(got["delta"] == 0.0, ref["delta"] == 0.0)
+        assert abs(got["predicted"] - ref["predicted"]) <= 1e-9 * abs(ref["predicted"])
 
 
 @pytest.mark.parametrize("kind", KINDS)

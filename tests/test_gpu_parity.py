@@ -64,8 +64,8 @@ def test_step_matches_oracle(oracle, backend, name, lam):
 
 
 def test_large_window_global_factor_path(oracle, backend):
-    """30 keyframes, 8 cameras, track length up to 25: N_r = 457 exceeds the
-    shared-memory factor and takes the global-memory Cholesky."""
+    """30 keyframes, 8 cameras, track length up to 25: N_r = 457 takes the wide
+    factorization sequence (panels and trailing tiles over the whole GPU)."""
     w = synth.SynthWindow(replace(synth.C3, landmarks=4000), 3)
     nr, L = w.retained_dim(), w.L
     assert nr > 232
@@ -77,6 +77,32 @@ def test_large_window_global_factor_path(oracle, backend):
     assert got["status"] == 0
     assert rel(got["delta"], ref["delta"]) < 1e-8
     assert abs(got["trial_cost"] - ref["trial_cost"]) <= 1e-10 * abs(ref["trial_cost"])
+
+
+@pytest.mark.parametrize("refinement", [0, 1])
+def test_wide_and_narrow_windows_in_one_batch(oracle, backend, refinement):
+    """Two wide windows of different widths (457 and 307 retained columns: the wide
+    sequence runs panels up to the wider one) and a narrow one (k_factor) in one
+    batch, with and without a refinement step: every step against the oracle, and
+    the wide window's step equal to its step solved alone."""
+    ws = [synth.SynthWindow(replace(synth.C3, landmarks=4000), 3), synth.SynthWindow(SPECS["c1"], 4),
+          synth.SynthWindow(replace(synth.C3, keyframes=20, landmarks=1500), 5)]
+    assert [w.retained_dim() >= 288 for w in ws] == [True, False, True]
+    s = backend.Solver(refinement=refinement)
+    s.set_windows(ws)
+    s.step(1e-4)
+    steps = [s.read_step(i) for i in range(3)]
+    s.close()
+    for w, got in zip(ws, steps):
+        ref = oracle.step(w.window, w.retained_dim(), w.L, 1e-4)
+        assert got["status"] == 0
+        assert rel(got["delta"], ref["delta"]) < 1e-8
+        assert abs(got["predicted"] - ref["predicted"]) <= 1e-9 * abs(ref["predicted"])
+    alone = backend.Solver(refinement=refinement)
+    alone.set_windows([ws[2]])
+    alone.step(1e-4)
+    assert rel(alone.read_step(0)["delta"], steps[2]["delta"]) < 1e-9
+    alone.close()
 
 
 @pytest.mark.parametrize("name,iterations", [("c1", 1), ("c2", 5), ("shared_calib", 5), ("no_imu_no_prior", 4)])
