@@ -27,7 +27,6 @@
 namespace cgmli {
 size_t linearizeSmemBytes(int maxNs, bool mixed);
 size_t factorSmemBytes(int maxNr);
-size_t widePanelSmemBytes(int maxNr);
 size_t wideFinishSmemBytes(int maxNr);
 cudaError_t configureKernels(size_t linSmem, size_t facSmem, size_t wideSmem);
 int launchIteration(const DevBatch& B, const LaunchPlan& P, int refinement, int maxIterations, int probe, double* Sdebug,
@@ -124,7 +123,7 @@ struct cgmli_solver {
     size_t linSmem = 0, facSmem = 0;
     // wide windows (isWideWindow): factored by the multi-launch sequence
     int numWide = 0, wideCols = 0, wideCharts = 0;
-    size_t widePanelSmem = 0, wideFinishSmem = 0;
+    size_t wideFinishSmem = 0;
     HVec<int> hWideList;
     DArray<int> wideList, facFailed;
     DArray<double> facVec;
@@ -277,7 +276,7 @@ struct cgmli_solver {
         P.facSmem = facSmem; P.maxNs = maxNs;
         P.linShape = hb.plan.linShape; P.trialShape = hb.plan.trialShape;
         P.numWide = numWide; P.wideCols = wideCols; P.wideCharts = wideCharts;
-        P.widePanelSmem = widePanelSmem; P.wideFinishSmem = wideFinishSmem;
+        P.wideFinishSmem = wideFinishSmem;
         return P;
     }
     void collectKernelTimes() {
@@ -488,10 +487,9 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
         }
         S->numWide = wide;
         S->facSmem = factorSmemBytes(narrow);
-        S->widePanelSmem = S->numWide ? widePanelSmemBytes(S->wideCols) : 0;
         S->wideFinishSmem = S->numWide ? wideFinishSmemBytes(S->wideCols) : 0;
     }
-    CK(configureKernels(S->linSmem, S->facSmem, std::max(S->widePanelSmem, S->wideFinishSmem)));
+    CK(configureKernels(S->linSmem, S->facSmem, S->wideFinishSmem));
     const long long lm = hb.totalLm;
     S->hWin.assign(S->win.begin(), S->win.end());  // pinned staging: the copy stays asynchronous
     CK(S->dWin.upload(S->hWin, st));

@@ -228,7 +228,7 @@ struct LaunchPlan {
     int numWide;             // wide windows (B.wideList)
     int wideCols;            // largest wide Nr: panels and trailing tiles of the sequence
     int wideCharts;          // some wide window has solve-time charts
-    size_t widePanelSmem, wideFinishSmem;
+    size_t wideFinishSmem;
 };
 
 }  // namespace cgmli

@@ -741,9 +741,14 @@ __device__ void blockedSolve(const double* L, int n, double* v, double* blk) {
         }
         __syncthreads();
         for (int r = k0 + bw + tid; r < n; r += blockDim.x) {
-            double s = 0;
-            for (int c = 0; c < bw; ++c) s += L[r + (long long)(k0 + c) * n] * v[k0 + c];
-            v[r] -= s;
+            double s0 = 0, s1 = 0;
+            int c = 0;
+            for (; c + 2 <= bw; c += 2) {
+                s0 += L[r + (long long)(k0 + c) * n] * v[k0 + c];
+                s1 += L[r + (long long)(k0 + c + 1) * n] * v[k0 + c + 1];
+            }
+            if (c < bw) s0 += L[r + (long long)(k0 + c) * n] * v[k0 + c];
+            v[r] -= s0 + s1;
         }
         __syncthreads();
     }
@@ -751,9 +756,14 @@ __device__ void blockedSolve(const double* L, int n, double* v, double* blk) {
         const int bw = min(kPanel, n - k0);
         // v[k0 + c] -= sum_{r >= k0 + bw} L[r, k0 + c] v[r]
         for (int c = warp; c < bw; c += nw) {
-            double s = 0;
-            for (int r = k0 + bw + lane; r < n; r += 32) s += L[r + (long long)(k0 + c) * n] * v[r];
-            s = warpSum(s);
+            double s0 = 0, s1 = 0;
+            int r = k0 + bw + lane;
+            for (; r + 32 < n; r += 64) {
+                s0 += L[r + (long long)(k0 + c) * n] * v[r];
+                s1 += L[r + 32 + (long long)(k0 + c) * n] * v[r + 32];
+            }
+            if (r < n) s0 += L[r + (long long)(k0 + c) * n] * v[r];
+            const double s = warpSum(s0 + s1);
             if (lane == 0) v[k0 + c] -= s;
         }
         for (int t = tid; t < bw * bw; t += blockDim.x) {
@@ -790,16 +800,29 @@ constexpr int kFacPanel = 32;
 // h = S_undamped v from the stored upper triangle (A[p + q n], p < q) and diagonal hd.
 __device__ void undampedProduct(const double* A, const double* hd, int n, const double* v, double* h) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+    // four independent sums per loop keep four L2 loads in flight per thread
     for (int i = tid; i < n; i += blockDim.x) {  // columns j > i of row i: consecutive i coalesce
-        double s = hd[i] * v[i];
-        for (int j = i + 1; j < n; ++j) s += A[i + (long long)j * n] * v[j];
-        h[i] = s;
+        double s0 = hd[i] * v[i], s1 = 0, s2 = 0, s3 = 0;
+        int j = i + 1;
+        for (; j + 4 <= n; j += 4) {
+            s0 += A[i + (long long)j * n] * v[j];
+            s1 += A[i + (long long)(j + 1) * n] * v[j + 1];
+            s2 += A[i + (long long)(j + 2) * n] * v[j + 2];
+            s3 += A[i + (long long)(j + 3) * n] * v[j + 3];
+        }
+        for (; j < n; ++j) s0 += A[i + (long long)j * n] * v[j];
+        h[i] = (s0 + s1) + (s2 + s3);
     }
     __syncthreads();
     for (int i = warp; i < n; i += nw) {  // rows j < i of column i
-        double s = 0;
-        for (int j = lane; j < i; j += 32) s += A[j + (long long)i * n] * v[j];
-        s = warpSum(s);
+        double s0 = 0, s1 = 0;
+        int j = lane;
+        for (; j + 32 < i; j += 64) {
+            s0 += A[j + (long long)i * n] * v[j];
+            s1 += A[j + 32 + (long long)i * n] * v[j + 32];
+        }
+        if (j < i) s0 += A[j + (long long)i * n] * v[j];
+        const double s = warpSum(s0 + s1);
         if (lane == 0) h[i] += s;
     }
     __syncthreads();
@@ -979,9 +1002,14 @@ __device__ void factorTail(const DevBatch& B, const WinDesc& wd, int wdx, double
     for (int k0 = ((n - 1) / kFacPanel) * kFacPanel; k0 >= 0; k0 -= kFacPanel) {
         const int bw = min(kFacPanel, n - k0);
         for (int c = warp; c < bw; c += nw) {
-            double s = 0;
-            for (int r = k0 + bw + lane; r < n; r += 32) s += A[r + (long long)(k0 + c) * n] * x[r];
-            s = warpSum(s);
+            double s0 = 0, s1 = 0;
+            int r = k0 + bw + lane;
+            for (; r + 32 < n; r += 64) {
+                s0 += A[r + (long long)(k0 + c) * n] * x[r];
+                s1 += A[r + 32 + (long long)(k0 + c) * n] * x[r + 32];
+            }
+            if (r < n) s0 += A[r + (long long)(k0 + c) * n] * x[r];
+            const double s = warpSum(s0 + s1);
             if (lane == 0) x[k0 + c] -= s;
         }
         for (int t = tid; t < bw * bw; t += blockDim.x) {
@@ -1158,16 +1186,22 @@ __global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int re
 // ---- wide windows -----------------------------------------------------------------------
 // A window whose reduced system has kWideCols columns or more (configuration 3's
 // single large window) is factored by a launch sequence that spreads the work over
-// the GPU instead of one CTA: the assembly by column blocks (k_wide_assemble), the
-// solve-time charts and the debug copy (k_wide_prepare, one CTA), then per panel of
-// kFacPanel columns its left-looking factorization with the forward substitution
-// (k_wide_panel, one CTA per window) and the trailing update A22 -= L21 L21^T with
-// one warp per 32 x 32 tile (k_wide_trailing, L21 read from the L2-resident slot),
-// and finally the backward substitution, the refinement steps and the prediction
-// (k_wide_finish, one CTA).  The arithmetic is k_factor's operation for operation
-// (a trailing tile sums the same products in the same order), so both paths give
-// the same increment bit for bit.  Per-window vectors between the kernels:
-// B.facVec + 3 vec0 holds x (n), the undamped diagonal (n) and the damping (n).
+// the GPU instead of one CTA (k_factor skips it).  The damped system is assembled
+// by column blocks (k_wide_assemble); the solve-time charts and the debug copy run
+// in one CTA (k_wide_prepare).  Then, per panel of kFacPanel columns:
+//   - its diagonal block is factored by one warp, lane i owning row i, with the
+//     forward substitution of the right-hand side over the block
+//     (factorDiagWarp: a right-looking sweep with warp-level sync only);
+//   - the rows below it are solved against that block (L21 = A21 L11^-T), one
+//     thread per row with the row in registers, and each row's right-hand side
+//     entry takes its update y2 -= L21 y1 on the way (k_wide_trsm);
+//   - the trailing lower triangle A22 -= L21 L21^T is updated by one warp per
+//     32 x 32 tile on the FP64 tensor path, L21 read from the L2-resident slot;
+//     the warp holding the first trailing tile, which is the next panel's
+//     diagonal block, factors it as soon as its update is written (k_wide_trailing).
+// The backward substitution, the refinement steps and the prediction follow in one
+// CTA (k_wide_finish, the tail k_factor uses).  Per-window vectors between the
+// kernels: B.facVec + 3 vec0 holds x (n), the undamped diagonal (n) and the damping (n).
 __global__ void __launch_bounds__(256) k_wide_assemble(DevBatch B) {
     const int wdx = B.wideList[blockIdx.x];
     if (B.lm[wdx].mode == kModeDone) return;
@@ -1219,36 +1253,119 @@ __global__ void __launch_bounds__(kFactorThreads) k_wide_prepare(DevBatch B, dou
     if (Sdebug) storeSdebug(A, n, Sdebug + wd.dense0);
 }
 
-__global__ void __launch_bounds__(kFactorThreads) k_wide_panel(DevBatch B, int k0) {
+// Cholesky of one panel's diagonal block by one warp, in place in T (bw x bw lower,
+// row-major with stride kDiagStride), with the forward substitution of x1 (bw
+// entries); T's diagonal becomes L's.  Lane i holds row i in registers; column c's
+// pivot and the entries L[j][c] of the rank-1 update come by shuffles, so the
+// block needs no shared-memory round trip between columns.  Returns false
+// (uniform over the warp) on a pivot that is not positive and finite.
+constexpr int kDiagStride = kFacPanel + 1;
+__device__ bool factorDiagWarp(double* T, int bw, double* x1) {
+    const int lane = threadIdx.x & 31;
+    double r[kFacPanel];
+#pragma unroll
+    for (int j = 0; j < kFacPanel; ++j) r[j] = (lane < bw && j <= lane) ? T[lane * kDiagStride + j] : 0.0;
+    double xi = lane < bw ? x1[lane] : 0.0;
+    bool ok = true;
+#pragma unroll
+    for (int c = 0; c < kFacPanel; ++c) {
+        if (c < bw && ok) {  // uniform over the warp
+            const double d = __shfl_sync(0xffffffffu, r[c], c);
+            if (!(d > 0) || !isfinite(d)) {
+                ok = false;  // every lane received the same d
+            } else {
+                const double l = sqrt(d);
+                const double lic = lane > c ? r[c] / l : (lane == c ? l : 0.0);  // L[lane][c]
+                if (lane >= c) r[c] = lic;
+                const double yc = __shfl_sync(0xffffffffu, xi, c) / l;
+                if (lane == c) xi = yc;
+                else if (lane > c) xi -= lic * yc;
+#pragma unroll
+                for (int j = c + 1; j < kFacPanel; ++j) {  // row lane, columns c < j <= lane
+                    const double ljc = __shfl_sync(0xffffffffu, lic, j);
+                    if (lane >= j) r[j] -= lic * ljc;
+                }
+            }
+        }
+    }
+    if (!ok) return false;
+#pragma unroll
+    for (int j = 0; j < kFacPanel; ++j)
+        if (lane < bw && j <= lane) T[lane * kDiagStride + j] = r[j];
+    if (lane < bw) x1[lane] = xi;
+    return true;
+}
+
+// The diagonal block at k0 of window w: staged from A, factored by the calling warp,
+// written back (L11, its diagonal as the roots).  Returns false on a failed pivot.
+__device__ bool wideDiagBlock(const DevBatch& B, const WinDesc& wd, int k0, double* T) {
+    const int lane = threadIdx.x & 31, n = wd.Nr, bw = min(kFacPanel, n - k0);
+    double* A = B.Sglob + wd.dense0;
+    double* x = B.facVec + 3ll * wd.vec0;
+    for (int q = lane; q < bw * bw; q += 32) {
+        const int i = q / bw, j = q % bw;
+        if (j <= i) T[i * kDiagStride + j] = A[(k0 + i) + (long long)(k0 + j) * n];
+    }
+    __syncwarp();
+    if (!factorDiagWarp(T, bw, x + k0)) return false;
+    for (int q = lane; q < bw * bw; q += 32) {
+        const int i = q / bw, j = q % bw;
+        if (j <= i) A[(k0 + i) + (long long)(k0 + j) * n] = T[i * kDiagStride + j];
+    }
+    return true;
+}
+
+// The first panel's diagonal block (the later ones are factored by k_wide_trailing).
+__global__ void __launch_bounds__(32) k_wide_diag(DevBatch B) {
+    const int wdx = B.wideList[blockIdx.x];
+    if (B.lm[wdx].mode == kModeDone) return;
+    __shared__ double T[kFacPanel * kDiagStride];
+    if (!wideDiagBlock(B, B.win[wdx], 0, T) && threadIdx.x == 0) B.facFailed[wdx] = 1;
+}
+
+// Rows below the panel at k0: L21 = A21 L11^-T by forward substitution, one thread
+// per row (the row's bw entries in registers), and y2 -= L21 y1 for the row.
+__global__ void __launch_bounds__(kFactorThreads) k_wide_trsm(DevBatch B, int k0) {
     const int wdx = B.wideList[blockIdx.x];
     if (B.lm[wdx].mode == kModeDone) return;
     const WinDesc wd = B.win[wdx];
     const int n = wd.Nr;
     if (k0 >= n || B.facFailed[wdx]) return;
-    extern __shared__ __align__(16) double smem[];
-    __shared__ int failed;
-    double* P = smem;
+    const int bw = min(kFacPanel, n - k0), r0 = k0 + bw + blockIdx.y * blockDim.x;
+    if (r0 >= n) return;  // uniform over the CTA
+    __shared__ double L[kFacPanel * kDiagStride], y1[kFacPanel], inv[kFacPanel];
     double* A = B.Sglob + wd.dense0;
     double* x = B.facVec + 3ll * wd.vec0;
-    const int tid = threadIdx.x;
-    const int bw = min(kFacPanel, n - k0), m = n - k0, mp = bw + ((m - bw + 31) & ~31);
-    if (tid == 0) failed = 0;
-    for (int t = tid; t < mp * kFacPanel; t += blockDim.x) {
-        const int c = t / mp, r = t % mp;
-        P[r + c * mp] = (c < bw && r < m && r >= c) ? A[(k0 + r) + (long long)(k0 + c) * n] : 0.0;
+    for (int q = threadIdx.x; q < bw * bw; q += blockDim.x) {
+        const int i = q / bw, j = q % bw;
+        L[i * kDiagStride + j] = j <= i ? A[(k0 + i) + (long long)(k0 + j) * n] : 0.0;
+    }
+    if (threadIdx.x < bw) {
+        y1[threadIdx.x] = x[k0 + threadIdx.x];
+        inv[threadIdx.x] = 1.0 / A[(k0 + threadIdx.x) + (long long)(k0 + threadIdx.x) * n];
     }
     __syncthreads();
-    if (!factorPanel(P, mp, m, bw, x + k0, &failed)) {
-        if (tid == 0) B.facFailed[wdx] = 1;
-        return;
+    const int r = r0 + threadIdx.x;
+    if (r >= n) return;
+    double a[kFacPanel];
+#pragma unroll
+    for (int c = 0; c < kFacPanel; ++c) a[c] = c < bw ? A[r + (long long)(k0 + c) * n] : 0.0;
+    double y = 0;
+#pragma unroll
+    for (int c = 0; c < kFacPanel; ++c) {
+        if (c < bw) {
+            double s0 = a[c], s1 = 0;
+#pragma unroll
+            for (int k = 0; k < c; k += 2) {
+                s0 -= a[k] * L[c * kDiagStride + k];
+                if (k + 1 < c) s1 -= a[k + 1] * L[c * kDiagStride + k + 1];
+            }
+            a[c] = (s0 + s1) * inv[c];
+            A[r + (long long)(k0 + c) * n] = a[c];
+            y += a[c] * y1[c];
+        }
     }
-    __syncthreads();
-    storePanel(P, mp, m, bw, A, n, k0);
-    for (int i = tid; i < m - bw; i += blockDim.x) {  // right-hand side below the panel: y2 -= L21 y1
-        double s = 0;
-        for (int c = 0; c < bw; ++c) s += P[bw + i + c * mp] * x[k0 + c];
-        x[k0 + bw + i] -= s;
-    }
+    x[r] -= y;
 }
 
 __global__ void __launch_bounds__(kFactorThreads) k_wide_trailing(DevBatch B, int k0) {
@@ -1267,6 +1384,11 @@ __global__ void __launch_bounds__(kFactorThreads) k_wide_trailing(DevBatch B, in
     // L21 column k = A's column k0 + k from row k0 + bw; rows past n (padding of the
     // last tile) read the next column's top, inside the slot, and only reach masked entries
     trailingTile(A + (k0 + bw) + (long long)k0 * n, n, rb, cb, bw, m2, A, n, k0);
+    if (t == 0) {  // tile (0, 0) is the next panel's diagonal block, complete now
+        __shared__ double T[kFacPanel * kDiagStride];
+        __syncwarp();
+        if (!wideDiagBlock(B, wd, k0 + bw, T) && (threadIdx.x & 31) == 0) B.facFailed[wdx] = 1;
+    }
 }
 
 __global__ void __launch_bounds__(kFactorThreads) k_wide_finish(DevBatch B, int refinement) {
@@ -1746,10 +1868,6 @@ size_t linearizeSmemBytes(int maxNs, bool mixed) {  // the widest shape's
     return m;
 }
 size_t schurSmemBytes() { return kSchurSmemDoubles * sizeof(double); }
-size_t widePanelSmemBytes(int maxNr) {  // one staged panel over the padded rows
-    const size_t npad = (((size_t)maxNr + 31) & ~(size_t)31) + kFacPanel;
-    return npad * kFacPanel * sizeof(double);
-}
 size_t wideFinishSmemBytes(int maxNr) { return (4 * (size_t)maxNr + kFacPanel * kFacPanel) * sizeof(double); }
 size_t factorSmemBytes(int maxNr) {
     // one panel of kFacPanel columns over the padded rows, four n-vectors, the diagonal block
@@ -1772,13 +1890,11 @@ cudaError_t configureKernels(size_t linSmem, size_t facSmem, size_t wideSmem) {
     if ((e = cudaFuncGetAttributes(&pm, k_lin_pairs<true>)) != cudaSuccess) return e;
     if ((e = cudaFuncGetAttributes(&fa, k_factor)) != cudaSuccess) return e;
     if ((e = cudaFuncGetAttributes(&sa, k_lin_schur)) != cudaSuccess) return e;
-    cudaFuncAttributes wp, wf;
-    if ((e = cudaFuncGetAttributes(&wp, k_wide_panel)) != cudaSuccess) return e;
+    cudaFuncAttributes wf;
     if ((e = cudaFuncGetAttributes(&wf, k_wide_finish)) != cudaSuccess) return e;
-    const size_t wideMax = (size_t)optin - std::max(wp.sharedSizeBytes, wf.sharedSizeBytes);
+    const size_t wideMax = (size_t)optin - wf.sharedSizeBytes;
     if (wideSmem > wideMax) return cudaErrorInvalidValue;
-    for (auto k : {k_wide_panel, k_wide_finish})
-        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wideMax)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_wide_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wideMax)) != cudaSuccess) return e;
     const size_t linMax = (size_t)optin - std::max(la.sharedSizeBytes, lm.sharedSizeBytes), facMax = (size_t)optin - fa.sharedSizeBytes;
     const size_t schMax = (size_t)optin - sa.sharedSizeBytes;
     const size_t pairMax = (size_t)optin - std::max(pa.sharedSizeBytes, pm.sharedSizeBytes);
@@ -1858,14 +1974,14 @@ int launchIterationParts(const DevBatch& B, const LaunchPlan& P, int refinement,
     if (P.numWide > 0) {  // the wide sequence (windows of at least kWideCols columns)
         run(CGMLI_KERNEL_FACTOR, [&] { k_wide_assemble<<<dim3(P.numWide, (P.wideCols + 31) / 32), 256, 0, s>>>(B); });
         if (P.wideCharts || Sdebug) run(CGMLI_KERNEL_FACTOR, [&] { k_wide_prepare<<<P.numWide, kFactorThreads, 0, s>>>(B, Sdebug); });
-        for (int k0 = 0; k0 < P.wideCols; k0 += kFacPanel) {
-            run(CGMLI_KERNEL_FACTOR, [&] { k_wide_panel<<<P.numWide, kFactorThreads, P.widePanelSmem, s>>>(B, k0); });
+        run(CGMLI_KERNEL_FACTOR, [&] { k_wide_diag<<<P.numWide, 32, 0, s>>>(B); });
+        for (int k0 = 0; k0 + kFacPanel < P.wideCols; k0 += kFacPanel) {
             const int m2 = P.wideCols - k0 - kFacPanel;
-            if (m2 > 0) {
-                const int nb2 = (m2 + 31) >> 5, tiles = nb2 * (nb2 + 1) / 2;
-                const dim3 grid(P.numWide, (tiles + kFactorThreads / 32 - 1) / (kFactorThreads / 32));
-                run(CGMLI_KERNEL_FACTOR, [&] { k_wide_trailing<<<grid, kFactorThreads, 0, s>>>(B, k0); });
-            }
+            const dim3 rows(P.numWide, (m2 + kFactorThreads - 1) / kFactorThreads);
+            run(CGMLI_KERNEL_FACTOR, [&] { k_wide_trsm<<<rows, kFactorThreads, 0, s>>>(B, k0); });
+            const int nb2 = (m2 + 31) >> 5, tiles = nb2 * (nb2 + 1) / 2;
+            const dim3 grid(P.numWide, (tiles + kFactorThreads / 32 - 1) / (kFactorThreads / 32));
+            run(CGMLI_KERNEL_FACTOR, [&] { k_wide_trailing<<<grid, kFactorThreads, 0, s>>>(B, k0); });
         }
         run(CGMLI_KERNEL_FACTOR, [&] { k_wide_finish<<<P.numWide, kFactorThreads, P.wideFinishSmem, s>>>(B, refinement); });
     }
