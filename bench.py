@@ -73,7 +73,10 @@ def parse():
     p.add_argument("--gate-iterations", type=int, default=10, help="iteration budget of the gated-solve row (0: off)")
     p.add_argument("--imu-rigs", type=int, default=512, help="rigs of the IMU preintegration batch, 11 keyframes each (0: off)")
     p.add_argument("--imu-cpu-sample", type=int, default=1024, help="intervals preintegrated by the oracle for its CPU rate")
-    p.add_argument("--mixed-steps", type=int, default=10, help="timed solves of the batch in mixed precision (0: off)")
+    p.add_argument("--mixed-steps", type=int, default=10, help="timed solves of the batch in the other precision (0: off)")
+    p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+                   help="precision of the headline solve, the end-to-end and the served rows (the batched configuration "
+                        "states FP32 evaluation with FP64 reduced solves: mixed)")
     return p.parse_args()
 
 
@@ -116,12 +119,24 @@ def aggregate_rate(world: int, windows_per_rank: int, steps: int, max_ms: float)
     return world * windows_per_rank * steps / (max_ms / 1000.0)
 
 
+PRECISION_TEXT = {
+    "mixed": "FP64 factor evaluation with its Jacobian blocks and weights rounded to FP32, FP32 staged rows; FP64 residuals, "
+             "landmark sums, gradients, reduced system and Cholesky",
+    "fp64": "FP64 factor evaluation and accumulation, FP64 Cholesky",
+}
+DTYPE = {"mixed": "f32+f64", "fp64": "f64"}
+
+
+def headline_precision(args):
+    return abi.PRECISION_MIXED if args.precision == "mixed" else abi.PRECISION_FP64
+
+
 def config_dict(args, world):
     return {
         "workload": "batched windows: K~U{6..15}, L~logU(200,5000), 4 cams, IMU+prior, 24+1 calib, 5 LM it",
         "windows_per_gpu": args.windows, "lm_iterations": args.iterations, "seed": args.seed,
         "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (no flush needed)",
-        "precision": "fp64 factor eval and accumulation, fp64 Cholesky",
+        "precision": PRECISION_TEXT[args.precision],
         "launch": "one CUDA graph per solve, captured on the second solve of the batch and replayed",
     }
 
@@ -221,7 +236,7 @@ def run_served(args, local, backend):
     rates = [float(x) for x in args.serve_rates.split(",") if x.strip()]
     pool = synth.make_windows("c4", args.serve_pool, seed=args.seed + 500)
     rigs = 128
-    server = backend.Server(device=local, iterations=1, policy=abi.MARGIN_OLD)
+    server = backend.Server(device=local, iterations=1, policy=abi.MARGIN_OLD, precision=headline_precision(args))
     # warm-up: repeated full-pool bursts, so that both solvers reach their working
     # size (growing pinned staging later would synchronize the device mid-trace)
     for _ in range(4):
@@ -385,7 +400,8 @@ def run_e2e_pipelined(args, local, backend, windows, rank):
     extra = synth.make_windows("c4", 3 * args.windows, seed=rank_seed(args.seed, rank) + 7777)
     pool = list(windows) + extra
     init = [w.state_vector() for w in pool]
-    server = backend.Server(device=local, iterations=args.iterations, policy=abi.MARGIN_OLD, max_batch_windows=args.windows)
+    server = backend.Server(device=local, iterations=args.iterations, policy=abi.MARGIN_OLD, max_batch_windows=args.windows,
+                            precision=headline_precision(args))
     victims = [-1] * len(pool)
     for _ in range(2):  # warm-up: both solvers and their pinned staging reach the batch size
         server.replay(pool, victims, np.zeros(len(pool)))
@@ -507,70 +523,77 @@ def run_imu(args, local, backend):
 
 
 def run_mixed(args, local, backend, windows, init, solver, dist):
-    """The batch in CGMLI_PRECISION_MIXED: device time of the same solve, and its
-    accuracy against the FP64 path (first step dx of every window, final states)."""
+    """The batch in the other precision (FP64 when the headline is mixed): device time
+    of the same solve, and the mixed form's accuracy against FP64 (first step dx of
+    every window, final states after the solve)."""
     for w, x in zip(windows, init):
         w.set_state_vector(x)
-    mixed = backend.Solver(device=local, precision=abi.PRECISION_MIXED)
-    mixed.set_tuning(**solver.get_tuning())
-    mixed.set_windows(windows)
-    mixed.checkpoint()
+    other_prec = abi.PRECISION_FP64 if args.precision == "mixed" else abi.PRECISION_MIXED
+    other = backend.Solver(device=local, precision=other_prec)
+    other.set_tuning(**{k: v for k, v in solver.get_tuning().items() if k != "ms"})
+    other.set_windows(windows)
+    other.checkpoint()
+    mixed, f64 = (solver, other) if args.precision == "mixed" else (other, solver)
     # first LM step at lambda = 1e-4 from the initial states, both precisions
     solver.rollback()
     solver.step(1e-4)
-    mixed.step(1e-4)
+    other.step(1e-4)
     dx_retained, dx_all = 0.0, 0.0
     for i, w in enumerate(windows):
         nr = w.retained_dim()
-        a, b = mixed.read_step(i)["delta"], solver.read_step(i)["delta"]
+        a, b = mixed.read_step(i)["delta"], f64.read_step(i)["delta"]
         dx_retained = max(dx_retained, float(np.linalg.norm(a[:nr] - b[:nr]) / max(np.linalg.norm(b[:nr]), 1e-300)))
         dx_all = max(dx_all, float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)))
     for _ in range(max(3, args.warmup)):
-        mixed.rollback()
-        mixed.solve(args.iterations)
-        mixed.synchronize()
+        other.rollback()
+        other.solve(args.iterations)
+        other.synchronize()
     ms = []
     for _ in range(args.mixed_steps):
-        mixed.rollback()
-        mixed.solve(args.iterations)
-        mixed.synchronize()
-        ms.append(mixed.timing()[0])
-    mixed.kernel_times(enable=1)
+        other.rollback()
+        other.solve(args.iterations)
+        other.synchronize()
+        ms.append(other.timing()[0])
+    other.kernel_times(enable=1)
     for _ in range(args.mixed_steps):
-        mixed.rollback()
-        mixed.solve(args.iterations)
-        mixed.synchronize()
-    kt = mixed.kernel_times(enable=-1)
-    mixed.kernel_times(enable=0)
+        other.rollback()
+        other.solve(args.iterations)
+        other.synchronize()
+    kt = other.kernel_times(enable=-1)
+    other.kernel_times(enable=0)
     total = max_over_ranks(sum(ms), dist)
-    # final states of both precisions, relative to the distance travelled
-    solver.rollback()
-    solver.solve(args.iterations)
-    solver.synchronize()
-    solver.read_states()
+    # final states of both precisions, relative to the states
+    f64.rollback()
+    f64.solve(args.iterations)
+    f64.synchronize()
+    f64.read_states()
     x64 = [w.state_vector() for w in windows]
-    c64 = [r.final_cost for r in solver.reports()]
-    a64 = [r.accepted_steps for r in solver.reports()]
+    c64 = [r.final_cost for r in f64.reports()]
+    a64 = [r.accepted_steps for r in f64.reports()]
+    mixed.rollback()
+    mixed.solve(args.iterations)
+    mixed.synchronize()
     mixed.read_states()
     same = [i for i, r in enumerate(mixed.reports()) if r.accepted_steps == a64[i]]
     state_err = max(float(np.linalg.norm(windows[i].state_vector() - x64[i]) / np.linalg.norm(x64[i])) for i in same)
     cost_err = max(abs(mixed.reports()[i].final_cost - c64[i]) / abs(c64[i]) for i in same)
     statuses = {}
-    for r in mixed.reports():
+    for r in other.reports():
         key = abi.ERRORS.get(r.status, r.status)
         statuses[key] = statuses.get(key, 0) + 1
     for w, x in zip(windows, init):
         w.set_state_vector(x)
     solver.rollback()
-    mixed.close()
-    return {"windows_per_s": args.windows * len(ms) / (total / 1e3), "ms_per_step": total / len(ms), "steps": len(ms),
-            "step_dx_rel_err_vs_fp64_max": {"retained": dx_retained, "all": dx_all, "bar": 1e-6},
-            "final_vs_fp64_max": {"state_rel": state_err, "cost_rel": cost_err, "windows_compared": len(same),
-                                  "windows_with_other_accept_count": len(windows) - len(same)},
+    other.close()
+    other_name = "fp64" if args.precision == "mixed" else "mixed"
+    return {"precision": other_name, "windows_per_s": args.windows * len(ms) / (total / 1e3), "ms_per_step": total / len(ms),
+            "steps": len(ms),
+            "mixed_step_dx_rel_err_vs_fp64_max": {"retained": dx_retained, "all": dx_all, "bar": 1e-6},
+            "mixed_final_vs_fp64_max": {"state_rel": state_err, "cost_rel": cost_err, "windows_compared": len(same),
+                                        "windows_with_other_accept_count": len(windows) - len(same)},
             "window_status": statuses,
             "kernel_ms_per_step": {k: v[0] / len(ms) for k, v in kt.items()},
-            "precision": "fp32 Jacobians, robust weights, compensated fp32 landmark Hessian sums; fp64 residuals, gradients, "
-                         "reduced system, Cholesky"}
+            "precision_detail": PRECISION_TEXT[other_name]}
 
 
 def run_reference(args, world, rank):
@@ -631,7 +654,7 @@ def main():
 
     windows = synth.make_windows("c4", args.windows, seed=rank_seed(args.seed, rank))
     init = [w.state_vector() for w in windows]
-    solver = backend.Solver(device=local)
+    solver = backend.Solver(device=local, precision=headline_precision(args))
     # the work decomposition comes from the autotuner (timed on this batch); it
     # leaves the batch set with the fastest one
     tuning = solver.autotune(windows, args.iterations)
@@ -729,7 +752,7 @@ def main():
     h2d = sum(window_bytes(w)[0] for w in windows)
     d2h = sum(window_bytes(w)[1] for w in windows)
     e2e_times = []
-    e2e_solver = backend.Solver(device=local)
+    e2e_solver = backend.Solver(device=local, precision=headline_precision(args))
     e2e_solver.set_tuning(**{k: v for k, v in tuning.items() if k != "ms"})
     for it in range(1 + max(1, args.steps // 2)):
         for w, x in zip(windows, init):
@@ -759,7 +782,7 @@ def main():
     plain = None
     if rank == 0 and args.plain_windows > 0:
         pw = windows[:args.plain_windows]
-        ps = backend.Solver(device=local)
+        ps = backend.Solver(device=local, precision=headline_precision(args))
         lat = []
         for i, w in enumerate(pw):
             w.set_state_vector(init[i])
@@ -776,7 +799,8 @@ def main():
         lat.sort()
         plain = {"windows_per_s": 1000.0 / statistics.mean(lat), "p50_ms": lat[len(lat) // 2],
                  "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))], "windows": len(lat),
-                 "workload": f"the first {len(lat)} windows of the batch, each solved alone ({args.iterations} LM iterations)"}
+                 "workload": f"the first {len(lat)} windows of the batch, each solved alone ({args.iterations} LM iterations, "
+                             f"{args.precision}, as the batched value)"}
 
     served = run_served(args, local, backend) if rank == 0 and args.serve_rates.strip() else None
     configs = run_configs(args, local, backend) if rank == 0 and not args.no_configs else None
@@ -823,12 +847,12 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup),
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic", "config": dict(config_dict(args, world), tuning=tuning),
+            "dtype": DTYPE[args.precision], "data": "synthetic", "config": dict(config_dict(args, world), tuning=tuning),
             "clocks": clocks.summary(), "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
             "cpu_baseline": cpu_baseline, "plain_path": plain,
             "served_vs_plain": (value / world) / plain["windows_per_s"] if plain else None,
             "served": served, "marginalization": marg, "configs": configs, "imu_preintegration": imu,
-            "nis_gate": gated, "calibration_information": calib, "mixed_precision": mixed,
+            "nis_gate": gated, "calibration_information": calib, "other_precision": mixed,
             "batch_latency_ms": {"p50": sorted(dev_ms)[len(dev_ms) // 2], "p99": max(dev_ms)},
             "window_status": statuses, "wall_s": wall,
         }

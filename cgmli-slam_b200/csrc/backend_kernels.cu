@@ -797,11 +797,31 @@ __device__ void blockedSolve(const double* L, int n, double* v, double* blk) {
 // diagonal in shared memory, for the prediction (and refinement) products.
 constexpr int kFacPanel = 32;
 
-// h = S_undamped v from the stored upper triangle (A[p + q n], p < q) and diagonal hd.
+// a[0..32) of every lane -> the warp's sum of a[lane] in lane `lane`, by recursive
+// halving: at offset o each lane keeps the half of its entries its bit o selects and
+// adds its partner's copy of that half (31 shuffles for 32 sums instead of 160).
+__device__ __forceinline__ double transposeSum(double (&a)[32]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        const bool hi = (lane & o) != 0;
+#pragma unroll
+        for (int k = 0; k < o; ++k) {
+            const double send = hi ? a[k] : a[k + o];
+            const double keep = hi ? a[k + o] : a[k];
+            a[k] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    }
+    return a[0];
+}
+
+// h = S_undamped v from the stored upper triangle (A[p + q n], p < q) and diagonal hd:
+// a thread per row for the columns right of the diagonal (consecutive rows coalesce,
+// four independent sums keep four loads in flight), a warp per column for the rows
+// above it.  The form for the narrow windows of a batch (many CTAs per GPU).
 __device__ void undampedProduct(const double* A, const double* hd, int n, const double* v, double* h) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
-    // four independent sums per loop keep four L2 loads in flight per thread
-    for (int i = tid; i < n; i += blockDim.x) {  // columns j > i of row i: consecutive i coalesce
+    for (int i = tid; i < n; i += blockDim.x) {
         double s0 = hd[i] * v[i], s1 = 0, s2 = 0, s3 = 0;
         int j = i + 1;
         for (; j + 4 <= n; j += 4) {
@@ -814,7 +834,7 @@ __device__ void undampedProduct(const double* A, const double* hd, int n, const 
         h[i] = (s0 + s1) + (s2 + s3);
     }
     __syncthreads();
-    for (int i = warp; i < n; i += nw) {  // rows j < i of column i
+    for (int i = warp; i < n; i += nw) {
         double s0 = 0, s1 = 0;
         int j = lane;
         for (; j + 32 < i; j += 64) {
@@ -826,6 +846,47 @@ __device__ void undampedProduct(const double* A, const double* hd, int n, const 
         if (lane == 0) h[i] += s;
     }
     __syncthreads();
+}
+
+// The same product for a lone wide window (one CTA over a large system), by blocks of
+// 32 columns: every warp owns a fixed set of 32-row chunks, its lanes
+// read their rows' 32 entries of the block (one coalesced load per column, 32 in
+// flight), add the row part to h and accumulate the column part, which is folded
+// across the warp (transposeSum) and across warps in shared memory.
+__device__ void undampedProductBlocks(const double* A, const double* hd, int n, const double* v, double* h) {
+    constexpr int kWarps = kFactorThreads / 32;
+    __shared__ double colPart[kWarps * 32];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int i = tid; i < n; i += blockDim.x) h[i] = hd[i] * v[i];
+    __syncthreads();
+    for (int j0 = 0; j0 < n; j0 += 32) {
+        const int jw = min(32, n - j0);
+        double acc[32];
+#pragma unroll
+        for (int c = 0; c < 32; ++c) acc[c] = 0.0;
+        for (int i0 = warp * 32; i0 < j0 + jw; i0 += kWarps * 32) {  // rows above the block's columns
+            const int i = i0 + lane;
+            const double vi = i < n ? v[i] : 0.0;
+            double row = 0;
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+                if (c < jw && i < j0 + c) {  // strict upper: row i, column j0 + c
+                    const double a = A[i + (long long)(j0 + c) * n];
+                    acc[c] += a * vi;
+                    row += a * v[j0 + c];
+                }
+            }
+            if (i < n) h[i] += row;  // row i belongs to this warp in every block
+        }
+        colPart[warp * 32 + lane] = transposeSum(acc);
+        __syncthreads();
+        if (tid < jw) {
+            double t = 0;
+            for (int w = 0; w < kWarps; ++w) t += colPart[w * 32 + tid];
+            h[j0 + tid] += t;
+        }
+        __syncthreads();
+    }
 }
 
 // Solve-time charts of one window's reduced system (kCol* per retained column),
@@ -990,43 +1051,90 @@ __device__ __forceinline__ void trailingTile(const double* V, long long ldv, int
 // refinement steps against the assembled FP64 system and the predicted
 // reduction of the state part; writes dr, predState and solveStatus.  x, hd,
 // h (scratch), blk and dmp are the CTA's shared vectors.
+template <bool kBlocks>
 __device__ void factorTail(const DevBatch& B, const WinDesc& wd, int wdx, double lambda, int refinement, const double* A, double* x,
                            const double* hd, double* h, double* blk, const double* dmp, double* red) {
+    auto product = [&](const double* v, double* out) {
+        if constexpr (kBlocks) undampedProductBlocks(A, hd, wd.Nr, v, out);
+        else undampedProduct(A, hd, wd.Nr, v, out);
+    };
     const int n = wd.Nr, Npc = wd.Npc, K = wd.K;
     const bool charts = wd.charts != 0;
     const double* acc = B.acc + wd.acc0;
     const long long nS = (long long)Npc * (Npc + 1) / 2;
     const double* rhsOut = B.rhs + wd.vec0;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+    __shared__ double colPart[kFactorThreads];  // per warp, 32 column sums of the backward substitution
     // ---- backward substitution L^T x = y by panels (L lower in A)
     for (int k0 = ((n - 1) / kFacPanel) * kFacPanel; k0 >= 0; k0 -= kFacPanel) {
         const int bw = min(kFacPanel, n - k0);
-        for (int c = warp; c < bw; c += nw) {
-            double s0 = 0, s1 = 0;
-            int r = k0 + bw + lane;
-            for (; r + 32 < n; r += 64) {
-                s0 += A[r + (long long)(k0 + c) * n] * x[r];
-                s1 += A[r + 32 + (long long)(k0 + c) * n] * x[r + 32];
+        if (!kBlocks) {  // x[k0 + c] -= sum over the rows below of L[r][k0 + c] x[r]: a warp per column
+            for (int c = warp; c < bw; c += nw) {
+                double s0 = 0, s1 = 0;
+                int r = k0 + bw + lane;
+                for (; r + 32 < n; r += 64) {
+                    s0 += A[r + (long long)(k0 + c) * n] * x[r];
+                    s1 += A[r + 32 + (long long)(k0 + c) * n] * x[r + 32];
+                }
+                if (r < n) s0 += A[r + (long long)(k0 + c) * n] * x[r];
+                const double s = warpSum(s0 + s1);
+                if (lane == 0) x[k0 + c] -= s;
             }
-            if (r < n) s0 += A[r + (long long)(k0 + c) * n] * x[r];
-            const double s = warpSum(s0 + s1);
-            if (lane == 0) x[k0 + c] -= s;
-        }
-        for (int t = tid; t < bw * bw; t += blockDim.x) {
-            const int c = t / bw, r = t % bw;
-            blk[r + c * kFacPanel] = r >= c ? A[(k0 + r) + (long long)(k0 + c) * n] : 0.0;
-        }
-        __syncthreads();
-        if (warp == 0) {  // lane r holds y_r; column sweep x_c = y_c / L_cc, y_r -= L[c][r] x_c (r < c)
-            double y = lane < bw ? x[k0 + lane] : 0.0;
-            for (int c = bw - 1; c >= 0; --c) {
-                const double xc = __shfl_sync(0xffffffffu, y, c) / blk[c + c * kFacPanel];
-                if (lane < c) y -= blk[c + lane * kFacPanel] * xc;
-                if (lane == c) y = xc;
+        } else if (k0 + bw < n) {  // the same by row chunks: lanes own rows, 32 column sums folded per warp
+            double acc[32];
+#pragma unroll
+            for (int c = 0; c < 32; ++c) acc[c] = 0.0;
+            for (int r0 = k0 + bw + warp * 32; r0 < n; r0 += nw * 32) {
+                const int r = r0 + lane;
+                const double xr = r < n ? x[r] : 0.0;
+#pragma unroll
+                for (int c = 0; c < 32; ++c)
+                    if (c < bw && r < n) acc[c] += A[r + (long long)(k0 + c) * n] * xr;
             }
-            if (lane < bw) x[k0 + lane] = y;
+            colPart[warp * 32 + lane] = transposeSum(acc);
+            __syncthreads();
+            if (tid < bw) {
+                double t = 0;
+                for (int w = 0; w < nw; ++w) t += colPart[w * 32 + tid];
+                x[k0 + tid] -= t;
+            }
         }
-        __syncthreads();
+        if constexpr (kBlocks) {  // warp 0: lane r holds y_r and column r of the block (32 loads in flight)
+            __syncthreads();
+            if (warp == 0) {
+                double col[kFacPanel];
+#pragma unroll
+                for (int c = 0; c < kFacPanel; ++c) col[c] = (lane < c && c < bw) ? A[(k0 + c) + (long long)(k0 + lane) * n] : 0.0;
+                const double inv = lane < bw ? 1.0 / A[(k0 + lane) + (long long)(k0 + lane) * n] : 0.0;
+                double y = lane < bw ? x[k0 + lane] : 0.0;
+#pragma unroll
+                for (int c = kFacPanel - 1; c >= 0; --c) {
+                    if (c < bw) {
+                        const double xc = __shfl_sync(0xffffffffu, y, c) * __shfl_sync(0xffffffffu, inv, c);
+                        if (lane < c) y -= col[c] * xc;
+                        if (lane == c) y = xc;
+                    }
+                }
+                if (lane < bw) x[k0 + lane] = y;
+            }
+            __syncthreads();
+        } else {
+            for (int t = tid; t < bw * bw; t += blockDim.x) {
+                const int c = t / bw, r = t % bw;
+                blk[r + c * kFacPanel] = r >= c ? A[(k0 + r) + (long long)(k0 + c) * n] : 0.0;
+            }
+            __syncthreads();
+            if (warp == 0) {  // lane r holds y_r; column sweep x_c = y_c / L_cc, y_r -= L[c][r] x_c (r < c)
+                double y = lane < bw ? x[k0 + lane] : 0.0;
+                for (int c = bw - 1; c >= 0; --c) {
+                    const double xc = __shfl_sync(0xffffffffu, y, c) / blk[c + c * kFacPanel];
+                    if (lane < c) y -= blk[c + lane * kFacPanel] * xc;
+                    if (lane == c) y = xc;
+                }
+                if (lane < bw) x[k0 + lane] = y;
+            }
+            __syncthreads();
+        }
     }
     double* dr = B.dr + wd.vec0;
     for (int i = tid; i < n; i += blockDim.x) dr[i] = x[i];
@@ -1034,7 +1142,7 @@ __device__ void factorTail(const DevBatch& B, const WinDesc& wd, int wdx, double
     // ---- iterative refinement against the assembled FP64 system
     for (int it = 0; it < refinement; ++it) {
         if (charts) {
-            undampedProduct(A, hd, n, dr, h);
+            product(dr, h);
             for (int i = tid; i < n; i += blockDim.x) x[i] = chartFixed(B, wd, i) ? 0.0 : rhsOut[i] - (h[i] + dmp[i] * dr[i]);
             __syncthreads();
             blockedSolve(A, n, x, blk);
@@ -1044,7 +1152,7 @@ __device__ void factorTail(const DevBatch& B, const WinDesc& wd, int wdx, double
         }
         for (int i = tid; i < n; i += blockDim.x) x[i] = dampingOf(B, wd, i, lambda);  // damping of row i, kept in x for this pass
         __syncthreads();
-        undampedProduct(A, hd, n, dr, h);
+        product(dr, h);
         for (int i = tid; i < n; i += blockDim.x) x[i] = rhsOf(B, wd, i) - (h[i] + x[i] * dr[i]);
         __syncthreads();
         blockedSolve(A, n, x, blk);
@@ -1053,7 +1161,7 @@ __device__ void factorTail(const DevBatch& B, const WinDesc& wd, int wdx, double
     }
     // predicted reduction of the state part with the undamped (S_visual + H_ret):
     //   -dx^T (g_r + 0.5 (S_v + H_ret) dx); the landmark terms are added per landmark.
-    undampedProduct(A, hd, n, dr, h);
+    product(dr, h);
     auto gradient = [&](int i) {  // g_r + G_v of column i (the full gradient, without the Schur term)
         double g = B.gret[wd.vec0 + i];
         const int p = pcOfRetained(i, K);
@@ -1180,7 +1288,7 @@ __global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int re
         if (tid == 0) B.solveStatus[wdx] = CGMLI_E_NOT_PD;
         return;
     }
-    factorTail(B, wd, wdx, lambda, refinement, A, x, hd, da, blk, dmp, red);
+    factorTail<false>(B, wd, wdx, lambda, refinement, A, x, hd, da, blk, dmp, red);
 }
 
 // ---- wide windows -----------------------------------------------------------------------
@@ -1191,7 +1299,7 @@ __global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int re
 // in one CTA (k_wide_prepare).  Then, per panel of kFacPanel columns:
 //   - its diagonal block is factored by one warp, lane i owning row i, with the
 //     forward substitution of the right-hand side over the block
-//     (factorDiagWarp: a right-looking sweep with warp-level sync only);
+//     (wideDiagBlock: a right-looking sweep in registers, warp-level sync only);
 //   - the rows below it are solved against that block (L21 = A21 L11^-T), one
 //     thread per row with the row in registers, and each row's right-hand side
 //     entry takes its update y2 -= L21 y1 on the way (k_wide_trsm);
@@ -1253,19 +1361,21 @@ __global__ void __launch_bounds__(kFactorThreads) k_wide_prepare(DevBatch B, dou
     if (Sdebug) storeSdebug(A, n, Sdebug + wd.dense0);
 }
 
-// Cholesky of one panel's diagonal block by one warp, in place in T (bw x bw lower,
-// row-major with stride kDiagStride), with the forward substitution of x1 (bw
-// entries); T's diagonal becomes L's.  Lane i holds row i in registers; column c's
-// pivot and the entries L[j][c] of the rank-1 update come by shuffles, so the
-// block needs no shared-memory round trip between columns.  Returns false
-// (uniform over the warp) on a pivot that is not positive and finite.
+// Cholesky of the diagonal block at k0 of window w by the calling warp, with the
+// forward substitution of x over the block; the block is written back as L11 (its
+// diagonal the roots).  Lane i holds row i in registers, read and written with one
+// coalesced access per column (32 loads in flight); column c's pivot and the entries
+// L[j][c] of the rank-1 update come by shuffles, so the sweep needs no memory round
+// trip.  Returns false (uniform over the warp) on a pivot that is not positive and finite.
 constexpr int kDiagStride = kFacPanel + 1;
-__device__ bool factorDiagWarp(double* T, int bw, double* x1) {
-    const int lane = threadIdx.x & 31;
+__device__ bool wideDiagBlock(const DevBatch& B, const WinDesc& wd, int k0) {
+    const int lane = threadIdx.x & 31, n = wd.Nr, bw = min(kFacPanel, n - k0);
+    double* A = B.Sglob + wd.dense0;
+    double* x = B.facVec + 3ll * wd.vec0;
     double r[kFacPanel];
 #pragma unroll
-    for (int j = 0; j < kFacPanel; ++j) r[j] = (lane < bw && j <= lane) ? T[lane * kDiagStride + j] : 0.0;
-    double xi = lane < bw ? x1[lane] : 0.0;
+    for (int j = 0; j < kFacPanel; ++j) r[j] = (lane < bw && j <= lane) ? A[(k0 + lane) + (long long)(k0 + j) * n] : 0.0;
+    double xi = lane < bw ? x[k0 + lane] : 0.0;
     bool ok = true;
 #pragma unroll
     for (int c = 0; c < kFacPanel; ++c) {
@@ -1274,10 +1384,10 @@ __device__ bool factorDiagWarp(double* T, int bw, double* x1) {
             if (!(d > 0) || !isfinite(d)) {
                 ok = false;  // every lane received the same d
             } else {
-                const double l = sqrt(d);
-                const double lic = lane > c ? r[c] / l : (lane == c ? l : 0.0);  // L[lane][c]
+                const double il = rsqrt(d), l = d * il;  // one reciprocal square root per column
+                const double lic = lane > c ? r[c] * il : (lane == c ? l : 0.0);  // L[lane][c]
                 if (lane >= c) r[c] = lic;
-                const double yc = __shfl_sync(0xffffffffu, xi, c) / l;
+                const double yc = __shfl_sync(0xffffffffu, xi, c) * il;
                 if (lane == c) xi = yc;
                 else if (lane > c) xi -= lic * yc;
 #pragma unroll
@@ -1291,27 +1401,8 @@ __device__ bool factorDiagWarp(double* T, int bw, double* x1) {
     if (!ok) return false;
 #pragma unroll
     for (int j = 0; j < kFacPanel; ++j)
-        if (lane < bw && j <= lane) T[lane * kDiagStride + j] = r[j];
-    if (lane < bw) x1[lane] = xi;
-    return true;
-}
-
-// The diagonal block at k0 of window w: staged from A, factored by the calling warp,
-// written back (L11, its diagonal as the roots).  Returns false on a failed pivot.
-__device__ bool wideDiagBlock(const DevBatch& B, const WinDesc& wd, int k0, double* T) {
-    const int lane = threadIdx.x & 31, n = wd.Nr, bw = min(kFacPanel, n - k0);
-    double* A = B.Sglob + wd.dense0;
-    double* x = B.facVec + 3ll * wd.vec0;
-    for (int q = lane; q < bw * bw; q += 32) {
-        const int i = q / bw, j = q % bw;
-        if (j <= i) T[i * kDiagStride + j] = A[(k0 + i) + (long long)(k0 + j) * n];
-    }
-    __syncwarp();
-    if (!factorDiagWarp(T, bw, x + k0)) return false;
-    for (int q = lane; q < bw * bw; q += 32) {
-        const int i = q / bw, j = q % bw;
-        if (j <= i) A[(k0 + i) + (long long)(k0 + j) * n] = T[i * kDiagStride + j];
-    }
+        if (lane < bw && j <= lane) A[(k0 + lane) + (long long)(k0 + j) * n] = r[j];
+    if (lane < bw) x[k0 + lane] = xi;
     return true;
 }
 
@@ -1319,8 +1410,7 @@ __device__ bool wideDiagBlock(const DevBatch& B, const WinDesc& wd, int k0, doub
 __global__ void __launch_bounds__(32) k_wide_diag(DevBatch B) {
     const int wdx = B.wideList[blockIdx.x];
     if (B.lm[wdx].mode == kModeDone) return;
-    __shared__ double T[kFacPanel * kDiagStride];
-    if (!wideDiagBlock(B, B.win[wdx], 0, T) && threadIdx.x == 0) B.facFailed[wdx] = 1;
+    if (!wideDiagBlock(B, B.win[wdx], 0) && threadIdx.x == 0) B.facFailed[wdx] = 1;
 }
 
 // Rows below the panel at k0: L21 = A21 L11^-T by forward substitution, one thread
@@ -1336,9 +1426,11 @@ __global__ void __launch_bounds__(kFactorThreads) k_wide_trsm(DevBatch B, int k0
     __shared__ double L[kFacPanel * kDiagStride], y1[kFacPanel], inv[kFacPanel];
     double* A = B.Sglob + wd.dense0;
     double* x = B.facVec + 3ll * wd.vec0;
-    for (int q = threadIdx.x; q < bw * bw; q += blockDim.x) {
-        const int i = q / bw, j = q % bw;
-        L[i * kDiagStride + j] = j <= i ? A[(k0 + i) + (long long)(k0 + j) * n] : 0.0;
+    static_assert(kFacPanel * kFacPanel == 4 * kFactorThreads, "four staged entries per thread");
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {  // by columns (coalesced), four loads in flight
+        const int q = threadIdx.x + u * kFactorThreads, i = q % kFacPanel, j = q / kFacPanel;
+        L[i * kDiagStride + j] = (i < bw && j <= i) ? A[(k0 + i) + (long long)(k0 + j) * n] : 0.0;
     }
     if (threadIdx.x < bw) {
         y1[threadIdx.x] = x[k0 + threadIdx.x];
@@ -1385,9 +1477,8 @@ __global__ void __launch_bounds__(kFactorThreads) k_wide_trailing(DevBatch B, in
     // last tile) read the next column's top, inside the slot, and only reach masked entries
     trailingTile(A + (k0 + bw) + (long long)k0 * n, n, rb, cb, bw, m2, A, n, k0);
     if (t == 0) {  // tile (0, 0) is the next panel's diagonal block, complete now
-        __shared__ double T[kFacPanel * kDiagStride];
         __syncwarp();
-        if (!wideDiagBlock(B, wd, k0 + bw, T) && (threadIdx.x & 31) == 0) B.facFailed[wdx] = 1;
+        if (!wideDiagBlock(B, wd, k0 + bw) && (threadIdx.x & 31) == 0) B.facFailed[wdx] = 1;
     }
 }
 
@@ -1408,9 +1499,10 @@ __global__ void __launch_bounds__(kFactorThreads) k_wide_finish(DevBatch B, int 
     double* h = dmp + n;
     double* blk = h + n;
     const double* src = B.facVec + 3ll * wd.vec0;
+#pragma unroll 4
     for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) x[i] = src[i];
     __syncthreads();
-    factorTail(B, wd, wdx, B.lm[wdx].lambda, refinement, B.Sglob + wd.dense0, x, hd, h, blk, dmp, red);
+    factorTail<true>(B, wd, wdx, B.lm[wdx].lambda, refinement, B.Sglob + wd.dense0, x, hd, h, blk, dmp, red);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1570,7 +1662,8 @@ __global__ void __launch_bounds__(256) k_lm_update(DevBatch B, int maxIterations
     __shared__ double red[32];
     double cost = 0, pred = 0, trial = 0, mx = 0;
     int valid = 1, tvalid = 1;
-    for (int i = threadIdx.x; i < wd.L; i += blockDim.x) {
+#pragma unroll 4
+    for (int i = threadIdx.x; i < wd.L; i += blockDim.x) {  // unrolled: four landmarks' loads in flight
         const int l = wd.lm0 + i;
         cost += B.lmCost[l];
         pred += B.lmPred[l];
