@@ -60,7 +60,8 @@ def parse():
     p.add_argument("--windows", type=int, default=512)
     p.add_argument("--iterations", type=int, default=5)
     p.add_argument("--seed", type=int, default=20260101)
-    p.add_argument("--cpu-sample", type=int, default=24, help="windows timed on the host for the CPU baseline")
+    p.add_argument("--cpu-sample", type=int, default=48,
+                   help="windows timed on the host for the CPU baseline and the reference arm (every len/n-th of the batch)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--plain-windows", type=int, default=64, help="windows of the batch solved one at a time for the plain path")
     p.add_argument("--marg-steps", type=int, default=3, help="timed batched marginalizations of the solved batch (0: off)")
@@ -87,10 +88,16 @@ def dist_env():
     return world, rank, local
 
 
-# k_lin_landmark + k_lin_pairs + k_lin_schur DRAM read + write per observation (ncu,
-# 64-window batch): mostly the 448-byte staged row written by the landmark pass and
-# read back in key order by the J^T J pass
-LIN_DRAM_BYTES_PER_OBS = 1536
+# k_lin_landmark + k_lin_pairs + k_lin_schur DRAM read + write per observation, by
+# precision: dram__bytes_read.sum + dram__bytes_write.sum of the three kernels of one
+# linearization of the first 64 windows of the batch (451,950 observations) in an ncu
+# capture (profiles/lin_traffic_c4x64.md).  Mostly the staged weighted rows (224 bytes
+# mixed, 448 FP64) written by the landmark pass and read back in key order.
+LIN_DRAM_BYTES_PER_OBS = {"mixed": 990.6, "fp64": 1536.0}
+# the landmark pass's limiter (profiles/lin_landmark_mixed_c4x64.md): FP64 pipe and
+# issue fractions of the single-kernel capture
+LIN_LANDMARK_PROFILE = {"fp64_pipe_pct": 11.0, "issue_active_pct": 21.1, "dram_throughput_pct": 5.6, "warps_active_pct": 13.4,
+                        "registers": 168, "top_stall": "long scoreboard (4.7 per issue)"}
 
 
 def rank_seed(seed: int, rank: int) -> int:
@@ -596,6 +603,26 @@ def run_mixed(args, local, backend, windows, init, solver, dist):
             "precision_detail": PRECISION_TEXT[other_name]}
 
 
+def strided_sample(windows, n):
+    """Every (len / n)-th window of the batch, from the offset whose sample has the mean
+    observation count closest to the batch's, so that the CPU sample has the batch's size
+    distribution; returns the indices and a size summary of sample and batch."""
+    stride = max(1, len(windows) // max(1, n))
+    F = np.array([w.window.num_observations for w in windows], dtype=np.float64)
+    # the offset whose sample's mean observation count is closest to the batch's
+    offset = min(range(stride), key=lambda o: abs(F[o::stride][:n].mean() - F.mean()))
+    idx = list(range(offset, len(windows), stride))[:n]
+
+    def summary(ws):
+        L = np.array([w.window.num_landmarks for w in ws])
+        K = np.array([w.window.num_keyframes for w in ws])
+        F = np.array([w.window.num_observations for w in ws])
+        return {"windows": len(ws), "landmarks_p10_p50_p90": [int(np.percentile(L, q)) for q in (10, 50, 90)],
+                "keyframes_mean": round(float(K.mean()), 2), "observations_mean": round(float(F.mean()), 1)}
+
+    return idx, {"stride": stride, "offset": offset, "sample": summary([windows[i] for i in idx]), "batch": summary(windows)}
+
+
 def run_reference(args, world, rank):
     """CPU path of the reference algorithm on the host cores (FP64 oracle)."""
     if rank != 0:
@@ -603,9 +630,11 @@ def run_reference(args, world, rank):
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O  # CPU arm: the only place bench.py runs the oracle besides cpu_baseline
 
-    n = max(1, args.cpu_sample)
     threads = os.cpu_count() or 1
-    windows = synth.make_windows("c4", n, seed=args.seed)
+    batch = synth.make_windows("c4", args.windows, seed=args.seed)
+    idx, dist_info = strided_sample(batch, max(1, min(args.cpu_sample, args.windows)))
+    windows = [batch[i] for i in idx]
+    n = len(windows)
     init = [w.state_vector() for w in windows]
     arr = synth.window_array(windows)
     for _ in range(max(0, min(args.warmup, 1))):
@@ -626,7 +655,9 @@ def run_reference(args, world, rank):
         "warmup": args.warmup, "ms_per_step": 1000 * total / len(times), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_dict(args, world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{n} windows of the batched workload per step, {args.iterations} LM iterations, FP64 oracle"},
+                         "sample": f"{n} windows of the batched workload per step (every {dist_info['stride']}th of the "
+                                   f"{args.windows}), {args.iterations} LM iterations, FP64 oracle",
+                         "sample_sizes": dist_info},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "reference Ceres/Eigen CPU path cannot be built offline; the FP64 C++ restatement runs on all host threads",
     }
@@ -710,9 +741,12 @@ def main():
     # DRAM traffic of one linearization launch over the batch: the per-observation
     # read + write bytes of the three kernels in an ncu capture of the first 64
     # windows (451,950 observations), scaled by this batch's observations
-    traffic = LIN_DRAM_BYTES_PER_OBS * sum(w.window.num_observations for w in windows)
+    traffic = LIN_DRAM_BYTES_PER_OBS[args.precision] * sum(w.window.num_observations for w in windows)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "traffic_source": "ncu capture of 64 windows, scaled by observations",
+                "traffic": traffic, "traffic_source": "ncu dram bytes of the three kernels on the first 64 windows, per observation, "
+                                                      "scaled by this batch's observations",
+                "limiter": "FP64 issue and dependent-load latency, not HBM: the landmark pass's single-kernel capture",
+                "landmark_pass_profile": LIN_LANDMARK_PROFILE,
                 "algorithmic_bytes_per_launch": bytes_per_solve / max(1, args.iterations),
                 "kernel": "k_lin_landmark + k_lin_pairs + k_lin_schur", "peak_source": peak_kind,
                 "launch_avg_ms": lin_ms / max(1, lin_calls), "window_linearizations_per_step": lin_passes,
@@ -817,11 +851,12 @@ def main():
         sys.path.insert(0, str(ROOT / "oracle"))
         import oracle as O  # cpu_baseline leg
 
-        n = max(1, min(args.cpu_sample, args.windows))
         threads = os.cpu_count() or 1
-        sample = windows[:n]
-        for w, x in zip(sample, init):
-            w.set_state_vector(x)
+        idx, dist_info = strided_sample(windows, max(1, min(args.cpu_sample, args.windows)))
+        n = len(idx)
+        sample = [windows[i] for i in idx]
+        for i in idx:
+            windows[i].set_state_vector(init[i])
         arr = synth.window_array(sample)
         t2 = time.perf_counter()
         st, reps = O.lm_solve_batch(arr, n, args.iterations, threads)
@@ -834,14 +869,15 @@ def main():
         cpu_states = [w.state_vector() for w in sample]
         solver.read_states()
         errs = []
-        for w, xc, x0 in zip(sample, cpu_states, init[:n]):
+        for w, xc, x0 in zip(sample, cpu_states, [init[i] for i in idx]):
             xg = w.state_vector()
             errs.append(float(np.linalg.norm(xg - xc) / max(np.linalg.norm(xc - x0), 1e-300)))
         for w, x in zip(windows, init):
             w.set_state_vector(x)
         cpu_baseline = {"value": n / cpu_s, "unit": UNIT, "cores": threads, "kind": "port",
-                        "sample": f"first {n} windows of the batch, {args.iterations} LM iterations, FP64 oracle on {threads} threads",
-                        "final_state_rel_err_vs_fp64_max": max(errs)}
+                        "sample": f"{n} windows of the batch (every {dist_info['stride']}th), {args.iterations} LM iterations, "
+                                  f"FP64 oracle on {threads} threads",
+                        "sample_sizes": dist_info, "final_state_rel_err_vs_fp64_max": max(errs)}
 
     if rank == 0:
         line = {

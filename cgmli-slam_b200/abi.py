@@ -88,7 +88,16 @@ class SolverOptions(C.Structure):
 class ServerOptions(C.Structure):
     _fields_ = [("device", C.c_int), ("max_batch_windows", C.c_int), ("memory_budget_bytes", C.c_longlong),
                 ("iterations", C.c_int), ("policy", C.c_int), ("nis_threshold", C.c_double), ("max_refits", C.c_int),
-                ("pre_gate", C.c_int), ("precision", C.c_int)]
+                ("pre_gate", C.c_int), ("precision", C.c_int), ("imu_params", ImuParameters),
+                ("imu_gyro_threshold", C.c_double), ("imu_accel_threshold", C.c_double),
+                ("calibration_include_prior", C.c_int)]
+
+
+class ServerRequest(C.Structure):
+    _fields_ = [("window", C.POINTER(Window)), ("victim_kf", C.c_int), ("imu_sample_time_ns", C.POINTER(C.c_longlong)),
+                ("imu_sample_readings", C.POINTER(C.c_double)), ("num_imu_samples", C.c_int), ("imu_range", C.POINTER(C.c_int)),
+                ("imu_t0_ns", C.POINTER(C.c_longlong)), ("imu_t1_ns", C.POINTER(C.c_longlong)),
+                ("calibration_information", C.c_int)]
 
 
 class SolveReport(C.Structure):
@@ -156,6 +165,10 @@ def declare_backend(lib: C.CDLL) -> C.CDLL:
     _proto(lib, "cgmli_server_create", C.c_int, [C.POINTER(ServerOptions), C.POINTER(C.c_void_p)])
     _proto(lib, "cgmli_server_destroy", None, [V])
     _proto(lib, "cgmli_server_submit", C.c_int, [V, W, C.c_int, ll_p])
+    _proto(lib, "cgmli_server_submit_request", C.c_int, [V, C.POINTER(ServerRequest), ll_p])
+    _proto(lib, "cgmli_server_read_imu", C.c_int, [V, C.c_longlong, C.POINTER(FrozenImu), c_int_p])
+    _proto(lib, "cgmli_server_read_calibration_information", C.c_int,
+           [V, C.c_longlong, c_int_p, c_int_p, c_int_p, c_int_p, c_double_p, c_double_p])
     _proto(lib, "cgmli_server_poll", C.c_int, [V, C.c_longlong, C.c_int, C.POINTER(SolveReport), c_double_p])
     _proto(lib, "cgmli_server_read_prior", C.c_int,
            [V, C.c_longlong, c_int_p, c_int_p, c_int_p, c_int_p, c_int_p, c_double_p, c_double_p, c_double_p])
@@ -213,7 +226,7 @@ BACKEND_SYMBOLS = [
     "cgmli_solver_calibration_information", "cgmli_solver_read_calibration_information", "cgmli_topology_check_tuned",
     "cgmli_solver_set_tuning", "cgmli_solver_get_tuning", "cgmli_solver_autotune",
     "cgmli_solver_device_bytes", "cgmli_server_device_bytes", "cgmli_solver_evaluate", "cgmli_solver_read_factors",
-    "cgmli_solver_solve_host",
+    "cgmli_solver_solve_host", "cgmli_server_submit_request", "cgmli_server_read_imu", "cgmli_server_read_calibration_information",
 ]
 KERNEL_NAMES = ["zero_acc", "linearize", "retained", "factor", "candidate", "backsub_trial", "retained_trial", "lm_update", "accept",
                 "lin_pairs", "lin_schur"]

@@ -369,8 +369,14 @@ class Server:
 
     def __init__(self, device: int = 0, iterations: int = 1, policy: int = abi.MARGIN_OLD, max_batch_windows: int = 512,
                  memory_budget_bytes: int = 40 << 30, nis_threshold: float = 0.0, max_refits: int = 3, pre_gate: bool = False,
-                 precision: int = abi.PRECISION_FP64):
+                 precision: int = abi.PRECISION_FP64, imu_params=None, imu_gyro_threshold: float = 3e-4,
+                 imu_accel_threshold: float = 0.02, calibration_include_prior: bool = True):
         opt = abi.ServerOptions()
+        if imu_params is not None:
+            opt.imu_params = imu_params
+        opt.imu_gyro_threshold = imu_gyro_threshold
+        opt.imu_accel_threshold = imu_accel_threshold
+        opt.calibration_include_prior = int(calibration_include_prior)
         opt.device = device
         opt.max_batch_windows = max_batch_windows
         opt.memory_budget_bytes = memory_budget_bytes
@@ -403,6 +409,53 @@ class Server:
         _check(lib().cgmli_server_submit(self._h, C.byref(w), victim, C.byref(t)), "cgmli_server_submit")
         self._keep[t.value] = window
         return t.value
+
+    def submit_request(self, window, victim: int = -1, imu=None, calibration: bool = False) -> int:
+        """A request with its optional parts: imu = (time_ns, readings, ranges, t0_ns, t1_ns)
+        for the window's IMU factors (refreshed before the solve), calibration = the
+        conditional calibration information at the solved states."""
+        w = window.window if hasattr(window, "window") else window
+        req = abi.ServerRequest()
+        req.window = C.pointer(w)
+        req.victim_kf = victim
+        keep = [window, req]
+        if imu is not None:
+            t, rd, rg, t0, t1 = (np.ascontiguousarray(imu[0], np.int64), np.ascontiguousarray(imu[1], np.float64),
+                                 np.ascontiguousarray(imu[2], np.int32), np.ascontiguousarray(imu[3], np.int64),
+                                 np.ascontiguousarray(imu[4], np.int64))
+            ll = C.POINTER(C.c_longlong)
+            req.imu_sample_time_ns = t.ctypes.data_as(ll)
+            req.imu_sample_readings = rd.ctypes.data_as(abi.c_double_p)
+            req.num_imu_samples = len(t)
+            req.imu_range = rg.ctypes.data_as(abi.c_int_p)
+            req.imu_t0_ns = t0.ctypes.data_as(ll)
+            req.imu_t1_ns = t1.ctypes.data_as(ll)
+            keep += [t, rd, rg, t0, t1]
+        req.calibration_information = int(calibration)
+        tk = C.c_longlong()
+        _check(lib().cgmli_server_submit_request(self._h, C.byref(req), C.byref(tk)), "cgmli_server_submit_request")
+        self._keep[tk.value] = keep
+        return tk.value
+
+    def read_imu(self, ticket: int, count: int):
+        """(factors after the refresh, how many were re-preintegrated)."""
+        out = (abi.FrozenImu * max(count, 1))()
+        n = C.c_int()
+        _check(lib().cgmli_server_read_imu(self._h, ticket, out, C.byref(n)), "cgmli_server_read_imu")
+        return list(out)[:count], n.value
+
+    def read_calibration_information(self, ticket: int) -> dict:
+        size, nb = C.c_int(), C.c_int()
+        code = lib().cgmli_server_read_calibration_information(self._h, ticket, C.byref(size), C.byref(nb), None, None, None, None)
+        if code != 0:
+            return dict(status=code)
+        n, b = size.value, nb.value
+        kinds, idx = np.zeros(b, np.int32), np.zeros(b, np.int32)
+        cond, ev = np.zeros(n * n), np.zeros(n)
+        _check(lib().cgmli_server_read_calibration_information(self._h, ticket, C.byref(size), C.byref(nb),
+                                                               kinds.ctypes.data_as(abi.c_int_p), idx.ctypes.data_as(abi.c_int_p),
+                                                               _p(cond), _p(ev)), "cgmli_server_read_calibration_information")
+        return dict(status=0, size=n, kinds=kinds, index=idx, conditional=cond.reshape(n, n), eigenvalues=ev)
 
     def poll(self, ticket: int, wait: bool = True):
         """(report, latency_ms) once complete, None while pending (wait=False)."""

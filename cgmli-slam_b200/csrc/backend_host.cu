@@ -851,19 +851,23 @@ int cgmli_solver_set_imu_samples(cgmli_solver* S, const cgmli_imu_parameters* pa
     int lo = num_samples, hi = 0;
     for (int i = 0; i < count; ++i) {
         const int b = range[2 * i], e = range[2 * i + 1];
+        if (b == e && b >= 0 && b <= num_samples) continue;  // no samples: the refresh keeps the factor
         if (b < 0 || e > num_samples || e - b < 2)
             return fail(CGMLI_E_INVALID, "set_imu_samples: factor " + std::to_string(i) + ": sample range outside the samples or shorter than 2");
         lo = std::min(lo, b);
         hi = std::max(hi, e);
     }
+    if (hi <= lo) lo = hi = 0;  // every factor without samples
     CK(cudaSetDevice(S->device));
     cudaStream_t st = S->stream;
     const size_t span = (size_t)(hi - lo);
     CK(S->imuTimes.reserve(span)); CK(S->imuReadings.reserve(6 * span));
     CK(S->imuRanges.reserve(2 * (size_t)count)); CK(S->imuT0.reserve(count)); CK(S->imuT1.reserve(count));
     CK(S->imuStatus.reserve(count)); CK(S->imuRefreshed.reserve(count)); CK(S->imuRefreshScratch.reserve(count));
-    CK(cudaMemcpyAsync(S->imuTimes.p, sample_time_ns + lo, span * sizeof(long long), cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(S->imuReadings.p, sample_readings + 6 * (size_t)lo, 6 * span * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (span) {
+        CK(cudaMemcpyAsync(S->imuTimes.p, sample_time_ns + lo, span * sizeof(long long), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(S->imuReadings.p, sample_readings + 6 * (size_t)lo, 6 * span * sizeof(double), cudaMemcpyHostToDevice, st));
+    }
     CK(cudaMemcpyAsync(S->imuRanges.p, range, 2 * (size_t)count * sizeof(int), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(S->imuT0.p, t0_ns, count * sizeof(long long), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(S->imuT1.p, t1_ns, count * sizeof(long long), cudaMemcpyHostToDevice, st));
@@ -1382,7 +1386,8 @@ static int marginalizeImpl(cgmli_solver* S, const int* victim_kf, int policy, bo
             for (int b = 0; b < d.priorBlocks; ++b)
                 sbInPrior = sbInPrior || (hb.priorKind[d.priorBlk0 + b] == CGMLI_PRIOR_SPEED_BIAS && hb.priorIndex[d.priorBlk0 + b] == d.kf0 + v);
             S->mergeState[w] = CGMLI_IMU_MERGE_BRIDGE;
-            if (incident == 2 && left >= 0 && right >= 0 && !sbInPrior && S->haveImuSamples) {
+            const auto hasSamples = [&](int q) { return q >= 0 && S->hImuRange[2 * q + 1] > S->hImuRange[2 * q]; };
+            if (incident == 2 && left >= 0 && right >= 0 && !sbInPrior && S->haveImuSamples && hasSamples(left) && hasSamples(right)) {
                 const int lb = S->hImuRange[2 * left], le = S->hImuRange[2 * left + 1];
                 const int rb = S->hImuRange[2 * right], re = S->hImuRange[2 * right + 1];
                 if (S->hImuT1[left] != S->hImuT0[right] || rb < lb || rb > le || re < le) {

@@ -1297,16 +1297,16 @@ __global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int re
 // the GPU instead of one CTA (k_factor skips it).  The damped system is assembled
 // by column blocks (k_wide_assemble); the solve-time charts and the debug copy run
 // in one CTA (k_wide_prepare).  Then, per panel of kFacPanel columns:
-//   - its diagonal block is factored by one warp, lane i owning row i, with the
-//     forward substitution of the right-hand side over the block
-//     (wideDiagBlock: a right-looking sweep in registers, warp-level sync only);
+//   - its diagonal block is factored by one CTA, with the forward substitution
+//     of the right-hand side over the block
+//     (wideDiagBlock: right-looking over the CTA, one barrier per column);
 //   - the rows below it are solved against that block (L21 = A21 L11^-T), one
 //     thread per row with the row in registers, and each row's right-hand side
 //     entry takes its update y2 -= L21 y1 on the way (k_wide_trsm);
 //   - the trailing lower triangle A22 -= L21 L21^T is updated by one warp per
 //     32 x 32 tile on the FP64 tensor path, L21 read from the L2-resident slot;
-//     the warp holding the first trailing tile, which is the next panel's
-//     diagonal block, factors it as soon as its update is written (k_wide_trailing).
+//     the CTA holding the first trailing tile, which is the next panel's
+//     diagonal block, factors it as soon as its tiles are written (k_wide_trailing).
 // The backward substitution, the refinement steps and the prediction follow in one
 // CTA (k_wide_finish, the tail k_factor uses).  Per-window vectors between the
 // kernels: B.facVec + 3 vec0 holds x (n), the undamped diagonal (n) and the damping (n).
@@ -1361,53 +1361,58 @@ __global__ void __launch_bounds__(kFactorThreads) k_wide_prepare(DevBatch B, dou
     if (Sdebug) storeSdebug(A, n, Sdebug + wd.dense0);
 }
 
-// Cholesky of the diagonal block at k0 of window w by the calling warp, with the
-// forward substitution of x over the block; the block is written back as L11 (its
-// diagonal the roots).  Lane i holds row i in registers, read and written with one
-// coalesced access per column (32 loads in flight); column c's pivot and the entries
-// L[j][c] of the rank-1 update come by shuffles, so the sweep needs no memory round
-// trip.  Returns false (uniform over the warp) on a pivot that is not positive and finite.
+// Cholesky of the diagonal block at k0 of window w by the whole CTA, with the forward
+// substitution of x over the block; the block is written back as L11 (its diagonal
+// the roots).  Right-looking on the unscaled columns: for pivot c every thread
+// updates its entries (i, j), c < j <= i, by T[i][c] T[j][c] / d_c (four entries of
+// the 32 x 32 block per thread, one barrier per column), and x_i -= T[i][c] x_c / d_c;
+// the columns are scaled by 1 / sqrt(d_c) at the end.  A single warp doing the same
+// sweep in registers took about 20 k cycles (in-order issue of ~120 dependent
+// instructions per column); the CTA takes one update and one barrier per column.
+// Returns false (uniform over the CTA) on a pivot that is not positive and finite.
 constexpr int kDiagStride = kFacPanel + 1;
 __device__ bool wideDiagBlock(const DevBatch& B, const WinDesc& wd, int k0) {
-    const int lane = threadIdx.x & 31, n = wd.Nr, bw = min(kFacPanel, n - k0);
+    static_assert(kFacPanel * kFacPanel == 4 * kFactorThreads, "four block entries per thread");
+    __shared__ double T[kFacPanel * kDiagStride], xs[kFacPanel];
+    const int tid = threadIdx.x, n = wd.Nr, bw = min(kFacPanel, n - k0);
     double* A = B.Sglob + wd.dense0;
     double* x = B.facVec + 3ll * wd.vec0;
-    double r[kFacPanel];
+    int ei[4], ej[4];
 #pragma unroll
-    for (int j = 0; j < kFacPanel; ++j) r[j] = (lane < bw && j <= lane) ? A[(k0 + lane) + (long long)(k0 + j) * n] : 0.0;
-    double xi = lane < bw ? x[k0 + lane] : 0.0;
-    bool ok = true;
+    for (int u = 0; u < 4; ++u) {  // entry (i, j), by columns: consecutive threads read consecutive rows
+        const int q = tid + u * kFactorThreads;
+        ei[u] = q % kFacPanel;
+        ej[u] = q / kFacPanel;
+        if (ei[u] < bw && ej[u] <= ei[u]) T[ei[u] * kDiagStride + ej[u]] = A[(k0 + ei[u]) + (long long)(k0 + ej[u]) * n];
+    }
+    if (tid < bw) xs[tid] = x[k0 + tid];
+    __syncthreads();
+    for (int c = 0; c < bw; ++c) {
+        const double d = T[c * kDiagStride + c];
+        if (!(d > 0) || !isfinite(d)) return false;  // every thread read the same d
+        const double invd = 1.0 / d;
 #pragma unroll
-    for (int c = 0; c < kFacPanel; ++c) {
-        if (c < bw && ok) {  // uniform over the warp
-            const double d = __shfl_sync(0xffffffffu, r[c], c);
-            if (!(d > 0) || !isfinite(d)) {
-                ok = false;  // every lane received the same d
-            } else {
-                const double il = rsqrt(d), l = d * il;  // one reciprocal square root per column
-                const double lic = lane > c ? r[c] * il : (lane == c ? l : 0.0);  // L[lane][c]
-                if (lane >= c) r[c] = lic;
-                const double yc = __shfl_sync(0xffffffffu, xi, c) * il;
-                if (lane == c) xi = yc;
-                else if (lane > c) xi -= lic * yc;
+        for (int u = 0; u < 4; ++u) {
+            const int i = ei[u], j = ej[u];
+            if (j > c && i >= j && i < bw) T[i * kDiagStride + j] -= T[i * kDiagStride + c] * T[j * kDiagStride + c] * invd;
+        }
+        if (tid > c && tid < bw) xs[tid] -= T[tid * kDiagStride + c] * xs[c] * invd;
+        __syncthreads();
+    }
 #pragma unroll
-                for (int j = c + 1; j < kFacPanel; ++j) {  // row lane, columns c < j <= lane
-                    const double ljc = __shfl_sync(0xffffffffu, lic, j);
-                    if (lane >= j) r[j] -= lic * ljc;
-                }
-            }
+    for (int u = 0; u < 4; ++u) {
+        const int i = ei[u], j = ej[u];
+        if (i < bw && j <= i) {
+            const double l = sqrt(T[j * kDiagStride + j]);
+            A[(k0 + i) + (long long)(k0 + j) * n] = i == j ? l : T[i * kDiagStride + j] / l;
         }
     }
-    if (!ok) return false;
-#pragma unroll
-    for (int j = 0; j < kFacPanel; ++j)
-        if (lane < bw && j <= lane) A[(k0 + lane) + (long long)(k0 + j) * n] = r[j];
-    if (lane < bw) x[k0 + lane] = xi;
+    if (tid < bw) x[k0 + tid] = xs[tid] / sqrt(T[tid * kDiagStride + tid]);
     return true;
 }
 
 // The first panel's diagonal block (the later ones are factored by k_wide_trailing).
-__global__ void __launch_bounds__(32) k_wide_diag(DevBatch B) {
+__global__ void __launch_bounds__(kFactorThreads) k_wide_diag(DevBatch B) {
     const int wdx = B.wideList[blockIdx.x];
     if (B.lm[wdx].mode == kModeDone) return;
     if (!wideDiagBlock(B, B.win[wdx], 0) && threadIdx.x == 0) B.facFailed[wdx] = 1;
@@ -1460,6 +1465,41 @@ __global__ void __launch_bounds__(kFactorThreads) k_wide_trsm(DevBatch B, int k0
     x[r] -= y;
 }
 
+// trailingTile for a full panel (bw = kFacPanel, every trailing update of the wide
+// sequence): the eight k-steps' operands are loaded before the first MMA, so the warp
+// waits for one round of L2 loads instead of eight; the MMAs and their order are
+// trailingTile's.
+__device__ __forceinline__ void trailingTileFull(const double* V, long long ldv, int rb, int cb, int m2, double* A, int n, int k0) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, kr = lane & 3;
+    double a[kFacPanel / 4][4], b[kFacPanel / 4][4];
+#pragma unroll
+    for (int st = 0; st < kFacPanel / 4; ++st) {
+        const double* row = V + (long long)(4 * st + kr) * ldv;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            a[st][q] = row[rb * 32 + 8 * q + g];
+            b[st][q] = row[cb * 32 + 8 * q + g];
+        }
+    }
+    double acc[4][8];
+    zeroTile(acc);
+#pragma unroll
+    for (int st = 0; st < kFacPanel / 4; ++st)
+#pragma unroll
+        for (int I = 0; I < 4; ++I)
+#pragma unroll
+            for (int J = 0; J < 4; ++J) mmaF64Tile(acc[I][2 * J], acc[I][2 * J + 1], a[st][I], b[st][J]);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int i = tileRowMma(rb, lane, r);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int j = tileCol(cb, lane, c);
+            if (i < m2 && j < m2 && i >= j) A[(k0 + kFacPanel + i) + (long long)(k0 + kFacPanel + j) * n] -= acc[r][c];
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kFactorThreads) k_wide_trailing(DevBatch B, int k0) {
     const int wdx = B.wideList[blockIdx.x];
     if (B.lm[wdx].mode == kModeDone) return;
@@ -1469,16 +1509,19 @@ __global__ void __launch_bounds__(kFactorThreads) k_wide_trailing(DevBatch B, in
     const int bw = min(kFacPanel, n - k0), m2 = n - k0 - bw;
     const int nb2 = (m2 + 31) >> 5, tiles = nb2 * (nb2 + 1) / 2;
     const int t = blockIdx.y * (kFactorThreads / 32) + (threadIdx.x >> 5);
-    if (m2 <= 0 || t >= tiles) return;  // per warp: the kernel has no barrier
-    int cb, rb;
-    tileOf(t, nb2, cb, rb);
+    if (m2 <= 0) return;  // uniform over the CTA
     double* A = B.Sglob + wd.dense0;
-    // L21 column k = A's column k0 + k from row k0 + bw; rows past n (padding of the
-    // last tile) read the next column's top, inside the slot, and only reach masked entries
-    trailingTile(A + (k0 + bw) + (long long)k0 * n, n, rb, cb, bw, m2, A, n, k0);
-    if (t == 0) {  // tile (0, 0) is the next panel's diagonal block, complete now
-        __syncwarp();
-        if (!wideDiagBlock(B, wd, k0 + bw) && (threadIdx.x & 31) == 0) B.facFailed[wdx] = 1;
+    if (t < tiles) {
+        int cb, rb;
+        tileOf(t, nb2, cb, rb);
+        // L21 column k = A's column k0 + k from row k0 + bw; rows past n (padding of the
+        // last tile) read the next column's top, inside the slot, and only reach masked entries
+        if (bw == kFacPanel) trailingTileFull(A + (k0 + bw) + (long long)k0 * n, n, rb, cb, m2, A, n, k0);
+        else trailingTile(A + (k0 + bw) + (long long)k0 * n, n, rb, cb, bw, m2, A, n, k0);
+    }
+    if (blockIdx.y == 0) {  // tile (0, 0), this CTA's first, is the next panel's diagonal block
+        __syncthreads();
+        if (!wideDiagBlock(B, wd, k0 + bw) && threadIdx.x == 0) B.facFailed[wdx] = 1;
     }
 }
 
@@ -2067,7 +2110,7 @@ int launchIterationParts(const DevBatch& B, const LaunchPlan& P, int refinement,
     if (P.numWide > 0) {  // the wide sequence (windows of at least kWideCols columns)
         run(CGMLI_KERNEL_FACTOR, [&] { k_wide_assemble<<<dim3(P.numWide, (P.wideCols + 31) / 32), 256, 0, s>>>(B); });
         if (P.wideCharts || Sdebug) run(CGMLI_KERNEL_FACTOR, [&] { k_wide_prepare<<<P.numWide, kFactorThreads, 0, s>>>(B, Sdebug); });
-        run(CGMLI_KERNEL_FACTOR, [&] { k_wide_diag<<<P.numWide, 32, 0, s>>>(B); });
+        run(CGMLI_KERNEL_FACTOR, [&] { k_wide_diag<<<P.numWide, kFactorThreads, 0, s>>>(B); });
         for (int k0 = 0; k0 + kFacPanel < P.wideCols; k0 += kFacPanel) {
             const int m2 = P.wideCols - k0 - kFacPanel;
             const dim3 rows(P.numWide, (m2 + kFactorThreads - 1) / kFactorThreads);

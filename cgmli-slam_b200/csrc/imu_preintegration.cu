@@ -136,6 +136,10 @@ __global__ void __launch_bounds__(kImuWarps * 32) k_imu_preintegrate(const ImuLa
         bg = ld3(L.biases + 6 * iv);
         ba = ld3(L.biases + 6 * iv + 3);
     } else {
+        if (L.ranges[2 * iv] == L.ranges[2 * iv + 1]) {  // a factor without samples keeps its value
+            if (lane == 0) { status[iv] = CGMLI_OK; L.refreshed[iv] = 0; }
+            return;
+        }
         const double* x = L.sb + 9ll * L.kf[iv];
         bg = ld3(x + 3);
         ba = ld3(x + 6);

@@ -13,6 +13,7 @@
 #include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <deque>
 #include <memory>
 #include <mutex>
@@ -45,6 +46,15 @@ struct Request {
     // gated solve: the window's gate report and rejected factors
     cgmli_gate_report gate{};
     std::vector<unsigned char> rejected;
+    // IMU samples for the refresh before the solve (num_imu_samples 0: none) and the
+    // factors after it
+    cgmli_server_request extra{};
+    std::vector<cgmli_frozen_imu> imu;
+    int imuRefreshed = 0;
+    // calibration information at the solved states (extra.calibration_information)
+    int calibStatus = CGMLI_E_INVALID, calibSize = 0, calibBlocks = 0;
+    std::vector<int> calibKind, calibIndex;
+    std::vector<double> calibConditional, calibEvals;
 };
 
 // Device bytes a window occupies in a batch (observation, landmark and dense
@@ -79,6 +89,7 @@ struct cgmli_server {
         int solver = 0;
         bool marg = false;
         int status = CGMLI_OK;
+        bool imu = false;  // the batch carries IMU samples (refreshed factors are read back)
         double launchMs = 0;
         double phaseMs[3] = {0, 0, 0};  // host time of set_windows, the solve launch, the marginalization launch
     };
@@ -101,16 +112,81 @@ struct cgmli_server {
         }
         const auto t0 = Clock::now();
         b.status = cgmli_solver_set_windows(S, b.windows.data(), n);
+        if (b.status == CGMLI_OK) b.status = refreshImu(b);
         const auto t1 = Clock::now();
         if (b.status == CGMLI_OK)
             b.status = opt.nis_threshold > 0 ? cgmli_solver_solve_gated(S, opt.iterations, opt.nis_threshold, opt.max_refits, opt.pre_gate)
                                              : cgmli_solver_solve(S, opt.iterations);
+        if (b.status == CGMLI_OK) calibration(b);
         const auto t2 = Clock::now();
         if (b.status == CGMLI_OK && b.marg) b.status = cgmli_solver_marginalize(S, victims.data(), opt.policy);
         const auto t3 = Clock::now();
         b.phaseMs[0] = std::chrono::duration<double, std::milli>(t1 - t0).count();
         b.phaseMs[1] = std::chrono::duration<double, std::milli>(t2 - t1).count();
         b.phaseMs[2] = std::chrono::duration<double, std::milli>(t3 - t2).count();
+    }
+
+    // The batch's IMU samples, when a request brought some: every IMU factor of the
+    // batch in order, a request's ranges moved into the concatenated samples, the
+    // factors of windows without samples with empty ranges (kept as given); then the
+    // refresh, enqueued before the solve.
+    int refreshImu(Batch& b) {
+        bool any = false;
+        for (Request* r : b.reqs) any = any || r->extra.num_imu_samples > 0;
+        if (!any) return CGMLI_OK;
+        std::vector<long long> times, t0, t1;
+        std::vector<double> readings;
+        std::vector<int> range;
+        for (Request* r : b.reqs) {
+            const cgmli_server_request& x = r->extra;
+            const int nimu = r->window.num_imu, base = (int)times.size();
+            if (x.num_imu_samples > 0) {
+                times.insert(times.end(), x.imu_sample_time_ns, x.imu_sample_time_ns + x.num_imu_samples);
+                readings.insert(readings.end(), x.imu_sample_readings, x.imu_sample_readings + 6ll * x.num_imu_samples);
+            }
+            for (int q = 0; q < nimu; ++q) {
+                const bool has = x.num_imu_samples > 0;
+                range.push_back(has ? base + x.imu_range[2 * q] : 0);
+                range.push_back(has ? base + x.imu_range[2 * q + 1] : 0);
+                t0.push_back(has ? x.imu_t0_ns[q] : 0);
+                t1.push_back(has ? x.imu_t1_ns[q] : 0);
+            }
+        }
+        cgmli_solver* S = solver[b.solver];
+        int st = cgmli_solver_set_imu_samples(S, &opt.imu_params, times.data(), readings.data(), (int)times.size(), range.data(),
+                                              t0.data(), t1.data());
+        if (st == CGMLI_OK) st = cgmli_solver_refresh_imu(S, opt.imu_gyro_threshold, opt.imu_accel_threshold, nullptr);
+        b.imu = true;
+        return st;
+    }
+    // The conditional calibration information of the windows that asked for it, read
+    // back before the marginalization reuses the same device buffers (this waits for
+    // the batch's solve).
+    void calibration(Batch& b) {
+        bool any = false;
+        for (Request* r : b.reqs) any = any || r->extra.calibration_information;
+        if (!any) return;
+        cgmli_solver* S = solver[b.solver];
+        const int st = cgmli_solver_calibration_information(S, opt.calibration_include_prior);
+        for (int i = 0; i < (int)b.reqs.size(); ++i) {
+            Request* r = b.reqs[i];
+            if (!r->extra.calibration_information) continue;
+            r->calibStatus = st;
+            if (st != CGMLI_OK) continue;
+            int size = 0, nb = 0;
+            int rs = cgmli_solver_read_calibration_information(S, i, &size, &nb, nullptr, nullptr, nullptr, nullptr);
+            if (rs == CGMLI_OK) {
+                r->calibKind.resize(nb);
+                r->calibIndex.resize(nb);
+                r->calibConditional.resize((size_t)size * size);
+                r->calibEvals.resize(size);
+                rs = cgmli_solver_read_calibration_information(S, i, &size, &nb, r->calibKind.data(), r->calibIndex.data(),
+                                                               r->calibConditional.data(), r->calibEvals.data());
+            }
+            r->calibStatus = rs;
+            r->calibSize = size;
+            r->calibBlocks = nb;
+        }
     }
 
     // Waits for a launched batch and records its results.
@@ -133,6 +209,14 @@ struct cgmli_server {
                 continue;
             }
             r->report = reps[i];
+            if (b.imu && r->extra.num_imu_samples > 0 && r->window.num_imu > 0) {
+                r->imu.resize(r->window.num_imu);
+                const int is = cgmli_solver_read_imu(S, i, r->imu.data());
+                if (is != CGMLI_OK && r->report.status == CGMLI_OK) r->report.status = is;
+                r->imuRefreshed = 0;
+                for (int q = 0; q < r->window.num_imu; ++q)
+                    r->imuRefreshed += std::memcmp(&r->imu[q], &r->window.imu[q], sizeof(cgmli_frozen_imu)) != 0 ? 1 : 0;
+            }
             if (opt.nis_threshold > 0) {
                 r->rejected.resize(r->window.num_observations);
                 const int gs = cgmli_solver_read_gate(S, i, &r->gate, r->rejected.data());
@@ -262,6 +346,8 @@ int cgmli_server_create(const cgmli_server_options* options, cgmli_server** out)
         return setLastError(CGMLI_E_INVALID, "server: unknown marginalization policy");
     if (!(options->nis_threshold >= 0) || options->max_refits < 0 || options->max_refits > 64)
         return setLastError(CGMLI_E_INVALID, "server: nis_threshold < 0 or max_refits outside 0..64");
+    if (!(options->imu_gyro_threshold >= 0) || !(options->imu_accel_threshold >= 0))
+        return setLastError(CGMLI_E_INVALID, "server: negative or NaN IMU refresh threshold");
     if (options->precision != CGMLI_PRECISION_FP64 && options->precision != CGMLI_PRECISION_MIXED)
         return setLastError(CGMLI_E_INVALID, "server: unknown precision");
     auto* s = new cgmli_server();
@@ -297,24 +383,50 @@ void cgmli_server_destroy(cgmli_server* s) {
 }
 
 namespace {
-int submitAt(cgmli_server* s, cgmli_window* window, int victim_kf, Clock::time_point arrival, long long* ticket);
+int submitAt(cgmli_server* s, cgmli_window* window, int victim_kf, Clock::time_point arrival, long long* ticket,
+             const cgmli_server_request* extra = nullptr);
 }
 
 int cgmli_server_submit(cgmli_server* s, cgmli_window* window, int victim_kf, long long* ticket) {
     return submitAt(s, window, victim_kf, Clock::now(), ticket);
 }
 
+int cgmli_server_submit_request(cgmli_server* s, const cgmli_server_request* request, long long* ticket) {
+    if (!request) return setLastError(CGMLI_E_INVALID, "server: null request");
+    return submitAt(s, request->window, request->victim_kf, Clock::now(), ticket, request);
+}
+
 namespace {
-int submitAt(cgmli_server* s, cgmli_window* window, int victim_kf, Clock::time_point arrival, long long* ticket) {
+// The IMU part of a request: every factor's range inside the request's samples.
+int validateImuPart(const cgmli_window& w, const cgmli_server_request& x, std::string& why) {
+    if (x.num_imu_samples == 0) return CGMLI_OK;
+    if (x.num_imu_samples < 2 || !x.imu_sample_time_ns || !x.imu_sample_readings || (w.num_imu > 0 && (!x.imu_range || !x.imu_t0_ns || !x.imu_t1_ns))) {
+        why = "server: IMU samples need times, readings, ranges and interval ends (and at least 2 samples)";
+        return CGMLI_E_INVALID;
+    }
+    for (int q = 0; q < w.num_imu; ++q) {
+        const int b = x.imu_range[2 * q], e = x.imu_range[2 * q + 1];
+        if (b < 0 || e > x.num_imu_samples || e - b < 2) {
+            why = "server: IMU factor " + std::to_string(q) + ": sample range outside the request's samples or shorter than 2";
+            return CGMLI_E_INVALID;
+        }
+    }
+    return CGMLI_OK;
+}
+
+int submitAt(cgmli_server* s, cgmli_window* window, int victim_kf, Clock::time_point arrival, long long* ticket,
+             const cgmli_server_request* extra) {
     if (!s || !window || !ticket) return setLastError(CGMLI_E_INVALID, "server: null server, window or ticket");
     std::string why;
-    const int st = cgmli::validateWindow(*window, 0, why);
+    int st = cgmli::validateWindow(*window, 0, why);
+    if (st == CGMLI_OK && extra) st = validateImuPart(*window, *extra, why);
     if (st != CGMLI_OK) return setLastError(st, why.c_str());
     if (victim_kf < -1 || victim_kf >= window->num_keyframes) return setLastError(CGMLI_E_INVALID, "server: victim keyframe out of range");
     auto r = std::make_shared<Request>();
     r->window = *window;
     r->victim = victim_kf;
     r->submitted = arrival;
+    if (extra) r->extra = *extra;
     {
         std::lock_guard<std::mutex> lock(s->mu);
         if (s->stopping) return setLastError(CGMLI_E_INVALID, "server: stopping");
@@ -445,6 +557,40 @@ int cgmli_server_read_gate(cgmli_server* s, long long ticket, cgmli_gate_report*
     if (!r.complete) return setLastError(CGMLI_E_PENDING, "server: request not complete");
     *report = r.gate;
     if (rejected && !r.rejected.empty()) std::copy(r.rejected.begin(), r.rejected.end(), rejected);
+    return CGMLI_OK;
+}
+
+int cgmli_server_read_imu(cgmli_server* s, long long ticket, cgmli_frozen_imu* imu, int* refreshed) {
+    if (!s || !imu) return setLastError(CGMLI_E_INVALID, "server: null server or buffer");
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->requests.find(ticket);
+    if (it == s->requests.end()) return setLastError(CGMLI_E_INVALID, "server: unknown ticket");
+    const Request& r = *it->second;
+    if (!r.complete) return setLastError(CGMLI_E_PENDING, "server: request not complete");
+    if (r.extra.num_imu_samples == 0) return setLastError(CGMLI_E_INVALID, "server: the request brought no IMU samples");
+    if (r.imu.size() != (size_t)r.window.num_imu) return setLastError(r.report.status ? r.report.status : CGMLI_E_INVALID,
+                                                                      "server: the request's IMU factors were not read back");
+    std::copy(r.imu.begin(), r.imu.end(), imu);
+    if (refreshed) *refreshed = r.imuRefreshed;
+    return CGMLI_OK;
+}
+
+int cgmli_server_read_calibration_information(cgmli_server* s, long long ticket, int* size, int* num_blocks, int* block_kind,
+                                              int* block_index, double* conditional, double* eigenvalues) {
+    if (!s || !size || !num_blocks) return setLastError(CGMLI_E_INVALID, "server: null server or size outputs");
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->requests.find(ticket);
+    if (it == s->requests.end()) return setLastError(CGMLI_E_INVALID, "server: unknown ticket");
+    const Request& r = *it->second;
+    if (!r.complete) return setLastError(CGMLI_E_PENDING, "server: request not complete");
+    if (!r.extra.calibration_information) return setLastError(CGMLI_E_INVALID, "server: the request did not ask for the calibration information");
+    if (r.calibStatus != CGMLI_OK) return setLastError(r.calibStatus, "server: the calibration information failed for this window");
+    *size = r.calibSize;
+    *num_blocks = r.calibBlocks;
+    if (block_kind) std::copy(r.calibKind.begin(), r.calibKind.end(), block_kind);
+    if (block_index) std::copy(r.calibIndex.begin(), r.calibIndex.end(), block_index);
+    if (conditional) std::copy(r.calibConditional.begin(), r.calibConditional.end(), conditional);
+    if (eigenvalues) std::copy(r.calibEvals.begin(), r.calibEvals.end(), eigenvalues);
     return CGMLI_OK;
 }
 

@@ -482,6 +482,9 @@ int cgmli_imu_last_timing(double *kernel_ms);
  * enqueues the work (no host round trip); otherwise it waits, stores the number
  * of replaced factors and returns CGMLI_E_INVALID / _E_NONFINITE for a factor
  * whose samples or result were bad (such a factor keeps its previous value).
+ * A factor whose range is empty (range[2q] == range[2q+1]) has no samples: the
+ * refresh keeps it as given (the served mode uses this for windows that bring no
+ * samples).
  * cgmli_solver_read_imu copies window w's current factors (num_imu) to the host. */
 int cgmli_solver_set_imu_samples(cgmli_solver *solver, const cgmli_imu_parameters *params, const long long *sample_time_ns,
                                  const double *sample_readings, int num_samples, const int *range, const long long *t0_ns,
@@ -516,7 +519,32 @@ typedef struct cgmli_server_options {
     int max_refits;                 /* refits of the gated solve (reference: 3) */
     int pre_gate;                   /* gated solve: gate at the submitted states first */
     int precision;                  /* CGMLI_PRECISION_FP64 or _MIXED (cgmli_solver_options) */
+    /* requests with IMU samples (cgmli_server_submit_request): the model of the
+       samples and the drift thresholds of the refresh before the solve
+       (cgmli_solver_refresh_imu; the reference's FixedLagBackend uses 3e-4 and 0.02) */
+    cgmli_imu_parameters imu_params;
+    double imu_gyro_threshold, imu_accel_threshold;
+    int calibration_include_prior;  /* requests for the calibration information: include the prior */
 } cgmli_server_options;
+
+/* A served request with the optional parts of a backend step around the solve:
+ * the IMU samples of the window's IMU factors, so that factors whose bias drifted
+ * are re-preintegrated on the device before the solve (the resident refresh of
+ * FixedLagBackend.cpp:395-411; layout as cgmli_solver_set_imu_samples for this
+ * window's factors, ranges into this request's samples), and the conditional
+ * calibration information at the solved states (cgmli_solver_calibration_information;
+ * BackendOptimizer::calibrationInformation, BackendOptimizer.cpp:1084-1170).
+ * The arrays are the caller's and stay valid until the request completes. */
+typedef struct cgmli_server_request {
+    cgmli_window *window;
+    int victim_kf;                      /* -1: no marginalization */
+    const long long *imu_sample_time_ns;
+    const double *imu_sample_readings;  /* 6 per sample: gyro, accelerometer */
+    int num_imu_samples;                /* 0: no samples (the factors are used as given) */
+    const int *imu_range;               /* 2 per IMU factor of the window */
+    const long long *imu_t0_ns, *imu_t1_ns;
+    int calibration_information;        /* 1: compute it for this request */
+} cgmli_server_request;
 typedef struct cgmli_server cgmli_server;
 
 int cgmli_server_create(const cgmli_server_options *options, cgmli_server **out);
@@ -528,6 +556,16 @@ int cgmli_server_submit(cgmli_server *server, cgmli_window *window, int victim_k
  * that failed) and the submit-to-completion latency once the request is
  * complete; CGMLI_E_PENDING while it is not and wait == 0.  wait != 0 blocks. */
 int cgmli_server_poll(cgmli_server *server, long long ticket, int wait, cgmli_solve_report *report, double *latency_ms);
+/* cgmli_server_submit with the optional IMU samples and calibration request. */
+int cgmli_server_submit_request(cgmli_server *server, const cgmli_server_request *request, long long *ticket);
+/* The IMU factors (num_imu) of a completed request with samples, after the refresh;
+ * refreshed = how many were re-preintegrated. */
+int cgmli_server_read_imu(cgmli_server *server, long long ticket, cgmli_frozen_imu *imu, int *refreshed);
+/* The calibration information of a completed request that asked for it, laid out
+ * as cgmli_solver_read_calibration_information (sizes first with NULL buffers);
+ * the calibration call's status when it failed for this window. */
+int cgmli_server_read_calibration_information(cgmli_server *server, long long ticket, int *size, int *num_blocks, int *block_kind,
+                                              int *block_index, double *conditional, double *eigenvalues);
 /* Prior of a completed request with a victim, laid out as cgmli_solver_read_prior
  * (sizes first with NULL buffers). */
 int cgmli_server_read_prior(cgmli_server *server, long long ticket, int *rank, int *cols, int *num_blocks, int *block_kind,

@@ -134,3 +134,89 @@ def test_two_solvers_stay_within_the_memory_budget(backend):
     held = server.device_bytes()
     server.close()
     assert 0 < held <= budget
+
+
+def _imu_window(backend, seed):
+    """A window whose IMU factors are preintegrated on the device from a sample
+    stream, with three keyframes' biases then moved (two past the refresh
+    thresholds); returns the window and the samples of its factors."""
+    from dataclasses import replace
+    w = synth.SynthWindow(replace(synth.C1, keyframes=6, landmarks=200), seed)
+    K, nimu = w.K, w.window.num_imu
+    kf = np.array([w.window.imu_kf[q] for q in range(nimu)])
+    s = synth.imu_stream(1, K, seed + 1)
+    prm = synth.imu_parameters()
+    sb = w.speed_bias().reshape(K, 9)
+    args = (s.time_ns, s.readings, s.ranges[kf], s.t0_ns[kf], s.t1_ns[kf])
+    built = backend.imu_preintegrate(prm, *args, sb[kf, 3:9])
+    for q in range(nimu):
+        w.window.imu[q] = built[q]
+    sb[kf[1], 3] += 1e-3
+    sb[kf[3], 7] += 0.05
+    sb[kf[2], 4] += 1e-4
+    return w, prm, args
+
+
+def test_served_imu_refresh_equals_the_solver(backend):
+    """A request with IMU samples: the server refreshes the drifted factors before
+    the solve exactly as cgmli_solver_set_imu_samples + _refresh_imu do, and a
+    request without samples in the same server keeps its factors as given."""
+    w1, prm, args = _imu_window(backend, 61)
+    w2, _, _ = _imu_window(backend, 61)
+    plain, _, _ = _imu_window(backend, 63)
+    nimu = w1.window.num_imu
+    s = backend.Solver()
+    s.set_windows([w1])
+    s.set_imu_samples(prm, *args)
+    assert s.refresh_imu() == 2
+    ref_imu = s.read_imu(0, nimu)
+    s.solve(3)
+    s.synchronize()
+    s.read_states()
+    x_ref = w1.state_vector()
+    s.close()
+    x_plain0 = plain.state_vector()
+    x_plain, _, _ = _alone(backend, _imu_window(backend, 63)[0], -1, 3)
+    srv = backend.Server(iterations=3, imu_params=prm)
+    t1 = srv.submit_request(w2, -1, imu=args)
+    t2 = srv.submit_request(plain, -1)
+    rep1, _ = srv.poll(t1)
+    rep2, _ = srv.poll(t2)
+    assert rep1.status == 0 and rep2.status == 0
+    got, refreshed = srv.read_imu(t1, nimu)
+    assert refreshed == 2
+    assert all(bytes(a) == bytes(b) for a, b in zip(got, ref_imu))
+    assert rel(w2.state_vector(), x_ref) < 1e-8  # another window may share the batch: FP64 reduction order
+    assert rel(plain.state_vector() - x_plain0, x_plain - x_plain0) < 1e-8
+    with pytest.raises(backend.BackendError):
+        srv.read_imu(t2, nimu)  # that request brought no samples
+    srv.close()
+
+
+def test_served_calibration_information_equals_the_solver(backend):
+    """A request for the calibration information (with the prior) and a
+    marginalization: the server reads the information back before the
+    marginalization reuses the device buffers; both equal the solver's."""
+    from dataclasses import replace
+    spec = replace(synth.C2, landmarks=400)
+    w1, w2 = synth.SynthWindow(spec, 71), synth.SynthWindow(spec, 71)
+    s = backend.Solver()
+    s.set_windows([w1])
+    s.solve(2)
+    s.calibration_information(True)
+    ref = s.read_calibration_information(0)
+    s.marginalize([0], abi.MARGIN_OLD)
+    ref_prior = s.read_prior(0)
+    s.close()
+    assert ref["status"] == 0
+    srv = backend.Server(iterations=2, calibration_include_prior=True)
+    t = srv.submit_request(w2, 0, calibration=True)
+    rep, _ = srv.poll(t)
+    assert rep.status == 0
+    got = srv.read_calibration_information(t)
+    assert got["status"] == 0 and np.array_equal(got["kinds"], ref["kinds"])
+    assert rel(got["conditional"], ref["conditional"]) < 1e-10
+    prior = srv.read_prior(t)
+    A, Ar = prior["A"], ref_prior["A"]
+    assert prior["rank"] == ref_prior["rank"] and rel(A.T @ A, Ar.T @ Ar) < 1e-10
+    srv.close()
