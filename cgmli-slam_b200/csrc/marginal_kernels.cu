@@ -1037,7 +1037,7 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_fast(MargBatch M) {
             const double vi = v[i], wi = wv[i];
             for (int j = lane; j < m; j += 32) row[j] -= vi * wv[j] + wi * v[j];
         }
-        for (int i = tid; i < m; i += blockDim.x) reflectors[(k + 1 + i) * n + k] = v[i];
+        for (int i = tid; i < m; i += blockDim.x) reflectors[k * n + (k + 1 + i)] = v[i];  // row k, right of the diagonal
         __syncthreads();
     }
     if (tid == 0) {
@@ -1301,9 +1301,21 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_fast(MargBatch M) {
 // intact (shared memory), and fails with CGMLI_E_NONFINITE otherwise.
 constexpr int kTriSmemN = 110;
 constexpr int kQlMaxIterations = 60;
+constexpr int kTriReflBlock = 8;        // reflectors staged together in the back-transformation
+constexpr int kTriStageMaxRows = 64;    // eigenvector rows staged together (global-memory case)
 __host__ __device__ constexpr size_t triVecBytes(int n) { return sizeof(double) * 7 * (size_t)n; }  // d, e, tau, 2 x (cos, sin)
+// the shared-memory case also stages the reflector block after S and V
 __host__ __device__ constexpr size_t triSmemBytes(int n) {
-    return (n <= kTriSmemN ? sizeof(double) * 2 * (size_t)n * n : 0) + triVecBytes(n);
+    return (n <= kTriSmemN ? sizeof(double) * 2 * (size_t)n * n : 0) + triVecBytes(n) + sizeof(double) * kTriReflBlock * (size_t)n;
+}
+// global-memory case: the vectors, R staged eigenvector rows and the reflector block
+__host__ __device__ constexpr size_t triStageBytes(int n, int rows) {
+    return triVecBytes(n) + sizeof(double) * ((size_t)rows + kTriReflBlock) * (size_t)n;
+}
+// rows of V the global-memory case stages with `bytes` of dynamic shared memory (>= 1)
+__host__ __device__ inline int triStageRows(int n, long long bytes) {
+    const long long rows = (bytes / (long long)sizeof(double) - 7ll * n - (long long)kTriReflBlock * n) / n;
+    return (int)(rows < 1 ? 1 : rows > kTriStageMaxRows ? kTriStageMaxRows : rows);
 }
 __global__ void __launch_bounds__(kEigenThreads) k_marg_tridiag(MargBatch M) {
     const int w = M.bigFirst[blockIdx.x];
@@ -1395,7 +1407,8 @@ __global__ void __launch_bounds__(kEigenThreads) k_marg_tridiag(MargBatch M) {
             for (int j = lane; j < m; j += 32) row[j] -= vi * p[j] + wi * v[j];
         }
         __syncthreads();
-        for (int i = tid; i < m; i += blockDim.x) S[(size_t)(k + 1 + i) * n + k] = v[i];  // keep the reflector
+        // keep the reflector in row k right of the diagonal (contiguous; no later step reads there)
+        for (int i = tid; i < m; i += blockDim.x) S[(size_t)k * n + (k + 1 + i)] = v[i];
         __syncthreads();
     }
     if (tid == 0) {
@@ -1562,21 +1575,45 @@ __global__ void __launch_bounds__(kEigenThreads) k_marg_tridiag(MargBatch M) {
         }
         return;
     }
-    // 3. U = Q V: H_k acts on components k + 1.. of every eigenvector, for k = n - 3 down to 0
-    for (int k = n - 3; k >= 0; --k) {
-        const double tk = tau[k];
-        if (tk == 0.0) continue;  // uniform
-        const int m = n - k - 1;
-        for (int i = tid; i < m; i += blockDim.x) rc[i] = S[(size_t)(k + 1 + i) * n + k];
-        __syncthreads();
-        for (int j = warp; j < n; j += nw) {
-            double* u = Vt + (size_t)j * n + (k + 1);
-            double z = 0;
-            for (int i = lane; i < m; i += 32) z += rc[i] * u[i];
-            z = tk * mWarpSum(z);
-            for (int i = lane; i < m; i += 32) u[i] -= z * rc[i];
+    // 3. U = Q V: H_k acts on components k + 1.. of every eigenvector, for k = n - 3 down to 0.
+    // With V in global memory, batches of R eigenvector rows are staged in shared memory
+    // and every reflector is applied to a batch while it is there; the reflectors come
+    // kTriReflBlock at a time (one round of coalesced loads per block).
+    const int R = inShared ? n : triStageRows(n, M.triSmem);
+    double* Bt = inShared ? Vt : rs + 2 * n;                       // R x n rows of V
+    double* rb = inShared ? rs + 2 * n : Bt + (size_t)R * n;         // kTriReflBlock reflectors, n apart
+    for (int j0 = 0; j0 < n; j0 += R) {
+        const int rows = min(R, n - j0);
+        if (!inShared) {
+            for (long long t = tid; t < (long long)rows * n; t += blockDim.x) Bt[t] = Vt[(size_t)j0 * n + t];
+            __syncthreads();
         }
-        __syncthreads();
+        for (int kb = n - 3; kb >= 0; kb -= kTriReflBlock) {
+            const int nk = min(kTriReflBlock, kb + 1);  // reflectors kb, kb - 1, .., kb - nk + 1
+            for (int q = 0; q < nk; ++q) {
+                const int k = kb - q, m = n - k - 1;
+                for (int i = tid; i < m; i += blockDim.x) rb[(size_t)q * n + i] = S[(size_t)k * n + (k + 1 + i)];
+            }
+            __syncthreads();
+            for (int q = 0; q < nk; ++q) {
+                const int k = kb - q, m = n - k - 1;
+                const double tk = tau[k];
+                if (tk == 0.0) continue;  // uniform
+                const double* v = rb + (size_t)q * n;
+                for (int j = warp; j < rows; j += nw) {
+                    double* u = Bt + (size_t)j * n + (k + 1);
+                    double z = 0;
+                    for (int i = lane; i < m; i += 32) z += v[i] * u[i];
+                    z = tk * mWarpSum(z);
+                    for (int i = lane; i < m; i += 32) u[i] -= z * v[i];
+                }
+                __syncthreads();
+            }
+        }
+        if (!inShared) {
+            for (long long t = tid; t < (long long)rows * n; t += blockDim.x) Vt[(size_t)j0 * n + t] = Bt[t];
+            __syncthreads();
+        }
     }
     // the prior from (lambda, U) as the Jacobi path forms it; eigenvector i is column i of V
     double* ev = M.evals + mw.vec0;
@@ -1997,7 +2034,10 @@ cudaError_t configureMarginalization(size_t visualSmem, size_t rowsSmem, int max
     if ((e = cudaFuncGetAttributes(&ta, k_marg_tridiag)) != cudaSuccess) return e;
     // windows up to kTriSmemN columns in shared memory, the vectors of the widest one
     const int triN = maxNr < 1 ? 1 : (maxNr > kMargMaxSep ? kMargMaxSep : maxNr);
-    *triSmem = (long long)std::max(triSmemBytes(triN < kTriSmemN ? triN : kTriSmemN), triVecBytes(triN));
+    // the largest shared-memory window, or the widest window's vectors with its staged rows
+    // (as many as fit under 200 KB, at most kTriStageMaxRows, at least one)
+    const int stageRows = std::max(1, std::min(kTriStageMaxRows, (int)((200ll * 1024 / sizeof(double) - 7ll * triN - (long long)kTriReflBlock * triN) / std::max(triN, 1))));
+    *triSmem = (long long)std::max(triSmemBytes(triN < kTriSmemN ? triN : kTriSmemN), triStageBytes(triN, stageRows));
     if (*triSmem > (long long)optin - (long long)ta.sharedSizeBytes) return cudaErrorInvalidValue;
     return cudaFuncSetAttribute(k_marg_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<long long>(*triSmem, 1));
 }
