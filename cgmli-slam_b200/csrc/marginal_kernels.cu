@@ -933,12 +933,19 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_victim(MargBatch M) {
 // windows are left to the eigen path (k_marg_tridiag), which takes over this
 // path's tridiagonal form: the reflectors in the window's prior slot, d, e and
 // tau in its victim scratch (fast[w] = 2).
-constexpr int kFastMaxN = 160;    // E in shared memory up to this width
-constexpr int kFastMaxFree = 32;  // null directions handled by the projection
+constexpr int kFastMaxN = 160;        // E in shared memory up to this width
+constexpr int kFastPackedMaxN = 220;  // above it, the tridiagonalization still runs in shared memory on the packed lower triangle
+constexpr int kFastMaxFree = 32;      // null directions handled by the projection
 __host__ __device__ constexpr size_t fastVecBytes(int n) { return sizeof(double) * 5 * (size_t)n + sizeof(int) * 3 * (size_t)n; }
 __host__ __device__ constexpr size_t fastSmemBytes(int n) {
     return n <= kFastMaxN ? sizeof(double) * (size_t)n * n + fastVecBytes(n) : fastVecBytes(n);
 }
+// the vectors (rounded to whole doubles), then the packed lower triangle of E
+__host__ __device__ constexpr size_t fastPackedOffset(int n) { return (fastVecBytes(n) + sizeof(double) - 1) / sizeof(double); }
+__host__ __device__ constexpr size_t fastPackedBytes(int n) {
+    return sizeof(double) * (fastPackedOffset(n) + (size_t)n * (n + 1) / 2);
+}
+__device__ __forceinline__ int packedRow(int r) { return r * (r + 1) / 2; }  // row r of a packed lower triangle
 
 // Number of eigenvalues of the symmetric tridiagonal (d, e) below x, e[i]
 // coupling i and i + 1.
@@ -953,6 +960,83 @@ __device__ int sturmCount(const double* d, const double* e, int n, double x, dou
         if (q < 0) ++c;
     }
     return c;
+}
+
+// Householder tridiagonalization of the symmetric E held as its packed lower triangle
+// Pk (row r at packedRow(r)) by the CTA: the same reflectors and the same tau as the
+// full-square loop of k_marg_fast (d, e, tau and the reflectors saved alike), with
+// the trailing update on the lower triangle only.  Row r of the trailing block reads
+// its entries left of the diagonal along its packed row and those right of it down
+// the packed column.  d[n - 2], e[n - 2] and d[n - 1] are set at the end (thread 0).
+__device__ void fastTridiagonalPacked(double* Pk, int n, double* v, double* p, double* wv, double* d, double* e, double* reflectors,
+                                      double* saved, double* sc) {
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+    for (int k = 0; k + 2 < n; ++k) {
+        const int m = n - k - 1;
+        if (warp == 0) {
+            double sigma = 0;
+            for (int i = lane; i < m; i += 32) {
+                const double x = Pk[packedRow(k + 1 + i) + k];
+                v[i] = x;
+                sigma += x * x;
+            }
+            sigma = mWarpSum(sigma);
+            __syncwarp();
+            if (lane == 0) {
+                d[k] = Pk[packedRow(k) + k];
+                if (sigma == 0.0) {
+                    e[k] = 0.0;
+                    sc[0] = 0.0;
+                } else {
+                    const double x0 = v[0];
+                    const double alpha = x0 >= 0 ? -sqrt(sigma) : sqrt(sigma);
+                    e[k] = alpha;
+                    v[0] = x0 - alpha;
+                    sc[0] = 1.0 / (sigma - x0 * alpha);
+                }
+                saved[2 * n + k] = sc[0];
+            }
+        }
+        __syncthreads();
+        const double tau = sc[0];
+        if (tau == 0.0) {
+            __syncthreads();  // every warp has read sc before warp 0 writes the next column's
+            continue;
+        }
+        for (int i = warp; i < m; i += nw) {  // p = tau S v over the trailing block
+            const int r = k + 1 + i;
+            const double* row = Pk + packedRow(r);
+            double sum = 0;
+            for (int j = lane; j < m; j += 32) {
+                const int c = k + 1 + j;
+                sum += (c <= r ? row[c] : Pk[packedRow(c) + r]) * v[j];
+            }
+            sum = mWarpSum(sum);
+            if (lane == 0) p[i] = tau * sum;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            double pv = 0;
+            for (int i = lane; i < m; i += 32) pv += p[i] * v[i];
+            const double K = 0.5 * tau * mWarpSum(pv);
+            for (int i = lane; i < m; i += 32) wv[i] = p[i] - K * v[i];
+        }
+        __syncthreads();
+        for (int i = warp; i < m; i += nw) {  // lower triangle of the trailing block
+            double* row = Pk + packedRow(k + 1 + i) + (k + 1);
+            const double vi = v[i], wi = wv[i];
+            for (int j = lane; j <= i; j += 32) row[j] -= vi * wv[j] + wi * v[j];
+        }
+        for (int i = tid; i < m; i += blockDim.x) reflectors[k * n + (k + 1 + i)] = v[i];  // row k, right of the diagonal
+        __syncthreads();
+    }
+    if (tid == 0) {
+        if (n >= 2) {
+            d[n - 2] = Pk[packedRow(n - 2) + (n - 2)];
+            e[n - 2] = Pk[packedRow(n - 1) + (n - 2)];
+        }
+        d[n - 1] = Pk[packedRow(n - 1) + (n - 1)];
+    }
 }
 
 __global__ void __launch_bounds__(kMargThreads) k_marg_fast(MargBatch M) {
@@ -976,12 +1060,22 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_fast(MargBatch M) {
     __shared__ double sc[8];
     __shared__ int isc[2];
     // the tridiagonal form for the eigen path, should this path decline the window:
-    // each reflector in its column of the prior's slot (row-major, below the
-    // subdiagonal), d, e and tau in the victim solve's scratch
+    // each reflector in its row of the prior's slot (row-major, right of the
+    // diagonal), d, e and tau in the victim solve's scratch
     double* reflectors = M.A + mw.sep0;
     double* saved = M.X + mw.x0;
     __shared__ double G[kFastMaxFree * kFastMaxFree], h[kFastMaxFree];
     const double* E = M.sepH + mw.sep0;
+    // windows above kFastMaxN: the tridiagonalization on the packed lower triangle in
+    // shared memory when it fits the launch (the rest of this path stays in global memory)
+    const bool packed = !inShared && n <= kFastPackedMaxN && (long long)fastPackedBytes(n) <= M.fastSmem;
+    if (packed) {
+        double* Pk = fsm + fastPackedOffset(n);
+        for (int r = warp; r < n; r += nw)
+            for (int c = lane; c <= r; c += 32) Pk[packedRow(r) + c] = E[(size_t)r * n + c];
+        __syncthreads();
+        fastTridiagonalPacked(Pk, n, v, p, wv, d, e, reflectors, saved, sc);
+    } else {
     for (int t = tid; t < n * n; t += blockDim.x) S[t] = E[t];
     __syncthreads();
     // Householder tridiagonalization (eigenvalues only)
@@ -1046,6 +1140,10 @@ __global__ void __launch_bounds__(kMargThreads) k_marg_fast(MargBatch M) {
             e[n - 2] = S[(n - 1) * n + (n - 2)];
         }
         d[n - 1] = S[(n - 1) * n + (n - 1)];
+    }
+    }  // packed
+    __syncthreads();
+    if (tid == 0) {
         e[n - 1] = 0.0;
         double lo = INFINITY, hi = -INFINITY, emax = 0;
         for (int i = 0; i < n; ++i) {
@@ -2012,11 +2110,13 @@ cudaError_t configureMarginalization(size_t visualSmem, size_t rowsSmem, int max
     if (e != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_marg_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rowsSmem)) != cudaSuccess)
         return e;
-    *fastSmem = maxFastNr > 0 ? (long long)std::max(fastSmemBytes(maxFastNr < kFastMaxN ? maxFastNr : kFastMaxN),
-                                                   fastSmemBytes(maxFastNr < kMargMaxSep ? maxFastNr : kMargMaxSep))
+    // the widest shared-memory window, the widest packed one, the widest window's vectors
+    *fastSmem = maxFastNr > 0 ? (long long)std::max({fastSmemBytes(maxFastNr < kFastMaxN ? maxFastNr : kFastMaxN),
+                                                    maxFastNr > kFastMaxN ? fastPackedBytes(std::min(maxFastNr, kFastPackedMaxN)) : (size_t)0,
+                                                    fastSmemBytes(maxFastNr < kMargMaxSep ? maxFastNr : kMargMaxSep)})
                               : 0;
-    if ((e = cudaFuncSetAttribute(k_marg_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fastSmemBytes(kFastMaxN))) !=
-        cudaSuccess)
+    if ((e = cudaFuncSetAttribute(k_marg_fast, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)std::max(fastSmemBytes(kFastMaxN), fastPackedBytes(kFastPackedMaxN)))) != cudaSuccess)
         return e;
     int dev = 0, optin = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
