@@ -1585,8 +1585,12 @@ __global__ void __launch_bounds__(kEigenThreads) k_marg_tridiag(MargBatch M) {
                         double s = 1.0, c = 1.0, p = 0.0;
                         bool split = false;
                         count = 0;
+                        // d[i], d[i + 1] and e[i] of a step are not yet written by this chase: they
+                        // are carried in registers and the next step's are loaded ahead
+                        double ei = e[m - 1], di = d[m - 1], dip1 = d[m];
                         for (int i = m - 1; i >= l; --i) {
-                            const double f = s * e[i], bq = c * e[i];
+                            const double en = i > l ? e[i - 1] : 0.0, dn = i > l ? d[i - 1] : 0.0;
+                            const double f = s * ei, bq = c * ei;
                             const double q = f * f + g * g;
                             if (q > 1e-280 && q < 1e280) {  // one reciprocal square root for r, c and s
                                 const double rq = rsqrt(q);
@@ -1602,19 +1606,22 @@ __global__ void __launch_bounds__(kEigenThreads) k_marg_tridiag(MargBatch M) {
                             }
                             e[i + 1] = r;
                             if (r == 0.0) {  // the bulge vanished: deflate and restart the chase
-                                d[i + 1] -= p;
+                                d[i + 1] = dip1 - p;
                                 e[m] = 0.0;
                                 split = true;
                                 break;
                             }
-                            g = d[i + 1] - p;
-                            r = (d[i] - g) * s + 2.0 * c * bq;
+                            g = dip1 - p;
+                            r = (di - g) * s + 2.0 * c * bq;
                             p = s * r;
                             d[i + 1] = g + p;
                             g = c * r - bq;
                             cb[count] = c;
                             sb[count] = s;
                             ++count;
+                            dip1 = di;
+                            di = dn;
+                            ei = en;
                         }
                         if (!split) {
                             d[l] -= p;
@@ -1698,12 +1705,22 @@ __global__ void __launch_bounds__(kEigenThreads) k_marg_tridiag(MargBatch M) {
                 const double tk = tau[k];
                 if (tk == 0.0) continue;  // uniform
                 const double* v = rb + (size_t)q * n;
-                for (int j = warp; j < rows; j += nw) {
+                // eight threads per eigenvector row (a reduction of three shuffles), four rows per
+                // warp; the loop bound is uniform over the warp, so every lane reaches the shuffles
+                const int g = tid & 7;
+                for (int j0 = warp * 4; j0 < rows; j0 += nw * 4) {
+                    const int j = j0 + ((tid >> 3) & 3);
+                    const bool active = j < rows;
                     double* u = Bt + (size_t)j * n + (k + 1);
                     double z = 0;
-                    for (int i = lane; i < m; i += 32) z += v[i] * u[i];
-                    z = tk * mWarpSum(z);
-                    for (int i = lane; i < m; i += 32) u[i] -= z * v[i];
+                    if (active)
+                        for (int i = g; i < m; i += 8) z += v[i] * u[i];
+                    z += __shfl_xor_sync(0xffffffffu, z, 4);
+                    z += __shfl_xor_sync(0xffffffffu, z, 2);
+                    z += __shfl_xor_sync(0xffffffffu, z, 1);
+                    z *= tk;
+                    if (active)
+                        for (int i = g; i < m; i += 8) u[i] -= z * v[i];
                 }
                 __syncthreads();
             }
