@@ -34,6 +34,8 @@ int launchIteration(const DevBatch& B, const LaunchPlan& P, int refinement, int 
 int launchIterationParts(const DevBatch& B, const LaunchPlan& P, int refinement, int maxIterations, int probe, double* Sdebug,
                          cudaStream_t s, LaunchHook hook, void* ctx, int parts);
 void launchEvaluate(const DevBatch& B, int derivatives, double* out, int* valid, cudaStream_t s);
+void launchGatherObservations(const DevBatch& B, const int* obOrig, const double* const src[4], double* const dst[4],
+                              cudaStream_t s);
 void launchAddHost(const DevBatch& B, const double* hostH, const double* hostG, const double* hostCost, const unsigned char* flag,
                    int trial, cudaStream_t s);
 int launchLmInit(const DevBatch& B, double lambda0, cudaStream_t s);
@@ -108,6 +110,13 @@ struct cgmli_solver {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // ev0 / ev1 bracket the last timed call; before the first one they were never
+    // recorded, and querying them would leave an error for the next launch check
+    bool timed = false;
+    void readTiming() {
+        float ms = 0;
+        if (timed && cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess) lastMs = ms;
+    }
     // CUDA graph of a whole solve: captured when the same launch sequence (device
     // pointers, work decomposition, iteration budget, options) is solved a second
     // time in a row, replayed while it stays the same; a new topology is solved
@@ -148,6 +157,9 @@ struct cgmli_solver {
     DArray<int> lmValid, lmTrialValid;
     DArray<int> obKf, obCam, obSlot, obXslot;
     DArray<double> obBearing, obP, obVel, obTime;
+    // the payload as uploaded (each window's caller order) and its device-order map
+    DArray<double> obSrcBearing, obSrcP, obSrcVel, obSrcTime;
+    DArray<int> obOrig;
     DArray<double> pose[2], sb[2], ext[2], td[2], rho[2], rotKf[2], rotExt[2];
     DArray<double> imu;
     DArray<int> imuKf;
@@ -255,7 +267,8 @@ struct cgmli_solver {
         auto add = [&](const auto&... a) { ((t += (long long)(a.cap * sizeof(*a.p))), ...); };
         add(dWin, dLm, dRuns, dTiles, dPairChunks, dSchurChunks, schurCols, lmUmap, obLm, keyOrder, bigFirst, keyRows, sch, camR, camT,
             camExt, lmWin, lmKf, lmCam, lmObsBegin, lmNs, lmNx, lmSupp0, supp, lmC0, lmBearing, lmVel, lmTime, lmC, lmD, lmG, lmCost,
-            lmDelta, lmPred, lmTrial, lmMaxInc, lmValid, lmTrialValid, obKf, obCam, obSlot, obXslot, obBearing, obP, obVel, obTime);
+            lmDelta, lmPred, lmTrial, lmMaxInc, lmValid, lmTrialValid, obKf, obCam, obSlot, obXslot, obBearing, obP, obVel, obTime,
+            obSrcBearing, obSrcP, obSrcVel, obSrcTime, obOrig);
         for (int k = 0; k < 2; ++k) add(pose[k], sb[k], ext[k], td[k], rho[k], rotKf[k], rotExt[k]);
         add(imu, imuKf, priorKind, priorIndex, priorCol, priorOff, priorA, priorR0, priorRef, Hret, gret, costRet, trialRet, acc, dr,
             rhs, Sglob, imuScratch, priorScratch, predState, out, Sdebug, retValid, solveStatus);
@@ -295,14 +308,15 @@ struct cgmli_solver {
         if (stream) cudaStreamSynchronize(stream);
         if (graphExec) cudaGraphExecDestroy(graphExec);
         DArray<double>* dbl[] = {&camR, &camT, &lmBearing, &lmVel, &lmTime, &lmC, &lmD, &lmG, &lmCost, &lmDelta, &lmPred, &lmTrial,
-                                 &lmMaxInc, &obBearing, &obP, &obVel, &obTime, &pose[0], &pose[1], &sb[0], &sb[1], &ext[0], &ext[1],
+                                 &lmMaxInc, &obBearing, &obP, &obVel, &obTime, &obSrcBearing, &obSrcP, &obSrcVel, &obSrcTime,
+                                 &pose[0], &pose[1], &sb[0], &sb[1], &ext[0], &ext[1],
                                  &rotKf[0], &rotKf[1], &rotExt[0], &rotExt[1],
                                  &td[0], &td[1], &rho[0], &rho[1], &imu, &priorA, &priorR0, &priorRef, &Hret, &gret, &costRet,
                                  &trialRet, &acc, &dr, &rhs, &Sglob, &imuScratch, &priorScratch, &predState, &out, &Sdebug};
         for (auto* a : dbl) a->release();
         DArray<int>* ints[] = {&camExt, &lmWin, &lmKf, &lmCam, &lmObsBegin, &lmNs, &lmSupp0, &supp, &lmValid, &lmTrialValid, &obKf,
                                &obCam, &obSlot, &imuKf, &priorKind, &priorIndex, &priorCol, &priorOff, &retValid,
-                               &solveStatus, &lmNx, &obXslot};
+                               &solveStatus, &lmNx, &obXslot, &obOrig};
         for (auto* a : ints) a->release();
         lmC0.release(); dWin.release(); dLm.release(); dRuns.release(); dTiles.release();
         dPairChunks.release(); dSchurChunks.release(); schurCols.release(); lmUmap.release(); obLm.release(); keyOrder.release(); bigFirst.release(); keyRows.release(); sch.release();
@@ -443,6 +457,8 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
             cudaError_t e = cudaSuccess;
             auto res = [&](auto& dev, size_t n) { if (e == cudaSuccess) e = dev.reserve(n); };
             res(S->obBearing, 3 * ob); res(S->obP, 6 * ob); res(S->obVel, 3 * ob); res(S->obTime, ob);
+            res(S->obSrcBearing, 3 * ob); res(S->obSrcP, 6 * ob); res(S->obSrcVel, 3 * ob); res(S->obSrcTime, ob);
+            res(S->obOrig, ob);
             res(S->obKf, ob); res(S->obCam, ob); res(S->obSlot, ob); res(S->obXslot, ob); res(S->obLm, ob); res(S->keyOrder, ob);
             res(S->lmWin, lmn); res(S->lmKf, lmn); res(S->lmCam, lmn); res(S->lmNs, lmn); res(S->lmNx, lmn);
             res(S->lmBearing, 3 * lmn); res(S->lmVel, 3 * lmn); res(S->lmTime, lmn); res(S->rho[0], lmn);
@@ -451,8 +467,8 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
         const WinDesc& a = hb.win[w0];
         const WinDesc& b = hb.win[w1 - 1];
         const size_t o0 = a.obs0, on = (size_t)b.obs0 + b.F - o0, l0 = a.lm0, ln = (size_t)b.lm0 + b.L - l0;
-        part(S->obBearing, hb.obBearing, 3 * o0, 3 * on); part(S->obP, hb.obP, 6 * o0, 6 * on);
-        part(S->obVel, hb.obVel, 3 * o0, 3 * on); part(S->obTime, hb.obTime, o0, on);
+        part(S->obSrcBearing, hb.obBearing, 3 * o0, 3 * on); part(S->obSrcP, hb.obP, 6 * o0, 6 * on);
+        part(S->obSrcVel, hb.obVel, 3 * o0, 3 * on); part(S->obSrcTime, hb.obTime, o0, on); part(S->obOrig, hb.obOrig, o0, on);
         part(S->obKf, hb.obKf, o0, on); part(S->obCam, hb.obCam, o0, on); part(S->obSlot, hb.obSlot, o0, on);
         part(S->obXslot, hb.obXslot, o0, on); part(S->obLm, hb.obLm, o0, on); part(S->keyOrder, hb.keyOrder, o0, on);
         part(S->lmWin, hb.lmWin, l0, ln); part(S->lmKf, hb.lmKf, l0, ln); part(S->lmCam, hb.lmCam, l0, ln);
@@ -573,6 +589,13 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     B.wideList = S->numWide ? S->wideList.p : nullptr;
     B.facVec = S->numWide ? S->facVec.p : nullptr;
     B.facFailed = S->numWide ? S->facFailed.p : nullptr;
+    {
+        // the observation payload into device order (after every upload above on this stream)
+        const double* const src[4] = {S->obSrcBearing.p, S->obSrcP.p, S->obSrcVel.p, S->obSrcTime.p};
+        double* const dst[4] = {S->obBearing.p, S->obP.p, S->obVel.p, S->obTime.p};
+        launchGatherObservations(B, S->obOrig.p, src, dst, st);
+        CK(cudaGetLastError());
+    }
     CK(cudaMemsetAsync(S->costRet.p, 0, count * sizeof(double), st));
     CK(cudaMemsetAsync(S->trialRet.p, 0, count * sizeof(double), st));
     CK(S->obRejected.reserve(std::max(1, S->totalObs))); CK(S->gateCounts.reserve((size_t)kGateCounts * count));
@@ -660,6 +683,7 @@ static int runIterations(cgmli_solver* S, int iterations, int probe, double* Sde
             CK(cudaEventRecord(S->ev0, st));
             CK(cudaGraphLaunch(S->graphExec, st));
             CK(cudaEventRecord(S->ev1, st));
+            S->timed = true;
             S->lastLaunches = S->graphLaunches;
             return CGMLI_OK;
         }
@@ -671,6 +695,7 @@ static int runIterations(cgmli_solver* S, int iterations, int probe, double* Sde
                                     S->profile ? profileHook : nullptr, S);
     CK(cudaGetLastError());
     CK(cudaEventRecord(S->ev1, st));
+    S->timed = true;
     S->lastLaunches = launches;
     return CGMLI_OK;
 }
@@ -806,6 +831,7 @@ int cgmli_solver_solve_gated(cgmli_solver* S, int max_iterations, double nis_thr
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(S->ev1, st));
+    S->timed = true;
     S->lastLaunches = launches;
     return CGMLI_OK;
 }
@@ -935,8 +961,7 @@ int cgmli_solver_read_imu(cgmli_solver* S, int window, cgmli_frozen_imu* imu) {
 int cgmli_solver_synchronize(cgmli_solver* S) {
     if (!S) return fail(CGMLI_E_INVALID, "null solver");
     CK(cudaStreamSynchronize(S->stream));
-    float ms = 0;
-    if (cudaEventElapsedTime(&ms, S->ev0, S->ev1) == cudaSuccess) S->lastMs = ms;
+    S->readTiming();
     if (S->profile) S->collectKernelTimes();
     return CGMLI_OK;
 }
@@ -1203,6 +1228,7 @@ int cgmli_solver_solve_host(cgmli_solver* S, int max_iterations, const unsigned 
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(S->ev1, st));
+    S->timed = true;
     S->lastLaunches = launches;
     S->lastKey.clear();  // the next plain solve of this batch is not a repeat of a captured one
     return CGMLI_OK;
@@ -1736,6 +1762,7 @@ static int marginalizeImpl(cgmli_solver* S, const int* victim_kf, int policy, bo
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(S->ev1, st));
+    S->timed = true;
     // the formation buffers now hold one or the other result
     S->haveMarg = !calib;
     S->haveCalib = calib;
@@ -1751,8 +1778,7 @@ int cgmli_solver_read_prior(cgmli_solver* S, int window, int* rank, int* cols, i
     const int W = (int)S->margWin.size();
     if (!S->margCached) {
         CK(cudaStreamSynchronize(S->stream));
-        float ms = 0;
-        if (cudaEventElapsedTime(&ms, S->ev0, S->ev1) == cudaSuccess) S->lastMs = ms;
+        S->readTiming();
         HostBatch& hb = S->hb;
         sizeTo(S->hMargA, S->margSepTotal);
         sizeTo(S->hMargR0, S->margVecTotal);

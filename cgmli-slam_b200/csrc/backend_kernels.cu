@@ -1988,8 +1988,34 @@ __global__ void k_add_host(DevBatch B, const double* hostH, const double* hostG,
     if (threadIdx.x == 0) B.costRet[w] += hostCost[w];
 }
 
+// Observation payload (bearing 3, information square root 6, bearing velocity 3,
+// time 1) from each window's caller order into device order: obOrig is the
+// caller's index within the window, the window's obs0 its base.  One thread per
+// observation; the source runs are contiguous within a landmark.
+__global__ void k_gather_obs(const DevBatch B, const int* __restrict__ obOrig, const double* __restrict__ srcBearing,
+                             const double* __restrict__ srcP, const double* __restrict__ srcVel, const double* __restrict__ srcTime,
+                             double* __restrict__ bearing, double* __restrict__ P, double* __restrict__ vel, double* __restrict__ time) {
+    for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < B.numObs; o += gridDim.x * blockDim.x) {
+        const long long f = (long long)B.win[B.lmWin[B.obLm[o]]].obs0 + obOrig[o];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            bearing[3ll * o + k] = srcBearing[3 * f + k];
+            vel[3ll * o + k] = srcVel[3 * f + k];
+        }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) P[6ll * o + k] = srcP[6 * f + k];
+        time[o] = srcTime[f];
+    }
+}
+
 // ---------------------------------------------------------------------------------------
 // host-side launchers (called by backend_host.cu)
+void launchGatherObservations(const DevBatch& B, const int* obOrig, const double* const src[4], double* const dst[4],
+                              cudaStream_t s) {
+    if (B.numObs <= 0) return;
+    const int blocks = (int)std::min<long long>((B.numObs + 255) / 256, 148ll * 8);
+    k_gather_obs<<<blocks, 256, 0, s>>>(B, obOrig, src[0], src[1], src[2], src[3], dst[0], dst[1], dst[2], dst[3]);
+}
 void launchEvaluate(const DevBatch& B, int derivatives, double* out, int* valid, cudaStream_t s) {
     k_rotations<<<B.numWindows, 64, 0, s>>>(B);
     if (B.numObs > 0) k_evaluate<<<(B.numObs + 127) / 128, 128, 0, s>>>(B, derivatives, out, valid);

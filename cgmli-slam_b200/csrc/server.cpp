@@ -57,8 +57,9 @@ struct Request {
     std::vector<double> calibConditional, calibEvals;
 };
 
-// Device bytes a window occupies in a batch (observation, landmark and dense
-// per-window arrays, both state buffers, the staged rows and the marginalization).
+// Device bytes a window occupies in a batch (observation arrays and the uploaded
+// payload they are gathered from, landmark and dense per-window arrays, both state
+// buffers, the staged rows and the marginalization).
 // The solvers' device arrays are grow-only and grow by at least half their size,
 // so a batch whose windows need N bytes can leave a solver holding up to 1.5 N:
 // admission counts kGrowth times the footprint.
@@ -67,7 +68,7 @@ long long footprint(const cgmli_window& w) {
     const long long F = w.num_observations, L = w.num_landmarks, K = w.num_keyframes;
     const long long ncal = (w.estimate_extrinsics ? 6ll * w.num_extrinsics : 0) + (w.estimate_td ? 1 : 0);
     const long long Nr = 15 * K + ncal, Npc = 6 * K + ncal, m = 15 * K + 6ll * w.num_extrinsics + 1;
-    return F * (120 + 448) + L * (160 + 8 * (6 * 12 + 7)) + 8 * (3 * Nr * Nr + Npc * Npc + 4 * m * m) + 4096;
+    return F * (120 + 108 + 448) + L * (160 + 8 * (6 * 12 + 7)) + 8 * (3 * Nr * Nr + Npc * Npc + 4 * m * m) + 4096;
 }
 }  // namespace
 

@@ -56,7 +56,36 @@ struct WindowPart {
     int maxNs = 1;
     int status = CGMLI_OK;
     std::string why;
+    // scratch of the build
+    int ranges = 1;                      // landmark ranges of kBuildRange (steps A and C)
+    std::vector<int> nkf, nx;            // per landmark: support keyframes, support extrinsics
+    std::vector<const int*> sup;         // per landmark: its support list (in flat)
+    std::vector<std::vector<int>> flat;  // per landmark range: the support lists of its landmarks
+    std::vector<int> order;              // device position -> landmark
+    std::vector<int> obStart;            // device position -> its first observation in the batch
+    std::vector<int> rangeStatus;        // per landmark range
+    // support order: length, keyframes, then extrinsics (the shorter keyframe list
+    // first where one is a prefix of the other)
+    bool less(int a, int b) const {
+        const int la = nkf[a] + nx[a], lb = nkf[b] + nx[b];
+        if (la != lb) return la < lb;
+        const int* pa = sup[a];
+        const int* pb = sup[b];
+        const int n = std::min(nkf[a], nkf[b]);
+        for (int j = 0; j < n; ++j)
+            if (pa[j] != pb[j]) return pa[j] < pb[j];
+        if (nkf[a] != nkf[b]) return nkf[a] < nkf[b];
+        for (int j = nkf[a]; j < la; ++j)
+            if (pa[j] != pb[j]) return pa[j] < pb[j];
+        return false;
+    }
+    bool same(int a, int b) const {
+        return nkf[a] == nkf[b] && nx[a] == nx[b] && std::equal(sup[a], sup[a] + nkf[a] + nx[a], sup[b]);
+    }
 };
+// Landmarks per work item of the build's range steps: a large window is split
+// over several threads.
+constexpr int kBuildRange = 256;
 }  // namespace
 
 int validateWindow(const cgmli_window& w, int index, std::string& why) {
@@ -203,12 +232,100 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
     sizeTo(hb.priorA, pA); sizeTo(hb.priorR0, pR); sizeTo(hb.priorRef, pRef);
     hb.lmObsBegin[lm] = ob;
     const int runLen = plan.runLandmarks > 0 ? plan.runLandmarks : runLength(lm);
-    // ---- phase 1: every window on its own thread
+    // ---- phase 1, in four steps so that a large window is built by several threads:
+    //  A (ranges of a window's landmarks): support lists, and the range sorted by support;
+    //  B (per window): states and rig; the sorted ranges merged into the device order;
+    //    runs and tiles; offsets of each landmark's support, cross-vector entries and
+    //    observations;
+    //  C (ranges of the device order): landmark and observation arrays;
+    //  D (two items per window): the key order of the J^T J pass; the Schur chunks.
     std::vector<WindowPart> part(count);
-    auto phase1 = [&](int i) {
+    for (int i = 0; i < count; ++i) {
+        const int L = hb.win[i].L;
+        WindowPart& P = part[i];
+        P.ranges = std::max(1, (L + kBuildRange - 1) / kBuildRange);
+        P.nkf.resize(L);
+        P.nx.resize(L);
+        P.sup.resize(L);
+        P.order.resize(L);
+        P.obStart.resize(L);
+        P.flat.resize(P.ranges);
+        P.rangeStatus.assign(P.ranges, CGMLI_OK);
+    }
+    auto stepA = [&](int i, int r) {
         const auto& w = windows[i];
         const WinDesc& d = hb.win[i];
         WindowPart& P = part[i];
+        const int l0 = r * kBuildRange, l1 = std::min(d.L, l0 + kBuildRange);
+        if (l0 >= l1) return;
+        // supports: keyframes (anchor first, then observers ascending), then the
+        // extrinsic blocks the observations touch (anchor camera's first, then ascending)
+        std::vector<int>& flat = P.flat[r];
+        flat.clear();
+        flat.reserve((size_t)2 * (w.lm_obs_begin[l1] - w.lm_obs_begin[l0]) + 2 * (l1 - l0) + 1);
+        for (int l = l0; l < l1; ++l) {
+            const int b = w.lm_obs_begin[l], e = w.lm_obs_begin[l + 1];
+            const int s0 = (int)flat.size();
+            flat.push_back(w.lm_anchor_kf[l]);
+            for (int f = b; f < e; ++f) {
+                const int k = w.obs_kf[f];
+                bool seen = false;
+                for (int j = s0; j < (int)flat.size(); ++j) seen = seen || flat[j] == k;
+                if (!seen) {  // insertion into the sorted tail (after the anchor)
+                    flat.push_back(k);
+                    for (int j = (int)flat.size() - 1; j > s0 + 1 && flat[j - 1] > flat[j]; --j) std::swap(flat[j - 1], flat[j]);
+                }
+            }
+            P.nkf[l] = (int)flat.size() - s0;
+            if (P.nkf[l] > kMaxSupport) {
+                P.rangeStatus[r] = CGMLI_E_LIMIT;
+                return;
+            }
+            const int x0 = (int)flat.size();
+            if (d.estExt) {
+                flat.push_back(w.cam_ext[w.lm_anchor_cam[l]]);
+                for (int f = b; f < e; ++f) {
+                    const int x = w.cam_ext[w.obs_cam[f]];
+                    bool seen = false;
+                    for (int j = x0; j < (int)flat.size(); ++j) seen = seen || flat[j] == x;
+                    if (!seen) {
+                        flat.push_back(x);
+                        for (int j = (int)flat.size() - 1; j > x0 + 1 && flat[j - 1] > flat[j]; --j) std::swap(flat[j - 1], flat[j]);
+                    }
+                }
+            }
+            P.nx[l] = (int)flat.size() - x0;
+        }
+        // the observation payload of these landmarks in the caller's order (one
+        // contiguous range); the device gathers it into device order through obOrig
+        {
+            const long long b0 = w.lm_obs_begin[l0], n = w.lm_obs_begin[l1] - b0, o0 = d.obs0 + b0;
+            std::memcpy(&hb.obBearing[3 * o0], &w.obs_bearing[3 * b0], sizeof(double) * 3 * n);
+            std::memcpy(&hb.obP[6 * o0], &w.obs_P[6 * b0], sizeof(double) * 6 * n);
+            if (w.obs_velocity) std::memcpy(&hb.obVel[3 * o0], &w.obs_velocity[3 * b0], sizeof(double) * 3 * n);
+            else std::memset(&hb.obVel[3 * o0], 0, sizeof(double) * 3 * n);
+            if (w.obs_time) std::memcpy(&hb.obTime[o0], &w.obs_time[b0], sizeof(double) * n);
+            else std::memset(&hb.obTime[o0], 0, sizeof(double) * n);
+        }
+        // the list is final: point each landmark at its support
+        for (int l = l0, s = 0; l < l1; ++l) {
+            P.sup[l] = flat.data() + s;
+            s += P.nkf[l] + P.nx[l];
+        }
+        // the range in support order (stable); step B merges the ranges
+        for (int l = l0; l < l1; ++l) P.order[l] = l;
+        std::stable_sort(P.order.begin() + l0, P.order.begin() + l1, [&P](int a, int b) { return P.less(a, b); });
+    };
+    auto stepB = [&](int i) {
+        const auto& w = windows[i];
+        const WinDesc& d = hb.win[i];
+        WindowPart& P = part[i];
+        for (int r = 0; r < P.ranges; ++r)
+            if (P.rangeStatus[r] != CGMLI_OK) {
+                P.status = P.rangeStatus[r];
+                P.why = "landmark support above 64 keyframes";
+                return;
+            }
         // states, rig, IMU, prior
         std::memcpy(&hb.pose[7ll * d.kf0], w.poses, sizeof(double) * 7 * d.K);
         {
@@ -257,87 +374,27 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
                 std::memcpy(&hb.priorRef[pRef0[i]], w.prior_ref, sizeof(double) * amb);
             }
         }
-        // supports: keyframes (anchor first, then observers ascending), then the
-        // extrinsic blocks the observations touch (anchor camera's first, then ascending)
+        // device order: landmarks sorted (stably) by support, so that equal supports are
+        // adjacent; merging the stably sorted ranges pairwise, the left range first on
+        // ties, gives the stable sort of the whole window
         const int L = d.L;
-        std::vector<int> supStart(L + 1), nkf(L), nx(L);
-        std::vector<int> flat;
-        flat.reserve((size_t)2 * d.F + 2 * L + 1);
-        for (int l = 0; l < L; ++l) {
-            supStart[l] = (int)flat.size();
-            const int b = w.lm_obs_begin[l], e = w.lm_obs_begin[l + 1];
-            const int s0 = (int)flat.size();
-            flat.push_back(w.lm_anchor_kf[l]);
-            for (int f = b; f < e; ++f) {
-                const int k = w.obs_kf[f];
-                bool seen = false;
-                for (int j = s0; j < (int)flat.size(); ++j) seen = seen || flat[j] == k;
-                if (!seen) {  // insertion into the sorted tail (after the anchor)
-                    flat.push_back(k);
-                    for (int j = (int)flat.size() - 1; j > s0 + 1 && flat[j - 1] > flat[j]; --j) std::swap(flat[j - 1], flat[j]);
-                }
+        auto less = [&P](int a, int b) { return P.less(a, b); };
+        for (int width = 1; width < P.ranges; width *= 2)
+            for (int r = 0; r + width < P.ranges; r += 2 * width) {
+                const auto first = P.order.begin() + (long long)r * kBuildRange;
+                const auto mid = P.order.begin() + (long long)(r + width) * kBuildRange;
+                const auto last = P.order.begin() + std::min<long long>(L, (long long)(r + 2 * width) * kBuildRange);
+                std::inplace_merge(first, mid, last, less);
             }
-            nkf[l] = (int)flat.size() - s0;
-            if (nkf[l] > kMaxSupport) {
-                P.status = CGMLI_E_LIMIT;
-                P.why = "landmark support above 64 keyframes";
-                return;
-            }
-            const int x0 = (int)flat.size();
-            if (d.estExt) {
-                flat.push_back(w.cam_ext[w.lm_anchor_cam[l]]);
-                for (int f = b; f < e; ++f) {
-                    const int x = w.cam_ext[w.obs_cam[f]];
-                    bool seen = false;
-                    for (int j = x0; j < (int)flat.size(); ++j) seen = seen || flat[j] == x;
-                    if (!seen) {
-                        flat.push_back(x);
-                        for (int j = (int)flat.size() - 1; j > x0 + 1 && flat[j - 1] > flat[j]; --j) std::swap(flat[j - 1], flat[j]);
-                    }
-                }
-            }
-            nx[l] = (int)flat.size() - x0;
-        }
-        supStart[L] = (int)flat.size();
-        // device order: landmarks sorted (stably) by support, so that equal supports are adjacent;
-        // key: (support length, keyframes, separator, extrinsics)
-        std::vector<int> order(L);
-        for (int l = 0; l < L; ++l) order[l] = l;
-        auto lessSupport = [&](int a, int b) {
-            const int la = supStart[a + 1] - supStart[a], lb = supStart[b + 1] - supStart[b];
-            if (la != lb) return la < lb;
-            const int* pa = &flat[supStart[a]];
-            const int* pb = &flat[supStart[b]];
-            const int n = std::min(nkf[a], nkf[b]);
-            for (int j = 0; j < n; ++j)
-                if (pa[j] != pb[j]) return pa[j] < pb[j];
-            if (nkf[a] != nkf[b]) return nkf[a] < nkf[b];  // the shorter keyframe list meets the separator first
-            for (int j = nkf[a]; j < la; ++j)
-                if (pa[j] != pb[j]) return pa[j] < pb[j];
-            return false;
-        };
-        std::stable_sort(order.begin(), order.end(), lessSupport);
-        // landmark and observation arrays in device order
-        int obPos = d.obs0;
-        int tileObs = 0, runLms = 0;
-        auto sameSupport = [&](int a, int b) { return !lessSupport(a, b) && !lessSupport(b, a); };
+        // runs of landmarks (a new run at a support change once a run holds runLen
+        // landmarks, and at 4 runLen), tiles of at most kMaxTrackChunk observations,
+        // and the window-local offsets of supports and cross-vector entries
+        int obPos = d.obs0, tileObs = 0, runLms = 0;
+        long long suppSize = 0;
         for (int q = 0; q < L; ++q) {
-            if (q + 8 < L) {  // the support order jumps through the caller's arrays: fetch ahead
-                const int lp = order[q + 8], bp = w.lm_obs_begin[lp];
-                __builtin_prefetch(&w.obs_kf[bp]);
-                __builtin_prefetch(&w.obs_cam[bp]);
-                __builtin_prefetch(&w.obs_bearing[3ll * bp]);
-                __builtin_prefetch(&w.obs_P[6ll * bp]);
-                __builtin_prefetch(&w.obs_P[6ll * bp + 8]);
-                if (w.obs_velocity) __builtin_prefetch(&w.obs_velocity[3ll * bp]);
-                if (w.obs_time) __builtin_prefetch(&w.obs_time[bp]);
-                __builtin_prefetch(&w.lm_anchor_bearing[3ll * lp]);
-                __builtin_prefetch(&w.rho[lp]);
-                __builtin_prefetch(&flat[supStart[lp]]);
-            }
-            const int l = order[q], g = d.lm0 + q;
-            const int b = w.lm_obs_begin[l], e = w.lm_obs_begin[l + 1], nobs = e - b;
-            const bool newGroup = q == 0 || !sameSupport(order[q - 1], l);
+            const int l = P.order[q], g = d.lm0 + q;
+            const int nobs = w.lm_obs_begin[l + 1] - w.lm_obs_begin[l];
+            const bool newGroup = q == 0 || !P.same(P.order[q - 1], l);
             if (q == 0 || (runLms >= runLen && newGroup) || runLms >= 4 * runLen) {
                 if (!P.runs.empty()) P.runs.back().z = (int)P.tiles.size();
                 if (!P.tiles.empty()) P.tiles.back().y = g;
@@ -352,44 +409,64 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
             }
             tileObs += nobs;
             ++runLms;
+            const int width = P.nkf[l] + P.nx[l];
+            hb.lmSupp0[g] = (int)suppSize;  // window-local, fixed up after the prefix sum
+            suppSize += width;
+            const int ns = 6 * width + (d.estTd ? 1 : 0);
+            hb.lmC0[g] = P.cross;  // window-local
+            P.cross += ns;
+            P.maxNs = std::max(P.maxNs, ns);
+            P.obStart[q] = obPos;
+            obPos += nobs;
+        }
+        if (L) {
+            P.tiles.back().y = d.lm0 + L;
+            P.runs.back().z = (int)P.tiles.size();
+        }
+        P.supp.resize(suppSize);
+    };
+    auto stepC = [&](int i, int r) {
+        const auto& w = windows[i];
+        const WinDesc& d = hb.win[i];
+        WindowPart& P = part[i];
+        const int L = d.L;
+        const int q0 = r * kBuildRange, q1 = std::min(L, q0 + kBuildRange);
+        for (int q = q0; q < q1; ++q) {
+            if (q + 8 < L) {  // the support order jumps through the caller's arrays: fetch ahead
+                const int lp = P.order[q + 8], bp = w.lm_obs_begin[lp];
+                __builtin_prefetch(&w.obs_kf[bp]);
+                __builtin_prefetch(&w.obs_cam[bp]);
+                __builtin_prefetch(&w.lm_anchor_bearing[3ll * lp]);
+                __builtin_prefetch(&w.rho[lp]);
+                __builtin_prefetch(P.sup[lp]);
+            }
+            const int l = P.order[q], g = d.lm0 + q;
+            const int b = w.lm_obs_begin[l], nobs = w.lm_obs_begin[l + 1] - b;
+            const int nk = P.nkf[l], nxl = P.nx[l];
+            const int* sl = P.sup[l];
             hb.lmPerm[g] = l;
             hb.lmWin[g] = i;
             hb.lmKf[g] = d.kf0 + w.lm_anchor_kf[l];
             hb.lmCam[g] = d.cam0 + w.lm_anchor_cam[l];
-            hb.lmObsBegin[g] = obPos;
+            hb.lmObsBegin[g] = P.obStart[q];
             for (int k = 0; k < 3; ++k) {
                 hb.lmBearing[3ll * g + k] = w.lm_anchor_bearing[3 * l + k];
                 hb.lmVel[3ll * g + k] = w.lm_anchor_velocity ? w.lm_anchor_velocity[3 * l + k] : 0.0;
             }
             hb.lmTime[g] = w.lm_anchor_time ? w.lm_anchor_time[l] : 0.0;
-            hb.lmNs[g] = nkf[l];
-            hb.lmNx[g] = nx[l];
-            hb.lmSupp0[g] = (int)P.supp.size();  // window-local, fixed up after the prefix sum
-            const int* sl = &flat[supStart[l]];
-            P.supp.insert(P.supp.end(), sl, sl + nkf[l] + nx[l]);
-            const int ns = 6 * (nkf[l] + nx[l]) + (d.estTd ? 1 : 0);
-            hb.lmC0[g] = P.cross;  // window-local
-            P.cross += ns;
-            P.maxNs = std::max(P.maxNs, ns);
+            hb.lmNs[g] = nk;
+            hb.lmNx[g] = nxl;
+            std::copy(sl, sl + nk + nxl, P.supp.begin() + hb.lmSupp0[g]);
             hb.rho[g] = w.rho[l];
             hb.lmFixed[g] = w.lm_fixed ? w.lm_fixed[l] : 0;
             // observations sorted by observer keyframe (slot order), stable
             int fo[kMaxTrackChunk];
-            bool inOrder = true;
             for (int k = 0; k < nobs; ++k) {
                 int j = k;
                 fo[j] = b + k;
-                while (j > 0 && w.obs_kf[fo[j - 1]] > w.obs_kf[fo[j]]) { std::swap(fo[j - 1], fo[j]); --j; inOrder = false; }
+                while (j > 0 && w.obs_kf[fo[j - 1]] > w.obs_kf[fo[j]]) { std::swap(fo[j - 1], fo[j]); --j; }
             }
-            if (inOrder && nobs > 0) {  // the usual case: the observation arrays copy as runs
-                const size_t o0 = (size_t)obPos;
-                std::memcpy(&hb.obBearing[3 * o0], &w.obs_bearing[3ll * b], sizeof(double) * 3 * nobs);
-                std::memcpy(&hb.obP[6 * o0], &w.obs_P[6ll * b], sizeof(double) * 6 * nobs);
-                if (w.obs_velocity) std::memcpy(&hb.obVel[3 * o0], &w.obs_velocity[3ll * b], sizeof(double) * 3 * nobs);
-                else std::memset(&hb.obVel[3 * o0], 0, sizeof(double) * 3 * nobs);
-                if (w.obs_time) std::memcpy(&hb.obTime[o0], &w.obs_time[b], sizeof(double) * nobs);
-                else std::memset(&hb.obTime[o0], 0, sizeof(double) * nobs);
-            }
+            int obPos = P.obStart[q];
             for (int k = 0; k < nobs; ++k) {
                 const int f = fo[k], o = obPos++;
                 hb.obLm[o] = g;
@@ -402,45 +479,43 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
                 int xs = 0;
                 if (d.estExt) {
                     const int x = w.cam_ext[w.obs_cam[f]];
-                    while (sl[nkf[l] + xs] != x) ++xs;
+                    while (sl[nk + xs] != x) ++xs;
                 }
                 hb.obXslot[o] = xs;
-                if (inOrder) continue;
-                for (int k2 = 0; k2 < 3; ++k2) {
-                    hb.obBearing[3ll * o + k2] = w.obs_bearing[3 * f + k2];
-                    hb.obVel[3ll * o + k2] = w.obs_velocity ? w.obs_velocity[3 * f + k2] : 0.0;
-                }
-                for (int k2 = 0; k2 < 6; ++k2) hb.obP[6ll * o + k2] = w.obs_P[6 * f + k2];
-                hb.obTime[o] = w.obs_time ? w.obs_time[f] : 0.0;
             }
         }
-        if (L) {
-            P.tiles.back().y = d.lm0 + L;
-            P.runs.back().z = (int)P.tiles.size();
+    };
+    auto stepD = [&](int i, int which) {
+        const WinDesc& d = hb.win[i];
+        WindowPart& P = part[i];
+        const int L = d.L;
+        (void)L;
+        if (which == 0) {
+            // key order (anchor kf, observer kf, anchor ext, observer ext) of the J^T J pass
+            const int F = d.F;
+            auto keyOf = [&](int o) {
+                const int g = hb.obLm[o];
+                const int a = hb.lmKf[g] - d.kf0, bkf = hb.obKf[o] - d.kf0;
+                const int ea = hb.camExt[hb.lmCam[g]] - d.ext0, eb = hb.camExt[hb.obCam[o]] - d.ext0;
+                return ((long long)(a * d.K + bkf) * d.E + ea) * d.E + eb;
+            };
+            const long long buckets = (long long)d.K * d.K * d.E * d.E;
+            int* ko = F ? &hb.keyOrder[d.obs0] : nullptr;
+            if (buckets <= 4ll * F + 4096) {
+                std::vector<int> cnt(buckets + 1, 0);
+                for (int g = 0; g < F; ++g) ++cnt[keyOf(d.obs0 + g) + 1];
+                for (long long k = 0; k < buckets; ++k) cnt[k + 1] += cnt[k];
+                for (int g = 0; g < F; ++g) ko[cnt[keyOf(d.obs0 + g)]++] = d.obs0 + g;
+            } else {
+                std::vector<std::pair<long long, int>> kv(F);
+                for (int g = 0; g < F; ++g) kv[g] = {keyOf(d.obs0 + g), d.obs0 + g};
+                std::sort(kv.begin(), kv.end());
+                for (int g = 0; g < F; ++g) ko[g] = kv[g].second;
+            }
+            for (int c0 = 0; c0 < F; c0 += plan.pairChunk)
+                P.pairChunks.push_back(make_int4(i, d.obs0 + c0, d.obs0 + std::min(F, c0 + plan.pairChunk), 0));
+            return;
         }
-        // key order (anchor kf, observer kf, anchor ext, observer ext) of the J^T J pass
-        const int F = d.F;
-        auto keyOf = [&](int o) {
-            const int g = hb.obLm[o];
-            const int a = hb.lmKf[g] - d.kf0, bkf = hb.obKf[o] - d.kf0;
-            const int ea = hb.camExt[hb.lmCam[g]] - d.ext0, eb = hb.camExt[hb.obCam[o]] - d.ext0;
-            return ((long long)(a * d.K + bkf) * d.E + ea) * d.E + eb;
-        };
-        const long long buckets = (long long)d.K * d.K * d.E * d.E;
-        int* ko = F ? &hb.keyOrder[d.obs0] : nullptr;
-        if (buckets <= 4ll * F + 4096) {
-            std::vector<int> cnt(buckets + 1, 0);
-            for (int g = 0; g < F; ++g) ++cnt[keyOf(d.obs0 + g) + 1];
-            for (long long k = 0; k < buckets; ++k) cnt[k + 1] += cnt[k];
-            for (int g = 0; g < F; ++g) ko[cnt[keyOf(d.obs0 + g)]++] = d.obs0 + g;
-        } else {
-            std::vector<std::pair<long long, int>> kv(F);
-            for (int g = 0; g < F; ++g) kv[g] = {keyOf(d.obs0 + g), d.obs0 + g};
-            std::sort(kv.begin(), kv.end());
-            for (int g = 0; g < F; ++g) ko[g] = kv[g].second;
-        }
-        for (int c0 = 0; c0 < F; c0 += plan.pairChunk)
-            P.pairChunks.push_back(make_int4(i, d.obs0 + c0, d.obs0 + std::min(F, c0 + plan.pairChunk), 0));
         // Schur chunks: runs of consecutive landmarks whose support columns
         // together fit the chunk's shared rows (schurChunkFits); the column
         // union of each chunk and every landmark's map into it.  Unions are kept
@@ -514,11 +589,49 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
             if (L > q0) closeChunk(L);
         }
     };
-    // in up to four ranges of windows when a caller streams the finished ranges
+    // A batch of at least two windows per thread, or of small windows only, keeps the
+    // threads busy with whole windows, largest first so that no thread is left with a
+    // large one at the end; otherwise the steps run one after the other, each split
+    // over the threads.  In up to four ranges of windows when a caller streams the
+    // finished ranges.
+    int maxL = 0;
+    for (int i = 0; i < count; ++i) maxL = std::max(maxL, hb.win[i].L);
+    const bool whole = count >= 2 * threads || maxL <= 4 * kBuildRange;
     const int ranges = ready && count >= 4 * threads ? 4 : 1;
-    for (int r = 0; r < ranges; ++r) {
-        const int w0 = (int)((long long)count * r / ranges), w1 = (int)((long long)count * (r + 1) / ranges);
-        parallelFor(w1 - w0, threads, [&](int k) { phase1(w0 + k); });
+    std::vector<int2> items;
+    std::vector<int> bySize;
+    for (int rg = 0; rg < ranges; ++rg) {
+        const int w0 = (int)((long long)count * rg / ranges), w1 = (int)((long long)count * (rg + 1) / ranges);
+        if (whole) {
+            bySize.resize(w1 - w0);
+            for (int k = 0; k < w1 - w0; ++k) bySize[k] = w0 + k;
+            std::stable_sort(bySize.begin(), bySize.end(), [&](int a, int b) {
+                return hb.win[a].F + hb.win[a].L > hb.win[b].F + hb.win[b].L;
+            });
+            parallelFor(w1 - w0, threads, [&](int k) {
+                const int i = bySize[k];
+                for (int r = 0; r < part[i].ranges; ++r) stepA(i, r);
+                stepB(i);
+                if (part[i].status != CGMLI_OK) return;
+                for (int r = 0; r < part[i].ranges; ++r) stepC(i, r);
+                stepD(i, 0);
+                stepD(i, 1);
+            });
+        } else {
+            items.clear();
+            for (int i = w0; i < w1; ++i)
+                for (int r = 0; r < part[i].ranges; ++r) items.push_back(make_int2(i, r));
+            parallelFor((int)items.size(), threads, [&](int k) { stepA(items[k].x, items[k].y); });
+            parallelFor(w1 - w0, threads, [&](int k) { stepB(w0 + k); });
+            bool failed = false;
+            for (int i = w0; i < w1; ++i) failed = failed || part[i].status != CGMLI_OK;
+            if (failed) break;
+            parallelFor((int)items.size(), threads, [&](int k) { stepC(items[k].x, items[k].y); });
+            parallelFor(2 * (w1 - w0), threads, [&](int k) { stepD(w0 + k / 2, k % 2); });
+        }
+        bool failed = false;
+        for (int i = w0; i < w1; ++i) failed = failed || part[i].status != CGMLI_OK;
+        if (failed) break;
         if (ready) (*ready)(w0, w1);
     }
     for (int i = 0; i < count; ++i)

@@ -186,6 +186,8 @@ struct HostBatch {
     // observations (device order)
     HVec<int> obKf, obCam, obSlot, obXslot, obLm, keyOrder;
     HVec<int> obOrig;        // device observation -> observation index within its window
+    // observation payload in each window's caller order (from WinDesc::obs0); the
+    // device gathers it into device order through obOrig
     HVec<double> obBearing, obP, obVel, obTime;
     // states
     HVec<double> pose, sb, ext, td, rho;

@@ -220,3 +220,20 @@ def test_solver_device_bytes_grow_only(backend):
     a = s.device_bytes()
     s.set_windows([synth.SynthWindow(replace(SPEC, landmarks=100), 81)])
     assert s.device_bytes() == a > 0
+
+
+def test_synchronize_and_timing_before_the_first_solve(backend):
+    """A caller may synchronize (and read the timing) right after set_windows:
+    the timing events were never recorded then, and the next solve (with or
+    without per-kernel events) must still launch cleanly."""
+    s = backend.Solver()
+    s.set_windows([synth.SynthWindow(SPEC, 82)])
+    s.synchronize()
+    assert s.timing()[0] == 0.0
+    s.kernel_times(1)
+    s.solve(1)
+    s.synchronize()
+    kt = s.kernel_times(-1)
+    s.kernel_times(0)
+    assert kt["linearize"][1] == 1 and kt["factor"][1] >= 1
+    assert s.timing()[0] > 0

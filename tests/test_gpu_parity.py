@@ -63,6 +63,40 @@ def test_step_matches_oracle(oracle, backend, name, lam):
     assert got["trial_valid"] and abs(got["trial_cost"] - ref["trial_cost"]) <= 1e-10 * abs(ref["trial_cost"])
 
 
+def _reverse_tracks(w):
+    """Reverses every landmark's observations in the caller's arrays (keyframes
+    descending), so that the device order differs from the caller's within each
+    track and the uploaded payload is gathered through a non-trivial map."""
+    win = w.window
+    F, L = win.num_observations, win.num_landmarks
+    beg = np.ctypeslib.as_array(win.lm_obs_begin, shape=(L + 1,))
+    fields = [(win.obs_kf, 1), (win.obs_cam, 1), (win.obs_bearing, 3), (win.obs_P, 6)]
+    if win.obs_velocity:
+        fields.append((win.obs_velocity, 3))
+    for ptr, k in fields:
+        a = np.ctypeslib.as_array(ptr, shape=(F * k,)).reshape(F, k)
+        for l in range(L):
+            a[beg[l]:beg[l + 1]] = a[beg[l]:beg[l + 1]][::-1].copy()
+
+
+@pytest.mark.parametrize("name", ["shared_calib", "long_tracks_8cam"])
+def test_step_with_tracks_out_of_keyframe_order(oracle, backend, name):
+    w = synth.SynthWindow(SPECS[name], 23)
+    _reverse_tracks(w)
+    nr, L = w.retained_dim(), w.L
+    ref = oracle.step(w.window, nr, L, 1e-4)
+    assert ref["status"] == 0
+    s = backend.Solver()
+    s.set_windows([w])
+    s.step(1e-4)
+    got = s.read_step(0)
+    S, rhs = s.read_reduced(0)
+    assert got["status"] == 0
+    assert rel(S, ref["S"]) < 1e-12
+    assert rel(rhs, ref["rhs"]) < 1e-11
+    assert rel(got["delta"], ref["delta"]) < 1e-9
+
+
 def test_large_window_global_factor_path(oracle, backend):
     """30 keyframes, 8 cameras, track length up to 25: N_r = 457 takes the wide
     factorization sequence (panels and trailing tiles over the whole GPU)."""

@@ -115,7 +115,7 @@ def _footprint(win):
     F, L, K = win.num_observations, win.num_landmarks, win.num_keyframes
     ncal = (6 * win.num_extrinsics if win.estimate_extrinsics else 0) + (1 if win.estimate_td else 0)
     Nr, Npc, m = 15 * K + ncal, 6 * K + ncal, 15 * K + 6 * win.num_extrinsics + 1
-    return F * (120 + 448) + L * (160 + 8 * (6 * 12 + 7)) + 8 * (3 * Nr * Nr + Npc * Npc + 4 * m * m) + 4096
+    return F * (120 + 108 + 448) + L * (160 + 8 * (6 * 12 + 7)) + 8 * (3 * Nr * Nr + Npc * Npc + 4 * m * m) + 4096
 
 
 def test_two_solvers_stay_within_the_memory_budget(backend):
