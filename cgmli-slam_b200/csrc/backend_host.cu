@@ -1496,30 +1496,53 @@ static int marginalizeImpl(cgmli_solver* S, const int* victim_kf, int policy, bo
         if (mw.tdCol >= 0) mw.visTd = addVis(mw.tdCol, 1);
         mw.nv = (int)P.visCols.size();
         mw.rowsPath = mw.nv <= kRowsMaxN;
-        // eliminated landmarks: local column blocks in order of first use
+        // eliminated landmarks: local column blocks in order of first use; a block is
+        // known by its first column, stamped with the landmark that last used it.  The
+        // anchor's pose and extrinsic and td are first met in a landmark's first
+        // observation, so later observations look up only the observer's blocks.
         int obsCount = 0;
+        std::vector<int> stamp(n, -1), local(n, 0);
+        long long nob = 0, colBound = 0;
         for (int g : elimLm) {
-            MargElim me{g, w, 0, (int)P.cols.size(), obsCount};
-            int blkStart[4 * kMaxTrackChunk + 1], blkLocal[4 * kMaxTrackChunk + 1], nblk = 0;
+            const int k = hb.lmObsBegin[g + 1] - hb.lmObsBegin[g];
+            nob += k;
+            colBound += 13 + 12ll * k;
+        }
+        P.obsMap.resize(5 * nob);
+        P.cols.resize(colBound);
+        P.elims.reserve(elimLm.size());
+        int* om = P.obsMap.data();
+        int* cp = P.cols.data();
+        for (int g : elimLm) {
+            MargElim me{g, w, 0, (int)(cp - P.cols.data()), obsCount};
             auto localOf = [&](int start, int size) {
                 if (start < 0) return -1;
-                for (int i = 0; i < nblk; ++i)
-                    if (blkStart[i] == start) return blkLocal[i];
-                blkStart[nblk] = start;
-                blkLocal[nblk] = me.nc;
-                ++nblk;
-                for (int c = 0; c < size; ++c) P.cols.push_back(start + c);
+                if (stamp[start] == g) return local[start];
+                stamp[start] = g;
+                local[start] = me.nc;
+                for (int c = 0; c < size; ++c) *cp++ = start + c;
                 me.nc += size;
                 return me.nc - size;
             };
             const int a = hb.lmKf[g], ea = hb.camExt[hb.lmCam[g]];
-            for (int f = hb.lmObsBegin[g]; f < hb.lmObsBegin[g + 1]; ++f) {
+            const int f0 = hb.lmObsBegin[g], f1 = hb.lmObsBegin[g + 1];
+            int la = -1, lea = -1, ltd = -1;
+            for (int f = f0; f < f1; ++f) {
                 const int b = hb.obKf[f], eb = hb.camExt[hb.obCam[f]];
-                P.obsMap.push_back(localOf(poseCol[a], 6));
-                P.obsMap.push_back(localOf(poseCol[b], 6));
-                P.obsMap.push_back(localOf(extCol[ea], 6));
-                P.obsMap.push_back(localOf(extCol[eb], 6));
-                P.obsMap.push_back(mw.tdCol >= 0 ? localOf(mw.tdCol, 1) : -1);
+                if (f == f0) {
+                    la = localOf(poseCol[a], 6);
+                    om[1] = localOf(poseCol[b], 6);
+                    lea = localOf(extCol[ea], 6);
+                    om[3] = localOf(extCol[eb], 6);
+                    ltd = localOf(mw.tdCol, 1);
+                } else {
+                    om[1] = localOf(poseCol[b], 6);
+                    om[3] = localOf(extCol[eb], 6);
+                }
+                om[0] = la;
+                om[2] = lea;
+                om[4] = ltd;
+                om += 5;
                 ++obsCount;
             }
             if (me.nc > kMargMaxNc) {
@@ -1530,6 +1553,7 @@ static int marginalizeImpl(cgmli_solver* S, const int* victim_kf, int policy, bo
             P.maxNc = std::max(P.maxNc, me.nc);
             P.elims.push_back(me);
         }
+        P.cols.resize(cp - P.cols.data());
         // dense-row chunks: 2 rows per observation and 1 per landmark, at most
         // 96 (72 above 192 visual columns)
         if (mw.rowsPath && !P.elims.empty()) {
