@@ -136,6 +136,7 @@ def declare_backend(lib: C.CDLL) -> C.CDLL:
     _proto(lib, "cgmli_default_options", None, [C.POINTER(SolverOptions)])
     _proto(lib, "cgmli_topology_check", C.c_int, [W, C.c_int, C.c_int, c_double_p])
     _proto(lib, "cgmli_topology_check_tuned", C.c_int, [W, C.c_int, C.c_int, C.POINTER(Tuning), c_double_p])
+    _proto(lib, "cgmli_topology_digest", C.c_int, [W, C.c_int, C.c_int, C.POINTER(Tuning), C.POINTER(C.c_ulonglong)])
     _proto(lib, "cgmli_solver_create", C.c_int, [C.c_int, C.POINTER(SolverOptions), C.POINTER(C.c_void_p)])
     _proto(lib, "cgmli_solver_destroy", None, [S])
     _proto(lib, "cgmli_solver_set_windows", C.c_int, [S, W, C.c_int])
@@ -223,7 +224,7 @@ BACKEND_SYMBOLS = [
     "cgmli_server_read_prior", "cgmli_server_release", "cgmli_server_replay", "cgmli_server_read_gate", "cgmli_imu_preintegrate",
     "cgmli_imu_last_timing", "cgmli_solver_set_imu_samples", "cgmli_solver_refresh_imu", "cgmli_solver_read_imu",
     "cgmli_solver_solve_gated", "cgmli_solver_read_gate", "cgmli_solver_set_imu_merge_limits", "cgmli_solver_read_merged_imu",
-    "cgmli_solver_calibration_information", "cgmli_solver_read_calibration_information", "cgmli_topology_check_tuned",
+    "cgmli_solver_calibration_information", "cgmli_solver_read_calibration_information", "cgmli_topology_check_tuned", "cgmli_topology_digest",
     "cgmli_solver_set_tuning", "cgmli_solver_get_tuning", "cgmli_solver_autotune",
     "cgmli_solver_device_bytes", "cgmli_server_device_bytes", "cgmli_solver_evaluate", "cgmli_solver_read_factors",
     "cgmli_solver_solve_host", "cgmli_server_submit_request", "cgmli_server_read_imu", "cgmli_server_read_calibration_information",

@@ -391,6 +391,34 @@ int cgmli_topology_check_tuned(const cgmli_window* windows, int count, int threa
     return CGMLI_OK;
 }
 
+int cgmli_topology_digest(const cgmli_window* windows, int count, int threads, const cgmli_tuning* tuning,
+                          unsigned long long* digest) {
+    if (!windows || count < 1 || !digest) return fail(CGMLI_E_INVALID, "empty window list or null digest");
+    PlanParams plan;
+    if (planOf(tuning, plan) != CGMLI_OK) return CGMLI_E_INVALID;
+    HostBatch hb;
+    std::string why;
+    const int st = buildHostBatch(windows, count, threads, hb, why, nullptr, plan);
+    if (st != CGMLI_OK) return fail(st, why);
+    unsigned long long h = 1469598103934665603ull;
+    auto mix = [&](const auto& v) {
+        const unsigned char* b = reinterpret_cast<const unsigned char*>(v.data());
+        for (size_t i = 0; i < v.size() * sizeof(v[0]); ++i) {
+            h ^= b[i];
+            h *= 1099511628211ull;
+        }
+    };
+    mix(hb.runs); mix(hb.tiles); mix(hb.pairChunks); mix(hb.schurChunks); mix(hb.schurCols); mix(hb.lmUmap);
+    mix(hb.lmPerm); mix(hb.camR); mix(hb.camT); mix(hb.camExt); mix(hb.lmWin); mix(hb.lmKf); mix(hb.lmCam); mix(hb.lmObsBegin);
+    mix(hb.lmNs); mix(hb.lmNx); mix(hb.lmSupp0); mix(hb.supp); mix(hb.lmC0); mix(hb.lmBearing); mix(hb.lmVel); mix(hb.lmTime);
+    mix(hb.obKf); mix(hb.obCam); mix(hb.obSlot); mix(hb.obXslot); mix(hb.obLm); mix(hb.keyOrder); mix(hb.obOrig);
+    mix(hb.obBearing); mix(hb.obP); mix(hb.obVel); mix(hb.obTime); mix(hb.pose); mix(hb.sb); mix(hb.ext); mix(hb.td);
+    mix(hb.rho); mix(hb.colChart); mix(hb.lmFixed); mix(hb.imu); mix(hb.imuKf); mix(hb.priorKind); mix(hb.priorIndex);
+    mix(hb.priorCol); mix(hb.priorOff); mix(hb.priorA); mix(hb.priorR0); mix(hb.priorRef);
+    *digest = h;
+    return CGMLI_OK;
+}
+
 void cgmli_default_options(cgmli_solver_options* o) {
     o->precision = CGMLI_PRECISION_FP64;
     o->refinement_steps = 0;

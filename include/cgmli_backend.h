@@ -195,6 +195,13 @@ typedef struct cgmli_tuning {
 /* cgmli_topology_check with a given work decomposition (NULL: the default). */
 int cgmli_topology_check_tuned(const cgmli_window *windows, int count, int threads, const cgmli_tuning *tuning,
                                double *seconds);
+/* 64-bit FNV-1a digest of the device layout the host builds for the batch (every
+ * index, work-unit and staged array, in upload order), built on up to `threads`
+ * host threads without touching a CUDA device.  The layout does not depend on the
+ * thread count: the digest is the same for any `threads`.  A diagnostic with no
+ * counterpart in the reference. */
+int cgmli_topology_digest(const cgmli_window *windows, int count, int threads, const cgmli_tuning *tuning,
+                          unsigned long long *digest);
 
 /* Replaces VisualCudaWorkspace construction (src/backend/BackendOptimizer.cpp:334-341). */
 int cgmli_solver_create(int device, const cgmli_solver_options *options, cgmli_solver **out);

@@ -94,3 +94,34 @@ def test_tuning_outside_its_ranges_is_rejected(lib, tuning):
     arr = synth.window_array(windows)
     t = abi.Tuning(*tuning, 0.0)
     assert lib.cgmli_topology_check_tuned(arr, len(arr), 0, C.byref(t), None) == abi.E_INVALID
+
+
+def _digest(lib, windows, threads, tuning=None):
+    arr = synth.window_array(windows)
+    out = C.c_ulonglong()
+    code = lib.cgmli_topology_digest(arr, len(arr), threads, C.byref(tuning) if tuning else None, C.byref(out))
+    assert code == 0, lib.cgmli_last_error().decode()
+    return out.value
+
+
+def test_layout_is_the_same_for_any_thread_count(lib):
+    """A batch with a window of several thousand landmarks and few windows is built in
+    range steps split over the threads; a batch of many windows is built window by
+    window, largest first.  Either way the layout (the digest of every uploaded array)
+    does not depend on the thread count, and every such build keeps the invariants."""
+    big = [synth.SynthWindow(replace(synth.C3, keyframes=14, landmarks=3000), 4),
+           synth.SynthWindow(replace(synth.C1, landmarks=300), 5)]
+    many = synth.make_windows("c4", 20, seed=23)
+    for windows in (big, many):
+        digests = {_digest(lib, windows, t) for t in (1, 2, 3, 8)}
+        assert len(digests) == 1
+        for t in (1, 3):
+            code, _, why = check(lib, windows, t)
+            assert code == 0, why
+
+
+def test_layout_digest_sees_the_decomposition(lib):
+    windows = synth.make_windows("c4", 6, seed=29)
+    a = _digest(lib, windows, 2, abi.Tuning(8, 32, 128, 0, 0, 0.0))
+    b = _digest(lib, windows, 2, abi.Tuning(16, 32, 128, 0, 0, 0.0))
+    assert a != b
