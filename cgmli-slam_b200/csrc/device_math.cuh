@@ -249,14 +249,16 @@ __device__ inline bool evalBearingFactor(const FactorIn& in, bool derivatives, F
     const m3 Rca = ldm3(in.Rca), Rcb = ldm3(in.Rcb);
     const d3 tca = ld3(in.tca), tcb = ld3(in.tcb);
     const d3 local = mv(Rca, (1 / rho) * ba) + tca;
-    m3 Ra, Rb, W, cameraRotation;
+    // Ra and Rb are loaded again where the extrinsic derivatives need them, so that
+    // they are not held across the residual
+    m3 W, cameraRotation;
     d3 pc, bodyA, world, observerBody;
     if (same) {
         pc = mtv(Rcb, local - tcb);
         cameraRotation = mul(tr(Rcb), Rca);
     } else {
-        Ra = ldm3(in.Ra);
-        Rb = ldm3(in.Rb);
+        const m3 Ra = ldm3(in.Ra);
+        const m3 Rb = ldm3(in.Rb);
         const m3 Rea = ldm3(in.Rea), Reb = ldm3(in.Reb);
         const d3 tea = ld3(in.xea), teb = ld3(in.xeb);
         W = tr(mul(mul(Rb, Reb), Rcb));
@@ -290,9 +292,8 @@ __device__ inline bool evalBearingFactor(const FactorIn& in, bool derivatives, F
     double P[6];
 #pragma unroll
     for (int i = 0; i < 6; ++i) P[i] = in.meas[i];
-    m3 K = {{0, 0, 0, 0, 0, 0, 0, 0, 0}};
     if (movingMeasured) {
-        K = skew(cross(in.measured, bb));
+        const m3 K = skew(cross(in.measured, bb));
         const m3 transport = madd(madd(eye3(), K), mscl(1 / denominator, mul(K, K)));
         rowTimesM(in.meas, tr(transport), P);
     }
@@ -312,6 +313,23 @@ __device__ inline bool evalBearingFactor(const FactorIn& in, bool derivatives, F
         red[3 * r + 1] = (proj.y - pn * n.y) / range;
         red[3 * r + 2] = (proj.z - pn * n.z) / range;
     }
+    // the derivatives through the camera rotation first (depth, and the anchor-side
+    // term of the time offset), so that the rotation is not held further
+    const bool tdTerm = timeDerivative && (movingAnchor || movingMeasured);
+    double jt0 = 0, jt1 = 0;
+    {
+        double RC[6];
+        rowTimesM(red, cameraRotation, RC);
+        const d3 q = (-1 / (rho * rho)) * ba;
+        o.Jrho[0] = RC[0] * q.x + RC[1] * q.y + RC[2] * q.z;
+        o.Jrho[1] = RC[3] * q.x + RC[4] * q.y + RC[5] * q.z;
+        if (!isfinite(o.Jrho[0]) || !isfinite(o.Jrho[1])) return false;
+        if (tdTerm) {
+            const d3 qt = (1 / rho) * da;
+            jt0 = RC[0] * qt.x + RC[1] * qt.y + RC[2] * qt.z;
+            jt1 = RC[3] * qt.x + RC[4] * qt.y + RC[5] * qt.z;
+        }
+    }
 #pragma unroll
     for (int i = 0; i < 12; ++i) { o.Ja[i] = 0; o.Jb[i] = 0; o.Jea[i] = 0; o.Jeb[i] = 0; }
     if (!same) {
@@ -326,9 +344,9 @@ __device__ inline bool evalBearingFactor(const FactorIn& in, bool derivatives, F
         if (in.wantExt) {
             if (!unitPose(in.xea) || !unitPose(in.xeb)) return false;
             double DR[6];
-            rowTimesM(D, Ra, DR);
+            rowTimesM(D, ldm3(in.Ra), DR);
             poseBlock(DR, bodyA, 1.0, o.Jea);
-            rowTimesM(D, Rb, DR);
+            rowTimesM(D, ldm3(in.Rb), DR);
             poseBlock(DR, observerBody, -1.0, in.splitExt ? o.Jeb : o.Jb);  // temporarily in Jb when shared
             if (!in.splitExt) {
                 // shared extrinsic: sum both sides into Jea, restore the observer pose block
@@ -339,29 +357,22 @@ __device__ inline bool evalBearingFactor(const FactorIn& in, bool derivatives, F
             }
         }
     }
-    {
-        double RC[6];
-        rowTimesM(red, cameraRotation, RC);
-        const d3 q = (-1 / (rho * rho)) * ba;
-        o.Jrho[0] = RC[0] * q.x + RC[1] * q.y + RC[2] * q.z;
-        o.Jrho[1] = RC[3] * q.x + RC[4] * q.y + RC[5] * q.z;
-        if (!isfinite(o.Jrho[0]) || !isfinite(o.Jrho[1])) return false;
-    }
     o.Jtd[0] = o.Jtd[1] = 0;
-    if (timeDerivative && (movingAnchor || movingMeasured)) {
+    if (tdTerm) {
         const m3 Jb = madd(mscl(f, msub(mscl(-1, outer(bb, n)), mscl(c, eye3()))), mscl(g, outer(u, n)));
+        double PJ[6];
+        rowTimesM(P, Jb, PJ);
+        jt0 = jt0 + PJ[0] * db.x + PJ[1] * db.y + PJ[2] * db.z;
+        jt1 = jt1 + PJ[3] * db.x + PJ[4] * db.y + PJ[5] * db.z;
+        m3 K = {{0, 0, 0, 0, 0, 0, 0, 0, 0}};
+        if (movingMeasured) K = skew(cross(in.measured, bb));
         const m3 dK = skew(cross(in.measured, db));
         const m3 dR = msub(madd(dK, mscl(1 / denominator, madd(mul(dK, K), mul(K, dK)))),
                            mscl(dot(in.measured, db) / (denominator * denominator), mul(K, K)));
-        double RC[6], PJ[6], MdR[6];
-        rowTimesM(red, cameraRotation, RC);
-        rowTimesM(P, Jb, PJ);
+        double MdR[6];
         rowTimesM(in.meas, tr(dR), MdR);
-        const d3 q = (1 / rho) * da;
-#pragma unroll
-        for (int r = 0; r < 2; ++r)
-            o.Jtd[r] = RC[3 * r] * q.x + RC[3 * r + 1] * q.y + RC[3 * r + 2] * q.z + PJ[3 * r] * db.x + PJ[3 * r + 1] * db.y +
-                       PJ[3 * r + 2] * db.z + MdR[3 * r] * logarithm.x + MdR[3 * r + 1] * logarithm.y + MdR[3 * r + 2] * logarithm.z;
+        o.Jtd[0] = jt0 + MdR[0] * logarithm.x + MdR[1] * logarithm.y + MdR[2] * logarithm.z;
+        o.Jtd[1] = jt1 + MdR[3] * logarithm.x + MdR[4] * logarithm.y + MdR[5] * logarithm.z;
         if (!isfinite(o.Jtd[0]) || !isfinite(o.Jtd[1])) return false;
     }
     return true;
