@@ -249,10 +249,11 @@ __device__ inline bool evalBearingFactor(const FactorIn& in, bool derivatives, F
     const m3 Rca = ldm3(in.Rca), Rcb = ldm3(in.Rcb);
     const d3 tca = ld3(in.tca), tcb = ld3(in.tcb);
     const d3 local = mv(Rca, (1 / rho) * ba) + tca;
-    // Ra and Rb are loaded again where the extrinsic derivatives need them, so that
-    // they are not held across the residual
+    // Ra and Rb, and the points in the body frames that the pose derivatives need, are
+    // formed again where the derivatives are taken (the same operations on the same
+    // inputs, so the same values), so that they are not held across the residual
     m3 W, cameraRotation;
-    d3 pc, bodyA, world, observerBody;
+    d3 pc;
     if (same) {
         pc = mtv(Rcb, local - tcb);
         cameraRotation = mul(tr(Rcb), Rca);
@@ -263,19 +264,16 @@ __device__ inline bool evalBearingFactor(const FactorIn& in, bool derivatives, F
         const d3 tea = ld3(in.xea), teb = ld3(in.xeb);
         W = tr(mul(mul(Rb, Reb), Rcb));
         cameraRotation = mul(W, mul(mul(Ra, Rea), Rca));
-        bodyA = mv(Rea, local) + tea;
-        const d3 separation = ld3(in.xa) - ld3(in.xb);
         if (!in.splitExt) {
+            const d3 separation = ld3(in.xa) - ld3(in.xb);
             const d3 offset = mv(W, (mv(Ra, mv(Rea, tca) + tea) - mv(Rb, mv(Reb, tcb) + teb)) + separation);
             pc = mv(cameraRotation, (1 / rho) * ba) + offset;
         } else {
+            const d3 bodyA = mv(Rea, local) + tea;
             const d3 wpt = mv(Ra, bodyA) + ld3(in.xa);
             const d3 ob = mtv(Rb, wpt - ld3(in.xb));
             pc = mtv(Rcb, mtv(Reb, ob - teb) - tcb);
         }
-        const d3 rotated = mv(Ra, bodyA);
-        world = rotated + ld3(in.xa);
-        observerBody = mtv(Rb, rotated + separation);
     }
     const double range = norm(pc);
     if (!finite3(pc) || !isfinite(range) || range < 1e-10) return false;
@@ -337,6 +335,10 @@ __device__ inline bool evalBearingFactor(const FactorIn& in, bool derivatives, F
         if (!unitPose(in.xa) || !unitPose(in.xb)) return false;
         double D[6];
         rowTimesM(red, W, D);
+        const d3 bodyA = mv(ldm3(in.Rea), mv(ldm3(in.Rca), (1 / rho) * ba) + ld3(in.tca)) + ld3(in.xea);
+        const d3 rotated = mv(ldm3(in.Ra), bodyA);
+        const d3 world = rotated + ld3(in.xa);
+        const d3 observerBody = mtv(ldm3(in.Rb), rotated + (ld3(in.xa) - ld3(in.xb)));
         if (!in.sameKf) {
             poseBlock(D, world, 1.0, o.Ja);
             poseBlock(D, world, -1.0, o.Jb);
