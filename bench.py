@@ -94,11 +94,11 @@ def dist_env():
 # linearization of the first 64 windows of the batch (451,950 observations) in an ncu
 # capture (profiles/lin_traffic_c4x64.md).  Mostly the staged weighted rows (224 bytes
 # mixed, 448 FP64) written by the landmark pass and read back in key order.
-LIN_DRAM_BYTES_PER_OBS = {"mixed": 990.6, "fp64": 1536.0}
+LIN_DRAM_BYTES_PER_OBS = {"mixed": 910.3, "fp64": 1536.0}
 # the landmark pass's limiter (profiles/lin_landmark_mixed_c4x64.md): FP64 pipe and
 # issue fractions of the single-kernel capture
-LIN_LANDMARK_PROFILE = {"fp64_pipe_pct": 11.0, "issue_active_pct": 21.1, "dram_throughput_pct": 5.6, "warps_active_pct": 13.4,
-                        "registers": 168, "top_stall": "long scoreboard (4.7 per issue)"}
+LIN_LANDMARK_PROFILE = {"fp64_pipe_pct": 11.6, "issue_active_pct": 22.0, "dram_throughput_pct": 5.1, "warps_active_pct": 13.5,
+                        "registers": 168, "top_stall": "long scoreboard (4.4 per issue)"}
 
 
 def rank_seed(seed: int, rank: int) -> int:
