@@ -168,6 +168,7 @@ def declare_backend(lib: C.CDLL) -> C.CDLL:
     _proto(lib, "cgmli_server_submit", C.c_int, [V, W, C.c_int, ll_p])
     _proto(lib, "cgmli_server_submit_request", C.c_int, [V, C.POINTER(ServerRequest), ll_p])
     _proto(lib, "cgmli_server_read_imu", C.c_int, [V, C.c_longlong, C.POINTER(FrozenImu), c_int_p])
+    _proto(lib, "cgmli_server_read_merged_imu", C.c_int, [V, C.c_longlong, c_int_p, C.POINTER(FrozenImu)])
     _proto(lib, "cgmli_server_read_calibration_information", C.c_int,
            [V, C.c_longlong, c_int_p, c_int_p, c_int_p, c_int_p, c_double_p, c_double_p])
     _proto(lib, "cgmli_server_poll", C.c_int, [V, C.c_longlong, C.c_int, C.POINTER(SolveReport), c_double_p])
@@ -227,7 +228,7 @@ BACKEND_SYMBOLS = [
     "cgmli_solver_calibration_information", "cgmli_solver_read_calibration_information", "cgmli_topology_check_tuned", "cgmli_topology_digest",
     "cgmli_solver_set_tuning", "cgmli_solver_get_tuning", "cgmli_solver_autotune",
     "cgmli_solver_device_bytes", "cgmli_server_device_bytes", "cgmli_solver_evaluate", "cgmli_solver_read_factors",
-    "cgmli_solver_solve_host", "cgmli_server_submit_request", "cgmli_server_read_imu", "cgmli_server_read_calibration_information",
+    "cgmli_solver_solve_host", "cgmli_server_submit_request", "cgmli_server_read_imu", "cgmli_server_read_merged_imu", "cgmli_server_read_calibration_information",
 ]
 KERNEL_NAMES = ["zero_acc", "linearize", "retained", "factor", "candidate", "backsub_trial", "retained_trial", "lm_update", "accept",
                 "lin_pairs", "lin_schur"]

@@ -444,6 +444,14 @@ class Server:
         _check(lib().cgmli_server_read_imu(self._h, ticket, out, C.byref(n)), "cgmli_server_read_imu")
         return list(out)[:count], n.value
 
+    def read_merged_imu(self, ticket: int):
+        """(outcome CGMLI_IMU_MERGE_*, merged factor or None) of a request marginalized
+        with the IMU merge."""
+        state = C.c_int()
+        f = abi.FrozenImu()
+        _check(lib().cgmli_server_read_merged_imu(self._h, ticket, C.byref(state), C.byref(f)), "cgmli_server_read_merged_imu")
+        return state.value, (f if state.value == abi.IMU_MERGE_REINTEGRATED else None)
+
     def read_calibration_information(self, ticket: int) -> dict:
         size, nb = C.c_int(), C.c_int()
         code = lib().cgmli_server_read_calibration_information(self._h, ticket, C.byref(size), C.byref(nb), None, None, None, None)

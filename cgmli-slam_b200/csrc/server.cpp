@@ -53,6 +53,10 @@ struct Request {
     int imuRefreshed = 0;
     // calibration information at the solved states (extra.calibration_information)
     int calibStatus = CGMLI_E_INVALID, calibSize = 0, calibBlocks = 0;
+    // CGMLI_MARGIN_SECOND_NEW_IMU_MERGE: the merge's outcome and, when re-integrated,
+    // the merged factor (mergeStatus: the read's code when it failed)
+    int mergeState = CGMLI_IMU_MERGE_NONE, mergeStatus = CGMLI_OK;
+    cgmli_frozen_imu merged{};
     std::vector<int> calibKind, calibIndex;
     std::vector<double> calibConditional, calibEvals;
 };
@@ -223,6 +227,8 @@ struct cgmli_server {
                 const int gs = cgmli_solver_read_gate(S, i, &r->gate, r->rejected.data());
                 if (gs != CGMLI_OK && r->report.status == CGMLI_OK) r->report.status = gs;
             }
+            if (r->victim >= 0 && r->report.status == CGMLI_OK && opt.policy == CGMLI_MARGIN_SECOND_NEW_IMU_MERGE)
+                r->mergeStatus = cgmli_solver_read_merged_imu(S, i, &r->mergeState, &r->merged);
             if (r->victim >= 0 && r->report.status == CGMLI_OK) {
                 int rank = 0, cols = 0, nb = 0;
                 int ps = cgmli_solver_read_prior(S, i, &rank, &cols, &nb, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
@@ -343,7 +349,8 @@ int cgmli_server_create(const cgmli_server_options* options, cgmli_server** out)
     if (!options || !out) return setLastError(CGMLI_E_INVALID, "server: null options or output handle");
     *out = nullptr;
     if (options->iterations < 1) return setLastError(CGMLI_E_INVALID, "server: iterations < 1");
-    if (options->policy != CGMLI_MARGIN_OLD && options->policy != CGMLI_MARGIN_SECOND_NEW)
+    if (options->policy != CGMLI_MARGIN_OLD && options->policy != CGMLI_MARGIN_SECOND_NEW &&
+        options->policy != CGMLI_MARGIN_SECOND_NEW_IMU_MERGE)
         return setLastError(CGMLI_E_INVALID, "server: unknown marginalization policy");
     if (!(options->nis_threshold >= 0) || options->max_refits < 0 || options->max_refits > 64)
         return setLastError(CGMLI_E_INVALID, "server: nis_threshold < 0 or max_refits outside 0..64");
@@ -573,6 +580,22 @@ int cgmli_server_read_imu(cgmli_server* s, long long ticket, cgmli_frozen_imu* i
                                                                       "server: the request's IMU factors were not read back");
     std::copy(r.imu.begin(), r.imu.end(), imu);
     if (refreshed) *refreshed = r.imuRefreshed;
+    return CGMLI_OK;
+}
+
+int cgmli_server_read_merged_imu(cgmli_server* s, long long ticket, int* state, cgmli_frozen_imu* imu) {
+    if (!s || !state) return setLastError(CGMLI_E_INVALID, "server: null server or state output");
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->requests.find(ticket);
+    if (it == s->requests.end()) return setLastError(CGMLI_E_INVALID, "server: unknown ticket");
+    const Request& r = *it->second;
+    if (!r.complete) return setLastError(CGMLI_E_PENDING, "server: request not complete");
+    if (s->opt.policy != CGMLI_MARGIN_SECOND_NEW_IMU_MERGE || r.victim < 0)
+        return setLastError(CGMLI_E_INVALID, "server: the request had no IMU-merge marginalization");
+    if (r.report.status != CGMLI_OK) return setLastError(r.report.status, "server: request failed");
+    if (r.mergeStatus != CGMLI_OK) return setLastError(r.mergeStatus, "server: the merged factor could not be read");
+    *state = r.mergeState;
+    if (imu && r.mergeState == CGMLI_IMU_MERGE_REINTEGRATED) *imu = r.merged;
     return CGMLI_OK;
 }
 

@@ -520,7 +520,9 @@ typedef struct cgmli_server_options {
     long long memory_budget_bytes;  /* 0: 40 GiB; device bytes of both solvers together (see
                                        cgmli_server_device_bytes) */
     int iterations;                 /* LM iterations per request, >= 1 */
-    int policy;                     /* CGMLI_MARGIN_OLD or _SECOND_NEW for requests with a victim */
+    int policy;                     /* CGMLI_MARGIN_OLD, _SECOND_NEW or _SECOND_NEW_IMU_MERGE for requests
+                                       with a victim (the merge needs the request's IMU samples; default
+                                       limits of cgmli_solver_set_imu_merge_limits) */
     double nis_threshold;           /* > 0: solve with the NIS gate and outlier refits
                                        (cgmli_solver_solve_gated); 0: plain solve */
     int max_refits;                 /* refits of the gated solve (reference: 3) */
@@ -573,6 +575,11 @@ int cgmli_server_read_imu(cgmli_server *server, long long ticket, cgmli_frozen_i
  * the calibration call's status when it failed for this window. */
 int cgmli_server_read_calibration_information(cgmli_server *server, long long ticket, int *size, int *num_blocks, int *block_kind,
                                               int *block_index, double *conditional, double *eigenvalues);
+/* Outcome of a completed request's IMU merge (server policy
+ * CGMLI_MARGIN_SECOND_NEW_IMU_MERGE, request with a victim), as
+ * cgmli_solver_read_merged_imu: *state is CGMLI_IMU_MERGE_*, and imu (may be NULL)
+ * receives the merged factor when it was re-integrated. */
+int cgmli_server_read_merged_imu(cgmli_server *server, long long ticket, int *state, cgmli_frozen_imu *imu);
 /* Prior of a completed request with a victim, laid out as cgmli_solver_read_prior
  * (sizes first with NULL buffers). */
 int cgmli_server_read_prior(cgmli_server *server, long long ticket, int *rank, int *cols, int *num_blocks, int *block_kind,

@@ -224,3 +224,41 @@ def test_served_calibration_information_equals_the_solver(backend):
     A, Ar = prior["A"], ref_prior["A"]
     assert prior["rank"] == ref_prior["rank"] and rel(A.T @ A, Ar.T @ Ar) < 1e-8
     srv.close()
+
+
+def test_served_imu_merge_equals_the_solver(backend):
+    """A server with the IMU-merge policy: a request with IMU samples and the
+    second-newest keyframe as victim gets the same merged factor and the same prior
+    as the solver given the same samples (refresh, solve, merge); a request without
+    samples in the same server keeps the Schur bridge."""
+    w1, prm, args = _imu_window(backend, 65)
+    w2, _, _ = _imu_window(backend, 65)
+    plain, _, _ = _imu_window(backend, 67)
+    v = w1.K - 2
+    s = backend.Solver()
+    s.set_windows([w1])
+    s.set_imu_samples(prm, *args)
+    s.refresh_imu()
+    s.solve(2)
+    s.marginalize([v], abi.MARGIN_SECOND_NEW_IMU_MERGE)
+    ref_prior = s.read_prior(0)
+    ref_state, ref_f = s.read_merged_imu(0)
+    s.close()
+    assert ref_state == abi.IMU_MERGE_REINTEGRATED
+    srv = backend.Server(iterations=2, imu_params=prm, policy=abi.MARGIN_SECOND_NEW_IMU_MERGE)
+    t1 = srv.submit_request(w2, v, imu=args)
+    t2 = srv.submit_request(plain, plain.K - 2)
+    rep1, _ = srv.poll(t1)
+    rep2, _ = srv.poll(t2)
+    assert rep1.status == 0 and rep2.status == 0
+    state, f = srv.read_merged_imu(t1)
+    assert state == abi.IMU_MERGE_REINTEGRATED
+    for name in ("delta_quaternion", "delta_velocity", "delta_position", "rotation_gyro", "velocity_gyro", "position_gyro",
+                 "velocity_accel", "position_accel", "gyros", "reference_bias"):
+        assert rel(getattr(f, name), getattr(ref_f, name)) < 1e-7, name  # the solved bias it is taken at: 1e-8 drift
+    got = srv.read_prior(t1)
+    A, Ar = got["A"], ref_prior["A"]
+    assert got["rank"] == ref_prior["rank"] and got["cols"] == ref_prior["cols"]
+    assert rel(A.T @ A, Ar.T @ Ar) < 1e-7
+    assert srv.read_merged_imu(t2)[0] == abi.IMU_MERGE_BRIDGE
+    srv.close()
