@@ -114,6 +114,9 @@ struct DevBatch {
     const int* wideList;
     double* facVec;
     int* facFailed;
+    // per wide window (at its wideList position times (ceil(wideCols / 32) + 1) wideCols):
+    // the row parts of the undamped product by 32-column block, then its column parts
+    double* wideProd;
     double* out;     // per-window scratch for read-back (costs)
 };
 

@@ -1053,7 +1053,7 @@ __device__ __forceinline__ void trailingTile(const double* V, long long ldv, int
 // h (scratch), blk and dmp are the CTA's shared vectors.
 template <bool kBlocks>
 __device__ void factorTail(const DevBatch& B, const WinDesc& wd, int wdx, double lambda, int refinement, const double* A, double* x,
-                           const double* hd, double* h, double* blk, const double* dmp, double* red) {
+                           const double* hd, double* h, double* blk, const double* dmp, double* red, bool solveOnly = false) {
     auto product = [&](const double* v, double* out) {
         if constexpr (kBlocks) undampedProductBlocks(A, hd, wd.Nr, v, out);
         else undampedProduct(A, hd, wd.Nr, v, out);
@@ -1139,6 +1139,7 @@ __device__ void factorTail(const DevBatch& B, const WinDesc& wd, int wdx, double
     double* dr = B.dr + wd.vec0;
     for (int i = tid; i < n; i += blockDim.x) dr[i] = x[i];
     __syncthreads();
+    if (solveOnly) return;  // the product and the prediction follow in other kernels
     // ---- iterative refinement against the assembled FP64 system
     for (int it = 0; it < refinement; ++it) {
         if (charts) {
@@ -1310,6 +1311,11 @@ __global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int re
 // The backward substitution, the refinement steps and the prediction follow in one
 // CTA (k_wide_finish, the tail k_factor uses).  Per-window vectors between the
 // kernels: B.facVec + 3 vec0 holds x (n), the undamped diagonal (n) and the damping (n).
+// A wide window without solve-time charts or refinement steps finishes in three
+// kernels (k_wide_finish's solve, k_wide_product, k_wide_predict); otherwise
+// k_wide_finish runs the whole tail in one CTA.
+__device__ __forceinline__ bool wideSplitTail(const WinDesc& wd, int refinement) { return refinement == 0 && wd.charts == 0; }
+
 __global__ void __launch_bounds__(256) k_wide_assemble(DevBatch B) {
     const int wdx = B.wideList[blockIdx.x];
     if (B.lm[wdx].mode == kModeDone) return;
@@ -1545,7 +1551,82 @@ __global__ void __launch_bounds__(kFactorThreads) k_wide_finish(DevBatch B, int 
 #pragma unroll 4
     for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) x[i] = src[i];
     __syncthreads();
-    factorTail<true>(B, wd, wdx, B.lm[wdx].lambda, refinement, B.Sglob + wd.dense0, x, hd, h, blk, dmp, red);
+    factorTail<true>(B, wd, wdx, B.lm[wdx].lambda, refinement, B.Sglob + wd.dense0, x, hd, h, blk, dmp, red,
+                     wideSplitTail(wd, refinement));
+}
+
+// Without charts or refinement steps, the undamped product h = S dr of the
+// prediction is spread over the GPU: one CTA per 32-column block of the stored upper
+// triangle (A[i + j n], i < j) forms each row's part over the block's columns (rows
+// above them, lanes over rows, a coalesced load per column) and the block's column
+// sums (folded across the warp and then across the warps in a fixed order); the
+// prediction kernel adds them in block order.  h_i = hd_i dr_i + sum over blocks of
+// the row parts + the column part of i's own block.
+__global__ void __launch_bounds__(kFactorThreads) k_wide_product(DevBatch B, int refinement, int wideCols) {
+    const int wdx = B.wideList[blockIdx.x];
+    if (B.lm[wdx].mode == kModeDone || B.facFailed[wdx]) return;
+    const WinDesc wd = B.win[wdx];
+    const int n = wd.Nr, j0 = 32 * blockIdx.y;
+    if (!wideSplitTail(wd, refinement) || j0 >= n) return;
+    const int nbMax = (wideCols + 31) / 32, jw = min(32, n - j0);
+    double* rowPart = B.wideProd + (size_t)blockIdx.x * (nbMax + 1) * wideCols + (size_t)blockIdx.y * wideCols;
+    double* colPart = B.wideProd + (size_t)blockIdx.x * (nbMax + 1) * wideCols + (size_t)nbMax * wideCols;
+    const double* A = B.Sglob + wd.dense0;
+    const double* v = B.dr + wd.vec0;
+    constexpr int kWarps = kFactorThreads / 32;
+    __shared__ double part[kWarps * 32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double acc[32];
+#pragma unroll
+    for (int c = 0; c < 32; ++c) acc[c] = 0.0;
+    for (int i0 = warp * 32; i0 < j0 + jw; i0 += kWarps * 32) {
+        const int i = i0 + lane;
+        const double vi = i < n ? v[i] : 0.0;
+        double row = 0;
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+            if (c < jw && i < j0 + c) {  // strict upper: row i, column j0 + c
+                const double a = A[i + (long long)(j0 + c) * n];
+                acc[c] += a * vi;
+                row += a * v[j0 + c];
+            }
+        }
+        if (i < j0 + jw) rowPart[i] = row;
+    }
+    part[warp * 32 + lane] = transposeSum(acc);
+    __syncthreads();
+    if (threadIdx.x < jw) {
+        double t = 0;
+        for (int w = 0; w < kWarps; ++w) t += part[w * 32 + threadIdx.x];
+        colPart[j0 + threadIdx.x] = t;
+    }
+}
+
+// The prediction of a split tail: -dx^T (g + 0.5 h) with h summed from the parts.
+__global__ void __launch_bounds__(kFactorThreads) k_wide_predict(DevBatch B, int refinement, int wideCols) {
+    const int wdx = B.wideList[blockIdx.x];
+    if (B.lm[wdx].mode == kModeDone || B.facFailed[wdx]) return;
+    const WinDesc wd = B.win[wdx];
+    if (!wideSplitTail(wd, refinement)) return;
+    const int n = wd.Nr, K = wd.K, Npc = wd.Npc, nbMax = (wideCols + 31) / 32, nb = (n + 31) / 32;
+    const double* prod = B.wideProd + (size_t)blockIdx.x * (nbMax + 1) * wideCols;
+    const double* hd = B.facVec + 3ll * wd.vec0 + n;
+    const double* dr = B.dr + wd.vec0;
+    const double* acc = B.acc + wd.acc0;
+    const long long nS = (long long)Npc * (Npc + 1) / 2;
+    __shared__ double red[32];
+    double pred = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double h = hd[i] * dr[i];
+        for (int b = i / 32; b < nb; ++b) h += prod[(size_t)b * wideCols + i];
+        h += prod[(size_t)nbMax * wideCols + i];
+        double g = B.gret[wd.vec0 + i];
+        const int p = pcOfRetained(i, K);
+        if (p >= 0) g += acc[nS + Npc + p];
+        pred += -dr[i] * (g + 0.5 * h);
+    }
+    pred = blockSum(pred, red);
+    if (threadIdx.x == 0) { B.predState[wdx] = pred; B.solveStatus[wdx] = CGMLI_OK; }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -2146,6 +2227,11 @@ int launchIterationParts(const DevBatch& B, const LaunchPlan& P, int refinement,
             run(CGMLI_KERNEL_FACTOR, [&] { k_wide_trailing<<<grid, kFactorThreads, 0, s>>>(B, k0); });
         }
         run(CGMLI_KERNEL_FACTOR, [&] { k_wide_finish<<<P.numWide, kFactorThreads, P.wideFinishSmem, s>>>(B, refinement); });
+        if (refinement == 0) {  // windows without charts: the product over the GPU, then the prediction
+            const dim3 blocks(P.numWide, (P.wideCols + 31) / 32);
+            run(CGMLI_KERNEL_FACTOR, [&] { k_wide_product<<<blocks, kFactorThreads, 0, s>>>(B, refinement, P.wideCols); });
+            run(CGMLI_KERNEL_FACTOR, [&] { k_wide_predict<<<P.numWide, kFactorThreads, 0, s>>>(B, refinement, P.wideCols); });
+        }
     }
     run(CGMLI_KERNEL_CANDIDATE, [&] { k_candidate<<<W, 128, 0, s>>>(B); });
     if (B.numLandmarks > 0) {
