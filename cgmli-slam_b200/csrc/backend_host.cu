@@ -135,7 +135,7 @@ struct cgmli_solver {
     size_t wideFinishSmem = 0;
     HVec<int> hWideList;
     DArray<int> wideList, facFailed;
-    DArray<double> facVec, wideProd;
+    DArray<double> facVec, wideProd, wideL21;
     int totalKf = 0, totalExt = 0, totalCam = 0, totalLm = 0, totalObs = 0, totalImu = 0;
     // device arrays
     DArray<WinDesc> dWin;
@@ -275,7 +275,7 @@ struct cgmli_solver {
         add(dMargWin, dMargElim, margCols, margObsMap, margPoseCol, margSbCol, margExtCol, margRank, margStatus, margFast, margVisCol,
             margVisPose, margVisExt, margSlow, margChunks, margItems, margH, margB, margSepH, margSepV, margSepB, margEvals, margA,
             margR0, margX, margMaxD, margStats, dMargOrder);
-        add(colChart, lmFixed, evalOut, evalValid, hostH, hostG, hostCost, hostFlag, wideList, facFailed, facVec, wideProd);
+        add(colChart, lmFixed, evalOut, evalValid, hostH, hostG, hostCost, hostFlag, wideList, facFailed, facVec, wideProd, wideL21);
         add(obRejected, gateCounts, gateStats, imuTimes, imuT0, imuT1, imuReadings, imuRanges, imuStatus, imuRefreshed,
             imuRefreshScratch, mergeRange, mergeKf, mergeStatus, mergeFlag, mergeT0, mergeT1, mergeOut, calibWork0, calibWork, calibCond,
             calibEvals, snapPose, snapSb, snapExt, snapTd, snapRho);
@@ -321,7 +321,7 @@ struct cgmli_solver {
         lmC0.release(); dWin.release(); dLm.release(); dRuns.release(); dTiles.release();
         dPairChunks.release(); dSchurChunks.release(); schurCols.release(); lmUmap.release(); obLm.release(); keyOrder.release(); bigFirst.release(); keyRows.release(); sch.release();
         snapPose.release(); snapSb.release(); snapExt.release(); snapTd.release(); snapRho.release();
-        wideList.release(); facFailed.release(); facVec.release(); wideProd.release();
+        wideList.release(); facFailed.release(); facVec.release(); wideProd.release(); wideL21.release();
         imuTimes.release(); imuT0.release(); imuT1.release(); imuReadings.release(); imuRanges.release(); imuStatus.release();
         imuRefreshed.release(); imuRefreshScratch.release();
         obRejected.release(); gateCounts.release(); gateStats.release();
@@ -577,6 +577,7 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
         CK(S->facVec.reserve(3 * (size_t)hb.vec));
         CK(S->facFailed.reserve(count));
         CK(S->wideProd.reserve((size_t)S->numWide * ((S->wideCols + 31) / 32 + 1) * S->wideCols));
+        CK(S->wideL21.reserve((size_t)S->numWide * 2 * 32 * S->wideCols));
     }
     CK(S->acc.reserve(hb.acc)); CK(S->sch.reserve(hb.sch)); CK(S->imuScratch.reserve(hb.imuScratch));
     CK(S->priorScratch.reserve(hb.priorScratch));
@@ -619,6 +620,7 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     B.facVec = S->numWide ? S->facVec.p : nullptr;
     B.facFailed = S->numWide ? S->facFailed.p : nullptr;
     B.wideProd = S->numWide ? S->wideProd.p : nullptr;
+    B.wideL21 = S->numWide ? S->wideL21.p : nullptr;
     {
         // the observation payload into device order (after every upload above on this stream)
         const double* const src[4] = {S->obSrcBearing.p, S->obSrcP.p, S->obSrcVel.p, S->obSrcTime.p};

@@ -117,6 +117,9 @@ struct DevBatch {
     // per wide window (at its wideList position times (ceil(wideCols / 32) + 1) wideCols):
     // the row parts of the undamped product by 32-column block, then its column parts
     double* wideProd;
+    // per wide window, two panel buffers (by panel parity) of 32 x wideCols: a panel's
+    // solved L21 (k-major) until it is stored into Sglob
+    double* wideL21;
     double* out;     // per-window scratch for read-back (costs)
 };
 

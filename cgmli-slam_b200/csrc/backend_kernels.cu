@@ -1297,20 +1297,18 @@ __global__ void __launch_bounds__(kFactorThreads, 2) k_factor(DevBatch B, int re
 // single large window) is factored by a launch sequence that spreads the work over
 // the GPU instead of one CTA (k_factor skips it).  The damped system is assembled
 // by column blocks (k_wide_assemble); the solve-time charts and the debug copy run
-// in one CTA (k_wide_prepare).  Then, per panel of kFacPanel columns:
-//   - its diagonal block is factored by one CTA, with the forward substitution
-//     of the right-hand side over the block
-//     (wideDiagBlock: right-looking over the CTA, one barrier per column);
-//   - the rows below it are solved against that block (L21 = A21 L11^-T), one
-//     thread per row with the row in registers, and each row's right-hand side
-//     entry takes its update y2 -= L21 y1 on the way (k_wide_trsm);
-//   - the trailing lower triangle A22 -= L21 L21^T is updated by one warp per
-//     32 x 32 tile on the FP64 tensor path, L21 read from the L2-resident slot;
-//     the CTA holding the first trailing tile, which is the next panel's
-//     diagonal block, factors it as soon as its tiles are written (k_wide_trailing).
-// The backward substitution, the refinement steps and the prediction follow in one
-// CTA (k_wide_finish, the tail k_factor uses).  Per-window vectors between the
-// kernels: B.facVec + 3 vec0 holds x (n), the undamped diagonal (n) and the damping (n).
+// in one CTA (k_wide_prepare).  The first diagonal block is factored by one CTA
+// (k_wide_diag; wideDiagBlock: right-looking over the CTA, one barrier per column,
+// the forward substitution of the right-hand side over the block on the way).  Then
+// one launch per panel of kFacPanel columns (k_wide_update): every warp owns a
+// 32 x 32 tile of the trailing update A22 -= L21 L21^T on the FP64 tensor path and
+// first solves the row blocks of L21 it needs against the panel's diagonal block
+// (one lane per row, the row in registers); the warps of the diagonal tiles keep
+// L21 in a panel buffer and apply y2 -= L21 y1; the first CTA holds tile (0, 0)
+// alone and factors the next diagonal block as soon as it is written.  The
+// backward substitution, the refinement steps and the prediction follow
+// (k_wide_finish, the tail k_factor uses).  Per-window vectors between the kernels:
+// B.facVec + 3 vec0 holds x (n), the undamped diagonal (n) and the damping (n).
 // A wide window without solve-time charts or refinement steps finishes in three
 // kernels (k_wide_finish's solve, k_wide_product, k_wide_predict); otherwise
 // k_wide_finish runs the whole tail in one CTA.
@@ -1424,114 +1422,132 @@ __global__ void __launch_bounds__(kFactorThreads) k_wide_diag(DevBatch B) {
     if (!wideDiagBlock(B, B.win[wdx], 0) && threadIdx.x == 0) B.facFailed[wdx] = 1;
 }
 
-// Rows below the panel at k0: L21 = A21 L11^-T by forward substitution, one thread
-// per row (the row's bw entries in registers), and y2 -= L21 y1 for the row.
-__global__ void __launch_bounds__(kFactorThreads) k_wide_trsm(DevBatch B, int k0) {
+// One panel's update in one launch: every warp owns a 32 x 32 tile (rb >= cb) of
+// A22 -= L21 L21^T and first solves the two row blocks of L21 it needs against the
+// panel's factored diagonal block (the same forward substitution as k_wide_trsm, one
+// lane per row, so the same values; a block is solved by every warp that needs it,
+// which keeps the row solves off the chain of launches).  A22 and the unsolved A21
+// are both read during the launch, so L21 goes to a per-panel buffer (two, by panel
+// parity) and reaches A in the next panel's launch or in k_wide_finish; the warp of
+// a diagonal tile writes its block there and updates the right-hand side y2 -= L21 y1
+// of its rows.  The first CTA holds tile (0, 0) alone and then factors the next
+// diagonal block.
+constexpr int kUpdStride = 2 * kFacPanel + 1;  // per warp: k-major rows of the two blocks (odd stride)
+size_t wideUpdateSmemBytes() {
+    return sizeof(double) * (kFacPanel * kDiagStride + 2 * kFacPanel + (size_t)(kFactorThreads / 32) * kFacPanel * kUpdStride);
+}
+__device__ __forceinline__ double* wideL21(const DevBatch& B, int slot, int panel, int wideCols) {
+    return B.wideL21 + ((size_t)slot * 2 + (panel & 1)) * kFacPanel * wideCols;
+}
+// The L21 block of panel `panel` (rows below it, k-major: row r - (k0 + 32) at entry
+// k * wideCols) into A's columns of that panel.
+__device__ void wideStoreL21(const DevBatch& B, const WinDesc& wd, int slot, int panel, int wideCols, int tid, int threads) {
+    const int n = wd.Nr, k0 = panel * kFacPanel, rows = n - k0 - kFacPanel;
+    const double* Ls = wideL21(B, slot, panel, wideCols);
+    double* A = B.Sglob + wd.dense0;
+    for (long long e = tid; e < (long long)rows * kFacPanel; e += threads) {
+        const int c = (int)(e / rows), r = (int)(e % rows);
+        A[(k0 + kFacPanel + r) + (long long)(k0 + c) * n] = Ls[(size_t)c * wideCols + r];
+    }
+}
+__global__ void __launch_bounds__(kFactorThreads) k_wide_update(DevBatch B, int k0, int wideCols) {
     const int wdx = B.wideList[blockIdx.x];
     if (B.lm[wdx].mode == kModeDone) return;
     const WinDesc wd = B.win[wdx];
-    const int n = wd.Nr;
-    if (k0 >= n || B.facFailed[wdx]) return;
-    const int bw = min(kFacPanel, n - k0), r0 = k0 + bw + blockIdx.y * blockDim.x;
-    if (r0 >= n) return;  // uniform over the CTA
-    __shared__ double L[kFacPanel * kDiagStride], y1[kFacPanel], inv[kFacPanel];
+    const int n = wd.Nr, panel = k0 / kFacPanel;
+    if (B.facFailed[wdx]) return;
+    if (panel > 0 && k0 < n)  // the previous panel's L21, spread over this launch's CTAs
+        wideStoreL21(B, wd, blockIdx.x, panel - 1, wideCols, blockIdx.y * blockDim.x + threadIdx.x, gridDim.y * blockDim.x);
+    if (k0 + kFacPanel >= n) return;  // uniform over the CTA
+    const int m2 = n - k0 - kFacPanel, nb2 = (m2 + 31) >> 5, tiles = nb2 * (nb2 + 1) / 2;
+    // the first CTA holds tile (0, 0) alone, so that the next diagonal block waits for
+    // that tile only; the other CTAs hold eight tiles each
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t = blockIdx.y == 0 ? (warp == 0 ? 0 : tiles) : 1 + (blockIdx.y - 1) * (kFactorThreads / 32) + warp;
+    if (blockIdx.y > 0 && 1 + (blockIdx.y - 1) * (kFactorThreads / 32) >= tiles) return;  // uniform over the CTA
+    extern __shared__ __align__(16) double usm[];
+    double* L = usm;                          // the diagonal block, row-major (stride kDiagStride)
+    double* inv = L + kFacPanel * kDiagStride;
+    double* y1 = inv + kFacPanel;
+    double* Vs = y1 + kFacPanel + (size_t)warp * kFacPanel * kUpdStride;
     double* A = B.Sglob + wd.dense0;
     double* x = B.facVec + 3ll * wd.vec0;
-    static_assert(kFacPanel * kFacPanel == 4 * kFactorThreads, "four staged entries per thread");
 #pragma unroll
     for (int u = 0; u < 4; ++u) {  // by columns (coalesced), four loads in flight
         const int q = threadIdx.x + u * kFactorThreads, i = q % kFacPanel, j = q / kFacPanel;
-        L[i * kDiagStride + j] = (i < bw && j <= i) ? A[(k0 + i) + (long long)(k0 + j) * n] : 0.0;
+        L[i * kDiagStride + j] = j <= i ? A[(k0 + i) + (long long)(k0 + j) * n] : 0.0;
     }
-    if (threadIdx.x < bw) {
+    if (threadIdx.x < kFacPanel) {
         y1[threadIdx.x] = x[k0 + threadIdx.x];
         inv[threadIdx.x] = 1.0 / A[(k0 + threadIdx.x) + (long long)(k0 + threadIdx.x) * n];
     }
     __syncthreads();
-    const int r = r0 + threadIdx.x;
-    if (r >= n) return;
-    double a[kFacPanel];
-#pragma unroll
-    for (int c = 0; c < kFacPanel; ++c) a[c] = c < bw ? A[r + (long long)(k0 + c) * n] : 0.0;
-    double y = 0;
-#pragma unroll
-    for (int c = 0; c < kFacPanel; ++c) {
-        if (c < bw) {
-            double s0 = a[c], s1 = 0;
-#pragma unroll
-            for (int k = 0; k < c; k += 2) {
-                s0 -= a[k] * L[c * kDiagStride + k];
-                if (k + 1 < c) s1 -= a[k + 1] * L[c * kDiagStride + k + 1];
-            }
-            a[c] = (s0 + s1) * inv[c];
-            A[r + (long long)(k0 + c) * n] = a[c];
-            y += a[c] * y1[c];
-        }
-    }
-    x[r] -= y;
-}
-
-// trailingTile for a full panel (bw = kFacPanel, every trailing update of the wide
-// sequence): the eight k-steps' operands are loaded before the first MMA, so the warp
-// waits for one round of L2 loads instead of eight; the MMAs and their order are
-// trailingTile's.
-__device__ __forceinline__ void trailingTileFull(const double* V, long long ldv, int rb, int cb, int m2, double* A, int n, int k0) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, kr = lane & 3;
-    double a[kFacPanel / 4][4], b[kFacPanel / 4][4];
-#pragma unroll
-    for (int st = 0; st < kFacPanel / 4; ++st) {
-        const double* row = V + (long long)(4 * st + kr) * ldv;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            a[st][q] = row[rb * 32 + 8 * q + g];
-            b[st][q] = row[cb * 32 + 8 * q + g];
-        }
-    }
-    double acc[4][8];
-    zeroTile(acc);
-#pragma unroll
-    for (int st = 0; st < kFacPanel / 4; ++st)
-#pragma unroll
-        for (int I = 0; I < 4; ++I)
-#pragma unroll
-            for (int J = 0; J < 4; ++J) mmaF64Tile(acc[I][2 * J], acc[I][2 * J + 1], a[st][I], b[st][J]);
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-        const int i = tileRowMma(rb, lane, r);
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const int j = tileCol(cb, lane, c);
-            if (i < m2 && j < m2 && i >= j) A[(k0 + kFacPanel + i) + (long long)(k0 + kFacPanel + j) * n] -= acc[r][c];
-        }
-    }
-}
-
-__global__ void __launch_bounds__(kFactorThreads) k_wide_trailing(DevBatch B, int k0) {
-    const int wdx = B.wideList[blockIdx.x];
-    if (B.lm[wdx].mode == kModeDone) return;
-    const WinDesc wd = B.win[wdx];
-    const int n = wd.Nr;
-    if (k0 >= n || B.facFailed[wdx]) return;
-    const int bw = min(kFacPanel, n - k0), m2 = n - k0 - bw;
-    const int nb2 = (m2 + 31) >> 5, tiles = nb2 * (nb2 + 1) / 2;
-    const int t = blockIdx.y * (kFactorThreads / 32) + (threadIdx.x >> 5);
-    if (m2 <= 0) return;  // uniform over the CTA
-    double* A = B.Sglob + wd.dense0;
     if (t < tiles) {
         int cb, rb;
         tileOf(t, nb2, cb, rb);
-        // L21 column k = A's column k0 + k from row k0 + bw; rows past n (padding of the
-        // last tile) read the next column's top, inside the slot, and only reach masked entries
-        if (bw == kFacPanel) trailingTileFull(A + (k0 + bw) + (long long)k0 * n, n, rb, cb, m2, A, n, k0);
-        else trailingTile(A + (k0 + bw) + (long long)k0 * n, n, rb, cb, bw, m2, A, n, k0);
+        double* Lcur = wideL21(B, blockIdx.x, panel, wideCols);
+        for (int h = 0; h < (rb == cb ? 1 : 2); ++h) {  // the row blocks rb, then cb
+            const int blk = h == 0 ? rb : cb, rl = blk * 32 + lane, r = k0 + kFacPanel + rl;
+            double a[kFacPanel];
+#pragma unroll
+            for (int c = 0; c < kFacPanel; ++c) a[c] = r < n ? A[r + (long long)(k0 + c) * n] : 0.0;
+            double y = 0;
+#pragma unroll
+            for (int c = 0; c < kFacPanel; ++c) {
+                double s0 = a[c], s1 = 0;
+#pragma unroll
+                for (int k = 0; k < c; k += 2) {
+                    s0 -= a[k] * L[c * kDiagStride + k];
+                    if (k + 1 < c) s1 -= a[k + 1] * L[c * kDiagStride + k + 1];
+                }
+                a[c] = (s0 + s1) * inv[c];
+                y += a[c] * y1[c];
+                Vs[c * kUpdStride + 32 * h + lane] = a[c];
+            }
+            if (rb == cb && r < n) {  // this block's owner: L21 to the panel buffer, y2 -= L21 y1
+#pragma unroll
+                for (int c = 0; c < kFacPanel; ++c) Lcur[(size_t)c * wideCols + rl] = a[c];
+                x[r] -= y;
+            }
+        }
+        __syncwarp();
+        // the tile from the staged blocks (trailingTileFull's operands and MMA order)
+        const int g = lane >> 2, kr = lane & 3, cOff = rb == cb ? 0 : 32;
+        double av[kFacPanel / 4][4], bv[kFacPanel / 4][4];
+#pragma unroll
+        for (int st = 0; st < kFacPanel / 4; ++st) {
+            const double* row = Vs + (4 * st + kr) * kUpdStride;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                av[st][q] = row[8 * q + g];
+                bv[st][q] = row[cOff + 8 * q + g];
+            }
+        }
+        double acc[4][8];
+        zeroTile(acc);
+#pragma unroll
+        for (int st = 0; st < kFacPanel / 4; ++st)
+#pragma unroll
+            for (int I = 0; I < 4; ++I)
+#pragma unroll
+                for (int J = 0; J < 4; ++J) mmaF64Tile(acc[I][2 * J], acc[I][2 * J + 1], av[st][I], bv[st][J]);
+#pragma unroll
+        for (int rr = 0; rr < 4; ++rr) {
+            const int i = tileRowMma(rb, lane, rr);
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                const int j = tileCol(cb, lane, c);
+                if (i < m2 && j < m2 && i >= j) A[(k0 + kFacPanel + i) + (long long)(k0 + kFacPanel + j) * n] -= acc[rr][c];
+            }
+        }
     }
     if (blockIdx.y == 0) {  // tile (0, 0), this CTA's first, is the next panel's diagonal block
         __syncthreads();
-        if (!wideDiagBlock(B, wd, k0 + bw) && threadIdx.x == 0) B.facFailed[wdx] = 1;
+        if (!wideDiagBlock(B, wd, k0 + kFacPanel) && threadIdx.x == 0) B.facFailed[wdx] = 1;
     }
 }
 
-__global__ void __launch_bounds__(kFactorThreads) k_wide_finish(DevBatch B, int refinement) {
+__global__ void __launch_bounds__(kFactorThreads) k_wide_finish(DevBatch B, int refinement, int wideCols) {
     const int wdx = B.wideList[blockIdx.x];
     if (B.lm[wdx].mode == kModeDone) return;
     const WinDesc wd = B.win[wdx];
@@ -1540,6 +1556,8 @@ __global__ void __launch_bounds__(kFactorThreads) k_wide_finish(DevBatch B, int 
         if (threadIdx.x == 0) B.solveStatus[wdx] = CGMLI_E_NOT_PD;
         return;
     }
+    if (n > kFacPanel)  // the last panel's L21 (the earlier ones reached A in the later panels' launches)
+        wideStoreL21(B, wd, blockIdx.x, (n - kFacPanel - 1) / kFacPanel, wideCols, threadIdx.x, blockDim.x);
     extern __shared__ __align__(16) double smem[];
     __shared__ double red[32];
     double* x = smem;
@@ -2138,6 +2156,11 @@ cudaError_t configureKernels(size_t linSmem, size_t facSmem, size_t wideSmem) {
     const size_t wideMax = (size_t)optin - wf.sharedSizeBytes;
     if (wideSmem > wideMax) return cudaErrorInvalidValue;
     if ((e = cudaFuncSetAttribute(k_wide_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wideMax)) != cudaSuccess) return e;
+    cudaFuncAttributes wu;
+    if ((e = cudaFuncGetAttributes(&wu, k_wide_update)) != cudaSuccess) return e;
+    if (wideUpdateSmemBytes() > (size_t)optin - wu.sharedSizeBytes) return cudaErrorInvalidValue;
+    if ((e = cudaFuncSetAttribute(k_wide_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wideUpdateSmemBytes())) != cudaSuccess)
+        return e;
     const size_t linMax = (size_t)optin - std::max(la.sharedSizeBytes, lm.sharedSizeBytes), facMax = (size_t)optin - fa.sharedSizeBytes;
     const size_t schMax = (size_t)optin - sa.sharedSizeBytes;
     const size_t pairMax = (size_t)optin - std::max(pa.sharedSizeBytes, pm.sharedSizeBytes);
@@ -2219,14 +2242,11 @@ int launchIterationParts(const DevBatch& B, const LaunchPlan& P, int refinement,
         if (P.wideCharts || Sdebug) run(CGMLI_KERNEL_FACTOR, [&] { k_wide_prepare<<<P.numWide, kFactorThreads, 0, s>>>(B, Sdebug); });
         run(CGMLI_KERNEL_FACTOR, [&] { k_wide_diag<<<P.numWide, kFactorThreads, 0, s>>>(B); });
         for (int k0 = 0; k0 + kFacPanel < P.wideCols; k0 += kFacPanel) {
-            const int m2 = P.wideCols - k0 - kFacPanel;
-            const dim3 rows(P.numWide, (m2 + kFactorThreads - 1) / kFactorThreads);
-            run(CGMLI_KERNEL_FACTOR, [&] { k_wide_trsm<<<rows, kFactorThreads, 0, s>>>(B, k0); });
-            const int nb2 = (m2 + 31) >> 5, tiles = nb2 * (nb2 + 1) / 2;
-            const dim3 grid(P.numWide, (tiles + kFactorThreads / 32 - 1) / (kFactorThreads / 32));
-            run(CGMLI_KERNEL_FACTOR, [&] { k_wide_trailing<<<grid, kFactorThreads, 0, s>>>(B, k0); });
+            const int m2 = P.wideCols - k0 - kFacPanel, nb2 = (m2 + 31) >> 5, tiles = nb2 * (nb2 + 1) / 2;
+            const dim3 grid(P.numWide, 1 + (tiles - 1 + kFactorThreads / 32 - 1) / (kFactorThreads / 32));
+            run(CGMLI_KERNEL_FACTOR, [&] { k_wide_update<<<grid, kFactorThreads, wideUpdateSmemBytes(), s>>>(B, k0, P.wideCols); });
         }
-        run(CGMLI_KERNEL_FACTOR, [&] { k_wide_finish<<<P.numWide, kFactorThreads, P.wideFinishSmem, s>>>(B, refinement); });
+        run(CGMLI_KERNEL_FACTOR, [&] { k_wide_finish<<<P.numWide, kFactorThreads, P.wideFinishSmem, s>>>(B, refinement, P.wideCols); });
         if (refinement == 0) {  // windows without charts: the product over the GPU, then the prediction
             const dim3 blocks(P.numWide, (P.wideCols + 31) / 32);
             run(CGMLI_KERNEL_FACTOR, [&] { k_wide_product<<<blocks, kFactorThreads, 0, s>>>(B, refinement, P.wideCols); });
