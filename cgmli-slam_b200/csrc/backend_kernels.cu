@@ -1491,16 +1491,20 @@ __global__ void __launch_bounds__(kFactorThreads) k_wide_update(DevBatch B, int 
             double a[kFacPanel];
 #pragma unroll
             for (int c = 0; c < kFacPanel; ++c) a[c] = r < n ? A[r + (long long)(k0 + c) * n] : 0.0;
+            // four partial sums per entry, so the chain from one entry to the next is
+            // about a quarter of its dot product
             double y = 0;
 #pragma unroll
             for (int c = 0; c < kFacPanel; ++c) {
-                double s0 = a[c], s1 = 0;
+                double s0 = a[c], s1 = 0, s2 = 0, s3 = 0;
 #pragma unroll
-                for (int k = 0; k < c; k += 2) {
+                for (int k = 0; k < c; k += 4) {
                     s0 -= a[k] * L[c * kDiagStride + k];
                     if (k + 1 < c) s1 -= a[k + 1] * L[c * kDiagStride + k + 1];
+                    if (k + 2 < c) s2 -= a[k + 2] * L[c * kDiagStride + k + 2];
+                    if (k + 3 < c) s3 -= a[k + 3] * L[c * kDiagStride + k + 3];
                 }
-                a[c] = (s0 + s1) * inv[c];
+                a[c] = ((s0 + s1) + (s2 + s3)) * inv[c];
                 y += a[c] * y1[c];
                 Vs[c * kUpdStride + 32 * h + lane] = a[c];
             }
