@@ -1456,15 +1456,43 @@ __global__ void __launch_bounds__(kFactorThreads) k_wide_update(DevBatch B, int 
     const WinDesc wd = B.win[wdx];
     const int n = wd.Nr, panel = k0 / kFacPanel;
     if (B.facFailed[wdx]) return;
-    if (panel > 0 && k0 < n)  // the previous panel's L21, spread over this launch's CTAs
-        wideStoreL21(B, wd, blockIdx.x, panel - 1, wideCols, blockIdx.y * blockDim.x + threadIdx.x, gridDim.y * blockDim.x);
-    if (k0 + kFacPanel >= n) return;  // uniform over the CTA
+    // the previous panel's L21 into the factor, off the first CTA's chain: by the other
+    // CTAs when there are any (after their tiles), else by the first after its work
+    const bool storeHere = panel > 0 && k0 < n && (gridDim.y == 1 || blockIdx.y > 0);
+    auto storePrevious = [&]() {
+        if (!storeHere) return;
+        const int helpers = gridDim.y == 1 ? 1 : gridDim.y - 1, rank = gridDim.y == 1 ? 0 : blockIdx.y - 1;
+        wideStoreL21(B, wd, blockIdx.x, panel - 1, wideCols, rank * blockDim.x + threadIdx.x, helpers * blockDim.x);
+    };
+    if (k0 + kFacPanel >= n) {  // uniform over the CTA
+        storePrevious();
+        return;
+    }
     const int m2 = n - k0 - kFacPanel, nb2 = (m2 + 31) >> 5, tiles = nb2 * (nb2 + 1) / 2;
     // the first CTA holds tile (0, 0) alone, so that the next diagonal block waits for
     // that tile only; the other CTAs hold eight tiles each
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int t = blockIdx.y == 0 ? (warp == 0 ? 0 : tiles) : 1 + (blockIdx.y - 1) * (kFactorThreads / 32) + warp;
-    if (blockIdx.y > 0 && 1 + (blockIdx.y - 1) * (kFactorThreads / 32) >= tiles) return;  // uniform over the CTA
+    if (blockIdx.y > 0 && 1 + (blockIdx.y - 1) * (kFactorThreads / 32) >= tiles) {  // uniform over the CTA
+        storePrevious();
+        return;
+    }
+    // the tile's current entries, loaded now so that their latency hides behind the
+    // staging and the row solves
+    int rb = 0, cb = 0;
+    if (t < tiles) tileOf(t, nb2, cb, rb);
+    double old[4][8];
+    if (t < tiles) {
+#pragma unroll
+        for (int rr = 0; rr < 4; ++rr) {
+            const int i = tileRowMma(rb, lane, rr);
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                const int j = tileCol(cb, lane, c);
+                old[rr][c] = (i < m2 && j < m2 && i >= j) ? B.Sglob[wd.dense0 + (k0 + kFacPanel + i) + (long long)(k0 + kFacPanel + j) * n] : 0.0;
+            }
+        }
+    }
     extern __shared__ __align__(16) double usm[];
     double* L = usm;                          // the diagonal block, row-major (stride kDiagStride)
     double* inv = L + kFacPanel * kDiagStride;
@@ -1483,8 +1511,6 @@ __global__ void __launch_bounds__(kFactorThreads) k_wide_update(DevBatch B, int 
     }
     __syncthreads();
     if (t < tiles) {
-        int cb, rb;
-        tileOf(t, nb2, cb, rb);
         double* Lcur = wideL21(B, blockIdx.x, panel, wideCols);
         for (int h = 0; h < (rb == cb ? 1 : 2); ++h) {  // the row blocks rb, then cb
             const int blk = h == 0 ? rb : cb, rl = blk * 32 + lane, r = k0 + kFacPanel + rl;
@@ -1541,7 +1567,7 @@ __global__ void __launch_bounds__(kFactorThreads) k_wide_update(DevBatch B, int 
 #pragma unroll
             for (int c = 0; c < 8; ++c) {
                 const int j = tileCol(cb, lane, c);
-                if (i < m2 && j < m2 && i >= j) A[(k0 + kFacPanel + i) + (long long)(k0 + kFacPanel + j) * n] -= acc[rr][c];
+                if (i < m2 && j < m2 && i >= j) A[(k0 + kFacPanel + i) + (long long)(k0 + kFacPanel + j) * n] = old[rr][c] - acc[rr][c];
             }
         }
     }
@@ -1549,6 +1575,7 @@ __global__ void __launch_bounds__(kFactorThreads) k_wide_update(DevBatch B, int 
         __syncthreads();
         if (!wideDiagBlock(B, wd, k0 + kFacPanel) && threadIdx.x == 0) B.facFailed[wdx] = 1;
     }
+    storePrevious();
 }
 
 __global__ void __launch_bounds__(kFactorThreads) k_wide_finish(DevBatch B, int refinement, int wideCols) {
