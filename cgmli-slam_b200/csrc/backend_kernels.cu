@@ -1326,8 +1326,9 @@ __global__ void __launch_bounds__(256) k_wide_assemble(DevBatch B) {
     double* hd = x + n;
     double* dmp = hd + n;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    // the rows of each column are split over gridDim.z CTAs (32-row strips, strided)
     for (int j = j0 + warp; j < min(n, j0 + 32); j += nw)
-        for (int i = j + lane; i < n; i += 32) {
+        for (int i = j + lane + 32 * (int)blockIdx.z; i < n; i += 32 * (int)gridDim.z) {
             const double v = assembleEntryCol(B, wd, i, j, lambda, false);
             if (i == j) {
                 hd[i] = v;
@@ -1337,7 +1338,7 @@ __global__ void __launch_bounds__(256) k_wide_assemble(DevBatch B) {
                 A[j + (long long)i * n] = v;
             }
         }
-    if (blockIdx.y == 0) {
+    if (blockIdx.y == 0 && blockIdx.z == 0) {
         double* rhsOut = B.rhs + wd.vec0;
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
             const double r = rhsOf(B, wd, i);
@@ -2269,7 +2270,7 @@ int launchIterationParts(const DevBatch& B, const LaunchPlan& P, int refinement,
     if (parts & kIterStep) {
     run(CGMLI_KERNEL_FACTOR, [&] { k_factor<<<W, kFactorThreads, P.facSmem, s>>>(B, refinement, Sdebug); });
     if (P.numWide > 0) {  // the wide sequence (windows of at least kWideCols columns)
-        run(CGMLI_KERNEL_FACTOR, [&] { k_wide_assemble<<<dim3(P.numWide, (P.wideCols + 31) / 32), 256, 0, s>>>(B); });
+        run(CGMLI_KERNEL_FACTOR, [&] { k_wide_assemble<<<dim3(P.numWide, (P.wideCols + 31) / 32, 4), 256, 0, s>>>(B); });
         if (P.wideCharts || Sdebug) run(CGMLI_KERNEL_FACTOR, [&] { k_wide_prepare<<<P.numWide, kFactorThreads, 0, s>>>(B, Sdebug); });
         run(CGMLI_KERNEL_FACTOR, [&] { k_wide_diag<<<P.numWide, kFactorThreads, 0, s>>>(B); });
         for (int k0 = 0; k0 + kFacPanel < P.wideCols; k0 += kFacPanel) {
