@@ -79,6 +79,18 @@ int cudaFail(cudaError_t e, const char* what) {
         if (e_ != cudaSuccess) return cudaFail(e_, #call);      \
     } while (0)
 
+// Stream the calling solver entry point works on, for stream-ordered growth of its
+// arrays (nullptr: plain cudaMalloc / cudaFree).  cudaFree waits for the whole
+// device, so a solver growing an array in one thread would stall behind another
+// solver's work; ordered on the solver's own stream, the old block is released
+// after the solver's earlier kernels and the new one is ready for its later ones.
+thread_local cudaStream_t tlsAllocStream = nullptr;
+struct AllocStreamScope {
+    cudaStream_t prev;
+    explicit AllocStreamScope(cudaStream_t s) : prev(tlsAllocStream) { tlsAllocStream = s; }
+    ~AllocStreamScope() { tlsAllocStream = prev; }
+};
+
 // Grow-only device array (src/common/CudaArray.hpp:10-39 keeps the same policy);
 // it grows by at least half its size, so batches of slowly rising size do not
 // reallocate at every call.
@@ -86,14 +98,20 @@ template <class T>
 struct DArray {
     T* p = nullptr;
     size_t cap = 0;
+    bool pooled = false;  // allocated stream-ordered (freed the same way)
     cudaError_t reserve(size_t n) {
         if (n <= cap) return cudaSuccess;
-        if (p) cudaFree(p);
-        p = nullptr;
+        free(tlsAllocStream);
         const size_t want = std::max<size_t>(std::max(n, cap + cap / 2), 1);
-        cap = 0;
-        const cudaError_t e = cudaMalloc(&p, want * sizeof(T));
+        cudaError_t e;
+        if (tlsAllocStream) {
+            e = cudaMallocAsync(reinterpret_cast<void**>(&p), want * sizeof(T), tlsAllocStream);
+            pooled = e == cudaSuccess;
+        } else {
+            e = cudaMalloc(&p, want * sizeof(T));
+        }
         if (e == cudaSuccess) cap = want;
+        else p = nullptr;
         return e;
     }
     template <class V>
@@ -102,7 +120,16 @@ struct DArray {
         if (e != cudaSuccess || v.empty()) return e;
         return cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
     }
-    void release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
+    void release() { free(nullptr); }
+    void free(cudaStream_t s) {
+        if (p) {
+            if (pooled && s) cudaFreeAsync(p, s);
+            else cudaFree(p);
+        }
+        p = nullptr;
+        cap = 0;
+        pooled = false;
+    }
 };
 }  // namespace
 
@@ -461,6 +488,7 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     if (!S || !windows || count < 1) return fail(CGMLI_E_INVALID, "null solver or empty window list");
     CK(cudaSetDevice(S->device));
     cudaStream_t st = S->stream;
+    const AllocStreamScope ordered(st);
     // the previous batch's uploads read the pinned host arrays that are rebuilt now
     CK(cudaStreamSynchronize(st));
     S->haveSnapshot = false;
@@ -1361,6 +1389,7 @@ int cgmli_solver_read_calibration_information(cgmli_solver* S, int window, int* 
 static int marginalizeImpl(cgmli_solver* S, const int* victim_kf, int policy, bool calib, bool includePrior) {
     const int W = (int)S->win.size();
     CK(cudaSetDevice(S->device));
+    const AllocStreamScope ordered(S->stream);
     // ---- phase A (parallel over windows): elimination set, columns, local maps
     struct Part {
         std::vector<MargElim> elims;   // col0 / obs0 window-local
