@@ -130,6 +130,7 @@ struct DevBatch {
 // (row <= column) of the m x m information, row-major.
 constexpr int kMargMaxNc = 200;     // marginalization columns touched by one eliminated landmark
 constexpr int kMargMaxSep = 1024;   // separator columns (Jacobi pair tables hold 512 pairs)
+constexpr int kPriorMaxCols = kMargMaxSep;  // tangent columns of a window's prior (what a marginalization forms)
 constexpr int kMargThreads = 512;   // victim CTAs
 constexpr int kEigenThreads = 512;  // eigen CTAs
 // Schur chunks of the linearization (k_lin_schur): rows x padded width of the

@@ -594,15 +594,24 @@ __global__ void __launch_bounds__(256, 2) k_retained(DevBatch B, int trial) {
         __syncthreads();
     }
     if (wd.priorRank > 0) {
-        const int rank = wd.priorRank, cols = wd.priorCols;
+        const int rank = wd.priorRank, cols = wd.priorCols;  // cols <= kPriorMaxCols (host check)
         double* ps = B.priorScratch + wd.priorScratch0;
         double* delta = ps;           // cols
         double* D = delta + cols;     // cols x 6
         double* r = D + 6ll * cols;   // rank
         double* J = r + rank;         // rank x cols
+        // per prior column: its retained column (-1: none) and its block's first column,
+        // negated minus one for a block whose tangent is its ambient (speed/bias, td)
+        __shared__ int pcol[kPriorMaxCols], poff[kPriorMaxCols];
         for (int b = threadIdx.x; b < wd.priorBlocks; b += blockDim.x) {
             const int pb = wd.priorBlk0 + b;
             const int kind = B.priorKind[pb], off = B.priorOff[pb];
+            const int width = kind == CGMLI_PRIOR_SPEED_BIAS ? 9 : kind == CGMLI_PRIOR_TIME_OFFSET ? 1 : 6, col = B.priorCol[pb];
+            const bool chart = kind == CGMLI_PRIOR_POSE || kind == CGMLI_PRIOR_EXTRINSIC;
+            for (int c = 0; c < width; ++c) {
+                pcol[off + c] = col < 0 ? -1 : col + c;
+                poff[off + c] = chart ? off : -1 - off;
+            }
             const double* x = blockValue(B, buf, kind, B.priorIndex[pb], wdx);
             // reference offset: ambient sizes accumulate in block order
             int aoff = 0;
@@ -632,38 +641,33 @@ __global__ void __launch_bounds__(256, 2) k_retained(DevBatch B, int trial) {
         if (!trial) {
             // J = A * blockdiag(D)
             for (long long e = threadIdx.x; e < (long long)rank * cols; e += blockDim.x) {
-                const int i = (int)(e / cols), c = (int)(e % cols);
-                // block of column c
-                int pb = wd.priorBlk0;
-                while (pb + 1 < wd.priorBlk0 + wd.priorBlocks && B.priorOff[pb + 1] <= c) ++pb;
-                const int kind = B.priorKind[pb], off = B.priorOff[pb];
+                const int i = (int)(e / cols), c = (int)(e % cols), po = poff[c];
                 double v;
-                if (kind == CGMLI_PRIOR_POSE || kind == CGMLI_PRIOR_EXTRINSIC) {
+                if (po >= 0) {
                     v = 0;
-                    for (int j = 0; j < 6; ++j) v += A[(long long)i * cols + off + j] * D[6ll * (off + j) + (c - off)];
+                    for (int j = 0; j < 6; ++j) v += A[(long long)i * cols + po + j] * D[6ll * (po + j) + (c - po)];
                 } else {
                     v = A[(long long)i * cols + c];
                 }
                 J[e] = v;
             }
             __syncthreads();
+            // J^T J on the upper triangle, written to both halves, and J^T r
             for (long long e = threadIdx.x; e < (long long)cols * (cols + 1); e += blockDim.x) {
                 const int p = (int)(e / cols), q = (int)(e % cols);
-                int bp = wd.priorBlk0, bq = wd.priorBlk0;
-                const int pp = p < cols ? p : q;
-                while (bp + 1 < wd.priorBlk0 + wd.priorBlocks && B.priorOff[bp + 1] <= pp) ++bp;
-                while (bq + 1 < wd.priorBlk0 + wd.priorBlocks && B.priorOff[bq + 1] <= q) ++bq;
-                const int colP = B.priorCol[bp], colQ = B.priorCol[bq];
                 if (p < cols) {
-                    if (colP < 0 || colQ < 0) continue;
+                    const int rp = pcol[p], rq = pcol[q];
+                    if (p > q || rp < 0 || rq < 0) continue;
                     double v = 0;
                     for (int i = 0; i < rank; ++i) v += J[(long long)i * cols + p] * J[(long long)i * cols + q];
-                    H[(long long)(colP + p - B.priorOff[bp]) * Nr + colQ + q - B.priorOff[bq]] += v;
+                    H[(long long)rp * Nr + rq] += v;
+                    if (p != q) H[(long long)rq * Nr + rp] += v;
                 } else {
-                    if (colQ < 0) continue;
+                    const int rq = pcol[q];
+                    if (rq < 0) continue;
                     double v = 0;
                     for (int i = 0; i < rank; ++i) v += J[(long long)i * cols + q] * r[i];
-                    g[colQ + q - B.priorOff[bq]] += v;
+                    g[rq] += v;
                 }
             }
         }

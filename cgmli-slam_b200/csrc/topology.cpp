@@ -125,11 +125,18 @@ int validateWindow(const cgmli_window& w, int index, std::string& why) {
     if (w.prior_rank > 0) {
         if (!w.prior_block_kind || !w.prior_block_index || !w.prior_ref || !w.prior_A || !w.prior_r0 || w.prior_num_blocks < 1)
             return bad("missing prior arrays");
+        int cols = 0;
         for (int b = 0; b < w.prior_num_blocks; ++b) {
             const int k = w.prior_block_kind[b], i = w.prior_block_index[b];
             if (k < 0 || k > 3) return bad("prior block kind");
             if ((k <= 1 && (i < 0 || i >= w.num_keyframes)) || (k == 2 && (i < 0 || i >= w.num_extrinsics)) || (k == 3 && !w.td))
                 return bad("prior block index");
+            cols += tangentOf(k);
+        }
+        if (cols > kPriorMaxCols) {
+            std::snprintf(buf, sizeof buf, "window %d: prior above 1024 tangent columns", index);
+            why = buf;
+            return CGMLI_E_LIMIT;
         }
     }
     if (w.kf_fixed)

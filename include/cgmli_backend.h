@@ -119,7 +119,7 @@ typedef struct cgmli_window {
     const int *prior_block_kind;  /* prior_num_blocks, CGMLI_PRIOR_* */
     const int *prior_block_index; /* prior_num_blocks */
     const double *prior_ref;    /* concatenated ambient references (7, 9, 7 or 1 per block) */
-    const double *prior_A;      /* prior_rank x (sum of tangent sizes), row-major */
+    const double *prior_A;      /* prior_rank x (sum of tangent sizes, at most 1024: CGMLI_E_LIMIT), row-major */
     const double *prior_r0;     /* prior_rank */
     /* Solve-time charts: blocks held constant and restricted tangents for the LM
      * solve only, as the reference sets them on its Ceres problem for one solve
