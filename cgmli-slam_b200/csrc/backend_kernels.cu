@@ -537,23 +537,25 @@ __global__ void __launch_bounds__(256, 2) k_retained(DevBatch B, int trial) {
     if (threadIdx.x == 0) bad = 0;
     double* H = B.Hret + wd.dense0;
     double* g = B.gret + wd.vec0;
+    // IMU factors: per factor 930 doubles of scratch, the raw error and Jacobian
+    // [e 15 | U 450] (one thread each, U cleared beforehand by the whole CTA), then the
+    // whitened [r 15 | J 450] = W [e | U] with one thread per output entry, which also
+    // finds a non-finite U (every entry of U enters one of those sums)
+    double* scratch = B.imuScratch + wd.imuScratch0;
     if (!trial) {
         for (long long i = threadIdx.x; i < (long long)Nr * Nr; i += blockDim.x) H[i] = 0.0;
         for (int i = threadIdx.x; i < Nr; i += blockDim.x) g[i] = 0.0;
+        for (int t = threadIdx.x; t < 450 * wd.nImu; t += blockDim.x) scratch[930ll * (t / 450) + 15 + t % 450] = 0.0;
     }
     __syncthreads();
     double cost = 0;
     const cgmli_frozen_imu* imus = reinterpret_cast<const cgmli_frozen_imu*>(B.imu);
-    // IMU factors: per factor 930 doubles of scratch, the raw error and Jacobian
-    // [e 15 | U 450] (one thread each), then the whitened [r 15 | J 450] = W [e | U]
-    // with one thread per output entry
-    double* scratch = B.imuScratch + wd.imuScratch0;
     for (int i = threadIdx.x; i < wd.nImu; i += blockDim.x) {
         const int gi = wd.imu0 + i;
         const int k = B.imuKf[gi];
         double* raw = scratch + 930ll * i;
         if (!evalImuRaw(imus[gi], B.pose[buf] + 7ll * k, B.sb[buf] + 9ll * k, B.pose[buf] + 7ll * (k + 1), B.sb[buf] + 9ll * (k + 1),
-                        raw, trial ? nullptr : raw + 15))
+                        raw, trial ? nullptr : raw + 15, true))
             atomicOr(&bad, 1);
     }
     __syncthreads();

@@ -57,8 +57,10 @@ __device__ inline Sensor sensorState(const cgmli_frozen_imu& imu, const double* 
     s.v = ld3(sb) + s.lever;
     return s;
 }
+// prepared: U is already zero (the caller cleared it in parallel) and the caller
+// checks U's finiteness itself (through every product it forms from U).
 __device__ inline bool evalImuRaw(const cgmli_frozen_imu& imu, const double* p0, const double* sb0, const double* p1,
-                                  const double* sb1, double* e, double* U) {
+                                  const double* sb1, double* e, double* U, bool prepared = false) {
     const Sensor s0 = sensorState(imu, p0, sb0, 0), s1 = sensorState(imu, p1, sb1, 1);
     const m3 A = colmajor(imu.rotation_gyro), V = colmajor(imu.velocity_gyro), P = colmajor(imu.position_gyro),
              Va = colmajor(imu.velocity_accel), Pa = colmajor(imu.position_accel);
@@ -89,7 +91,8 @@ __device__ inline bool evalImuRaw(const cgmli_frozen_imu& imu, const double* p0,
         Jrot.a[j] = c1.x; Jrot.a[3 + j] = c1.y; Jrot.a[6 + j] = c1.z;
         Jbias.a[j] = c2.x; Jbias.a[3 + j] = c2.y; Jbias.a[6 + j] = c2.z;
     }
-    for (int i = 0; i < 450; ++i) U[i] = 0;
+    if (!prepared)
+        for (int i = 0; i < 450; ++i) U[i] = 0;
     const int col0[4] = {0, 6, 15, 21};
     for (int k = 0; k < 4; ++k) {
         const bool first = k < 2;
@@ -127,8 +130,9 @@ __device__ inline bool evalImuRaw(const cgmli_frozen_imu& imu, const double* p0,
             }
         }
     }
-    for (int i = 0; i < 450; ++i)
-        if (!isfinite(U[i])) return false;
+    if (!prepared)
+        for (int i = 0; i < 450; ++i)
+            if (!isfinite(U[i])) return false;
     return true;
 }
 __device__ inline bool evalImu(const cgmli_frozen_imu& imu, const double* p0, const double* sb0, const double* p1, const double* sb1,
