@@ -458,14 +458,37 @@ __global__ void __launch_bounds__(256) k_marg_retained(DevBatch B, MargBatch M) 
     const int nImu = mw.imuAll ? wd.nImu : 2;
     auto factorAt = [&](int q) { return mw.imuAll ? (q < nImu ? wd.imu0 + q : -1) : mw.imu[q]; };
     for (int q0 = 0; q0 < nImu; q0 += 2) {
+        // the raw error and Jacobian of each factor by one thread (its Jacobian cleared
+        // first by the CTA), then the whitening W [e | U] in place, a thread per column
+        // (evalImu's products in its order); a non-finite U shows in those products
+        for (int t = threadIdx.x; t < 2 * 450; t += blockDim.x) sc[465 * (t / 450) + 15 + t % 450] = 0.0;
+        __syncthreads();
         if (threadIdx.x < 2 && factorAt(q0 + threadIdx.x) >= 0) {
             const int gi = factorAt(q0 + threadIdx.x), k = B.imuKf[gi];
-            double* r = sc + 465 * threadIdx.x;
-            if (!evalImu(imus[gi], B.pose[0] + 7ll * k, B.sb[0] + 9ll * k, B.pose[0] + 7ll * (k + 1), B.sb[0] + 9ll * (k + 1), r,
-                         r + 15))
+            double* raw = sc + 465 * threadIdx.x;
+            if (!evalImuRaw(imus[gi], B.pose[0] + 7ll * k, B.sb[0] + 9ll * k, B.pose[0] + 7ll * (k + 1), B.sb[0] + 9ll * (k + 1), raw,
+                            raw + 15, true))
                 bad = 1;
-            else
-                for (int i = 0; i < 15; ++i) cost += 0.5 * r[i] * r[i];
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < 2 * 31; t += blockDim.x) {
+            const int q = t / 31, c = t % 31;
+            if (factorAt(q0 + q) < 0) continue;
+            const double* W = imus[factorAt(q0 + q)].whitening;  // column-major 15 x 15
+            double* f = sc + 465 * q;
+            double u[15];
+            for (int mm = 0; mm < 15; ++mm) u[mm] = c < 30 ? f[15 + 30 * mm + c] : f[mm];
+            for (int i = 0; i < 15; ++i) {
+                double v = 0;
+                for (int mm = 0; mm < 15; ++mm) v += W[i + 15 * mm] * u[mm];
+                if (!isfinite(v)) bad = 1;
+                if (c < 30) {
+                    f[15 + 30 * i + c] = v;
+                } else {
+                    f[i] = v;
+                    cost += 0.5 * v * v;
+                }
+            }
         }
         __syncthreads();
         for (int q = 0; q < 2; ++q) {
@@ -495,15 +518,26 @@ __global__ void __launch_bounds__(256) k_marg_retained(DevBatch B, MargBatch M) 
         __syncthreads();  // the scratch is rewritten by the next pair
     }
     if (mw.hasPrior && wd.priorRank > 0 && !bad) {
-        const int rank = wd.priorRank, cols = wd.priorCols;
+        const int rank = wd.priorRank, cols = wd.priorCols;  // cols <= kPriorMaxCols (host check)
         double* ps = B.priorScratch + wd.priorScratch0;
         double* delta = ps;
         double* D = delta + cols;
         double* r = D + 6ll * cols;
         double* J = r + rank;
+        // per prior column: its marginalization column and its block's first column,
+        // negated minus one for a block whose tangent is its ambient (speed/bias, td)
+        __shared__ int mcol[kPriorMaxCols], poff[kPriorMaxCols];
         for (int bk = threadIdx.x; bk < wd.priorBlocks; bk += blockDim.x) {
             const int pb = wd.priorBlk0 + bk;
-            const int kind = B.priorKind[pb], off = B.priorOff[pb];
+            const int kind = B.priorKind[pb], off = B.priorOff[pb], gi = B.priorIndex[pb];
+            const int width = kind == CGMLI_PRIOR_SPEED_BIAS ? 9 : kind == CGMLI_PRIOR_TIME_OFFSET ? 1 : 6;
+            const int base = kind == CGMLI_PRIOR_POSE ? M.poseCol[gi] : kind == CGMLI_PRIOR_SPEED_BIAS ? M.sbCol[gi]
+                             : kind == CGMLI_PRIOR_EXTRINSIC ? M.extCol[gi] : mw.tdCol;
+            const bool chart = kind == CGMLI_PRIOR_POSE || kind == CGMLI_PRIOR_EXTRINSIC;
+            for (int c = 0; c < width; ++c) {
+                mcol[off + c] = base + c;
+                poff[off + c] = chart ? off : -1 - off;
+            }
             int aoff = 0;
             for (int q = wd.priorBlk0; q < pb; ++q) {
                 const int kq = B.priorKind[q];
@@ -529,37 +563,23 @@ __global__ void __launch_bounds__(256) k_marg_retained(DevBatch B, MargBatch M) 
             if (!isfinite(v)) bad = 1;
             cost += 0.5 * v * v;
         }
-        auto blockOf = [&](int c) {
-            int pb = wd.priorBlk0;
-            while (pb + 1 < wd.priorBlk0 + wd.priorBlocks && B.priorOff[pb + 1] <= c) ++pb;
-            return pb;
-        };
         for (long long e = threadIdx.x; e < (long long)rank * cols; e += blockDim.x) {
-            const int i = (int)(e / cols), c = (int)(e % cols);
-            const int pb = blockOf(c);
-            const int kind = B.priorKind[pb], off = B.priorOff[pb];
+            const int i = (int)(e / cols), c = (int)(e % cols), po = poff[c];
             double v;
-            if (kind == CGMLI_PRIOR_POSE || kind == CGMLI_PRIOR_EXTRINSIC) {
+            if (po >= 0) {
                 v = 0;
-                for (int j = 0; j < 6; ++j) v += A[(long long)i * cols + off + j] * D[6ll * (off + j) + (c - off)];
+                for (int j = 0; j < 6; ++j) v += A[(long long)i * cols + po + j] * D[6ll * (po + j) + (c - po)];
             } else {
                 v = A[(long long)i * cols + c];
             }
             J[e] = v;
         }
         __syncthreads();
-        auto colOf = [&](int c) {
-            const int pb = blockOf(c);
-            const int kind = B.priorKind[pb], gi = B.priorIndex[pb], off = B.priorOff[pb];
-            const int base = kind == CGMLI_PRIOR_POSE ? M.poseCol[gi] : kind == CGMLI_PRIOR_SPEED_BIAS ? M.sbCol[gi]
-                             : kind == CGMLI_PRIOR_EXTRINSIC ? M.extCol[gi] : mw.tdCol;
-            return base + (c - off);
-        };
         for (long long e = threadIdx.x; e < (long long)cols * (cols + 1); e += blockDim.x) {
             const int p = (int)(e / cols), q = (int)(e % cols);
-            const int cq = colOf(q);
+            const int cq = mcol[q];
             if (p < cols) {
-                const int cp = colOf(p);
+                const int cp = mcol[p];
                 if (cp > cq) continue;
                 double v = 0;
                 for (int i = 0; i < rank; ++i) v += J[(long long)i * cols + p] * J[(long long)i * cols + q];
