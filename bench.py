@@ -76,6 +76,7 @@ def parse():
     p.add_argument("--imu-rigs", type=int, default=512, help="rigs of the IMU preintegration batch, 11 keyframes each (0: off)")
     p.add_argument("--imu-cpu-sample", type=int, default=1024, help="intervals preintegrated by the oracle for its CPU rate")
     p.add_argument("--mixed-steps", type=int, default=10, help="timed solves of the batch in the other precision (0: off)")
+    p.add_argument("--det-steps", type=int, default=5, help="timed solves of the batch with deterministic sums (0: off)")
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                    help="precision of the headline solve, the end-to-end and the served rows (the batched configuration "
                         "states FP32 evaluation with FP64 reduced solves: mixed)")
@@ -530,6 +531,77 @@ def run_imu(args, local, backend):
     return out
 
 
+def run_deterministic(args, local, backend, windows, init, solver, dist):
+    """The batch with deterministic sums (cgmli_tuning.deterministic = 1): device time of
+    the same solve at the headline precision, its pair and Schur pass times, and what
+    it buys: two solves give the same bits, and the batch's first window solved alone
+    gives the same bits as inside the batch."""
+    prec = abi.PRECISION_MIXED if args.precision == "mixed" else abi.PRECISION_FP64
+    for w, x in zip(windows, init):
+        w.set_state_vector(x)
+    det = backend.Solver(device=local, precision=prec)
+    tuning = {k: v for k, v in solver.get_tuning().items() if k != "ms"}
+    det.set_tuning(**dict(tuning, deterministic=1))
+    det.set_windows(windows)
+    det.checkpoint()
+    for _ in range(max(3, args.warmup)):
+        det.rollback()
+        det.solve(args.iterations)
+        det.synchronize()
+    ms = []
+    for _ in range(args.det_steps):
+        det.rollback()
+        det.solve(args.iterations)
+        det.synchronize()
+        ms.append(det.timing()[0])
+    det.kernel_times(enable=1)
+    for _ in range(args.det_steps):
+        det.rollback()
+        det.solve(args.iterations)
+        det.synchronize()
+    kt = det.kernel_times(enable=-1)
+    det.kernel_times(enable=0)
+    total = max_over_ranks(sum(ms), dist)
+    runs = []
+    for _ in range(2):
+        det.rollback()
+        det.solve(args.iterations)
+        det.synchronize()
+        det.read_states()
+        runs.append([w.state_vector().copy() for w in windows])
+    repeat_bitwise = all(np.array_equal(a, b) for a, b in zip(*runs))
+    # the atomic form twice: its run-to-run drift is the scale of the difference
+    # between the two forms (the same arithmetic in another order of additions)
+    atomic = []
+    for _ in range(2):
+        solver.rollback()
+        solver.solve(args.iterations)
+        solver.synchronize()
+        solver.read_states()
+        atomic.append([w.state_vector().copy() for w in windows])
+
+    def worst(xs, ys):
+        return max(float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)) for a, b in zip(xs, ys))
+    det.close()
+    windows[0].set_state_vector(init[0])
+    alone = backend.Solver(device=local, precision=prec)
+    alone.set_tuning(**dict(tuning, deterministic=1))
+    alone.set_windows([windows[0]])
+    alone.solve(args.iterations)
+    alone.synchronize()
+    alone.read_states()
+    alone_bitwise = bool(np.array_equal(windows[0].state_vector(), runs[0][0]))
+    alone.close()
+    for w, x in zip(windows, init):
+        w.set_state_vector(x)
+    solver.rollback()
+    # lin_schur holds the Schur pass and the slot reduction (k_det_reduce)
+    per = {n: kt[n][0] / args.det_steps for n in ("lin_pairs", "lin_schur")}
+    return {"windows_per_s": args.windows * len(ms) / (total / 1e3), "ms_per_step": total / len(ms), "steps": len(ms),
+            "kernel_ms_per_step": per, "repeat_bitwise": repeat_bitwise, "alone_equals_batch_bitwise": alone_bitwise,
+            "state_rel_vs_atomic_max": worst(runs[0], atomic[0]), "atomic_repeat_state_rel_max": worst(atomic[1], atomic[0])}
+
+
 def run_mixed(args, local, backend, windows, init, solver, dist):
     """The batch in the other precision (FP64 when the headline is mixed): device time
     of the same solve, and the mixed form's accuracy against FP64 (first step dx of
@@ -850,6 +922,7 @@ def main():
     imu = run_imu(args, local, backend) if rank == 0 and args.imu_rigs > 0 else None
     gated = run_gated(args, local, backend, windows, init) if rank == 0 and args.gate_iterations > 0 else None
     mixed = run_mixed(args, local, backend, windows, init, solver, dist) if args.mixed_steps > 0 else None
+    deterministic = run_deterministic(args, local, backend, windows, init, solver, dist) if args.det_steps > 0 else None
 
     statuses = {}
     for r in reports:
@@ -898,7 +971,7 @@ def main():
             "cpu_baseline": cpu_baseline, "plain_path": plain,
             "served_vs_plain": (value / world) / plain["windows_per_s"] if plain else None,
             "served": served, "marginalization": marg, "configs": configs, "imu_preintegration": imu,
-            "nis_gate": gated, "calibration_information": calib, "other_precision": mixed,
+            "nis_gate": gated, "calibration_information": calib, "other_precision": mixed, "deterministic": deterministic,
             "batch_latency_ms": {"p50": sorted(dev_ms)[len(dev_ms) // 2], "p99": max(dev_ms)},
             "window_status": statuses, "wall_s": wall,
         }

@@ -52,7 +52,7 @@ class ImuParameters(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("run_landmarks", C.c_int), ("pair_chunk", C.c_int), ("schur_rows", C.c_int), ("lin_shape", C.c_int),
-                ("trial_shape", C.c_int), ("ms", C.c_double)]
+                ("trial_shape", C.c_int), ("deterministic", C.c_int), ("ms", C.c_double)]
 
 
 class GateReport(C.Structure):

@@ -159,16 +159,18 @@ class Solver:
         return nr.value, nl.value
 
     def set_tuning(self, run_landmarks: int = 0, pair_chunk: int = 0, schur_rows: int = 0, lin_shape: int = 0,
-                   trial_shape: int = 0) -> None:
-        """Work decomposition and kernel shapes of the next set_windows (0: the default of each)."""
-        t = abi.Tuning(run_landmarks, pair_chunk, schur_rows, lin_shape, trial_shape, 0.0)
+                   trial_shape: int = 0, deterministic: int = 0) -> None:
+        """Work decomposition and kernel shapes of the next set_windows (0: the default of each);
+        deterministic=1 sums the J^T J and Schur passes in a fixed order (bitwise-reproducible
+        windows, alone or in any batch)."""
+        t = abi.Tuning(run_landmarks, pair_chunk, schur_rows, lin_shape, trial_shape, deterministic, 0.0)
         _check(lib().cgmli_solver_set_tuning(self._h, C.byref(t)), "cgmli_solver_set_tuning")
 
     def get_tuning(self) -> dict:
         t = abi.Tuning()
         _check(lib().cgmli_solver_get_tuning(self._h, C.byref(t)), "cgmli_solver_get_tuning")
         return dict(run_landmarks=t.run_landmarks, pair_chunk=t.pair_chunk, schur_rows=t.schur_rows, lin_shape=t.lin_shape,
-                    trial_shape=t.trial_shape)
+                    trial_shape=t.trial_shape, deterministic=t.deterministic)
 
     def autotune(self, windows, iterations: int) -> dict:
         """Times candidate work decompositions on these windows, keeps the fastest
@@ -179,7 +181,7 @@ class Solver:
         self._windows = arr
         self.count = len(arr)
         return dict(run_landmarks=t.run_landmarks, pair_chunk=t.pair_chunk, schur_rows=t.schur_rows, lin_shape=t.lin_shape,
-                    trial_shape=t.trial_shape, ms=t.ms)
+                    trial_shape=t.trial_shape, deterministic=t.deterministic, ms=t.ms)
 
     def device_bytes(self) -> int:
         n = C.c_longlong()

@@ -169,7 +169,8 @@ struct cgmli_solver {
     DArray<WinLM> dLm;
     DArray<int4> dRuns;
     DArray<int2> dTiles;
-    DArray<int4> dPairChunks, dSchurChunks;
+    DArray<int4> dPairChunks, dSchurChunks, dDetPairs, dDetSchur;
+    DArray<double> detSlots;  // deterministic mode: per-unit partial sums
     DArray<int> schurCols;
     DArray<unsigned short> lmUmap;
     DArray<int> obLm, keyOrder, bigFirst;
@@ -292,6 +293,7 @@ struct cgmli_solver {
     long long deviceBytes() const {
         long long t = 0;
         auto add = [&](const auto&... a) { ((t += (long long)(a.cap * sizeof(*a.p))), ...); };
+        add(dDetPairs, dDetSchur, detSlots);
         add(dWin, dLm, dRuns, dTiles, dPairChunks, dSchurChunks, schurCols, lmUmap, obLm, keyOrder, bigFirst, keyRows, sch, camR, camT,
             camExt, lmWin, lmKf, lmCam, lmObsBegin, lmNs, lmNx, lmSupp0, supp, lmC0, lmBearing, lmVel, lmTime, lmC, lmD, lmG, lmCost,
             lmDelta, lmPred, lmTrial, lmMaxInc, lmValid, lmTrialValid, obKf, obCam, obSlot, obXslot, obBearing, obP, obVel, obTime,
@@ -313,6 +315,8 @@ struct cgmli_solver {
         P.runs = dRuns.p; P.tiles = dTiles.p; P.numTiles = (int)hb.tiles.size();
         P.pairChunks = dPairChunks.p; P.numPairChunks = (int)hb.pairChunks.size();
         P.schurChunks = dSchurChunks.p; P.numSchurChunks = (int)hb.schurChunks.size();
+        P.detPairs = dDetPairs.p; P.numDetPairs = (int)hb.detPairs.size();
+        P.detSchur = dDetSchur.p; P.numDetSchur = (int)hb.detSchur.size();
         P.facSmem = facSmem; P.maxNs = maxNs;
         P.linShape = hb.plan.linShape; P.trialShape = hb.plan.trialShape;
         P.numWide = numWide; P.wideCols = wideCols; P.wideCharts = wideCharts;
@@ -346,6 +350,7 @@ struct cgmli_solver {
                                &solveStatus, &lmNx, &obXslot, &obOrig};
         for (auto* a : ints) a->release();
         lmC0.release(); dWin.release(); dLm.release(); dRuns.release(); dTiles.release();
+        dDetPairs.release(); dDetSchur.release(); detSlots.release();
         dPairChunks.release(); dSchurChunks.release(); schurCols.release(); lmUmap.release(); obLm.release(); keyOrder.release(); bigFirst.release(); keyRows.release(); sch.release();
         snapPose.release(); snapSb.release(); snapExt.release(); snapTd.release(); snapRho.release();
         wideList.release(); facFailed.release(); facVec.release(); wideProd.release(); wideL21.release();
@@ -390,6 +395,8 @@ static int planOf(const cgmli_tuning* t, PlanParams& p) {
         return fail(CGMLI_E_INVALID, "tuning: schur_rows outside 8..128");
     if (t->lin_shape < 0 || t->lin_shape >= kLinShapes) return fail(CGMLI_E_INVALID, "tuning: lin_shape outside 0..3");
     if (t->trial_shape < 0 || t->trial_shape >= kTrialShapes) return fail(CGMLI_E_INVALID, "tuning: trial_shape outside 0..2");
+    if (t->deterministic != 0 && t->deterministic != 1) return fail(CGMLI_E_INVALID, "tuning: deterministic not 0 or 1");
+    p.deterministic = t->deterministic;
     p.linShape = t->lin_shape;
     p.trialShape = t->trial_shape;
     p.runLandmarks = t->run_landmarks;
@@ -442,6 +449,11 @@ int cgmli_topology_digest(const cgmli_window* windows, int count, int threads, c
     mix(hb.obBearing); mix(hb.obP); mix(hb.obVel); mix(hb.obTime); mix(hb.pose); mix(hb.sb); mix(hb.ext); mix(hb.td);
     mix(hb.rho); mix(hb.colChart); mix(hb.lmFixed); mix(hb.imu); mix(hb.imuKf); mix(hb.priorKind); mix(hb.priorIndex);
     mix(hb.priorCol); mix(hb.priorOff); mix(hb.priorA); mix(hb.priorR0); mix(hb.priorRef);
+    mix(hb.detPairs); mix(hb.detSchur);
+    for (const WinDesc& d : hb.win) {
+        const long long det[3] = {d.det0, d.detPairs, d.detSchur};
+        mix(std::vector<long long>(det, det + 3));
+    }
     *digest = h;
     return CGMLI_OK;
 }
@@ -578,6 +590,11 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     CK(S->dTiles.upload(hb.tiles, st));
     CK(S->dPairChunks.upload(hb.pairChunks, st));
     CK(S->dSchurChunks.upload(hb.schurChunks, st));
+    if (hb.plan.deterministic) {
+        CK(S->dDetPairs.upload(hb.detPairs, st));
+        CK(S->dDetSchur.upload(hb.detSchur, st));
+        CK(S->detSlots.reserve(hb.detSlots));
+    }
     CK(S->schurCols.upload(hb.schurCols, st));
     CK(S->lmUmap.upload(hb.lmUmap, st));
     CK(S->camR.upload(hb.camR, st)); CK(S->camT.upload(hb.camT, st)); CK(S->camExt.upload(hb.camExt, st));
@@ -649,6 +666,7 @@ int cgmli_solver_set_windows(cgmli_solver* S, const cgmli_window* windows, int c
     B.facFailed = S->numWide ? S->facFailed.p : nullptr;
     B.wideProd = S->numWide ? S->wideProd.p : nullptr;
     B.wideL21 = S->numWide ? S->wideL21.p : nullptr;
+    B.detSlots = hb.plan.deterministic ? S->detSlots.p : nullptr;
     {
         // the observation payload into device order (after every upload above on this stream)
         const double* const src[4] = {S->obSrcBearing.p, S->obSrcP.p, S->obSrcVel.p, S->obSrcTime.p};
@@ -782,6 +800,7 @@ int cgmli_solver_get_tuning(cgmli_solver* S, cgmli_tuning* tuning) {
     tuning->schur_rows = S->tune.schurRows;
     tuning->lin_shape = S->tune.linShape;
     tuning->trial_shape = S->tune.trialShape;
+    tuning->deterministic = S->tune.deterministic;
     tuning->ms = 0.0;
     return CGMLI_OK;
 }
@@ -861,6 +880,7 @@ int cgmli_solver_autotune(cgmli_solver* S, const cgmli_window* windows, int coun
         best->schur_rows = cur.schurRows;
         best->lin_shape = cur.linShape;
         best->trial_shape = cur.trialShape;
+        best->deterministic = cur.deterministic;
         best->ms = bestMs;
     }
     return CGMLI_OK;

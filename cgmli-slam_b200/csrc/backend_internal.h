@@ -42,6 +42,11 @@ struct WinDesc {
     double huber, minInv;
     int charts;   // 1: some retained column is fixed or on the rotation-only chart (colChart)
     int fixedLm;  // 1: some landmark's inverse distance is held constant (lmFixed)
+    // deterministic sums (cgmli_solver_options::deterministic): the window's slots in
+    // DevBatch::detSlots, each Npc(Npc+1)/2 + Npc doubles (packed upper triangle, then a
+    // vector): detPairs slots of J^T J and G_v, then detSchur slots of the Schur term and B_v
+    long long det0;
+    int detPairs, detSchur;
 };
 // Solve-time chart of a retained column (DevBatch::colChart).  A rotation-only
 // extrinsic keeps its translation: its tangent theta maps to the full left
@@ -120,6 +125,7 @@ struct DevBatch {
     // per wide window, two panel buffers (by panel parity) of 32 x wideCols: a panel's
     // solved L21 (k-major) until it is stored into Sglob
     double* wideL21;
+    double* detSlots;  // deterministic mode: per-unit partial sums (WinDesc::det0)
     double* out;     // per-window scratch for read-back (costs)
 };
 
@@ -138,6 +144,14 @@ constexpr int kEigenThreads = 512;  // eigen CTAs
 constexpr int kSchurThreads = 256;
 constexpr int kSchurSmemDoubles = 8192;
 constexpr int kSchurMaxRows = 128;
+// Deterministic mode: a window's pair chunks and its Schur chunks are split into
+// contiguous units, each summed into a slot of its own: about kDetUnitObs key-ordered
+// observations per pair unit and kDetSchurChunksPerUnit Schur chunks per Schur unit
+// (enough units to fill the GPU without a tail of long units from the largest windows),
+// at most kDetMaxSlots units of each kind per window (the slots' memory).
+constexpr int kDetMaxSlots = 128;
+constexpr int kDetUnitObs = 256;
+constexpr int kDetSchurChunksPerUnit = 2;
 inline bool schurChunkFits(int rows, int unionCols) {
     const int np = (unionCols + 1 + 31) / 32 * 32;
     return rows <= kSchurMaxRows && (long long)rows * np <= kSchurSmemDoubles;
@@ -236,6 +250,13 @@ struct LaunchPlan {
     int wideCols;            // largest wide Nr: panels and trailing tiles of the sequence
     int wideCharts;          // some wide window has solve-time charts
     size_t wideFinishSmem;
+    // deterministic mode (WinDesc::det0): pair units {window, first key-ordered position,
+    // end, slot} (one warp each) and Schur units {first Schur chunk, end chunk, slot,
+    // window} (one CTA each); 0 units: the atomic form
+    const int4* detPairs;
+    int numDetPairs;
+    const int4* detSchur;
+    int numDetSchur;
 };
 
 }  // namespace cgmli

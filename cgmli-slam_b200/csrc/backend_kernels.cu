@@ -325,21 +325,36 @@ __device__ __forceinline__ void mmaF64(double& d0, double& d1, double a, double 
                  : "d"(a), "d"(b));
 }
 
-template <bool Mixed>
+//
+// Det: the work unit is a deterministic unit {window, first position, end, slot}
+// (several consecutive chunks of one window); its sums go with plain adds into the
+// unit's own slot, which only this warp writes, and k_det_reduce adds a window's
+// slots in unit order.
+template <bool Mixed, bool Det>
 __global__ void __launch_bounds__(kPairWarps * 32) k_lin_pairs(DevBatch B, const int4* chunks, int numChunks) {
     extern __shared__ double smemRaw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ci = blockIdx.x * kPairWarps + warp;
     if (ci >= numChunks) return;
-    const int4 ch = chunks[ci];  // {window, first key-ordered position, end, -}
+    const int4 ch = chunks[ci];  // {window, first key-ordered position, end, - or slot}
     const int wdx = ch.x;
     if (B.lm[wdx].mode != kModeLinearize) return;
     double* rows = smemRaw + (size_t)warp * kPairRows * kPairStride;
     const WinDesc wd = B.win[wdx];
     const int K = wd.K, Npc = wd.Npc;
     const int tdCol = 6 * K + (wd.estExt ? 6 * wd.E : 0);
-    double* JJ = B.acc + wd.acc0;
-    double* Gv = JJ + (long long)Npc * (Npc + 1) / 2 + Npc;
+    const long long tri = (long long)Npc * (Npc + 1) / 2;
+    double* JJ;
+    double* Gv;
+    if constexpr (Det) {
+        JJ = B.detSlots + wd.det0 + (long long)ch.w * (tri + Npc);
+        Gv = JJ + tri;
+        for (long long e = lane; e < tri + Npc; e += 32) JJ[e] = 0.0;
+        __syncwarp();
+    } else {
+        JJ = B.acc + wd.acc0;
+        Gv = JJ + tri + Npc;
+    }
     // fragment coordinates: k-step row kr = lane % 4 (observation kr / 2, row kr % 2),
     // column lane / 4 within an 8-column block; accumulator row lane / 4, columns 2 (lane % 4) + {0, 1}
     const int kr = lane & 3, cIn = lane >> 2;
@@ -359,6 +374,31 @@ __global__ void __launch_bounds__(kPairWarps * 32) k_lin_pairs(DevBatch B, const
             if (c < 24) return (wd.estExt && split) ? 6 * K + 6 * xb + c - 18 : -1;
             return wd.estTd ? tdCol : -1;
         };
+        if constexpr (!Det) {
+            int t = 0;
+#pragma unroll
+            for (int I = 0; I < 4; ++I)
+#pragma unroll
+                for (int J = I; J < 4; ++J, ++t)
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        const int i = 8 * I + cIn, j = 8 * J + 2 * kr + e;
+                        const double v = g[t][e];
+                        g[t][e] = 0.0;
+                        if (v == 0.0 || i > j || i >= 25 || j > 25) continue;
+                        const int ci2 = colOf(i);
+                        if (ci2 < 0) continue;
+                        if (j == 25) { atomicAdd(&Gv[ci2], v); continue; }
+                        const int cj = colOf(j);
+                        if (cj < 0) continue;
+                        atomicAdd(&JJ[ci2 <= cj ? upIdx(ci2, cj, Npc) : upIdx(cj, ci2, Npc)], v);
+                    }
+            cur = -1;
+            return;
+        }
+        // Det: destination of each held entry (offset from the slot: G_v follows the
+        // triangle), -1: none
+        int off[10][2];
         int t = 0;
 #pragma unroll
         for (int I = 0; I < 4; ++I)
@@ -367,16 +407,32 @@ __global__ void __launch_bounds__(kPairWarps * 32) k_lin_pairs(DevBatch B, const
 #pragma unroll
                 for (int e = 0; e < 2; ++e) {
                     const int i = 8 * I + cIn, j = 8 * J + 2 * kr + e;
-                    const double v = g[t][e];
-                    g[t][e] = 0.0;
-                    if (v == 0.0 || i > j || i >= 25 || j > 25) continue;
+                    off[t][e] = -1;
+                    if (g[t][e] == 0.0 || i > j || i >= 25 || j > 25) continue;
                     const int ci2 = colOf(i);
                     if (ci2 < 0) continue;
-                    if (j == 25) { atomicAdd(&Gv[ci2], v); continue; }
-                    const int cj = colOf(j);
-                    if (cj < 0) continue;
-                    atomicAdd(&JJ[ci2 <= cj ? upIdx(ci2, cj, Npc) : upIdx(cj, ci2, Npc)], v);
+                    if (j == 25) {
+                        off[t][e] = (int)(Gv - JJ) + ci2;
+                    } else {
+                        const int cj = colOf(j);
+                        if (cj >= 0) off[t][e] = (int)(ci2 <= cj ? upIdx(ci2, cj, Npc) : upIdx(cj, ci2, Npc));
+                    }
                 }
+        // one run's entries land on distinct destinations (colOf is injective): every
+        // load is issued before any store, so they overlap
+        double old[10][2];
+#pragma unroll
+        for (int q = 0; q < 10; ++q)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) old[q][e] = off[q][e] >= 0 ? JJ[off[q][e]] : 0.0;
+#pragma unroll
+        for (int q = 0; q < 10; ++q)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                if (off[q][e] >= 0) JJ[off[q][e]] = old[q][e] + g[q][e];
+                g[q][e] = 0.0;
+            }
+        __syncwarp();  // the next run's adds may reach the same entries from other lanes
         cur = -1;
     };
     // the chunk is staged kPairRows rows at a time; a run of equal keys that
@@ -455,15 +511,11 @@ __global__ void __launch_bounds__(kPairWarps * 32) k_lin_pairs(DevBatch B, const
 // path (mma.sync m8n8k4, dense_tiles.cuh);
 // spare warps split the rows when the tiles are fewer than the warps.  Every
 // tile is added to the window's Schur sum once per chunk.
-__global__ void __launch_bounds__(kSchurThreads, 3) k_lin_schur(DevBatch B, const int4* chunks) {
-    extern __shared__ __align__(16) double Rw[];
-    const int4 ch = chunks[blockIdx.x];  // {window, first landmark, end landmark, offset of the column list}
-    const int wdx = ch.x;
-    const int mode = B.lm[wdx].mode;
-    if (mode == kModeDone) return;
-    const WinDesc wd = B.win[wdx];
-    const double lambda = B.lm[wdx].lambda;
-    const int Npc = wd.Npc;
+// One chunk into sch / Bv (the window's sums, or in Det mode the unit's slot: its
+// tiles' parts then add in a fixed order with plain adds).
+template <bool Det>
+__device__ __forceinline__ void schurChunk(const DevBatch& B, const int4 ch, const WinDesc& wd, double lambda, double* sch,
+                                           double* Bv, double* Rw) {
     const int nu = B.schurCols[ch.w];
     const int* U = B.schurCols + ch.w + 1;
     const int n = nu + 1, np = (n + 31) & ~31, nb = np >> 5, ntiles = nb * (nb + 1) / 2;
@@ -484,27 +536,136 @@ __global__ void __launch_bounds__(kSchurThreads, 3) k_lin_schur(DevBatch B, cons
         if (lane == 0) row[nu] = scale * B.lmG[l];
     }
     __syncthreads();
-    double* sch = B.sch + wd.sch0;
-    double* Bv = B.acc + wd.acc0 + (long long)Npc * (Npc + 1) / 2 + 2ll * Npc;
     const int wpt = ntiles < nw ? nw / ntiles : 1;  // warps per tile (row split)
-    for (int u = warp; u < ntiles * wpt; u += nw) {
-        const int t = u / wpt, part = u % wpt;
-        int bi, bj;
-        tileOf(t, nb, bi, bj);
-        double acc[4][8];
-        zeroTile(acc);
-        rankUpdateMma<false>(acc, Rw, bi * 32, bj * 32, part, rows, wpt, np);
+    auto addTile = [&](const double (&acc)[4][8], int bi, int bj) {
+        if constexpr (!Det) {
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const int i = tileRowMma(bi, lane, r);
+            for (int r = 0; r < 4; ++r) {
+                const int i = tileRowMma(bi, lane, r);
 #pragma unroll
-            for (int c = 0; c < 8; ++c) {
-                const int j = tileCol(bj, lane, c);
-                const double v = acc[r][c];
-                if (i > j || j >= n || i >= nu || v == 0.0) continue;
-                if (j < nu) atomicAdd(&sch[upIdx(U[i], U[j], Npc)], v);
-                else atomicAdd(&Bv[U[i]], v);
+                for (int c = 0; c < 8; ++c) {
+                    const int j = tileCol(bj, lane, c);
+                    const double v = acc[r][c];
+                    if (i > j || j >= n || i >= nu || v == 0.0) continue;
+                    atomicAdd(j < nu ? sch + upIdx(U[i], U[j], wd.Npc) : Bv + U[i], v);
+                }
             }
+        } else {
+            // a tile's entries land on distinct destinations: per half tile every load is
+            // issued before any store, so they overlap
+            const int bvOff = (int)(Bv - sch);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                int off[2][8];
+                double old[2][8];
+#pragma unroll
+                for (int r = 0; r < 2; ++r) {
+                    const int i = tileRowMma(bi, lane, 2 * h + r);
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) {
+                        const int j = tileCol(bj, lane, c);
+                        off[r][c] = (i > j || j >= n || i >= nu || acc[2 * h + r][c] == 0.0)
+                                        ? -1
+                                        : (j < nu ? (int)upIdx(U[i], U[j], wd.Npc) : bvOff + U[i]);
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < 2; ++r)
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) old[r][c] = off[r][c] >= 0 ? sch[off[r][c]] : 0.0;
+#pragma unroll
+                for (int r = 0; r < 2; ++r)
+#pragma unroll
+                    for (int c = 0; c < 8; ++c)
+                        if (off[r][c] >= 0) sch[off[r][c]] = old[r][c] + acc[2 * h + r][c];
+            }
+        }
+    };
+    if constexpr (!Det) {
+        for (int u = warp; u < ntiles * wpt; u += nw) {
+            const int t = u / wpt, part = u % wpt;
+            int bi, bj;
+            tileOf(t, nb, bi, bj);
+            double acc[4][8];
+            zeroTile(acc);
+            rankUpdateMma<false>(acc, Rw, bi * 32, bj * 32, part, rows, wpt, np);
+            addTile(acc, bi, bj);
+        }
+    } else {
+        // every warp runs the same rounds; a tile's parts (wpt > 1: one round, one part
+        // per warp) add in part order between barriers, distinct tiles never collide
+        for (int u0 = 0; u0 < ntiles * wpt; u0 += nw) {
+            const int u = u0 + warp;
+            const bool active = u < ntiles * wpt;
+            const int t = u / wpt, part = u % wpt;
+            int bi = 0, bj = 0;
+            double acc[4][8];
+            zeroTile(acc);
+            if (active) {
+                tileOf(t, nb, bi, bj);
+                rankUpdateMma<false>(acc, Rw, bi * 32, bj * 32, part, rows, wpt, np);
+            }
+            for (int p = 0; p < wpt; ++p) {
+                __syncthreads();
+                if (active && part == p) addTile(acc, bi, bj);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kSchurThreads, 3) k_lin_schur(DevBatch B, const int4* chunks) {
+    extern __shared__ __align__(16) double Rw[];
+    const int4 ch = chunks[blockIdx.x];  // {window, first landmark, end landmark, offset of the column list}
+    const int wdx = ch.x;
+    if (B.lm[wdx].mode == kModeDone) return;
+    const WinDesc wd = B.win[wdx];
+    const long long tri = (long long)wd.Npc * (wd.Npc + 1) / 2;
+    schurChunk<false>(B, ch, wd, B.lm[wdx].lambda, B.sch + wd.sch0, B.acc + wd.acc0 + tri + 2ll * wd.Npc, Rw);
+}
+
+// Deterministic Schur pass: a unit {first chunk, end chunk, slot, window} of one
+// window's consecutive chunks per CTA, summed in chunk order into the unit's slot.
+__global__ void __launch_bounds__(kSchurThreads, 2) k_lin_schur_det(DevBatch B, const int4* chunks, const int4* units) {
+    extern __shared__ __align__(16) double Rw[];
+    const int4 un = units[blockIdx.x];
+    const int wdx = un.w;
+    if (B.lm[wdx].mode == kModeDone) return;
+    const WinDesc wd = B.win[wdx];
+    const long long tri = (long long)wd.Npc * (wd.Npc + 1) / 2;
+    double* slot = B.detSlots + wd.det0 + (long long)(wd.detPairs + un.z) * (tri + wd.Npc);
+    for (long long e = threadIdx.x; e < tri + wd.Npc; e += blockDim.x) slot[e] = 0.0;
+    const double lambda = B.lm[wdx].lambda;
+    for (int c = un.x; c < un.y; ++c) {
+        __syncthreads();  // the slot is cleared / the previous chunk's rows and adds are done
+        schurChunk<true>(B, chunks[c], wd, lambda, slot, slot + tri, Rw);
+    }
+}
+
+// Deterministic mode: a window's sums from its units' slots, added in unit order
+// (J^T J and G_v of windows at a new point, the Schur term and B_v of every window
+// still iterating: the entries k_zero_acc cleared).
+__global__ void k_det_reduce(DevBatch B) {
+    const int w = blockIdx.x;
+    const int mode = B.lm[w].mode;
+    if (mode == kModeDone) return;
+    const WinDesc wd = B.win[w];
+    const int Npc = wd.Npc;
+    const long long tri = (long long)Npc * (Npc + 1) / 2, len = tri + Npc;
+    const double* slots = B.detSlots + wd.det0;
+    double* JJ = B.acc + wd.acc0;
+    double* sch = B.sch + wd.sch0;
+    for (long long e = (long long)blockIdx.y * blockDim.x + threadIdx.x; e < len; e += (long long)gridDim.y * blockDim.x) {
+        if (mode == kModeLinearize && wd.detPairs > 0) {
+            double v = 0.0;
+            for (int k = 0; k < wd.detPairs; ++k) v += slots[(long long)k * len + e];
+            if (e < tri) JJ[e] = v;
+            else JJ[tri + Npc + (e - tri)] = v;  // G_v
+        }
+        if (wd.detSchur > 0) {
+            double v = 0.0;
+            for (int k = 0; k < wd.detSchur; ++k) v += slots[(long long)(wd.detPairs + k) * len + e];
+            if (e < tri) sch[e] = v;
+            else JJ[tri + 2ll * Npc + (e - tri)] = v;  // B_v
         }
     }
 }
@@ -2182,13 +2343,14 @@ cudaError_t configureKernels(size_t linSmem, size_t facSmem, size_t wideSmem) {
     cudaError_t e = cudaGetDevice(&device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     if (e != cudaSuccess) return e;
-    cudaFuncAttributes la, lm, fa, sa, pa, pm;
+    cudaFuncAttributes la, lm, fa, sa, sd, pa, pm;
     if ((e = cudaFuncGetAttributes(&la, k_lin_landmark<false, 6, 2>)) != cudaSuccess) return e;
     if ((e = cudaFuncGetAttributes(&lm, k_lin_landmark<true, 6, 2>)) != cudaSuccess) return e;
-    if ((e = cudaFuncGetAttributes(&pa, k_lin_pairs<false>)) != cudaSuccess) return e;
-    if ((e = cudaFuncGetAttributes(&pm, k_lin_pairs<true>)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&pa, k_lin_pairs<false, false>)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&pm, k_lin_pairs<true, false>)) != cudaSuccess) return e;
     if ((e = cudaFuncGetAttributes(&fa, k_factor)) != cudaSuccess) return e;
     if ((e = cudaFuncGetAttributes(&sa, k_lin_schur)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&sd, k_lin_schur_det)) != cudaSuccess) return e;
     cudaFuncAttributes wf;
     if ((e = cudaFuncGetAttributes(&wf, k_wide_finish)) != cudaSuccess) return e;
     const size_t wideMax = (size_t)optin - wf.sharedSizeBytes;
@@ -2200,15 +2362,16 @@ cudaError_t configureKernels(size_t linSmem, size_t facSmem, size_t wideSmem) {
     if ((e = cudaFuncSetAttribute(k_wide_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wideUpdateSmemBytes())) != cudaSuccess)
         return e;
     const size_t linMax = (size_t)optin - std::max(la.sharedSizeBytes, lm.sharedSizeBytes), facMax = (size_t)optin - fa.sharedSizeBytes;
-    const size_t schMax = (size_t)optin - sa.sharedSizeBytes;
+    const size_t schMax = (size_t)optin - std::max(sa.sharedSizeBytes, sd.sharedSizeBytes);
     const size_t pairMax = (size_t)optin - std::max(pa.sharedSizeBytes, pm.sharedSizeBytes);
     if (linSmem > linMax || facSmem > facMax || schurSmemBytes() > schMax || pairCtaBytes() > pairMax) return cudaErrorInvalidValue;
-    for (auto k : {k_lin_pairs<false>, k_lin_pairs<true>})
+    for (auto k : {k_lin_pairs<false, false>, k_lin_pairs<true, false>, k_lin_pairs<false, true>, k_lin_pairs<true, true>})
         if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pairCtaBytes())) != cudaSuccess) return e;
     for (auto k : {k_lin_landmark<false, 6, 2>, k_lin_landmark<true, 6, 2>, k_lin_landmark<false, 8, 1>, k_lin_landmark<true, 8, 1>,
                    k_lin_landmark<false, 4, 3>, k_lin_landmark<true, 4, 3>, k_lin_landmark<false, 6, 1>, k_lin_landmark<true, 6, 1>})
         if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)linMax)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_lin_schur, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)schMax)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_lin_schur_det, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)schMax)) != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)facMax);
 }
 
@@ -2263,14 +2426,24 @@ int launchIterationParts(const DevBatch& B, const LaunchPlan& P, int refinement,
     if (parts & kIterLinearize) {
     run(CGMLI_KERNEL_ZERO, [&] { k_zero_acc<<<W, 256, 0, s>>>(B); });
     if (B.numRuns > 0) run(CGMLI_KERNEL_LINEARIZE, [&] { launchLinLandmark(B, P, s); });
+    const bool det = B.detSlots != nullptr;
     if (P.numPairChunks > 0)
         run(CGMLI_KERNEL_LIN_PAIRS, [&] {
-            const int blocks = (P.numPairChunks + kPairWarps - 1) / kPairWarps;
-            if (B.mixed) k_lin_pairs<true><<<blocks, kPairWarps * 32, pairCtaBytes(), s>>>(B, P.pairChunks, P.numPairChunks);
-            else k_lin_pairs<false><<<blocks, kPairWarps * 32, pairCtaBytes(), s>>>(B, P.pairChunks, P.numPairChunks);
+            const int4* units = det ? P.detPairs : P.pairChunks;
+            const int n = det ? P.numDetPairs : P.numPairChunks, blocks = (n + kPairWarps - 1) / kPairWarps;
+            const size_t smem = pairCtaBytes();
+            if (B.mixed && det) k_lin_pairs<true, true><<<blocks, kPairWarps * 32, smem, s>>>(B, units, n);
+            else if (B.mixed) k_lin_pairs<true, false><<<blocks, kPairWarps * 32, smem, s>>>(B, units, n);
+            else if (det) k_lin_pairs<false, true><<<blocks, kPairWarps * 32, smem, s>>>(B, units, n);
+            else k_lin_pairs<false, false><<<blocks, kPairWarps * 32, smem, s>>>(B, units, n);
         });
     if (P.numSchurChunks > 0)
-        run(CGMLI_KERNEL_LIN_SCHUR, [&] { k_lin_schur<<<P.numSchurChunks, kSchurThreads, schurSmemBytes(), s>>>(B, P.schurChunks); });
+        run(CGMLI_KERNEL_LIN_SCHUR, [&] {
+            if (det) k_lin_schur_det<<<P.numDetSchur, kSchurThreads, schurSmemBytes(), s>>>(B, P.schurChunks, P.detSchur);
+            else k_lin_schur<<<P.numSchurChunks, kSchurThreads, schurSmemBytes(), s>>>(B, P.schurChunks);
+        });
+    if (det && (P.numPairChunks > 0 || P.numSchurChunks > 0))
+        run(CGMLI_KERNEL_LIN_SCHUR, [&] { k_det_reduce<<<dim3(W, 4), 256, 0, s>>>(B); });
     run(CGMLI_KERNEL_RETAINED, [&] { k_retained<<<W, 256, 0, s>>>(B, 0); });
     }
     if (parts & kIterStep) {

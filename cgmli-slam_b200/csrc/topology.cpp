@@ -694,6 +694,43 @@ int buildHostBatch(const cgmli_window* windows, int count, int threads, HostBatc
         std::copy(P.schurCols.begin(), P.schurCols.end(), hb.schurCols.begin() + schurColBase[i]);
         std::copy(P.umap.get(), P.umap.get() + P.cross, hb.lmUmap.begin() + crossBase[i]);
     });
+    // ---- deterministic mode: each window's pair chunks and Schur chunks in contiguous
+    // units (kDetUnitObs observations, kDetSchurChunksPerUnit chunks; at most kDetMaxSlots
+    // of each), each with a slot of its own.  The units follow from the window alone, so
+    // a window's sums are the same alone and in any batch.
+    hb.detSlots = 0;
+    if (!plan.deterministic) {
+        sizeTo(hb.detPairs, 0);
+        sizeTo(hb.detSchur, 0);
+        return CGMLI_OK;
+    }
+    int nPairUnits = 0, nSchurUnits = 0;
+    for (int i = 0; i < count; ++i) {
+        WinDesc& d = hb.win[i];
+        const int np = pairBase[i + 1] - pairBase[i], ns = schurBase[i + 1] - schurBase[i];
+        d.detPairs = std::min({kDetMaxSlots, np, (d.F + kDetUnitObs - 1) / kDetUnitObs});
+        d.detSchur = std::min(kDetMaxSlots, (ns + kDetSchurChunksPerUnit - 1) / kDetSchurChunksPerUnit);
+        d.det0 = hb.detSlots;
+        hb.detSlots += (long long)(d.detPairs + d.detSchur) * ((long long)d.Npc * (d.Npc + 1) / 2 + d.Npc);
+        nPairUnits += d.detPairs;
+        nSchurUnits += d.detSchur;
+    }
+    sizeTo(hb.detPairs, nPairUnits);
+    sizeTo(hb.detSchur, nSchurUnits);
+    for (int i = 0, pu = 0, su = 0; i < count; ++i) {
+        const WinDesc& d = hb.win[i];
+        const int np = pairBase[i + 1] - pairBase[i], ns = schurBase[i + 1] - schurBase[i];
+        for (int g = 0; g < d.detPairs; ++g) {
+            const int c0 = pairBase[i] + (int)((long long)g * np / d.detPairs);
+            const int c1 = pairBase[i] + (int)((long long)(g + 1) * np / d.detPairs);
+            hb.detPairs[pu++] = make_int4(i, hb.pairChunks[c0].y, hb.pairChunks[c1 - 1].z, g);
+        }
+        for (int g = 0; g < d.detSchur; ++g) {
+            const int c0 = schurBase[i] + (int)((long long)g * ns / d.detSchur);
+            const int c1 = schurBase[i] + (int)((long long)(g + 1) * ns / d.detSchur);
+            hb.detSchur[su++] = make_int4(c0, c1, g, i);
+        }
+    }
     return CGMLI_OK;
 }
 
@@ -784,6 +821,35 @@ int checkHostBatch(const cgmli_window* windows, int count, const HostBatch& hb, 
     }
     for (int g = 0; g < hb.totalLm; ++g)
         if (schCover[g] != 1) return bad(-1, "Schur chunks do not cover every landmark once");
+    // deterministic units: a window's units tile its observations (pairs) and its Schur
+    // chunks in slot order, and the slots stay inside the slot array
+    if (hb.plan.deterministic) {
+        std::vector<int> nextObs(count), nextChunk(count), nextPair(count, 0), nextSchur(count, 0);
+        for (int i = 0; i < count; ++i) nextObs[i] = hb.win[i].obs0;
+        for (int c = 0; c < (int)hb.schurChunks.size(); ++c)
+            if (c == 0 || hb.schurChunks[c - 1].x != hb.schurChunks[c].x) nextChunk[hb.schurChunks[c].x] = c;
+        for (const int4& u : hb.detPairs) {
+            if (u.x < 0 || u.x >= count || u.w != nextPair[u.x] || u.y != nextObs[u.x] || u.z <= u.y) return bad(u.x, "pair unit");
+            ++nextPair[u.x];
+            nextObs[u.x] = u.z;
+        }
+        for (const int4& u : hb.detSchur) {
+            if (u.w < 0 || u.w >= count || u.z != nextSchur[u.w] || u.x != nextChunk[u.w] || u.y <= u.x ||
+                u.y > (int)hb.schurChunks.size() || hb.schurChunks[u.y - 1].x != u.w)
+                return bad(u.w, "Schur unit");
+            ++nextSchur[u.w];
+            nextChunk[u.w] = u.y;
+        }
+        long long slots = 0;
+        for (int i = 0; i < count; ++i) {
+            const WinDesc& d = hb.win[i];
+            if (nextPair[i] != d.detPairs || nextSchur[i] != d.detSchur || d.detPairs > kDetMaxSlots ||
+                d.detSchur > kDetMaxSlots || (d.F > 0 && nextObs[i] != d.obs0 + d.F) || d.det0 != slots)
+                return bad(i, "deterministic units do not cover the window");
+            slots += (long long)(d.detPairs + d.detSchur) * ((long long)d.Npc * (d.Npc + 1) / 2 + d.Npc);
+        }
+        if (slots != hb.detSlots) return bad(-1, "deterministic slot array size");
+    }
     return CGMLI_OK;
 }
 

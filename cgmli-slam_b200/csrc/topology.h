@@ -164,6 +164,7 @@ struct PlanParams {
     int schurRows = kSchurMaxRows;
     int linShape = 0;      // kLinShapeTable entry of the landmark pass
     int trialShape = 0;    // kTrialShapeTable entry of the trial pass
+    int deterministic = 0; // 1: per-unit slots of the visual sums (WinDesc::det0)
 };
 
 struct HostBatch {
@@ -173,6 +174,9 @@ struct HostBatch {
     HVec<int2> tiles;        // {first landmark, end landmark}
     HVec<int4> pairChunks;   // {window, first key-ordered position, end, -}
     HVec<int4> schurChunks;  // {window, first landmark, end landmark, offset in schurCols}
+    HVec<int4> detPairs;     // deterministic mode: {window, first key-ordered position, end, slot}
+    HVec<int4> detSchur;     // deterministic mode: {first Schur chunk, end chunk, slot, window}
+    long long detSlots = 0;  // doubles of all windows' slots
     HVec<int> schurCols;     // per Schur chunk: count, then the ascending visual columns of its landmarks
     HVec<unsigned short> lmUmap;  // per cross-vector entry: position of its column in the chunk's list
     HVec<int> lmPerm;        // device landmark -> landmark index within its window

@@ -190,6 +190,15 @@ typedef struct cgmli_tuning {
     int lin_shape;      /* landmark pass: 0: 6 warps x 2 CTAs per SM (168 registers), 1: 8 x 1 (255),
                            2: 4 x 3 (168), 3: 6 x 1 (255) */
     int trial_shape;    /* trial pass: 0: 8 warps x 2 CTAs per SM (128 registers), 1: 8 x 1 (255), 2: 4 x 4 (128) */
+    int deterministic;  /* 0: the J^T J and Schur passes add their work units into each window's
+                           sums with FP64 atomics (order of additions set by scheduling);
+                           1: each window's pair chunks and Schur chunks are split into
+                           contiguous units (about 256 observations, 2 Schur chunks; at most
+                           128 of each), every unit sums into a slot of its own and
+                           one reduction adds a window's slots in unit order, so that a window's
+                           result is bitwise the same alone, in any batch, and eager or as a
+                           graph (the reference sums with FP64 atomics,
+                           src/backend/VisualCudaBatch.cu:85-93).  The autotuner keeps it. */
     double ms;          /* cgmli_solver_autotune: device time of the timed solve */
 } cgmli_tuning;
 /* cgmli_topology_check with a given work decomposition (NULL: the default). */

@@ -326,7 +326,8 @@ def test_tuning_keeps_the_step(backend):
         s = backend.Solver()
         s.set_tuning(*tuning)
         s.set_windows(windows)
-        assert s.get_tuning() == dict(zip(("run_landmarks", "pair_chunk", "schur_rows", "lin_shape", "trial_shape"), tuning))
+        assert s.get_tuning() == dict(zip(("run_landmarks", "pair_chunk", "schur_rows", "lin_shape", "trial_shape"), tuning),
+                                      deterministic=0)
         s.step(1e-4)
         for i in range(len(windows)):
             a, b = s.read_step(i), ref.read_step(i)
@@ -341,7 +342,8 @@ def test_autotune(backend):
     assert best["ms"] > 0 and best["run_landmarks"] >= 2
     assert 8 <= best["pair_chunk"] <= 1024 and 8 <= best["schur_rows"] <= 128
     assert 0 <= best["lin_shape"] <= 3 and 0 <= best["trial_shape"] <= 2
-    assert s.get_tuning() == {k: best[k] for k in ("run_landmarks", "pair_chunk", "schur_rows", "lin_shape", "trial_shape")}
+    assert s.get_tuning() == {k: best[k] for k in ("run_landmarks", "pair_chunk", "schur_rows", "lin_shape", "trial_shape",
+                                                   "deterministic")}
     # the batch is left set with the chosen decomposition and the given states
     ref = backend.Solver()
     ref.set_windows(windows)

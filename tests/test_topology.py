@@ -75,11 +75,13 @@ def test_window_above_visual_limit_is_rejected(lib):
     assert code == 9  # CGMLI_E_LIMIT
 
 
-@pytest.mark.parametrize("tuning", [(2, 8, 8, 0, 0), (8, 64, 32, 1, 2), (64, 1024, 128, 3, 1), (0, 0, 0, 2, 0), (4096, 128, 16, 0, 0)])
+@pytest.mark.parametrize("tuning", [(2, 8, 8, 0, 0, 0), (8, 64, 32, 1, 2, 0), (64, 1024, 128, 3, 1, 0), (0, 0, 0, 2, 0, 0),
+                                    (4096, 128, 16, 0, 0, 0), (0, 0, 0, 0, 0, 1), (2, 8, 8, 0, 0, 1), (64, 1024, 128, 3, 1, 1)])
 def test_tuned_layout(lib, tuning):
     """Every work decomposition the autotuner may pick keeps the invariants
     (runs cover each landmark once, pair chunks and Schur chunks within their
-    limits and windows)."""
+    limits and windows; in deterministic mode the units tile each window's chunks
+    in slot order and the slots fill the slot array)."""
     windows = synth.make_windows("c4", 12, seed=17)
     arr = synth.window_array(windows)
     t = abi.Tuning(*tuning, 0.0)
@@ -87,8 +89,9 @@ def test_tuned_layout(lib, tuning):
     assert code == 0, lib.cgmli_last_error().decode()
 
 
-@pytest.mark.parametrize("tuning", [(-1, 32, 128, 0, 0), (0, 4, 128, 0, 0), (0, 2048, 128, 0, 0), (0, 32, 4, 0, 0), (0, 32, 256, 0, 0),
-                                    (0, 32, 128, 4, 0), (0, 32, 128, 0, 3), (0, 32, 128, -1, 0)])
+@pytest.mark.parametrize("tuning", [(-1, 32, 128, 0, 0, 0), (0, 4, 128, 0, 0, 0), (0, 2048, 128, 0, 0, 0), (0, 32, 4, 0, 0, 0),
+                                    (0, 32, 256, 0, 0, 0), (0, 32, 128, 4, 0, 0), (0, 32, 128, 0, 3, 0), (0, 32, 128, -1, 0, 0),
+                                    (0, 32, 128, 0, 0, 2), (0, 32, 128, 0, 0, -1)])
 def test_tuning_outside_its_ranges_is_rejected(lib, tuning):
     windows = synth.make_windows("c4", 2, seed=3)
     arr = synth.window_array(windows)
@@ -122,6 +125,21 @@ def test_layout_is_the_same_for_any_thread_count(lib):
 
 def test_layout_digest_sees_the_decomposition(lib):
     windows = synth.make_windows("c4", 6, seed=29)
-    a = _digest(lib, windows, 2, abi.Tuning(8, 32, 128, 0, 0, 0.0))
-    b = _digest(lib, windows, 2, abi.Tuning(16, 32, 128, 0, 0, 0.0))
-    assert a != b
+    a = _digest(lib, windows, 2, abi.Tuning(8, 32, 128, 0, 0, 0, 0.0))
+    b = _digest(lib, windows, 2, abi.Tuning(16, 32, 128, 0, 0, 0, 0.0))
+    c = _digest(lib, windows, 2, abi.Tuning(8, 32, 128, 0, 0, 1, 0.0))
+    assert len({a, b, c}) == 3
+
+
+def test_deterministic_units_follow_the_window_alone(lib):
+    """Deterministic mode splits each window's pair and Schur chunks into units by the
+    window alone (in chunk order, at most 128 of each): the layout is the same for any
+    thread count (range steps or whole windows) and keeps the unit invariants."""
+    det = abi.Tuning(0, 32, 128, 0, 0, 1, 0.0)
+    big = [synth.SynthWindow(replace(synth.C3, keyframes=14, landmarks=3000), 4),
+           synth.SynthWindow(replace(synth.C1, landmarks=300), 5)]
+    many = synth.make_windows("c4", 20, seed=23)
+    for windows in (big, many):
+        assert len({_digest(lib, windows, t, det) for t in (1, 2, 3, 8)}) == 1
+        arr = synth.window_array(windows)
+        assert lib.cgmli_topology_check_tuned(arr, len(arr), 3, C.byref(det), None) == 0, lib.cgmli_last_error().decode()
