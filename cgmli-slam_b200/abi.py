@@ -90,7 +90,7 @@ class ServerOptions(C.Structure):
                 ("iterations", C.c_int), ("policy", C.c_int), ("nis_threshold", C.c_double), ("max_refits", C.c_int),
                 ("pre_gate", C.c_int), ("precision", C.c_int), ("imu_params", ImuParameters),
                 ("imu_gyro_threshold", C.c_double), ("imu_accel_threshold", C.c_double),
-                ("calibration_include_prior", C.c_int)]
+                ("calibration_include_prior", C.c_int), ("deterministic", C.c_int)]
 
 
 class ServerRequest(C.Structure):

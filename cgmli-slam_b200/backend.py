@@ -372,8 +372,9 @@ class Server:
     def __init__(self, device: int = 0, iterations: int = 1, policy: int = abi.MARGIN_OLD, max_batch_windows: int = 512,
                  memory_budget_bytes: int = 40 << 30, nis_threshold: float = 0.0, max_refits: int = 3, pre_gate: bool = False,
                  precision: int = abi.PRECISION_FP64, imu_params=None, imu_gyro_threshold: float = 3e-4,
-                 imu_accel_threshold: float = 0.02, calibration_include_prior: bool = True):
+                 imu_accel_threshold: float = 0.02, calibration_include_prior: bool = True, deterministic: bool = False):
         opt = abi.ServerOptions()
+        opt.deterministic = int(deterministic)
         if imu_params is not None:
             opt.imu_params = imu_params
         opt.imu_gyro_threshold = imu_gyro_threshold

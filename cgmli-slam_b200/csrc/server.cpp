@@ -358,6 +358,8 @@ int cgmli_server_create(const cgmli_server_options* options, cgmli_server** out)
         return setLastError(CGMLI_E_INVALID, "server: negative or NaN IMU refresh threshold");
     if (options->precision != CGMLI_PRECISION_FP64 && options->precision != CGMLI_PRECISION_MIXED)
         return setLastError(CGMLI_E_INVALID, "server: unknown precision");
+    if (options->deterministic != 0 && options->deterministic != 1)
+        return setLastError(CGMLI_E_INVALID, "server: deterministic not 0 or 1");
     auto* s = new cgmli_server();
     s->opt = *options;
     if (s->opt.max_batch_windows <= 0) s->opt.max_batch_windows = 512;
@@ -366,7 +368,12 @@ int cgmli_server_create(const cgmli_server_options* options, cgmli_server** out)
     cgmli_default_options(&so);
     so.precision = options->precision;
     for (int k = 0; k < 2; ++k) {
-        const int st = cgmli_solver_create(options->device, &so, &s->solver[k]);
+        int st = cgmli_solver_create(options->device, &so, &s->solver[k]);
+        if (st == CGMLI_OK && options->deterministic) {
+            cgmli_tuning t{};
+            t.deterministic = 1;
+            st = cgmli_solver_set_tuning(s->solver[k], &t);
+        }
         if (st != CGMLI_OK) {
             for (auto* sv : s->solver) cgmli_solver_destroy(sv);
             delete s;

@@ -543,6 +543,10 @@ typedef struct cgmli_server_options {
     cgmli_imu_parameters imu_params;
     double imu_gyro_threshold, imu_accel_threshold;
     int calibration_include_prior;  /* requests for the calibration information: include the prior */
+    int deterministic;              /* 1: the solvers sum with cgmli_tuning.deterministic = 1, so a request's
+                                       solved states and report are bitwise those of its window solved
+                                       alone that way, whatever batch it joins (the marginal prior stays
+                                       at rounding level: the marginalization adds with atomics) */
 } cgmli_server_options;
 
 /* A served request with the optional parts of a backend step around the solve:

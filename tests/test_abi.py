@@ -60,16 +60,18 @@ def test_ctypes_layout_of_served_requests(tmp_path):
     """cgmli_server_request and the IMU / calibration tail of cgmli_server_options."""
     src = tmp_path / "sizes3.c"
     src.write_text(f'#include "{HEADER}"\n#include <stdio.h>\n#include <stddef.h>\n'
-                   "int main(){printf(\"%zu %zu %zu %zu %zu %zu\\n\", sizeof(cgmli_server_request),"
+                   "int main(){printf(\"%zu %zu %zu %zu %zu %zu %zu\\n\", sizeof(cgmli_server_request),"
                    " offsetof(cgmli_server_request, num_imu_samples), offsetof(cgmli_server_request, calibration_information),"
                    " offsetof(cgmli_server_options, imu_params), offsetof(cgmli_server_options, imu_accel_threshold),"
-                   " offsetof(cgmli_server_options, calibration_include_prior)); return 0;}\n")
+                   " offsetof(cgmli_server_options, calibration_include_prior), offsetof(cgmli_server_options, deterministic));"
+                   " return 0;}\n")
     exe = tmp_path / "sizes3"
     subprocess.run(["gcc", str(src), "-o", str(exe)], check=True)
     got = list(map(int, subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()))
     assert got == [C.sizeof(abi.ServerRequest), abi.ServerRequest.num_imu_samples.offset,
                    abi.ServerRequest.calibration_information.offset, abi.ServerOptions.imu_params.offset,
-                   abi.ServerOptions.imu_accel_threshold.offset, abi.ServerOptions.calibration_include_prior.offset]
+                   abi.ServerOptions.imu_accel_threshold.offset, abi.ServerOptions.calibration_include_prior.offset,
+                   abi.ServerOptions.deterministic.offset]
 
 
 def test_served_request_validation_without_gpu():
@@ -82,6 +84,15 @@ def test_served_request_validation_without_gpu():
     srv = C.c_void_p()
     assert lib.cgmli_server_create(C.byref(so), C.byref(srv)) == abi.E_INVALID and not srv.value
     assert b"threshold" in lib.cgmli_last_error()
+
+
+def test_server_deterministic_flag_is_validated_without_gpu():
+    lib = abi.declare_backend(C.CDLL(str(build_backend())))
+    so = abi.ServerOptions()
+    so.iterations, so.policy, so.max_refits, so.deterministic = 1, abi.MARGIN_OLD, 3, 2
+    srv = C.c_void_p()
+    assert lib.cgmli_server_create(C.byref(so), C.byref(srv)) == abi.E_INVALID and not srv.value
+    assert b"deterministic" in lib.cgmli_last_error()
 
 
 def test_unknown_precision_is_rejected_before_any_device_work():

@@ -68,6 +68,36 @@ def test_served_equals_alone(backend, budget, precision):
     server.close()
 
 
+def test_served_deterministic_equals_alone_bitwise(backend):
+    """With deterministic sums on both sides, every request's solved states and report
+    are bit for bit those of its window solved alone, whatever batches the scheduler
+    forms (batches of up to 4 windows here, mixed precision, 3 iterations)."""
+    n, iterations = 10, 3
+    alone_windows = synth.make_windows("c4", n, seed=654)
+    served_windows = synth.make_windows("c4", n, seed=654)
+    victims = [0 if i % 3 else -1 for i in range(n)]
+    ref = []
+    for w in alone_windows:
+        s = backend.Solver(precision=abi.PRECISION_MIXED)
+        s.set_tuning(deterministic=1)
+        s.set_windows([w])
+        s.solve(iterations)
+        s.synchronize()
+        s.read_states()
+        r = s.reports()[0]
+        ref.append((w.state_vector().copy(), (r.iterations, r.accepted_steps, r.status, r.final_cost)))
+        s.close()
+    server = backend.Server(iterations=iterations, policy=abi.MARGIN_OLD, max_batch_windows=4, precision=abi.PRECISION_MIXED,
+                            deterministic=True)
+    tickets = [server.submit(w, v) for w, v in zip(served_windows, victims)]
+    for i, t in enumerate(tickets):
+        rep, _ = server.poll(t, wait=True)
+        assert (rep.iterations, rep.accepted_steps, rep.status, rep.final_cost) == ref[i][1]
+        assert np.array_equal(served_windows[i].state_vector(), ref[i][0])
+        server.release(t)
+    server.close()
+
+
 def test_invalid_request_rejected_at_submit(backend):
     w = synth.SynthWindow(synth.C1, 4)
     arr = synth.window_array([w])
