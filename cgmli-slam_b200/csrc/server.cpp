@@ -9,6 +9,7 @@
 // callers' windows, records the reports and priors, and frees the solver.  The
 // host work of one batch therefore overlaps both the device work and the
 // read-back of the other, and requests arriving meanwhile join the next batch.
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstdio>
@@ -63,16 +64,23 @@ struct Request {
 
 // Device bytes a window occupies in a batch (observation arrays and the uploaded
 // payload they are gathered from, landmark and dense per-window arrays, both state
-// buffers, the staged rows and the marginalization).
+// buffers, the staged rows and the marginalization; with deterministic sums, the
+// slots of its pair units (about 256 observations each) and of its Schur units
+// (estimated at 64 landmarks each), at most 128 of each kind).
 // The solvers' device arrays are grow-only and grow by at least half their size,
 // so a batch whose windows need N bytes can leave a solver holding up to 1.5 N:
 // admission counts kGrowth times the footprint.
 constexpr double kGrowth = 1.5;
-long long footprint(const cgmli_window& w) {
+long long footprint(const cgmli_window& w, bool deterministic) {
     const long long F = w.num_observations, L = w.num_landmarks, K = w.num_keyframes;
     const long long ncal = (w.estimate_extrinsics ? 6ll * w.num_extrinsics : 0) + (w.estimate_td ? 1 : 0);
     const long long Nr = 15 * K + ncal, Npc = 6 * K + ncal, m = 15 * K + 6ll * w.num_extrinsics + 1;
-    return F * (120 + 108 + 448) + L * (160 + 8 * (6 * 12 + 7)) + 8 * (3 * Nr * Nr + Npc * Npc + 4 * m * m) + 4096;
+    long long bytes = F * (120 + 108 + 448) + L * (160 + 8 * (6 * 12 + 7)) + 8 * (3 * Nr * Nr + Npc * Npc + 4 * m * m) + 4096;
+    if (deterministic) {
+        const long long units = std::min(128ll, (F + 255) / 256) + std::min(128ll, L / 64 + 1);
+        bytes += 8 * units * (Npc * (Npc + 1) / 2 + Npc);
+    }
+    return bytes;
 }
 }  // namespace
 
@@ -283,7 +291,7 @@ struct cgmli_server {
                 if (busy[cur]) freed.wait(lock, [&] { return !busy[cur]; });  // stopping with queued requests
                 long long bytes = 0;
                 while (!queue.empty() && (int)next->reqs.size() < opt.max_batch_windows) {
-                    const long long f = (long long)(kGrowth * (double)footprint(queue.front()->window));
+                    const long long f = (long long)(kGrowth * (double)footprint(queue.front()->window, opt.deterministic != 0));
                     if (!next->reqs.empty() && bytes + f > perSolver) break;
                     bytes += f;
                     next->reqs.push_back(queue.front());
